@@ -1,0 +1,133 @@
+/* gamgpu.h -- C ABI of the B200 GAMERA MHD step.
+ *
+ * The entry points replace the CPU time step of the reference's GAMERA solver
+ * (Kaiju/MAGE, Fortran) for a single-domain grid. Fortran callers bind them
+ * with ISO_C_BINDING; Python binds them with ctypes.
+ *
+ * Conventions
+ *  - Every entry point returns an int status, GAM_OK (0) on success. On error
+ *    gam_last_error(h) returns a message; the handle stays usable.
+ *  - Host arrays are the reference's own Fortran arrays, passed by c_loc:
+ *    column-major, i fastest, including the nG = 4 ghost layers.
+ *      cell arrays  A(isg:ieg,   jsg:jeg,   ksg:keg,   1:nc)
+ *      face arrays  A(isg:ieg+1, jsg:jeg+1, ksg:keg+1, 1:nc)
+ *    with isg = 1-nG, ieg = Nip+nG (likewise j, k). No pointer is retained
+ *    past a call.
+ *  - One handle per host thread; calls on a handle are serialised on the
+ *    handle's CUDA stream. Handles are independent of each other.
+ */
+#ifndef GAMGPU_H
+#define GAMGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    GAM_OK = 0,
+    GAM_EINVAL = 1,        /* bad argument / unsupported option            */
+    GAM_EBADDIM = 2,       /* Nip%8 != 0 or Nip < 16 (init.F90:817-826)    */
+    GAM_ECUDA = 3,         /* CUDA runtime error                           */
+    GAM_EDT_BAD = 4,       /* dt dropped 10x or below limDT0 (step.F90:111-128) */
+    GAM_EDT_DISASTER = 5,  /* dt <= TINY or no finite dt (step.F90:102-105,131-134) */
+    GAM_ESTATE = 6,        /* call out of order (e.g. step before geometry) */
+    GAM_EHOOK = 7          /* a Model%Hack* hook is set: not supported on the GPU */
+};
+
+enum { GAM_BC_PERIODIC = 0, GAM_BC_NONE = 1 };
+enum { GAM_RECON_8CENT = 0, GAM_RECON_7UP = 1 };
+enum { GAM_FP64 = 0, GAM_FP32 = 1 };
+
+/* Model keys of the step. Defaults of the reference (init.F90:312-484):
+ * gamma 5/3, pdmb 0.75, CFL min(0.5/(pdmb+0.5),0.3), Vd0 0.5, cHogH = cHogM
+ * = 0.25, floors 1e-12, rmeth 8CENT, lfmlim T, limDT0 1e-3. */
+typedef struct gam_params {
+    int32_t Nip, Njp, Nkp;  /* active cells per direction                  */
+    int32_t nG;             /* ghost layers; must be 4                       */
+    double gamma, CFL, pdmb, Vd0, cHogH, cHogM, dFloor, pFloor;
+    double tFin;            /* Model%tFin: dt is clamped to land on it       */
+    double dt0;             /* Model%dt0: 0 disables the dt0-based checks    */
+    double limDT0;          /* Model%limDT0                                  */
+    double fixedTimestep;   /* > 0: Model%fixedTimestep with this dt         */
+    int32_t rmeth;          /* GAM_RECON_8CENT or GAM_RECON_7UP              */
+    int32_t doLFMLim, doMHD, doBackground, do25D;
+    int32_t precision;      /* GAM_FP64 (drop-in) or GAM_FP32 (bulk FP32)    */
+    int32_t strict;         /* 1: kernels without FMA contraction            */
+    int32_t bc[6];          /* INI, OUTI, INJ, OUTJ, INK, OUTK: GAM_BC_*     */
+} gam_params;
+
+typedef struct gam_handle gam_handle;
+
+/* Fill p with the reference defaults for an Nip x Njp x Nkp grid. */
+int gam_default_params(gam_params* p, int32_t Nip, int32_t Njp, int32_t Nkp);
+
+/* Replaces Hatch/initSolver allocation (init.F90:38-59, 486-509). */
+int gam_create(const gam_params* p, gam_handle** out);
+int gam_destroy(gam_handle* h);
+const char* gam_last_error(gam_handle* h);
+
+/* Corner coordinates xyz(isg:ieg+1,jsg:jeg+1,ksg:keg+1,1:3). The FP64 metric
+ * (face areas/centroids/triads, volumes, barycentres, CFL lengths, edge
+ * lengths/triads, edge B maps) is computed on the GPU.
+ * Replaces Corners2Grid + ebGeom (init.F90:793-1137). */
+int gam_set_geometry(gam_handle* h, const double* xyz);
+
+/* The Fortran-precomputed Grid_T arrays (gamtypes.F90:168-250), as an
+ * alternative to gam_set_geometry for drivers that already hold them:
+ * face(f,3) xfc(f,3,3) Tf(f,9,3) volume(c) xyzcc(c,3) di,dj,dk(c)
+ * edge(f,3) Te(f,9,3) Teb(f,4,3); f = face-sized, c = cell-sized. */
+int gam_set_geometry_arrays(gam_handle* h, const double* face, const double* xfc, const double* Tf,
+                            const double* volume, const double* xyzcc, const double* di, const double* dj,
+                            const double* dk, const double* edge, const double* Te, const double* Teb);
+
+/* Copy back the metric (same layout as gam_set_geometry_arrays). */
+int gam_get_geometry_arrays(gam_handle* h, double* face, double* xfc, double* Tf, double* volume, double* xyzcc,
+                            double* di, double* dj, double* dk, double* edge, double* Te, double* Teb);
+
+/* State%Gas(c,5), State%magFlux(f,3), State%Bxyz(c,3) and the previous state
+ * oState%Gas, oState%magFlux, with State%time, oState%time, Model%dt and
+ * Model%ts. Replaces the in-memory state of gamApp_T (gamtypes.F90:301-321). */
+int gam_upload_state(gam_handle* h, const double* Gas, const double* magFlux, const double* Bxyz,
+                     const double* oGas, const double* omagFlux, double time, double otime, double dt, int32_t ts);
+int gam_download_state(gam_handle* h, double* Gas, double* magFlux, double* Bxyz, double* oGas,
+                       double* omagFlux, double* time, double* otime, double* dt, int32_t* ts);
+
+/* nsteps x stepGamera (gamapp.F90:73-91): AdvanceMHD, t += dt, CalcDT,
+ * EnforceBCs, bFlux2Fld. On return *dt and *t hold Model%dt and Model%t.
+ * A failed CalcDT stops the sequence with GAM_EDT_BAD / GAM_EDT_DISASTER and
+ * leaves the state as the reference leaves it when it stops (after the
+ * update, before the boundary conditions). */
+int gam_step(gam_handle* h, int32_t nsteps, double* dt, double* t);
+
+/* CalcDT on the current state (step.F90:58-168), without changing Model%dt. */
+int gam_calc_dt(gam_handle* h, double* dt);
+
+/* Sum over active cells of |div B| (gridutils.F90:717-770). */
+int gam_divb(gam_handle* h, double* total);
+
+/* Volume-weighted totals over active cells of the five conserved variables
+ * (mass, momentum x/y/z, energy), FP64 deterministic tree reduction. */
+int gam_totals(gam_handle* h, double out[5]);
+
+/* Wall time of the last gam_step call measured with CUDA events (ms). */
+int gam_last_step_ms(gam_handle* h, double* ms);
+
+/* gamApp_T%AdvanceModel(dt) (gamtypessub.F90:74-90): one step, then steps
+ * while Model%t < t_start + dt. */
+int gam_advance_model(gam_handle* h, double dt, double* t_out);
+
+/* Problem set-up on the device from the metric already set, then the
+ * reference's initialisation order (init.F90:190-246): Bxyz, first boundary
+ * conditions, oState = State, first CalcDT, oState%time = t - dt.
+ *   gam_init_orszag_tang: initOT2D (prob.F90:74-119)
+ *   gam_init_blast_wave : initBW (prob.F90:190-298), vector-potential field;
+ *     bw = {x0, y0, z0, D0, P0, pRat, dRat, rC, B0}; needs gam_set_geometry. */
+int gam_init_orszag_tang(gam_handle* h);
+int gam_init_blast_wave(gam_handle* h, const double bw[9]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GAMGPU_H */

@@ -1,0 +1,609 @@
+// C ABI of the GAMERA step (include/gamgpu.h): handle, device memory, layout
+// conversion, step sequencing with CUDA graphs, diagnostics.
+#include <cuda_runtime.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <string>
+#include <vector>
+#include "../../include/gamgpu.h"
+#include "gam_layout.cuh"
+#include "gam_types.cuh"
+
+// variant launchers (gam_step_strict.cu, gam_step_fast.cu)
+void gam_strict_step_f64(const Ctx<double>& C, int cur, cudaStream_t s);
+void gam_strict_dt_f64(const Ctx<double>& C, int cur, cudaStream_t s);
+void gam_fast_step_f64(const Ctx<double>& C, int cur, cudaStream_t s);
+void gam_fast_dt_f64(const Ctx<double>& C, int cur, cudaStream_t s);
+void gam_fast_step_f32(const Ctx<float>& C, int cur, cudaStream_t s);
+void gam_fast_dt_f32(const Ctx<float>& C, int cur, cudaStream_t s);
+// set-up (gam_geom.cu)
+void gam_geom_fortran_to_box_d(const GamBox& b, const double* src, double* dst, bool face, int nc, cudaStream_t s);
+void gam_geom_fortran_to_box_f(const GamBox& b, const double* src, float* dst, bool face, int nc, cudaStream_t s);
+void gam_geom_box_to_fortran_d(const GamBox& b, const double* src, double* dst, bool face, int nc, cudaStream_t s);
+void gam_geom_box_to_fortran_f(const GamBox& b, const float* src, double* dst, bool face, int nc, cudaStream_t s);
+void gam_geom_fill(double* p, long n, double v, cudaStream_t s);
+void gam_geom_d2f(const double* src, float* dst, long n, cudaStream_t s);
+void gam_geom_metric(const GamBox& b, const double* xyz, double* face, double* xfc, double* Tf, double* vol,
+                     double* xyzcc, double* dijk, double* dl, double* edge, double* Te, double* Teb, cudaStream_t s);
+void gam_geom_ic_ot(const GamBox& b, const double* xyzcc, const double* face, double* Gas, double* mf, double gamma,
+                    cudaStream_t s);
+void gam_geom_ic_bw(const GamBox& b, const double* xyz, const double* vol, double* Gas, double* mf, double* lA,
+                    double gamma, const double* bw, bool doMHD, cudaStream_t s);
+// diagnostics (gam_diag.cu)
+void gam_diag_divb(const GamBox& b, const double* mf, double* partial, double* out, cudaStream_t s);
+void gam_diag_divb_f(const GamBox& b, const float* mf, double* partial, double* out, cudaStream_t s);
+void gam_diag_totals(const GamBox& b, const double* Gas, const double* vol, double* partial, double* out,
+                     cudaStream_t s);
+void gam_diag_totals_f(const GamBox& b, const float* Gas, const float* vol, double* partial, double* out,
+                       cudaStream_t s);
+void gam_diag_min3(const GamBox& b, const double* dijk, double* dl, cudaStream_t s);
+int gam_diag_partials(const GamBox& b);
+
+// FP64 metric, always held (the FP32 form rounds it once)
+struct GeoD {
+    double *vol, *xyzcc, *dl, *dijk, *face, *xfc, *Tf, *edge, *Te, *Teb, *xyz;
+};
+
+struct gam_handle {
+    gam_params p;
+    GamBox b;
+    cudaStream_t s = nullptr;
+    bool f32 = false;
+    std::vector<void*> allocs;
+    GeoD gd{};
+    // bulk views in the compute precision
+    Ctx<double> cd{};
+    Ctx<float> cf{};
+    GamScalars* sc = nullptr;   // device
+    double* staging = nullptr;  // device, Fortran-layout transfer buffer
+    double* partial = nullptr;  // device, reduction partials
+    double* dres = nullptr;     // device, reduction results
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    int cur = 0;
+    bool haveGeo = false, haveState = false, haveXyz = false;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double lastMs = 0.0;
+    std::string err;
+};
+
+static int fail(gam_handle* h, int code, const std::string& msg) {
+    if (h) h->err = msg;
+    return code;
+}
+#define CK(h, call)                                                                            \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess)                                                                 \
+            return fail(h, GAM_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_));    \
+    } while (0)
+
+template <class T> static T* dalloc(gam_handle* h, long n, cudaError_t* e) {
+    void* p = nullptr;
+    *e = cudaMalloc(&p, sizeof(T) * (size_t)n);
+    if (*e == cudaSuccess) {
+        h->allocs.push_back(p);
+        cudaMemsetAsync(p, 0, sizeof(T) * (size_t)n, h->s);
+    }
+    return (T*)p;
+}
+
+extern "C" int gam_default_params(gam_params* p, int32_t Nip, int32_t Njp, int32_t Nkp) {
+    if (!p) return GAM_EINVAL;
+    memset(p, 0, sizeof(*p));
+    p->Nip = Nip; p->Njp = Njp; p->Nkp = Nkp; p->nG = 4;
+    p->gamma = 5.0 / 3.0;
+    p->pdmb = 0.75;
+    p->CFL = 0.5 / (p->pdmb + 0.5) < 0.3 ? 0.5 / (p->pdmb + 0.5) : 0.3;
+    p->Vd0 = 0.5; p->cHogH = 0.25; p->cHogM = 0.25;
+    p->dFloor = 1.0e-12; p->pFloor = 1.0e-12;
+    p->tFin = 1.0; p->dt0 = 0.0; p->limDT0 = 1.0e-3; p->fixedTimestep = -1.0;
+    p->rmeth = GAM_RECON_8CENT; p->doLFMLim = 1; p->doMHD = 1; p->doBackground = 0; p->do25D = (Nkp == 1);
+    p->precision = GAM_FP64; p->strict = 0;
+    for (int n = 0; n < 6; n++) p->bc[n] = GAM_BC_PERIODIC;
+    return GAM_OK;
+}
+
+template <class R> static void fill_dev_params(DevParams<R>& P, const gam_params& p) {
+    P.gamma = (R)p.gamma;
+    P.gm1 = (R)(p.gamma - 1);
+    P.CFL = (R)p.CFL;
+    P.pdmb = (R)p.pdmb;
+    P.Vd0 = (R)p.Vd0;
+    P.cHogH = (R)p.cHogH;
+    P.dFloor = (R)p.dFloor;
+    P.pFloor = (R)p.pFloor;
+    P.doMHD = p.doMHD; P.doLFMLim = p.doLFMLim; P.do25D = p.do25D; P.doBackground = p.doBackground;
+    P.up7 = p.rmeth == GAM_RECON_7UP;
+    for (int n = 0; n < 6; n++) P.bc[n] = p.bc[n];
+}
+
+template <class R> static int alloc_bulk(gam_handle* h, Ctx<R>& C) {
+    cudaError_t e = cudaSuccess;
+    const long fs = h->b.fs;
+#define A(ptr, n)                                                   \
+    do {                                                            \
+        ptr = dalloc<R>(h, (n) * fs, &e);                           \
+        if (e != cudaSuccess) return fail(h, GAM_ECUDA, "cudaMalloc failed (out of device memory?)"); \
+    } while (0)
+    for (int q = 0; q < 2; q++) {
+        A(C.st[q].Gas, 5);
+        A(C.st[q].mf, 3);
+        A(C.st[q].B, 3);
+    }
+    A(C.w.Wh, 5); A(C.w.Wn, 5); A(C.w.VdV, 3); A(C.w.Bh, 3);
+    A(C.w.bh, 3); A(C.w.bn, 3); A(C.w.Bnf, 3); A(C.w.Vf, 9); A(C.w.E, 3);
+    A(C.w.gF, 15); A(C.w.mF, 9);
+    if (sizeof(R) == sizeof(double)) {
+        C.g.vol = (const R*)h->gd.vol; C.g.xyzcc = (const R*)h->gd.xyzcc; C.g.dl = (const R*)h->gd.dl;
+        C.g.face = (const R*)h->gd.face; C.g.xfc = (const R*)h->gd.xfc; C.g.Tf = (const R*)h->gd.Tf;
+        C.g.edge = (const R*)h->gd.edge; C.g.Te = (const R*)h->gd.Te; C.g.Teb = (const R*)h->gd.Teb;
+    } else {
+        R *vol, *xyzcc, *dl, *face, *xfc, *Tf, *edge, *Te, *Teb;
+        A(vol, 1); A(xyzcc, 3); A(dl, 1); A(face, 3); A(xfc, 9); A(Tf, 27); A(edge, 3); A(Te, 27); A(Teb, 12);
+        C.g.vol = vol; C.g.xyzcc = xyzcc; C.g.dl = dl; C.g.face = face; C.g.xfc = xfc; C.g.Tf = Tf;
+        C.g.edge = edge; C.g.Te = Te; C.g.Teb = Teb;
+    }
+#undef A
+    C.g.fcB0 = C.g.bFlux0 = C.g.edgB0 = C.g.B0 = C.g.dpB0 = nullptr;
+    C.b = h->b;
+    fill_dev_params(C.P, h->p);
+    C.sc = h->sc;
+    C.gamma = h->p.gamma;
+    C.gm1 = h->p.gamma - 1;
+    return GAM_OK;
+}
+
+extern "C" int gam_create(const gam_params* p, gam_handle** out) {
+    if (!p || !out) return GAM_EINVAL;
+    *out = nullptr;
+    gam_handle* h = new gam_handle();
+    h->p = *p;
+    auto bad = [&](int code, const char* m) {
+        h->err = m;
+        *out = h;
+        return code;
+    };
+    if (p->nG != 4) return bad(GAM_EINVAL, "nG must be 4");
+    if (p->Nip < 16 || p->Nip % 8 != 0) return bad(GAM_EBADDIM, "Grid I-size must be >= 16 and divisible by 8");
+    if (p->Njp < 1 || p->Nkp < 1) return bad(GAM_EBADDIM, "Njp and Nkp must be >= 1");
+    if (p->do25D && p->Nkp != 1) return bad(GAM_EBADDIM, "do25D needs Nkp == 1");
+    if (!p->do25D && (p->Njp < 4 || p->Nkp < 4)) return bad(GAM_EBADDIM, "3-D grids need Njp, Nkp >= 4");
+    if (p->doBackground) return bad(GAM_EINVAL, "background field: use the dipole set-up entry points");
+    if (p->precision != GAM_FP64 && p->precision != GAM_FP32) return bad(GAM_EINVAL, "unknown precision");
+    if (p->precision == GAM_FP32 && p->strict) return bad(GAM_EINVAL, "strict applies to the FP64 form only");
+    for (int n = 0; n < 6; n++)
+        if (p->bc[n] != GAM_BC_PERIODIC && p->bc[n] != GAM_BC_NONE) return bad(GAM_EINVAL, "unsupported boundary kind");
+    if (p->do25D && (p->bc[4] != GAM_BC_PERIODIC || p->bc[5] != GAM_BC_PERIODIC))
+        return bad(GAM_EINVAL, "do25D replicates k: the k boundaries must be periodic");
+    h->b = gam_make_box(p->Nip, p->Njp, p->Nkp);
+    h->f32 = p->precision == GAM_FP32;
+    if (cudaStreamCreateWithFlags(&h->s, cudaStreamNonBlocking) != cudaSuccess) return bad(GAM_ECUDA, "no CUDA device");
+    cudaEventCreate(&h->ev0);
+    cudaEventCreate(&h->ev1);
+    cudaError_t e = cudaSuccess;
+    const long fs = h->b.fs;
+    GeoD& g = h->gd;
+#define AD(ptr, n)                                                     \
+    do {                                                               \
+        ptr = dalloc<double>(h, (n) * fs, &e);                         \
+        if (e != cudaSuccess) return bad(GAM_ECUDA, "cudaMalloc failed (out of device memory?)"); \
+    } while (0)
+    AD(g.vol, 1); AD(g.xyzcc, 3); AD(g.dl, 1); AD(g.dijk, 3); AD(g.face, 3); AD(g.xfc, 9); AD(g.Tf, 27);
+    AD(g.edge, 3); AD(g.Te, 27); AD(g.Teb, 12); AD(g.xyz, 3);
+#undef AD
+    // staging: the largest Fortran array passed through (Tf/Te: 27 face-sized comps)
+    long nface = (long)(h->b.Ni + 1) * (h->b.Nj + 1) * (h->b.Nk + 1);
+    h->staging = dalloc<double>(h, 27 * nface, &e);
+    if (e != cudaSuccess) return bad(GAM_ECUDA, "cudaMalloc failed (staging)");
+    h->partial = dalloc<double>(h, 8 * (long)gam_diag_partials(h->b), &e);
+    h->dres = dalloc<double>(h, 16, &e);
+    h->sc = dalloc<GamScalars>(h, 1, &e);
+    if (e != cudaSuccess) return bad(GAM_ECUDA, "cudaMalloc failed");
+    int rc = h->f32 ? alloc_bulk<float>(h, h->cf) : alloc_bulk<double>(h, h->cd);
+    if (rc != GAM_OK) {
+        *out = h;
+        return rc;
+    }
+    GamScalars s0;
+    memset(&s0, 0, sizeof(s0));
+    s0.tFin = p->tFin; s0.dt0 = p->dt0; s0.limDT0 = p->limDT0; s0.CFL = p->CFL;
+    s0.fixedTimestep = p->fixedTimestep > 0;
+    s0.dt = p->fixedTimestep > 0 ? p->fixedTimestep : 0.0;
+    double hugedt = 1.0e12;
+    memcpy(&s0.dtmin_bits, &hugedt, 8);
+    if (cudaMemcpyAsync(h->sc, &s0, sizeof(s0), cudaMemcpyHostToDevice, h->s) != cudaSuccess ||
+        cudaStreamSynchronize(h->s) != cudaSuccess)
+        return bad(GAM_ECUDA, "initialisation copy failed");
+    *out = h;
+    return GAM_OK;
+}
+
+extern "C" int gam_destroy(gam_handle* h) {
+    if (!h) return GAM_EINVAL;
+    if (h->s) cudaStreamSynchronize(h->s);
+    for (int q = 0; q < 2; q++)
+        if (h->graph[q]) cudaGraphExecDestroy(h->graph[q]);
+    for (void* p : h->allocs) cudaFree(p);
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->s) cudaStreamDestroy(h->s);
+    delete h;
+    return GAM_OK;
+}
+
+extern "C" const char* gam_last_error(gam_handle* h) { return h ? h->err.c_str() : "null handle"; }
+
+static long n_face(const GamBox& b) { return (long)(b.Ni + 1) * (b.Nj + 1) * (b.Nk + 1); }
+static long n_cell(const GamBox& b) { return (long)b.Ni * b.Nj * b.Nk; }
+
+// host Fortran array -> FP64 box array
+static int up_d(gam_handle* h, const double* src, double* dst, bool face, int nc) {
+    long n = (face ? n_face(h->b) : n_cell(h->b)) * nc;
+    CK(h, cudaMemcpyAsync(h->staging, src, sizeof(double) * n, cudaMemcpyHostToDevice, h->s));
+    gam_geom_fortran_to_box_d(h->b, h->staging, dst, face, nc, h->s);
+    return GAM_OK;
+}
+template <class R> static int up_r(gam_handle* h, const double* src, R* dst, bool face, int nc) {
+    long n = (face ? n_face(h->b) : n_cell(h->b)) * nc;
+    CK(h, cudaMemcpyAsync(h->staging, src, sizeof(double) * n, cudaMemcpyHostToDevice, h->s));
+    if (sizeof(R) == sizeof(double))
+        gam_geom_fortran_to_box_d(h->b, h->staging, (double*)dst, face, nc, h->s);
+    else
+        gam_geom_fortran_to_box_f(h->b, h->staging, (float*)dst, face, nc, h->s);
+    return GAM_OK;
+}
+template <class R> static int down_r(gam_handle* h, const R* src, double* dst, bool face, int nc) {
+    long n = (face ? n_face(h->b) : n_cell(h->b)) * nc;
+    if (sizeof(R) == sizeof(double))
+        gam_geom_box_to_fortran_d(h->b, (const double*)src, h->staging, face, nc, h->s);
+    else
+        gam_geom_box_to_fortran_f(h->b, (const float*)src, h->staging, face, nc, h->s);
+    CK(h, cudaMemcpyAsync(dst, h->staging, sizeof(double) * n, cudaMemcpyDeviceToHost, h->s));
+    CK(h, cudaStreamSynchronize(h->s));
+    return GAM_OK;
+}
+
+// FP32 form: round the FP64 metric once into the FP32 copies
+static void sync_geo_f32(gam_handle* h) {
+    if (!h->f32) return;
+    Geo<float>& g = h->cf.g;
+    const long fs = h->b.fs;
+    gam_geom_d2f(h->gd.vol, (float*)g.vol, fs, h->s);
+    gam_geom_d2f(h->gd.xyzcc, (float*)g.xyzcc, 3 * fs, h->s);
+    gam_geom_d2f(h->gd.dl, (float*)g.dl, fs, h->s);
+    gam_geom_d2f(h->gd.face, (float*)g.face, 3 * fs, h->s);
+    gam_geom_d2f(h->gd.xfc, (float*)g.xfc, 9 * fs, h->s);
+    gam_geom_d2f(h->gd.Tf, (float*)g.Tf, 27 * fs, h->s);
+    gam_geom_d2f(h->gd.edge, (float*)g.edge, 3 * fs, h->s);
+    gam_geom_d2f(h->gd.Te, (float*)g.Te, 27 * fs, h->s);
+    gam_geom_d2f(h->gd.Teb, (float*)g.Teb, 12 * fs, h->s);
+}
+
+extern "C" int gam_set_geometry(gam_handle* h, const double* xyz) {
+    if (!h || !xyz) return GAM_EINVAL;
+    int rc = up_d(h, xyz, h->gd.xyz, true, 3);
+    if (rc) return rc;
+    GeoD& g = h->gd;
+    gam_geom_metric(h->b, g.xyz, g.face, g.xfc, g.Tf, g.vol, g.xyzcc, g.dijk, g.dl, g.edge, g.Te, g.Teb, h->s);
+    sync_geo_f32(h);
+    CK(h, cudaGetLastError());
+    CK(h, cudaStreamSynchronize(h->s));
+    h->haveGeo = true;
+    h->haveXyz = true;
+    return GAM_OK;
+}
+
+extern "C" int gam_set_geometry_arrays(gam_handle* h, const double* face, const double* xfc, const double* Tf,
+                                       const double* volume, const double* xyzcc, const double* di, const double* dj,
+                                       const double* dk, const double* edge, const double* Te, const double* Teb) {
+    if (!h || !face || !xfc || !Tf || !volume || !xyzcc || !di || !dj || !dk || !edge || !Te || !Teb) return GAM_EINVAL;
+    GeoD& g = h->gd;
+    const long fs = h->b.fs;
+    int rc;
+    if ((rc = up_d(h, face, g.face, true, 3))) return rc;
+    if ((rc = up_d(h, xfc, g.xfc, true, 9))) return rc;
+    if ((rc = up_d(h, Tf, g.Tf, true, 27))) return rc;
+    if ((rc = up_d(h, volume, g.vol, false, 1))) return rc;
+    if ((rc = up_d(h, xyzcc, g.xyzcc, false, 3))) return rc;
+    if ((rc = up_d(h, di, g.dijk, false, 1))) return rc;
+    if ((rc = up_d(h, dj, g.dijk + fs, false, 1))) return rc;
+    if ((rc = up_d(h, dk, g.dijk + 2 * fs, false, 1))) return rc;
+    if ((rc = up_d(h, edge, g.edge, true, 3))) return rc;
+    if ((rc = up_d(h, Te, g.Te, true, 27))) return rc;
+    if ((rc = up_d(h, Teb, g.Teb, true, 12))) return rc;
+    gam_diag_min3(h->b, g.dijk, g.dl, h->s);
+    sync_geo_f32(h);
+    CK(h, cudaGetLastError());
+    CK(h, cudaStreamSynchronize(h->s));
+    h->haveGeo = true;
+    return GAM_OK;
+}
+
+extern "C" int gam_get_geometry_arrays(gam_handle* h, double* face, double* xfc, double* Tf, double* volume,
+                                       double* xyzcc, double* di, double* dj, double* dk, double* edge, double* Te,
+                                       double* Teb) {
+    if (!h) return GAM_EINVAL;
+    if (!h->haveGeo) return fail(h, GAM_ESTATE, "no geometry set");
+    GeoD& g = h->gd;
+    const long fs = h->b.fs;
+    int rc = GAM_OK;
+    if (face && (rc = down_r<double>(h, g.face, face, true, 3))) return rc;
+    if (xfc && (rc = down_r<double>(h, g.xfc, xfc, true, 9))) return rc;
+    if (Tf && (rc = down_r<double>(h, g.Tf, Tf, true, 27))) return rc;
+    if (volume && (rc = down_r<double>(h, g.vol, volume, false, 1))) return rc;
+    if (xyzcc && (rc = down_r<double>(h, g.xyzcc, xyzcc, false, 3))) return rc;
+    if (di && (rc = down_r<double>(h, g.dijk, di, false, 1))) return rc;
+    if (dj && (rc = down_r<double>(h, g.dijk + fs, dj, false, 1))) return rc;
+    if (dk && (rc = down_r<double>(h, g.dijk + 2 * fs, dk, false, 1))) return rc;
+    if (edge && (rc = down_r<double>(h, g.edge, edge, true, 3))) return rc;
+    if (Te && (rc = down_r<double>(h, g.Te, Te, true, 27))) return rc;
+    if (Teb && (rc = down_r<double>(h, g.Teb, Teb, true, 12))) return rc;
+    return GAM_OK;
+}
+
+template <class R>
+static int upload_state_t(gam_handle* h, Ctx<R>& C, const double* Gas, const double* magFlux, const double* Bxyz,
+                          const double* oGas, const double* omagFlux) {
+    int rc;
+    h->cur = 0;
+    if ((rc = up_r<R>(h, Gas, C.st[0].Gas, false, 5))) return rc;
+    if ((rc = up_r<R>(h, magFlux, C.st[0].mf, true, 3))) return rc;
+    if ((rc = up_r<R>(h, Bxyz, C.st[0].B, false, 3))) return rc;
+    if ((rc = up_r<R>(h, oGas, C.st[1].Gas, false, 5))) return rc;
+    if ((rc = up_r<R>(h, omagFlux, C.st[1].mf, true, 3))) return rc;
+    return GAM_OK;
+}
+
+static int set_scalars(gam_handle* h, double time, double otime, double dt, int32_t ts) {
+    GamScalars s;
+    CK(h, cudaMemcpyAsync(&s, h->sc, sizeof(s), cudaMemcpyDeviceToHost, h->s));
+    CK(h, cudaStreamSynchronize(h->s));
+    s.time = time; s.otime = otime; s.t = time; s.dt = dt; s.ts = ts;
+    s.status = 0; s.halted = 0; s.nbad = 0;
+    double hugedt = 1.0e12;
+    memcpy(&s.dtmin_bits, &hugedt, 8);
+    CK(h, cudaMemcpyAsync(h->sc, &s, sizeof(s), cudaMemcpyHostToDevice, h->s));
+    CK(h, cudaStreamSynchronize(h->s));
+    return GAM_OK;
+}
+
+extern "C" int gam_upload_state(gam_handle* h, const double* Gas, const double* magFlux, const double* Bxyz,
+                                const double* oGas, const double* omagFlux, double time, double otime, double dt,
+                                int32_t ts) {
+    if (!h || !Gas || !magFlux || !Bxyz || !oGas || !omagFlux) return GAM_EINVAL;
+    int rc = h->f32 ? upload_state_t<float>(h, h->cf, Gas, magFlux, Bxyz, oGas, omagFlux)
+                    : upload_state_t<double>(h, h->cd, Gas, magFlux, Bxyz, oGas, omagFlux);
+    if (rc) return rc;
+    if ((rc = set_scalars(h, time, otime, dt, ts))) return rc;
+    CK(h, cudaStreamSynchronize(h->s));
+    h->haveState = true;
+    return GAM_OK;
+}
+
+template <class R>
+static int download_state_t(gam_handle* h, Ctx<R>& C, double* Gas, double* magFlux, double* Bxyz, double* oGas,
+                            double* omagFlux) {
+    int rc;
+    const StateBuf<R>& S = C.st[h->cur];
+    const StateBuf<R>& O = C.st[1 - h->cur];
+    if (Gas && (rc = down_r<R>(h, S.Gas, Gas, false, 5))) return rc;
+    if (magFlux && (rc = down_r<R>(h, S.mf, magFlux, true, 3))) return rc;
+    if (Bxyz && (rc = down_r<R>(h, S.B, Bxyz, false, 3))) return rc;
+    if (oGas && (rc = down_r<R>(h, O.Gas, oGas, false, 5))) return rc;
+    if (omagFlux && (rc = down_r<R>(h, O.mf, omagFlux, true, 3))) return rc;
+    return GAM_OK;
+}
+
+extern "C" int gam_download_state(gam_handle* h, double* Gas, double* magFlux, double* Bxyz, double* oGas,
+                                  double* omagFlux, double* time, double* otime, double* dt, int32_t* ts) {
+    if (!h) return GAM_EINVAL;
+    if (!h->haveState) return fail(h, GAM_ESTATE, "no state uploaded");
+    int rc = h->f32 ? download_state_t<float>(h, h->cf, Gas, magFlux, Bxyz, oGas, omagFlux)
+                    : download_state_t<double>(h, h->cd, Gas, magFlux, Bxyz, oGas, omagFlux);
+    if (rc) return rc;
+    GamScalars s;
+    CK(h, cudaMemcpy(&s, h->sc, sizeof(s), cudaMemcpyDeviceToHost));
+    if (time) *time = s.time;
+    if (otime) *otime = s.otime;
+    if (dt) *dt = s.dt;
+    if (ts) *ts = s.ts;
+    return GAM_OK;
+}
+
+static void launch_one(gam_handle* h, int cur) {
+    if (h->f32)
+        gam_fast_step_f32(h->cf, cur, h->s);
+    else if (h->p.strict)
+        gam_strict_step_f64(h->cd, cur, h->s);
+    else
+        gam_fast_step_f64(h->cd, cur, h->s);
+}
+
+static int ensure_graph(gam_handle* h, int cur) {
+    if (h->graph[cur]) return GAM_OK;
+    cudaGraph_t g;
+    CK(h, cudaStreamBeginCapture(h->s, cudaStreamCaptureModeThreadLocal));
+    launch_one(h, cur);
+    CK(h, cudaStreamEndCapture(h->s, &g));
+    CK(h, cudaGraphInstantiate(&h->graph[cur], g, 0));
+    cudaGraphDestroy(g);
+    return GAM_OK;
+}
+
+extern "C" int gam_step(gam_handle* h, int32_t nsteps, double* dt, double* t) {
+    if (!h || nsteps < 0) return GAM_EINVAL;
+    if (!h->haveGeo) return fail(h, GAM_ESTATE, "gam_step before gam_set_geometry");
+    if (!h->haveState) return fail(h, GAM_ESTATE, "gam_step before gam_upload_state");
+    int rc;
+    if ((rc = ensure_graph(h, 0))) return rc;
+    if ((rc = ensure_graph(h, 1))) return rc;
+    CK(h, cudaEventRecord(h->ev0, h->s));
+    for (int n = 0; n < nsteps; n++) {
+        CK(h, cudaGraphLaunch(h->graph[h->cur], h->s));
+        h->cur = 1 - h->cur;
+    }
+    CK(h, cudaEventRecord(h->ev1, h->s));
+    GamScalars s;
+    CK(h, cudaMemcpyAsync(&s, h->sc, sizeof(s), cudaMemcpyDeviceToHost, h->s));
+    CK(h, cudaStreamSynchronize(h->s));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+    h->lastMs = ms;
+    if (dt) *dt = s.dt;
+    if (t) *t = s.t;
+    if (s.halted) {
+        // the halted step already swapped buffers like a completed one; later
+        // steps did nothing and must not count as swaps
+        return fail(h, s.status == 5 ? GAM_EDT_DISASTER : GAM_EDT_BAD,
+                    s.status == 5 ? "CalcDT: timestep too small or not finite" : "CalcDT: timestep dropped");
+    }
+    return GAM_OK;
+}
+
+extern "C" int gam_advance_model(gam_handle* h, double dt, double* t_out) {
+    if (!h) return GAM_EINVAL;
+    GamScalars s;
+    CK(h, cudaMemcpy(&s, h->sc, sizeof(s), cudaMemcpyDeviceToHost));
+    const double target = s.t + dt;
+    double ddt, t;
+    int rc = gam_step(h, 1, &ddt, &t);
+    while (rc == GAM_OK && t < target) rc = gam_step(h, 1, &ddt, &t);
+    if (t_out) *t_out = t;
+    return rc;
+}
+
+extern "C" int gam_last_step_ms(gam_handle* h, double* ms) {
+    if (!h || !ms) return GAM_EINVAL;
+    *ms = h->lastMs;
+    return GAM_OK;
+}
+
+extern "C" int gam_calc_dt(gam_handle* h, double* dt) {
+    if (!h || !dt) return GAM_EINVAL;
+    if (!h->haveGeo || !h->haveState) return fail(h, GAM_ESTATE, "gam_calc_dt needs geometry and state");
+    GamScalars s;
+    CK(h, cudaMemcpyAsync(&s, h->sc, sizeof(s), cudaMemcpyDeviceToHost, h->s));
+    CK(h, cudaStreamSynchronize(h->s));
+    if (s.fixedTimestep) {
+        *dt = s.dt;
+        return GAM_OK;
+    }
+    double hugedt = 1.0e12;
+    unsigned long long hb;
+    memcpy(&hb, &hugedt, 8);
+    CK(h, cudaMemcpyAsync(&h->sc->dtmin_bits, &hb, 8, cudaMemcpyHostToDevice, h->s));
+    if (h->f32)
+        gam_fast_dt_f32(h->cf, h->cur, h->s);
+    else if (h->p.strict)
+        gam_strict_dt_f64(h->cd, h->cur, h->s);
+    else
+        gam_fast_dt_f64(h->cd, h->cur, h->s);
+    unsigned long long bits;
+    CK(h, cudaMemcpyAsync(&bits, &h->sc->dtmin_bits, 8, cudaMemcpyDeviceToHost, h->s));
+    CK(h, cudaMemcpyAsync(&h->sc->dtmin_bits, &hb, 8, cudaMemcpyHostToDevice, h->s));
+    CK(h, cudaStreamSynchronize(h->s));
+    double dtMin;
+    memcpy(&dtMin, &bits, 8);
+    // step.F90:158-166 clamps (the ts > 0 failure checks belong to a step)
+    double d = dtMin;
+    if (s.t + d > s.tFin) d = (s.tFin - s.t) > 1.0e-12 ? (s.tFin - s.t) : 1.0e-12;
+    if (s.dt0 > 1.0e-12 && d > 10.0 * s.dt0) d = 10.0 * s.dt0;
+    *dt = d;
+    if (dtMin == hugedt) return fail(h, GAM_EDT_DISASTER, "no timestep was smaller than HUGE");
+    return GAM_OK;
+}
+
+extern "C" int gam_divb(gam_handle* h, double* total) {
+    if (!h || !total) return GAM_EINVAL;
+    if (!h->haveState) return fail(h, GAM_ESTATE, "no state");
+    if (h->f32)
+        gam_diag_divb_f(h->b, h->cf.st[h->cur].mf, h->partial, h->dres, h->s);
+    else
+        gam_diag_divb(h->b, h->cd.st[h->cur].mf, h->partial, h->dres, h->s);
+    CK(h, cudaMemcpyAsync(total, h->dres, 8, cudaMemcpyDeviceToHost, h->s));
+    CK(h, cudaStreamSynchronize(h->s));
+    return GAM_OK;
+}
+
+extern "C" int gam_totals(gam_handle* h, double out[5]) {
+    if (!h || !out) return GAM_EINVAL;
+    if (!h->haveState || !h->haveGeo) return fail(h, GAM_ESTATE, "no state");
+    if (h->f32)
+        gam_diag_totals_f(h->b, h->cf.st[h->cur].Gas, h->cf.g.vol, h->partial, h->dres, h->s);
+    else
+        gam_diag_totals(h->b, h->cd.st[h->cur].Gas, h->gd.vol, h->partial, h->dres, h->s);
+    CK(h, cudaMemcpyAsync(out, h->dres, 5 * 8, cudaMemcpyDeviceToHost, h->s));
+    CK(h, cudaStreamSynchronize(h->s));
+    return GAM_OK;
+}
+
+// ------------------------------------------------------------ problem set-up
+// Initial conditions computed on the GPU from the metric already set
+// (prob.F90 initOT2D / initBW), followed by the reference's initialisation
+// order (init.F90:190-244): Bxyz from fluxes, oState = State, boundary
+// conditions, first CalcDT, oState%time = t - dt.
+template <class R> static int finish_init(gam_handle* h, Ctx<R>& C, double* Gas64, double* mf64, double t0) {
+    // Gas64/mf64: FP64 box arrays holding the IC
+    const long fs = h->b.fs;
+    for (int q = 0; q < 2; q++) {
+        if (sizeof(R) == sizeof(double)) {
+            cudaMemcpyAsync(C.st[q].Gas, Gas64, 5 * fs * sizeof(double), cudaMemcpyDeviceToDevice, h->s);
+            cudaMemcpyAsync(C.st[q].mf, mf64, 3 * fs * sizeof(double), cudaMemcpyDeviceToDevice, h->s);
+        } else {
+            gam_geom_d2f(Gas64, (float*)C.st[q].Gas, 5 * fs, h->s);
+            gam_geom_d2f(mf64, (float*)C.st[q].mf, 3 * fs, h->s);
+        }
+    }
+    CK(h, cudaGetLastError());
+    h->cur = 0;
+    h->haveState = true;
+    int rc = set_scalars(h, t0, t0, 0.0, 0);
+    if (rc) return rc;
+    return GAM_OK;
+}
+
+void gam_strict_init_f64(const Ctx<double>& C, int cur, cudaStream_t s);
+void gam_fast_init_f64(const Ctx<double>& C, int cur, cudaStream_t s);
+void gam_fast_init_f32(const Ctx<float>& C, int cur, cudaStream_t s);
+
+static int init_common(gam_handle* h, double* Gas64, double* mf64) {
+    int rc = h->f32 ? finish_init<float>(h, h->cf, Gas64, mf64, 0.0) : finish_init<double>(h, h->cd, Gas64, mf64, 0.0);
+    if (rc) return rc;
+    // Bxyz of State, first BCs, copy to oState (init.F90:217-238)
+    if (h->f32)
+        gam_fast_init_f32(h->cf, 0, h->s);
+    else if (h->p.strict)
+        gam_strict_init_f64(h->cd, 0, h->s);
+    else
+        gam_fast_init_f64(h->cd, 0, h->s);
+    CK(h, cudaGetLastError());
+    double dt;
+    rc = gam_calc_dt(h, &dt);
+    if (rc) return rc;
+    // Model%dt = CalcDT; oState%time = State%time - Model%dt (init.F90:241-246)
+    return set_scalars(h, 0.0, -dt, dt, 0);
+}
+
+extern "C" int gam_init_orszag_tang(gam_handle* h) {
+    if (!h) return GAM_EINVAL;
+    if (!h->haveGeo) return fail(h, GAM_ESTATE, "set the geometry first");
+    double* Gas64 = h->staging;
+    double* mf64 = h->staging + 5 * h->b.fs;
+    if (8 * h->b.fs > 27 * n_face(h->b)) return fail(h, GAM_EINVAL, "staging too small");
+    gam_geom_fill(Gas64, 8 * h->b.fs, 0.0, h->s);
+    gam_geom_ic_ot(h->b, h->gd.xyzcc, h->gd.face, Gas64, mf64, h->p.gamma, h->s);
+    return init_common(h, Gas64, mf64);
+}
+
+extern "C" int gam_init_blast_wave(gam_handle* h, const double* bw9) {
+    if (!h || !bw9) return GAM_EINVAL;
+    if (!h->haveXyz) return fail(h, GAM_ESTATE, "the blast-wave IC integrates over cells: call gam_set_geometry first");
+    if (11 * h->b.fs > 27 * n_face(h->b)) return fail(h, GAM_EINVAL, "staging too small");
+    double* Gas64 = h->staging;
+    double* mf64 = h->staging + 5 * h->b.fs;
+    double* lA = h->staging + 8 * h->b.fs;
+    gam_geom_fill(Gas64, 8 * h->b.fs, 0.0, h->s);
+    gam_geom_ic_bw(h->b, h->gd.xyz, h->gd.vol, Gas64, mf64, lA, h->p.gamma, bw9, h->p.doMHD != 0, h->s);
+    return init_common(h, Gas64, mf64);
+}

@@ -1,0 +1,515 @@
+// One-time FP64 set-up on the GPU: the grid metric from corner coordinates
+// (Corners2Grid + ebGeom, init.F90:793-1137, with the 12-point Gauss rules of
+// quadrature.F90), the problem initial conditions used by the benchmarks
+// (initOT2D prob.F90:74-119; initBW prob.F90:190-298 with GasIC2State and
+// VectorPot2Flux, gridutils.F90:144-237), and the layout conversions between
+// the Fortran arrays and the padded device box.
+//
+// Built with -fmad=false: each expression is evaluated in the reference's
+// order with IEEE rounding, so the metric equals an IEEE-strict CPU
+// evaluation of the same formulas bit for bit.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "gam_layout.cuh"
+#include "gam_types.cuh"
+
+namespace gam_geom {
+
+static constexpr double TINY = 1.0e-12;
+
+__constant__ double c_gA[12] = {
+    0.1252334085114689154724, 0.3678314989981801937527, 0.5873179542866174472967,
+    0.7699026741943046870369, 0.9041172563704748566785, 0.9815606342467192506906,
+    -0.1252334085114689154724, -0.3678314989981801937527, -0.5873179542866174472967,
+    -0.7699026741943046870369, -0.9041172563704748566785, -0.9815606342467192506906};
+__constant__ double c_gW[12] = {
+    0.2491470458134027850006, 0.233492536538354808761, 0.203167426723065921749,
+    0.160078328543346226335, 0.1069393259953184309603, 0.0471753363865118271946,
+    0.2491470458134027850006, 0.233492536538354808761, 0.203167426723065921749,
+    0.160078328543346226335, 0.1069393259953184309603, 0.0471753363865118271946};
+
+__device__ __forceinline__ long lidx(const GamBox& b, int ii, int jj, int kk) {
+    return (long)ii + (long)b.sx * jj + b.sk * kk;
+}
+__device__ __forceinline__ bool tid3(int n0, int n1, int n2, int& a, int& c, int& e) {
+    a = blockIdx.x * blockDim.x + threadIdx.x;
+    c = blockIdx.y * blockDim.y + threadIdx.y;
+    e = blockIdx.z * blockDim.z + threadIdx.z;
+    return a < n0 && c < n1 && e < n2;
+}
+
+// NORM2 as gfortran evaluates it (scaled sum of squares)
+__device__ double norm2s(const double* a) {
+    double scale = 1.0, res = 0.0;
+    for (int q = 0; q < 3; q++) {
+        if (a[q] != 0.0) {
+            double ax = fabs(a[q]);
+            if (scale < ax) {
+                double val = scale / ax;
+                res = 1.0 + res * val * val;
+                scale = ax;
+            } else {
+                double val = ax / scale;
+                res += val * val;
+            }
+        }
+    }
+    return scale * sqrt(res);
+}
+__device__ __forceinline__ void cross3(const double* a, const double* b, double* c) {
+    c[0] = a[1] * b[2] - a[2] * b[1];
+    c[1] = a[2] * b[0] - a[0] * b[2];
+    c[2] = a[0] * b[1] - a[1] * b[0];
+}
+__device__ __forceinline__ double X(const GamBox& b, const double* xyz, int ii, int jj, int kk, int x) {
+    return xyz[x * b.fs + lidx(b, ii, jj, kk)];
+}
+
+// ------------------------------------------------------------ layout copies
+// Fortran array (n0 x n1 x n2 x nc, i fastest) <-> box (fs-strided components)
+template <class T>
+__global__ void k_f2box(GamBox b, const double* __restrict__ src, T* __restrict__ dst, int n0, int n1, int n2,
+                        int nc) {
+    int i, j, k;
+    if (!tid3(n0, n1, n2, i, j, k)) return;
+    for (int c = 0; c < nc; c++) {
+        long s = (long)i + (long)n0 * (j + (long)n1 * (k + (long)n2 * c));
+        dst[c * b.fs + lidx(b, i, j, k)] = (T)src[s];
+    }
+}
+template <class T>
+__global__ void k_box2f(GamBox b, const T* __restrict__ src, double* __restrict__ dst, int n0, int n1, int n2,
+                        int nc) {
+    int i, j, k;
+    if (!tid3(n0, n1, n2, i, j, k)) return;
+    for (int c = 0; c < nc; c++) {
+        long s = (long)i + (long)n0 * (j + (long)n1 * (k + (long)n2 * c));
+        dst[s] = (double)src[c * b.fs + lidx(b, i, j, k)];
+    }
+}
+__global__ void k_fill(double* p, long n, double v) {
+    long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (t < n) p[t] = v;
+}
+__global__ void k_d2f(const double* __restrict__ s, float* __restrict__ d, long n) {
+    long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (t < n) d[t] = (float)s[t];
+}
+
+// ------------------------------------------------------------ metric
+// Face area, centroid and triad (init.F90:843-905, quadrature.F90:159-221)
+__global__ void k_geo_faces(GamBox b, const double* __restrict__ xyz, double* face, double* xfc, double* Tf, int d) {
+    int ii, jj, kk;
+    const int dI = d == 0, dJ = d == 1, dK = d == 2;
+    if (!tid3(b.Ni + dI, b.Nj + dJ, b.Nk + dK, ii, jj, kk)) return;
+    int a1[3] = {0, 0, 0}, a2[3] = {0, 0, 0};
+    if (d == 0) { a1[1] = 1; a2[2] = 1; }
+    else if (d == 1) { a1[2] = 1; a2[0] = 1; }
+    else { a1[0] = 1; a2[1] = 1; }
+    double f0[3], f1[3], f2[3], f3[3];
+    for (int x = 0; x < 3; x++) {
+        f0[x] = X(b, xyz, ii, jj, kk, x);
+        f1[x] = X(b, xyz, ii + a1[0], jj + a1[1], kk + a1[2], x);
+        f2[x] = X(b, xyz, ii + a2[0], jj + a2[1], kk + a2[2], x);
+        f3[x] = X(b, xyz, ii + a1[0] + a2[0], jj + a1[1] + a2[1], kk + a1[2] + a2[2], x);
+    }
+    double dx[3], dy[3], dz[3];
+    dx[0] = f1[0] - f0[0]; dx[1] = f2[0] - f0[0]; dx[2] = f3[0] + f0[0] - f2[0] - f1[0];
+    dy[0] = f1[1] - f0[1]; dy[1] = f2[1] - f0[1]; dy[2] = f3[1] + f0[1] - f2[1] - f1[1];
+    dz[0] = f1[2] - f0[2]; dz[1] = f2[2] - f0[2]; dz[2] = f3[2] + f0[2] - f2[2] - f1[2];
+    double fA = 0.0, m[3] = {0.0, 0.0, 0.0};
+    double A1[3] = {0.0, 0.0, 0.0};
+    for (int i = 0; i < 12; i++)
+        for (int j = 0; j < 12; j++) {
+            double eta = 0.5 * (1 + c_gA[i]), psi = 0.5 * (1 + c_gA[j]);
+            double w = c_gW[i] * c_gW[j];
+            double xp = f0[0] + dx[0] * eta + dx[1] * psi + dx[2] * eta * psi;
+            double yp = f0[1] + dy[0] * eta + dy[1] * psi + dy[2] * eta * psi;
+            double zp = f0[2] + dz[0] * eta + dz[1] * psi + dz[2] * eta * psi;
+            double etaV[3] = {dx[0] + dx[2] * psi, dy[0] + dy[2] * psi, dz[0] + dz[2] * psi};
+            double psiV[3] = {dx[1] + dx[2] * eta, dy[1] + dy[2] * eta, dz[1] + dz[2] * eta};
+            double c[3];
+            cross3(etaV, psiV, c);
+            double area = 0.25 * norm2s(c) * w;
+            A1[0] = A1[0] + area * 1.0;  // IdVec integrand: area in component 1
+            m[0] = m[0] + area * xp;
+            m[1] = m[1] + area * yp;
+            m[2] = m[2] + area * zp;
+        }
+    fA = A1[0];
+    const long cI = lidx(b, ii, jj, kk);
+    for (int x = 0; x < 3; x++) xfc[(x + 3 * d) * b.fs + cI] = m[x] / fA;
+    face[d * b.fs + cI] = fA;
+    double dT1[3], dT2[3];
+    for (int x = 0; x < 3; x++) {
+        if (d == 0) {
+            dT1[x] = 0.5 * (X(b, xyz, ii, jj + 1, kk + 1, x) - X(b, xyz, ii, jj, kk + 1, x)) +
+                     0.5 * (X(b, xyz, ii, jj + 1, kk, x) - X(b, xyz, ii, jj, kk, x));
+            dT2[x] = 0.5 * (X(b, xyz, ii, jj + 1, kk + 1, x) - X(b, xyz, ii, jj + 1, kk, x)) +
+                     0.5 * (X(b, xyz, ii, jj, kk + 1, x) - X(b, xyz, ii, jj, kk, x));
+        } else if (d == 1) {
+            dT1[x] = 0.5 * (X(b, xyz, ii + 1, jj, kk + 1, x) - X(b, xyz, ii + 1, jj, kk, x)) +
+                     0.5 * (X(b, xyz, ii, jj, kk + 1, x) - X(b, xyz, ii, jj, kk, x));
+            dT2[x] = 0.5 * (X(b, xyz, ii + 1, jj, kk + 1, x) - X(b, xyz, ii, jj, kk + 1, x)) +
+                     0.5 * (X(b, xyz, ii + 1, jj, kk, x) - X(b, xyz, ii, jj, kk, x));
+        } else {
+            dT1[x] = 0.5 * (X(b, xyz, ii + 1, jj + 1, kk, x) - X(b, xyz, ii, jj + 1, kk, x)) +
+                     0.5 * (X(b, xyz, ii + 1, jj, kk, x) - X(b, xyz, ii, jj, kk, x));
+            dT2[x] = 0.5 * (X(b, xyz, ii + 1, jj + 1, kk, x) - X(b, xyz, ii + 1, jj, kk, x)) +
+                     0.5 * (X(b, xyz, ii, jj + 1, kk, x) - X(b, xyz, ii, jj, kk, x));
+        }
+    }
+    double c[3], eN[3], eT1[3], eT2[3], c2[3];
+    cross3(dT1, dT2, c);
+    double nc = norm2s(c);
+    for (int x = 0; x < 3; x++) eN[x] = c[x] / nc;
+    double n2 = norm2s(dT2);
+    for (int x = 0; x < 3; x++) eT2[x] = dT2[x] / n2;
+    cross3(eT2, eN, c2);
+    double nc2 = norm2s(c2);
+    for (int x = 0; x < 3; x++) eT1[x] = c2[x] / nc2;
+    for (int x = 0; x < 3; x++) {
+        Tf[(0 + x + 9 * d) * b.fs + cI] = eN[x];
+        Tf[(3 + x + 9 * d) * b.fs + cI] = eT1[x];
+        Tf[(6 + x + 9 * d) * b.fs + cI] = eT2[x];
+    }
+}
+
+__device__ __forceinline__ double detJ(const double J[3][3]) {
+    return J[0][0] * (J[1][1] * J[2][2] - J[1][2] * J[2][1]) - J[0][1] * (J[1][0] * J[2][2] - J[1][2] * J[2][0]) +
+           J[0][2] * (J[1][0] * J[2][1] - J[1][1] * J[2][0]);
+}
+__device__ __forceinline__ void cell_corners(const GamBox& b, const double* xyz, int ii, int jj, int kk,
+                                             double C[8][3]) {
+    const int o[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0}, {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
+    for (int n = 0; n < 8; n++)
+        for (int x = 0; x < 3; x++) C[n][x] = X(b, xyz, ii + o[n][0], jj + o[n][1], kk + o[n][2], x);
+}
+// One point of GaussianVolumeIntegral (quadrature.F90:42-100): position and
+// Jacobian weight dJ*wijk of Gauss point (i,j,k)
+__device__ __forceinline__ void gauss_point(const double C[8][3], int i, int j, int k, double* xp, double& wgt) {
+    const int iS[8] = {-1, +1, +1, -1, -1, +1, +1, -1};
+    const int jS[8] = {-1, -1, +1, +1, -1, -1, +1, +1};
+    const int kS[8] = {-1, -1, -1, -1, +1, +1, +1, +1};
+    double wijk = c_gW[i] * c_gW[j] * c_gW[k];
+    double iScl[8], jScl[8], kScl[8];
+    for (int n = 0; n < 8; n++) {
+        iScl[n] = iS[n] < 0 ? 1 - c_gA[i] : 1 + c_gA[i];
+        jScl[n] = jS[n] < 0 ? 1 - c_gA[j] : 1 + c_gA[j];
+        kScl[n] = kS[n] < 0 ? 1 - c_gA[k] : 1 + c_gA[k];
+    }
+    double J[3][3];
+    for (int x = 0; x < 3; x++) {
+        double s = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+        for (int n = 0; n < 8; n++) s += C[n][x] * (iScl[n] * jScl[n] * kScl[n]);
+        for (int n = 0; n < 8; n++) s1 += C[n][x] * ((double)iS[n] * jScl[n] * kScl[n]);
+        for (int n = 0; n < 8; n++) s2 += C[n][x] * (iScl[n] * (double)jS[n] * kScl[n]);
+        for (int n = 0; n < 8; n++) s3 += C[n][x] * (iScl[n] * jScl[n] * (double)kS[n]);
+        xp[x] = 0.125 * s;
+        J[x][0] = 0.125 * s1;
+        J[x][1] = 0.125 * s2;
+        J[x][2] = 0.125 * s3;
+    }
+    double dJ = fabs(detJ(J));
+    wgt = dJ * wijk;
+}
+// Volume and barycentre (init.F90:912-940)
+__global__ void k_geo_cells(GamBox b, const double* __restrict__ xyz, double* vol, double* xyzcc) {
+    int ii, jj, kk;
+    if (!tid3(b.Ni, b.Nj, b.Nk, ii, jj, kk)) return;
+    double C[8][3];
+    cell_corners(b, xyz, ii, jj, kk, C);
+    double I[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int i = 0; i < 12; i++)
+        for (int j = 0; j < 12; j++)
+            for (int k = 0; k < 12; k++) {
+                double xp[3], wg;
+                gauss_point(C, i, j, k, xp, wg);
+                I[0] = I[0] + wg * 1.0;
+                I[1] = I[1] + wg * xp[0];
+                I[2] = I[2] + wg * xp[1];
+                I[3] = I[3] + wg * xp[2];
+            }
+    const long c = lidx(b, ii, jj, kk);
+    vol[c] = I[0];
+    for (int x = 0; x < 3; x++) xyzcc[x * b.fs + c] = I[1 + x] / I[0];
+}
+// CFL lengths di,dj,dk (init.F90:944-957) and their minimum
+__global__ void k_geo_dijk(GamBox b, const double* __restrict__ vol, const double* __restrict__ face, double* dijk,
+                           double* dl) {
+    int ii, jj, kk;
+    if (!tid3(b.Ni, b.Nj, b.Nk, ii, jj, kk)) return;
+    const long c = lidx(b, ii, jj, kk);
+    const long fs = b.fs;
+    double fA = fmax(face[c + 1], face[c]);
+    double di = vol[c] / fA;
+    fA = fmax(face[fs + c + b.sx], face[fs + c]);
+    double dj = vol[c] / fA;
+    fA = fmax(face[2 * fs + c + b.sk], face[2 * fs + c]);
+    double dk = vol[c] / fA;
+    dijk[c] = di;
+    dijk[fs + c] = dj;
+    dijk[2 * fs + c] = dk;
+    double m = di;
+    if (dj < m) m = dj;
+    if (dk < m) m = dk;
+    dl[c] = m;
+}
+// Edge length and triad (init.F90:958-1041)
+__global__ void k_geo_edges(GamBox b, const double* __restrict__ xyz, double* edge, double* Te, int d) {
+    int a0, a1, a2;
+    // ranges: is..ie, js..je, ks..ke in box coordinates (maximal bounds, init.F90:963-987)
+    int is = 0, ie = b.Ni, js = 0, je = b.Nj, ks = 0, ke = b.Nk;
+    if (d == 0) { ie = b.Ni - 1; ks = 1; ke = b.Nk - 1; }
+    else if (d == 1) { je = b.Nj - 1; is = 1; ie = b.Ni - 1; }
+    else { ke = b.Nk - 1; js = 1; je = b.Nj - 1; }
+    if (!tid3(ie - is + 1, je - js + 1, ke - ks + 1, a0, a1, a2)) return;
+    const int ii = is + a0, jj = js + a1, kk = ks + a2;
+    double dEdge[3], eAvg[3];
+    for (int x = 0; x < 3; x++) {
+        if (d == 0) {
+            dEdge[x] = X(b, xyz, ii + 1, jj, kk, x) - X(b, xyz, ii, jj, kk, x);
+            eAvg[x] = 0.5 * (X(b, xyz, ii, jj, kk + 1, x) - X(b, xyz, ii, jj, kk - 1, x) + X(b, xyz, ii + 1, jj, kk + 1, x) -
+                             X(b, xyz, ii + 1, jj, kk - 1, x));
+        } else if (d == 1) {
+            dEdge[x] = X(b, xyz, ii, jj + 1, kk, x) - X(b, xyz, ii, jj, kk, x);
+            eAvg[x] = 0.5 * (X(b, xyz, ii + 1, jj, kk, x) - X(b, xyz, ii - 1, jj, kk, x) + X(b, xyz, ii + 1, jj + 1, kk, x) -
+                             X(b, xyz, ii - 1, jj + 1, kk, x));
+        } else {
+            dEdge[x] = X(b, xyz, ii, jj, kk + 1, x) - X(b, xyz, ii, jj, kk, x);
+            eAvg[x] = 0.5 * (X(b, xyz, ii, jj + 1, kk, x) - X(b, xyz, ii, jj - 1, kk, x) + X(b, xyz, ii, jj + 1, kk + 1, x) -
+                             X(b, xyz, ii, jj - 1, kk + 1, x));
+        }
+    }
+    double eN[3], eT1[3], eT2[3], c[3];
+    double nE = norm2s(dEdge);
+    for (int x = 0; x < 3; x++) eN[x] = dEdge[x] / nE;
+    cross3(eAvg, eN, c);
+    double nc = norm2s(c);
+    for (int x = 0; x < 3; x++) eT1[x] = c[x] / nc;
+    cross3(eN, eT1, c);
+    nc = norm2s(c);
+    for (int x = 0; x < 3; x++) eT2[x] = c[x] / nc;
+    const long ci = lidx(b, ii, jj, kk);
+    edge[d * b.fs + ci] = norm2s(dEdge);
+    for (int x = 0; x < 3; x++) {
+        Te[(0 + x + 9 * d) * b.fs + ci] = eN[x];
+        Te[(3 + x + 9 * d) * b.fs + ci] = eT1[x];
+        Te[(6 + x + 9 * d) * b.fs + ci] = eT2[x];
+    }
+}
+// ebGeom (init.F90:1075-1137): edge B maps over active edges
+__global__ void k_geo_teb(GamBox b, const double* __restrict__ face, const double* __restrict__ Tf,
+                          const double* __restrict__ Te, double* Teb, int c0, int dNorm, int dT1, int dT2) {
+    int a0, a1, a2;
+    const int G = GAM_NG;
+    if (!tid3(b.Nip + 1, b.Njp + 1, b.Nkp + 1, a0, a1, a2)) return;
+    const int ii = G + a0, jj = G + a1, kk = G + a2;
+    const long c = lidx(b, ii, jj, kk);
+    const long fs = b.fs;
+    const long s = dT2 == 0 ? 1L : (dT2 == 1 ? (long)b.sx : b.sk);
+    const double w6[8] = {0.0 / 60.0, 1.0 / 60.0, -8.0 / 60.0, 37.0 / 60.0, 37.0 / 60.0, -8.0 / 60.0, 1.0 / 60.0, 0.0 / 60.0};
+    double fA[8];
+    for (int n = 0; n < 8; n++) fA[n] = face[dT1 * fs + c + (n - 4) * s];
+    double fAi = 0.0;
+    for (int n = 0; n < 8; n++) fAi += w6[n] * fA[n];
+    double Nec[3];
+    for (int x = 0; x < 3; x++) {
+        double acc = 0.0;
+        for (int n = 0; n < 8; n++) acc += (Tf[(x + 9 * dT1) * fs + c + (n - 4) * s] * fA[n]) * w6[n];
+        Nec[x] = acc / fAi;
+    }
+    double t1[3], t2[3];
+    for (int x = 0; x < 3; x++) {
+        t1[x] = Te[(3 + x + 9 * dNorm) * fs + c];
+        t2[x] = Te[(6 + x + 9 * dNorm) * fs + c];
+    }
+    double dxT = 0.0, dyT = 0.0;
+    for (int x = 0; x < 3; x++) dxT += Nec[x] * t1[x];
+    for (int x = 0; x < 3; x++) dyT += Nec[x] * t2[x];
+    double dScl = sqrt(dxT * dxT + dyT * dyT);
+    if (dScl <= TINY) dScl = 1.0;
+    Teb[(c0 + 0 + 4 * dNorm) * fs + c] = dxT / dScl;
+    Teb[(c0 + 1 + 4 * dNorm) * fs + c] = dyT / dScl;
+}
+
+// ------------------------------------------------------------ problems
+// initOT2D (prob.F90:74-119) over is..ie+1 (x) js..je+1 (x) ks..ke+1
+__global__ void k_ic_ot(GamBox b, const double* __restrict__ xyzcc, const double* __restrict__ face, double* Gas,
+                        double* mf, double gamma) {
+    int a0, a1, a2;
+    const int G = GAM_NG;
+    if (!tid3(b.Nip + 1, b.Njp + 1, b.Nkp + 1, a0, a1, a2)) return;
+    const long c = lidx(b, G + a0, G + a1, G + a2);
+    const long fs = b.fs;
+    const double PI = 3.141592653589793;
+    double Rho0 = 25.0 / (36.0 * PI), P0 = 5 / (12.0 * PI), B0 = 1 / sqrt(4.0 * PI);
+    double xc = xyzcc[c], yc = xyzcc[fs + c];
+    double Vx = -sin(2 * PI * yc), Vy = sin(2 * PI * xc), Vz = 0.0;
+    double KinE = 0.5 * Rho0 * (Vx * Vx + Vy * Vy + Vz * Vz);
+    Gas[c] = Rho0;
+    Gas[fs + c] = Vx * Rho0;
+    Gas[2 * fs + c] = Vy * Rho0;
+    Gas[3 * fs + c] = Vz * Rho0;
+    Gas[4 * fs + c] = KinE + P0 / (gamma - 1);
+    mf[c] = (-B0 * sin(2 * PI * yc)) * face[c];
+    mf[fs + c] = (B0 * sin(4 * PI * xc)) * face[fs + c];
+    mf[2 * fs + c] = 0.0;
+}
+// GasIC2State with the blast-wave profile (prob.F90:280-297) on active cells
+__global__ void k_ic_bw_gas(GamBox b, const double* __restrict__ xyz, const double* __restrict__ vol, double* Gas,
+                            double gamma, double x0, double y0, double z0, double D0, double P0, double pRat,
+                            double dRat, double rC) {
+    int a0, a1, a2;
+    const int G = GAM_NG;
+    if (!tid3(b.Nip, b.Njp, b.Nkp, a0, a1, a2)) return;
+    const int ii = G + a0, jj = G + a1, kk = G + a2;
+    double C[8][3];
+    cell_corners(b, xyz, ii, jj, kk, C);
+    double I[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int i = 0; i < 12; i++)
+        for (int j = 0; j < 12; j++)
+            for (int k = 0; k < 12; k++) {
+                double xp[3], wg;
+                gauss_point(C, i, j, k, xp, wg);
+                double R = sqrt((xp[0] - x0) * (xp[0] - x0) + (xp[1] - y0) * (xp[1] - y0) + (xp[2] - z0) * (xp[2] - z0));
+                double Dv = D0, Pv = P0;
+                if (R <= rC) { Dv = dRat * Dv; Pv = pRat * Pv; }
+                double Wp[5] = {Dv, 0.0, 0.0, 0.0, Pv};
+                for (int v = 0; v < 5; v++) I[v] = I[v] + wg * Wp[v];
+            }
+    const long c = lidx(b, ii, jj, kk);
+    const long fs = b.fs;
+    double dV = vol[c];
+    for (int v = 0; v < 5; v++) I[v] = I[v] / dV;
+    double D = I[0];
+    double Mx = D * I[1], My = D * I[2], Mz = D * I[3];
+    double P = I[4];
+    double KinE = 0.5 * (Mx * Mx + My * My + Mz * Mz) / D;
+    double IntE = P / (gamma - 1.0);
+    Gas[c] = D;
+    Gas[fs + c] = Mx;
+    Gas[2 * fs + c] = My;
+    Gas[3 * fs + c] = Mz;
+    Gas[4 * fs + c] = IntE + KinE;
+}
+// VectorPot2Flux edge integrals of A = (0, bSclz x, bScl (y - x)) (gridutils.F90:193-237)
+__device__ __forceinline__ double edge_int_dot(const double* e1, const double* e2, double bScl, double bSclz) {
+    double dR2[3], xBar[3], eInt[3] = {0.0, 0.0, 0.0};
+    for (int x = 0; x < 3; x++) { dR2[x] = 0.5 * (e2[x] - e1[x]); xBar[x] = 0.5 * (e2[x] + e1[x]); }
+    for (int i = 0; i < 12; i++) {
+        double xp[3];
+        for (int x = 0; x < 3; x++) xp[x] = xBar[x] + c_gA[i] * dR2[x];
+        double Ap[3] = {0.0, bSclz * xp[0], bScl * (xp[1] - xp[0])};
+        for (int x = 0; x < 3; x++) eInt[x] = eInt[x] + 0.5 * c_gW[i] * Ap[x];
+    }
+    double s = 0.0;  // dot_product(eInt, e1 - e2) with e1 the far corner
+    for (int x = 0; x < 3; x++) s += eInt[x] * (e1[x] - e2[x]);
+    return s;
+}
+__global__ void k_ic_bw_lA(GamBox b, const double* __restrict__ xyz, double* lA, double bScl, double bSclz) {
+    int ii, jj, kk;
+    if (!tid3(b.Ni - 1, b.Nj - 1, b.Nk - 1, ii, jj, kk)) return;
+    double e0[3], eI[3], eJ[3], eK[3];
+    for (int x = 0; x < 3; x++) {
+        e0[x] = X(b, xyz, ii, jj, kk, x);
+        eI[x] = X(b, xyz, ii + 1, jj, kk, x);
+        eJ[x] = X(b, xyz, ii, jj + 1, kk, x);
+        eK[x] = X(b, xyz, ii, jj, kk + 1, x);
+    }
+    const long c = lidx(b, ii, jj, kk);
+    lA[c] = edge_int_dot(eI, e0, bScl, bSclz);
+    lA[b.fs + c] = edge_int_dot(eJ, e0, bScl, bSclz);
+    lA[2 * b.fs + c] = edge_int_dot(eK, e0, bScl, bSclz);
+}
+__global__ void k_ic_bw_flux(GamBox b, const double* __restrict__ lA, double* mf) {
+    int ii, jj, kk;
+    if (!tid3(b.Ni - 1, b.Nj - 1, b.Nk - 1, ii, jj, kk)) return;
+    const long c = lidx(b, ii, jj, kk), fs = b.fs, sj = b.sx, sk = b.sk;
+    const double* I = lA;
+    const double* J = lA + fs;
+    const double* K = lA + 2 * fs;
+    mf[c] = J[c] - J[c + sk] + K[c + sj] - K[c];
+    mf[fs + c] = -(I[c] - I[c + sk] + K[c + 1] - K[c]);
+    mf[2 * fs + c] = I[c] - I[c + sj] + J[c + 1] - J[c];
+}
+
+}  // namespace gam_geom
+
+// ------------------------------------------------------------ host wrappers
+using namespace gam_geom;
+
+static inline dim3 g3(int n0, int n1, int n2, dim3 blk) {
+    return dim3((n0 + blk.x - 1) / blk.x, (n1 + blk.y - 1) / blk.y, (n2 + blk.z - 1) / blk.z);
+}
+
+void gam_geom_fortran_to_box_d(const GamBox& b, const double* src, double* dst, bool face, int nc, cudaStream_t s) {
+    dim3 blk(32, 4, 1);
+    int n0 = b.Ni + face, n1 = b.Nj + face, n2 = b.Nk + face;
+    k_f2box<double><<<g3(n0, n1, n2, blk), blk, 0, s>>>(b, src, dst, n0, n1, n2, nc);
+}
+void gam_geom_fortran_to_box_f(const GamBox& b, const double* src, float* dst, bool face, int nc, cudaStream_t s) {
+    dim3 blk(32, 4, 1);
+    int n0 = b.Ni + face, n1 = b.Nj + face, n2 = b.Nk + face;
+    k_f2box<float><<<g3(n0, n1, n2, blk), blk, 0, s>>>(b, src, dst, n0, n1, n2, nc);
+}
+void gam_geom_box_to_fortran_d(const GamBox& b, const double* src, double* dst, bool face, int nc, cudaStream_t s) {
+    dim3 blk(32, 4, 1);
+    int n0 = b.Ni + face, n1 = b.Nj + face, n2 = b.Nk + face;
+    k_box2f<double><<<g3(n0, n1, n2, blk), blk, 0, s>>>(b, src, dst, n0, n1, n2, nc);
+}
+void gam_geom_box_to_fortran_f(const GamBox& b, const float* src, double* dst, bool face, int nc, cudaStream_t s) {
+    dim3 blk(32, 4, 1);
+    int n0 = b.Ni + face, n1 = b.Nj + face, n2 = b.Nk + face;
+    k_box2f<float><<<g3(n0, n1, n2, blk), blk, 0, s>>>(b, src, dst, n0, n1, n2, nc);
+}
+void gam_geom_fill(double* p, long n, double v, cudaStream_t s) {
+    if (n > 0) k_fill<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(p, n, v);
+}
+void gam_geom_d2f(const double* src, float* dst, long n, cudaStream_t s) {
+    if (n > 0) k_d2f<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(src, dst, n);
+}
+
+// Metric from corners already in the box layout (xyz: 3 comps).
+// dijk: 3 comps; dl: min(di,dj,dk).
+void gam_geom_metric(const GamBox& b, const double* xyz, double* face, double* xfc, double* Tf, double* vol,
+                     double* xyzcc, double* dijk, double* dl, double* edge, double* Te, double* Teb, cudaStream_t s) {
+    const long fs = b.fs;
+    gam_geom_fill(face, 3 * fs, 1.0, s);
+    gam_geom_fill(xfc, 9 * fs, 0.0, s);
+    gam_geom_fill(Tf, 27 * fs, 0.0, s);
+    gam_geom_fill(edge, 3 * fs, 1.0, s);
+    gam_geom_fill(Te, 27 * fs, 0.0, s);
+    gam_geom_fill(Teb, 12 * fs, 1.0, s);
+    dim3 blk(32, 4, 1);
+    for (int d = 0; d < 3; d++)
+        k_geo_faces<<<g3(b.Ni + (d == 0), b.Nj + (d == 1), b.Nk + (d == 2), blk), blk, 0, s>>>(b, xyz, face, xfc, Tf, d);
+    dim3 blkv(64, 1, 1);
+    k_geo_cells<<<g3(b.Ni, b.Nj, b.Nk, blkv), blkv, 0, s>>>(b, xyz, vol, xyzcc);
+    k_geo_dijk<<<g3(b.Ni, b.Nj, b.Nk, blk), blk, 0, s>>>(b, vol, face, dijk, dl);
+    for (int d = 0; d < 3; d++) k_geo_edges<<<g3(b.Ni + 1, b.Nj + 1, b.Nk + 1, blk), blk, 0, s>>>(b, xyz, edge, Te, d);
+    for (int dN = 0; dN < 3; dN++) {
+        int T1 = (dN + 1) % 3, T2 = (dN + 2) % 3;
+        k_geo_teb<<<g3(b.Nip + 1, b.Njp + 1, b.Nkp + 1, blk), blk, 0, s>>>(b, face, Tf, Te, Teb, 0, dN, T1, T2);
+        k_geo_teb<<<g3(b.Nip + 1, b.Njp + 1, b.Nkp + 1, blk), blk, 0, s>>>(b, face, Tf, Te, Teb, 2, dN, T2, T1);
+    }
+}
+
+void gam_geom_ic_ot(const GamBox& b, const double* xyzcc, const double* face, double* Gas, double* mf, double gamma,
+                    cudaStream_t s) {
+    dim3 blk(32, 4, 1);
+    k_ic_ot<<<g3(b.Nip + 1, b.Njp + 1, b.Nkp + 1, blk), blk, 0, s>>>(b, xyzcc, face, Gas, mf, gamma);
+}
+// bw: x0,y0,z0,D0,P0,pRat,dRat,rC,B0; lA: 3-component scratch
+void gam_geom_ic_bw(const GamBox& b, const double* xyz, const double* vol, double* Gas, double* mf, double* lA,
+                    double gamma, const double* bw, bool doMHD, cudaStream_t s) {
+    dim3 blkv(64, 1, 1);
+    k_ic_bw_gas<<<g3(b.Nip, b.Njp, b.Nkp, blkv), blkv, 0, s>>>(b, xyz, vol, Gas, gamma, bw[0], bw[1], bw[2], bw[3], bw[4],
+                                                              bw[5], bw[6], bw[7]);
+    if (!doMHD) return;
+    const double bScl = bw[8] / (double)sqrtf(2.0f);  // prob.F90:252 divides by the default-real sqrt(2.0)
+    gam_geom_fill(lA, 3 * b.fs, 0.0, s);
+    dim3 blk(32, 4, 1);
+    k_ic_bw_lA<<<g3(b.Ni - 1, b.Nj - 1, b.Nk - 1, blk), blk, 0, s>>>(b, xyz, lA, bScl, 0.0);
+    k_ic_bw_flux<<<g3(b.Ni - 1, b.Nj - 1, b.Nk - 1, blk), blk, 0, s>>>(b, lA, mf);
+}

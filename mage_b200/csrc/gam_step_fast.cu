@@ -1,0 +1,11 @@
+// Step kernels of the product path (FMA contraction on): FP64 drop-in form
+// and FP32 precision form.
+#define GAM_NS gam_fast
+#include "gam_step_impl.cuh"
+
+void gam_fast_step_f64(const Ctx<double>& C, int cur, cudaStream_t s) { gam_fast::launch_step<double>(C, cur, s); }
+void gam_fast_dt_f64(const Ctx<double>& C, int cur, cudaStream_t s) { gam_fast::launch_dt_only<double>(C, cur, s); }
+void gam_fast_step_f32(const Ctx<float>& C, int cur, cudaStream_t s) { gam_fast::launch_step<float>(C, cur, s); }
+void gam_fast_dt_f32(const Ctx<float>& C, int cur, cudaStream_t s) { gam_fast::launch_dt_only<float>(C, cur, s); }
+void gam_fast_init_f64(const Ctx<double>& C, int cur, cudaStream_t s) { gam_fast::launch_init<double>(C, cur, s); }
+void gam_fast_init_f32(const Ctx<float>& C, int cur, cudaStream_t s) { gam_fast::launch_init<float>(C, cur, s); }

@@ -1,0 +1,923 @@
+// Kernels of one GAMERA MHD time step on sm_100a.
+//
+// This header is compiled twice (gam_step_strict.cu without FMA contraction,
+// gam_step_fast.cu with it) inside the namespace named by GAM_NS, and each
+// kernel is templated on the real type R of the bulk data (double for the
+// drop-in form, float for the precision form; scalars, the dt reduction and
+// the totals stay double).
+//
+// Step = stepGamera (gamapp.F90:73-91):
+//   k_step_begin     AdvanceMHD time trap, AB2 spacing      (mhdgroup.F90:25-31, 457)
+//   k_predict        Predictor/PredictCell/ExtrapAB2 + bFlux2Fld of the
+//                    half state; per-cell primitives of both states and
+//                    per-face B = flux/area, computed once for all stencils
+//                                                           (mhdgroup.F90:444-615)
+//   k_mom2face(eD)   Mom2Face                               (fields.F90:235-285)
+//   k_vxb(eD)        GetCornerV/D/B, EdgeLRs, edge EMF      (fields.F90:184-228, 288-517)
+//   k_stress(d)      Fluxes: recon + PDM, MagKinFlux, GasKinFlux, HOGS
+//                                                           (stress.F90:204-599, recon.F90)
+//   k_update_faces   E2Flux on the new buffer               (fields.F90:18-51)
+//   k_update_cells   Flux2Deltas, CellReynolds, bFlux2Fld, CellMaxwell, and the
+//                    per-cell CFL dt with a block min       (stress.F90:148-194,
+//                    mhdgroup.F90:79-329, gridutils.F90:49-106)
+//   k_dt_finalize    time bookkeeping + CalcDT checks       (gamapp.F90:110-111, step.F90:58-168)
+//   k_bc_periodic    EnforceBCs (periodic / none) fused with bFlux2Fld of
+//                    the cells whose faces changed          (bcs.F90:279-450, gamapp.F90:86-88)
+//
+// Every expression keeps the reference's evaluation order (Fortran a+b+c is
+// (a+b)+c, x**2.0 is x*x, dot_product is a sequential sum from 0), so the
+// strict build reproduces an IEEE-strict CPU step bit for bit.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "gam_layout.cuh"
+#include "gam_math.cuh"
+#include "gam_types.cuh"
+
+#ifndef GAM_NS
+#error "GAM_NS must name the namespace of this build"
+#endif
+
+namespace GAM_NS {
+
+static constexpr double TINY = 1.0e-12;
+static constexpr double HUGE_DT = 1.0e12;
+static constexpr double PI_D = 3.141592653589793;
+
+// interpolation weights (recon.F90:22-23, 28-29)
+__device__ __forceinline__ double w8(int n) {
+    switch (n) {
+        case 0: return -3.0 / 840.0;
+        case 1: return 29.0 / 840.0;
+        case 2: return -139.0 / 840.0;
+        case 3: return 533.0 / 840.0;
+        case 4: return 533.0 / 840.0;
+        case 5: return -139.0 / 840.0;
+        case 6: return 29.0 / 840.0;
+        default: return -3.0 / 840.0;
+    }
+}
+__device__ __forceinline__ double up7c(int n) {
+    switch (n) {
+        case 0: return -3.0 / 420.0;
+        case 1: return 25.0 / 420.0;
+        case 2: return -101.0 / 420.0;
+        case 3: return 319.0 / 420.0;
+        case 4: return 214.0 / 420.0;
+        case 5: return -38.0 / 420.0;
+        default: return 4.0 / 420.0;
+    }
+}
+
+template <class R> __device__ __forceinline__ R Rc(double x) { return (R)x; }
+
+template <class R> struct Mth;
+template <> struct Mth<double> {
+    static __device__ __forceinline__ double erfc_(double x) { return gam::gam_erfc(x); }
+    static __device__ __forceinline__ double exp_(double x) { return gam::gam_exp(x); }
+    static __device__ __forceinline__ double sqrt_(double x) { return sqrt(x); }
+};
+template <> struct Mth<float> {
+    static __device__ __forceinline__ float erfc_(float x) { return erfcf(x); }
+    static __device__ __forceinline__ float exp_(float x) { return expf(x); }
+    static __device__ __forceinline__ float sqrt_(float x) { return sqrtf(x); }
+};
+
+// std::max / std::min semantics: max(a,b) = (a < b) ? b : a, min(a,b) = (b < a) ? b : a
+template <class R> __device__ __forceinline__ R rmax(R a, R b) { return (a < b) ? b : a; }
+template <class R> __device__ __forceinline__ R rmin(R a, R b) { return (b < a) ? b : a; }
+template <class R> __device__ __forceinline__ R sgn1(R b) { return copysign((R)1, b); }
+
+__device__ __forceinline__ bool thread_ijk(const Range& r, int& ii, int& jj, int& kk) {
+    ii = r.i0 + blockIdx.x * blockDim.x + threadIdx.x;
+    jj = r.j0 + blockIdx.y * blockDim.y + threadIdx.y;
+    kk = r.k0 + blockIdx.z * blockDim.z + threadIdx.z;
+    return ii <= r.i1 && jj <= r.j1 && kk <= r.k1;
+}
+
+__device__ __forceinline__ long lidx(const GamBox& b, int ii, int jj, int kk) {
+    return (long)ii + (long)b.sx * jj + b.sk * kk;
+}
+__device__ __forceinline__ long dstride(const GamBox& b, int d) { return d == 0 ? 1L : (d == 1 ? (long)b.sx : b.sk); }
+
+// ----------------------------------------------------------------- recon
+// pdmLR (recon.F90:231-272) on a 4-point limiter stencil nq[0..3] = cells -2..1
+template <class R>
+__device__ __forceinline__ void pdm_lr(R pdmb, const R* v, R Qi, R& Ql, R& Qr) {
+    R v0 = v[0], v1 = v[1], v2 = v[2], v3 = v[3];
+    R maxV = rmax(v1, v2), minV = rmin(v1, v2);
+    R vN = rmax(minV, rmin(Qi, maxV));
+    R dv0 = pdmb * (v1 - v0), dv1 = pdmb * (v2 - v1), dv2 = pdmb * (v3 - v2);
+    R s0 = sgn1(dv0), s1 = sgn1(dv1), s2 = sgn1(dv2);
+    R q0 = fabs(s0 + s1), q1 = fabs(s1 + s2);
+    R dvL = vN - v1, dvR = v2 - vN;
+    Ql = vN - s1 * rmax((R)0, fabs(dvL) - q0 * fabs(dv0));
+    Qr = vN + s1 * rmax((R)0, fabs(dvR) - q1 * fabs(dv2));
+}
+// PDM (recon.F90:275-301)
+template <class R>
+__device__ __forceinline__ R pdm1(R pdmb, R q0, R q1, R q2, R qI) {
+    R maxQ = rmax(q1, q2), minQ = rmin(q1, q2);
+    R qN = rmax(minQ, rmin(qI, maxQ));
+    R dq0 = pdmb * (q1 - q0), dq1 = pdmb * (q2 - q1);
+    R s0 = sgn1(dq0), s1 = sgn1(dq1);
+    R s01 = fabs(s0 + s1);
+    R dqL = qN - q1;
+    return qN - s1 * rmax((R)0, fabs(dqL) - s01 * fabs(dq0));
+}
+// GetLRs = Cen8LRs (recon.F90:125-158) or Up7LRs (:162-198) on
+// dV[0..7] (cells -4..3), q[0..7], limiter nq[0..3], volume interpolant Vi.
+template <class R>
+__device__ __forceinline__ void get_lrs(const DevParams<R>& P, const R* dV, const R* q, const R* nq, R Vi, R& Ql,
+                                        R& Qr) {
+    R QdV[8];
+#pragma unroll
+    for (int n = 0; n < 8; n++) QdV[n] = dV[n] * q[n];
+    if (!P.up7) {
+        R s = (R)0;
+#pragma unroll
+        for (int n = 0; n < 8; n++) s += Rc<R>(w8(n)) * QdV[n];
+        R Qi = s / Vi;
+        pdm_lr(P.pdmb, nq, Qi, Ql, Qr);
+    } else {
+        R a = QdV[0] * Rc<R>(up7c(0));
+#pragma unroll
+        for (int n = 1; n < 7; n++) a = a + QdV[n] * Rc<R>(up7c(n));
+        R b = QdV[7] * Rc<R>(up7c(0));
+#pragma unroll
+        for (int n = 1; n < 7; n++) b = b + QdV[7 - n] * Rc<R>(up7c(n));
+        Ql = a / Vi;
+        Qr = b / Vi;
+        Ql = pdm1(P.pdmb, nq[0], nq[1], nq[2], Ql);
+        Qr = pdm1(P.pdmb, nq[3], nq[2], nq[1], Qr);
+    }
+}
+template <class R> __device__ __forceinline__ R central8(const R* q) {
+    R s = (R)0;
+#pragma unroll
+    for (int n = 0; n < 8; n++) s += Rc<R>(w8(n)) * q[n];
+    return s;
+}
+
+// ----------------------------------------------------------------- EOS
+// BlockCon2Prim (recon.F90:62-91)
+template <class R>
+__device__ __forceinline__ void block_c2p(const DevParams<R>& P, const R* U, R* W) {
+    R D = rmax(U[0], P.dFloor);
+    R Mx = U[1], My = U[2], Mz = U[3], E = U[4];
+    R KinE = (R)0.5 * (Mx * Mx + My * My + Mz * Mz) / D;
+    R Pr = rmax(P.gm1 * (E - KinE), P.pFloor);
+    W[0] = D;
+    W[1] = Mx / D;
+    W[2] = My / D;
+    W[3] = Mz / D;
+    W[4] = Pr;
+}
+// CellC2P (gamutils.F90:301-321)
+template <class R>
+__device__ __forceinline__ void cell_c2p(const DevParams<R>& P, const R* U, R* W) {
+    R rho = U[0];
+    R Vx = U[1] / rho, Vy = U[2] / rho, Vz = U[3] / rho;
+    R E = U[4];
+    R KinE = (R)0.5 * rho * (Vx * Vx + Vy * Vy + Vz * Vz);
+    W[0] = rmax(rho, P.dFloor);
+    W[1] = Vx;
+    W[2] = Vy;
+    W[3] = Vz;
+    W[4] = rmax(P.gm1 * (E - KinE), P.pFloor);
+}
+// CellP2C (gamutils.F90:362-383)
+template <class R>
+__device__ __forceinline__ void cell_p2c(const DevParams<R>& P, const R* W, R* U) {
+    R rho = rmax(W[0], P.dFloor);
+    R Vx = W[1], Vy = W[2], Vz = W[3];
+    R IntE = rmax(W[4], P.pFloor) / P.gm1;
+    R KinE = (R)0.5 * rho * (Vx * Vx + Vy * Vy + Vz * Vz);
+    U[0] = rho;
+    U[1] = rho * Vx;
+    U[2] = rho * Vy;
+    U[3] = rho * Vz;
+    U[4] = IntE + KinE;
+}
+
+// gamCellBxyz (gridutils.F90:648-680) from the six face fluxes of cell c
+template <class R>
+__device__ __forceinline__ void cell_bxyz(const GamBox& b, const Geo<R>& g, long c, R fI, R fIp, R fJ, R fJp, R fK,
+                                          R fKp, R* B) {
+    const long fs = b.fs;
+    R dV = g.vol[c];
+    R Div = fIp - fI + fJp - fJ + fKp - fK;
+#pragma unroll
+    for (int x = 0; x < 3; x++) {
+        R xfI = g.xfc[(x + 0) * fs + c];
+        R xfJ = g.xfc[(x + 3) * fs + c];
+        R xfK = g.xfc[(x + 6) * fs + c];
+        R xfIp = g.xfc[(x + 0) * fs + c + 1];
+        R xfJp = g.xfc[(x + 3) * fs + c + b.sx];
+        R xfKp = g.xfc[(x + 6) * fs + c + b.sk];
+        R t = (fIp * xfIp + fJp * xfJp + fKp * xfKp - fI * xfI - fJ * xfJ - fK * xfK) / dV;
+        B[x] = t - Div * g.xyzcc[x * fs + c] / dV;
+    }
+}
+
+// ----------------------------------------------------------------- kernels
+// AdvanceMHD entry: time trap and AB2 spacing (mhdgroup.F90:25-31, 457)
+__global__ void k_step_begin(GamScalars* sc) {
+    if (sc->halted) return;
+    if (fabs(sc->otime - sc->time) < TINY) sc->otime = sc->time - sc->dt;
+    sc->odt = sc->time - sc->otime;
+    sc->pdt = 0.5 * sc->dt;
+}
+
+// Predictor over every face and cell of the ghosted box.
+template <class R>
+__global__ void __launch_bounds__(256) k_predict(GamBox b, DevParams<R> P, Geo<R> g, StateBuf<R> cur,
+                                                 StateBuf<R> old, Work<R> w, const GamScalars* sc) {
+    if (sc->halted) return;
+    int ii, jj, kk;
+    Range r{0, b.Ni, 0, b.Nj, 0, b.Nk};
+    if (!thread_ijk(r, ii, jj, kk)) return;
+    const long fs = b.fs;
+    const long c = lidx(b, ii, jj, kk);
+    const R pdt = (R)sc->pdt, odt = (R)sc->odt;
+    const bool isCell = ii < b.Ni && jj < b.Nj && kk < b.Nk;
+    R hm[3];
+    if (P.doMHD) {
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            R Q = cur.mf[d * fs + c], oQ = old.mf[d * fs + c];
+            R dQ = (Q - oQ) / odt;
+            hm[d] = Q + pdt * dQ;  // ExtrapAB2
+            R A = g.face[d * fs + c];
+            R Am = rmax(A, (R)TINY);
+            w.bh[d * fs + c] = hm[d] / Am;
+            w.Bnf[d * fs + c] = hm[d] / A;
+            w.bn[d * fs + c] = Q / Am;
+        }
+    }
+    if (!isCell) return;
+    // PredictCell (mhdgroup.F90:528-562)
+    R Q[5], oQ[5], W[5], oW[5], pW[5], pQ[5];
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+        Q[v] = cur.Gas[v * fs + c];
+        oQ[v] = old.Gas[v * fs + c];
+    }
+    cell_c2p(P, oQ, oW);
+    cell_c2p(P, Q, W);
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+        R dQ = (W[v] - oW[v]) / odt;
+        pW[v] = W[v] + pdt * dQ;
+    }
+    pW[0] = rmax(pW[0], P.dFloor);
+    pW[4] = rmax(pW[4], P.pFloor);
+    cell_p2c(P, pW, pQ);
+    R Wh[5], Wn[5];
+    block_c2p(P, pQ, Wh);
+    block_c2p(P, Q, Wn);
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+        w.Wh[v * fs + c] = Wh[v];
+        w.Wn[v * fs + c] = Wn[v];
+    }
+    const R vol = g.vol[c];
+    const R Dm = rmax(pQ[0], P.dFloor);
+#pragma unroll
+    for (int x = 0; x < 3; x++) w.VdV[x * fs + c] = vol * pQ[1 + x] / Dm;
+    if (P.doMHD) {
+        // upper faces of this cell, recomputed with the same ExtrapAB2
+        R up[3];
+        const long off[3] = {1, (long)b.sx, b.sk};
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            long cu = c + off[d];
+            R Qu = cur.mf[d * fs + cu], oQu = old.mf[d * fs + cu];
+            R dQ = (Qu - oQu) / odt;
+            up[d] = Qu + pdt * dQ;
+        }
+        R B[3];
+        cell_bxyz(b, g, c, hm[0], up[0], hm[1], up[1], hm[2], up[2], B);
+#pragma unroll
+        for (int x = 0; x < 3; x++) w.Bh[x * fs + c] = B[x];
+    }
+}
+
+// Edge geometry of the EMF in direction eD (fields.F90:84-170): face
+// direction dT1 (Mom2Face sweep), dT2 (corner sweep)
+__device__ __forceinline__ void edge_dirs(int eD, int& dT1, int& dT2) {
+    dT1 = (eD + 1) % 3;
+    dT2 = (eD + 2) % 3;
+}
+
+// Mom2Face for edge direction eD over the reference's loop range.
+template <class R>
+__global__ void __launch_bounds__(256) k_mom2face(GamBox b, DevParams<R> P, Geo<R> g, Work<R> w, int eD, Range r,
+                                                  const GamScalars* sc) {
+    if (sc->halted) return;
+    int ii, jj, kk;
+    if (!thread_ijk(r, ii, jj, kk)) return;
+    int dT1, dT2;
+    edge_dirs(eD, dT1, dT2);
+    const long fs = b.fs;
+    const long c = lidx(b, ii, jj, kk);
+    const long s = dstride(b, dT1);
+    R vol[8];
+#pragma unroll
+    for (int n = 0; n < 8; n++) vol[n] = g.vol[c + (n - 4) * s];
+    R dV = rmax(central8(vol), (R)TINY);
+#pragma unroll
+    for (int x = 0; x < 3; x++) {
+        R q[8];
+#pragma unroll
+        for (int n = 0; n < 8; n++) q[n] = w.VdV[x * fs + c + (n - 4) * s];
+        w.Vf[(x + 3 * eD) * fs + c] = central8(q) / dV;
+    }
+}
+
+// EdgeLRs (fields.F90:288-362): flux of faces of direction a, stencil along b
+template <class R>
+__device__ __forceinline__ void edge_lrs(const GamBox& b, const DevParams<R>& P, const Geo<R>& g, const Work<R>& w,
+                                         long c, int a, int bd, R* area, R& bL, R& bR, R& fA) {
+    const long fs = b.fs;
+    const long s = dstride(b, bd);
+    R mag[8], nmag[4];
+#pragma unroll
+    for (int n = 0; n < 8; n++) {
+        area[n] = g.face[a * fs + c + (n - 4) * s];
+        mag[n] = w.bh[a * fs + c + (n - 4) * s];
+    }
+#pragma unroll
+    for (int m = 0; m < 4; m++) nmag[m] = P.doLFMLim ? w.bn[a * fs + c + (m - 2) * s] : w.bh[a * fs + c + (m - 2) * s];
+    R Vi = central8(area);
+    get_lrs(P, area, mag, nmag, Vi, bL, bR);
+    fA = central8(area);
+    bL = bL * fA;
+    bR = bR * fA;
+}
+
+// VxB edge loop for direction eD (fields.F90:184-228).
+template <class R>
+__global__ void __launch_bounds__(128) k_vxb(GamBox b, DevParams<R> P, Geo<R> g, Work<R> w, int eD, Range r,
+                                             const GamScalars* sc) {
+    if (sc->halted) return;
+    int ii, jj, kk;
+    if (!thread_ijk(r, ii, jj, kk)) return;
+    int dT1, dT2;
+    edge_dirs(eD, dT1, dT2);
+    const long fs = b.fs;
+    const long c = lidx(b, ii, jj, kk);
+    // GetCornerD (fields.F90:427-454): normal-plane unit offsets e1 < e2
+    const int e1 = eD == 0 ? 1 : 0, e2 = eD == 2 ? 1 : 2;
+    const long s1 = dstride(b, e1), s2 = dstride(b, e2);
+    R Dc = (R)0.25 * (w.Wh[c] + w.Wh[c - s1] + w.Wh[c - s2] + w.Wh[c - s1 - s2]);
+    // GetCornerB: EdgeLRs for dT1 faces along dT2 and dT2 faces along dT1
+    R area1[8], area2[8];
+    R bT1L, bT1R, fA1, bT2L, bT2R, fA2;
+    edge_lrs(b, P, g, w, c, dT1, dT2, area1, bT1L, bT1R, fA1);
+    edge_lrs(b, P, g, w, c, dT2, dT1, area2, bT2L, bT2R, fA2);
+    // GetCornerV (fields.F90:457-517); its area stencil equals area1
+    R dA = rmax(central8(area1), (R)TINY);
+    R VC[3];
+    const long s2v = dstride(b, dT2);
+#pragma unroll
+    for (int x = 0; x < 3; x++) {
+        R acc = (R)0;
+#pragma unroll
+        for (int n = 0; n < 8; n++) acc += Rc<R>(w8(n)) * (area1[n] * w.Vf[(x + 3 * eD) * fs + c + (n - 4) * s2v]);
+        VC[x] = acc / dA;
+    }
+    const R* Te = g.Te;
+    R v1 = VC[0] * Te[(3 + 9 * eD) * fs + c] + VC[1] * Te[(4 + 9 * eD) * fs + c] + VC[2] * Te[(5 + 9 * eD) * fs + c];
+    R v2 = VC[0] * Te[(6 + 9 * eD) * fs + c] + VC[1] * Te[(7 + 9 * eD) * fs + c] + VC[2] * Te[(8 + 9 * eD) * fs + c];
+    R vDiff = Mth<R>::sqrt_(v1 * v1 + v2 * v2);
+    R xni = g.Teb[(0 + 4 * eD) * fs + c], yni = g.Teb[(1 + 4 * eD) * fs + c];
+    R xnj = g.Teb[(2 + 4 * eD) * fs + c], ynj = g.Teb[(3 + 4 * eD) * fs + c];
+    R detT = (R)1 / (xni * ynj - xnj * yni);
+    R bT1 = (R)0.5 * (bT1L + bT1R) / fA1;
+    R bT2 = (R)0.5 * (bT2L + bT2R) / fA2;
+    R db1 = (bT1R - bT1L) / fA1;
+    R db2 = (bT2R - bT2L) / fA2;
+    R Jd = db2 - db1;
+    R b1 = detT * (ynj * bT1 - yni * bT2);
+    R b2 = detT * (-(xnj * bT1) + xni * bT2);
+    if (P.doBackground) {
+        b1 = b1 + (R)g.edgB0[(0 + 2 * eD) * fs + c];
+        b2 = b2 + (R)g.edgB0[(1 + 2 * eD) * fs + c];
+    }
+    R vA = Mth<R>::sqrt_(b1 * b1 + b2 * b2) / Mth<R>::sqrt_(Dc);
+    vDiff = vDiff + vA;
+    const R edge = g.edge[eD * fs + c];
+    vDiff = rmin(vDiff, P.CFL * edge / (R)sc->dt);
+    R e = -(v1 * b2 - v2 * b1) + P.Vd0 * vDiff * Jd;
+    w.E[eD * fs + c] = e * edge;
+}
+
+// One-sided Gaussian-moment fluxes for one side q (sgn = -1 LEFT, +1 RIGHT).
+// MagKinFlux (stress.F90:513-599), Boris off.
+template <class R>
+__device__ __forceinline__ void mag_kin_flux(const DevParams<R>& P, R sgn, const R* W, const R* Bm, R Bn,
+                                             const R* T, const double* B0, double B0n, R* mF, R& bbD, R& VaD) {
+    R D = W[0], Pr = W[4];
+    R Bx = Bm[0], By = Bm[1], Bz = Bm[2];
+    R dPb = (R)0.5 * (Bx * Bx + By * By + Bz * Bz);
+    R Va2;
+    R B0x = (R)0, B0y = (R)0, B0z = (R)0;
+    if (P.doBackground) {
+        B0x = (R)B0[0]; B0y = (R)B0[1]; B0z = (R)B0[2];
+        R sx = Bx + B0x, sy = By + B0y, sz = Bz + B0z;
+        Va2 = (sx * sx + sy * sy + sz * sz) / D;
+        bbD = bbD + (R)0.5 * (sx * sx + sy * sy + sz * sz);
+    } else {
+        Va2 = (R)2 * dPb / D;
+        bbD = bbD + (R)0.5 * (Bx * Bx + By * By + Bz * Bz);
+    }
+    R Vac2 = Va2;
+    R Nx = T[0], Ny = T[1], Nz = T[2];
+    R Vn = Nx * W[1] + Ny * W[2] + Nz * W[3];
+    R lambda = (R)1 / ((R)2 * Pr / D + Vac2);
+    R Vn0 = (R)0.5 * Mth<R>::erfc_(sgn * Mth<R>::sqrt_(lambda) * Vn);
+    VaD = VaD + (R)0.5 * Mth<R>::sqrt_(Vac2);
+    mF[0] = mF[0] + Vn0 * (dPb * Nx - Bx * Bn);
+    mF[1] = mF[1] + Vn0 * (dPb * Ny - By * Bn);
+    mF[2] = mF[2] + Vn0 * (dPb * Nz - Bz * Bn);
+    if (P.doBackground) {
+        R B0nR = (R)B0n;
+        R BdB0 = B0x * Bx + B0y * By + B0z * Bz;
+        mF[0] = mF[0] + Vn0 * (-(B0x * Bn) - Bx * B0nR + BdB0 * Nx);
+        mF[1] = mF[1] + Vn0 * (-(B0y * Bn) - By * B0nR + BdB0 * Ny);
+        mF[2] = mF[2] + Vn0 * (-(B0z * Bn) - Bz * B0nR + BdB0 * Nz);
+    }
+}
+// GasKinFlux (stress.F90:432-511)
+template <class R>
+__device__ __forceinline__ void gas_kin_flux(const DevParams<R>& P, R sgn, const R* W, const R* T, R* gF, R* dW) {
+    R D = W[0], Pr = W[4], Vx = W[1], Vy = W[2], Vz = W[3];
+    R E = (R)0.5 * D * (Vx * Vx + Vy * Vy + Vz * Vz) + Pr / P.gm1;
+    R lambda = D / ((R)2 * Pr);
+    R Vn = T[0] * Vx + T[1] * Vy + T[2] * Vz;
+    R Vt1 = T[3] * Vx + T[4] * Vy + T[5] * Vz;
+    R Vt2 = T[6] * Vx + T[7] * Vy + T[8] * Vz;
+    R Vn0 = (R)0.5 * Mth<R>::erfc_(sgn * Mth<R>::sqrt_(lambda) * Vn);
+    R Vn1 = Vn * Vn0 - (R)0.5 * sgn * Mth<R>::exp_(-(lambda * Vn * Vn)) / Mth<R>::sqrt_((R)PI_D * lambda);
+    gF[0] = gF[0] + D * Vn1;
+    gF[4] = gF[4] + (E + (R)0.5 * Pr) * Vn1 + (R)0.5 * Pr * Vn0 * Vn;
+    R fMn = D * Vn * Vn1 + Pr * Vn0;
+    R fMt1 = D * Vt1 * Vn1;
+    R fMt2 = D * Vt2 * Vn1;
+    R fMx = T[0] * fMn + T[3] * fMt1 + T[6] * fMt2;
+    R fMy = T[1] * fMn + T[4] * fMt1 + T[7] * fMt2;
+    R fMz = T[2] * fMn + T[5] * fMt1 + T[8] * fMt2;
+    gF[1] = gF[1] + fMx;
+    gF[2] = gF[2] + fMy;
+    gF[3] = gF[3] + fMz;
+    dW[0] = dW[0] + sgn * D;
+    dW[1] = dW[1] + sgn * D * Vx;
+    dW[2] = dW[2] + sgn * D * Vy;
+    dW[3] = dW[3] + sgn * D * Vz;
+    dW[4] = dW[4] + sgn * E;
+}
+
+// Face fluxes of direction d (Fluxes, stress.F90:204-429).
+template <class R>
+__global__ void __launch_bounds__(128) k_stress(GamBox b, DevParams<R> P, Geo<R> g, StateBuf<R> cur, Work<R> w,
+                                                int d, Range r, const GamScalars* sc) {
+    if (sc->halted) return;
+    int ii, jj, kk;
+    if (!thread_ijk(r, ii, jj, kk)) return;
+    const long fs = b.fs;
+    const long c = lidx(b, ii, jj, kk);
+    const long s = dstride(b, d);
+    R vol[8];
+#pragma unroll
+    for (int n = 0; n < 8; n++) vol[n] = g.vol[c + (n - 4) * s];
+    const R Vi = central8(vol);
+    R T[9];
+#pragma unroll
+    for (int n = 0; n < 9; n++) T[n] = g.Tf[(n + 9 * d) * fs + c];
+    const R fa = g.face[d * fs + c];
+    R MagL[3] = {(R)0, (R)0, (R)0}, MagR[3] = {(R)0, (R)0, (R)0};
+    R Bn = (R)0;
+    double B0[3] = {0.0, 0.0, 0.0}, B0n = 0.0;
+    if (P.doMHD) {
+#pragma unroll
+        for (int x = 0; x < 3; x++) {
+            R q[8], nq[4];
+#pragma unroll
+            for (int n = 0; n < 8; n++) q[n] = w.Bh[x * fs + c + (n - 4) * s];
+#pragma unroll
+            for (int m = 0; m < 4; m++)
+                nq[m] = P.doLFMLim ? cur.B[x * fs + c + (m - 2) * s] : w.Bh[x * fs + c + (m - 2) * s];
+            get_lrs(P, vol, q, nq, Vi, MagL[x], MagR[x]);
+        }
+        Bn = w.Bnf[d * fs + c];
+        if (P.doBackground) {
+#pragma unroll
+            for (int x = 0; x < 3; x++) B0[x] = g.fcB0[(x + 3 * d) * fs + c];
+            B0n = g.bFlux0[d * fs + c] / (double)fa;
+        }
+    }
+    R WL[5], WR[5];
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+        R q[8], nq[4];
+#pragma unroll
+        for (int n = 0; n < 8; n++) q[n] = w.Wh[v * fs + c + (n - 4) * s];
+#pragma unroll
+        for (int m = 0; m < 4; m++)
+            nq[m] = P.doLFMLim ? w.Wn[v * fs + c + (m - 2) * s] : w.Wh[v * fs + c + (m - 2) * s];
+        get_lrs(P, vol, q, nq, Vi, WL[v], WR[v]);
+    }
+    R VaD = (R)0, bbD = (R)0;
+    if (P.doMHD) {
+        R mF[3] = {(R)0, (R)0, (R)0};
+        mag_kin_flux(P, (R)-1, WL, MagL, Bn, T, B0, B0n, mF, bbD, VaD);
+        mag_kin_flux(P, (R)1, WR, MagR, Bn, T, B0, B0n, mF, bbD, VaD);
+#pragma unroll
+        for (int x = 0; x < 3; x++) w.mF[(x + 3 * d) * fs + c] = fa * mF[x];
+    }
+    R gF[5] = {(R)0, (R)0, (R)0, (R)0, (R)0}, dW[5] = {(R)0, (R)0, (R)0, (R)0, (R)0};
+    gas_kin_flux(P, (R)-1, WL, T, gF, dW);
+    gas_kin_flux(P, (R)1, WR, T, gF, dW);
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+        R gv = gF[v] - (R)1 * P.cHogH * VaD * dW[v];
+        w.gF[(v + 5 * d) * fs + c] = fa * gv;
+    }
+}
+
+// E2Flux into the new buffer; faces outside its range are copied.
+template <class R>
+__global__ void __launch_bounds__(256) k_update_faces(GamBox b, DevParams<R> P, StateBuf<R> cur, StateBuf<R> nxt,
+                                                      Work<R> w, const GamScalars* sc) {
+    if (sc->halted) return;
+    int ii, jj, kk;
+    Range r{0, b.Ni, 0, b.Nj, 0, b.Nk};
+    if (!thread_ijk(r, ii, jj, kk)) return;
+    const long fs = b.fs;
+    const long c = lidx(b, ii, jj, kk);
+    const int G = GAM_NG;
+    const bool inr = P.doMHD && ii >= G && ii <= G + b.Nip && jj >= G && jj <= G + b.Njp && kk >= G && kk <= G + b.Nkp;
+    if (!inr) {
+#pragma unroll
+        for (int x = 0; x < 3; x++) nxt.mf[x * fs + c] = cur.mf[x * fs + c];
+        return;
+    }
+    const R* E = w.E;
+    const long sj = b.sx, sk = b.sk;
+    const R dt = (R)sc->dt;
+    R dfi = E[2 * fs + c + sj] - E[2 * fs + c] - E[1 * fs + c + sk] + E[1 * fs + c];
+    R dfj = E[0 * fs + c + sk] - E[0 * fs + c] - E[2 * fs + c + 1] + E[2 * fs + c];
+    R dfk = E[1 * fs + c + 1] - E[1 * fs + c] - E[0 * fs + c + sj] + E[0 * fs + c];
+    nxt.mf[0 * fs + c] = cur.mf[0 * fs + c] - dt * dfi;
+    nxt.mf[1 * fs + c] = cur.mf[1 * fs + c] - dt * dfj;
+    nxt.mf[2 * fs + c] = cur.mf[2 * fs + c] - dt * dfk;
+}
+
+__device__ __forceinline__ unsigned long long dbits(double x) { return (unsigned long long)__double_as_longlong(x); }
+
+// CellDT (gridutils.F90:49-106), evaluated in FP64
+template <class R>
+__device__ __forceinline__ double cell_dt(const DevParams<R>& P, const double* U, const double* Bt, double dl,
+                                          double gamma, double gm1, double CFL) {
+    double rho = U[0];
+    double Vx = U[1] / rho, Vy = U[2] / rho, Vz = U[3] / rho;
+    double MagV = sqrt(Vx * Vx + Vy * Vy + Vz * Vz);
+    double ke = 0.5 * rho * (MagV * MagV);
+    double e = U[4] - ke;
+    double Pr = gm1 * e;
+    double Cs = sqrt(gamma * Pr / rho);
+    double Valf = 0.0;
+    if (P.doMHD) {
+        double MagB = sqrt(Bt[0] * Bt[0] + Bt[1] * Bt[1] + Bt[2] * Bt[2]);
+        Valf = MagB / sqrt(rho);
+    }
+    double vCFL = MagV + sqrt(Cs * Cs + Valf * Valf) + 0.0;
+    return CFL * dl / vCFL;
+}
+
+// Flux2Deltas + CellReynolds + bFlux2Fld + CellMaxwell for active cells,
+// copy + bFlux2Fld for ghost cells, then the CFL dt of cells in the dt range.
+template <class R>
+__global__ void __launch_bounds__(128) k_update_cells(GamBox b, DevParams<R> P, Geo<R> g, StateBuf<R> cur,
+                                                      StateBuf<R> nxt, Work<R> w, GamScalars* sc, double gamma_d,
+                                                      double gm1_d) {
+    __shared__ double smin[32];
+    if (sc->halted) return;
+    int ii, jj, kk;
+    Range r{0, b.Ni - 1, 0, b.Nj - 1, 0, b.Nk - 1};
+    const bool ok = thread_ijk(r, ii, jj, kk);
+    double mydt = HUGE_DT;
+    bool bad = false;
+    if (ok) {
+        const long fs = b.fs;
+        const long c = lidx(b, ii, jj, kk);
+        const int G = GAM_NG;
+        const bool active = ii >= G && ii < G + b.Nip && jj >= G && jj < G + b.Njp && kk >= G && kk < G + b.Nkp;
+        const R dt = (R)sc->dt;
+        R U[5];
+        R Bc[3] = {(R)0, (R)0, (R)0};
+        if (P.doMHD) {
+            const long sj = b.sx, sk = b.sk;
+            cell_bxyz(b, g, c, nxt.mf[c], nxt.mf[c + 1], nxt.mf[fs + c], nxt.mf[fs + c + sj], nxt.mf[2 * fs + c],
+                      nxt.mf[2 * fs + c + sk], Bc);
+#pragma unroll
+            for (int x = 0; x < 3; x++) nxt.B[x * fs + c] = Bc[x];
+        }
+        if (active) {
+            const long sj = b.sx, sk = b.sk;
+            const R dV = g.vol[c];
+#pragma unroll
+            for (int v = 0; v < 5; v++) {
+                const R* gI = w.gF + (v + 0) * fs;
+                const R* gJ = w.gF + (v + 5) * fs;
+                const R* gK = w.gF + (v + 10) * fs;
+                R dGasH = (gI[c] - gI[c + 1] + gJ[c] - gJ[c + sj] + gK[c] - gK[c + sk]) / dV;
+                U[v] = cur.Gas[v * fs + c] + dt * dGasH;
+            }
+            if (P.doMHD) {
+                R dGasM[3];
+#pragma unroll
+                for (int x = 0; x < 3; x++) {
+                    const R* mI = w.mF + (x + 0) * fs;
+                    const R* mJ = w.mF + (x + 3) * fs;
+                    const R* mK = w.mF + (x + 6) * fs;
+                    dGasM[x] = (mI[c] - mI[c + 1] + mJ[c] - mJ[c + sj] + mK[c] - mK[c + sk]) / dV;
+                    if (P.doBackground) dGasM[x] = dGasM[x] + (R)g.dpB0[x * fs + c];
+                }
+                // CellMaxwell (mhdgroup.F90:299-329)
+                R D = rmax(U[0], P.dFloor);
+                R Mx = U[1], My = U[2], Mz = U[3], TotE = U[4];
+                R KinE = (R)0.5 * (Mx * Mx + My * My + Mz * Mz) / D;
+                R Pr = rmax(P.gm1 * (TotE - KinE), P.pFloor);
+                Mx = Mx + dt * dGasM[0];
+                My = My + dt * dGasM[1];
+                Mz = Mz + dt * dGasM[2];
+                KinE = (R)0.5 * (Mx * Mx + My * My + Mz * Mz) / D;
+                U[0] = D;
+                U[1] = Mx;
+                U[2] = My;
+                U[3] = Mz;
+                U[4] = KinE + Pr / P.gm1;
+            }
+        } else {
+#pragma unroll
+            for (int v = 0; v < 5; v++) U[v] = cur.Gas[v * fs + c];
+        }
+#pragma unroll
+        for (int v = 0; v < 5; v++) nxt.Gas[v * fs + c] = U[v];
+        // dt range isDT..ieDT = is-1..ie+1 (init.F90:511-530, single domain)
+        const bool indt = ii >= G - 1 && ii <= G + b.Nip && jj >= G - 1 && jj <= G + b.Njp && kk >= G - 1 &&
+                          kk <= G + b.Nkp;
+        if (indt && !sc->fixedTimestep) {
+            double Ud[5], Bt[3];
+#pragma unroll
+            for (int v = 0; v < 5; v++) Ud[v] = (double)U[v];
+#pragma unroll
+            for (int x = 0; x < 3; x++) {
+                Bt[x] = (double)Bc[x];
+                if (P.doBackground) Bt[x] = Bt[x] + g.B0[x * fs + c];
+            }
+            double dtc = cell_dt(P, Ud, Bt, (double)g.dl[c], gamma_d, gm1_d, sc->CFL);
+            if (dtc > 0.0 && dtc < 1.0e300) mydt = dtc;  // finite positive
+            else bad = true;
+        }
+    }
+    // block min
+    for (int o = 16; o > 0; o >>= 1) mydt = fmin(mydt, __shfl_xor_sync(0xffffffffu, mydt, o));
+    const int lane = (threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z)) & 31;
+    const int wid = (threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z)) >> 5;
+    const int nw = (blockDim.x * blockDim.y * blockDim.z + 31) >> 5;
+    if (lane == 0) smin[wid] = mydt;
+    unsigned anybad = __syncthreads_or(bad ? 1 : 0);
+    if (wid == 0) {
+        double v = lane < nw ? smin[lane] : HUGE_DT;
+        for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+        if (lane == 0) {
+            if (v < HUGE_DT) atomicMin(&sc->dtmin_bits, dbits(v));
+            if (anybad) atomicAdd(&sc->nbad, 1);
+        }
+    }
+}
+
+// UpdateStateData time bookkeeping + CalcDT decisions (gamapp.F90:110-111,
+// mhdgroup.F90:106, step.F90:58-168). A failure halts the remaining kernels.
+__global__ void k_dt_finalize(GamScalars* sc) {
+    if (sc->halted) return;
+    sc->otime = sc->time;          // CopyState (mhdgroup.F90:255)
+    sc->time = sc->time + sc->dt;  // mhdgroup.F90:106
+    sc->ts = sc->ts + 1;
+    sc->t = sc->t + sc->dt;
+    if (sc->fixedTimestep) return;
+    const double dtOld = sc->dt;
+    double dtMin = __longlong_as_double((long long)sc->dtmin_bits);
+    sc->dtmin_bits = dbits(HUGE_DT);
+    bool isDisaster = (dtMin == HUGE_DT) || sc->nbad > 0;
+    bool isBad = false;
+    if (sc->ts > 0) {
+        if (dtOld / dtMin >= 10.0) isBad = true;
+        if (sc->dt0 > TINY && dtMin / sc->dt0 <= sc->limDT0) isBad = true;
+        if (dtMin <= TINY) isDisaster = true;
+    }
+    double dt = dtMin;
+    if (sc->t + dt > sc->tFin) dt = fmax(sc->tFin - sc->t, TINY);
+    if (sc->dt0 > TINY && dt > 10.0 * sc->dt0) dt = 10.0 * sc->dt0;
+    sc->dt = dt;
+    if (isDisaster) { sc->status = 5; sc->halted = 1; }
+    else if (isBad) { sc->status = 4; sc->halted = 1; }
+}
+
+// Source index of a ghost value under the composed boundary maps of one
+// direction. n = number of active cells; face = this index is a face normal
+// to this direction (gets the upper-face offset rule of periodic_o*, bcs.F90).
+__device__ __forceinline__ int bc_map(int x, int n, int kind_lo, int kind_hi, bool normalFace, bool do25D) {
+    const int G = GAM_NG;
+    if (do25D) {  // periodic_*bcK with Model%do25D: replicate ks (bcs.F90:387-394, 423-429)
+        if (x >= G - 4 && x < G) return G;
+        if (x > G && x <= G + 4) return G;
+        return x;
+    }
+    if (x < G) return kind_lo == 0 ? x + n : x;
+    if (normalFace) {
+        if (x >= G + n + 1 && x <= G + n + 4) return kind_hi == 0 ? x - n : x;
+        return x;
+    }
+    if (x >= G + n && x <= G + n + 3) return kind_hi == 0 ? x - n : x;
+    return x;
+}
+
+// EnforceBCs for periodic / no-op boundaries as one gather, followed by the
+// final bFlux2Fld of every cell whose value or faces it changed.
+// copyB: fill ghost Bxyz by the same gather instead of recomputing it (the
+// initial EnforceBCs of CalcGridInfo, init.F90:226-238, has no bFlux2Fld after it).
+template <class R>
+__global__ void __launch_bounds__(256) k_bc(GamBox b, DevParams<R> P, Geo<R> g, StateBuf<R> s, const GamScalars* sc,
+                                            int copyB) {
+    if (sc->halted) return;
+    int ii, jj, kk;
+    Range r{0, b.Ni, 0, b.Nj, 0, b.Nk};
+    if (!thread_ijk(r, ii, jj, kk)) return;
+    const long fs = b.fs;
+    const long c = lidx(b, ii, jj, kk);
+    const bool k25 = P.do25D != 0;
+    // faces
+    int fi[3], fj[3], fk[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        fi[d] = bc_map(ii, b.Nip, P.bc[0], P.bc[1], d == 0, false);
+        fj[d] = bc_map(jj, b.Njp, P.bc[2], P.bc[3], d == 1, false);
+        fk[d] = k25 ? bc_map(kk, b.Nkp, 0, 0, d == 2, true) : bc_map(kk, b.Nkp, P.bc[4], P.bc[5], d == 2, false);
+        if (k25 && kk == b.Nk) fk[d] = kk;  // keg+1 is outside the replicated slices
+    }
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        if (fi[d] != ii || fj[d] != jj || fk[d] != kk) s.mf[d * fs + c] = s.mf[d * fs + lidx(b, fi[d], fj[d], fk[d])];
+    }
+    if (ii >= b.Ni || jj >= b.Nj || kk >= b.Nk) return;
+    // cell
+    int ci = bc_map(ii, b.Nip, P.bc[0], P.bc[1], false, false);
+    int cj = bc_map(jj, b.Njp, P.bc[2], P.bc[3], false, false);
+    int ck = k25 ? bc_map(kk, b.Nkp, 0, 0, false, true) : bc_map(kk, b.Nkp, P.bc[4], P.bc[5], false, false);
+    const bool cellMapped = ci != ii || cj != jj || ck != kk;
+    if (cellMapped) {
+        long src = lidx(b, ci, cj, ck);
+#pragma unroll
+        for (int v = 0; v < 5; v++) s.Gas[v * fs + c] = s.Gas[v * fs + src];
+        if (copyB) {
+#pragma unroll
+            for (int x = 0; x < 3; x++) s.B[x * fs + c] = s.B[x * fs + src];
+        }
+    }
+    if (!P.doMHD || copyB) return;
+    // the six faces of this cell after the boundary fill
+    auto srcf = [&](int d, int a, int bb, int cc) -> long {
+        int x = bc_map(a, b.Nip, P.bc[0], P.bc[1], d == 0, false);
+        int y = bc_map(bb, b.Njp, P.bc[2], P.bc[3], d == 1, false);
+        int z = k25 ? bc_map(cc, b.Nkp, 0, 0, d == 2, true) : bc_map(cc, b.Nkp, P.bc[4], P.bc[5], d == 2, false);
+        if (k25 && cc == b.Nk) z = cc;
+        return lidx(b, x, y, z);
+    };
+    long fI = srcf(0, ii, jj, kk), fIp = srcf(0, ii + 1, jj, kk);
+    long fJ = srcf(1, ii, jj, kk), fJp = srcf(1, ii, jj + 1, kk);
+    long fK = srcf(2, ii, jj, kk), fKp = srcf(2, ii, jj, kk + 1);
+    const bool facesMapped = fI != c || fIp != c + 1 || fJ != c || fJp != c + b.sx || fK != c || fKp != c + b.sk;
+    const int G = GAM_NG;
+    const bool ghost = ii < G || ii >= G + b.Nip || jj < G || jj >= G + b.Njp || kk < G || kk >= G + b.Nkp;
+    if (!(ghost || facesMapped)) return;
+    R B[3];
+    cell_bxyz(b, g, c, s.mf[fI], s.mf[fIp], s.mf[fs + fJ], s.mf[fs + fJp], s.mf[2 * fs + fK], s.mf[2 * fs + fKp], B);
+#pragma unroll
+    for (int x = 0; x < 3; x++) s.B[x * fs + c] = B[x];
+}
+
+// CalcDT on a state without changing it (gam_calc_dt): min of CellDT over
+// the dt range into sc->dtmin_bits.
+template <class R>
+__global__ void __launch_bounds__(128) k_dt_only(GamBox b, DevParams<R> P, Geo<R> g, StateBuf<R> s,
+                                                 GamScalars* sc, double gamma_d, double gm1_d) {
+    int ii, jj, kk;
+    const int G = GAM_NG;
+    Range r{G - 1, G + b.Nip, G - 1, G + b.Njp, G - 1, G + b.Nkp};
+    double mydt = HUGE_DT;
+    if (thread_ijk(r, ii, jj, kk)) {
+        const long fs = b.fs;
+        const long c = lidx(b, ii, jj, kk);
+        double Ud[5], Bt[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int v = 0; v < 5; v++) Ud[v] = (double)s.Gas[v * fs + c];
+        if (P.doMHD) {
+#pragma unroll
+            for (int x = 0; x < 3; x++) {
+                Bt[x] = (double)s.B[x * fs + c];
+                if (P.doBackground) Bt[x] = Bt[x] + g.B0[x * fs + c];
+            }
+        }
+        double dtc = cell_dt(P, Ud, Bt, (double)g.dl[c], gamma_d, gm1_d, sc->CFL);
+        if (dtc > 0.0 && dtc < 1.0e300) mydt = dtc;
+    }
+    for (int o = 16; o > 0; o >>= 1) mydt = fmin(mydt, __shfl_xor_sync(0xffffffffu, mydt, o));
+    if ((threadIdx.x & 31) == 0 && mydt < HUGE_DT) atomicMin(&sc->dtmin_bits, dbits(mydt));
+}
+
+
+// bFlux2Fld over every cell of a state (gridutils.F90:281-301)
+template <class R>
+__global__ void __launch_bounds__(128) k_bfield_all(GamBox b, Geo<R> g, StateBuf<R> s) {
+    int ii, jj, kk;
+    Range r{0, b.Ni - 1, 0, b.Nj - 1, 0, b.Nk - 1};
+    if (!thread_ijk(r, ii, jj, kk)) return;
+    const long fs = b.fs;
+    const long c = lidx(b, ii, jj, kk);
+    R B[3];
+    cell_bxyz(b, g, c, s.mf[c], s.mf[c + 1], s.mf[fs + c], s.mf[fs + c + b.sx], s.mf[2 * fs + c], s.mf[2 * fs + c + b.sk], B);
+#pragma unroll
+    for (int x = 0; x < 3; x++) s.B[x * fs + c] = B[x];
+}
+
+// ----------------------------------------------------------------- launches
+static inline dim3 grid_for(const Range& r, dim3 blk) {
+    return dim3((unsigned)((r.i1 - r.i0 + 1 + blk.x - 1) / blk.x), (unsigned)((r.j1 - r.j0 + 1 + blk.y - 1) / blk.y),
+                (unsigned)((r.k1 - r.k0 + 1 + blk.z - 1) / blk.z));
+}
+
+// One stepGamera on stream s; st[cur] is State (n), st[1-cur] holds oState
+// (n-1) on entry and State (n+1) on exit.
+template <class R> void launch_step(const Ctx<R>& C, int cur, cudaStream_t s) {
+    const GamBox& b = C.b;
+    const int G = GAM_NG;
+    const StateBuf<R> S = C.st[cur], O = C.st[1 - cur];
+    const dim3 blk(32, 4, 1);
+    const Range all{0, b.Ni, 0, b.Nj, 0, b.Nk};
+    const Range cells{0, b.Ni - 1, 0, b.Nj - 1, 0, b.Nk - 1};
+    const int kke = C.P.do25D ? G : G + b.Nkp - 1;  // last active k of the stress sweep
+    k_step_begin<<<1, 1, 0, s>>>(C.sc);
+    k_predict<R><<<grid_for(all, blk), blk, 0, s>>>(b, C.P, C.g, S, O, C.w, C.sc);
+    if (C.P.doMHD) {
+        const Range mf[3] = {{0, b.Ni - 1, G, G + b.Njp, 0, b.Nk - 1},
+                             {0, b.Ni - 1, 0, b.Nj - 1, G, G + b.Nkp},
+                             {G, G + b.Nip, 0, b.Nj - 1, 0, b.Nk - 1}};
+        const Range ed[3] = {{G, G + b.Nip - 1, G, G + b.Njp, G, G + b.Nkp},
+                             {G, G + b.Nip, G, G + b.Njp - 1, G, G + b.Nkp},
+                             {G, G + b.Nip, G, G + b.Njp, G, G + b.Nkp - 1}};
+        for (int eD = 0; eD < 3; eD++) {
+            k_mom2face<R><<<grid_for(mf[eD], blk), blk, 0, s>>>(b, C.P, C.g, C.w, eD, mf[eD], C.sc);
+            k_vxb<R><<<grid_for(ed[eD], blk), blk, 0, s>>>(b, C.P, C.g, C.w, eD, ed[eD], C.sc);
+        }
+    }
+    const Range fr[3] = {{G, G + b.Nip, G, G + b.Njp - 1, G, kke},
+                         {G, G + b.Nip - 1, G, G + b.Njp, G, kke},
+                         {G, G + b.Nip - 1, G, G + b.Njp - 1, G, G + b.Nkp}};
+    const int nFlx = C.P.do25D ? 2 : 3;
+    for (int d = 0; d < nFlx; d++) k_stress<R><<<grid_for(fr[d], blk), blk, 0, s>>>(b, C.P, C.g, S, C.w, d, fr[d], C.sc);
+    k_update_faces<R><<<grid_for(all, blk), blk, 0, s>>>(b, C.P, S, O, C.w, C.sc);
+    k_update_cells<R><<<grid_for(cells, blk), blk, 0, s>>>(b, C.P, C.g, S, O, C.w, C.sc, C.gamma, C.gm1);
+    k_dt_finalize<<<1, 1, 0, s>>>(C.sc);
+    k_bc<R><<<grid_for(all, blk), blk, 0, s>>>(b, C.P, C.g, O, C.sc, 0);
+}
+
+// CalcDT on st[cur] into sc->dtmin_bits (the caller resets it first).
+template <class R> void launch_dt_only(const Ctx<R>& C, int cur, cudaStream_t s) {
+    const GamBox& b = C.b;
+    const int G = GAM_NG;
+    const dim3 blk(32, 4, 1);
+    const Range r{G - 1, G + b.Nip, G - 1, G + b.Njp, G - 1, G + b.Nkp};
+    k_dt_only<R><<<grid_for(r, blk), blk, 0, s>>>(b, C.P, C.g, C.st[cur], C.sc, C.gamma, C.gm1);
+}
+
+// CalcGridInfo after the initial condition (init.F90:217-238): Bxyz from the
+// fluxes, first EnforceBCs, oState = State.
+template <class R> void launch_init(const Ctx<R>& C, int cur, cudaStream_t s) {
+    const GamBox& b = C.b;
+    const dim3 blk(32, 4, 1);
+    const Range all{0, b.Ni, 0, b.Nj, 0, b.Nk};
+    const Range cells{0, b.Ni - 1, 0, b.Nj - 1, 0, b.Nk - 1};
+    const StateBuf<R> S = C.st[cur], O = C.st[1 - cur];
+    if (C.P.doMHD) k_bfield_all<R><<<grid_for(cells, blk), blk, 0, s>>>(b, C.g, S);
+    k_bc<R><<<grid_for(all, blk), blk, 0, s>>>(b, C.P, C.g, S, C.sc, 1);
+    cudaMemcpyAsync(O.Gas, S.Gas, 5 * b.fs * sizeof(R), cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(O.mf, S.mf, 3 * b.fs * sizeof(R), cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(O.B, S.B, 3 * b.fs * sizeof(R), cudaMemcpyDeviceToDevice, s);
+}
+
+}  // namespace GAM_NS

@@ -1,0 +1,9 @@
+// FP64 step kernels without FMA contraction (built with -fmad=false): every
+// operation is one IEEE-rounded +, -, *, / or sqrt in the reference's order,
+// so the result equals an IEEE-strict CPU evaluation of the same step.
+#define GAM_NS gam_strict
+#include "gam_step_impl.cuh"
+
+void gam_strict_step_f64(const Ctx<double>& C, int cur, cudaStream_t s) { gam_strict::launch_step<double>(C, cur, s); }
+void gam_strict_dt_f64(const Ctx<double>& C, int cur, cudaStream_t s) { gam_strict::launch_dt_only<double>(C, cur, s); }
+void gam_strict_init_f64(const Ctx<double>& C, int cur, cudaStream_t s) { gam_strict::launch_init<double>(C, cur, s); }

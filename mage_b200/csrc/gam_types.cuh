@@ -1,0 +1,63 @@
+// Device-side views of the GAMERA Model/Grid/State/Solver data, shared by
+// every build variant of the step kernels and by the C ABI.
+#pragma once
+#include "gam_layout.cuh"
+
+template <class R> struct DevParams {
+    R gamma, gm1, CFL, pdmb, Vd0, cHogH, dFloor, pFloor;
+    int doMHD, doLFMLim, do25D, doBackground, up7;
+    int bc[6];
+};
+
+template <class R> struct Geo {  // Grid_T arrays on the device (gamtypes.F90:168-250)
+    const R* vol;    // cell
+    const R* xyzcc;  // cell, 3
+    const R* dl;     // cell, min(di,dj,dk)
+    const R* face;   // face, 3
+    const R* xfc;    // face, 9: x + 3*d
+    const R* Tf;     // face, 27: n + 9*d
+    const R* edge;   // edge, 3
+    const R* Te;     // edge, 27: n + 9*d
+    const R* Teb;    // edge, 12: q + 4*d
+    const double* fcB0;    // face, 9  (background; FP64 in both forms)
+    const double* bFlux0;  // face, 3
+    const double* edgB0;   // edge, 6: c + 2*d
+    const double* B0;      // cell, 3
+    const double* dpB0;    // cell, 3
+};
+
+template <class R> struct StateBuf {
+    R* Gas;  // cell, 5
+    R* mf;   // face, 3
+    R* B;    // cell, 3
+};
+
+template <class R> struct Work {
+    R* Wh;   // cell, 5: primitives of the half state (BlockCon2Prim)
+    R* Wn;   // cell, 5: primitives of state n (limiter stencils)
+    R* VdV;  // cell, 3: volume * momentum / max(density, dFloor) of the half state
+    R* Bh;   // cell, 3: Bxyz of the half state
+    R* bh;   // face, 3: half-state flux / max(area, TINY)
+    R* bn;   // face, 3: state-n flux / max(area, TINY)
+    R* Bnf;  // face, 3: half-state flux / area
+    R* Vf;   // cell, 9: Vf(x) for edge direction eD at x + 3*eD
+    R* E;    // edge, 3
+    R* gF;   // face, 15: gas flux v + 5*d (already times face area)
+    R* mF;   // face, 9: magnetic flux x + 3*d
+};
+
+struct Range {  // inclusive box-index range
+    int i0, i1, j0, j1, k0, k1;
+};
+
+
+// Everything one step launch needs.
+template <class R> struct Ctx {
+    GamBox b;
+    DevParams<R> P;
+    Geo<R> g;
+    StateBuf<R> st[2];   // double buffer: st[cur] = State (n), st[1-cur] = oState (n-1) -> State (n+1)
+    Work<R> w;
+    GamScalars* sc;
+    double gamma, gm1;
+};

@@ -1,0 +1,254 @@
+"""Host side of the B200 GAMERA step: ctypes binding of include/gamgpu.h.
+
+Mirrors the reference's app interface for the step (gamApp_T,
+src/base/types/gamtypes.F90:301-321): ``init_model`` sets up the Grid and the
+State, ``step_gamera`` is ``stepGamera`` (src/gamera/gamapp.F90:73-91) and
+``advance_model`` is ``gamApp_T%AdvanceModel`` (src/gamera/gamtypessub.F90:74-90).
+
+Arrays cross the boundary in the reference's Fortran layout: a Fortran array
+``A(isg:ieg, jsg:jeg, ksg:keg, 1:nc)`` (i fastest) is a C-ordered numpy
+array of shape ``(nc, Nk, Nj, Ni)``; face-centred arrays have ``+1`` in the
+three grid dimensions. The CUDA library is required: there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgamgpu.so")
+
+GAM_OK, GAM_EINVAL, GAM_EBADDIM, GAM_ECUDA, GAM_EDT_BAD, GAM_EDT_DISASTER, GAM_ESTATE, GAM_EHOOK = range(8)
+BC_PERIODIC, BC_NONE = 0, 1
+RECON_8CENT, RECON_7UP = 0, 1
+FP64, FP32 = 0, 1
+
+_ERRNAMES = {1: "GAM_EINVAL", 2: "GAM_EBADDIM", 3: "GAM_ECUDA", 4: "GAM_EDT_BAD", 5: "GAM_EDT_DISASTER",
+             6: "GAM_ESTATE", 7: "GAM_EHOOK"}
+
+
+class GamError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{_ERRNAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+class _Params(C.Structure):
+    _fields_ = [
+        ("Nip", C.c_int32), ("Njp", C.c_int32), ("Nkp", C.c_int32), ("nG", C.c_int32),
+        ("gamma", C.c_double), ("CFL", C.c_double), ("pdmb", C.c_double), ("Vd0", C.c_double),
+        ("cHogH", C.c_double), ("cHogM", C.c_double), ("dFloor", C.c_double), ("pFloor", C.c_double),
+        ("tFin", C.c_double), ("dt0", C.c_double), ("limDT0", C.c_double), ("fixedTimestep", C.c_double),
+        ("rmeth", C.c_int32), ("doLFMLim", C.c_int32), ("doMHD", C.c_int32), ("doBackground", C.c_int32),
+        ("do25D", C.c_int32), ("precision", C.c_int32), ("strict", C.c_int32), ("bc", C.c_int32 * 6),
+    ]
+
+
+EXPORTED = (
+    "gam_default_params", "gam_create", "gam_destroy", "gam_last_error", "gam_set_geometry",
+    "gam_set_geometry_arrays", "gam_get_geometry_arrays", "gam_upload_state", "gam_download_state", "gam_step",
+    "gam_calc_dt", "gam_divb", "gam_totals", "gam_last_step_ms", "gam_advance_model", "gam_init_orszag_tang",
+    "gam_init_blast_wave",
+)
+
+_lib = None
+_dp = C.POINTER(C.c_double)
+
+
+def load_library(path: str = LIB_PATH) -> C.CDLL:
+    """Load libgamgpu.so (built by __graft_entry__.build() / mage_b200/csrc/Makefile)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise GamError(GAM_ECUDA, f"{path} is missing: build the CUDA library first (make -C mage_b200/csrc)")
+    L = C.CDLL(path)
+    L.gam_default_params.argtypes = [C.POINTER(_Params), C.c_int32, C.c_int32, C.c_int32]
+    L.gam_create.argtypes = [C.POINTER(_Params), C.POINTER(C.c_void_p)]
+    L.gam_destroy.argtypes = [C.c_void_p]
+    L.gam_last_error.argtypes = [C.c_void_p]
+    L.gam_last_error.restype = C.c_char_p
+    L.gam_set_geometry.argtypes = [C.c_void_p, _dp]
+    L.gam_set_geometry_arrays.argtypes = [C.c_void_p] + [_dp] * 11
+    L.gam_get_geometry_arrays.argtypes = [C.c_void_p] + [_dp] * 11
+    L.gam_upload_state.argtypes = [C.c_void_p] + [_dp] * 5 + [C.c_double, C.c_double, C.c_double, C.c_int32]
+    L.gam_download_state.argtypes = [C.c_void_p] + [_dp] * 5 + [_dp, _dp, _dp, C.POINTER(C.c_int32)]
+    L.gam_step.argtypes = [C.c_void_p, C.c_int32, _dp, _dp]
+    L.gam_calc_dt.argtypes = [C.c_void_p, _dp]
+    L.gam_divb.argtypes = [C.c_void_p, _dp]
+    L.gam_totals.argtypes = [C.c_void_p, _dp]
+    L.gam_last_step_ms.argtypes = [C.c_void_p, _dp]
+    L.gam_advance_model.argtypes = [C.c_void_p, C.c_double, _dp]
+    L.gam_init_orszag_tang.argtypes = [C.c_void_p]
+    L.gam_init_blast_wave.argtypes = [C.c_void_p, _dp]
+    _lib = L
+    return L
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(_dp)
+
+
+@dataclass
+class GamParams:
+    """Model keys of the step; defaults are the reference's (init.F90:312-484)."""
+    Nip: int
+    Njp: int
+    Nkp: int
+    gamma: float = 5.0 / 3.0
+    CFL: float = 0.3
+    pdmb: float = 0.75
+    Vd0: float = 0.5
+    cHogH: float = 0.25
+    cHogM: float = 0.25
+    dFloor: float = 1.0e-12
+    pFloor: float = 1.0e-12
+    tFin: float = 1.0e30
+    dt0: float = 0.0
+    limDT0: float = 1.0e-3
+    fixedTimestep: float = -1.0
+    rmeth: int = RECON_8CENT
+    doLFMLim: bool = True
+    doMHD: bool = True
+    doBackground: bool = False
+    do25D: bool = False
+    precision: int = FP64
+    strict: bool = False
+    bc: tuple = field(default_factory=lambda: (BC_PERIODIC,) * 6)
+
+    def to_c(self) -> _Params:
+        p = _Params()
+        p.nG = 4
+        for f, _ in _Params._fields_:
+            if f == "nG":
+                continue
+            if f == "bc":
+                p.bc[:] = list(self.bc)
+            else:
+                setattr(p, f, getattr(self, f))
+        return p
+
+    @property
+    def dims(self):
+        return self.Nip + 8, self.Njp + 8, self.Nkp + 8
+
+
+GEOMETRY_ARRAYS = (("face", "face", 3), ("xfc", "face", 9), ("Tf", "face", 27), ("volume", "cell", 1),
+                   ("xyzcc", "cell", 3), ("di", "cell", 1), ("dj", "cell", 1), ("dk", "cell", 1),
+                   ("edge", "face", 3), ("Te", "face", 27), ("Teb", "face", 12))
+
+
+class GameraGPU:
+    """One GAMERA app whose Grid and State live on the GPU."""
+
+    def __init__(self, params: GamParams):
+        self.L = load_library()
+        self.params = params
+        self._cp = params.to_c()
+        h = C.c_void_p()
+        rc = self.L.gam_create(C.byref(self._cp), C.byref(h))
+        self.h = h
+        self._check(rc)
+        self.Ni, self.Nj, self.Nk = params.dims
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h is not None and h.value:
+            self.L.gam_destroy(h)
+            self.h = None
+
+    def close(self):
+        self.__del__()
+
+    def _check(self, rc: int):
+        if rc != GAM_OK:
+            msg = self.L.gam_last_error(self.h).decode() if self.h and self.h.value else ""
+            raise GamError(rc, msg)
+
+    def shape(self, kind: str, nc: int):
+        if kind == "cell":
+            return (nc, self.Nk, self.Nj, self.Ni)
+        return (nc, self.Nk + 1, self.Nj + 1, self.Ni + 1)
+
+    # --- grid ---------------------------------------------------------------
+    def set_geometry(self, xyz: np.ndarray):
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+        assert xyz.shape == self.shape("face", 3), xyz.shape
+        self._check(self.L.gam_set_geometry(self.h, _ptr(xyz)))
+
+    def set_geometry_arrays(self, arrs: dict):
+        args = []
+        keep = []
+        for name, kind, nc in GEOMETRY_ARRAYS:
+            a = np.ascontiguousarray(arrs[name], dtype=np.float64).reshape(self.shape(kind, nc))
+            keep.append(a)
+            args.append(_ptr(a))
+        self._check(self.L.gam_set_geometry_arrays(self.h, *args))
+
+    def get_geometry_arrays(self) -> dict:
+        out = {name: np.zeros(self.shape(kind, nc)) for name, kind, nc in GEOMETRY_ARRAYS}
+        self._check(self.L.gam_get_geometry_arrays(self.h, *[_ptr(out[n]) for n, _, _ in GEOMETRY_ARRAYS]))
+        return out
+
+    # --- state --------------------------------------------------------------
+    def upload_state(self, Gas, magFlux, Bxyz, oGas, omagFlux, time: float, otime: float, dt: float, ts: int = 0):
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (Gas, magFlux, Bxyz, oGas, omagFlux)]
+        shapes = [self.shape("cell", 5), self.shape("face", 3), self.shape("cell", 3), self.shape("cell", 5),
+                  self.shape("face", 3)]
+        for a, s in zip(arrs, shapes):
+            assert a.shape == s, (a.shape, s)
+        self._check(self.L.gam_upload_state(self.h, *[_ptr(a) for a in arrs], time, otime, dt, int(ts)))
+
+    def download_state(self) -> dict:
+        out = {"Gas": np.zeros(self.shape("cell", 5)), "magFlux": np.zeros(self.shape("face", 3)),
+               "Bxyz": np.zeros(self.shape("cell", 3)), "oGas": np.zeros(self.shape("cell", 5)),
+               "omagFlux": np.zeros(self.shape("face", 3))}
+        t, ot, dt, ts = C.c_double(), C.c_double(), C.c_double(), C.c_int32()
+        self._check(self.L.gam_download_state(self.h, *[_ptr(out[k]) for k in ("Gas", "magFlux", "Bxyz", "oGas",
+                                                                               "omagFlux")],
+                                              C.byref(t), C.byref(ot), C.byref(dt), C.byref(ts)))
+        out.update(time=t.value, otime=ot.value, dt=dt.value, ts=ts.value)
+        return out
+
+    # --- problems -------------------------------------------------------------
+    def init_orszag_tang(self):
+        self._check(self.L.gam_init_orszag_tang(self.h))
+
+    def init_blast_wave(self, x0=0.5, y0=0.5, z0=0.5, D0=1.0, P0=0.1, pRat=100.0, dRat=1.0, rC=0.1, B0=1.0):
+        bw = np.array([x0, y0, z0, D0, P0, pRat, dRat, rC, B0], dtype=np.float64)
+        self._check(self.L.gam_init_blast_wave(self.h, _ptr(bw)))
+
+    # --- stepping -------------------------------------------------------------
+    def step_gamera(self, n: int = 1):
+        """n x stepGamera; returns (Model%dt, Model%t)."""
+        dt, t = C.c_double(), C.c_double()
+        self._check(self.L.gam_step(self.h, int(n), C.byref(dt), C.byref(t)))
+        return dt.value, t.value
+
+    def advance_model(self, dt: float) -> float:
+        t = C.c_double()
+        self._check(self.L.gam_advance_model(self.h, float(dt), C.byref(t)))
+        return t.value
+
+    def calc_dt(self) -> float:
+        dt = C.c_double()
+        self._check(self.L.gam_calc_dt(self.h, C.byref(dt)))
+        return dt.value
+
+    def divb(self) -> float:
+        v = C.c_double()
+        self._check(self.L.gam_divb(self.h, C.byref(v)))
+        return v.value
+
+    def totals(self) -> np.ndarray:
+        out = np.zeros(5)
+        self._check(self.L.gam_totals(self.h, _ptr(out)))
+        return out
+
+    def last_step_ms(self) -> float:
+        v = C.c_double()
+        self._check(self.L.gam_last_step_ms(self.h, C.byref(v)))
+        return v.value

@@ -1,0 +1,50 @@
+"""Corner grids for the GAMERA step (host side, FP64).
+
+Corner arrays use the reference's memory layout: Fortran
+``xyz(isg:ieg+1, jsg:jeg+1, ksg:keg+1, 1:3)`` with i fastest, which in numpy
+is a C-ordered array of shape ``(3, Nk+1, Nj+1, Ni+1)`` (component, k, j, i),
+``Ni = Nip + 2*nG``, ``nG = 4``, and corner index ``i`` running from
+``isg = 1 - nG`` to ``ieg + 1 = Nip + nG + 1``.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+NG = 4
+
+
+def _axis(n: int, lo: float, hi: float) -> np.ndarray:
+    """Corner coordinates along one axis, init.F90:684-689 (genGridXML):
+    ``x = min + (i-1)*dx`` with ``dx = (max-min)/N`` for i = isg .. ieg+1."""
+    dx = (hi - lo) / n
+    i = np.arange(1 - NG, n + NG + 2, dtype=np.float64)
+    return lo + (i - 1.0) * dx
+
+
+def uniform_corners(Nip: int, Njp: int, Nkp: int, bounds=(0.0, 1.0, 0.0, 1.0, 0.0, 1.0)) -> np.ndarray:
+    """Uniform Cartesian corners (genGridXML without doCyl/doSph/doWarp)."""
+    x1 = _axis(Nip, bounds[0], bounds[1])
+    x2 = _axis(Njp, bounds[2], bounds[3])
+    x3 = _axis(Nkp, bounds[4], bounds[5])
+    xyz = np.empty((3, x3.size, x2.size, x1.size), dtype=np.float64)
+    xyz[0] = x1[None, None, :]
+    xyz[1] = x2[None, :, None]
+    xyz[2] = x3[:, None, None]
+    return xyz
+
+
+def warped_periodic_corners(Nip: int, Njp: int, Nkp: int, amp: float = 0.05) -> np.ndarray:
+    """Non-orthogonal curvilinear corners on the unit cube:
+    ``x = xi + amp*s, y = eta + amp*s, z = zeta + amp*s`` with
+    ``s = sin(2 pi xi) sin(2 pi eta) sin(2 pi zeta)``. The map commutes with unit
+    shifts, so the grid is triply periodic; ghost corners use the same formula."""
+    u = uniform_corners(Nip, Njp, Nkp)
+    xi, eta, zeta = u[0], u[1], u[2]
+    s = np.sin(2.0 * np.pi * xi) * np.sin(2.0 * np.pi * eta) * np.sin(2.0 * np.pi * zeta)
+    return np.stack([xi + amp * s, eta + amp * s, zeta + amp * s]).astype(np.float64)
+
+
+def dims(xyz: np.ndarray):
+    """(Nip, Njp, Nkp) of a corner array."""
+    _, nk1, nj1, ni1 = xyz.shape
+    return ni1 - 1 - 2 * NG, nj1 - 1 - 2 * NG, nk1 - 1 - 2 * NG

@@ -1,0 +1,1571 @@
+// ORACLE -- test infrastructure only. CPU restatement of the GAMERA MHD step of
+// the Kaiju/MAGE reference (Fortran 2008 + OpenMP), used as the checker for the
+// CUDA implementation and as the timed CPU baseline. Nothing in the product
+// imports, links or calls this file.
+//
+// Each routine follows one Fortran routine of the reference, cited as
+// file:line (paths relative to the reference project root), and keeps its
+// data layout (column-major, i fastest, nG = 4 ghosts, lower bound isg = 1-nG),
+// its 16-wide i-bricks (BRICKSIZE, CMakeLists.txt:44-47), its loop order and the
+// evaluation order of every arithmetic expression (Fortran evaluates a+b+c as
+// (a+b)+c, and x**2.0 is folded to x*x by the compiler). Intent: bitwise the
+// same arithmetic as an IEEE-strict build of the reference.
+//
+// Build variants (oracle/Makefile):
+//   strict : -O2 -fno-fast-math -ffp-contract=off, libm erfc/exp  (parity oracle)
+//   gm     : as strict but erfc/exp from mage_b200/csrc/gam_math.cuh, so the
+//            only remaining difference to the GPU is FMA contraction / order
+//   fast   : -O3 -march=native -ffast-math, mirroring the reference Release
+//            flags (cmake/compilers.cmake:49,138); timed CPU baseline.
+//
+// Choices where the reference source cannot pin the arithmetic (no Fortran
+// compiler is available to run it):
+//   * NORM2 is evaluated with gfortran's scaled algorithm (norm2s below);
+//   * default-real literals follow standard Fortran kinds: only sqrt(2.0) in
+//     initBW (prob.F90:246-252) is inexact and is taken in single precision;
+//   * dot_product is the sequential sum starting from 0.
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+#include <algorithm>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#ifdef GAM_ORACLE_OWN_MATH
+#include "../mage_b200/csrc/gam_math.cuh"
+#define O_ERFC(x) gam::gam_erfc(x)
+#define O_EXP(x) gam::gam_exp(x)
+#else
+#define O_ERFC(x) std::erfc(x)
+#define O_EXP(x) std::exp(x)
+#endif
+
+namespace orc {
+
+// ---------------------------------------------------------------- constants
+// src/base/kdefs.F90:14-21, src/base/defs/gdefs.F90:8-30
+static const double TINY = 1.0e-12, HUGE_ = 1.0e12;
+static const double PI = 3.141592653589793;  // 4*atan(1) in double
+enum { NVAR = 5, NDIM = 3, recLen = 8, limLen = 4, vecLen = 16, Nr2 = 4, Nl2 = 2 };
+enum { DEN = 0, MOMX = 1, MOMY = 2, MOMZ = 3, ENERGY = 4 };
+enum { VELX = 1, VELY = 2, VELZ = 3, PRESSURE = 4 };
+enum { IDIR = 0, JDIR = 1, KDIR = 2 };
+enum { XDIR = 0, YDIR = 1, ZDIR = 2 };
+enum { NORMX = 0, NORMY, NORMZ, TAN1X, TAN1Y, TAN1Z, TAN2X, TAN2Y, TAN2Z };
+enum { XNQI = 0, YNQI, XNQJ, YNQJ };
+enum { LEFT = 0, RIGHT = 1 };
+static const int SgnLR[2] = {-1, 1};  // stress.F90:19
+
+// boundary kinds (a subset of bcs.F90)
+enum { BC_PERIODIC = 0, BC_NONE = 1 };
+
+// interpolation weights, recon.F90:22-23,28-29
+static double interpWgt[8], interpWgt6[8], Up7C[7];
+static void init_weights() {
+    const int w8[8] = {-3, 29, -139, 533, 533, -139, 29, -3};
+    const int w6[8] = {0, 1, -8, 37, 37, -8, 1, 0};
+    const int u7[7] = {-3, 25, -101, 319, 214, -38, 4};
+    for (int n = 0; n < 8; n++) interpWgt[n] = (double)w8[n] / 840.0;
+    for (int n = 0; n < 8; n++) interpWgt6[n] = (double)w6[n] / 60.0;
+    for (int n = 0; n < 7; n++) Up7C[n] = (double)u7[n] / 420.0;
+}
+
+// Gauss-Legendre 12 point, quadrature.F90:10-27
+static const double gA[12] = {
+    0.1252334085114689154724, 0.3678314989981801937527, 0.5873179542866174472967,
+    0.7699026741943046870369, 0.9041172563704748566785, 0.9815606342467192506906,
+    -0.1252334085114689154724, -0.3678314989981801937527, -0.5873179542866174472967,
+    -0.7699026741943046870369, -0.9041172563704748566785, -0.9815606342467192506906};
+static const double gWgt[12] = {
+    0.2491470458134027850006, 0.233492536538354808761, 0.203167426723065921749,
+    0.160078328543346226335, 0.1069393259953184309603, 0.0471753363865118271946,
+    0.2491470458134027850006, 0.233492536538354808761, 0.203167426723065921749,
+    0.160078328543346226335, 0.1069393259953184309603, 0.0471753363865118271946};
+
+// ---------------------------------------------------------------- arrays
+// Fortran array A(l0:u0, l1:u1, l2:u2, 0:nc-1), column-major.
+struct F4 {
+    std::vector<double> v;
+    int l0 = 0, l1 = 0, l2 = 0, n0 = 0, n1 = 0, n2 = 0, nc = 0;
+    void alloc(int a0, int b0, int a1, int b1, int a2, int b2, int ncomp, double fill = 0.0) {
+        l0 = a0; l1 = a1; l2 = a2;
+        n0 = b0 - a0 + 1; n1 = b1 - a1 + 1; n2 = b2 - a2 + 1; nc = ncomp;
+        v.assign((size_t)n0 * n1 * n2 * nc, fill);
+    }
+    inline size_t idx(int i, int j, int k, int c) const {
+        return (size_t)(i - l0) + (size_t)n0 * ((size_t)(j - l1) + (size_t)n1 * ((size_t)(k - l2) + (size_t)n2 * c));
+    }
+    inline double& operator()(int i, int j, int k, int c = 0) { return v[idx(i, j, k, c)]; }
+    inline double operator()(int i, int j, int k, int c = 0) const { return v[idx(i, j, k, c)]; }
+    inline double* comp(int c) { return v.data() + (size_t)n0 * n1 * n2 * c; }
+    inline const double* comp(int c) const { return v.data() + (size_t)n0 * n1 * n2 * c; }
+    void fill(double x) { std::fill(v.begin(), v.end(), x); }
+};
+
+struct Params {  // mirrored by oracle/oracle.py (ctypes)
+    int Nip, Njp, Nkp;
+    int doMHD, doLFMLim, do25D, doBackground, up7, fixedTimestep;
+    double gamma, CFL, pdmb, Vd0, cHogH, cHogM, dFloor, pFloor;
+    double tFin, dt0, limDT0, fixedDT;
+    int bc[6];
+};
+
+struct Model {
+    double gamma, CFL, Vd0, cHogH, cHogM;
+    double t = 0, tFin, dt = 0, dt0 = 0, limDT0;
+    int ts = 0;
+    bool fixedTimestep, doMHD, doLFMLim, do25D, doBackground, up7;
+};
+
+struct Grid {
+    int Nip, Njp, Nkp, Ni, Nj, Nk;
+    int is, ie, js, je, ks, ke, isg, ieg, jsg, jeg, ksg, keg;
+    int isDT, ieDT, jsDT, jeDT, ksDT, keDT;
+    F4 xyz, xyzcc, xfc, di, dj, dk, volume, Tf, Te, Teb, face, edge;
+    F4 fcB0, edgB0, B0, bFlux0, dpB0;  // background (cell-sized, background.F90:43-47)
+    int bc[6];
+    // allocation helpers
+    void cellArr(F4& a, int nc, double f = 0.0) const { a.alloc(isg, ieg, jsg, jeg, ksg, keg, nc, f); }
+    void faceArr(F4& a, int nc, double f = 0.0) const { a.alloc(isg, ieg + 1, jsg, jeg + 1, ksg, keg + 1, nc, f); }
+};
+
+struct State {
+    double time = -HUGE_;
+    F4 Gas, magFlux, Efld, Bxyz;
+};
+
+// global limiter parameters (recon.F90:27 pdmb, gdefs.F90:12 floors)
+static double pdmb = 0.75, dFloor = TINY, pFloor = TINY;
+
+static inline double sgn(double b) { return std::copysign(1.0, b); }  // sign(1.0,b)
+
+// gfortran NORM2: scaled sum of squares
+static inline double norm2s(const double* a, int n) {
+    double scale = 1.0, res = 0.0;
+    for (int q = 0; q < n; q++) {
+        if (a[q] != 0.0) {
+            double ax = std::fabs(a[q]);
+            if (scale < ax) {
+                double val = scale / ax;
+                res = 1.0 + res * val * val;
+                scale = ax;
+            } else {
+                double val = ax / scale;
+                res += val * val;
+            }
+        }
+    }
+    return scale * std::sqrt(res);
+}
+static inline void cross(const double* a, const double* b, double* c) {  // math.F90:265-274
+    c[0] = a[1] * b[2] - a[2] * b[1];
+    c[1] = a[2] * b[0] - a[0] * b[2];
+    c[2] = a[0] * b[1] - a[1] * b[0];
+}
+static inline double dot3(const double* a, const double* b) {
+    double s = 0.0;
+    for (int q = 0; q < 3; q++) s += a[q] * b[q];
+    return s;
+}
+
+// ---------------------------------------------------------------- EOS
+// gamutils.F90:301-321 CellC2P
+static void CellC2P(const Model& M, const double* Con, double* Prim) {
+    double rho = Con[DEN];
+    double Vx = Con[MOMX] / rho, Vy = Con[MOMY] / rho, Vz = Con[MOMZ] / rho;
+    double E = Con[ENERGY];
+    double KinE = 0.5 * rho * (Vx * Vx + Vy * Vy + Vz * Vz);
+    Prim[DEN] = std::max(rho, dFloor);
+    Prim[VELX] = Vx;
+    Prim[VELY] = Vy;
+    Prim[VELZ] = Vz;
+    Prim[PRESSURE] = std::max((M.gamma - 1) * (E - KinE), pFloor);
+}
+// gamutils.F90:362-383 CellP2C
+static void CellP2C(const Model& M, const double* Prim, double* Con) {
+    double rho = std::max(Prim[DEN], dFloor);
+    double Vx = Prim[VELX], Vy = Prim[VELY], Vz = Prim[VELZ];
+    double IntE = std::max(Prim[PRESSURE], pFloor) / (M.gamma - 1);
+    double KinE = 0.5 * rho * (Vx * Vx + Vy * Vy + Vz * Vz);
+    Con[DEN] = rho;
+    Con[MOMX] = rho * Vx;
+    Con[MOMY] = rho * Vy;
+    Con[MOMZ] = rho * Vz;
+    Con[ENERGY] = IntE + KinE;
+}
+
+// ---------------------------------------------------------------- loaders
+// gamutils.F90:64-130 gamLoadBlock / gamLoadBlockI. Qb[n][i], n = 0..2*Nx2-1
+// stands for offset n-Nx2 along direction d from (iS,j,k).
+static inline void loadBlock(const Grid& G, const double* Q, bool iface, int iS, int j, int k, int iMax,
+                             int d, int Nx2, double (*Qb)[vecLen]) {
+    long ni = iface ? G.Ni + 1 : G.Ni, nj = iface ? G.Nj + 1 : G.Nj;
+    long l0 = (iS - G.isg) + (long)(j - G.jsg) * ni + (long)(k - G.ksg) * ni * nj;
+    long nSt = (d == IDIR) ? 1 : (d == JDIR ? ni : ni * nj);
+    for (int n = 0; n < 2 * Nx2; n++)
+        for (int i = 0; i < vecLen; i++) Qb[n][i] = 0.0;
+    for (int n = -Nx2; n < Nx2; n++) {
+        long l = l0 + nSt * n;
+        for (int i = 0; i < iMax; i++) Qb[n + Nx2][i] = Q[l + i];
+    }
+}
+
+// ---------------------------------------------------------------- recon
+// recon.F90:202-214 Central8
+static inline void Central8(const double (*Qb)[vecLen], double* Qi) {
+    for (int i = 0; i < vecLen; i++) {
+        double s = 0.0;
+        for (int n = 0; n < recLen; n++) s += interpWgt[n] * Qb[n][i];
+        Qi[i] = s;
+    }
+}
+// recon.F90:231-272 pdmLR
+static inline void pdmLR(const double (*Qb)[vecLen], const double* Qi, double* Ql, double* Qr) {
+    for (int i = 0; i < vecLen; i++) {
+        double v0 = Qb[0][i], v1 = Qb[1][i], v2 = Qb[2][i], v3 = Qb[3][i];
+        double maxV = std::max(v1, v2), minV = std::min(v1, v2);
+        double vN = std::max(minV, std::min(Qi[i], maxV));
+        double dv0 = pdmb * (v1 - v0), dv1 = pdmb * (v2 - v1), dv2 = pdmb * (v3 - v2);
+        double s0 = sgn(dv0), s1 = sgn(dv1), s2 = sgn(dv2);
+        double q0 = std::fabs(s0 + s1), q1 = std::fabs(s1 + s2);
+        double dvL = vN - v1, dvR = v2 - vN;
+        Ql[i] = vN - s1 * std::max(0.0, std::fabs(dvL) - q0 * std::fabs(dv0));
+        Qr[i] = vN + s1 * std::max(0.0, std::fabs(dvR) - q1 * std::fabs(dv2));
+    }
+}
+// recon.F90:275-301 PDM
+static inline double PDM(double q0, double q1, double q2, double qI) {
+    double maxQ = std::max(q1, q2), minQ = std::min(q1, q2);
+    double qN = std::max(minQ, std::min(qI, maxQ));
+    double dq0 = pdmb * (q1 - q0), dq1 = pdmb * (q2 - q1);
+    double s0 = sgn(dq0), s1 = sgn(dq1);
+    double s01 = std::fabs(s0 + s1);
+    double dqL = qN - q1;
+    return qN - s1 * std::max(0.0, std::fabs(dqL) - s01 * std::fabs(dq0));
+}
+// recon.F90:304-310 Up7
+static inline double Up7(double q0, double q1, double q2, double q3, double q4, double q5, double q6) {
+    return q0 * Up7C[0] + q1 * Up7C[1] + q2 * Up7C[2] + q3 * Up7C[3] + q4 * Up7C[4] + q5 * Up7C[5] +
+           q6 * Up7C[6];
+}
+// recon.F90:125-158 Cen8LRs and :162-198 Up7LRs (the GetLRs choice, init.F90:441-454)
+static bool g_up7 = false;
+static void GetLRs(const double (*dV)[vecLen], const double (*nQ)[vecLen], const double (*Q)[vecLen],
+                   const double* Vi, double* Ql, double* Qr) {
+    double QdV[recLen][vecLen];
+    for (int n = 0; n < recLen; n++)
+        for (int i = 0; i < vecLen; i++) QdV[n][i] = dV[n][i] * Q[n][i];
+    if (!g_up7) {
+        double Qi[vecLen];
+        Central8(QdV, Qi);
+        for (int i = 0; i < vecLen; i++) Qi[i] = Qi[i] / Vi[i];
+        pdmLR(nQ, Qi, Ql, Qr);
+    } else {
+        for (int i = 0; i < vecLen; i++) {
+            Ql[i] = Up7(QdV[0][i], QdV[1][i], QdV[2][i], QdV[3][i], QdV[4][i], QdV[5][i], QdV[6][i]) / Vi[i];
+            Qr[i] = Up7(QdV[7][i], QdV[6][i], QdV[5][i], QdV[4][i], QdV[3][i], QdV[2][i], QdV[1][i]) / Vi[i];
+            Ql[i] = PDM(nQ[0][i], nQ[1][i], nQ[2][i], Ql[i]);
+            Qr[i] = PDM(nQ[3][i], nQ[2][i], nQ[1][i], Qr[i]);
+        }
+    }
+}
+// recon.F90:96-122 BlockLRs
+static void BlockLRs(const double (*VolB)[vecLen], const double (*nQb)[limLen][vecLen],
+                     const double (*Qb)[recLen][vecLen], double (*Ql)[vecLen], double (*Qr)[vecLen], int NumV) {
+    double Vi[vecLen];
+    Central8(VolB, Vi);
+    for (int nv = 0; nv < NumV; nv++) GetLRs(VolB, nQb[nv], Qb[nv], Vi, Ql[nv], Qr[nv]);
+}
+// recon.F90:39-93 BlockStateLRs with its BlockCon2Prim
+static void BlockCon2Prim(const Model& M, const double (*inCon)[recLen][vecLen], double (*oPrim)[recLen][vecLen],
+                          int xLen) {
+    for (int n = 0; n < xLen; n++)
+        for (int i = 0; i < vecLen; i++) {
+            double D = std::max(inCon[DEN][n][i], dFloor);
+            double Mx = inCon[MOMX][n][i], My = inCon[MOMY][n][i], Mz = inCon[MOMZ][n][i];
+            double E = inCon[ENERGY][n][i];
+            double KinE = 0.5 * (Mx * Mx + My * My + Mz * Mz) / D;
+            double P = std::max((M.gamma - 1) * (E - KinE), pFloor);
+            oPrim[DEN][n][i] = D;
+            oPrim[VELX][n][i] = Mx / D;
+            oPrim[VELY][n][i] = My / D;
+            oPrim[VELZ][n][i] = Mz / D;
+            oPrim[PRESSURE][n][i] = P;
+        }
+}
+
+// ---------------------------------------------------------------- fluxes
+// stress.F90:432-511 GasKinFlux
+static void GasKinFlux(const Model& M, int q, const double (*PrimLRB)[vecLen], const double (*TfB)[vecLen],
+                       double (*gFlxB)[vecLen], double (*dW)[vecLen]) {
+    const double s = (double)SgnLR[q];
+    for (int i = 0; i < vecLen; i++) {
+        double D = PrimLRB[DEN][i], P = PrimLRB[PRESSURE][i];
+        double Vx = PrimLRB[VELX][i], Vy = PrimLRB[VELY][i], Vz = PrimLRB[VELZ][i];
+        double E = 0.5 * D * (Vx * Vx + Vy * Vy + Vz * Vz) + P / (M.gamma - 1);
+        double lambda = D / (2 * P);
+        double Vn = TfB[NORMX][i] * Vx + TfB[NORMY][i] * Vy + TfB[NORMZ][i] * Vz;
+        double Vt1 = TfB[TAN1X][i] * Vx + TfB[TAN1Y][i] * Vy + TfB[TAN1Z][i] * Vz;
+        double Vt2 = TfB[TAN2X][i] * Vx + TfB[TAN2Y][i] * Vy + TfB[TAN2Z][i] * Vz;
+        double Vn0 = 0.5 * O_ERFC(s * std::sqrt(lambda) * Vn);
+        double Vn1 = Vn * Vn0 - 0.5 * s * O_EXP(-(lambda * Vn * Vn)) / std::sqrt(PI * lambda);
+        gFlxB[DEN][i] = gFlxB[DEN][i] + D * Vn1;
+        gFlxB[ENERGY][i] = gFlxB[ENERGY][i] + (E + 0.5 * P) * Vn1 + 0.5 * P * Vn0 * Vn;
+        double fMn = D * Vn * Vn1 + P * Vn0;
+        double fMt1 = D * Vt1 * Vn1;
+        double fMt2 = D * Vt2 * Vn1;
+        double fMx = TfB[NORMX][i] * fMn + TfB[TAN1X][i] * fMt1 + TfB[TAN2X][i] * fMt2;
+        double fMy = TfB[NORMY][i] * fMn + TfB[TAN1Y][i] * fMt1 + TfB[TAN2Y][i] * fMt2;
+        double fMz = TfB[NORMZ][i] * fMn + TfB[TAN1Z][i] * fMt1 + TfB[TAN2Z][i] * fMt2;
+        gFlxB[MOMX][i] = gFlxB[MOMX][i] + fMx;
+        gFlxB[MOMY][i] = gFlxB[MOMY][i] + fMy;
+        gFlxB[MOMZ][i] = gFlxB[MOMZ][i] + fMz;
+        dW[DEN][i] = dW[DEN][i] + s * D;
+        dW[MOMX][i] = dW[MOMX][i] + s * D * Vx;
+        dW[MOMY][i] = dW[MOMY][i] + s * D * Vy;
+        dW[MOMZ][i] = dW[MOMZ][i] + s * D * Vz;
+        dW[ENERGY][i] = dW[ENERGY][i] + s * E;
+    }
+}
+// stress.F90:513-599 MagKinFlux (Boris off: Vac2 = Va2)
+static void MagKinFlux(const Model& M, int q, const double (*PrimLRB)[vecLen], const double (*MagLRB)[vecLen],
+                       const double* Bn, const double (*TfB)[vecLen], double (*mFlxB)[vecLen],
+                       const double (*B0)[vecLen], const double* B0n, double* bbD, double* VaD) {
+    const double s = (double)SgnLR[q];
+    for (int i = 0; i < vecLen; i++) {
+        double D = PrimLRB[DEN][i], P = PrimLRB[PRESSURE][i];
+        double Bx = MagLRB[XDIR][i], By = MagLRB[YDIR][i], Bz = MagLRB[ZDIR][i];
+        double B0x = B0[XDIR][i], B0y = B0[YDIR][i], B0z = B0[ZDIR][i];
+        double dPb = 0.5 * (Bx * Bx + By * By + Bz * Bz);
+        double Va2;
+        if (M.doBackground) {
+            double sx = Bx + B0x, sy = By + B0y, sz = Bz + B0z;
+            Va2 = (sx * sx + sy * sy + sz * sz) / D;
+            bbD[i] = bbD[i] + 0.5 * (sx * sx + sy * sy + sz * sz);
+        } else {
+            Va2 = 2 * dPb / D;
+            bbD[i] = bbD[i] + 0.5 * (Bx * Bx + By * By + Bz * Bz);
+        }
+        double Vac2 = Va2;
+        double Vx = PrimLRB[VELX][i], Vy = PrimLRB[VELY][i], Vz = PrimLRB[VELZ][i];
+        double Nx = TfB[NORMX][i], Ny = TfB[NORMY][i], Nz = TfB[NORMZ][i];
+        double Vn = Nx * Vx + Ny * Vy + Nz * Vz;
+        double lambda = 1 / (2 * P / D + Vac2);
+        double Vn0 = 0.5 * O_ERFC(s * std::sqrt(lambda) * Vn);
+        VaD[i] = VaD[i] + 0.5 * std::sqrt(Vac2);
+        mFlxB[XDIR][i] = mFlxB[XDIR][i] + Vn0 * (dPb * Nx - Bx * Bn[i]);
+        mFlxB[YDIR][i] = mFlxB[YDIR][i] + Vn0 * (dPb * Ny - By * Bn[i]);
+        mFlxB[ZDIR][i] = mFlxB[ZDIR][i] + Vn0 * (dPb * Nz - Bz * Bn[i]);
+        if (M.doBackground) {
+            double BdB0 = B0x * Bx + B0y * By + B0z * Bz;
+            mFlxB[XDIR][i] = mFlxB[XDIR][i] + Vn0 * (-(B0x * Bn[i]) - Bx * B0n[i] + BdB0 * Nx);
+            mFlxB[YDIR][i] = mFlxB[YDIR][i] + Vn0 * (-(B0y * Bn[i]) - By * B0n[i] + BdB0 * Ny);
+            mFlxB[ZDIR][i] = mFlxB[ZDIR][i] + Vn0 * (-(B0z * Bn[i]) - Bz * B0n[i] + BdB0 * Nz);
+        }
+    }
+}
+
+// gFlx(i,j,k,nv,d) stored as F4 with component nv + 5*d; mFlx with x + 3*d
+// stress.F90:204-429 Fluxes
+static void Fluxes(const Model& M, const Grid& G, const State& nS, const State& hS, int iB, int j, int k, int dN,
+                   F4& gFlx, F4& mFlx) {
+    int ie = G.ie + (dN == IDIR ? 1 : 0);
+    int iMax = std::min((int)vecLen, ie - iB + 1);
+    int isB = iB;
+
+    double VolB[recLen][vecLen];
+    double ConB[NVAR][recLen][vecLen], MagB[NDIM][recLen][vecLen];
+    double nConB[NVAR][limLen][vecLen], nMagB[NDIM][limLen][vecLen];
+    double TfB[9][vecLen], faB[vecLen];
+    double PrimL[NVAR][vecLen], PrimR[NVAR][vecLen], MagL[NDIM][vecLen], MagR[NDIM][vecLen];
+    double gFlxB[NVAR][vecLen], mFlxB[NDIM][vecLen], dW[NVAR][vecLen], VaD[vecLen], bbD[vecLen];
+    double B0[NDIM][vecLen], B0n[vecLen], Bn[vecLen];
+    std::memset(gFlxB, 0, sizeof(gFlxB));
+    std::memset(mFlxB, 0, sizeof(mFlxB));
+    std::memset(dW, 0, sizeof(dW));
+    std::memset(VaD, 0, sizeof(VaD));
+    std::memset(bbD, 0, sizeof(bbD));
+    std::memset(TfB, 0, sizeof(TfB));
+    std::memset(faB, 0, sizeof(faB));
+    std::memset(B0, 0, sizeof(B0));
+    std::memset(Bn, 0, sizeof(Bn));
+    std::memset(B0n, 0, sizeof(B0n));
+    std::memset(MagL, 0, sizeof(MagL));
+    std::memset(MagR, 0, sizeof(MagR));
+
+    loadBlock(G, G.volume.comp(0), false, iB, j, k, iMax, dN, Nr2, VolB);
+    for (int i = 0; i < iMax; i++) {
+        for (int n = 0; n < 9; n++) TfB[n][i] = G.Tf(isB + i, j, k, n + 9 * dN);
+        faB[i] = G.face(isB + i, j, k, dN);
+    }
+    if (M.doMHD) {
+        for (int nv = 0; nv < NDIM; nv++) {
+            loadBlock(G, hS.Bxyz.comp(nv), false, iB, j, k, iMax, dN, Nr2, MagB[nv]);
+            const State& lS = M.doLFMLim ? nS : hS;
+            loadBlock(G, lS.Bxyz.comp(nv), false, iB, j, k, iMax, dN, Nl2, nMagB[nv]);
+        }
+        BlockLRs(VolB, nMagB, MagB, MagL, MagR, NDIM);
+        for (int i = 0; i < iMax; i++) Bn[i] = hS.magFlux(isB + i, j, k, dN) / faB[i];
+        if (M.doBackground) {
+            for (int i = 0; i < iMax; i++) {
+                for (int d = 0; d < NDIM; d++) B0[d][i] = G.fcB0(isB + i, j, k, d + 3 * dN);
+                B0n[i] = G.bFlux0(isB + i, j, k, dN) / faB[i];
+            }
+        }
+    }
+    for (int nv = 0; nv < NVAR; nv++) {
+        loadBlock(G, hS.Gas.comp(nv), false, iB, j, k, iMax, dN, Nr2, ConB[nv]);
+        const State& lS = M.doLFMLim ? nS : hS;
+        loadBlock(G, lS.Gas.comp(nv), false, iB, j, k, iMax, dN, Nl2, nConB[nv]);
+    }
+    {  // BlockStateLRs
+        double PrimB[NVAR][recLen][vecLen], nPrimB[NVAR][recLen][vecLen];
+        double nConB8[NVAR][recLen][vecLen];
+        for (int nv = 0; nv < NVAR; nv++)
+            for (int n = 0; n < limLen; n++)
+                for (int i = 0; i < vecLen; i++) nConB8[nv][n][i] = nConB[nv][n][i];
+        BlockCon2Prim(M, nConB8, nPrimB, limLen);
+        BlockCon2Prim(M, ConB, PrimB, recLen);
+        double nPrim4[NVAR][limLen][vecLen];
+        for (int nv = 0; nv < NVAR; nv++)
+            for (int n = 0; n < limLen; n++)
+                for (int i = 0; i < vecLen; i++) nPrim4[nv][n][i] = nPrimB[nv][n][i];
+        BlockLRs(VolB, nPrim4, PrimB, PrimL, PrimR, NVAR);
+    }
+    if (M.doMHD) {
+        MagKinFlux(M, LEFT, PrimL, MagL, Bn, TfB, mFlxB, B0, B0n, bbD, VaD);
+        MagKinFlux(M, RIGHT, PrimR, MagR, Bn, TfB, mFlxB, B0, B0n, bbD, VaD);
+        for (int nv = 0; nv < NDIM; nv++)
+            for (int i = 0; i < iMax; i++) mFlx(isB + i, j, k, nv + 3 * dN) = faB[i] * mFlxB[nv][i];
+    }
+    std::memset(gFlxB, 0, sizeof(gFlxB));
+    std::memset(dW, 0, sizeof(dW));
+    GasKinFlux(M, LEFT, PrimL, TfB, gFlxB, dW);
+    GasKinFlux(M, RIGHT, PrimR, TfB, gFlxB, dW);
+    const double alphaS = 1.0;
+    for (int nv = 0; nv < NVAR; nv++)
+        for (int i = 0; i < iMax; i++) gFlxB[nv][i] = gFlxB[nv][i] - alphaS * M.cHogH * VaD[i] * dW[nv][i];
+    for (int nv = 0; nv < NVAR; nv++)
+        for (int i = 0; i < iMax; i++) gFlx(isB + i, j, k, nv + 5 * dN) = faB[i] * gFlxB[nv][i];
+}
+
+// stress.F90:41-198 CalcStress
+static void CalcStress(const Model& M, const Grid& G, const State& nS, const State& hS, F4& gFlx, F4& mFlx,
+                       F4& dGasH, F4& dGasM) {
+    int nFlx = M.do25D ? 2 : 3;
+    int ks = G.ks, ke = M.do25D ? G.ks : G.ke;
+#pragma omp parallel
+    {
+        for (int d = 0; d < nFlx; d++) {
+            if (d == IDIR) {
+#pragma omp for collapse(2) nowait
+                for (int k = ks; k <= ke; k++)
+                    for (int j = G.js; j <= G.je; j++)
+                        for (int iB = G.is; iB <= G.ie + 1; iB += vecLen) Fluxes(M, G, nS, hS, iB, j, k, d, gFlx, mFlx);
+            } else if (d == JDIR) {
+#pragma omp for collapse(2) nowait
+                for (int k = ks; k <= ke; k++)
+                    for (int iB = G.is; iB <= G.ie; iB += vecLen)
+                        for (int j = G.js; j <= G.je + 1; j++) Fluxes(M, G, nS, hS, iB, j, k, d, gFlx, mFlx);
+            } else {
+#pragma omp for collapse(2) nowait
+                for (int j = G.js; j <= G.je; j++)
+                    for (int iB = G.is; iB <= G.ie; iB += vecLen)
+                        for (int k = ks; k <= ke + 1; k++) Fluxes(M, G, nS, hS, iB, j, k, d, gFlx, mFlx);
+            }
+        }
+    }
+#pragma omp parallel for collapse(2)
+    for (int k = G.ks; k <= G.ke; k++)
+        for (int j = G.js; j <= G.je; j++)
+            for (int i = G.is; i <= G.ie; i++) {
+                double dV = G.volume(i, j, k);
+                for (int nv = 0; nv < NVAR; nv++)
+                    dGasH(i, j, k, nv) = (gFlx(i, j, k, nv + 5 * IDIR) - gFlx(i + 1, j, k, nv + 5 * IDIR) +
+                                          gFlx(i, j, k, nv + 5 * JDIR) - gFlx(i, j + 1, k, nv + 5 * JDIR) +
+                                          gFlx(i, j, k, nv + 5 * KDIR) - gFlx(i, j, k + 1, nv + 5 * KDIR)) /
+                                         dV;
+                if (M.doMHD) {
+                    for (int x = 0; x < NDIM; x++) {
+                        dGasM(i, j, k, x) = (mFlx(i, j, k, x + 3 * IDIR) - mFlx(i + 1, j, k, x + 3 * IDIR) +
+                                             mFlx(i, j, k, x + 3 * JDIR) - mFlx(i, j + 1, k, x + 3 * JDIR) +
+                                             mFlx(i, j, k, x + 3 * KDIR) - mFlx(i, j, k + 1, x + 3 * KDIR)) /
+                                            dV;
+                        if (M.doBackground) dGasM(i, j, k, x) = dGasM(i, j, k, x) + G.dpB0(i, j, k, x);
+                    }
+                }
+            }
+}
+
+// ---------------------------------------------------------------- E field
+static void getNormalPlane(int dN, int* e1, int* e2) {  // metric.F90:174-190
+    e1[0] = e1[1] = e1[2] = 0;
+    e2[0] = e2[1] = e2[2] = 0;
+    if (dN == IDIR) { e1[1] = 1; e2[2] = 1; }
+    else if (dN == JDIR) { e1[0] = 1; e2[2] = 1; }
+    else { e1[0] = 1; e2[1] = 1; }
+}
+// fields.F90:235-285 Mom2Face
+static void Mom2Face(const Grid& G, const F4& W, double (*VfB)[vecLen], int iB, int j, int k, int iMax, int dT) {
+    double VolB[recLen][vecLen], DenB[recLen][vecLen], MomB[3][recLen][vecLen], VelB[3][recLen][vecLen];
+    double dV[vecLen];
+    loadBlock(G, G.volume.comp(0), false, iB, j, k, iMax, dT, Nr2, VolB);
+    loadBlock(G, W.comp(DEN), false, iB, j, k, iMax, dT, Nr2, DenB);
+    for (int d = 0; d < 3; d++) loadBlock(G, W.comp(MOMX + d), false, iB, j, k, iMax, dT, Nr2, MomB[d]);
+    for (int d = 0; d < 3; d++)
+        for (int i = 0; i < vecLen; i++) VfB[d][i] = 0.0;
+    for (int n = 0; n < recLen; n++)
+        for (int i = 0; i < iMax; i++)
+            for (int d = 0; d < 3; d++) VelB[d][n][i] = VolB[n][i] * MomB[d][n][i] / std::max(DenB[n][i], dFloor);
+    for (int i = 0; i < iMax; i++) {
+        double s = 0.0;
+        for (int n = 0; n < recLen; n++) s += interpWgt[n] * VolB[n][i];
+        dV[i] = std::max(s, TINY);
+    }
+    for (int d = 0; d < 3; d++)
+        for (int i = 0; i < iMax; i++) {
+            double s = 0.0;
+            for (int n = 0; n < recLen; n++) s += interpWgt[n] * VelB[d][n][i];
+            VfB[d][i] = s / dV[i];
+        }
+}
+// fields.F90:457-517 GetCornerV
+static void GetCornerV(const Grid& G, const F4& Vf, double* v1, double* v2, double* vDiff, int iB, int j, int k,
+                       int iMax, int dN, int dT1, int dT2) {
+    double AreaB[recLen][vecLen], VelB[recLen][vecLen], VxyzC[3][vecLen], dA[vecLen];
+    std::memset(VxyzC, 0, sizeof(VxyzC));
+    std::memset(dA, 0, sizeof(dA));
+    loadBlock(G, G.face.comp(dT1), true, iB, j, k, iMax, dT2, Nr2, AreaB);
+    for (int i = 0; i < iMax; i++) {
+        double s = 0.0;
+        for (int n = 0; n < recLen; n++) s += interpWgt[n] * AreaB[n][i];
+        dA[i] = std::max(s, TINY);
+    }
+    for (int d = 0; d < 3; d++) {
+        loadBlock(G, Vf.comp(d), false, iB, j, k, iMax, dT2, Nr2, VelB);
+        for (int i = 0; i < iMax; i++) {
+            double s = 0.0;
+            for (int n = 0; n < recLen; n++) s += interpWgt[n] * (AreaB[n][i] * VelB[n][i]);
+            VxyzC[d][i] = s / dA[i];
+        }
+    }
+    for (int i = 0; i < iMax; i++) {
+        int iG = iB + i;
+        v1[i] = VxyzC[XDIR][i] * G.Te(iG, j, k, TAN1X + 9 * dN) + VxyzC[YDIR][i] * G.Te(iG, j, k, TAN1Y + 9 * dN) +
+                VxyzC[ZDIR][i] * G.Te(iG, j, k, TAN1Z + 9 * dN);
+        v2[i] = VxyzC[XDIR][i] * G.Te(iG, j, k, TAN2X + 9 * dN) + VxyzC[YDIR][i] * G.Te(iG, j, k, TAN2Y + 9 * dN) +
+                VxyzC[ZDIR][i] * G.Te(iG, j, k, TAN2Z + 9 * dN);
+        vDiff[i] = std::sqrt(v1[i] * v1[i] + v2[i] * v2[i]);
+    }
+}
+// fields.F90:427-454 GetCornerD
+static void GetCornerD(const Grid& G, const F4& Gas, double* Dc, int iB, int j, int k, int iMax, int dN) {
+    int e1[3], e2[3];
+    getNormalPlane(dN, e1, e2);
+    for (int i = 0; i < iMax; i++) {
+        int iG = iB + i;
+        Dc[i] = 0.25 * (Gas(iG, j, k, DEN) + Gas(iG - e1[0], j - e1[1], k - e1[2], DEN) +
+                        Gas(iG - e2[0], j - e2[1], k - e2[2], DEN) +
+                        Gas(iG - e1[0] - e2[0], j - e1[1] - e2[1], k - e1[2] - e2[2], DEN));
+    }
+}
+// fields.F90:288-362 EdgeLRs
+static void EdgeLRs(const Model& M, const Grid& G, const F4& bFluxn, const F4& bFluxHf, double* bL, double* bR,
+                    double* fA, int iB, int j, int k, int iMax, int dN, int dT1, int dT2) {
+    double AreaB[recLen][vecLen], VolB[recLen][vecLen], nAreaB[limLen][vecLen];
+    double MagB[1][recLen][vecLen], nMagB[1][limLen][vecLen], MagLB[1][vecLen], MagRB[1][vecLen];
+    for (int i = 0; i < vecLen; i++) fA[i] = bL[i] = bR[i] = 0.0;
+    std::memset(VolB, 0, sizeof(VolB));
+    loadBlock(G, G.face.comp(dT1), true, iB, j, k, iMax, dT2, Nr2, AreaB);
+    loadBlock(G, bFluxHf.comp(dT1), true, iB, j, k, iMax, dT2, Nr2, MagB[0]);
+    loadBlock(G, G.face.comp(dT1), true, iB, j, k, iMax, dT2, Nl2, nAreaB);
+    loadBlock(G, (M.doLFMLim ? bFluxn : bFluxHf).comp(dT1), true, iB, j, k, iMax, dT2, Nl2, nMagB[0]);
+    for (int i = 0; i < iMax; i++) {
+        for (int n = 0; n < recLen; n++) VolB[n][i] = AreaB[n][i];
+        for (int n = 0; n < recLen; n++) MagB[0][n][i] = MagB[0][n][i] / std::max(AreaB[n][i], TINY);
+        for (int n = 0; n < limLen; n++) nMagB[0][n][i] = nMagB[0][n][i] / std::max(nAreaB[n][i], TINY);
+    }
+    BlockLRs(VolB, nMagB, MagB, MagLB, MagRB, 1);
+    for (int i = 0; i < vecLen; i++) {
+        bL[i] = MagLB[0][i];
+        bR[i] = MagRB[0][i];
+    }
+    for (int i = 0; i < iMax; i++) {
+        double s = 0.0;
+        for (int n = 0; n < recLen; n++) s += interpWgt[n] * AreaB[n][i];
+        fA[i] = s;
+        bL[i] = bL[i] * fA[i];
+        bR[i] = bR[i] * fA[i];
+    }
+}
+// fields.F90:365-424 GetCornerB
+static void GetCornerB(const Model& M, const Grid& G, const F4& bFluxn, const F4& bFluxHf, double* b1, double* b2,
+                       double* Jd, int iB, int j, int k, int iMax, int dN, int dT1, int dT2) {
+    double bT1L[vecLen], bT1R[vecLen], fA1[vecLen], bT2L[vecLen], bT2R[vecLen], fA2[vecLen];
+    EdgeLRs(M, G, bFluxn, bFluxHf, bT1L, bT1R, fA1, iB, j, k, iMax, dN, dT1, dT2);
+    EdgeLRs(M, G, bFluxn, bFluxHf, bT2L, bT2R, fA2, iB, j, k, iMax, dN, dT2, dT1);
+    for (int i = 0; i < iMax; i++) {
+        int iG = iB + i;
+        double xni = G.Teb(iG, j, k, XNQI + 4 * dN), yni = G.Teb(iG, j, k, YNQI + 4 * dN);
+        double xnj = G.Teb(iG, j, k, XNQJ + 4 * dN), ynj = G.Teb(iG, j, k, YNQJ + 4 * dN);
+        double detT = 1.0 / (xni * ynj - xnj * yni);
+        double bT1 = 0.5 * (bT1L[i] + bT1R[i]) / fA1[i];
+        double bT2 = 0.5 * (bT2L[i] + bT2R[i]) / fA2[i];
+        double db1 = (bT1R[i] - bT1L[i]) / fA1[i];
+        double db2 = (bT2R[i] - bT2L[i]) / fA2[i];
+        Jd[i] = db2 - db1;
+        b1[i] = detT * (ynj * bT1 - yni * bT2);
+        b2[i] = detT * (-(xnj * bT1) + xni * bT2);
+        if (M.doBackground) {
+            b1[i] = b1[i] + G.edgB0(iG, j, k, 0 + 2 * dN);
+            b2[i] = b2[i] + G.edgB0(iG, j, k, 1 + 2 * dN);
+        }
+    }
+}
+// fields.F90:70-232 CalcElecField
+static void CalcElecField(const Model& M, const Grid& G, const State& nS, const State& hS, F4& Vf, F4& E) {
+    E.fill(0.0);
+    for (int eD = 0; eD < 3; eD++) {
+        int dT1, dT2, ie, je, ke;
+        if (eD == IDIR) {
+            dT1 = JDIR; dT2 = KDIR;
+            ie = G.ie; je = G.je + 1; ke = G.ke + 1;
+#pragma omp parallel for collapse(2)
+            for (int k = G.ksg; k <= G.keg; k++)
+                for (int iB = G.isg; iB <= G.ieg; iB += vecLen)
+                    for (int j = G.js; j <= G.je + 1; j++) {
+                        int iMax = std::min((int)vecLen, G.ieg - iB + 1);
+                        double VelB[3][vecLen];
+                        Mom2Face(G, hS.Gas, VelB, iB, j, k, iMax, dT1);
+                        for (int i = 0; i < iMax; i++)
+                            for (int d = 0; d < 3; d++) Vf(iB + i, j, k, d) = VelB[d][i];
+                    }
+        } else if (eD == JDIR) {
+            dT1 = KDIR; dT2 = IDIR;
+            ie = G.ie + 1; je = G.je; ke = G.ke + 1;
+#pragma omp parallel for collapse(2)
+            for (int j = G.jsg; j <= G.jeg; j++)
+                for (int iB = G.isg; iB <= G.ieg; iB += vecLen)
+                    for (int k = G.ks; k <= G.ke + 1; k++) {
+                        int iMax = std::min((int)vecLen, G.ieg - iB + 1);
+                        double VelB[3][vecLen];
+                        Mom2Face(G, hS.Gas, VelB, iB, j, k, iMax, dT1);
+                        for (int i = 0; i < iMax; i++)
+                            for (int d = 0; d < 3; d++) Vf(iB + i, j, k, d) = VelB[d][i];
+                    }
+        } else {
+            dT1 = IDIR; dT2 = JDIR;
+            ie = G.ie + 1; je = G.je + 1; ke = G.ke;
+#pragma omp parallel for collapse(2)
+            for (int k = G.ksg; k <= G.keg; k++)
+                for (int j = G.jsg; j <= G.jeg; j++)
+                    for (int iB = G.is; iB <= G.ie + 1; iB += vecLen) {
+                        int iMax = std::min((int)vecLen, G.ie + 1 - iB + 1);
+                        double VelB[3][vecLen];
+                        Mom2Face(G, hS.Gas, VelB, iB, j, k, iMax, dT1);
+                        for (int i = 0; i < iMax; i++)
+                            for (int d = 0; d < 3; d++) Vf(iB + i, j, k, d) = VelB[d][i];
+                    }
+        }
+#pragma omp parallel for collapse(2)
+        for (int k = G.ks; k <= ke; k++)
+            for (int j = G.js; j <= je; j++)
+                for (int iB = G.is; iB <= ie; iB += vecLen) {
+                    int iMax = std::min((int)vecLen, ie - iB + 1);
+                    double v1[vecLen], v2[vecLen], vDiff[vecLen], Dc[vecLen], b1[vecLen], b2[vecLen], Jd[vecLen];
+                    for (int i = 0; i < vecLen; i++) vDiff[i] = 0.0;
+                    GetCornerV(G, Vf, v1, v2, vDiff, iB, j, k, iMax, eD, dT1, dT2);
+                    GetCornerD(G, hS.Gas, Dc, iB, j, k, iMax, eD);
+                    GetCornerB(M, G, nS.magFlux, hS.magFlux, b1, b2, Jd, iB, j, k, iMax, eD, dT1, dT2);
+                    for (int i = 0; i < iMax; i++) {
+                        int iG = iB + i;
+                        double vA = std::sqrt(b1[i] * b1[i] + b2[i] * b2[i]) / std::sqrt(Dc[i]);
+                        vDiff[i] = vDiff[i] + vA;
+                        vDiff[i] = std::min(vDiff[i], M.CFL * G.edge(iG, j, k, eD) / M.dt);
+                        double e = -(v1[i] * b2[i] - v2[i] * b1[i]) + M.Vd0 * vDiff[i] * Jd[i];
+                        E(iG, j, k, eD) = e * G.edge(iG, j, k, eD);
+                    }
+                }
+    }
+}
+// fields.F90:18-51 E2Flux
+static void E2Flux(const Grid& G, F4& magFlux, const F4& E, double dt) {
+#pragma omp parallel for collapse(2)
+    for (int k = G.ks; k <= G.ke + 1; k++)
+        for (int j = G.js; j <= G.je + 1; j++)
+            for (int i = G.is; i <= G.ie + 1; i++) {
+                double dfi = E(i, j + 1, k, KDIR) - E(i, j, k, KDIR) - E(i, j, k + 1, JDIR) + E(i, j, k, JDIR);
+                double dfj = E(i, j, k + 1, IDIR) - E(i, j, k, IDIR) - E(i + 1, j, k, KDIR) + E(i, j, k, KDIR);
+                double dfk = E(i + 1, j, k, JDIR) - E(i, j, k, JDIR) - E(i, j + 1, k, IDIR) + E(i, j, k, IDIR);
+                magFlux(i, j, k, IDIR) = magFlux(i, j, k, IDIR) - dt * dfi;
+                magFlux(i, j, k, JDIR) = magFlux(i, j, k, JDIR) - dt * dfj;
+                magFlux(i, j, k, KDIR) = magFlux(i, j, k, KDIR) - dt * dfk;
+            }
+}
+
+// ---------------------------------------------------------------- field from flux
+// gridutils.F90:648-680 gamCellBxyz
+static inline void gamCellBxyz(const Grid& G, const F4& mf, int i, int j, int k, double* B) {
+    double dV = G.volume(i, j, k);
+    double fI = mf(i, j, k, IDIR), fJ = mf(i, j, k, JDIR), fK = mf(i, j, k, KDIR);
+    double fIp = mf(i + 1, j, k, IDIR), fJp = mf(i, j + 1, k, JDIR), fKp = mf(i, j, k + 1, KDIR);
+    double Div = fIp - fI + fJp - fJ + fKp - fK;
+    for (int x = 0; x < 3; x++) {
+        double xfI = G.xfc(i, j, k, x + 3 * IDIR), xfJ = G.xfc(i, j, k, x + 3 * JDIR), xfK = G.xfc(i, j, k, x + 3 * KDIR);
+        double xfIp = G.xfc(i + 1, j, k, x + 3 * IDIR), xfJp = G.xfc(i, j + 1, k, x + 3 * JDIR),
+               xfKp = G.xfc(i, j, k + 1, x + 3 * KDIR);
+        double b = (fIp * xfIp + fJp * xfJp + fKp * xfKp - fI * xfI - fJ * xfJ - fK * xfK) / dV;
+        B[x] = b - Div * G.xyzcc(i, j, k, x) / dV;
+    }
+}
+// gridutils.F90:281-301 bFlux2Fld
+static void bFlux2Fld(const Grid& G, const F4& magFlux, F4& Bxyz) {
+#pragma omp parallel for collapse(2)
+    for (int k = G.ksg; k <= G.keg; k++)
+        for (int j = G.jsg; j <= G.jeg; j++)
+            for (int i = G.isg; i <= G.ieg; i++) {
+                double B[3];
+                gamCellBxyz(G, magFlux, i, j, k, B);
+                for (int x = 0; x < 3; x++) Bxyz(i, j, k, x) = B[x];
+            }
+}
+
+// ---------------------------------------------------------------- update
+// mhdgroup.F90:299-329 CellMaxwell
+static void CellMaxwell(const Model& M, double* U, const double* dGasM, double dt) {
+    double D = std::max(U[DEN], dFloor);
+    double Mx = U[MOMX], My = U[MOMY], Mz = U[MOMZ], TotE = U[ENERGY];
+    double KinE = 0.5 * (Mx * Mx + My * My + Mz * Mz) / D;
+    double P = std::max((M.gamma - 1) * (TotE - KinE), pFloor);
+    Mx = Mx + dt * dGasM[XDIR];
+    My = My + dt * dGasM[YDIR];
+    Mz = Mz + dt * dGasM[ZDIR];
+    KinE = 0.5 * (Mx * Mx + My * My + Mz * Mz) / D;
+    U[DEN] = D;
+    U[MOMX] = Mx;
+    U[MOMY] = My;
+    U[MOMZ] = Mz;
+    U[ENERGY] = KinE + P / (M.gamma - 1);
+}
+static void CopyState(const Grid& G, const State& a, State& b) {  // mhdgroup.F90:202-256
+    b.Gas.v = a.Gas.v;
+    b.Bxyz.v = a.Bxyz.v;
+    b.magFlux.v = a.magFlux.v;
+    b.time = a.time;
+}
+// mhdgroup.F90:79-200 applyUpdate (single fluid, no Boris)
+static void applyUpdate(const Model& M, const Grid& G, State& S, State& oS, double dt, const F4& dGasH,
+                        const F4& dGasM, const F4& E) {
+    CopyState(G, S, oS);
+    S.time = S.time + dt;
+#pragma omp parallel for collapse(2)
+    for (int k = G.ks; k <= G.ke; k++)
+        for (int j = G.js; j <= G.je; j++)
+            for (int i = G.is; i <= G.ie; i++)
+                for (int nv = 0; nv < NVAR; nv++)  // CellReynolds with Model%dt (mhdgroup.F90:121)
+                    S.Gas(i, j, k, nv) = S.Gas(i, j, k, nv) + M.dt * dGasH(i, j, k, nv);
+    if (!M.doMHD) return;
+    E2Flux(G, S.magFlux, E, dt);
+    bFlux2Fld(G, S.magFlux, S.Bxyz);
+#pragma omp parallel for collapse(2)
+    for (int k = G.ks; k <= G.ke; k++)
+        for (int j = G.js; j <= G.je; j++)
+            for (int i = G.is; i <= G.ie; i++) {
+                double U[NVAR], dPm[NDIM];
+                for (int nv = 0; nv < NVAR; nv++) U[nv] = S.Gas(i, j, k, nv);
+                for (int x = 0; x < NDIM; x++) dPm[x] = dGasM(i, j, k, x);
+                CellMaxwell(M, U, dPm, dt);
+                for (int nv = 0; nv < NVAR; nv++) S.Gas(i, j, k, nv) = U[nv];
+            }
+}
+// mhdgroup.F90:709-717 ExtrapAB2
+static inline double ExtrapAB2(double dt, double Q, double oQ, double odt) {
+    double dQ = (Q - oQ) / odt;
+    return Q + dt * dQ;
+}
+// mhdgroup.F90:444-615 Predictor + PredictCell (AB2, single fluid)
+static void Predictor(const Model& M, const Grid& G, const State& S, const State& oS, State& pS, double pdt) {
+    double odt = S.time - oS.time;
+    if (M.doMHD) {
+#pragma omp parallel for collapse(2)
+        for (int k = G.ksg; k <= G.keg + 1; k++)
+            for (int j = G.jsg; j <= G.jeg + 1; j++)
+                for (int i = G.isg; i <= G.ieg + 1; i++)
+                    for (int d = 0; d < 3; d++)
+                        pS.magFlux(i, j, k, d) = ExtrapAB2(pdt, S.magFlux(i, j, k, d), oS.magFlux(i, j, k, d), odt);
+    }
+    bFlux2Fld(G, pS.magFlux, pS.Bxyz);
+#pragma omp parallel for collapse(2)
+    for (int k = G.ksg; k <= G.keg; k++)
+        for (int j = G.jsg; j <= G.jeg; j++)
+            for (int i = G.isg; i <= G.ieg; i++) {
+                double Q[NVAR], oQ[NVAR], W[NVAR], oW[NVAR], pW[NVAR], pQ[NVAR];
+                for (int nv = 0; nv < NVAR; nv++) {
+                    Q[nv] = S.Gas(i, j, k, nv);
+                    oQ[nv] = oS.Gas(i, j, k, nv);
+                }
+                CellC2P(M, oQ, oW);
+                CellC2P(M, Q, W);
+                for (int nv = 0; nv < NVAR; nv++) pW[nv] = ExtrapAB2(pdt, W[nv], oW[nv], odt);
+                pW[DEN] = std::max(pW[DEN], dFloor);
+                pW[PRESSURE] = std::max(pW[PRESSURE], pFloor);
+                CellP2C(M, pW, pQ);
+                for (int nv = 0; nv < NVAR; nv++) pS.Gas(i, j, k, nv) = pQ[nv];
+            }
+}
+
+// ---------------------------------------------------------------- BCs
+// bcs.F90:279-450 periodic_{i,o}bc{I,J,K}
+static inline bool isCellCenterG(const Grid& G, int i, int j, int k) {
+    return k <= G.keg && j <= G.jeg && i <= G.ieg && k >= G.ksg && j >= G.jsg && i >= G.isg;
+}
+static void periodic_ibcI(const Grid& G, State& S) {
+    for (int k = G.ksg; k <= G.keg + 1; k++)
+        for (int j = G.jsg; j <= G.jeg + 1; j++)
+            for (int n = 1; n <= 4; n++) {
+                int ig = G.is - n, is2 = G.ie - n + 1;
+                if (isCellCenterG(G, ig, j, k)) {
+                    for (int v = 0; v < NVAR; v++) S.Gas(ig, j, k, v) = S.Gas(is2, j, k, v);
+                    for (int x = 0; x < 3; x++) S.Bxyz(ig, j, k, x) = S.Bxyz(is2, j, k, x);
+                }
+                for (int x = 0; x < 3; x++) S.magFlux(ig, j, k, x) = S.magFlux(is2, j, k, x);
+            }
+}
+static void periodic_obcI(const Grid& G, State& S) {
+    for (int k = G.ksg; k <= G.keg + 1; k++)
+        for (int j = G.jsg; j <= G.jeg + 1; j++)
+            for (int n = 1; n <= 4; n++) {
+                int ig = G.ie + n, is2 = G.is + n - 1;
+                if (isCellCenterG(G, ig, j, k)) {
+                    for (int v = 0; v < NVAR; v++) S.Gas(ig, j, k, v) = S.Gas(is2, j, k, v);
+                    for (int x = 0; x < 3; x++) S.Bxyz(ig, j, k, x) = S.Bxyz(is2, j, k, x);
+                }
+                S.magFlux(ig, j, k, JDIR) = S.magFlux(is2, j, k, JDIR);
+                S.magFlux(ig, j, k, KDIR) = S.magFlux(is2, j, k, KDIR);
+                S.magFlux(ig + 1, j, k, IDIR) = S.magFlux(G.is + n, j, k, IDIR);
+            }
+}
+static void periodic_ibcJ(const Grid& G, State& S) {
+    for (int k = G.ksg; k <= G.keg + 1; k++)
+        for (int i = G.isg; i <= G.ieg + 1; i++)
+            for (int n = 1; n <= 4; n++) {
+                int jg = G.js - n, js2 = G.je - n + 1;
+                if (isCellCenterG(G, i, jg, k)) {
+                    for (int v = 0; v < NVAR; v++) S.Gas(i, jg, k, v) = S.Gas(i, js2, k, v);
+                    for (int x = 0; x < 3; x++) S.Bxyz(i, jg, k, x) = S.Bxyz(i, js2, k, x);
+                }
+                for (int x = 0; x < 3; x++) S.magFlux(i, jg, k, x) = S.magFlux(i, js2, k, x);
+            }
+}
+static void periodic_obcJ(const Grid& G, State& S) {
+    for (int k = G.ksg; k <= G.keg + 1; k++)
+        for (int i = G.isg; i <= G.ieg + 1; i++)
+            for (int n = 1; n <= 4; n++) {
+                int jg = G.je + n, js2 = G.js + n - 1;
+                if (isCellCenterG(G, i, jg, k)) {
+                    for (int v = 0; v < NVAR; v++) S.Gas(i, jg, k, v) = S.Gas(i, js2, k, v);
+                    for (int x = 0; x < 3; x++) S.Bxyz(i, jg, k, x) = S.Bxyz(i, js2, k, x);
+                }
+                S.magFlux(i, jg, k, IDIR) = S.magFlux(i, js2, k, IDIR);
+                S.magFlux(i, jg, k, KDIR) = S.magFlux(i, js2, k, KDIR);
+                S.magFlux(i, jg + 1, k, JDIR) = S.magFlux(i, G.js + n, k, JDIR);
+            }
+}
+static void periodic_ibcK(const Model& M, const Grid& G, State& S) {
+    if (M.do25D) {
+        for (int n = 1; n <= 4; n++) {
+            int kg = G.ks - n;
+            for (int j = G.jsg; j <= G.jeg; j++)
+                for (int i = G.isg; i <= G.ieg; i++) {
+                    for (int v = 0; v < NVAR; v++) S.Gas(i, j, kg, v) = S.Gas(i, j, G.ks, v);
+                    for (int x = 0; x < 3; x++) S.Bxyz(i, j, kg, x) = S.Bxyz(i, j, G.ks, x);
+                }
+            for (int j = G.jsg; j <= G.jeg + 1; j++)
+                for (int i = G.isg; i <= G.ieg + 1; i++)
+                    for (int x = 0; x < 3; x++) S.magFlux(i, j, kg, x) = S.magFlux(i, j, G.ks, x);
+        }
+        return;
+    }
+    for (int j = G.jsg; j <= G.jeg + 1; j++)
+        for (int i = G.isg; i <= G.ieg + 1; i++)
+            for (int n = 1; n <= 4; n++) {
+                int kg = G.ks - n, ks2 = G.ke - n + 1;
+                if (isCellCenterG(G, i, j, kg)) {
+                    for (int v = 0; v < NVAR; v++) S.Gas(i, j, kg, v) = S.Gas(i, j, ks2, v);
+                    for (int x = 0; x < 3; x++) S.Bxyz(i, j, kg, x) = S.Bxyz(i, j, ks2, x);
+                }
+                for (int x = 0; x < 3; x++) S.magFlux(i, j, kg, x) = S.magFlux(i, j, ks2, x);
+            }
+}
+static void periodic_obcK(const Model& M, const Grid& G, State& S) {
+    if (M.do25D) {
+        for (int n = 1; n <= 4; n++) {
+            int kg = G.ks + n;
+            for (int j = G.jsg; j <= G.jeg; j++)
+                for (int i = G.isg; i <= G.ieg; i++) {
+                    for (int v = 0; v < NVAR; v++) S.Gas(i, j, kg, v) = S.Gas(i, j, G.ks, v);
+                    for (int x = 0; x < 3; x++) S.Bxyz(i, j, kg, x) = S.Bxyz(i, j, G.ks, x);
+                }
+            for (int j = G.jsg; j <= G.jeg + 1; j++)
+                for (int i = G.isg; i <= G.ieg + 1; i++)
+                    for (int x = 0; x < 3; x++) S.magFlux(i, j, kg, x) = S.magFlux(i, j, G.ks, x);
+        }
+        return;
+    }
+    for (int j = G.jsg; j <= G.jeg + 1; j++)
+        for (int i = G.isg; i <= G.ieg + 1; i++)
+            for (int n = 1; n <= 4; n++) {
+                int kg = G.ke + n, ks2 = G.ks + n - 1;
+                if (isCellCenterG(G, i, j, kg)) {
+                    for (int v = 0; v < NVAR; v++) S.Gas(i, j, kg, v) = S.Gas(i, j, ks2, v);
+                    for (int x = 0; x < 3; x++) S.Bxyz(i, j, kg, x) = S.Bxyz(i, j, ks2, x);
+                }
+                S.magFlux(i, j, kg, IDIR) = S.magFlux(i, j, ks2, IDIR);
+                S.magFlux(i, j, kg, JDIR) = S.magFlux(i, j, ks2, JDIR);
+                S.magFlux(i, j, kg + 1, KDIR) = S.magFlux(i, j, G.ks + n, KDIR);
+            }
+}
+// step.F90:17-55 EnforceBCs (single domain: every boundary is owned)
+static void EnforceBCs(const Model& M, const Grid& G, State& S) {
+    if (G.bc[0] == BC_PERIODIC) periodic_ibcI(G, S);
+    if (G.bc[1] == BC_PERIODIC) periodic_obcI(G, S);
+    if (G.bc[2] == BC_PERIODIC) periodic_ibcJ(G, S);
+    if (G.bc[3] == BC_PERIODIC) periodic_obcJ(G, S);
+    if (G.bc[4] == BC_PERIODIC) periodic_ibcK(M, G, S);
+    if (G.bc[5] == BC_PERIODIC) periodic_obcK(M, G, S);
+}
+
+// ---------------------------------------------------------------- dt
+// gridutils.F90:49-106 CellDT (single fluid, no resistivity, no Boris)
+static inline double CellDT(const Model& M, const Grid& G, const State& S, int i, int j, int k) {
+    double rho = S.Gas(i, j, k, DEN);
+    double Vx = S.Gas(i, j, k, MOMX) / rho, Vy = S.Gas(i, j, k, MOMY) / rho, Vz = S.Gas(i, j, k, MOMZ) / rho;
+    double MagV = std::sqrt(Vx * Vx + Vy * Vy + Vz * Vz);
+    double ke = 0.5 * rho * (MagV * MagV);
+    double e = S.Gas(i, j, k, ENERGY) - ke;
+    double P = (M.gamma - 1) * e;
+    double Cs = std::sqrt(M.gamma * P / rho);
+    double Vfl = MagV, Valf = 0.0, Vdiff = 0.0;
+    if (M.doMHD) {
+        double Bx = S.Bxyz(i, j, k, XDIR), By = S.Bxyz(i, j, k, YDIR), Bz = S.Bxyz(i, j, k, ZDIR);
+        if (M.doBackground) {
+            Bx = Bx + G.B0(i, j, k, XDIR);
+            By = By + G.B0(i, j, k, YDIR);
+            Bz = Bz + G.B0(i, j, k, ZDIR);
+        }
+        double MagB = std::sqrt(Bx * Bx + By * By + Bz * Bz);
+        Valf = MagB / std::sqrt(rho);
+    }
+    double vCFL = Vfl + std::sqrt(Cs * Cs + Valf * Valf) + Vdiff;
+    double dl = std::min(std::min(G.di(i, j, k), G.dj(i, j, k)), G.dk(i, j, k));
+    return M.CFL * dl / vCFL;
+}
+enum { ST_OK = 0, ST_DT_BAD = 1, ST_DT_DISASTER = 2 };
+// step.F90:58-168 CalcDT; failure cases return a status instead of stopping
+static double CalcDT(Model& M, const Grid& G, const State& S, int* status) {
+    *status = ST_OK;
+    if (M.fixedTimestep) return M.dt;
+    double dtOld = M.dt, dtMin = HUGE_;
+#pragma omp parallel for collapse(2) reduction(min : dtMin)
+    for (int k = G.ksDT; k <= G.keDT; k++)
+        for (int j = G.jsDT; j <= G.jeDT; j++)
+            for (int i = G.isDT; i <= G.ieDT; i++) dtMin = std::min(CellDT(M, G, S, i, j, k), dtMin);
+    bool isDisaster = (dtMin == HUGE_), isBad = false;
+    double dt = dtMin;
+    if (M.ts > 0) {
+        if (dtOld / dtMin >= 10) isBad = true;
+        if (M.dt0 > TINY && dtMin / M.dt0 <= M.limDT0) isBad = true;
+        if (dtMin <= TINY) isDisaster = true;
+    }
+    if (isDisaster) *status = ST_DT_DISASTER;
+    else if (isBad) *status = ST_DT_BAD;
+    if (M.t + dt > M.tFin) dt = std::max(M.tFin - M.t, TINY);
+    if (M.dt0 > TINY && dt > 10.0 * M.dt0) dt = 10.0 * M.dt0;
+    return dt;
+}
+
+// ---------------------------------------------------------------- geometry
+// quadrature.F90:331-343 faceDeltas
+static void faceDeltas(const double* f0, const double* f1, const double* f2, const double* f3, double* dx,
+                       double* dy, double* dz) {
+    dx[0] = f1[0] - f0[0]; dx[1] = f2[0] - f0[0]; dx[2] = f3[0] + f0[0] - f2[0] - f1[0];
+    dy[0] = f1[1] - f0[1]; dy[1] = f2[1] - f0[1]; dy[2] = f3[1] + f0[1] - f2[1] - f1[1];
+    dz[0] = f1[2] - f0[2]; dz[1] = f2[2] - f0[2]; dz[2] = f3[2] + f0[2] - f2[2] - f1[2];
+}
+// quadrature.F90:159-221 GaussianFaceIntegral for the two lazy integrands the
+// metric needs (IdVec -> area, rVec -> first moment); metric.F90:302-327
+static void GaussianFaceIntegral(const double* f0, const double* f1, const double* f2, const double* f3, bool rvec,
+                                 double* fInt) {
+    double dx[3], dy[3], dz[3];
+    faceDeltas(f0, f1, f2, f3, dx, dy, dz);
+    fInt[0] = fInt[1] = fInt[2] = 0.0;
+    for (int i = 0; i < 12; i++)
+        for (int j = 0; j < 12; j++) {
+            double eta = 0.5 * (1 + gA[i]), psi = 0.5 * (1 + gA[j]);
+            double w = gWgt[i] * gWgt[j];
+            double xp = f0[0] + dx[0] * eta + dx[1] * psi + dx[2] * eta * psi;
+            double yp = f0[1] + dy[0] * eta + dy[1] * psi + dy[2] * eta * psi;
+            double zp = f0[2] + dz[0] * eta + dz[1] * psi + dz[2] * eta * psi;
+            double Ax = rvec ? xp : 1.0, Ay = rvec ? yp : 1.0, Az = rvec ? zp : 1.0;
+            double etaV[3] = {dx[0] + dx[2] * psi, dy[0] + dy[2] * psi, dz[0] + dz[2] * psi};
+            double psiV[3] = {dx[1] + dx[2] * eta, dy[1] + dy[2] * eta, dz[1] + dz[2] * eta};
+            double c[3];
+            cross(etaV, psiV, c);
+            double area = 0.25 * norm2s(c, 3) * w;
+            fInt[0] = fInt[0] + area * Ax;
+            fInt[1] = fInt[1] + area * Ay;
+            fInt[2] = fInt[2] + area * Az;
+        }
+}
+static inline double DetJ(const double J[3][3]) {  // math.F90:470-478 (J[row][col])
+    return J[0][0] * (J[1][1] * J[2][2] - J[1][2] * J[2][1]) - J[0][1] * (J[1][0] * J[2][2] - J[1][2] * J[2][0]) +
+           J[0][2] * (J[1][0] * J[2][1] - J[1][1] * J[2][0]);
+}
+// quadrature.F90:42-100 GaussianVolumeIntegral; W(x,y,z) -> 5 values
+template <class Fn>
+static void GaussianVolumeIntegral(const double xyzC[8][3], Fn W, double* wInt) {
+    static const int iS[8] = {-1, +1, +1, -1, -1, +1, +1, -1};
+    static const int jS[8] = {-1, -1, +1, +1, -1, -1, +1, +1};
+    static const int kS[8] = {-1, -1, -1, -1, +1, +1, +1, +1};
+    for (int v = 0; v < 5; v++) wInt[v] = 0.0;
+    for (int i = 0; i < 12; i++)
+        for (int j = 0; j < 12; j++)
+            for (int k = 0; k < 12; k++) {
+                double wijk = gWgt[i] * gWgt[j] * gWgt[k];
+                double iScl[8], jScl[8], kScl[8];
+                for (int n = 0; n < 8; n++) {
+                    iScl[n] = iS[n] < 0 ? 1 - gA[i] : 1 + gA[i];
+                    jScl[n] = jS[n] < 0 ? 1 - gA[j] : 1 + gA[j];
+                    kScl[n] = kS[n] < 0 ? 1 - gA[k] : 1 + gA[k];
+                }
+                double xp[3], Jac[3][3];
+                for (int x = 0; x < 3; x++) {
+                    double s = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+                    for (int n = 0; n < 8; n++) s += xyzC[n][x] * (iScl[n] * jScl[n] * kScl[n]);
+                    for (int n = 0; n < 8; n++) s1 += xyzC[n][x] * ((double)iS[n] * jScl[n] * kScl[n]);
+                    for (int n = 0; n < 8; n++) s2 += xyzC[n][x] * (iScl[n] * (double)jS[n] * kScl[n]);
+                    for (int n = 0; n < 8; n++) s3 += xyzC[n][x] * (iScl[n] * jScl[n] * (double)kS[n]);
+                    xp[x] = 0.125 * s;
+                    Jac[x][0] = 0.125 * s1;
+                    Jac[x][1] = 0.125 * s2;
+                    Jac[x][2] = 0.125 * s3;
+                }
+                double dJ = std::fabs(DetJ(Jac));
+                double Wp[5];
+                W(xp[0], xp[1], xp[2], Wp);
+                for (int v = 0; v < 5; v++) wInt[v] = wInt[v] + dJ * wijk * Wp[v];
+            }
+}
+static void cellCoords(const Grid& G, int i, int j, int k, double xyzC[8][3]) {  // metric.F90:153-171
+    const int o[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0}, {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
+    for (int n = 0; n < 8; n++)
+        for (int x = 0; x < 3; x++) xyzC[n][x] = G.xyz(i + o[n][0], j + o[n][1], k + o[n][2], x);
+}
+static void faceCoords(const Grid& G, int i, int j, int k, int d, double* f0, double* f1, double* f2,
+                       double* f3) {  // metric.F90:98-128
+    int a1[3], a2[3];
+    if (d == IDIR) { int t1[3] = {0, 1, 0}, t2[3] = {0, 0, 1}; std::memcpy(a1, t1, 12); std::memcpy(a2, t2, 12); }
+    else if (d == JDIR) { int t1[3] = {0, 0, 1}, t2[3] = {1, 0, 0}; std::memcpy(a1, t1, 12); std::memcpy(a2, t2, 12); }
+    else { int t1[3] = {1, 0, 0}, t2[3] = {0, 1, 0}; std::memcpy(a1, t1, 12); std::memcpy(a2, t2, 12); }
+    for (int x = 0; x < 3; x++) {
+        f0[x] = G.xyz(i, j, k, x);
+        f1[x] = G.xyz(i + a1[0], j + a1[1], k + a1[2], x);
+        f2[x] = G.xyz(i + a2[0], j + a2[1], k + a2[2], x);
+        f3[x] = G.xyz(i + a1[0] + a2[0], j + a1[1] + a2[1], k + a1[2] + a2[2], x);
+    }
+}
+// init.F90:1075-1137 ebGeom
+static void ebGeom(const Grid& G, F4& Teb, int c0, int dNorm, int dT1, int dT2) {
+    int ie = G.ie + 1;
+#pragma omp parallel for collapse(2)
+    for (int k = G.ks; k <= G.ke + 1; k++)
+        for (int j = G.js; j <= G.je + 1; j++)
+            for (int iB = G.is; iB <= ie; iB += vecLen) {
+                int iMax = std::min((int)vecLen, ie - iB + 1);
+                double fArB[recLen][vecLen], N[3][recLen][vecLen];
+                loadBlock(G, G.face.comp(dT1), true, iB, j, k, iMax, dT2, Nr2, fArB);
+                for (int x = 0; x < 3; x++) loadBlock(G, G.Tf.comp(NORMX + x + 9 * dT1), true, iB, j, k, iMax, dT2, Nr2, N[x]);
+                for (int i = 0; i < iMax; i++) {
+                    int iG = iB + i;
+                    double fAi = 0.0;
+                    for (int n = 0; n < recLen; n++) fAi += interpWgt6[n] * fArB[n][i];
+                    double Nec[3];
+                    for (int x = 0; x < 3; x++) {
+                        double s = 0.0;
+                        for (int n = 0; n < recLen; n++) s += (N[x][n][i] * fArB[n][i]) * interpWgt6[n];
+                        Nec[x] = s / fAi;
+                    }
+                    double t1[3] = {G.Te(iG, j, k, TAN1X + 9 * dNorm), G.Te(iG, j, k, TAN1Y + 9 * dNorm),
+                                    G.Te(iG, j, k, TAN1Z + 9 * dNorm)};
+                    double t2[3] = {G.Te(iG, j, k, TAN2X + 9 * dNorm), G.Te(iG, j, k, TAN2Y + 9 * dNorm),
+                                    G.Te(iG, j, k, TAN2Z + 9 * dNorm)};
+                    double dxT = dot3(Nec, t1), dyT = dot3(Nec, t2);
+                    double dScl = std::sqrt(dxT * dxT + dyT * dyT);
+                    if (dScl <= TINY) dScl = 1.0;
+                    Teb(iG, j, k, c0 + 0 + 4 * dNorm) = dxT / dScl;
+                    Teb(iG, j, k, c0 + 1 + 4 * dNorm) = dyT / dScl;
+                }
+            }
+}
+// init.F90:793-1072 Corners2Grid
+static void Corners2Grid(const Model& M, Grid& G) {
+    G.cellArr(G.xyzcc, 3);
+    G.faceArr(G.xfc, 9);
+    G.faceArr(G.face, 3, 1.0);
+    G.faceArr(G.Tf, 27);
+    for (int d = 0; d < 3; d++) {
+        int DelI = d == IDIR, DelJ = d == JDIR, DelK = d == KDIR;
+#pragma omp parallel for collapse(2)
+        for (int k = G.ksg; k <= G.keg + DelK; k++)
+            for (int j = G.jsg; j <= G.jeg + DelJ; j++)
+                for (int i = G.isg; i <= G.ieg + DelI; i++) {
+                    double f0[3], f1[3], f2[3], f3[3], fInt[3];
+                    faceCoords(G, i, j, k, d, f0, f1, f2, f3);
+                    GaussianFaceIntegral(f0, f1, f2, f3, false, fInt);
+                    double fA = fInt[0];
+                    GaussianFaceIntegral(f0, f1, f2, f3, true, fInt);
+                    for (int x = 0; x < 3; x++) G.xfc(i, j, k, x + 3 * d) = fInt[x] / fA;
+                    G.face(i, j, k, d) = fA;
+                    double dT1[3], dT2[3];
+                    for (int x = 0; x < 3; x++) {
+                        if (d == IDIR) {
+                            dT1[x] = 0.5 * (G.xyz(i, j + 1, k + 1, x) - G.xyz(i, j, k + 1, x)) +
+                                     0.5 * (G.xyz(i, j + 1, k, x) - G.xyz(i, j, k, x));
+                            dT2[x] = 0.5 * (G.xyz(i, j + 1, k + 1, x) - G.xyz(i, j + 1, k, x)) +
+                                     0.5 * (G.xyz(i, j, k + 1, x) - G.xyz(i, j, k, x));
+                        } else if (d == JDIR) {
+                            dT1[x] = 0.5 * (G.xyz(i + 1, j, k + 1, x) - G.xyz(i + 1, j, k, x)) +
+                                     0.5 * (G.xyz(i, j, k + 1, x) - G.xyz(i, j, k, x));
+                            dT2[x] = 0.5 * (G.xyz(i + 1, j, k + 1, x) - G.xyz(i, j, k + 1, x)) +
+                                     0.5 * (G.xyz(i + 1, j, k, x) - G.xyz(i, j, k, x));
+                        } else {
+                            dT1[x] = 0.5 * (G.xyz(i + 1, j + 1, k, x) - G.xyz(i, j + 1, k, x)) +
+                                     0.5 * (G.xyz(i + 1, j, k, x) - G.xyz(i, j, k, x));
+                            dT2[x] = 0.5 * (G.xyz(i + 1, j + 1, k, x) - G.xyz(i + 1, j, k, x)) +
+                                     0.5 * (G.xyz(i, j + 1, k, x) - G.xyz(i, j, k, x));
+                        }
+                    }
+                    double c[3], eN[3], eT1[3], eT2[3], c2[3];
+                    cross(dT1, dT2, c);
+                    double nc = norm2s(c, 3);
+                    for (int x = 0; x < 3; x++) eN[x] = c[x] / nc;
+                    double n2 = norm2s(dT2, 3);
+                    for (int x = 0; x < 3; x++) eT2[x] = dT2[x] / n2;
+                    cross(eT2, eN, c2);
+                    double nc2 = norm2s(c2, 3);
+                    for (int x = 0; x < 3; x++) eT1[x] = c2[x] / nc2;
+                    for (int x = 0; x < 3; x++) {
+                        G.Tf(i, j, k, NORMX + x + 9 * d) = eN[x];
+                        G.Tf(i, j, k, TAN1X + x + 9 * d) = eT1[x];
+                        G.Tf(i, j, k, TAN2X + x + 9 * d) = eT2[x];
+                    }
+                }
+    }
+    G.cellArr(G.volume, 1);
+    G.cellArr(G.di, 1);
+    G.cellArr(G.dj, 1);
+    G.cellArr(G.dk, 1);
+#pragma omp parallel for collapse(2)
+    for (int k = G.ksg; k <= G.keg; k++)
+        for (int j = G.jsg; j <= G.jeg; j++)
+            for (int i = G.isg; i <= G.ieg; i++) {
+                double xyzC[8][3], ijkDV[5];
+                cellCoords(G, i, j, k, xyzC);
+                GaussianVolumeIntegral(xyzC, [](double x, double y, double z, double* W) {
+                    W[0] = 1; W[1] = x; W[2] = y; W[3] = z; W[4] = 0;
+                }, ijkDV);
+                G.volume(i, j, k) = ijkDV[0];
+                for (int x = 0; x < 3; x++) G.xyzcc(i, j, k, x) = ijkDV[1 + x] / ijkDV[0];
+            }
+#pragma omp parallel for collapse(2)
+    for (int k = G.ksg; k <= G.keg; k++)
+        for (int j = G.jsg; j <= G.jeg; j++)
+            for (int i = G.isg; i <= G.ieg; i++) {
+                double fA = std::max(G.face(i + 1, j, k, IDIR), G.face(i, j, k, IDIR));
+                G.di(i, j, k) = G.volume(i, j, k) / fA;
+                fA = std::max(G.face(i, j + 1, k, JDIR), G.face(i, j, k, JDIR));
+                G.dj(i, j, k) = G.volume(i, j, k) / fA;
+                fA = std::max(G.face(i, j, k + 1, KDIR), G.face(i, j, k, KDIR));
+                G.dk(i, j, k) = G.volume(i, j, k) / fA;
+            }
+    G.faceArr(G.edge, 3, 1.0);
+    G.faceArr(G.Te, 27);
+    for (int d = 0; d < 3; d++) {
+        int is = G.isg, ie = G.ieg + 1, js = G.jsg, je = G.jeg + 1, ks = G.ksg, ke = G.keg + 1;
+        if (d == IDIR) { ie = G.ieg; ks = G.ksg + 1; ke = G.keg; }
+        else if (d == JDIR) { je = G.jeg; is = G.isg + 1; ie = G.ieg; }
+        else { ke = G.keg; js = G.jsg + 1; je = G.jeg; }
+#pragma omp parallel for collapse(2)
+        for (int k = ks; k <= ke; k++)
+            for (int j = js; j <= je; j++)
+                for (int i = is; i <= ie; i++) {
+                    double dEdge[3], eAvg[3];
+                    for (int x = 0; x < 3; x++) {
+                        if (d == IDIR) {
+                            dEdge[x] = G.xyz(i + 1, j, k, x) - G.xyz(i, j, k, x);
+                            eAvg[x] = 0.5 * (G.xyz(i, j, k + 1, x) - G.xyz(i, j, k - 1, x) + G.xyz(i + 1, j, k + 1, x) -
+                                             G.xyz(i + 1, j, k - 1, x));
+                        } else if (d == JDIR) {
+                            dEdge[x] = G.xyz(i, j + 1, k, x) - G.xyz(i, j, k, x);
+                            eAvg[x] = 0.5 * (G.xyz(i + 1, j, k, x) - G.xyz(i - 1, j, k, x) + G.xyz(i + 1, j + 1, k, x) -
+                                             G.xyz(i - 1, j + 1, k, x));
+                        } else {
+                            dEdge[x] = G.xyz(i, j, k + 1, x) - G.xyz(i, j, k, x);
+                            eAvg[x] = 0.5 * (G.xyz(i, j + 1, k, x) - G.xyz(i, j - 1, k, x) + G.xyz(i, j + 1, k + 1, x) -
+                                             G.xyz(i, j - 1, k + 1, x));
+                        }
+                    }
+                    double eN[3], eT1[3], eT2[3], c[3];
+                    double nE = norm2s(dEdge, 3);
+                    for (int x = 0; x < 3; x++) eN[x] = dEdge[x] / nE;
+                    cross(eAvg, eN, c);
+                    double nc = norm2s(c, 3);
+                    for (int x = 0; x < 3; x++) eT1[x] = c[x] / nc;
+                    cross(eN, eT1, c);
+                    nc = norm2s(c, 3);
+                    for (int x = 0; x < 3; x++) eT2[x] = c[x] / nc;
+                    G.edge(i, j, k, d) = norm2s(dEdge, 3);
+                    for (int x = 0; x < 3; x++) {
+                        G.Te(i, j, k, NORMX + x + 9 * d) = eN[x];
+                        G.Te(i, j, k, TAN1X + x + 9 * d) = eT1[x];
+                        G.Te(i, j, k, TAN2X + x + 9 * d) = eT2[x];
+                    }
+                }
+    }
+    G.faceArr(G.Teb, 12, 1.0);
+    for (int dNorm = 0; dNorm < 3; dNorm++) {
+        int T1 = (dNorm + 1) % 3, T2 = (dNorm + 2) % 3;
+        ebGeom(G, G.Teb, XNQI, dNorm, T1, T2);
+        ebGeom(G, G.Teb, XNQJ, dNorm, T2, T1);
+    }
+    (void)M;
+}
+// init.F90:511-530 SetDomain (single domain owns all boundaries)
+static void SetDomain(Grid& G) {
+    G.isDT = G.is - 1; G.ieDT = G.ie + 1;
+    G.jsDT = G.js - 1; G.jeDT = G.je + 1;
+    G.ksDT = G.ks - 1; G.keDT = G.ke + 1;
+}
+
+// ---------------------------------------------------------------- problems
+// prob.F90:74-119 initOT2D
+static void initOT2D(const Model& M, const Grid& G, State& S) {
+    double Rho0 = 25.0 / (36.0 * PI), P0 = 5 / (12.0 * PI), B0 = 1 / std::sqrt(4.0 * PI);
+    for (int k = G.ks; k <= G.ke + 1; k++)
+        for (int j = G.js; j <= G.je + 1; j++)
+            for (int i = G.is; i <= G.ie + 1; i++) {
+                double xc = G.xyzcc(i, j, k, 0), yc = G.xyzcc(i, j, k, 1);
+                S.Gas(i, j, k, DEN) = Rho0;
+                double Vx = -std::sin(2 * PI * yc), Vy = std::sin(2 * PI * xc), Vz = 0.0;
+                double KinE = 0.5 * Rho0 * (Vx * Vx + Vy * Vy + Vz * Vz);
+                S.Gas(i, j, k, MOMX) = Vx * Rho0;
+                S.Gas(i, j, k, MOMY) = Vy * Rho0;
+                S.Gas(i, j, k, MOMZ) = Vz * Rho0;
+                S.Gas(i, j, k, ENERGY) = KinE + P0 / (M.gamma - 1);
+                S.magFlux(i, j, k, XDIR) = (-B0 * std::sin(2 * PI * yc)) * G.face(i, j, k, XDIR);
+                S.magFlux(i, j, k, YDIR) = (B0 * std::sin(4 * PI * xc)) * G.face(i, j, k, YDIR);
+                S.magFlux(i, j, k, ZDIR) = 0.0;
+            }
+}
+struct BWParams { double x0, y0, z0, D0, P0, pRat, dRat, rC, B0; };
+// prob.F90:190-298 initBW (doB0 = F, doBz = F), with gridutils.F90:144-189
+// GasIC2State and :193-237 VectorPot2Flux
+static void initBW(const Model& M, const Grid& G, State& S, const BWParams& bp) {
+    const double bScl = bp.B0 / (double)std::sqrt(2.0f);  // default-real sqrt(2.0)
+    const double bSclz = 0.0;
+    auto W = [&](double x, double y, double z, double* Wp) {
+        double R = std::sqrt((x - bp.x0) * (x - bp.x0) + (y - bp.y0) * (y - bp.y0) + (z - bp.z0) * (z - bp.z0));
+        double D = bp.D0, P = bp.P0;
+        if (R <= bp.rC) { D = bp.dRat * D; P = bp.pRat * P; }
+        Wp[0] = D; Wp[1] = 0.0; Wp[2] = 0.0; Wp[3] = 0.0; Wp[4] = P;
+    };
+#pragma omp parallel for collapse(2)
+    for (int k = G.ks; k <= G.ke; k++)
+        for (int j = G.js; j <= G.je; j++)
+            for (int i = G.is; i <= G.ie; i++) {
+                double xyzC[8][3], ijkW[5];
+                cellCoords(G, i, j, k, xyzC);
+                double dV = G.volume(i, j, k);
+                GaussianVolumeIntegral(xyzC, W, ijkW);
+                for (int v = 0; v < 5; v++) ijkW[v] = ijkW[v] / dV;
+                double D = ijkW[DEN];
+                double Mx = D * ijkW[VELX], My = D * ijkW[VELY], Mz = D * ijkW[VELZ];
+                double P = ijkW[PRESSURE];
+                double KinE = 0.5 * (Mx * Mx + My * My + Mz * Mz) / D;
+                double IntE = P / (M.gamma - 1.0);
+                S.Gas(i, j, k, DEN) = D;
+                S.Gas(i, j, k, MOMX) = Mx;
+                S.Gas(i, j, k, MOMY) = My;
+                S.Gas(i, j, k, MOMZ) = Mz;
+                S.Gas(i, j, k, ENERGY) = IntE + KinE;
+            }
+    if (!M.doMHD) return;
+    auto Axyz = [&](const double* p, double* A) {
+        A[0] = 0.0;
+        A[1] = bSclz * p[0];
+        A[2] = bScl * (p[1] - p[0]);
+    };
+    // quadrature.F90:345-370 GaussianEdgeIntegral(e1,e2)
+    auto edgeInt = [&](const double* e1, const double* e2, double* eInt) {
+        double dR2[3], xBar[3];
+        for (int x = 0; x < 3; x++) { dR2[x] = 0.5 * (e2[x] - e1[x]); xBar[x] = 0.5 * (e2[x] + e1[x]); }
+        eInt[0] = eInt[1] = eInt[2] = 0.0;
+        for (int i = 0; i < 12; i++) {
+            double xp[3], Ap[3];
+            for (int x = 0; x < 3; x++) xp[x] = xBar[x] + gA[i] * dR2[x];
+            Axyz(xp, Ap);
+            for (int x = 0; x < 3; x++) eInt[x] = eInt[x] + 0.5 * gWgt[i] * Ap[x];
+        }
+    };
+    F4 lA;
+    G.cellArr(lA, 3);
+#pragma omp parallel for collapse(2)
+    for (int k = G.ksg; k <= G.keg - 1; k++)
+        for (int j = G.jsg; j <= G.jeg - 1; j++)
+            for (int i = G.isg; i <= G.ieg - 1; i++) {
+                double e0[3], eI[3], eJ[3], eK[3], t[3], dd[3];
+                for (int x = 0; x < 3; x++) {
+                    e0[x] = G.xyz(i, j, k, x); eI[x] = G.xyz(i + 1, j, k, x);
+                    eJ[x] = G.xyz(i, j + 1, k, x); eK[x] = G.xyz(i, j, k + 1, x);
+                }
+                edgeInt(eI, e0, t);
+                for (int x = 0; x < 3; x++) dd[x] = eI[x] - e0[x];
+                lA(i, j, k, IDIR) = dot3(t, dd);
+                edgeInt(eJ, e0, t);
+                for (int x = 0; x < 3; x++) dd[x] = eJ[x] - e0[x];
+                lA(i, j, k, JDIR) = dot3(t, dd);
+                edgeInt(eK, e0, t);
+                for (int x = 0; x < 3; x++) dd[x] = eK[x] - e0[x];
+                lA(i, j, k, KDIR) = dot3(t, dd);
+            }
+#pragma omp parallel for collapse(2)
+    for (int k = G.ksg; k <= G.keg - 1; k++)
+        for (int j = G.jsg; j <= G.jeg - 1; j++)
+            for (int i = G.isg; i <= G.ieg - 1; i++) {
+                S.magFlux(i, j, k, IDIR) = lA(i, j, k, JDIR) - lA(i, j, k + 1, JDIR) + lA(i, j + 1, k, KDIR) - lA(i, j, k, KDIR);
+                S.magFlux(i, j, k, JDIR) =
+                    -(lA(i, j, k, IDIR) - lA(i, j, k + 1, IDIR) + lA(i + 1, j, k, KDIR) - lA(i, j, k, KDIR));
+                S.magFlux(i, j, k, KDIR) = lA(i, j, k, IDIR) - lA(i, j + 1, k, IDIR) + lA(i + 1, j, k, JDIR) - lA(i, j, k, JDIR);
+            }
+}
+
+// ---------------------------------------------------------------- app
+struct App {
+    Model M;
+    Grid G;
+    State S, oS, hS;
+    F4 gFlx, mFlx, dGasH, dGasM, Vf;
+    int status = 0;
+};
+
+static void allocState(const Grid& G, State& S) {
+    G.cellArr(S.Gas, NVAR);
+    G.faceArr(S.magFlux, 3);
+    G.cellArr(S.Efld, 3);
+    G.cellArr(S.Bxyz, 3);
+}
+
+// mhdgroup.F90:16-76 AdvanceMHD
+static void AdvanceMHD(App& A, double dt) {
+    if (std::fabs(A.oS.time - A.S.time) < TINY) A.oS.time = A.S.time - A.M.dt;
+    Predictor(A.M, A.G, A.S, A.oS, A.hS, 0.5 * dt);
+    if (A.M.doMHD) CalcElecField(A.M, A.G, A.S, A.hS, A.Vf, A.S.Efld);
+    CalcStress(A.M, A.G, A.S, A.hS, A.gFlx, A.mFlx, A.dGasH, A.dGasM);
+    applyUpdate(A.M, A.G, A.S, A.oS, dt, A.dGasH, A.dGasM, A.S.Efld);
+}
+// gamapp.F90:73-113 stepGamera + UpdateStateData
+static int stepGamera(App& A) {
+    AdvanceMHD(A, A.M.dt);
+    A.M.ts = A.M.ts + 1;
+    A.M.t = A.M.t + A.M.dt;
+    int st;
+    A.M.dt = CalcDT(A.M, A.G, A.S, &st);
+    if (st != ST_OK) return st;  // the reference stops here (step.F90:143-153)
+    EnforceBCs(A.M, A.G, A.S);
+    bFlux2Fld(A.G, A.S.magFlux, A.S.Bxyz);
+    return ST_OK;
+}
+
+}  // namespace orc
+
+// ====================================================================== C API
+using namespace orc;
+
+extern "C" {
+
+struct OrcScalars {
+    double t, dt, dt0, time, otime;
+    int ts, status;
+};
+
+void* orc_create(const Params* p, const double* xyz) {
+    init_weights();
+    App* A = new App();
+    Model& M = A->M;
+    Grid& G = A->G;
+    M.gamma = p->gamma; M.CFL = p->CFL; M.Vd0 = p->Vd0; M.cHogH = p->cHogH; M.cHogM = p->cHogM;
+    M.tFin = p->tFin; M.dt0 = p->dt0; M.limDT0 = p->limDT0;
+    M.fixedTimestep = p->fixedTimestep != 0;
+    M.dt = M.fixedTimestep ? p->fixedDT : 0.0;
+    M.doMHD = p->doMHD != 0; M.doLFMLim = p->doLFMLim != 0; M.do25D = p->do25D != 0;
+    M.doBackground = p->doBackground != 0; M.up7 = p->up7 != 0;
+    g_up7 = M.up7;
+    pdmb = p->pdmb; dFloor = p->dFloor; pFloor = p->pFloor;
+    G.Nip = p->Nip; G.Njp = p->Njp; G.Nkp = p->Nkp;
+    G.Ni = G.Nip + 8; G.Nj = G.Njp + 8; G.Nk = G.Nkp + 8;
+    G.is = 1; G.ie = G.Nip; G.js = 1; G.je = G.Njp; G.ks = 1; G.ke = G.Nkp;
+    G.isg = G.is - 4; G.ieg = G.ie + 4; G.jsg = G.js - 4; G.jeg = G.je + 4; G.ksg = G.ks - 4; G.keg = G.ke + 4;
+    for (int n = 0; n < 6; n++) G.bc[n] = p->bc[n];
+    G.faceArr(G.xyz, 3);
+    std::memcpy(G.xyz.v.data(), xyz, G.xyz.v.size() * sizeof(double));
+    SetDomain(G);
+    Corners2Grid(M, G);
+    allocState(G, A->S);
+    A->S.time = M.t;  // allocState sets State%time = Model%t (gamutils.F90:199)
+    allocState(G, A->oS);
+    allocState(G, A->hS);
+    G.cellArr(A->gFlx, 15);
+    G.cellArr(A->mFlx, 9);
+    G.cellArr(A->dGasH, 5);
+    G.cellArr(A->dGasM, 3);
+    G.cellArr(A->Vf, 3);
+    return A;
+}
+
+void orc_destroy(void* h) { delete (App*)h; }
+
+// Pointers to internal Fortran-ordered arrays, for numpy views.
+// which: 0 Gas,1 magFlux,2 Bxyz,3 oGas,4 omagFlux,5 oBxyz,6 xyzcc,7 xfc,8 volume,
+// 9 di,10 dj,11 dk,12 Tf,13 Te,14 Teb,15 face,16 edge,17 Efld,18 hGas,19 hmagFlux,20 hBxyz,
+// 21 dGasH, 22 dGasM, 23 xyz
+double* orc_array(void* h, int which, long* n) {
+    App* A = (App*)h;
+    F4* a = nullptr;
+    switch (which) {
+        case 0: a = &A->S.Gas; break;
+        case 1: a = &A->S.magFlux; break;
+        case 2: a = &A->S.Bxyz; break;
+        case 3: a = &A->oS.Gas; break;
+        case 4: a = &A->oS.magFlux; break;
+        case 5: a = &A->oS.Bxyz; break;
+        case 6: a = &A->G.xyzcc; break;
+        case 7: a = &A->G.xfc; break;
+        case 8: a = &A->G.volume; break;
+        case 9: a = &A->G.di; break;
+        case 10: a = &A->G.dj; break;
+        case 11: a = &A->G.dk; break;
+        case 12: a = &A->G.Tf; break;
+        case 13: a = &A->G.Te; break;
+        case 14: a = &A->G.Teb; break;
+        case 15: a = &A->G.face; break;
+        case 16: a = &A->G.edge; break;
+        case 17: a = &A->S.Efld; break;
+        case 18: a = &A->hS.Gas; break;
+        case 19: a = &A->hS.magFlux; break;
+        case 20: a = &A->hS.Bxyz; break;
+        case 21: a = &A->dGasH; break;
+        case 22: a = &A->dGasM; break;
+        case 23: a = &A->G.xyz; break;
+        default: *n = 0; return nullptr;
+    }
+    *n = (long)a->v.size();
+    return a->v.data();
+}
+
+void orc_ic_ot(void* h) {
+    App* A = (App*)h;
+    initOT2D(A->M, A->G, A->S);
+}
+void orc_ic_bw(void* h, const double* bwp) {
+    App* A = (App*)h;
+    BWParams bp{bwp[0], bwp[1], bwp[2], bwp[3], bwp[4], bwp[5], bwp[6], bwp[7], bwp[8]};
+    initBW(A->M, A->G, A->S, bp);
+}
+
+// init.F90:190-244 (CalcGridInfo after the IC): Bxyz, oState, first BCs, first dt.
+int orc_init_finish(void* h) {
+    App* A = (App*)h;
+    A->oS.Gas.v = A->S.Gas.v;
+    if (A->M.doMHD) {
+        bFlux2Fld(A->G, A->S.magFlux, A->S.Bxyz);
+        A->oS.magFlux.v = A->S.magFlux.v;
+        A->oS.Bxyz.v = A->S.Bxyz.v;
+    }
+    EnforceBCs(A->M, A->G, A->S);
+    CopyState(A->G, A->S, A->oS);
+    A->oS.Efld.v = A->S.Efld.v;
+    int st;
+    A->M.dt = CalcDT(A->M, A->G, A->S, &st);
+    A->oS.time = A->S.time - A->M.dt;
+    return st;
+}
+
+void orc_set_time(void* h, double t) {
+    App* A = (App*)h;
+    A->M.t = t;
+    A->S.time = t;
+}
+
+int orc_step(void* h, int n) {
+    App* A = (App*)h;
+    for (int s = 0; s < n; s++) {
+        int st = stepGamera(*A);
+        if (st != ST_OK) { A->status = st; return st; }
+    }
+    return ST_OK;
+}
+
+void orc_scalars(void* h, OrcScalars* o) {
+    App* A = (App*)h;
+    o->t = A->M.t; o->dt = A->M.dt; o->dt0 = A->M.dt0; o->time = A->S.time; o->otime = A->oS.time;
+    o->ts = A->M.ts; o->status = A->status;
+}
+void orc_set_scalars(void* h, const OrcScalars* o) {
+    App* A = (App*)h;
+    A->M.t = o->t; A->M.dt = o->dt; A->M.dt0 = o->dt0; A->S.time = o->time; A->oS.time = o->otime;
+    A->M.ts = o->ts;
+}
+
+// gridutils.F90:717-770 DivB (sequential sum, no background)
+double orc_divb(void* h) {
+    App* A = (App*)h;
+    const Grid& G = A->G;
+    const F4& mf = A->S.magFlux;
+    double tot = 0.0;
+    for (int k = G.ks; k <= G.ke; k++)
+        for (int j = G.js; j <= G.je; j++)
+            for (int i = G.is; i <= G.ie; i++) {
+                double dFi = mf(i, j, k, IDIR) - mf(i + 1, j, k, IDIR);
+                double dFj = mf(i, j, k, JDIR) - mf(i, j + 1, k, JDIR);
+                double dFk = mf(i, j, k, KDIR) - mf(i, j, k + 1, KDIR);
+                tot = tot + std::fabs(dFi + dFj + dFk + 0.0 + 0.0 + 0.0);
+            }
+    return tot;
+}
+
+// Known-answer hooks for tests/gamera/testgamutils.pf
+void orc_c2p(double gamma, const double* con, double* prim) {
+    Model M; M.gamma = gamma;
+    dFloor = TINY; pFloor = TINY;
+    CellC2P(M, con, prim);
+}
+void orc_p2c(double gamma, const double* prim, double* con) {
+    Model M; M.gamma = gamma;
+    dFloor = TINY; pFloor = TINY;
+    CellP2C(M, prim, con);
+}
+double orc_erfc(double x) { return O_ERFC(x); }
+double orc_exp(double x) { return O_EXP(x); }
+int orc_num_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+}  // extern "C"

@@ -1,0 +1,32 @@
+"""The C-ABI library loads and exports every entry point include/gamgpu.h
+declares (no GPU work)."""
+import ctypes as C
+import os
+import re
+
+from mage_b200 import gamera
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared():
+    src = open(os.path.join(ROOT, "include", "gamgpu.h")).read()
+    return sorted(set(re.findall(r"\b(?:int|const char\*)\s+(gam_\w+)\s*\(", src)))
+
+
+def test_header_lists_all_python_bindings():
+    assert set(declared()) == set(gamera.EXPORTED)
+
+
+def test_library_exports_every_symbol():
+    lib = C.CDLL(gamera.LIB_PATH)
+    for name in declared():
+        assert hasattr(lib, name), name
+
+
+def test_default_params_match_reference():
+    L = gamera.load_library()
+    p = gamera._Params()
+    assert L.gam_default_params(C.byref(p), 64, 64, 1) == 0
+    assert abs(p.gamma - 5.0 / 3.0) < 1e-15 and p.pdmb == 0.75 and abs(p.CFL - 0.3) < 1e-15
+    assert p.Vd0 == 0.5 and p.cHogH == 0.25 and p.dFloor == 1e-12 and p.do25D == 1 and p.nG == 4

@@ -1,0 +1,153 @@
+"""CPU tests of the oracle (the CPU restatement of the reference step):
+pinned against the reference's own known-answer tests and invariants."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from mage_b200 import grids
+from oracle import oracle as orc
+from tests.helpers import make_oracle
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def _frac(s):
+    if isinstance(s, str) and "/" in s:
+        a, b = s.split("/")
+        return float(a) / float(b)
+    return float(s)
+
+
+@pytest.mark.parametrize("variant", ["strict", "gm"])
+def test_gamutils_kat(oracle_built, variant):
+    """tests/gamera/testgamutils.pf:24-112 (CellP2C / CellC2P known answers)."""
+    k = json.load(open(os.path.join(GOLD, "gamutils_kat.json")))
+    gamma = _frac(k["gamma"])
+    prim = np.array([_frac(x) for x in k["prim"]])
+    con = np.array(k["con"])
+    c = orc.p2c(prim, gamma, variant)
+    assert np.all(np.abs(c - con) <= np.array(k["p2c_tol"]))
+    p = orc.c2p(con, gamma, variant)
+    assert np.all(np.abs(p - prim) <= np.array(k["c2p_tol"]))
+    c2 = orc.p2c(orc.c2p(con, gamma, variant), gamma, variant)
+    assert np.all(np.abs(c2 - con) <= np.array(k["c2c_tol"]))
+    p2 = orc.c2p(orc.p2c(prim, gamma, variant), gamma, variant)
+    assert np.all(np.abs(p2 - prim) <= np.array(k["p2p_tol"]))
+
+
+def test_metric_box(oracle_built):
+    """tests/gamera/testmetric.pf: the box (1,1,1)-(2,3,4) as cell (1,1,1) of a
+    uniform grid; the quadrature metric reproduces its centre, face centres and
+    areas (Corners2Grid, init.F90:793-1072)."""
+    m = json.load(open(os.path.join(GOLD, "metric_kat.json")))
+    xyz = grids.uniform_corners(16, 4, 4, bounds=(1.0, 17.0, 1.0, 9.0, 1.0, 13.0))
+    o = orc.Oracle(orc.OracleParams(16, 4, 4), xyz)
+    c = (slice(None), 4, 4, 4)  # Fortran (1,1,1) -> box index 4 (isg = -3)
+    assert np.allclose(o.array("xyzcc")[c], m["cell_center"], rtol=0, atol=1e-13)
+    xfc = o.array("xfc")[c].reshape(3, 3)  # [d][x]
+    for d, name in enumerate("IJK"):
+        assert np.allclose(xfc[d], m["face_center"][name], rtol=0, atol=1e-13)
+    face = o.array("face")[c]
+    assert np.allclose(face, [6.0, 3.0, 2.0], rtol=1e-14)
+    assert abs(o.array("volume")[0, 4, 4, 4] - 6.0) < 1e-13
+    # corner array of the box matches the reference corner ordering
+    for d, name in enumerate("IJK"):
+        f = m["face_coords"][name]
+        assert np.allclose(xyz[:, 4, 4, 4], f[0])
+    # face triads are orthonormal, normal along the face direction
+    Tf = o.array("Tf")[c].reshape(3, 3, 3)  # [d][vec][x]
+    for d in range(3):
+        assert np.allclose(Tf[d] @ Tf[d].T, np.eye(3), atol=1e-14)
+        assert abs(Tf[d][0][d] - 1.0) < 1e-14
+
+
+def _ulps(a, ref):
+    import mpmath as mp  # noqa: F401  (only needed for the string refs)
+    ref = float(ref)
+    if ref == 0.0:
+        return 0.0 if a == 0.0 else np.inf
+    return abs(a - ref) / np.spacing(abs(ref))
+
+
+def test_erfc_exp_golden(oracle_built):
+    """Self-written FP64 erfc/exp (mage_b200/csrc/gam_math.cuh, via the 'gm'
+    oracle build) against 40-digit reference values: <= 8 ulp for erfc,
+    <= 2 ulp for exp, in the normal range."""
+    g = json.load(open(os.path.join(GOLD, "erfc_exp.json")))
+    L = orc.lib("gm")
+    for xh, ref in g["erfc"]:
+        x = float.fromhex(xh)
+        r = float(ref)
+        if r < 1e-300:
+            continue
+        assert _ulps(L.orc_erfc(x), ref) <= 8.0, (x, L.orc_erfc(x), ref)
+    for xh, ref in g["exp"]:
+        x = float.fromhex(xh)
+        r = float(ref)
+        if r < 1e-300 or r > 1e300:
+            continue
+        assert _ulps(L.orc_exp(x), ref) <= 2.0, (x, L.orc_exp(x), ref)
+
+
+def ot_symmetry(Gas, N):
+    """Symmetry violation of the Orszag-Tang state, tests/cases/testCases.pf:198-216."""
+    G = Gas[:, 4, 4:4 + N, 4:4 + N]  # k = ks slice, active (j, i)
+    F = G[:, ::-1, ::-1].copy()
+    F[1:3] *= -1.0
+    return float(np.sqrt(((G - F) ** 2).sum(axis=0)).sum() / (N * N))
+
+
+@pytest.mark.parametrize("Nk", [1, 4])
+def test_ot_symmetry(oracle_built, Nk):
+    """OT point symmetry (testCases.pf:183-225 asserts <= 1e-11)."""
+    N = 32
+    o, _ = make_oracle("ot", (N, N, Nk))
+    assert o.step(40) == 0
+    assert ot_symmetry(o.array("Gas"), N) <= 1e-11
+
+
+def test_conservation_and_divb(oracle_built):
+    """Periodic curvilinear blast wave: mass and Cartesian momentum are
+    conserved to round-off (the fluxes telescope), div B stays at round-off
+    (DivB, gridutils.F90:717-770). Plasma energy is not conserved by itself:
+    CellMaxwell (mhdgroup.F90:299-329) exchanges it with the field."""
+    o, _ = make_oracle("bw", (16, 16, 16))
+    vol = o.array("volume")[0, 4:-4, 4:-4, 4:-4]
+
+    def tot():
+        G = o.array("Gas")[:, 4:-4, 4:-4, 4:-4]
+        return np.array([(G[v] * vol).sum() for v in range(5)])
+
+    t0 = tot()
+    phi = np.abs(o.array("magFlux")).sum()
+    assert o.step(10) == 0
+    t1 = tot()
+    assert abs(t1[0] - t0[0]) / t0[0] < 1e-13
+    mscale = np.abs(o.array("Gas")[1:4, 4:-4, 4:-4, 4:-4] * vol).sum()
+    assert np.abs(t1[1:4] - t0[1:4]).max() < 1e-13 * mscale
+    assert o.divb() < 1e-12 * phi
+
+
+def test_variants_agree(oracle_built):
+    """libm erfc/exp vs the self-written ones vs -ffast-math: the same step to
+    well below 1e-12 after 20 steps."""
+    ref, _ = make_oracle("ot", (32, 32, 4), "strict")
+    ref.step(20)
+    for v in ("gm", "fast"):
+        o, _ = make_oracle("ot", (32, 32, 4), v)
+        o.step(20)
+        a, b = o.array("Gas"), ref.array("Gas")
+        assert np.abs(a - b).max() / np.abs(b).max() < 1e-12
+
+
+def test_dt_drop_is_reported(oracle_built):
+    """A state whose CFL dt falls 10x is flagged bad (step.F90:111-115) instead
+    of continuing; the fault is planted on the host."""
+    o, _ = make_oracle("ot", (32, 32, 4))
+    assert o.step(2) == 0
+    G = o.array("Gas")
+    G[1, 5, 10, 10] = 60.0 * G[0, 5, 10, 10]  # one active cell at |v| = 60
+    G[4, 5, 10, 10] = 0.5 * G[1, 5, 10, 10] ** 2 / G[0, 5, 10, 10] + 1.0
+    assert o.step(1) == 1  # ST_DT_BAD
