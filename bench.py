@@ -1,0 +1,346 @@
+#!/usr/bin/env python
+"""Throughput of the B200 GAMERA MHD step (one JSON line on rank 0).
+
+Workload (default): the 3-D MHD blast wave on the non-orthogonal curvilinear
+192^3 grid x = xi + 0.05 sin(2 pi xi) sin(2 pi eta) sin(2 pi zeta) (y, z
+likewise) on the unit cube, triply periodic; rho = 1, p = 0.1 outside and
+p = 10 inside r < 0.1, B = (1,1,0)/sqrt(2), gamma = 5/3, CFL 0.3, FP64 drop-in
+form. A step is one stepGamera over the whole grid; the metric is cell-updates/s
+(= 1000 x the reference's kZCs, src/gamera/output.F90:64-85).
+
+  value : device time of K steps (CUDA events on the library's stream, inputs
+          resident in HBM; the step's arrays, ~13 GB, are far larger than L2)
+  e2e   : the same metric through the C ABI with host buffers: every step
+          uploads State and oState from pinned host memory, runs one step and
+          reads the new State back
+  fp32  : the precision form on the same workload, with its error vs FP64
+  cpu_baseline : the CPU restatement (-O3 -ffast-math, all host threads) on a
+          bounded number of steps of the same workload
+
+--impl reference times that CPU restatement alone (the reference is Fortran and
+no Fortran compiler exists on these machines), on rank 0.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+# Algorithmic bytes per cell-update (compulsory traffic of a fused step that
+# reads the metric once): 27 state values + 79 metric values, FP64 / FP32.
+BYTES_PER_CELL = {"f64": 8 * (27 + 79), "f32": 4 * (27 + 79)}
+KERNELS_PER_STEP = 15  # begin, predict, 3x(mom2face, vxb), 3x stress, faces, cells, dt, bc
+
+WORKLOADS = {
+    "blast192": {"N": (192, 192, 192), "problem": "bw",
+                 "desc": "3-D MHD blast wave, curvilinear periodic 192^3 (200^3 with ghosts), configs[1]"},
+    "ot128": {"N": (128, 128, 4), "problem": "ot", "desc": "Orszag-Tang 128x128x4, periodic, configs[0]"},
+}
+
+
+def env_rank():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+
+
+def corners(w):
+    from mage_b200 import grids
+    N = w["N"]
+    return grids.warped_periodic_corners(*N) if w["problem"] == "bw" else grids.uniform_corners(*N)
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def committed_traffic(workload, dtype):
+    """DRAM bytes per cell-update of one step from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(p):
+        return None
+    d = json.load(open(p))
+    return d.get(workload, {}).get(dtype)
+
+
+def cpu_sample(g, w, params, budget_s=12.0, max_steps=6):
+    """Bounded CPU baseline: the oracle (fast build, all host threads) on the
+    same workload; metric and state are taken from the GPU set-up."""
+    from oracle.oracle import Oracle, OracleParams
+    from tests.helpers import GEO_FROM_ORACLE
+    N = w["N"]
+    op = OracleParams(*N, do25D=(N[2] == 1), CFL=params.CFL, noMetric=True)
+    xyz = np.zeros((3, N[2] + 9, N[1] + 9, N[0] + 9))
+    o = Oracle(op, xyz, "fast")
+    geo = g.get_geometry_arrays()
+    for name, v in geo.items():
+        o.array(GEO_FROM_ORACLE[name])[...] = v
+    del geo
+    s = g.download_state()
+    for k in ("Gas", "magFlux", "Bxyz", "oGas", "omagFlux"):
+        o.array(k)[...] = s[k]
+    o.set_scalars(t=s["time"], dt=s["dt"], time=s["time"], otime=s["otime"], ts=s["ts"])
+    del s
+    o.step(1)  # warm-up
+    n, t0 = 0, time.perf_counter()
+    while n < max_steps:
+        o.step(1)
+        n += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    el = time.perf_counter() - t0
+    cells = N[0] * N[1] * N[2]
+    return {"value": cells * n / el, "unit": "cell-updates/s", "cores": int(o.L.orc_num_threads()),
+            "kind": "port", "sample": f"{n} timed steps (after 1 warm-up) of the full {N[0]}x{N[1]}x{N[2]} grid, "
+                                      f"oracle -O3 -march=native -ffast-math, OpenMP"}
+
+
+def run_reference(args):
+    """CPU restatement of the reference step on all host threads (rank 0)."""
+    rank, _, world = env_rank()
+    if rank != 0:
+        return
+    os.environ.setdefault("OMP_PROC_BIND", "close")
+    from oracle.oracle import Oracle, OracleParams
+    w = WORKLOADS[args.workload]
+    N = w["N"]
+    xyz = corners(w)
+    o = Oracle(OracleParams(*N, do25D=(N[2] == 1)), xyz, "fast")
+    if w["problem"] == "bw":
+        o.ic_blast_wave()
+    else:
+        o.ic_orszag_tang()
+    o.init_finish()
+    for _ in range(max(1, min(args.warmup, 2))):
+        o.step(1)
+    budget = 90.0
+    n, t0 = 0, time.perf_counter()
+    while n < args.steps:
+        o.step(1)
+        n += 1
+        if time.perf_counter() - t0 > budget:
+            break
+    el = time.perf_counter() - t0
+    cells = N[0] * N[1] * N[2]
+    v = cells * n / el
+    cores = int(o.L.orc_num_threads())
+    line = {"metric": "cell-updates/s", "value": v, "unit": "cell-updates/s", "n_gpus": world, "steps": n,
+            "warmup": args.warmup, "ms_per_step": 1e3 * el / n, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": w["desc"], "grid": list(N), "precision": "FP64"},
+            "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": cores, "kind": "port",
+                             "sample": f"{n} timed steps of the full grid after warm-up (time budget {budget:.0f} s); "
+                                       "CPU restatement of the Fortran step, -O3 -march=native -ffast-math, OpenMP"},
+            "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="gamgpu", choices=["gamgpu", "reference"])
+    ap.add_argument("--workload", default="blast192", choices=sorted(WORKLOADS))
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-fp32", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    rank, local, world = env_rank()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    from mage_b200.gamera import GameraGPU, GamParams, FP32
+
+    w = WORKLOADS[args.workload]
+    N = w["N"]
+    cells = N[0] * N[1] * N[2]
+    xyz = corners(w)
+
+    def make(prec):
+        g = GameraGPU(GamParams(*N, do25D=(N[2] == 1), precision=prec))
+        g.set_geometry(xyz)
+        if w["problem"] == "bw":
+            g.init_blast_wave()
+        else:
+            g.init_orszag_tang()
+        return g
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- FP64 drop-in: device-resident throughput
+    g = make(0)
+    g.step_gamera(args.warmup)
+    barrier()
+    clk = ClockSampler(local)
+    clk.start()
+    g.step_gamera(args.steps)
+    ms = g.last_step_ms()
+    clocks = clk.stop()
+    barrier()
+    ms = max_over_ranks(ms)
+    value = world * cells * args.steps / (ms / 1e3)
+    per_gpu = cells * args.steps / (ms / 1e3)
+
+    # ---- e2e through the C ABI with pinned host buffers
+    st = g.download_state()
+    host = {k: torch.from_numpy(st[k]).pin_memory().numpy() for k in ("Gas", "magFlux", "Bxyz", "oGas", "omagFlux")}
+    h2d = sum(host[k].nbytes for k in host)
+    d2h = host["Gas"].nbytes + host["magFlux"].nbytes + host["Bxyz"].nbytes
+    time_, otime_, dt_, ts_ = st["time"], st["otime"], st["dt"], st["ts"]
+    del st
+    out = {k: torch.empty(host[k].shape, dtype=torch.float64).pin_memory().numpy() for k in ("Gas", "magFlux", "Bxyz")}
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        g.upload_state(host["Gas"], host["magFlux"], host["Bxyz"], host["oGas"], host["omagFlux"], time_, otime_, dt_,
+                       ts_)
+        dt_, t_ = g.step_gamera(1)
+        r = g.download_state(into=out, old=False)
+        # the host driver keeps oState = the previous State
+        host["oGas"], host["Gas"] = host["Gas"], out["Gas"].copy()
+        host["omagFlux"], host["magFlux"] = host["magFlux"], out["magFlux"].copy()
+        host["Bxyz"] = out["Bxyz"].copy()
+        otime_, time_, ts_ = time_, r["time"], r["ts"]
+    barrier()
+    e2e_s = max_over_ranks((time.perf_counter() - t0))
+    e2e_value = world * cells * args.e2e_steps / e2e_s
+    del host, out
+
+    # ---- FP32 precision form
+    fp32 = None
+    if not args.no_fp32:
+        g32 = make(FP32)
+        g32.step_gamera(args.warmup)
+        barrier()
+        g32.step_gamera(args.steps)
+        ms32 = max_over_ranks(g32.last_step_ms())
+        v32 = world * cells * args.steps / (ms32 / 1e3)
+        # error vs FP64 after the same number of steps from the same start
+        a = make(0)
+        b = make(FP32)
+        nerr = 20
+        a.step_gamera(nerr)
+        b.step_gamera(nerr)
+        A, B = a.download_state(old=False)["Gas"], b.download_state(old=False)["Gas"]
+        A, B = A[:, 4:-4, 4:-4, 4:-4], B[:, 4:-4, 4:-4, 4:-4]
+        errs = {name: float(np.linalg.norm(B[v] - A[v]) / np.linalg.norm(A[v]))
+                for v, name in enumerate(("rho", "mx", "my", "mz", "energy")) if np.abs(A[v]).max() > 1e-8}
+        fp32 = {"value": v32, "unit": "cell-updates/s", "ms_per_step": ms32 / args.steps, "speedup_vs_fp64": v32 / value,
+                "rel_l2_vs_fp64": errs, "error_after_steps": nerr,
+                "roofline_frac": (v32 / world) * BYTES_PER_CELL["f32"] / 1e9 / measured_peak()[0]}
+        del g32, a, b
+
+    peak, peak_kind = measured_peak()
+    achieved = per_gpu * BYTES_PER_CELL["f64"] / 1e9
+    traffic = committed_traffic(args.workload, "f64")
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_sample(g, w, g.params)
+    if rank == 0:
+        line = {
+            "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": w["desc"], "grid": list(N), "precision": "FP64 drop-in",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                       "l2": "inputs larger than L2 (~13 GB of state, metric and work arrays per step)"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
+                         "bytes_per_cell_update": BYTES_PER_CELL["f64"],
+                         "traffic": None if traffic is None else traffic * cells,
+                         "unit_of_launch": "one step (CUDA graph of the step's kernels) over the whole grid"},
+            "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "steps": args.e2e_steps},
+            "fp32": fp32,
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+            "gpu_launches": KERNELS_PER_STEP * args.steps,
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

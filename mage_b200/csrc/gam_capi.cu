@@ -438,26 +438,28 @@ extern "C" int gam_step(gam_handle* h, int32_t nsteps, double* dt, double* t) {
     int rc;
     if ((rc = ensure_graph(h, 0))) return rc;
     if ((rc = ensure_graph(h, 1))) return rc;
-    CK(h, cudaEventRecord(h->ev0, h->s));
-    for (int n = 0; n < nsteps; n++) {
-        CK(h, cudaGraphLaunch(h->graph[h->cur], h->s));
-        h->cur = 1 - h->cur;
-    }
-    CK(h, cudaEventRecord(h->ev1, h->s));
     GamScalars s;
+    CK(h, cudaMemcpyAsync(&s, h->sc, sizeof(s), cudaMemcpyDeviceToHost, h->s));
+    CK(h, cudaStreamSynchronize(h->s));
+    if (s.halted)
+        return fail(h, s.status == 5 ? GAM_EDT_DISASTER : GAM_EDT_BAD, "a previous step failed CalcDT; upload a state");
+    const int ts0 = s.ts, cur0 = h->cur;
+    CK(h, cudaEventRecord(h->ev0, h->s));
+    for (int n = 0; n < nsteps; n++) CK(h, cudaGraphLaunch(h->graph[(cur0 + n) & 1], h->s));
+    CK(h, cudaEventRecord(h->ev1, h->s));
     CK(h, cudaMemcpyAsync(&s, h->sc, sizeof(s), cudaMemcpyDeviceToHost, h->s));
     CK(h, cudaStreamSynchronize(h->s));
     float ms = 0.f;
     cudaEventElapsedTime(&ms, h->ev0, h->ev1);
     h->lastMs = ms;
+    // every executed step (the failing one included) swapped the buffers once;
+    // steps after a failure returned at once
+    h->cur = (cur0 + (s.ts - ts0)) & 1;
     if (dt) *dt = s.dt;
     if (t) *t = s.t;
-    if (s.halted) {
-        // the halted step already swapped buffers like a completed one; later
-        // steps did nothing and must not count as swaps
+    if (s.halted)
         return fail(h, s.status == 5 ? GAM_EDT_DISASTER : GAM_EDT_BAD,
-                    s.status == 5 ? "CalcDT: timestep too small or not finite" : "CalcDT: timestep dropped");
-    }
+                    s.status == 5 ? "CalcDT: timestep too small or not finite" : "CalcDT: timestep dropped 10x or below limDT0");
     return GAM_OK;
 }
 

@@ -202,14 +202,22 @@ class GameraGPU:
             assert a.shape == s, (a.shape, s)
         self._check(self.L.gam_upload_state(self.h, *[_ptr(a) for a in arrs], time, otime, dt, int(ts)))
 
-    def download_state(self) -> dict:
-        out = {"Gas": np.zeros(self.shape("cell", 5)), "magFlux": np.zeros(self.shape("face", 3)),
-               "Bxyz": np.zeros(self.shape("cell", 3)), "oGas": np.zeros(self.shape("cell", 5)),
-               "omagFlux": np.zeros(self.shape("face", 3))}
+    def download_state(self, into: dict | None = None, old: bool = True) -> dict:
+        """State (and with ``old`` the previous state) in Fortran layout;
+        ``into`` may supply preallocated (e.g. pinned) arrays."""
+        names = ("Gas", "magFlux", "Bxyz", "oGas", "omagFlux") if old else ("Gas", "magFlux", "Bxyz")
+        kinds = {"Gas": ("cell", 5), "magFlux": ("face", 3), "Bxyz": ("cell", 3), "oGas": ("cell", 5),
+                 "omagFlux": ("face", 3)}
+        out = {}
+        for k in names:
+            a = into.get(k) if into else None
+            if a is None:
+                a = np.zeros(self.shape(*kinds[k]))
+            assert a.shape == self.shape(*kinds[k]) and a.dtype == np.float64 and a.flags.c_contiguous
+            out[k] = a
+        ptrs = [(_ptr(out[k]) if k in out else None) for k in ("Gas", "magFlux", "Bxyz", "oGas", "omagFlux")]
         t, ot, dt, ts = C.c_double(), C.c_double(), C.c_double(), C.c_int32()
-        self._check(self.L.gam_download_state(self.h, *[_ptr(out[k]) for k in ("Gas", "magFlux", "Bxyz", "oGas",
-                                                                               "omagFlux")],
-                                              C.byref(t), C.byref(ot), C.byref(dt), C.byref(ts)))
+        self._check(self.L.gam_download_state(self.h, *ptrs, C.byref(t), C.byref(ot), C.byref(dt), C.byref(ts)))
         out.update(time=t.value, otime=ot.value, dt=dt.value, ts=ts.value)
         return out
 

@@ -112,6 +112,7 @@ struct Params {  // mirrored by oracle/oracle.py (ctypes)
     double gamma, CFL, pdmb, Vd0, cHogH, cHogM, dFloor, pFloor;
     double tFin, dt0, limDT0, fixedDT;
     int bc[6];
+    int noMetric;  // 1: allocate the metric with its fill values only (arrays set by the caller)
 };
 
 struct Model {
@@ -1423,7 +1424,13 @@ void* orc_create(const Params* p, const double* xyz) {
     G.faceArr(G.xyz, 3);
     std::memcpy(G.xyz.v.data(), xyz, G.xyz.v.size() * sizeof(double));
     SetDomain(G);
-    Corners2Grid(M, G);
+    if (p->noMetric) {
+        G.cellArr(G.xyzcc, 3); G.faceArr(G.xfc, 9); G.faceArr(G.face, 3, 1.0); G.faceArr(G.Tf, 27);
+        G.cellArr(G.volume, 1); G.cellArr(G.di, 1); G.cellArr(G.dj, 1); G.cellArr(G.dk, 1);
+        G.faceArr(G.edge, 3, 1.0); G.faceArr(G.Te, 27); G.faceArr(G.Teb, 12, 1.0);
+    } else {
+        Corners2Grid(M, G);
+    }
     allocState(G, A->S);
     A->S.time = M.t;  // allocState sets State%time = Model%t (gamutils.F90:199)
     allocState(G, A->oS);

@@ -38,7 +38,7 @@ class _Params(C.Structure):
         ("gamma", C.c_double), ("CFL", C.c_double), ("pdmb", C.c_double), ("Vd0", C.c_double),
         ("cHogH", C.c_double), ("cHogM", C.c_double), ("dFloor", C.c_double), ("pFloor", C.c_double),
         ("tFin", C.c_double), ("dt0", C.c_double), ("limDT0", C.c_double), ("fixedDT", C.c_double),
-        ("bc", C.c_int * 6),
+        ("bc", C.c_int * 6), ("noMetric", C.c_int),
     ]
 
 
@@ -72,6 +72,7 @@ class OracleParams:
     limDT0: float = 1.0e-3
     fixedDT: float = 0.0
     bc: tuple = field(default_factory=lambda: (BC_PERIODIC,) * 6)
+    noMetric: bool = False
 
     def to_c(self) -> _Params:
         p = _Params()

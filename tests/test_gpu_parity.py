@@ -1,0 +1,166 @@
+"""GPU parity tests: the CUDA step (through the C ABI) against the oracle.
+
+* strict build (no FMA contraction) vs the oracle built with the same
+  self-written erfc/exp: identical bits after N steps;
+* product build (FMA contraction) vs the IEEE-strict oracle with libm
+  erfc/exp: <= 1e-12 relative (max-norm per variable) after N steps;
+* GPU metric from corners and GPU initial conditions vs the oracle's;
+* FP32 form: relative L2 error per conserved variable vs FP64, stated.
+"""
+import numpy as np
+import pytest
+
+from mage_b200 import grids
+from mage_b200.gamera import GameraGPU, GamParams, GamError, GAM_EDT_BAD, GEOMETRY_ARRAYS, FP32
+from tests.helpers import make_oracle, gpu_from_oracle, rel_err, GEO_FROM_ORACLE
+
+pytestmark = pytest.mark.gpu
+
+STATE = ("Gas", "magFlux", "Bxyz", "oGas", "omagFlux")
+
+CASES = [("ot", (32, 32, 4)), ("ot", (32, 32, 1)), ("bw", (16, 16, 16)), ("bw", (24, 16, 16))]
+
+
+@pytest.mark.parametrize("prob,N", CASES)
+def test_strict_step_is_bit_exact(oracle_built, prob, N):
+    o, _ = make_oracle(prob, N, variant="gm")
+    g = gpu_from_oracle(o, strict=True)
+    for nst in (1, 9):
+        assert o.step(nst) == 0
+        dt, t = g.step_gamera(nst)
+        s = g.download_state()
+        for k in STATE:
+            assert np.array_equal(s[k], o.array(k)), (prob, N, nst, k, rel_err(s[k], o.array(k)))
+        sc = o.scalars()
+        assert dt == sc["dt"] and t == sc["t"] and s["time"] == sc["time"] and s["otime"] == sc["otime"]
+        assert s["ts"] == sc["ts"]
+
+
+@pytest.mark.parametrize("prob,N,nst", [("ot", (128, 128, 4), 100), ("bw", (32, 32, 32), 40)])
+def test_product_step_matches_reference(oracle_built, prob, N, nst):
+    """Configuration C1 (OT 128x128x4, 100 steps) and a 32^3 curvilinear blast
+    wave: product kernels vs the IEEE-strict restatement with libm erfc/exp,
+    <= 1e-12 relative per conserved variable and face flux."""
+    o, _ = make_oracle(prob, N, variant="strict")
+    g = gpu_from_oracle(o, strict=False)
+    assert o.step(nst) == 0
+    dt, t = g.step_gamera(nst)
+    s = g.download_state()
+    worst = 0.0
+    for k, nc in (("Gas", 5), ("magFlux", 3)):
+        for v in range(nc):
+            e = rel_err(s[k][v], o.array(k)[v])
+            worst = max(worst, e)
+            assert e <= 1e-12, (k, v, e)
+    assert abs(dt - o.scalars()["dt"]) <= 1e-12 * dt
+    print(f"{prob} {N} {nst} steps: worst relative max-norm error {worst:.3e}")
+
+
+def test_metric_from_corners_is_bit_exact(oracle_built):
+    """gam_set_geometry (GPU Corners2Grid + ebGeom) == oracle metric."""
+    N = (16, 16, 16)
+    xyz = grids.warped_periodic_corners(*N)
+    from oracle.oracle import Oracle, OracleParams
+    o = Oracle(OracleParams(*N), xyz, "gm")
+    g = GameraGPU(GamParams(*N, strict=True))
+    g.set_geometry(xyz)
+    geo = g.get_geometry_arrays()
+    for name, _, _ in GEOMETRY_ARRAYS:
+        assert np.array_equal(geo[name], o.array(GEO_FROM_ORACLE[name])), name
+
+
+def test_blast_wave_init_is_bit_exact(oracle_built):
+    """gam_init_blast_wave (GPU GasIC2State + VectorPot2Flux + init order) ==
+    oracle initBW + CalcGridInfo."""
+    N = (16, 16, 16)
+    o, xyz = make_oracle("bw", N, variant="gm")
+    g = GameraGPU(GamParams(*N, strict=True))
+    g.set_geometry(xyz)
+    g.init_blast_wave()
+    s = g.download_state()
+    for k in STATE:
+        assert np.array_equal(s[k], o.array(k)), k
+    sc = o.scalars()
+    assert s["dt"] == sc["dt"] and s["otime"] == sc["otime"]
+
+
+def test_orszag_tang_init(oracle_built):
+    """gam_init_orszag_tang vs initOT2D: equal up to the device sin (<= 4 ulp)."""
+    N = (32, 32, 4)
+    o, xyz = make_oracle("ot", N, variant="gm")
+    g = GameraGPU(GamParams(*N, strict=True))
+    g.set_geometry(xyz)
+    g.init_orszag_tang()
+    s = g.download_state()
+    for k in ("Gas", "magFlux", "Bxyz"):
+        assert rel_err(s[k], o.array(k)) < 1e-15, k
+
+
+@pytest.mark.parametrize("prob,N,nst", [("ot", (128, 128, 4), 100), ("bw", (32, 32, 32), 40)])
+def test_fp32_form_error_vs_fp64(oracle_built, prob, N, nst):
+    """Precision form: relative L2 error per conserved variable vs the FP64
+    oracle after nst steps (the bound is the target of the precision form)."""
+    o, _ = make_oracle(prob, N, variant="strict")
+    g = gpu_from_oracle(o, precision=FP32)
+    assert o.step(nst) == 0
+    g.step_gamera(nst)
+    s = g.download_state()
+    G, R = s["Gas"][:, 4:-4, 4:-4, 4:-4], o.array("Gas")[:, 4:-4, 4:-4, 4:-4]
+    errs = []
+    for v in range(5):
+        if np.abs(R[v]).max() < 1e-8:  # identically zero component (e.g. Mz)
+            continue
+        errs.append(np.linalg.norm(G[v] - R[v]) / np.linalg.norm(R[v]))
+    print(f"{prob} {N}: FP32 relative L2 errors per variable: {['%.2e' % e for e in errs]}")
+    assert max(errs) <= 1e-5
+
+
+def test_dt_failure_stops_like_reference(oracle_built):
+    """A planted 10x dt drop: the GPU returns GAM_EDT_BAD and keeps the
+    post-update, pre-BC state the reference stops with (step.F90:143-153)."""
+    o, _ = make_oracle("ot", (32, 32, 4), variant="gm")
+    assert o.step(2) == 0
+    G = o.array("Gas")
+    G[1, 5, 10, 10] = 60.0 * G[0, 5, 10, 10]
+    G[4, 5, 10, 10] = 0.5 * G[1, 5, 10, 10] ** 2 / G[0, 5, 10, 10] + 1.0
+    g = gpu_from_oracle(o, strict=True)
+    assert o.step(3) == 1
+    with pytest.raises(GamError) as ei:
+        g.step_gamera(3)
+    assert ei.value.code == GAM_EDT_BAD
+    s = g.download_state()
+    for k in ("Gas", "magFlux"):
+        assert np.array_equal(s[k], o.array(k)), k
+
+
+def test_diagnostics(oracle_built):
+    o, _ = make_oracle("bw", (16, 16, 16), variant="gm")
+    g = gpu_from_oracle(o, strict=True)
+    o.step(5)
+    g.step_gamera(5)
+    assert abs(g.divb() - o.divb()) <= 1e-14 + 1e-6 * o.divb()
+    vol = o.array("volume")[0, 4:-4, 4:-4, 4:-4]
+    Gs = o.array("Gas")[:, 4:-4, 4:-4, 4:-4]
+    ref = np.array([(Gs[v] * vol).sum() for v in range(5)])
+    assert np.allclose(g.totals(), ref, rtol=1e-13, atol=1e-15)
+    dt = g.calc_dt()
+    assert abs(dt - o.scalars()["dt"]) <= 1e-15 * dt
+
+
+def test_advance_model_and_determinism(oracle_built):
+    """AdvanceModel semantics (gamtypessub.F90:74-90) and run-to-run identity."""
+    o, _ = make_oracle("ot", (32, 32, 4), variant="gm")
+    g1 = gpu_from_oracle(o, strict=False)
+    g2 = gpu_from_oracle(o, strict=False)
+    t = g1.advance_model(0.02)
+    assert t >= 0.02
+    n = g1.download_state()["ts"]
+    g2.step_gamera(n)
+    a, b = g1.download_state(), g2.download_state()
+    for k in STATE:
+        assert np.array_equal(a[k], b[k])
+
+
+def test_bad_dimensions_rejected():
+    with pytest.raises(GamError):
+        GameraGPU(GamParams(20, 16, 16))  # Nip % 8 != 0 (init.F90:817-826)
