@@ -42,6 +42,8 @@ KERNELS_PER_STEP = 15  # begin, predict, 3x(mom2face, vxb), 3x stress, faces, ce
 WORKLOADS = {
     "blast192": {"N": (192, 192, 192), "problem": "bw",
                  "desc": "3-D MHD blast wave, curvilinear periodic 192^3 (200^3 with ghosts), configs[1]"},
+    "blast96": {"N": (96, 96, 96), "problem": "bw",
+                "desc": "3-D MHD blast wave, curvilinear periodic 96^3 (profiling size)"},
     "ot128": {"N": (128, 128, 4), "problem": "ot", "desc": "Orszag-Tang 128x128x4, periodic, configs[0]"},
 }
 
@@ -70,7 +72,7 @@ class ClockSampler:
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -199,13 +201,14 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="gamgpu", choices=["gamgpu", "reference"])
     ap.add_argument("--workload", default="blast192", choices=sorted(WORKLOADS))
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp32", action="store_true")
+    ap.add_argument("--strict", action="store_true", help="time the FP64 kernels built without FMA contraction")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -226,8 +229,8 @@ def main():
     cells = N[0] * N[1] * N[2]
     xyz = corners(w)
 
-    def make(prec):
-        g = GameraGPU(GamParams(*N, do25D=(N[2] == 1), precision=prec))
+    def make(prec, strict=False):
+        g = GameraGPU(GamParams(*N, do25D=(N[2] == 1), precision=prec, strict=strict))
         g.set_geometry(xyz)
         if w["problem"] == "bw":
             g.init_blast_wave()
@@ -248,7 +251,7 @@ def main():
         return float(t.item())
 
     # ---- FP64 drop-in: device-resident throughput
-    g = make(0)
+    g = make(0, args.strict)
     g.step_gamera(args.warmup)
     barrier()
     clk = ClockSampler(local)
@@ -262,29 +265,35 @@ def main():
     per_gpu = cells * args.steps / (ms / 1e3)
 
     # ---- e2e through the C ABI with pinned host buffers
-    st = g.download_state()
-    host = {k: torch.from_numpy(st[k]).pin_memory().numpy() for k in ("Gas", "magFlux", "Bxyz", "oGas", "omagFlux")}
-    h2d = sum(host[k].nbytes for k in host)
-    d2h = host["Gas"].nbytes + host["magFlux"].nbytes + host["Bxyz"].nbytes
-    time_, otime_, dt_, ts_ = st["time"], st["otime"], st["dt"], st["ts"]
-    del st
-    out = {k: torch.empty(host[k].shape, dtype=torch.float64).pin_memory().numpy() for k in ("Gas", "magFlux", "Bxyz")}
-    barrier()
-    t0 = time.perf_counter()
-    for _ in range(args.e2e_steps):
-        g.upload_state(host["Gas"], host["magFlux"], host["Bxyz"], host["oGas"], host["omagFlux"], time_, otime_, dt_,
-                       ts_)
-        dt_, t_ = g.step_gamera(1)
-        r = g.download_state(into=out, old=False)
-        # the host driver keeps oState = the previous State
-        host["oGas"], host["Gas"] = host["Gas"], out["Gas"].copy()
-        host["omagFlux"], host["magFlux"] = host["magFlux"], out["magFlux"].copy()
-        host["Bxyz"] = out["Bxyz"].copy()
-        otime_, time_, ts_ = time_, r["time"], r["ts"]
-    barrier()
-    e2e_s = max_over_ranks((time.perf_counter() - t0))
-    e2e_value = world * cells * args.e2e_steps / e2e_s
-    del host, out
+    e2e_value, h2d, d2h = None, 0, 0
+    if args.e2e_steps > 0:
+        st = g.download_state()
+
+        def pinned(a):
+            return torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+
+        cur = {k: pinned(st[k]) for k in ("Gas", "magFlux", "Bxyz")}
+        old = {"Gas": pinned(st["oGas"]), "magFlux": pinned(st["omagFlux"])}
+        spare = {k: pinned(np.empty_like(st[k])) for k in ("Gas", "magFlux", "Bxyz")}
+        h2d = sum(cur[k].nbytes for k in cur) + old["Gas"].nbytes + old["magFlux"].nbytes
+        d2h = sum(cur[k].nbytes for k in cur)
+        time_, otime_, dt_, ts_ = st["time"], st["otime"], st["dt"], st["ts"]
+        del st
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            g.upload_state(cur["Gas"], cur["magFlux"], cur["Bxyz"], old["Gas"], old["magFlux"], time_, otime_, dt_, ts_)
+            g.step_gamera(1)
+            r = g.download_state(into=spare, old=False)
+            # the host driver keeps oState = the previous State; rotate the pinned buffers
+            old["Gas"], old["magFlux"], spare["Gas"], spare["magFlux"] = cur["Gas"], cur["magFlux"], old["Gas"], old["magFlux"]
+            cur["Gas"], cur["magFlux"] = r["Gas"], r["magFlux"]
+            cur["Bxyz"], spare["Bxyz"] = r["Bxyz"], cur["Bxyz"]
+            otime_, time_, dt_, ts_ = time_, r["time"], r["dt"], r["ts"]
+        barrier()
+        e2e_s = max_over_ranks((time.perf_counter() - t0))
+        e2e_value = world * cells * args.e2e_steps / e2e_s
+        del cur, old, spare
 
     # ---- FP32 precision form
     fp32 = None
@@ -321,7 +330,8 @@ def main():
             "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": w["desc"], "grid": list(N), "precision": "FP64 drop-in",
+            "config": {"workload": w["desc"], "grid": list(N),
+                       "precision": "FP64 drop-in" + (" (strict: no FMA contraction)" if args.strict else ""),
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                        "l2": "inputs larger than L2 (~13 GB of state, metric and work arrays per step)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
@@ -330,7 +340,9 @@ def main():
                          "traffic": None if traffic is None else traffic * cells,
                          "unit_of_launch": "one step (CUDA graph of the step's kernels) over the whole grid"},
             "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "steps": args.e2e_steps},
+                    "steps": args.e2e_steps,
+                    "what": "per step: gam_upload_state (State+oState from pinned host memory), gam_step(1), "
+                            "gam_download_state (new State to pinned host memory)"},
             "fp32": fp32,
             "cpu_baseline": cpu,
             "clocks": clocks,
