@@ -39,23 +39,11 @@ sys.path.insert(0, ROOT)
 BYTES_PER_CELL = {"f64": 8 * (27 + 79), "f32": 4 * (27 + 79)}
 KERNELS_PER_STEP = 15  # begin, predict, 3x(mom2face, vxb), 3x stress, faces, cells, dt, bc
 
-WORKLOADS = {
-    "blast192": {"N": (192, 192, 192), "problem": "bw",
-                 "desc": "3-D MHD blast wave, curvilinear periodic 192^3 (200^3 with ghosts), configs[1]"},
-    "blast96": {"N": (96, 96, 96), "problem": "bw",
-                "desc": "3-D MHD blast wave, curvilinear periodic 96^3 (profiling size)"},
-    "ot128": {"N": (128, 128, 4), "problem": "ot", "desc": "Orszag-Tang 128x128x4, periodic, configs[0]"},
-}
+from mage_b200.workloads import WORKLOADS, corners  # noqa: E402
 
 
 def env_rank():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
-
-
-def corners(w):
-    from mage_b200 import grids
-    N = w["N"]
-    return grids.warped_periodic_corners(*N) if w["problem"] == "bw" else grids.uniform_corners(*N)
 
 
 class ClockSampler:

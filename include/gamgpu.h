@@ -114,6 +114,13 @@ int gam_totals(gam_handle* h, double out[5]);
 /* Wall time of the last gam_step call measured with CUDA events (ms). */
 int gam_last_step_ms(gam_handle* h, double* ms);
 
+/* Diagnostic: device time (ms) of each kernel of one step, averaged over
+ * reps repeated launches on the current state, in step order: ms[0] begin,
+ * [1] predictor, [2..7] Mom2Face/VxB for E_i, E_j, E_k, [8..10] fluxes i/j/k,
+ * [11] face update, [12] cell update + dt, [13] dt decision, [14] boundary
+ * fill (n >= 15). The state is left as it was. */
+int gam_profile_step(gam_handle* h, int32_t reps, double* ms, int32_t n);
+
 /* gamApp_T%AdvanceModel(dt) (gamtypessub.F90:74-90): one step, then steps
  * while Model%t < t_start + dt. */
 int gam_advance_model(gam_handle* h, double dt, double* t_out);

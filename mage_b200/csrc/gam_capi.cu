@@ -17,6 +17,12 @@ void gam_fast_step_f64(const Ctx<double>& C, int cur, cudaStream_t s);
 void gam_fast_dt_f64(const Ctx<double>& C, int cur, cudaStream_t s);
 void gam_fast_step_f32(const Ctx<float>& C, int cur, cudaStream_t s);
 void gam_fast_dt_f32(const Ctx<float>& C, int cur, cudaStream_t s);
+void gam_strict_prepare_f64();
+void gam_strict_profile_f64(const Ctx<double>& C, int cur, cudaStream_t s, int reps, double* ms);
+void gam_fast_profile_f64(const Ctx<double>& C, int cur, cudaStream_t s, int reps, double* ms);
+void gam_fast_profile_f32(const Ctx<float>& C, int cur, cudaStream_t s, int reps, double* ms);
+void gam_fast_prepare_f64();
+void gam_fast_prepare_f32();
 // set-up (gam_geom.cu)
 void gam_geom_fortran_to_box_d(const GamBox& b, const double* src, double* dst, bool face, int nc, cudaStream_t s);
 void gam_geom_fortran_to_box_f(const GamBox& b, const double* src, float* dst, bool face, int nc, cudaStream_t s);
@@ -131,8 +137,8 @@ template <class R> static int alloc_bulk(gam_handle* h, Ctx<R>& C) {
         A(C.st[q].mf, 3);
         A(C.st[q].B, 3);
     }
-    A(C.w.Wh, 5); A(C.w.Wn, 5); A(C.w.VdV, 3); A(C.w.Bh, 3);
-    A(C.w.bh, 3); A(C.w.bn, 3); A(C.w.Bnf, 3); A(C.w.Vf, 9); A(C.w.E, 3);
+    A(C.w.QW, 5); A(C.w.QB, 3); A(C.w.Dh, 1); A(C.w.Wn, 5); A(C.w.Bl, 3); A(C.w.VdV, 3);
+    A(C.w.abh, 3); A(C.w.bn, 3); A(C.w.Bnf, 3); A(C.w.AVf, 9); A(C.w.E, 3);
     A(C.w.gF, 15); A(C.w.mF, 9);
     if (sizeof(R) == sizeof(double)) {
         C.g.vol = (const R*)h->gd.vol; C.g.xyzcc = (const R*)h->gd.xyzcc; C.g.dl = (const R*)h->gd.dl;
@@ -200,6 +206,12 @@ extern "C" int gam_create(const gam_params* p, gam_handle** out) {
     h->dres = dalloc<double>(h, 16, &e);
     h->sc = dalloc<GamScalars>(h, 1, &e);
     if (e != cudaSuccess) return bad(GAM_ECUDA, "cudaMalloc failed");
+    if (h->f32)
+        gam_fast_prepare_f32();
+    else if (p->strict)
+        gam_strict_prepare_f64();
+    else
+        gam_fast_prepare_f64();
     int rc = h->f32 ? alloc_bulk<float>(h, h->cf) : alloc_bulk<double>(h, h->cd);
     if (rc != GAM_OK) {
         *out = h;
@@ -473,6 +485,25 @@ extern "C" int gam_advance_model(gam_handle* h, double dt, double* t_out) {
     while (rc == GAM_OK && t < target) rc = gam_step(h, 1, &ddt, &t);
     if (t_out) *t_out = t;
     return rc;
+}
+
+extern "C" int gam_profile_step(gam_handle* h, int32_t reps, double* ms, int32_t n) {
+    if (!h || !ms || n < 15 || reps < 1) return GAM_EINVAL;
+    if (!h->haveGeo || !h->haveState) return fail(h, GAM_ESTATE, "gam_profile_step needs geometry and state");
+    GamScalars s;
+    CK(h, cudaMemcpyAsync(&s, h->sc, sizeof(s), cudaMemcpyDeviceToHost, h->s));
+    CK(h, cudaStreamSynchronize(h->s));
+    if (h->f32)
+        gam_fast_profile_f32(h->cf, h->cur, h->s, reps, ms);
+    else if (h->p.strict)
+        gam_strict_profile_f64(h->cd, h->cur, h->s, reps, ms);
+    else
+        gam_fast_profile_f64(h->cd, h->cur, h->s, reps, ms);
+    // restore the scalars the repeated kernels touched (dt reduction)
+    CK(h, cudaMemcpyAsync(h->sc, &s, sizeof(s), cudaMemcpyHostToDevice, h->s));
+    CK(h, cudaStreamSynchronize(h->s));
+    CK(h, cudaGetLastError());
+    return GAM_OK;
 }
 
 extern "C" int gam_last_step_ms(gam_handle* h, double* ms) {

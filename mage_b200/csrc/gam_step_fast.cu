@@ -9,3 +9,7 @@ void gam_fast_step_f32(const Ctx<float>& C, int cur, cudaStream_t s) { gam_fast:
 void gam_fast_dt_f32(const Ctx<float>& C, int cur, cudaStream_t s) { gam_fast::launch_dt_only<float>(C, cur, s); }
 void gam_fast_init_f64(const Ctx<double>& C, int cur, cudaStream_t s) { gam_fast::launch_init<double>(C, cur, s); }
 void gam_fast_init_f32(const Ctx<float>& C, int cur, cudaStream_t s) { gam_fast::launch_init<float>(C, cur, s); }
+void gam_fast_prepare_f64() { gam_fast::prepare<double>(); }
+void gam_fast_prepare_f32() { gam_fast::prepare<float>(); }
+void gam_fast_profile_f64(const Ctx<double>& C, int cur, cudaStream_t s, int reps, double* ms) { gam_fast::profile_step<double>(C, cur, s, reps, ms); }
+void gam_fast_profile_f32(const Ctx<float>& C, int cur, cudaStream_t s, int reps, double* ms) { gam_fast::profile_step<float>(C, cur, s, reps, ms); }

@@ -126,14 +126,17 @@ __device__ __forceinline__ R pdm1(R pdmb, R q0, R q1, R q2, R qI) {
     R dqL = qN - q1;
     return qN - s1 * rmax((R)0, fabs(dqL) - s01 * fabs(dq0));
 }
-// GetLRs = Cen8LRs (recon.F90:125-158) or Up7LRs (:162-198) on
-// dV[0..7] (cells -4..3), q[0..7], limiter nq[0..3], volume interpolant Vi.
-template <class R>
-__device__ __forceinline__ void get_lrs(const DevParams<R>& P, const R* dV, const R* q, const R* nq, R Vi, R& Ql,
-                                        R& Qr) {
-    R QdV[8];
+template <class R> __device__ __forceinline__ R central8(const R* q) {
+    R s = (R)0;
 #pragma unroll
-    for (int n = 0; n < 8; n++) QdV[n] = dV[n] * q[n];
+    for (int n = 0; n < 8; n++) s += Rc<R>(w8(n)) * q[n];
+    return s;
+}
+// GetLRs = Cen8LRs (recon.F90:125-158) or Up7LRs (:162-198) on the volume
+// weighted stencil QdV[0..7] = dV*Q at cells -4..3 (precomputed per cell),
+// limiter nq[0..3] at cells -2..1, and the volume interpolant Vi.
+template <class R>
+__device__ __forceinline__ void lrs_from_qdv(const DevParams<R>& P, const R* QdV, const R* nq, R Vi, R& Ql, R& Qr) {
     if (!P.up7) {
         R s = (R)0;
 #pragma unroll
@@ -152,12 +155,6 @@ __device__ __forceinline__ void get_lrs(const DevParams<R>& P, const R* dV, cons
         Ql = pdm1(P.pdmb, nq[0], nq[1], nq[2], Ql);
         Qr = pdm1(P.pdmb, nq[3], nq[2], nq[1], Qr);
     }
-}
-template <class R> __device__ __forceinline__ R central8(const R* q) {
-    R s = (R)0;
-#pragma unroll
-    for (int n = 0; n < 8; n++) s += Rc<R>(w8(n)) * q[n];
-    return s;
 }
 
 // ----------------------------------------------------------------- EOS
@@ -230,7 +227,11 @@ __global__ void k_step_begin(GamScalars* sc) {
     sc->pdt = 0.5 * sc->dt;
 }
 
-// Predictor over every face and cell of the ghosted box.
+// Predictor over every face and cell of the ghosted box. Besides the half
+// state it stores the operands every later stencil uses, each computed once:
+// volume * primitive (the recon operand QdV of Cen8LRs/Up7LRs), the limiter
+// primitives, volume * momentum / density (Mom2Face), and per face
+// area * flux/max(area,TINY) and flux/max(area,TINY) (EdgeLRs), flux/area (Fluxes).
 template <class R>
 __global__ void __launch_bounds__(256) k_predict(GamBox b, DevParams<R> P, Geo<R> g, StateBuf<R> cur,
                                                  StateBuf<R> old, Work<R> w, const GamScalars* sc) {
@@ -251,9 +252,10 @@ __global__ void __launch_bounds__(256) k_predict(GamBox b, DevParams<R> P, Geo<R
             hm[d] = Q + pdt * dQ;  // ExtrapAB2
             R A = g.face[d * fs + c];
             R Am = rmax(A, (R)TINY);
-            w.bh[d * fs + c] = hm[d] / Am;
+            R bh = hm[d] / Am;
+            w.abh[d * fs + c] = A * bh;
             w.Bnf[d * fs + c] = hm[d] / A;
-            w.bn[d * fs + c] = Q / Am;
+            w.bn[d * fs + c] = P.doLFMLim ? Q / Am : bh;
         }
     }
     if (!isCell) return;
@@ -276,13 +278,14 @@ __global__ void __launch_bounds__(256) k_predict(GamBox b, DevParams<R> P, Geo<R
     cell_p2c(P, pW, pQ);
     R Wh[5], Wn[5];
     block_c2p(P, pQ, Wh);
-    block_c2p(P, Q, Wn);
+    if (P.doLFMLim) block_c2p(P, Q, Wn);
+    const R vol = g.vol[c];
 #pragma unroll
     for (int v = 0; v < 5; v++) {
-        w.Wh[v * fs + c] = Wh[v];
-        w.Wn[v * fs + c] = Wn[v];
+        w.QW[v * fs + c] = vol * Wh[v];
+        w.Wn[v * fs + c] = P.doLFMLim ? Wn[v] : Wh[v];
     }
-    const R vol = g.vol[c];
+    w.Dh[c] = Wh[0];
     const R Dm = rmax(pQ[0], P.dFloor);
 #pragma unroll
     for (int x = 0; x < 3; x++) w.VdV[x * fs + c] = vol * pQ[1 + x] / Dm;
@@ -300,7 +303,10 @@ __global__ void __launch_bounds__(256) k_predict(GamBox b, DevParams<R> P, Geo<R
         R B[3];
         cell_bxyz(b, g, c, hm[0], up[0], hm[1], up[1], hm[2], up[2], B);
 #pragma unroll
-        for (int x = 0; x < 3; x++) w.Bh[x * fs + c] = B[x];
+        for (int x = 0; x < 3; x++) {
+            w.QB[x * fs + c] = vol * B[x];
+            if (!P.doLFMLim) w.Bl[x * fs + c] = B[x];
+        }
     }
 }
 
@@ -311,7 +317,8 @@ __device__ __forceinline__ void edge_dirs(int eD, int& dT1, int& dT2) {
     dT2 = (eD + 2) % 3;
 }
 
-// Mom2Face for edge direction eD over the reference's loop range.
+// Mom2Face for edge direction eD over the reference's loop range; stores
+// area(dT1) * Vf, the operand of GetCornerV's weighted interpolation.
 template <class R>
 __global__ void __launch_bounds__(256) k_mom2face(GamBox b, DevParams<R> P, Geo<R> g, Work<R> w, int eD, Range r,
                                                   const GamScalars* sc) {
@@ -327,12 +334,13 @@ __global__ void __launch_bounds__(256) k_mom2face(GamBox b, DevParams<R> P, Geo<
 #pragma unroll
     for (int n = 0; n < 8; n++) vol[n] = g.vol[c + (n - 4) * s];
     R dV = rmax(central8(vol), (R)TINY);
+    const R A = g.face[dT1 * fs + c];
 #pragma unroll
     for (int x = 0; x < 3; x++) {
         R q[8];
 #pragma unroll
         for (int n = 0; n < 8; n++) q[n] = w.VdV[x * fs + c + (n - 4) * s];
-        w.Vf[(x + 3 * eD) * fs + c] = central8(q) / dV;
+        w.AVf[(x + 3 * eD) * fs + c] = A * (central8(q) / dV);
     }
 }
 
@@ -342,17 +350,17 @@ __device__ __forceinline__ void edge_lrs(const GamBox& b, const DevParams<R>& P,
                                          long c, int a, int bd, R* area, R& bL, R& bR, R& fA) {
     const long fs = b.fs;
     const long s = dstride(b, bd);
-    R mag[8], nmag[4];
+    R qdv[8], nmag[4];
 #pragma unroll
     for (int n = 0; n < 8; n++) {
         area[n] = g.face[a * fs + c + (n - 4) * s];
-        mag[n] = w.bh[a * fs + c + (n - 4) * s];
+        qdv[n] = w.abh[a * fs + c + (n - 4) * s];
     }
 #pragma unroll
-    for (int m = 0; m < 4; m++) nmag[m] = P.doLFMLim ? w.bn[a * fs + c + (m - 2) * s] : w.bh[a * fs + c + (m - 2) * s];
-    R Vi = central8(area);
-    get_lrs(P, area, mag, nmag, Vi, bL, bR);
-    fA = central8(area);
+    for (int m = 0; m < 4; m++) nmag[m] = w.bn[a * fs + c + (m - 2) * s];
+    const R Vi = central8(area);
+    lrs_from_qdv(P, qdv, nmag, Vi, bL, bR);
+    fA = Vi;  // dot_product(interpWgt, AreaB) again: the same value
     bL = bL * fA;
     bR = bR * fA;
 }
@@ -371,21 +379,21 @@ __global__ void __launch_bounds__(128) k_vxb(GamBox b, DevParams<R> P, Geo<R> g,
     // GetCornerD (fields.F90:427-454): normal-plane unit offsets e1 < e2
     const int e1 = eD == 0 ? 1 : 0, e2 = eD == 2 ? 1 : 2;
     const long s1 = dstride(b, e1), s2 = dstride(b, e2);
-    R Dc = (R)0.25 * (w.Wh[c] + w.Wh[c - s1] + w.Wh[c - s2] + w.Wh[c - s1 - s2]);
+    R Dc = (R)0.25 * (w.Dh[c] + w.Dh[c - s1] + w.Dh[c - s2] + w.Dh[c - s1 - s2]);
     // GetCornerB: EdgeLRs for dT1 faces along dT2 and dT2 faces along dT1
     R area1[8], area2[8];
     R bT1L, bT1R, fA1, bT2L, bT2R, fA2;
     edge_lrs(b, P, g, w, c, dT1, dT2, area1, bT1L, bT1R, fA1);
     edge_lrs(b, P, g, w, c, dT2, dT1, area2, bT2L, bT2R, fA2);
     // GetCornerV (fields.F90:457-517); its area stencil equals area1
-    R dA = rmax(central8(area1), (R)TINY);
+    R dA = rmax(fA1, (R)TINY);
     R VC[3];
     const long s2v = dstride(b, dT2);
 #pragma unroll
     for (int x = 0; x < 3; x++) {
         R acc = (R)0;
 #pragma unroll
-        for (int n = 0; n < 8; n++) acc += Rc<R>(w8(n)) * (area1[n] * w.Vf[(x + 3 * eD) * fs + c + (n - 4) * s2v]);
+        for (int n = 0; n < 8; n++) acc += Rc<R>(w8(n)) * w.AVf[(x + 3 * eD) * fs + c + (n - 4) * s2v];
         VC[x] = acc / dA;
     }
     const R* Te = g.Te;
@@ -479,43 +487,102 @@ __device__ __forceinline__ void gas_kin_flux(const DevParams<R>& P, R sgn, const
     dW[4] = dW[4] + sgn * E;
 }
 
-// Face fluxes of direction d (Fluxes, stress.F90:204-429).
-template <class R>
-__global__ void __launch_bounds__(128) k_stress(GamBox b, DevParams<R> P, Geo<R> g, StateBuf<R> cur, Work<R> w,
-                                                int d, Range r, const GamScalars* sc) {
+// Face fluxes of direction D (Fluxes, stress.F90:204-429), one face per
+// thread. A block of 32 x 8 threads covers a tile of 32 x 8 faces; its stencil
+// operands (volume, volume*primitives and volume*B of the half state, limiter
+// primitives and B) are first staged in shared memory with coalesced loads
+// issued back to back, then every thread reconstructs from shared memory.
+//   D = I: faces i0..i0+31 (x) 8 rows j, cells i0-4..i0+35   -> [var][8][40]
+//   D = J: faces 32 columns (x) j0..j0+7, cells j0-4..j0+10  -> [var][15][32]
+//   D = K: as J along k
+template <int D> struct STile {
+    static constexpr int NX = D == 0 ? 40 : 32;  // smem row length (i)
+    static constexpr int NY = D == 0 ? 8 : 15;   // smem rows
+};
+static constexpr int STRESS_NV = 17;  // vol, QW(5), QB(3), Wn(5), Bl(3)
+
+template <class R, int D> static constexpr size_t stress_smem() {
+    return sizeof(R) * STRESS_NV * STile<D>::NX * STile<D>::NY;
+}
+
+template <class R, int D>
+__global__ void __launch_bounds__(256, 2) k_stress(GamBox b, DevParams<R> P, Geo<R> g, const R* __restrict__ Blim,
+                                                   Work<R> w, Range r, const GamScalars* sc) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    R* sm = reinterpret_cast<R*>(smem_raw);
     if (sc->halted) return;
-    int ii, jj, kk;
-    if (!thread_ijk(r, ii, jj, kk)) return;
+    constexpr int NX = STile<D>::NX, NY = STile<D>::NY, NXY = NX * NY;
     const long fs = b.fs;
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + 32 * ty;
+    // tile origin (face indices)
+    int i0, a0, cz;  // a0: first face along the second tile axis; cz: fixed third index
+    i0 = r.i0 + 32 * blockIdx.x;
+    a0 = (D == 2 ? r.k0 : r.j0) + 8 * blockIdx.y;
+    cz = (D == 2 ? r.j0 : r.k0) + blockIdx.z;
+    const int nv = P.doMHD ? STRESS_NV : 11;
+    // ---- stage the stencil operands
+    for (int q = tid; q < nv * NXY; q += 256) {
+        const int v = q / NXY, rem = q - v * NXY, row = rem / NX, col = rem - row * NX;
+        int ii, jj, kk;
+        if (D == 0) { ii = i0 - 4 + col; jj = a0 + row; kk = cz; }
+        else if (D == 1) { ii = i0 + col; jj = a0 - 4 + row; kk = cz; }
+        else { ii = i0 + col; jj = cz; kk = a0 - 4 + row; }
+        R val = (R)0;
+        if (ii >= 0 && ii < b.Ni && jj >= 0 && jj < b.Nj && kk >= 0 && kk < b.Nk) {
+            const long c = lidx(b, ii, jj, kk);
+            const R* src;
+            if (v == 0) src = g.vol;
+            else if (v < 6) src = w.QW + (v - 1) * fs;
+            else if (v < 9 && P.doMHD) src = w.QB + (v - 6) * fs;
+            else {
+                const int u = P.doMHD ? v - 9 : v - 6;  // limiter block
+                src = u < 5 ? w.Wn + u * fs : Blim + (u - 5) * fs;
+            }
+            val = src[c];
+        }
+        sm[q] = val;
+    }
+    __syncthreads();
+    // ---- this thread's face
+    int ii, jj, kk;
+    if (D == 0) { ii = i0 + tx; jj = a0 + ty; kk = cz; }
+    else if (D == 1) { ii = i0 + tx; jj = a0 + ty; kk = cz; }
+    else { ii = i0 + tx; jj = cz; kk = a0 + ty; }
+    if (ii > r.i1 || (D == 2 ? kk > r.k1 : jj > r.j1)) return;
     const long c = lidx(b, ii, jj, kk);
-    const long s = dstride(b, d);
-    R vol[8];
-#pragma unroll
-    for (int n = 0; n < 8; n++) vol[n] = g.vol[c + (n - 4) * s];
-    const R Vi = central8(vol);
+    // smem offset of stencil point n (n = 0..7 -> cells -4..3) of variable v
+    auto at = [&](int v, int n) -> R {
+        if (D == 0) return sm[v * NXY + ty * NX + tx + n];
+        return sm[v * NXY + (ty + n) * NX + tx];
+    };
+    // face data, issued early
     R T[9];
 #pragma unroll
-    for (int n = 0; n < 9; n++) T[n] = g.Tf[(n + 9 * d) * fs + c];
-    const R fa = g.face[d * fs + c];
+    for (int n = 0; n < 9; n++) T[n] = g.Tf[(n + 9 * D) * fs + c];
+    const R fa = g.face[D * fs + c];
+    R vol[8];
+#pragma unroll
+    for (int n = 0; n < 8; n++) vol[n] = at(0, n);
+    const R Vi = central8(vol);
     R MagL[3] = {(R)0, (R)0, (R)0}, MagR[3] = {(R)0, (R)0, (R)0};
     R Bn = (R)0;
     double B0[3] = {0.0, 0.0, 0.0}, B0n = 0.0;
+    const int lim0 = P.doMHD ? 9 : 6;  // first limiter variable
     if (P.doMHD) {
+        Bn = w.Bnf[D * fs + c];
 #pragma unroll
         for (int x = 0; x < 3; x++) {
             R q[8], nq[4];
 #pragma unroll
-            for (int n = 0; n < 8; n++) q[n] = w.Bh[x * fs + c + (n - 4) * s];
+            for (int n = 0; n < 8; n++) q[n] = at(6 + x, n);
 #pragma unroll
-            for (int m = 0; m < 4; m++)
-                nq[m] = P.doLFMLim ? cur.B[x * fs + c + (m - 2) * s] : w.Bh[x * fs + c + (m - 2) * s];
-            get_lrs(P, vol, q, nq, Vi, MagL[x], MagR[x]);
+            for (int m = 0; m < 4; m++) nq[m] = at(lim0 + 5 + x, m + 2);
+            lrs_from_qdv(P, q, nq, Vi, MagL[x], MagR[x]);
         }
-        Bn = w.Bnf[d * fs + c];
         if (P.doBackground) {
 #pragma unroll
-            for (int x = 0; x < 3; x++) B0[x] = g.fcB0[(x + 3 * d) * fs + c];
-            B0n = g.bFlux0[d * fs + c] / (double)fa;
+            for (int x = 0; x < 3; x++) B0[x] = g.fcB0[(x + 3 * D) * fs + c];
+            B0n = g.bFlux0[D * fs + c] / (double)fa;
         }
     }
     R WL[5], WR[5];
@@ -523,11 +590,10 @@ __global__ void __launch_bounds__(128) k_stress(GamBox b, DevParams<R> P, Geo<R>
     for (int v = 0; v < 5; v++) {
         R q[8], nq[4];
 #pragma unroll
-        for (int n = 0; n < 8; n++) q[n] = w.Wh[v * fs + c + (n - 4) * s];
+        for (int n = 0; n < 8; n++) q[n] = at(1 + v, n);
 #pragma unroll
-        for (int m = 0; m < 4; m++)
-            nq[m] = P.doLFMLim ? w.Wn[v * fs + c + (m - 2) * s] : w.Wh[v * fs + c + (m - 2) * s];
-        get_lrs(P, vol, q, nq, Vi, WL[v], WR[v]);
+        for (int m = 0; m < 4; m++) nq[m] = at(lim0 + v, m + 2);
+        lrs_from_qdv(P, q, nq, Vi, WL[v], WR[v]);
     }
     R VaD = (R)0, bbD = (R)0;
     if (P.doMHD) {
@@ -535,7 +601,7 @@ __global__ void __launch_bounds__(128) k_stress(GamBox b, DevParams<R> P, Geo<R>
         mag_kin_flux(P, (R)-1, WL, MagL, Bn, T, B0, B0n, mF, bbD, VaD);
         mag_kin_flux(P, (R)1, WR, MagR, Bn, T, B0, B0n, mF, bbD, VaD);
 #pragma unroll
-        for (int x = 0; x < 3; x++) w.mF[(x + 3 * d) * fs + c] = fa * mF[x];
+        for (int x = 0; x < 3; x++) w.mF[(x + 3 * D) * fs + c] = fa * mF[x];
     }
     R gF[5] = {(R)0, (R)0, (R)0, (R)0, (R)0}, dW[5] = {(R)0, (R)0, (R)0, (R)0, (R)0};
     gas_kin_flux(P, (R)-1, WL, T, gF, dW);
@@ -543,7 +609,7 @@ __global__ void __launch_bounds__(128) k_stress(GamBox b, DevParams<R> P, Geo<R>
 #pragma unroll
     for (int v = 0; v < 5; v++) {
         R gv = gF[v] - (R)1 * P.cHogH * VaD * dW[v];
-        w.gF[(v + 5 * d) * fs + c] = fa * gv;
+        w.gF[(v + 5 * D) * fs + c] = fa * gv;
     }
 }
 
@@ -861,9 +927,12 @@ static inline dim3 grid_for(const Range& r, dim3 blk) {
                 (unsigned)((r.k1 - r.k0 + 1 + blk.z - 1) / blk.z));
 }
 
-// One stepGamera on stream s; st[cur] is State (n), st[1-cur] holds oState
-// (n-1) on entry and State (n+1) on exit.
-template <class R> void launch_step(const Ctx<R>& C, int cur, cudaStream_t s) {
+// The kernels of one stepGamera in order, each handed to f(id, launch) with
+// id: 0 begin, 1 predict, 2/3 mom2face/vxb I, 4/5 J, 6/7 K, 8/9/10 stress
+// I/J/K, 11 update_faces, 12 update_cells, 13 dt_finalize, 14 bc.
+// st[cur] is State (n); st[1-cur] holds oState (n-1) on entry and State
+// (n+1) on exit.
+template <class R, class F> void for_each_kernel(const Ctx<R>& C, int cur, cudaStream_t s, F&& f) {
     const GamBox& b = C.b;
     const int G = GAM_NG;
     const StateBuf<R> S = C.st[cur], O = C.st[1 - cur];
@@ -871,8 +940,8 @@ template <class R> void launch_step(const Ctx<R>& C, int cur, cudaStream_t s) {
     const Range all{0, b.Ni, 0, b.Nj, 0, b.Nk};
     const Range cells{0, b.Ni - 1, 0, b.Nj - 1, 0, b.Nk - 1};
     const int kke = C.P.do25D ? G : G + b.Nkp - 1;  // last active k of the stress sweep
-    k_step_begin<<<1, 1, 0, s>>>(C.sc);
-    k_predict<R><<<grid_for(all, blk), blk, 0, s>>>(b, C.P, C.g, S, O, C.w, C.sc);
+    f(0, [&] { k_step_begin<<<1, 1, 0, s>>>(C.sc); });
+    f(1, [&] { k_predict<R><<<grid_for(all, blk), blk, 0, s>>>(b, C.P, C.g, S, O, C.w, C.sc); });
     if (C.P.doMHD) {
         const Range mf[3] = {{0, b.Ni - 1, G, G + b.Njp, 0, b.Nk - 1},
                              {0, b.Ni - 1, 0, b.Nj - 1, G, G + b.Nkp},
@@ -881,19 +950,63 @@ template <class R> void launch_step(const Ctx<R>& C, int cur, cudaStream_t s) {
                              {G, G + b.Nip, G, G + b.Njp - 1, G, G + b.Nkp},
                              {G, G + b.Nip, G, G + b.Njp, G, G + b.Nkp - 1}};
         for (int eD = 0; eD < 3; eD++) {
-            k_mom2face<R><<<grid_for(mf[eD], blk), blk, 0, s>>>(b, C.P, C.g, C.w, eD, mf[eD], C.sc);
-            k_vxb<R><<<grid_for(ed[eD], blk), blk, 0, s>>>(b, C.P, C.g, C.w, eD, ed[eD], C.sc);
+            f(2 + 2 * eD, [&] { k_mom2face<R><<<grid_for(mf[eD], blk), blk, 0, s>>>(b, C.P, C.g, C.w, eD, mf[eD], C.sc); });
+            f(3 + 2 * eD, [&] { k_vxb<R><<<grid_for(ed[eD], blk), blk, 0, s>>>(b, C.P, C.g, C.w, eD, ed[eD], C.sc); });
         }
     }
     const Range fr[3] = {{G, G + b.Nip, G, G + b.Njp - 1, G, kke},
                          {G, G + b.Nip - 1, G, G + b.Njp, G, kke},
                          {G, G + b.Nip - 1, G, G + b.Njp - 1, G, G + b.Nkp}};
-    const int nFlx = C.P.do25D ? 2 : 3;
-    for (int d = 0; d < nFlx; d++) k_stress<R><<<grid_for(fr[d], blk), blk, 0, s>>>(b, C.P, C.g, S, C.w, d, fr[d], C.sc);
-    k_update_faces<R><<<grid_for(all, blk), blk, 0, s>>>(b, C.P, S, O, C.w, C.sc);
-    k_update_cells<R><<<grid_for(cells, blk), blk, 0, s>>>(b, C.P, C.g, S, O, C.w, C.sc, C.gamma, C.gm1);
-    k_dt_finalize<<<1, 1, 0, s>>>(C.sc);
-    k_bc<R><<<grid_for(all, blk), blk, 0, s>>>(b, C.P, C.g, O, C.sc, 0);
+    const R* Blim = C.P.doLFMLim ? S.B : C.w.Bl;
+    const dim3 sblk(32, 8, 1);
+    auto sgrid = [&](const Range& r, int D) {
+        const int ni = r.i1 - r.i0 + 1, nj = r.j1 - r.j0 + 1, nk = r.k1 - r.k0 + 1;
+        if (D == 2) return dim3((ni + 31) / 32, (nk + 7) / 8, nj);
+        return dim3((ni + 31) / 32, (nj + 7) / 8, nk);
+    };
+    f(8, [&] { k_stress<R, 0><<<sgrid(fr[0], 0), sblk, stress_smem<R, 0>(), s>>>(b, C.P, C.g, Blim, C.w, fr[0], C.sc); });
+    f(9, [&] { k_stress<R, 1><<<sgrid(fr[1], 1), sblk, stress_smem<R, 1>(), s>>>(b, C.P, C.g, Blim, C.w, fr[1], C.sc); });
+    if (!C.P.do25D)
+        f(10, [&] { k_stress<R, 2><<<sgrid(fr[2], 2), sblk, stress_smem<R, 2>(), s>>>(b, C.P, C.g, Blim, C.w, fr[2], C.sc); });
+    f(11, [&] { k_update_faces<R><<<grid_for(all, blk), blk, 0, s>>>(b, C.P, S, O, C.w, C.sc); });
+    f(12, [&] { k_update_cells<R><<<grid_for(cells, blk), blk, 0, s>>>(b, C.P, C.g, S, O, C.w, C.sc, C.gamma, C.gm1); });
+    f(13, [&] { k_dt_finalize<<<1, 1, 0, s>>>(C.sc); });
+    f(14, [&] { k_bc<R><<<grid_for(all, blk), blk, 0, s>>>(b, C.P, C.g, O, C.sc, 0); });
+}
+
+template <class R> void launch_step(const Ctx<R>& C, int cur, cudaStream_t s) {
+    for_each_kernel(C, cur, s, [](int, auto&& L) { L(); });
+}
+
+// Device time of each kernel of a step (ms, average of reps back-to-back
+// launches; ms[15]). The kernels after k_step_begin read their inputs and
+// write other arrays, so repeating one changes nothing; the time bookkeeping
+// kernels are not run.
+template <class R> void profile_step(const Ctx<R>& C, int cur, cudaStream_t s, int reps, double* ms) {
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    for (int q = 0; q < 15; q++) ms[q] = 0.0;
+    for_each_kernel(C, cur, s, [&](int id, auto&& L) {
+        if (id == 0 || id == 13) return;
+        L();  // warm
+        cudaEventRecord(e0, s);
+        for (int r = 0; r < reps; r++) L();
+        cudaEventRecord(e1, s);
+        cudaEventSynchronize(e1);
+        float t = 0.f;
+        cudaEventElapsedTime(&t, e0, e1);
+        ms[id] = t / reps;
+    });
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+}
+
+// Kernel attributes that must be set before a launch is captured in a graph.
+template <class R> void prepare() {
+    cudaFuncSetAttribute(k_stress<R, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stress_smem<R, 0>());
+    cudaFuncSetAttribute(k_stress<R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stress_smem<R, 1>());
+    cudaFuncSetAttribute(k_stress<R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stress_smem<R, 2>());
 }
 
 // CalcDT on st[cur] into sc->dtmin_bits (the caller resets it first).

@@ -33,14 +33,16 @@ template <class R> struct StateBuf {
 };
 
 template <class R> struct Work {
-    R* Wh;   // cell, 5: primitives of the half state (BlockCon2Prim)
-    R* Wn;   // cell, 5: primitives of state n (limiter stencils)
+    R* QW;   // cell, 5: volume * primitives of the half state (BlockCon2Prim), the recon operand
+    R* QB;   // cell, 3: volume * Bxyz of the half state
+    R* Dh;   // cell, 1: half-state density (GetCornerD)
+    R* Wn;   // cell, 5: limiter primitives (state n with lfmlim, else the half state)
+    R* Bl;   // cell, 3: limiter Bxyz without lfmlim (= half-state Bxyz); lfmlim uses State%Bxyz
     R* VdV;  // cell, 3: volume * momentum / max(density, dFloor) of the half state
-    R* Bh;   // cell, 3: Bxyz of the half state
-    R* bh;   // face, 3: half-state flux / max(area, TINY)
-    R* bn;   // face, 3: state-n flux / max(area, TINY)
+    R* abh;  // face, 3: area * (half-state flux / max(area, TINY)), the EdgeLRs recon operand
+    R* bn;   // face, 3: limiter flux / max(area, TINY)
     R* Bnf;  // face, 3: half-state flux / area
-    R* Vf;   // cell, 9: Vf(x) for edge direction eD at x + 3*eD
+    R* AVf;  // cell, 9: area(dT1) * Vf(x) for edge direction eD at x + 3*eD
     R* E;    // edge, 3
     R* gF;   // face, 15: gas flux v + 5*d (already times face area)
     R* mF;   // face, 9: magnetic flux x + 3*d

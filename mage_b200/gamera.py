@@ -51,7 +51,7 @@ EXPORTED = (
     "gam_default_params", "gam_create", "gam_destroy", "gam_last_error", "gam_set_geometry",
     "gam_set_geometry_arrays", "gam_get_geometry_arrays", "gam_upload_state", "gam_download_state", "gam_step",
     "gam_calc_dt", "gam_divb", "gam_totals", "gam_last_step_ms", "gam_advance_model", "gam_init_orszag_tang",
-    "gam_init_blast_wave",
+    "gam_init_blast_wave", "gam_profile_step",
 )
 
 _lib = None
@@ -84,6 +84,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     L.gam_advance_model.argtypes = [C.c_void_p, C.c_double, _dp]
     L.gam_init_orszag_tang.argtypes = [C.c_void_p]
     L.gam_init_blast_wave.argtypes = [C.c_void_p, _dp]
+    L.gam_profile_step.argtypes = [C.c_void_p, C.c_int32, _dp, C.c_int32]
     _lib = L
     return L
 
@@ -255,6 +256,15 @@ class GameraGPU:
         out = np.zeros(5)
         self._check(self.L.gam_totals(self.h, _ptr(out)))
         return out
+
+    KERNEL_NAMES = ("begin", "predict", "mom2face_i", "vxb_i", "mom2face_j", "vxb_j", "mom2face_k", "vxb_k",
+                    "stress_i", "stress_j", "stress_k", "update_faces", "update_cells", "dt_finalize", "bc")
+
+    def profile_step(self, reps: int = 5) -> dict:
+        """Device time (ms) of each kernel of one step (diagnostic)."""
+        ms = np.zeros(15)
+        self._check(self.L.gam_profile_step(self.h, int(reps), _ptr(ms), 15))
+        return dict(zip(self.KERNEL_NAMES, ms.tolist()))
 
     def last_step_ms(self) -> float:
         v = C.c_double()

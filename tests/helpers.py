@@ -33,23 +33,16 @@ def make_oracle(problem: str, N, variant="strict", **kw):
 
 def gpu_from_oracle(o: Oracle, precision=0, strict=False, **kw) -> GameraGPU:
     p = o.p
-    gp = GamParams(p.Nip, p.Njp, p.Nkp, gamma=p.gamma, CFL=p.CFL, pdmb=p.pdmb, Vd0=p.Vd0, cHogH=p.cHogH,
-                   cHogM=p.cHogM, dFloor=p.dFloor, pFloor=p.pFloor, tFin=p.tFin, dt0=p.dt0, limDT0=p.limDT0,
-                   rmeth=1 if p.up7 else 0, doLFMLim=p.doLFMLim, doMHD=p.doMHD, do25D=p.do25D,
-                   precision=precision, strict=strict, **kw)
-    g = GameraGPU(gp)
+    args = dict(gamma=p.gamma, CFL=p.CFL, pdmb=p.pdmb, Vd0=p.Vd0, cHogH=p.cHogH, cHogM=p.cHogM, dFloor=p.dFloor,
+                pFloor=p.pFloor, tFin=p.tFin, dt0=p.dt0, limDT0=p.limDT0, rmeth=1 if p.up7 else 0,
+                doLFMLim=p.doLFMLim, doMHD=p.doMHD, do25D=p.do25D, precision=precision, strict=strict)
+    args.update(kw)
+    g = GameraGPU(GamParams(p.Nip, p.Njp, p.Nkp, **args))
     g.set_geometry_arrays({n: o.array(GEO_FROM_ORACLE[n]) for n, _, _ in GEOMETRY_ARRAYS})
     sc = o.scalars()
     g.upload_state(o.array("Gas"), o.array("magFlux"), o.array("Bxyz"), o.array("oGas"), o.array("omagFlux"),
                    sc["time"], sc["otime"], sc["dt"], sc["ts"])
     return g
-
-
-def active(a: np.ndarray, face=False):
-    """Active-region view (with the upper face layer for face arrays)."""
-    e = 1 if face else 0
-    return a[:, 4:a.shape[1] - 4 + e - (1 if face else 0) + (1 if face else 0) - e + e,
-             4:a.shape[2] - 4, 4:a.shape[3] - 4]
 
 
 def rel_err(a, b):
