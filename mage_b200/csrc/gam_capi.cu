@@ -157,6 +157,8 @@ template <class R> static int alloc_bulk(gam_handle* h, Ctx<R>& C) {
     C.sc = h->sc;
     C.gamma = h->p.gamma;
     C.gm1 = h->p.gamma - 1;
+    const char* kv = getenv("GAM_KVAR");  // launch-configuration experiments
+    C.kvar = kv ? atoi(kv) : 0;
     return GAM_OK;
 }
 

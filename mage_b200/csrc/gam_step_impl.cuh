@@ -31,6 +31,7 @@
 
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <type_traits>
 #include "gam_layout.cuh"
 #include "gam_math.cuh"
 #include "gam_types.cuh"
@@ -488,95 +489,40 @@ __device__ __forceinline__ void gas_kin_flux(const DevParams<R>& P, R sgn, const
 }
 
 // Face fluxes of direction D (Fluxes, stress.F90:204-429), one face per
-// thread. A block of 32 x 8 threads covers a tile of 32 x 8 faces; its stencil
-// operands (volume, volume*primitives and volume*B of the half state, limiter
-// primitives and B) are first staged in shared memory with coalesced loads
-// issued back to back, then every thread reconstructs from shared memory.
-//   D = I: faces i0..i0+31 (x) 8 rows j, cells i0-4..i0+35   -> [var][8][40]
-//   D = J: faces 32 columns (x) j0..j0+7, cells j0-4..j0+10  -> [var][15][32]
-//   D = K: as J along k
-template <int D> struct STile {
-    static constexpr int NX = D == 0 ? 40 : 32;  // smem row length (i)
-    static constexpr int NY = D == 0 ? 8 : 15;   // smem rows
-};
-static constexpr int STRESS_NV = 17;  // vol, QW(5), QB(3), Wn(5), Bl(3)
-
-template <class R, int D> static constexpr size_t stress_smem() {
-    return sizeof(R) * STRESS_NV * STile<D>::NX * STile<D>::NY;
-}
-
-template <class R, int D>
-__global__ void __launch_bounds__(256, 2) k_stress(GamBox b, DevParams<R> P, Geo<R> g, const R* __restrict__ Blim,
-                                                   Work<R> w, Range r, const GamScalars* sc) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    R* sm = reinterpret_cast<R*>(smem_raw);
+// thread. The stencil operands are the per-cell products volume*primitive and
+// volume*B of the half state (QdV of Cen8LRs) and the limiter values, read
+// along D through L1; MINB bounds the registers for occupancy.
+template <class R, int D, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_stress(GamBox b, DevParams<R> P, Geo<R> g, const R* __restrict__ Blim,
+                                                      Work<R> w, Range r, const GamScalars* sc) {
     if (sc->halted) return;
-    constexpr int NX = STile<D>::NX, NY = STile<D>::NY, NXY = NX * NY;
-    const long fs = b.fs;
-    const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + 32 * ty;
-    // tile origin (face indices)
-    int i0, a0, cz;  // a0: first face along the second tile axis; cz: fixed third index
-    i0 = r.i0 + 32 * blockIdx.x;
-    a0 = (D == 2 ? r.k0 : r.j0) + 8 * blockIdx.y;
-    cz = (D == 2 ? r.j0 : r.k0) + blockIdx.z;
-    const int nv = P.doMHD ? STRESS_NV : 11;
-    // ---- stage the stencil operands
-    for (int q = tid; q < nv * NXY; q += 256) {
-        const int v = q / NXY, rem = q - v * NXY, row = rem / NX, col = rem - row * NX;
-        int ii, jj, kk;
-        if (D == 0) { ii = i0 - 4 + col; jj = a0 + row; kk = cz; }
-        else if (D == 1) { ii = i0 + col; jj = a0 - 4 + row; kk = cz; }
-        else { ii = i0 + col; jj = cz; kk = a0 - 4 + row; }
-        R val = (R)0;
-        if (ii >= 0 && ii < b.Ni && jj >= 0 && jj < b.Nj && kk >= 0 && kk < b.Nk) {
-            const long c = lidx(b, ii, jj, kk);
-            const R* src;
-            if (v == 0) src = g.vol;
-            else if (v < 6) src = w.QW + (v - 1) * fs;
-            else if (v < 9 && P.doMHD) src = w.QB + (v - 6) * fs;
-            else {
-                const int u = P.doMHD ? v - 9 : v - 6;  // limiter block
-                src = u < 5 ? w.Wn + u * fs : Blim + (u - 5) * fs;
-            }
-            val = src[c];
-        }
-        sm[q] = val;
-    }
-    __syncthreads();
-    // ---- this thread's face
     int ii, jj, kk;
-    if (D == 0) { ii = i0 + tx; jj = a0 + ty; kk = cz; }
-    else if (D == 1) { ii = i0 + tx; jj = a0 + ty; kk = cz; }
-    else { ii = i0 + tx; jj = cz; kk = a0 + ty; }
-    if (ii > r.i1 || (D == 2 ? kk > r.k1 : jj > r.j1)) return;
+    if (!thread_ijk(r, ii, jj, kk)) return;
+    const long fs = b.fs;
     const long c = lidx(b, ii, jj, kk);
-    // smem offset of stencil point n (n = 0..7 -> cells -4..3) of variable v
-    auto at = [&](int v, int n) -> R {
-        if (D == 0) return sm[v * NXY + ty * NX + tx + n];
-        return sm[v * NXY + (ty + n) * NX + tx];
-    };
-    // face data, issued early
+    const long s = D == 0 ? 1L : (D == 1 ? (long)b.sx : b.sk);
     R T[9];
 #pragma unroll
     for (int n = 0; n < 9; n++) T[n] = g.Tf[(n + 9 * D) * fs + c];
     const R fa = g.face[D * fs + c];
     R vol[8];
 #pragma unroll
-    for (int n = 0; n < 8; n++) vol[n] = at(0, n);
+    for (int n = 0; n < 8; n++) vol[n] = g.vol[c + (n - 4) * s];
     const R Vi = central8(vol);
     R MagL[3] = {(R)0, (R)0, (R)0}, MagR[3] = {(R)0, (R)0, (R)0};
     R Bn = (R)0;
     double B0[3] = {0.0, 0.0, 0.0}, B0n = 0.0;
-    const int lim0 = P.doMHD ? 9 : 6;  // first limiter variable
     if (P.doMHD) {
         Bn = w.Bnf[D * fs + c];
 #pragma unroll
         for (int x = 0; x < 3; x++) {
             R q[8], nq[4];
+            const R* qp = w.QB + x * fs + c - 4 * s;
+            const R* lp = Blim + x * fs + c - 2 * s;
 #pragma unroll
-            for (int n = 0; n < 8; n++) q[n] = at(6 + x, n);
+            for (int n = 0; n < 8; n++) q[n] = qp[n * s];
 #pragma unroll
-            for (int m = 0; m < 4; m++) nq[m] = at(lim0 + 5 + x, m + 2);
+            for (int m = 0; m < 4; m++) nq[m] = lp[m * s];
             lrs_from_qdv(P, q, nq, Vi, MagL[x], MagR[x]);
         }
         if (P.doBackground) {
@@ -589,10 +535,12 @@ __global__ void __launch_bounds__(256, 2) k_stress(GamBox b, DevParams<R> P, Geo
 #pragma unroll
     for (int v = 0; v < 5; v++) {
         R q[8], nq[4];
+        const R* qp = w.QW + v * fs + c - 4 * s;
+        const R* lp = w.Wn + v * fs + c - 2 * s;
 #pragma unroll
-        for (int n = 0; n < 8; n++) q[n] = at(1 + v, n);
+        for (int n = 0; n < 8; n++) q[n] = qp[n * s];
 #pragma unroll
-        for (int m = 0; m < 4; m++) nq[m] = at(lim0 + v, m + 2);
+        for (int m = 0; m < 4; m++) nq[m] = lp[m * s];
         lrs_from_qdv(P, q, nq, Vi, WL[v], WR[v]);
     }
     R VaD = (R)0, bbD = (R)0;
@@ -958,16 +906,19 @@ template <class R, class F> void for_each_kernel(const Ctx<R>& C, int cur, cudaS
                          {G, G + b.Nip - 1, G, G + b.Njp, G, kke},
                          {G, G + b.Nip - 1, G, G + b.Njp - 1, G, G + b.Nkp}};
     const R* Blim = C.P.doLFMLim ? S.B : C.w.Bl;
-    const dim3 sblk(32, 8, 1);
-    auto sgrid = [&](const Range& r, int D) {
-        const int ni = r.i1 - r.i0 + 1, nj = r.j1 - r.j0 + 1, nk = r.k1 - r.k0 + 1;
-        if (D == 2) return dim3((ni + 31) / 32, (nk + 7) / 8, nj);
-        return dim3((ni + 31) / 32, (nj + 7) / 8, nk);
+    auto stress = [&](auto Dc) {
+        constexpr int D = decltype(Dc)::value;
+        const Range& r = fr[D];
+        switch (C.kvar) {
+            case 1: k_stress<R, D, 4><<<grid_for(r, blk), blk, 0, s>>>(b, C.P, C.g, Blim, C.w, r, C.sc); break;
+            case 2: k_stress<R, D, 5><<<grid_for(r, blk), blk, 0, s>>>(b, C.P, C.g, Blim, C.w, r, C.sc); break;
+            case 3: k_stress<R, D, 6><<<grid_for(r, blk), blk, 0, s>>>(b, C.P, C.g, Blim, C.w, r, C.sc); break;
+            default: k_stress<R, D, 1><<<grid_for(r, blk), blk, 0, s>>>(b, C.P, C.g, Blim, C.w, r, C.sc); break;
+        }
     };
-    f(8, [&] { k_stress<R, 0><<<sgrid(fr[0], 0), sblk, stress_smem<R, 0>(), s>>>(b, C.P, C.g, Blim, C.w, fr[0], C.sc); });
-    f(9, [&] { k_stress<R, 1><<<sgrid(fr[1], 1), sblk, stress_smem<R, 1>(), s>>>(b, C.P, C.g, Blim, C.w, fr[1], C.sc); });
-    if (!C.P.do25D)
-        f(10, [&] { k_stress<R, 2><<<sgrid(fr[2], 2), sblk, stress_smem<R, 2>(), s>>>(b, C.P, C.g, Blim, C.w, fr[2], C.sc); });
+    f(8, [&] { stress(std::integral_constant<int, 0>()); });
+    f(9, [&] { stress(std::integral_constant<int, 1>()); });
+    if (!C.P.do25D) f(10, [&] { stress(std::integral_constant<int, 2>()); });
     f(11, [&] { k_update_faces<R><<<grid_for(all, blk), blk, 0, s>>>(b, C.P, S, O, C.w, C.sc); });
     f(12, [&] { k_update_cells<R><<<grid_for(cells, blk), blk, 0, s>>>(b, C.P, C.g, S, O, C.w, C.sc, C.gamma, C.gm1); });
     f(13, [&] { k_dt_finalize<<<1, 1, 0, s>>>(C.sc); });
@@ -1003,11 +954,7 @@ template <class R> void profile_step(const Ctx<R>& C, int cur, cudaStream_t s, i
 }
 
 // Kernel attributes that must be set before a launch is captured in a graph.
-template <class R> void prepare() {
-    cudaFuncSetAttribute(k_stress<R, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stress_smem<R, 0>());
-    cudaFuncSetAttribute(k_stress<R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stress_smem<R, 1>());
-    cudaFuncSetAttribute(k_stress<R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stress_smem<R, 2>());
-}
+template <class R> void prepare() {}
 
 // CalcDT on st[cur] into sc->dtmin_bits (the caller resets it first).
 template <class R> void launch_dt_only(const Ctx<R>& C, int cur, cudaStream_t s) {
