@@ -233,8 +233,8 @@ __global__ void k_step_begin(GamScalars* sc) {
 // volume * primitive (the recon operand QdV of Cen8LRs/Up7LRs), the limiter
 // primitives, volume * momentum / density (Mom2Face), and per face
 // area * flux/max(area,TINY) and flux/max(area,TINY) (EdgeLRs), flux/area (Fluxes).
-template <class R>
-__global__ void __launch_bounds__(256) k_predict(GamBox b, DevParams<R> P, Geo<R> g, StateBuf<R> cur,
+template <class R, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_predict(GamBox b, DevParams<R> P, Geo<R> g, StateBuf<R> cur,
                                                  StateBuf<R> old, Work<R> w, const GamScalars* sc) {
     if (sc->halted) return;
     int ii, jj, kk;
@@ -613,8 +613,8 @@ __device__ __forceinline__ double cell_dt(const DevParams<R>& P, const double* U
 
 // Flux2Deltas + CellReynolds + bFlux2Fld + CellMaxwell for active cells,
 // copy + bFlux2Fld for ghost cells, then the CFL dt of cells in the dt range.
-template <class R>
-__global__ void __launch_bounds__(128) k_update_cells(GamBox b, DevParams<R> P, Geo<R> g, StateBuf<R> cur,
+template <class R, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_update_cells(GamBox b, DevParams<R> P, Geo<R> g, StateBuf<R> cur,
                                                       StateBuf<R> nxt, Work<R> w, GamScalars* sc, double gamma_d,
                                                       double gm1_d) {
     __shared__ double smin[32];
@@ -765,13 +765,69 @@ __device__ __forceinline__ int bc_map(int x, int n, int kind_lo, int kind_hi, bo
 // final bFlux2Fld of every cell whose value or faces it changed.
 // copyB: fill ghost Bxyz by the same gather instead of recomputing it (the
 // initial EnforceBCs of CalcGridInfo, init.F90:226-238, has no bFlux2Fld after it).
+// The boundary fill only touches indices outside the deep interior
+// [G+1, G+N-2]^3 (ghost cells/faces and the cells whose faces they are):
+// the launch enumerates that shell. Per dimension, the "outer" indices are
+// [0, G] and [G+N-1, Nmax]; all of [0, Nmax] when the interior is empty.
+struct Shell {
+    int nx, ny, nz;         // face-box extents (Ni+1, Nj+1, Nk+1)
+    int a[3], bnd[3];       // deep interior [a, bnd] per dimension (empty if bnd < a)
+    long nA, nB, nC;        // counts of the three parts
+};
+static inline Shell make_shell(const GamBox& b) {
+    Shell sh;
+    sh.nx = b.Ni + 1; sh.ny = b.Nj + 1; sh.nz = b.Nk + 1;
+    const int N[3] = {b.Nip, b.Njp, b.Nkp}, M[3] = {sh.nx, sh.ny, sh.nz};
+    int nout[3], nin[3];
+    for (int d = 0; d < 3; d++) {
+        sh.a[d] = GAM_NG + 1;
+        sh.bnd[d] = GAM_NG + N[d] - 2;
+        nin[d] = sh.bnd[d] >= sh.a[d] ? sh.bnd[d] - sh.a[d] + 1 : 0;
+        nout[d] = M[d] - nin[d];
+    }
+    sh.nA = (long)nout[2] * sh.ny * sh.nx;
+    sh.nB = (long)nin[2] * nout[1] * sh.nx;
+    sh.nC = (long)nin[2] * nin[1] * nout[0];
+    return sh;
+}
+__device__ __forceinline__ int outer_coord(int o, int a, int bnd) { return (bnd >= a && o >= a) ? o - a + bnd + 1 : o; }
+__device__ __forceinline__ bool shell_ijk(const Shell& sh, long t, int& ii, int& jj, int& kk) {
+    if (t < sh.nA) {
+        ii = (int)(t % sh.nx);
+        long q = t / sh.nx;
+        jj = (int)(q % sh.ny);
+        kk = outer_coord((int)(q / sh.ny), sh.a[2], sh.bnd[2]);
+        return true;
+    }
+    t -= sh.nA;
+    if (t < sh.nB) {
+        ii = (int)(t % sh.nx);
+        long q = t / sh.nx;
+        const int nout1 = sh.ny - (sh.bnd[1] >= sh.a[1] ? sh.bnd[1] - sh.a[1] + 1 : 0);
+        jj = outer_coord((int)(q % nout1), sh.a[1], sh.bnd[1]);
+        kk = sh.a[2] + (int)(q / nout1);
+        return true;
+    }
+    t -= sh.nB;
+    if (t < sh.nC) {
+        const int nout0 = sh.nx - (sh.bnd[0] >= sh.a[0] ? sh.bnd[0] - sh.a[0] + 1 : 0);
+        ii = outer_coord((int)(t % nout0), sh.a[0], sh.bnd[0]);
+        long q = t / nout0;
+        const int nin1 = sh.bnd[1] - sh.a[1] + 1;
+        jj = sh.a[1] + (int)(q % nin1);
+        kk = sh.a[2] + (int)(q / nin1);
+        return true;
+    }
+    return false;
+}
+
 template <class R>
 __global__ void __launch_bounds__(256) k_bc(GamBox b, DevParams<R> P, Geo<R> g, StateBuf<R> s, const GamScalars* sc,
-                                            int copyB) {
+                                            int copyB, Shell sh) {
     if (sc->halted) return;
     int ii, jj, kk;
-    Range r{0, b.Ni, 0, b.Nj, 0, b.Nk};
-    if (!thread_ijk(r, ii, jj, kk)) return;
+    const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (!shell_ijk(sh, t, ii, jj, kk)) return;
     const long fs = b.fs;
     const long c = lidx(b, ii, jj, kk);
     const bool k25 = P.do25D != 0;
@@ -889,7 +945,13 @@ template <class R, class F> void for_each_kernel(const Ctx<R>& C, int cur, cudaS
     const Range cells{0, b.Ni - 1, 0, b.Nj - 1, 0, b.Nk - 1};
     const int kke = C.P.do25D ? G : G + b.Nkp - 1;  // last active k of the stress sweep
     f(0, [&] { k_step_begin<<<1, 1, 0, s>>>(C.sc); });
-    f(1, [&] { k_predict<R><<<grid_for(all, blk), blk, 0, s>>>(b, C.P, C.g, S, O, C.w, C.sc); });
+    const dim3 pblk(32, 8, 1);
+    f(1, [&] {
+        if (C.kvar & 8)
+            k_predict<R, 4><<<grid_for(all, pblk), pblk, 0, s>>>(b, C.P, C.g, S, O, C.w, C.sc);
+        else
+            k_predict<R, 1><<<grid_for(all, pblk), pblk, 0, s>>>(b, C.P, C.g, S, O, C.w, C.sc);
+    });
     if (C.P.doMHD) {
         const Range mf[3] = {{0, b.Ni - 1, G, G + b.Njp, 0, b.Nk - 1},
                              {0, b.Ni - 1, 0, b.Nj - 1, G, G + b.Nkp},
@@ -909,20 +971,27 @@ template <class R, class F> void for_each_kernel(const Ctx<R>& C, int cur, cudaS
     auto stress = [&](auto Dc) {
         constexpr int D = decltype(Dc)::value;
         const Range& r = fr[D];
-        switch (C.kvar) {
-            case 1: k_stress<R, D, 4><<<grid_for(r, blk), blk, 0, s>>>(b, C.P, C.g, Blim, C.w, r, C.sc); break;
-            case 2: k_stress<R, D, 5><<<grid_for(r, blk), blk, 0, s>>>(b, C.P, C.g, Blim, C.w, r, C.sc); break;
-            case 3: k_stress<R, D, 6><<<grid_for(r, blk), blk, 0, s>>>(b, C.P, C.g, Blim, C.w, r, C.sc); break;
-            default: k_stress<R, D, 1><<<grid_for(r, blk), blk, 0, s>>>(b, C.P, C.g, Blim, C.w, r, C.sc); break;
+        switch (C.kvar & 3) {
+            case 1: k_stress<R, D, 1><<<grid_for(r, blk), blk, 0, s>>>(b, C.P, C.g, Blim, C.w, r, C.sc); break;
+            case 2: k_stress<R, D, 7><<<grid_for(r, blk), blk, 0, s>>>(b, C.P, C.g, Blim, C.w, r, C.sc); break;
+            case 3: k_stress<R, D, 8><<<grid_for(r, blk), blk, 0, s>>>(b, C.P, C.g, Blim, C.w, r, C.sc); break;
+            default: k_stress<R, D, 6><<<grid_for(r, blk), blk, 0, s>>>(b, C.P, C.g, Blim, C.w, r, C.sc); break;
         }
     };
     f(8, [&] { stress(std::integral_constant<int, 0>()); });
     f(9, [&] { stress(std::integral_constant<int, 1>()); });
     if (!C.P.do25D) f(10, [&] { stress(std::integral_constant<int, 2>()); });
     f(11, [&] { k_update_faces<R><<<grid_for(all, blk), blk, 0, s>>>(b, C.P, S, O, C.w, C.sc); });
-    f(12, [&] { k_update_cells<R><<<grid_for(cells, blk), blk, 0, s>>>(b, C.P, C.g, S, O, C.w, C.sc, C.gamma, C.gm1); });
+    f(12, [&] {
+        if (C.kvar & 4)
+            k_update_cells<R, 8><<<grid_for(cells, blk), blk, 0, s>>>(b, C.P, C.g, S, O, C.w, C.sc, C.gamma, C.gm1);
+        else
+            k_update_cells<R, 1><<<grid_for(cells, blk), blk, 0, s>>>(b, C.P, C.g, S, O, C.w, C.sc, C.gamma, C.gm1);
+    });
     f(13, [&] { k_dt_finalize<<<1, 1, 0, s>>>(C.sc); });
-    f(14, [&] { k_bc<R><<<grid_for(all, blk), blk, 0, s>>>(b, C.P, C.g, O, C.sc, 0); });
+    const Shell sh = make_shell(b);
+    const long nsh = sh.nA + sh.nB + sh.nC;
+    f(14, [&] { k_bc<R><<<(unsigned)((nsh + 255) / 256), 256, 0, s>>>(b, C.P, C.g, O, C.sc, 0, sh); });
 }
 
 template <class R> void launch_step(const Ctx<R>& C, int cur, cudaStream_t s) {
@@ -974,7 +1043,9 @@ template <class R> void launch_init(const Ctx<R>& C, int cur, cudaStream_t s) {
     const Range cells{0, b.Ni - 1, 0, b.Nj - 1, 0, b.Nk - 1};
     const StateBuf<R> S = C.st[cur], O = C.st[1 - cur];
     if (C.P.doMHD) k_bfield_all<R><<<grid_for(cells, blk), blk, 0, s>>>(b, C.g, S);
-    k_bc<R><<<grid_for(all, blk), blk, 0, s>>>(b, C.P, C.g, S, C.sc, 1);
+    const Shell sh = make_shell(b);
+    const long nsh = sh.nA + sh.nB + sh.nC;
+    k_bc<R><<<(unsigned)((nsh + 255) / 256), 256, 0, s>>>(b, C.P, C.g, S, C.sc, 1, sh);
     cudaMemcpyAsync(O.Gas, S.Gas, 5 * b.fs * sizeof(R), cudaMemcpyDeviceToDevice, s);
     cudaMemcpyAsync(O.mf, S.mf, 3 * b.fs * sizeof(R), cudaMemcpyDeviceToDevice, s);
     cudaMemcpyAsync(O.B, S.B, 3 * b.fs * sizeof(R), cudaMemcpyDeviceToDevice, s);
