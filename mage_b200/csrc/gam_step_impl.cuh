@@ -948,9 +948,9 @@ template <class R, class F> void for_each_kernel(const Ctx<R>& C, int cur, cudaS
     const dim3 pblk(32, 8, 1);
     f(1, [&] {
         if (C.kvar & 8)
-            k_predict<R, 4><<<grid_for(all, pblk), pblk, 0, s>>>(b, C.P, C.g, S, O, C.w, C.sc);
-        else
             k_predict<R, 1><<<grid_for(all, pblk), pblk, 0, s>>>(b, C.P, C.g, S, O, C.w, C.sc);
+        else
+            k_predict<R, 4><<<grid_for(all, pblk), pblk, 0, s>>>(b, C.P, C.g, S, O, C.w, C.sc);
     });
     if (C.P.doMHD) {
         const Range mf[3] = {{0, b.Ni - 1, G, G + b.Njp, 0, b.Nk - 1},
@@ -984,9 +984,9 @@ template <class R, class F> void for_each_kernel(const Ctx<R>& C, int cur, cudaS
     f(11, [&] { k_update_faces<R><<<grid_for(all, blk), blk, 0, s>>>(b, C.P, S, O, C.w, C.sc); });
     f(12, [&] {
         if (C.kvar & 4)
-            k_update_cells<R, 8><<<grid_for(cells, blk), blk, 0, s>>>(b, C.P, C.g, S, O, C.w, C.sc, C.gamma, C.gm1);
-        else
             k_update_cells<R, 1><<<grid_for(cells, blk), blk, 0, s>>>(b, C.P, C.g, S, O, C.w, C.sc, C.gamma, C.gm1);
+        else
+            k_update_cells<R, 8><<<grid_for(cells, blk), blk, 0, s>>>(b, C.P, C.g, S, O, C.w, C.sc, C.gamma, C.gm1);
     });
     f(13, [&] { k_dt_finalize<<<1, 1, 0, s>>>(C.sc); });
     const Shell sh = make_shell(b);

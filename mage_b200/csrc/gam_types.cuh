@@ -62,5 +62,5 @@ template <class R> struct Ctx {
     Work<R> w;
     GamScalars* sc;
     double gamma, gm1;
-    int kvar;  // launch-configuration variant (occupancy tuning; 0 = default)
+    int kvar;  // launch-configuration variant for tuning runs (GAM_KVAR); 0 = the tuned default
 };
