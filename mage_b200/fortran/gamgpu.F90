@@ -1,0 +1,111 @@
+! ISO_C_BINDING interface of libgamgpu.so (include/gamgpu.h) for the Fortran
+! driver of GAMERA. The host arrays are the driver's own State_T / Grid_T
+! allocatables, passed with c_loc: column-major, ghosts included, no copies.
+!
+! Usage in gamApp_T%AdvanceModel (gamtypessub.F90): see INTEGRATION.md.
+module gamgpu
+    use, intrinsic :: iso_c_binding
+    implicit none
+
+    integer(c_int), parameter :: GAM_OK = 0, GAM_EINVAL = 1, GAM_EBADDIM = 2, GAM_ECUDA = 3, &
+                                 GAM_EDT_BAD = 4, GAM_EDT_DISASTER = 5, GAM_ESTATE = 6, GAM_EHOOK = 7
+    integer(c_int), parameter :: GAM_BC_PERIODIC = 0, GAM_BC_NONE = 1
+    integer(c_int), parameter :: GAM_RECON_8CENT = 0, GAM_RECON_7UP = 1
+    integer(c_int), parameter :: GAM_FP64 = 0, GAM_FP32 = 1
+
+    type, bind(C) :: gam_params
+        integer(c_int32_t) :: Nip, Njp, Nkp, nG
+        real(c_double) :: gamma, CFL, pdmb, Vd0, cHogH, cHogM, dFloor, pFloor
+        real(c_double) :: tFin, dt0, limDT0, fixedTimestep
+        integer(c_int32_t) :: rmeth, doLFMLim, doMHD, doBackground, do25D, precision, strict
+        integer(c_int32_t) :: bc(6)
+    end type gam_params
+
+    interface
+        integer(c_int) function gam_default_params(p, Nip, Njp, Nkp) bind(C, name="gam_default_params")
+            import :: c_int, c_int32_t, gam_params
+            type(gam_params), intent(out) :: p
+            integer(c_int32_t), value :: Nip, Njp, Nkp
+        end function
+        integer(c_int) function gam_create(p, h) bind(C, name="gam_create")
+            import :: c_int, c_ptr, gam_params
+            type(gam_params), intent(in) :: p
+            type(c_ptr), intent(out) :: h
+        end function
+        integer(c_int) function gam_destroy(h) bind(C, name="gam_destroy")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h
+        end function
+        type(c_ptr) function gam_last_error(h) bind(C, name="gam_last_error")
+            import :: c_ptr
+            type(c_ptr), value :: h
+        end function
+        integer(c_int) function gam_set_geometry(h, xyz) bind(C, name="gam_set_geometry")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h, xyz
+        end function
+        integer(c_int) function gam_set_geometry_arrays(h, face, xfc, Tf, volume, xyzcc, di, dj, dk, edge, Te, Teb) &
+                bind(C, name="gam_set_geometry_arrays")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h, face, xfc, Tf, volume, xyzcc, di, dj, dk, edge, Te, Teb
+        end function
+        integer(c_int) function gam_upload_state(h, Gas, magFlux, Bxyz, oGas, omagFlux, time, otime, dt, ts) &
+                bind(C, name="gam_upload_state")
+            import :: c_int, c_ptr, c_double, c_int32_t
+            type(c_ptr), value :: h, Gas, magFlux, Bxyz, oGas, omagFlux
+            real(c_double), value :: time, otime, dt
+            integer(c_int32_t), value :: ts
+        end function
+        integer(c_int) function gam_download_state(h, Gas, magFlux, Bxyz, oGas, omagFlux, time, otime, dt, ts) &
+                bind(C, name="gam_download_state")
+            import :: c_int, c_ptr, c_double, c_int32_t
+            type(c_ptr), value :: h, Gas, magFlux, Bxyz, oGas, omagFlux
+            real(c_double), intent(out) :: time, otime, dt
+            integer(c_int32_t), intent(out) :: ts
+        end function
+        integer(c_int) function gam_step(h, nsteps, dt, t) bind(C, name="gam_step")
+            import :: c_int, c_ptr, c_double, c_int32_t
+            type(c_ptr), value :: h
+            integer(c_int32_t), value :: nsteps
+            real(c_double), intent(out) :: dt, t
+        end function
+        integer(c_int) function gam_advance_model(h, dt, t) bind(C, name="gam_advance_model")
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: h
+            real(c_double), value :: dt
+            real(c_double), intent(out) :: t
+        end function
+        integer(c_int) function gam_calc_dt(h, dt) bind(C, name="gam_calc_dt")
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: h
+            real(c_double), intent(out) :: dt
+        end function
+        integer(c_int) function gam_divb(h, total) bind(C, name="gam_divb")
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: h
+            real(c_double), intent(out) :: total
+        end function
+        integer(c_int) function gam_totals(h, out) bind(C, name="gam_totals")
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: h
+            real(c_double), intent(out) :: out(5)
+        end function
+    end interface
+
+contains
+
+    !> Error text of the last failed call on h, as a Fortran string.
+    function gam_error_string(h) result(msg)
+        type(c_ptr), intent(in) :: h
+        character(len=256) :: msg
+        character(kind=c_char), pointer :: cs(:)
+        integer :: n
+        msg = ""
+        call c_f_pointer(gam_last_error(h), cs, [256])
+        do n = 1, 256
+            if (cs(n) == c_null_char) exit
+            msg(n:n) = cs(n)
+        enddo
+    end function gam_error_string
+
+end module gamgpu
