@@ -134,6 +134,25 @@ int gam_advance_model(gam_handle* h, double dt, double* t_out);
 int gam_init_orszag_tang(gam_handle* h);
 int gam_init_blast_wave(gam_handle* h, const double bw[9]);
 
+/* Conserved totals for callers that cannot allocate device memory.
+ * No counterpart in the reference. Some callers cannot call cudaMalloc while
+ * they run: their device memory belongs to another framework's pool, or they
+ * reserve everything at start-up because allocation synchronises the device
+ * and can fail once memory is fragmented. This entry point allocates nothing:
+ * it reads the caller's device arrays State%Gas (Fortran layout, ghosts
+ * included) and Grid%volume (cell-sized), enqueues the reduction on `stream`
+ * (a cudaStream_t; 0 = default stream) and writes the five volume-weighted
+ * totals (mass, momentum x/y/z, energy) to the caller's device buffer out[5].
+ * Its block partial sums live in a fixed file-scope device array of 320 KiB,
+ * held on every device that loads the library until the process exits, which
+ * limits a call to Nip*Njp*Nkp <= 67,108,864 active cells; larger grids are
+ * rejected with GAM_EINVAL and a message in err (errlen bytes, may be NULL).
+ * The first call on a device looks up that array's address (set-up): make it
+ * before any stream capture. All calls share the array: calls whose kernels
+ * overlap on the GPU (different streams or devices in flight at once) race. */
+int gam_totals_noalloc(const double* Gas, const double* volume, int32_t Nip, int32_t Njp, int32_t Nkp, double* out,
+                       void* stream, char* err, int32_t errlen);
+
 #ifdef __cplusplus
 }
 #endif

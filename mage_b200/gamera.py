@@ -51,7 +51,7 @@ EXPORTED = (
     "gam_default_params", "gam_create", "gam_destroy", "gam_last_error", "gam_set_geometry",
     "gam_set_geometry_arrays", "gam_get_geometry_arrays", "gam_upload_state", "gam_download_state", "gam_step",
     "gam_calc_dt", "gam_divb", "gam_totals", "gam_last_step_ms", "gam_advance_model", "gam_init_orszag_tang",
-    "gam_init_blast_wave", "gam_profile_step",
+    "gam_init_blast_wave", "gam_profile_step", "gam_totals_noalloc",
 )
 
 _lib = None
@@ -85,6 +85,8 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     L.gam_init_orszag_tang.argtypes = [C.c_void_p]
     L.gam_init_blast_wave.argtypes = [C.c_void_p, _dp]
     L.gam_profile_step.argtypes = [C.c_void_p, C.c_int32, _dp, C.c_int32]
+    L.gam_totals_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p,
+                                     C.c_void_p, C.c_char_p, C.c_int32]
     _lib = L
     return L
 
