@@ -2,7 +2,8 @@
  *
  * The entry points replace the CPU time step of the reference's GAMERA solver
  * (Kaiju/MAGE, Fortran) for a single-domain grid. Fortran callers bind them
- * with ISO_C_BINDING; Python binds them with ctypes.
+ * with ISO_C_BINDING (module gamgpu, mage_b200/fortran/gamgpu.F90); Python
+ * binds them with ctypes (mage_b200/gamera.py).
  *
  * Conventions
  *  - Every entry point returns an int status, GAM_OK (0) on success. On error
@@ -36,7 +37,11 @@ enum {
     GAM_EHOOK = 7          /* a Model%Hack* hook is set: not supported on the GPU */
 };
 
-enum { GAM_BC_PERIODIC = 0, GAM_BC_NONE = 1 };
+/* Boundary kinds (EnforceBCs, step.F90:17-55). Per side: INI periodic, none or
+ * GAM_BC_SPHIN (bcs.F90:934-957); OUTI periodic, none or GAM_BC_WIND (constant
+ * solar wind, apps/wind.F90:206-391); INJ/OUTJ periodic, none or
+ * GAM_BC_ZEROGRAD (bcs.F90:853-892); INK/OUTK periodic or none. */
+enum { GAM_BC_PERIODIC = 0, GAM_BC_NONE = 1, GAM_BC_ZEROGRAD = 2, GAM_BC_SPHIN = 3, GAM_BC_WIND = 4 };
 enum { GAM_RECON_8CENT = 0, GAM_RECON_7UP = 1 };
 enum { GAM_FP64 = 0, GAM_FP32 = 1 };
 
@@ -133,6 +138,36 @@ int gam_advance_model(gam_handle* h, double dt, double* t_out);
  *     bw = {x0, y0, z0, D0, P0, pRat, dRat, rC, B0}; needs gam_set_geometry. */
 int gam_init_orszag_tang(gam_handle* h);
 int gam_init_blast_wave(gam_handle* h, const double bw[9]);
+
+/* Background field (doBackground = 1; Grid_T fcB0, bFlux0, edgB0, B0, dpB0,
+ * gamtypes.F90:233-242). All five are cell-sized Fortran arrays with ghosts:
+ * fcB0(.., 3, 3) (component, face), bFlux0(.., 3), edgB0(.., 2, 3), B0(.., 3),
+ * dpB0(.., 3).
+ *   gam_set_background       : the driver's own arrays, as AddB0 left them
+ *                              (background.F90:20-167)
+ *   gam_get_background       : copy back (any pointer may be NULL)
+ *   gam_set_background_dipole: AddB0 on the device for the dipole field of
+ *                              moment (0, 0, M0) (msphutils.F90:534-551);
+ *                              needs gam_set_geometry */
+int gam_set_background(gam_handle* h, const double* fcB0, const double* bFlux0, const double* edgB0,
+                       const double* B0, const double* dpB0);
+int gam_get_background(gam_handle* h, double* fcB0, double* bFlux0, double* edgB0, double* B0, double* dpB0);
+int gam_set_background_dipole(gam_handle* h, double M0);
+
+/* Solar-wind state of the outer-I boundary (bc[1] = GAM_BC_WIND), constant in
+ * space and time: wind = {rho, P, Vx, Vy, Vz, Bx, By, Bz}. The blend weights
+ * (wgtWind, apps/wind.F90:180-203) and the wind face fluxes of the ghost
+ * layers are computed here once from the metric. Replaces the windBC_T set-up
+ * of the driver (apps/wind.F90:40-176) for a constant wind. */
+int gam_set_wind(gam_handle* h, const double wind[8]);
+
+/* Dipole-in-wind start: the wind state in every active cell with the density
+ * perturbed by amp*u (u uniform in [-1, 1), SplitMix64 of seed and the Fortran
+ * cell index), the wind's uniform field as face fluxes of A = (B x r)/2
+ * (VectorPot2Flux, gridutils.F90:193-237), then the initialisation order
+ * above. Sets the wind boundary state when bc[1] = GAM_BC_WIND. Needs
+ * gam_set_geometry, and the background field when doBackground. */
+int gam_init_dipole_wind(gam_handle* h, const double wind[8], uint64_t seed, double amp);
 
 /* Conserved totals for callers that cannot allocate device memory.
  * No counterpart in the reference. Some callers cannot call cudaMalloc while

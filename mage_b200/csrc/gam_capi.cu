@@ -36,6 +36,11 @@ void gam_geom_ic_ot(const GamBox& b, const double* xyzcc, const double* face, do
                     cudaStream_t s);
 void gam_geom_ic_bw(const GamBox& b, const double* xyz, const double* vol, double* Gas, double* mf, double* lA,
                     double gamma, const double* bw, bool doMHD, cudaStream_t s);
+void gam_geom_ic_wind(const GamBox& b, const double* xyz, double* Gas, double* mf, double* lA, double gamma,
+                      double dFloor, double pFloor, const double* wind, uint64_t seed, double amp, cudaStream_t s);
+void gam_geom_b0_dipole(const GamBox& b, const double* xyz, const double* face, const double* vol, const double* Te,
+                        double M0, double* fcB0, double* bFlux0, double* edgB0, double* B0, double* dpB0, double* fS,
+                        cudaStream_t s);
 // diagnostics (gam_diag.cu)
 void gam_diag_divb(const GamBox& b, const double* mf, double* partial, double* out, cudaStream_t s);
 void gam_diag_divb_f(const GamBox& b, const float* mf, double* partial, double* out, cudaStream_t s);
@@ -51,9 +56,17 @@ struct GeoD {
     double *vol, *xyzcc, *dl, *dijk, *face, *xfc, *Tf, *edge, *Te, *Teb, *xyz;
 };
 
+// background field (FP64 in both forms), present when doBackground
+struct BgD {
+    double *fcB0, *bFlux0, *edgB0, *B0, *dpB0;
+};
+
 struct gam_handle {
     gam_params p;
     GamBox b;
+    BgD bg{};
+    double* windTab = nullptr;  // device: wC, wF(3), sF(3) of the solar-wind BC
+    bool haveBg = false, haveWind = false;
     cudaStream_t s = nullptr;
     bool f32 = false;
     std::vector<void*> allocs;
@@ -151,7 +164,11 @@ template <class R> static int alloc_bulk(gam_handle* h, Ctx<R>& C) {
         C.g.edge = edge; C.g.Te = Te; C.g.Teb = Teb;
     }
 #undef A
-    C.g.fcB0 = C.g.bFlux0 = C.g.edgB0 = C.g.B0 = C.g.dpB0 = nullptr;
+    C.g.fcB0 = h->bg.fcB0;
+    C.g.bFlux0 = h->bg.bFlux0;
+    C.g.edgB0 = h->bg.edgB0;
+    C.g.B0 = h->bg.B0;
+    C.g.dpB0 = h->bg.dpB0;
     C.b = h->b;
     fill_dev_params(C.P, h->p);
     C.sc = h->sc;
@@ -177,13 +194,27 @@ extern "C" int gam_create(const gam_params* p, gam_handle** out) {
     if (p->Njp < 1 || p->Nkp < 1) return bad(GAM_EBADDIM, "Njp and Nkp must be >= 1");
     if (p->do25D && p->Nkp != 1) return bad(GAM_EBADDIM, "do25D needs Nkp == 1");
     if (!p->do25D && (p->Njp < 4 || p->Nkp < 4)) return bad(GAM_EBADDIM, "3-D grids need Njp, Nkp >= 4");
-    if (p->doBackground) return bad(GAM_EINVAL, "background field: use the dipole set-up entry points");
     if (p->precision != GAM_FP64 && p->precision != GAM_FP32) return bad(GAM_EINVAL, "unknown precision");
     if (p->precision == GAM_FP32 && p->strict) return bad(GAM_EINVAL, "strict applies to the FP64 form only");
-    for (int n = 0; n < 6; n++)
-        if (p->bc[n] != GAM_BC_PERIODIC && p->bc[n] != GAM_BC_NONE) return bad(GAM_EINVAL, "unsupported boundary kind");
+    {
+        // boundary kinds per side: inner I periodic/none/SphIn, outer I
+        // periodic/none/wind, J periodic/none/zero-gradient, K periodic/none
+        const int* c = p->bc;
+        auto in = [](int v, int a, int b2, int c2) { return v == a || v == b2 || v == c2; };
+        if (!in(c[0], GAM_BC_PERIODIC, GAM_BC_NONE, GAM_BC_SPHIN) || !in(c[1], GAM_BC_PERIODIC, GAM_BC_NONE, GAM_BC_WIND) ||
+            !in(c[2], GAM_BC_PERIODIC, GAM_BC_NONE, GAM_BC_ZEROGRAD) ||
+            !in(c[3], GAM_BC_PERIODIC, GAM_BC_NONE, GAM_BC_ZEROGRAD) || !in(c[4], GAM_BC_PERIODIC, GAM_BC_NONE, -1) ||
+            !in(c[5], GAM_BC_PERIODIC, GAM_BC_NONE, -1))
+            return bad(GAM_EINVAL, "unsupported boundary kind for this side");
+        for (int d = 0; d < 3; d++)
+            if ((c[2 * d] == GAM_BC_PERIODIC) != (c[2 * d + 1] == GAM_BC_PERIODIC))
+                return bad(GAM_EINVAL, "a periodic direction needs both sides periodic");
+        if (c[0] == GAM_BC_PERIODIC && (c[2] == GAM_BC_ZEROGRAD || c[3] == GAM_BC_ZEROGRAD))
+            return bad(GAM_EINVAL, "zero-gradient J with periodic I is not supported");
+    }
     if (p->do25D && (p->bc[4] != GAM_BC_PERIODIC || p->bc[5] != GAM_BC_PERIODIC))
         return bad(GAM_EINVAL, "do25D replicates k: the k boundaries must be periodic");
+    if (p->doBackground && !p->doMHD) return bad(GAM_EINVAL, "a background field needs doMHD");
     h->b = gam_make_box(p->Nip, p->Njp, p->Nkp);
     h->f32 = p->precision == GAM_FP32;
     if (cudaStreamCreateWithFlags(&h->s, cudaStreamNonBlocking) != cudaSuccess) return bad(GAM_ECUDA, "no CUDA device");
@@ -199,7 +230,14 @@ extern "C" int gam_create(const gam_params* p, gam_handle** out) {
     } while (0)
     AD(g.vol, 1); AD(g.xyzcc, 3); AD(g.dl, 1); AD(g.dijk, 3); AD(g.face, 3); AD(g.xfc, 9); AD(g.Tf, 27);
     AD(g.edge, 3); AD(g.Te, 27); AD(g.Teb, 12); AD(g.xyz, 3);
+    if (p->doBackground) {
+        AD(h->bg.fcB0, 9); AD(h->bg.bFlux0, 3); AD(h->bg.edgB0, 6); AD(h->bg.B0, 3); AD(h->bg.dpB0, 3);
+    }
 #undef AD
+    if (p->bc[1] == GAM_BC_WIND) {
+        h->windTab = dalloc<double>(h, 7L * 4 * (h->b.Nj + 1) * (h->b.Nk + 1), &e);
+        if (e != cudaSuccess) return bad(GAM_ECUDA, "cudaMalloc failed (wind tables)");
+    }
     // staging: the largest Fortran array passed through (Tf/Te: 27 face-sized comps)
     long nface = (long)(h->b.Ni + 1) * (h->b.Nj + 1) * (h->b.Nk + 1);
     h->staging = dalloc<double>(h, 27 * nface, &e);
@@ -449,6 +487,8 @@ extern "C" int gam_step(gam_handle* h, int32_t nsteps, double* dt, double* t) {
     if (!h || nsteps < 0) return GAM_EINVAL;
     if (!h->haveGeo) return fail(h, GAM_ESTATE, "gam_step before gam_set_geometry");
     if (!h->haveState) return fail(h, GAM_ESTATE, "gam_step before gam_upload_state");
+    if (h->p.doBackground && !h->haveBg) return fail(h, GAM_ESTATE, "doBackground: set the background field first");
+    if (h->p.bc[1] == GAM_BC_WIND && !h->haveWind) return fail(h, GAM_ESTATE, "wind boundary: call gam_set_wind first");
     int rc;
     if ((rc = ensure_graph(h, 0))) return rc;
     if ((rc = ensure_graph(h, 1))) return rc;
@@ -640,5 +680,162 @@ extern "C" int gam_init_blast_wave(gam_handle* h, const double* bw9) {
     double* lA = h->staging + 8 * h->b.fs;
     gam_geom_fill(Gas64, 8 * h->b.fs, 0.0, h->s);
     gam_geom_ic_bw(h->b, h->gd.xyz, h->gd.vol, Gas64, mf64, lA, h->p.gamma, bw9, h->p.doMHD != 0, h->s);
+    return init_common(h, Gas64, mf64);
+}
+
+// ------------------------------------------------------------ background field and solar wind
+static void drop_graphs(gam_handle* h) {
+    for (int q = 0; q < 2; q++)
+        if (h->graph[q]) {
+            cudaGraphExecDestroy(h->graph[q]);
+            h->graph[q] = nullptr;
+        }
+}
+
+extern "C" int gam_set_background(gam_handle* h, const double* fcB0, const double* bFlux0, const double* edgB0,
+                                  const double* B0, const double* dpB0) {
+    if (!h || !fcB0 || !bFlux0 || !edgB0 || !B0 || !dpB0) return GAM_EINVAL;
+    if (!h->p.doBackground) return fail(h, GAM_ESTATE, "the handle was created without doBackground");
+    int rc;
+    if ((rc = up_d(h, fcB0, h->bg.fcB0, false, 9))) return rc;
+    if ((rc = up_d(h, bFlux0, h->bg.bFlux0, false, 3))) return rc;
+    if ((rc = up_d(h, edgB0, h->bg.edgB0, false, 6))) return rc;
+    if ((rc = up_d(h, B0, h->bg.B0, false, 3))) return rc;
+    if ((rc = up_d(h, dpB0, h->bg.dpB0, false, 3))) return rc;
+    CK(h, cudaGetLastError());
+    CK(h, cudaStreamSynchronize(h->s));
+    h->haveBg = true;
+    return GAM_OK;
+}
+
+extern "C" int gam_get_background(gam_handle* h, double* fcB0, double* bFlux0, double* edgB0, double* B0,
+                                  double* dpB0) {
+    if (!h) return GAM_EINVAL;
+    if (!h->haveBg) return fail(h, GAM_ESTATE, "no background field set");
+    int rc = GAM_OK;
+    if (fcB0 && (rc = down_r<double>(h, h->bg.fcB0, fcB0, false, 9))) return rc;
+    if (bFlux0 && (rc = down_r<double>(h, h->bg.bFlux0, bFlux0, false, 3))) return rc;
+    if (edgB0 && (rc = down_r<double>(h, h->bg.edgB0, edgB0, false, 6))) return rc;
+    if (B0 && (rc = down_r<double>(h, h->bg.B0, B0, false, 3))) return rc;
+    if (dpB0 && (rc = down_r<double>(h, h->bg.dpB0, dpB0, false, 3))) return rc;
+    return GAM_OK;
+}
+
+extern "C" int gam_set_background_dipole(gam_handle* h, double M0) {
+    if (!h) return GAM_EINVAL;
+    if (!h->p.doBackground) return fail(h, GAM_ESTATE, "the handle was created without doBackground");
+    if (!h->haveXyz) return fail(h, GAM_ESTATE, "the dipole background integrates over cells: call gam_set_geometry first");
+    if (9 * h->b.fs > 27 * n_face(h->b)) return fail(h, GAM_EINVAL, "staging too small");
+    const GeoD& g = h->gd;
+    gam_geom_b0_dipole(h->b, g.xyz, g.face, g.vol, g.Te, M0, h->bg.fcB0, h->bg.bFlux0, h->bg.edgB0, h->bg.B0,
+                       h->bg.dpB0, h->staging, h->s);
+    CK(h, cudaGetLastError());
+    CK(h, cudaStreamSynchronize(h->s));
+    h->haveBg = true;
+    return GAM_OK;
+}
+
+// math.F90:332-343 normVec
+static void norm_vec(const double* a, double* out) {
+    double nA = sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+    for (int x = 0; x < 3; x++) out[x] = nA <= 1.0e-12 ? 0.0 : a[x] / nA;
+}
+// math.F90:97-111 RampDown
+static double ramp_down(double r, double rC, double lC) {
+    if (r <= rC) return 1.0;
+    if (r >= rC + lC) return 0.0;
+    double rScl = (r - rC) / lC;
+    double eArg = -1.0 / (1.0 - rScl * rScl);
+    return exp(eArg + 1.0);
+}
+// apps/wind.F90:180-203 wgtWind for a constant wind velocity V: 1 where the
+// point faces the wind, ramping to 0 over 90 degrees behind it
+static double wgt_wind(const double* V, const double* xyz) {
+    double nHat[3], vHat[3], mv[3];
+    norm_vec(xyz, nHat);
+    norm_vec(V, vHat);
+    for (int x = 0; x < 3; x++) mv[x] = -vHat[x];
+    double dTh = acos(mv[0] * nHat[0] + mv[1] * nHat[1] + mv[2] * nHat[2]) * 180.0 / 3.141592653589793;
+    return ramp_down(dTh, 90.0, 90.0);
+}
+
+// The wind blend weights and wind face fluxes of the 4 outer-I ghost layers,
+// from the FP64 metric (host libm acos/exp, like the CPU code).
+extern "C" int gam_set_wind(gam_handle* h, const double wind[8]) {
+    if (!h || !wind) return GAM_EINVAL;
+    if (h->p.bc[1] != GAM_BC_WIND) return fail(h, GAM_ESTATE, "the outer I boundary is not the solar wind");
+    if (!h->haveGeo) return fail(h, GAM_ESTATE, "set the geometry first");
+    const GamBox& b = h->b;
+    const int G = 4, i0 = G + b.Nip;  // slab i0 .. i0+4 (ghost cells i0..i0+3, faces up to i0+4)
+    const long nrow = (long)(b.Nj + 1) * (b.Nk + 1);
+    const long nw = 4 * nrow;
+    // components: xyzcc 3, xfc 9, Tf normals 9, face 3
+    std::vector<double> sl(24 * 5 * nrow);
+    auto slab = [&](const double* comp, int q) -> cudaError_t {
+        return cudaMemcpy2DAsync(sl.data() + (size_t)q * 5 * nrow, 5 * sizeof(double), comp + i0,
+                                 (size_t)b.sx * sizeof(double), 5 * sizeof(double), (size_t)nrow,
+                                 cudaMemcpyDeviceToHost, h->s);
+    };
+    const GeoD& g = h->gd;
+    const long fs = b.fs;
+    int q = 0;
+    for (int x = 0; x < 3; x++) CK(h, slab(g.xyzcc + x * fs, q++));
+    for (int x = 0; x < 9; x++) CK(h, slab(g.xfc + x * fs, q++));
+    for (int d = 0; d < 3; d++)
+        for (int x = 0; x < 3; x++) CK(h, slab(g.Tf + (x + 9 * d) * fs, q++));
+    for (int d = 0; d < 3; d++) CK(h, slab(g.face + d * fs, q++));
+    CK(h, cudaStreamSynchronize(h->s));
+    auto at = [&](int comp, long row, int o) { return sl[(size_t)comp * 5 * nrow + (size_t)row * 5 + o]; };
+    const double V[3] = {wind[2], wind[3], wind[4]}, Bsw[3] = {wind[5], wind[6], wind[7]};
+    std::vector<double> tab(7 * nw, 0.0);
+    double* wC = tab.data();
+    double* wF = tab.data() + nw;
+    double* sF = tab.data() + 4 * nw;
+    for (int kk = 0; kk <= b.Nk; kk++)
+        for (int jj = 0; jj <= b.Nj; jj++) {
+            const long row = jj + (long)(b.Nj + 1) * kk;
+            for (int n = 1; n <= 4; n++) {
+                const long wi = (n - 1) + 4 * row;
+                const int o = n - 1;  // ghost cell ig = i0 + n - 1
+                if (jj < b.Nj && kk < b.Nk) {
+                    double xc[3] = {at(0, row, o), at(1, row, o), at(2, row, o)};
+                    wC[wi] = wgt_wind(V, xc);
+                }
+                for (int d = 0; d < 3; d++) {
+                    const int oo = d == 0 ? o + 1 : o;  // I face ig+1; J, K faces of cell ig
+                    double xf[3] = {at(3 + 3 * d, row, oo), at(4 + 3 * d, row, oo), at(5 + 3 * d, row, oo)};
+                    double nH[3] = {at(12 + 3 * d, row, oo), at(13 + 3 * d, row, oo), at(14 + 3 * d, row, oo)};
+                    wF[d * nw + wi] = wgt_wind(V, xf);
+                    sF[d * nw + wi] = at(21 + d, row, oo) * (nH[0] * Bsw[0] + nH[1] * Bsw[1] + nH[2] * Bsw[2]);
+                }
+            }
+        }
+    CK(h, cudaMemcpyAsync(h->windTab, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice, h->s));
+    CK(h, cudaStreamSynchronize(h->s));
+    WindData W;
+    for (int v = 0; v < 8; v++) W.state[v] = wind[v];
+    W.wC = h->windTab;
+    W.wF = h->windTab + nw;
+    W.sF = h->windTab + 4 * nw;
+    W.nw = nw;
+    h->cd.P.wind = W;
+    h->cf.P.wind = W;
+    drop_graphs(h);
+    h->haveWind = true;
+    return GAM_OK;
+}
+
+extern "C" int gam_init_dipole_wind(gam_handle* h, const double wind[8], uint64_t seed, double amp) {
+    if (!h || !wind) return GAM_EINVAL;
+    if (!h->haveXyz) return fail(h, GAM_ESTATE, "the vector potential is integrated along edges: call gam_set_geometry first");
+    if (h->p.doBackground && !h->haveBg) return fail(h, GAM_ESTATE, "set the background field first");
+    if (11 * h->b.fs > 27 * n_face(h->b)) return fail(h, GAM_EINVAL, "staging too small");
+    int rc;
+    if (h->p.bc[1] == GAM_BC_WIND && (rc = gam_set_wind(h, wind))) return rc;
+    double* Gas64 = h->staging;
+    double* mf64 = h->staging + 5 * h->b.fs;
+    double* lA = h->staging + 8 * h->b.fs;
+    gam_geom_fill(Gas64, 8 * h->b.fs, 0.0, h->s);
+    gam_geom_ic_wind(h->b, h->gd.xyz, Gas64, mf64, lA, h->p.gamma, h->p.dFloor, h->p.pFloor, wind, seed, amp, h->s);
     return init_common(h, Gas64, mf64);
 }

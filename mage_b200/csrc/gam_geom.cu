@@ -393,21 +393,41 @@ __global__ void k_ic_bw_gas(GamBox b, const double* __restrict__ xyz, const doub
     Gas[3 * fs + c] = Mz;
     Gas[4 * fs + c] = IntE + KinE;
 }
-// VectorPot2Flux edge integrals of A = (0, bSclz x, bScl (y - x)) (gridutils.F90:193-237)
-__device__ __forceinline__ double edge_int_dot(const double* e1, const double* e2, double bScl, double bSclz) {
+// Vector potentials handed to VectorPot2Flux (gridutils.F90:193-237):
+// the blast wave's A = (0, bSclz x, bScl (y - x)) (prob.F90:252-262) and a
+// uniform field B as A = (B x r)/2.
+struct PotBW {
+    double bScl, bSclz;
+    __device__ void operator()(const double* p, double* A) const {
+        A[0] = 0.0;
+        A[1] = bSclz * p[0];
+        A[2] = bScl * (p[1] - p[0]);
+    }
+};
+struct PotUniform {
+    double B[3];
+    __device__ void operator()(const double* p, double* A) const {
+        A[0] = 0.5 * (B[1] * p[2] - B[2] * p[1]);
+        A[1] = 0.5 * (B[2] * p[0] - B[0] * p[2]);
+        A[2] = 0.5 * (B[0] * p[1] - B[1] * p[0]);
+    }
+};
+// GaussianEdgeIntegral (quadrature.F90:345-370) of A along e2 -> e1, dotted
+// with e1 - e2 (e1 the far corner)
+template <class Pot> __device__ __forceinline__ double edge_int_dot(const double* e1, const double* e2, const Pot& pot) {
     double dR2[3], xBar[3], eInt[3] = {0.0, 0.0, 0.0};
     for (int x = 0; x < 3; x++) { dR2[x] = 0.5 * (e2[x] - e1[x]); xBar[x] = 0.5 * (e2[x] + e1[x]); }
     for (int i = 0; i < 12; i++) {
-        double xp[3];
+        double xp[3], Ap[3];
         for (int x = 0; x < 3; x++) xp[x] = xBar[x] + c_gA[i] * dR2[x];
-        double Ap[3] = {0.0, bSclz * xp[0], bScl * (xp[1] - xp[0])};
+        pot(xp, Ap);
         for (int x = 0; x < 3; x++) eInt[x] = eInt[x] + 0.5 * c_gW[i] * Ap[x];
     }
-    double s = 0.0;  // dot_product(eInt, e1 - e2) with e1 the far corner
+    double s = 0.0;
     for (int x = 0; x < 3; x++) s += eInt[x] * (e1[x] - e2[x]);
     return s;
 }
-__global__ void k_ic_bw_lA(GamBox b, const double* __restrict__ xyz, double* lA, double bScl, double bSclz) {
+template <class Pot> __global__ void k_ic_lA(GamBox b, const double* __restrict__ xyz, double* lA, Pot pot) {
     int ii, jj, kk;
     if (!tid3(b.Ni - 1, b.Nj - 1, b.Nk - 1, ii, jj, kk)) return;
     double e0[3], eI[3], eJ[3], eK[3];
@@ -418,11 +438,11 @@ __global__ void k_ic_bw_lA(GamBox b, const double* __restrict__ xyz, double* lA,
         eK[x] = X(b, xyz, ii, jj, kk + 1, x);
     }
     const long c = lidx(b, ii, jj, kk);
-    lA[c] = edge_int_dot(eI, e0, bScl, bSclz);
-    lA[b.fs + c] = edge_int_dot(eJ, e0, bScl, bSclz);
-    lA[2 * b.fs + c] = edge_int_dot(eK, e0, bScl, bSclz);
+    lA[c] = edge_int_dot(eI, e0, pot);
+    lA[b.fs + c] = edge_int_dot(eJ, e0, pot);
+    lA[2 * b.fs + c] = edge_int_dot(eK, e0, pot);
 }
-__global__ void k_ic_bw_flux(GamBox b, const double* __restrict__ lA, double* mf) {
+__global__ void k_ic_flux(GamBox b, const double* __restrict__ lA, double* mf) {
     int ii, jj, kk;
     if (!tid3(b.Ni - 1, b.Nj - 1, b.Nk - 1, ii, jj, kk)) return;
     const long c = lidx(b, ii, jj, kk), fs = b.fs, sj = b.sx, sk = b.sk;
@@ -434,6 +454,158 @@ __global__ void k_ic_bw_flux(GamBox b, const double* __restrict__ lA, double* mf
     mf[2 * fs + c] = I[c] - I[c + sj] + J[c + 1] - J[c];
 }
 
+
+// Counter-based uniform deviate in [-1, 1): SplitMix64 (Steele, Lea, Flood
+// 2014) of seed and index; integer arithmetic, so host and device agree.
+__device__ __forceinline__ double rng_uniform(uint64_t seed, uint64_t idx) {
+    uint64_t z = seed * 0x9E3779B97F4A7C15ULL + idx + 0x632BE59BD9B4E019ULL;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    z = z ^ (z >> 31);
+    return (double)(z >> 11) * (1.0 / 9007199254740992.0) * 2.0 - 1.0;
+}
+// Dipole-in-wind start on the active cells: the wind state (rho, P, V) with
+// the density perturbed by amp*u, u keyed by the Fortran cell index
+// (i-isg) + Ni*((j-jsg) + Nj*(k-ksg)); CellP2C (gamutils.F90:362-383).
+__global__ void k_ic_wind_gas(GamBox b, double* Gas, double gamma, double dFloor, double pFloor, double rho, double P,
+                              double Vx, double Vy, double Vz, uint64_t seed, double amp) {
+    int a0, a1, a2;
+    const int G = GAM_NG;
+    if (!tid3(b.Nip, b.Njp, b.Nkp, a0, a1, a2)) return;
+    const int ii = G + a0, jj = G + a1, kk = G + a2;
+    const uint64_t idx = (uint64_t)ii + (uint64_t)b.Ni * ((uint64_t)jj + (uint64_t)b.Nj * (uint64_t)kk);
+    const double u = rng_uniform(seed, idx);
+    const double W0 = rho * (1.0 + amp * u);
+    const double D = W0 < dFloor ? dFloor : W0;
+    const double IntE = (P < pFloor ? pFloor : P) / (gamma - 1);
+    const double KinE = 0.5 * D * (Vx * Vx + Vy * Vy + Vz * Vz);
+    const long c = lidx(b, ii, jj, kk), fs = b.fs;
+    Gas[c] = D;
+    Gas[fs + c] = D * Vx;
+    Gas[2 * fs + c] = D * Vy;
+    Gas[3 * fs + c] = D * Vz;
+    Gas[4 * fs + c] = IntE + KinE;
+}
+
+// Dipole field of moment (0, 0, M0) (msphutils.F90:534-551)
+__device__ __forceinline__ void dipole(double M0, const double* r, double* B) {
+    const double rad = norm2s(r);
+    const double m[3] = {0.0, 0.0, M0};
+    const double d = m[0] * r[0] + m[1] * r[1] + m[2] * r[2];
+    const double p5 = pow(rad, 5.0), p3 = pow(rad, 3.0);
+    for (int x = 0; x < 3; x++) B[x] = 3 * d * r[x] / p5 - m[x] / p3;
+}
+// AddB0 face part (background.F90:60-95) on every ghosted cell and face
+// direction d: bFlux0 (GaussianFaceFlux, quadrature.F90:105-151), fcB0
+// (GaussianFaceIntegral / face area) and the face stress (GaussianFaceStress,
+// quadrature.F90:223-280); the three share the quadrature points.
+__global__ void k_b0_faces(GamBox b, const double* __restrict__ xyz, const double* __restrict__ face, double M0,
+                           double* bFlux0, double* fcB0, double* fS) {
+    int ii, jj, kk;
+    if (!tid3(b.Ni, b.Nj, b.Nk * 3, ii, jj, kk)) return;
+    const int d = kk % 3;
+    kk /= 3;
+    int a1[3] = {0, 0, 0}, a2[3] = {0, 0, 0};
+    if (d == 0) { a1[1] = 1; a2[2] = 1; }
+    else if (d == 1) { a1[2] = 1; a2[0] = 1; }
+    else { a1[0] = 1; a2[1] = 1; }
+    double f0[3], f1[3], f2[3], f3[3];
+    for (int x = 0; x < 3; x++) {
+        f0[x] = X(b, xyz, ii, jj, kk, x);
+        f1[x] = X(b, xyz, ii + a1[0], jj + a1[1], kk + a1[2], x);
+        f2[x] = X(b, xyz, ii + a2[0], jj + a2[1], kk + a2[2], x);
+        f3[x] = X(b, xyz, ii + a1[0] + a2[0], jj + a1[1] + a2[1], kk + a1[2] + a2[2], x);
+    }
+    double dx[3], dy[3], dz[3];
+    dx[0] = f1[0] - f0[0]; dx[1] = f2[0] - f0[0]; dx[2] = f3[0] + f0[0] - f2[0] - f1[0];
+    dy[0] = f1[1] - f0[1]; dy[1] = f2[1] - f0[1]; dy[2] = f3[1] + f0[1] - f2[1] - f1[1];
+    dz[0] = f1[2] - f0[2]; dz[1] = f2[2] - f0[2]; dz[2] = f3[2] + f0[2] - f2[2] - f1[2];
+    double flx = 0.0, fInt[3] = {0.0, 0.0, 0.0}, Mbb[3] = {0.0, 0.0, 0.0};
+    for (int i = 0; i < 12; i++)
+        for (int j = 0; j < 12; j++) {
+            double eta = 0.5 * (1 + c_gA[i]), psi = 0.5 * (1 + c_gA[j]);
+            double w = c_gW[i] * c_gW[j];
+            double p[3] = {f0[0] + dx[0] * eta + dx[1] * psi + dx[2] * eta * psi,
+                           f0[1] + dy[0] * eta + dy[1] * psi + dy[2] * eta * psi,
+                           f0[2] + dz[0] * eta + dz[1] * psi + dz[2] * eta * psi};
+            double B[3];
+            dipole(M0, p, B);
+            double etaV[3] = {dx[0] + dx[2] * psi, dy[0] + dy[2] * psi, dz[0] + dz[2] * psi};
+            double psiV[3] = {dx[1] + dx[2] * eta, dy[1] + dy[2] * eta, dz[1] + dz[2] * eta};
+            double c[3], dS[3];
+            cross3(etaV, psiV, c);
+            for (int x = 0; x < 3; x++) dS[x] = 0.25 * w * c[x];
+            flx = flx + (dS[0] * B[0] + dS[1] * B[1] + dS[2] * B[2]);
+            double area = 0.25 * norm2s(c) * w;
+            for (int x = 0; x < 3; x++) fInt[x] = fInt[x] + area * B[x];
+            double BB = B[0] * B[0] + B[1] * B[1] + B[2] * B[2];
+            double BdS = B[0] * dS[0] + B[1] * dS[1] + B[2] * dS[2];
+            for (int x = 0; x < 3; x++) Mbb[x] = Mbb[x] + 0.5 * BB * dS[x] - B[x] * BdS;
+        }
+    const long c = lidx(b, ii, jj, kk), fs = b.fs;
+    bFlux0[d * fs + c] = flx;
+    const double fA = face[d * fs + c];
+    for (int x = 0; x < 3; x++) fcB0[(x + 3 * d) * fs + c] = fInt[x] / fA;
+    for (int x = 0; x < 3; x++) fS[(x + 3 * d) * fs + c] = Mbb[x];
+}
+// AddB0 edge part (background.F90:97-131): GaussianEdgeIntegral of the dipole
+// along each edge projected on the edge's two tangents
+__global__ void k_b0_edges(GamBox b, const double* __restrict__ xyz, const double* __restrict__ Te, double M0,
+                           double* edgB0) {
+    int ii, jj, kk;
+    if (!tid3(b.Ni, b.Nj, b.Nk * 3, ii, jj, kk)) return;
+    const int d = kk % 3;
+    kk /= 3;
+    const int o[3] = {d == 0, d == 1, d == 2};
+    double e1[3], e2[3];
+    for (int x = 0; x < 3; x++) {
+        e1[x] = X(b, xyz, ii, jj, kk, x);
+        e2[x] = X(b, xyz, ii + o[0], jj + o[1], kk + o[2], x);
+    }
+    double dR2[3], xBar[3], eInt[3] = {0.0, 0.0, 0.0};
+    for (int x = 0; x < 3; x++) { dR2[x] = 0.5 * (e2[x] - e1[x]); xBar[x] = 0.5 * (e2[x] + e1[x]); }
+    for (int i = 0; i < 12; i++) {
+        double xp[3], Ap[3];
+        for (int x = 0; x < 3; x++) xp[x] = xBar[x] + c_gA[i] * dR2[x];
+        dipole(M0, xp, Ap);
+        for (int x = 0; x < 3; x++) eInt[x] = eInt[x] + 0.5 * c_gW[i] * Ap[x];
+    }
+    const long c = lidx(b, ii, jj, kk), fs = b.fs;
+    edgB0[(0 + 2 * d) * fs + c] = eInt[0] * Te[(3 + 9 * d) * fs + c] + eInt[1] * Te[(4 + 9 * d) * fs + c] +
+                                  eInt[2] * Te[(5 + 9 * d) * fs + c];
+    edgB0[(1 + 2 * d) * fs + c] = eInt[0] * Te[(6 + 9 * d) * fs + c] + eInt[1] * Te[(7 + 9 * d) * fs + c] +
+                                  eInt[2] * Te[(8 + 9 * d) * fs + c];
+}
+// AddB0 cell average (background.F90:133-150): GaussianVolumeIntegral / volume
+__global__ void k_b0_cells(GamBox b, const double* __restrict__ xyz, const double* __restrict__ vol, double M0,
+                           double* B0) {
+    int ii, jj, kk;
+    if (!tid3(b.Ni, b.Nj, b.Nk, ii, jj, kk)) return;
+    double C[8][3];
+    cell_corners(b, xyz, ii, jj, kk, C);
+    double I[3] = {0.0, 0.0, 0.0};
+    for (int i = 0; i < 12; i++)
+        for (int j = 0; j < 12; j++)
+            for (int k = 0; k < 12; k++) {
+                double xp[3], wg, A[3];
+                gauss_point(C, i, j, k, xp, wg);
+                dipole(M0, xp, A);
+                for (int x = 0; x < 3; x++) I[x] = I[x] + wg * A[x];
+            }
+    const long c = lidx(b, ii, jj, kk), fs = b.fs;
+    for (int x = 0; x < 3; x++) B0[x * fs + c] = I[x] / vol[c];
+}
+// dpB0 = -div(face stress)/volume on the active cells (background.F90:152-165)
+__global__ void k_b0_dp(GamBox b, const double* __restrict__ fS, const double* __restrict__ vol, double* dpB0) {
+    int a0, a1, a2;
+    const int G = GAM_NG;
+    if (!tid3(b.Nip, b.Njp, b.Nkp, a0, a1, a2)) return;
+    const long c = lidx(b, G + a0, G + a1, G + a2), fs = b.fs;
+    for (int x = 0; x < 3; x++)
+        dpB0[x * fs + c] = -(fS[x * fs + c + 1] - fS[x * fs + c] + fS[(x + 3) * fs + c + b.sx] - fS[(x + 3) * fs + c] +
+                             fS[(x + 6) * fs + c + b.sk] - fS[(x + 6) * fs + c]) /
+                           vol[c];
+}
 }  // namespace gam_geom
 
 // ------------------------------------------------------------ host wrappers
@@ -510,6 +682,39 @@ void gam_geom_ic_bw(const GamBox& b, const double* xyz, const double* vol, doubl
     const double bScl = bw[8] / (double)sqrtf(2.0f);  // prob.F90:252 divides by the default-real sqrt(2.0)
     gam_geom_fill(lA, 3 * b.fs, 0.0, s);
     dim3 blk(32, 4, 1);
-    k_ic_bw_lA<<<g3(b.Ni - 1, b.Nj - 1, b.Nk - 1, blk), blk, 0, s>>>(b, xyz, lA, bScl, 0.0);
-    k_ic_bw_flux<<<g3(b.Ni - 1, b.Nj - 1, b.Nk - 1, blk), blk, 0, s>>>(b, lA, mf);
+    k_ic_lA<PotBW><<<g3(b.Ni - 1, b.Nj - 1, b.Nk - 1, blk), blk, 0, s>>>(b, xyz, lA, PotBW{bScl, 0.0});
+    k_ic_flux<<<g3(b.Ni - 1, b.Nj - 1, b.Nk - 1, blk), blk, 0, s>>>(b, lA, mf);
+}
+
+// Dipole-in-wind initial state: gas on the active cells, face fluxes of the
+// wind's uniform field (B x r)/2 through VectorPot2Flux. wind: rho, P, Vx, Vy,
+// Vz, Bx, By, Bz. lA: 3-component scratch.
+void gam_geom_ic_wind(const GamBox& b, const double* xyz, double* Gas, double* mf, double* lA, double gamma,
+                      double dFloor, double pFloor, const double* wind, uint64_t seed, double amp, cudaStream_t s) {
+    dim3 blk(32, 4, 1);
+    k_ic_wind_gas<<<g3(b.Nip, b.Njp, b.Nkp, blk), blk, 0, s>>>(b, Gas, gamma, dFloor, pFloor, wind[0], wind[1], wind[2],
+                                                              wind[3], wind[4], seed, amp);
+    gam_geom_fill(lA, 3 * b.fs, 0.0, s);
+    PotUniform pot{{wind[5], wind[6], wind[7]}};
+    k_ic_lA<PotUniform><<<g3(b.Ni - 1, b.Nj - 1, b.Nk - 1, blk), blk, 0, s>>>(b, xyz, lA, pot);
+    k_ic_flux<<<g3(b.Ni - 1, b.Nj - 1, b.Nk - 1, blk), blk, 0, s>>>(b, lA, mf);
+}
+// AddB0 for the dipole (background.F90:20-167): fills the five background
+// arrays (zeroed first) on the ghosted cell range; fS: 9-component scratch.
+void gam_geom_b0_dipole(const GamBox& b, const double* xyz, const double* face, const double* vol, const double* Te,
+                        double M0, double* fcB0, double* bFlux0, double* edgB0, double* B0, double* dpB0, double* fS,
+                        cudaStream_t s) {
+    const long fs = b.fs;
+    gam_geom_fill(fcB0, 9 * fs, 0.0, s);
+    gam_geom_fill(bFlux0, 3 * fs, 0.0, s);
+    gam_geom_fill(edgB0, 6 * fs, 0.0, s);
+    gam_geom_fill(B0, 3 * fs, 0.0, s);
+    gam_geom_fill(dpB0, 3 * fs, 0.0, s);
+    gam_geom_fill(fS, 9 * fs, 0.0, s);
+    dim3 blk(32, 4, 1);
+    k_b0_faces<<<g3(b.Ni, b.Nj, 3 * b.Nk, blk), blk, 0, s>>>(b, xyz, face, M0, bFlux0, fcB0, fS);
+    k_b0_edges<<<g3(b.Ni, b.Nj, 3 * b.Nk, blk), blk, 0, s>>>(b, xyz, Te, M0, edgB0);
+    dim3 blkv(64, 1, 1);
+    k_b0_cells<<<g3(b.Ni, b.Nj, b.Nk, blkv), blkv, 0, s>>>(b, xyz, vol, M0, B0);
+    k_b0_dp<<<g3(b.Nip, b.Njp, b.Nkp, blk), blk, 0, s>>>(b, fS, vol, dpB0);
 }

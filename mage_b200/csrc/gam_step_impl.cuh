@@ -742,33 +742,201 @@ __global__ void k_dt_finalize(GamScalars* sc) {
     else if (isBad) { sc->status = 4; sc->halted = 1; }
 }
 
-// Source index of a ghost value under the composed boundary maps of one
-// direction. n = number of active cells; face = this index is a face normal
-// to this direction (gets the upper-face offset rule of periodic_o*, bcs.F90).
-__device__ __forceinline__ int bc_map(int x, int n, int kind_lo, int kind_hi, bool normalFace, bool do25D) {
+// Boundary kinds: 0 periodic, 1 none, 2 zero-gradient, 3 inner sphere,
+// 4 solar wind (include/gamgpu.h).
+enum { BCK_PERIODIC = 0, BCK_NONE = 1, BCK_ZEROGRAD = 2, BCK_SPHIN = 3, BCK_WIND = 4 };
+
+// Gather maps of the boundary conditions that copy values (bcs.F90:279-450
+// periodic, :799-892 zero-gradient, :934-957 SphIn). x is the box index along
+// the BC's direction, n the active count, normal = the value sits on a face
+// normal to that direction. Returns the source index (x when untouched).
+__device__ __forceinline__ int bmap_lo(int kind, int x, int n) {
     const int G = GAM_NG;
-    if (do25D) {  // periodic_*bcK with Model%do25D: replicate ks (bcs.F90:387-394, 423-429)
-        if (x >= G - 4 && x < G) return G;
-        if (x > G && x <= G + 4) return G;
+    if (x >= G) return x;
+    if (kind == BCK_PERIODIC) return x + n;
+    if (kind == BCK_ZEROGRAD || kind == BCK_SPHIN) return G;
+    return x;
+}
+__device__ __forceinline__ int bmap_hi(int kind, int x, int n, bool normal) {
+    const int G = GAM_NG;
+    if (normal) {
+        if (x < G + n + 1 || x > G + n + 4) return x;
+        if (kind == BCK_PERIODIC) return x - n;
+        if (kind == BCK_ZEROGRAD) return G + n;  // magFlux(je+n+1,JDIR) = magFlux(je+1,JDIR)
         return x;
     }
-    if (x < G) return kind_lo == 0 ? x + n : x;
-    if (normalFace) {
-        if (x >= G + n + 1 && x <= G + n + 4) return kind_hi == 0 ? x - n : x;
-        return x;
-    }
-    if (x >= G + n && x <= G + n + 3) return kind_hi == 0 ? x - n : x;
+    if (x < G + n || x > G + n + 3) return x;
+    if (kind == BCK_PERIODIC) return x - n;
+    if (kind == BCK_ZEROGRAD) return G + n - 1;
+    return x;
+}
+// do25D periodic k: every ghost slab copies ks (bcs.F90:387-394, 423-429)
+__device__ __forceinline__ int bmap_25d(int x) {
+    const int G = GAM_NG;
+    if ((x >= G - 4 && x < G) || (x > G && x <= G + 4)) return G;
     return x;
 }
 
-// EnforceBCs for periodic / no-op boundaries as one gather, followed by the
-// final bFlux2Fld of every cell whose value or faces it changed.
-// copyB: fill ghost Bxyz by the same gather instead of recomputing it (the
-// initial EnforceBCs of CalcGridInfo, init.F90:226-238, has no bFlux2Fld after it).
-// The boundary fill only touches indices outside the deep interior
-// [G+1, G+N-2]^3 (ghost cells/faces and the cells whose faces they are):
-// the launch enumerates that shell. Per dimension, the "outer" indices are
-// [0, G] and [G+N-1, Nmax]; all of [0, Nmax] when the interior is empty.
+// Source of value (ii,jj,kk) of component comp (-1 cell, 0..2 face normal)
+// after the K, then J, then I boundary conditions that are gathers (the
+// reference applies INI, OUTI, INJ, OUTJ, INK, OUTK in that order, so a value
+// ends up copied from the I-map of the J-map of the K-map of its index). Each
+// map applies only over its loop ranges: periodic over the whole box,
+// zero-gradient and SphIn over cell ranges of the other two indices. The
+// non-periodic I sides (SphIn, wind) were applied before, in place. withB:
+// follow only the BCs that also copy Bxyz (periodic; zero-gradient does not).
+template <class R>
+__device__ __forceinline__ void bc_source(const GamBox& b, const DevParams<R>& P, int comp, bool withB, int& ii,
+                                          int& jj, int& kk) {
+    if (P.do25D)
+        kk = bmap_25d(kk);
+    else if (P.bc[4] == BCK_PERIODIC) {
+        kk = bmap_lo(BCK_PERIODIC, kk, b.Nkp);
+        kk = bmap_hi(BCK_PERIODIC, kk, b.Nkp, comp == 2);
+    }
+    if (P.bc[2] == BCK_PERIODIC || (!withB && ii < b.Ni && kk < b.Nk)) {
+        jj = bmap_lo(P.bc[2], jj, b.Njp);
+        jj = bmap_hi(P.bc[3], jj, b.Njp, comp == 1);
+    }
+    if (P.bc[0] == BCK_PERIODIC) {
+        ii = bmap_lo(BCK_PERIODIC, ii, b.Nip);
+        ii = bmap_hi(BCK_PERIODIC, ii, b.Nip, comp == 0);
+    }
+}
+
+// norm2 as gfortran evaluates it (scaled sum of squares)
+__device__ __forceinline__ double norm2s3(const double* a) {
+    double scale = 1.0, res = 0.0;
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+        if (a[q] != 0.0) {
+            double ax = fabs(a[q]);
+            if (scale < ax) {
+                double val = scale / ax;
+                res = 1.0 + res * val * val;
+                scale = ax;
+            } else {
+                double val = ax / scale;
+                res += val * val;
+            }
+        }
+    }
+    return scale * sqrt(res);
+}
+
+// The non-periodic I boundaries, in place: the SphIn copy on the inner side
+// (bcs.F90:934-957) and the solar-wind blend on the outer side
+// (apps/wind.F90:206-300), for ghost layer n = 1..4 of every (j, k).
+template <class R>
+__global__ void __launch_bounds__(256) k_bc_iside(GamBox b, DevParams<R> P, Geo<R> g, StateBuf<R> s,
+                                                  const GamScalars* sc) {
+    if (sc->halted) return;
+    const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    const int n = 1 + (int)(t & 3);
+    const long q = t >> 2;
+    const int jj = (int)(q % (b.Nj + 1)), kk = (int)(q / (b.Nj + 1));
+    if (kk > b.Nk) return;
+    const long fs = b.fs;
+    const int G = GAM_NG;
+    const bool cellJK = jj < b.Nj && kk < b.Nk;
+    if (P.bc[0] == BCK_SPHIN && cellJK) {
+        const long dst = lidx(b, G - n, jj, kk), src = lidx(b, G, jj, kk);
+#pragma unroll
+        for (int v = 0; v < 5; v++) s.Gas[v * fs + dst] = s.Gas[v * fs + src];
+#pragma unroll
+        for (int x = 0; x < 3; x++) s.mf[x * fs + dst] = s.mf[x * fs + src];
+#pragma unroll
+        for (int x = 0; x < 3; x++) s.B[x * fs + dst] = s.B[x * fs + src];
+    }
+    if (P.bc[1] != BCK_WIND) return;
+    const WindData& W = P.wind;
+    const long wi = (n - 1) + 4 * (jj + (long)(b.Nj + 1) * kk);
+    const int ig = G + b.Nip - 1 + n, ip = G + b.Nip - 1;
+    if (cellJK) {
+        const double MinMach = 1.0;
+        const double wSW = W.wC[wi], wMHD = 1.0 - wSW;
+        R gW_sw[5] = {(R)0, (R)0, (R)0, (R)0, (R)0}, gW_in[5] = {(R)0, (R)0, (R)0, (R)0, (R)0};
+        if (wSW > TINY) {
+            gW_sw[0] = (R)W.state[0];
+            gW_sw[4] = (R)W.state[1];
+            gW_sw[1] = (R)W.state[2];
+            gW_sw[2] = (R)W.state[3];
+            gW_sw[3] = (R)W.state[4];
+        }
+        if (wMHD > TINY) {
+            const long cp = lidx(b, ip, jj, kk);
+            R gCon[5], Bin[3];
+#pragma unroll
+            for (int v = 0; v < 5; v++) gCon[v] = s.Gas[v * fs + cp];
+#pragma unroll
+            for (int x = 0; x < 3; x++) Bin[x] = s.B[x * fs + cp];
+            cell_c2p(P, gCon, gW_in);
+            // Con2Fast (gamutils.F90:255-269) with CellPress2Cs (:238-253)
+            R rho = rmax(gCon[0], P.dFloor);
+            R Vx = gCon[1] / rho, Vy = gCon[2] / rho, Vz = gCon[3] / rho;
+            R KinE = (R)0.5 * rho * (Vx * Vx + Vy * Vy + Vz * Vz);
+            R Pr = rmax(P.gm1 * (gCon[4] - KinE), P.pFloor);
+            R Cs = Mth<R>::sqrt_(P.gamma * Pr / rho);
+            double Bd[3] = {(double)Bin[0], (double)Bin[1], (double)Bin[2]};
+            R MagB = (R)norm2s3(Bd);
+            R Va = MagB / Mth<R>::sqrt_(gCon[0]);
+            R Cx = Mth<R>::sqrt_(Cs * Cs + Va * Va);
+            const long cf = lidx(b, ip + 1, jj, kk);
+            R nH[3] = {g.Tf[0 * fs + cf], g.Tf[1 * fs + cf], g.Tf[2 * fs + cf]};
+            R V[3] = {gW_in[1], gW_in[2], gW_in[3]};
+            R dn = V[0] * nH[0] + V[1] * nH[1] + V[2] * nH[2];
+            if (dn < (R)MinMach * Cx) {
+#pragma unroll
+                for (int x = 0; x < 3; x++) V[x] = V[x] - dn * nH[x] + (R)MinMach * Cx * nH[x];
+            }
+            gW_in[1] = V[0];
+            gW_in[2] = V[1];
+            gW_in[3] = V[2];
+        }
+        R gW[5], gC[5];
+#pragma unroll
+        for (int v = 0; v < 5; v++) gW[v] = (R)wSW * gW_sw[v] + (R)wMHD * gW_in[v];
+        cell_p2c(P, gW, gC);
+        const long cg = lidx(b, ig, jj, kk);
+#pragma unroll
+        for (int v = 0; v < 5; v++) s.Gas[v * fs + cg] = gC[v];
+    }
+    // face fluxes: I face ig+1, J and K faces of cell ig
+    {
+        const double w = W.wF[wi];
+        const long cI = lidx(b, ig + 1, jj, kk), cin = lidx(b, ip + 1, jj, kk);
+        s.mf[cI] = (R)w * (R)W.sF[wi] + ((R)1 - (R)w) * s.mf[cin];
+    }
+#pragma unroll
+    for (int d = 1; d < 3; d++) {
+        const double w = W.wF[d * W.nw + wi];
+        const long cg = lidx(b, ig, jj, kk), cin = lidx(b, ip, jj, kk);
+        s.mf[d * fs + cg] = (R)w * (R)W.sF[d * W.nw + wi] + ((R)1 - (R)w) * s.mf[d * fs + cin];
+    }
+}
+// Bxyz of the wind ghost cells from their new fluxes (apps/wind.F90:341-351)
+template <class R>
+__global__ void __launch_bounds__(256) k_bc_wind_b(GamBox b, Geo<R> g, StateBuf<R> s, const GamScalars* sc) {
+    if (sc->halted) return;
+    const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    const int n = 1 + (int)(t & 3);
+    const long q = t >> 2;
+    const int jj = (int)(q % b.Nj), kk = (int)(q / b.Nj);
+    if (kk >= b.Nk) return;
+    const long fs = b.fs;
+    const long c = lidx(b, GAM_NG + b.Nip - 1 + n, jj, kk);
+    R B[3];
+    cell_bxyz(b, g, c, s.mf[c], s.mf[c + 1], s.mf[fs + c], s.mf[fs + c + b.sx], s.mf[2 * fs + c], s.mf[2 * fs + c + b.sk], B);
+#pragma unroll
+    for (int x = 0; x < 3; x++) s.B[x * fs + c] = B[x];
+}
+
+// The gather boundary conditions (periodic, zero-gradient J) as one pass over
+// the ghost shell, then the final bFlux2Fld of every ghost cell and of every
+// cell whose faces changed. copyB: the initial EnforceBCs of CalcGridInfo
+// (init.F90:226-238), which copies Bxyz with the BCs instead of recomputing it.
+// The launch enumerates the shell outside the deep interior [G+1, G+N-2]^3;
+// per dimension the "outer" indices are [0, G] and [G+N-1, Nmax].
 struct Shell {
     int nx, ny, nz;         // face-box extents (Ni+1, Nj+1, Nk+1)
     int a[3], bnd[3];       // deep interior [a, bnd] per dimension (empty if bnd < a)
@@ -830,47 +998,43 @@ __global__ void __launch_bounds__(256) k_bc(GamBox b, DevParams<R> P, Geo<R> g, 
     if (!shell_ijk(sh, t, ii, jj, kk)) return;
     const long fs = b.fs;
     const long c = lidx(b, ii, jj, kk);
-    const bool k25 = P.do25D != 0;
     // faces
-    int fi[3], fj[3], fk[3];
 #pragma unroll
     for (int d = 0; d < 3; d++) {
-        fi[d] = bc_map(ii, b.Nip, P.bc[0], P.bc[1], d == 0, false);
-        fj[d] = bc_map(jj, b.Njp, P.bc[2], P.bc[3], d == 1, false);
-        fk[d] = k25 ? bc_map(kk, b.Nkp, 0, 0, d == 2, true) : bc_map(kk, b.Nkp, P.bc[4], P.bc[5], d == 2, false);
-        if (k25 && kk == b.Nk) fk[d] = kk;  // keg+1 is outside the replicated slices
-    }
-#pragma unroll
-    for (int d = 0; d < 3; d++) {
-        if (fi[d] != ii || fj[d] != jj || fk[d] != kk) s.mf[d * fs + c] = s.mf[d * fs + lidx(b, fi[d], fj[d], fk[d])];
+        int x = ii, y = jj, z = kk;
+        bc_source(b, P, d, false, x, y, z);
+        if (x != ii || y != jj || z != kk) s.mf[d * fs + c] = s.mf[d * fs + lidx(b, x, y, z)];
     }
     if (ii >= b.Ni || jj >= b.Nj || kk >= b.Nk) return;
     // cell
-    int ci = bc_map(ii, b.Nip, P.bc[0], P.bc[1], false, false);
-    int cj = bc_map(jj, b.Njp, P.bc[2], P.bc[3], false, false);
-    int ck = k25 ? bc_map(kk, b.Nkp, 0, 0, false, true) : bc_map(kk, b.Nkp, P.bc[4], P.bc[5], false, false);
-    const bool cellMapped = ci != ii || cj != jj || ck != kk;
-    if (cellMapped) {
-        long src = lidx(b, ci, cj, ck);
+    {
+        int x = ii, y = jj, z = kk;
+        bc_source(b, P, -1, false, x, y, z);
+        if (x != ii || y != jj || z != kk) {
+            const long src = lidx(b, x, y, z);
 #pragma unroll
-        for (int v = 0; v < 5; v++) s.Gas[v * fs + c] = s.Gas[v * fs + src];
+            for (int v = 0; v < 5; v++) s.Gas[v * fs + c] = s.Gas[v * fs + src];
+        }
         if (copyB) {
+            int xb = ii, yb = jj, zb = kk;
+            bc_source(b, P, -1, true, xb, yb, zb);
+            if (xb != ii || yb != jj || zb != kk) {
+                const long src = lidx(b, xb, yb, zb);
 #pragma unroll
-            for (int x = 0; x < 3; x++) s.B[x * fs + c] = s.B[x * fs + src];
+                for (int q = 0; q < 3; q++) s.B[q * fs + c] = s.B[q * fs + src];
+            }
         }
     }
     if (!P.doMHD || copyB) return;
     // the six faces of this cell after the boundary fill
-    auto srcf = [&](int d, int a, int bb, int cc) -> long {
-        int x = bc_map(a, b.Nip, P.bc[0], P.bc[1], d == 0, false);
-        int y = bc_map(bb, b.Njp, P.bc[2], P.bc[3], d == 1, false);
-        int z = k25 ? bc_map(cc, b.Nkp, 0, 0, d == 2, true) : bc_map(cc, b.Nkp, P.bc[4], P.bc[5], d == 2, false);
-        if (k25 && cc == b.Nk) z = cc;
+    auto srcf = [&](int d, int a0, int a1, int a2) -> long {
+        int x = a0, y = a1, z = a2;
+        bc_source(b, P, d, false, x, y, z);
         return lidx(b, x, y, z);
     };
-    long fI = srcf(0, ii, jj, kk), fIp = srcf(0, ii + 1, jj, kk);
-    long fJ = srcf(1, ii, jj, kk), fJp = srcf(1, ii, jj + 1, kk);
-    long fK = srcf(2, ii, jj, kk), fKp = srcf(2, ii, jj, kk + 1);
+    const long fI = srcf(0, ii, jj, kk), fIp = srcf(0, ii + 1, jj, kk);
+    const long fJ = srcf(1, ii, jj, kk), fJp = srcf(1, ii, jj + 1, kk);
+    const long fK = srcf(2, ii, jj, kk), fKp = srcf(2, ii, jj, kk + 1);
     const bool facesMapped = fI != c || fIp != c + 1 || fJ != c || fJp != c + b.sx || fK != c || fKp != c + b.sk;
     const int G = GAM_NG;
     const bool ghost = ii < G || ii >= G + b.Nip || jj < G || jj >= G + b.Njp || kk < G || kk >= G + b.Nkp;
@@ -879,6 +1043,25 @@ __global__ void __launch_bounds__(256) k_bc(GamBox b, DevParams<R> P, Geo<R> g, 
     cell_bxyz(b, g, c, s.mf[fI], s.mf[fIp], s.mf[fs + fJ], s.mf[fs + fJp], s.mf[2 * fs + fK], s.mf[2 * fs + fKp], B);
 #pragma unroll
     for (int x = 0; x < 3; x++) s.B[x * fs + c] = B[x];
+}
+
+// All boundary conditions of one EnforceBCs (+ final bFlux2Fld unless copyB).
+template <class R> void launch_bcs(const Ctx<R>& C, const StateBuf<R>& S, cudaStream_t s, int copyB) {
+    const GamBox& b = C.b;
+    const bool iside = C.P.bc[0] == BCK_SPHIN || C.P.bc[1] == BCK_WIND;
+    if (iside) {
+        const long n = 4L * (b.Nj + 1) * (b.Nk + 1);
+        k_bc_iside<R><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(b, C.P, C.g, S, C.sc);
+        // the wind's own Bxyz of its ghost cells matters only where no final
+        // bFlux2Fld follows (the initial fill); a step recomputes every ghost
+        if (C.P.bc[1] == BCK_WIND && copyB) {
+            const long m = 4L * b.Nj * b.Nk;
+            k_bc_wind_b<R><<<(unsigned)((m + 255) / 256), 256, 0, s>>>(b, C.g, S, C.sc);
+        }
+    }
+    const Shell sh = make_shell(b);
+    const long nsh = sh.nA + sh.nB + sh.nC;
+    k_bc<R><<<(unsigned)((nsh + 255) / 256), 256, 0, s>>>(b, C.P, C.g, S, C.sc, copyB, sh);
 }
 
 // CalcDT on a state without changing it (gam_calc_dt): min of CellDT over
@@ -989,9 +1172,7 @@ template <class R, class F> void for_each_kernel(const Ctx<R>& C, int cur, cudaS
             k_update_cells<R, 8><<<grid_for(cells, blk), blk, 0, s>>>(b, C.P, C.g, S, O, C.w, C.sc, C.gamma, C.gm1);
     });
     f(13, [&] { k_dt_finalize<<<1, 1, 0, s>>>(C.sc); });
-    const Shell sh = make_shell(b);
-    const long nsh = sh.nA + sh.nB + sh.nC;
-    f(14, [&] { k_bc<R><<<(unsigned)((nsh + 255) / 256), 256, 0, s>>>(b, C.P, C.g, O, C.sc, 0, sh); });
+    f(14, [&] { launch_bcs(C, O, s, 0); });
 }
 
 template <class R> void launch_step(const Ctx<R>& C, int cur, cudaStream_t s) {
@@ -1043,9 +1224,7 @@ template <class R> void launch_init(const Ctx<R>& C, int cur, cudaStream_t s) {
     const Range cells{0, b.Ni - 1, 0, b.Nj - 1, 0, b.Nk - 1};
     const StateBuf<R> S = C.st[cur], O = C.st[1 - cur];
     if (C.P.doMHD) k_bfield_all<R><<<grid_for(cells, blk), blk, 0, s>>>(b, C.g, S);
-    const Shell sh = make_shell(b);
-    const long nsh = sh.nA + sh.nB + sh.nC;
-    k_bc<R><<<(unsigned)((nsh + 255) / 256), 256, 0, s>>>(b, C.P, C.g, S, C.sc, 1, sh);
+    launch_bcs(C, S, s, 1);
     cudaMemcpyAsync(O.Gas, S.Gas, 5 * b.fs * sizeof(R), cudaMemcpyDeviceToDevice, s);
     cudaMemcpyAsync(O.mf, S.mf, 3 * b.fs * sizeof(R), cudaMemcpyDeviceToDevice, s);
     cudaMemcpyAsync(O.B, S.B, 3 * b.fs * sizeof(R), cudaMemcpyDeviceToDevice, s);

@@ -3,10 +3,24 @@
 #pragma once
 #include "gam_layout.cuh"
 
+// Solar-wind boundary data (apps/wind.F90:206-391) for a constant wind: the
+// blend weights and wind face fluxes depend only on the grid and the wind
+// direction, so they are computed once on the host (libm acos/exp, the same
+// expressions as wgtWind/RampDown) and stored for the 4 ghost layers:
+// entry (n-1) + 4*(j + (Nj+1)*k) for ghost layer n = 1..4.
+struct WindData {
+    double state[8];    // rho, P, Vx, Vy, Vz, Bx, By, Bz
+    const double* wC;   // weight at the ghost cell centre
+    const double* wF;   // 3 x: weight at the I face ie+n+1, J face and K face of the ghost cell
+    const double* sF;   // 3 x: wind flux through those faces
+    long nw;            // entries per array
+};
+
 template <class R> struct DevParams {
     R gamma, gm1, CFL, pdmb, Vd0, cHogH, dFloor, pFloor;
     int doMHD, doLFMLim, do25D, doBackground, up7;
     int bc[6];
+    WindData wind;
 };
 
 template <class R> struct Geo {  // Grid_T arrays on the device (gamtypes.F90:168-250)

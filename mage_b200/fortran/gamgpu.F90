@@ -2,14 +2,16 @@
 ! driver of GAMERA. The host arrays are the driver's own State_T / Grid_T
 ! allocatables, passed with c_loc: column-major, ghosts included, no copies.
 !
-! Usage in gamApp_T%AdvanceModel (gamtypessub.F90): see INTEGRATION.md.
+! Intended caller: gamApp_T%AdvanceModel (gamtypessub.F90:74-90), which uploads
+! State/oState, calls gam_advance_model and downloads the new State.
 module gamgpu
     use, intrinsic :: iso_c_binding
     implicit none
 
     integer(c_int), parameter :: GAM_OK = 0, GAM_EINVAL = 1, GAM_EBADDIM = 2, GAM_ECUDA = 3, &
                                  GAM_EDT_BAD = 4, GAM_EDT_DISASTER = 5, GAM_ESTATE = 6, GAM_EHOOK = 7
-    integer(c_int), parameter :: GAM_BC_PERIODIC = 0, GAM_BC_NONE = 1
+    integer(c_int), parameter :: GAM_BC_PERIODIC = 0, GAM_BC_NONE = 1, GAM_BC_ZEROGRAD = 2, GAM_BC_SPHIN = 3, &
+                                 GAM_BC_WIND = 4
     integer(c_int), parameter :: GAM_RECON_8CENT = 0, GAM_RECON_7UP = 1
     integer(c_int), parameter :: GAM_FP64 = 0, GAM_FP32 = 1
 
@@ -89,6 +91,31 @@ module gamgpu
             import :: c_int, c_ptr, c_double
             type(c_ptr), value :: h
             real(c_double), intent(out) :: out(5)
+        end function
+        integer(c_int) function gam_set_background(h, fcB0, bFlux0, edgB0, B0, dpB0) bind(C, name="gam_set_background")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h, fcB0, bFlux0, edgB0, B0, dpB0
+        end function
+        integer(c_int) function gam_get_background(h, fcB0, bFlux0, edgB0, B0, dpB0) bind(C, name="gam_get_background")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h, fcB0, bFlux0, edgB0, B0, dpB0
+        end function
+        integer(c_int) function gam_set_background_dipole(h, M0) bind(C, name="gam_set_background_dipole")
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: h
+            real(c_double), value :: M0
+        end function
+        integer(c_int) function gam_set_wind(h, wind) bind(C, name="gam_set_wind")
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: h
+            real(c_double), intent(in) :: wind(8)
+        end function
+        integer(c_int) function gam_init_dipole_wind(h, wind, seed, amp) bind(C, name="gam_init_dipole_wind")
+            import :: c_int, c_ptr, c_double, c_int64_t
+            type(c_ptr), value :: h
+            real(c_double), intent(in) :: wind(8)
+            integer(c_int64_t), value :: seed
+            real(c_double), value :: amp
         end function
     end interface
 

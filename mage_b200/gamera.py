@@ -22,7 +22,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libgamgpu.so")
 
 GAM_OK, GAM_EINVAL, GAM_EBADDIM, GAM_ECUDA, GAM_EDT_BAD, GAM_EDT_DISASTER, GAM_ESTATE, GAM_EHOOK = range(8)
-BC_PERIODIC, BC_NONE = 0, 1
+BC_PERIODIC, BC_NONE, BC_ZEROGRAD, BC_SPHIN, BC_WIND = 0, 1, 2, 3, 4
 RECON_8CENT, RECON_7UP = 0, 1
 FP64, FP32 = 0, 1
 
@@ -51,8 +51,13 @@ EXPORTED = (
     "gam_default_params", "gam_create", "gam_destroy", "gam_last_error", "gam_set_geometry",
     "gam_set_geometry_arrays", "gam_get_geometry_arrays", "gam_upload_state", "gam_download_state", "gam_step",
     "gam_calc_dt", "gam_divb", "gam_totals", "gam_last_step_ms", "gam_advance_model", "gam_init_orszag_tang",
-    "gam_init_blast_wave", "gam_profile_step", "gam_totals_noalloc",
+    "gam_init_blast_wave", "gam_profile_step", "gam_totals_noalloc", "gam_set_background", "gam_get_background",
+    "gam_set_background_dipole", "gam_set_wind", "gam_init_dipole_wind",
 )
+
+# Background-field arrays (Grid_T, gamtypes.F90:233-242): name, components;
+# all cell-sized with ghosts
+BACKGROUND_ARRAYS = (("fcB0", 9), ("bFlux0", 3), ("edgB0", 6), ("B0", 3), ("dpB0", 3))
 
 _lib = None
 _dp = C.POINTER(C.c_double)
@@ -85,6 +90,11 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     L.gam_init_orszag_tang.argtypes = [C.c_void_p]
     L.gam_init_blast_wave.argtypes = [C.c_void_p, _dp]
     L.gam_profile_step.argtypes = [C.c_void_p, C.c_int32, _dp, C.c_int32]
+    L.gam_set_background.argtypes = [C.c_void_p] + [_dp] * 5
+    L.gam_get_background.argtypes = [C.c_void_p] + [_dp] * 5
+    L.gam_set_background_dipole.argtypes = [C.c_void_p, C.c_double]
+    L.gam_set_wind.argtypes = [C.c_void_p, _dp]
+    L.gam_init_dipole_wind.argtypes = [C.c_void_p, _dp, C.c_uint64, C.c_double]
     L.gam_totals_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p,
                                      C.c_void_p, C.c_char_p, C.c_int32]
     _lib = L
@@ -231,6 +241,34 @@ class GameraGPU:
     def init_blast_wave(self, x0=0.5, y0=0.5, z0=0.5, D0=1.0, P0=0.1, pRat=100.0, dRat=1.0, rC=0.1, B0=1.0):
         bw = np.array([x0, y0, z0, D0, P0, pRat, dRat, rC, B0], dtype=np.float64)
         self._check(self.L.gam_init_blast_wave(self.h, _ptr(bw)))
+
+    # --- background field and solar wind --------------------------------------
+    def set_background(self, arrs: dict):
+        """Upload fcB0, bFlux0, edgB0, B0, dpB0 (Fortran layout, cell-sized)."""
+        keep = [np.ascontiguousarray(arrs[n], dtype=np.float64).reshape(self.shape("cell", nc))
+                for n, nc in BACKGROUND_ARRAYS]
+        self._check(self.L.gam_set_background(self.h, *[_ptr(a) for a in keep]))
+
+    def get_background(self) -> dict:
+        out = {n: np.zeros(self.shape("cell", nc)) for n, nc in BACKGROUND_ARRAYS}
+        self._check(self.L.gam_get_background(self.h, *[_ptr(out[n]) for n, _ in BACKGROUND_ARRAYS]))
+        return out
+
+    def set_background_dipole(self, M0: float):
+        """AddB0 on the device for the dipole of moment (0, 0, M0)."""
+        self._check(self.L.gam_set_background_dipole(self.h, float(M0)))
+
+    def set_wind(self, wind):
+        """Constant solar wind {rho, P, Vx, Vy, Vz, Bx, By, Bz} of the outer-I boundary."""
+        w = np.ascontiguousarray(wind, dtype=np.float64)
+        assert w.shape == (8,)
+        self._check(self.L.gam_set_wind(self.h, _ptr(w)))
+
+    def init_dipole_wind(self, wind, seed: int = 31337, amp: float = 0.01):
+        """Wind state with a seeded density perturbation and the wind's uniform field."""
+        w = np.ascontiguousarray(wind, dtype=np.float64)
+        assert w.shape == (8,)
+        self._check(self.L.gam_init_dipole_wind(self.h, _ptr(w), int(seed), float(amp)))
 
     # --- stepping -------------------------------------------------------------
     def step_gamera(self, n: int = 1):

@@ -48,3 +48,25 @@ def dims(xyz: np.ndarray):
     """(Nip, Njp, Nkp) of a corner array."""
     _, nk1, nj1, ni1 = xyz.shape
     return ni1 - 1 - 2 * NG, nj1 - 1 - 2 * NG, nk1 - 1 - 2 * NG
+
+
+def spherical_corners(Nr: int, Nth: int, Nph: int, r0: float = 2.0, r1: float = 30.0, th0: float = 0.05,
+                      th1: float = float(np.pi) - 0.05) -> np.ndarray:
+    """Spherical-polar corners: r log-spaced on [r0, r1], theta uniform on
+    [th0, th1], phi uniform on [0, 2 pi) (periodic), x = r sin(th) cos(ph),
+    y = r sin(th) sin(ph), z = r cos(th). Ghost corners continue the same
+    formulas (as genGridXML does for doSph, init.F90:668-690)."""
+    i = np.arange(1 - NG, Nr + NG + 2, dtype=np.float64)
+    j = np.arange(1 - NG, Nth + NG + 2, dtype=np.float64)
+    k = np.arange(1 - NG, Nph + NG + 2, dtype=np.float64)
+    r = r0 * (r1 / r0) ** ((i - 1.0) / Nr)
+    th = th0 + (th1 - th0) * (j - 1.0) / Nth
+    ph = 2.0 * np.pi * (k - 1.0) / Nph
+    R = r[None, None, :]
+    TH = th[None, :, None]
+    PH = ph[:, None, None]
+    xyz = np.empty((3, k.size, j.size, i.size), dtype=np.float64)
+    xyz[0] = R * np.sin(TH) * np.cos(PH)
+    xyz[1] = R * np.sin(TH) * np.sin(PH)
+    xyz[2] = R * np.cos(TH) * np.ones_like(PH)
+    return xyz

@@ -60,8 +60,8 @@ enum { XNQI = 0, YNQI, XNQJ, YNQJ };
 enum { LEFT = 0, RIGHT = 1 };
 static const int SgnLR[2] = {-1, 1};  // stress.F90:19
 
-// boundary kinds (a subset of bcs.F90)
-enum { BC_PERIODIC = 0, BC_NONE = 1 };
+// boundary kinds (a subset of bcs.F90 / apps/wind.F90)
+enum { BC_PERIODIC = 0, BC_NONE = 1, BC_ZEROGRAD = 2, BC_SPHIN = 3, BC_WIND = 4 };
 
 // interpolation weights, recon.F90:22-23,28-29
 static double interpWgt[8], interpWgt6[8], Up7C[7];
@@ -113,6 +113,8 @@ struct Params {  // mirrored by oracle/oracle.py (ctypes)
     double tFin, dt0, limDT0, fixedDT;
     int bc[6];
     int noMetric;  // 1: allocate the metric with its fill values only (arrays set by the caller)
+    double M0;           // dipole moment (code units) of the background field, m = (0,0,M0)
+    double wind[8];      // constant solar wind: rho, P, Vx, Vy, Vz, Bx, By, Bz (code units)
 };
 
 struct Model {
@@ -120,6 +122,8 @@ struct Model {
     double t = 0, tFin, dt = 0, dt0 = 0, limDT0;
     int ts = 0;
     bool fixedTimestep, doMHD, doLFMLim, do25D, doBackground, up7;
+    double M0 = 0.0;
+    double wind[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 };
 
 struct Grid {
@@ -931,11 +935,19 @@ static void periodic_obcK(const Model& M, const Grid& G, State& S) {
             }
 }
 // step.F90:17-55 EnforceBCs (single domain: every boundary is owned)
+static void SphIn(const Grid& G, State& S);
+static void zeroGrad_ibcJ(const Grid& G, State& S);
+static void zeroGrad_obcJ(const Grid& G, State& S);
+static void WindBC(const Model& M, const Grid& G, State& S);
 static void EnforceBCs(const Model& M, const Grid& G, State& S) {
     if (G.bc[0] == BC_PERIODIC) periodic_ibcI(G, S);
+    else if (G.bc[0] == BC_SPHIN) SphIn(G, S);
     if (G.bc[1] == BC_PERIODIC) periodic_obcI(G, S);
+    else if (G.bc[1] == BC_WIND) WindBC(M, G, S);
     if (G.bc[2] == BC_PERIODIC) periodic_ibcJ(G, S);
+    else if (G.bc[2] == BC_ZEROGRAD) zeroGrad_ibcJ(G, S);
     if (G.bc[3] == BC_PERIODIC) periodic_obcJ(G, S);
+    else if (G.bc[3] == BC_ZEROGRAD) zeroGrad_obcJ(G, S);
     if (G.bc[4] == BC_PERIODIC) periodic_ibcK(M, G, S);
     if (G.bc[5] == BC_PERIODIC) periodic_obcK(M, G, S);
 }
@@ -1273,44 +1285,8 @@ static void initOT2D(const Model& M, const Grid& G, State& S) {
             }
 }
 struct BWParams { double x0, y0, z0, D0, P0, pRat, dRat, rC, B0; };
-// prob.F90:190-298 initBW (doB0 = F, doBz = F), with gridutils.F90:144-189
-// GasIC2State and :193-237 VectorPot2Flux
-static void initBW(const Model& M, const Grid& G, State& S, const BWParams& bp) {
-    const double bScl = bp.B0 / (double)std::sqrt(2.0f);  // default-real sqrt(2.0)
-    const double bSclz = 0.0;
-    auto W = [&](double x, double y, double z, double* Wp) {
-        double R = std::sqrt((x - bp.x0) * (x - bp.x0) + (y - bp.y0) * (y - bp.y0) + (z - bp.z0) * (z - bp.z0));
-        double D = bp.D0, P = bp.P0;
-        if (R <= bp.rC) { D = bp.dRat * D; P = bp.pRat * P; }
-        Wp[0] = D; Wp[1] = 0.0; Wp[2] = 0.0; Wp[3] = 0.0; Wp[4] = P;
-    };
-#pragma omp parallel for collapse(2)
-    for (int k = G.ks; k <= G.ke; k++)
-        for (int j = G.js; j <= G.je; j++)
-            for (int i = G.is; i <= G.ie; i++) {
-                double xyzC[8][3], ijkW[5];
-                cellCoords(G, i, j, k, xyzC);
-                double dV = G.volume(i, j, k);
-                GaussianVolumeIntegral(xyzC, W, ijkW);
-                for (int v = 0; v < 5; v++) ijkW[v] = ijkW[v] / dV;
-                double D = ijkW[DEN];
-                double Mx = D * ijkW[VELX], My = D * ijkW[VELY], Mz = D * ijkW[VELZ];
-                double P = ijkW[PRESSURE];
-                double KinE = 0.5 * (Mx * Mx + My * My + Mz * Mz) / D;
-                double IntE = P / (M.gamma - 1.0);
-                S.Gas(i, j, k, DEN) = D;
-                S.Gas(i, j, k, MOMX) = Mx;
-                S.Gas(i, j, k, MOMY) = My;
-                S.Gas(i, j, k, MOMZ) = Mz;
-                S.Gas(i, j, k, ENERGY) = IntE + KinE;
-            }
-    if (!M.doMHD) return;
-    auto Axyz = [&](const double* p, double* A) {
-        A[0] = 0.0;
-        A[1] = bSclz * p[0];
-        A[2] = bScl * (p[1] - p[0]);
-    };
-    // quadrature.F90:345-370 GaussianEdgeIntegral(e1,e2)
+// gridutils.F90:193-237 VectorPot2Flux, with quadrature.F90:345-370 GaussianEdgeIntegral
+template <class Fn> static void VectorPot2Flux(const Grid& G, State& S, Fn Axyz) {
     auto edgeInt = [&](const double* e1, const double* e2, double* eInt) {
         double dR2[3], xBar[3];
         for (int x = 0; x < 3; x++) { dR2[x] = 0.5 * (e2[x] - e1[x]); xBar[x] = 0.5 * (e2[x] + e1[x]); }
@@ -1351,6 +1327,343 @@ static void initBW(const Model& M, const Grid& G, State& S, const BWParams& bp) 
                 S.magFlux(i, j, k, JDIR) =
                     -(lA(i, j, k, IDIR) - lA(i, j, k + 1, IDIR) + lA(i + 1, j, k, KDIR) - lA(i, j, k, KDIR));
                 S.magFlux(i, j, k, KDIR) = lA(i, j, k, IDIR) - lA(i, j + 1, k, IDIR) + lA(i + 1, j, k, JDIR) - lA(i, j, k, JDIR);
+            }
+}
+
+// Counter-based uniform deviate in [-1, 1) (SplitMix64 of seed and index).
+static inline double rng_uniform(uint64_t seed, uint64_t idx) {
+    uint64_t z = seed * 0x9E3779B97F4A7C15ULL + idx + 0x632BE59BD9B4E019ULL;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    z = z ^ (z >> 31);
+    return (double)(z >> 11) * (1.0 / 9007199254740992.0) * 2.0 - 1.0;
+}
+// Dipole-in-wind start: the constant wind state in every active cell with a
+// relative density perturbation amp*u (u from rng_uniform keyed by the
+// Fortran cell index), and the wind's uniform field as face fluxes of the
+// potential A = (B x r)/2. The dipole itself is the background field (AddB0).
+static void initDipoleWind(const Model& M, const Grid& G, State& S, uint64_t seed, double amp) {
+    const double* w = M.wind;
+#pragma omp parallel for collapse(2)
+    for (int k = G.ks; k <= G.ke; k++)
+        for (int j = G.js; j <= G.je; j++)
+            for (int i = G.is; i <= G.ie; i++) {
+                uint64_t idx = (uint64_t)(i - G.isg) + (uint64_t)G.Ni * ((uint64_t)(j - G.jsg) + (uint64_t)G.Nj * (uint64_t)(k - G.ksg));
+                double u = rng_uniform(seed, idx);
+                double W[5] = {w[0] * (1.0 + amp * u), w[2], w[3], w[4], w[1]};
+                double U[5];
+                CellP2C(M, W, U);
+                for (int v = 0; v < 5; v++) S.Gas(i, j, k, v) = U[v];
+            }
+    const double B[3] = {w[5], w[6], w[7]};
+    VectorPot2Flux(G, S, [&](const double* p, double* A) {
+        A[0] = 0.5 * (B[1] * p[2] - B[2] * p[1]);
+        A[1] = 0.5 * (B[2] * p[0] - B[0] * p[2]);
+        A[2] = 0.5 * (B[0] * p[1] - B[1] * p[0]);
+    });
+}
+
+// prob.F90:190-298 initBW (doB0 = F, doBz = F), with gridutils.F90:144-189
+// GasIC2State and :193-237 VectorPot2Flux
+static void initBW(const Model& M, const Grid& G, State& S, const BWParams& bp) {
+    const double bScl = bp.B0 / (double)std::sqrt(2.0f);  // default-real sqrt(2.0)
+    const double bSclz = 0.0;
+    auto W = [&](double x, double y, double z, double* Wp) {
+        double R = std::sqrt((x - bp.x0) * (x - bp.x0) + (y - bp.y0) * (y - bp.y0) + (z - bp.z0) * (z - bp.z0));
+        double D = bp.D0, P = bp.P0;
+        if (R <= bp.rC) { D = bp.dRat * D; P = bp.pRat * P; }
+        Wp[0] = D; Wp[1] = 0.0; Wp[2] = 0.0; Wp[3] = 0.0; Wp[4] = P;
+    };
+#pragma omp parallel for collapse(2)
+    for (int k = G.ks; k <= G.ke; k++)
+        for (int j = G.js; j <= G.je; j++)
+            for (int i = G.is; i <= G.ie; i++) {
+                double xyzC[8][3], ijkW[5];
+                cellCoords(G, i, j, k, xyzC);
+                double dV = G.volume(i, j, k);
+                GaussianVolumeIntegral(xyzC, W, ijkW);
+                for (int v = 0; v < 5; v++) ijkW[v] = ijkW[v] / dV;
+                double D = ijkW[DEN];
+                double Mx = D * ijkW[VELX], My = D * ijkW[VELY], Mz = D * ijkW[VELZ];
+                double P = ijkW[PRESSURE];
+                double KinE = 0.5 * (Mx * Mx + My * My + Mz * Mz) / D;
+                double IntE = P / (M.gamma - 1.0);
+                S.Gas(i, j, k, DEN) = D;
+                S.Gas(i, j, k, MOMX) = Mx;
+                S.Gas(i, j, k, MOMY) = My;
+                S.Gas(i, j, k, MOMZ) = Mz;
+                S.Gas(i, j, k, ENERGY) = IntE + KinE;
+            }
+    if (!M.doMHD) return;
+    VectorPot2Flux(G, S, [&](const double* p, double* A) {
+        A[0] = 0.0;
+        A[1] = bSclz * p[0];
+        A[2] = bScl * (p[1] - p[0]);
+    });
+}
+
+// ---------------------------------------------------------------- background field
+// msphutils.F90:534-551 Dipole, m = (0,0,M0)
+static void Dipole(double M0, const double* r, double* A) {
+    double rad = norm2s(r, 3);
+    double m[3] = {0.0, 0.0, M0};
+    double d = dot3(m, r);
+    double p5 = std::pow(rad, 5.0), p3 = std::pow(rad, 3.0);
+    for (int x = 0; x < 3; x++) A[x] = 3 * d * r[x] / p5 - m[x] / p3;
+}
+// quadrature.F90:105-151 GaussianFaceFlux
+template <class Fn>
+static double GaussianFaceFlux(const double* f0, const double* f1, const double* f2, const double* f3, Fn Axyz) {
+    double dx[3], dy[3], dz[3];
+    faceDeltas(f0, f1, f2, f3, dx, dy, dz);
+    double flx = 0.0;
+    for (int i = 0; i < 12; i++)
+        for (int j = 0; j < 12; j++) {
+            double eta = 0.5 * (1 + gA[i]), psi = 0.5 * (1 + gA[j]);
+            double w = gWgt[i] * gWgt[j];
+            double p[3] = {f0[0] + dx[0] * eta + dx[1] * psi + dx[2] * eta * psi,
+                           f0[1] + dy[0] * eta + dy[1] * psi + dy[2] * eta * psi,
+                           f0[2] + dz[0] * eta + dz[1] * psi + dz[2] * eta * psi};
+            double A[3];
+            Axyz(p, A);
+            double etaV[3] = {dx[0] + dx[2] * psi, dy[0] + dy[2] * psi, dz[0] + dz[2] * psi};
+            double psiV[3] = {dx[1] + dx[2] * eta, dy[1] + dy[2] * eta, dz[1] + dz[2] * eta};
+            double c[3], N[3];
+            cross(etaV, psiV, c);
+            for (int x = 0; x < 3; x++) N[x] = 0.25 * w * c[x];
+            flx = flx + dot3(N, A);
+        }
+    return flx;
+}
+// quadrature.F90:159-221 GaussianFaceIntegral (first moment only) and
+// :223-280 GaussianFaceStress, for a vector field
+template <class Fn>
+static void GaussianFaceIntStress(const double* f0, const double* f1, const double* f2, const double* f3, Fn Axyz,
+                                  double* fInt, double* Mbb) {
+    double dx[3], dy[3], dz[3];
+    faceDeltas(f0, f1, f2, f3, dx, dy, dz);
+    for (int x = 0; x < 3; x++) fInt[x] = Mbb[x] = 0.0;
+    for (int i = 0; i < 12; i++)
+        for (int j = 0; j < 12; j++) {
+            double eta = 0.5 * (1 + gA[i]), psi = 0.5 * (1 + gA[j]);
+            double w = gWgt[i] * gWgt[j];
+            double p[3] = {f0[0] + dx[0] * eta + dx[1] * psi + dx[2] * eta * psi,
+                           f0[1] + dy[0] * eta + dy[1] * psi + dy[2] * eta * psi,
+                           f0[2] + dz[0] * eta + dz[1] * psi + dz[2] * eta * psi};
+            double B[3];
+            Axyz(p, B);
+            double etaV[3] = {dx[0] + dx[2] * psi, dy[0] + dy[2] * psi, dz[0] + dz[2] * psi};
+            double psiV[3] = {dx[1] + dx[2] * eta, dy[1] + dy[2] * eta, dz[1] + dz[2] * eta};
+            double c[3], dS[3];
+            cross(etaV, psiV, c);
+            double area = 0.25 * norm2s(c, 3) * w;
+            for (int x = 0; x < 3; x++) fInt[x] = fInt[x] + area * B[x];
+            for (int x = 0; x < 3; x++) dS[x] = 0.25 * w * c[x];
+            double BB = dot3(B, B), BdS = dot3(B, dS);
+            for (int x = 0; x < 3; x++) Mbb[x] = Mbb[x] + 0.5 * BB * dS[x] - B[x] * BdS;
+        }
+}
+// quadrature.F90:345-370 GaussianEdgeIntegral
+template <class Fn>
+static void GaussianEdgeIntegral(const double* e1, const double* e2, Fn Axyz, double* eInt) {
+    double dR2[3], xBar[3];
+    for (int x = 0; x < 3; x++) { dR2[x] = 0.5 * (e2[x] - e1[x]); xBar[x] = 0.5 * (e2[x] + e1[x]); }
+    eInt[0] = eInt[1] = eInt[2] = 0.0;
+    for (int i = 0; i < 12; i++) {
+        double xp[3], Ap[3];
+        for (int x = 0; x < 3; x++) xp[x] = xBar[x] + gA[i] * dR2[x];
+        Axyz(xp, Ap);
+        for (int x = 0; x < 3; x++) eInt[x] = eInt[x] + 0.5 * gWgt[i] * Ap[x];
+    }
+}
+// background.F90:20-167 AddB0 for the dipole
+static void AddB0(const Model& M, Grid& G) {
+    G.cellArr(G.fcB0, 9);
+    G.cellArr(G.edgB0, 6);
+    G.cellArr(G.B0, 3);
+    G.cellArr(G.bFlux0, 3);
+    G.cellArr(G.dpB0, 3);
+    F4 fS;  // faceStress(i,j,k,d,x) at x + 3*d
+    G.cellArr(fS, 9);
+    const double M0 = M.M0;
+    auto B0f = [M0](const double* p, double* A) { Dipole(M0, p, A); };
+#pragma omp parallel for collapse(2)
+    for (int k = G.ksg; k <= G.keg; k++)
+        for (int j = G.jsg; j <= G.jeg; j++)
+            for (int i = G.isg; i <= G.ieg; i++) {
+                for (int d = 0; d < 3; d++) {
+                    double f0[3], f1[3], f2[3], f3[3], fInt[3], Mbb[3];
+                    faceCoords(G, i, j, k, d, f0, f1, f2, f3);
+                    G.bFlux0(i, j, k, d) = GaussianFaceFlux(f0, f1, f2, f3, B0f);
+                    GaussianFaceIntStress(f0, f1, f2, f3, B0f, fInt, Mbb);
+                    for (int x = 0; x < 3; x++) G.fcB0(i, j, k, x + 3 * d) = fInt[x] / G.face(i, j, k, d);
+                    for (int x = 0; x < 3; x++) fS(i, j, k, x + 3 * d) = Mbb[x];
+                }
+                for (int d = 0; d < 3; d++) {
+                    double e1[3], e2[3], eInt[3];
+                    int o[3] = {d == 0, d == 1, d == 2};
+                    for (int x = 0; x < 3; x++) {
+                        e1[x] = G.xyz(i, j, k, x);
+                        e2[x] = G.xyz(i + o[0], j + o[1], k + o[2], x);
+                    }
+                    GaussianEdgeIntegral(e1, e2, B0f, eInt);
+                    G.edgB0(i, j, k, 0 + 2 * d) = eInt[XDIR] * G.Te(i, j, k, TAN1X + 9 * d) +
+                                                  eInt[YDIR] * G.Te(i, j, k, TAN1Y + 9 * d) +
+                                                  eInt[ZDIR] * G.Te(i, j, k, TAN1Z + 9 * d);
+                    G.edgB0(i, j, k, 1 + 2 * d) = eInt[XDIR] * G.Te(i, j, k, TAN2X + 9 * d) +
+                                                  eInt[YDIR] * G.Te(i, j, k, TAN2Y + 9 * d) +
+                                                  eInt[ZDIR] * G.Te(i, j, k, TAN2Z + 9 * d);
+                }
+                double xyzC[8][3], ijkB[5];
+                cellCoords(G, i, j, k, xyzC);
+                GaussianVolumeIntegral(xyzC, [M0](double x, double y, double z, double* W) {
+                    double p[3] = {x, y, z}, A[3];
+                    Dipole(M0, p, A);
+                    W[0] = A[0]; W[1] = A[1]; W[2] = A[2]; W[3] = 0.0; W[4] = 0.0;
+                }, ijkB);
+                for (int x = 0; x < 3; x++) G.B0(i, j, k, x) = ijkB[x] / G.volume(i, j, k);
+            }
+#pragma omp parallel for collapse(2)
+    for (int k = G.ks; k <= G.ke; k++)
+        for (int j = G.js; j <= G.je; j++)
+            for (int i = G.is; i <= G.ie; i++)
+                for (int x = 0; x < 3; x++)
+                    G.dpB0(i, j, k, x) = -(fS(i + 1, j, k, x + 0) - fS(i, j, k, x + 0) + fS(i, j + 1, k, x + 3) -
+                                           fS(i, j, k, x + 3) + fS(i, j, k + 1, x + 6) - fS(i, j, k, x + 6)) /
+                                         G.volume(i, j, k);
+}
+
+// ---------------------------------------------------------------- more BCs
+// bcs.F90:934-957 SphIn
+static void SphIn(const Grid& G, State& S) {
+    for (int k = G.ksg; k <= G.keg; k++)
+        for (int j = G.jsg; j <= G.jeg; j++)
+            for (int n = 1; n <= 4; n++) {
+                int ig = G.is - n;
+                for (int v = 0; v < NVAR; v++) S.Gas(ig, j, k, v) = S.Gas(G.is, j, k, v);
+                for (int x = 0; x < 3; x++) S.magFlux(ig, j, k, x) = S.magFlux(G.is, j, k, x);
+                for (int x = 0; x < 3; x++) S.Bxyz(ig, j, k, x) = S.Bxyz(G.is, j, k, x);
+            }
+}
+// bcs.F90:853-892 zeroGrad_ibcJ / zeroGrad_obcJ
+static void zeroGrad_ibcJ(const Grid& G, State& S) {
+    for (int k = G.ksg; k <= G.keg; k++)
+        for (int n = 1; n <= 4; n++)
+            for (int i = G.isg; i <= G.ieg; i++) {
+                for (int v = 0; v < NVAR; v++) S.Gas(i, G.js - n, k, v) = S.Gas(i, G.js, k, v);
+                for (int x = 0; x < 3; x++) S.magFlux(i, G.js - n, k, x) = S.magFlux(i, G.js, k, x);
+            }
+}
+static void zeroGrad_obcJ(const Grid& G, State& S) {
+    for (int k = G.ksg; k <= G.keg; k++)
+        for (int n = 1; n <= 4; n++)
+            for (int i = G.isg; i <= G.ieg; i++) {
+                for (int v = 0; v < NVAR; v++) S.Gas(i, G.je + n, k, v) = S.Gas(i, G.je, k, v);
+                S.magFlux(i, G.je + n, k, IDIR) = S.magFlux(i, G.je, k, IDIR);
+                S.magFlux(i, G.je + n, k, KDIR) = S.magFlux(i, G.je, k, KDIR);
+                S.magFlux(i, G.je + n + 1, k, JDIR) = S.magFlux(i, G.je + 1, k, JDIR);
+            }
+}
+// math.F90:332-343 normVec
+static inline void normVec(const double* a, double* out) {
+    double nA = std::sqrt(dot3(a, a));
+    for (int x = 0; x < 3; x++) out[x] = nA <= TINY ? 0.0 : a[x] / nA;
+}
+// math.F90:97-111 RampDown
+static inline double RampDown(double r, double rC, double lC) {
+    if (r <= rC) return 1.0;
+    if (r >= rC + lC) return 0.0;
+    double rScl = (r - rC) / lC;
+    double eArg = -1.0 / (1.0 - rScl * rScl);
+    return std::exp(eArg + 1.0);
+}
+// apps/wind.F90:180-203 wgtWind for a constant wind velocity V
+static double wgtWind(const double* V, const double* xyz) {
+    double nHat[3], vHat[3], mv[3];
+    normVec(xyz, nHat);
+    normVec(V, vHat);
+    for (int x = 0; x < 3; x++) mv[x] = -vHat[x];
+    double dTh = std::acos(dot3(mv, nHat)) * 180.0 / PI;
+    return RampDown(dTh, 90.0, 90.0);
+}
+// gamutils.F90:238-253 CellPress2Cs and :255-269 Con2Fast (Boris off)
+static double Con2Fast(const Model& M, const double* gCon, const double* B) {
+    double rho = std::max(gCon[DEN], dFloor);
+    double Vx = gCon[MOMX] / rho, Vy = gCon[MOMY] / rho, Vz = gCon[MOMZ] / rho;
+    double KinE = 0.5 * rho * (Vx * Vx + Vy * Vy + Vz * Vz);
+    double P = std::max((M.gamma - 1) * (gCon[ENERGY] - KinE), pFloor);
+    double Cs = std::sqrt(M.gamma * P / rho);
+    double D = gCon[DEN];
+    double MagB = norm2s(B, 3);
+    double Va = MagB / std::sqrt(D);
+    return std::sqrt(Cs * Cs + Va * Va);
+}
+// apps/wind.F90:206-374 WindBC with a constant wind (GetWindAt is then
+// independent of position and time), single fluid, no ring
+static void WindBC(const Model& M, const Grid& G, State& S) {
+    const double MinMach = 1.0;
+    const double* w = M.wind;  // rho, P, V(3), B(3)
+    const double Vsw[3] = {w[2], w[3], w[4]}, Bsw[3] = {w[5], w[6], w[7]};
+    const int ip = G.ie;
+#pragma omp parallel for collapse(2)
+    for (int k = G.ksg; k <= G.keg + 1; k++)
+        for (int j = G.jsg; j <= G.jeg + 1; j++)
+            for (int n = 1; n <= 4; n++) {
+                const int ig = G.ie + n;
+                if (isCellCenterG(G, ig, j, k)) {
+                    double gW_sw[5] = {0, 0, 0, 0, 0}, gW_in[5] = {0, 0, 0, 0, 0};
+                    double xcc[3] = {G.xyzcc(ig, j, k, 0), G.xyzcc(ig, j, k, 1), G.xyzcc(ig, j, k, 2)};
+                    double wSW = wgtWind(Vsw, xcc);
+                    double wMHD = 1.0 - wSW;
+                    if (wSW > TINY) {
+                        gW_sw[DEN] = w[0];
+                        gW_sw[PRESSURE] = w[1];
+                        for (int x = 0; x < 3; x++) gW_sw[VELX + x] = Vsw[x];
+                    }
+                    if (wMHD > TINY) {
+                        double gCon[5], B_in[3];
+                        for (int v = 0; v < 5; v++) gCon[v] = S.Gas(ip, j, k, v);
+                        for (int x = 0; x < 3; x++) B_in[x] = S.Bxyz(ip, j, k, x);
+                        CellC2P(M, gCon, gW_in);
+                        double Cx = Con2Fast(M, gCon, B_in);
+                        double V[3] = {gW_in[VELX], gW_in[VELY], gW_in[VELZ]};
+                        double nHat[3] = {G.Tf(ip + 1, j, k, NORMX), G.Tf(ip + 1, j, k, NORMY), G.Tf(ip + 1, j, k, NORMZ)};
+                        if (dot3(V, nHat) < MinMach * Cx) {
+                            double dn = dot3(V, nHat);
+                            for (int x = 0; x < 3; x++) V[x] = V[x] - dn * nHat[x] + MinMach * Cx * nHat[x];
+                        }
+                        for (int x = 0; x < 3; x++) gW_in[VELX + x] = V[x];
+                    }
+                    double gW[5], gCon[5];
+                    for (int v = 0; v < 5; v++) gW[v] = wSW * gW_sw[v] + wMHD * gW_in[v];
+                    CellP2C(M, gW, gCon);
+                    for (int v = 0; v < 5; v++) S.Gas(ig, j, k, v) = gCon[v];
+                }
+                // face fluxes: I at ig+1, J and K at ig
+                {
+                    double xf[3] = {G.xfc(ig + 1, j, k, 0), G.xfc(ig + 1, j, k, 1), G.xfc(ig + 1, j, k, 2)};
+                    double wSW = wgtWind(Vsw, xf);
+                    double nH[3] = {G.Tf(ig + 1, j, k, NORMX), G.Tf(ig + 1, j, k, NORMY), G.Tf(ig + 1, j, k, NORMZ)};
+                    double swFlx = G.face(ig + 1, j, k, IDIR) * dot3(nH, Bsw);
+                    double inFlx = S.magFlux(ip + 1, j, k, IDIR);
+                    S.magFlux(ig + 1, j, k, IDIR) = wSW * swFlx + (1 - wSW) * inFlx;
+                }
+                for (int d = 1; d < 3; d++) {
+                    double xf[3] = {G.xfc(ig, j, k, 0 + 3 * d), G.xfc(ig, j, k, 1 + 3 * d), G.xfc(ig, j, k, 2 + 3 * d)};
+                    double wSW = wgtWind(Vsw, xf);
+                    double nH[3] = {G.Tf(ig, j, k, NORMX + 9 * d), G.Tf(ig, j, k, NORMY + 9 * d), G.Tf(ig, j, k, NORMZ + 9 * d)};
+                    double swFlx = G.face(ig, j, k, d) * dot3(nH, Bsw);
+                    double inFlx = S.magFlux(ip, j, k, d);
+                    S.magFlux(ig, j, k, d) = wSW * swFlx + (1 - wSW) * inFlx;
+                }
+            }
+#pragma omp parallel for collapse(2)
+    for (int k = G.ksg; k <= G.keg; k++)
+        for (int j = G.jsg; j <= G.jeg; j++)
+            for (int n = 1; n <= 4; n++) {
+                double B[3];
+                gamCellBxyz(G, S.magFlux, G.ie + n, j, k, B);
+                for (int x = 0; x < 3; x++) S.Bxyz(G.ie + n, j, k, x) = B[x];
             }
 }
 
@@ -1414,6 +1727,8 @@ void* orc_create(const Params* p, const double* xyz) {
     M.dt = M.fixedTimestep ? p->fixedDT : 0.0;
     M.doMHD = p->doMHD != 0; M.doLFMLim = p->doLFMLim != 0; M.do25D = p->do25D != 0;
     M.doBackground = p->doBackground != 0; M.up7 = p->up7 != 0;
+    M.M0 = p->M0;
+    for (int n = 0; n < 8; n++) M.wind[n] = p->wind[n];
     g_up7 = M.up7;
     pdmb = p->pdmb; dFloor = p->dFloor; pFloor = p->pFloor;
     G.Nip = p->Nip; G.Njp = p->Njp; G.Nkp = p->Nkp;
@@ -1430,6 +1745,7 @@ void* orc_create(const Params* p, const double* xyz) {
         G.faceArr(G.edge, 3, 1.0); G.faceArr(G.Te, 27); G.faceArr(G.Teb, 12, 1.0);
     } else {
         Corners2Grid(M, G);
+        if (M.doBackground) AddB0(M, G);
     }
     allocState(G, A->S);
     A->S.time = M.t;  // allocState sets State%time = Model%t (gamutils.F90:199)
@@ -1477,6 +1793,11 @@ double* orc_array(void* h, int which, long* n) {
         case 21: a = &A->dGasH; break;
         case 22: a = &A->dGasM; break;
         case 23: a = &A->G.xyz; break;
+        case 24: a = &A->G.fcB0; break;
+        case 25: a = &A->G.bFlux0; break;
+        case 26: a = &A->G.edgB0; break;
+        case 27: a = &A->G.B0; break;
+        case 28: a = &A->G.dpB0; break;
         default: *n = 0; return nullptr;
     }
     *n = (long)a->v.size();
@@ -1486,6 +1807,15 @@ double* orc_array(void* h, int which, long* n) {
 void orc_ic_ot(void* h) {
     App* A = (App*)h;
     initOT2D(A->M, A->G, A->S);
+}
+void orc_ic_dipole_wind(void* h, double amp, unsigned long long seed) {
+    App* A = (App*)h;
+    initDipoleWind(A->M, A->G, A->S, (uint64_t)seed, amp);
+}
+void orc_set_background_noalloc(void* h) {  // allocate the B0 arrays (caller fills them)
+    App* A = (App*)h;
+    A->G.cellArr(A->G.fcB0, 9); A->G.cellArr(A->G.edgB0, 6); A->G.cellArr(A->G.B0, 3);
+    A->G.cellArr(A->G.bFlux0, 3); A->G.cellArr(A->G.dpB0, 3);
 }
 void orc_ic_bw(void* h, const double* bwp) {
     App* A = (App*)h;

@@ -22,6 +22,9 @@ VARIANTS = ("strict", "gm", "fast")
 
 BC_PERIODIC = 0
 BC_NONE = 1
+BC_ZEROGRAD = 2
+BC_SPHIN = 3
+BC_WIND = 4
 
 
 def build(quiet: bool = True) -> None:
@@ -38,7 +41,7 @@ class _Params(C.Structure):
         ("gamma", C.c_double), ("CFL", C.c_double), ("pdmb", C.c_double), ("Vd0", C.c_double),
         ("cHogH", C.c_double), ("cHogM", C.c_double), ("dFloor", C.c_double), ("pFloor", C.c_double),
         ("tFin", C.c_double), ("dt0", C.c_double), ("limDT0", C.c_double), ("fixedDT", C.c_double),
-        ("bc", C.c_int * 6), ("noMetric", C.c_int),
+        ("bc", C.c_int * 6), ("noMetric", C.c_int), ("M0", C.c_double), ("wind", C.c_double * 8),
     ]
 
 
@@ -73,12 +76,16 @@ class OracleParams:
     fixedDT: float = 0.0
     bc: tuple = field(default_factory=lambda: (BC_PERIODIC,) * 6)
     noMetric: bool = False
+    M0: float = 0.0
+    wind: tuple = (0.0,) * 8
 
     def to_c(self) -> _Params:
         p = _Params()
         for f, _ in _Params._fields_:
             if f == "bc":
                 p.bc[:] = list(self.bc)
+            elif f == "wind":
+                p.wind[:] = list(self.wind)
             else:
                 setattr(p, f, getattr(self, f))
         return p
@@ -91,7 +98,9 @@ _ARR = {"Gas": (0, "cell", 5), "magFlux": (1, "face", 3), "Bxyz": (2, "cell", 3)
         "Tf": (12, "face", 27), "Te": (13, "face", 27), "Teb": (14, "face", 12),
         "face": (15, "face", 3), "edge": (16, "face", 3), "Efld": (17, "cell", 3),
         "hGas": (18, "cell", 5), "hmagFlux": (19, "face", 3), "hBxyz": (20, "cell", 3),
-        "dGasH": (21, "cell", 5), "dGasM": (22, "cell", 3), "xyz": (23, "face", 3)}
+        "dGasH": (21, "cell", 5), "dGasM": (22, "cell", 3), "xyz": (23, "face", 3),
+        "fcB0": (24, "cell", 9), "bFlux0": (25, "cell", 3), "edgB0": (26, "cell", 6), "B0": (27, "cell", 3),
+        "dpB0": (28, "cell", 3)}
 
 _libs: dict = {}
 
@@ -109,6 +118,8 @@ def lib(variant: str = "strict") -> C.CDLL:
         L.orc_array.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_long)]
         L.orc_ic_ot.argtypes = [C.c_void_p]
         L.orc_ic_bw.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+        L.orc_ic_dipole_wind.argtypes = [C.c_void_p, C.c_double, C.c_ulonglong]
+        L.orc_set_background_noalloc.argtypes = [C.c_void_p]
         L.orc_init_finish.argtypes = [C.c_void_p]
         L.orc_init_finish.restype = C.c_int
         L.orc_step.argtypes = [C.c_void_p, C.c_int]
@@ -164,6 +175,12 @@ class Oracle:
     def ic_blast_wave(self, x0=0.5, y0=0.5, z0=0.5, D0=1.0, P0=0.1, pRat=100.0, dRat=1.0, rC=0.1, B0=1.0):
         a = np.array([x0, y0, z0, D0, P0, pRat, dRat, rC, B0], dtype=np.float64)
         self.L.orc_ic_bw(self.h, _dptr(a))
+
+    def ic_dipole_wind(self, amp: float = 0.01, seed: int = 31337):
+        self.L.orc_ic_dipole_wind(self.h, amp, seed)
+
+    def alloc_background(self):
+        self.L.orc_set_background_noalloc(self.h)
 
     def init_finish(self) -> int:
         return self.L.orc_init_finish(self.h)
