@@ -35,11 +35,14 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 # Algorithmic bytes per cell-update (compulsory traffic of a fused step that
-# reads the metric once): 27 state values + 79 metric values, FP64 / FP32.
+# reads the metric once): 27 state values + 79 metric values, FP64 / FP32;
+# with a background field 24 more values, FP64 in both forms.
 BYTES_PER_CELL = {"f64": 8 * (27 + 79), "f32": 4 * (27 + 79)}
+BYTES_PER_CELL_B0 = {"f64": 8 * (27 + 79 + 24), "f32": 4 * (27 + 79) + 8 * 24}
 KERNELS_PER_STEP = 15  # begin, predict, 3x(mom2face, vxb), 3x stress, faces, cells, dt, bc
+DIPOLE_WORKLOAD, DIPOLE_STEPS = "dipole96", 500
 
-from mage_b200.workloads import WORKLOADS, corners  # noqa: E402
+from mage_b200.workloads import WORKLOADS, corners, make_app  # noqa: E402
 
 
 def env_rank():
@@ -196,6 +199,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp32", action="store_true")
+    ap.add_argument("--no-dipole", action="store_true", help="skip the dipole-in-wind FP64/FP32 section")
     ap.add_argument("--strict", action="store_true", help="time the FP64 kernels built without FMA contraction")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -210,7 +214,7 @@ def main():
         import torch.distributed as dist
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
-    from mage_b200.gamera import GameraGPU, GamParams, FP32
+    from mage_b200.gamera import FP32
 
     w = WORKLOADS[args.workload]
     N = w["N"]
@@ -218,13 +222,7 @@ def main():
     xyz = corners(w)
 
     def make(prec, strict=False):
-        g = GameraGPU(GamParams(*N, do25D=(N[2] == 1), precision=prec, strict=strict))
-        g.set_geometry(xyz)
-        if w["problem"] == "bw":
-            g.init_blast_wave()
-        else:
-            g.init_orszag_tang()
-        return g
+        return make_app(args.workload, prec, strict, xyz=xyz)
 
     def barrier():
         torch.cuda.synchronize()
@@ -304,11 +302,43 @@ def main():
                 for v, name in enumerate(("rho", "mx", "my", "mz", "energy")) if np.abs(A[v]).max() > 1e-8}
         fp32 = {"value": v32, "unit": "cell-updates/s", "ms_per_step": ms32 / args.steps, "speedup_vs_fp64": v32 / value,
                 "rel_l2_vs_fp64": errs, "error_after_steps": nerr,
-                "roofline_frac": (v32 / world) * BYTES_PER_CELL["f32"] / 1e9 / measured_peak()[0]}
+                "roofline_frac": (v32 / world) * (BYTES_PER_CELL_B0 if w["problem"] == "dipole" else BYTES_PER_CELL)["f32"]
+                / 1e9 / measured_peak()[0]}
         del g32, a, b
 
+    # ---- dipole in a solar wind (spherical grid, background field): FP64 and
+    # FP32 from the same start for DIPOLE_STEPS steps, throughput of the timed
+    # part and the FP32 error at the end
+    dip = None
+    if not args.no_dipole and w["problem"] != "dipole":
+        wd = WORKLOADS[DIPOLE_WORKLOAD]
+        Nd = wd["N"]
+        cd = Nd[0] * Nd[1] * Nd[2]
+        xyzd = corners(wd)
+        dip = {"workload": wd["desc"], "grid": list(Nd), "steps": DIPOLE_STEPS, "unit": "cell-updates/s"}
+        final = {}
+        for prec, name in ((0, "fp64"), (FP32, "fp32")):
+            gd = make_app(DIPOLE_WORKLOAD, prec, xyz=xyzd)
+            gd.step_gamera(args.warmup)
+            barrier()
+            gd.step_gamera(DIPOLE_STEPS - args.warmup)
+            msd = max_over_ranks(gd.last_step_ms())
+            vd = world * cd * (DIPOLE_STEPS - args.warmup) / (msd / 1e3)
+            bpc = BYTES_PER_CELL_B0["f64" if prec == 0 else "f32"]
+            dip[name] = {"value": vd, "ms_per_step": msd / (DIPOLE_STEPS - args.warmup), "bytes_per_cell_update": bpc,
+                         "roofline_frac": (vd / world) * bpc / 1e9 / measured_peak()[0]}
+            final[name] = gd.download_state(old=False)["Gas"][:, 4:-4, 4:-4, 4:-4]
+            del gd
+        dip["speedup_fp32_vs_fp64"] = dip["fp32"]["value"] / dip["fp64"]["value"]
+        A, B = final["fp64"], final["fp32"]
+        dip["rel_l2_fp32_vs_fp64"] = {name: float(np.linalg.norm(B[v] - A[v]) / np.linalg.norm(A[v]))
+                                      for v, name in enumerate(("rho", "mx", "my", "mz", "energy"))
+                                      if np.abs(A[v]).max() > 1e-8}
+        del final, A, B
+
     peak, peak_kind = measured_peak()
-    achieved = per_gpu * BYTES_PER_CELL["f64"] / 1e9
+    bpc = BYTES_PER_CELL_B0 if w["problem"] == "dipole" else BYTES_PER_CELL
+    achieved = per_gpu * bpc["f64"] / 1e9
     traffic = committed_traffic(args.workload, "f64")
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -324,7 +354,7 @@ def main():
                        "l2": "inputs larger than L2 (~13 GB of state, metric and work arrays per step)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
-                         "bytes_per_cell_update": BYTES_PER_CELL["f64"],
+                         "bytes_per_cell_update": bpc["f64"],
                          "traffic": None if traffic is None else traffic * cells,
                          "unit_of_launch": "one step (CUDA graph of the step's kernels) over the whole grid"},
             "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
@@ -332,6 +362,7 @@ def main():
                     "what": "per step: gam_upload_state (State+oState from pinned host memory), gam_step(1), "
                             "gam_download_state (new State to pinned host memory)"},
             "fp32": fp32,
+            "dipole": dip,
             "cpu_baseline": cpu,
             "clocks": clocks,
             "gpu_launches": KERNELS_PER_STEP * args.steps,
