@@ -1,0 +1,511 @@
+"""Differentiable stepGamera in PyTorch operations (FP64 or FP32, CPU or GPU).
+
+The same step as the CUDA kernels of ``csrc/gam_step_impl.cuh`` (periodic
+boundaries, no background field, 8CENT or 7UP reconstruction, LFM limiter,
+fixed dt), written as whole-array tensor expressions so that autograd gives its
+reverse mode. It is the gradient reference of the differentiation form and its
+first implementation: ``loss_and_grad`` runs N steps with sqrt(N)-style
+checkpointing (segments are recomputed during the reverse sweep).
+
+Arrays use the padded-box convention of the CUDA code without padding: every
+field is a tensor ``(nc, Nk+1, Nj+1, Ni+1)`` indexed ``[c, kk, jj, ii]`` with box
+index ``ii = i - isg`` (Ni = Nip + 8); cell fields leave the last slot of each
+axis unused. Routines and their reference (file:line):
+
+  predictor        Predictor / PredictCell / ExtrapAB2   mhdgroup.F90:444-615,709-717
+  mom2face, vxb    CalcElecField / Mom2Face / EdgeLRs     fields.F90:70-517
+  stress           Fluxes / GasKinFlux / MagKinFlux       stress.F90:204-599
+  recon            Cen8LRs / Up7LRs / pdmLR / PDM         recon.F90:125-301
+  update           applyUpdate / E2Flux / CellMaxwell     mhdgroup.F90:79-329, fields.F90:18-51
+  bcs              EnforceBCs (periodic) + bFlux2Fld      step.F90:17-55, bcs.F90:279-450
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+G = 4
+TINY = 1.0e-12
+PI = 3.141592653589793
+W8 = (-3.0 / 840.0, 29.0 / 840.0, -139.0 / 840.0, 533.0 / 840.0, 533.0 / 840.0, -139.0 / 840.0, 29.0 / 840.0,
+      -3.0 / 840.0)
+UP7 = (-3.0 / 420.0, 25.0 / 420.0, -101.0 / 420.0, 319.0 / 420.0, 214.0 / 420.0, -38.0 / 420.0, 4.0 / 420.0)
+
+
+@dataclass
+class DiffParams:
+    Nip: int
+    Njp: int
+    Nkp: int
+    gamma: float = 5.0 / 3.0
+    CFL: float = 0.3
+    pdmb: float = 0.75
+    Vd0: float = 0.5
+    cHogH: float = 0.25
+    dFloor: float = 1.0e-12
+    pFloor: float = 1.0e-12
+    up7: bool = False
+
+
+# ----------------------------------------------------------------- helpers
+def rmax(a, b):
+    """std::max: (a < b) ? b : a."""
+    return torch.where(a < b, b, a)
+
+
+def rmin(a, b):
+    """std::min: (b < a) ? b : a."""
+    return torch.where(b < a, b, a)
+
+
+def safe_sqrt(x):
+    """sqrt with a zero (sub)gradient at 0 instead of inf * 0."""
+    pos = x > 0
+    return torch.where(pos, torch.sqrt(torch.where(pos, x, torch.ones_like(x))), torch.zeros_like(x))
+
+
+def win(a, rng, off=(0, 0, 0)):
+    """a[..., k, j, i] over the inclusive box range rng = (i0, i1, j0, j1, k0, k1)
+    shifted by off = (di, dj, dk)."""
+    i0, i1, j0, j1, k0, k1 = rng
+    di, dj, dk = off
+    return a[..., k0 + dk:k1 + dk + 1, j0 + dj:j1 + dj + 1, i0 + di:i1 + di + 1]
+
+
+def unit(d, n):
+    o = [0, 0, 0]
+    o[d] = n
+    return tuple(o)
+
+
+def add(o1, o2):
+    return (o1[0] + o2[0], o1[1] + o2[1], o1[2] + o2[2])
+
+
+def put(base, rng, val):
+    """Copy of base with val written over the box range rng (autograd-safe)."""
+    out = base.clone()
+    i0, i1, j0, j1, k0, k1 = rng
+    out[..., k0:k1 + 1, j0:j1 + 1, i0:i1 + 1] = val
+    return out
+
+
+def central8(q):
+    s = torch.zeros_like(q[0])
+    for n in range(8):
+        s = s + W8[n] * q[n]
+    return s
+
+
+def pdm_lr(pdmb, v, Qi):
+    """pdmLR (recon.F90:231-272) on the 4-point limiter stencil v[0..3]."""
+    v0, v1, v2, v3 = v
+    maxV, minV = rmax(v1, v2), rmin(v1, v2)
+    vN = rmax(minV, rmin(Qi, maxV))
+    dv0, dv1, dv2 = pdmb * (v1 - v0), pdmb * (v2 - v1), pdmb * (v3 - v2)
+    one = torch.ones_like(vN)
+    s0, s1, s2 = torch.copysign(one, dv0), torch.copysign(one, dv1), torch.copysign(one, dv2)
+    q0, q1 = torch.abs(s0 + s1), torch.abs(s1 + s2)
+    dvL, dvR = vN - v1, v2 - vN
+    zero = torch.zeros_like(vN)
+    Ql = vN - s1 * rmax(zero, torch.abs(dvL) - q0 * torch.abs(dv0))
+    Qr = vN + s1 * rmax(zero, torch.abs(dvR) - q1 * torch.abs(dv2))
+    return Ql, Qr
+
+
+def pdm1(pdmb, q0, q1, q2, qI):
+    """PDM (recon.F90:275-301)."""
+    maxQ, minQ = rmax(q1, q2), rmin(q1, q2)
+    qN = rmax(minQ, rmin(qI, maxQ))
+    dq0, dq1 = pdmb * (q1 - q0), pdmb * (q2 - q1)
+    one = torch.ones_like(qN)
+    s0, s1 = torch.copysign(one, dq0), torch.copysign(one, dq1)
+    s01 = torch.abs(s0 + s1)
+    dqL = qN - q1
+    return qN - s1 * rmax(torch.zeros_like(qN), torch.abs(dqL) - s01 * torch.abs(dq0))
+
+
+def lrs_from_qdv(P: DiffParams, qdv, nq, Vi):
+    """Cen8LRs / Up7LRs on the volume-weighted stencil qdv[0..7] (cells -4..3),
+    limited by PDM on nq[0..3] (cells -2..1)."""
+    if not P.up7:
+        Qi = central8(qdv) / Vi
+        return pdm_lr(P.pdmb, nq, Qi)
+    a = qdv[0] * UP7[0]
+    for n in range(1, 7):
+        a = a + qdv[n] * UP7[n]
+    b = qdv[7] * UP7[0]
+    for n in range(1, 7):
+        b = b + qdv[7 - n] * UP7[n]
+    Ql, Qr = a / Vi, b / Vi
+    return pdm1(P.pdmb, nq[0], nq[1], nq[2], Ql), pdm1(P.pdmb, nq[3], nq[2], nq[1], Qr)
+
+
+def cell_c2p(P, U):
+    rho = U[0]
+    Vx, Vy, Vz = U[1] / rho, U[2] / rho, U[3] / rho
+    KinE = 0.5 * rho * (Vx * Vx + Vy * Vy + Vz * Vz)
+    return [rmax(rho, torch.full_like(rho, P.dFloor)), Vx, Vy, Vz,
+            rmax((P.gamma - 1) * (U[4] - KinE), torch.full_like(rho, P.pFloor))]
+
+
+def cell_p2c(P, W):
+    rho = rmax(W[0], torch.full_like(W[0], P.dFloor))
+    Vx, Vy, Vz = W[1], W[2], W[3]
+    IntE = rmax(W[4], torch.full_like(W[4], P.pFloor)) / (P.gamma - 1)
+    KinE = 0.5 * rho * (Vx * Vx + Vy * Vy + Vz * Vz)
+    return [rho, rho * Vx, rho * Vy, rho * Vz, IntE + KinE]
+
+
+def block_c2p(P, U):
+    D = rmax(U[0], torch.full_like(U[0], P.dFloor))
+    Mx, My, Mz = U[1], U[2], U[3]
+    KinE = 0.5 * (Mx * Mx + My * My + Mz * Mz) / D
+    Pr = rmax((P.gamma - 1) * (U[4] - KinE), torch.full_like(D, P.pFloor))
+    return [D, Mx / D, My / D, Mz / D, Pr]
+
+
+# ----------------------------------------------------------------- grid
+class Grid:
+    """Metric tensors in the unpadded box convention (from the C ABI's
+    Fortran-layout geometry arrays)."""
+
+    def __init__(self, P: DiffParams, geo: dict, xyzcc_np=None, dtype=torch.float64, device="cpu"):
+        self.P = P
+        self.Ni, self.Nj, self.Nk = P.Nip + 2 * G, P.Njp + 2 * G, P.Nkp + 2 * G
+        self.dtype, self.device = dtype, device
+
+        def face(a):
+            return torch.as_tensor(np.ascontiguousarray(a), dtype=dtype, device=device)
+
+        def cell(a):
+            a = np.asarray(a)
+            out = np.zeros((a.shape[0], self.Nk + 1, self.Nj + 1, self.Ni + 1))
+            out[:, :self.Nk, :self.Nj, :self.Ni] = a
+            return torch.as_tensor(out, dtype=dtype, device=device)
+
+        self.face = face(geo["face"])
+        self.xfc = face(geo["xfc"])
+        self.Tf = face(geo["Tf"])
+        self.edge = face(geo["edge"])
+        self.Te = face(geo["Te"])
+        self.Teb = face(geo["Teb"])
+        self.vol = cell(geo["volume"])[0]
+        self.xyzcc = cell(geo["xyzcc"])
+        self._bc_maps()
+
+    def cell_box(self, a):
+        """Fortran-layout cell array (nc, Nk, Nj, Ni) -> box tensor."""
+        a = torch.as_tensor(np.asarray(a), dtype=self.dtype, device=self.device)
+        out = torch.zeros((a.shape[0], self.Nk + 1, self.Nj + 1, self.Ni + 1), dtype=self.dtype, device=self.device)
+        out[:, :self.Nk, :self.Nj, :self.Ni] = a
+        return out
+
+    def face_box(self, a):
+        return torch.as_tensor(np.ascontiguousarray(a), dtype=self.dtype, device=self.device)
+
+    def _bc_maps(self):
+        """Flat gather indices of the periodic boundary fill (bcs.F90:279-450):
+        cell values and each face component, composed over the three directions."""
+        P = self.P
+        nx, ny, nz = self.Ni + 1, self.Nj + 1, self.Nk + 1
+        n = (P.Nip, P.Njp, P.Nkp)
+
+        def m(x, nn, normal):
+            x = x.copy()
+            lo = x < G
+            x[lo] = x[lo] + nn
+            if normal:
+                hi = (x >= G + nn + 1) & (x <= G + nn + 4)
+            else:
+                hi = (x >= G + nn) & (x <= G + nn + 3)
+            x[hi] = x[hi] - nn
+            return x
+
+        kk, jj, ii = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+        self.bc_src = {}
+        for comp in (-1, 0, 1, 2):
+            si = m(ii, n[0], comp == 0)
+            sj = m(jj, n[1], comp == 1)
+            sk = m(kk, n[2], comp == 2)
+            src = (sk * ny + sj) * nx + si
+            if comp == -1:  # cell values: the cell box only
+                keep = (ii >= self.Ni) | (jj >= self.Nj) | (kk >= self.Nk)
+                src = np.where(keep, (kk * ny + jj) * nx + ii, src)
+            self.bc_src[comp] = torch.as_tensor(src.reshape(-1), device=self.device)
+
+    def bxyz(self, mf):
+        """gamCellBxyz (gridutils.F90:648-680) on every cell of the box."""
+        rc = (0, self.Ni - 1, 0, self.Nj - 1, 0, self.Nk - 1)
+        fI, fIp = win(mf[0], rc), win(mf[0], rc, (1, 0, 0))
+        fJ, fJp = win(mf[1], rc), win(mf[1], rc, (0, 1, 0))
+        fK, fKp = win(mf[2], rc), win(mf[2], rc, (0, 0, 1))
+        dV = win(self.vol, rc)
+        Div = fIp - fI + fJp - fJ + fKp - fK
+        B = []
+        for x in range(3):
+            t = (fIp * win(self.xfc[x], rc, (1, 0, 0)) + fJp * win(self.xfc[x + 3], rc, (0, 1, 0)) +
+                 fKp * win(self.xfc[x + 6], rc, (0, 0, 1)) - fI * win(self.xfc[x], rc) -
+                 fJ * win(self.xfc[x + 3], rc) - fK * win(self.xfc[x + 6], rc)) / dV
+            B.append(t - Div * win(self.xyzcc[x], rc) / dV)
+        return put(torch.zeros_like(mf), rc, torch.stack(B))
+
+
+# ----------------------------------------------------------------- the step
+def step(g: Grid, cur: dict, old: dict, dt: float, odt: float):
+    """One stepGamera with a fixed dt. cur/old: {"Gas": (5,...), "mf": (3,...),
+    "B": (3,...)} box tensors of State (n) and oState (n-1); odt = time - otime
+    after the AdvanceMHD time trap. Returns State (n+1) (boundaries filled)."""
+    P = g.P
+    Ni, Nj, Nk = g.Ni, g.Nj, g.Nk
+    pdt = 0.5 * dt
+    gm1 = P.gamma - 1
+    allf = (0, Ni, 0, Nj, 0, Nk)
+    allc = (0, Ni - 1, 0, Nj - 1, 0, Nk - 1)
+
+    # --- Predictor (every face and cell of the box)
+    Q, oQ = cur["mf"], old["mf"]
+    hm = Q + pdt * ((Q - oQ) / odt)
+    A = g.face
+    Am = rmax(A, torch.full_like(A, TINY))
+    bh = hm / Am
+    abh = A * bh
+    Bnf = hm / A
+    bn = Q / Am
+    Uc = [win(cur["Gas"][v], allc) for v in range(5)]
+    Uo = [win(old["Gas"][v], allc) for v in range(5)]
+    W, oW = cell_c2p(P, Uc), cell_c2p(P, Uo)
+    pW = [W[v] + pdt * ((W[v] - oW[v]) / odt) for v in range(5)]
+    pW[0] = rmax(pW[0], torch.full_like(pW[0], P.dFloor))
+    pW[4] = rmax(pW[4], torch.full_like(pW[4], P.pFloor))
+    pQ = cell_p2c(P, pW)
+    Wh = block_c2p(P, pQ)
+    Wn = block_c2p(P, Uc)
+    vol = win(g.vol, allc)
+    zeros5 = torch.zeros_like(cur["Gas"])
+    QW = put(zeros5, allc, torch.stack([vol * Wh[v] for v in range(5)]))
+    WnB = put(zeros5, allc, torch.stack(Wn))
+    Dh = put(torch.zeros_like(g.vol), allc, Wh[0])
+    Dm = rmax(pQ[0], torch.full_like(pQ[0], P.dFloor))
+    VdV = put(torch.zeros_like(cur["B"]), allc, torch.stack([vol * pQ[1 + x] / Dm for x in range(3)]))
+    QB = g.bxyz(hm) * g.vol
+    Blim = cur["B"]
+
+    # --- CalcElecField
+    Np = (P.Nip, P.Njp, P.Nkp)
+    mf_r = [(0, Ni - 1, G, G + Np[1], 0, Nk - 1), (0, Ni - 1, 0, Nj - 1, G, G + Np[2]), (G, G + Np[0], 0, Nj - 1, 0, Nk - 1)]
+    ed_r = [(G, G + Np[0] - 1, G, G + Np[1], G, G + Np[2]), (G, G + Np[0], G, G + Np[1] - 1, G, G + Np[2]),
+            (G, G + Np[0], G, G + Np[1], G, G + Np[2] - 1)]
+    E = []
+    for eD in range(3):
+        dT1, dT2 = (eD + 1) % 3, (eD + 2) % 3
+        r = mf_r[eD]
+        dV = rmax(central8([win(g.vol, r, unit(dT1, n - 4)) for n in range(8)]), torch.full_like(win(g.vol, r), TINY))
+        Af = win(A[dT1], r)
+        AVf = torch.zeros_like(cur["B"])
+        AVf = put(AVf, r, torch.stack([Af * (central8([win(VdV[x], r, unit(dT1, n - 4)) for n in range(8)]) / dV)
+                                       for x in range(3)]))
+        r = ed_r[eD]
+        e1 = 1 if eD == 0 else 0
+        e2 = 1 if eD == 2 else 2
+        o1, o2 = unit(e1, -1), unit(e2, -1)
+        Dc = 0.25 * (win(Dh, r) + win(Dh, r, o1) + win(Dh, r, o2) + win(Dh, r, add(o1, o2)))
+
+        def edge_lrs(a, bd):
+            area = [win(A[a], r, unit(bd, n - 4)) for n in range(8)]
+            qdv = [win(abh[a], r, unit(bd, n - 4)) for n in range(8)]
+            nmag = [win(bn[a], r, unit(bd, m - 2)) for m in range(4)]
+            Vi = central8(area)
+            bL, bR = lrs_from_qdv(P, qdv, nmag, Vi)
+            return bL * Vi, bR * Vi, Vi
+
+        bT1L, bT1R, fA1 = edge_lrs(dT1, dT2)
+        bT2L, bT2R, fA2 = edge_lrs(dT2, dT1)
+        dA = rmax(fA1, torch.full_like(fA1, TINY))
+        VC = [central8([win(AVf[x], r, unit(dT2, n - 4)) for n in range(8)]) / dA for x in range(3)]
+        Te = [win(g.Te[q + 9 * eD], r) for q in range(9)]
+        v1 = VC[0] * Te[3] + VC[1] * Te[4] + VC[2] * Te[5]
+        v2 = VC[0] * Te[6] + VC[1] * Te[7] + VC[2] * Te[8]
+        vDiff = safe_sqrt(v1 * v1 + v2 * v2)
+        xni, yni, xnj, ynj = (win(g.Teb[q + 4 * eD], r) for q in range(4))
+        detT = 1.0 / (xni * ynj - xnj * yni)
+        bT1 = 0.5 * (bT1L + bT1R) / fA1
+        bT2 = 0.5 * (bT2L + bT2R) / fA2
+        db1 = (bT1R - bT1L) / fA1
+        db2 = (bT2R - bT2L) / fA2
+        Jd = db2 - db1
+        b1 = detT * (ynj * bT1 - yni * bT2)
+        b2 = detT * (-(xnj * bT1) + xni * bT2)
+        vA = safe_sqrt(b1 * b1 + b2 * b2) / torch.sqrt(Dc)
+        vDiff = vDiff + vA
+        edge = win(g.edge[eD], r)
+        vDiff = rmin(vDiff, P.CFL * edge / dt)
+        e = -(v1 * b2 - v2 * b1) + P.Vd0 * vDiff * Jd
+        E.append(put(torch.zeros_like(g.vol), r, e * edge))
+
+    # --- CalcStress
+    fr = [(G, G + Np[0], G, G + Np[1] - 1, G, G + Np[2] - 1), (G, G + Np[0] - 1, G, G + Np[1], G, G + Np[2] - 1),
+          (G, G + Np[0] - 1, G, G + Np[1] - 1, G, G + Np[2])]
+    gF, mF = [], []
+    for D in range(3):
+        r = fr[D]
+        T = [win(g.Tf[n + 9 * D], r) for n in range(9)]
+        fa = win(A[D], r)
+        Vi = central8([win(g.vol, r, unit(D, n - 4)) for n in range(8)])
+        Bn = win(Bnf[D], r)
+        Mag = [lrs_from_qdv(P, [win(QB[x], r, unit(D, n - 4)) for n in range(8)],
+                            [win(Blim[x], r, unit(D, m - 2)) for m in range(4)], Vi) for x in range(3)]
+        Wlr = [lrs_from_qdv(P, [win(QW[v], r, unit(D, n - 4)) for n in range(8)],
+                            [win(WnB[v], r, unit(D, m - 2)) for m in range(4)], Vi) for v in range(5)]
+        mFx = [torch.zeros_like(fa) for _ in range(3)]
+        gFv = [torch.zeros_like(fa) for _ in range(5)]
+        dW = [torch.zeros_like(fa) for _ in range(5)]
+        VaD = torch.zeros_like(fa)
+        for side, sgn in ((0, -1.0), (1, 1.0)):
+            Wq = [Wlr[v][side] for v in range(5)]
+            Bq = [Mag[x][side] for x in range(3)]
+            # MagKinFlux (stress.F90:513-599), no background, Boris off
+            Dq, Pr = Wq[0], Wq[4]
+            dPb = 0.5 * (Bq[0] * Bq[0] + Bq[1] * Bq[1] + Bq[2] * Bq[2])
+            Va2 = 2.0 * dPb / Dq
+            Vn = T[0] * Wq[1] + T[1] * Wq[2] + T[2] * Wq[3]
+            lam = 1.0 / (2.0 * Pr / Dq + Va2)
+            Vn0 = 0.5 * torch.special.erfc(sgn * torch.sqrt(lam) * Vn)
+            VaD = VaD + 0.5 * safe_sqrt(Va2)
+            for x in range(3):
+                mFx[x] = mFx[x] + Vn0 * (dPb * T[x] - Bq[x] * Bn)
+            # GasKinFlux (stress.F90:432-511)
+            Vx, Vy, Vz = Wq[1], Wq[2], Wq[3]
+            Eg = 0.5 * Dq * (Vx * Vx + Vy * Vy + Vz * Vz) + Pr / gm1
+            lam = Dq / (2.0 * Pr)
+            Vn = T[0] * Vx + T[1] * Vy + T[2] * Vz
+            Vt1 = T[3] * Vx + T[4] * Vy + T[5] * Vz
+            Vt2 = T[6] * Vx + T[7] * Vy + T[8] * Vz
+            Vn0 = 0.5 * torch.special.erfc(sgn * torch.sqrt(lam) * Vn)
+            Vn1 = Vn * Vn0 - 0.5 * sgn * torch.exp(-(lam * Vn * Vn)) / torch.sqrt(PI * lam)
+            gFv[0] = gFv[0] + Dq * Vn1
+            gFv[4] = gFv[4] + (Eg + 0.5 * Pr) * Vn1 + 0.5 * Pr * Vn0 * Vn
+            fMn = Dq * Vn * Vn1 + Pr * Vn0
+            fMt1 = Dq * Vt1 * Vn1
+            fMt2 = Dq * Vt2 * Vn1
+            gFv[1] = gFv[1] + (T[0] * fMn + T[3] * fMt1 + T[6] * fMt2)
+            gFv[2] = gFv[2] + (T[1] * fMn + T[4] * fMt1 + T[7] * fMt2)
+            gFv[3] = gFv[3] + (T[2] * fMn + T[5] * fMt1 + T[8] * fMt2)
+            dW[0] = dW[0] + sgn * Dq
+            dW[1] = dW[1] + sgn * Dq * Vx
+            dW[2] = dW[2] + sgn * Dq * Vy
+            dW[3] = dW[3] + sgn * Dq * Vz
+            dW[4] = dW[4] + sgn * Eg
+        mF.append(put(torch.zeros_like(cur["B"]), r, torch.stack([fa * mFx[x] for x in range(3)])))
+        gF.append(put(zeros5, r, torch.stack([fa * (gFv[v] - 1.0 * P.cHogH * VaD * dW[v]) for v in range(5)])))
+
+    # --- applyUpdate: E2Flux on the active faces, then the cells
+    inr = (G, G + Np[0], G, G + Np[1], G, G + Np[2])
+    dfi = win(E[2], inr, (0, 1, 0)) - win(E[2], inr) - win(E[1], inr, (0, 0, 1)) + win(E[1], inr)
+    dfj = win(E[0], inr, (0, 0, 1)) - win(E[0], inr) - win(E[2], inr, (1, 0, 0)) + win(E[2], inr)
+    dfk = win(E[1], inr, (1, 0, 0)) - win(E[1], inr) - win(E[0], inr, (0, 1, 0)) + win(E[0], inr)
+    mfn = put(cur["mf"], inr, torch.stack([win(cur["mf"][0], inr) - dt * dfi, win(cur["mf"][1], inr) - dt * dfj,
+                                          win(cur["mf"][2], inr) - dt * dfk]))
+    act = (G, G + Np[0] - 1, G, G + Np[1] - 1, G, G + Np[2] - 1)
+    dV = win(g.vol, act)
+    U = []
+    for v in range(5):
+        dGasH = (win(gF[0][v], act) - win(gF[0][v], act, (1, 0, 0)) + win(gF[1][v], act) -
+                 win(gF[1][v], act, (0, 1, 0)) + win(gF[2][v], act) - win(gF[2][v], act, (0, 0, 1))) / dV
+        U.append(win(cur["Gas"][v], act) + dt * dGasH)
+    dGasM = [(win(mF[0][x], act) - win(mF[0][x], act, (1, 0, 0)) + win(mF[1][x], act) - win(mF[1][x], act, (0, 1, 0)) +
+              win(mF[2][x], act) - win(mF[2][x], act, (0, 0, 1))) / dV for x in range(3)]
+    # CellMaxwell (mhdgroup.F90:299-329)
+    Dn = rmax(U[0], torch.full_like(U[0], P.dFloor))
+    Mx, My, Mz, TotE = U[1], U[2], U[3], U[4]
+    KinE = 0.5 * (Mx * Mx + My * My + Mz * Mz) / Dn
+    Pr = rmax(gm1 * (TotE - KinE), torch.full_like(Dn, P.pFloor))
+    Mx, My, Mz = Mx + dt * dGasM[0], My + dt * dGasM[1], Mz + dt * dGasM[2]
+    KinE = 0.5 * (Mx * Mx + My * My + Mz * Mz) / Dn
+    Gas = put(cur["Gas"], act, torch.stack([Dn, Mx, My, Mz, KinE + Pr / gm1]))
+
+    # --- EnforceBCs (periodic gather) and the final bFlux2Fld
+    shp = Gas.shape
+    Gas = Gas.reshape(5, -1)[:, g.bc_src[-1]].reshape(shp)
+    mfs = mfn.reshape(3, -1)
+    mfn = torch.stack([mfs[d][g.bc_src[d]] for d in range(3)]).reshape(mfn.shape)
+    return {"Gas": Gas, "mf": mfn, "B": g.bxyz(mfn)}
+
+
+def run(g: Grid, cur: dict, old: dict, dt: float, nsteps: int, odt0: float | None = None):
+    """nsteps fixed-dt steps; the AB2 spacing is odt0 for the first step
+    (time - otime of the start), dt afterwards. Returns (State, oState)."""
+    odt = dt if odt0 is None else odt0
+    for _ in range(nsteps):
+        nxt = step(g, cur, old, dt, odt)
+        old, cur = cur, nxt
+        odt = dt
+    return cur, old
+
+
+def loss_b2(g: Grid, state: dict, lo=0.6, hi=0.8):
+    """Sum of |B|^2 over the active cells whose centre lies in [lo, hi]^3."""
+    P = g.P
+    act = (G, G + P.Nip - 1, G, G + P.Njp - 1, G, G + P.Nkp - 1)
+    xc = win(g.xyzcc, act)
+    m = ((xc >= lo) & (xc <= hi)).all(dim=0)
+    B = win(state["B"], act)
+    return ((B * B).sum(dim=0) * m).sum()
+
+
+def loss_and_grad(g: Grid, Gas0, mf0, dt: float, nsteps: int, seg: int | None = None, lossf=loss_b2):
+    """Loss after nsteps from the start State = oState = (Gas0, mf0, bxyz(mf0))
+    (otime = time - dt) and its gradient w.r.t. Gas0 and mf0.
+
+    Checkpointing: the forward sweep keeps only the (State, oState) pair at the
+    start of each segment of seg steps (default ~sqrt(nsteps)); the reverse
+    sweep recomputes one segment at a time with autograd and carries the
+    adjoint of the pair backwards."""
+    seg = seg or max(1, int(round(nsteps ** 0.5)))
+    with torch.no_grad():
+        cur = {"Gas": Gas0, "mf": mf0, "B": g.bxyz(mf0)}
+        old = dict(cur)
+        ckpt = []
+        n = 0
+        while n < nsteps:
+            ckpt.append((n, {k: v.clone() for k, v in cur.items()}, {k: v.clone() for k, v in old.items()}))
+            m = min(seg, nsteps - n)
+            cur, old = run(g, cur, old, dt, m)
+            n += m
+    # reverse sweep
+    lam_cur = lam_old = None
+    loss_val = None
+    for idx in range(len(ckpt) - 1, -1, -1):
+        n0, c0, o0 = ckpt[idx]
+        m = min(seg, nsteps - n0)
+        first = n0 == 0
+        if first:
+            G0 = Gas0.detach().clone().requires_grad_(True)
+            F0 = mf0.detach().clone().requires_grad_(True)
+            c = {"Gas": G0, "mf": F0, "B": g.bxyz(F0)}
+            o = c
+            leaves = [G0, F0]
+        else:
+            c = {k: v.detach().clone().requires_grad_(True) for k, v in c0.items()}
+            o = {k: v.detach().clone().requires_grad_(True) for k, v in o0.items()}
+            leaves = [c[k] for k in ("Gas", "mf", "B")] + [o[k] for k in ("Gas", "mf", "B")]
+        with torch.enable_grad():
+            ce, oe = run(g, c, o, dt, m)
+            if lam_cur is None:
+                L = lossf(g, ce)
+                loss_val = float(L.detach())
+                outs, grads = [L], [torch.ones_like(L)]
+            else:
+                outs, grads = [], []
+                for k in ("Gas", "mf", "B"):
+                    outs += [ce[k], oe[k]]
+                    grads += [lam_cur[k], lam_old[k]]
+            gl = torch.autograd.grad(outs, leaves, grads, allow_unused=True)
+        gl = [torch.zeros_like(x) if gv is None else gv for x, gv in zip(leaves, gl)]
+        if first:
+            return loss_val, gl[0], gl[1]
+        lam_cur = dict(zip(("Gas", "mf", "B"), gl[:3]))
+        lam_old = dict(zip(("Gas", "mf", "B"), gl[3:]))
+    raise AssertionError("unreachable")
