@@ -198,13 +198,15 @@ class Grid:
 
     def cell_box(self, a):
         """Fortran-layout cell array (nc, Nk, Nj, Ni) -> box tensor."""
-        a = torch.as_tensor(np.asarray(a), dtype=self.dtype, device=self.device)
+        a = a if torch.is_tensor(a) else torch.as_tensor(np.asarray(a))
+        a = a.to(dtype=self.dtype, device=self.device)
         out = torch.zeros((a.shape[0], self.Nk + 1, self.Nj + 1, self.Ni + 1), dtype=self.dtype, device=self.device)
         out[:, :self.Nk, :self.Nj, :self.Ni] = a
         return out
 
     def face_box(self, a):
-        return torch.as_tensor(np.ascontiguousarray(a), dtype=self.dtype, device=self.device)
+        a = a if torch.is_tensor(a) else torch.as_tensor(np.ascontiguousarray(a))
+        return a.to(dtype=self.dtype, device=self.device)
 
     def _bc_maps(self):
         """Flat gather indices of the periodic boundary fill (bcs.F90:279-450):
