@@ -152,8 +152,8 @@ def cpu_sample(g, w, params, budget_s=12.0, max_steps=6):
 def adjoint_section(N=(64, 64, 64), nsteps=20, sigma=1e-3, seed=2024):
     """Differentiation form on the curvilinear blast wave: loss = sum of |B|^2
     over cells centred in [0.6, 0.8]^3 after nsteps fixed-dt steps from the
-    blast-wave start with seeded Gaussian noise (relative sigma on rho, v, P;
-    absolute on the face fluxes); gradient w.r.t. the start Gas and fluxes by
+    blast-wave start with seeded Gaussian noise (relative sigma on rho and P,
+    absolute on v, sigma x face area on the face fluxes); gradient w.r.t. the start Gas and fluxes by
     the checkpointed reverse mode of mage_b200.diffstep, FP64 and FP32, and a
     central difference of the CUDA forward along a random direction."""
     import torch
@@ -186,7 +186,9 @@ def adjoint_section(N=(64, 64, 64), nsteps=20, sigma=1e-3, seed=2024):
             W = [W[0] * (1 + sigma * noise()), W[1] + sigma * noise(), W[2] + sigma * noise(), W[3] + sigma * noise(),
                  W[4] * (1 + sigma * noise())]
             Gas0 = g.cell_box(torch.stack(cell_p2c(g.P, W)))
-            mf0 = g.face_box(st["magFlux"]) + sigma * torch.as_tensor(rng.standard_normal(g.face.shape), device="cuda")
+            # flux noise of sigma in field units: sigma * face area
+            mf0 = g.face_box(st["magFlux"]) + sigma * g.face * torch.as_tensor(rng.standard_normal(g.face.shape),
+                                                                             device="cuda")
             Gas64, mf64 = Gas0, mf0
         else:
             Gas0, mf0 = Gas64.float(), mf64.float()
@@ -219,7 +221,7 @@ def adjoint_section(N=(64, 64, 64), nsteps=20, sigma=1e-3, seed=2024):
         gpu.step_gamera(nsteps)
         return float(loss_b2(g, {"B": g.cell_box(gpu.download_state(old=False)["Bxyz"])}))
 
-    eps = 1e-7
+    eps = 1e-8
     fd = (cuda_loss(Gas64 + eps * vG, mf64 + eps * vF) - cuda_loss(Gas64 - eps * vG, mf64 - eps * vF)) / (2 * eps)
     ad = float((grads["fp64"][0] * vG).sum() + (grads["fp64"][1] * vF).sum())
     out["fd_check"] = {"eps": eps, "central_difference_cuda": fd, "reverse_mode": ad, "rel_err": abs(fd - ad) / abs(ad)}
