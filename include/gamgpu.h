@@ -169,6 +169,14 @@ int gam_set_wind(gam_handle* h, const double wind[8]);
  * gam_set_geometry, and the background field when doBackground. */
 int gam_init_dipole_wind(gam_handle* h, const double wind[8], uint64_t seed, double amp);
 
+/* Restart files: State and oState with ghosts, t, State/oState time, dt, dt0
+ * and ts in one binary file (72-byte header "GAMRST01", then Gas, magFlux,
+ * Bxyz, oGas, omagFlux as float64 Fortran-ordered arrays). Stands in for the
+ * restart dump of writeH5Res / readH5Restart (src/gamera/gioH5.F90:636-858),
+ * which is HDF5; reading needs a handle of the same grid size. */
+int gam_write_restart(gam_handle* h, const char* path);
+int gam_read_restart(gam_handle* h, const char* path);
+
 /* Conserved totals for callers that cannot allocate device memory.
  * No counterpart in the reference. Some callers cannot call cudaMalloc while
  * they run: their device memory belongs to another framework's pool, or they

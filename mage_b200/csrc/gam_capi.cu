@@ -30,6 +30,7 @@ void gam_geom_box_to_fortran_d(const GamBox& b, const double* src, double* dst, 
 void gam_geom_box_to_fortran_f(const GamBox& b, const float* src, double* dst, bool face, int nc, cudaStream_t s);
 void gam_geom_fill(double* p, long n, double v, cudaStream_t s);
 void gam_geom_d2f(const double* src, float* dst, long n, cudaStream_t s);
+void gam_geom_dxf(const GamBox& b, const double* xfc, const double* xyzcc, float* dxf, cudaStream_t s);
 void gam_geom_metric(const GamBox& b, const double* xyz, double* face, double* xfc, double* Tf, double* vol,
                      double* xyzcc, double* dijk, double* dl, double* edge, double* Te, double* Teb, cudaStream_t s);
 void gam_geom_ic_ot(const GamBox& b, const double* xyzcc, const double* face, double* Gas, double* mf, double gamma,
@@ -157,11 +158,13 @@ template <class R> static int alloc_bulk(gam_handle* h, Ctx<R>& C) {
         C.g.vol = (const R*)h->gd.vol; C.g.xyzcc = (const R*)h->gd.xyzcc; C.g.dl = (const R*)h->gd.dl;
         C.g.face = (const R*)h->gd.face; C.g.xfc = (const R*)h->gd.xfc; C.g.Tf = (const R*)h->gd.Tf;
         C.g.edge = (const R*)h->gd.edge; C.g.Te = (const R*)h->gd.Te; C.g.Teb = (const R*)h->gd.Teb;
+        C.g.dxf = nullptr;
     } else {
-        R *vol, *xyzcc, *dl, *face, *xfc, *Tf, *edge, *Te, *Teb;
+        R *vol, *xyzcc, *dl, *face, *xfc, *Tf, *edge, *Te, *Teb, *dxf;
         A(vol, 1); A(xyzcc, 3); A(dl, 1); A(face, 3); A(xfc, 9); A(Tf, 27); A(edge, 3); A(Te, 27); A(Teb, 12);
+        A(dxf, 18);
         C.g.vol = vol; C.g.xyzcc = xyzcc; C.g.dl = dl; C.g.face = face; C.g.xfc = xfc; C.g.Tf = Tf;
-        C.g.edge = edge; C.g.Te = Te; C.g.Teb = Teb;
+        C.g.edge = edge; C.g.Te = Te; C.g.Teb = Teb; C.g.dxf = dxf;
     }
 #undef A
     C.g.fcB0 = h->bg.fcB0;
@@ -330,6 +333,7 @@ static void sync_geo_f32(gam_handle* h) {
     gam_geom_d2f(h->gd.edge, (float*)g.edge, 3 * fs, h->s);
     gam_geom_d2f(h->gd.Te, (float*)g.Te, 27 * fs, h->s);
     gam_geom_d2f(h->gd.Teb, (float*)g.Teb, 12 * fs, h->s);
+    gam_geom_dxf(h->b, h->gd.xfc, h->gd.xyzcc, (float*)g.dxf, h->s);
 }
 
 extern "C" int gam_set_geometry(gam_handle* h, const double* xyz) {
@@ -529,23 +533,54 @@ extern "C" int gam_advance_model(gam_handle* h, double dt, double* t_out) {
     return rc;
 }
 
+// The update and boundary kernels write the other state buffer, which holds
+// oState: it is copied aside and put back, like the scalars, so the state is
+// left as it was. The AB2 spacing the step kernels read is set the way
+// k_step_begin sets it (mhdgroup.F90:25-31), also before the first step.
+template <class R> static int profile_t(gam_handle* h, Ctx<R>& C, int32_t reps, double* ms, GamScalars s) {
+    const long fs = h->b.fs;
+    const StateBuf<R>& O = C.st[1 - h->cur];
+    R* save = nullptr;
+    CK(h, cudaMalloc(&save, 11 * fs * sizeof(R)));
+    auto cp = [&](R* d, const R* src, long n) { return cudaMemcpyAsync(d, src, n * sizeof(R), cudaMemcpyDeviceToDevice, h->s); };
+    cudaError_t e = cp(save, O.Gas, 5 * fs);
+    if (e == cudaSuccess) e = cp(save + 5 * fs, O.mf, 3 * fs);
+    if (e == cudaSuccess) e = cp(save + 8 * fs, O.B, 3 * fs);
+    GamScalars t = s;
+    if (fabs(t.otime - t.time) < 1.0e-12) t.otime = t.time - t.dt;
+    t.odt = t.time - t.otime;
+    t.pdt = 0.5 * t.dt;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h->sc, &t, sizeof(t), cudaMemcpyHostToDevice, h->s);
+    if (e == cudaSuccess) {
+        if (h->f32)
+            gam_fast_profile_f32(h->cf, h->cur, h->s, reps, ms);
+        else if (h->p.strict)
+            gam_strict_profile_f64(h->cd, h->cur, h->s, reps, ms);
+        else
+            gam_fast_profile_f64(h->cd, h->cur, h->s, reps, ms);
+        e = cudaGetLastError();
+    }
+    cudaError_t e2 = cp(O.Gas, save, 5 * fs);
+    if (e2 == cudaSuccess) e2 = cp(O.mf, save + 5 * fs, 3 * fs);
+    if (e2 == cudaSuccess) e2 = cp(O.B, save + 8 * fs, 3 * fs);
+    // restore the scalars the repeated kernels touched (dt reduction, AB2 spacing)
+    if (e2 == cudaSuccess) e2 = cudaMemcpyAsync(h->sc, &s, sizeof(s), cudaMemcpyHostToDevice, h->s);
+    if (e2 == cudaSuccess) e2 = cudaStreamSynchronize(h->s);
+    cudaFree(save);
+    CK(h, e);
+    CK(h, e2);
+    return GAM_OK;
+}
+
 extern "C" int gam_profile_step(gam_handle* h, int32_t reps, double* ms, int32_t n) {
     if (!h || !ms || n < 15 || reps < 1) return GAM_EINVAL;
     if (!h->haveGeo || !h->haveState) return fail(h, GAM_ESTATE, "gam_profile_step needs geometry and state");
+    if (h->p.doBackground && !h->haveBg) return fail(h, GAM_ESTATE, "doBackground: set the background field first");
+    if (h->p.bc[1] == GAM_BC_WIND && !h->haveWind) return fail(h, GAM_ESTATE, "wind boundary: call gam_set_wind first");
     GamScalars s;
     CK(h, cudaMemcpyAsync(&s, h->sc, sizeof(s), cudaMemcpyDeviceToHost, h->s));
     CK(h, cudaStreamSynchronize(h->s));
-    if (h->f32)
-        gam_fast_profile_f32(h->cf, h->cur, h->s, reps, ms);
-    else if (h->p.strict)
-        gam_strict_profile_f64(h->cd, h->cur, h->s, reps, ms);
-    else
-        gam_fast_profile_f64(h->cd, h->cur, h->s, reps, ms);
-    // restore the scalars the repeated kernels touched (dt reduction)
-    CK(h, cudaMemcpyAsync(h->sc, &s, sizeof(s), cudaMemcpyHostToDevice, h->s));
-    CK(h, cudaStreamSynchronize(h->s));
-    CK(h, cudaGetLastError());
-    return GAM_OK;
+    return h->f32 ? profile_t<float>(h, h->cf, reps, ms, s) : profile_t<double>(h, h->cd, reps, ms, s);
 }
 
 extern "C" int gam_last_step_ms(gam_handle* h, double* ms) {
@@ -838,4 +873,74 @@ extern "C" int gam_init_dipole_wind(gam_handle* h, const double wind[8], uint64_
     gam_geom_fill(Gas64, 8 * h->b.fs, 0.0, h->s);
     gam_geom_ic_wind(h->b, h->gd.xyz, Gas64, mf64, lA, h->p.gamma, h->p.dFloor, h->p.pFloor, wind, seed, amp, h->s);
     return init_common(h, Gas64, mf64);
+}
+
+// ------------------------------------------------------------ restart files
+// A binary stand-in for the restart dump of writeH5Res / readH5Restart
+// (src/gamera/gioH5.F90:636-858): State and oState with their ghosts, the
+// times, ts, dt and dt0. Layout: a 72-byte header (magic "GAMRST01", Nip, Njp,
+// Nkp as int32, one int32 zero, t, State%time, oState%time, dt, dt0 as
+// float64, ts as int32, one int32 zero), then Gas, magFlux, Bxyz, oGas,
+// omagFlux as float64 Fortran-ordered arrays with ghosts, little endian.
+struct GamRestartHeader {
+    char magic[8];
+    int32_t Nip, Njp, Nkp, zero0;
+    double t, time, otime, dt, dt0;
+    int32_t ts, zero1;
+};
+static_assert(sizeof(GamRestartHeader) == 72, "restart header layout");
+
+extern "C" int gam_write_restart(gam_handle* h, const char* path) {
+    if (!h || !path) return GAM_EINVAL;
+    if (!h->haveState) return fail(h, GAM_ESTATE, "no state to write");
+    const long nc = n_cell(h->b), nf = n_face(h->b);
+    std::vector<double> Gas(5 * nc), mf(3 * nf), B(3 * nc), oGas(5 * nc), omf(3 * nf);
+    GamRestartHeader hd;
+    memset(&hd, 0, sizeof(hd));
+    memcpy(hd.magic, "GAMRST01", 8);
+    hd.Nip = h->p.Nip; hd.Njp = h->p.Njp; hd.Nkp = h->p.Nkp;
+    int rc = gam_download_state(h, Gas.data(), mf.data(), B.data(), oGas.data(), omf.data(), &hd.time, &hd.otime,
+                                &hd.dt, &hd.ts);
+    if (rc) return rc;
+    GamScalars s;
+    CK(h, cudaMemcpy(&s, h->sc, sizeof(s), cudaMemcpyDeviceToHost));
+    hd.t = s.t;
+    hd.dt0 = s.dt0;
+    FILE* f = fopen(path, "wb");
+    if (!f) return fail(h, GAM_EINVAL, std::string("cannot open ") + path + " for writing");
+    bool ok = fwrite(&hd, sizeof(hd), 1, f) == 1;
+    for (auto* v : {&Gas, &mf, &B, &oGas, &omf}) ok = ok && fwrite(v->data(), sizeof(double), v->size(), f) == v->size();
+    ok = (fclose(f) == 0) && ok;
+    if (!ok) return fail(h, GAM_EINVAL, std::string("write to ") + path + " failed");
+    return GAM_OK;
+}
+
+extern "C" int gam_read_restart(gam_handle* h, const char* path) {
+    if (!h || !path) return GAM_EINVAL;
+    FILE* f = fopen(path, "rb");
+    if (!f) return fail(h, GAM_EINVAL, std::string("cannot open ") + path);
+    GamRestartHeader hd;
+    if (fread(&hd, sizeof(hd), 1, f) != 1 || memcmp(hd.magic, "GAMRST01", 8) != 0) {
+        fclose(f);
+        return fail(h, GAM_EINVAL, std::string(path) + " is not a restart file of this library");
+    }
+    if (hd.Nip != h->p.Nip || hd.Njp != h->p.Njp || hd.Nkp != h->p.Nkp) {
+        fclose(f);
+        return fail(h, GAM_EBADDIM, "restart grid size differs from the handle's");
+    }
+    const long nc = n_cell(h->b), nf = n_face(h->b);
+    std::vector<double> Gas(5 * nc), mf(3 * nf), B(3 * nc), oGas(5 * nc), omf(3 * nf);
+    bool ok = true;
+    for (auto* v : {&Gas, &mf, &B, &oGas, &omf}) ok = ok && fread(v->data(), sizeof(double), v->size(), f) == v->size();
+    fclose(f);
+    if (!ok) return fail(h, GAM_EINVAL, std::string(path) + " is truncated");
+    int rc = gam_upload_state(h, Gas.data(), mf.data(), B.data(), oGas.data(), omf.data(), hd.time, hd.otime, hd.dt,
+                              hd.ts);
+    if (rc) return rc;
+    GamScalars s;
+    CK(h, cudaMemcpy(&s, h->sc, sizeof(s), cudaMemcpyDeviceToHost));
+    s.t = hd.t;
+    s.dt0 = hd.dt0;
+    CK(h, cudaMemcpy(h->sc, &s, sizeof(s), cudaMemcpyHostToDevice));
+    return GAM_OK;
 }

@@ -606,6 +606,21 @@ __global__ void k_b0_dp(GamBox b, const double* __restrict__ fS, const double* _
                              fS[(x + 6) * fs + c + b.sk] - fS[(x + 6) * fs + c]) /
                            vol[c];
 }
+
+// Face centroid minus cell centroid (FP64, rounded once) for the six faces of
+// every cell of the box: dxf[(x + 3*f)], f = I-, I+, J-, J+, K-, K+.
+__global__ void k_dxf(GamBox b, const double* __restrict__ xfc, const double* __restrict__ xyzcc, float* dxf) {
+    int ii, jj, kk;
+    if (!tid3(b.Ni, b.Nj, b.Nk, ii, jj, kk)) return;
+    const long c = lidx(b, ii, jj, kk), fs = b.fs;
+    const long up[3] = {1, (long)b.sx, b.sk};
+    for (int d = 0; d < 3; d++)
+        for (int x = 0; x < 3; x++) {
+            const double xc = xyzcc[x * fs + c];
+            dxf[(x + 3 * (2 * d)) * fs + c] = (float)(xfc[(x + 3 * d) * fs + c] - xc);
+            dxf[(x + 3 * (2 * d + 1)) * fs + c] = (float)(xfc[(x + 3 * d) * fs + c + up[d]] - xc);
+        }
+}
 }  // namespace gam_geom
 
 // ------------------------------------------------------------ host wrappers
@@ -717,4 +732,9 @@ void gam_geom_b0_dipole(const GamBox& b, const double* xyz, const double* face, 
     dim3 blkv(64, 1, 1);
     k_b0_cells<<<g3(b.Ni, b.Nj, b.Nk, blkv), blkv, 0, s>>>(b, xyz, vol, M0, B0);
     k_b0_dp<<<g3(b.Nip, b.Njp, b.Nkp, blk), blk, 0, s>>>(b, fS, vol, dpB0);
+}
+
+void gam_geom_dxf(const GamBox& b, const double* xfc, const double* xyzcc, float* dxf, cudaStream_t s) {
+    dim3 blk(32, 4, 1);
+    k_dxf<<<g3(b.Ni, b.Nj, b.Nk, blk), blk, 0, s>>>(b, xfc, xyzcc, dxf);
 }

@@ -33,6 +33,11 @@ template <class R> struct Geo {  // Grid_T arrays on the device (gamtypes.F90:16
     const R* edge;   // edge, 3
     const R* Te;     // edge, 27: n + 9*d
     const R* Teb;    // edge, 12: q + 4*d
+    // FP32 form only: face centroid minus cell centroid for the six faces of
+    // a cell, x + 3*f with f = I-, I+, J-, J+, K-, K+ (computed in FP64, rounded
+    // once). Replaces xfc and xyzcc in bFlux2Fld, whose absolute coordinates
+    // lose the cell-size differences when rounded to FP32.
+    const R* dxf;    // cell, 18
     const double* fcB0;    // face, 9  (background; FP64 in both forms)
     const double* bFlux0;  // face, 3
     const double* edgB0;   // edge, 6: c + 2*d

@@ -110,6 +110,16 @@ module gamgpu
             type(c_ptr), value :: h
             real(c_double), intent(in) :: wind(8)
         end function
+        integer(c_int) function gam_write_restart(h, path) bind(C, name="gam_write_restart")
+            import :: c_int, c_ptr, c_char
+            type(c_ptr), value :: h
+            character(kind=c_char), intent(in) :: path(*)
+        end function
+        integer(c_int) function gam_read_restart(h, path) bind(C, name="gam_read_restart")
+            import :: c_int, c_ptr, c_char
+            type(c_ptr), value :: h
+            character(kind=c_char), intent(in) :: path(*)
+        end function
         integer(c_int) function gam_init_dipole_wind(h, wind, seed, amp) bind(C, name="gam_init_dipole_wind")
             import :: c_int, c_ptr, c_double, c_int64_t
             type(c_ptr), value :: h

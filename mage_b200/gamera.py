@@ -52,7 +52,7 @@ EXPORTED = (
     "gam_set_geometry_arrays", "gam_get_geometry_arrays", "gam_upload_state", "gam_download_state", "gam_step",
     "gam_calc_dt", "gam_divb", "gam_totals", "gam_last_step_ms", "gam_advance_model", "gam_init_orszag_tang",
     "gam_init_blast_wave", "gam_profile_step", "gam_totals_noalloc", "gam_set_background", "gam_get_background",
-    "gam_set_background_dipole", "gam_set_wind", "gam_init_dipole_wind",
+    "gam_set_background_dipole", "gam_set_wind", "gam_init_dipole_wind", "gam_write_restart", "gam_read_restart",
 )
 
 # Background-field arrays (Grid_T, gamtypes.F90:233-242): name, components;
@@ -94,6 +94,8 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     L.gam_get_background.argtypes = [C.c_void_p] + [_dp] * 5
     L.gam_set_background_dipole.argtypes = [C.c_void_p, C.c_double]
     L.gam_set_wind.argtypes = [C.c_void_p, _dp]
+    L.gam_write_restart.argtypes = [C.c_void_p, C.c_char_p]
+    L.gam_read_restart.argtypes = [C.c_void_p, C.c_char_p]
     L.gam_init_dipole_wind.argtypes = [C.c_void_p, _dp, C.c_uint64, C.c_double]
     L.gam_totals_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p,
                                      C.c_void_p, C.c_char_p, C.c_int32]
@@ -269,6 +271,15 @@ class GameraGPU:
         w = np.ascontiguousarray(wind, dtype=np.float64)
         assert w.shape == (8,)
         self._check(self.L.gam_init_dipole_wind(self.h, _ptr(w), int(seed), float(amp)))
+
+    # --- restart files --------------------------------------------------------
+    def write_restart(self, path: str):
+        """State, oState, times, ts, dt and dt0 to a binary restart file."""
+        self._check(self.L.gam_write_restart(self.h, os.fsencode(path)))
+
+    def read_restart(self, path: str):
+        """Load a restart file written by write_restart (same grid size)."""
+        self._check(self.L.gam_read_restart(self.h, os.fsencode(path)))
 
     # --- stepping -------------------------------------------------------------
     def step_gamera(self, n: int = 1):

@@ -208,3 +208,62 @@ def test_advance_model_and_determinism(oracle_built):
 def test_bad_dimensions_rejected():
     with pytest.raises(GamError):
         GameraGPU(GamParams(20, 16, 16))  # Nip % 8 != 0 (init.F90:817-826)
+
+
+def test_profile_step_leaves_state_unchanged():
+    """gam_profile_step right after the set-up and between steps: the state
+    and the following steps are those of an app that was never profiled."""
+    N = (16, 16, 16)
+    xyz = grids.warped_periodic_corners(*N)
+    apps = []
+    for prof in (False, True):
+        g = GameraGPU(GamParams(*N))
+        g.set_geometry(xyz)
+        g.init_blast_wave()
+        if prof:
+            before = g.download_state()
+            ms = g.profile_step(2)
+            assert all(v >= 0 for v in ms.values())
+            after = g.download_state()
+            for k in STATE:
+                assert np.array_equal(before[k], after[k]), k
+        g.step_gamera(3)
+        if prof:
+            g.profile_step(2)
+        g.step_gamera(2)
+        apps.append(g.download_state())
+    for k in STATE:
+        assert np.array_equal(apps[0][k], apps[1][k]), k
+
+
+def test_restart_round_trip(tmp_path):
+    """gam_write_restart / gam_read_restart: a handle restarted from the file
+    continues exactly like the one that wrote it."""
+    N = (16, 16, 16)
+    xyz = grids.warped_periodic_corners(*N)
+    a = GameraGPU(GamParams(*N))
+    a.set_geometry(xyz)
+    a.init_blast_wave()
+    a.step_gamera(3)
+    path = str(tmp_path / "bw16.rst")
+    a.write_restart(path)
+    b = GameraGPU(GamParams(*N))
+    b.set_geometry(xyz)
+    b.read_restart(path)
+    sa, sb = a.download_state(), b.download_state()
+    for k in STATE + ("time", "otime", "dt", "ts"):
+        assert np.array_equal(sa[k], sb[k]), k
+    ra, rb = a.step_gamera(4), b.step_gamera(4)
+    assert ra == rb
+    sa, sb = a.download_state(), b.download_state()
+    for k in STATE:
+        assert np.array_equal(sa[k], sb[k]), k
+    c = GameraGPU(GamParams(24, 16, 16))
+    with pytest.raises(GamError) as e:
+        c.read_restart(path)
+    assert e.value.code == 2  # GAM_EBADDIM
+    junk = tmp_path / "junk.rst"
+    junk.write_bytes(b"not a restart file" * 8)
+    with pytest.raises(GamError) as e:
+        b.read_restart(str(junk))
+    assert e.value.code == 1  # GAM_EINVAL
