@@ -47,6 +47,9 @@ class DiffParams:
     dFloor: float = 1.0e-12
     pFloor: float = 1.0e-12
     up7: bool = False
+    # boundary kinds per side (INI, OUTI, INJ, OUTJ, INK, OUTK): 0 periodic,
+    # 1 none, 2 zero-gradient (J), 3 inner sphere (inner I), 4 solar wind (outer I)
+    bc: tuple = (0, 0, 0, 0, 0, 0)
 
 
 # ----------------------------------------------------------------- helpers
@@ -172,7 +175,8 @@ class Grid:
     """Metric tensors in the unpadded box convention (from the C ABI's
     Fortran-layout geometry arrays)."""
 
-    def __init__(self, P: DiffParams, geo: dict, xyzcc_np=None, dtype=torch.float64, device="cpu"):
+    def __init__(self, P: DiffParams, geo: dict, background: dict | None = None, wind=None, dtype=torch.float64,
+                 device="cpu"):
         self.P = P
         self.Ni, self.Nj, self.Nk = P.Nip + 2 * G, P.Njp + 2 * G, P.Nkp + 2 * G
         self.dtype, self.device = dtype, device
@@ -194,7 +198,60 @@ class Grid:
         self.Teb = face(geo["Teb"])
         self.vol = cell(geo["volume"])[0]
         self.xyzcc = cell(geo["xyzcc"])
+        # background field (AddB0 arrays, cell-sized; kept in FP64 like the CUDA forms)
+        self.bg = None
+        if background is not None:
+            self.bg = {k: torch.as_tensor(self._cellpad(background[k]), dtype=torch.float64, device=device)
+                       for k in ("fcB0", "bFlux0", "edgB0", "B0", "dpB0")}
+        self.wind = None
+        if P.bc[1] == 4:
+            assert wind is not None, "the solar-wind boundary needs the wind state"
+            self.wind = self._wind_tables(geo, np.asarray(wind, dtype=np.float64))
         self._bc_maps()
+
+    def _cellpad(self, a):
+        a = np.asarray(a)
+        out = np.zeros((a.shape[0], self.Nk + 1, self.Nj + 1, self.Ni + 1))
+        out[:, :self.Nk, :self.Nj, :self.Ni] = a
+        return out
+
+    def _wind_tables(self, geo, w):
+        """Blend weights (wgtWind, apps/wind.F90:180-203; RampDown, math.F90:97-111)
+        and wind face fluxes of the 4 outer-I ghost layers, as gam_set_wind
+        computes them: cell weight at ig = ie+n, I-face weight/flux at ig+1,
+        J- and K-face weights/fluxes at ig, for every (j, k) of the face box."""
+        P = self.P
+        i0 = G + P.Nip
+        V, Bsw = w[2:5], w[5:8]
+
+        def norm_vec(a):
+            nA = np.sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2])
+            safe = np.where(nA <= 1e-12, 1.0, nA)
+            return np.where(nA <= 1e-12, 0.0, a / safe)
+
+        def wgt(x):
+            nH = norm_vec(x)
+            vH = norm_vec(V.reshape(3, *([1] * (x.ndim - 1))))
+            dTh = np.arccos(-vH[0] * nH[0] + -vH[1] * nH[1] + -vH[2] * nH[2]) * 180.0 / PI
+            rScl = (dTh - 90.0) / 90.0
+            with np.errstate(divide="ignore", invalid="ignore", over="ignore"):
+                ramp = np.exp(-1.0 / (1.0 - rScl * rScl) + 1.0)
+            return np.where(dTh <= 90.0, 1.0, np.where(dTh >= 180.0, 0.0, ramp))
+
+        xcc = np.asarray(geo["xyzcc"])[:, :, :, i0:i0 + 4]          # (3, Nk, Nj, 4)
+        xfc = np.asarray(geo["xfc"])
+        Tf = np.asarray(geo["Tf"])
+        face = np.asarray(geo["face"])
+        t = {"wC": wgt(xcc)}
+        for d in range(3):
+            sl = slice(i0 + 1, i0 + 5) if d == 0 else slice(i0, i0 + 4)
+            xf = xfc[3 * d:3 * d + 3, :, :, sl]
+            nH = Tf[9 * d:9 * d + 3, :, :, sl]
+            t[f"wF{d}"] = wgt(xf)
+            t[f"sF{d}"] = face[d, :, :, sl] * (nH[0] * Bsw[0] + nH[1] * Bsw[1] + nH[2] * Bsw[2])
+        out = {k: torch.as_tensor(v, dtype=self.dtype, device=self.device) for k, v in t.items()}
+        out["state"] = w
+        return out
 
     def cell_box(self, a):
         """Fortran-layout cell array (nc, Nk, Nj, Ni) -> box tensor."""
@@ -209,29 +266,47 @@ class Grid:
         return a.to(dtype=self.dtype, device=self.device)
 
     def _bc_maps(self):
-        """Flat gather indices of the periodic boundary fill (bcs.F90:279-450):
-        cell values and each face component, composed over the three directions."""
+        """Flat gather indices of the boundary conditions that copy values
+        (periodic bcs.F90:279-450, zero-gradient J :853-892), composed in the
+        reference's order: the value at (i, j, k) comes from the I map of the J
+        map of the K map of its index; the zero-gradient J map applies over the
+        cell ranges of i and k only. SphIn and the wind are applied in place
+        before the gather (step())."""
         P = self.P
         nx, ny, nz = self.Ni + 1, self.Nj + 1, self.Nk + 1
         n = (P.Nip, P.Njp, P.Nkp)
+        bc = P.bc
 
-        def m(x, nn, normal):
+        def lo(kind, x, nn):
             x = x.copy()
-            lo = x < G
-            x[lo] = x[lo] + nn
-            if normal:
-                hi = (x >= G + nn + 1) & (x <= G + nn + 4)
-            else:
-                hi = (x >= G + nn) & (x <= G + nn + 3)
-            x[hi] = x[hi] - nn
+            m = x < G
+            if kind == 0:
+                x[m] = x[m] + nn
+            elif kind == 2:
+                x[m] = G
+            return x
+
+        def hi(kind, x, nn, normal):
+            x = x.copy()
+            m = ((x >= G + nn + 1) & (x <= G + nn + 4)) if normal else ((x >= G + nn) & (x <= G + nn + 3))
+            if kind == 0:
+                x[m] = x[m] - nn
+            elif kind == 2:
+                x[m] = (G + nn) if normal else (G + nn - 1)
             return x
 
         kk, jj, ii = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
         self.bc_src = {}
         for comp in (-1, 0, 1, 2):
-            si = m(ii, n[0], comp == 0)
-            sj = m(jj, n[1], comp == 1)
-            sk = m(kk, n[2], comp == 2)
+            sk = kk
+            if bc[4] == 0:
+                sk = hi(0, lo(0, sk, n[2]), n[2], comp == 2)
+            sjm = hi(bc[3], lo(bc[2], jj, n[1]), n[1], comp == 1)
+            cond = np.ones_like(ii, dtype=bool) if bc[2] == 0 else ((ii < self.Ni) & (sk < self.Nk))
+            sj = np.where(cond, sjm, jj)
+            si = ii
+            if bc[0] == 0:
+                si = hi(0, lo(0, si, n[0]), n[0], comp == 0)
             src = (sk * ny + sj) * nx + si
             if comp == -1:  # cell values: the cell box only
                 keep = (ii >= self.Ni) | (jj >= self.Nj) | (kk >= self.Nk)
@@ -340,6 +415,9 @@ def step(g: Grid, cur: dict, old: dict, dt: float, odt: float):
         Jd = db2 - db1
         b1 = detT * (ynj * bT1 - yni * bT2)
         b2 = detT * (-(xnj * bT1) + xni * bT2)
+        if g.bg is not None:
+            b1 = b1 + win(g.bg["edgB0"][0 + 2 * eD], r).to(b1.dtype)
+            b2 = b2 + win(g.bg["edgB0"][1 + 2 * eD], r).to(b2.dtype)
         vA = safe_sqrt(b1 * b1 + b2 * b2) / torch.sqrt(Dc)
         vDiff = vDiff + vA
         edge = win(g.edge[eD], r)
@@ -365,19 +443,30 @@ def step(g: Grid, cur: dict, old: dict, dt: float, odt: float):
         gFv = [torch.zeros_like(fa) for _ in range(5)]
         dW = [torch.zeros_like(fa) for _ in range(5)]
         VaD = torch.zeros_like(fa)
+        if g.bg is not None:
+            B0f = [win(g.bg["fcB0"][x + 3 * D], r).to(fa.dtype) for x in range(3)]
+            B0n = (win(g.bg["bFlux0"][D], r) / win(A[D], r).double()).to(fa.dtype)
         for side, sgn in ((0, -1.0), (1, 1.0)):
             Wq = [Wlr[v][side] for v in range(5)]
             Bq = [Mag[x][side] for x in range(3)]
-            # MagKinFlux (stress.F90:513-599), no background, Boris off
+            # MagKinFlux (stress.F90:513-599), Boris off
             Dq, Pr = Wq[0], Wq[4]
             dPb = 0.5 * (Bq[0] * Bq[0] + Bq[1] * Bq[1] + Bq[2] * Bq[2])
-            Va2 = 2.0 * dPb / Dq
+            if g.bg is not None:
+                sx, sy, sz = Bq[0] + B0f[0], Bq[1] + B0f[1], Bq[2] + B0f[2]
+                Va2 = (sx * sx + sy * sy + sz * sz) / Dq
+            else:
+                Va2 = 2.0 * dPb / Dq
             Vn = T[0] * Wq[1] + T[1] * Wq[2] + T[2] * Wq[3]
             lam = 1.0 / (2.0 * Pr / Dq + Va2)
             Vn0 = 0.5 * torch.special.erfc(sgn * torch.sqrt(lam) * Vn)
             VaD = VaD + 0.5 * safe_sqrt(Va2)
             for x in range(3):
                 mFx[x] = mFx[x] + Vn0 * (dPb * T[x] - Bq[x] * Bn)
+            if g.bg is not None:
+                BdB0 = B0f[0] * Bq[0] + B0f[1] * Bq[1] + B0f[2] * Bq[2]
+                for x in range(3):
+                    mFx[x] = mFx[x] + Vn0 * (-(B0f[x] * Bn) - Bq[x] * B0n + BdB0 * T[x])
             # GasKinFlux (stress.F90:432-511)
             Vx, Vy, Vz = Wq[1], Wq[2], Wq[3]
             Eg = 0.5 * Dq * (Vx * Vx + Vy * Vy + Vz * Vz) + Pr / gm1
@@ -419,6 +508,8 @@ def step(g: Grid, cur: dict, old: dict, dt: float, odt: float):
         U.append(win(cur["Gas"][v], act) + dt * dGasH)
     dGasM = [(win(mF[0][x], act) - win(mF[0][x], act, (1, 0, 0)) + win(mF[1][x], act) - win(mF[1][x], act, (0, 1, 0)) +
               win(mF[2][x], act) - win(mF[2][x], act, (0, 0, 1))) / dV for x in range(3)]
+    if g.bg is not None:
+        dGasM = [dGasM[x] + win(g.bg["dpB0"][x], act).to(dV.dtype) for x in range(3)]
     # CellMaxwell (mhdgroup.F90:299-329)
     Dn = rmax(U[0], torch.full_like(U[0], P.dFloor))
     Mx, My, Mz, TotE = U[1], U[2], U[3], U[4]
@@ -428,12 +519,72 @@ def step(g: Grid, cur: dict, old: dict, dt: float, odt: float):
     KinE = 0.5 * (Mx * Mx + My * My + Mz * Mz) / Dn
     Gas = put(cur["Gas"], act, torch.stack([Dn, Mx, My, Mz, KinE + Pr / gm1]))
 
-    # --- EnforceBCs (periodic gather) and the final bFlux2Fld
+    # --- EnforceBCs: inner sphere and solar wind in place, then the gathers
+    # (periodic, zero-gradient J), then the final bFlux2Fld
+    if P.bc[0] == 3 or P.bc[1] == 4:
+        Gas, mfn = _iside_bcs(g, Gas, mfn, g.bxyz(mfn))
     shp = Gas.shape
     Gas = Gas.reshape(5, -1)[:, g.bc_src[-1]].reshape(shp)
     mfs = mfn.reshape(3, -1)
     mfn = torch.stack([mfs[d][g.bc_src[d]] for d in range(3)]).reshape(mfn.shape)
     return {"Gas": Gas, "mf": mfn, "B": g.bxyz(mfn)}
+
+
+def _iside_bcs(g: Grid, Gas, mf, B):
+    """SphIn (bcs.F90:934-957) and the constant-wind WindBC (apps/wind.F90:206-374)
+    on the 4 ghost layers of each I side; B is the Bxyz of the updated state."""
+    P = g.P
+    Ni, Nj, Nk = g.Ni, g.Nj, g.Nk
+    ip = G + P.Nip - 1
+    cellsJK = (slice(0, Nk), slice(0, Nj))
+    if P.bc[0] == 3:
+        gsrc = Gas[:, :Nk, :Nj, G].clone()
+        fsrc = mf[:, :Nk, :Nj, G].clone()
+        Gas = Gas.clone()
+        mf = mf.clone()
+        for n in range(1, 5):
+            Gas[:, :Nk, :Nj, G - n] = gsrc
+            mf[:, :Nk, :Nj, G - n] = fsrc
+    if P.bc[1] == 4:
+        W = g.wind
+        w = W["state"]
+        gC = [Gas[v][cellsJK + (ip,)] for v in range(5)]
+        Bin = [B[x][cellsJK + (ip,)] for x in range(3)]
+        gW_in = cell_c2p(P, gC)
+        # Con2Fast (gamutils.F90:238-269)
+        rho = rmax(gC[0], torch.full_like(gC[0], P.dFloor))
+        Vx, Vy, Vz = gC[1] / rho, gC[2] / rho, gC[3] / rho
+        KinE = 0.5 * rho * (Vx * Vx + Vy * Vy + Vz * Vz)
+        Pr = rmax((P.gamma - 1) * (gC[4] - KinE), torch.full_like(rho, P.pFloor))
+        Cs = torch.sqrt(P.gamma * Pr / rho)
+        MagB = safe_sqrt(Bin[0] * Bin[0] + Bin[1] * Bin[1] + Bin[2] * Bin[2])
+        Va = MagB / torch.sqrt(gC[0])
+        Cx = torch.sqrt(Cs * Cs + Va * Va)
+        nH = [g.Tf[q][cellsJK + (ip + 1,)] for q in range(3)]
+        V = [gW_in[1], gW_in[2], gW_in[3]]
+        dn = V[0] * nH[0] + V[1] * nH[1] + V[2] * nH[2]
+        fix = dn < Cx  # MinMach = 1
+        V = [torch.where(fix, V[x] - dn * nH[x] + Cx * nH[x], V[x]) for x in range(3)]
+        fin = [mf[0, :, :, ip + 1].clone(), mf[1, :, :, ip].clone(), mf[2, :, :, ip].clone()]
+        Gas = Gas.clone()
+        mf = mf.clone()
+        for n in range(1, 5):
+            wSW = W["wC"][:, :, n - 1]
+            wMHD = 1.0 - wSW
+            sw = (wSW > TINY).to(wSW.dtype)
+            mh = (wMHD > TINY).to(wSW.dtype)
+            gW_sw = [sw * w[0], sw * w[2], sw * w[3], sw * w[4], sw * w[1]]
+            gWi = [mh * gW_in[0], mh * V[0], mh * V[1], mh * V[2], mh * gW_in[4]]
+            gW = [wSW * gW_sw[v] + wMHD * gWi[v] for v in range(5)]
+            gCn = cell_p2c(P, gW)
+            for v in range(5):
+                Gas[v, :Nk, :Nj, ip + n] = gCn[v]
+            wI = W["wF0"][:, :, n - 1]
+            mf[0, :, :, ip + n + 1] = wI * W["sF0"][:, :, n - 1] + (1.0 - wI) * fin[0]
+            for d in (1, 2):
+                wd = W[f"wF{d}"][:, :, n - 1]
+                mf[d, :, :, ip + n] = wd * W[f"sF{d}"][:, :, n - 1] + (1.0 - wd) * fin[d]
+    return Gas, mf
 
 
 def run(g: Grid, cur: dict, old: dict, dt: float, nsteps: int, odt0: float | None = None):
@@ -457,14 +608,17 @@ def loss_b2(g: Grid, state: dict, lo=0.6, hi=0.8):
     return ((B * B).sum(dim=0) * m).sum()
 
 
-def loss_and_grad(g: Grid, Gas0, mf0, dt: float, nsteps: int, seg: int | None = None, lossf=loss_b2):
+def loss_and_grad(g: Grid, Gas0, mf0, dt: float, nsteps: int, seg: int | None = None, lossf=loss_b2,
+                  per_step: bool = False):
     """Loss after nsteps from the start State = oState = (Gas0, mf0, bxyz(mf0))
     (otime = time - dt) and its gradient w.r.t. Gas0 and mf0.
 
     Checkpointing: the forward sweep keeps only the (State, oState) pair at the
     start of each segment of seg steps (default ~sqrt(nsteps)); the reverse
-    sweep recomputes one segment at a time with autograd and carries the
-    adjoint of the pair backwards."""
+    sweep recomputes one segment at a time and carries the adjoint of the pair
+    backwards. per_step: within a segment, recompute and store the states
+    without a graph, then differentiate one step at a time (two-level
+    checkpointing: memory of one step's graph plus seg states)."""
     seg = seg or max(1, int(round(nsteps ** 0.5)))
     with torch.no_grad():
         cur = {"Gas": Gas0, "mf": mf0, "B": g.bxyz(mf0)}
@@ -476,38 +630,50 @@ def loss_and_grad(g: Grid, Gas0, mf0, dt: float, nsteps: int, seg: int | None = 
             m = min(seg, nsteps - n)
             cur, old = run(g, cur, old, dt, m)
             n += m
-    # reverse sweep
+        del cur, old
     lam_cur = lam_old = None
     loss_val = None
     for idx in range(len(ckpt) - 1, -1, -1):
-        n0, c0, o0 = ckpt[idx]
+        n0, c0, o0 = ckpt.pop()
         m = min(seg, nsteps - n0)
-        first = n0 == 0
-        if first:
-            G0 = Gas0.detach().clone().requires_grad_(True)
-            F0 = mf0.detach().clone().requires_grad_(True)
-            c = {"Gas": G0, "mf": F0, "B": g.bxyz(F0)}
-            o = c
-            leaves = [G0, F0]
+        if per_step:
+            sts = [(c0, o0)]
+            with torch.no_grad():
+                c, o = c0, o0
+                for _ in range(m - 1):
+                    c, o = run(g, c, o, dt, 1)
+                    sts.append((c, o))
+            units = [(n0 + k, sts[k][0], sts[k][1], 1) for k in range(m - 1, -1, -1)]
         else:
-            c = {k: v.detach().clone().requires_grad_(True) for k, v in c0.items()}
-            o = {k: v.detach().clone().requires_grad_(True) for k, v in o0.items()}
-            leaves = [c[k] for k in ("Gas", "mf", "B")] + [o[k] for k in ("Gas", "mf", "B")]
-        with torch.enable_grad():
-            ce, oe = run(g, c, o, dt, m)
-            if lam_cur is None:
-                L = lossf(g, ce)
-                loss_val = float(L.detach())
-                outs, grads = [L], [torch.ones_like(L)]
+            units = [(n0, c0, o0, m)]
+        for ns, cs, os_, mm in units:
+            first = ns == 0
+            if first:
+                G0 = Gas0.detach().clone().requires_grad_(True)
+                F0 = mf0.detach().clone().requires_grad_(True)
+                c = {"Gas": G0, "mf": F0, "B": g.bxyz(F0)}
+                o = c
+                leaves = [G0, F0]
             else:
-                outs, grads = [], []
-                for k in ("Gas", "mf", "B"):
-                    outs += [ce[k], oe[k]]
-                    grads += [lam_cur[k], lam_old[k]]
-            gl = torch.autograd.grad(outs, leaves, grads, allow_unused=True)
-        gl = [torch.zeros_like(x) if gv is None else gv for x, gv in zip(leaves, gl)]
-        if first:
-            return loss_val, gl[0], gl[1]
-        lam_cur = dict(zip(("Gas", "mf", "B"), gl[:3]))
-        lam_old = dict(zip(("Gas", "mf", "B"), gl[3:]))
+                c = {k: v.detach().clone().requires_grad_(True) for k, v in cs.items()}
+                o = {k: v.detach().clone().requires_grad_(True) for k, v in os_.items()}
+                leaves = [c[k] for k in ("Gas", "mf", "B")] + [o[k] for k in ("Gas", "mf", "B")]
+            with torch.enable_grad():
+                ce, oe = run(g, c, o, dt, mm)
+                if lam_cur is None:
+                    L = lossf(g, ce)
+                    loss_val = float(L.detach())
+                    outs, grads = [L], [torch.ones_like(L)]
+                else:
+                    outs, grads = [], []
+                    for k in ("Gas", "mf", "B"):
+                        outs += [ce[k], oe[k]]
+                        grads += [lam_cur[k], lam_old[k]]
+                gl = torch.autograd.grad(outs, leaves, grads, allow_unused=True)
+            gl = [torch.zeros_like(x) if gv is None else gv for x, gv in zip(leaves, gl)]
+            del ce, oe, outs, grads, c, o
+            if first:
+                return loss_val, gl[0], gl[1]
+            lam_cur = dict(zip(("Gas", "mf", "B"), gl[:3]))
+            lam_old = dict(zip(("Gas", "mf", "B"), gl[3:]))
     raise AssertionError("unreachable")

@@ -69,3 +69,35 @@ def test_gradient_checkpointing_and_finite_differences(oracle_built):
     fd = (Lf(Gas0 + eps * vG, mf0 + eps * vF) - Lf(Gas0 - eps * vG, mf0 - eps * vF)) / (2 * eps)
     ad = float((gG * vG).sum() + (gF * vF).sum())
     assert abs(fd - ad) <= 1e-6 * abs(ad), (fd, ad)
+
+
+def test_per_step_checkpointing_matches(oracle_built):
+    N, dt, nst = (12, 12, 12), 1e-3, 5
+    o, g = _setup(N, dt)
+    Gas0 = g.cell_box(o.array("Gas"))
+    mf0 = g.face_box(o.array("magFlux"))
+    L, gG, gF = loss_and_grad(g, Gas0, mf0, dt, nst, seg=2)
+    L2, gG2, gF2 = loss_and_grad(g, Gas0, mf0, dt, nst, seg=2, per_step=True)
+    assert L == L2 and torch.equal(gG, gG2) and torch.equal(gF, gF2)
+
+
+def test_dipole_wind_forward_matches_oracle(oracle_built):
+    """Background field, inner sphere, solar wind and zero-gradient J in the
+    PyTorch step: 5 steps equal the oracle to <= 1e-14 relative."""
+    from mage_b200 import dipole
+    bcs = (3, 4, 2, 2, 0, 0)
+    N, dt = (16, 8, 8), 5e-6
+    w = dipole.wind_code_units()
+    o = Oracle(OracleParams(*N, doBackground=True, M0=dipole.M0, wind=w, bc=bcs, fixedTimestep=True, fixedDT=dt),
+               grids.spherical_corners(*N), "strict")
+    o.ic_dipole_wind(0.01, 31337)
+    assert o.init_finish() == 0
+    sc = o.scalars()
+    g = Grid(DiffParams(*N, bc=bcs), {n: o.array(GEO_FROM_ORACLE[n]) for n in GEO_FROM_ORACLE},
+             background={k: o.array(k) for k in ("fcB0", "bFlux0", "edgB0", "B0", "dpB0")}, wind=w)
+    c5, _ = run(g, _state(g, o), _state(g, o, old=True), dt, 5, odt0=sc["time"] - sc["otime"])
+    assert o.step(5) == 0
+    for name, t, ref in (("Gas", c5["Gas"], o.array("Gas")), ("mf", c5["mf"], o.array("magFlux")),
+                         ("B", c5["B"], o.array("Bxyz"))):
+        a = t.numpy()[:, :ref.shape[1], :ref.shape[2], :ref.shape[3]]
+        assert np.abs(a - ref).max() <= 1e-14 * np.abs(ref).max(), name
