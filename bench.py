@@ -149,95 +149,6 @@ def cpu_sample(g, w, params, budget_s=12.0, max_steps=6):
                                       f"oracle -O3 -march=native -ffast-math, OpenMP"}
 
 
-def adjoint_section(N=(64, 64, 64), nsteps=20, sigma=1e-3, seed=2024):
-    """Differentiation form on the curvilinear blast wave: loss = sum of |B|^2
-    over cells centred in [0.6, 0.8]^3 after nsteps fixed-dt steps from the
-    blast-wave start with seeded Gaussian noise (relative sigma on rho and P,
-    absolute on v, sigma x face area on the face fluxes); gradient w.r.t. the start Gas and fluxes by
-    the checkpointed reverse mode of mage_b200.diffstep, FP64 and FP32, and a
-    central difference of the CUDA forward along a random direction."""
-    import torch
-    from mage_b200.diffstep import DiffParams, Grid, loss_and_grad, loss_b2, cell_c2p, cell_p2c
-    from mage_b200.gamera import GameraGPU, GamParams
-    xyz = grids_mod().warped_periodic_corners(*N)
-    g0 = GameraGPU(GamParams(*N))
-    g0.set_geometry(xyz)
-    g0.init_blast_wave()
-    dt = 0.5 * g0.download_state(old=False)["dt"]
-    st = g0.download_state(old=False)
-    geo = g0.get_geometry_arrays()
-    del g0
-    gpu = GameraGPU(GamParams(*N, fixedTimestep=dt))
-    gpu.set_geometry(xyz)
-    rng = np.random.default_rng(seed)
-    out = {"workload": f"curvilinear blast wave {N[0]}x{N[1]}x{N[2]}, {nsteps} fixed-dt steps, loss = sum |B|^2 "
-                       "over cells centred in [0.6,0.8]^3, gradient w.r.t. the start Gas and face fluxes",
-           "impl": "PyTorch reverse mode of the step restatement (mage_b200.diffstep), checkpoint every "
-                   f"{max(1, int(round(nsteps ** 0.5)))} steps"}
-    grads = {}
-    for name, dtype in (("fp64", torch.float64), ("fp32", torch.float32)):
-        g = Grid(DiffParams(*N), geo, dtype=dtype, device="cuda")
-        if name == "fp64":
-            W = cell_c2p(g.P, list(torch.as_tensor(st["Gas"], device="cuda")))
-
-            def noise():
-                return torch.as_tensor(rng.standard_normal(W[0].shape), device="cuda")
-
-            W = [W[0] * (1 + sigma * noise()), W[1] + sigma * noise(), W[2] + sigma * noise(), W[3] + sigma * noise(),
-                 W[4] * (1 + sigma * noise())]
-            Gas0 = g.cell_box(torch.stack(cell_p2c(g.P, W)))
-            # flux noise of sigma in field units: sigma * face area
-            mf0 = g.face_box(st["magFlux"]) + sigma * g.face * torch.as_tensor(rng.standard_normal(g.face.shape),
-                                                                             device="cuda")
-            Gas64, mf64 = Gas0, mf0
-        else:
-            Gas0, mf0 = Gas64.float(), mf64.float()
-        torch.cuda.synchronize()
-        torch.cuda.reset_peak_memory_stats()
-        t0 = time.perf_counter()
-        L, gG, gF = loss_and_grad(g, Gas0, mf0, dt, nsteps)
-        torch.cuda.synchronize()
-        el = time.perf_counter() - t0
-        out[name] = {"loss": L, "fwd_plus_adjoint_s": el,
-                     "peak_hbm_gb": torch.cuda.max_memory_allocated() / 1e9}
-        grads[name] = (gG.double(), gF.double())
-        del g
-    num = (grads["fp32"][0] - grads["fp64"][0]).norm() ** 2 + (grads["fp32"][1] - grads["fp64"][1]).norm() ** 2
-    den = grads["fp64"][0].norm() ** 2 + grads["fp64"][1].norm() ** 2
-    out["fp32_grad_rel_l2_vs_fp64"] = float((num / den).sqrt())
-    # central difference of the CUDA forward (product build) along a random direction
-    g = Grid(DiffParams(*N), geo, device="cuda")
-    vG = torch.as_tensor(rng.standard_normal(Gas64.shape), device="cuda") * Gas64.abs()
-    vF = torch.as_tensor(rng.standard_normal(mf64.shape), device="cuda")
-
-    def cuda_loss(Gx, Fx):
-        with torch.no_grad():
-            B = g.bxyz(Fx)
-        Nk, Nj, Ni = g.Nk, g.Nj, g.Ni
-        Gas = np.ascontiguousarray(Gx[:, :Nk, :Nj, :Ni].cpu().numpy())
-        mf = np.ascontiguousarray(Fx.cpu().numpy())
-        Bx = np.ascontiguousarray(B[:, :Nk, :Nj, :Ni].cpu().numpy())
-        gpu.upload_state(Gas, mf, Bx, Gas, mf, 0.0, -dt, dt, 0)
-        gpu.step_gamera(nsteps)
-        return float(loss_b2(g, {"B": g.cell_box(gpu.download_state(old=False)["Bxyz"])}))
-
-    # the limiter's kinks make the central difference converge to the reverse
-    # mode linearly in eps (a kink crossed inside +-eps adds a jump term)
-    ad = float((grads["fp64"][0] * vG).sum() + (grads["fp64"][1] * vF).sum())
-    out["fd_check"] = {"reverse_mode": ad, "central_difference_cuda": {}, "rel_err": {}}
-    for eps in (1e-8, 1e-10):
-        fd = (cuda_loss(Gas64 + eps * vG, mf64 + eps * vF) - cuda_loss(Gas64 - eps * vG, mf64 - eps * vF)) / (2 * eps)
-        out["fd_check"]["central_difference_cuda"][f"{eps:g}"] = fd
-        out["fd_check"]["rel_err"][f"{eps:g}"] = abs(fd - ad) / abs(ad)
-    out["cuda_forward_loss"] = cuda_loss(Gas64, mf64)
-    return out
-
-
-def grids_mod():
-    from mage_b200 import grids
-    return grids
-
-
 def run_reference(args):
     """CPU restatement of the reference step on all host threads (rank 0)."""
     rank, _, world = env_rank()
@@ -428,7 +339,8 @@ def main():
 
     adj = None
     if not args.no_adjoint and rank == 0:
-        adj = adjoint_section()
+        from mage_b200.diffbench import c4
+        adj = c4()
 
     peak, peak_kind = measured_peak()
     bpc = BYTES_PER_CELL_B0 if w["problem"] == "dipole" else BYTES_PER_CELL

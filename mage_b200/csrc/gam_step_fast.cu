@@ -1,6 +1,7 @@
 // Step kernels of the product path (FMA contraction on): FP64 drop-in form
 // and FP32 precision form.
 #define GAM_NS gam_fast
+#define GAM_CUDA_MATH 1
 #include "gam_step_impl.cuh"
 
 void gam_fast_step_f64(const Ctx<double>& C, int cur, cudaStream_t s) { gam_fast::launch_step<double>(C, cur, s); }

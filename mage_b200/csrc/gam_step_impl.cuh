@@ -75,8 +75,15 @@ template <class R> __device__ __forceinline__ R Rc(double x) { return (R)x; }
 
 template <class R> struct Mth;
 template <> struct Mth<double> {
+#ifdef GAM_CUDA_MATH
+    // product build: CUDA's erfc/exp (a few ulp, like libm's, and cheaper)
+    static __device__ __forceinline__ double erfc_(double x) { return erfc(x); }
+    static __device__ __forceinline__ double exp_(double x) { return exp(x); }
+#else
+    // strict build: the self-written erfc/exp shared with the CPU restatement
     static __device__ __forceinline__ double erfc_(double x) { return gam::gam_erfc(x); }
     static __device__ __forceinline__ double exp_(double x) { return gam::gam_exp(x); }
+#endif
     static __device__ __forceinline__ double sqrt_(double x) { return sqrt(x); }
 };
 template <> struct Mth<float> {
@@ -1135,6 +1142,7 @@ template <class R, class F> void for_each_kernel(const Ctx<R>& C, int cur, cudaS
     const int G = GAM_NG;
     const StateBuf<R> S = C.st[cur], O = C.st[1 - cur];
     const dim3 blk(32, 4, 1);
+    const dim3 sblk(16, 8, 1);  // flux kernels: 8 rows per block for the J-direction stencil reuse
     const Range all{0, b.Ni, 0, b.Nj, 0, b.Nk};
     const Range cells{0, b.Ni - 1, 0, b.Nj - 1, 0, b.Nk - 1};
     const int kke = C.P.do25D ? G : G + b.Nkp - 1;  // last active k of the stress sweep
@@ -1166,10 +1174,10 @@ template <class R, class F> void for_each_kernel(const Ctx<R>& C, int cur, cudaS
         constexpr int D = decltype(Dc)::value;
         const Range& r = fr[D];
         switch (C.kvar & 3) {
-            case 1: k_stress<R, D, 1><<<grid_for(r, blk), blk, 0, s>>>(b, C.P, C.g, Blim, C.w, r, C.sc); break;
-            case 2: k_stress<R, D, 7><<<grid_for(r, blk), blk, 0, s>>>(b, C.P, C.g, Blim, C.w, r, C.sc); break;
-            case 3: k_stress<R, D, 8><<<grid_for(r, blk), blk, 0, s>>>(b, C.P, C.g, Blim, C.w, r, C.sc); break;
-            default: k_stress<R, D, 6><<<grid_for(r, blk), blk, 0, s>>>(b, C.P, C.g, Blim, C.w, r, C.sc); break;
+            case 1: k_stress<R, D, 1><<<grid_for(r, sblk), sblk, 0, s>>>(b, C.P, C.g, Blim, C.w, r, C.sc); break;
+            case 2: k_stress<R, D, 7><<<grid_for(r, sblk), sblk, 0, s>>>(b, C.P, C.g, Blim, C.w, r, C.sc); break;
+            case 3: k_stress<R, D, 8><<<grid_for(r, sblk), sblk, 0, s>>>(b, C.P, C.g, Blim, C.w, r, C.sc); break;
+            default: k_stress<R, D, 6><<<grid_for(r, sblk), sblk, 0, s>>>(b, C.P, C.g, Blim, C.w, r, C.sc); break;
         }
     };
     f(8, [&] { stress(std::integral_constant<int, 0>()); });

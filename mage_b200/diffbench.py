@@ -1,0 +1,177 @@
+"""Measurements of the differentiation form (one JSON line).
+
+  python -m mage_b200.diffbench c4            # 64^3 curvilinear blast wave, 20 steps
+  python -m mage_b200.diffbench c5 --steps 200  # 192x192x256 dipole in the wind
+
+c4: loss = sum of |B|^2 over the cells centred in [0.6, 0.8]^3 after N fixed-dt
+steps from the blast-wave start with seeded Gaussian noise (relative sigma on
+rho and P, absolute on v, sigma x face area on the face fluxes); gradient
+w.r.t. the start Gas and face fluxes in FP64 and FP32 (checkpoint every
+~sqrt(N) steps), and central differences of the CUDA product step and of the
+PyTorch forward along a random direction.
+
+c5: the dipole-in-wind set-up on the spherical 192x192x256 grid (background
+field, inner sphere, solar wind, zero-gradient axis); loss = sum of |Bxyz|^2
+(the field without the dipole) over active cells with r < 6; FP32 and FP64
+gradients with checkpoints every 14 steps and one step's graph at a time.
+
+Both report the time of forward + reverse sweep, peak device memory and the
+FP32 gradient's relative L2 distance from the FP64 one.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import time
+
+import numpy as np
+import torch
+
+from mage_b200 import dipole, grids
+from mage_b200.diffstep import DiffParams, Grid, cell_c2p, cell_p2c, loss_and_grad, loss_b2, run, win, G
+from mage_b200.gamera import GameraGPU, GamParams
+from mage_b200.workloads import DIPOLE_BCS
+
+
+def _fortran(g: Grid, Gx, Fx):
+    with torch.no_grad():
+        B = g.bxyz(Fx)
+    Nk, Nj, Ni = g.Nk, g.Nj, g.Ni
+    return (np.ascontiguousarray(Gx[:, :Nk, :Nj, :Ni].double().cpu().numpy()),
+            np.ascontiguousarray(Fx.double().cpu().numpy()),
+            np.ascontiguousarray(B[:, :Nk, :Nj, :Ni].double().cpu().numpy()))
+
+
+def _rel_l2(a, b):
+    num = sum(float((x.double() - y.double()).norm() ** 2) for x, y in zip(a, b))
+    den = sum(float(y.double().norm() ** 2) for y in b)
+    return (num / den) ** 0.5
+
+
+def _timed(fn):
+    torch.cuda.synchronize()
+    torch.cuda.reset_peak_memory_stats()
+    t0 = time.perf_counter()
+    out = fn()
+    torch.cuda.synchronize()
+    return out, time.perf_counter() - t0, torch.cuda.max_memory_allocated() / 1e9
+
+
+def c4(N=(64, 64, 64), nsteps=20, sigma=1e-3, seed=2024):
+    xyz = grids.warped_periodic_corners(*N)
+    g0 = GameraGPU(GamParams(*N))
+    g0.set_geometry(xyz)
+    g0.init_blast_wave()
+    st = g0.download_state(old=False)
+    dt = 0.5 * st["dt"]
+    geo = g0.get_geometry_arrays()
+    del g0
+    gpu = GameraGPU(GamParams(*N, fixedTimestep=dt))
+    gpu.set_geometry(xyz)
+    rng = np.random.default_rng(seed)
+    g = Grid(DiffParams(*N), geo, device="cuda")
+    W = cell_c2p(g.P, list(torch.as_tensor(st["Gas"], device="cuda")))
+
+    def noise(shape):
+        return torch.as_tensor(rng.standard_normal(shape), device="cuda")
+
+    sh = W[0].shape
+    W = [W[0] * (1 + sigma * noise(sh)), W[1] + sigma * noise(sh), W[2] + sigma * noise(sh), W[3] + sigma * noise(sh),
+         W[4] * (1 + sigma * noise(sh))]
+    Gas64 = g.cell_box(torch.stack(cell_p2c(g.P, W)))
+    mf64 = g.face_box(st["magFlux"]) + sigma * g.face * noise(g.face.shape)
+    out = {"config": f"curvilinear blast wave {N[0]}x{N[1]}x{N[2]}, {nsteps} fixed-dt steps (dt = {dt:.4g})",
+           "loss": "sum |B|^2 over cells centred in [0.6,0.8]^3", "wrt": "start Gas and face fluxes",
+           "impl": "PyTorch reverse mode of the step restatement (mage_b200.diffstep), checkpoint every "
+                   f"{max(1, int(round(nsteps ** 0.5)))} steps"}
+    grads = {}
+    for name, dtype in (("fp64", torch.float64), ("fp32", torch.float32)):
+        gg = g if dtype == torch.float64 else Grid(DiffParams(*N), geo, dtype=dtype, device="cuda")
+        (L, gG, gF), el, mem = _timed(lambda: loss_and_grad(gg, Gas64.to(dtype), mf64.to(dtype), dt, nsteps))
+        out[name] = {"loss": L, "fwd_plus_adjoint_s": el, "peak_hbm_gb": mem}
+        grads[name] = (gG, gF)
+    out["fp32_grad_rel_l2_vs_fp64"] = _rel_l2(grads["fp32"], grads["fp64"])
+    vG = noise(Gas64.shape) * Gas64.abs()
+    vF = noise(mf64.shape)
+    ad = float((grads["fp64"][0] * vG).sum() + (grads["fp64"][1] * vF).sum())
+
+    def cuda_loss(Gx, Fx):
+        Gas, mf, B = _fortran(g, Gx, Fx)
+        gpu.upload_state(Gas, mf, B, Gas, mf, 0.0, -dt, dt, 0)
+        gpu.step_gamera(nsteps)
+        return float(loss_b2(g, {"B": g.cell_box(gpu.download_state(old=False)["Bxyz"])}))
+
+    def torch_loss(Gx, Fx):
+        with torch.no_grad():
+            c = {"Gas": Gx, "mf": Fx, "B": g.bxyz(Fx)}
+            ce, _ = run(g, c, c, dt, nsteps)
+            return float(loss_b2(g, ce))
+
+    # the limiter's kinks make a central difference approach the reverse mode
+    # linearly in eps (each kink crossed inside +-eps adds a jump term)
+    fd = {"reverse_mode": ad, "cuda": {}, "torch": {}}
+    for eps in (1e-8, 1e-10):
+        for name, f in (("cuda", cuda_loss), ("torch", torch_loss)):
+            d = (f(Gas64 + eps * vG, mf64 + eps * vF) - f(Gas64 - eps * vG, mf64 - eps * vF)) / (2 * eps)
+            fd[name][f"{eps:g}"] = {"central_difference": d, "rel_err": abs(d - ad) / abs(ad)}
+    out["fd_check"] = fd
+    out["forward_loss_cuda_vs_torch"] = [cuda_loss(Gas64, mf64), torch_loss(Gas64, mf64)]
+    return out
+
+
+def c5(N=(192, 192, 256), nsteps=200, seg=14, precisions=("fp32", "fp64")):
+    w = dipole.wind_code_units()
+    xyz = grids.spherical_corners(*N)
+    gpu = GameraGPU(GamParams(*N, doBackground=True, bc=DIPOLE_BCS))
+    gpu.set_geometry(xyz)
+    gpu.set_background_dipole(dipole.M0)
+    gpu.init_dipole_wind(w)
+    st = gpu.download_state(old=False)
+    dt = 0.5 * st["dt"]
+    geo = gpu.get_geometry_arrays()
+    bg = gpu.get_background()
+    del gpu
+    P = DiffParams(*N, bc=DIPOLE_BCS)
+    out = {"config": f"dipole in a solar wind, spherical {N[0]}x{N[1]}x{N[2]}, {nsteps} fixed-dt steps (dt = {dt:.4g})",
+           "loss": "sum |Bxyz|^2 (field without the dipole) over active cells with r < 6",
+           "wrt": "start Gas and face fluxes",
+           "impl": f"PyTorch reverse mode (mage_b200.diffstep), checkpoint every {seg} steps, one step's graph at a time"}
+    grads = {}
+    for name in precisions:
+        dtype = torch.float64 if name == "fp64" else torch.float32
+        g = Grid(P, geo, background=bg, wind=w, dtype=dtype, device="cuda")
+        act = (G, G + N[0] - 1, G, G + N[1] - 1, G, G + N[2] - 1)
+        xc = win(g.xyzcc, act).double()
+        mask = ((xc * xc).sum(dim=0) < 36.0).to(dtype)
+
+        def lossf(gr, state):
+            B = win(state["B"], act)
+            return ((B * B).sum(dim=0) * mask).sum()
+
+        Gas0, mf0 = g.cell_box(st["Gas"]), g.face_box(st["magFlux"])
+        (L, gG, gF), el, mem = _timed(lambda: loss_and_grad(g, Gas0, mf0, dt, nsteps, seg=seg, lossf=lossf,
+                                                             per_step=True))
+        out[name] = {"loss": L, "fwd_plus_adjoint_s": el, "s_per_step": el / nsteps, "peak_hbm_gb": mem}
+        grads[name] = (gG.cpu(), gF.cpu())
+        del g, Gas0, mf0, gG, gF
+        torch.cuda.empty_cache()
+    if "fp32" in grads and "fp64" in grads:
+        out["fp32_grad_rel_l2_vs_fp64"] = _rel_l2(grads["fp32"], grads["fp64"])
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("config", choices=["c4", "c5"])
+    ap.add_argument("--steps", type=int, default=None)
+    ap.add_argument("--precisions", default="fp32,fp64")
+    a = ap.parse_args()
+    if a.config == "c4":
+        res = c4(nsteps=a.steps or 20)
+    else:
+        res = c5(nsteps=a.steps or 200, precisions=tuple(a.precisions.split(",")))
+    print(json.dumps(res), flush=True)
+
+
+if __name__ == "__main__":
+    main()
