@@ -43,8 +43,10 @@ void gam_geom_b0_dipole(const GamBox& b, const double* xyz, const double* face, 
                         double M0, double* fcB0, double* bFlux0, double* edgB0, double* B0, double* dpB0, double* fS,
                         cudaStream_t s);
 // diagnostics (gam_diag.cu)
-void gam_diag_divb(const GamBox& b, const double* mf, double* partial, double* out, cudaStream_t s);
-void gam_diag_divb_f(const GamBox& b, const float* mf, double* partial, double* out, cudaStream_t s);
+void gam_diag_divb(const GamBox& b, const double* mf, const double* bFlux0, double* partial, double* out,
+                   cudaStream_t s);
+void gam_diag_divb_f(const GamBox& b, const float* mf, const double* bFlux0, double* partial, double* out,
+                     cudaStream_t s);
 void gam_diag_totals(const GamBox& b, const double* Gas, const double* vol, double* partial, double* out,
                      cudaStream_t s);
 void gam_diag_totals_f(const GamBox& b, const float* Gas, const float* vol, double* partial, double* out,
@@ -627,10 +629,12 @@ extern "C" int gam_calc_dt(gam_handle* h, double* dt) {
 extern "C" int gam_divb(gam_handle* h, double* total) {
     if (!h || !total) return GAM_EINVAL;
     if (!h->haveState) return fail(h, GAM_ESTATE, "no state");
+    // DivB's total includes the background fluxes (doTot, gridutils.F90:749-753)
+    const double* b0 = (h->p.doBackground && h->haveBg) ? h->bg.bFlux0 : nullptr;
     if (h->f32)
-        gam_diag_divb_f(h->b, h->cf.st[h->cur].mf, h->partial, h->dres, h->s);
+        gam_diag_divb_f(h->b, h->cf.st[h->cur].mf, b0, h->partial, h->dres, h->s);
     else
-        gam_diag_divb(h->b, h->cd.st[h->cur].mf, h->partial, h->dres, h->s);
+        gam_diag_divb(h->b, h->cd.st[h->cur].mf, b0, h->partial, h->dres, h->s);
     CK(h, cudaMemcpyAsync(total, h->dres, 8, cudaMemcpyDeviceToHost, h->s));
     CK(h, cudaStreamSynchronize(h->s));
     return GAM_OK;

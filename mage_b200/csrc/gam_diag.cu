@@ -33,7 +33,9 @@ template <int NV> __device__ void block_sum(double (*sh)[NT], double* acc, doubl
         for (int v = 0; v < NV; v++) out[v] = sh[v][0];
 }
 
-template <class R> __global__ void k_divb(GamBox b, const R* __restrict__ mf, double* partial) {
+// bFlux0: background face fluxes (Model%doBackground) or null
+template <class R> __global__ void k_divb(GamBox b, const R* __restrict__ mf, const double* __restrict__ bFlux0,
+                                          double* partial) {
     __shared__ double sh[1][NT];
     const long n = (long)b.Nip * b.Njp * b.Nkp;
     const long fs = b.fs;
@@ -45,7 +47,13 @@ template <class R> __global__ void k_divb(GamBox b, const R* __restrict__ mf, do
         double dFi = (double)mf[c] - (double)mf[c + 1];
         double dFj = (double)mf[fs + c] - (double)mf[fs + c + b.sx];
         double dFk = (double)mf[2 * fs + c] - (double)mf[2 * fs + c + b.sk];
-        acc[0] += fabs(dFi + dFj + dFk);
+        double dFi0 = 0.0, dFj0 = 0.0, dFk0 = 0.0;
+        if (bFlux0) {
+            dFi0 = bFlux0[c] - bFlux0[c + 1];
+            dFj0 = bFlux0[fs + c] - bFlux0[fs + c + b.sx];
+            dFk0 = bFlux0[2 * fs + c] - bFlux0[2 * fs + c + b.sk];
+        }
+        acc[0] += fabs(dFi + dFj + dFk + dFi0 + dFj0 + dFk0);
     }
     block_sum<1>(sh, acc, partial + blockIdx.x);
 }
@@ -88,12 +96,14 @@ __global__ void k_min3(GamBox b, const double* __restrict__ dijk, double* dl) {
 
 int gam_diag_partials(const GamBox&) { return NB; }
 
-void gam_diag_divb(const GamBox& b, const double* mf, double* partial, double* out, cudaStream_t s) {
-    k_divb<double><<<NB, NT, 0, s>>>(b, mf, partial);
+void gam_diag_divb(const GamBox& b, const double* mf, const double* bFlux0, double* partial, double* out,
+                   cudaStream_t s) {
+    k_divb<double><<<NB, NT, 0, s>>>(b, mf, bFlux0, partial);
     k_final<1><<<1, NT, 0, s>>>(partial, out);
 }
-void gam_diag_divb_f(const GamBox& b, const float* mf, double* partial, double* out, cudaStream_t s) {
-    k_divb<float><<<NB, NT, 0, s>>>(b, mf, partial);
+void gam_diag_divb_f(const GamBox& b, const float* mf, const double* bFlux0, double* partial, double* out,
+                     cudaStream_t s) {
+    k_divb<float><<<NB, NT, 0, s>>>(b, mf, bFlux0, partial);
     k_final<1><<<1, NT, 0, s>>>(partial, out);
 }
 void gam_diag_totals(const GamBox& b, const double* Gas, const double* vol, double* partial, double* out,

@@ -262,29 +262,49 @@ __global__ void __launch_bounds__(256, MINB) k_predict(GamBox b, DevParams<R> P,
     const long c = lidx(b, ii, jj, kk);
     const R pdt = (R)sc->pdt, odt = (R)sc->odt;
     const bool isCell = ii < b.Ni && jj < b.Nj && kk < b.Nk;
+    // The state and work pointers may alias as far as the compiler knows, so
+    // every state load is issued before the first store.
+    R fQ[3], foQ[3], fA[3], Q[5], oQ[5], uQ[3], uoQ[3];
+    if (P.doMHD) {
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            fQ[d] = cur.mf[d * fs + c];
+            foQ[d] = old.mf[d * fs + c];
+            fA[d] = g.face[d * fs + c];
+        }
+    }
+    if (isCell) {
+#pragma unroll
+        for (int v = 0; v < 5; v++) {
+            Q[v] = cur.Gas[v * fs + c];
+            oQ[v] = old.Gas[v * fs + c];
+        }
+        if (P.doMHD) {
+            const long off[3] = {1, (long)b.sx, b.sk};
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                uQ[d] = cur.mf[d * fs + c + off[d]];
+                uoQ[d] = old.mf[d * fs + c + off[d]];
+            }
+        }
+    }
     R hm[3];
     if (P.doMHD) {
 #pragma unroll
         for (int d = 0; d < 3; d++) {
-            R Q = cur.mf[d * fs + c], oQ = old.mf[d * fs + c];
-            R dQ = (Q - oQ) / odt;
-            hm[d] = Q + pdt * dQ;  // ExtrapAB2
-            R A = g.face[d * fs + c];
+            R dQ = (fQ[d] - foQ[d]) / odt;
+            hm[d] = fQ[d] + pdt * dQ;  // ExtrapAB2
+            R A = fA[d];
             R Am = rmax(A, (R)TINY);
             R bh = hm[d] / Am;
             w.abh[d * fs + c] = A * bh;
             w.Bnf[d * fs + c] = hm[d] / A;
-            w.bn[d * fs + c] = P.doLFMLim ? Q / Am : bh;
+            w.bn[d * fs + c] = P.doLFMLim ? fQ[d] / Am : bh;
         }
     }
     if (!isCell) return;
     // PredictCell (mhdgroup.F90:528-562)
-    R Q[5], oQ[5], W[5], oW[5], pW[5], pQ[5];
-#pragma unroll
-    for (int v = 0; v < 5; v++) {
-        Q[v] = cur.Gas[v * fs + c];
-        oQ[v] = old.Gas[v * fs + c];
-    }
+    R W[5], oW[5], pW[5], pQ[5];
     cell_c2p(P, oQ, oW);
     cell_c2p(P, Q, W);
 #pragma unroll
@@ -311,13 +331,10 @@ __global__ void __launch_bounds__(256, MINB) k_predict(GamBox b, DevParams<R> P,
     if (P.doMHD) {
         // upper faces of this cell, recomputed with the same ExtrapAB2
         R up[3];
-        const long off[3] = {1, (long)b.sx, b.sk};
 #pragma unroll
         for (int d = 0; d < 3; d++) {
-            long cu = c + off[d];
-            R Qu = cur.mf[d * fs + cu], oQu = old.mf[d * fs + cu];
-            R dQ = (Qu - oQu) / odt;
-            up[d] = Qu + pdt * dQ;
+            R dQ = (uQ[d] - uoQ[d]) / odt;
+            up[d] = uQ[d] + pdt * dQ;
         }
         R B[3];
         cell_bxyz(b, g, c, hm[0], up[0], hm[1], up[1], hm[2], up[2], B);
@@ -354,13 +371,16 @@ __global__ void __launch_bounds__(256) k_mom2face(GamBox b, DevParams<R> P, Geo<
     for (int n = 0; n < 8; n++) vol[n] = g.vol[c + (n - 4) * s];
     R dV = rmax(central8(vol), (R)TINY);
     const R A = g.face[dT1 * fs + c];
+    R out[3];
 #pragma unroll
     for (int x = 0; x < 3; x++) {
         R q[8];
 #pragma unroll
         for (int n = 0; n < 8; n++) q[n] = w.VdV[x * fs + c + (n - 4) * s];
-        w.AVf[(x + 3 * eD) * fs + c] = A * (central8(q) / dV);
+        out[x] = A * (central8(q) / dV);
     }
+#pragma unroll
+    for (int x = 0; x < 3; x++) w.AVf[(x + 3 * eD) * fs + c] = out[x];
 }
 
 // EdgeLRs (fields.F90:288-362): flux of faces of direction a, stencil along b
@@ -654,8 +674,6 @@ __global__ void __launch_bounds__(128, MINB) k_update_cells(GamBox b, DevParams<
             const long sj = b.sx, sk = b.sk;
             cell_bxyz(b, g, c, nxt.mf[c], nxt.mf[c + 1], nxt.mf[fs + c], nxt.mf[fs + c + sj], nxt.mf[2 * fs + c],
                       nxt.mf[2 * fs + c + sk], Bc);
-#pragma unroll
-            for (int x = 0; x < 3; x++) nxt.B[x * fs + c] = Bc[x];
         }
         if (active) {
             const long sj = b.sx, sk = b.sk;
@@ -697,9 +715,8 @@ __global__ void __launch_bounds__(128, MINB) k_update_cells(GamBox b, DevParams<
 #pragma unroll
             for (int v = 0; v < 5; v++) U[v] = cur.Gas[v * fs + c];
         }
-#pragma unroll
-        for (int v = 0; v < 5; v++) nxt.Gas[v * fs + c] = U[v];
-        // dt range isDT..ieDT = is-1..ie+1 (init.F90:511-530, single domain)
+        // dt range isDT..ieDT = is-1..ie+1 (init.F90:511-530, single domain);
+        // evaluated before the stores so that none of its loads waits on them
         const bool indt = ii >= G - 1 && ii <= G + b.Nip && jj >= G - 1 && jj <= G + b.Njp && kk >= G - 1 &&
                           kk <= G + b.Nkp;
         if (indt && !sc->fixedTimestep) {
@@ -714,6 +731,12 @@ __global__ void __launch_bounds__(128, MINB) k_update_cells(GamBox b, DevParams<
             double dtc = cell_dt(P, Ud, Bt, (double)g.dl[c], gamma_d, gm1_d, sc->CFL);
             if (dtc > 0.0 && dtc < 1.0e300) mydt = dtc;  // finite positive
             else bad = true;
+        }
+#pragma unroll
+        for (int v = 0; v < 5; v++) nxt.Gas[v * fs + c] = U[v];
+        if (P.doMHD) {
+#pragma unroll
+            for (int x = 0; x < 3; x++) nxt.B[x * fs + c] = Bc[x];
         }
     }
     // block min
@@ -1152,7 +1175,7 @@ template <class R, class F> void for_each_kernel(const Ctx<R>& C, int cur, cudaS
         if (C.kvar & 8)
             k_predict<R, 1><<<grid_for(all, pblk), pblk, 0, s>>>(b, C.P, C.g, S, O, C.w, C.sc);
         else
-            k_predict<R, 4><<<grid_for(all, pblk), pblk, 0, s>>>(b, C.P, C.g, S, O, C.w, C.sc);
+            k_predict<R, sizeof(R) == 8 ? 3 : 4><<<grid_for(all, pblk), pblk, 0, s>>>(b, C.P, C.g, S, O, C.w, C.sc);
     });
     if (C.P.doMHD) {
         const Range mf[3] = {{0, b.Ni - 1, G, G + b.Njp, 0, b.Nk - 1},

@@ -108,9 +108,10 @@ def c4(N=(64, 64, 64), nsteps=20, sigma=1e-3, seed=2024):
             return float(loss_b2(g, ce))
 
     # the limiter's kinks make a central difference approach the reverse mode
-    # linearly in eps (each kink crossed inside +-eps adds a jump term)
+    # only as eps -> 0 (each kink crossed inside +-eps adds a jump term; on
+    # 64^3 the difference is 1e-2 at eps 1e-9 and 1e-5 at 1e-11)
     fd = {"reverse_mode": ad, "cuda": {}, "torch": {}}
-    for eps in (1e-8, 1e-10):
+    for eps in (1e-9, 1e-10, 1e-11):
         for name, f in (("cuda", cuda_loss), ("torch", torch_loss)):
             d = (f(Gas64 + eps * vG, mf64 + eps * vF) - f(Gas64 - eps * vG, mf64 - eps * vF)) / (2 * eps)
             fd[name][f"{eps:g}"] = {"central_difference": d, "rel_err": abs(d - ad) / abs(ad)}

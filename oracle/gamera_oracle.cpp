@@ -1879,7 +1879,13 @@ double orc_divb(void* h) {
                 double dFi = mf(i, j, k, IDIR) - mf(i + 1, j, k, IDIR);
                 double dFj = mf(i, j, k, JDIR) - mf(i, j + 1, k, JDIR);
                 double dFk = mf(i, j, k, KDIR) - mf(i, j, k + 1, KDIR);
-                tot = tot + std::fabs(dFi + dFj + dFk + 0.0 + 0.0 + 0.0);
+                double dFi0 = 0.0, dFj0 = 0.0, dFk0 = 0.0;
+                if (A->M.doBackground) {  // gridutils.F90:749-753 (doTot)
+                    dFi0 = G.bFlux0(i, j, k, IDIR) - G.bFlux0(i + 1, j, k, IDIR);
+                    dFj0 = G.bFlux0(i, j, k, JDIR) - G.bFlux0(i, j + 1, k, JDIR);
+                    dFk0 = G.bFlux0(i, j, k, KDIR) - G.bFlux0(i, j, k + 1, KDIR);
+                }
+                tot = tot + std::fabs(dFi + dFj + dFk + dFi0 + dFj0 + dFk0);
             }
     return tot;
 }

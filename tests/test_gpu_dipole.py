@@ -63,6 +63,8 @@ def test_dipole_wind_strict_is_bit_exact(oracle_built):
             assert np.array_equal(s[k], o.array(k)), (nst, k, rel_err(s[k], o.array(k)))
         sc = o.scalars()
         assert dt == sc["dt"] and t == sc["t"] and s["ts"] == sc["ts"]
+    # DivB with the background fluxes (gridutils.F90:717-770): same terms, another summation order
+    assert abs(g.divb() - o.divb()) <= 1e-12 * o.divb()
 
 
 def test_dipole_background_on_gpu(oracle_built):
