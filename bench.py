@@ -149,6 +149,78 @@ def cpu_sample(g, w, params, budget_s=12.0, max_steps=6):
                                       f"oracle -O3 -march=native -ffast-math, OpenMP"}
 
 
+def slab_main(args, w, rank, local, world, dist, barrier, max_over_ranks):
+    """N > 1 GPUs: the grid of N slabs of the workload's size stacked in k (weak
+    scaling: every GPU keeps a 192^3 slab), one slab per rank, halo exchange
+    over NCCL and a global dt every step (mage_b200.tiling)."""
+    import torch
+    from mage_b200 import grids
+    from mage_b200.tiling import Slabs
+    N = w["N"]
+    Ng = (N[0], N[1], N[2] * world)
+    cells = N[0] * N[1] * N[2]
+    sl = Slabs(Ng, grids.warped_periodic_corners(*Ng), world, comm="dist" if dist is not None else None,
+               strict=args.strict)
+    sl.step(args.warmup)
+    barrier()
+    clk = ClockSampler(local)
+    clk.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    sl.step(args.steps)
+    e1.record()
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    value = world * cells * args.steps / (ms / 1e3)
+    # e2e: each rank's slab through the C ABI from pinned host buffers
+    e2e_value, h2d, d2h = None, 0, 0
+    if args.e2e_steps > 0:
+        g = sl.apps[0]
+        st = g.download_state()
+        pin = {k: torch.from_numpy(np.ascontiguousarray(st[k])).pin_memory().numpy()
+               for k in ("Gas", "magFlux", "Bxyz", "oGas", "omagFlux")}
+        spare = {k: torch.from_numpy(np.empty_like(st[k])).pin_memory().numpy() for k in ("Gas", "magFlux", "Bxyz")}
+        h2d = sum(pin[k].nbytes for k in pin)
+        d2h = pin["Gas"].nbytes + pin["magFlux"].nbytes + pin["Bxyz"].nbytes
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            g.upload_state(pin["Gas"], pin["magFlux"], pin["Bxyz"], pin["oGas"], pin["omagFlux"], st["time"],
+                           st["otime"], st["dt"], st["ts"])
+            sl.step(1)
+            g.download_state(into=spare, old=False)
+        barrier()
+        e2e_value = world * cells * args.e2e_steps / max_over_ranks(time.perf_counter() - t0)
+    peak, peak_kind = measured_peak()
+    achieved = (cells * args.steps / (ms / 1e3)) * BYTES_PER_CELL["f64"] / 1e9
+    if rank == 0:
+        line = {
+            "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": w["desc"] + f", {world} slabs stacked in k: global {Ng[0]}x{Ng[1]}x{Ng[2]}",
+                       "grid": list(Ng), "precision": "FP64 drop-in",
+                       "parallelism": f"k-slabs x{world}, depth-4 halo exchange over NCCL, global dt each step",
+                       "l2": "inputs larger than L2 (~13 GB of state, metric and work arrays per GPU)"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_kind": peak_kind, "bytes_per_cell_update": BYTES_PER_CELL["f64"], "traffic": None,
+                         "unit_of_launch": "one step per GPU"},
+            "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "steps": args.e2e_steps,
+                    "what": "per step and rank: gam_upload_state of the slab from pinned host memory, one tiled step "
+                            "(halo exchange included), gam_download_state of the slab's State"},
+            "cpu_baseline": None,
+            "clocks": clocks,
+            "gpu_launches": 21 * args.steps,
+        }
+        print(json.dumps(line), flush=True)
+    del sl
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def run_reference(args):
     """CPU restatement of the reference step on all host threads (rank 0)."""
     rank, _, world = env_rank()
@@ -201,6 +273,8 @@ def main():
     ap.add_argument("--no-fp32", action="store_true")
     ap.add_argument("--no-dipole", action="store_true", help="skip the dipole-in-wind FP64/FP32 section")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the differentiation-form section")
+    ap.add_argument("--replicas", action="store_true", help="N>1: independent replicas instead of k-slabs")
+    ap.add_argument("--slabs", action="store_true", help="k-slab path also on one GPU (its halo sent to itself)")
     ap.add_argument("--strict", action="store_true", help="time the FP64 kernels built without FMA contraction")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -236,6 +310,9 @@ def main():
         t = torch.tensor([x], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
+
+    if (world > 1 or args.slabs) and w["problem"] == "bw" and not args.replicas:
+        return slab_main(args, w, rank, local, world, dist, barrier, max_over_ranks)
 
     # ---- FP64 drop-in: device-resident throughput
     g = make(0, args.strict)

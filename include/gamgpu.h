@@ -41,7 +41,8 @@ enum {
  * GAM_BC_SPHIN (bcs.F90:934-957); OUTI periodic, none or GAM_BC_WIND (constant
  * solar wind, apps/wind.F90:206-391); INJ/OUTJ periodic, none or
  * GAM_BC_ZEROGRAD (bcs.F90:853-892); INK/OUTK periodic or none. */
-enum { GAM_BC_PERIODIC = 0, GAM_BC_NONE = 1, GAM_BC_ZEROGRAD = 2, GAM_BC_SPHIN = 3, GAM_BC_WIND = 4 };
+enum { GAM_BC_PERIODIC = 0, GAM_BC_NONE = 1, GAM_BC_ZEROGRAD = 2, GAM_BC_SPHIN = 3, GAM_BC_WIND = 4,
+       GAM_BC_HALO = 5 /* INK and OUTK of a k-slab: filled by the caller's halo exchange */ };
 enum { GAM_RECON_8CENT = 0, GAM_RECON_7UP = 1 };
 enum { GAM_FP64 = 0, GAM_FP32 = 1 };
 
@@ -176,6 +177,37 @@ int gam_init_dipole_wind(gam_handle* h, const double wind[8], uint64_t seed, dou
  * which is HDF5; reading needs a handle of the same grid size. */
 int gam_write_restart(gam_handle* h, const char* path);
 int gam_read_restart(gam_handle* h, const char* path);
+
+/* k-slab tiling (the MPI step of gamAppMpi_T, gamapp_mpi.F90:495-782, for a
+ * decomposition along k; one handle per GPU, bc[4] = bc[5] = GAM_BC_HALO).
+ * A step is
+ *   gam_step_begin(h)                      predictor .. cell update
+ *   gam_dt_partial(h, &bits, &nbad)        this slab's dt candidate
+ *   (caller: min of bits and sum of nbad over all slabs, e.g. an NCCL
+ *    all-reduce; bits are the IEEE-754 bits of a positive double, so the
+ *    integer min is the double min)
+ *   gam_step_end(h, bits, nbad, &dt, &t)   dt decision, local boundaries
+ *   gam_halo_pack(h, 0|1, buf) / send / receive / gam_halo_unpack(h, 0|1, buf, 0)
+ * Side 0 of a pack is what goes down to the slab below (it fills that slab's
+ * side-1 ghosts), side 1 what goes up. Buffers are device memory of
+ * gam_halo_bytes bytes; pack and unpack return after their kernels finished.
+ * After a gam_init_*: exchange with copyB = 1 (Bxyz copied, like the first
+ * EnforceBCs), then gam_init_finish_halo (oState = State, this slab's CalcDT),
+ * min over slabs, gam_set_start(h, dt). With one slab that sends to itself the
+ * result equals the periodic single-domain step bit for bit. */
+/* Whether this slab is the lowest / highest in k: CalcDT's range (isDT..ieDT =
+ * is-1..ie+1, init.F90:511-530) takes the ghost layer below / above only on
+ * the grid's own edges, not where a neighbour's cells are. Call before the
+ * gam_init_* of the slab (default: both, as for the whole grid). */
+int gam_set_slab_edges(gam_handle* h, int32_t lowest, int32_t highest);
+int gam_halo_bytes(gam_handle* h, int64_t* bytes);
+int gam_halo_pack(gam_handle* h, int32_t side, void* dev_buf);
+int gam_halo_unpack(gam_handle* h, int32_t side, const void* dev_buf, int32_t copyB);
+int gam_init_finish_halo(gam_handle* h, double* dt_local);
+int gam_set_start(gam_handle* h, double dt);
+int gam_step_begin(gam_handle* h);
+int gam_dt_partial(gam_handle* h, uint64_t* dtmin_bits, int32_t* nbad);
+int gam_step_end(gam_handle* h, uint64_t dtmin_bits, int32_t nbad, double* dt, double* t);
 
 /* Conserved totals for callers that cannot allocate device memory.
  * No counterpart in the reference. Some callers cannot call cudaMalloc while

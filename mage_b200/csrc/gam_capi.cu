@@ -22,6 +22,12 @@ void gam_strict_profile_f64(const Ctx<double>& C, int cur, cudaStream_t s, int r
 void gam_fast_profile_f64(const Ctx<double>& C, int cur, cudaStream_t s, int reps, double* ms);
 void gam_fast_profile_f32(const Ctx<float>& C, int cur, cudaStream_t s, int reps, double* ms);
 void gam_fast_prepare_f64();
+void gam_fast_phase_f64(const Ctx<double>& C, int cur, cudaStream_t s, int phase);
+void gam_fast_phase_f32(const Ctx<float>& C, int cur, cudaStream_t s, int phase);
+void gam_strict_phase_f64(const Ctx<double>& C, int cur, cudaStream_t s, int phase);
+void gam_fast_halo_f64(const Ctx<double>& C, int cur, cudaStream_t s, int side, int unpack, int copyB, void* buf);
+void gam_fast_halo_f32(const Ctx<float>& C, int cur, cudaStream_t s, int side, int unpack, int copyB, void* buf);
+void gam_strict_halo_f64(const Ctx<double>& C, int cur, cudaStream_t s, int side, int unpack, int copyB, void* buf);
 void gam_fast_prepare_f32();
 // set-up (gam_geom.cu)
 void gam_geom_fortran_to_box_d(const GamBox& b, const double* src, double* dst, bool face, int nc, cudaStream_t s);
@@ -82,6 +88,7 @@ struct gam_handle {
     double* partial = nullptr;  // device, reduction partials
     double* dres = nullptr;     // device, reduction results
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    cudaGraphExec_t pgraph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [parity][phase] (k-slab steps)
     int cur = 0;
     bool haveGeo = false, haveState = false, haveXyz = false;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -138,6 +145,7 @@ template <class R> static void fill_dev_params(DevParams<R>& P, const gam_params
     P.doMHD = p.doMHD; P.doLFMLim = p.doLFMLim; P.do25D = p.do25D; P.doBackground = p.doBackground;
     P.up7 = p.rmeth == GAM_RECON_7UP;
     for (int n = 0; n < 6; n++) P.bc[n] = p.bc[n];
+    P.dtKlo = P.dtKhi = 1;
 }
 
 template <class R> static int alloc_bulk(gam_handle* h, Ctx<R>& C) {
@@ -208,12 +216,14 @@ extern "C" int gam_create(const gam_params* p, gam_handle** out) {
         auto in = [](int v, int a, int b2, int c2) { return v == a || v == b2 || v == c2; };
         if (!in(c[0], GAM_BC_PERIODIC, GAM_BC_NONE, GAM_BC_SPHIN) || !in(c[1], GAM_BC_PERIODIC, GAM_BC_NONE, GAM_BC_WIND) ||
             !in(c[2], GAM_BC_PERIODIC, GAM_BC_NONE, GAM_BC_ZEROGRAD) ||
-            !in(c[3], GAM_BC_PERIODIC, GAM_BC_NONE, GAM_BC_ZEROGRAD) || !in(c[4], GAM_BC_PERIODIC, GAM_BC_NONE, -1) ||
-            !in(c[5], GAM_BC_PERIODIC, GAM_BC_NONE, -1))
+            !in(c[3], GAM_BC_PERIODIC, GAM_BC_NONE, GAM_BC_ZEROGRAD) ||
+            !in(c[4], GAM_BC_PERIODIC, GAM_BC_NONE, GAM_BC_HALO) || !in(c[5], GAM_BC_PERIODIC, GAM_BC_NONE, GAM_BC_HALO))
             return bad(GAM_EINVAL, "unsupported boundary kind for this side");
         for (int d = 0; d < 3; d++)
             if ((c[2 * d] == GAM_BC_PERIODIC) != (c[2 * d + 1] == GAM_BC_PERIODIC))
                 return bad(GAM_EINVAL, "a periodic direction needs both sides periodic");
+        if ((c[4] == GAM_BC_HALO) != (c[5] == GAM_BC_HALO))
+            return bad(GAM_EINVAL, "a k-slab exchanges both k sides");
         if (c[0] == GAM_BC_PERIODIC && (c[2] == GAM_BC_ZEROGRAD || c[3] == GAM_BC_ZEROGRAD))
             return bad(GAM_EINVAL, "zero-gradient J with periodic I is not supported");
     }
@@ -279,8 +289,11 @@ extern "C" int gam_create(const gam_params* p, gam_handle** out) {
 extern "C" int gam_destroy(gam_handle* h) {
     if (!h) return GAM_EINVAL;
     if (h->s) cudaStreamSynchronize(h->s);
-    for (int q = 0; q < 2; q++)
+    for (int q = 0; q < 2; q++) {
         if (h->graph[q]) cudaGraphExecDestroy(h->graph[q]);
+        for (int ph = 0; ph < 2; ph++)
+            if (h->pgraph[q][ph]) cudaGraphExecDestroy(h->pgraph[q][ph]);
+    }
     for (void* p : h->allocs) cudaFree(p);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
@@ -495,6 +508,8 @@ extern "C" int gam_step(gam_handle* h, int32_t nsteps, double* dt, double* t) {
     if (!h->haveState) return fail(h, GAM_ESTATE, "gam_step before gam_upload_state");
     if (h->p.doBackground && !h->haveBg) return fail(h, GAM_ESTATE, "doBackground: set the background field first");
     if (h->p.bc[1] == GAM_BC_WIND && !h->haveWind) return fail(h, GAM_ESTATE, "wind boundary: call gam_set_wind first");
+    if (h->p.bc[4] == GAM_BC_HALO)
+        return fail(h, GAM_ESTATE, "a k-slab steps with gam_step_begin / gam_step_end and a halo exchange");
     int rc;
     if ((rc = ensure_graph(h, 0))) return rc;
     if ((rc = ensure_graph(h, 1))) return rc;
@@ -692,6 +707,9 @@ static int init_common(gam_handle* h, double* Gas64, double* mf64) {
     else
         gam_fast_init_f64(h->cd, 0, h->s);
     CK(h, cudaGetLastError());
+    // a k-slab's ghosts arrive with the first halo exchange; the caller
+    // finishes with gam_init_finish_halo and gam_set_start
+    if (h->p.bc[4] == GAM_BC_HALO) return GAM_OK;
     double dt;
     rc = gam_calc_dt(h, &dt);
     if (rc) return rc;
@@ -946,5 +964,142 @@ extern "C" int gam_read_restart(gam_handle* h, const char* path) {
     s.t = hd.t;
     s.dt0 = hd.dt0;
     CK(h, cudaMemcpy(h->sc, &s, sizeof(s), cudaMemcpyHostToDevice));
+    return GAM_OK;
+}
+
+// ------------------------------------------------------------ k-slab tiling
+static void launch_phase(gam_handle* h, int cur, int phase) {
+    if (h->f32)
+        gam_fast_phase_f32(h->cf, cur, h->s, phase);
+    else if (h->p.strict)
+        gam_strict_phase_f64(h->cd, cur, h->s, phase);
+    else
+        gam_fast_phase_f64(h->cd, cur, h->s, phase);
+}
+static int ensure_phase_graph(gam_handle* h, int cur, int phase) {
+    if (h->pgraph[cur][phase]) return GAM_OK;
+    cudaGraph_t g;
+    CK(h, cudaStreamBeginCapture(h->s, cudaStreamCaptureModeThreadLocal));
+    launch_phase(h, cur, phase);
+    CK(h, cudaStreamEndCapture(h->s, &g));
+    CK(h, cudaGraphInstantiate(&h->pgraph[cur][phase], g, 0));
+    cudaGraphDestroy(g);
+    return GAM_OK;
+}
+static int require_slab(gam_handle* h) {
+    if (h->p.bc[4] != GAM_BC_HALO) return fail(h, GAM_ESTATE, "the handle is not a k-slab (bc[4] = bc[5] = GAM_BC_HALO)");
+    if (!h->haveGeo || !h->haveState) return fail(h, GAM_ESTATE, "set the geometry and the state first");
+    return GAM_OK;
+}
+
+extern "C" int gam_halo_bytes(gam_handle* h, int64_t* bytes) {
+    if (!h || !bytes) return GAM_EINVAL;
+    *bytes = 11L * 4 * (h->b.Ni + 1) * (h->b.Nj + 1) * (h->f32 ? 4 : 8);
+    return GAM_OK;
+}
+
+static int halo_call(gam_handle* h, int side, int unpack, int copyB, void* buf) {
+    if (!h || !buf || (side != 0 && side != 1)) return GAM_EINVAL;
+    int rc = require_slab(h);
+    if (rc) return rc;
+    if (h->f32)
+        gam_fast_halo_f32(h->cf, h->cur, h->s, side, unpack, copyB, buf);
+    else if (h->p.strict)
+        gam_strict_halo_f64(h->cd, h->cur, h->s, side, unpack, copyB, buf);
+    else
+        gam_fast_halo_f64(h->cd, h->cur, h->s, side, unpack, copyB, buf);
+    CK(h, cudaGetLastError());
+    CK(h, cudaStreamSynchronize(h->s));
+    return GAM_OK;
+}
+extern "C" int gam_halo_pack(gam_handle* h, int32_t side, void* dev_buf) { return halo_call(h, side, 0, 0, dev_buf); }
+extern "C" int gam_halo_unpack(gam_handle* h, int32_t side, const void* dev_buf, int32_t copyB) {
+    return halo_call(h, side, 1, copyB ? 1 : 0, const_cast<void*>(dev_buf));
+}
+
+extern "C" int gam_init_finish_halo(gam_handle* h, double* dt_local) {
+    if (!h || !dt_local) return GAM_EINVAL;
+    int rc = require_slab(h);
+    if (rc) return rc;
+    const long fs = h->b.fs;
+    const size_t w = h->f32 ? 4 : 8;
+    void* S[3] = {h->f32 ? (void*)h->cf.st[h->cur].Gas : (void*)h->cd.st[h->cur].Gas,
+                  h->f32 ? (void*)h->cf.st[h->cur].mf : (void*)h->cd.st[h->cur].mf,
+                  h->f32 ? (void*)h->cf.st[h->cur].B : (void*)h->cd.st[h->cur].B};
+    void* O[3] = {h->f32 ? (void*)h->cf.st[1 - h->cur].Gas : (void*)h->cd.st[1 - h->cur].Gas,
+                  h->f32 ? (void*)h->cf.st[1 - h->cur].mf : (void*)h->cd.st[1 - h->cur].mf,
+                  h->f32 ? (void*)h->cf.st[1 - h->cur].B : (void*)h->cd.st[1 - h->cur].B};
+    const long nc[3] = {5, 3, 3};
+    for (int q = 0; q < 3; q++) CK(h, cudaMemcpyAsync(O[q], S[q], nc[q] * fs * w, cudaMemcpyDeviceToDevice, h->s));
+    return gam_calc_dt(h, dt_local);
+}
+
+extern "C" int gam_set_start(gam_handle* h, double dt) {
+    if (!h) return GAM_EINVAL;
+    return set_scalars(h, 0.0, -dt, dt, 0);
+}
+
+extern "C" int gam_step_begin(gam_handle* h) {
+    if (!h) return GAM_EINVAL;
+    int rc = require_slab(h);
+    if (rc) return rc;
+    GamScalars s;
+    CK(h, cudaMemcpyAsync(&s, h->sc, sizeof(s), cudaMemcpyDeviceToHost, h->s));
+    CK(h, cudaStreamSynchronize(h->s));
+    if (s.halted) return fail(h, s.status == 5 ? GAM_EDT_DISASTER : GAM_EDT_BAD, "a previous step failed CalcDT");
+    if ((rc = ensure_phase_graph(h, h->cur, 0))) return rc;
+    if ((rc = ensure_phase_graph(h, h->cur, 1))) return rc;
+    CK(h, cudaEventRecord(h->ev0, h->s));
+    CK(h, cudaGraphLaunch(h->pgraph[h->cur][0], h->s));
+    return GAM_OK;
+}
+
+extern "C" int gam_dt_partial(gam_handle* h, uint64_t* dtmin_bits, int32_t* nbad) {
+    if (!h || !dtmin_bits || !nbad) return GAM_EINVAL;
+    GamScalars s;
+    CK(h, cudaMemcpyAsync(&s, h->sc, sizeof(s), cudaMemcpyDeviceToHost, h->s));
+    CK(h, cudaStreamSynchronize(h->s));
+    *dtmin_bits = s.dtmin_bits;
+    *nbad = s.nbad;
+    return GAM_OK;
+}
+
+extern "C" int gam_step_end(gam_handle* h, uint64_t dtmin_bits, int32_t nbad, double* dt, double* t) {
+    if (!h) return GAM_EINVAL;
+    int rc = require_slab(h);
+    if (rc) return rc;
+    unsigned long long bits = dtmin_bits;
+    int nb = nbad;
+    CK(h, cudaMemcpyAsync(&h->sc->dtmin_bits, &bits, sizeof(bits), cudaMemcpyHostToDevice, h->s));
+    CK(h, cudaMemcpyAsync(&h->sc->nbad, &nb, sizeof(nb), cudaMemcpyHostToDevice, h->s));
+    CK(h, cudaGraphLaunch(h->pgraph[h->cur][1], h->s));
+    CK(h, cudaEventRecord(h->ev1, h->s));
+    GamScalars s;
+    CK(h, cudaMemcpyAsync(&s, h->sc, sizeof(s), cudaMemcpyDeviceToHost, h->s));
+    CK(h, cudaStreamSynchronize(h->s));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+    h->lastMs = ms;
+    h->cur ^= 1;
+    if (dt) *dt = s.dt;
+    if (t) *t = s.t;
+    if (s.halted)
+        return fail(h, s.status == 5 ? GAM_EDT_DISASTER : GAM_EDT_BAD,
+                    s.status == 5 ? "CalcDT: timestep too small or not finite" : "CalcDT: timestep dropped 10x or below limDT0");
+    return GAM_OK;
+}
+
+extern "C" int gam_set_slab_edges(gam_handle* h, int32_t lowest, int32_t highest) {
+    if (!h) return GAM_EINVAL;
+    if (h->p.bc[4] != GAM_BC_HALO) return fail(h, GAM_ESTATE, "the handle is not a k-slab");
+    h->cd.P.dtKlo = h->cf.P.dtKlo = lowest ? 1 : 0;
+    h->cd.P.dtKhi = h->cf.P.dtKhi = highest ? 1 : 0;
+    drop_graphs(h);
+    for (int q = 0; q < 2; q++)
+        for (int ph = 0; ph < 2; ph++)
+            if (h->pgraph[q][ph]) {
+                cudaGraphExecDestroy(h->pgraph[q][ph]);
+                h->pgraph[q][ph] = nullptr;
+            }
     return GAM_OK;
 }

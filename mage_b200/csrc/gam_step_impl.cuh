@@ -717,8 +717,8 @@ __global__ void __launch_bounds__(128, MINB) k_update_cells(GamBox b, DevParams<
         }
         // dt range isDT..ieDT = is-1..ie+1 (init.F90:511-530, single domain);
         // evaluated before the stores so that none of its loads waits on them
-        const bool indt = ii >= G - 1 && ii <= G + b.Nip && jj >= G - 1 && jj <= G + b.Njp && kk >= G - 1 &&
-                          kk <= G + b.Nkp;
+        const bool indt = ii >= G - 1 && ii <= G + b.Nip && jj >= G - 1 && jj <= G + b.Njp && kk >= G - P.dtKlo &&
+                          kk <= G + b.Nkp - 1 + P.dtKhi;
         if (indt && !sc->fixedTimestep) {
             double Ud[5], Bt[3];
 #pragma unroll
@@ -1112,7 +1112,7 @@ __global__ void __launch_bounds__(128) k_dt_only(GamBox b, DevParams<R> P, Geo<R
                                                  GamScalars* sc, double gamma_d, double gm1_d) {
     int ii, jj, kk;
     const int G = GAM_NG;
-    Range r{G - 1, G + b.Nip, G - 1, G + b.Njp, G - 1, G + b.Nkp};
+    Range r{G - 1, G + b.Nip, G - 1, G + b.Njp, G - P.dtKlo, G + b.Nkp - 1 + P.dtKhi};
     double mydt = HUGE_DT;
     if (thread_ijk(r, ii, jj, kk)) {
         const long fs = b.fs;
@@ -1253,7 +1253,7 @@ template <class R> void launch_dt_only(const Ctx<R>& C, int cur, cudaStream_t s)
     const GamBox& b = C.b;
     const int G = GAM_NG;
     const dim3 blk(32, 4, 1);
-    const Range r{G - 1, G + b.Nip, G - 1, G + b.Njp, G - 1, G + b.Nkp};
+    const Range r{G - 1, G + b.Nip, G - 1, G + b.Njp, G - C.P.dtKlo, G + b.Nkp - 1 + C.P.dtKhi};
     k_dt_only<R><<<grid_for(r, blk), blk, 0, s>>>(b, C.P, C.g, C.st[cur], C.sc, C.gamma, C.gm1);
 }
 
@@ -1270,6 +1270,81 @@ template <class R> void launch_init(const Ctx<R>& C, int cur, cudaStream_t s) {
     cudaMemcpyAsync(O.Gas, S.Gas, 5 * b.fs * sizeof(R), cudaMemcpyDeviceToDevice, s);
     cudaMemcpyAsync(O.mf, S.mf, 3 * b.fs * sizeof(R), cudaMemcpyDeviceToDevice, s);
     cudaMemcpyAsync(O.B, S.B, 3 * b.fs * sizeof(R), cudaMemcpyDeviceToDevice, s);
+}
+
+// ----------------------------------------------------------------- k-slab tiling
+// One step in two phases for a caller that reduces dt over several domains:
+// phase 0 = begin .. cell update (the dt candidates in sc->dtmin_bits and
+// sc->nbad), phase 1 = dt decision and boundary fill. The caller writes the
+// global min / count into sc between them (gamapp_mpi.F90:495-512).
+template <class R> void launch_step_phase(const Ctx<R>& C, int cur, cudaStream_t s, int phase) {
+    for_each_kernel(C, cur, s, [&](int id, auto&& L) {
+        if ((id <= 12) == (phase == 0)) L();
+    });
+}
+
+// Halo of a k-slab (the depth-4 exchange of updateMpiBCs/haloUpdate,
+// gamapp_mpi.F90:573-782, for a decomposition along k): 11 components
+// (Gas 0-4, magFlux 5-7, Bxyz 8-10) x 4 layers x the full ghosted i x j
+// extent, element (q, l, jj, ii) at ((q * 4 + l) * (Nj+1) + jj) * (Ni+1) + ii.
+// Pack side 0 = what this domain sends down (cells and I, J faces at
+// k = G..G+3, K faces at G+1..G+4: the neighbour's upper ghosts); side 1 =
+// what it sends up (everything at k = Nkp..Nkp+3: the neighbour's lower
+// ghosts). Unpack side 0 fills this domain's lower ghosts (k = 0..3), side 1
+// its upper ghosts (cells, I and J faces at G+Nkp.., K faces at G+Nkp+1..),
+// the same indices the periodic K rule of bcs.F90:397-450 uses.
+__device__ __forceinline__ int halo_k(const GamBox& b, int side, bool unpack, int q, int l) {
+    const int G = GAM_NG;
+    const bool kface = q == 7;
+    if (!unpack) return side == 0 ? G + l + (kface ? 1 : 0) : b.Nkp + l;
+    return side == 0 ? l : G + b.Nkp + l + (kface ? 1 : 0);
+}
+template <class R> __device__ __forceinline__ R* halo_ptr(const StateBuf<R>& S, long fs, int q) {
+    return q < 5 ? S.Gas + (long)q * fs : (q < 8 ? S.mf + (long)(q - 5) * fs : S.B + (long)(q - 8) * fs);
+}
+template <class R>
+__global__ void __launch_bounds__(256) k_halo(GamBox b, StateBuf<R> S, R* __restrict__ buf, int side, int unpack,
+                                              int copyB) {
+    const long nx = b.Ni + 1, ny = b.Nj + 1;
+    const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (t >= 4 * nx * ny) return;
+    const int ii = (int)(t % nx), jj = (int)((t / nx) % ny), l = (int)(t / (nx * ny));
+    const long fs = b.fs;
+    for (int q = 0; q < 11; q++) {
+        if (unpack && q >= 8 && !copyB) break;
+        const long c = lidx(b, ii, jj, halo_k(b, side, unpack != 0, q, l));
+        const long e = ((long)(q * 4 + l) * ny + jj) * nx + ii;
+        R* p = halo_ptr(S, fs, q);
+        if (unpack)
+            p[c] = buf[e];
+        else
+            buf[e] = p[c];
+    }
+}
+// Bxyz of the unpacked ghost cells from their faces (the final bFlux2Fld)
+template <class R>
+__global__ void __launch_bounds__(256) k_halo_bxyz(GamBox b, Geo<R> g, StateBuf<R> S, int side) {
+    const long nx = b.Ni, ny = b.Nj;
+    const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (t >= 4 * nx * ny) return;
+    const int ii = (int)(t % nx), jj = (int)((t / nx) % ny), l = (int)(t / (nx * ny));
+    const int kk = side == 0 ? l : GAM_NG + b.Nkp + l;
+    const long fs = b.fs, c = lidx(b, ii, jj, kk);
+    R B[3];
+    cell_bxyz(b, g, c, S.mf[c], S.mf[c + 1], S.mf[fs + c], S.mf[fs + c + b.sx], S.mf[2 * fs + c],
+              S.mf[2 * fs + c + b.sk], B);
+#pragma unroll
+    for (int x = 0; x < 3; x++) S.B[x * fs + c] = B[x];
+}
+template <class R> void launch_halo(const Ctx<R>& C, int cur, cudaStream_t s, int side, int unpack, int copyB, void* buf) {
+    const GamBox& b = C.b;
+    const StateBuf<R> S = C.st[cur];
+    const long n = 4L * (b.Ni + 1) * (b.Nj + 1);
+    k_halo<R><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(b, S, (R*)buf, side, unpack, copyB);
+    if (unpack && !copyB && C.P.doMHD) {
+        const long m = 4L * b.Ni * b.Nj;
+        k_halo_bxyz<R><<<(unsigned)((m + 255) / 256), 256, 0, s>>>(b, C.g, S, side);
+    }
 }
 
 }  // namespace GAM_NS

@@ -20,6 +20,9 @@ template <class R> struct DevParams {
     R gamma, gm1, CFL, pdmb, Vd0, cHogH, dFloor, pFloor;
     int doMHD, doLFMLim, do25D, doBackground, up7;
     int bc[6];
+    // CalcDT covers the ghost layer below / above the active k range (1, the
+    // reference's isDT..ieDT); a k-slab drops it where a neighbour's cells lie
+    int dtKlo, dtKhi;
     WindData wind;
 };
 

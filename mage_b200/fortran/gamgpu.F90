@@ -11,7 +11,7 @@ module gamgpu
     integer(c_int), parameter :: GAM_OK = 0, GAM_EINVAL = 1, GAM_EBADDIM = 2, GAM_ECUDA = 3, &
                                  GAM_EDT_BAD = 4, GAM_EDT_DISASTER = 5, GAM_ESTATE = 6, GAM_EHOOK = 7
     integer(c_int), parameter :: GAM_BC_PERIODIC = 0, GAM_BC_NONE = 1, GAM_BC_ZEROGRAD = 2, GAM_BC_SPHIN = 3, &
-                                 GAM_BC_WIND = 4
+                                 GAM_BC_WIND = 4, GAM_BC_HALO = 5
     integer(c_int), parameter :: GAM_RECON_8CENT = 0, GAM_RECON_7UP = 1
     integer(c_int), parameter :: GAM_FP64 = 0, GAM_FP32 = 1
 
@@ -109,6 +109,55 @@ module gamgpu
             import :: c_int, c_ptr, c_double
             type(c_ptr), value :: h
             real(c_double), intent(in) :: wind(8)
+        end function
+        ! k-slab tiling: the MPI driver (gamAppMpi_T) packs/unpacks halos in
+        ! device buffers and reduces dt between gam_step_begin and gam_step_end
+        integer(c_int) function gam_set_slab_edges(h, lowest, highest) bind(C, name="gam_set_slab_edges")
+            import :: c_int, c_ptr, c_int32_t
+            type(c_ptr), value :: h
+            integer(c_int32_t), value :: lowest, highest
+        end function
+        integer(c_int) function gam_halo_bytes(h, nbytes) bind(C, name="gam_halo_bytes")
+            import :: c_int, c_ptr, c_int64_t
+            type(c_ptr), value :: h
+            integer(c_int64_t), intent(out) :: nbytes
+        end function
+        integer(c_int) function gam_halo_pack(h, side, dev_buf) bind(C, name="gam_halo_pack")
+            import :: c_int, c_ptr, c_int32_t
+            type(c_ptr), value :: h, dev_buf
+            integer(c_int32_t), value :: side
+        end function
+        integer(c_int) function gam_halo_unpack(h, side, dev_buf, copyB) bind(C, name="gam_halo_unpack")
+            import :: c_int, c_ptr, c_int32_t
+            type(c_ptr), value :: h, dev_buf
+            integer(c_int32_t), value :: side, copyB
+        end function
+        integer(c_int) function gam_init_finish_halo(h, dt) bind(C, name="gam_init_finish_halo")
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: h
+            real(c_double), intent(out) :: dt
+        end function
+        integer(c_int) function gam_set_start(h, dt) bind(C, name="gam_set_start")
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: h
+            real(c_double), value :: dt
+        end function
+        integer(c_int) function gam_step_begin(h) bind(C, name="gam_step_begin")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h
+        end function
+        integer(c_int) function gam_dt_partial(h, bits, nbad) bind(C, name="gam_dt_partial")
+            import :: c_int, c_ptr, c_int64_t, c_int32_t
+            type(c_ptr), value :: h
+            integer(c_int64_t), intent(out) :: bits
+            integer(c_int32_t), intent(out) :: nbad
+        end function
+        integer(c_int) function gam_step_end(h, bits, nbad, dt, t) bind(C, name="gam_step_end")
+            import :: c_int, c_ptr, c_int64_t, c_int32_t, c_double
+            type(c_ptr), value :: h
+            integer(c_int64_t), value :: bits
+            integer(c_int32_t), value :: nbad
+            real(c_double), intent(out) :: dt, t
         end function
         integer(c_int) function gam_write_restart(h, path) bind(C, name="gam_write_restart")
             import :: c_int, c_ptr, c_char

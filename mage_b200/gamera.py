@@ -22,7 +22,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libgamgpu.so")
 
 GAM_OK, GAM_EINVAL, GAM_EBADDIM, GAM_ECUDA, GAM_EDT_BAD, GAM_EDT_DISASTER, GAM_ESTATE, GAM_EHOOK = range(8)
-BC_PERIODIC, BC_NONE, BC_ZEROGRAD, BC_SPHIN, BC_WIND = 0, 1, 2, 3, 4
+BC_PERIODIC, BC_NONE, BC_ZEROGRAD, BC_SPHIN, BC_WIND, BC_HALO = 0, 1, 2, 3, 4, 5
 RECON_8CENT, RECON_7UP = 0, 1
 FP64, FP32 = 0, 1
 
@@ -53,6 +53,8 @@ EXPORTED = (
     "gam_calc_dt", "gam_divb", "gam_totals", "gam_last_step_ms", "gam_advance_model", "gam_init_orszag_tang",
     "gam_init_blast_wave", "gam_profile_step", "gam_totals_noalloc", "gam_set_background", "gam_get_background",
     "gam_set_background_dipole", "gam_set_wind", "gam_init_dipole_wind", "gam_write_restart", "gam_read_restart",
+    "gam_halo_bytes", "gam_halo_pack", "gam_halo_unpack", "gam_init_finish_halo", "gam_set_start", "gam_step_begin",
+    "gam_dt_partial", "gam_step_end", "gam_set_slab_edges",
 )
 
 # Background-field arrays (Grid_T, gamtypes.F90:233-242): name, components;
@@ -95,6 +97,15 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     L.gam_set_background_dipole.argtypes = [C.c_void_p, C.c_double]
     L.gam_set_wind.argtypes = [C.c_void_p, _dp]
     L.gam_write_restart.argtypes = [C.c_void_p, C.c_char_p]
+    L.gam_halo_bytes.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
+    L.gam_set_slab_edges.argtypes = [C.c_void_p, C.c_int32, C.c_int32]
+    L.gam_halo_pack.argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
+    L.gam_halo_unpack.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32]
+    L.gam_init_finish_halo.argtypes = [C.c_void_p, _dp]
+    L.gam_set_start.argtypes = [C.c_void_p, C.c_double]
+    L.gam_step_begin.argtypes = [C.c_void_p]
+    L.gam_dt_partial.argtypes = [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_int32)]
+    L.gam_step_end.argtypes = [C.c_void_p, C.c_uint64, C.c_int32, _dp, _dp]
     L.gam_read_restart.argtypes = [C.c_void_p, C.c_char_p]
     L.gam_init_dipole_wind.argtypes = [C.c_void_p, _dp, C.c_uint64, C.c_double]
     L.gam_totals_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p,
@@ -271,6 +282,42 @@ class GameraGPU:
         w = np.ascontiguousarray(wind, dtype=np.float64)
         assert w.shape == (8,)
         self._check(self.L.gam_init_dipole_wind(self.h, _ptr(w), int(seed), float(amp)))
+
+    # --- k-slab tiling (see mage_b200.tiling) --------------------------------------
+    def set_slab_edges(self, lowest: bool, highest: bool):
+        self._check(self.L.gam_set_slab_edges(self.h, int(lowest), int(highest)))
+
+    def halo_bytes(self) -> int:
+        n = C.c_int64()
+        self._check(self.L.gam_halo_bytes(self.h, C.byref(n)))
+        return n.value
+
+    def halo_pack(self, side: int, dev_ptr: int):
+        self._check(self.L.gam_halo_pack(self.h, int(side), C.c_void_p(dev_ptr)))
+
+    def halo_unpack(self, side: int, dev_ptr: int, copyB: bool = False):
+        self._check(self.L.gam_halo_unpack(self.h, int(side), C.c_void_p(dev_ptr), int(copyB)))
+
+    def init_finish_halo(self) -> float:
+        dt = C.c_double()
+        self._check(self.L.gam_init_finish_halo(self.h, C.byref(dt)))
+        return dt.value
+
+    def set_start(self, dt: float):
+        self._check(self.L.gam_set_start(self.h, float(dt)))
+
+    def step_begin(self):
+        self._check(self.L.gam_step_begin(self.h))
+
+    def dt_partial(self):
+        bits, nbad = C.c_uint64(), C.c_int32()
+        self._check(self.L.gam_dt_partial(self.h, C.byref(bits), C.byref(nbad)))
+        return bits.value, nbad.value
+
+    def step_end(self, bits: int, nbad: int):
+        dt, t = C.c_double(), C.c_double()
+        self._check(self.L.gam_step_end(self.h, C.c_uint64(bits), int(nbad), C.byref(dt), C.byref(t)))
+        return dt.value, t.value
 
     # --- restart files --------------------------------------------------------
     def write_restart(self, path: str):
