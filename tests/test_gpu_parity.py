@@ -267,3 +267,20 @@ def test_restart_round_trip(tmp_path):
     with pytest.raises(GamError) as e:
         b.read_restart(str(junk))
     assert e.value.code == 1  # GAM_EINVAL
+
+
+@pytest.mark.parametrize("kw", [dict(up7=True), dict(doLFMLim=False), dict(doMHD=False),
+                                dict(up7=True, doLFMLim=False)], ids=["7UP", "noLFMLim", "hydro", "7UP-noLFMLim"])
+def test_strict_model_options_bit_exact(oracle_built, kw):
+    """Model options of the step (initModel keys, init.F90:312-484): 7UP
+    reconstruction (recon.F90:162-198), the limiter on the half state instead
+    of the n-state (doLFMLim = F), and hydrodynamics without magnetic field
+    (doMHD = F): the strict build equals the gm oracle bit for bit."""
+    o, _ = make_oracle("bw", (16, 16, 16), variant="gm", **kw)
+    g = gpu_from_oracle(o, strict=True)
+    assert o.step(10) == 0
+    dt, t = g.step_gamera(10)
+    s = g.download_state()
+    for k in STATE:
+        assert np.array_equal(s[k], o.array(k)), (kw, k, rel_err(s[k], o.array(k)))
+    assert dt == o.scalars()["dt"]
