@@ -209,6 +209,27 @@ int gam_step_begin(gam_handle* h);
 int gam_dt_partial(gam_handle* h, uint64_t* dtmin_bits, int32_t* nbad);
 int gam_step_end(gam_handle* h, uint64_t dtmin_bits, int32_t nbad, double* dt, double* t);
 
+/* Flux stage of the step and its hand-written adjoint (differentiation form),
+ * on caller-owned device arrays in the unpadded box layout: each field is
+ * (nc, Nk+1, Nj+1, Ni+1) contiguous, i fastest, Ni = Nip + 8 (cell fields
+ * leave the last slot of each axis unused). Inputs: QW = volume x half-state
+ * primitives (5), Wn = limiter primitives (5), QB = volume x half-state Bxyz
+ * (3), Blim = limiter Bxyz (3), Bnf = half-state flux / area (3), volume (1),
+ * face (3), Tf (27: n + 9 d), fcB0 (9) and bFlux0 (3) in FP64 when
+ * doBackground. gam_flux_forward writes gF (15: v + 5 d) and mF (9: x + 3 d)
+ * over the face ranges of CalcStress (stress.F90:41-198); gam_flux_adjoint
+ * adds the adjoints of those inputs for the given adjoints dgF, dmF (callers
+ * zero dQW, dWn, dQB, dBlim, dBnf first). fp32 = 1: float arrays (fcB0/bFlux0
+ * stay double). 8CENT reconstruction, 3-D; enqueued on stream (cudaStream_t,
+ * 0 = default). No counterpart in the reference, which has no adjoint. */
+int gam_flux_forward(const gam_params* p, int32_t fp32, const void* QW, const void* Wn, const void* QB,
+                     const void* Blim, const void* Bnf, const void* volume, const void* face, const void* Tf,
+                     const double* fcB0, const double* bFlux0, void* gF, void* mF, void* stream);
+int gam_flux_adjoint(const gam_params* p, int32_t fp32, const void* QW, const void* Wn, const void* QB,
+                     const void* Blim, const void* Bnf, const void* volume, const void* face, const void* Tf,
+                     const double* fcB0, const double* bFlux0, const void* dgF, const void* dmF, void* dQW,
+                     void* dWn, void* dQB, void* dBlim, void* dBnf, void* stream);
+
 /* Conserved totals for callers that cannot allocate device memory.
  * No counterpart in the reference. Some callers cannot call cudaMalloc while
  * they run: their device memory belongs to another framework's pool, or they

@@ -1,0 +1,389 @@
+// Flux stage of the step (CalcStress / Fluxes / GasKinFlux / MagKinFlux,
+// stress.F90:41-599, with Cen8LRs + pdmLR, recon.F90:125-272) and its
+// hand-written reverse mode, on caller-owned device arrays in the unpadded box
+// layout (component-major (nc, Nk+1, Nj+1, Ni+1), i fastest). The forward is
+// the product step's own flux kernel; the adjoint recomputes each face's
+// states and fluxes and runs them backwards:
+//   outputs  gF (15: v + 5*d), mF (9: x + 3*d), already times the face area
+//   inputs   QW = volume * half-state primitives (5), Wn limiter primitives (5),
+//            QB = volume * half-state Bxyz (3), Blim limiter Bxyz (3),
+//            Bnf = half-state flux / area (3)
+// The adjoint accumulates (atomicAdd) into dQW, dWn, dQB, dBlim, dBnf, which
+// the caller zeroes. Non-smooth points follow the forward's branches: a
+// max/min passes the adjoint to the operand it selected, |x| and sign(x) have
+// a zero derivative at 0, sqrt(Va^2) a zero derivative at 0.
+#include <string.h>
+#define GAM_NS gam_adj
+#define GAM_CUDA_MATH 1
+#include "gam_step_impl.cuh"
+
+namespace gam_adj {
+
+__device__ GamScalars g_adj_scalars;  // zero: not halted
+
+__device__ __forceinline__ double sgnz(double x) { return x > 0.0 ? 1.0 : (x < 0.0 ? -1.0 : 0.0); }
+
+// reverse of lrs_from_qdv (8CENT) for one variable: scatter the adjoints of
+// Ql, Qr to the 8-point operand stencil and the 4-point limiter stencil
+template <class R>
+__device__ void lrs_adj(R pdmb, const R* qdv, const R* v, R Vi, double aL, double aR, double* aq, double* av) {
+    R s = (R)0;
+#pragma unroll
+    for (int n = 0; n < 8; n++) s += Rc<R>(w8(n)) * qdv[n];
+    const R Qi = s / Vi;
+    const R v0 = v[0], v1 = v[1], v2 = v[2], v3 = v[3];
+    const R maxV = rmax(v1, v2), minV = rmin(v1, v2);
+    const R t = rmin(Qi, maxV);
+    const R vN = rmax(minV, t);
+    const R dv0 = pdmb * (v1 - v0), dv1 = pdmb * (v2 - v1), dv2 = pdmb * (v3 - v2);
+    const R s0 = sgn1(dv0), s1 = sgn1(dv1), s2 = sgn1(dv2);
+    const R q0 = fabs(s0 + s1), q1 = fabs(s1 + s2);
+    const R dvL = vN - v1, dvR = v2 - vN;
+    const R uL = fabs(dvL) - q0 * fabs(dv0), uR = fabs(dvR) - q1 * fabs(dv2);
+    double a_vN = aL + aR;
+    const double a_mL = -(double)s1 * aL, a_mR = (double)s1 * aR;
+    const double a_uL = ((R)0 < uL) ? a_mL : 0.0, a_uR = ((R)0 < uR) ? a_mR : 0.0;
+    const double a_dvL = a_uL * sgnz(dvL), a_dv0 = -a_uL * q0 * sgnz(dv0);
+    const double a_dvR = a_uR * sgnz(dvR), a_dv2 = -a_uR * q1 * sgnz(dv2);
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    a_vN += a_dvL;
+    a1 -= a_dvL;
+    a2 += a_dvR;
+    a_vN -= a_dvR;
+    a1 += pdmb * a_dv0;
+    a0 -= pdmb * a_dv0;
+    a3 += pdmb * a_dv2;
+    a2 -= pdmb * a_dv2;
+    double a_t = 0.0, a_minV = 0.0, a_maxV = 0.0, a_Qi = 0.0;
+    if (minV < t) a_t = a_vN; else a_minV = a_vN;
+    if (maxV < Qi) a_maxV = a_t; else a_Qi = a_t;
+    if (v2 < v1) a2 += a_minV; else a1 += a_minV;
+    if (v1 < v2) a2 += a_maxV; else a1 += a_maxV;
+    const double a_s = a_Qi / (double)Vi;
+#pragma unroll
+    for (int n = 0; n < 8; n++) aq[n] = w8(n) * a_s;
+    av[0] = a0; av[1] = a1; av[2] = a2; av[3] = a3;
+}
+
+// reverse of mag_kin_flux for one side: adjoints aM (of the mF sums) and aVaD
+// (of the VaD sum) -> a_W (5), a_B (3), a_Bn
+template <class R>
+__device__ void mag_adj(const DevParams<R>& P, double sgn, const R* W, const R* Bm, R Bn, const R* T, const double* B0,
+                        double B0n, const double* aM, double aVaD, double* aW, double* aB, double& aBn) {
+    const double D = W[0], Pr = W[4];
+    const double Bx = Bm[0], By = Bm[1], Bz = Bm[2];
+    const double N[3] = {T[0], T[1], T[2]};
+    const double dPb = 0.5 * (Bx * Bx + By * By + Bz * Bz);
+    double S[3] = {Bx, By, Bz};
+    double Va2;
+    if (P.doBackground) {
+        S[0] += B0[0]; S[1] += B0[1]; S[2] += B0[2];
+        Va2 = (S[0] * S[0] + S[1] * S[1] + S[2] * S[2]) / D;
+    } else {
+        Va2 = 2.0 * dPb / D;
+    }
+    const double Vn = N[0] * W[1] + N[1] * W[2] + N[2] * W[3];
+    const double den = 2.0 * Pr / D + Va2;
+    const double lam = 1.0 / den;
+    const double s = sqrt(lam);
+    const double z = sgn * s * Vn;
+    const double Vn0 = 0.5 * erfc(z);
+    const double B[3] = {Bx, By, Bz};
+    double C[3];
+    for (int x = 0; x < 3; x++) C[x] = dPb * N[x] - B[x] * (double)Bn;
+    double BdB0 = 0.0;
+    if (P.doBackground) {
+        BdB0 = B0[0] * Bx + B0[1] * By + B0[2] * Bz;
+        for (int x = 0; x < 3; x++) C[x] += -(B0[x] * (double)Bn) - B[x] * B0n + BdB0 * N[x];
+    }
+    double a_Vn0 = 0.0, a_dPb = 0.0, a_Va2 = 0.0, a_Vn = 0.0, sumCN = 0.0;
+    for (int x = 0; x < 3; x++) {
+        a_Vn0 += aM[x] * C[x];
+        const double aC = aM[x] * Vn0;
+        a_dPb += aC * N[x];
+        aB[x] += -aC * (double)Bn;
+        aBn += -aC * B[x];
+        if (P.doBackground) {
+            aB[x] += -aC * B0n;
+            aBn += -aC * B0[x];
+            sumCN += aC * N[x];
+        }
+    }
+    if (P.doBackground)
+        for (int x = 0; x < 3; x++) aB[x] += sumCN * B0[x];
+    if (Va2 > 0.0) a_Va2 += aVaD * 0.25 / sqrt(Va2);
+    const double a_z = a_Vn0 * (-exp(-z * z) / sqrt(PI_D));
+    const double a_s = a_z * sgn * Vn;
+    a_Vn += a_z * sgn * s;
+    const double a_lam = a_s * 0.5 / s;
+    const double a_den = -a_lam * lam * lam;
+    aW[4] += a_den * 2.0 / D;
+    aW[0] += -a_den * 2.0 * Pr / (D * D);
+    a_Va2 += a_den;
+    if (P.doBackground) {
+        for (int x = 0; x < 3; x++) aB[x] += a_Va2 * 2.0 * S[x] / D;
+        aW[0] += -a_Va2 * (S[0] * S[0] + S[1] * S[1] + S[2] * S[2]) / (D * D);
+    } else {
+        a_dPb += a_Va2 * 2.0 / D;
+        aW[0] += -a_Va2 * 2.0 * dPb / (D * D);
+    }
+    for (int x = 0; x < 3; x++) {
+        aW[1 + x] += a_Vn * N[x];
+        aB[x] += a_dPb * B[x];
+    }
+}
+
+// reverse of gas_kin_flux for one side: adjoints aG (of the gF sums) and aD
+// (of the dW sums) -> a_W (5)
+template <class R>
+__device__ void gas_adj(const DevParams<R>& P, double sgn, const R* W, const R* T, const double* aG, const double* aDW,
+                        double* aW) {
+    const double D = W[0], Pr = W[4], V[3] = {W[1], W[2], W[3]};
+    const double gm1 = P.gm1;
+    const double V2 = V[0] * V[0] + V[1] * V[1] + V[2] * V[2];
+    const double E = 0.5 * D * V2 + Pr / gm1;
+    const double lam = D / (2.0 * Pr);
+    double N[3], T1[3], T2[3];
+    for (int x = 0; x < 3; x++) { N[x] = T[x]; T1[x] = T[3 + x]; T2[x] = T[6 + x]; }
+    const double Vn = N[0] * V[0] + N[1] * V[1] + N[2] * V[2];
+    const double Vt1 = T1[0] * V[0] + T1[1] * V[1] + T1[2] * V[2];
+    const double Vt2 = T2[0] * V[0] + T2[1] * V[1] + T2[2] * V[2];
+    const double s = sqrt(lam);
+    const double z = sgn * s * Vn;
+    const double Vn0 = 0.5 * erfc(z);
+    const double ex = exp(-(lam * Vn * Vn));
+    const double sq = sqrt(PI_D * lam);
+    const double Vn1 = Vn * Vn0 - 0.5 * sgn * ex / sq;
+    double a_fMn = 0.0, a_fMt1 = 0.0, a_fMt2 = 0.0;
+    for (int x = 0; x < 3; x++) {
+        a_fMn += aG[1 + x] * N[x];
+        a_fMt1 += aG[1 + x] * T1[x];
+        a_fMt2 += aG[1 + x] * T2[x];
+    }
+    double a_Vn1 = aG[0] * D + aG[4] * (E + 0.5 * Pr) + a_fMn * D * Vn + a_fMt1 * D * Vt1 + a_fMt2 * D * Vt2;
+    double a_Vn0 = aG[4] * 0.5 * Pr * Vn + a_fMn * Pr;
+    double a_D = aG[0] * Vn1 + a_fMn * Vn * Vn1 + a_fMt1 * Vt1 * Vn1 + a_fMt2 * Vt2 * Vn1 + aDW[0] * sgn;
+    for (int x = 0; x < 3; x++) a_D += aDW[1 + x] * sgn * V[x];
+    const double a_E = aG[4] * Vn1 + aDW[4] * sgn;
+    double a_Pr = aG[4] * (0.5 * Vn1 + 0.5 * Vn0 * Vn) + a_fMn * Vn0;
+    double a_Vn = aG[4] * 0.5 * Pr * Vn0 + a_fMn * D * Vn1;
+    const double a_Vt1 = a_fMt1 * D * Vn1, a_Vt2 = a_fMt2 * D * Vn1;
+    double a_V[3];
+    for (int x = 0; x < 3; x++) a_V[x] = aDW[1 + x] * sgn * D;
+    // Vn1 = Vn Vn0 - 0.5 sgn ex / sq
+    a_Vn += a_Vn1 * Vn0;
+    a_Vn0 += a_Vn1 * Vn;
+    const double a_ex = -a_Vn1 * 0.5 * sgn / sq;
+    const double a_sq = a_Vn1 * 0.5 * sgn * ex / (sq * sq);
+    double a_lam = a_sq * PI_D * 0.5 / sq;
+    a_lam += -a_ex * ex * Vn * Vn;
+    a_Vn += -a_ex * ex * 2.0 * lam * Vn;
+    const double a_z = a_Vn0 * (-exp(-z * z) / sqrt(PI_D));
+    const double a_s = a_z * sgn * Vn;
+    a_Vn += a_z * sgn * s;
+    a_lam += a_s * 0.5 / s;
+    a_D += a_lam / (2.0 * Pr);
+    a_Pr += -a_lam * D / (2.0 * Pr * Pr);
+    a_D += a_E * 0.5 * V2;
+    for (int x = 0; x < 3; x++) a_V[x] += a_E * D * V[x];
+    a_Pr += a_E / gm1;
+    for (int x = 0; x < 3; x++) a_V[x] += a_Vn * N[x] + a_Vt1 * T1[x] + a_Vt2 * T2[x];
+    aW[0] += a_D;
+    aW[1] += a_V[0];
+    aW[2] += a_V[1];
+    aW[3] += a_V[2];
+    aW[4] += a_Pr;
+}
+
+// Adjoint of the face fluxes of direction D over the range r (one face per
+// thread): recompute, then reverse.
+template <class R, int D>
+__global__ void __launch_bounds__(128) k_stress_adj(GamBox b, DevParams<R> P, Geo<R> g, const R* __restrict__ Blim,
+                                                    Work<R> w, Range r, const R* __restrict__ dgF,
+                                                    const R* __restrict__ dmF, R* dQW, R* dWn, R* dQB, R* dBlim,
+                                                    R* dBnf) {
+    int ii, jj, kk;
+    if (!thread_ijk(r, ii, jj, kk)) return;
+    const long fs = b.fs;
+    const long c = lidx(b, ii, jj, kk);
+    const long s = D == 0 ? 1L : (D == 1 ? (long)b.sx : b.sk);
+    R T[9];
+    for (int n = 0; n < 9; n++) T[n] = g.Tf[(n + 9 * D) * fs + c];
+    const R fa = g.face[D * fs + c];
+    R vol[8];
+    for (int n = 0; n < 8; n++) vol[n] = g.vol[c + (n - 4) * s];
+    const R Vi = central8(vol);
+    // forward states
+    R WL[5], WR[5], MagL[3] = {(R)0, (R)0, (R)0}, MagR[3] = {(R)0, (R)0, (R)0};
+    R qW[5][8], nW[5][4], qB[3][8], nB[3][4];
+    for (int v = 0; v < 5; v++) {
+        for (int n = 0; n < 8; n++) qW[v][n] = w.QW[v * fs + c + (n - 4) * s];
+        for (int m = 0; m < 4; m++) nW[v][m] = w.Wn[v * fs + c + (m - 2) * s];
+        lrs_from_qdv(P, qW[v], nW[v], Vi, WL[v], WR[v]);
+    }
+    R Bn = (R)0;
+    double B0[3] = {0.0, 0.0, 0.0}, B0n = 0.0;
+    if (P.doMHD) {
+        Bn = w.Bnf[D * fs + c];
+        for (int x = 0; x < 3; x++) {
+            for (int n = 0; n < 8; n++) qB[x][n] = w.QB[x * fs + c + (n - 4) * s];
+            for (int m = 0; m < 4; m++) nB[x][m] = Blim[x * fs + c + (m - 2) * s];
+            lrs_from_qdv(P, qB[x], nB[x], Vi, MagL[x], MagR[x]);
+        }
+        if (P.doBackground) {
+            for (int x = 0; x < 3; x++) B0[x] = g.fcB0[(x + 3 * D) * fs + c];
+            B0n = g.bFlux0[D * fs + c] / (double)fa;
+        }
+    }
+    R VaD = (R)0, bbD = (R)0;
+    if (P.doMHD) {
+        R mFs[3] = {(R)0, (R)0, (R)0};
+        mag_kin_flux(P, (R)-1, WL, MagL, Bn, T, B0, B0n, mFs, bbD, VaD);
+        mag_kin_flux(P, (R)1, WR, MagR, Bn, T, B0, B0n, mFs, bbD, VaD);
+    }
+    R gFs[5] = {(R)0, (R)0, (R)0, (R)0, (R)0}, dW[5] = {(R)0, (R)0, (R)0, (R)0, (R)0};
+    gas_kin_flux(P, (R)-1, WL, T, gFs, dW);
+    gas_kin_flux(P, (R)1, WR, T, gFs, dW);
+    // reverse of the outputs gF = fa (gFs - cHogH VaD dW), mF = fa mFs
+    double aG[5], aDW[5], aVaD = 0.0, aM[3] = {0.0, 0.0, 0.0};
+    for (int v = 0; v < 5; v++) {
+        const double Gv = dgF[(v + 5 * D) * fs + c];
+        aG[v] = (double)fa * Gv;
+        aDW[v] = -(double)fa * P.cHogH * (double)VaD * Gv;
+        aVaD += -(double)fa * P.cHogH * Gv * (double)dW[v];
+    }
+    double aWL[5] = {0, 0, 0, 0, 0}, aWR[5] = {0, 0, 0, 0, 0}, aBL[3] = {0, 0, 0}, aBR[3] = {0, 0, 0}, aBn = 0.0;
+    gas_adj(P, -1.0, WL, T, aG, aDW, aWL);
+    gas_adj(P, 1.0, WR, T, aG, aDW, aWR);
+    if (P.doMHD) {
+        for (int x = 0; x < 3; x++) aM[x] = (double)fa * dmF[(x + 3 * D) * fs + c];
+        mag_adj(P, -1.0, WL, MagL, Bn, T, B0, B0n, aM, aVaD, aWL, aBL, aBn);
+        mag_adj(P, 1.0, WR, MagR, Bn, T, B0, B0n, aM, aVaD, aWR, aBR, aBn);
+        dBnf[D * fs + c] += (R)aBn;
+    }
+    // reverse of the reconstruction: scatter to the stencils
+    double aq[8], av[4];
+    for (int v = 0; v < 5; v++) {
+        lrs_adj(P.pdmb, qW[v], nW[v], Vi, aWL[v], aWR[v], aq, av);
+        for (int n = 0; n < 8; n++) atomicAdd(&dQW[v * fs + c + (n - 4) * s], (R)aq[n]);
+        for (int m = 0; m < 4; m++) atomicAdd(&dWn[v * fs + c + (m - 2) * s], (R)av[m]);
+    }
+    if (P.doMHD)
+        for (int x = 0; x < 3; x++) {
+            lrs_adj(P.pdmb, qB[x], nB[x], Vi, aBL[x], aBR[x], aq, av);
+            for (int n = 0; n < 8; n++) atomicAdd(&dQB[x * fs + c + (n - 4) * s], (R)aq[n]);
+            for (int m = 0; m < 4; m++) atomicAdd(&dBlim[x * fs + c + (m - 2) * s], (R)av[m]);
+        }
+}
+
+}  // namespace gam_adj
+
+// ------------------------------------------------------------ C ABI
+#include "../../include/gamgpu.h"
+
+namespace {
+GamBox torch_box(int Nip, int Njp, int Nkp) {
+    GamBox b;
+    b.Nip = Nip; b.Njp = Njp; b.Nkp = Nkp;
+    b.Ni = Nip + 2 * GAM_NG; b.Nj = Njp + 2 * GAM_NG; b.Nk = Nkp + 2 * GAM_NG;
+    b.sx = b.Ni + 1;
+    b.sk = (long)b.sx * (b.Nj + 1);
+    b.nbox = b.sk * (b.Nk + 1);
+    b.fs = b.nbox;
+    return b;
+}
+template <class R> DevParams<R> dev_params(const gam_params* p) {
+    DevParams<R> P;
+    memset(&P, 0, sizeof(P));
+    P.gamma = (R)p->gamma; P.gm1 = (R)(p->gamma - 1); P.CFL = (R)p->CFL; P.pdmb = (R)p->pdmb; P.Vd0 = (R)p->Vd0;
+    P.cHogH = (R)p->cHogH; P.dFloor = (R)p->dFloor; P.pFloor = (R)p->pFloor;
+    P.doMHD = p->doMHD; P.doLFMLim = p->doLFMLim; P.do25D = p->do25D; P.doBackground = p->doBackground;
+    P.up7 = p->rmeth == GAM_RECON_7UP;
+    for (int n = 0; n < 6; n++) P.bc[n] = p->bc[n];
+    P.dtKlo = P.dtKhi = 1;
+    return P;
+}
+template <class R>
+int flux_call(const gam_params* p, const void* QW, const void* Wn, const void* QB, const void* Blim, const void* Bnf,
+              const void* vol, const void* face, const void* Tf, const double* fcB0, const double* bFlux0, void* gF,
+              void* mF, const void* dgF, const void* dmF, void* dQW, void* dWn, void* dQB, void* dBlim, void* dBnf,
+              cudaStream_t s) {
+    using namespace gam_adj;
+    const GamBox b = torch_box(p->Nip, p->Njp, p->Nkp);
+    const DevParams<R> P = dev_params<R>(p);
+    Geo<R> g;
+    memset(&g, 0, sizeof(g));
+    g.vol = (const R*)vol; g.face = (const R*)face; g.Tf = (const R*)Tf;
+    g.fcB0 = fcB0; g.bFlux0 = bFlux0;
+    Work<R> w;
+    memset(&w, 0, sizeof(w));
+    w.QW = (R*)QW; w.Wn = (R*)Wn; w.QB = (R*)QB; w.Bnf = (R*)Bnf; w.gF = (R*)gF; w.mF = (R*)mF;
+    GamScalars* sc = nullptr;
+    if (cudaGetSymbolAddress((void**)&sc, g_adj_scalars) != cudaSuccess) return GAM_ECUDA;
+    const int G = GAM_NG;
+    const Range fr[3] = {{G, G + b.Nip, G, G + b.Njp - 1, G, G + b.Nkp - 1},
+                         {G, G + b.Nip - 1, G, G + b.Njp, G, G + b.Nkp - 1},
+                         {G, G + b.Nip - 1, G, G + b.Njp - 1, G, G + b.Nkp}};
+    const dim3 blk(16, 8, 1);
+    auto grid = [&](const Range& r) {
+        return dim3((unsigned)((r.i1 - r.i0 + 1 + blk.x - 1) / blk.x), (unsigned)((r.j1 - r.j0 + 1 + blk.y - 1) / blk.y),
+                    (unsigned)((r.k1 - r.k0 + 1 + blk.z - 1) / blk.z));
+    };
+    const R* Bl = (const R*)Blim;
+    if (!dgF) {
+        k_stress<R, 0, 1><<<grid(fr[0]), blk, 0, s>>>(b, P, g, Bl, w, fr[0], sc);
+        k_stress<R, 1, 1><<<grid(fr[1]), blk, 0, s>>>(b, P, g, Bl, w, fr[1], sc);
+        k_stress<R, 2, 1><<<grid(fr[2]), blk, 0, s>>>(b, P, g, Bl, w, fr[2], sc);
+    } else {
+        const R* a = (const R*)dgF;
+        const R* m = (const R*)dmF;
+        k_stress_adj<R, 0><<<grid(fr[0]), blk, 0, s>>>(b, P, g, Bl, w, fr[0], a, m, (R*)dQW, (R*)dWn, (R*)dQB,
+                                                        (R*)dBlim, (R*)dBnf);
+        k_stress_adj<R, 1><<<grid(fr[1]), blk, 0, s>>>(b, P, g, Bl, w, fr[1], a, m, (R*)dQW, (R*)dWn, (R*)dQB,
+                                                        (R*)dBlim, (R*)dBnf);
+        k_stress_adj<R, 2><<<grid(fr[2]), blk, 0, s>>>(b, P, g, Bl, w, fr[2], a, m, (R*)dQW, (R*)dWn, (R*)dQB,
+                                                        (R*)dBlim, (R*)dBnf);
+    }
+    return cudaGetLastError() == cudaSuccess ? GAM_OK : GAM_ECUDA;
+}
+int check(const gam_params* p, int32_t fp32) {
+    if (!p) return GAM_EINVAL;
+    if (p->rmeth != GAM_RECON_8CENT) return GAM_EINVAL;  // the adjoint covers 8CENT
+    if (p->nG != 4 || p->Nip < 1 || p->Njp < 1 || p->Nkp < 1 || p->do25D) return GAM_EBADDIM;
+    (void)fp32;
+    return GAM_OK;
+}
+}  // namespace
+
+extern "C" int gam_flux_forward(const gam_params* p, int32_t fp32, const void* QW, const void* Wn, const void* QB,
+                                const void* Blim, const void* Bnf, const void* volume, const void* face,
+                                const void* Tf, const double* fcB0, const double* bFlux0, void* gF, void* mF,
+                                void* stream) {
+    int rc = check(p, fp32);
+    if (rc) return rc;
+    if (!QW || !Wn || !QB || !Blim || !Bnf || !volume || !face || !Tf || !gF || !mF) return GAM_EINVAL;
+    if (p->doBackground && (!fcB0 || !bFlux0)) return GAM_EINVAL;
+    cudaStream_t s = (cudaStream_t)stream;
+    return fp32 ? flux_call<float>(p, QW, Wn, QB, Blim, Bnf, volume, face, Tf, fcB0, bFlux0, gF, mF, nullptr, nullptr,
+                                   nullptr, nullptr, nullptr, nullptr, nullptr, s)
+                : flux_call<double>(p, QW, Wn, QB, Blim, Bnf, volume, face, Tf, fcB0, bFlux0, gF, mF, nullptr, nullptr,
+                                    nullptr, nullptr, nullptr, nullptr, nullptr, s);
+}
+
+extern "C" int gam_flux_adjoint(const gam_params* p, int32_t fp32, const void* QW, const void* Wn, const void* QB,
+                                const void* Blim, const void* Bnf, const void* volume, const void* face,
+                                const void* Tf, const double* fcB0, const double* bFlux0, const void* dgF,
+                                const void* dmF, void* dQW, void* dWn, void* dQB, void* dBlim, void* dBnf,
+                                void* stream) {
+    int rc = check(p, fp32);
+    if (rc) return rc;
+    if (!QW || !Wn || !QB || !Blim || !Bnf || !volume || !face || !Tf || !dgF || !dmF || !dQW || !dWn || !dQB ||
+        !dBlim || !dBnf)
+        return GAM_EINVAL;
+    if (p->doBackground && (!fcB0 || !bFlux0)) return GAM_EINVAL;
+    cudaStream_t s = (cudaStream_t)stream;
+    return fp32 ? flux_call<float>(p, QW, Wn, QB, Blim, Bnf, volume, face, Tf, fcB0, bFlux0, nullptr, nullptr, dgF,
+                                   dmF, dQW, dWn, dQB, dBlim, dBnf, s)
+                : flux_call<double>(p, QW, Wn, QB, Blim, Bnf, volume, face, Tf, fcB0, bFlux0, nullptr, nullptr, dgF,
+                                    dmF, dQW, dWn, dQB, dBlim, dBnf, s);
+}

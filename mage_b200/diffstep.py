@@ -203,6 +203,9 @@ class Grid:
         if background is not None:
             self.bg = {k: torch.as_tensor(self._cellpad(background[k]), dtype=torch.float64, device=device)
                        for k in ("fcB0", "bFlux0", "edgB0", "B0", "dpB0")}
+        # the flux stage and its adjoint as hand-written CUDA kernels (on CUDA
+        # tensors, 8CENT); False: the PyTorch expressions and autograd
+        self.cuda_flux = torch.device(device).type == "cuda" and not P.up7
         self.wind = None
         if P.bc[1] == 4:
             assert wind is not None, "the solar-wind boundary needs the wind state"
@@ -429,7 +432,11 @@ def step(g: Grid, cur: dict, old: dict, dt: float, odt: float):
     fr = [(G, G + Np[0], G, G + Np[1] - 1, G, G + Np[2] - 1), (G, G + Np[0] - 1, G, G + Np[1], G, G + Np[2] - 1),
           (G, G + Np[0] - 1, G, G + Np[1] - 1, G, G + Np[2])]
     gF, mF = [], []
-    for D in range(3):
+    if g.cuda_flux:
+        gFa, mFa = _FluxFn.apply(QW, WnB, QB, Blim, Bnf, g)
+        gF = [gFa[5 * D:5 * D + 5] for D in range(3)]
+        mF = [mFa[3 * D:3 * D + 3] for D in range(3)]
+    for D in ([] if g.cuda_flux else range(3)):
         r = fr[D]
         T = [win(g.Tf[n + 9 * D], r) for n in range(9)]
         fa = win(A[D], r)
@@ -528,6 +535,71 @@ def step(g: Grid, cur: dict, old: dict, dt: float, odt: float):
     mfs = mfn.reshape(3, -1)
     mfn = torch.stack([mfs[d][g.bc_src[d]] for d in range(3)]).reshape(mfn.shape)
     return {"Gas": Gas, "mf": mfn, "B": g.bxyz(mfn)}
+
+
+def _flux_params(g: Grid):
+    from mage_b200.gamera import GamParams
+    P = g.P
+    gp = GamParams(P.Nip, P.Njp, P.Nkp, gamma=P.gamma, CFL=P.CFL, pdmb=P.pdmb, Vd0=P.Vd0, cHogH=P.cHogH,
+                   dFloor=P.dFloor, pFloor=P.pFloor, doBackground=g.bg is not None)
+    return gp.to_c()
+
+
+class _FluxFn(torch.autograd.Function):
+    """CalcStress on the GPU (gam_flux_forward) with the hand-written adjoint
+    (gam_flux_adjoint) as its backward."""
+
+    @staticmethod
+    def forward(ctx, QW, Wn, QB, Blim, Bnf, g):
+        import ctypes as C
+        from mage_b200.gamera import load_library
+        L = load_library()
+        ins = [t.contiguous() for t in (QW, Wn, QB, Blim, Bnf)]
+        shp = g.face.shape[1:]
+        gF = torch.zeros((15,) + tuple(shp), dtype=QW.dtype, device=QW.device)
+        mF = torch.zeros((9,) + tuple(shp), dtype=QW.dtype, device=QW.device)
+        p = _flux_params(g)
+        bg = g.bg
+        geo = [g.vol.contiguous(), g.face.contiguous(), g.Tf.contiguous()]
+        fc = bg["fcB0"].contiguous().data_ptr() if bg is not None else None
+        bf = bg["bFlux0"].contiguous().data_ptr() if bg is not None else None
+        st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+        rc = L.gam_flux_forward(C.byref(p), int(QW.dtype == torch.float32), *[C.c_void_p(t.data_ptr()) for t in ins],
+                                *[C.c_void_p(t.data_ptr()) for t in geo],
+                                C.cast(C.c_void_p(fc), C.POINTER(C.c_double)) if fc else None,
+                                C.cast(C.c_void_p(bf), C.POINTER(C.c_double)) if bf else None,
+                                C.c_void_p(gF.data_ptr()), C.c_void_p(mF.data_ptr()), st)
+        if rc != 0:
+            raise RuntimeError(f"gam_flux_forward failed ({rc})")
+        ctx.save_for_backward(*ins)
+        ctx.g = g
+        return gF, mF
+
+    @staticmethod
+    def backward(ctx, dgF, dmF):
+        import ctypes as C
+        from mage_b200.gamera import load_library
+        L = load_library()
+        g = ctx.g
+        ins = ctx.saved_tensors
+        dgF = torch.zeros_like(ins[0][:1]).expand(15, *ins[0].shape[1:]).contiguous() if dgF is None else dgF.contiguous()
+        dmF = torch.zeros_like(ins[0][:1]).expand(9, *ins[0].shape[1:]).contiguous() if dmF is None else dmF.contiguous()
+        outs = [torch.zeros_like(t) for t in ins]
+        p = _flux_params(g)
+        bg = g.bg
+        geo = [g.vol.contiguous(), g.face.contiguous(), g.Tf.contiguous()]
+        fc = bg["fcB0"].contiguous().data_ptr() if bg is not None else None
+        bf = bg["bFlux0"].contiguous().data_ptr() if bg is not None else None
+        st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+        rc = L.gam_flux_adjoint(C.byref(p), int(ins[0].dtype == torch.float32),
+                                *[C.c_void_p(t.data_ptr()) for t in ins], *[C.c_void_p(t.data_ptr()) for t in geo],
+                                C.cast(C.c_void_p(fc), C.POINTER(C.c_double)) if fc else None,
+                                C.cast(C.c_void_p(bf), C.POINTER(C.c_double)) if bf else None,
+                                C.c_void_p(dgF.data_ptr()), C.c_void_p(dmF.data_ptr()),
+                                *[C.c_void_p(t.data_ptr()) for t in outs], st)
+        if rc != 0:
+            raise RuntimeError(f"gam_flux_adjoint failed ({rc})")
+        return (*outs, None)
 
 
 def _iside_bcs(g: Grid, Gas, mf, B):
