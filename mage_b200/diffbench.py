@@ -12,7 +12,7 @@ PyTorch forward along a random direction.
 
 c5: the dipole-in-wind set-up on the spherical 192x192x256 grid (background
 field, inner sphere, solar wind, zero-gradient axis) with 1e-3 relative noise
-on the conserved variables; loss = sum of |Bxyz|^2
+on the conserved variables and 1e-3 x face area on the face fluxes; loss = sum of |Bxyz|^2
 (the field without the dipole) over active cells with r < 6; FP32 and FP64
 gradients with checkpoints every 14 steps and one step's graph at a time.
 
@@ -142,11 +142,12 @@ def c5(N=(192, 192, 256), nsteps=200, seg=14, precisions=("fp32", "fp64"), seed=
     bg = gpu.get_background()
     del gpu
     P = DiffParams(*N, bc=DIPOLE_BCS)
-    # relative noise 1e-3 on the conserved variables: the wind start is uniform
-    # in v and P, and at exact ties of the limiter the two precisions would
-    # pick different (equally valid) subgradients
+    # noise on the conserved variables and the fluxes: the wind start is
+    # uniform in v, P and B, and at exact ties of the limiter the two precisions
+    # would pick different (equally valid) subgradients
     rng = np.random.default_rng(seed)
     G64 = st["Gas"] * (1 + 1e-3 * rng.standard_normal(st["Gas"].shape))
+    F64 = st["magFlux"] + 1e-3 * np.asarray(geo["face"]) * rng.standard_normal(st["magFlux"].shape)
     out = {"config": f"dipole in a solar wind, spherical {N[0]}x{N[1]}x{N[2]}, {nsteps} fixed-dt steps (dt = {dt:.4g})",
            "loss": "sum |Bxyz|^2 (field without the dipole) over active cells with r < 6",
            "wrt": "start Gas and face fluxes",
@@ -164,7 +165,7 @@ def c5(N=(192, 192, 256), nsteps=200, seg=14, precisions=("fp32", "fp64"), seed=
             B = win(state["B"], act)
             return ((B * B).sum(dim=0) * mask).sum()
 
-        Gas0, mf0 = g.cell_box(G64).to(dtype), g.face_box(st["magFlux"])
+        Gas0, mf0 = g.cell_box(G64).to(dtype), g.face_box(F64)
         (L, gG, gF), el, mem = _timed(lambda: loss_and_grad(g, Gas0, mf0, dt, nsteps, seg=seg, lossf=lossf,
                                                              per_step=True))
         out[name] = {"loss": L, "fwd_plus_adjoint_s": el, "s_per_step": el / nsteps, "peak_hbm_gb": mem}

@@ -61,9 +61,10 @@ def _grads(g, Gas0, mf0, dt, nst, cuda_flux, **kw):
 
 
 def test_hand_written_flux_adjoint_matches_autograd():
-    """The flux stage's hand-written CUDA adjoint (gam_flux_adjoint) inside the
-    reverse sweep gives the gradient of the pure-autograd sweep to <= 1e-11
-    relative (L2), FP64; the CUDA flux forward changes the loss by <= 1e-14."""
+    """The hand-written CUDA adjoints of the flux stage (gam_flux_adjoint) and
+    of the electric-field stage (gam_efield_adjoint) inside the reverse sweep
+    give the gradient of the pure-autograd sweep to <= 1e-11 relative (L2),
+    FP64; their CUDA forwards change the loss by <= 1e-14."""
     N, dt, nst = (16, 16, 16), 5e-4, 4
     gpu = GameraGPU(GamParams(*N))
     gpu.set_geometry(grids.warped_periodic_corners(*N))
@@ -95,12 +96,12 @@ def test_hand_written_flux_adjoint_dipole():
     g = Grid(DiffParams(*N, bc=DIPOLE_BCS), gpu.get_geometry_arrays(), background=gpu.get_background(), wind=w,
              device="cuda")
     dt = 0.5 * st["dt"]
-    # the wind start is uniform in v and P: exact ties in the limiter, where the
+    # the wind start is uniform in v, P and B: exact ties in the limiter, where the
     # two sweeps may pick different (equally valid) subgradients; noise lifts them
     rng = np.random.default_rng(5)
     Gas0 = g.cell_box(st["Gas"]) * (1 + 1e-3 * torch.as_tensor(rng.standard_normal((5,) + g.face.shape[1:]),
                                                                device="cuda"))
-    mf0 = g.face_box(st["magFlux"])
+    mf0 = g.face_box(st["magFlux"]) + 1e-3 * g.face * torch.as_tensor(rng.standard_normal(g.face.shape), device="cuda")
     act = (4, 4 + N[0] - 1, 4, 4 + N[1] - 1, 4, 4 + N[2] - 1)
 
     def lossf(gr, state):
