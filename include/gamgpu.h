@@ -230,6 +230,23 @@ int gam_flux_adjoint(const gam_params* p, int32_t fp32, const void* QW, const vo
                      const double* fcB0, const double* bFlux0, const void* dgF, const void* dmF, void* dQW,
                      void* dWn, void* dQB, void* dBlim, void* dBnf, void* stream);
 
+/* Electric-field stage (CalcElecField: Mom2Face and the edge EMF loop,
+ * fields.F90:70-517) and its hand-written adjoint, in the layout above.
+ * Inputs: Dh = half-state density (1), abh = area x flux/max(area,TINY) (3),
+ * bn = limiter flux/max(area,TINY) (3), VdV = volume x momentum/density (3),
+ * volume, face (3), edge (3), Te (27), Teb (12), edgB0 (6, FP64) when
+ * doBackground, dt; AVf is a 9-component scratch array. gam_efield_forward
+ * writes E (3) over the edge ranges; gam_efield_adjoint adds the adjoints of
+ * Dh, abh, bn and VdV for the adjoint dE (caller-zeroed outputs; dAVf is a
+ * 3-component scratch array). No counterpart in the reference. */
+int gam_efield_forward(const gam_params* p, int32_t fp32, const void* Dh, const void* abh, const void* bn,
+                       const void* VdV, const void* volume, const void* face, const void* edge, const void* Te,
+                       const void* Teb, const double* edgB0, double dt, void* AVf, void* E, void* stream);
+int gam_efield_adjoint(const gam_params* p, int32_t fp32, const void* Dh, const void* abh, const void* bn,
+                       const void* VdV, const void* volume, const void* face, const void* edge, const void* Te,
+                       const void* Teb, const double* edgB0, double dt, void* AVf, const void* dE, void* dDh,
+                       void* dabh, void* dbn, void* dVdV, void* dAVf, void* stream);
+
 /* Conserved totals for callers that cannot allocate device memory.
  * No counterpart in the reference. Some callers cannot call cudaMalloc while
  * they run: their device memory belongs to another framework's pool, or they

@@ -276,6 +276,137 @@ __global__ void __launch_bounds__(128) k_stress_adj(GamBox b, DevParams<R> P, Ge
         }
 }
 
+
+// reverse of edge_lrs (EdgeLRs for faces of direction a along bd): adjoints of
+// bL*Vi, bR*Vi -> the abh (8) and bn (4) stencils
+template <class R>
+__device__ void edge_lrs_adj(const GamBox& b, const DevParams<R>& P, const Geo<R>& g, const Work<R>& w, long c, int a,
+                             int bd, double aBL, double aBR, R* dabh, R* dbn) {
+    const long fs = b.fs;
+    const long s = dstride(b, bd);
+    R qdv[8], area[8], nmag[4];
+    for (int n = 0; n < 8; n++) {
+        area[n] = g.face[a * fs + c + (n - 4) * s];
+        qdv[n] = w.abh[a * fs + c + (n - 4) * s];
+    }
+    for (int m = 0; m < 4; m++) nmag[m] = w.bn[a * fs + c + (m - 2) * s];
+    const R Vi = central8(area);
+    double aq[8], av[4];
+    lrs_adj(P.pdmb, qdv, nmag, Vi, aBL * (double)Vi, aBR * (double)Vi, aq, av);
+    for (int n = 0; n < 8; n++) atomicAdd(&dabh[a * fs + c + (n - 4) * s], (R)aq[n]);
+    for (int m = 0; m < 4; m++) atomicAdd(&dbn[a * fs + c + (m - 2) * s], (R)av[m]);
+}
+
+// Adjoint of the edge EMF of direction eD (k_vxb) over the range r: dE ->
+// dDh, dabh, dbn, dAVf (the AVf of this eD, 3 components, caller-zeroed)
+template <class R>
+__global__ void __launch_bounds__(128) k_vxb_adj(GamBox b, DevParams<R> P, Geo<R> g, Work<R> w, int eD, Range r,
+                                                 double dt, const R* __restrict__ dE, R* dDh, R* dabh, R* dbn,
+                                                 R* dAVf) {
+    int ii, jj, kk;
+    if (!thread_ijk(r, ii, jj, kk)) return;
+    int dT1, dT2;
+    edge_dirs(eD, dT1, dT2);
+    const long fs = b.fs;
+    const long c = lidx(b, ii, jj, kk);
+    const int e1 = eD == 0 ? 1 : 0, e2 = eD == 2 ? 1 : 2;
+    const long s1 = dstride(b, e1), s2 = dstride(b, e2);
+    // forward recompute (k_vxb)
+    const R Dc = (R)0.25 * (w.Dh[c] + w.Dh[c - s1] + w.Dh[c - s2] + w.Dh[c - s1 - s2]);
+    R area1[8], area2[8];
+    R bT1L, bT1R, fA1, bT2L, bT2R, fA2;
+    edge_lrs(b, P, g, w, c, dT1, dT2, area1, bT1L, bT1R, fA1);
+    edge_lrs(b, P, g, w, c, dT2, dT1, area2, bT2L, bT2R, fA2);
+    const R dA = rmax(fA1, (R)TINY);
+    R VC[3];
+    const long s2v = dstride(b, dT2);
+    for (int x = 0; x < 3; x++) {
+        R acc = (R)0;
+        for (int n = 0; n < 8; n++) acc += Rc<R>(w8(n)) * w.AVf[(x + 3 * eD) * fs + c + (n - 4) * s2v];
+        VC[x] = acc / dA;
+    }
+    const R* Te = g.Te;
+    R T1[3], T2[3];
+    for (int x = 0; x < 3; x++) {
+        T1[x] = Te[(3 + x + 9 * eD) * fs + c];
+        T2[x] = Te[(6 + x + 9 * eD) * fs + c];
+    }
+    const R v1 = VC[0] * T1[0] + VC[1] * T1[1] + VC[2] * T1[2];
+    const R v2 = VC[0] * T2[0] + VC[1] * T2[1] + VC[2] * T2[2];
+    const R vD0 = Mth<R>::sqrt_(v1 * v1 + v2 * v2);
+    const R xni = g.Teb[(0 + 4 * eD) * fs + c], yni = g.Teb[(1 + 4 * eD) * fs + c];
+    const R xnj = g.Teb[(2 + 4 * eD) * fs + c], ynj = g.Teb[(3 + 4 * eD) * fs + c];
+    const R detT = (R)1 / (xni * ynj - xnj * yni);
+    const R bT1 = (R)0.5 * (bT1L + bT1R) / fA1;
+    const R bT2 = (R)0.5 * (bT2L + bT2R) / fA2;
+    const R db1 = (bT1R - bT1L) / fA1;
+    const R db2 = (bT2R - bT2L) / fA2;
+    const R Jd = db2 - db1;
+    R b1 = detT * (ynj * bT1 - yni * bT2);
+    R b2 = detT * (-(xnj * bT1) + xni * bT2);
+    if (P.doBackground) {
+        b1 = b1 + (R)g.edgB0[(0 + 2 * eD) * fs + c];
+        b2 = b2 + (R)g.edgB0[(1 + 2 * eD) * fs + c];
+    }
+    const R m = Mth<R>::sqrt_(b1 * b1 + b2 * b2), q = Mth<R>::sqrt_(Dc);
+    const R vA = m / q;
+    const R vDp = vD0 + vA;
+    const R edge = g.edge[eD * fs + c];
+    const R cap = P.CFL * edge / (R)dt;
+    const R vDiff = rmin(vDp, cap);
+    // reverse
+    const double a_e = (double)dE[eD * fs + c] * (double)edge;
+    const double a_v1 = -a_e * b2, a_b2e = -a_e * v1, a_v2 = a_e * b1, a_b1e = a_e * v2;
+    const double a_vDiff = a_e * P.Vd0 * Jd, a_Jd = a_e * P.Vd0 * vDiff;
+    const double a_vDp = (cap < vDp) ? 0.0 : a_vDiff;
+    double a_b1 = a_b1e, a_b2 = a_b2e, a_v1t = a_v1, a_v2t = a_v2;
+    const double a_m = a_vDp / (double)q;
+    const double a_q = -a_vDp * (double)m / ((double)q * (double)q);
+    const double a_Dc = a_q * 0.5 / (double)q;
+    if (m > (R)0) {
+        a_b1 += a_m * b1 / m;
+        a_b2 += a_m * b2 / m;
+    }
+    if (vD0 > (R)0) {
+        a_v1t += a_vDp * v1 / vD0;
+        a_v2t += a_vDp * v2 / vD0;
+    }
+    const double a_bT1 = a_b1 * detT * ynj - a_b2 * detT * xnj;
+    const double a_bT2 = -a_b1 * detT * yni + a_b2 * detT * xni;
+    const double a_db2 = a_Jd, a_db1 = -a_Jd;
+    const double aT1R = a_db1 / fA1 + a_bT1 * 0.5 / fA1, aT1L = -a_db1 / fA1 + a_bT1 * 0.5 / fA1;
+    const double aT2R = a_db2 / fA2 + a_bT2 * 0.5 / fA2, aT2L = -a_db2 / fA2 + a_bT2 * 0.5 / fA2;
+    edge_lrs_adj(b, P, g, w, c, dT1, dT2, aT1L, aT1R, dabh, dbn);
+    edge_lrs_adj(b, P, g, w, c, dT2, dT1, aT2L, aT2R, dabh, dbn);
+    for (int x = 0; x < 3; x++) {
+        const double aVC = a_v1t * T1[x] + a_v2t * T2[x];
+        for (int n = 0; n < 8; n++) atomicAdd(&dAVf[x * fs + c + (n - 4) * s2v], (R)(w8(n) * aVC / (double)dA));
+    }
+    const long cc[4] = {c, c - s1, c - s2, c - s1 - s2};
+    for (int n = 0; n < 4; n++) atomicAdd(&dDh[cc[n]], (R)(0.25 * a_Dc));
+}
+
+// Adjoint of Mom2Face for edge direction eD over the range r: dAVf -> dVdV
+template <class R>
+__global__ void __launch_bounds__(256) k_m2f_adj(GamBox b, Geo<R> g, int eD, Range r, const R* __restrict__ dAVf,
+                                                 R* dVdV) {
+    int ii, jj, kk;
+    if (!thread_ijk(r, ii, jj, kk)) return;
+    int dT1, dT2;
+    edge_dirs(eD, dT1, dT2);
+    const long fs = b.fs;
+    const long c = lidx(b, ii, jj, kk);
+    const long s = dstride(b, dT1);
+    R vol[8];
+    for (int n = 0; n < 8; n++) vol[n] = g.vol[c + (n - 4) * s];
+    const R dV = rmax(central8(vol), (R)TINY);
+    const R A = g.face[dT1 * fs + c];
+    for (int x = 0; x < 3; x++) {
+        const double a = (double)dAVf[x * fs + c] * (double)A / (double)dV;
+        if (a == 0.0) continue;
+        for (int n = 0; n < 8; n++) atomicAdd(&dVdV[x * fs + c + (n - 4) * s], (R)(w8(n) * a));
+    }
+}
 }  // namespace gam_adj
 
 // ------------------------------------------------------------ C ABI
@@ -386,4 +517,88 @@ extern "C" int gam_flux_adjoint(const gam_params* p, int32_t fp32, const void* Q
                                    dmF, dQW, dWn, dQB, dBlim, dBnf, s)
                 : flux_call<double>(p, QW, Wn, QB, Blim, Bnf, volume, face, Tf, fcB0, bFlux0, nullptr, nullptr, dgF,
                                     dmF, dQW, dWn, dQB, dBlim, dBnf, s);
+}
+
+namespace {
+template <class R>
+int efield_call(const gam_params* p, const void* Dh, const void* abh, const void* bn, const void* VdV, const void* vol,
+                const void* face, const void* edge, const void* Te, const void* Teb, const double* edgB0, double dt,
+                void* AVf, void* E, const void* dE, void* dDh, void* dabh, void* dbn, void* dVdV, void* dAVf,
+                cudaStream_t s) {
+    using namespace gam_adj;
+    const GamBox b = torch_box(p->Nip, p->Njp, p->Nkp);
+    const DevParams<R> P = dev_params<R>(p);
+    Geo<R> g;
+    memset(&g, 0, sizeof(g));
+    g.vol = (const R*)vol; g.face = (const R*)face; g.edge = (const R*)edge; g.Te = (const R*)Te; g.Teb = (const R*)Teb;
+    g.edgB0 = edgB0;
+    Work<R> w;
+    memset(&w, 0, sizeof(w));
+    w.Dh = (R*)Dh; w.abh = (R*)abh; w.bn = (R*)bn; w.VdV = (R*)VdV; w.AVf = (R*)AVf; w.E = (R*)E;
+    GamScalars hs;
+    memset(&hs, 0, sizeof(hs));
+    hs.dt = dt;
+    if (cudaMemcpyToSymbolAsync(g_adj_scalars, &hs, sizeof(hs), 0, cudaMemcpyHostToDevice, s) != cudaSuccess)
+        return GAM_ECUDA;
+    GamScalars* sc = nullptr;
+    if (cudaGetSymbolAddress((void**)&sc, g_adj_scalars) != cudaSuccess) return GAM_ECUDA;
+    const int G = GAM_NG;
+    const Range mf[3] = {{0, b.Ni - 1, G, G + b.Njp, 0, b.Nk - 1},
+                         {0, b.Ni - 1, 0, b.Nj - 1, G, G + b.Nkp},
+                         {G, G + b.Nip, 0, b.Nj - 1, 0, b.Nk - 1}};
+    const Range ed[3] = {{G, G + b.Nip - 1, G, G + b.Njp, G, G + b.Nkp},
+                         {G, G + b.Nip, G, G + b.Njp - 1, G, G + b.Nkp},
+                         {G, G + b.Nip, G, G + b.Njp, G, G + b.Nkp - 1}};
+    const dim3 blk(32, 4, 1);
+    auto grid = [&](const Range& r) {
+        return dim3((unsigned)((r.i1 - r.i0 + 1 + blk.x - 1) / blk.x), (unsigned)((r.j1 - r.j0 + 1 + blk.y - 1) / blk.y),
+                    (unsigned)((r.k1 - r.k0 + 1 + blk.z - 1) / blk.z));
+    };
+    for (int eD = 0; eD < 3; eD++) {
+        k_mom2face<R><<<grid(mf[eD]), blk, 0, s>>>(b, P, g, w, eD, mf[eD], sc);
+        if (!dE) {
+            k_vxb<R><<<grid(ed[eD]), blk, 0, s>>>(b, P, g, w, eD, ed[eD], sc);
+        } else {
+            if (cudaMemsetAsync(dAVf, 0, 3 * b.fs * sizeof(R), s) != cudaSuccess) return GAM_ECUDA;
+            k_vxb_adj<R><<<grid(ed[eD]), blk, 0, s>>>(b, P, g, w, eD, ed[eD], dt, (const R*)dE, (R*)dDh, (R*)dabh,
+                                                       (R*)dbn, (R*)dAVf);
+            k_m2f_adj<R><<<grid(mf[eD]), blk, 0, s>>>(b, g, eD, mf[eD], (const R*)dAVf, (R*)dVdV);
+        }
+    }
+    return cudaGetLastError() == cudaSuccess ? GAM_OK : GAM_ECUDA;
+}
+}  // namespace
+
+extern "C" int gam_efield_forward(const gam_params* p, int32_t fp32, const void* Dh, const void* abh, const void* bn,
+                                  const void* VdV, const void* volume, const void* face, const void* edge,
+                                  const void* Te, const void* Teb, const double* edgB0, double dt, void* AVf, void* E,
+                                  void* stream) {
+    int rc = check(p, fp32);
+    if (rc) return rc;
+    if (!Dh || !abh || !bn || !VdV || !volume || !face || !edge || !Te || !Teb || !AVf || !E || !(dt > 0.0))
+        return GAM_EINVAL;
+    if (p->doBackground && !edgB0) return GAM_EINVAL;
+    cudaStream_t s = (cudaStream_t)stream;
+    return fp32 ? efield_call<float>(p, Dh, abh, bn, VdV, volume, face, edge, Te, Teb, edgB0, dt, AVf, E, nullptr,
+                                     nullptr, nullptr, nullptr, nullptr, nullptr, s)
+                : efield_call<double>(p, Dh, abh, bn, VdV, volume, face, edge, Te, Teb, edgB0, dt, AVf, E, nullptr,
+                                      nullptr, nullptr, nullptr, nullptr, nullptr, s);
+}
+
+extern "C" int gam_efield_adjoint(const gam_params* p, int32_t fp32, const void* Dh, const void* abh, const void* bn,
+                                  const void* VdV, const void* volume, const void* face, const void* edge,
+                                  const void* Te, const void* Teb, const double* edgB0, double dt, void* AVf,
+                                  const void* dE, void* dDh, void* dabh, void* dbn, void* dVdV, void* dAVf,
+                                  void* stream) {
+    int rc = check(p, fp32);
+    if (rc) return rc;
+    if (!Dh || !abh || !bn || !VdV || !volume || !face || !edge || !Te || !Teb || !AVf || !dE || !dDh || !dabh ||
+        !dbn || !dVdV || !dAVf || !(dt > 0.0))
+        return GAM_EINVAL;
+    if (p->doBackground && !edgB0) return GAM_EINVAL;
+    cudaStream_t s = (cudaStream_t)stream;
+    return fp32 ? efield_call<float>(p, Dh, abh, bn, VdV, volume, face, edge, Te, Teb, edgB0, dt, AVf, nullptr, dE,
+                                     dDh, dabh, dbn, dVdV, dAVf, s)
+                : efield_call<double>(p, Dh, abh, bn, VdV, volume, face, edge, Te, Teb, edgB0, dt, AVf, nullptr, dE,
+                                      dDh, dabh, dbn, dVdV, dAVf, s);
 }

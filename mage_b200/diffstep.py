@@ -379,7 +379,10 @@ def step(g: Grid, cur: dict, old: dict, dt: float, odt: float):
     ed_r = [(G, G + Np[0] - 1, G, G + Np[1], G, G + Np[2]), (G, G + Np[0], G, G + Np[1] - 1, G, G + Np[2]),
             (G, G + Np[0], G, G + Np[1], G, G + Np[2] - 1)]
     E = []
-    for eD in range(3):
+    if g.cuda_flux:
+        Ea = _EFieldFn.apply(Dh, abh, bn, VdV, g, dt)
+        E = [Ea[0], Ea[1], Ea[2]]
+    for eD in ([] if g.cuda_flux else range(3)):
         dT1, dT2 = (eD + 1) % 3, (eD + 2) % 3
         r = mf_r[eD]
         dV = rmax(central8([win(g.vol, r, unit(dT1, n - 4)) for n in range(8)]), torch.full_like(win(g.vol, r), TINY))
@@ -600,6 +603,61 @@ class _FluxFn(torch.autograd.Function):
         if rc != 0:
             raise RuntimeError(f"gam_flux_adjoint failed ({rc})")
         return (*outs, None)
+
+
+def _ptr(t):
+    import ctypes as C
+    return C.c_void_p(t.data_ptr())
+
+
+class _EFieldFn(torch.autograd.Function):
+    """CalcElecField on the GPU (gam_efield_forward: Mom2Face + the edge EMF
+    kernels) with the hand-written adjoint (gam_efield_adjoint) as backward."""
+
+    @staticmethod
+    def forward(ctx, Dh, abh, bn, VdV, g, dt):
+        import ctypes as C
+        from mage_b200.gamera import load_library
+        L = load_library()
+        ins = [t.contiguous() for t in (Dh, abh, bn, VdV)]
+        shp = tuple(g.face.shape[1:])
+        AVf = torch.zeros((9,) + shp, dtype=abh.dtype, device=abh.device)
+        E = torch.zeros((3,) + shp, dtype=abh.dtype, device=abh.device)
+        p = _flux_params(g)
+        geo = [g.vol.contiguous(), g.face.contiguous(), g.edge.contiguous(), g.Te.contiguous(), g.Teb.contiguous()]
+        eb = g.bg["edgB0"].contiguous().data_ptr() if g.bg is not None else None
+        st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+        rc = L.gam_efield_forward(C.byref(p), int(abh.dtype == torch.float32), *[_ptr(t) for t in ins],
+                                  *[_ptr(t) for t in geo], C.cast(C.c_void_p(eb), C.POINTER(C.c_double)) if eb else None,
+                                  float(dt), _ptr(AVf), _ptr(E), st)
+        if rc != 0:
+            raise RuntimeError(f"gam_efield_forward failed ({rc})")
+        ctx.save_for_backward(*ins)
+        ctx.g, ctx.dt = g, dt
+        return E
+
+    @staticmethod
+    def backward(ctx, dE):
+        import ctypes as C
+        from mage_b200.gamera import load_library
+        L = load_library()
+        g = ctx.g
+        ins = ctx.saved_tensors
+        shp = tuple(g.face.shape[1:])
+        dE = dE.contiguous()
+        outs = [torch.zeros_like(t) for t in ins]
+        AVf = torch.zeros((9,) + shp, dtype=ins[1].dtype, device=ins[1].device)
+        dAVf = torch.zeros((3,) + shp, dtype=ins[1].dtype, device=ins[1].device)
+        p = _flux_params(g)
+        geo = [g.vol.contiguous(), g.face.contiguous(), g.edge.contiguous(), g.Te.contiguous(), g.Teb.contiguous()]
+        eb = g.bg["edgB0"].contiguous().data_ptr() if g.bg is not None else None
+        st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+        rc = L.gam_efield_adjoint(C.byref(p), int(ins[1].dtype == torch.float32), *[_ptr(t) for t in ins],
+                                  *[_ptr(t) for t in geo], C.cast(C.c_void_p(eb), C.POINTER(C.c_double)) if eb else None,
+                                  float(ctx.dt), _ptr(AVf), _ptr(dE), *[_ptr(t) for t in outs], _ptr(dAVf), st)
+        if rc != 0:
+            raise RuntimeError(f"gam_efield_adjoint failed ({rc})")
+        return (*outs, None, None)
 
 
 def _iside_bcs(g: Grid, Gas, mf, B):
