@@ -247,6 +247,27 @@ int gam_efield_adjoint(const gam_params* p, int32_t fp32, const void* Dh, const 
                        const void* Teb, const double* edgB0, double dt, void* AVf, const void* dE, void* dDh,
                        void* dabh, void* dbn, void* dVdV, void* dAVf, void* stream);
 
+/* Predictor (Predictor/PredictCell, mhdgroup.F90:444-615) and update
+ * (applyUpdate/E2Flux/CellMaxwell, mhdgroup.F90:79-329, fields.F90:18-51)
+ * stages and their hand-written adjoints, in the layout above; arrays are
+ * passed as arrays of device pointers.
+ * gam_predict_stage: st = {curGas, curMf, oldGas, oldMf}, geo = {volume, face,
+ *   xfc, xyzcc, dxf (fp32 only: face centroid - cell centroid, 18)}, pdt = dt/2,
+ *   odt = time - otime. Forward (out != NULL): out = {QW, Wn, Dh, VdV, QB, abh,
+ *   Bnf, bn}. Adjoint (out == NULL): din = the adjoints of those eight, aB = a
+ *   3-component scratch array; adds into dst = {dcurGas, dcurMf, doldGas,
+ *   doldMf}. LFM limiter (doLFMLim = 1) only.
+ * gam_update_stage: in = {curGas, curMf, E, gF, mF}, geo = {volume, xfc, xyzcc,
+ *   dxf}, dpB0 (FP64) with doBackground. Forward: out = {nxtGas, nxtMf, nxtB
+ *   (scratch)}. Adjoint: din = {dnxtGas, dnxtMf}, scratch sU (5) and sM (3);
+ *   adds into dst = {dcurGas, dcurMf, dE, dgF, dmF}.
+ * No counterpart in the reference. */
+int gam_predict_stage(const gam_params* p, int32_t fp32, const void* const* st, const void* const* geo, double pdt,
+                      double odt, void* const* out, const void* const* din, void* aB, void* const* dst, void* stream);
+int gam_update_stage(const gam_params* p, int32_t fp32, const void* const* in, const void* const* geo,
+                     const double* dpB0, double dt, void* const* out, const void* const* din, void* sU, void* sM,
+                     void* const* dst, void* stream);
+
 /* Conserved totals for callers that cannot allocate device memory.
  * No counterpart in the reference. Some callers cannot call cudaMalloc while
  * they run: their device memory belongs to another framework's pool, or they

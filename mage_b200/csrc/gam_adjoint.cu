@@ -407,6 +407,305 @@ __global__ void __launch_bounds__(256) k_m2f_adj(GamBox b, Geo<R> g, int eD, Ran
         for (int n = 0; n < 8; n++) atomicAdd(&dVdV[x * fs + c + (n - 4) * s], (R)(w8(n) * a));
     }
 }
+
+// ----------------------------------------------------------------- predictor and update
+// reverse of cell_c2p (CellC2P): aW (5) -> aU (5)
+__device__ void c2p_adj(double dF, double pF, double gm1, const double* U, const double* aW, double* aU) {
+    const double rho = U[0];
+    const double V[3] = {U[1] / rho, U[2] / rho, U[3] / rho};
+    const double KinE = 0.5 * rho * (V[0] * V[0] + V[1] * V[1] + V[2] * V[2]);
+    const double p = gm1 * (U[4] - KinE);
+    double a_rho = (rho < dF) ? 0.0 : aW[0];
+    double a_V[3] = {aW[1], aW[2], aW[3]};
+    double a_E = 0.0, a_KinE = 0.0;
+    if (!(p < pF)) { a_E = aW[4] * gm1; a_KinE = -aW[4] * gm1; }
+    a_rho += a_KinE * 0.5 * (V[0] * V[0] + V[1] * V[1] + V[2] * V[2]);
+    for (int x = 0; x < 3; x++) a_V[x] += a_KinE * rho * V[x];
+    for (int x = 0; x < 3; x++) {
+        aU[1 + x] += a_V[x] / rho;
+        a_rho += -a_V[x] * V[x] / rho;
+    }
+    aU[0] += a_rho;
+    aU[4] += a_E;
+}
+// reverse of cell_p2c (CellP2C): aU (5) -> aW (5)
+__device__ void p2c_adj(double dF, double pF, double gm1, const double* W, const double* aU, double* aW) {
+    const double rho = W[0] < dF ? dF : W[0];
+    const double V[3] = {W[1], W[2], W[3]};
+    const double V2 = V[0] * V[0] + V[1] * V[1] + V[2] * V[2];
+    double a_rho = aU[0] + aU[4] * 0.5 * V2;
+    for (int x = 0; x < 3; x++) {
+        a_rho += aU[1 + x] * V[x];
+        aW[1 + x] += aU[1 + x] * rho + aU[4] * rho * V[x];
+    }
+    aW[4] += (W[4] < pF) ? 0.0 : aU[4] / gm1;
+    aW[0] += (W[0] < dF) ? 0.0 : a_rho;
+}
+// reverse of block_c2p (BlockCon2Prim): aW (5) -> aU (5)
+__device__ void bc2p_adj(double dF, double pF, double gm1, const double* U, const double* aW, double* aU) {
+    const double D = U[0] < dF ? dF : U[0];
+    const double M[3] = {U[1], U[2], U[3]};
+    const double M2 = M[0] * M[0] + M[1] * M[1] + M[2] * M[2];
+    const double KinE = 0.5 * M2 / D;
+    const double p = gm1 * (U[4] - KinE);
+    double a_D = aW[0], a_M[3];
+    for (int x = 0; x < 3; x++) {
+        a_M[x] = aW[1 + x] / D;
+        a_D += -aW[1 + x] * M[x] / (D * D);
+    }
+    double a_E = 0.0, a_KinE = 0.0;
+    if (!(p < pF)) { a_E = aW[4] * gm1; a_KinE = -aW[4] * gm1; }
+    for (int x = 0; x < 3; x++) a_M[x] += a_KinE * M[x] / D;
+    a_D += -a_KinE * 0.5 * M2 / (D * D);
+    aU[0] += (U[0] < dF) ? 0.0 : a_D;
+    for (int x = 0; x < 3; x++) aU[1 + x] += a_M[x];
+    aU[4] += a_E;
+}
+
+// d B_x / d (flux of face f of cell c), f = 0..5 (I-, I+, J-, J+, K-, K+), as
+// in gamCellBxyz: (xfc - xyzcc)/V with the sign of the face
+template <class R>
+__device__ __forceinline__ double dbdf(const GamBox& b, const Geo<R>& g, long c, int f, int x) {
+    const long fs = b.fs;
+    const int d = f >> 1, up = f & 1;
+    double off;
+    if constexpr (std::is_same<R, float>::value) {
+        off = g.dxf[(x + 3 * f) * fs + c];
+    } else {
+        const long cf = c + (up ? dstride(b, d) : 0L);
+        off = (double)g.xfc[(x + 3 * d) * fs + cf] - (double)g.xyzcc[x * fs + c];
+    }
+    return (up ? off : -off) / (double)g.vol[c];
+}
+
+// predictor adjoint, cells: dQW, dWn, dDh, dVdV, dQB -> dGas, doGas; writes
+// aB = volume * dQB (the adjoint of the half-state Bxyz) for the face pass
+template <class R>
+__global__ void __launch_bounds__(128) k_predict_adj_cells(GamBox b, DevParams<R> P, Geo<R> g, StateBuf<R> cur,
+                                                           StateBuf<R> old, double pdt, double odt, Work<R> dw,
+                                                           R* dGas, R* doGas, R* aB) {
+    int ii, jj, kk;
+    Range r{0, b.Ni - 1, 0, b.Nj - 1, 0, b.Nk - 1};
+    if (!thread_ijk(r, ii, jj, kk)) return;
+    const long fs = b.fs, c = lidx(b, ii, jj, kk);
+    const double dF = P.dFloor, pF = P.pFloor, gm1 = P.gm1;
+    double Q[5], oQ[5], W[5], oW[5], pW[5], pWf[5], pQ[5];
+    for (int v = 0; v < 5; v++) { Q[v] = cur.Gas[v * fs + c]; oQ[v] = old.Gas[v * fs + c]; }
+    auto c2p = [&](const double* U, double* Wo) {
+        const double rho = U[0];
+        const double Vx = U[1] / rho, Vy = U[2] / rho, Vz = U[3] / rho;
+        const double KinE = 0.5 * rho * (Vx * Vx + Vy * Vy + Vz * Vz);
+        Wo[0] = rho < dF ? dF : rho; Wo[1] = Vx; Wo[2] = Vy; Wo[3] = Vz;
+        const double pp = gm1 * (U[4] - KinE);
+        Wo[4] = pp < pF ? pF : pp;
+    };
+    c2p(Q, W);
+    c2p(oQ, oW);
+    for (int v = 0; v < 5; v++) pW[v] = W[v] + pdt * ((W[v] - oW[v]) / odt);
+    for (int v = 0; v < 5; v++) pWf[v] = pW[v];
+    pWf[0] = pW[0] < dF ? dF : pW[0];
+    pWf[4] = pW[4] < pF ? pF : pW[4];
+    {
+        const double rho = pWf[0] < dF ? dF : pWf[0];
+        const double IntE = (pWf[4] < pF ? pF : pWf[4]) / gm1;
+        const double KinE = 0.5 * rho * (pWf[1] * pWf[1] + pWf[2] * pWf[2] + pWf[3] * pWf[3]);
+        pQ[0] = rho; pQ[1] = rho * pWf[1]; pQ[2] = rho * pWf[2]; pQ[3] = rho * pWf[3]; pQ[4] = IntE + KinE;
+    }
+    const double vol = g.vol[c];
+    double aWh[5], apQ[5] = {0, 0, 0, 0, 0};
+    for (int v = 0; v < 5; v++) aWh[v] = vol * (double)dw.QW[v * fs + c];
+    aWh[0] += dw.Dh[c];
+    const double Dm = pQ[0] < dF ? dF : pQ[0];
+    double aDm = 0.0;
+    for (int x = 0; x < 3; x++) {
+        const double a = dw.VdV[x * fs + c];
+        apQ[1 + x] += vol * a / Dm;
+        aDm += -vol * pQ[1 + x] * a / (Dm * Dm);
+    }
+    if (!(pQ[0] < dF)) apQ[0] += aDm;
+    bc2p_adj(dF, pF, gm1, pQ, aWh, apQ);
+    double apWf[5] = {0, 0, 0, 0, 0};
+    p2c_adj(dF, pF, gm1, pWf, apQ, apWf);
+    double apW[5];
+    for (int v = 0; v < 5; v++) apW[v] = apWf[v];
+    apW[0] = (pW[0] < dF) ? 0.0 : apWf[0];
+    apW[4] = (pW[4] < pF) ? 0.0 : apWf[4];
+    double aW[5], aoW[5];
+    for (int v = 0; v < 5; v++) {
+        aW[v] = apW[v] + apW[v] * pdt / odt;
+        aoW[v] = -apW[v] * pdt / odt;
+    }
+    double aQ[5] = {0, 0, 0, 0, 0}, aoQ[5] = {0, 0, 0, 0, 0};
+    c2p_adj(dF, pF, gm1, Q, aW, aQ);
+    c2p_adj(dF, pF, gm1, oQ, aoW, aoQ);
+    double aWn[5];
+    for (int v = 0; v < 5; v++) aWn[v] = dw.Wn[v * fs + c];
+    bc2p_adj(dF, pF, gm1, Q, aWn, aQ);
+    for (int v = 0; v < 5; v++) {
+        dGas[v * fs + c] += (R)aQ[v];
+        doGas[v * fs + c] += (R)aoQ[v];
+    }
+    if (P.doMHD)
+        for (int x = 0; x < 3; x++) aB[x * fs + c] = (R)(vol * (double)dw.QB[x * fs + c]);
+}
+
+// predictor adjoint, faces: dabh, dBnf, dbn and the Bxyz adjoints of the two
+// cells sharing the face -> dmf, domf
+template <class R>
+__global__ void __launch_bounds__(256) k_predict_adj_faces(GamBox b, DevParams<R> P, Geo<R> g, double pdt, double odt,
+                                                           Work<R> dw, const R* __restrict__ aB, R* dmf, R* domf) {
+    int ii, jj, kk;
+    Range r{0, b.Ni, 0, b.Nj, 0, b.Nk};
+    if (!thread_ijk(r, ii, jj, kk)) return;
+    const long fs = b.fs, c = lidx(b, ii, jj, kk);
+    if (!P.doMHD) return;
+    const int ijk[3] = {ii, jj, kk}, n[3] = {b.Ni, b.Nj, b.Nk};
+    for (int d = 0; d < 3; d++) {
+        const double A = g.face[d * fs + c];
+        const double Am = A < TINY ? TINY : A;
+        double ahm = (double)dw.abh[d * fs + c] * A / Am + (double)dw.Bnf[d * fs + c] / A;
+        // cells c (this is its lower face d) and c - s_d (its upper face)
+        bool inLo = true, inUp = true;
+        for (int e = 0; e < 3; e++) {
+            const int lo = ijk[e] - (e == d ? 1 : 0);
+            if (ijk[e] >= n[e]) inLo = false;
+            if (lo < 0 || lo >= n[e]) inUp = false;
+        }
+        if (inLo)
+            for (int x = 0; x < 3; x++) ahm += (double)aB[x * fs + c] * dbdf(b, g, c, 2 * d, x);
+        if (inUp) {
+            const long cu = c - dstride(b, d);
+            for (int x = 0; x < 3; x++) ahm += (double)aB[x * fs + cu] * dbdf(b, g, cu, 2 * d + 1, x);
+        }
+        dmf[d * fs + c] += (R)(ahm + ahm * pdt / odt + (double)dw.bn[d * fs + c] / Am);
+        domf[d * fs + c] += (R)(-ahm * pdt / odt);
+    }
+}
+
+// update adjoint, cells: dnxtGas -> dcurGas, and the scaled adjoints
+// sU = dt aU / V, sM = dt aM / V of the active cells for the face pass
+template <class R>
+__global__ void __launch_bounds__(128) k_update_adj_cells(GamBox b, DevParams<R> P, Geo<R> g, StateBuf<R> cur,
+                                                          Work<R> w, double dt, const R* __restrict__ dnGas, R* dGas,
+                                                          R* sU, R* sM) {
+    int ii, jj, kk;
+    Range r{0, b.Ni - 1, 0, b.Nj - 1, 0, b.Nk - 1};
+    if (!thread_ijk(r, ii, jj, kk)) return;
+    const long fs = b.fs, c = lidx(b, ii, jj, kk);
+    const int G = GAM_NG;
+    const bool active = ii >= G && ii < G + b.Nip && jj >= G && jj < G + b.Njp && kk >= G && kk < G + b.Nkp;
+    if (!active) {
+        for (int v = 0; v < 5; v++) dGas[v * fs + c] += dnGas[v * fs + c];
+        return;
+    }
+    const double dF = P.dFloor, pF = P.pFloor, gm1 = P.gm1;
+    const double dV = g.vol[c];
+    const long sj = b.sx, sk = b.sk;
+    double U[5], dGasM[3] = {0, 0, 0};
+    for (int v = 0; v < 5; v++) {
+        const R* gI = w.gF + (v + 0) * fs;
+        const R* gJ = w.gF + (v + 5) * fs;
+        const R* gK = w.gF + (v + 10) * fs;
+        const double dGasH = ((double)gI[c] - gI[c + 1] + gJ[c] - gJ[c + sj] + gK[c] - gK[c + sk]) / dV;
+        U[v] = (double)cur.Gas[v * fs + c] + dt * dGasH;
+    }
+    double aU[5], aM3[3] = {0, 0, 0};
+    double ao[5];
+    for (int v = 0; v < 5; v++) ao[v] = dnGas[v * fs + c];
+    if (P.doMHD) {
+        for (int x = 0; x < 3; x++) {
+            const R* mI = w.mF + (x + 0) * fs;
+            const R* mJ = w.mF + (x + 3) * fs;
+            const R* mK = w.mF + (x + 6) * fs;
+            dGasM[x] = ((double)mI[c] - mI[c + 1] + mJ[c] - mJ[c + sj] + mK[c] - mK[c + sk]) / dV;
+            if (P.doBackground) dGasM[x] += g.dpB0[x * fs + c];
+        }
+        // CellMaxwell (mhdgroup.F90:299-329) backwards
+        const double D = U[0] < dF ? dF : U[0];
+        const double M[3] = {U[1], U[2], U[3]};
+        const double KinE = 0.5 * (M[0] * M[0] + M[1] * M[1] + M[2] * M[2]) / D;
+        const double p = gm1 * (U[4] - KinE);
+        double Mn[3];
+        for (int x = 0; x < 3; x++) Mn[x] = M[x] + dt * dGasM[x];
+        const double Mn2 = Mn[0] * Mn[0] + Mn[1] * Mn[1] + Mn[2] * Mn[2];
+        double a_D = ao[0], a_Mn[3];
+        const double a_KinEn = ao[4], a_Pr = ao[4] / gm1;
+        for (int x = 0; x < 3; x++) a_Mn[x] = ao[1 + x] + a_KinEn * Mn[x] / D;
+        a_D += -a_KinEn * 0.5 * Mn2 / (D * D);
+        double a_M[3];
+        for (int x = 0; x < 3; x++) {
+            a_M[x] = a_Mn[x];
+            aM3[x] = a_Mn[x] * dt;
+        }
+        double a_U4 = 0.0, a_KinE = 0.0;
+        if (!(p < pF)) { a_U4 = a_Pr * gm1; a_KinE = -a_Pr * gm1; }
+        for (int x = 0; x < 3; x++) a_M[x] += a_KinE * M[x] / D;
+        a_D += -a_KinE * 0.5 * (M[0] * M[0] + M[1] * M[1] + M[2] * M[2]) / (D * D);
+        aU[0] = (U[0] < dF) ? 0.0 : a_D;
+        for (int x = 0; x < 3; x++) aU[1 + x] = a_M[x];
+        aU[4] = a_U4;
+    } else {
+        for (int v = 0; v < 5; v++) aU[v] = ao[v];
+    }
+    for (int v = 0; v < 5; v++) {
+        dGas[v * fs + c] += (R)aU[v];
+        sU[v * fs + c] = (R)(dt * aU[v] / dV);
+    }
+    for (int x = 0; x < 3; x++) sM[x * fs + c] = (R)(aM3[x] / dV);
+}
+
+// update adjoint, faces: face fluxes gF/mF from the two cells, E2Flux -> dE,
+// and dcurmf = dnxtmf (copied or updated faces alike)
+template <class R>
+__global__ void __launch_bounds__(256) k_update_adj_faces(GamBox b, DevParams<R> P, double dt,
+                                                          const R* __restrict__ sU, const R* __restrict__ sM,
+                                                          const R* __restrict__ dnmf, R* dmf, R* dgF, R* dmF, R* dE) {
+    int ii, jj, kk;
+    Range r{0, b.Ni, 0, b.Nj, 0, b.Nk};
+    if (!thread_ijk(r, ii, jj, kk)) return;
+    const long fs = b.fs, c = lidx(b, ii, jj, kk);
+    const int G = GAM_NG;
+    const int lo[3] = {G, G, G}, hi[3] = {G + b.Nip - 1, G + b.Njp - 1, G + b.Nkp - 1};
+    auto act = [&](int a0, int a1, int a2) {
+        return a0 >= lo[0] && a0 <= hi[0] && a1 >= lo[1] && a1 <= hi[1] && a2 >= lo[2] && a2 <= hi[2];
+    };
+    for (int d = 0; d < 3; d++) {
+        const bool inLo = act(ii, jj, kk);
+        const bool inUp = act(ii - (d == 0), jj - (d == 1), kk - (d == 2));
+        const long cu = c - dstride(b, d);
+        for (int v = 0; v < 5; v++) {
+            double a = 0.0;
+            if (inLo) a += sU[v * fs + c];
+            if (inUp) a -= sU[v * fs + cu];
+            dgF[(v + 5 * d) * fs + c] += (R)a;
+        }
+        if (P.doMHD)
+            for (int x = 0; x < 3; x++) {
+                double a = 0.0;
+                if (inLo) a += sM[x * fs + c];
+                if (inUp) a -= sM[x * fs + cu];
+                dmF[(x + 3 * d) * fs + c] += (R)a;
+            }
+        dmf[d * fs + c] += dnmf[d * fs + c];
+    }
+    if (!P.doMHD) return;
+    // E2Flux on the faces [G, G+Nip] x [G, G+Njp] x [G, G+Nkp] (k_update_faces)
+    auto inr = [&](int a0, int a1, int a2) {
+        return a0 >= G && a0 <= G + b.Nip && a1 >= G && a1 <= G + b.Njp && a2 >= G && a2 <= G + b.Nkp;
+    };
+    const long sj = b.sx, sk = b.sk;
+    auto A = [&](int q, int a0, int a1, int a2) -> double {
+        return inr(a0, a1, a2) ? (double)dnmf[q * fs + c + (a0 - ii) + (long)(a1 - jj) * sj + (long)(a2 - kk) * sk] : 0.0;
+    };
+    const double a0c = A(0, ii, jj, kk), a1c = A(1, ii, jj, kk), a2c = A(2, ii, jj, kk);
+    // mf0 -= dt (E2[+j] - E2 - E1[+k] + E1); mf1 -= dt (E0[+k] - E0 - E2[+i] + E2); mf2 -= dt (E1[+i] - E1 - E0[+j] + E0)
+    const double aE2 = -dt * (A(0, ii, jj - 1, kk) - a0c - A(1, ii - 1, jj, kk) + a1c);
+    const double aE1 = -dt * (-A(0, ii, jj, kk - 1) + a0c + A(2, ii - 1, jj, kk) - a2c);
+    const double aE0 = -dt * (A(1, ii, jj, kk - 1) - a1c - A(2, ii, jj - 1, kk) + a2c);
+    dE[c] += (R)aE0;
+    dE[fs + c] += (R)aE1;
+    dE[2 * fs + c] += (R)aE2;
+}
 }  // namespace gam_adj
 
 // ------------------------------------------------------------ C ABI
@@ -601,4 +900,116 @@ extern "C" int gam_efield_adjoint(const gam_params* p, int32_t fp32, const void*
                                      dDh, dabh, dbn, dVdV, dAVf, s)
                 : efield_call<double>(p, Dh, abh, bn, VdV, volume, face, edge, Te, Teb, edgB0, dt, AVf, nullptr, dE,
                                       dDh, dabh, dbn, dVdV, dAVf, s);
+}
+
+// ------------------------------------------------------------ predictor and update stages
+namespace {
+template <class R> Geo<R> geo_of(const void* vol, const void* face, const void* xfc, const void* xyzcc, const void* dxf,
+                                 const double* dpB0) {
+    Geo<R> g;
+    memset(&g, 0, sizeof(g));
+    g.vol = (const R*)vol; g.face = (const R*)face; g.xfc = (const R*)xfc; g.xyzcc = (const R*)xyzcc;
+    g.dxf = (const R*)dxf; g.dpB0 = dpB0;
+    return g;
+}
+int set_scalars(double dt, double pdt, double odt, cudaStream_t s, GamScalars** sc) {
+    GamScalars hs;
+    memset(&hs, 0, sizeof(hs));
+    hs.dt = dt; hs.pdt = pdt; hs.odt = odt; hs.fixedTimestep = 1;
+    if (cudaMemcpyToSymbolAsync(gam_adj::g_adj_scalars, &hs, sizeof(hs), 0, cudaMemcpyHostToDevice, s) != cudaSuccess)
+        return GAM_ECUDA;
+    return cudaGetSymbolAddress((void**)sc, gam_adj::g_adj_scalars) == cudaSuccess ? GAM_OK : GAM_ECUDA;
+}
+dim3 grid3(const Range& r, dim3 blk) {
+    return dim3((unsigned)((r.i1 - r.i0 + 1 + blk.x - 1) / blk.x), (unsigned)((r.j1 - r.j0 + 1 + blk.y - 1) / blk.y),
+                (unsigned)((r.k1 - r.k0 + 1 + blk.z - 1) / blk.z));
+}
+template <class R>
+int predict_call(const gam_params* p, const void* const* st, const void* const* geo, double pdt, double odt,
+                 void* const* out, const void* const* din, void* aB, void* const* dst, cudaStream_t s) {
+    using namespace gam_adj;
+    const GamBox b = torch_box(p->Nip, p->Njp, p->Nkp);
+    const DevParams<R> P = dev_params<R>(p);
+    const Geo<R> g = geo_of<R>(geo[0], geo[1], geo[2], geo[3], geo[4], nullptr);
+    StateBuf<R> cur{(R*)st[0], (R*)st[1], nullptr}, old{(R*)st[2], (R*)st[3], nullptr};
+    GamScalars* sc;
+    if (set_scalars(0.0, pdt, odt, s, &sc)) return GAM_ECUDA;
+    const Range all{0, b.Ni, 0, b.Nj, 0, b.Nk}, cells{0, b.Ni - 1, 0, b.Nj - 1, 0, b.Nk - 1};
+    if (out) {
+        Work<R> w;
+        memset(&w, 0, sizeof(w));
+        w.QW = (R*)out[0]; w.Wn = (R*)out[1]; w.Dh = (R*)out[2]; w.VdV = (R*)out[3]; w.QB = (R*)out[4];
+        w.abh = (R*)out[5]; w.Bnf = (R*)out[6]; w.bn = (R*)out[7];
+        const dim3 blk(32, 8, 1);
+        k_predict<R, 1><<<grid3(all, blk), blk, 0, s>>>(b, P, g, cur, old, w, sc);
+    } else {
+        Work<R> dw;
+        memset(&dw, 0, sizeof(dw));
+        dw.QW = (R*)din[0]; dw.Wn = (R*)din[1]; dw.Dh = (R*)din[2]; dw.VdV = (R*)din[3]; dw.QB = (R*)din[4];
+        dw.abh = (R*)din[5]; dw.Bnf = (R*)din[6]; dw.bn = (R*)din[7];
+        const dim3 blk(32, 4, 1);
+        k_predict_adj_cells<R><<<grid3(cells, blk), blk, 0, s>>>(b, P, g, cur, old, pdt, odt, dw, (R*)dst[0],
+                                                                  (R*)dst[2], (R*)aB);
+        k_predict_adj_faces<R><<<grid3(all, blk), blk, 0, s>>>(b, P, g, pdt, odt, dw, (const R*)aB, (R*)dst[1],
+                                                                (R*)dst[3]);
+    }
+    return cudaGetLastError() == cudaSuccess ? GAM_OK : GAM_ECUDA;
+}
+template <class R>
+int update_call(const gam_params* p, const void* const* in, const void* const* geo, const double* dpB0, double dt,
+                void* const* out, const void* const* din, void* sU, void* sM, void* const* dst, cudaStream_t s) {
+    using namespace gam_adj;
+    const GamBox b = torch_box(p->Nip, p->Njp, p->Nkp);
+    const DevParams<R> P = dev_params<R>(p);
+    const Geo<R> g = geo_of<R>(geo[0], nullptr, geo[1], geo[2], geo[3], dpB0);
+    // in: curGas, curMf, E, gF, mF
+    StateBuf<R> cur{(R*)in[0], (R*)in[1], nullptr};
+    Work<R> w;
+    memset(&w, 0, sizeof(w));
+    w.E = (R*)in[2]; w.gF = (R*)in[3]; w.mF = (R*)in[4];
+    GamScalars* sc;
+    if (set_scalars(dt, 0.0, 0.0, s, &sc)) return GAM_ECUDA;
+    const Range all{0, b.Ni, 0, b.Nj, 0, b.Nk}, cells{0, b.Ni - 1, 0, b.Nj - 1, 0, b.Nk - 1};
+    const dim3 blk(32, 4, 1);
+    if (out) {
+        StateBuf<R> nxt{(R*)out[0], (R*)out[1], (R*)out[2]};
+        k_update_faces<R><<<grid3(all, blk), blk, 0, s>>>(b, P, cur, nxt, w, sc);
+        const double gamma = p->gamma, gm1 = p->gamma - 1;
+        k_update_cells<R, 1><<<grid3(cells, blk), blk, 0, s>>>(b, P, g, cur, nxt, w, sc, gamma, gm1);
+    } else {
+        k_update_adj_cells<R><<<grid3(cells, blk), blk, 0, s>>>(b, P, g, cur, w, dt, (const R*)din[0], (R*)dst[0],
+                                                                 (R*)sU, (R*)sM);
+        k_update_adj_faces<R><<<grid3(all, blk), blk, 0, s>>>(b, P, dt, (const R*)sU, (const R*)sM, (const R*)din[1],
+                                                               (R*)dst[1], (R*)dst[3], (R*)dst[4], (R*)dst[2]);
+    }
+    return cudaGetLastError() == cudaSuccess ? GAM_OK : GAM_ECUDA;
+}
+}  // namespace
+
+// st: curGas, curMf, oldGas, oldMf; geo: volume, face, xfc, xyzcc, dxf (FP32 only, else NULL)
+// out (forward): QW, Wn, Dh, VdV, QB, abh, Bnf, bn
+// din (adjoint): their adjoints; dst: dcurGas, dcurMf, doldGas, doldMf (added to); aB: 3-component scratch
+extern "C" int gam_predict_stage(const gam_params* p, int32_t fp32, const void* const* st, const void* const* geo,
+                                 double pdt, double odt, void* const* out, const void* const* din, void* aB,
+                                 void* const* dst, void* stream) {
+    int rc = check(p, fp32);
+    if (rc) return rc;
+    if (!st || !geo || (!out && (!din || !aB || !dst)) || !p->doLFMLim) return GAM_EINVAL;
+    cudaStream_t s = (cudaStream_t)stream;
+    return fp32 ? predict_call<float>(p, st, geo, pdt, odt, out, din, aB, dst, s)
+                : predict_call<double>(p, st, geo, pdt, odt, out, din, aB, dst, s);
+}
+// in: curGas, curMf, E, gF, mF; geo: volume, xfc, xyzcc, dxf; dpB0 (FP64) when doBackground
+// out (forward): nxtGas, nxtMf, nxtB (scratch); din (adjoint): dnxtGas, dnxtMf
+// dst: dcurGas, dcurMf, dE, dgF, dmF (added to); sU (5) and sM (3) scratch
+extern "C" int gam_update_stage(const gam_params* p, int32_t fp32, const void* const* in, const void* const* geo,
+                                const double* dpB0, double dt, void* const* out, const void* const* din, void* sU,
+                                void* sM, void* const* dst, void* stream) {
+    int rc = check(p, fp32);
+    if (rc) return rc;
+    if (!in || !geo || (!out && (!din || !sU || !sM || !dst))) return GAM_EINVAL;
+    if (p->doBackground && !dpB0) return GAM_EINVAL;
+    cudaStream_t s = (cudaStream_t)stream;
+    return fp32 ? update_call<float>(p, in, geo, dpB0, dt, out, din, sU, sM, dst, s)
+                : update_call<double>(p, in, geo, dpB0, dt, out, din, sU, sM, dst, s);
 }

@@ -83,12 +83,14 @@ def c4(N=(64, 64, 64), nsteps=20, sigma=1e-3, seed=2024):
     mf64 = g.face_box(st["magFlux"]) + sigma * g.face * noise(g.face.shape)
     out = {"config": f"curvilinear blast wave {N[0]}x{N[1]}x{N[2]}, {nsteps} fixed-dt steps (dt = {dt:.4g})",
            "loss": "sum |B|^2 over cells centred in [0.6,0.8]^3", "wrt": "start Gas and face fluxes",
-           "impl": "reverse sweep of the step restatement (mage_b200.diffstep): flux stage by the hand-written CUDA "
-                   "adjoint (gam_flux_adjoint), the other stages by PyTorch autograd; checkpoint every "
+           "impl": "reverse sweep of the step restatement (mage_b200.diffstep): predictor, electric field, fluxes "
+                   "and update by hand-written CUDA adjoints (gam_predict_stage, gam_efield_adjoint, gam_flux_adjoint, "
+                   "gam_update_stage), boundary gathers and bFlux2Fld by PyTorch autograd; checkpoint every "
                    f"{max(1, int(round(nsteps ** 0.5)))} steps"}
     grads = {}
     for name, dtype in (("fp64", torch.float64), ("fp32", torch.float32)):
         gg = g if dtype == torch.float64 else Grid(DiffParams(*N), geo, dtype=dtype, device="cuda")
+        loss_and_grad(gg, Gas64.to(dtype), mf64.to(dtype), dt, 1)  # warm-up (library, kernels, allocator)
         (L, gG, gF), el, mem = _timed(lambda: loss_and_grad(gg, Gas64.to(dtype), mf64.to(dtype), dt, nsteps))
         out[name] = {"loss": L, "fwd_plus_adjoint_s": el, "peak_hbm_gb": mem}
         grads[name] = (gG, gF)
@@ -151,8 +153,9 @@ def c5(N=(192, 192, 256), nsteps=200, seg=14, precisions=("fp32", "fp64"), seed=
     out = {"config": f"dipole in a solar wind, spherical {N[0]}x{N[1]}x{N[2]}, {nsteps} fixed-dt steps (dt = {dt:.4g})",
            "loss": "sum |Bxyz|^2 (field without the dipole) over active cells with r < 6",
            "wrt": "start Gas and face fluxes",
-           "impl": "reverse sweep of mage_b200.diffstep: flux stage by the hand-written CUDA adjoint, the rest by "
-                   f"PyTorch autograd; checkpoint every {seg} steps, one step's graph at a time"}
+           "impl": "reverse sweep of mage_b200.diffstep: predictor, electric field, fluxes and update by "
+                   "hand-written CUDA adjoints, boundaries (inner sphere, wind, gathers) and bFlux2Fld by PyTorch "
+                   f"autograd; checkpoint every {seg} steps, one step's graph at a time"}
     grads = {}
     for name in precisions:
         dtype = torch.float64 if name == "fp64" else torch.float32
@@ -166,6 +169,7 @@ def c5(N=(192, 192, 256), nsteps=200, seg=14, precisions=("fp32", "fp64"), seed=
             return ((B * B).sum(dim=0) * mask).sum()
 
         Gas0, mf0 = g.cell_box(G64).to(dtype), g.face_box(F64)
+        loss_and_grad(g, Gas0, mf0, dt, 1, lossf=lossf)  # warm-up
         (L, gG, gF), el, mem = _timed(lambda: loss_and_grad(g, Gas0, mf0, dt, nsteps, seg=seg, lossf=lossf,
                                                              per_step=True))
         out[name] = {"loss": L, "fwd_plus_adjoint_s": el, "s_per_step": el / nsteps, "peak_hbm_gb": mem}

@@ -198,6 +198,23 @@ class Grid:
         self.Teb = face(geo["Teb"])
         self.vol = cell(geo["volume"])[0]
         self.xyzcc = cell(geo["xyzcc"])
+        # face centroid - cell centroid of the six faces of each cell (FP64,
+        # rounded once): the FP32 form's bFlux2Fld operand, as in the CUDA form
+        xf = np.ascontiguousarray(geo["xfc"], dtype=np.float64)
+        xc = np.zeros((3,) + xf.shape[1:])
+        xc[:, :self.Nk, :self.Nj, :self.Ni] = np.asarray(geo["xyzcc"])
+        off = np.zeros((18,) + xf.shape[1:])
+        for d in range(3):
+            up = [0, 0, 0]
+            up[2 - d] = 1
+            for x in range(3):
+                off[x + 3 * (2 * d)] = xf[x + 3 * d] - xc[x]
+                shifted = np.zeros_like(xf[x + 3 * d])
+                sl_dst = tuple(slice(0, n - u) for n, u in zip(shifted.shape, up))
+                sl_src = tuple(slice(u, n) for n, u in zip(shifted.shape, up))
+                shifted[sl_dst] = xf[x + 3 * d][sl_src]
+                off[x + 3 * (2 * d + 1)] = shifted - xc[x]
+        self.dxf = torch.as_tensor(off, dtype=dtype, device=device)
         # background field (AddB0 arrays, cell-sized; kept in FP64 like the CUDA forms)
         self.bg = None
         if background is not None:
@@ -323,6 +340,11 @@ class Grid:
         fJ, fJp = win(mf[1], rc), win(mf[1], rc, (0, 1, 0))
         fK, fKp = win(mf[2], rc), win(mf[2], rc, (0, 0, 1))
         dV = win(self.vol, rc)
+        if self.dtype == torch.float32:
+            d = self.dxf
+            B = [(fIp * win(d[x + 3], rc) + fJp * win(d[x + 9], rc) + fKp * win(d[x + 15], rc) - fI * win(d[x], rc) -
+                  fJ * win(d[x + 6], rc) - fK * win(d[x + 12], rc)) / dV for x in range(3)]
+            return put(torch.zeros_like(mf), rc, torch.stack(B))
         Div = fIp - fI + fJp - fJ + fKp - fK
         B = []
         for x in range(3):
@@ -334,18 +356,11 @@ class Grid:
 
 
 # ----------------------------------------------------------------- the step
-def step(g: Grid, cur: dict, old: dict, dt: float, odt: float):
-    """One stepGamera with a fixed dt. cur/old: {"Gas": (5,...), "mf": (3,...),
-    "B": (3,...)} box tensors of State (n) and oState (n-1); odt = time - otime
-    after the AdvanceMHD time trap. Returns State (n+1) (boundaries filled)."""
+def _predict_torch(g: Grid, cur: dict, old: dict, pdt: float, odt: float):
+    """Predictor (mhdgroup.F90:444-615) as tensor expressions."""
     P = g.P
     Ni, Nj, Nk = g.Ni, g.Nj, g.Nk
-    pdt = 0.5 * dt
-    gm1 = P.gamma - 1
-    allf = (0, Ni, 0, Nj, 0, Nk)
     allc = (0, Ni - 1, 0, Nj - 1, 0, Nk - 1)
-
-    # --- Predictor (every face and cell of the box)
     Q, oQ = cur["mf"], old["mf"]
     hm = Q + pdt * ((Q - oQ) / odt)
     A = g.face
@@ -371,6 +386,59 @@ def step(g: Grid, cur: dict, old: dict, dt: float, odt: float):
     Dm = rmax(pQ[0], torch.full_like(pQ[0], P.dFloor))
     VdV = put(torch.zeros_like(cur["B"]), allc, torch.stack([vol * pQ[1 + x] / Dm for x in range(3)]))
     QB = g.bxyz(hm) * g.vol
+    return QW, WnB, Dh, VdV, QB, abh, Bnf, bn
+
+
+def _update_torch(g: Grid, cur: dict, E, gF, mF, dt: float):
+    """applyUpdate: E2Flux, CellReynolds, CellMaxwell (mhdgroup.F90:79-329) as tensor expressions."""
+    P = g.P
+    gm1 = P.gamma - 1
+    Np = (P.Nip, P.Njp, P.Nkp)
+    inr = (G, G + Np[0], G, G + Np[1], G, G + Np[2])
+    dfi = win(E[2], inr, (0, 1, 0)) - win(E[2], inr) - win(E[1], inr, (0, 0, 1)) + win(E[1], inr)
+    dfj = win(E[0], inr, (0, 0, 1)) - win(E[0], inr) - win(E[2], inr, (1, 0, 0)) + win(E[2], inr)
+    dfk = win(E[1], inr, (1, 0, 0)) - win(E[1], inr) - win(E[0], inr, (0, 1, 0)) + win(E[0], inr)
+    mfn = put(cur["mf"], inr, torch.stack([win(cur["mf"][0], inr) - dt * dfi, win(cur["mf"][1], inr) - dt * dfj,
+                                          win(cur["mf"][2], inr) - dt * dfk]))
+    act = (G, G + Np[0] - 1, G, G + Np[1] - 1, G, G + Np[2] - 1)
+    dV = win(g.vol, act)
+    U = []
+    for v in range(5):
+        dGasH = (win(gF[0][v], act) - win(gF[0][v], act, (1, 0, 0)) + win(gF[1][v], act) -
+                 win(gF[1][v], act, (0, 1, 0)) + win(gF[2][v], act) - win(gF[2][v], act, (0, 0, 1))) / dV
+        U.append(win(cur["Gas"][v], act) + dt * dGasH)
+    dGasM = [(win(mF[0][x], act) - win(mF[0][x], act, (1, 0, 0)) + win(mF[1][x], act) - win(mF[1][x], act, (0, 1, 0)) +
+              win(mF[2][x], act) - win(mF[2][x], act, (0, 0, 1))) / dV for x in range(3)]
+    if g.bg is not None:
+        dGasM = [dGasM[x] + win(g.bg["dpB0"][x], act).to(dV.dtype) for x in range(3)]
+    # CellMaxwell (mhdgroup.F90:299-329)
+    Dn = rmax(U[0], torch.full_like(U[0], P.dFloor))
+    Mx, My, Mz, TotE = U[1], U[2], U[3], U[4]
+    KinE = 0.5 * (Mx * Mx + My * My + Mz * Mz) / Dn
+    Pr = rmax(gm1 * (TotE - KinE), torch.full_like(Dn, P.pFloor))
+    Mx, My, Mz = Mx + dt * dGasM[0], My + dt * dGasM[1], Mz + dt * dGasM[2]
+    KinE = 0.5 * (Mx * Mx + My * My + Mz * Mz) / Dn
+    Gas = put(cur["Gas"], act, torch.stack([Dn, Mx, My, Mz, KinE + Pr / gm1]))
+    return Gas, mfn
+
+
+def step(g: Grid, cur: dict, old: dict, dt: float, odt: float):
+    """One stepGamera with a fixed dt. cur/old: {"Gas": (5,...), "mf": (3,...),
+    "B": (3,...)} box tensors of State (n) and oState (n-1); odt = time - otime
+    after the AdvanceMHD time trap. Returns State (n+1) (boundaries filled)."""
+    P = g.P
+    Ni, Nj, Nk = g.Ni, g.Nj, g.Nk
+    pdt = 0.5 * dt
+    gm1 = P.gamma - 1
+    allf = (0, Ni, 0, Nj, 0, Nk)
+    allc = (0, Ni - 1, 0, Nj - 1, 0, Nk - 1)
+
+    # --- Predictor (every face and cell of the box)
+    A = g.face
+    if g.cuda_flux:
+        QW, WnB, Dh, VdV, QB, abh, Bnf, bn = _PredictFn.apply(cur["Gas"], cur["mf"], old["Gas"], old["mf"], g, pdt, odt)
+    else:
+        QW, WnB, Dh, VdV, QB, abh, Bnf, bn = _predict_torch(g, cur, old, pdt, odt)
     Blim = cur["B"]
 
     # --- CalcElecField
@@ -432,6 +500,7 @@ def step(g: Grid, cur: dict, old: dict, dt: float, odt: float):
         E.append(put(torch.zeros_like(g.vol), r, e * edge))
 
     # --- CalcStress
+    zeros5 = torch.zeros_like(cur["Gas"])
     fr = [(G, G + Np[0], G, G + Np[1] - 1, G, G + Np[2] - 1), (G, G + Np[0] - 1, G, G + Np[1], G, G + Np[2] - 1),
           (G, G + Np[0] - 1, G, G + Np[1] - 1, G, G + Np[2])]
     gF, mF = [], []
@@ -503,31 +572,10 @@ def step(g: Grid, cur: dict, old: dict, dt: float, odt: float):
         gF.append(put(zeros5, r, torch.stack([fa * (gFv[v] - 1.0 * P.cHogH * VaD * dW[v]) for v in range(5)])))
 
     # --- applyUpdate: E2Flux on the active faces, then the cells
-    inr = (G, G + Np[0], G, G + Np[1], G, G + Np[2])
-    dfi = win(E[2], inr, (0, 1, 0)) - win(E[2], inr) - win(E[1], inr, (0, 0, 1)) + win(E[1], inr)
-    dfj = win(E[0], inr, (0, 0, 1)) - win(E[0], inr) - win(E[2], inr, (1, 0, 0)) + win(E[2], inr)
-    dfk = win(E[1], inr, (1, 0, 0)) - win(E[1], inr) - win(E[0], inr, (0, 1, 0)) + win(E[0], inr)
-    mfn = put(cur["mf"], inr, torch.stack([win(cur["mf"][0], inr) - dt * dfi, win(cur["mf"][1], inr) - dt * dfj,
-                                          win(cur["mf"][2], inr) - dt * dfk]))
-    act = (G, G + Np[0] - 1, G, G + Np[1] - 1, G, G + Np[2] - 1)
-    dV = win(g.vol, act)
-    U = []
-    for v in range(5):
-        dGasH = (win(gF[0][v], act) - win(gF[0][v], act, (1, 0, 0)) + win(gF[1][v], act) -
-                 win(gF[1][v], act, (0, 1, 0)) + win(gF[2][v], act) - win(gF[2][v], act, (0, 0, 1))) / dV
-        U.append(win(cur["Gas"][v], act) + dt * dGasH)
-    dGasM = [(win(mF[0][x], act) - win(mF[0][x], act, (1, 0, 0)) + win(mF[1][x], act) - win(mF[1][x], act, (0, 1, 0)) +
-              win(mF[2][x], act) - win(mF[2][x], act, (0, 0, 1))) / dV for x in range(3)]
-    if g.bg is not None:
-        dGasM = [dGasM[x] + win(g.bg["dpB0"][x], act).to(dV.dtype) for x in range(3)]
-    # CellMaxwell (mhdgroup.F90:299-329)
-    Dn = rmax(U[0], torch.full_like(U[0], P.dFloor))
-    Mx, My, Mz, TotE = U[1], U[2], U[3], U[4]
-    KinE = 0.5 * (Mx * Mx + My * My + Mz * Mz) / Dn
-    Pr = rmax(gm1 * (TotE - KinE), torch.full_like(Dn, P.pFloor))
-    Mx, My, Mz = Mx + dt * dGasM[0], My + dt * dGasM[1], Mz + dt * dGasM[2]
-    KinE = 0.5 * (Mx * Mx + My * My + Mz * Mz) / Dn
-    Gas = put(cur["Gas"], act, torch.stack([Dn, Mx, My, Mz, KinE + Pr / gm1]))
+    if g.cuda_flux:
+        Gas, mfn = _UpdateFn.apply(cur["Gas"], cur["mf"], Ea, gFa, mFa, g, dt)
+    else:
+        Gas, mfn = _update_torch(g, cur, E, gF, mF, dt)
 
     # --- EnforceBCs: inner sphere and solar wind in place, then the gathers
     # (periodic, zero-gradient J), then the final bFlux2Fld
@@ -658,6 +706,109 @@ class _EFieldFn(torch.autograd.Function):
         if rc != 0:
             raise RuntimeError(f"gam_efield_adjoint failed ({rc})")
         return (*outs, None, None)
+
+
+def _vp(ptrs):
+    import ctypes as C
+    arr = (C.c_void_p * len(ptrs))(*[C.c_void_p(x) if x else None for x in ptrs])
+    return arr
+
+
+class _PredictFn(torch.autograd.Function):
+    """Predictor on the GPU (gam_predict_stage: the product step's predictor
+    kernel) with its hand-written adjoint as backward."""
+
+    @staticmethod
+    def forward(ctx, cG, cF, oG, oF, g, pdt, odt):
+        import ctypes as C
+        from mage_b200.gamera import load_library
+        L = load_library()
+        st = [t.contiguous() for t in (cG, cF, oG, oF)]
+        z5, z3, z1 = (torch.zeros_like(cG), torch.zeros_like(cF), torch.zeros_like(g.vol))
+        outs = [z5, z5.clone(), z1, torch.zeros_like(cF), torch.zeros_like(cF), torch.zeros_like(cF),
+                torch.zeros_like(cF), torch.zeros_like(cF)]
+        geo = _geo_ptrs(g)
+        rc = L.gam_predict_stage(C.byref(_flux_params(g)), int(cG.dtype == torch.float32),
+                                 _vp([t.data_ptr() for t in st]), _vp(geo), float(pdt), float(odt),
+                                 _vp([t.data_ptr() for t in outs]), None, None, None,
+                                 C.c_void_p(torch.cuda.current_stream().cuda_stream))
+        if rc != 0:
+            raise RuntimeError(f"gam_predict_stage failed ({rc})")
+        ctx.save_for_backward(*st)
+        ctx.g, ctx.pdt, ctx.odt = g, pdt, odt
+        return tuple(outs)
+
+    @staticmethod
+    def backward(ctx, *douts):
+        import ctypes as C
+        from mage_b200.gamera import load_library
+        L = load_library()
+        g = ctx.g
+        st = ctx.saved_tensors
+        shapes = [st[0], st[0], g.vol, st[1], st[1], st[1], st[1], st[1]]
+        din = [torch.zeros_like(ref) if d is None else d.contiguous() for d, ref in zip(douts, shapes)]
+        dst = [torch.zeros_like(t) for t in st]
+        aB = torch.zeros_like(st[1])
+        rc = L.gam_predict_stage(C.byref(_flux_params(g)), int(st[0].dtype == torch.float32),
+                                 _vp([t.data_ptr() for t in st]), _vp(_geo_ptrs(g)), float(ctx.pdt), float(ctx.odt),
+                                 None, _vp([t.data_ptr() for t in din]), C.c_void_p(aB.data_ptr()),
+                                 _vp([t.data_ptr() for t in dst]), C.c_void_p(torch.cuda.current_stream().cuda_stream))
+        if rc != 0:
+            raise RuntimeError(f"gam_predict_stage (adjoint) failed ({rc})")
+        return (*dst, None, None, None)
+
+
+def _geo_ptrs(g: Grid):
+    f32 = g.dtype == torch.float32
+    return [g.vol.data_ptr(), g.face.data_ptr(), g.xfc.data_ptr(), g.xyzcc.data_ptr(), g.dxf.data_ptr() if f32 else 0]
+
+
+class _UpdateFn(torch.autograd.Function):
+    """applyUpdate on the GPU (gam_update_stage: the product step's face and
+    cell update kernels) with its hand-written adjoint as backward."""
+
+    @staticmethod
+    def forward(ctx, cG, cF, E, gF, mF, g, dt):
+        import ctypes as C
+        from mage_b200.gamera import load_library
+        L = load_library()
+        ins = [t.contiguous() for t in (cG, cF, E, gF, mF)]
+        nG, nF, nB = torch.zeros_like(cG), torch.zeros_like(cF), torch.zeros_like(cF)
+        f32 = g.dtype == torch.float32
+        geo = [g.vol.data_ptr(), g.xfc.data_ptr(), g.xyzcc.data_ptr(), g.dxf.data_ptr() if f32 else 0]
+        dp = g.bg["dpB0"].contiguous().data_ptr() if g.bg is not None else None
+        rc = L.gam_update_stage(C.byref(_flux_params(g)), int(f32), _vp([t.data_ptr() for t in ins]), _vp(geo),
+                                C.cast(C.c_void_p(dp), C.POINTER(C.c_double)) if dp else None, float(dt),
+                                _vp([nG.data_ptr(), nF.data_ptr(), nB.data_ptr()]), None, None, None, None,
+                                C.c_void_p(torch.cuda.current_stream().cuda_stream))
+        if rc != 0:
+            raise RuntimeError(f"gam_update_stage failed ({rc})")
+        ctx.save_for_backward(*ins)
+        ctx.g, ctx.dt = g, dt
+        return nG, nF
+
+    @staticmethod
+    def backward(ctx, dG, dF):
+        import ctypes as C
+        from mage_b200.gamera import load_library
+        L = load_library()
+        g = ctx.g
+        ins = ctx.saved_tensors
+        dG = torch.zeros_like(ins[0]) if dG is None else dG.contiguous()
+        dF = torch.zeros_like(ins[1]) if dF is None else dF.contiguous()
+        dst = [torch.zeros_like(t) for t in ins]
+        sU, sM = torch.zeros_like(ins[0]), torch.zeros_like(ins[1])
+        f32 = g.dtype == torch.float32
+        geo = [g.vol.data_ptr(), g.xfc.data_ptr(), g.xyzcc.data_ptr(), g.dxf.data_ptr() if f32 else 0]
+        dp = g.bg["dpB0"].contiguous().data_ptr() if g.bg is not None else None
+        rc = L.gam_update_stage(C.byref(_flux_params(g)), int(f32), _vp([t.data_ptr() for t in ins]), _vp(geo),
+                                C.cast(C.c_void_p(dp), C.POINTER(C.c_double)) if dp else None, float(ctx.dt), None,
+                                _vp([dG.data_ptr(), dF.data_ptr()]), C.c_void_p(sU.data_ptr()),
+                                C.c_void_p(sM.data_ptr()), _vp([t.data_ptr() for t in dst]),
+                                C.c_void_p(torch.cuda.current_stream().cuda_stream))
+        if rc != 0:
+            raise RuntimeError(f"gam_update_stage (adjoint) failed ({rc})")
+        return (*dst, None, None)
 
 
 def _iside_bcs(g: Grid, Gas, mf, B):

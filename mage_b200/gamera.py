@@ -55,7 +55,7 @@ EXPORTED = (
     "gam_set_background_dipole", "gam_set_wind", "gam_init_dipole_wind", "gam_write_restart", "gam_read_restart",
     "gam_halo_bytes", "gam_halo_pack", "gam_halo_unpack", "gam_init_finish_halo", "gam_set_start", "gam_step_begin",
     "gam_dt_partial", "gam_step_end", "gam_set_slab_edges", "gam_flux_forward", "gam_flux_adjoint",
-    "gam_efield_forward", "gam_efield_adjoint",
+    "gam_efield_forward", "gam_efield_adjoint", "gam_predict_stage", "gam_update_stage",
 )
 
 # Background-field arrays (Grid_T, gamtypes.F90:233-242): name, components;
@@ -106,6 +106,11 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         [C.c_void_p] * 3
     L.gam_efield_adjoint.argtypes = [C.POINTER(_Params), C.c_int32] + [C.c_void_p] * 9 + [_dp, C.c_double] + \
         [C.c_void_p] * 8
+    _vpp = C.POINTER(C.c_void_p)
+    L.gam_predict_stage.argtypes = [C.POINTER(_Params), C.c_int32, _vpp, _vpp, C.c_double, C.c_double, _vpp, _vpp,
+                                    C.c_void_p, _vpp, C.c_void_p]
+    L.gam_update_stage.argtypes = [C.POINTER(_Params), C.c_int32, _vpp, _vpp, _dp, C.c_double, _vpp, _vpp,
+                                   C.c_void_p, C.c_void_p, _vpp, C.c_void_p]
     L.gam_halo_pack.argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
     L.gam_halo_unpack.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32]
     L.gam_init_finish_halo.argtypes = [C.c_void_p, _dp]
