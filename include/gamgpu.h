@@ -94,7 +94,11 @@ int gam_get_geometry_arrays(gam_handle* h, double* face, double* xfc, double* Tf
 
 /* State%Gas(c,5), State%magFlux(f,3), State%Bxyz(c,3) and the previous state
  * oState%Gas, oState%magFlux, with State%time, oState%time, Model%dt and
- * Model%ts. Replaces the in-memory state of gamApp_T (gamtypes.F90:301-321). */
+ * Model%ts. Replaces the in-memory state of gamApp_T (gamtypes.F90:301-321).
+ * oGas = omagFlux = NULL (after a first full upload): oState stays as it is
+ * on the device and only State crosses PCIe. After gam_step the device's
+ * oState is the State before that step (CopyState, mhdgroup.F90:202-256),
+ * i.e. the oState of a driver that steps one AdvanceModel at a time. */
 int gam_upload_state(gam_handle* h, const double* Gas, const double* magFlux, const double* Bxyz,
                      const double* oGas, const double* omagFlux, double time, double otime, double dt, int32_t ts);
 int gam_download_state(gam_handle* h, double* Gas, double* magFlux, double* Bxyz, double* oGas,

@@ -439,12 +439,31 @@ static int set_scalars(gam_handle* h, double time, double otime, double dt, int3
     return GAM_OK;
 }
 
+// oState kept on the device (oGas = omagFlux = NULL): only State is replaced;
+// after a step the other buffer holds the State before that step, which is
+// the driver's oState (CopyState, mhdgroup.F90:202-256)
+template <class R>
+static int upload_new_state_t(gam_handle* h, Ctx<R>& C, const double* Gas, const double* magFlux, const double* Bxyz) {
+    int rc;
+    if ((rc = up_r<R>(h, Gas, C.st[h->cur].Gas, false, 5))) return rc;
+    if ((rc = up_r<R>(h, magFlux, C.st[h->cur].mf, true, 3))) return rc;
+    if ((rc = up_r<R>(h, Bxyz, C.st[h->cur].B, false, 3))) return rc;
+    return GAM_OK;
+}
+
 extern "C" int gam_upload_state(gam_handle* h, const double* Gas, const double* magFlux, const double* Bxyz,
                                 const double* oGas, const double* omagFlux, double time, double otime, double dt,
                                 int32_t ts) {
-    if (!h || !Gas || !magFlux || !Bxyz || !oGas || !omagFlux) return GAM_EINVAL;
-    int rc = h->f32 ? upload_state_t<float>(h, h->cf, Gas, magFlux, Bxyz, oGas, omagFlux)
+    if (!h || !Gas || !magFlux || !Bxyz || (!oGas) != (!omagFlux)) return GAM_EINVAL;
+    int rc;
+    if (!oGas) {
+        if (!h->haveState) return fail(h, GAM_ESTATE, "oState can stay on the device only after a first full upload");
+        rc = h->f32 ? upload_new_state_t<float>(h, h->cf, Gas, magFlux, Bxyz)
+                    : upload_new_state_t<double>(h, h->cd, Gas, magFlux, Bxyz);
+    } else {
+        rc = h->f32 ? upload_state_t<float>(h, h->cf, Gas, magFlux, Bxyz, oGas, omagFlux)
                     : upload_state_t<double>(h, h->cd, Gas, magFlux, Bxyz, oGas, omagFlux);
+    }
     if (rc) return rc;
     if ((rc = set_scalars(h, time, otime, dt, ts))) return rc;
     CK(h, cudaStreamSynchronize(h->s));

@@ -405,8 +405,8 @@ __device__ __forceinline__ void edge_lrs(const GamBox& b, const DevParams<R>& P,
 }
 
 // VxB edge loop for direction eD (fields.F90:184-228).
-template <class R>
-__global__ void __launch_bounds__(128) k_vxb(GamBox b, DevParams<R> P, Geo<R> g, Work<R> w, int eD, Range r,
+template <class R, int MINB = 1>
+__global__ void __launch_bounds__(128, MINB) k_vxb(GamBox b, DevParams<R> P, Geo<R> g, Work<R> w, int eD, Range r,
                                              const GamScalars* sc) {
     if (sc->halted) return;
     int ii, jj, kk;
@@ -1186,7 +1186,14 @@ template <class R, class F> void for_each_kernel(const Ctx<R>& C, int cur, cudaS
                              {G, G + b.Nip, G, G + b.Njp, G, G + b.Nkp - 1}};
         for (int eD = 0; eD < 3; eD++) {
             f(2 + 2 * eD, [&] { k_mom2face<R><<<grid_for(mf[eD], blk), blk, 0, s>>>(b, C.P, C.g, C.w, eD, mf[eD], C.sc); });
-            f(3 + 2 * eD, [&] { k_vxb<R><<<grid_for(ed[eD], blk), blk, 0, s>>>(b, C.P, C.g, C.w, eD, ed[eD], C.sc); });
+            f(3 + 2 * eD, [&] {
+                if (C.kvar & 16)
+                    k_vxb<R, 10><<<grid_for(ed[eD], blk), blk, 0, s>>>(b, C.P, C.g, C.w, eD, ed[eD], C.sc);
+                else if (C.kvar & 32)
+                    k_vxb<R, 12><<<grid_for(ed[eD], blk), blk, 0, s>>>(b, C.P, C.g, C.w, eD, ed[eD], C.sc);
+                else
+                    k_vxb<R><<<grid_for(ed[eD], blk), blk, 0, s>>>(b, C.P, C.g, C.w, eD, ed[eD], C.sc);
+            });
         }
     }
     const Range fr[3] = {{G, G + b.Nip, G, G + b.Njp - 1, G, kke},
@@ -1200,7 +1207,7 @@ template <class R, class F> void for_each_kernel(const Ctx<R>& C, int cur, cudaS
             case 1: k_stress<R, D, 1><<<grid_for(r, sblk), sblk, 0, s>>>(b, C.P, C.g, Blim, C.w, r, C.sc); break;
             case 2: k_stress<R, D, 7><<<grid_for(r, sblk), sblk, 0, s>>>(b, C.P, C.g, Blim, C.w, r, C.sc); break;
             case 3: k_stress<R, D, 8><<<grid_for(r, sblk), sblk, 0, s>>>(b, C.P, C.g, Blim, C.w, r, C.sc); break;
-            default: k_stress<R, D, 6><<<grid_for(r, sblk), sblk, 0, s>>>(b, C.P, C.g, Blim, C.w, r, C.sc); break;
+            default: k_stress<R, D, sizeof(R) == 4 ? 8 : 6><<<grid_for(r, sblk), sblk, 0, s>>>(b, C.P, C.g, Blim, C.w, r, C.sc); break;
         }
     };
     f(8, [&] { stress(std::integral_constant<int, 0>()); });

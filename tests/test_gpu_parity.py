@@ -284,3 +284,24 @@ def test_strict_model_options_bit_exact(oracle_built, kw):
     for k in STATE:
         assert np.array_equal(s[k], o.array(k)), (kw, k, rel_err(s[k], o.array(k)))
     assert dt == o.scalars()["dt"]
+
+
+def test_upload_keeping_old_state_on_device():
+    """gam_upload_state with oGas = omagFlux = NULL keeps oState on the device:
+    a driver that downloads and re-uploads State around every step gets the
+    same steps as one that never leaves the device."""
+    N = (16, 16, 16)
+    xyz = grids.warped_periodic_corners(*N)
+    a, b = GameraGPU(GamParams(*N)), GameraGPU(GamParams(*N))
+    for g in (a, b):
+        g.set_geometry(xyz)
+        g.init_blast_wave()
+    a.step_gamera(4)
+    for _ in range(4):
+        s = b.download_state(old=False)
+        b.upload_state(s["Gas"], s["magFlux"], s["Bxyz"], None, None, s["time"], b.download_state()["otime"], s["dt"],
+                       s["ts"])
+        b.step_gamera(1)
+    sa, sb = a.download_state(), b.download_state()
+    for k in STATE:
+        assert np.array_equal(sa[k], sb[k]), k
