@@ -92,6 +92,8 @@ struct gam_handle {
     int cur = 0;
     bool haveGeo = false, haveState = false, haveXyz = false;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaStream_t aux[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t evs[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     double lastMs = 0.0;
     std::string err;
 };
@@ -272,6 +274,15 @@ extern "C" int gam_create(const gam_params* p, gam_handle** out) {
         *out = h;
         return rc;
     }
+    // side streams and events for the parallel branches of the step graph
+    for (int q = 0; q < 5; q++)
+        if (cudaStreamCreateWithFlags(&h->aux[q], cudaStreamNonBlocking) != cudaSuccess)
+            return bad(GAM_ECUDA, "stream creation failed");
+    for (int q = 0; q < 8; q++)
+        if (cudaEventCreateWithFlags(&h->evs[q], cudaEventDisableTiming) != cudaSuccess)
+            return bad(GAM_ECUDA, "event creation failed");
+    for (int q = 0; q < 5; q++) h->cd.aux[q] = h->cf.aux[q] = h->aux[q];
+    for (int q = 0; q < 8; q++) h->cd.ev[q] = h->cf.ev[q] = h->evs[q];
     GamScalars s0;
     memset(&s0, 0, sizeof(s0));
     s0.tFin = p->tFin; s0.dt0 = p->dt0; s0.limDT0 = p->limDT0; s0.CFL = p->CFL;
@@ -297,6 +308,10 @@ extern "C" int gam_destroy(gam_handle* h) {
     for (void* p : h->allocs) cudaFree(p);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
+    for (int q = 0; q < 8; q++)
+        if (h->evs[q]) cudaEventDestroy(h->evs[q]);
+    for (int q = 0; q < 5; q++)
+        if (h->aux[q]) cudaStreamDestroy(h->aux[q]);
     if (h->s) cudaStreamDestroy(h->s);
     delete h;
     return GAM_OK;

@@ -1160,7 +1160,7 @@ static inline dim3 grid_for(const Range& r, dim3 blk) {
 // I/J/K, 11 update_faces, 12 update_cells, 13 dt_finalize, 14 bc.
 // st[cur] is State (n); st[1-cur] holds oState (n-1) on entry and State
 // (n+1) on exit.
-template <class R, class F> void for_each_kernel(const Ctx<R>& C, int cur, cudaStream_t s, F&& f) {
+template <class R, class F> void for_each_kernel(const Ctx<R>& C, int cur, cudaStream_t& s, F&& f) {
     const GamBox& b = C.b;
     const int G = GAM_NG;
     const StateBuf<R> S = C.st[cur], O = C.st[1 - cur];
@@ -1189,7 +1189,7 @@ template <class R, class F> void for_each_kernel(const Ctx<R>& C, int cur, cudaS
             f(3 + 2 * eD, [&] {
                 if (C.kvar & 16)
                     k_vxb<R, 10><<<grid_for(ed[eD], blk), blk, 0, s>>>(b, C.P, C.g, C.w, eD, ed[eD], C.sc);
-                else if (C.kvar & 32)
+                else if ((C.kvar & 32) || sizeof(R) == 4)  // FP32: 12 blocks/SM (40 registers) measured best
                     k_vxb<R, 12><<<grid_for(ed[eD], blk), blk, 0, s>>>(b, C.P, C.g, C.w, eD, ed[eD], C.sc);
                 else
                     k_vxb<R><<<grid_for(ed[eD], blk), blk, 0, s>>>(b, C.P, C.g, C.w, eD, ed[eD], C.sc);
@@ -1224,8 +1224,54 @@ template <class R, class F> void for_each_kernel(const Ctx<R>& C, int cur, cudaS
     f(14, [&] { launch_bcs(C, O, s, 0); });
 }
 
+// One step. With side streams (C.aux, C.ev) the independent kernels run as
+// parallel branches of the captured graph: the three Mom2Face -> EMF chains
+// (then the face update) beside the three flux directions; the cell update
+// joins them. Every branch writes its own arrays, so the result is the same
+// bits as the sequential order.
 template <class R> void launch_step(const Ctx<R>& C, int cur, cudaStream_t s) {
-    for_each_kernel(C, cur, s, [](int, auto&& L) { L(); });
+    cudaStream_t cs = s;
+    if (!C.aux[0] || (C.kvar & 64)) {
+        for_each_kernel(C, cur, cs, [](int, auto&& L) { L(); });
+        return;
+    }
+    for_each_kernel(C, cur, cs, [&](int id, auto&& L) {
+        switch (id) {
+            case 0:
+            case 1:
+                cs = s;
+                L();
+                if (id == 1) {
+                    cudaEventRecord(C.ev[0], s);
+                    for (int q = 0; q < 5; q++) cudaStreamWaitEvent(C.aux[q], C.ev[0], 0);
+                }
+                return;
+            case 2: case 3: cs = C.aux[0]; break;
+            case 4: case 5: cs = C.aux[1]; break;
+            case 6: case 7: cs = C.aux[2]; break;
+            case 8: cs = s; break;
+            case 9: cs = C.aux[3]; break;
+            case 10: cs = C.aux[4]; break;
+            case 11:
+                cudaEventRecord(C.ev[1], C.aux[1]);
+                cudaEventRecord(C.ev[2], C.aux[2]);
+                cudaStreamWaitEvent(C.aux[0], C.ev[1], 0);
+                cudaStreamWaitEvent(C.aux[0], C.ev[2], 0);
+                cs = C.aux[0];
+                break;
+            case 12:
+                cudaEventRecord(C.ev[3], C.aux[0]);
+                cudaEventRecord(C.ev[4], C.aux[3]);
+                cudaEventRecord(C.ev[5], C.aux[4]);
+                cudaStreamWaitEvent(s, C.ev[3], 0);
+                cudaStreamWaitEvent(s, C.ev[4], 0);
+                cudaStreamWaitEvent(s, C.ev[5], 0);
+                cs = s;
+                break;
+            default: cs = s; break;
+        }
+        L();
+    });
 }
 
 // Device time of each kernel of a step (ms, average of reps back-to-back
@@ -1237,7 +1283,8 @@ template <class R> void profile_step(const Ctx<R>& C, int cur, cudaStream_t s, i
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     for (int q = 0; q < 15; q++) ms[q] = 0.0;
-    for_each_kernel(C, cur, s, [&](int id, auto&& L) {
+    cudaStream_t cs = s;
+    for_each_kernel(C, cur, cs, [&](int id, auto&& L) {
         if (id == 0 || id == 13) return;
         L();  // warm
         cudaEventRecord(e0, s);
@@ -1285,7 +1332,8 @@ template <class R> void launch_init(const Ctx<R>& C, int cur, cudaStream_t s) {
 // sc->nbad), phase 1 = dt decision and boundary fill. The caller writes the
 // global min / count into sc between them (gamapp_mpi.F90:495-512).
 template <class R> void launch_step_phase(const Ctx<R>& C, int cur, cudaStream_t s, int phase) {
-    for_each_kernel(C, cur, s, [&](int id, auto&& L) {
+    cudaStream_t cs = s;
+    for_each_kernel(C, cur, cs, [&](int id, auto&& L) {
         if ((id <= 12) == (phase == 0)) L();
     });
 }

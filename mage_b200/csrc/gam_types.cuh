@@ -85,4 +85,8 @@ template <class R> struct Ctx {
     GamScalars* sc;
     double gamma, gm1;
     int kvar;  // launch-configuration variant for tuning runs (GAM_KVAR); 0 = the tuned default
+    // side streams and fork/join events of the step graph (independent
+    // kernels of a step run as parallel branches); null: one stream
+    cudaStream_t aux[5];
+    cudaEvent_t ev[8];
 };
