@@ -159,6 +159,89 @@ module gamgpu
             integer(c_int32_t), value :: nbad
             real(c_double), intent(out) :: dt, t
         end function
+        integer(c_int) function gam_get_geometry_arrays(h, face, xfc, Tf, volume, xyzcc, di, dj, dk, edge, Te, Teb) &
+                bind(C, name="gam_get_geometry_arrays")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h, face, xfc, Tf, volume, xyzcc, di, dj, dk, edge, Te, Teb
+        end function
+        integer(c_int) function gam_init_orszag_tang(h) bind(C, name="gam_init_orszag_tang")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h
+        end function
+        integer(c_int) function gam_init_blast_wave(h, bw) bind(C, name="gam_init_blast_wave")
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: h
+            real(c_double), intent(in) :: bw(9)
+        end function
+        integer(c_int) function gam_profile_step(h, reps, ms, n) bind(C, name="gam_profile_step")
+            import :: c_int, c_ptr, c_int32_t, c_double
+            type(c_ptr), value :: h
+            integer(c_int32_t), value :: reps, n
+            real(c_double), intent(out) :: ms(n)
+        end function
+        integer(c_int) function gam_last_step_ms(h, ms) bind(C, name="gam_last_step_ms")
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: h
+            real(c_double), intent(out) :: ms
+        end function
+        integer(c_int) function gam_totals_noalloc(Gas, volume, Nip, Njp, Nkp, out, stream, err, errlen) &
+                bind(C, name="gam_totals_noalloc")
+            import :: c_int, c_ptr, c_int32_t
+            type(c_ptr), value :: Gas, volume, out, stream, err
+            integer(c_int32_t), value :: Nip, Njp, Nkp, errlen
+        end function
+        ! differentiation form: stage forwards and their hand-written adjoints on
+        ! device arrays (see include/gamgpu.h for the layouts)
+        integer(c_int) function gam_flux_forward(p, fp32, QW, Wn, QB, Blim, Bnf, volume, face, Tf, fcB0, bFlux0, gF, mF, &
+                stream) bind(C, name="gam_flux_forward")
+            import :: c_int, c_ptr, c_int32_t, gam_params
+            type(gam_params), intent(in) :: p
+            integer(c_int32_t), value :: fp32
+            type(c_ptr), value :: QW, Wn, QB, Blim, Bnf, volume, face, Tf, fcB0, bFlux0, gF, mF, stream
+        end function
+        integer(c_int) function gam_flux_adjoint(p, fp32, QW, Wn, QB, Blim, Bnf, volume, face, Tf, fcB0, bFlux0, dgF, &
+                dmF, dQW, dWn, dQB, dBlim, dBnf, stream) bind(C, name="gam_flux_adjoint")
+            import :: c_int, c_ptr, c_int32_t, gam_params
+            type(gam_params), intent(in) :: p
+            integer(c_int32_t), value :: fp32
+            type(c_ptr), value :: QW, Wn, QB, Blim, Bnf, volume, face, Tf, fcB0, bFlux0, dgF, dmF, dQW, dWn, dQB, dBlim, &
+                                  dBnf, stream
+        end function
+        integer(c_int) function gam_efield_forward(p, fp32, Dh, abh, bn, VdV, volume, face, edge, Te, Teb, edgB0, dt, AVf, &
+                E, stream) bind(C, name="gam_efield_forward")
+            import :: c_int, c_ptr, c_int32_t, c_double, gam_params
+            type(gam_params), intent(in) :: p
+            integer(c_int32_t), value :: fp32
+            type(c_ptr), value :: Dh, abh, bn, VdV, volume, face, edge, Te, Teb, edgB0, AVf, E, stream
+            real(c_double), value :: dt
+        end function
+        integer(c_int) function gam_efield_adjoint(p, fp32, Dh, abh, bn, VdV, volume, face, edge, Te, Teb, edgB0, dt, AVf, &
+                dE, dDh, dabh, dbn, dVdV, dAVf, stream) bind(C, name="gam_efield_adjoint")
+            import :: c_int, c_ptr, c_int32_t, c_double, gam_params
+            type(gam_params), intent(in) :: p
+            integer(c_int32_t), value :: fp32
+            type(c_ptr), value :: Dh, abh, bn, VdV, volume, face, edge, Te, Teb, edgB0, AVf, dE, dDh, dabh, dbn, dVdV, dAVf, &
+                                  stream
+            real(c_double), value :: dt
+        end function
+        integer(c_int) function gam_predict_stage(p, fp32, st, geo, pdt, odt, out, din, aB, dst, stream) &
+                bind(C, name="gam_predict_stage")
+            import :: c_int, c_ptr, c_int32_t, c_double, gam_params
+            type(gam_params), intent(in) :: p
+            integer(c_int32_t), value :: fp32
+            type(c_ptr), intent(in) :: st(4), geo(5)
+            real(c_double), value :: pdt, odt
+            type(c_ptr), value :: out, din, aB, dst, stream
+        end function
+        integer(c_int) function gam_update_stage(p, fp32, in, geo, dpB0, dt, out, din, sU, sM, dst, stream) &
+                bind(C, name="gam_update_stage")
+            import :: c_int, c_ptr, c_int32_t, c_double, gam_params
+            type(gam_params), intent(in) :: p
+            integer(c_int32_t), value :: fp32
+            type(c_ptr), intent(in) :: in(5), geo(4)
+            type(c_ptr), value :: dpB0, out, din, sU, sM, dst, stream
+            real(c_double), value :: dt
+        end function
         integer(c_int) function gam_write_restart(h, path) bind(C, name="gam_write_restart")
             import :: c_int, c_ptr, c_char
             type(c_ptr), value :: h

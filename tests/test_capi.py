@@ -30,3 +30,18 @@ def test_default_params_match_reference():
     assert L.gam_default_params(C.byref(p), 64, 64, 1) == 0
     assert abs(p.gamma - 5.0 / 3.0) < 1e-15 and p.pdmb == 0.75 and abs(p.CFL - 0.3) < 1e-15
     assert p.Vd0 == 0.5 and p.cHogH == 0.25 and p.dFloor == 1e-12 and p.do25D == 1 and p.nG == 4
+
+
+def test_fortran_module_binds_every_entry_point():
+    """mage_b200/fortran/gamgpu.F90 declares a bind(C) interface for every
+    function of the header, and its gam_params type has the C struct's fields
+    in the same order."""
+    src = open(os.path.join(ROOT, "mage_b200", "fortran", "gamgpu.F90")).read()
+    bound = set(re.findall(r'bind\(C, name="(gam_\w+)"\)', src))
+    assert set(declared()) <= bound, sorted(set(declared()) - bound)
+    body = src[src.index("type, bind(C) :: gam_params"):src.index("end type gam_params")]
+    names = []
+    for line in body.splitlines()[1:]:
+        if "::" in line:
+            names += [n.strip().split("(")[0] for n in line.split("::")[1].split(",") if n.strip()]
+    assert names == [f for f, _ in gamera._Params._fields_], names
