@@ -108,6 +108,13 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
+# Lane-instructions per active cell-update of the FP64 step: ncu sum of
+# smsp__inst_executed x 32 over one 96^3 step (profiles/
+# blast96_fp64_step_kernels_full.md: 17,920), scaled to 192^3 by the ratio of
+# ghosted to active cells ((200/192)^3 / (104/96)^3).
+INST_PER_CELL_F64 = 17920 * (200 / 192) ** 3 / (104 / 96) ** 3
+
+
 def committed_traffic(workload, dtype):
     """DRAM bytes per cell-update of one step from the committed ncu summary."""
     p = os.path.join(ROOT, "profiles", "traffic.json")
@@ -425,6 +432,11 @@ def main():
     bpc = BYTES_PER_CELL_B0 if w["problem"] == "dipole" else BYTES_PER_CELL
     achieved = per_gpu * bpc["f64"] / 1e9
     traffic = committed_traffic(args.workload, "f64")
+    # per-kernel device times of one step (CUDA events, each kernel repeated on
+    # the current state; gam_profile_step leaves the state unchanged)
+    kms = {k: v for k, v in g.profile_step(3).items() if v > 0}
+    ktot = sum(kms.values())
+    kernels = {k: {"ms": v, "share": v / ktot} for k, v in kms.items()}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_sample(g, w, g.params)
@@ -441,7 +453,16 @@ def main():
                          "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
                          "bytes_per_cell_update": bpc["f64"],
                          "traffic": None if traffic is None else traffic * cells,
-                         "unit_of_launch": "one step (CUDA graph of the step's kernels) over the whole grid"},
+                         "unit_of_launch": "one step (CUDA graph of the step's kernels) over the whole grid",
+                         "kernels_ms": kernels},
+            # the step is bound by instruction issue (FP64 arithmetic), not HBM
+            "issue_bound": {"lane_inst_per_cell_update": INST_PER_CELL_F64,
+                            "achieved_lane_inst_per_s": per_gpu * INST_PER_CELL_F64,
+                            "peak_lane_inst_per_s": 148 * 4 * 32 * clocks["sm_mhz"] * 1e6 if clocks.get("sm_mhz") else None,
+                            "frac": (per_gpu * INST_PER_CELL_F64 / (148 * 4 * 32 * clocks["sm_mhz"] * 1e6))
+                            if clocks.get("sm_mhz") else None,
+                            "note": "148 SMs x 4 schedulers x 1 warp-instruction (32 lanes) per clock at the median "
+                                    "SM clock sampled in the timed region"} if w["problem"] == "bw" else None,
             "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "steps": args.e2e_steps,
                     "what": "per step: gam_upload_state of the State from pinned host memory (oState stays on "
