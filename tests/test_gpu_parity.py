@@ -305,3 +305,21 @@ def test_upload_keeping_old_state_on_device():
     sa, sb = a.download_state(), b.download_state()
     for k in STATE:
         assert np.array_equal(sa[k], sb[k]), k
+
+
+@pytest.mark.parametrize("prec,bound", [(0, 1e-11), (FP32, 1e-4)], ids=["fp64", "fp32"])
+def test_orszag_tang_symmetry_on_gpu(prec, bound):
+    """Point symmetry of the Orszag-Tang vortex (tests/cases/testCases.pf:
+    183-225 asserts <= 1e-11 at t = 1 on 128^2): 128x128x4 (the C1 grid),
+    100 steps of the product build; the FP32 form to its own bound."""
+    N = 128
+    g = GameraGPU(GamParams(N, N, 4, precision=prec))
+    g.set_geometry(grids.uniform_corners(N, N, 4))
+    g.init_orszag_tang()
+    g.step_gamera(100)
+    Gas = g.download_state(old=False)["Gas"]
+    G = Gas[:, 4, 4:4 + N, 4:4 + N]
+    F = G[:, ::-1, ::-1].copy()
+    F[1:3] *= -1.0
+    sym = float(np.sqrt(((G - F) ** 2).sum(axis=0)).sum() / (N * N))
+    assert sym <= bound, sym
