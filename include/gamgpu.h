@@ -37,12 +37,18 @@ enum {
     GAM_EHOOK = 7          /* a Model%Hack* hook is set: not supported on the GPU */
 };
 
-/* Boundary kinds (EnforceBCs, step.F90:17-55). Per side: INI periodic, none or
- * GAM_BC_SPHIN (bcs.F90:934-957); OUTI periodic, none or GAM_BC_WIND (constant
- * solar wind, apps/wind.F90:206-391); INJ/OUTJ periodic, none or
- * GAM_BC_ZEROGRAD (bcs.F90:853-892); INK/OUTK periodic or none. */
+/* Boundary kinds (EnforceBCs, step.F90:17-55). Per side: INI periodic, none,
+ * GAM_BC_SPHIN (bcs.F90:934-957) or GAM_BC_INFLOW; OUTI periodic, none,
+ * GAM_BC_WIND (constant solar wind, apps/wind.F90:206-391) or GAM_BC_ZEROGRAD
+ * (zeroGrad_obcI, bcs.F90:820-850); INJ/OUTJ periodic, none or
+ * GAM_BC_ZEROGRAD (bcs.F90:853-892); INK/OUTK periodic or none.
+ * GAM_BC_INFLOW has no counterpart in the reference: the 4 inner-I ghost
+ * layers hold a uniform state (gam_set_inflow) and the face fluxes of its
+ * field, the shape of zeroGrad_obcI with a given state in place of the last
+ * active cell. */
 enum { GAM_BC_PERIODIC = 0, GAM_BC_NONE = 1, GAM_BC_ZEROGRAD = 2, GAM_BC_SPHIN = 3, GAM_BC_WIND = 4,
-       GAM_BC_HALO = 5 /* INK and OUTK of a k-slab: filled by the caller's halo exchange */ };
+       GAM_BC_HALO = 5 /* INK and OUTK of a k-slab: filled by the caller's halo exchange */,
+       GAM_BC_INFLOW = 6 };
 enum { GAM_RECON_8CENT = 0, GAM_RECON_7UP = 1 };
 enum { GAM_FP64 = 0, GAM_FP32 = 1 };
 
@@ -165,6 +171,15 @@ int gam_set_background_dipole(gam_handle* h, double M0);
  * layers are computed here once from the metric. Replaces the windBC_T set-up
  * of the driver (apps/wind.F90:40-176) for a constant wind. */
 int gam_set_wind(gam_handle* h, const double wind[8]);
+
+/* State of the uniform inner-I inflow (bc[0] = GAM_BC_INFLOW), same order as
+ * the wind: {rho, P, Vx, Vy, Vz, Bx, By, Bz}. Ghost cell is-n (n = 1..4, every
+ * j, k of the cell ranges) gets the conserved form of that state (CellP2C,
+ * gamutils.F90:362-383), its I face is-n and its J and K faces the flux
+ * face * (n . B), and, in the first boundary fill only, its Bxyz from those
+ * fluxes (steps recompute every ghost's Bxyz). Call before the initial
+ * condition; calling it later changes the boundary from the next step on. */
+int gam_set_inflow(gam_handle* h, const double state[8]);
 
 /* Dipole-in-wind start: the wind state in every active cell with the density
  * perturbed by amp*u (u uniform in [-1, 1), SplitMix64 of seed and the Fortran

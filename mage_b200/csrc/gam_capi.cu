@@ -75,7 +75,7 @@ struct gam_handle {
     GamBox b;
     BgD bg{};
     double* windTab = nullptr;  // device: wC, wF(3), sF(3) of the solar-wind BC
-    bool haveBg = false, haveWind = false;
+    bool haveBg = false, haveWind = false, haveInflow = false;
     cudaStream_t s = nullptr;
     bool f32 = false;
     std::vector<void*> allocs;
@@ -212,11 +212,13 @@ extern "C" int gam_create(const gam_params* p, gam_handle** out) {
     if (p->precision != GAM_FP64 && p->precision != GAM_FP32) return bad(GAM_EINVAL, "unknown precision");
     if (p->precision == GAM_FP32 && p->strict) return bad(GAM_EINVAL, "strict applies to the FP64 form only");
     {
-        // boundary kinds per side: inner I periodic/none/SphIn, outer I
-        // periodic/none/wind, J periodic/none/zero-gradient, K periodic/none
+        // boundary kinds per side: inner I periodic/none/SphIn/inflow, outer I
+        // periodic/none/wind/zero-gradient, J periodic/none/zero-gradient,
+        // K periodic/none (or halo)
         const int* c = p->bc;
         auto in = [](int v, int a, int b2, int c2) { return v == a || v == b2 || v == c2; };
-        if (!in(c[0], GAM_BC_PERIODIC, GAM_BC_NONE, GAM_BC_SPHIN) || !in(c[1], GAM_BC_PERIODIC, GAM_BC_NONE, GAM_BC_WIND) ||
+        if (!(in(c[0], GAM_BC_PERIODIC, GAM_BC_NONE, GAM_BC_SPHIN) || c[0] == GAM_BC_INFLOW) ||
+            !(in(c[1], GAM_BC_PERIODIC, GAM_BC_NONE, GAM_BC_WIND) || c[1] == GAM_BC_ZEROGRAD) ||
             !in(c[2], GAM_BC_PERIODIC, GAM_BC_NONE, GAM_BC_ZEROGRAD) ||
             !in(c[3], GAM_BC_PERIODIC, GAM_BC_NONE, GAM_BC_ZEROGRAD) ||
             !in(c[4], GAM_BC_PERIODIC, GAM_BC_NONE, GAM_BC_HALO) || !in(c[5], GAM_BC_PERIODIC, GAM_BC_NONE, GAM_BC_HALO))
@@ -542,6 +544,8 @@ extern "C" int gam_step(gam_handle* h, int32_t nsteps, double* dt, double* t) {
     if (!h->haveState) return fail(h, GAM_ESTATE, "gam_step before gam_upload_state");
     if (h->p.doBackground && !h->haveBg) return fail(h, GAM_ESTATE, "doBackground: set the background field first");
     if (h->p.bc[1] == GAM_BC_WIND && !h->haveWind) return fail(h, GAM_ESTATE, "wind boundary: call gam_set_wind first");
+    if (h->p.bc[0] == GAM_BC_INFLOW && !h->haveInflow)
+        return fail(h, GAM_ESTATE, "inflow boundary: call gam_set_inflow first");
     if (h->p.bc[4] == GAM_BC_HALO)
         return fail(h, GAM_ESTATE, "a k-slab steps with gam_step_begin / gam_step_end and a halo exchange");
     int rc;
@@ -731,6 +735,8 @@ void gam_fast_init_f64(const Ctx<double>& C, int cur, cudaStream_t s);
 void gam_fast_init_f32(const Ctx<float>& C, int cur, cudaStream_t s);
 
 static int init_common(gam_handle* h, double* Gas64, double* mf64) {
+    if (h->p.bc[0] == GAM_BC_INFLOW && !h->haveInflow)
+        return fail(h, GAM_ESTATE, "inflow boundary: call gam_set_inflow before the initial condition");
     int rc = h->f32 ? finish_init<float>(h, h->cf, Gas64, mf64, 0.0) : finish_init<double>(h, h->cd, Gas64, mf64, 0.0);
     if (rc) return rc;
     // Bxyz of State, first BCs, copy to oState (init.F90:217-238)
@@ -913,6 +919,19 @@ extern "C" int gam_set_wind(gam_handle* h, const double wind[8]) {
     h->cf.P.wind = W;
     drop_graphs(h);
     h->haveWind = true;
+    return GAM_OK;
+}
+
+extern "C" int gam_set_inflow(gam_handle* h, const double state[8]) {
+    if (!h || !state) return GAM_EINVAL;
+    if (h->p.bc[0] != GAM_BC_INFLOW) return fail(h, GAM_ESTATE, "the inner I boundary is not an inflow");
+    if (!(state[0] > 0.0)) return fail(h, GAM_EINVAL, "inflow density must be positive");
+    for (int v = 0; v < 8; v++) {
+        h->cd.P.inflow[v] = state[v];
+        h->cf.P.inflow[v] = state[v];
+    }
+    drop_graphs(h);
+    h->haveInflow = true;
     return GAM_OK;
 }
 

@@ -784,8 +784,8 @@ __global__ void k_dt_finalize(GamScalars* sc) {
 }
 
 // Boundary kinds: 0 periodic, 1 none, 2 zero-gradient, 3 inner sphere,
-// 4 solar wind (include/gamgpu.h).
-enum { BCK_PERIODIC = 0, BCK_NONE = 1, BCK_ZEROGRAD = 2, BCK_SPHIN = 3, BCK_WIND = 4 };
+// 4 solar wind, 6 uniform inflow (include/gamgpu.h).
+enum { BCK_PERIODIC = 0, BCK_NONE = 1, BCK_ZEROGRAD = 2, BCK_SPHIN = 3, BCK_WIND = 4, BCK_INFLOW = 6 };
 
 // Gather maps of the boundary conditions that copy values (bcs.F90:279-450
 // periodic, :799-892 zero-gradient, :934-957 SphIn). x is the box index along
@@ -865,9 +865,19 @@ __device__ __forceinline__ double norm2s3(const double* a) {
     return scale * sqrt(res);
 }
 
-// The non-periodic I boundaries, in place: the SphIn copy on the inner side
-// (bcs.F90:934-957) and the solar-wind blend on the outer side
-// (apps/wind.F90:206-300), for ghost layer n = 1..4 of every (j, k).
+// face * (n . B) on face d of box cell c (zeroGrad_obcI, bcs.F90:842-844)
+template <class R>
+__device__ __forceinline__ R face_proj(const GamBox& b, const Geo<R>& g, int d, long c, const R* B) {
+    const long fs = b.fs;
+    const R* n = g.Tf + (long)(9 * d) * fs + c;
+    return g.face[d * fs + c] * (B[0] * n[0] + B[1] * n[fs] + B[2] * n[2 * fs]);
+}
+
+// The non-periodic I boundaries, in place: the SphIn copy or the uniform
+// inflow on the inner side (bcs.F90:934-957), the solar-wind blend
+// (apps/wind.F90:206-300) or zeroGrad_obcI (bcs.F90:820-850) on the outer
+// side, for ghost layer n = 1..4 of every (j, k). Writes touch ghost cells and
+// ghost faces only; the reads are of the first / last active cell.
 template <class R>
 __global__ void __launch_bounds__(256) k_bc_iside(GamBox b, DevParams<R> P, Geo<R> g, StateBuf<R> s,
                                                   const GamScalars* sc) {
@@ -888,6 +898,29 @@ __global__ void __launch_bounds__(256) k_bc_iside(GamBox b, DevParams<R> P, Geo<
         for (int x = 0; x < 3; x++) s.mf[x * fs + dst] = s.mf[x * fs + src];
 #pragma unroll
         for (int x = 0; x < 3; x++) s.B[x * fs + dst] = s.B[x * fs + src];
+    }
+    if (P.bc[0] == BCK_INFLOW && cellJK) {
+        const double* w = P.inflow;
+        R gW[5] = {(R)w[0], (R)w[2], (R)w[3], (R)w[4], (R)w[1]}, gC[5];
+        cell_p2c(P, gW, gC);
+        const R Bin[3] = {(R)w[5], (R)w[6], (R)w[7]};
+        const long c = lidx(b, G - n, jj, kk);
+#pragma unroll
+        for (int v = 0; v < 5; v++) s.Gas[v * fs + c] = gC[v];
+#pragma unroll
+        for (int d = 0; d < 3; d++) s.mf[d * fs + c] = face_proj(b, g, d, c, Bin);
+    }
+    if (P.bc[1] == BCK_ZEROGRAD && cellJK) {
+        const int ie = G + b.Nip - 1;
+        const long cp = lidx(b, ie, jj, kk), cg = lidx(b, ie + n, jj, kk);
+#pragma unroll
+        for (int v = 0; v < 5; v++) s.Gas[v * fs + cg] = s.Gas[v * fs + cp];
+        R B[3];
+        cell_bxyz(b, g, cp, s.mf[cp], s.mf[cp + 1], s.mf[fs + cp], s.mf[fs + cp + b.sx], s.mf[2 * fs + cp],
+                  s.mf[2 * fs + cp + b.sk], B);
+        s.mf[cg + 1] = face_proj(b, g, 0, cg + 1, B);
+        s.mf[fs + cg] = face_proj(b, g, 1, cg, B);
+        s.mf[2 * fs + cg] = face_proj(b, g, 2, cg, B);
     }
     if (P.bc[1] != BCK_WIND) return;
     const WindData& W = P.wind;
@@ -955,9 +988,11 @@ __global__ void __launch_bounds__(256) k_bc_iside(GamBox b, DevParams<R> P, Geo<
         s.mf[d * fs + cg] = (R)w * (R)W.sF[d * W.nw + wi] + ((R)1 - (R)w) * s.mf[d * fs + cin];
     }
 }
-// Bxyz of the wind ghost cells from their new fluxes (apps/wind.F90:341-351)
+// Bxyz of the wind (apps/wind.F90:341-351) or inflow ghost cells from their
+// new fluxes: ig = ie + n (outer) or is - n (inner)
 template <class R>
-__global__ void __launch_bounds__(256) k_bc_wind_b(GamBox b, Geo<R> g, StateBuf<R> s, const GamScalars* sc) {
+__global__ void __launch_bounds__(256) k_bc_iside_b(GamBox b, Geo<R> g, StateBuf<R> s, const GamScalars* sc,
+                                                    int outer) {
     if (sc->halted) return;
     const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
     const int n = 1 + (int)(t & 3);
@@ -965,7 +1000,7 @@ __global__ void __launch_bounds__(256) k_bc_wind_b(GamBox b, Geo<R> g, StateBuf<
     const int jj = (int)(q % b.Nj), kk = (int)(q / b.Nj);
     if (kk >= b.Nk) return;
     const long fs = b.fs;
-    const long c = lidx(b, GAM_NG + b.Nip - 1 + n, jj, kk);
+    const long c = lidx(b, outer ? GAM_NG + b.Nip - 1 + n : GAM_NG - n, jj, kk);
     R B[3];
     cell_bxyz(b, g, c, s.mf[c], s.mf[c + 1], s.mf[fs + c], s.mf[fs + c + b.sx], s.mf[2 * fs + c], s.mf[2 * fs + c + b.sk], B);
 #pragma unroll
@@ -1089,16 +1124,19 @@ __global__ void __launch_bounds__(256) k_bc(GamBox b, DevParams<R> P, Geo<R> g, 
 // All boundary conditions of one EnforceBCs (+ final bFlux2Fld unless copyB).
 template <class R> void launch_bcs(const Ctx<R>& C, const StateBuf<R>& S, cudaStream_t s, int copyB) {
     const GamBox& b = C.b;
-    const bool iside = C.P.bc[0] == BCK_SPHIN || C.P.bc[1] == BCK_WIND;
+    const bool iside = C.P.bc[0] == BCK_SPHIN || C.P.bc[0] == BCK_INFLOW || C.P.bc[1] == BCK_WIND ||
+                       C.P.bc[1] == BCK_ZEROGRAD;
     if (iside) {
         const long n = 4L * (b.Nj + 1) * (b.Nk + 1);
         k_bc_iside<R><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(b, C.P, C.g, S, C.sc);
-        // the wind's own Bxyz of its ghost cells matters only where no final
-        // bFlux2Fld follows (the initial fill); a step recomputes every ghost
-        if (C.P.bc[1] == BCK_WIND && copyB) {
-            const long m = 4L * b.Nj * b.Nk;
-            k_bc_wind_b<R><<<(unsigned)((m + 255) / 256), 256, 0, s>>>(b, C.g, S, C.sc);
-        }
+        // the wind's and the inflow's own Bxyz of their ghost cells matter
+        // only where no final bFlux2Fld follows (the initial fill); a step
+        // recomputes every ghost
+        const long m = 4L * b.Nj * b.Nk;
+        if (C.P.bc[1] == BCK_WIND && copyB)
+            k_bc_iside_b<R><<<(unsigned)((m + 255) / 256), 256, 0, s>>>(b, C.g, S, C.sc, 1);
+        if (C.P.bc[0] == BCK_INFLOW && copyB)
+            k_bc_iside_b<R><<<(unsigned)((m + 255) / 256), 256, 0, s>>>(b, C.g, S, C.sc, 0);
     }
     const Shell sh = make_shell(b);
     const long nsh = sh.nA + sh.nB + sh.nC;

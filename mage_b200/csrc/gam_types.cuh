@@ -24,6 +24,7 @@ template <class R> struct DevParams {
     // reference's isDT..ieDT); a k-slab drops it where a neighbour's cells lie
     int dtKlo, dtKhi;
     WindData wind;
+    double inflow[8];  // uniform inner-I inflow (bc[0] = 6): rho, P, Vx, Vy, Vz, Bx, By, Bz
 };
 
 template <class R> struct Geo {  // Grid_T arrays on the device (gamtypes.F90:168-250)

@@ -1,6 +1,7 @@
 """Measurements of the differentiation form (one JSON line).
 
   python -m mage_b200.diffbench c4            # 64^3 curvilinear blast wave, 20 steps
+  python -m mage_b200.diffbench c4_inflow      # the same with an x-inflow / x-outflow
   python -m mage_b200.diffbench c5 --steps 200  # 192x192x256 dipole in the wind
 
 c4: loss = sum of |B|^2 over the cells centred in [0.6, 0.8]^3 after N fixed-dt
@@ -131,6 +132,78 @@ def c4(N=(64, 64, 64), nsteps=20, sigma=1e-3, seed=2024):
     return out
 
 
+INFLOW_BCS = (6, 2, 0, 0, 0, 0)
+INFLOW = (1.0, 0.1, 0.5, 0.0, 0.0, 0.5 ** 0.5, 0.5 ** 0.5, 0.3)
+
+
+def c4_inflow(N=(64, 64, 64), nsteps=20, sigma=1e-3, seed=2024):
+    """The c4 grid and start with a uniform inflow on the inner I side
+    (rho, P, V, B = INFLOW) and zeroGrad_obcI on the outer one (periodic J, K):
+    gradient of sum |B|^2 over the cells centred at x < 0.25 (the part of the
+    grid the inflow reaches in the run) w.r.t. the start state and the inflow's
+    (rho, P, Vx, Bz), and central differences of the CUDA product step per
+    inflow component."""
+    xyz = grids.warped_periodic_corners(*N)
+    g0 = GameraGPU(GamParams(*N, bc=INFLOW_BCS))
+    g0.set_geometry(xyz)
+    g0.set_inflow(INFLOW)
+    g0.init_blast_wave()
+    st = g0.download_state(old=False)
+    dt = 0.5 * st["dt"]
+    geo = g0.get_geometry_arrays()
+    del g0
+    gpu = GameraGPU(GamParams(*N, bc=INFLOW_BCS, fixedTimestep=dt))
+    gpu.set_geometry(xyz)
+    rng = np.random.default_rng(seed)
+    P = DiffParams(*N, bc=INFLOW_BCS)
+    G64 = st["Gas"] * (1 + sigma * rng.standard_normal(st["Gas"].shape))
+    F64 = st["magFlux"] + sigma * np.asarray(geo["face"]) * rng.standard_normal(st["magFlux"].shape)
+    names = ("rho", "P", "Vx", "Vy", "Vz", "Bx", "By", "Bz")
+    out = {"config": f"curvilinear blast wave {N[0]}x{N[1]}x{N[2]} with a uniform x-inflow "
+                     f"{dict(zip(names, INFLOW))} and zero-gradient x-outflow, {nsteps} fixed-dt steps (dt = {dt:.4g})",
+           "loss": "sum |B|^2 over cells centred at x < 0.25", "wrt": "start Gas, face fluxes and the inflow state"}
+    grads = {}
+    for name, dtype in (("fp64", torch.float64), ("fp32", torch.float32)):
+        g = Grid(P, geo, dtype=dtype, device="cuda", inflow=INFLOW)
+        act = (G, G + N[0] - 1, G, G + N[1] - 1, G, G + N[2] - 1)
+        mask = (win(g.xyzcc, act)[0].double() < 0.25).to(dtype)
+
+        def lossf(gr, state):
+            return ((win(state["B"], act) ** 2).sum(dim=0) * mask).sum()
+
+        Gas0, mf0 = g.cell_box(G64), g.face_box(F64)
+        loss_and_grad(g, Gas0, mf0, dt, 1, lossf=lossf, params=[g.inflow])  # warm-up
+        (L, gG, gF, (gp,)), el, mem = _timed(lambda: loss_and_grad(g, Gas0, mf0, dt, nsteps, lossf=lossf,
+                                                                    params=[g.inflow]))
+        out[name] = {"loss": L, "fwd_plus_adjoint_s": el, "peak_hbm_gb": mem,
+                     "dloss_dinflow": {names[q]: float(gp[q]) for q in (0, 1, 2, 7)}}
+        grads[name] = gp.double().cpu()
+        if name == "fp64":
+            lossf64 = lossf
+            g64 = g
+    out["fp32_inflow_grad_rel_l2_vs_fp64"] = float((grads["fp32"] - grads["fp64"]).norm() / grads["fp64"].norm())
+    Gas, mf = np.ascontiguousarray(G64), np.ascontiguousarray(F64)
+    with torch.no_grad():
+        B = np.ascontiguousarray(g64.bxyz(g64.face_box(F64))[:, :g64.Nk, :g64.Nj, :g64.Ni].cpu().numpy())
+
+    def cuda_loss(w):
+        gpu.set_inflow(w)
+        gpu.upload_state(Gas, mf, B, Gas, mf, 0.0, -dt, dt, 0)
+        gpu.step_gamera(nsteps)
+        return float(lossf64(g64, {"B": g64.cell_box(gpu.download_state(old=False)["Bxyz"])}))
+
+    base = np.asarray(INFLOW, dtype=np.float64)
+    fd = {}
+    for q in (0, 1, 2, 7):
+        e = np.zeros(8)
+        e[q] = 1e-6 * max(abs(base[q]), 1.0)
+        d = (cuda_loss(base + e) - cuda_loss(base - e)) / (2 * e[q])
+        ad = out["fp64"]["dloss_dinflow"][names[q]]
+        fd[names[q]] = {"central_difference": d, "reverse_mode": ad, "rel_err": abs(d - ad) / abs(ad)}
+    out["fd_check_eps_1e-6"] = fd
+    return out
+
+
 def c5(N=(192, 192, 256), nsteps=200, seg=14, precisions=("fp32", "fp64"), seed=2024):
     w = dipole.wind_code_units()
     xyz = grids.spherical_corners(*N)
@@ -183,12 +256,14 @@ def c5(N=(192, 192, 256), nsteps=200, seg=14, precisions=("fp32", "fp64"), seed=
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("config", choices=["c4", "c5"])
+    ap.add_argument("config", choices=["c4", "c4_inflow", "c5"])
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--precisions", default="fp32,fp64")
     a = ap.parse_args()
     if a.config == "c4":
         res = c4(nsteps=a.steps or 20)
+    elif a.config == "c4_inflow":
+        res = c4_inflow(nsteps=a.steps or 20)
     else:
         res = c5(nsteps=a.steps or 200, precisions=tuple(a.precisions.split(",")))
     print(json.dumps(res), flush=True)

@@ -48,7 +48,8 @@ class DiffParams:
     pFloor: float = 1.0e-12
     up7: bool = False
     # boundary kinds per side (INI, OUTI, INJ, OUTJ, INK, OUTK): 0 periodic,
-    # 1 none, 2 zero-gradient (J), 3 inner sphere (inner I), 4 solar wind (outer I)
+    # 1 none, 2 zero-gradient (J, outer I), 3 inner sphere (inner I), 4 solar
+    # wind (outer I), 6 uniform inflow (inner I)
     bc: tuple = (0, 0, 0, 0, 0, 0)
 
 
@@ -176,7 +177,7 @@ class Grid:
     Fortran-layout geometry arrays)."""
 
     def __init__(self, P: DiffParams, geo: dict, background: dict | None = None, wind=None, dtype=torch.float64,
-                 device="cpu"):
+                 device="cpu", inflow=None):
         self.P = P
         self.Ni, self.Nj, self.Nk = P.Nip + 2 * G, P.Njp + 2 * G, P.Nkp + 2 * G
         self.dtype, self.device = dtype, device
@@ -223,6 +224,12 @@ class Grid:
         # the flux stage and its adjoint as hand-written CUDA kernels (on CUDA
         # tensors, 8CENT); False: the PyTorch expressions and autograd
         self.cuda_flux = torch.device(device).type == "cuda" and not P.up7
+        # the inflow state {rho, P, Vx, Vy, Vz, Bx, By, Bz} of bc[0] = 6: a
+        # tensor, so that a caller may ask for gradients with respect to it
+        self.inflow = None
+        if P.bc[0] == 6:
+            assert inflow is not None, "the inflow boundary needs its state"
+            self.inflow = torch.as_tensor(inflow, dtype=dtype, device=device)
         self.wind = None
         if P.bc[1] == 4:
             assert wind is not None, "the solar-wind boundary needs the wind state"
@@ -579,7 +586,7 @@ def step(g: Grid, cur: dict, old: dict, dt: float, odt: float):
 
     # --- EnforceBCs: inner sphere and solar wind in place, then the gathers
     # (periodic, zero-gradient J), then the final bFlux2Fld
-    if P.bc[0] == 3 or P.bc[1] == 4:
+    if P.bc[0] in (3, 6) or P.bc[1] in (2, 4):
         Gas, mfn = _iside_bcs(g, Gas, mfn, g.bxyz(mfn))
     shp = Gas.shape
     Gas = Gas.reshape(5, -1)[:, g.bc_src[-1]].reshape(shp)
@@ -811,13 +818,41 @@ class _UpdateFn(torch.autograd.Function):
         return (*dst, None, None)
 
 
+def _face_proj(g: Grid, d: int, idx, B):
+    """face * (n . B) on face d at box index idx (zeroGrad_obcI, bcs.F90:842-844)."""
+    t = [g.Tf[q + 9 * d][idx] for q in range(3)]
+    return g.face[d][idx] * (B[0] * t[0] + B[1] * t[1] + B[2] * t[2])
+
+
 def _iside_bcs(g: Grid, Gas, mf, B):
-    """SphIn (bcs.F90:934-957) and the constant-wind WindBC (apps/wind.F90:206-374)
-    on the 4 ghost layers of each I side; B is the Bxyz of the updated state."""
+    """SphIn (bcs.F90:934-957) or the uniform inflow on the inner I side, the
+    constant-wind WindBC (apps/wind.F90:206-374) or zeroGrad_obcI
+    (bcs.F90:820-850) on the outer one, on their 4 ghost layers; B is the Bxyz
+    of the updated state."""
     P = g.P
     Ni, Nj, Nk = g.Ni, g.Nj, g.Nk
     ip = G + P.Nip - 1
     cellsJK = (slice(0, Nk), slice(0, Nj))
+    if P.bc[0] == 6:
+        w = g.inflow
+        gC = cell_p2c(P, [w[0], w[2], w[3], w[4], w[1]])
+        Gas = Gas.clone()
+        mf = mf.clone()
+        for n in range(1, 5):
+            for v in range(5):
+                Gas[v, :Nk, :Nj, G - n] = gC[v]
+            for d in range(3):
+                mf[d, :Nk, :Nj, G - n] = _face_proj(g, d, cellsJK + (G - n,), (w[5], w[6], w[7]))
+    if P.bc[1] == 2:
+        Bc = [B[x][cellsJK + (ip,)] for x in range(3)]
+        gsrc = Gas[:, :Nk, :Nj, ip].clone()
+        Gas = Gas.clone()
+        mf = mf.clone()
+        for n in range(1, 5):
+            Gas[:, :Nk, :Nj, ip + n] = gsrc
+            mf[0, :Nk, :Nj, ip + n + 1] = _face_proj(g, 0, cellsJK + (ip + n + 1,), Bc)
+            for d in (1, 2):
+                mf[d, :Nk, :Nj, ip + n] = _face_proj(g, d, cellsJK + (ip + n,), Bc)
     if P.bc[0] == 3:
         gsrc = Gas[:, :Nk, :Nj, G].clone()
         fsrc = mf[:, :Nk, :Nj, G].clone()
@@ -890,9 +925,11 @@ def loss_b2(g: Grid, state: dict, lo=0.6, hi=0.8):
 
 
 def loss_and_grad(g: Grid, Gas0, mf0, dt: float, nsteps: int, seg: int | None = None, lossf=loss_b2,
-                  per_step: bool = False):
+                  per_step: bool = False, params=None):
     """Loss after nsteps from the start State = oState = (Gas0, mf0, bxyz(mf0))
-    (otime = time - dt) and its gradient w.r.t. Gas0 and mf0.
+    (otime = time - dt) and its gradient w.r.t. Gas0 and mf0; with params (a
+    list of tensors the grid's boundaries use every step, e.g. [g.inflow])
+    also the gradients w.r.t. those, as a fourth result.
 
     Checkpointing: the forward sweep keeps only the (State, oState) pair at the
     start of each segment of seg steps (default ~sqrt(nsteps)); the reverse
@@ -912,6 +949,12 @@ def loss_and_grad(g: Grid, Gas0, mf0, dt: float, nsteps: int, seg: int | None = 
             cur, old = run(g, cur, old, dt, m)
             n += m
         del cur, old
+    params = list(params or [])
+    pleaves = [p.detach().requires_grad_(True) for p in params]
+    swaps = [(k, getattr(g, k)) for k in ("inflow",) if any(getattr(g, k) is p for p in params)]
+    for k, p in swaps:
+        setattr(g, k, pleaves[[id(q) for q in params].index(id(p))])
+    pacc = [torch.zeros_like(p) for p in pleaves]
     lam_cur = lam_old = None
     loss_val = None
     for idx in range(len(ckpt) - 1, -1, -1):
@@ -939,6 +982,7 @@ def loss_and_grad(g: Grid, Gas0, mf0, dt: float, nsteps: int, seg: int | None = 
                 c = {k: v.detach().clone().requires_grad_(True) for k, v in cs.items()}
                 o = {k: v.detach().clone().requires_grad_(True) for k, v in os_.items()}
                 leaves = [c[k] for k in ("Gas", "mf", "B")] + [o[k] for k in ("Gas", "mf", "B")]
+            leaves = leaves + pleaves
             with torch.enable_grad():
                 ce, oe = run(g, c, o, dt, mm)
                 if lam_cur is None:
@@ -952,8 +996,15 @@ def loss_and_grad(g: Grid, Gas0, mf0, dt: float, nsteps: int, seg: int | None = 
                         grads += [lam_cur[k], lam_old[k]]
                 gl = torch.autograd.grad(outs, leaves, grads, allow_unused=True)
             gl = [torch.zeros_like(x) if gv is None else gv for x, gv in zip(leaves, gl)]
+            if pleaves:
+                pacc = [a + b for a, b in zip(pacc, gl[len(gl) - len(pleaves):])]
+                gl = gl[:len(gl) - len(pleaves)]
             del ce, oe, outs, grads, c, o
             if first:
+                for k, p in swaps:
+                    setattr(g, k, p)
+                if params:
+                    return loss_val, gl[0], gl[1], pacc
                 return loss_val, gl[0], gl[1]
             lam_cur = dict(zip(("Gas", "mf", "B"), gl[:3]))
             lam_old = dict(zip(("Gas", "mf", "B"), gl[3:]))

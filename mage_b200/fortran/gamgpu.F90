@@ -11,7 +11,7 @@ module gamgpu
     integer(c_int), parameter :: GAM_OK = 0, GAM_EINVAL = 1, GAM_EBADDIM = 2, GAM_ECUDA = 3, &
                                  GAM_EDT_BAD = 4, GAM_EDT_DISASTER = 5, GAM_ESTATE = 6, GAM_EHOOK = 7
     integer(c_int), parameter :: GAM_BC_PERIODIC = 0, GAM_BC_NONE = 1, GAM_BC_ZEROGRAD = 2, GAM_BC_SPHIN = 3, &
-                                 GAM_BC_WIND = 4, GAM_BC_HALO = 5
+                                 GAM_BC_WIND = 4, GAM_BC_HALO = 5, GAM_BC_INFLOW = 6
     integer(c_int), parameter :: GAM_RECON_8CENT = 0, GAM_RECON_7UP = 1
     integer(c_int), parameter :: GAM_FP64 = 0, GAM_FP32 = 1
 
@@ -109,6 +109,11 @@ module gamgpu
             import :: c_int, c_ptr, c_double
             type(c_ptr), value :: h
             real(c_double), intent(in) :: wind(8)
+        end function
+        integer(c_int) function gam_set_inflow(h, state) bind(C, name="gam_set_inflow")
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: h
+            real(c_double), intent(in) :: state(8)
         end function
         ! k-slab tiling: the MPI driver (gamAppMpi_T) packs/unpacks halos in
         ! device buffers and reduces dt between gam_step_begin and gam_step_end

@@ -22,7 +22,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libgamgpu.so")
 
 GAM_OK, GAM_EINVAL, GAM_EBADDIM, GAM_ECUDA, GAM_EDT_BAD, GAM_EDT_DISASTER, GAM_ESTATE, GAM_EHOOK = range(8)
-BC_PERIODIC, BC_NONE, BC_ZEROGRAD, BC_SPHIN, BC_WIND, BC_HALO = 0, 1, 2, 3, 4, 5
+BC_PERIODIC, BC_NONE, BC_ZEROGRAD, BC_SPHIN, BC_WIND, BC_HALO, BC_INFLOW = 0, 1, 2, 3, 4, 5, 6
 RECON_8CENT, RECON_7UP = 0, 1
 FP64, FP32 = 0, 1
 
@@ -52,7 +52,7 @@ EXPORTED = (
     "gam_set_geometry_arrays", "gam_get_geometry_arrays", "gam_upload_state", "gam_download_state", "gam_step",
     "gam_calc_dt", "gam_divb", "gam_totals", "gam_last_step_ms", "gam_advance_model", "gam_init_orszag_tang",
     "gam_init_blast_wave", "gam_profile_step", "gam_totals_noalloc", "gam_set_background", "gam_get_background",
-    "gam_set_background_dipole", "gam_set_wind", "gam_init_dipole_wind", "gam_write_restart", "gam_read_restart",
+    "gam_set_background_dipole", "gam_set_wind", "gam_set_inflow", "gam_init_dipole_wind", "gam_write_restart", "gam_read_restart",
     "gam_halo_bytes", "gam_halo_pack", "gam_halo_unpack", "gam_init_finish_halo", "gam_set_start", "gam_step_begin",
     "gam_dt_partial", "gam_step_end", "gam_set_slab_edges", "gam_flux_forward", "gam_flux_adjoint",
     "gam_efield_forward", "gam_efield_adjoint", "gam_predict_stage", "gam_update_stage",
@@ -97,6 +97,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     L.gam_get_background.argtypes = [C.c_void_p] + [_dp] * 5
     L.gam_set_background_dipole.argtypes = [C.c_void_p, C.c_double]
     L.gam_set_wind.argtypes = [C.c_void_p, _dp]
+    L.gam_set_inflow.argtypes = [C.c_void_p, _dp]
     L.gam_write_restart.argtypes = [C.c_void_p, C.c_char_p]
     L.gam_halo_bytes.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
     L.gam_set_slab_edges.argtypes = [C.c_void_p, C.c_int32, C.c_int32]
@@ -293,6 +294,12 @@ class GameraGPU:
         w = np.ascontiguousarray(wind, dtype=np.float64)
         assert w.shape == (8,)
         self._check(self.L.gam_set_wind(self.h, _ptr(w)))
+
+    def set_inflow(self, state):
+        """Uniform inner-I inflow {rho, P, Vx, Vy, Vz, Bx, By, Bz} (bc[0] = BC_INFLOW)."""
+        w = np.ascontiguousarray(state, dtype=np.float64)
+        assert w.shape == (8,)
+        self._check(self.L.gam_set_inflow(self.h, _ptr(w)))
 
     def init_dipole_wind(self, wind, seed: int = 31337, amp: float = 0.01):
         """Wind state with a seeded density perturbation and the wind's uniform field."""

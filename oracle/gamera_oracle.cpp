@@ -60,8 +60,9 @@ enum { XNQI = 0, YNQI, XNQJ, YNQJ };
 enum { LEFT = 0, RIGHT = 1 };
 static const int SgnLR[2] = {-1, 1};  // stress.F90:19
 
-// boundary kinds (a subset of bcs.F90 / apps/wind.F90)
-enum { BC_PERIODIC = 0, BC_NONE = 1, BC_ZEROGRAD = 2, BC_SPHIN = 3, BC_WIND = 4 };
+// boundary kinds (a subset of bcs.F90 / apps/wind.F90; BC_INFLOW is a uniform
+// inflow of this library, with no counterpart in the reference)
+enum { BC_PERIODIC = 0, BC_NONE = 1, BC_ZEROGRAD = 2, BC_SPHIN = 3, BC_WIND = 4, BC_INFLOW = 6 };
 
 // interpolation weights, recon.F90:22-23,28-29
 static double interpWgt[8], interpWgt6[8], Up7C[7];
@@ -115,6 +116,7 @@ struct Params {  // mirrored by oracle/oracle.py (ctypes)
     int noMetric;  // 1: allocate the metric with its fill values only (arrays set by the caller)
     double M0;           // dipole moment (code units) of the background field, m = (0,0,M0)
     double wind[8];      // constant solar wind: rho, P, Vx, Vy, Vz, Bx, By, Bz (code units)
+    double inflow[8];    // uniform inner-I inflow state, same order as wind
 };
 
 struct Model {
@@ -124,6 +126,7 @@ struct Model {
     bool fixedTimestep, doMHD, doLFMLim, do25D, doBackground, up7;
     double M0 = 0.0;
     double wind[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    double inflow[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 };
 
 struct Grid {
@@ -939,11 +942,15 @@ static void SphIn(const Grid& G, State& S);
 static void zeroGrad_ibcJ(const Grid& G, State& S);
 static void zeroGrad_obcJ(const Grid& G, State& S);
 static void WindBC(const Model& M, const Grid& G, State& S);
+static void InflowBC(const Model& M, const Grid& G, State& S);
+static void zeroGrad_obcI(const Grid& G, State& S);
 static void EnforceBCs(const Model& M, const Grid& G, State& S) {
     if (G.bc[0] == BC_PERIODIC) periodic_ibcI(G, S);
     else if (G.bc[0] == BC_SPHIN) SphIn(G, S);
+    else if (G.bc[0] == BC_INFLOW) InflowBC(M, G, S);
     if (G.bc[1] == BC_PERIODIC) periodic_obcI(G, S);
     else if (G.bc[1] == BC_WIND) WindBC(M, G, S);
+    else if (G.bc[1] == BC_ZEROGRAD) zeroGrad_obcI(G, S);
     if (G.bc[2] == BC_PERIODIC) periodic_ibcJ(G, S);
     else if (G.bc[2] == BC_ZEROGRAD) zeroGrad_ibcJ(G, S);
     if (G.bc[3] == BC_PERIODIC) periodic_obcJ(G, S);
@@ -1564,6 +1571,53 @@ static void zeroGrad_obcJ(const Grid& G, State& S) {
                 S.magFlux(i, G.je + n + 1, k, JDIR) = S.magFlux(i, G.je + 1, k, JDIR);
             }
 }
+// bcs.F90:820-850 zeroGrad_obcI: gas copied from the last active cell, ghost
+// face fluxes from that cell's field projected on each face (Bxyz untouched)
+static void zeroGrad_obcI(const Grid& G, State& S) {
+    for (int k = G.ksg; k <= G.keg; k++)
+        for (int j = G.jsg; j <= G.jeg; j++) {
+            double B[3];
+            gamCellBxyz(G, S.magFlux, G.ie, j, k, B);
+            for (int n = 1; n <= 4; n++) {
+                const int ig = G.ie + n;
+                for (int v = 0; v < NVAR; v++) S.Gas(ig, j, k, v) = S.Gas(G.ie, j, k, v);
+                for (int d = 0; d < 3; d++) {
+                    const int fi = d == IDIR ? ig + 1 : ig;
+                    double nH[3] = {G.Tf(fi, j, k, NORMX + 9 * d), G.Tf(fi, j, k, NORMY + 9 * d),
+                                    G.Tf(fi, j, k, NORMZ + 9 * d)};
+                    S.magFlux(fi, j, k, d) = G.face(fi, j, k, d) * dot3(B, nH);
+                }
+            }
+        }
+}
+// Uniform inflow through the inner I side (a boundary of this library, shaped
+// like zeroGrad_obcI): every ghost cell gets the state {rho, P, V, B}, its
+// I face (is-n) and J, K faces the flux face * (n . B), and its Bxyz the
+// gamCellBxyz of those fluxes (as WindBC does for its ghosts).
+static void InflowBC(const Model& M, const Grid& G, State& S) {
+    const double* w = M.inflow;  // rho, P, V(3), B(3)
+    const double Bin[3] = {w[5], w[6], w[7]};
+    double gW[5] = {w[0], w[2], w[3], w[4], w[1]}, gCon[5];
+    CellP2C(M, gW, gCon);
+    for (int k = G.ksg; k <= G.keg; k++)
+        for (int j = G.jsg; j <= G.jeg; j++)
+            for (int n = 1; n <= 4; n++) {
+                const int ig = G.is - n;
+                for (int v = 0; v < NVAR; v++) S.Gas(ig, j, k, v) = gCon[v];
+                for (int d = 0; d < 3; d++) {
+                    double nH[3] = {G.Tf(ig, j, k, NORMX + 9 * d), G.Tf(ig, j, k, NORMY + 9 * d),
+                                    G.Tf(ig, j, k, NORMZ + 9 * d)};
+                    S.magFlux(ig, j, k, d) = G.face(ig, j, k, d) * dot3(Bin, nH);
+                }
+            }
+    for (int k = G.ksg; k <= G.keg; k++)
+        for (int j = G.jsg; j <= G.jeg; j++)
+            for (int n = 1; n <= 4; n++) {
+                double B[3];
+                gamCellBxyz(G, S.magFlux, G.is - n, j, k, B);
+                for (int x = 0; x < 3; x++) S.Bxyz(G.is - n, j, k, x) = B[x];
+            }
+}
 // math.F90:332-343 normVec
 static inline void normVec(const double* a, double* out) {
     double nA = std::sqrt(dot3(a, a));
@@ -1729,6 +1783,7 @@ void* orc_create(const Params* p, const double* xyz) {
     M.doBackground = p->doBackground != 0; M.up7 = p->up7 != 0;
     M.M0 = p->M0;
     for (int n = 0; n < 8; n++) M.wind[n] = p->wind[n];
+    for (int n = 0; n < 8; n++) M.inflow[n] = p->inflow[n];
     g_up7 = M.up7;
     pdmb = p->pdmb; dFloor = p->dFloor; pFloor = p->pFloor;
     G.Nip = p->Nip; G.Njp = p->Njp; G.Nkp = p->Nkp;

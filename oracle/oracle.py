@@ -25,6 +25,7 @@ BC_NONE = 1
 BC_ZEROGRAD = 2
 BC_SPHIN = 3
 BC_WIND = 4
+BC_INFLOW = 6
 
 
 def build(quiet: bool = True) -> None:
@@ -42,6 +43,7 @@ class _Params(C.Structure):
         ("cHogH", C.c_double), ("cHogM", C.c_double), ("dFloor", C.c_double), ("pFloor", C.c_double),
         ("tFin", C.c_double), ("dt0", C.c_double), ("limDT0", C.c_double), ("fixedDT", C.c_double),
         ("bc", C.c_int * 6), ("noMetric", C.c_int), ("M0", C.c_double), ("wind", C.c_double * 8),
+        ("inflow", C.c_double * 8),
     ]
 
 
@@ -78,14 +80,15 @@ class OracleParams:
     noMetric: bool = False
     M0: float = 0.0
     wind: tuple = (0.0,) * 8
+    inflow: tuple = (0.0,) * 8
 
     def to_c(self) -> _Params:
         p = _Params()
         for f, _ in _Params._fields_:
             if f == "bc":
                 p.bc[:] = list(self.bc)
-            elif f == "wind":
-                p.wind[:] = list(self.wind)
+            elif f in ("wind", "inflow"):
+                getattr(p, f)[:] = list(getattr(self, f))
             else:
                 setattr(p, f, getattr(self, f))
         return p
