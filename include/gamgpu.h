@@ -68,6 +68,10 @@ typedef struct gam_params {
     int32_t precision;      /* GAM_FP64 (drop-in) or GAM_FP32 (bulk FP32)    */
     int32_t strict;         /* 1: kernels without FMA contraction            */
     int32_t bc[6];          /* INI, OUTI, INJ, OUTJ, INK, OUTK: GAM_BC_*     */
+    int32_t doBoris;        /* physics/doBoris (init.F90:417-423): Boris-limited
+                               Alfven speed, Boris hogs and the nuclear option in
+                               the fluxes, CellBoris in the update */
+    double Ca;              /* physics/Ca, the Boris speed of light (code units) */
 } gam_params;
 
 typedef struct gam_handle gam_handle;

@@ -761,9 +761,9 @@ int flux_call(const gam_params* p, const void* QW, const void* Wn, const void* Q
     };
     const R* Bl = (const R*)Blim;
     if (!dgF) {
-        k_stress<R, 0, 1><<<grid(fr[0]), blk, 0, s>>>(b, P, g, Bl, w, fr[0], sc);
-        k_stress<R, 1, 1><<<grid(fr[1]), blk, 0, s>>>(b, P, g, Bl, w, fr[1], sc);
-        k_stress<R, 2, 1><<<grid(fr[2]), blk, 0, s>>>(b, P, g, Bl, w, fr[2], sc);
+        k_stress<R, 0, 1><<<grid(fr[0]), blk, 0, s>>>(b, P, g, Bl, w, fr[0], sc, nullptr, nullptr);
+        k_stress<R, 1, 1><<<grid(fr[1]), blk, 0, s>>>(b, P, g, Bl, w, fr[1], sc, nullptr, nullptr);
+        k_stress<R, 2, 1><<<grid(fr[2]), blk, 0, s>>>(b, P, g, Bl, w, fr[2], sc, nullptr, nullptr);
     } else {
         const R* a = (const R*)dgF;
         const R* m = (const R*)dmF;
@@ -779,6 +779,7 @@ int flux_call(const gam_params* p, const void* QW, const void* Wn, const void* Q
 int check(const gam_params* p, int32_t fp32) {
     if (!p) return GAM_EINVAL;
     if (p->rmeth != GAM_RECON_8CENT) return GAM_EINVAL;  // the adjoint covers 8CENT
+    if (p->doBoris) return GAM_EINVAL;                   // and the step without the Boris correction
     if (p->nG != 4 || p->Nip < 1 || p->Njp < 1 || p->Nkp < 1 || p->do25D) return GAM_EBADDIM;
     (void)fp32;
     return GAM_OK;

@@ -132,6 +132,8 @@ extern "C" int gam_default_params(gam_params* p, int32_t Nip, int32_t Njp, int32
     p->rmeth = GAM_RECON_8CENT; p->doLFMLim = 1; p->doMHD = 1; p->doBackground = 0; p->do25D = (Nkp == 1);
     p->precision = GAM_FP64; p->strict = 0;
     for (int n = 0; n < 6; n++) p->bc[n] = GAM_BC_PERIODIC;
+    p->doBoris = 0;
+    p->Ca = 1.0e12;  // HUGE (kdefs.F90:20), the reference's Ca without Boris
     return GAM_OK;
 }
 
@@ -142,6 +144,9 @@ template <class R> static void fill_dev_params(DevParams<R>& P, const gam_params
     P.pdmb = (R)p.pdmb;
     P.Vd0 = (R)p.Vd0;
     P.cHogH = (R)p.cHogH;
+    P.cHogM = (R)p.cHogM;
+    P.doBoris = p.doBoris;
+    P.Ca = p.Ca;
     P.dFloor = (R)p.dFloor;
     P.pFloor = (R)p.pFloor;
     P.doMHD = p.doMHD; P.doLFMLim = p.doLFMLim; P.do25D = p.do25D; P.doBackground = p.doBackground;
@@ -234,6 +239,7 @@ extern "C" int gam_create(const gam_params* p, gam_handle** out) {
     if (p->do25D && (p->bc[4] != GAM_BC_PERIODIC || p->bc[5] != GAM_BC_PERIODIC))
         return bad(GAM_EINVAL, "do25D replicates k: the k boundaries must be periodic");
     if (p->doBackground && !p->doMHD) return bad(GAM_EINVAL, "a background field needs doMHD");
+    if (p->doBoris && !(p->Ca > 0.0)) return bad(GAM_EINVAL, "doBoris needs Ca > 0");
     h->b = gam_make_box(p->Nip, p->Njp, p->Nkp);
     h->f32 = p->precision == GAM_FP32;
     if (cudaStreamCreateWithFlags(&h->s, cudaStreamNonBlocking) != cudaSuccess) return bad(GAM_ECUDA, "no CUDA device");

@@ -206,6 +206,50 @@ __device__ __forceinline__ void cell_p2c(const DevParams<R>& P, const R* W, R* U
     U[4] = IntE + KinE;
 }
 
+// norm2 as gfortran evaluates it (scaled sum of squares)
+__device__ __forceinline__ double norm2s3(const double* a) {
+    double scale = 1.0, res = 0.0;
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+        if (a[q] != 0.0) {
+            double ax = fabs(a[q]);
+            if (scale < ax) {
+                double val = scale / ax;
+                res = 1.0 + res * val * val;
+                scale = ax;
+            } else {
+                double val = ax / scale;
+                res += val * val;
+            }
+        }
+    }
+    return scale * sqrt(res);
+}
+// sqrt(2.0) of the nuclear option's interface speed (stress.F90:405): a
+// default-real constant in the reference, which gfortran folds to this float
+#define GAM_SQRT2_R4 ((double)1.41421354f)
+
+// PredictCell (mhdgroup.F90:528-562, AB2, single fluid): the half-step
+// conserved state from State n (Q) and n-1 (oQ)
+template <class R>
+__device__ __forceinline__ void predict_cell(const DevParams<R>& P, const R* Q, const R* oQ, R pdt, R odt, R* pQ) {
+    R W[5], oW[5], pW[5];
+    cell_c2p(P, oQ, oW);
+    cell_c2p(P, Q, W);
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+        R dQ = (W[v] - oW[v]) / odt;
+        pW[v] = W[v] + pdt * dQ;
+    }
+    pW[0] = rmax(pW[0], P.dFloor);
+    pW[4] = rmax(pW[4], P.pFloor);
+    cell_p2c(P, pW, pQ);
+}
+
+// Boris-limited speed Ca v / sqrt(Ca^2 + v^2) (fields.F90:211-213,
+// gridutils.F90:91-93, gamutils.F90:356-358)
+template <class T> __device__ __forceinline__ T boris_speed(T Ca, T v) { return Ca * v / sqrt(Ca * Ca + v * v); }
+
 // gamCellBxyz (gridutils.F90:648-680) from the six face fluxes of cell c
 template <class R>
 __device__ __forceinline__ void cell_bxyz(const GamBox& b, const Geo<R>& g, long c, R fI, R fIp, R fJ, R fJp, R fK,
@@ -303,18 +347,8 @@ __global__ void __launch_bounds__(256, MINB) k_predict(GamBox b, DevParams<R> P,
         }
     }
     if (!isCell) return;
-    // PredictCell (mhdgroup.F90:528-562)
-    R W[5], oW[5], pW[5], pQ[5];
-    cell_c2p(P, oQ, oW);
-    cell_c2p(P, Q, W);
-#pragma unroll
-    for (int v = 0; v < 5; v++) {
-        R dQ = (W[v] - oW[v]) / odt;
-        pW[v] = W[v] + pdt * dQ;
-    }
-    pW[0] = rmax(pW[0], P.dFloor);
-    pW[4] = rmax(pW[4], P.pFloor);
-    cell_p2c(P, pW, pQ);
+    R pQ[5];
+    predict_cell(P, Q, oQ, pdt, odt, pQ);
     R Wh[5], Wn[5];
     block_c2p(P, pQ, Wh);
     if (P.doLFMLim) block_c2p(P, Q, Wn);
@@ -454,6 +488,7 @@ __global__ void __launch_bounds__(128, MINB) k_vxb(GamBox b, DevParams<R> P, Geo
         b2 = b2 + (R)g.edgB0[(1 + 2 * eD) * fs + c];
     }
     R vA = Mth<R>::sqrt_(b1 * b1 + b2 * b2) / Mth<R>::sqrt_(Dc);
+    if (P.doBoris) vA = boris_speed((R)P.Ca, vA);
     vDiff = vDiff + vA;
     const R edge = g.edge[eD * fs + c];
     vDiff = rmin(vDiff, P.CFL * edge / (R)sc->dt);
@@ -462,8 +497,8 @@ __global__ void __launch_bounds__(128, MINB) k_vxb(GamBox b, DevParams<R> P, Geo
 }
 
 // One-sided Gaussian-moment fluxes for one side q (sgn = -1 LEFT, +1 RIGHT).
-// MagKinFlux (stress.F90:513-599), Boris off.
-template <class R>
+// MagKinFlux (stress.F90:513-599).
+template <class R, bool BORIS = false>
 __device__ __forceinline__ void mag_kin_flux(const DevParams<R>& P, R sgn, const R* W, const R* Bm, R Bn,
                                              const R* T, const double* B0, double B0n, R* mF, R& bbD, R& VaD) {
     R D = W[0], Pr = W[4];
@@ -481,6 +516,10 @@ __device__ __forceinline__ void mag_kin_flux(const DevParams<R>& P, R sgn, const
         bbD = bbD + (R)0.5 * (Bx * Bx + By * By + Bz * Bz);
     }
     R Vac2 = Va2;
+    if constexpr (BORIS) {  // Boris-corrected Va^2
+        const R Ca = (R)P.Ca;
+        Vac2 = Va2 / ((R)1 + (Va2 / (Ca * Ca)));
+    }
     R Nx = T[0], Ny = T[1], Nz = T[2];
     R Vn = Nx * W[1] + Ny * W[2] + Nz * W[3];
     R lambda = (R)1 / ((R)2 * Pr / D + Vac2);
@@ -530,9 +569,10 @@ __device__ __forceinline__ void gas_kin_flux(const DevParams<R>& P, R sgn, const
 // thread. The stencil operands are the per-cell products volume*primitive and
 // volume*B of the half state (QdV of Cen8LRs) and the limiter values, read
 // along D through L1; MINB bounds the registers for occupancy.
-template <class R, int D, int MINB>
+template <class R, int D, int MINB, bool BORIS = false>
 __global__ void __launch_bounds__(128, MINB) k_stress(GamBox b, DevParams<R> P, Geo<R> g, const R* __restrict__ Blim,
-                                                      Work<R> w, Range r, const GamScalars* sc) {
+                                                      Work<R> w, Range r, const GamScalars* sc,
+                                                      const R* __restrict__ gasN, const R* __restrict__ gasO) {
     if (sc->halted) return;
     int ii, jj, kk;
     if (!thread_ijk(r, ii, jj, kk)) return;
@@ -584,19 +624,53 @@ __global__ void __launch_bounds__(128, MINB) k_stress(GamBox b, DevParams<R> P, 
     R VaD = (R)0, bbD = (R)0;
     if (P.doMHD) {
         R mF[3] = {(R)0, (R)0, (R)0};
-        mag_kin_flux(P, (R)-1, WL, MagL, Bn, T, B0, B0n, mF, bbD, VaD);
-        mag_kin_flux(P, (R)1, WR, MagR, Bn, T, B0, B0n, mF, bbD, VaD);
+        mag_kin_flux<R, BORIS>(P, (R)-1, WL, MagL, Bn, T, B0, B0n, mF, bbD, VaD);
+        mag_kin_flux<R, BORIS>(P, (R)1, WR, MagR, Bn, T, B0, B0n, mF, bbD, VaD);
+        if constexpr (BORIS) {  // Boris hogs on the magnetic fluxes (stress.F90:335-349)
+            const R Ca = (R)P.Ca;
+#pragma unroll
+            for (int x = 0; x < 3; x++) {
+                R deeV = WR[1 + x] - WL[1 + x];
+                R deeP = bbD * deeV / (Ca * Ca);
+                mF[x] = mF[x] - P.cHogM * VaD * deeP;
+            }
+        }
 #pragma unroll
         for (int x = 0; x < 3; x++) w.mF[(x + 3 * D) * fs + c] = fa * mF[x];
     }
     R gF[5] = {(R)0, (R)0, (R)0, (R)0, (R)0}, dW[5] = {(R)0, (R)0, (R)0, (R)0, (R)0};
     gas_kin_flux(P, (R)-1, WL, T, gF, dW);
     gas_kin_flux(P, (R)1, WR, T, gF, dW);
+    R gv[5];
 #pragma unroll
-    for (int v = 0; v < 5; v++) {
-        R gv = gF[v] - (R)1 * P.cHogH * VaD * dW[v];
-        w.gF[(v + 5 * D) * fs + c] = fa * gv;
+    for (int v = 0; v < 5; v++) gv[v] = gF[v] - (R)1 * P.cHogH * VaD * dW[v];
+    if constexpr (BORIS) {
+        // the nuclear option (stress.F90:399-417, cLim = 1.5): where the mean
+        // interface speed reaches cLim Ca, diffuse with speed Ca on the jump of
+        // the half-step conserved state between the face's two cells, which is
+        // recomputed here (the predictor keeps primitives only)
+        double vl[3] = {(double)WL[1], (double)WL[2], (double)WL[3]}, vr[3] = {(double)WR[1], (double)WR[2], (double)WR[3]};
+        const R vL = (R)norm2s3(vl), vR = (R)norm2s3(vr);
+        const R Vn = Mth<R>::sqrt_(vL * vL + vR * vR) / (R)GAM_SQRT2_R4;
+        const R Ca = (R)P.Ca;
+        if (Vn >= (R)1.5 * Ca) {
+            R Ql[5], oQl[5], Qr[5], oQr[5], pQl[5], pQr[5];
+#pragma unroll
+            for (int v = 0; v < 5; v++) {
+                Ql[v] = gasN[v * fs + c - s];
+                oQl[v] = gasO[v * fs + c - s];
+                Qr[v] = gasN[v * fs + c];
+                oQr[v] = gasO[v * fs + c];
+            }
+            const R pdt = (R)sc->pdt, odt = (R)sc->odt;
+            predict_cell(P, Ql, oQl, pdt, odt, pQl);
+            predict_cell(P, Qr, oQr, pdt, odt, pQr);
+#pragma unroll
+            for (int v = 0; v < 5; v++) gv[v] = gv[v] - Ca * (pQr[v] - pQl[v]);
+        }
     }
+#pragma unroll
+    for (int v = 0; v < 5; v++) w.gF[(v + 5 * D) * fs + c] = fa * gv[v];
 }
 
 // E2Flux into the new buffer; faces outside its range are copied.
@@ -630,7 +704,7 @@ __global__ void __launch_bounds__(256) k_update_faces(GamBox b, DevParams<R> P, 
 __device__ __forceinline__ unsigned long long dbits(double x) { return (unsigned long long)__double_as_longlong(x); }
 
 // CellDT (gridutils.F90:49-106), evaluated in FP64
-template <class R>
+template <class R, bool BORIS>
 __device__ __forceinline__ double cell_dt(const DevParams<R>& P, const double* U, const double* Bt, double dl,
                                           double gamma, double gm1, double CFL) {
     double rho = U[0];
@@ -644,14 +718,64 @@ __device__ __forceinline__ double cell_dt(const DevParams<R>& P, const double* U
     if (P.doMHD) {
         double MagB = sqrt(Bt[0] * Bt[0] + Bt[1] * Bt[1] + Bt[2] * Bt[2]);
         Valf = MagB / sqrt(rho);
+        if constexpr (BORIS) Valf = boris_speed(P.Ca, Valf);
     }
     double vCFL = MagV + sqrt(Cs * Cs + Valf * Valf) + 0.0;
     return CFL * dl / vCFL;
 }
 
+// CellBoris (mhdgroup.F90:334-382, single fluid): U2 the hydro-updated state
+// (in place), U0 State n, B2 and B0 the total fields at n+1 and n
+template <class R>
+__device__ __forceinline__ void cell_boris(const DevParams<R>& P, R* U2, const R* U0, const R* B2, const R* B0,
+                                           const R* dGasH, const R* dGasM, R Ca, R dt) {
+    R W2[5];
+    cell_c2p(P, U2, W2);
+    const R D2 = rmax(W2[0], P.dFloor);
+    const R P2 = rmax(W2[4], P.pFloor);
+    const R D0 = rmax(U0[0], P.dFloor);
+    R V0[3], B1[3], dPGas[3], dPMag[3], bhat1[3], dMom[3];
+#pragma unroll
+    for (int x = 0; x < 3; x++) {
+        V0[x] = U0[1 + x] / D0;
+        B1[x] = (R)0.5 * (B2[x] + B0[x]);
+    }
+    const R alpha = (B1[0] * B1[0] + B1[1] * B1[1] + B1[2] * B1[2]) / (D2 * Ca * Ca);
+    const R dRho = dt * dGasH[0];
+#pragma unroll
+    for (int x = 0; x < 3; x++) {
+        dPGas[x] = dt * dGasH[1 + x];
+        dPMag[x] = dt * dGasM[x];
+    }
+    const R pCon = (R)1 / ((R)1 + alpha);
+    // normVec (math.F90:332-343)
+    const R nA = Mth<R>::sqrt_(B1[0] * B1[0] + B1[1] * B1[1] + B1[2] * B1[2]);
+#pragma unroll
+    for (int x = 0; x < 3; x++) bhat1[x] = nA <= (R)TINY ? (R)0 : B1[x] / nA;
+    if (alpha > (R)TINY) {
+        R sum[3];
+#pragma unroll
+        for (int x = 0; x < 3; x++) sum[x] = dPGas[x] + dPMag[x];
+        const R pg = dPGas[0] * bhat1[0] + dPGas[1] * bhat1[1] + dPGas[2] * bhat1[2];
+        const R ps = sum[0] * bhat1[0] + sum[1] * bhat1[1] + sum[2] * bhat1[2];
+        const R pv = V0[0] * bhat1[0] + V0[1] * bhat1[1] + V0[2] * bhat1[2];
+#pragma unroll
+        for (int x = 0; x < 3; x++)
+            dMom[x] = pg * bhat1[x] + pCon * (sum[x] - ps * bhat1[x]) + alpha * pCon * dRho * (V0[x] - pv * bhat1[x]);
+    } else {
+#pragma unroll
+        for (int x = 0; x < 3; x++) dMom[x] = dPGas[x] + dPMag[x];
+    }
+    W2[0] = D2;
+#pragma unroll
+    for (int x = 0; x < 3; x++) W2[1 + x] = (D0 * V0[x] + dMom[x]) / D2;
+    W2[4] = P2;
+    cell_p2c(P, W2, U2);
+}
+
 // Flux2Deltas + CellReynolds + bFlux2Fld + CellMaxwell for active cells,
 // copy + bFlux2Fld for ghost cells, then the CFL dt of cells in the dt range.
-template <class R, int MINB>
+template <class R, int MINB, bool BORIS = false>
 __global__ void __launch_bounds__(128, MINB) k_update_cells(GamBox b, DevParams<R> P, Geo<R> g, StateBuf<R> cur,
                                                       StateBuf<R> nxt, Work<R> w, GamScalars* sc, double gamma_d,
                                                       double gm1_d) {
@@ -678,13 +802,14 @@ __global__ void __launch_bounds__(128, MINB) k_update_cells(GamBox b, DevParams<
         if (active) {
             const long sj = b.sx, sk = b.sk;
             const R dV = g.vol[c];
+            R dGasH[5];
 #pragma unroll
             for (int v = 0; v < 5; v++) {
                 const R* gI = w.gF + (v + 0) * fs;
                 const R* gJ = w.gF + (v + 5) * fs;
                 const R* gK = w.gF + (v + 10) * fs;
-                R dGasH = (gI[c] - gI[c + 1] + gJ[c] - gJ[c + sj] + gK[c] - gK[c + sk]) / dV;
-                U[v] = cur.Gas[v * fs + c] + dt * dGasH;
+                dGasH[v] = (gI[c] - gI[c + 1] + gJ[c] - gJ[c + sj] + gK[c] - gK[c + sk]) / dV;
+                U[v] = cur.Gas[v * fs + c] + dt * dGasH[v];
             }
             if (P.doMHD) {
                 R dGasM[3];
@@ -696,6 +821,22 @@ __global__ void __launch_bounds__(128, MINB) k_update_cells(GamBox b, DevParams<
                     dGasM[x] = (mI[c] - mI[c + 1] + mJ[c] - mJ[c + sj] + mK[c] - mK[c + sk]) / dV;
                     if (P.doBackground) dGasM[x] = dGasM[x] + (R)g.dpB0[x * fs + c];
                 }
+                if constexpr (BORIS) {
+                    R U0[5], B2[3], B0[3];
+#pragma unroll
+                    for (int v = 0; v < 5; v++) U0[v] = cur.Gas[v * fs + c];
+#pragma unroll
+                    for (int x = 0; x < 3; x++) {
+                        B2[x] = Bc[x];
+                        B0[x] = cur.B[x * fs + c];
+                        if (P.doBackground) {
+                            const R b0 = (R)g.B0[x * fs + c];
+                            B2[x] = B2[x] + b0;
+                            B0[x] = B0[x] + b0;
+                        }
+                    }
+                    cell_boris(P, U, U0, B2, B0, dGasH, dGasM, (R)P.Ca, dt);
+                } else {
                 // CellMaxwell (mhdgroup.F90:299-329)
                 R D = rmax(U[0], P.dFloor);
                 R Mx = U[1], My = U[2], Mz = U[3], TotE = U[4];
@@ -710,6 +851,7 @@ __global__ void __launch_bounds__(128, MINB) k_update_cells(GamBox b, DevParams<
                 U[2] = My;
                 U[3] = Mz;
                 U[4] = KinE + Pr / P.gm1;
+                }
             }
         } else {
 #pragma unroll
@@ -728,7 +870,7 @@ __global__ void __launch_bounds__(128, MINB) k_update_cells(GamBox b, DevParams<
                 Bt[x] = (double)Bc[x];
                 if (P.doBackground) Bt[x] = Bt[x] + g.B0[x * fs + c];
             }
-            double dtc = cell_dt(P, Ud, Bt, (double)g.dl[c], gamma_d, gm1_d, sc->CFL);
+            double dtc = cell_dt<R, BORIS>(P, Ud, Bt, (double)g.dl[c], gamma_d, gm1_d, sc->CFL);
             if (dtc > 0.0 && dtc < 1.0e300) mydt = dtc;  // finite positive
             else bad = true;
         }
@@ -845,25 +987,6 @@ __device__ __forceinline__ void bc_source(const GamBox& b, const DevParams<R>& P
     }
 }
 
-// norm2 as gfortran evaluates it (scaled sum of squares)
-__device__ __forceinline__ double norm2s3(const double* a) {
-    double scale = 1.0, res = 0.0;
-#pragma unroll
-    for (int q = 0; q < 3; q++) {
-        if (a[q] != 0.0) {
-            double ax = fabs(a[q]);
-            if (scale < ax) {
-                double val = scale / ax;
-                res = 1.0 + res * val * val;
-                scale = ax;
-            } else {
-                double val = ax / scale;
-                res += val * val;
-            }
-        }
-    }
-    return scale * sqrt(res);
-}
 
 // face * (n . B) on face d of box cell c (zeroGrad_obcI, bcs.F90:842-844)
 template <class R>
@@ -954,6 +1077,7 @@ __global__ void __launch_bounds__(256) k_bc_iside(GamBox b, DevParams<R> P, Geo<
             double Bd[3] = {(double)Bin[0], (double)Bin[1], (double)Bin[2]};
             R MagB = (R)norm2s3(Bd);
             R Va = MagB / Mth<R>::sqrt_(gCon[0]);
+            if (P.doBoris) Va = boris_speed((R)P.Ca, Va);
             R Cx = Mth<R>::sqrt_(Cs * Cs + Va * Va);
             const long cf = lidx(b, ip + 1, jj, kk);
             R nH[3] = {g.Tf[0 * fs + cf], g.Tf[1 * fs + cf], g.Tf[2 * fs + cf]};
@@ -1165,7 +1289,8 @@ __global__ void __launch_bounds__(128) k_dt_only(GamBox b, DevParams<R> P, Geo<R
                 if (P.doBackground) Bt[x] = Bt[x] + g.B0[x * fs + c];
             }
         }
-        double dtc = cell_dt(P, Ud, Bt, (double)g.dl[c], gamma_d, gm1_d, sc->CFL);
+        double dtc = P.doBoris ? cell_dt<R, true>(P, Ud, Bt, (double)g.dl[c], gamma_d, gm1_d, sc->CFL)
+                                : cell_dt<R, false>(P, Ud, Bt, (double)g.dl[c], gamma_d, gm1_d, sc->CFL);
         if (dtc > 0.0 && dtc < 1.0e300) mydt = dtc;
     }
     for (int o = 16; o > 0; o >>= 1) mydt = fmin(mydt, __shfl_xor_sync(0xffffffffu, mydt, o));
@@ -1241,11 +1366,16 @@ template <class R, class F> void for_each_kernel(const Ctx<R>& C, int cur, cudaS
     auto stress = [&](auto Dc) {
         constexpr int D = decltype(Dc)::value;
         const Range& r = fr[D];
+        if (C.P.doBoris) {
+            k_stress<R, D, sizeof(R) == 4 ? 8 : 6, true><<<grid_for(r, sblk), sblk, 0, s>>>(b, C.P, C.g, Blim, C.w, r, C.sc,
+                                                                                        S.Gas, O.Gas);
+            return;
+        }
         switch (C.kvar & 3) {
-            case 1: k_stress<R, D, 1><<<grid_for(r, sblk), sblk, 0, s>>>(b, C.P, C.g, Blim, C.w, r, C.sc); break;
-            case 2: k_stress<R, D, 7><<<grid_for(r, sblk), sblk, 0, s>>>(b, C.P, C.g, Blim, C.w, r, C.sc); break;
-            case 3: k_stress<R, D, 8><<<grid_for(r, sblk), sblk, 0, s>>>(b, C.P, C.g, Blim, C.w, r, C.sc); break;
-            default: k_stress<R, D, sizeof(R) == 4 ? 8 : 6><<<grid_for(r, sblk), sblk, 0, s>>>(b, C.P, C.g, Blim, C.w, r, C.sc); break;
+            case 1: k_stress<R, D, 1><<<grid_for(r, sblk), sblk, 0, s>>>(b, C.P, C.g, Blim, C.w, r, C.sc, S.Gas, O.Gas); break;
+            case 2: k_stress<R, D, 7><<<grid_for(r, sblk), sblk, 0, s>>>(b, C.P, C.g, Blim, C.w, r, C.sc, S.Gas, O.Gas); break;
+            case 3: k_stress<R, D, 8><<<grid_for(r, sblk), sblk, 0, s>>>(b, C.P, C.g, Blim, C.w, r, C.sc, S.Gas, O.Gas); break;
+            default: k_stress<R, D, sizeof(R) == 4 ? 8 : 6><<<grid_for(r, sblk), sblk, 0, s>>>(b, C.P, C.g, Blim, C.w, r, C.sc, S.Gas, O.Gas); break;
         }
     };
     f(8, [&] { stress(std::integral_constant<int, 0>()); });
@@ -1253,7 +1383,9 @@ template <class R, class F> void for_each_kernel(const Ctx<R>& C, int cur, cudaS
     if (!C.P.do25D) f(10, [&] { stress(std::integral_constant<int, 2>()); });
     f(11, [&] { k_update_faces<R><<<grid_for(all, blk), blk, 0, s>>>(b, C.P, S, O, C.w, C.sc); });
     f(12, [&] {
-        if (C.kvar & 4)
+        if (C.P.doBoris)
+            k_update_cells<R, sizeof(R) == 8 ? 6 : 8, true><<<grid_for(cells, blk), blk, 0, s>>>(b, C.P, C.g, S, O, C.w, C.sc, C.gamma, C.gm1);
+        else if (C.kvar & 4)
             k_update_cells<R, 1><<<grid_for(cells, blk), blk, 0, s>>>(b, C.P, C.g, S, O, C.w, C.sc, C.gamma, C.gm1);
         else
             k_update_cells<R, 8><<<grid_for(cells, blk), blk, 0, s>>>(b, C.P, C.g, S, O, C.w, C.sc, C.gamma, C.gm1);

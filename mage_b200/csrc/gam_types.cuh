@@ -17,8 +17,10 @@ struct WindData {
 };
 
 template <class R> struct DevParams {
-    R gamma, gm1, CFL, pdmb, Vd0, cHogH, dFloor, pFloor;
+    R gamma, gm1, CFL, pdmb, Vd0, cHogH, cHogM, dFloor, pFloor;
     int doMHD, doLFMLim, do25D, doBackground, up7;
+    int doBoris;  // Boris correction with the speed of light Ca (init.F90:417-423)
+    double Ca;
     int bc[6];
     // CalcDT covers the ghost layer below / above the active k range (1, the
     // reference's isDT..ieDT); a k-slab drops it where a neighbour's cells lie

@@ -21,6 +21,8 @@ module gamgpu
         real(c_double) :: tFin, dt0, limDT0, fixedTimestep
         integer(c_int32_t) :: rmeth, doLFMLim, doMHD, doBackground, do25D, precision, strict
         integer(c_int32_t) :: bc(6)
+        integer(c_int32_t) :: doBoris
+        real(c_double) :: Ca
     end type gam_params
 
     interface

@@ -44,6 +44,7 @@ class _Params(C.Structure):
         ("tFin", C.c_double), ("dt0", C.c_double), ("limDT0", C.c_double), ("fixedTimestep", C.c_double),
         ("rmeth", C.c_int32), ("doLFMLim", C.c_int32), ("doMHD", C.c_int32), ("doBackground", C.c_int32),
         ("do25D", C.c_int32), ("precision", C.c_int32), ("strict", C.c_int32), ("bc", C.c_int32 * 6),
+        ("doBoris", C.c_int32), ("Ca", C.c_double),
     ]
 
 
@@ -157,6 +158,8 @@ class GamParams:
     precision: int = FP64
     strict: bool = False
     bc: tuple = field(default_factory=lambda: (BC_PERIODIC,) * 6)
+    doBoris: bool = False
+    Ca: float = 1.0e12
 
     def to_c(self) -> _Params:
         p = _Params()

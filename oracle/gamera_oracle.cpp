@@ -51,6 +51,11 @@ namespace orc {
 static const double TINY = 1.0e-12, HUGE_ = 1.0e12;
 static const double PI = 3.141592653589793;  // 4*atan(1) in double
 enum { NVAR = 5, NDIM = 3, recLen = 8, limLen = 4, vecLen = 16, Nr2 = 4, Nl2 = 2 };
+// stress.F90:20-25: the nuclear option's threshold cLim, and sqrt(2.0) of its
+// interface speed: a default-real (single precision) constant in the
+// reference, which gfortran folds to the float 1.41421354
+static const double cLim = 1.5;
+static const double SQRT2_R4 = (double)1.41421354f;
 enum { DEN = 0, MOMX = 1, MOMY = 2, MOMZ = 3, ENERGY = 4 };
 enum { VELX = 1, VELY = 2, VELZ = 3, PRESSURE = 4 };
 enum { IDIR = 0, JDIR = 1, KDIR = 2 };
@@ -117,6 +122,9 @@ struct Params {  // mirrored by oracle/oracle.py (ctypes)
     double M0;           // dipole moment (code units) of the background field, m = (0,0,M0)
     double wind[8];      // constant solar wind: rho, P, Vx, Vy, Vz, Bx, By, Bz (code units)
     double inflow[8];    // uniform inner-I inflow state, same order as wind
+    int doBoris;         // physics/doBoris (init.F90:417-423)
+    double Ca;           // physics/Ca: the Boris speed of light (code units)
+    int doAB3;           // sim/doAB3 (init.F90:377): third-order predictor with ooState
 };
 
 struct Model {
@@ -127,6 +135,9 @@ struct Model {
     double M0 = 0.0;
     double wind[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     double inflow[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    bool doBoris = false;
+    double Ca = 0.0;
+    bool doAB3 = false;
 };
 
 struct Grid {
@@ -178,6 +189,11 @@ static inline double dot3(const double* a, const double* b) {
     double s = 0.0;
     for (int q = 0; q < 3; q++) s += a[q] * b[q];
     return s;
+}
+// math.F90:332-343 normVec
+static inline void normVec(const double* a, double* out) {
+    double nA = std::sqrt(dot3(a, a));
+    for (int x = 0; x < 3; x++) out[x] = nA <= TINY ? 0.0 : a[x] / nA;
 }
 
 // ---------------------------------------------------------------- EOS
@@ -339,7 +355,7 @@ static void GasKinFlux(const Model& M, int q, const double (*PrimLRB)[vecLen], c
         dW[ENERGY][i] = dW[ENERGY][i] + s * E;
     }
 }
-// stress.F90:513-599 MagKinFlux (Boris off: Vac2 = Va2)
+// stress.F90:513-599 MagKinFlux
 static void MagKinFlux(const Model& M, int q, const double (*PrimLRB)[vecLen], const double (*MagLRB)[vecLen],
                        const double* Bn, const double (*TfB)[vecLen], double (*mFlxB)[vecLen],
                        const double (*B0)[vecLen], const double* B0n, double* bbD, double* VaD) {
@@ -358,7 +374,7 @@ static void MagKinFlux(const Model& M, int q, const double (*PrimLRB)[vecLen], c
             Va2 = 2 * dPb / D;
             bbD[i] = bbD[i] + 0.5 * (Bx * Bx + By * By + Bz * Bz);
         }
-        double Vac2 = Va2;
+        double Vac2 = M.doBoris ? Va2 / (1 + (Va2 / (M.Ca * M.Ca))) : Va2;  // Boris-corrected Va^2
         double Vx = PrimLRB[VELX][i], Vy = PrimLRB[VELY][i], Vz = PrimLRB[VELZ][i];
         double Nx = TfB[NORMX][i], Ny = TfB[NORMY][i], Nz = TfB[NORMZ][i];
         double Vn = Nx * Vx + Ny * Vy + Nz * Vz;
@@ -447,6 +463,14 @@ static void Fluxes(const Model& M, const Grid& G, const State& nS, const State& 
     if (M.doMHD) {
         MagKinFlux(M, LEFT, PrimL, MagL, Bn, TfB, mFlxB, B0, B0n, bbD, VaD);
         MagKinFlux(M, RIGHT, PrimR, MagR, Bn, TfB, mFlxB, B0, B0n, bbD, VaD);
+        if (M.doBoris) {  // stress.F90:335-349 Boris hogs on the magnetic fluxes
+            for (int i = 0; i < iMax; i++)
+                for (int x = 0; x < NDIM; x++) {
+                    double deeV = PrimR[VELX + x][i] - PrimL[VELX + x][i];
+                    double deeP = bbD[i] * deeV / (M.Ca * M.Ca);
+                    mFlxB[x][i] = mFlxB[x][i] - M.cHogM * VaD[i] * deeP;
+                }
+        }
         for (int nv = 0; nv < NDIM; nv++)
             for (int i = 0; i < iMax; i++) mFlx(isB + i, j, k, nv + 3 * dN) = faB[i] * mFlxB[nv][i];
     }
@@ -457,6 +481,19 @@ static void Fluxes(const Model& M, const Grid& G, const State& nS, const State& 
     const double alphaS = 1.0;
     for (int nv = 0; nv < NVAR; nv++)
         for (int i = 0; i < iMax; i++) gFlxB[nv][i] = gFlxB[nv][i] - alphaS * M.cHogH * VaD[i] * dW[nv][i];
+    if (M.doBoris) {  // stress.F90:399-417 the "nuclear option" (doNuke = T, cLim = 1.5)
+        for (int i = 0; i < iMax; i++) {
+            double vl[3] = {PrimL[VELX][i], PrimL[VELY][i], PrimL[VELZ][i]};
+            double vr[3] = {PrimR[VELX][i], PrimR[VELY][i], PrimR[VELZ][i]};
+            double vL = norm2s(vl, 3), vR = norm2s(vr, 3);
+            double Vn = std::sqrt(vL * vL + vR * vR) / SQRT2_R4;
+            if (Vn >= cLim * M.Ca)
+                for (int nv = 0; nv < NVAR; nv++) {
+                    double dCon = ConB[nv][Nr2][i] - ConB[nv][Nr2 - 1][i];
+                    gFlxB[nv][i] = gFlxB[nv][i] - M.Ca * dCon;
+                }
+        }
+    }
     for (int nv = 0; nv < NVAR; nv++)
         for (int i = 0; i < iMax; i++) gFlx(isB + i, j, k, nv + 5 * dN) = faB[i] * gFlxB[nv][i];
 }
@@ -692,6 +729,7 @@ static void CalcElecField(const Model& M, const Grid& G, const State& nS, const 
                     for (int i = 0; i < iMax; i++) {
                         int iG = iB + i;
                         double vA = std::sqrt(b1[i] * b1[i] + b2[i] * b2[i]) / std::sqrt(Dc[i]);
+                        if (M.doBoris) vA = M.Ca * vA / std::sqrt(M.Ca * M.Ca + vA * vA);  // fields.F90:211-213
                         vDiff[i] = vDiff[i] + vA;
                         vDiff[i] = std::min(vDiff[i], M.CFL * G.edge(iG, j, k, eD) / M.dt);
                         double e = -(v1[i] * b2[i] - v2[i] * b1[i]) + M.Vd0 * vDiff[i] * Jd[i];
@@ -759,15 +797,50 @@ static void CellMaxwell(const Model& M, double* U, const double* dGasM, double d
     U[MOMZ] = Mz;
     U[ENERGY] = KinE + P / (M.gamma - 1);
 }
+// mhdgroup.F90:334-382 CellBoris, single fluid; B2 and B0 are total fields
+// (background included) at n+1 and n, U2 the hydro-updated state, U0 State n
+static void CellBoris(const Model& M, double* U2, const double* U0, const double* B2, const double* B0,
+                      const double* dGasH, const double* dGasM, double Ca, double dt) {
+    double W2[NVAR];
+    CellC2P(M, U2, W2);
+    double D2 = std::max(W2[DEN], dFloor);
+    double P2 = std::max(W2[PRESSURE], pFloor);
+    double D0 = std::max(U0[DEN], dFloor);
+    double V0[3] = {U0[MOMX] / D0, U0[MOMY] / D0, U0[MOMZ] / D0};
+    double B1[3], dPGas[3], dPMag[3], bhat1[3], dMom[3];
+    for (int x = 0; x < 3; x++) B1[x] = 0.5 * (B2[x] + B0[x]);
+    double alpha = dot3(B1, B1) / (D2 * Ca * Ca);
+    double dRho = dt * dGasH[DEN];
+    for (int x = 0; x < 3; x++) {
+        dPGas[x] = dt * dGasH[MOMX + x];
+        dPMag[x] = dt * dGasM[x];
+    }
+    double pCon = 1.0 / (1.0 + alpha);
+    normVec(B1, bhat1);
+    if (alpha > TINY) {
+        double sum[3];
+        for (int x = 0; x < 3; x++) sum[x] = dPGas[x] + dPMag[x];
+        double pg = dot3(dPGas, bhat1), ps = dot3(sum, bhat1), pv = dot3(V0, bhat1);
+        for (int x = 0; x < 3; x++)
+            dMom[x] = pg * bhat1[x] + pCon * (sum[x] - ps * bhat1[x]) + alpha * pCon * dRho * (V0[x] - pv * bhat1[x]);
+    } else {
+        for (int x = 0; x < 3; x++) dMom[x] = dPGas[x] + dPMag[x];
+    }
+    W2[DEN] = D2;
+    for (int x = 0; x < 3; x++) W2[VELX + x] = (D0 * V0[x] + dMom[x]) / D2;
+    W2[PRESSURE] = P2;
+    CellP2C(M, W2, U2);
+}
 static void CopyState(const Grid& G, const State& a, State& b) {  // mhdgroup.F90:202-256
     b.Gas.v = a.Gas.v;
     b.Bxyz.v = a.Bxyz.v;
     b.magFlux.v = a.magFlux.v;
     b.time = a.time;
 }
-// mhdgroup.F90:79-200 applyUpdate (single fluid, no Boris)
-static void applyUpdate(const Model& M, const Grid& G, State& S, State& oS, double dt, const F4& dGasH,
+// mhdgroup.F90:79-200 applyUpdate (single fluid)
+static void applyUpdate(const Model& M, const Grid& G, State& S, State& oS, State& ooS, double dt, const F4& dGasH,
                         const F4& dGasM, const F4& E) {
+    if (M.doAB3) CopyState(G, oS, ooS);
     CopyState(G, S, oS);
     S.time = S.time + dt;
 #pragma omp parallel for collapse(2)
@@ -786,7 +859,24 @@ static void applyUpdate(const Model& M, const Grid& G, State& S, State& oS, doub
                 double U[NVAR], dPm[NDIM];
                 for (int nv = 0; nv < NVAR; nv++) U[nv] = S.Gas(i, j, k, nv);
                 for (int x = 0; x < NDIM; x++) dPm[x] = dGasM(i, j, k, x);
-                CellMaxwell(M, U, dPm, dt);
+                if (M.doBoris) {
+                    double oU[NVAR], B[3], oB[3], dPg[NVAR];
+                    for (int nv = 0; nv < NVAR; nv++) {
+                        oU[nv] = oS.Gas(i, j, k, nv);
+                        dPg[nv] = dGasH(i, j, k, nv);
+                    }
+                    for (int x = 0; x < 3; x++) {
+                        B[x] = S.Bxyz(i, j, k, x);
+                        oB[x] = oS.Bxyz(i, j, k, x);
+                        if (M.doBackground) {
+                            B[x] = B[x] + G.B0(i, j, k, x);
+                            oB[x] = oB[x] + G.B0(i, j, k, x);
+                        }
+                    }
+                    CellBoris(M, U, oU, B, oB, dPg, dPm, M.Ca, dt);
+                } else {
+                    CellMaxwell(M, U, dPm, dt);
+                }
                 for (int nv = 0; nv < NVAR; nv++) S.Gas(i, j, k, nv) = U[nv];
             }
 }
@@ -795,16 +885,30 @@ static inline double ExtrapAB2(double dt, double Q, double oQ, double odt) {
     double dQ = (Q - oQ) / odt;
     return Q + dt * dQ;
 }
-// mhdgroup.F90:444-615 Predictor + PredictCell (AB2, single fluid)
-static void Predictor(const Model& M, const Grid& G, const State& S, const State& oS, State& pS, double pdt) {
+// mhdgroup.F90:721-731 ExtrapAB3
+static inline double ExtrapAB3(double dt, double Q, double oQ, double ooQ, double odt, double oodt) {
+    double dQ = (Q - oQ) / odt;
+    double odQ = (oQ - ooQ) / oodt;
+    double tScl = (dt + odt) / (odt + oodt);
+    return Q + dt * dQ + dt * tScl * (dQ - odQ);
+}
+// mhdgroup.F90:444-615 Predictor + PredictCell (single fluid). With doAB3 the
+// face fluxes use ooState (:466-470) but the gas takes its third level from
+// oState (ooQ = oState%Gas, :500-502), as the reference does.
+static void Predictor(const Model& M, const Grid& G, const State& S, const State& oS, const State& ooS, State& pS,
+                      double pdt) {
     double odt = S.time - oS.time;
+    double oodt = M.doAB3 ? oS.time - ooS.time : 0.0;
     if (M.doMHD) {
 #pragma omp parallel for collapse(2)
         for (int k = G.ksg; k <= G.keg + 1; k++)
             for (int j = G.jsg; j <= G.jeg + 1; j++)
                 for (int i = G.isg; i <= G.ieg + 1; i++)
                     for (int d = 0; d < 3; d++)
-                        pS.magFlux(i, j, k, d) = ExtrapAB2(pdt, S.magFlux(i, j, k, d), oS.magFlux(i, j, k, d), odt);
+                        pS.magFlux(i, j, k, d) =
+                            M.doAB3 ? ExtrapAB3(pdt, S.magFlux(i, j, k, d), oS.magFlux(i, j, k, d),
+                                                ooS.magFlux(i, j, k, d), odt, oodt)
+                                    : ExtrapAB2(pdt, S.magFlux(i, j, k, d), oS.magFlux(i, j, k, d), odt);
     }
     bFlux2Fld(G, pS.magFlux, pS.Bxyz);
 #pragma omp parallel for collapse(2)
@@ -818,7 +922,13 @@ static void Predictor(const Model& M, const Grid& G, const State& S, const State
                 }
                 CellC2P(M, oQ, oW);
                 CellC2P(M, Q, W);
-                for (int nv = 0; nv < NVAR; nv++) pW[nv] = ExtrapAB2(pdt, W[nv], oW[nv], odt);
+                if (M.doAB3) {
+                    double ooW[NVAR];
+                    CellC2P(M, oQ, ooW);  // ooQ = oState%Gas
+                    for (int nv = 0; nv < NVAR; nv++) pW[nv] = ExtrapAB3(pdt, W[nv], oW[nv], ooW[nv], odt, oodt);
+                } else {
+                    for (int nv = 0; nv < NVAR; nv++) pW[nv] = ExtrapAB2(pdt, W[nv], oW[nv], odt);
+                }
                 pW[DEN] = std::max(pW[DEN], dFloor);
                 pW[PRESSURE] = std::max(pW[PRESSURE], pFloor);
                 CellP2C(M, pW, pQ);
@@ -979,6 +1089,7 @@ static inline double CellDT(const Model& M, const Grid& G, const State& S, int i
         }
         double MagB = std::sqrt(Bx * Bx + By * By + Bz * Bz);
         Valf = MagB / std::sqrt(rho);
+        if (M.doBoris) Valf = M.Ca * Valf / std::sqrt(M.Ca * M.Ca + Valf * Valf);  // gridutils.F90:91-93
     }
     double vCFL = Vfl + std::sqrt(Cs * Cs + Valf * Valf) + Vdiff;
     double dl = std::min(std::min(G.di(i, j, k), G.dj(i, j, k)), G.dk(i, j, k));
@@ -1618,11 +1729,6 @@ static void InflowBC(const Model& M, const Grid& G, State& S) {
                 for (int x = 0; x < 3; x++) S.Bxyz(G.is - n, j, k, x) = B[x];
             }
 }
-// math.F90:332-343 normVec
-static inline void normVec(const double* a, double* out) {
-    double nA = std::sqrt(dot3(a, a));
-    for (int x = 0; x < 3; x++) out[x] = nA <= TINY ? 0.0 : a[x] / nA;
-}
 // math.F90:97-111 RampDown
 static inline double RampDown(double r, double rC, double lC) {
     if (r <= rC) return 1.0;
@@ -1650,6 +1756,7 @@ static double Con2Fast(const Model& M, const double* gCon, const double* B) {
     double D = gCon[DEN];
     double MagB = norm2s(B, 3);
     double Va = MagB / std::sqrt(D);
+    if (M.doBoris) Va = M.Ca * Va / std::sqrt(M.Ca * M.Ca + Va * Va);  // gamutils.F90:356-358
     return std::sqrt(Cs * Cs + Va * Va);
 }
 // apps/wind.F90:206-374 WindBC with a constant wind (GetWindAt is then
@@ -1725,7 +1832,7 @@ static void WindBC(const Model& M, const Grid& G, State& S) {
 struct App {
     Model M;
     Grid G;
-    State S, oS, hS;
+    State S, oS, ooS, hS;
     F4 gFlx, mFlx, dGasH, dGasM, Vf;
     int status = 0;
 };
@@ -1740,10 +1847,10 @@ static void allocState(const Grid& G, State& S) {
 // mhdgroup.F90:16-76 AdvanceMHD
 static void AdvanceMHD(App& A, double dt) {
     if (std::fabs(A.oS.time - A.S.time) < TINY) A.oS.time = A.S.time - A.M.dt;
-    Predictor(A.M, A.G, A.S, A.oS, A.hS, 0.5 * dt);
+    Predictor(A.M, A.G, A.S, A.oS, A.ooS, A.hS, 0.5 * dt);
     if (A.M.doMHD) CalcElecField(A.M, A.G, A.S, A.hS, A.Vf, A.S.Efld);
     CalcStress(A.M, A.G, A.S, A.hS, A.gFlx, A.mFlx, A.dGasH, A.dGasM);
-    applyUpdate(A.M, A.G, A.S, A.oS, dt, A.dGasH, A.dGasM, A.S.Efld);
+    applyUpdate(A.M, A.G, A.S, A.oS, A.ooS, dt, A.dGasH, A.dGasM, A.S.Efld);
 }
 // gamapp.F90:73-113 stepGamera + UpdateStateData
 static int stepGamera(App& A) {
@@ -1768,6 +1875,7 @@ extern "C" {
 struct OrcScalars {
     double t, dt, dt0, time, otime;
     int ts, status;
+    double ootime;
 };
 
 void* orc_create(const Params* p, const double* xyz) {
@@ -1784,6 +1892,9 @@ void* orc_create(const Params* p, const double* xyz) {
     M.M0 = p->M0;
     for (int n = 0; n < 8; n++) M.wind[n] = p->wind[n];
     for (int n = 0; n < 8; n++) M.inflow[n] = p->inflow[n];
+    M.doBoris = p->doBoris != 0;
+    M.Ca = p->Ca;
+    M.doAB3 = p->doAB3 != 0;
     g_up7 = M.up7;
     pdmb = p->pdmb; dFloor = p->dFloor; pFloor = p->pFloor;
     G.Nip = p->Nip; G.Njp = p->Njp; G.Nkp = p->Nkp;
@@ -1805,6 +1916,7 @@ void* orc_create(const Params* p, const double* xyz) {
     allocState(G, A->S);
     A->S.time = M.t;  // allocState sets State%time = Model%t (gamutils.F90:199)
     allocState(G, A->oS);
+    allocState(G, A->ooS);
     allocState(G, A->hS);
     G.cellArr(A->gFlx, 15);
     G.cellArr(A->mFlx, 9);
@@ -1853,6 +1965,9 @@ double* orc_array(void* h, int which, long* n) {
         case 26: a = &A->G.edgB0; break;
         case 27: a = &A->G.B0; break;
         case 28: a = &A->G.dpB0; break;
+        case 29: a = &A->ooS.Gas; break;
+        case 30: a = &A->ooS.magFlux; break;
+        case 31: a = &A->ooS.Bxyz; break;
         default: *n = 0; return nullptr;
     }
     *n = (long)a->v.size();
@@ -1890,9 +2005,11 @@ int orc_init_finish(void* h) {
     EnforceBCs(A->M, A->G, A->S);
     CopyState(A->G, A->S, A->oS);
     A->oS.Efld.v = A->S.Efld.v;
+    if (A->M.doAB3) CopyState(A->G, A->S, A->ooS);  // init.F90:232
     int st;
     A->M.dt = CalcDT(A->M, A->G, A->S, &st);
     A->oS.time = A->S.time - A->M.dt;
+    if (A->M.doAB3) A->ooS.time = A->oS.time - A->M.dt;  // init.F90:238-241
     return st;
 }
 
@@ -1915,11 +2032,13 @@ void orc_scalars(void* h, OrcScalars* o) {
     App* A = (App*)h;
     o->t = A->M.t; o->dt = A->M.dt; o->dt0 = A->M.dt0; o->time = A->S.time; o->otime = A->oS.time;
     o->ts = A->M.ts; o->status = A->status;
+    o->ootime = A->ooS.time;
 }
 void orc_set_scalars(void* h, const OrcScalars* o) {
     App* A = (App*)h;
     A->M.t = o->t; A->M.dt = o->dt; A->M.dt0 = o->dt0; A->S.time = o->time; A->oS.time = o->otime;
     A->M.ts = o->ts;
+    A->ooS.time = o->ootime;
 }
 
 // gridutils.F90:717-770 DivB (sequential sum, no background)

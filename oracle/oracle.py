@@ -43,13 +43,15 @@ class _Params(C.Structure):
         ("cHogH", C.c_double), ("cHogM", C.c_double), ("dFloor", C.c_double), ("pFloor", C.c_double),
         ("tFin", C.c_double), ("dt0", C.c_double), ("limDT0", C.c_double), ("fixedDT", C.c_double),
         ("bc", C.c_int * 6), ("noMetric", C.c_int), ("M0", C.c_double), ("wind", C.c_double * 8),
-        ("inflow", C.c_double * 8),
+        ("inflow", C.c_double * 8), ("doBoris", C.c_int), ("Ca", C.c_double),
+        ("doAB3", C.c_int),
     ]
 
 
 class _Scalars(C.Structure):
     _fields_ = [("t", C.c_double), ("dt", C.c_double), ("dt0", C.c_double),
-                ("time", C.c_double), ("otime", C.c_double), ("ts", C.c_int), ("status", C.c_int)]
+                ("time", C.c_double), ("otime", C.c_double), ("ts", C.c_int), ("status", C.c_int),
+                ("ootime", C.c_double)]
 
 
 @dataclass
@@ -81,6 +83,9 @@ class OracleParams:
     M0: float = 0.0
     wind: tuple = (0.0,) * 8
     inflow: tuple = (0.0,) * 8
+    doBoris: bool = False
+    Ca: float = 0.0
+    doAB3: bool = False
 
     def to_c(self) -> _Params:
         p = _Params()
@@ -103,7 +108,7 @@ _ARR = {"Gas": (0, "cell", 5), "magFlux": (1, "face", 3), "Bxyz": (2, "cell", 3)
         "hGas": (18, "cell", 5), "hmagFlux": (19, "face", 3), "hBxyz": (20, "cell", 3),
         "dGasH": (21, "cell", 5), "dGasM": (22, "cell", 3), "xyz": (23, "face", 3),
         "fcB0": (24, "cell", 9), "bFlux0": (25, "cell", 3), "edgB0": (26, "cell", 6), "B0": (27, "cell", 3),
-        "dpB0": (28, "cell", 3)}
+        "dpB0": (28, "cell", 3), "ooGas": (29, "cell", 5), "oomagFlux": (30, "face", 3), "ooBxyz": (31, "cell", 3)}
 
 _libs: dict = {}
 

@@ -149,3 +149,30 @@ def test_dt_limit_is_reported(oracle_built):
     assert o.step(2) == 0
     o.set_scalars(dt0=1.0e5 * o.scalars()["dt"])
     assert o.step(1) == 1  # ST_DT_BAD
+
+
+def test_boris_limits(oracle_built):
+    """Boris correction in the oracle: with Ca -> HUGE it reduces to the step
+    without it (the Boris speed, Vac2 and CellBoris's alpha vanish; only
+    rounding differs), and a Ca below the flow speeds changes the solution
+    (Boris-limited speeds, hogs, the nuclear option) while keeping mass and
+    divB exact."""
+    N = (32, 32, 4)
+    xyz = grids.uniform_corners(*N)
+
+    def run(**kw):
+        o = orc.Oracle(orc.OracleParams(*N, **kw), xyz, "strict")
+        o.ic_orszag_tang()
+        assert o.init_finish() == 0
+        assert o.step(10) == 0
+        return o
+
+    a, b, c = run(), run(doBoris=True, Ca=1.0e12), run(doBoris=True, Ca=0.5)
+    ga, gb, gc = a.array("Gas"), b.array("Gas"), c.array("Gas")
+    act = (slice(None), slice(4, 8), slice(4, 36), slice(4, 36))
+    assert np.abs(gb - ga).max() <= 1e-12 * np.abs(ga).max()
+    d = float(np.abs(gc[act] - ga[act]).max() / np.abs(ga[act]).max())
+    assert d > 1e-3, d
+    m0 = a.array("Gas")[0][act[1:]].sum()
+    assert abs(gc[0][act[1:]].sum() - m0) <= 1e-12 * m0
+    assert c.divb() <= 1e-12 * np.abs(c.array("magFlux")).sum()
