@@ -72,6 +72,8 @@ typedef struct gam_params {
                                Alfven speed, Boris hogs and the nuclear option in
                                the fluxes, CellBoris in the update */
     double Ca;              /* physics/Ca, the Boris speed of light (code units) */
+    int32_t doAB3;          /* sim/doAB3 (init.F90:377): AB3 predictor with ooState
+                               (mhdgroup.F90:444-517, 721-731) */
 } gam_params;
 
 typedef struct gam_handle gam_handle;
@@ -184,6 +186,16 @@ int gam_set_wind(gam_handle* h, const double wind[8]);
  * fluxes (steps recompute every ghost's Bxyz). Call before the initial
  * condition; calling it later changes the boundary from the next step on. */
 int gam_set_inflow(gam_handle* h, const double state[8]);
+
+/* ooState of the AB3 predictor (doAB3): its face fluxes (Fortran
+ * magFlux(isg:ieg+1,...,1:3)) and time. The predictor reads nothing else of
+ * ooState: the gas takes its third level from oState (mhdgroup.F90:500-502).
+ * gam_upload_state with an oState sets ooState = oState at time otime - dt, the
+ * fallback of readH5Restart for a restart without ooState (gioH5.F90:797-802);
+ * a driver that holds ooState passes it here afterwards. The initial
+ * conditions set ooState = State at time otime - dt (init.F90:232-241). */
+int gam_set_oostate(gam_handle* h, const double* oomagFlux, double ootime);
+int gam_get_oostate(gam_handle* h, double* oomagFlux, double* ootime);
 
 /* Dipole-in-wind start: the wind state in every active cell with the density
  * perturbed by amp*u (u uniform in [-1, 1), SplitMix64 of seed and the Fortran

@@ -779,7 +779,7 @@ int flux_call(const gam_params* p, const void* QW, const void* Wn, const void* Q
 int check(const gam_params* p, int32_t fp32) {
     if (!p) return GAM_EINVAL;
     if (p->rmeth != GAM_RECON_8CENT) return GAM_EINVAL;  // the adjoint covers 8CENT
-    if (p->doBoris) return GAM_EINVAL;                   // and the step without the Boris correction
+    if (p->doBoris || p->doAB3) return GAM_EINVAL;      // and the step without Boris, with AB2
     if (p->nG != 4 || p->Nip < 1 || p->Njp < 1 || p->Nkp < 1 || p->do25D) return GAM_EBADDIM;
     (void)fp32;
     return GAM_OK;
@@ -942,7 +942,7 @@ int predict_call(const gam_params* p, const void* const* st, const void* const* 
         w.QW = (R*)out[0]; w.Wn = (R*)out[1]; w.Dh = (R*)out[2]; w.VdV = (R*)out[3]; w.QB = (R*)out[4];
         w.abh = (R*)out[5]; w.Bnf = (R*)out[6]; w.bn = (R*)out[7];
         const dim3 blk(32, 8, 1);
-        k_predict<R, 1><<<grid3(all, blk), blk, 0, s>>>(b, P, g, cur, old, w, sc);
+        k_predict<R, 1><<<grid3(all, blk), blk, 0, s>>>(b, P, g, cur, old, w, sc, nullptr);
     } else {
         Work<R> dw;
         memset(&dw, 0, sizeof(dw));
@@ -974,7 +974,7 @@ int update_call(const gam_params* p, const void* const* in, const void* const* g
     const dim3 blk(32, 4, 1);
     if (out) {
         StateBuf<R> nxt{(R*)out[0], (R*)out[1], (R*)out[2]};
-        k_update_faces<R><<<grid3(all, blk), blk, 0, s>>>(b, P, cur, nxt, w, sc);
+        k_update_faces<R><<<grid3(all, blk), blk, 0, s>>>(b, P, cur, nxt, w, sc, nullptr);
         const double gamma = p->gamma, gm1 = p->gamma - 1;
         k_update_cells<R, 1><<<grid3(cells, blk), blk, 0, s>>>(b, P, g, cur, nxt, w, sc, gamma, gm1);
     } else {

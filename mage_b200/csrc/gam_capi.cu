@@ -134,6 +134,7 @@ extern "C" int gam_default_params(gam_params* p, int32_t Nip, int32_t Njp, int32
     for (int n = 0; n < 6; n++) p->bc[n] = GAM_BC_PERIODIC;
     p->doBoris = 0;
     p->Ca = 1.0e12;  // HUGE (kdefs.F90:20), the reference's Ca without Boris
+    p->doAB3 = 0;
     return GAM_OK;
 }
 
@@ -147,6 +148,7 @@ template <class R> static void fill_dev_params(DevParams<R>& P, const gam_params
     P.cHogM = (R)p.cHogM;
     P.doBoris = p.doBoris;
     P.Ca = p.Ca;
+    P.doAB3 = p.doAB3;
     P.dFloor = (R)p.dFloor;
     P.pFloor = (R)p.pFloor;
     P.doMHD = p.doMHD; P.doLFMLim = p.doLFMLim; P.do25D = p.do25D; P.doBackground = p.doBackground;
@@ -171,6 +173,8 @@ template <class R> static int alloc_bulk(gam_handle* h, Ctx<R>& C) {
     A(C.w.QW, 5); A(C.w.QB, 3); A(C.w.Dh, 1); A(C.w.Wn, 5); A(C.w.Bl, 3); A(C.w.VdV, 3);
     A(C.w.abh, 3); A(C.w.bn, 3); A(C.w.Bnf, 3); A(C.w.AVf, 9); A(C.w.E, 3);
     A(C.w.gF, 15); A(C.w.mF, 9);
+    C.oomf = nullptr;
+    if (h->p.doAB3) A(C.oomf, 3);
     if (sizeof(R) == sizeof(double)) {
         C.g.vol = (const R*)h->gd.vol; C.g.xyzcc = (const R*)h->gd.xyzcc; C.g.dl = (const R*)h->gd.dl;
         C.g.face = (const R*)h->gd.face; C.g.xfc = (const R*)h->gd.xfc; C.g.Tf = (const R*)h->gd.Tf;
@@ -446,14 +450,18 @@ static int upload_state_t(gam_handle* h, Ctx<R>& C, const double* Gas, const dou
     if ((rc = up_r<R>(h, Bxyz, C.st[0].B, false, 3))) return rc;
     if ((rc = up_r<R>(h, oGas, C.st[1].Gas, false, 5))) return rc;
     if ((rc = up_r<R>(h, omagFlux, C.st[1].mf, true, 3))) return rc;
+    if (C.oomf) CK(h, cudaMemcpyAsync(C.oomf, C.st[1].mf, 3 * h->b.fs * sizeof(R), cudaMemcpyDeviceToDevice, h->s));
     return GAM_OK;
 }
 
-static int set_scalars(gam_handle* h, double time, double otime, double dt, int32_t ts) {
+// ooState time: otime - dt (init.F90:238-241 and the restart fallback,
+// gioH5.F90:800) unless keepOO (oState and ooState stay on the device)
+static int set_scalars(gam_handle* h, double time, double otime, double dt, int32_t ts, bool keepOO = false) {
     GamScalars s;
     CK(h, cudaMemcpyAsync(&s, h->sc, sizeof(s), cudaMemcpyDeviceToHost, h->s));
     CK(h, cudaStreamSynchronize(h->s));
     s.time = time; s.otime = otime; s.t = time; s.dt = dt; s.ts = ts;
+    if (!keepOO) s.ootime = otime - dt;
     s.status = 0; s.halted = 0; s.nbad = 0;
     double hugedt = 1.0e12;
     memcpy(&s.dtmin_bits, &hugedt, 8);
@@ -488,9 +496,37 @@ extern "C" int gam_upload_state(gam_handle* h, const double* Gas, const double* 
                     : upload_state_t<double>(h, h->cd, Gas, magFlux, Bxyz, oGas, omagFlux);
     }
     if (rc) return rc;
-    if ((rc = set_scalars(h, time, otime, dt, ts))) return rc;
+    if ((rc = set_scalars(h, time, otime, dt, ts, !oGas))) return rc;
     CK(h, cudaStreamSynchronize(h->s));
     h->haveState = true;
+    return GAM_OK;
+}
+
+template <class R> static int set_oo_t(gam_handle* h, Ctx<R>& C, const double* oomagFlux) {
+    return up_r<R>(h, oomagFlux, C.oomf, true, 3);
+}
+extern "C" int gam_set_oostate(gam_handle* h, const double* oomagFlux, double ootime) {
+    if (!h || !oomagFlux) return GAM_EINVAL;
+    if (!h->p.doAB3) return fail(h, GAM_ESTATE, "ooState is kept only with doAB3");
+    if (!h->haveState) return fail(h, GAM_ESTATE, "upload State and oState first");
+    int rc = h->f32 ? set_oo_t<float>(h, h->cf, oomagFlux) : set_oo_t<double>(h, h->cd, oomagFlux);
+    if (rc) return rc;
+    CK(h, cudaMemcpyAsync(&h->sc->ootime, &ootime, sizeof(double), cudaMemcpyHostToDevice, h->s));
+    CK(h, cudaStreamSynchronize(h->s));
+    return GAM_OK;
+}
+extern "C" int gam_get_oostate(gam_handle* h, double* oomagFlux, double* ootime) {
+    if (!h) return GAM_EINVAL;
+    if (!h->p.doAB3) return fail(h, GAM_ESTATE, "ooState is kept only with doAB3");
+    if (!h->haveState) return fail(h, GAM_ESTATE, "no state");
+    int rc = GAM_OK;
+    if (oomagFlux) rc = h->f32 ? down_r<float>(h, h->cf.oomf, oomagFlux, true, 3)
+                               : down_r<double>(h, h->cd.oomf, oomagFlux, true, 3);
+    if (rc) return rc;
+    if (ootime) {
+        CK(h, cudaMemcpyAsync(ootime, &h->sc->ootime, sizeof(double), cudaMemcpyDeviceToHost, h->s));
+        CK(h, cudaStreamSynchronize(h->s));
+    }
     return GAM_OK;
 }
 
@@ -602,14 +638,16 @@ template <class R> static int profile_t(gam_handle* h, Ctx<R>& C, int32_t reps, 
     const long fs = h->b.fs;
     const StateBuf<R>& O = C.st[1 - h->cur];
     R* save = nullptr;
-    CK(h, cudaMalloc(&save, 11 * fs * sizeof(R)));
+    CK(h, cudaMalloc(&save, 14 * fs * sizeof(R)));
     auto cp = [&](R* d, const R* src, long n) { return cudaMemcpyAsync(d, src, n * sizeof(R), cudaMemcpyDeviceToDevice, h->s); };
     cudaError_t e = cp(save, O.Gas, 5 * fs);
     if (e == cudaSuccess) e = cp(save + 5 * fs, O.mf, 3 * fs);
     if (e == cudaSuccess) e = cp(save + 8 * fs, O.B, 3 * fs);
+    if (e == cudaSuccess && C.oomf) e = cp(save + 11 * fs, C.oomf, 3 * fs);
     GamScalars t = s;
     if (fabs(t.otime - t.time) < 1.0e-12) t.otime = t.time - t.dt;
     t.odt = t.time - t.otime;
+    t.oodt = t.otime - t.ootime;
     t.pdt = 0.5 * t.dt;
     if (e == cudaSuccess) e = cudaMemcpyAsync(h->sc, &t, sizeof(t), cudaMemcpyHostToDevice, h->s);
     if (e == cudaSuccess) {
@@ -624,6 +662,7 @@ template <class R> static int profile_t(gam_handle* h, Ctx<R>& C, int32_t reps, 
     cudaError_t e2 = cp(O.Gas, save, 5 * fs);
     if (e2 == cudaSuccess) e2 = cp(O.mf, save + 5 * fs, 3 * fs);
     if (e2 == cudaSuccess) e2 = cp(O.B, save + 8 * fs, 3 * fs);
+    if (e2 == cudaSuccess && C.oomf) e2 = cp(C.oomf, save + 11 * fs, 3 * fs);
     // restore the scalars the repeated kernels touched (dt reduction, AB2 spacing)
     if (e2 == cudaSuccess) e2 = cudaMemcpyAsync(h->sc, &s, sizeof(s), cudaMemcpyHostToDevice, h->s);
     if (e2 == cudaSuccess) e2 = cudaStreamSynchronize(h->s);
@@ -1090,6 +1129,8 @@ extern "C" int gam_init_finish_halo(gam_handle* h, double* dt_local) {
                   h->f32 ? (void*)h->cf.st[1 - h->cur].B : (void*)h->cd.st[1 - h->cur].B};
     const long nc[3] = {5, 3, 3};
     for (int q = 0; q < 3; q++) CK(h, cudaMemcpyAsync(O[q], S[q], nc[q] * fs * w, cudaMemcpyDeviceToDevice, h->s));
+    void* oo = h->f32 ? (void*)h->cf.oomf : (void*)h->cd.oomf;
+    if (oo) CK(h, cudaMemcpyAsync(oo, S[1], 3 * fs * w, cudaMemcpyDeviceToDevice, h->s));  // ooState = State
     return gam_calc_dt(h, dt_local);
 }
 

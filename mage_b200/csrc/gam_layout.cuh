@@ -43,4 +43,5 @@ struct GamScalars {
     int halted;                        // set once a step failed; later kernels return at once
     int fixedTimestep;
     int nbad;                          // cells whose dt is not a finite positive number
+    double ootime, oodt;               // ooState time and oState - ooState spacing (doAB3)
 };

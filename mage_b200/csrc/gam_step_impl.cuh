@@ -246,6 +246,29 @@ __device__ __forceinline__ void predict_cell(const DevParams<R>& P, const R* Q, 
     cell_p2c(P, pW, pQ);
 }
 
+// ExtrapAB3 (mhdgroup.F90:721-731)
+template <class R> __device__ __forceinline__ R extrap_ab3(R dt, R Q, R oQ, R ooQ, R odt, R oodt) {
+    R dQ = (Q - oQ) / odt;
+    R odQ = (oQ - ooQ) / oodt;
+    R tScl = (dt + odt) / (odt + oodt);
+    return Q + dt * dQ + dt * tScl * (dQ - odQ);
+}
+// PredictCell with doAB3: the third level of the gas is oState's
+// (ooQ = oState%Gas, mhdgroup.F90:500-502), as in the reference
+template <class R>
+__device__ __forceinline__ void predict_cell_ab3(const DevParams<R>& P, const R* Q, const R* oQ, R pdt, R odt, R oodt,
+                                                 R* pQ) {
+    R W[5], oW[5], ooW[5], pW[5];
+    cell_c2p(P, oQ, oW);
+    cell_c2p(P, Q, W);
+    cell_c2p(P, oQ, ooW);
+#pragma unroll
+    for (int v = 0; v < 5; v++) pW[v] = extrap_ab3(pdt, W[v], oW[v], ooW[v], odt, oodt);
+    pW[0] = rmax(pW[0], P.dFloor);
+    pW[4] = rmax(pW[4], P.pFloor);
+    cell_p2c(P, pW, pQ);
+}
+
 // Boris-limited speed Ca v / sqrt(Ca^2 + v^2) (fields.F90:211-213,
 // gridutils.F90:91-93, gamutils.F90:356-358)
 template <class T> __device__ __forceinline__ T boris_speed(T Ca, T v) { return Ca * v / sqrt(Ca * Ca + v * v); }
@@ -287,6 +310,7 @@ __global__ void k_step_begin(GamScalars* sc) {
     if (sc->halted) return;
     if (fabs(sc->otime - sc->time) < TINY) sc->otime = sc->time - sc->dt;
     sc->odt = sc->time - sc->otime;
+    sc->oodt = sc->otime - sc->ootime;  // Predictor (mhdgroup.F90:459-463), used with doAB3
     sc->pdt = 0.5 * sc->dt;
 }
 
@@ -295,9 +319,10 @@ __global__ void k_step_begin(GamScalars* sc) {
 // volume * primitive (the recon operand QdV of Cen8LRs/Up7LRs), the limiter
 // primitives, volume * momentum / density (Mom2Face), and per face
 // area * flux/max(area,TINY) and flux/max(area,TINY) (EdgeLRs), flux/area (Fluxes).
-template <class R, int MINB>
+template <class R, int MINB, bool AB3 = false>
 __global__ void __launch_bounds__(256, MINB) k_predict(GamBox b, DevParams<R> P, Geo<R> g, StateBuf<R> cur,
-                                                 StateBuf<R> old, Work<R> w, const GamScalars* sc) {
+                                                 StateBuf<R> old, Work<R> w, const GamScalars* sc,
+                                                 const R* __restrict__ oomf) {
     if (sc->halted) return;
     int ii, jj, kk;
     Range r{0, b.Ni, 0, b.Nj, 0, b.Nk};
@@ -309,12 +334,14 @@ __global__ void __launch_bounds__(256, MINB) k_predict(GamBox b, DevParams<R> P,
     // The state and work pointers may alias as far as the compiler knows, so
     // every state load is issued before the first store.
     R fQ[3], foQ[3], fA[3], Q[5], oQ[5], uQ[3], uoQ[3];
+    R fooQ[3], uooQ[3];  // AB3: ooState fluxes of the lower / upper faces
     if (P.doMHD) {
 #pragma unroll
         for (int d = 0; d < 3; d++) {
             fQ[d] = cur.mf[d * fs + c];
             foQ[d] = old.mf[d * fs + c];
             fA[d] = g.face[d * fs + c];
+            if constexpr (AB3) fooQ[d] = oomf[d * fs + c];
         }
     }
     if (isCell) {
@@ -329,15 +356,22 @@ __global__ void __launch_bounds__(256, MINB) k_predict(GamBox b, DevParams<R> P,
             for (int d = 0; d < 3; d++) {
                 uQ[d] = cur.mf[d * fs + c + off[d]];
                 uoQ[d] = old.mf[d * fs + c + off[d]];
+                if constexpr (AB3) uooQ[d] = oomf[d * fs + c + off[d]];
             }
         }
     }
     R hm[3];
+    [[maybe_unused]] R oodt = (R)0;
+    if constexpr (AB3) oodt = (R)sc->oodt;
     if (P.doMHD) {
 #pragma unroll
         for (int d = 0; d < 3; d++) {
-            R dQ = (fQ[d] - foQ[d]) / odt;
-            hm[d] = fQ[d] + pdt * dQ;  // ExtrapAB2
+            if constexpr (AB3) {
+                hm[d] = extrap_ab3(pdt, fQ[d], foQ[d], fooQ[d], odt, oodt);
+            } else {
+                R dQ = (fQ[d] - foQ[d]) / odt;
+                hm[d] = fQ[d] + pdt * dQ;  // ExtrapAB2
+            }
             R A = fA[d];
             R Am = rmax(A, (R)TINY);
             R bh = hm[d] / Am;
@@ -348,7 +382,10 @@ __global__ void __launch_bounds__(256, MINB) k_predict(GamBox b, DevParams<R> P,
     }
     if (!isCell) return;
     R pQ[5];
-    predict_cell(P, Q, oQ, pdt, odt, pQ);
+    if constexpr (AB3)
+        predict_cell_ab3(P, Q, oQ, pdt, odt, oodt, pQ);
+    else
+        predict_cell(P, Q, oQ, pdt, odt, pQ);
     R Wh[5], Wn[5];
     block_c2p(P, pQ, Wh);
     if (P.doLFMLim) block_c2p(P, Q, Wn);
@@ -367,8 +404,12 @@ __global__ void __launch_bounds__(256, MINB) k_predict(GamBox b, DevParams<R> P,
         R up[3];
 #pragma unroll
         for (int d = 0; d < 3; d++) {
-            R dQ = (uQ[d] - uoQ[d]) / odt;
-            up[d] = uQ[d] + pdt * dQ;
+            if constexpr (AB3) {
+                up[d] = extrap_ab3(pdt, uQ[d], uoQ[d], uooQ[d], odt, oodt);
+            } else {
+                R dQ = (uQ[d] - uoQ[d]) / odt;
+                up[d] = uQ[d] + pdt * dQ;
+            }
         }
         R B[3];
         cell_bxyz(b, g, c, hm[0], up[0], hm[1], up[1], hm[2], up[2], B);
@@ -663,8 +704,14 @@ __global__ void __launch_bounds__(128, MINB) k_stress(GamBox b, DevParams<R> P, 
                 oQr[v] = gasO[v * fs + c];
             }
             const R pdt = (R)sc->pdt, odt = (R)sc->odt;
-            predict_cell(P, Ql, oQl, pdt, odt, pQl);
-            predict_cell(P, Qr, oQr, pdt, odt, pQr);
+            if (P.doAB3) {
+                const R oodt = (R)sc->oodt;
+                predict_cell_ab3(P, Ql, oQl, pdt, odt, oodt, pQl);
+                predict_cell_ab3(P, Qr, oQr, pdt, odt, oodt, pQr);
+            } else {
+                predict_cell(P, Ql, oQl, pdt, odt, pQl);
+                predict_cell(P, Qr, oQr, pdt, odt, pQr);
+            }
 #pragma unroll
             for (int v = 0; v < 5; v++) gv[v] = gv[v] - Ca * (pQr[v] - pQl[v]);
         }
@@ -673,10 +720,12 @@ __global__ void __launch_bounds__(128, MINB) k_stress(GamBox b, DevParams<R> P, 
     for (int v = 0; v < 5; v++) w.gF[(v + 5 * D) * fs + c] = fa * gv[v];
 }
 
-// E2Flux into the new buffer; faces outside its range are copied.
+// E2Flux into the new buffer; faces outside its range are copied. With
+// doAB3 the buffer's old content (oState, n-1) first moves to ooState
+// (CopyState(oState, ooState), mhdgroup.F90:100-102).
 template <class R>
 __global__ void __launch_bounds__(256) k_update_faces(GamBox b, DevParams<R> P, StateBuf<R> cur, StateBuf<R> nxt,
-                                                      Work<R> w, const GamScalars* sc) {
+                                                      Work<R> w, const GamScalars* sc, R* __restrict__ oomf) {
     if (sc->halted) return;
     int ii, jj, kk;
     Range r{0, b.Ni, 0, b.Nj, 0, b.Nk};
@@ -684,6 +733,10 @@ __global__ void __launch_bounds__(256) k_update_faces(GamBox b, DevParams<R> P, 
     const long fs = b.fs;
     const long c = lidx(b, ii, jj, kk);
     const int G = GAM_NG;
+    if (oomf) {
+#pragma unroll
+        for (int x = 0; x < 3; x++) oomf[x * fs + c] = nxt.mf[x * fs + c];
+    }
     const bool inr = P.doMHD && ii >= G && ii <= G + b.Nip && jj >= G && jj <= G + b.Njp && kk >= G && kk <= G + b.Nkp;
     if (!inr) {
 #pragma unroll
@@ -902,6 +955,7 @@ __global__ void __launch_bounds__(128, MINB) k_update_cells(GamBox b, DevParams<
 // mhdgroup.F90:106, step.F90:58-168). A failure halts the remaining kernels.
 __global__ void k_dt_finalize(GamScalars* sc) {
     if (sc->halted) return;
+    sc->ootime = sc->otime;        // CopyState(oState, ooState) (mhdgroup.F90:100-102)
     sc->otime = sc->time;          // CopyState (mhdgroup.F90:255)
     sc->time = sc->time + sc->dt;  // mhdgroup.F90:106
     sc->ts = sc->ts + 1;
@@ -1335,10 +1389,13 @@ template <class R, class F> void for_each_kernel(const Ctx<R>& C, int cur, cudaS
     f(0, [&] { k_step_begin<<<1, 1, 0, s>>>(C.sc); });
     const dim3 pblk(32, 8, 1);
     f(1, [&] {
-        if (C.kvar & 8)
-            k_predict<R, 1><<<grid_for(all, pblk), pblk, 0, s>>>(b, C.P, C.g, S, O, C.w, C.sc);
+        if (C.P.doAB3)
+            k_predict<R, sizeof(R) == 8 ? 3 : 4, true><<<grid_for(all, pblk), pblk, 0, s>>>(b, C.P, C.g, S, O, C.w, C.sc,
+                                                                                          C.oomf);
+        else if (C.kvar & 8)
+            k_predict<R, 1><<<grid_for(all, pblk), pblk, 0, s>>>(b, C.P, C.g, S, O, C.w, C.sc, nullptr);
         else
-            k_predict<R, sizeof(R) == 8 ? 3 : 4><<<grid_for(all, pblk), pblk, 0, s>>>(b, C.P, C.g, S, O, C.w, C.sc);
+            k_predict<R, sizeof(R) == 8 ? 3 : 4><<<grid_for(all, pblk), pblk, 0, s>>>(b, C.P, C.g, S, O, C.w, C.sc, nullptr);
     });
     if (C.P.doMHD) {
         const Range mf[3] = {{0, b.Ni - 1, G, G + b.Njp, 0, b.Nk - 1},
@@ -1381,7 +1438,7 @@ template <class R, class F> void for_each_kernel(const Ctx<R>& C, int cur, cudaS
     f(8, [&] { stress(std::integral_constant<int, 0>()); });
     f(9, [&] { stress(std::integral_constant<int, 1>()); });
     if (!C.P.do25D) f(10, [&] { stress(std::integral_constant<int, 2>()); });
-    f(11, [&] { k_update_faces<R><<<grid_for(all, blk), blk, 0, s>>>(b, C.P, S, O, C.w, C.sc); });
+    f(11, [&] { k_update_faces<R><<<grid_for(all, blk), blk, 0, s>>>(b, C.P, S, O, C.w, C.sc, C.oomf); });
     f(12, [&] {
         if (C.P.doBoris)
             k_update_cells<R, sizeof(R) == 8 ? 6 : 8, true><<<grid_for(cells, blk), blk, 0, s>>>(b, C.P, C.g, S, O, C.w, C.sc, C.gamma, C.gm1);
@@ -1494,6 +1551,7 @@ template <class R> void launch_init(const Ctx<R>& C, int cur, cudaStream_t s) {
     cudaMemcpyAsync(O.Gas, S.Gas, 5 * b.fs * sizeof(R), cudaMemcpyDeviceToDevice, s);
     cudaMemcpyAsync(O.mf, S.mf, 3 * b.fs * sizeof(R), cudaMemcpyDeviceToDevice, s);
     cudaMemcpyAsync(O.B, S.B, 3 * b.fs * sizeof(R), cudaMemcpyDeviceToDevice, s);
+    if (C.oomf) cudaMemcpyAsync(C.oomf, S.mf, 3 * b.fs * sizeof(R), cudaMemcpyDeviceToDevice, s);  // ooState = State
 }
 
 // ----------------------------------------------------------------- k-slab tiling

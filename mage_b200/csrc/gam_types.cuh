@@ -21,6 +21,7 @@ template <class R> struct DevParams {
     int doMHD, doLFMLim, do25D, doBackground, up7;
     int doBoris;  // Boris correction with the speed of light Ca (init.F90:417-423)
     double Ca;
+    int doAB3;    // third-order (AB3) predictor with ooState (init.F90:377)
     int bc[6];
     // CalcDT covers the ghost layer below / above the active k range (1, the
     // reference's isDT..ieDT); a k-slab drops it where a neighbour's cells lie
@@ -84,6 +85,7 @@ template <class R> struct Ctx {
     DevParams<R> P;
     Geo<R> g;
     StateBuf<R> st[2];   // double buffer: st[cur] = State (n), st[1-cur] = oState (n-1) -> State (n+1)
+    R* oomf;             // doAB3: ooState face fluxes (n-2), refreshed from oState by k_update_faces
     Work<R> w;
     GamScalars* sc;
     double gamma, gm1;

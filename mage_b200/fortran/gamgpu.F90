@@ -23,6 +23,7 @@ module gamgpu
         integer(c_int32_t) :: bc(6)
         integer(c_int32_t) :: doBoris
         real(c_double) :: Ca
+        integer(c_int32_t) :: doAB3
     end type gam_params
 
     interface
@@ -116,6 +117,19 @@ module gamgpu
             import :: c_int, c_ptr, c_double
             type(c_ptr), value :: h
             real(c_double), intent(in) :: state(8)
+        end function
+        ! ooState of the AB3 predictor (doAB3): magFlux(isg:ieg+1,jsg:jeg+1,ksg:keg+1,1:3) and time
+        integer(c_int) function gam_set_oostate(h, oomagFlux, ootime) bind(C, name="gam_set_oostate")
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: h
+            real(c_double), intent(in) :: oomagFlux(*)
+            real(c_double), value :: ootime
+        end function
+        integer(c_int) function gam_get_oostate(h, oomagFlux, ootime) bind(C, name="gam_get_oostate")
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: h
+            real(c_double), intent(out) :: oomagFlux(*)
+            real(c_double), intent(out) :: ootime
         end function
         ! k-slab tiling: the MPI driver (gamAppMpi_T) packs/unpacks halos in
         ! device buffers and reduces dt between gam_step_begin and gam_step_end

@@ -44,7 +44,7 @@ class _Params(C.Structure):
         ("tFin", C.c_double), ("dt0", C.c_double), ("limDT0", C.c_double), ("fixedTimestep", C.c_double),
         ("rmeth", C.c_int32), ("doLFMLim", C.c_int32), ("doMHD", C.c_int32), ("doBackground", C.c_int32),
         ("do25D", C.c_int32), ("precision", C.c_int32), ("strict", C.c_int32), ("bc", C.c_int32 * 6),
-        ("doBoris", C.c_int32), ("Ca", C.c_double),
+        ("doBoris", C.c_int32), ("Ca", C.c_double), ("doAB3", C.c_int32),
     ]
 
 
@@ -53,7 +53,7 @@ EXPORTED = (
     "gam_set_geometry_arrays", "gam_get_geometry_arrays", "gam_upload_state", "gam_download_state", "gam_step",
     "gam_calc_dt", "gam_divb", "gam_totals", "gam_last_step_ms", "gam_advance_model", "gam_init_orszag_tang",
     "gam_init_blast_wave", "gam_profile_step", "gam_totals_noalloc", "gam_set_background", "gam_get_background",
-    "gam_set_background_dipole", "gam_set_wind", "gam_set_inflow", "gam_init_dipole_wind", "gam_write_restart", "gam_read_restart",
+    "gam_set_background_dipole", "gam_set_wind", "gam_set_inflow", "gam_set_oostate", "gam_get_oostate", "gam_init_dipole_wind", "gam_write_restart", "gam_read_restart",
     "gam_halo_bytes", "gam_halo_pack", "gam_halo_unpack", "gam_init_finish_halo", "gam_set_start", "gam_step_begin",
     "gam_dt_partial", "gam_step_end", "gam_set_slab_edges", "gam_flux_forward", "gam_flux_adjoint",
     "gam_efield_forward", "gam_efield_adjoint", "gam_predict_stage", "gam_update_stage",
@@ -99,6 +99,8 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     L.gam_set_background_dipole.argtypes = [C.c_void_p, C.c_double]
     L.gam_set_wind.argtypes = [C.c_void_p, _dp]
     L.gam_set_inflow.argtypes = [C.c_void_p, _dp]
+    L.gam_set_oostate.argtypes = [C.c_void_p, _dp, C.c_double]
+    L.gam_get_oostate.argtypes = [C.c_void_p, _dp, _dp]
     L.gam_write_restart.argtypes = [C.c_void_p, C.c_char_p]
     L.gam_halo_bytes.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
     L.gam_set_slab_edges.argtypes = [C.c_void_p, C.c_int32, C.c_int32]
@@ -160,6 +162,7 @@ class GamParams:
     bc: tuple = field(default_factory=lambda: (BC_PERIODIC,) * 6)
     doBoris: bool = False
     Ca: float = 1.0e12
+    doAB3: bool = False
 
     def to_c(self) -> _Params:
         p = _Params()
@@ -248,6 +251,18 @@ class GameraGPU:
             assert a.shape == s, (a.shape, s)
         ptrs = [_ptr(a) for a in arrs] + ([None, None] if keep_old else [])
         self._check(self.L.gam_upload_state(self.h, *ptrs, time, otime, dt, int(ts)))
+
+    def set_oostate(self, oomagFlux, ootime: float):
+        """ooState face fluxes and time of the AB3 predictor (doAB3)."""
+        a = np.ascontiguousarray(oomagFlux, dtype=np.float64)
+        assert a.shape == self.shape("face", 3), a.shape
+        self._check(self.L.gam_set_oostate(self.h, _ptr(a), float(ootime)))
+
+    def get_oostate(self) -> dict:
+        a = np.zeros(self.shape("face", 3))
+        t = C.c_double()
+        self._check(self.L.gam_get_oostate(self.h, _ptr(a), C.byref(t)))
+        return {"oomagFlux": a, "ootime": t.value}
 
     def download_state(self, into: dict | None = None, old: bool = True) -> dict:
         """State (and with ``old`` the previous state) in Fortran layout;

@@ -176,3 +176,27 @@ def test_boris_limits(oracle_built):
     m0 = a.array("Gas")[0][act[1:]].sum()
     assert abs(gc[0][act[1:]].sum() - m0) <= 1e-12 * m0
     assert c.divb() <= 1e-12 * np.abs(c.array("magFlux")).sum()
+
+
+def test_ab3_predictor(oracle_built):
+    """AB3 (mhdgroup.F90:444-517, 721-731) in the oracle: its first step from
+    the start (State = oState = ooState) equals AB2's bit for bit, later steps
+    differ at the scheme's truncation level, and ooState trails oState by one
+    step in time."""
+    N = (16, 16, 16)
+    xyz = grids.warped_periodic_corners(*N)
+
+    def run(nst, **kw):
+        o = orc.Oracle(orc.OracleParams(*N, **kw), xyz, "strict")
+        o.ic_blast_wave()
+        assert o.init_finish() == 0
+        assert o.step(nst) == 0
+        return o
+
+    a1, b1 = run(1), run(1, doAB3=True)
+    assert np.array_equal(a1.array("Gas"), b1.array("Gas"))
+    a, b = run(10), run(10, doAB3=True)
+    d = float(np.linalg.norm(b.array("Gas") - a.array("Gas")) / np.linalg.norm(a.array("Gas")))
+    assert 0 < d < 1e-2, d
+    sc = b.scalars()
+    assert sc["ootime"] < sc["otime"] < sc["time"]
