@@ -34,7 +34,8 @@ enum {
     GAM_EDT_BAD = 4,       /* dt dropped 10x or below limDT0 (step.F90:111-128) */
     GAM_EDT_DISASTER = 5,  /* dt <= TINY or no finite dt (step.F90:102-105,131-134) */
     GAM_ESTATE = 6,        /* call out of order (e.g. step before geometry) */
-    GAM_EHOOK = 7          /* a Model%Hack* hook is set: not supported on the GPU */
+    GAM_EHOOK = 7,         /* a Model%Hack* hook is set: not supported on the GPU */
+    GAM_EBOUNDS = 8        /* bounds-check build only: a kernel's index check failed */
 };
 
 /* Boundary kinds (EnforceBCs, step.F90:17-55). Per side: INI periodic, none,
@@ -195,6 +196,17 @@ int gam_set_inflow(gam_handle* h, const double state[8]);
  * a driver that holds ooState passes it here afterwards. The initial
  * conditions set ooState = State at time otime - dt (init.F90:232-241). */
 int gam_set_oostate(gam_handle* h, const double* oomagFlux, double ootime);
+
+/* Bounds-check build (libgamgpu_check.so, compiled with -DGAM_BOUNDS_CHECK):
+ * every kernel checks the lowest and highest box index its stencils touch
+ * before any load, and a failed check records the kernel (its position in the
+ * step: 1 predictor, 2-7 Mom2Face/VxB, 8-10 fluxes, 11-12 update, 13 dt, 14
+ * boundaries, 15 halo, 16 other) and the index, skips the access and makes
+ * gam_step / gam_step_end / gam_calc_dt return GAM_EBOUNDS. Its device arrays
+ * start filled with NaN (all bits set) instead of zeros, so a read of memory
+ * nothing wrote shows up in the results. fired: 1 a check failed, 0 none,
+ * -1 this library was built without the checks. */
+int gam_bounds_status(gam_handle* h, int32_t* fired, int32_t* kernel, int64_t* index);
 int gam_get_oostate(gam_handle* h, double* oomagFlux, double* ootime);
 
 /* Dipole-in-wind start: the wind state in every active cell with the density

@@ -219,7 +219,7 @@ __global__ void __launch_bounds__(128) k_stress_adj(GamBox b, DevParams<R> P, Ge
     for (int v = 0; v < 5; v++) {
         for (int n = 0; n < 8; n++) qW[v][n] = w.QW[v * fs + c + (n - 4) * s];
         for (int m = 0; m < 4; m++) nW[v][m] = w.Wn[v * fs + c + (m - 2) * s];
-        lrs_from_qdv(P, qW[v], nW[v], Vi, WL[v], WR[v]);
+        lrs_from_qdv(P, qW[v], nW[v], Quot<R>(Vi), WL[v], WR[v]);
     }
     R Bn = (R)0;
     double B0[3] = {0.0, 0.0, 0.0}, B0n = 0.0;
@@ -228,7 +228,7 @@ __global__ void __launch_bounds__(128) k_stress_adj(GamBox b, DevParams<R> P, Ge
         for (int x = 0; x < 3; x++) {
             for (int n = 0; n < 8; n++) qB[x][n] = w.QB[x * fs + c + (n - 4) * s];
             for (int m = 0; m < 4; m++) nB[x][m] = Blim[x * fs + c + (m - 2) * s];
-            lrs_from_qdv(P, qB[x], nB[x], Vi, MagL[x], MagR[x]);
+            lrs_from_qdv(P, qB[x], nB[x], Quot<R>(Vi), MagL[x], MagR[x]);
         }
         if (P.doBackground) {
             for (int x = 0; x < 3; x++) B0[x] = g.fcB0[(x + 3 * D) * fs + c];

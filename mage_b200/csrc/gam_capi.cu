@@ -1,6 +1,7 @@
 // C ABI of the GAMERA step (include/gamgpu.h): handle, device memory, layout
 // conversion, step sequencing with CUDA graphs, diagnostics.
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -114,7 +115,11 @@ template <class T> static T* dalloc(gam_handle* h, long n, cudaError_t* e) {
     *e = cudaMalloc(&p, sizeof(T) * (size_t)n);
     if (*e == cudaSuccess) {
         h->allocs.push_back(p);
+#ifdef GAM_BOUNDS_CHECK
+        cudaMemsetAsync(p, 0xFF, sizeof(T) * (size_t)n, h->s);  // NaN canaries
+#else
         cudaMemsetAsync(p, 0, sizeof(T) * (size_t)n, h->s);
+#endif
     }
     return (T*)p;
 }
@@ -173,6 +178,15 @@ template <class R> static int alloc_bulk(gam_handle* h, Ctx<R>& C) {
     A(C.w.QW, 5); A(C.w.QB, 3); A(C.w.Dh, 1); A(C.w.Wn, 5); A(C.w.Bl, 3); A(C.w.VdV, 3);
     A(C.w.abh, 3); A(C.w.bn, 3); A(C.w.Bnf, 3); A(C.w.AVf, 9); A(C.w.E, 3);
     A(C.w.gF, 15); A(C.w.mF, 9);
+    // CalcElecField starts from E = 0 (fields.F90:88) and E2Flux
+    // (fields.F90:37-46) reads edges next to the computed ones, which stay
+    // zero; the edge kernels never write them, so E is zeroed once here, also
+    // in the bounds-check build whose other arrays start as NaN canaries
+    CK(h, cudaMemsetAsync(C.w.E, 0, 3 * fs * sizeof(R), h->s));
+    // a 2.5-D grid computes no K fluxes, and Flux2Deltas (stress.F90:150-190)
+    // still adds their difference: zero, as the solver's arrays start
+    CK(h, cudaMemsetAsync(C.w.gF, 0, 15 * fs * sizeof(R), h->s));
+    CK(h, cudaMemsetAsync(C.w.mF, 0, 9 * fs * sizeof(R), h->s));
     C.oomf = nullptr;
     if (h->p.doAB3) A(C.oomf, 3);
     if (sizeof(R) == sizeof(double)) {
@@ -302,6 +316,11 @@ extern "C" int gam_create(const gam_params* p, gam_handle** out) {
     s0.dt = p->fixedTimestep > 0 ? p->fixedTimestep : 0.0;
     double hugedt = 1.0e12;
     memcpy(&s0.dtmin_bits, &hugedt, 8);
+#ifdef GAM_BOUNDS_CHECK
+    // test hook: a smaller index limit than the box makes the checks fire on
+    // in-bounds indices, so the reporting path can be exercised safely
+    if (const char* lim = getenv("GAM_BOUNDS_LIMIT")) s0.oobLimit = atoll(lim);
+#endif
     if (cudaMemcpyAsync(h->sc, &s0, sizeof(s0), cudaMemcpyHostToDevice, h->s) != cudaSuccess ||
         cudaStreamSynchronize(h->s) != cudaSuccess)
         return bad(GAM_ECUDA, "initialisation copy failed");
@@ -580,6 +599,39 @@ static int ensure_graph(gam_handle* h, int cur) {
     return GAM_OK;
 }
 
+// After a synchronised call: GAM_EBOUNDS if a kernel's index check failed
+// (bounds-check build; the record stays until the handle is destroyed)
+static int check_bounds(gam_handle* h, const GamScalars& s) {
+#ifdef GAM_BOUNDS_CHECK
+    if (s.oob) {
+        char msg[160];
+        snprintf(msg, sizeof(msg), "bounds check failed in kernel %d at box index %lld", s.oobKernel, s.oobIndex);
+        return fail(h, GAM_EBOUNDS, msg);
+    }
+#else
+    (void)h;
+    (void)s;
+#endif
+    return GAM_OK;
+}
+
+extern "C" int gam_bounds_status(gam_handle* h, int32_t* fired, int32_t* kernel, int64_t* index) {
+    if (!h || !fired) return GAM_EINVAL;
+#ifdef GAM_BOUNDS_CHECK
+    GamScalars s;
+    CK(h, cudaMemcpyAsync(&s, h->sc, sizeof(s), cudaMemcpyDeviceToHost, h->s));
+    CK(h, cudaStreamSynchronize(h->s));
+    *fired = s.oob ? 1 : 0;
+    if (kernel) *kernel = s.oob ? s.oobKernel : 0;
+    if (index) *index = s.oob ? s.oobIndex : 0;
+#else
+    *fired = -1;
+    if (kernel) *kernel = 0;
+    if (index) *index = 0;
+#endif
+    return GAM_OK;
+}
+
 extern "C" int gam_step(gam_handle* h, int32_t nsteps, double* dt, double* t) {
     if (!h || nsteps < 0) return GAM_EINVAL;
     if (!h->haveGeo) return fail(h, GAM_ESTATE, "gam_step before gam_set_geometry");
@@ -599,9 +651,12 @@ extern "C" int gam_step(gam_handle* h, int32_t nsteps, double* dt, double* t) {
     if (s.halted)
         return fail(h, s.status == 5 ? GAM_EDT_DISASTER : GAM_EDT_BAD, "a previous step failed CalcDT; upload a state");
     const int ts0 = s.ts, cur0 = h->cur;
+    // host-side range with the reference's priority clock label (gamapp.F90:96-99)
+    nvtxRangePushA("Gamera");
     CK(h, cudaEventRecord(h->ev0, h->s));
     for (int n = 0; n < nsteps; n++) CK(h, cudaGraphLaunch(h->graph[(cur0 + n) & 1], h->s));
     CK(h, cudaEventRecord(h->ev1, h->s));
+    nvtxRangePop();
     CK(h, cudaMemcpyAsync(&s, h->sc, sizeof(s), cudaMemcpyDeviceToHost, h->s));
     CK(h, cudaStreamSynchronize(h->s));
     float ms = 0.f;
@@ -612,6 +667,7 @@ extern "C" int gam_step(gam_handle* h, int32_t nsteps, double* dt, double* t) {
     h->cur = (cur0 + (s.ts - ts0)) & 1;
     if (dt) *dt = s.dt;
     if (t) *t = s.t;
+    if (int rcb = check_bounds(h, s)) return rcb;
     if (s.halted)
         return fail(h, s.status == 5 ? GAM_EDT_DISASTER : GAM_EDT_BAD,
                     s.status == 5 ? "CalcDT: timestep too small or not finite" : "CalcDT: timestep dropped 10x or below limDT0");
@@ -715,6 +771,9 @@ extern "C" int gam_calc_dt(gam_handle* h, double* dt) {
     CK(h, cudaStreamSynchronize(h->s));
     double dtMin;
     memcpy(&dtMin, &bits, 8);
+    CK(h, cudaMemcpyAsync(&s, h->sc, sizeof(s), cudaMemcpyDeviceToHost, h->s));
+    CK(h, cudaStreamSynchronize(h->s));
+    if (int rcb = check_bounds(h, s)) return rcb;
     // step.F90:158-166 clamps (the ts > 0 failure checks belong to a step)
     double d = dtMin;
     if (s.t + d > s.tFin) d = (s.tFin - s.t) > 1.0e-12 ? (s.tFin - s.t) : 1.0e-12;
@@ -1183,6 +1242,7 @@ extern "C" int gam_step_end(gam_handle* h, uint64_t dtmin_bits, int32_t nbad, do
     h->cur ^= 1;
     if (dt) *dt = s.dt;
     if (t) *t = s.t;
+    if (int rcb = check_bounds(h, s)) return rcb;
     if (s.halted)
         return fail(h, s.status == 5 ? GAM_EDT_DISASTER : GAM_EDT_BAD,
                     s.status == 5 ? "CalcDT: timestep too small or not finite" : "CalcDT: timestep dropped 10x or below limDT0");

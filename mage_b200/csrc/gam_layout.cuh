@@ -44,4 +44,9 @@ struct GamScalars {
     int fixedTimestep;
     int nbad;                          // cells whose dt is not a finite positive number
     double ootime, oodt;               // ooState time and oState - ooState spacing (doAB3)
+    // bounds-check build (GAM_BOUNDS_CHECK): first failed index check
+    int oob;                           // 1 once a check failed
+    int oobKernel;                     // for_each_kernel id (15: halo, 16: other)
+    long long oobIndex;                // the offending linear box index
+    long long oobLimit;                // indices must be < this (0: the box size)
 };

@@ -2,6 +2,7 @@
 // and FP32 precision form.
 #define GAM_NS gam_fast
 #define GAM_CUDA_MATH 1
+#define GAM_FAST_RECIP 1  // shared divisors as one reciprocal (Quot)
 #include "gam_step_impl.cuh"
 
 void gam_fast_step_f64(const Ctx<double>& C, int cur, cudaStream_t s) { gam_fast::launch_step<double>(C, cur, s); }

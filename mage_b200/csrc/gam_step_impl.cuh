@@ -30,6 +30,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 #include <stdint.h>
 #include <type_traits>
 #include "gam_layout.cuh"
@@ -92,6 +93,22 @@ template <> struct Mth<float> {
     static __device__ __forceinline__ float sqrt_(float x) { return sqrtf(x); }
 };
 
+// Quotients a/d that share the divisor d. The product build (GAM_FAST_RECIP)
+// takes one reciprocal and multiplies (at most one ulp more than the division,
+// and a fraction of its instructions); every other build divides, so the
+// strict kernels keep the reference's IEEE operations.
+template <class R> struct Quot {
+#ifdef GAM_FAST_RECIP
+    R r;
+    __device__ __forceinline__ explicit Quot(R d) : r((R)1 / d) {}
+    __device__ __forceinline__ R operator()(R a) const { return a * r; }
+#else
+    R d;
+    __device__ __forceinline__ explicit Quot(R dd) : d(dd) {}
+    __device__ __forceinline__ R operator()(R a) const { return a / d; }
+#endif
+};
+
 // std::max / std::min semantics: max(a,b) = (a < b) ? b : a, min(a,b) = (b < a) ? b : a
 template <class R> __device__ __forceinline__ R rmax(R a, R b) { return (a < b) ? b : a; }
 template <class R> __device__ __forceinline__ R rmin(R a, R b) { return (b < a) ? b : a; }
@@ -144,12 +161,13 @@ template <class R> __device__ __forceinline__ R central8(const R* q) {
 // weighted stencil QdV[0..7] = dV*Q at cells -4..3 (precomputed per cell),
 // limiter nq[0..3] at cells -2..1, and the volume interpolant Vi.
 template <class R>
-__device__ __forceinline__ void lrs_from_qdv(const DevParams<R>& P, const R* QdV, const R* nq, R Vi, R& Ql, R& Qr) {
+__device__ __forceinline__ void lrs_from_qdv(const DevParams<R>& P, const R* QdV, const R* nq, const Quot<R>& Vi, R& Ql,
+                                             R& Qr) {
     if (!P.up7) {
         R s = (R)0;
 #pragma unroll
         for (int n = 0; n < 8; n++) s += Rc<R>(w8(n)) * QdV[n];
-        R Qi = s / Vi;
+        R Qi = Vi(s);
         pdm_lr(P.pdmb, nq, Qi, Ql, Qr);
     } else {
         R a = QdV[0] * Rc<R>(up7c(0));
@@ -158,8 +176,8 @@ __device__ __forceinline__ void lrs_from_qdv(const DevParams<R>& P, const R* QdV
         R b = QdV[7] * Rc<R>(up7c(0));
 #pragma unroll
         for (int n = 1; n < 7; n++) b = b + QdV[7 - n] * Rc<R>(up7c(n));
-        Ql = a / Vi;
-        Qr = b / Vi;
+        Ql = Vi(a);
+        Qr = Vi(b);
         Ql = pdm1(P.pdmb, nq[0], nq[1], nq[2], Ql);
         Qr = pdm1(P.pdmb, nq[3], nq[2], nq[1], Qr);
     }
@@ -170,20 +188,22 @@ __device__ __forceinline__ void lrs_from_qdv(const DevParams<R>& P, const R* QdV
 template <class R>
 __device__ __forceinline__ void block_c2p(const DevParams<R>& P, const R* U, R* W) {
     R D = rmax(U[0], P.dFloor);
+    const Quot<R> qD(D);
     R Mx = U[1], My = U[2], Mz = U[3], E = U[4];
-    R KinE = (R)0.5 * (Mx * Mx + My * My + Mz * Mz) / D;
+    R KinE = qD((R)0.5 * (Mx * Mx + My * My + Mz * Mz));
     R Pr = rmax(P.gm1 * (E - KinE), P.pFloor);
     W[0] = D;
-    W[1] = Mx / D;
-    W[2] = My / D;
-    W[3] = Mz / D;
+    W[1] = qD(Mx);
+    W[2] = qD(My);
+    W[3] = qD(Mz);
     W[4] = Pr;
 }
 // CellC2P (gamutils.F90:301-321)
 template <class R>
 __device__ __forceinline__ void cell_c2p(const DevParams<R>& P, const R* U, R* W) {
     R rho = U[0];
-    R Vx = U[1] / rho, Vy = U[2] / rho, Vz = U[3] / rho;
+    const Quot<R> qr(rho);
+    R Vx = qr(U[1]), Vy = qr(U[2]), Vz = qr(U[3]);
     R E = U[4];
     R KinE = (R)0.5 * rho * (Vx * Vx + Vy * Vy + Vz * Vz);
     W[0] = rmax(rho, P.dFloor);
@@ -232,13 +252,14 @@ __device__ __forceinline__ double norm2s3(const double* a) {
 // PredictCell (mhdgroup.F90:528-562, AB2, single fluid): the half-step
 // conserved state from State n (Q) and n-1 (oQ)
 template <class R>
-__device__ __forceinline__ void predict_cell(const DevParams<R>& P, const R* Q, const R* oQ, R pdt, R odt, R* pQ) {
+__device__ __forceinline__ void predict_cell(const DevParams<R>& P, const R* Q, const R* oQ, R pdt, const Quot<R>& odt,
+                                             R* pQ) {
     R W[5], oW[5], pW[5];
     cell_c2p(P, oQ, oW);
     cell_c2p(P, Q, W);
 #pragma unroll
     for (int v = 0; v < 5; v++) {
-        R dQ = (W[v] - oW[v]) / odt;
+        R dQ = odt(W[v] - oW[v]);
         pW[v] = W[v] + pdt * dQ;
     }
     pW[0] = rmax(pW[0], P.dFloor);
@@ -279,6 +300,7 @@ __device__ __forceinline__ void cell_bxyz(const GamBox& b, const Geo<R>& g, long
                                           R fKp, R* B) {
     const long fs = b.fs;
     R dV = g.vol[c];
+    const Quot<R> qV(dV);
     if constexpr (std::is_same<R, float>::value) {
         // sum of flux x (face centroid - cell centroid): the same value as the
         // form below, without the cancellation of absolute coordinates
@@ -286,7 +308,7 @@ __device__ __forceinline__ void cell_bxyz(const GamBox& b, const Geo<R>& g, long
         for (int x = 0; x < 3; x++) {
             const R* d = g.dxf + (long)x * fs + c;
             R t = fIp * d[3 * fs] + fJp * d[9 * fs] + fKp * d[15 * fs] - fI * d[0] - fJ * d[6 * fs] - fK * d[12 * fs];
-            B[x] = t / dV;
+            B[x] = qV(t);
         }
         return;
     }
@@ -299,10 +321,38 @@ __device__ __forceinline__ void cell_bxyz(const GamBox& b, const Geo<R>& g, long
         R xfIp = g.xfc[(x + 0) * fs + c + 1];
         R xfJp = g.xfc[(x + 3) * fs + c + b.sx];
         R xfKp = g.xfc[(x + 6) * fs + c + b.sk];
-        R t = (fIp * xfIp + fJp * xfJp + fKp * xfKp - fI * xfI - fJ * xfJ - fK * xfK) / dV;
-        B[x] = t - Div * g.xyzcc[x * fs + c] / dV;
+        R t = qV(fIp * xfIp + fJp * xfJp + fKp * xfKp - fI * xfI - fJ * xfJ - fK * xfK);
+        B[x] = t - qV(Div * g.xyzcc[x * fs + c]);
     }
 }
+
+// ----------------------------------------------------------------- bounds checks
+// Built with -DGAM_BOUNDS_CHECK (libgamgpu_check.so): every kernel checks the
+// lowest and highest linear box index its stencils will touch before loading
+// anything; a failed check records the kernel and the index in the scalars
+// and the thread returns without touching memory (no trap). The host reads
+// the record after the call. Without the macro the checks compile to nothing.
+#ifdef GAM_BOUNDS_CHECK
+__device__ __forceinline__ bool box_ok(const GamBox& b, long lo, long hi, const GamScalars* csc, int kid) {
+    GamScalars* sc = const_cast<GamScalars*>(csc);
+    const long lim = sc->oobLimit > 0 ? (long)sc->oobLimit : b.nbox;
+    if (lo >= 0 && hi < lim) return true;
+    if (atomicExch(&sc->oob, 1) == 0) {
+        sc->oobKernel = kid;
+        sc->oobIndex = lo < 0 ? lo : hi;
+    }
+    return false;
+}
+#define GAM_BOX_CHECK(lo, hi, kid) \
+    if (!box_ok(b, (long)(lo), (long)(hi), sc, (kid))) return
+// for kernels whose threads must reach a later barrier: a value, not a return
+#define GAM_BOX_OK(lo, hi, kid) box_ok(b, (long)(lo), (long)(hi), sc, (kid))
+#else
+#define GAM_BOX_OK(lo, hi, kid) true
+#define GAM_BOX_CHECK(lo, hi, kid) \
+    do {                           \
+    } while (0)
+#endif
 
 // ----------------------------------------------------------------- kernels
 // AdvanceMHD entry: time trap and AB2 spacing (mhdgroup.F90:25-31, 457)
@@ -331,6 +381,7 @@ __global__ void __launch_bounds__(256, MINB) k_predict(GamBox b, DevParams<R> P,
     const long c = lidx(b, ii, jj, kk);
     const R pdt = (R)sc->pdt, odt = (R)sc->odt;
     const bool isCell = ii < b.Ni && jj < b.Nj && kk < b.Nk;
+    GAM_BOX_CHECK(c, isCell ? c + b.sk : c, 1);
     // The state and work pointers may alias as far as the compiler knows, so
     // every state load is issued before the first store.
     R fQ[3], foQ[3], fA[3], Q[5], oQ[5], uQ[3], uoQ[3];
@@ -361,6 +412,7 @@ __global__ void __launch_bounds__(256, MINB) k_predict(GamBox b, DevParams<R> P,
         }
     }
     R hm[3];
+    const Quot<R> qodt(odt);
     [[maybe_unused]] R oodt = (R)0;
     if constexpr (AB3) oodt = (R)sc->oodt;
     if (P.doMHD) {
@@ -369,15 +421,16 @@ __global__ void __launch_bounds__(256, MINB) k_predict(GamBox b, DevParams<R> P,
             if constexpr (AB3) {
                 hm[d] = extrap_ab3(pdt, fQ[d], foQ[d], fooQ[d], odt, oodt);
             } else {
-                R dQ = (fQ[d] - foQ[d]) / odt;
+                R dQ = qodt(fQ[d] - foQ[d]);
                 hm[d] = fQ[d] + pdt * dQ;  // ExtrapAB2
             }
             R A = fA[d];
             R Am = rmax(A, (R)TINY);
-            R bh = hm[d] / Am;
+            const Quot<R> qAm(Am);
+            R bh = qAm(hm[d]);
             w.abh[d * fs + c] = A * bh;
             w.Bnf[d * fs + c] = hm[d] / A;
-            w.bn[d * fs + c] = P.doLFMLim ? fQ[d] / Am : bh;
+            w.bn[d * fs + c] = P.doLFMLim ? qAm(fQ[d]) : bh;
         }
     }
     if (!isCell) return;
@@ -385,7 +438,7 @@ __global__ void __launch_bounds__(256, MINB) k_predict(GamBox b, DevParams<R> P,
     if constexpr (AB3)
         predict_cell_ab3(P, Q, oQ, pdt, odt, oodt, pQ);
     else
-        predict_cell(P, Q, oQ, pdt, odt, pQ);
+        predict_cell(P, Q, oQ, pdt, qodt, pQ);
     R Wh[5], Wn[5];
     block_c2p(P, pQ, Wh);
     if (P.doLFMLim) block_c2p(P, Q, Wn);
@@ -397,8 +450,9 @@ __global__ void __launch_bounds__(256, MINB) k_predict(GamBox b, DevParams<R> P,
     }
     w.Dh[c] = Wh[0];
     const R Dm = rmax(pQ[0], P.dFloor);
+    const Quot<R> qDm(Dm);
 #pragma unroll
-    for (int x = 0; x < 3; x++) w.VdV[x * fs + c] = vol * pQ[1 + x] / Dm;
+    for (int x = 0; x < 3; x++) w.VdV[x * fs + c] = qDm(vol * pQ[1 + x]);
     if (P.doMHD) {
         // upper faces of this cell, recomputed with the same ExtrapAB2
         R up[3];
@@ -407,7 +461,7 @@ __global__ void __launch_bounds__(256, MINB) k_predict(GamBox b, DevParams<R> P,
             if constexpr (AB3) {
                 up[d] = extrap_ab3(pdt, uQ[d], uoQ[d], uooQ[d], odt, oodt);
             } else {
-                R dQ = (uQ[d] - uoQ[d]) / odt;
+                R dQ = qodt(uQ[d] - uoQ[d]);
                 up[d] = uQ[d] + pdt * dQ;
             }
         }
@@ -441,10 +495,12 @@ __global__ void __launch_bounds__(256) k_mom2face(GamBox b, DevParams<R> P, Geo<
     const long fs = b.fs;
     const long c = lidx(b, ii, jj, kk);
     const long s = dstride(b, dT1);
+    GAM_BOX_CHECK(c - 4 * s, c + 3 * s, 2 + 2 * eD);
     R vol[8];
 #pragma unroll
     for (int n = 0; n < 8; n++) vol[n] = g.vol[c + (n - 4) * s];
     R dV = rmax(central8(vol), (R)TINY);
+    const Quot<R> qdV(dV);
     const R A = g.face[dT1 * fs + c];
     R out[3];
 #pragma unroll
@@ -452,7 +508,7 @@ __global__ void __launch_bounds__(256) k_mom2face(GamBox b, DevParams<R> P, Geo<
         R q[8];
 #pragma unroll
         for (int n = 0; n < 8; n++) q[n] = w.VdV[x * fs + c + (n - 4) * s];
-        out[x] = A * (central8(q) / dV);
+        out[x] = A * qdV(central8(q));
     }
 #pragma unroll
     for (int x = 0; x < 3; x++) w.AVf[(x + 3 * eD) * fs + c] = out[x];
@@ -473,7 +529,7 @@ __device__ __forceinline__ void edge_lrs(const GamBox& b, const DevParams<R>& P,
 #pragma unroll
     for (int m = 0; m < 4; m++) nmag[m] = w.bn[a * fs + c + (m - 2) * s];
     const R Vi = central8(area);
-    lrs_from_qdv(P, qdv, nmag, Vi, bL, bR);
+    lrs_from_qdv(P, qdv, nmag, Quot<R>(Vi), bL, bR);
     fA = Vi;  // dot_product(interpWgt, AreaB) again: the same value
     bL = bL * fA;
     bR = bR * fA;
@@ -493,6 +549,11 @@ __global__ void __launch_bounds__(128, MINB) k_vxb(GamBox b, DevParams<R> P, Geo
     // GetCornerD (fields.F90:427-454): normal-plane unit offsets e1 < e2
     const int e1 = eD == 0 ? 1 : 0, e2 = eD == 2 ? 1 : 2;
     const long s1 = dstride(b, e1), s2 = dstride(b, e2);
+    {
+        const long sA = dstride(b, dT1), sB = dstride(b, dT2), sM = sA > sB ? sA : sB;
+        [[maybe_unused]] const long lo = c - s1 - s2 < c - 4 * sM ? c - s1 - s2 : c - 4 * sM;
+        GAM_BOX_CHECK(lo, c + 3 * sM, 3 + 2 * eD);
+    }
     R Dc = (R)0.25 * (w.Dh[c] + w.Dh[c - s1] + w.Dh[c - s2] + w.Dh[c - s1 - s2]);
     // GetCornerB: EdgeLRs for dT1 faces along dT2 and dT2 faces along dT1
     R area1[8], area2[8];
@@ -501,6 +562,7 @@ __global__ void __launch_bounds__(128, MINB) k_vxb(GamBox b, DevParams<R> P, Geo
     edge_lrs(b, P, g, w, c, dT2, dT1, area2, bT2L, bT2R, fA2);
     // GetCornerV (fields.F90:457-517); its area stencil equals area1
     R dA = rmax(fA1, (R)TINY);
+    const Quot<R> qdA(dA);
     R VC[3];
     const long s2v = dstride(b, dT2);
 #pragma unroll
@@ -508,7 +570,7 @@ __global__ void __launch_bounds__(128, MINB) k_vxb(GamBox b, DevParams<R> P, Geo
         R acc = (R)0;
 #pragma unroll
         for (int n = 0; n < 8; n++) acc += Rc<R>(w8(n)) * w.AVf[(x + 3 * eD) * fs + c + (n - 4) * s2v];
-        VC[x] = acc / dA;
+        VC[x] = qdA(acc);
     }
     const R* Te = g.Te;
     R v1 = VC[0] * Te[(3 + 9 * eD) * fs + c] + VC[1] * Te[(4 + 9 * eD) * fs + c] + VC[2] * Te[(5 + 9 * eD) * fs + c];
@@ -517,10 +579,11 @@ __global__ void __launch_bounds__(128, MINB) k_vxb(GamBox b, DevParams<R> P, Geo
     R xni = g.Teb[(0 + 4 * eD) * fs + c], yni = g.Teb[(1 + 4 * eD) * fs + c];
     R xnj = g.Teb[(2 + 4 * eD) * fs + c], ynj = g.Teb[(3 + 4 * eD) * fs + c];
     R detT = (R)1 / (xni * ynj - xnj * yni);
-    R bT1 = (R)0.5 * (bT1L + bT1R) / fA1;
-    R bT2 = (R)0.5 * (bT2L + bT2R) / fA2;
-    R db1 = (bT1R - bT1L) / fA1;
-    R db2 = (bT2R - bT2L) / fA2;
+    const Quot<R> qA1(fA1), qA2(fA2);
+    R bT1 = qA1((R)0.5 * (bT1L + bT1R));
+    R bT2 = qA2((R)0.5 * (bT2L + bT2R));
+    R db1 = qA1(bT1R - bT1L);
+    R db2 = qA2(bT2R - bT2L);
     R Jd = db2 - db1;
     R b1 = detT * (ynj * bT1 - yni * bT2);
     R b2 = detT * (-(xnj * bT1) + xni * bT2);
@@ -543,6 +606,7 @@ template <class R, bool BORIS = false>
 __device__ __forceinline__ void mag_kin_flux(const DevParams<R>& P, R sgn, const R* W, const R* Bm, R Bn,
                                              const R* T, const double* B0, double B0n, R* mF, R& bbD, R& VaD) {
     R D = W[0], Pr = W[4];
+    const Quot<R> qD(D);
     R Bx = Bm[0], By = Bm[1], Bz = Bm[2];
     R dPb = (R)0.5 * (Bx * Bx + By * By + Bz * Bz);
     R Va2;
@@ -550,10 +614,10 @@ __device__ __forceinline__ void mag_kin_flux(const DevParams<R>& P, R sgn, const
     if (P.doBackground) {
         B0x = (R)B0[0]; B0y = (R)B0[1]; B0z = (R)B0[2];
         R sx = Bx + B0x, sy = By + B0y, sz = Bz + B0z;
-        Va2 = (sx * sx + sy * sy + sz * sz) / D;
+        Va2 = qD(sx * sx + sy * sy + sz * sz);
         bbD = bbD + (R)0.5 * (sx * sx + sy * sy + sz * sz);
     } else {
-        Va2 = (R)2 * dPb / D;
+        Va2 = qD((R)2 * dPb);
         bbD = bbD + (R)0.5 * (Bx * Bx + By * By + Bz * Bz);
     }
     R Vac2 = Va2;
@@ -563,7 +627,7 @@ __device__ __forceinline__ void mag_kin_flux(const DevParams<R>& P, R sgn, const
     }
     R Nx = T[0], Ny = T[1], Nz = T[2];
     R Vn = Nx * W[1] + Ny * W[2] + Nz * W[3];
-    R lambda = (R)1 / ((R)2 * Pr / D + Vac2);
+    R lambda = (R)1 / (qD((R)2 * Pr) + Vac2);
     R Vn0 = (R)0.5 * Mth<R>::erfc_(sgn * Mth<R>::sqrt_(lambda) * Vn);
     VaD = VaD + (R)0.5 * Mth<R>::sqrt_(Vac2);
     mF[0] = mF[0] + Vn0 * (dPb * Nx - Bx * Bn);
@@ -620,6 +684,7 @@ __global__ void __launch_bounds__(128, MINB) k_stress(GamBox b, DevParams<R> P, 
     const long fs = b.fs;
     const long c = lidx(b, ii, jj, kk);
     const long s = D == 0 ? 1L : (D == 1 ? (long)b.sx : b.sk);
+    GAM_BOX_CHECK(c - 4 * s, c + 3 * s, 8 + D);
     R T[9];
 #pragma unroll
     for (int n = 0; n < 9; n++) T[n] = g.Tf[(n + 9 * D) * fs + c];
@@ -627,7 +692,7 @@ __global__ void __launch_bounds__(128, MINB) k_stress(GamBox b, DevParams<R> P, 
     R vol[8];
 #pragma unroll
     for (int n = 0; n < 8; n++) vol[n] = g.vol[c + (n - 4) * s];
-    const R Vi = central8(vol);
+    const Quot<R> Vi(central8(vol));
     R MagL[3] = {(R)0, (R)0, (R)0}, MagR[3] = {(R)0, (R)0, (R)0};
     R Bn = (R)0;
     double B0[3] = {0.0, 0.0, 0.0}, B0n = 0.0;
@@ -709,8 +774,9 @@ __global__ void __launch_bounds__(128, MINB) k_stress(GamBox b, DevParams<R> P, 
                 predict_cell_ab3(P, Ql, oQl, pdt, odt, oodt, pQl);
                 predict_cell_ab3(P, Qr, oQr, pdt, odt, oodt, pQr);
             } else {
-                predict_cell(P, Ql, oQl, pdt, odt, pQl);
-                predict_cell(P, Qr, oQr, pdt, odt, pQr);
+                const Quot<R> qodt(odt);
+                predict_cell(P, Ql, oQl, pdt, qodt, pQl);
+                predict_cell(P, Qr, oQr, pdt, qodt, pQr);
             }
 #pragma unroll
             for (int v = 0; v < 5; v++) gv[v] = gv[v] - Ca * (pQr[v] - pQl[v]);
@@ -733,6 +799,11 @@ __global__ void __launch_bounds__(256) k_update_faces(GamBox b, DevParams<R> P, 
     const long fs = b.fs;
     const long c = lidx(b, ii, jj, kk);
     const int G = GAM_NG;
+    {
+        const bool inr0 = P.doMHD && ii >= G && ii <= G + b.Nip && jj >= G && jj <= G + b.Njp && kk >= G &&
+                          kk <= G + b.Nkp;
+        GAM_BOX_CHECK(c, inr0 ? c + b.sk : c, 11);
+    }
     if (oomf) {
 #pragma unroll
         for (int x = 0; x < 3; x++) oomf[x * fs + c] = nxt.mf[x * fs + c];
@@ -761,7 +832,8 @@ template <class R, bool BORIS>
 __device__ __forceinline__ double cell_dt(const DevParams<R>& P, const double* U, const double* Bt, double dl,
                                           double gamma, double gm1, double CFL) {
     double rho = U[0];
-    double Vx = U[1] / rho, Vy = U[2] / rho, Vz = U[3] / rho;
+    const Quot<double> qr(rho);
+    double Vx = qr(U[1]), Vy = qr(U[2]), Vz = qr(U[3]);
     double MagV = sqrt(Vx * Vx + Vy * Vy + Vz * Vz);
     double ke = 0.5 * rho * (MagV * MagV);
     double e = U[4] - ke;
@@ -836,7 +908,8 @@ __global__ void __launch_bounds__(128, MINB) k_update_cells(GamBox b, DevParams<
     if (sc->halted) return;
     int ii, jj, kk;
     Range r{0, b.Ni - 1, 0, b.Nj - 1, 0, b.Nk - 1};
-    const bool ok = thread_ijk(r, ii, jj, kk);
+    bool ok = thread_ijk(r, ii, jj, kk);
+    ok = ok && GAM_BOX_OK(lidx(b, ii, jj, kk), lidx(b, ii, jj, kk) + b.sk, 12);
     double mydt = HUGE_DT;
     bool bad = false;
     if (ok) {
@@ -855,13 +928,14 @@ __global__ void __launch_bounds__(128, MINB) k_update_cells(GamBox b, DevParams<
         if (active) {
             const long sj = b.sx, sk = b.sk;
             const R dV = g.vol[c];
+            const Quot<R> qdV(dV);
             R dGasH[5];
 #pragma unroll
             for (int v = 0; v < 5; v++) {
                 const R* gI = w.gF + (v + 0) * fs;
                 const R* gJ = w.gF + (v + 5) * fs;
                 const R* gK = w.gF + (v + 10) * fs;
-                dGasH[v] = (gI[c] - gI[c + 1] + gJ[c] - gJ[c + sj] + gK[c] - gK[c + sk]) / dV;
+                dGasH[v] = qdV(gI[c] - gI[c + 1] + gJ[c] - gJ[c + sj] + gK[c] - gK[c + sk]);
                 U[v] = cur.Gas[v * fs + c] + dt * dGasH[v];
             }
             if (P.doMHD) {
@@ -871,7 +945,7 @@ __global__ void __launch_bounds__(128, MINB) k_update_cells(GamBox b, DevParams<
                     const R* mI = w.mF + (x + 0) * fs;
                     const R* mJ = w.mF + (x + 3) * fs;
                     const R* mK = w.mF + (x + 6) * fs;
-                    dGasM[x] = (mI[c] - mI[c + 1] + mJ[c] - mJ[c + sj] + mK[c] - mK[c + sk]) / dV;
+                    dGasM[x] = qdV(mI[c] - mI[c + 1] + mJ[c] - mJ[c + sj] + mK[c] - mK[c + sk]);
                     if (P.doBackground) dGasM[x] = dGasM[x] + (R)g.dpB0[x * fs + c];
                 }
                 if constexpr (BORIS) {
@@ -892,13 +966,14 @@ __global__ void __launch_bounds__(128, MINB) k_update_cells(GamBox b, DevParams<
                 } else {
                 // CellMaxwell (mhdgroup.F90:299-329)
                 R D = rmax(U[0], P.dFloor);
+                const Quot<R> qD(D);
                 R Mx = U[1], My = U[2], Mz = U[3], TotE = U[4];
-                R KinE = (R)0.5 * (Mx * Mx + My * My + Mz * Mz) / D;
+                R KinE = qD((R)0.5 * (Mx * Mx + My * My + Mz * Mz));
                 R Pr = rmax(P.gm1 * (TotE - KinE), P.pFloor);
                 Mx = Mx + dt * dGasM[0];
                 My = My + dt * dGasM[1];
                 Mz = Mz + dt * dGasM[2];
-                KinE = (R)0.5 * (Mx * Mx + My * My + Mz * Mz) / D;
+                KinE = qD((R)0.5 * (Mx * Mx + My * My + Mz * Mz));
                 U[0] = D;
                 U[1] = Mx;
                 U[2] = My;
@@ -1067,6 +1142,7 @@ __global__ void __launch_bounds__(256) k_bc_iside(GamBox b, DevParams<R> P, Geo<
     const long fs = b.fs;
     const int G = GAM_NG;
     const bool cellJK = jj < b.Nj && kk < b.Nk;
+    GAM_BOX_CHECK(lidx(b, 0, jj, kk), lidx(b, b.Ni, jj, kk), 14);  // the row this thread writes in
     if (P.bc[0] == BCK_SPHIN && cellJK) {
         const long dst = lidx(b, G - n, jj, kk), src = lidx(b, G, jj, kk);
 #pragma unroll
@@ -1090,6 +1166,7 @@ __global__ void __launch_bounds__(256) k_bc_iside(GamBox b, DevParams<R> P, Geo<
     if (P.bc[1] == BCK_ZEROGRAD && cellJK) {
         const int ie = G + b.Nip - 1;
         const long cp = lidx(b, ie, jj, kk), cg = lidx(b, ie + n, jj, kk);
+        GAM_BOX_CHECK(cp, cp + b.sk, 14);
 #pragma unroll
         for (int v = 0; v < 5; v++) s.Gas[v * fs + cg] = s.Gas[v * fs + cp];
         R B[3];
@@ -1179,6 +1256,7 @@ __global__ void __launch_bounds__(256) k_bc_iside_b(GamBox b, Geo<R> g, StateBuf
     if (kk >= b.Nk) return;
     const long fs = b.fs;
     const long c = lidx(b, outer ? GAM_NG + b.Nip - 1 + n : GAM_NG - n, jj, kk);
+    GAM_BOX_CHECK(c, c + b.sk, 14);
     R B[3];
     cell_bxyz(b, g, c, s.mf[c], s.mf[c + 1], s.mf[fs + c], s.mf[fs + c + b.sx], s.mf[2 * fs + c], s.mf[2 * fs + c + b.sk], B);
 #pragma unroll
@@ -1252,11 +1330,13 @@ __global__ void __launch_bounds__(256) k_bc(GamBox b, DevParams<R> P, Geo<R> g, 
     if (!shell_ijk(sh, t, ii, jj, kk)) return;
     const long fs = b.fs;
     const long c = lidx(b, ii, jj, kk);
+    GAM_BOX_CHECK(c, c, 14);
     // faces
 #pragma unroll
     for (int d = 0; d < 3; d++) {
         int x = ii, y = jj, z = kk;
         bc_source(b, P, d, false, x, y, z);
+        GAM_BOX_CHECK(lidx(b, x, y, z), lidx(b, x, y, z), 14);
         if (x != ii || y != jj || z != kk) s.mf[d * fs + c] = s.mf[d * fs + lidx(b, x, y, z)];
     }
     if (ii >= b.Ni || jj >= b.Nj || kk >= b.Nk) return;
@@ -1264,6 +1344,7 @@ __global__ void __launch_bounds__(256) k_bc(GamBox b, DevParams<R> P, Geo<R> g, 
     {
         int x = ii, y = jj, z = kk;
         bc_source(b, P, -1, false, x, y, z);
+        GAM_BOX_CHECK(lidx(b, x, y, z), lidx(b, x, y, z), 14);
         if (x != ii || y != jj || z != kk) {
             const long src = lidx(b, x, y, z);
 #pragma unroll
@@ -1272,6 +1353,7 @@ __global__ void __launch_bounds__(256) k_bc(GamBox b, DevParams<R> P, Geo<R> g, 
         if (copyB) {
             int xb = ii, yb = jj, zb = kk;
             bc_source(b, P, -1, true, xb, yb, zb);
+            GAM_BOX_CHECK(lidx(b, xb, yb, zb), lidx(b, xb, yb, zb), 14);
             if (xb != ii || yb != jj || zb != kk) {
                 const long src = lidx(b, xb, yb, zb);
 #pragma unroll
@@ -1289,6 +1371,14 @@ __global__ void __launch_bounds__(256) k_bc(GamBox b, DevParams<R> P, Geo<R> g, 
     const long fI = srcf(0, ii, jj, kk), fIp = srcf(0, ii + 1, jj, kk);
     const long fJ = srcf(1, ii, jj, kk), fJp = srcf(1, ii, jj + 1, kk);
     const long fK = srcf(2, ii, jj, kk), fKp = srcf(2, ii, jj, kk + 1);
+    {
+        long lo = fI, hi = fI;
+        for (long v : {fIp, fJ, fJp, fK, fKp}) {
+            lo = v < lo ? v : lo;
+            hi = v > hi ? v : hi;
+        }
+        GAM_BOX_CHECK(lo, hi, 14);
+    }
     const bool facesMapped = fI != c || fIp != c + 1 || fJ != c || fJp != c + b.sx || fK != c || fKp != c + b.sk;
     const int G = GAM_NG;
     const bool ghost = ii < G || ii >= G + b.Nip || jj < G || jj >= G + b.Njp || kk < G || kk >= G + b.Nkp;
@@ -1330,7 +1420,7 @@ __global__ void __launch_bounds__(128) k_dt_only(GamBox b, DevParams<R> P, Geo<R
     const int G = GAM_NG;
     Range r{G - 1, G + b.Nip, G - 1, G + b.Njp, G - P.dtKlo, G + b.Nkp - 1 + P.dtKhi};
     double mydt = HUGE_DT;
-    if (thread_ijk(r, ii, jj, kk)) {
+    if (thread_ijk(r, ii, jj, kk) && GAM_BOX_OK(lidx(b, ii, jj, kk), lidx(b, ii, jj, kk), 13)) {
         const long fs = b.fs;
         const long c = lidx(b, ii, jj, kk);
         double Ud[5], Bt[3] = {0.0, 0.0, 0.0};
@@ -1354,12 +1444,13 @@ __global__ void __launch_bounds__(128) k_dt_only(GamBox b, DevParams<R> P, Geo<R
 
 // bFlux2Fld over every cell of a state (gridutils.F90:281-301)
 template <class R>
-__global__ void __launch_bounds__(128) k_bfield_all(GamBox b, Geo<R> g, StateBuf<R> s) {
+__global__ void __launch_bounds__(128) k_bfield_all(GamBox b, Geo<R> g, StateBuf<R> s, const GamScalars* sc) {
     int ii, jj, kk;
     Range r{0, b.Ni - 1, 0, b.Nj - 1, 0, b.Nk - 1};
     if (!thread_ijk(r, ii, jj, kk)) return;
     const long fs = b.fs;
     const long c = lidx(b, ii, jj, kk);
+    GAM_BOX_CHECK(c, c + b.sk, 16);
     R B[3];
     cell_bxyz(b, g, c, s.mf[c], s.mf[c + 1], s.mf[fs + c], s.mf[fs + c + b.sx], s.mf[2 * fs + c], s.mf[2 * fs + c + b.sk], B);
 #pragma unroll
@@ -1505,6 +1596,14 @@ template <class R> void launch_step(const Ctx<R>& C, int cur, cudaStream_t s) {
 // launches; ms[15]). The kernels after k_step_begin read their inputs and
 // write other arrays, so repeating one changes nothing; the time bookkeeping
 // kernels are not run.
+// The reference's clock label of each kernel id of for_each_kernel
+// (gamapp.F90:96-99, mhdgroup.F90, fields.F90, stress.F90, step.F90 Tic/Toc)
+inline const char* kernel_label(int id) {
+    static const char* L[15] = {"Gamera", "Predictor", "Mom2Face", "VxB", "Mom2Face", "VxB", "Mom2Face", "VxB",
+                                "Fluxes", "Fluxes", "Fluxes", "CT-Update", "Maxwell", "DT", "BCs"};
+    return (id >= 0 && id < 15) ? L[id] : "Gamera";
+}
+
 template <class R> void profile_step(const Ctx<R>& C, int cur, cudaStream_t s, int reps, double* ms) {
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
@@ -1514,9 +1613,11 @@ template <class R> void profile_step(const Ctx<R>& C, int cur, cudaStream_t s, i
     for_each_kernel(C, cur, cs, [&](int id, auto&& L) {
         if (id == 0 || id == 13) return;
         L();  // warm
+        nvtxRangePushA(kernel_label(id));
         cudaEventRecord(e0, s);
         for (int r = 0; r < reps; r++) L();
         cudaEventRecord(e1, s);
+        nvtxRangePop();
         cudaEventSynchronize(e1);
         float t = 0.f;
         cudaEventElapsedTime(&t, e0, e1);
@@ -1546,7 +1647,7 @@ template <class R> void launch_init(const Ctx<R>& C, int cur, cudaStream_t s) {
     const Range all{0, b.Ni, 0, b.Nj, 0, b.Nk};
     const Range cells{0, b.Ni - 1, 0, b.Nj - 1, 0, b.Nk - 1};
     const StateBuf<R> S = C.st[cur], O = C.st[1 - cur];
-    if (C.P.doMHD) k_bfield_all<R><<<grid_for(cells, blk), blk, 0, s>>>(b, C.g, S);
+    if (C.P.doMHD) k_bfield_all<R><<<grid_for(cells, blk), blk, 0, s>>>(b, C.g, S, C.sc);
     launch_bcs(C, S, s, 1);
     cudaMemcpyAsync(O.Gas, S.Gas, 5 * b.fs * sizeof(R), cudaMemcpyDeviceToDevice, s);
     cudaMemcpyAsync(O.mf, S.mf, 3 * b.fs * sizeof(R), cudaMemcpyDeviceToDevice, s);
@@ -1587,7 +1688,7 @@ template <class R> __device__ __forceinline__ R* halo_ptr(const StateBuf<R>& S, 
 }
 template <class R>
 __global__ void __launch_bounds__(256) k_halo(GamBox b, StateBuf<R> S, R* __restrict__ buf, int side, int unpack,
-                                              int copyB) {
+                                              int copyB, const GamScalars* sc) {
     const long nx = b.Ni + 1, ny = b.Nj + 1;
     const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
     if (t >= 4 * nx * ny) return;
@@ -1596,6 +1697,7 @@ __global__ void __launch_bounds__(256) k_halo(GamBox b, StateBuf<R> S, R* __rest
     for (int q = 0; q < 11; q++) {
         if (unpack && q >= 8 && !copyB) break;
         const long c = lidx(b, ii, jj, halo_k(b, side, unpack != 0, q, l));
+        GAM_BOX_CHECK(c, c, 15);
         const long e = ((long)(q * 4 + l) * ny + jj) * nx + ii;
         R* p = halo_ptr(S, fs, q);
         if (unpack)
@@ -1606,13 +1708,14 @@ __global__ void __launch_bounds__(256) k_halo(GamBox b, StateBuf<R> S, R* __rest
 }
 // Bxyz of the unpacked ghost cells from their faces (the final bFlux2Fld)
 template <class R>
-__global__ void __launch_bounds__(256) k_halo_bxyz(GamBox b, Geo<R> g, StateBuf<R> S, int side) {
+__global__ void __launch_bounds__(256) k_halo_bxyz(GamBox b, Geo<R> g, StateBuf<R> S, int side, const GamScalars* sc) {
     const long nx = b.Ni, ny = b.Nj;
     const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
     if (t >= 4 * nx * ny) return;
     const int ii = (int)(t % nx), jj = (int)((t / nx) % ny), l = (int)(t / (nx * ny));
     const int kk = side == 0 ? l : GAM_NG + b.Nkp + l;
     const long fs = b.fs, c = lidx(b, ii, jj, kk);
+    GAM_BOX_CHECK(c, c + b.sk, 15);
     R B[3];
     cell_bxyz(b, g, c, S.mf[c], S.mf[c + 1], S.mf[fs + c], S.mf[fs + c + b.sx], S.mf[2 * fs + c],
               S.mf[2 * fs + c + b.sk], B);
@@ -1623,10 +1726,10 @@ template <class R> void launch_halo(const Ctx<R>& C, int cur, cudaStream_t s, in
     const GamBox& b = C.b;
     const StateBuf<R> S = C.st[cur];
     const long n = 4L * (b.Ni + 1) * (b.Nj + 1);
-    k_halo<R><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(b, S, (R*)buf, side, unpack, copyB);
+    k_halo<R><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(b, S, (R*)buf, side, unpack, copyB, C.sc);
     if (unpack && !copyB && C.P.doMHD) {
         const long m = 4L * b.Ni * b.Nj;
-        k_halo_bxyz<R><<<(unsigned)((m + 255) / 256), 256, 0, s>>>(b, C.g, S, side);
+        k_halo_bxyz<R><<<(unsigned)((m + 255) / 256), 256, 0, s>>>(b, C.g, S, side, C.sc);
     }
 }
 

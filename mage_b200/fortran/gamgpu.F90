@@ -9,7 +9,8 @@ module gamgpu
     implicit none
 
     integer(c_int), parameter :: GAM_OK = 0, GAM_EINVAL = 1, GAM_EBADDIM = 2, GAM_ECUDA = 3, &
-                                 GAM_EDT_BAD = 4, GAM_EDT_DISASTER = 5, GAM_ESTATE = 6, GAM_EHOOK = 7
+                                 GAM_EDT_BAD = 4, GAM_EDT_DISASTER = 5, GAM_ESTATE = 6, GAM_EHOOK = 7, &
+                                 GAM_EBOUNDS = 8
     integer(c_int), parameter :: GAM_BC_PERIODIC = 0, GAM_BC_NONE = 1, GAM_BC_ZEROGRAD = 2, GAM_BC_SPHIN = 3, &
                                  GAM_BC_WIND = 4, GAM_BC_HALO = 5, GAM_BC_INFLOW = 6
     integer(c_int), parameter :: GAM_RECON_8CENT = 0, GAM_RECON_7UP = 1
@@ -117,6 +118,13 @@ module gamgpu
             import :: c_int, c_ptr, c_double
             type(c_ptr), value :: h
             real(c_double), intent(in) :: state(8)
+        end function
+        ! record of the bounds-check build (libgamgpu_check.so); fired = -1 without checks
+        integer(c_int) function gam_bounds_status(h, fired, kernel, index) bind(C, name="gam_bounds_status")
+            import :: c_int, c_ptr, c_int32_t, c_int64_t
+            type(c_ptr), value :: h
+            integer(c_int32_t), intent(out) :: fired, kernel
+            integer(c_int64_t), intent(out) :: index
         end function
         ! ooState of the AB3 predictor (doAB3): magFlux(isg:ieg+1,jsg:jeg+1,ksg:keg+1,1:3) and time
         integer(c_int) function gam_set_oostate(h, oomagFlux, ootime) bind(C, name="gam_set_oostate")

@@ -20,14 +20,16 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libgamgpu.so")
+# the same library built with the kernels' index checks and NaN canaries
+CHECK_LIB_PATH = os.path.join(HERE, "libgamgpu_check.so")
 
-GAM_OK, GAM_EINVAL, GAM_EBADDIM, GAM_ECUDA, GAM_EDT_BAD, GAM_EDT_DISASTER, GAM_ESTATE, GAM_EHOOK = range(8)
+GAM_OK, GAM_EINVAL, GAM_EBADDIM, GAM_ECUDA, GAM_EDT_BAD, GAM_EDT_DISASTER, GAM_ESTATE, GAM_EHOOK, GAM_EBOUNDS = range(9)
 BC_PERIODIC, BC_NONE, BC_ZEROGRAD, BC_SPHIN, BC_WIND, BC_HALO, BC_INFLOW = 0, 1, 2, 3, 4, 5, 6
 RECON_8CENT, RECON_7UP = 0, 1
 FP64, FP32 = 0, 1
 
 _ERRNAMES = {1: "GAM_EINVAL", 2: "GAM_EBADDIM", 3: "GAM_ECUDA", 4: "GAM_EDT_BAD", 5: "GAM_EDT_DISASTER",
-             6: "GAM_ESTATE", 7: "GAM_EHOOK"}
+             6: "GAM_ESTATE", 7: "GAM_EHOOK", 8: "GAM_EBOUNDS"}
 
 
 class GamError(RuntimeError):
@@ -53,7 +55,7 @@ EXPORTED = (
     "gam_set_geometry_arrays", "gam_get_geometry_arrays", "gam_upload_state", "gam_download_state", "gam_step",
     "gam_calc_dt", "gam_divb", "gam_totals", "gam_last_step_ms", "gam_advance_model", "gam_init_orszag_tang",
     "gam_init_blast_wave", "gam_profile_step", "gam_totals_noalloc", "gam_set_background", "gam_get_background",
-    "gam_set_background_dipole", "gam_set_wind", "gam_set_inflow", "gam_set_oostate", "gam_get_oostate", "gam_init_dipole_wind", "gam_write_restart", "gam_read_restart",
+    "gam_set_background_dipole", "gam_set_wind", "gam_set_inflow", "gam_set_oostate", "gam_get_oostate", "gam_bounds_status", "gam_init_dipole_wind", "gam_write_restart", "gam_read_restart",
     "gam_halo_bytes", "gam_halo_pack", "gam_halo_unpack", "gam_init_finish_halo", "gam_set_start", "gam_step_begin",
     "gam_dt_partial", "gam_step_end", "gam_set_slab_edges", "gam_flux_forward", "gam_flux_adjoint",
     "gam_efield_forward", "gam_efield_adjoint", "gam_predict_stage", "gam_update_stage",
@@ -63,15 +65,15 @@ EXPORTED = (
 # all cell-sized with ghosts
 BACKGROUND_ARRAYS = (("fcB0", 9), ("bFlux0", 3), ("edgB0", 6), ("B0", 3), ("dpB0", 3))
 
-_lib = None
+_libs: dict = {}
 _dp = C.POINTER(C.c_double)
 
 
 def load_library(path: str = LIB_PATH) -> C.CDLL:
-    """Load libgamgpu.so (built by __graft_entry__.build() / mage_b200/csrc/Makefile)."""
-    global _lib
-    if _lib is not None:
-        return _lib
+    """Load libgamgpu.so (built by __graft_entry__.build() / mage_b200/csrc/Makefile),
+    or another build of it (CHECK_LIB_PATH)."""
+    if path in _libs:
+        return _libs[path]
     if not os.path.exists(path):
         raise GamError(GAM_ECUDA, f"{path} is missing: build the CUDA library first (make -C mage_b200/csrc)")
     L = C.CDLL(path)
@@ -126,7 +128,8 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     L.gam_init_dipole_wind.argtypes = [C.c_void_p, _dp, C.c_uint64, C.c_double]
     L.gam_totals_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p,
                                      C.c_void_p, C.c_char_p, C.c_int32]
-    _lib = L
+    L.gam_bounds_status.argtypes = [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int64)]
+    _libs[path] = L
     return L
 
 
@@ -189,8 +192,8 @@ GEOMETRY_ARRAYS = (("face", "face", 3), ("xfc", "face", 9), ("Tf", "face", 27), 
 class GameraGPU:
     """One GAMERA app whose Grid and State live on the GPU."""
 
-    def __init__(self, params: GamParams):
-        self.L = load_library()
+    def __init__(self, params: GamParams, lib_path: str = LIB_PATH):
+        self.L = load_library(lib_path)
         self.params = params
         self._cp = params.to_c()
         h = C.c_void_p()
@@ -257,6 +260,12 @@ class GameraGPU:
         a = np.ascontiguousarray(oomagFlux, dtype=np.float64)
         assert a.shape == self.shape("face", 3), a.shape
         self._check(self.L.gam_set_oostate(self.h, _ptr(a), float(ootime)))
+
+    def bounds_status(self) -> dict:
+        """Record of the bounds-check build: fired 1 / 0, or -1 without checks."""
+        f, k, i = C.c_int32(), C.c_int32(), C.c_int64()
+        self._check(self.L.gam_bounds_status(self.h, C.byref(f), C.byref(k), C.byref(i)))
+        return {"fired": f.value, "kernel": k.value, "index": i.value}
 
     def get_oostate(self) -> dict:
         a = np.zeros(self.shape("face", 3))

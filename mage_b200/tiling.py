@@ -21,7 +21,7 @@ from __future__ import annotations
 import numpy as np
 import torch
 
-from mage_b200.gamera import BC_HALO, BC_PERIODIC, FP32, GameraGPU, GamParams
+from mage_b200.gamera import BC_HALO, BC_PERIODIC, FP32, LIB_PATH, GameraGPU, GamParams
 
 NG = 4
 
@@ -37,7 +37,7 @@ class Slabs:
     """The slabs of one grid: all of them (comm=None) or this rank's (comm="dist")."""
 
     def __init__(self, N, xyz: np.ndarray, nslab: int, comm=None, precision: int = 0, strict: bool = False,
-                 problem: str = "bw"):
+                 problem: str = "bw", lib_path: str = LIB_PATH):
         Nip, Njp, Nkp = N
         assert Nkp % nslab == 0, "Nkp must divide into the slabs"
         self.nslab, self.comm = nslab, comm
@@ -54,7 +54,7 @@ class Slabs:
         bc = (BC_PERIODIC, BC_PERIODIC, BC_PERIODIC, BC_PERIODIC, BC_HALO, BC_HALO)
         self.apps = []
         for r in self.ranks:
-            g = GameraGPU(GamParams(Nip, Njp, self.nk, bc=bc, precision=precision, strict=strict))
+            g = GameraGPU(GamParams(Nip, Njp, self.nk, bc=bc, precision=precision, strict=strict), lib_path=lib_path)
             g.set_slab_edges(r == 0, r == nslab - 1)
             g.set_geometry(slab_corners(xyz, nslab, r))
             if problem == "bw":

@@ -4,7 +4,7 @@ the way the Fortran driver would feed it."""
 import numpy as np
 
 from mage_b200 import grids
-from mage_b200.gamera import GameraGPU, GamParams, GEOMETRY_ARRAYS
+from mage_b200.gamera import LIB_PATH, GameraGPU, GamParams, GEOMETRY_ARRAYS
 from oracle.oracle import Oracle, OracleParams
 
 # oracle array name -> C-ABI geometry name
@@ -31,13 +31,13 @@ def make_oracle(problem: str, N, variant="strict", **kw):
     return o, xyz
 
 
-def gpu_from_oracle(o: Oracle, precision=0, strict=False, **kw) -> GameraGPU:
+def gpu_from_oracle(o: Oracle, precision=0, strict=False, lib_path=LIB_PATH, **kw) -> GameraGPU:
     p = o.p
     args = dict(gamma=p.gamma, CFL=p.CFL, pdmb=p.pdmb, Vd0=p.Vd0, cHogH=p.cHogH, cHogM=p.cHogM, dFloor=p.dFloor,
                 pFloor=p.pFloor, tFin=p.tFin, dt0=p.dt0, limDT0=p.limDT0, rmeth=1 if p.up7 else 0,
                 doLFMLim=p.doLFMLim, doMHD=p.doMHD, do25D=p.do25D, precision=precision, strict=strict)
     args.update(kw)
-    g = GameraGPU(GamParams(p.Nip, p.Njp, p.Nkp, **args))
+    g = GameraGPU(GamParams(p.Nip, p.Njp, p.Nkp, **args), lib_path=lib_path)
     g.set_geometry_arrays({n: o.array(GEO_FROM_ORACLE[n]) for n, _, _ in GEOMETRY_ARRAYS})
     sc = o.scalars()
     g.upload_state(o.array("Gas"), o.array("magFlux"), o.array("Bxyz"), o.array("oGas"), o.array("omagFlux"),

@@ -19,9 +19,11 @@ def test_header_lists_all_python_bindings():
 
 
 def test_library_exports_every_symbol():
-    lib = C.CDLL(gamera.LIB_PATH)
-    for name in declared():
-        assert hasattr(lib, name), name
+    """Both builds: the product library and the bounds-check one."""
+    for path in (gamera.LIB_PATH, gamera.CHECK_LIB_PATH):
+        lib = C.CDLL(path)
+        for name in declared():
+            assert hasattr(lib, name), (path, name)
 
 
 def test_default_params_match_reference():
