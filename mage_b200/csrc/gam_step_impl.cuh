@@ -1502,8 +1502,10 @@ template <class R, class F> void for_each_kernel(const Ctx<R>& C, int cur, cudaS
                     k_vxb<R, 10><<<grid_for(ed[eD], blk), blk, 0, s>>>(b, C.P, C.g, C.w, eD, ed[eD], C.sc);
                 else if ((C.kvar & 32) || sizeof(R) == 4)  // FP32: 12 blocks/SM (40 registers) measured best
                     k_vxb<R, 12><<<grid_for(ed[eD], blk), blk, 0, s>>>(b, C.P, C.g, C.w, eD, ed[eD], C.sc);
-                else
+                else if (C.kvar & 128)
                     k_vxb<R><<<grid_for(ed[eD], blk), blk, 0, s>>>(b, C.P, C.g, C.w, eD, ed[eD], C.sc);
+                else  // FP64: 8 blocks/SM (64 registers)
+                    k_vxb<R, 8><<<grid_for(ed[eD], blk), blk, 0, s>>>(b, C.P, C.g, C.w, eD, ed[eD], C.sc);
             });
         }
     }
@@ -1523,7 +1525,8 @@ template <class R, class F> void for_each_kernel(const Ctx<R>& C, int cur, cudaS
             case 1: k_stress<R, D, 1><<<grid_for(r, sblk), sblk, 0, s>>>(b, C.P, C.g, Blim, C.w, r, C.sc, S.Gas, O.Gas); break;
             case 2: k_stress<R, D, 7><<<grid_for(r, sblk), sblk, 0, s>>>(b, C.P, C.g, Blim, C.w, r, C.sc, S.Gas, O.Gas); break;
             case 3: k_stress<R, D, 8><<<grid_for(r, sblk), sblk, 0, s>>>(b, C.P, C.g, Blim, C.w, r, C.sc, S.Gas, O.Gas); break;
-            default: k_stress<R, D, sizeof(R) == 4 ? 8 : 6><<<grid_for(r, sblk), sblk, 0, s>>>(b, C.P, C.g, Blim, C.w, r, C.sc, S.Gas, O.Gas); break;
+            // FP64: 8 blocks/SM for the I and J sweeps, 7 for K (measured); FP32: 8
+            default: k_stress<R, D, (sizeof(R) == 4 || D < 2) ? 8 : 7><<<grid_for(r, sblk), sblk, 0, s>>>(b, C.P, C.g, Blim, C.w, r, C.sc, S.Gas, O.Gas); break;
         }
     };
     f(8, [&] { stress(std::integral_constant<int, 0>()); });
