@@ -46,6 +46,7 @@ namespace GAM_NS {
 static constexpr double TINY = 1.0e-12;
 static constexpr double HUGE_DT = 1.0e12;
 static constexpr double PI_D = 3.141592653589793;
+static constexpr double SQRT_PI_D = 1.7724538509055159;  // sqrt(pi) rounded to double
 
 // interpolation weights (recon.F90:22-23, 28-29)
 __device__ __forceinline__ double w8(int n) {
@@ -86,11 +87,13 @@ template <> struct Mth<double> {
     static __device__ __forceinline__ double exp_(double x) { return gam::gam_exp(x); }
 #endif
     static __device__ __forceinline__ double sqrt_(double x) { return sqrt(x); }
+    static __device__ __forceinline__ double rsqrt_(double x) { return rsqrt(x); }
 };
 template <> struct Mth<float> {
     static __device__ __forceinline__ float erfc_(float x) { return erfcf(x); }
     static __device__ __forceinline__ float exp_(float x) { return expf(x); }
     static __device__ __forceinline__ float sqrt_(float x) { return sqrtf(x); }
+    static __device__ __forceinline__ float rsqrt_(float x) { return rsqrtf(x); }
 };
 
 // Quotients a/d that share the divisor d. The product build (GAM_FAST_RECIP)
@@ -627,8 +630,14 @@ __device__ __forceinline__ void mag_kin_flux(const DevParams<R>& P, R sgn, const
     }
     R Nx = T[0], Ny = T[1], Nz = T[2];
     R Vn = Nx * W[1] + Ny * W[2] + Nz * W[3];
+#ifdef GAM_FAST_RECIP
+    // sqrt(1/x) as one reciprocal square root (about one ulp)
+    const R sqlam = Mth<R>::rsqrt_(qD((R)2 * Pr) + Vac2);
+#else
     R lambda = (R)1 / (qD((R)2 * Pr) + Vac2);
-    R Vn0 = (R)0.5 * Mth<R>::erfc_(sgn * Mth<R>::sqrt_(lambda) * Vn);
+    const R sqlam = Mth<R>::sqrt_(lambda);
+#endif
+    R Vn0 = (R)0.5 * Mth<R>::erfc_(sgn * sqlam * Vn);
     VaD = VaD + (R)0.5 * Mth<R>::sqrt_(Vac2);
     mF[0] = mF[0] + Vn0 * (dPb * Nx - Bx * Bn);
     mF[1] = mF[1] + Vn0 * (dPb * Ny - By * Bn);
@@ -650,8 +659,14 @@ __device__ __forceinline__ void gas_kin_flux(const DevParams<R>& P, R sgn, const
     R Vn = T[0] * Vx + T[1] * Vy + T[2] * Vz;
     R Vt1 = T[3] * Vx + T[4] * Vy + T[5] * Vz;
     R Vt2 = T[6] * Vx + T[7] * Vy + T[8] * Vz;
-    R Vn0 = (R)0.5 * Mth<R>::erfc_(sgn * Mth<R>::sqrt_(lambda) * Vn);
+    const R sqlam = Mth<R>::sqrt_(lambda);
+    R Vn0 = (R)0.5 * Mth<R>::erfc_(sgn * sqlam * Vn);
+#ifdef GAM_FAST_RECIP
+    // sqrt(pi lambda) = sqrt(pi) sqrt(lambda): one square root instead of two
+    R Vn1 = Vn * Vn0 - (R)0.5 * sgn * Mth<R>::exp_(-(lambda * Vn * Vn)) / ((R)SQRT_PI_D * sqlam);
+#else
     R Vn1 = Vn * Vn0 - (R)0.5 * sgn * Mth<R>::exp_(-(lambda * Vn * Vn)) / Mth<R>::sqrt_((R)PI_D * lambda);
+#endif
     gF[0] = gF[0] + D * Vn1;
     gF[4] = gF[4] + (E + (R)0.5 * Pr) * Vn1 + (R)0.5 * Pr * Vn0 * Vn;
     R fMn = D * Vn * Vn1 + Pr * Vn0;
