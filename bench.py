@@ -110,9 +110,9 @@ def measured_peak():
 
 # Lane-instructions per active cell-update of the FP64 step: ncu sum of
 # smsp__inst_executed x 32 over one 96^3 step (profiles/
-# blast96_fp64_step_kernels_full.md: 17,920), scaled to 192^3 by the ratio of
+# blast96_fp64_step_kernels_full.md: 14,776), scaled to 192^3 by the ratio of
 # ghosted to active cells ((200/192)^3 / (104/96)^3).
-INST_PER_CELL_F64 = 17920 * (200 / 192) ** 3 / (104 / 96) ** 3
+INST_PER_CELL_F64 = 14776 * (200 / 192) ** 3 / (104 / 96) ** 3
 
 
 def committed_traffic(workload, dtype):
