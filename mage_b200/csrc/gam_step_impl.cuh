@@ -1511,16 +1511,19 @@ template <class R, class F> void for_each_kernel(const Ctx<R>& C, int cur, cudaS
                              {G, G + b.Nip, G, G + b.Njp - 1, G, G + b.Nkp},
                              {G, G + b.Nip, G, G + b.Njp, G, G + b.Nkp - 1}};
         for (int eD = 0; eD < 3; eD++) {
-            f(2 + 2 * eD, [&] { k_mom2face<R><<<grid_for(mf[eD], blk), blk, 0, s>>>(b, C.P, C.g, C.w, eD, mf[eD], C.sc); });
+            // edge directions whose stencils run along k (Mom2Face of eD = 1, VxB of eD = 0, 1)
+            const dim3 mb = (eD == 1 && (C.kvar & 1024)) ? dim3(32, 1, 4) : blk;
+            const dim3 vb = (eD < 2 && (C.kvar & 512)) ? dim3(32, 1, 4) : blk;
+            f(2 + 2 * eD, [&] { k_mom2face<R><<<grid_for(mf[eD], mb), mb, 0, s>>>(b, C.P, C.g, C.w, eD, mf[eD], C.sc); });
             f(3 + 2 * eD, [&] {
                 if (C.kvar & 16)
-                    k_vxb<R, 10><<<grid_for(ed[eD], blk), blk, 0, s>>>(b, C.P, C.g, C.w, eD, ed[eD], C.sc);
+                    k_vxb<R, 10><<<grid_for(ed[eD], vb), vb, 0, s>>>(b, C.P, C.g, C.w, eD, ed[eD], C.sc);
                 else if ((C.kvar & 32) || sizeof(R) == 4)  // FP32: 12 blocks/SM (40 registers) measured best
-                    k_vxb<R, 12><<<grid_for(ed[eD], blk), blk, 0, s>>>(b, C.P, C.g, C.w, eD, ed[eD], C.sc);
+                    k_vxb<R, 12><<<grid_for(ed[eD], vb), vb, 0, s>>>(b, C.P, C.g, C.w, eD, ed[eD], C.sc);
                 else if (C.kvar & 128)
-                    k_vxb<R><<<grid_for(ed[eD], blk), blk, 0, s>>>(b, C.P, C.g, C.w, eD, ed[eD], C.sc);
+                    k_vxb<R><<<grid_for(ed[eD], vb), vb, 0, s>>>(b, C.P, C.g, C.w, eD, ed[eD], C.sc);
                 else  // FP64: 8 blocks/SM (64 registers)
-                    k_vxb<R, 8><<<grid_for(ed[eD], blk), blk, 0, s>>>(b, C.P, C.g, C.w, eD, ed[eD], C.sc);
+                    k_vxb<R, 8><<<grid_for(ed[eD], vb), vb, 0, s>>>(b, C.P, C.g, C.w, eD, ed[eD], C.sc);
             });
         }
     }
@@ -1531,17 +1534,24 @@ template <class R, class F> void for_each_kernel(const Ctx<R>& C, int cur, cudaS
     auto stress = [&](auto Dc) {
         constexpr int D = decltype(Dc)::value;
         const Range& r = fr[D];
+        // K sweep: blocks that extend along k share its 8-point stencil planes
+        // in L1 (16x1x8 measured 5 % faster than 16x8x1 on the K sweep)
+        const dim3 sbk = D != 2           ? sblk
+                         : (C.kvar & 256)  ? sblk
+                         : (C.kvar & 2048) ? dim3(32, 1, 4)
+                         : (C.kvar & 4096) ? dim3(8, 1, 16)
+                                           : dim3(16, 1, 8);
         if (C.P.doBoris) {
-            k_stress<R, D, sizeof(R) == 4 ? 8 : 6, true><<<grid_for(r, sblk), sblk, 0, s>>>(b, C.P, C.g, Blim, C.w, r, C.sc,
+            k_stress<R, D, sizeof(R) == 4 ? 8 : 6, true><<<grid_for(r, sbk), sbk, 0, s>>>(b, C.P, C.g, Blim, C.w, r, C.sc,
                                                                                         S.Gas, O.Gas);
             return;
         }
         switch (C.kvar & 3) {
-            case 1: k_stress<R, D, 1><<<grid_for(r, sblk), sblk, 0, s>>>(b, C.P, C.g, Blim, C.w, r, C.sc, S.Gas, O.Gas); break;
-            case 2: k_stress<R, D, 7><<<grid_for(r, sblk), sblk, 0, s>>>(b, C.P, C.g, Blim, C.w, r, C.sc, S.Gas, O.Gas); break;
-            case 3: k_stress<R, D, 8><<<grid_for(r, sblk), sblk, 0, s>>>(b, C.P, C.g, Blim, C.w, r, C.sc, S.Gas, O.Gas); break;
+            case 1: k_stress<R, D, 1><<<grid_for(r, sbk), sbk, 0, s>>>(b, C.P, C.g, Blim, C.w, r, C.sc, S.Gas, O.Gas); break;
+            case 2: k_stress<R, D, 7><<<grid_for(r, sbk), sbk, 0, s>>>(b, C.P, C.g, Blim, C.w, r, C.sc, S.Gas, O.Gas); break;
+            case 3: k_stress<R, D, 8><<<grid_for(r, sbk), sbk, 0, s>>>(b, C.P, C.g, Blim, C.w, r, C.sc, S.Gas, O.Gas); break;
             // FP64: 8 blocks/SM for the I and J sweeps, 7 for K (measured); FP32: 8
-            default: k_stress<R, D, (sizeof(R) == 4 || D < 2) ? 8 : 7><<<grid_for(r, sblk), sblk, 0, s>>>(b, C.P, C.g, Blim, C.w, r, C.sc, S.Gas, O.Gas); break;
+            default: k_stress<R, D, (sizeof(R) == 4 || D < 2) ? 8 : 7><<<grid_for(r, sbk), sbk, 0, s>>>(b, C.P, C.g, Blim, C.w, r, C.sc, S.Gas, O.Gas); break;
         }
     };
     f(8, [&] { stress(std::integral_constant<int, 0>()); });
