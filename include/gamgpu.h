@@ -179,6 +179,23 @@ int gam_set_background_dipole(gam_handle* h, double M0);
  * of the driver (apps/wind.F90:40-176) for a constant wind. */
 int gam_set_wind(gam_handle* h, const double wind[8]);
 
+/* A solar-wind time series for the outer-I wind boundary (bc[1] = GAM_BC_WIND)
+ * in place of the constant wind: n >= 2 rows at uniformly spaced times t
+ * (readWind's check, apps/wind.F90:691-699) of density, pressure, velocity
+ * V[3*r+x] and field B[3*r+x], in code units (the driver converts its file as
+ * readWind does, :655-668); xyzBS[3*r+x] the bow-shock marker (NULL: the
+ * origin); Bx0, ByC, BzC the tilted-front coefficients (Bx = Bx0 + ByC*By +
+ * BzC*Bz replaces the series' Bx, :720-727). Each boundary fill takes the
+ * wind at every ghost cell and face at its lag time along the front
+ * (RefreshWind, GetWindAt, wgtWind, :116-203; InterpWind and InterpWgts,
+ * :766-868, with the reference's doWindInterp = F: the row at or below the
+ * time; a null field before the first row, no spin-up sequence). The weights
+ * use CUDA's acos and exp. With doBoris a series faster than Ca is refused
+ * (:744-750). The initial condition still comes from gam_init_dipole_wind's
+ * constant state; call this after it. */
+int gam_set_wind_series(gam_handle* h, int32_t n, const double* t, const double* rho, const double* P,
+                        const double* V, const double* B, const double* xyzBS, double Bx0, double ByC, double BzC);
+
 /* State of the uniform inner-I inflow (bc[0] = GAM_BC_INFLOW), same order as
  * the wind: {rho, P, Vx, Vy, Vz, Bx, By, Bz}. Ghost cell is-n (n = 1..4, every
  * j, k of the cell ranges) gets the conserved form of that state (CellP2C,

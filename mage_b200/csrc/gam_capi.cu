@@ -5,6 +5,7 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <algorithm>
 #include <string>
 #include <vector>
 #include "../../include/gamgpu.h"
@@ -1013,7 +1014,7 @@ extern "C" int gam_set_wind(gam_handle* h, const double wind[8]) {
         }
     CK(h, cudaMemcpyAsync(h->windTab, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice, h->s));
     CK(h, cudaStreamSynchronize(h->s));
-    WindData W;
+    WindData W{};  // n = 0: the constant wind (a series set before is dropped)
     for (int v = 0; v < 8; v++) W.state[v] = wind[v];
     W.wC = h->windTab;
     W.wF = h->windTab + nw;
@@ -1021,6 +1022,50 @@ extern "C" int gam_set_wind(gam_handle* h, const double wind[8]) {
     W.nw = nw;
     h->cd.P.wind = W;
     h->cf.P.wind = W;
+    drop_graphs(h);
+    h->haveWind = true;
+    return GAM_OK;
+}
+
+extern "C" int gam_set_wind_series(gam_handle* h, int32_t n, const double* t, const double* rho, const double* P,
+                                   const double* V, const double* B, const double* xyzBS, double Bx0, double ByC,
+                                   double BzC) {
+    if (!h || !t || !rho || !P || !V || !B) return GAM_EINVAL;
+    if (h->p.bc[1] != GAM_BC_WIND) return fail(h, GAM_ESTATE, "the outer I boundary is not the solar wind");
+    if (n < 2) return fail(h, GAM_EINVAL, "a wind series needs at least two rows");
+    double dtMin = t[1] - t[0], dtMax = dtMin, vMax = 0.0;
+    for (int r = 1; r + 1 < n; r++) {
+        dtMin = std::min(dtMin, t[r + 1] - t[r]);
+        dtMax = std::max(dtMax, t[r + 1] - t[r]);
+    }
+    if (!(dtMin > 0.0) || fabs(dtMin - dtMax) > 1.0e-6 * sqrt(dtMin * dtMin + dtMax * dtMax))
+        return fail(h, GAM_EINVAL, "the wind series needs increasing, uniformly spaced times");
+    std::vector<double> tab(12 * (size_t)n);
+    for (int r = 0; r < n; r++) {
+        double* q = tab.data() + 12 * (size_t)r;
+        q[0] = t[r];
+        q[1] = rho[r];
+        for (int x = 0; x < 3; x++) q[2 + x] = V[3 * r + x];
+        q[5] = P[r];
+        for (int x = 0; x < 3; x++) q[6 + x] = B[3 * r + x];
+        q[6] = Bx0 + ByC * q[7] + BzC * q[8];  // readWind (apps/wind.F90:723-727)
+        for (int x = 0; x < 3; x++) q[9 + x] = xyzBS ? xyzBS[3 * r + x] : 0.0;
+        vMax = std::max(vMax, sqrt(q[2] * q[2] + q[3] * q[3] + q[4] * q[4]));
+    }
+    if (h->p.doBoris && vMax >= h->p.Ca) return fail(h, GAM_EINVAL, "the solar wind is faster than the Boris speed Ca");
+    cudaError_t e = cudaSuccess;
+    double* d = dalloc<double>(h, 12L * n, &e);
+    if (e != cudaSuccess) return fail(h, GAM_ECUDA, "cudaMalloc failed (wind series)");
+    CK(h, cudaMemcpyAsync(d, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice, h->s));
+    CK(h, cudaStreamSynchronize(h->s));
+    for (WindData* W : {&h->cd.P.wind, &h->cf.P.wind}) {
+        W->n = n;
+        W->tMin = *std::min_element(t, t + n);
+        W->tMax = *std::max_element(t, t + n);
+        W->dtW = dtMin;
+        W->Bx0 = Bx0; W->ByC = ByC; W->BzC = BzC;
+        W->ts = d;
+    }
     drop_graphs(h);
     h->haveWind = true;
     return GAM_OK;

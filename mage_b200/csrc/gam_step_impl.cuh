@@ -1140,6 +1140,72 @@ __device__ __forceinline__ R face_proj(const GamBox& b, const Geo<R>& g, int d, 
     return g.face[d * fs + c] * (B[0] * n[0] + B[1] * n[fs] + B[2] * n[2 * fs]);
 }
 
+// ---- the solar-wind time series (apps/wind.F90), in FP64 in both forms.
+// InterpWgts (:825-868) with doWindInterp = F: the row at or below t (0-based)
+__device__ __forceinline__ int wind_row(const WindData& W, double t) {
+    if (t >= W.tMax) return W.n - 1;
+    if (t <= W.tMin) return 0;
+    const int i0 = (int)floor((t - W.tMin) / W.dtW) + 1;  // 1-based, as the reference
+    return i0 + 1 <= W.n ? i0 - 1 : W.n - 2;
+}
+// InterpWind (:766-809) without the spin-up sequence
+__device__ __forceinline__ void wind_interp(const WindData& W, double t, double& D, double& P, double* V, double* B) {
+    const double* r = W.ts + 12 * wind_row(W, t);
+    D = r[1];
+    V[0] = r[2]; V[1] = r[3]; V[2] = r[4];
+    P = r[5];
+    B[1] = r[7];
+    B[2] = r[8];
+    B[0] = W.Bx0 + W.ByC * B[1] + W.BzC * B[2];
+    if (t <= W.tMin) B[0] = B[1] = B[2] = 0.0;
+}
+// PlaceWind (:812-822) and RefreshWind (:116-157) at time t
+__device__ __forceinline__ void wind_refresh(const WindData& W, double t, double* xyzW, double* vFr) {
+    const double* r = W.ts + 12 * wind_row(W, t);
+    xyzW[0] = r[9]; xyzW[1] = r[10]; xyzW[2] = r[11];
+    double D, P, V0[3], B[3];
+    wind_interp(W, t, D, P, V0, B);
+    const double vSpd = -norm2s3(V0);
+    const double bcc = sqrt(W.ByC * W.ByC + W.BzC * W.BzC);
+    const double btt = sqrt(1.0 + bcc * bcc);
+    if (bcc > TINY) {
+        const double CosBp = W.ByC / bcc, SinBp = W.BzC / bcc, CosF = 1.0 / btt, SinF = bcc / btt;
+        vFr[0] = vSpd * (CosF * CosF);
+        vFr[1] = -(vSpd * CosF * SinF * CosBp);
+        vFr[2] = -(vSpd * CosF * SinF * SinBp);
+    } else {
+        vFr[0] = vSpd; vFr[1] = 0.0; vFr[2] = 0.0;
+    }
+}
+// GetWindAt (:160-176): the wind rewound by the lag time to xyz
+__device__ __forceinline__ void wind_at(const WindData& W, const double* xyzW, const double* vFr, const double* xyz,
+                                        double t, double& D, double& P, double* V, double* B) {
+    const double vMag = norm2s3(vFr);
+    const double DelT = ((xyz[0] - xyzW[0]) * vFr[0] + (xyz[1] - xyzW[1]) * vFr[1] + (xyz[2] - xyzW[2]) * vFr[2]) /
+                        (vMag * vMag);
+    wind_interp(W, t - DelT, D, P, V, B);
+}
+// wgtWind (:180-203) with RampDown (math.F90:97-111); CUDA's acos and exp
+__device__ __forceinline__ double wind_weight(const WindData& W, const double* xyzW, const double* vFr,
+                                              const double* xyz, double t) {
+    double D, P, V[3], B[3];
+    wind_at(W, xyzW, vFr, xyz, t, D, P, V, B);
+    const double nA = sqrt(xyz[0] * xyz[0] + xyz[1] * xyz[1] + xyz[2] * xyz[2]);
+    const double vA = sqrt(V[0] * V[0] + V[1] * V[1] + V[2] * V[2]);
+    double c = 0.0;
+#pragma unroll
+    for (int x = 0; x < 3; x++) {
+        const double nh = nA <= TINY ? 0.0 : xyz[x] / nA;
+        const double vh = vA <= TINY ? 0.0 : V[x] / vA;
+        c = x == 0 ? (-vh) * nh : c + (-vh) * nh;
+    }
+    const double dTh = acos(c) * 180.0 / PI_D;
+    if (dTh <= 90.0) return 1.0;
+    if (dTh >= 180.0) return 0.0;
+    const double rScl = (dTh - 90.0) / 90.0;
+    return exp(-1.0 / (1.0 - rScl * rScl) + 1.0);
+}
+
 // The non-periodic I boundaries, in place: the SphIn copy or the uniform
 // inflow on the inner side (bcs.F90:934-957), the solar-wind blend
 // (apps/wind.F90:206-300) or zeroGrad_obcI (bcs.F90:820-850) on the outer
@@ -1195,16 +1261,34 @@ __global__ void __launch_bounds__(256) k_bc_iside(GamBox b, DevParams<R> P, Geo<
     const WindData& W = P.wind;
     const long wi = (n - 1) + 4 * (jj + (long)(b.Nj + 1) * kk);
     const int ig = G + b.Nip - 1 + n, ip = G + b.Nip - 1;
+    // a time series: RefreshWind at Model%t (the time after this step's
+    // update), then the wind at each point's lag time (apps/wind.F90:218-223)
+    const bool series = W.n > 0;
+    const double tnow = sc->t;
+    double xyzW[3] = {0.0, 0.0, 0.0}, vFr[3] = {-1.0, 0.0, 0.0};
+    if (series) wind_refresh(W, tnow, xyzW, vFr);
     if (cellJK) {
         const double MinMach = 1.0;
-        const double wSW = W.wC[wi], wMHD = 1.0 - wSW;
+        double wSW, Dsw = W.state[0], Psw = W.state[1], Vsw[3] = {W.state[2], W.state[3], W.state[4]};
+        if (series) {
+            const long cg = lidx(b, ig, jj, kk);
+            const double xc[3] = {(double)g.xyzcc[cg], (double)g.xyzcc[fs + cg], (double)g.xyzcc[2 * fs + cg]};
+            wSW = wind_weight(W, xyzW, vFr, xc, tnow);
+            if (wSW > TINY) {
+                double Bsw[3];
+                wind_at(W, xyzW, vFr, xc, tnow, Dsw, Psw, Vsw, Bsw);
+            }
+        } else {
+            wSW = W.wC[wi];
+        }
+        const double wMHD = 1.0 - wSW;
         R gW_sw[5] = {(R)0, (R)0, (R)0, (R)0, (R)0}, gW_in[5] = {(R)0, (R)0, (R)0, (R)0, (R)0};
         if (wSW > TINY) {
-            gW_sw[0] = (R)W.state[0];
-            gW_sw[4] = (R)W.state[1];
-            gW_sw[1] = (R)W.state[2];
-            gW_sw[2] = (R)W.state[3];
-            gW_sw[3] = (R)W.state[4];
+            gW_sw[0] = (R)Dsw;
+            gW_sw[4] = (R)Psw;
+            gW_sw[1] = (R)Vsw[0];
+            gW_sw[2] = (R)Vsw[1];
+            gW_sw[3] = (R)Vsw[2];
         }
         if (wMHD > TINY) {
             const long cp = lidx(b, ip, jj, kk);
@@ -1246,16 +1330,24 @@ __global__ void __launch_bounds__(256) k_bc_iside(GamBox b, DevParams<R> P, Geo<
         for (int v = 0; v < 5; v++) s.Gas[v * fs + cg] = gC[v];
     }
     // face fluxes: I face ig+1, J and K faces of cell ig
-    {
-        const double w = W.wF[wi];
-        const long cI = lidx(b, ig + 1, jj, kk), cin = lidx(b, ip + 1, jj, kk);
-        s.mf[cI] = (R)w * (R)W.sF[wi] + ((R)1 - (R)w) * s.mf[cin];
-    }
 #pragma unroll
-    for (int d = 1; d < 3; d++) {
-        const double w = W.wF[d * W.nw + wi];
-        const long cg = lidx(b, ig, jj, kk), cin = lidx(b, ip, jj, kk);
-        s.mf[d * fs + cg] = (R)w * (R)W.sF[d * W.nw + wi] + ((R)1 - (R)w) * s.mf[d * fs + cin];
+    for (int d = 0; d < 3; d++) {
+        const long cf = lidx(b, d == 0 ? ig + 1 : ig, jj, kk), cin = lidx(b, d == 0 ? ip + 1 : ip, jj, kk);
+        double w, sw;
+        if (series) {
+            // WindMagFlux (apps/wind.F90:378-391) with Project2Face (bcs.F90:250-263)
+            const double xf[3] = {(double)g.xfc[(3 * d) * fs + cf], (double)g.xfc[(3 * d + 1) * fs + cf],
+                                  (double)g.xfc[(3 * d + 2) * fs + cf]};
+            w = wind_weight(W, xyzW, vFr, xf, tnow);
+            double D, Pw, V[3], Bf[3];
+            wind_at(W, xyzW, vFr, xf, tnow, D, Pw, V, Bf);
+            const R* nh = g.Tf + (long)(9 * d) * fs + cf;
+            sw = (double)g.face[d * fs + cf] * ((double)nh[0] * Bf[0] + (double)nh[fs] * Bf[1] + (double)nh[2 * fs] * Bf[2]);
+        } else {
+            w = W.wF[d * W.nw + wi];
+            sw = W.sF[d * W.nw + wi];
+        }
+        s.mf[d * fs + cf] = (R)w * (R)sw + ((R)1 - (R)w) * s.mf[d * fs + cin];
     }
 }
 // Bxyz of the wind (apps/wind.F90:341-351) or inflow ghost cells from their

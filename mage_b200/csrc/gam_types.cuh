@@ -14,6 +14,11 @@ struct WindData {
     const double* wF;   // 3 x: weight at the I face ie+n+1, J face and K face of the ghost cell
     const double* sF;   // 3 x: wind flux through those faces
     long nw;            // entries per array
+    // time series (gam_set_wind_series, apps/wind.F90 WindBC_T): n rows of
+    // t, D, Vx, Vy, Vz, P, Bx, By, Bz, xBS, yBS, zBS; n = 0: the constant wind
+    int n;
+    double tMin, tMax, dtW, Bx0, ByC, BzC;
+    const double* ts;
 };
 
 template <class R> struct DevParams {

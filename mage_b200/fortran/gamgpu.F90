@@ -114,6 +114,16 @@ module gamgpu
             type(c_ptr), value :: h
             real(c_double), intent(in) :: wind(8)
         end function
+        ! solar-wind time series: t(n), rho(n), P(n), V(3,n), B(3,n), xyzBS(3,n) or c_null_ptr
+        integer(c_int) function gam_set_wind_series(h, n, t, rho, P, V, B, xyzBS, Bx0, ByC, BzC) &
+                bind(C, name="gam_set_wind_series")
+            import :: c_int, c_ptr, c_int32_t, c_double
+            type(c_ptr), value :: h
+            integer(c_int32_t), value :: n
+            real(c_double), intent(in) :: t(*), rho(*), P(*), V(*), B(*)
+            type(c_ptr), value :: xyzBS
+            real(c_double), value :: Bx0, ByC, BzC
+        end function
         integer(c_int) function gam_set_inflow(h, state) bind(C, name="gam_set_inflow")
             import :: c_int, c_ptr, c_double
             type(c_ptr), value :: h

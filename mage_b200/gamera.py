@@ -55,7 +55,7 @@ EXPORTED = (
     "gam_set_geometry_arrays", "gam_get_geometry_arrays", "gam_upload_state", "gam_download_state", "gam_step",
     "gam_calc_dt", "gam_divb", "gam_totals", "gam_last_step_ms", "gam_advance_model", "gam_init_orszag_tang",
     "gam_init_blast_wave", "gam_profile_step", "gam_totals_noalloc", "gam_set_background", "gam_get_background",
-    "gam_set_background_dipole", "gam_set_wind", "gam_set_inflow", "gam_set_oostate", "gam_get_oostate", "gam_bounds_status", "gam_init_dipole_wind", "gam_write_restart", "gam_read_restart",
+    "gam_set_background_dipole", "gam_set_wind", "gam_set_wind_series", "gam_set_inflow", "gam_set_oostate", "gam_get_oostate", "gam_bounds_status", "gam_init_dipole_wind", "gam_write_restart", "gam_read_restart",
     "gam_halo_bytes", "gam_halo_pack", "gam_halo_unpack", "gam_init_finish_halo", "gam_set_start", "gam_step_begin",
     "gam_dt_partial", "gam_step_end", "gam_set_slab_edges", "gam_flux_forward", "gam_flux_adjoint",
     "gam_efield_forward", "gam_efield_adjoint", "gam_predict_stage", "gam_update_stage",
@@ -101,6 +101,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     L.gam_set_background_dipole.argtypes = [C.c_void_p, C.c_double]
     L.gam_set_wind.argtypes = [C.c_void_p, _dp]
     L.gam_set_inflow.argtypes = [C.c_void_p, _dp]
+    L.gam_set_wind_series.argtypes = [C.c_void_p, C.c_int32] + [_dp] * 6 + [C.c_double] * 3
     L.gam_set_oostate.argtypes = [C.c_void_p, _dp, C.c_double]
     L.gam_get_oostate.argtypes = [C.c_void_p, _dp, _dp]
     L.gam_write_restart.argtypes = [C.c_void_p, C.c_char_p]
@@ -321,6 +322,15 @@ class GameraGPU:
         w = np.ascontiguousarray(wind, dtype=np.float64)
         assert w.shape == (8,)
         self._check(self.L.gam_set_wind(self.h, _ptr(w)))
+
+    def set_wind_series(self, t, rho, P, V, B, xyzBS=None, Bx0=0.0, ByC=0.0, BzC=0.0):
+        """Solar-wind time series of the outer-I boundary (code units); V, B, xyzBS are (n, 3)."""
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (t, rho, P, V, B)]
+        xb = None if xyzBS is None else np.ascontiguousarray(xyzBS, dtype=np.float64)
+        n = arrs[0].size
+        assert arrs[1].size == n and arrs[2].size == n and arrs[3].shape == (n, 3) and arrs[4].shape == (n, 3)
+        self._check(self.L.gam_set_wind_series(self.h, n, *[_ptr(a) for a in arrs], None if xb is None else _ptr(xb),
+                                               float(Bx0), float(ByC), float(BzC)))
 
     def set_inflow(self, state):
         """Uniform inner-I inflow {rho, P, Vx, Vy, Vz, Bx, By, Bz} (bc[0] = BC_INFLOW)."""

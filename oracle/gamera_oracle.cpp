@@ -138,6 +138,13 @@ struct Model {
     bool doBoris = false;
     double Ca = 0.0;
     bool doAB3 = false;
+    // solar-wind time series of WindBC_T (apps/wind.F90:28-53, readWind
+    // :619-763), code units, 0-based rows; n = 0: the constant wind above
+    struct WindSeries {
+        int n = 0;
+        std::vector<double> tW, Q, B, xyzBS;  // Q: n x (D, Vx, Vy, Vz, P); B, xyzBS: n x 3
+        double tMin = 0, tMax = 0, dtW = 0, Bx0 = 0, ByC = 0, BzC = 0;
+    } ws;
 };
 
 struct Grid {
@@ -1759,6 +1766,81 @@ static double Con2Fast(const Model& M, const double* gCon, const double* B) {
     if (M.doBoris) Va = M.Ca * Va / std::sqrt(M.Ca * M.Ca + Va * Va);  // gamutils.F90:356-358
     return std::sqrt(Cs * Cs + Va * Va);
 }
+// apps/wind.F90:825-868 InterpWgts; the reference keeps doWindInterp = F, so
+// the weights are always (1, 0): the wind holds the row at or below t
+static void InterpWgts(const Model::WindSeries& W, double t, double& w0, double& w1, int& i0, int& i1) {
+    if (t >= W.tMax) {
+        i0 = W.n; i1 = i0; w0 = 1.0; w1 = 0.0;
+    } else if (t <= W.tMin) {
+        i0 = 1; i1 = i0; w0 = 1.0; w1 = 0.0;
+    } else {
+        i0 = (int)std::floor((t - W.tMin) / W.dtW) + 1;
+        i1 = i0 + 1;
+        if (i1 <= W.n) {
+            double dT = W.tW[i1 - 1] - W.tW[i0 - 1];
+            w0 = (W.tW[i1 - 1] - t) / dT;
+            w1 = (t - W.tW[i0 - 1]) / dT;
+        } else {
+            i1 = W.n; i0 = i1 - 1; w0 = 0.0; w1 = 1.0;
+        }
+    }
+    w0 = 1.0;  // doWindInterp = F (wind.F90:19, :862-866)
+    w1 = 0.0;
+}
+// apps/wind.F90:766-809 InterpWind (no spin-up sequence: a null field before tMin)
+static void InterpWind(const Model::WindSeries& W, double t, double& D, double& P, double* V, double* B) {
+    double w0, w1;
+    int i0, i1;
+    InterpWgts(W, t, w0, w1, i0, i1);
+    const int a = i0 - 1, b = i1 - 1;
+    D = w0 * W.Q[5 * a + 0] + w1 * W.Q[5 * b + 0];
+    P = w0 * W.Q[5 * a + 4] + w1 * W.Q[5 * b + 4];
+    for (int x = 0; x < 3; x++) V[x] = w0 * W.Q[5 * a + 1 + x] + w1 * W.Q[5 * b + 1 + x];
+    for (int x = 0; x < 3; x++) B[x] = w0 * W.B[3 * a + x] + w1 * W.B[3 * b + x];
+    B[0] = W.Bx0 + W.ByC * B[1] + W.BzC * B[2];
+    if (t <= W.tMin) B[0] = B[1] = B[2] = 0.0;
+}
+// apps/wind.F90:812-822 PlaceWind and :116-157 RefreshWind at time t
+static void RefreshWind(const Model::WindSeries& W, double t, double* xyzW, double* vFr) {
+    double w0, w1;
+    int i0, i1;
+    InterpWgts(W, t, w0, w1, i0, i1);
+    for (int x = 0; x < 3; x++) xyzW[x] = w0 * W.xyzBS[3 * (i0 - 1) + x] + w1 * W.xyzBS[3 * (i1 - 1) + x];
+    double D, P, V0[3], B[3];
+    InterpWind(W, t, D, P, V0, B);
+    double vSpd = -norm2s(V0, 3);
+    double bcc = std::sqrt(W.ByC * W.ByC + W.BzC * W.BzC);
+    double btt = std::sqrt(1 + bcc * bcc);
+    if (bcc > TINY) {
+        double CosBp = W.ByC / bcc, SinBp = W.BzC / bcc;
+        double CosF = 1.0 / btt, SinF = bcc / btt;
+        vFr[0] = vSpd * (CosF * CosF);
+        vFr[1] = -(vSpd * CosF * SinF * CosBp);
+        vFr[2] = -(vSpd * CosF * SinF * SinBp);
+    } else {
+        vFr[0] = vSpd; vFr[1] = 0.0; vFr[2] = 0.0;
+    }
+}
+// apps/wind.F90:160-176 GetWindAt: the wind rewound by the lag time to xyz
+static void GetWindAt(const Model::WindSeries& W, const double* xyzW, const double* vFr, const double* xyz,
+                      double t, double& D, double& P, double* V, double* B) {
+    double vMag = norm2s(vFr, 3);
+    double d[3] = {xyz[0] - xyzW[0], xyz[1] - xyzW[1], xyz[2] - xyzW[2]};
+    double DelT = dot3(d, vFr) / (vMag * vMag);
+    InterpWind(W, t - DelT, D, P, V, B);
+}
+// apps/wind.F90:180-203 wgtWind with the wind at xyz and t
+static double wgtWindTS(const Model::WindSeries& W, const double* xyzW, const double* vFr, const double* xyz,
+                        double t) {
+    double nHat[3], vHat[3], mv[3], D, P, V[3], B[3];
+    normVec(xyz, nHat);
+    GetWindAt(W, xyzW, vFr, xyz, t, D, P, V, B);
+    normVec(V, vHat);
+    for (int x = 0; x < 3; x++) mv[x] = -vHat[x];
+    double dTh = std::acos(dot3(mv, nHat)) * 180.0 / PI;
+    return RampDown(dTh, 90.0, 90.0);
+}
+
 // apps/wind.F90:206-374 WindBC with a constant wind (GetWindAt is then
 // independent of position and time), single fluid, no ring
 static void WindBC(const Model& M, const Grid& G, State& S) {
@@ -1766,6 +1848,23 @@ static void WindBC(const Model& M, const Grid& G, State& S) {
     const double* w = M.wind;  // rho, P, V(3), B(3)
     const double Vsw[3] = {w[2], w[3], w[4]}, Bsw[3] = {w[5], w[6], w[7]};
     const int ip = G.ie;
+    // a time series: RefreshWind at Model%t, then the wind at each point's lag time
+    const bool ts = M.ws.n > 0;
+    double xyzW[3] = {0.0, 0.0, 0.0}, vFr[3] = {-1.0, 0.0, 0.0};
+    if (ts) RefreshWind(M.ws, M.t, xyzW, vFr);
+    auto weight = [&](const double* xyz) { return ts ? wgtWindTS(M.ws, xyzW, vFr, xyz, M.t) : wgtWind(Vsw, xyz); };
+    auto windAt = [&](const double* xyz, double& D, double& P, double* V, double* B) {
+        if (ts) {
+            GetWindAt(M.ws, xyzW, vFr, xyz, M.t, D, P, V, B);
+            return;
+        }
+        D = w[0];
+        P = w[1];
+        for (int x = 0; x < 3; x++) {
+            V[x] = Vsw[x];
+            B[x] = Bsw[x];
+        }
+    };
 #pragma omp parallel for collapse(2)
     for (int k = G.ksg; k <= G.keg + 1; k++)
         for (int j = G.jsg; j <= G.jeg + 1; j++)
@@ -1774,12 +1873,14 @@ static void WindBC(const Model& M, const Grid& G, State& S) {
                 if (isCellCenterG(G, ig, j, k)) {
                     double gW_sw[5] = {0, 0, 0, 0, 0}, gW_in[5] = {0, 0, 0, 0, 0};
                     double xcc[3] = {G.xyzcc(ig, j, k, 0), G.xyzcc(ig, j, k, 1), G.xyzcc(ig, j, k, 2)};
-                    double wSW = wgtWind(Vsw, xcc);
+                    double wSW = weight(xcc);
                     double wMHD = 1.0 - wSW;
                     if (wSW > TINY) {
-                        gW_sw[DEN] = w[0];
-                        gW_sw[PRESSURE] = w[1];
-                        for (int x = 0; x < 3; x++) gW_sw[VELX + x] = Vsw[x];
+                        double D, P, V[3], B[3];
+                        windAt(xcc, D, P, V, B);
+                        gW_sw[DEN] = D;
+                        gW_sw[PRESSURE] = P;
+                        for (int x = 0; x < 3; x++) gW_sw[VELX + x] = V[x];
                     }
                     if (wMHD > TINY) {
                         double gCon[5], B_in[3];
@@ -1803,17 +1904,21 @@ static void WindBC(const Model& M, const Grid& G, State& S) {
                 // face fluxes: I at ig+1, J and K at ig
                 {
                     double xf[3] = {G.xfc(ig + 1, j, k, 0), G.xfc(ig + 1, j, k, 1), G.xfc(ig + 1, j, k, 2)};
-                    double wSW = wgtWind(Vsw, xf);
+                    double wSW = weight(xf);
                     double nH[3] = {G.Tf(ig + 1, j, k, NORMX), G.Tf(ig + 1, j, k, NORMY), G.Tf(ig + 1, j, k, NORMZ)};
-                    double swFlx = G.face(ig + 1, j, k, IDIR) * dot3(nH, Bsw);
+                    double D, P, V[3], Bf[3];
+                    windAt(xf, D, P, V, Bf);
+                    double swFlx = G.face(ig + 1, j, k, IDIR) * dot3(nH, Bf);  // Project2Face, bcs.F90:250-263
                     double inFlx = S.magFlux(ip + 1, j, k, IDIR);
                     S.magFlux(ig + 1, j, k, IDIR) = wSW * swFlx + (1 - wSW) * inFlx;
                 }
                 for (int d = 1; d < 3; d++) {
                     double xf[3] = {G.xfc(ig, j, k, 0 + 3 * d), G.xfc(ig, j, k, 1 + 3 * d), G.xfc(ig, j, k, 2 + 3 * d)};
-                    double wSW = wgtWind(Vsw, xf);
+                    double wSW = weight(xf);
                     double nH[3] = {G.Tf(ig, j, k, NORMX + 9 * d), G.Tf(ig, j, k, NORMY + 9 * d), G.Tf(ig, j, k, NORMZ + 9 * d)};
-                    double swFlx = G.face(ig, j, k, d) * dot3(nH, Bsw);
+                    double D, P, V[3], Bf[3];
+                    windAt(xf, D, P, V, Bf);
+                    double swFlx = G.face(ig, j, k, d) * dot3(nH, Bf);
                     double inFlx = S.magFlux(ip, j, k, d);
                     S.magFlux(ig, j, k, d) = wSW * swFlx + (1 - wSW) * inFlx;
                 }
@@ -2042,6 +2147,33 @@ void orc_set_scalars(void* h, const OrcScalars* o) {
 }
 
 // gridutils.F90:717-770 DivB (sequential sum, no background)
+// the solar-wind time series (code units; xyzBS may be null: the bow-shock
+// marker at the origin, readWind's default, apps/wind.F90:731)
+void orc_set_wind_series(void* h, int n, const double* t, const double* rho, const double* P, const double* V,
+                         const double* B, const double* xyzBS, double Bx0, double ByC, double BzC) {
+    App* A = (App*)h;
+    Model::WindSeries& W = A->M.ws;
+    W.n = n;
+    W.tW.assign(t, t + n);
+    W.Q.assign(5 * (size_t)n, 0.0);
+    W.B.assign(3 * (size_t)n, 0.0);
+    W.xyzBS.assign(3 * (size_t)n, 0.0);
+    for (int r = 0; r < n; r++) {
+        W.Q[5 * r + 0] = rho[r];
+        for (int x = 0; x < 3; x++) W.Q[5 * r + 1 + x] = V[3 * r + x];
+        W.Q[5 * r + 4] = P[r];
+        for (int x = 0; x < 3; x++) W.B[3 * r + x] = B[3 * r + x];
+        W.B[3 * r + 0] = Bx0 + ByC * W.B[3 * r + 1] + BzC * W.B[3 * r + 2];  // readWind :723-727
+        if (xyzBS)
+            for (int x = 0; x < 3; x++) W.xyzBS[3 * r + x] = xyzBS[3 * r + x];
+    }
+    W.tMin = *std::min_element(W.tW.begin(), W.tW.end());
+    W.tMax = *std::max_element(W.tW.begin(), W.tW.end());
+    W.dtW = n > 1 ? W.tW[1] - W.tW[0] : 1.0;
+    for (int r = 1; r + 1 < n; r++) W.dtW = std::min(W.dtW, W.tW[r + 1] - W.tW[r]);
+    W.Bx0 = Bx0; W.ByC = ByC; W.BzC = BzC;
+}
+
 double orc_divb(void* h) {
     App* A = (App*)h;
     const Grid& G = A->G;

@@ -142,6 +142,7 @@ def lib(variant: str = "strict") -> C.CDLL:
             getattr(L, f).argtypes = [C.c_double]
             getattr(L, f).restype = C.c_double
         L.orc_num_threads.restype = C.c_int
+        L.orc_set_wind_series.argtypes = [C.c_void_p, C.c_int] + [C.POINTER(C.c_double)] * 6 + [C.c_double] * 3
         _libs[variant] = L
     return _libs[variant]
 
@@ -207,6 +208,14 @@ class Oracle:
         for k, v in kw.items():
             setattr(s, k, v)
         self.L.orc_set_scalars(self.h, C.byref(s))
+
+    def set_wind_series(self, t, rho, P, V, B, xyzBS=None, Bx0=0.0, ByC=0.0, BzC=0.0):
+        """Solar-wind time series of the outer-I wind boundary (code units)."""
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (t, rho, P, V, B)]
+        xb = None if xyzBS is None else np.ascontiguousarray(xyzBS, dtype=np.float64)
+        self._ws = arrs + [xb]
+        self.L.orc_set_wind_series(self.h, len(arrs[0]), *[_dptr(a) for a in arrs], None if xb is None else _dptr(xb),
+                                   Bx0, ByC, BzC)
 
     def divb(self) -> float:
         return self.L.orc_divb(self.h)

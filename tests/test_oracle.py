@@ -200,3 +200,45 @@ def test_ab3_predictor(oracle_built):
     assert 0 < d < 1e-2, d
     sc = b.scalars()
     assert sc["ootime"] < sc["otime"] < sc["time"]
+
+
+def _dipole_oracle(N=(16, 8, 8), series=None):
+    from mage_b200 import dipole
+    w = dipole.wind_code_units()
+    o = orc.Oracle(orc.OracleParams(*N, doBackground=True, M0=dipole.M0, wind=w, bc=(3, 4, 2, 2, 0, 0)),
+                   grids.spherical_corners(*N), "strict")
+    o.ic_dipole_wind(0.01, 31337)
+    if series is not None:
+        o.set_wind_series(**series)
+    assert o.init_finish() == 0
+    return o, w
+
+
+def test_wind_series_restates_the_constant_wind(oracle_built):
+    """A time series (apps/wind.F90:116-203, 766-868) whose rows all hold the
+    constant wind, with Bx0 = Bx and ByC = BzC = 0 so that readWind's tilted
+    front (Bx = Bx0 + ByC By + BzC Bz) keeps Bx, steps exactly like the
+    constant wind; a series that changes after 2 time units differs."""
+    from mage_b200 import dipole
+    w = dipole.wind_code_units()
+    # rows cover every lag time of the grid (|DelT| <= 30 / 4 here), so no
+    # point sees the null field of times before the series
+    n = 21
+    t = np.linspace(-100.0, 100.0, n)
+    const = dict(t=t, rho=np.full(n, w[0]), P=np.full(n, w[1]), V=np.tile(w[2:5], (n, 1)),
+                 B=np.tile(w[5:8], (n, 1)), Bx0=w[5])
+    a, _ = _dipole_oracle()
+    b, _ = _dipole_oracle(series=const)
+    assert a.step(5) == 0 and b.step(5) == 0
+    for k in ("Gas", "magFlux", "Bxyz"):
+        assert np.array_equal(a.array(k), b.array(k)), k
+    # a denser wind from t = 0 on: the ghost shell changes
+    var = dict(const)
+    rho = const["rho"].copy()
+    rho[t >= 0.0] *= 2.0
+    var["rho"] = rho
+    c, _ = _dipole_oracle(series=var)
+    assert c.step(1) == 0
+    a1, _ = _dipole_oracle()
+    assert a1.step(1) == 0
+    assert not np.array_equal(a1.array("Gas"), c.array("Gas"))
