@@ -346,7 +346,7 @@ def main():
         cur = {k: pinned(st[k]) for k in ("Gas", "magFlux", "Bxyz")}
         old = {"Gas": pinned(st["oGas"]), "magFlux": pinned(st["omagFlux"])}
         spare = {k: pinned(np.empty_like(st[k])) for k in ("Gas", "magFlux", "Bxyz")}
-        h2d = sum(cur[k].nbytes for k in cur)
+        h2d = cur["Gas"].nbytes + cur["magFlux"].nbytes
         d2h = sum(cur[k].nbytes for k in cur)
         time_, otime_, dt_, ts_ = st["time"], st["otime"], st["dt"], st["ts"]
         del st
@@ -355,7 +355,8 @@ def main():
         for _ in range(args.e2e_steps):
             # the driver's oState is the State before the last step, which the
             # device still holds: only the State crosses PCIe
-            g.upload_state(cur["Gas"], cur["magFlux"], cur["Bxyz"], None, None, time_, otime_, dt_, ts_)
+            # Bxyz is bFlux2Fld of the fluxes: computed on the device, not sent
+            g.upload_state(cur["Gas"], cur["magFlux"], None, None, None, time_, otime_, dt_, ts_)
             g.step_gamera(1)
             r = g.download_state(into=spare, old=False)
             # the host driver keeps oState = the previous State; rotate the pinned buffers
@@ -465,9 +466,10 @@ def main():
                                     "SM clock sampled in the timed region"} if w["problem"] == "bw" else None,
             "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "steps": args.e2e_steps,
-                    "what": "per step: gam_upload_state of the State from pinned host memory (oState stays on "
-                            "the device: the State before the last step), gam_step(1), gam_download_state (new State "
-                            "to pinned host memory)"},
+                    "what": "per step: gam_upload_state of State%Gas and State%magFlux from pinned host memory "
+                            "(Bxyz computed from the fluxes on the device; oState stays on the device: the State "
+                            "before the last step), gam_step(1), gam_download_state (new Gas, magFlux, Bxyz to "
+                            "pinned host memory)"},
             "fp32": fp32,
             "dipole": dip,
             "adjoint": adj,

@@ -111,7 +111,10 @@ int gam_get_geometry_arrays(gam_handle* h, double* face, double* xfc, double* Tf
  * oGas = omagFlux = NULL (after a first full upload): oState stays as it is
  * on the device and only State crosses PCIe. After gam_step the device's
  * oState is the State before that step (CopyState, mhdgroup.F90:202-256),
- * i.e. the oState of a driver that steps one AdvanceModel at a time. */
+ * i.e. the oState of a driver that steps one AdvanceModel at a time.
+ * Bxyz = NULL: State%Bxyz is computed on the device from the uploaded fluxes
+ * (bFlux2Fld, gridutils.F90:281-301, which every step and the
+ * initialisation end with), so only Gas and magFlux cross PCIe. */
 int gam_upload_state(gam_handle* h, const double* Gas, const double* magFlux, const double* Bxyz,
                      const double* oGas, const double* omagFlux, double time, double otime, double dt, int32_t ts);
 int gam_download_state(gam_handle* h, double* Gas, double* magFlux, double* Bxyz, double* oGas,

@@ -460,6 +460,23 @@ extern "C" int gam_get_geometry_arrays(gam_handle* h, double* face, double* xfc,
     return GAM_OK;
 }
 
+void gam_fast_bfield_f64(const Ctx<double>& C, int cur, cudaStream_t s);
+void gam_fast_bfield_f32(const Ctx<float>& C, int cur, cudaStream_t s);
+void gam_strict_bfield_f64(const Ctx<double>& C, int cur, cudaStream_t s);
+// State%Bxyz from State%magFlux on the device (a NULL Bxyz upload): the
+// bFlux2Fld every step and the initialisation end with (gamapp.F90:88,
+// init.F90:205), with this handle's kernels
+static int state_bfield(gam_handle* h) {
+    if (h->f32)
+        gam_fast_bfield_f32(h->cf, h->cur, h->s);
+    else if (h->p.strict)
+        gam_strict_bfield_f64(h->cd, h->cur, h->s);
+    else
+        gam_fast_bfield_f64(h->cd, h->cur, h->s);
+    CK(h, cudaGetLastError());
+    return GAM_OK;
+}
+
 template <class R>
 static int upload_state_t(gam_handle* h, Ctx<R>& C, const double* Gas, const double* magFlux, const double* Bxyz,
                           const double* oGas, const double* omagFlux) {
@@ -467,7 +484,8 @@ static int upload_state_t(gam_handle* h, Ctx<R>& C, const double* Gas, const dou
     h->cur = 0;
     if ((rc = up_r<R>(h, Gas, C.st[0].Gas, false, 5))) return rc;
     if ((rc = up_r<R>(h, magFlux, C.st[0].mf, true, 3))) return rc;
-    if ((rc = up_r<R>(h, Bxyz, C.st[0].B, false, 3))) return rc;
+    if (Bxyz && (rc = up_r<R>(h, Bxyz, C.st[0].B, false, 3))) return rc;
+    if (!Bxyz && (rc = state_bfield(h))) return rc;
     if ((rc = up_r<R>(h, oGas, C.st[1].Gas, false, 5))) return rc;
     if ((rc = up_r<R>(h, omagFlux, C.st[1].mf, true, 3))) return rc;
     if (C.oomf) CK(h, cudaMemcpyAsync(C.oomf, C.st[1].mf, 3 * h->b.fs * sizeof(R), cudaMemcpyDeviceToDevice, h->s));
@@ -498,14 +516,16 @@ static int upload_new_state_t(gam_handle* h, Ctx<R>& C, const double* Gas, const
     int rc;
     if ((rc = up_r<R>(h, Gas, C.st[h->cur].Gas, false, 5))) return rc;
     if ((rc = up_r<R>(h, magFlux, C.st[h->cur].mf, true, 3))) return rc;
-    if ((rc = up_r<R>(h, Bxyz, C.st[h->cur].B, false, 3))) return rc;
+    if (Bxyz && (rc = up_r<R>(h, Bxyz, C.st[h->cur].B, false, 3))) return rc;
+    if (!Bxyz && (rc = state_bfield(h))) return rc;
     return GAM_OK;
 }
 
 extern "C" int gam_upload_state(gam_handle* h, const double* Gas, const double* magFlux, const double* Bxyz,
                                 const double* oGas, const double* omagFlux, double time, double otime, double dt,
                                 int32_t ts) {
-    if (!h || !Gas || !magFlux || !Bxyz || (!oGas) != (!omagFlux)) return GAM_EINVAL;
+    if (!h || !Gas || !magFlux || (!oGas) != (!omagFlux)) return GAM_EINVAL;
+    if (!Bxyz && !h->haveGeo) return fail(h, GAM_ESTATE, "Bxyz = NULL is computed from the fluxes: set the geometry first");
     int rc;
     if (!oGas) {
         if (!h->haveState) return fail(h, GAM_ESTATE, "oState can stay on the device only after a first full upload");

@@ -10,6 +10,8 @@ void gam_fast_dt_f64(const Ctx<double>& C, int cur, cudaStream_t s) { gam_fast::
 void gam_fast_step_f32(const Ctx<float>& C, int cur, cudaStream_t s) { gam_fast::launch_step<float>(C, cur, s); }
 void gam_fast_dt_f32(const Ctx<float>& C, int cur, cudaStream_t s) { gam_fast::launch_dt_only<float>(C, cur, s); }
 void gam_fast_init_f64(const Ctx<double>& C, int cur, cudaStream_t s) { gam_fast::launch_init<double>(C, cur, s); }
+void gam_fast_bfield_f64(const Ctx<double>& C, int cur, cudaStream_t s) { gam_fast::launch_bfield<double>(C, cur, s); }
+void gam_fast_bfield_f32(const Ctx<float>& C, int cur, cudaStream_t s) { gam_fast::launch_bfield<float>(C, cur, s); }
 void gam_fast_init_f32(const Ctx<float>& C, int cur, cudaStream_t s) { gam_fast::launch_init<float>(C, cur, s); }
 void gam_fast_prepare_f64() { gam_fast::prepare<double>(); }
 void gam_fast_prepare_f32() { gam_fast::prepare<float>(); }

@@ -1761,6 +1761,14 @@ template <class R> void launch_dt_only(const Ctx<R>& C, int cur, cudaStream_t s)
 
 // CalcGridInfo after the initial condition (init.F90:217-238): Bxyz from the
 // fluxes, first EnforceBCs, oState = State.
+// bFlux2Fld of State (st[cur]) over every cell (gridutils.F90:281-301)
+template <class R> void launch_bfield(const Ctx<R>& C, int cur, cudaStream_t s) {
+    const GamBox& b = C.b;
+    const dim3 blk(32, 4, 1);
+    const Range cells{0, b.Ni - 1, 0, b.Nj - 1, 0, b.Nk - 1};
+    k_bfield_all<R><<<grid_for(cells, blk), blk, 0, s>>>(b, C.g, C.st[cur], C.sc);
+}
+
 template <class R> void launch_init(const Ctx<R>& C, int cur, cudaStream_t s) {
     const GamBox& b = C.b;
     const dim3 blk(32, 4, 1);

@@ -245,15 +245,16 @@ class GameraGPU:
     # --- state --------------------------------------------------------------
     def upload_state(self, Gas, magFlux, Bxyz, oGas, omagFlux, time: float, otime: float, dt: float, ts: int = 0):
         """oGas = omagFlux = None: oState stays on the device (after a step it is
-        the State before that step); only State is copied."""
+        the State before that step); only State is copied. Bxyz = None: computed
+        from magFlux on the device (bFlux2Fld)."""
         keep_old = oGas is None and omagFlux is None
         src = (Gas, magFlux, Bxyz) if keep_old else (Gas, magFlux, Bxyz, oGas, omagFlux)
-        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in src]
+        arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in src]
         shapes = [self.shape("cell", 5), self.shape("face", 3), self.shape("cell", 3), self.shape("cell", 5),
                   self.shape("face", 3)]
         for a, s in zip(arrs, shapes):
-            assert a.shape == s, (a.shape, s)
-        ptrs = [_ptr(a) for a in arrs] + ([None, None] if keep_old else [])
+            assert a is None or a.shape == s, (a.shape, s)
+        ptrs = [None if a is None else _ptr(a) for a in arrs] + ([None, None] if keep_old else [])
         self._check(self.L.gam_upload_state(self.h, *ptrs, time, otime, dt, int(ts)))
 
     def set_oostate(self, oomagFlux, ootime: float):

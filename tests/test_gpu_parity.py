@@ -323,3 +323,22 @@ def test_orszag_tang_symmetry_on_gpu(prec, bound):
     F[1:3] *= -1.0
     sym = float(np.sqrt(((G - F) ** 2).sum(axis=0)).sum() / (N * N))
     assert sym <= bound, sym
+
+
+def test_upload_without_bxyz(oracle_built):
+    """gam_upload_state with Bxyz = NULL computes State%Bxyz from the uploaded
+    fluxes on the device (bFlux2Fld, which every step ends with): after oracle
+    steps the result equals the oracle's Bxyz bit for bit (strict build), and
+    the run continues bit-exact."""
+    o, _ = make_oracle("bw", (16, 16, 16), variant="gm")
+    assert o.step(3) == 0
+    g = gpu_from_oracle(o, strict=True)
+    sc = o.scalars()
+    g.upload_state(o.array("Gas"), o.array("magFlux"), None, o.array("oGas"), o.array("omagFlux"), sc["time"],
+                   sc["otime"], sc["dt"], sc["ts"])
+    assert np.array_equal(g.download_state()["Bxyz"], o.array("Bxyz"))
+    assert o.step(5) == 0
+    g.step_gamera(5)
+    s = g.download_state()
+    for k in STATE:
+        assert np.array_equal(s[k], o.array(k)), k
