@@ -18,7 +18,10 @@ pytestmark = pytest.mark.gpu
 
 STATE = ("Gas", "magFlux", "Bxyz", "oGas", "omagFlux")
 
-CASES = [("ot", (32, 32, 4)), ("ot", (32, 32, 1)), ("bw", (16, 16, 16)), ("bw", (24, 16, 16))]
+# the last two: ragged J and K sizes (not multiples of 8, J and K of different
+# sizes), the smallest 3-D grid the step takes in J and K (4), and I = 40
+CASES = [("ot", (32, 32, 4)), ("ot", (32, 32, 1)), ("bw", (16, 16, 16)), ("bw", (24, 16, 16)), ("bw", (16, 5, 7)),
+         ("bw", (40, 4, 6))]
 
 
 @pytest.mark.parametrize("prob,N", CASES)
