@@ -172,6 +172,53 @@ def block_c2p(P, U):
 
 
 # ----------------------------------------------------------------- grid
+def _gather_adjoint_plan(src: torch.Tensor):
+    """Static plan for the adjoint of out[j] = x[src[j]] (the boundary
+    gather): positions that are their own source keep their adjoint, every
+    other position's adjoint is added to its source. The sources that receive
+    are grouped with their (at most K) destinations in a padded table, so the
+    reverse sum runs as K gathers in a fixed order (deterministic, unlike an
+    atomic scatter)."""
+    s = src.cpu().numpy()
+    n = s.size
+    j = np.arange(n)
+    self_src = s == j
+    gj = j[~self_src]
+    gs = s[~self_src]
+    order = np.argsort(gs, kind="stable")
+    gj, gs = gj[order], gs[order]
+    uniq, start, counts = np.unique(gs, return_index=True, return_counts=True)
+    K = int(counts.max()) if counts.size else 0
+    table = np.full((uniq.size, max(K, 1)), n, dtype=np.int64)  # n: a zero slot appended in backward
+    for k in range(K):
+        has = counts > k
+        table[has, k] = gj[start[has] + k]
+    dev = src.device
+    return {"keep": torch.as_tensor(self_src, device=dev), "recv": torch.as_tensor(uniq, device=dev),
+            "table": torch.as_tensor(table, device=dev), "K": K}
+
+
+class _GatherFn(torch.autograd.Function):
+    """x[:, src] with the deterministic reverse of _gather_adjoint_plan."""
+
+    @staticmethod
+    def forward(ctx, x, src, plan):
+        ctx.plan = plan
+        return x[:, src]
+
+    @staticmethod
+    def backward(ctx, g):
+        p = ctx.plan
+        gx = g * p["keep"].to(g.dtype)
+        if p["K"]:
+            gz = torch.cat([g, torch.zeros_like(g[:, :1])], dim=1)
+            acc = gz[:, p["table"][:, 0]]
+            for k in range(1, p["K"]):
+                acc = acc + gz[:, p["table"][:, k]]
+            gx[:, p["recv"]] += acc
+        return gx, None, None
+
+
 class Grid:
     """Metric tensors in the unpadded box convention (from the C ABI's
     Fortran-layout geometry arrays)."""
@@ -339,6 +386,7 @@ class Grid:
                 keep = (ii >= self.Ni) | (jj >= self.Nj) | (kk >= self.Nk)
                 src = np.where(keep, (kk * ny + jj) * nx + ii, src)
             self.bc_src[comp] = torch.as_tensor(src.reshape(-1), device=self.device)
+        self.bc_adj = {c: _gather_adjoint_plan(self.bc_src[c]) for c in self.bc_src}
 
     def bxyz(self, mf):
         """gamCellBxyz (gridutils.F90:648-680) on every cell of the box."""
@@ -589,9 +637,9 @@ def step(g: Grid, cur: dict, old: dict, dt: float, odt: float):
     if P.bc[0] in (3, 6) or P.bc[1] in (2, 4):
         Gas, mfn = _iside_bcs(g, Gas, mfn, g.bxyz(mfn))
     shp = Gas.shape
-    Gas = Gas.reshape(5, -1)[:, g.bc_src[-1]].reshape(shp)
+    Gas = _GatherFn.apply(Gas.reshape(5, -1), g.bc_src[-1], g.bc_adj[-1]).reshape(shp)
     mfs = mfn.reshape(3, -1)
-    mfn = torch.stack([mfs[d][g.bc_src[d]] for d in range(3)]).reshape(mfn.shape)
+    mfn = torch.stack([_GatherFn.apply(mfs[d:d + 1], g.bc_src[d], g.bc_adj[d])[0] for d in range(3)]).reshape(mfn.shape)
     return {"Gas": Gas, "mf": mfn, "B": g.bxyz(mfn)}
 
 
