@@ -1527,6 +1527,118 @@ static void initBW(const Model& M, const Grid& G, State& S, const BWParams& bp) 
     });
 }
 
+// ---------------------------------------------------------------- the reference's test problems
+// Default-real literals of the reference (single precision under gfortran),
+// as the double they become in mixed expressions
+static inline double R4(double x) { return (double)(float)x; }
+
+// gridutils.F90:144-189 GasIC2State: cell averages of the primitive function W
+template <class Fn> static void GasIC2State(const Model& M, const Grid& G, State& S, Fn W) {
+#pragma omp parallel for collapse(2)
+    for (int k = G.ks; k <= G.ke; k++)
+        for (int j = G.js; j <= G.je; j++)
+            for (int i = G.is; i <= G.ie; i++) {
+                double xyzC[8][3], ijkW[5];
+                cellCoords(G, i, j, k, xyzC);
+                double dV = G.volume(i, j, k);
+                GaussianVolumeIntegral(xyzC, W, ijkW);
+                for (int v = 0; v < 5; v++) ijkW[v] = ijkW[v] / dV;
+                double D = ijkW[DEN];
+                double Mx = D * ijkW[VELX], My = D * ijkW[VELY], Mz = D * ijkW[VELZ];
+                double P = ijkW[PRESSURE];
+                double KinE = 0.5 * (Mx * Mx + My * My + Mz * Mz) / D;
+                double IntE = P / (M.gamma - 1.0);
+                S.Gas(i, j, k, DEN) = D;
+                S.Gas(i, j, k, MOMX) = Mx;
+                S.Gas(i, j, k, MOMY) = My;
+                S.Gas(i, j, k, MOMZ) = Mz;
+                S.Gas(i, j, k, ENERGY) = IntE + KinE;
+            }
+}
+// pointwise gas at the cell centres of is..ie+1 (the loops of initADV1D,
+// initADV2D, initLoop, prob.F90:690, 758, 461) with zero face fluxes there
+template <class Fn> static void PointGas(const Model& M, const Grid& G, State& S, Fn W, bool zeroFlux) {
+    for (int k = G.ks; k <= G.ke + 1; k++)
+        for (int j = G.js; j <= G.je + 1; j++)
+            for (int i = G.is; i <= G.ie + 1; i++) {
+                double Wp[5];
+                W(G.xyzcc(i, j, k, 0), G.xyzcc(i, j, k, 1), G.xyzcc(i, j, k, 2), Wp);
+                double Rho = Wp[0], Vx = Wp[1], Vy = Wp[2], Vz = Wp[3], P = Wp[4];
+                S.Gas(i, j, k, DEN) = Rho;
+                S.Gas(i, j, k, MOMX) = Rho * Vx;
+                S.Gas(i, j, k, MOMY) = Rho * Vy;
+                S.Gas(i, j, k, MOMZ) = Rho * Vz;
+                double KinE = 0.5 * Rho * (Vx * Vx + Vy * Vy + Vz * Vz);
+                S.Gas(i, j, k, ENERGY) = KinE + P / (M.gamma - 1);
+                if (zeroFlux)
+                    for (int d = 0; d < 3; d++) S.magFlux(i, j, k, d) = 0.0;
+            }
+}
+// prob.F90:671-736 initADV1D: four shapes advected at speed 1 on [-1, 1]
+static void initADV1D(const Model& M, const Grid& G, State& S) {
+    PointGas(M, G, S, [](double xc, double, double, double* W) {
+        double Rho0 = R4(0.1);
+        double a = (xc + R4(0.7)) / R4(0.05);
+        double Rho1 = std::exp(-(a * a));
+        double Rho2 = std::fabs(xc + R4(0.3)) <= R4(0.1) ? 1.0 : 0.0;
+        double Rho3 = std::fabs(xc - R4(0.1)) <= R4(0.1) ? 1.0 - std::fabs(10.0 * (xc - R4(0.1))) : 0.0;
+        double q = (double)(0.1f * 0.1f) - (xc - 0.5) * (xc - 0.5);  // 0.1**2: a default-real constant
+        double Rho4 = q >= 0 ? 10.0 * std::sqrt(q) : 0.0;
+        W[0] = Rho0 + Rho1 + Rho2 + Rho3 + Rho4;
+        W[1] = 1.0; W[2] = 0.0; W[3] = 0.0; W[4] = 1.0;
+    }, true);
+}
+// prob.F90:739-797 initADV2D: a disc of twice the density advected at V0
+// along alpha (degrees from y), zero field
+static void initADV2D(const Model& M, const Grid& G, State& S, double V0, double alpha) {
+    const double Rho0 = 1.0, P0 = 1.0, R0 = 0.3, x0 = 0.0, y0 = 0.0;
+    PointGas(M, G, S, [&](double xc, double yc, double, double* W) {
+        double r = std::sqrt((xc - x0) * (xc - x0) + (yc - y0) * (yc - y0));
+        W[0] = r < R0 ? Rho0 * 2.0 : Rho0;
+        W[1] = V0 * std::sin(alpha * PI / 180.0);
+        W[2] = V0 * std::cos(alpha * PI / 180.0);
+        W[3] = 0.0;
+        W[4] = P0;
+    }, true);
+}
+// prob.F90:436-500 initLoop: a weak field loop (Az = max(0, A0 (R0 - r)))
+// advected at V0 along alpha
+static void initLoop2D(const Model& M, const Grid& G, State& S, double V0, double alpha) {
+    const double Rho0 = 1.0, P0 = 1.0, Vz0 = 0.0, A0 = 1.0e-3, R0 = 0.3, x0 = 0.0, y0 = 0.0;
+    PointGas(M, G, S, [&](double, double, double, double* W) {
+        W[0] = Rho0;
+        W[1] = V0 * std::sin(alpha * PI / 180.0);
+        W[2] = V0 * std::cos(alpha * PI / 180.0);
+        W[3] = Vz0;
+        W[4] = P0;
+    }, false);
+    VectorPot2Flux(G, S, [&](const double* p, double* A) {
+        double r = std::sqrt((p[0] - x0) * (p[0] - x0) + (p[1] - y0) * (p[1] - y0));
+        A[0] = 0.0;
+        A[1] = 0.0;
+        A[2] = std::max(0.0, A0 * (R0 - r));
+    });
+}
+// prob.F90:1027-1083 initALFVEN: circularly polarised Alfven wave along alp
+static void initAlfven(const Model& M, const Grid& G, State& S, double alp) {
+    const double Rho0 = 1.0, P0 = R4(0.1), B_para = 1.0, V_para = 0.0;
+    GasIC2State(M, G, S, [&](double x, double y, double, double* W) {
+        double ph = 2 * PI * (x * std::cos(alp) + y * std::sin(alp));
+        W[0] = Rho0;
+        W[1] = V_para * std::cos(alp) - R4(0.1) * std::sin(ph) * std::sin(alp);
+        W[2] = V_para * std::sin(alp) + R4(0.1) * std::sin(ph) * std::cos(alp);
+        W[3] = R4(0.1) * std::cos(ph);
+        W[4] = P0;
+    });
+    VectorPot2Flux(G, S, [&](const double* p, double* A) {
+        double x = p[0], y = p[1], z = p[2];
+        double ph = 2 * PI * (x * std::cos(alp) + y * std::sin(alp));
+        A[0] = B_para * std::sin(alp) * z;
+        A[1] = -1.0 * B_para * std::cos(alp) * z + R4(0.1) * std::sin(ph) / (2 * PI * std::cos(alp));
+        A[2] = R4(0.1) * std::cos(ph) / (2 * PI);
+    });
+}
+
 // ---------------------------------------------------------------- background field
 // msphutils.F90:534-551 Dipole, m = (0,0,M0)
 static void Dipole(double M0, const double* r, double* A) {
@@ -2172,6 +2284,17 @@ void orc_set_wind_series(void* h, int n, const double* t, const double* rho, con
     W.dtW = n > 1 ? W.tW[1] - W.tW[0] : 1.0;
     for (int r = 1; r + 1 < n; r++) W.dtW = std::min(W.dtW, W.tW[r + 1] - W.tW[r]);
     W.Bx0 = Bx0; W.ByC = ByC; W.BzC = BzC;
+}
+
+// the reference's test problems (prob.F90), parameters as in its decks
+void orc_ic_case(void* h, int which, double a, double b) {
+    App* A = (App*)h;
+    switch (which) {
+        case 0: initADV1D(A->M, A->G, A->S); break;
+        case 1: initADV2D(A->M, A->G, A->S, a, b); break;
+        case 2: initLoop2D(A->M, A->G, A->S, a, b); break;
+        default: initAlfven(A->M, A->G, A->S, a); break;
+    }
 }
 
 double orc_divb(void* h) {

@@ -142,6 +142,7 @@ def lib(variant: str = "strict") -> C.CDLL:
             getattr(L, f).argtypes = [C.c_double]
             getattr(L, f).restype = C.c_double
         L.orc_num_threads.restype = C.c_int
+        L.orc_ic_case.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double]
         L.orc_set_wind_series.argtypes = [C.c_void_p, C.c_int] + [C.POINTER(C.c_double)] * 6 + [C.c_double] * 3
         _libs[variant] = L
     return _libs[variant]
@@ -208,6 +209,11 @@ class Oracle:
         for k, v in kw.items():
             setattr(s, k, v)
         self.L.orc_set_scalars(self.h, C.byref(s))
+
+    def ic_case(self, name: str, a: float = 0.0, b: float = 0.0):
+        """The reference's test problems (prob.F90): 'adv1d'; 'adv2d' and 'loop2d'
+        with a = V0, b = alpha (degrees); 'alfven' with a = alp (radians)."""
+        self.L.orc_ic_case(self.h, {"adv1d": 0, "adv2d": 1, "loop2d": 2, "alfven": 3}[name], a, b)
 
     def set_wind_series(self, t, rho, P, V, B, xyzBS=None, Bx0=0.0, ByC=0.0, BzC=0.0):
         """Solar-wind time series of the outer-I wind boundary (code units)."""

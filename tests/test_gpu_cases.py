@@ -1,0 +1,75 @@
+"""The reference's own problem tests (tests/cases/testCases.pf) on the GPU
+product build, with their decks' parameters and pass criteria. The initial
+state comes from the CPU restatement of the problem set-ups (prob.F90) and is
+handed over through the C ABI; the GPU steps to tFin (the last dt lands on it).
+
+* testAdv1D / testAdv1D_8CENT (:114-180): L2 of the density after one
+  advection period <= 7e-3 (hydro, 128 cells; here 128 x 4 x 1 in 2.5-D, the
+  GPU's smallest J extent, each row checked);
+* testLoop2D (:32-58): total |face flux| kept to 0.5 %, dissipation <= 5 %;
+* testAdv2D (:60-86): total density kept to 0.01 %, dissipation <= 5 %;
+* testAlfven (:88-112): total |face flux| kept to 0.1 %, dissipation <= 1 %.
+"""
+import numpy as np
+import pytest
+
+from mage_b200 import grids
+from oracle.oracle import Oracle, OracleParams
+from tests.helpers import gpu_from_oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def _to_tfin(g, tFin):
+    t = g.download_state(old=False)["time"]
+    while tFin - t > 1e-15:
+        _, t = g.step_gamera(1)
+    return g.download_state(old=False)
+
+
+def _setup(N, bounds, case, a=0.0, b=0.0, **kw):
+    xyz = grids.uniform_corners(*N, bounds=bounds)
+    o = Oracle(OracleParams(*N, do25D=True, **kw), xyz, "strict")
+    o.ic_case(case, a, b)
+    assert o.init_finish() == 0
+    return o, gpu_from_oracle(o)
+
+
+@pytest.mark.parametrize("up7", [True, False], ids=["7UP", "8CENT"])
+def test_adv1d(oracle_built, up7):
+    o, g = _setup((128, 4, 1), (-1.0, 1.0, -0.5, 0.5, -0.5, 0.5), "adv1d", doMHD=False, gamma=1.4, pdmb=4.0,
+                  CFL=0.5 / 4.5, up7=up7, tFin=2.0)
+    # (the rows differ in the last bits from the start: the cell centres come
+    # from the metric's quadrature)
+    sD = o.array("Gas")[0, 4, 4:8, 4:132].copy()
+    s = _to_tfin(g, 2.0)
+    eD = s["Gas"][0, 4, 4:8, 4:132]
+    for row in range(4):
+        L2 = float(np.linalg.norm(sD[row] - eD[row]) / 128)
+        assert L2 <= 7.0e-3, (row, L2)
+
+
+def _flux_norm(mf):
+    return np.sqrt((mf * mf).sum(axis=0))
+
+
+@pytest.mark.parametrize("case,tol_total,tol_diss", [("loop2d", 0.005, 0.05), ("adv2d", 1.0e-4, 0.05)])
+def test_advected_loop_and_disc(oracle_built, case, tol_total, tol_diss):
+    o, g = _setup((256, 256, 1), (-0.5, 0.5, -0.5, 0.5, -0.5, 0.5), case, 1.41421356237, 45.0, pdmb=4.0,
+                  CFL=0.5 / 4.5, tFin=1.0)
+    q0 = _flux_norm(o.array("magFlux")) if case == "loop2d" else o.array("Gas")[0].copy()
+    s = _to_tfin(g, 1.0)
+    q1 = _flux_norm(s["magFlux"]) if case == "loop2d" else s["Gas"][0]
+    tot0 = q0.sum()
+    assert abs(q1.sum() - tot0) / tot0 <= tol_total, abs(q1.sum() - tot0) / tot0
+    assert np.abs(q0 - q1).sum() / tot0 <= tol_diss, np.abs(q0 - q1).sum() / tot0
+
+
+def test_alfven(oracle_built):
+    o, g = _setup((128, 256, 1), (0.0, 2.0, 0.0, 1.15470053838, -0.5, 0.5), "alfven", 1.0471975512, tFin=1.0)
+    q0 = _flux_norm(o.array("magFlux"))
+    s = _to_tfin(g, 1.0)
+    q1 = _flux_norm(s["magFlux"])
+    tot0 = q0.sum()
+    assert abs(q1.sum() - tot0) / tot0 <= 0.001, abs(q1.sum() - tot0) / tot0
+    assert np.abs(q0 - q1).sum() / tot0 <= 0.01, np.abs(q0 - q1).sum() / tot0

@@ -242,3 +242,22 @@ def test_wind_series_restates_the_constant_wind(oracle_built):
     a1, _ = _dipole_oracle()
     assert a1.step(1) == 0
     assert not np.array_equal(a1.array("Gas"), c.array("Gas"))
+
+
+@pytest.mark.parametrize("up7", [True, False], ids=["7UP", "8CENT"])
+def test_reference_adv1d_case(oracle_built, up7):
+    """tests/cases/testCases.pf:114-180 (testAdv1D, testAdv1D_8CENT) with its
+    decks adv1d.xml / adv1d_8cent.xml: hydro (gamma 1.4 from initADV1D,
+    prob.F90:671-736), pdmb 4 (so CFL = 0.5/4.5), 128 cells on [-1, 1], one
+    advection period (tFin 2); L2 = norm2(start - end density) / Nip <= 7e-3."""
+    N = (128, 1, 1)
+    xyz = grids.uniform_corners(*N, bounds=(-1.0, 1.0, -0.5, 0.5, -0.5, 0.5))
+    o = orc.Oracle(orc.OracleParams(*N, doMHD=False, gamma=1.4, pdmb=4.0, CFL=min(0.5 / 4.5, 0.3), up7=up7, tFin=2.0),
+                   xyz, "strict")
+    o.ic_case("adv1d")
+    assert o.init_finish() == 0
+    sD = o.array("Gas")[0, 4, 4, 4:132].copy()
+    while o.scalars()["t"] < 2.0:
+        assert o.step(1) == 0
+    L2 = float(np.linalg.norm(sD - o.array("Gas")[0, 4, 4, 4:132]) / 128)
+    assert L2 <= 7.0e-3, L2
