@@ -175,6 +175,17 @@ int gam_set_background(gam_handle* h, const double* fcB0, const double* bFlux0, 
 int gam_get_background(gam_handle* h, double* fcB0, double* bFlux0, double* edgB0, double* B0, double* dpB0);
 int gam_set_background_dipole(gam_handle* h, double M0);
 
+/* The reference's test problems (src/gamera/prob.F90) as initial conditions,
+ * then the initialisation order of gam_init_orszag_tang:
+ *   GAM_IC_ADV1D   initADV1D (:671-736), four shapes advected at speed 1
+ *                  (the reference sets gamma 1.4 for it: pass it in gam_params)
+ *   GAM_IC_ADV2D   initADV2D (:739-797), a = V0, b = alpha (degrees)
+ *   GAM_IC_LOOP2D  initLoop (:436-500), a = V0, b = alpha (degrees)
+ *   GAM_IC_ALFVEN  initALFVEN (:1027-1083), a = alp (radians)
+ * with the other prob/ keys at the reference's defaults. Needs gam_set_geometry. */
+enum { GAM_IC_ADV1D = 2, GAM_IC_ADV2D = 3, GAM_IC_LOOP2D = 4, GAM_IC_ALFVEN = 5 };
+int gam_init_test_problem(gam_handle* h, int32_t which, double a, double b);
+
 /* Solar-wind state of the outer-I boundary (bc[1] = GAM_BC_WIND), constant in
  * space and time: wind = {rho, P, Vx, Vy, Vz, Bx, By, Bz}. The blend weights
  * (wgtWind, apps/wind.F90:180-203) and the wind face fluxes of the ghost

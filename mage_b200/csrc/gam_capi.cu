@@ -43,6 +43,8 @@ void gam_geom_metric(const GamBox& b, const double* xyz, double* face, double* x
                      double* xyzcc, double* dijk, double* dl, double* edge, double* Te, double* Teb, cudaStream_t s);
 void gam_geom_ic_ot(const GamBox& b, const double* xyzcc, const double* face, double* Gas, double* mf, double gamma,
                     cudaStream_t s);
+void gam_geom_ic_case(const GamBox& b, const double* xyz, const double* xyzcc, const double* vol, double* Gas,
+                      double* mf, double* lA, double gamma, int which, double a, double bb, cudaStream_t s);
 void gam_geom_ic_bw(const GamBox& b, const double* xyz, const double* vol, double* Gas, double* mf, double* lA,
                     double gamma, const double* bw, bool doMHD, cudaStream_t s);
 void gam_geom_ic_wind(const GamBox& b, const double* xyz, double* Gas, double* mf, double* lA, double gamma,
@@ -233,6 +235,9 @@ extern "C" int gam_create(const gam_params* p, gam_handle** out) {
     if (p->Njp < 1 || p->Nkp < 1) return bad(GAM_EBADDIM, "Njp and Nkp must be >= 1");
     if (p->do25D && p->Nkp != 1) return bad(GAM_EBADDIM, "do25D needs Nkp == 1");
     if (!p->do25D && (p->Njp < 4 || p->Nkp < 4)) return bad(GAM_EBADDIM, "3-D grids need Njp, Nkp >= 4");
+    // the ghost fill is one gather whose sources are active cells: a periodic
+    // direction needs as many active layers as ghost layers
+    if (p->Njp < 4) return bad(GAM_EBADDIM, "Njp must be >= 4 (4 ghost layers are filled from active layers)");
     if (p->precision != GAM_FP64 && p->precision != GAM_FP32) return bad(GAM_EINVAL, "unknown precision");
     if (p->precision == GAM_FP32 && p->strict) return bad(GAM_EINVAL, "strict applies to the FP64 form only");
     {
@@ -890,6 +895,19 @@ extern "C" int gam_init_orszag_tang(gam_handle* h) {
     if (8 * h->b.fs > 27 * n_face(h->b)) return fail(h, GAM_EINVAL, "staging too small");
     gam_geom_fill(Gas64, 8 * h->b.fs, 0.0, h->s);
     gam_geom_ic_ot(h->b, h->gd.xyzcc, h->gd.face, Gas64, mf64, h->p.gamma, h->s);
+    return init_common(h, Gas64, mf64);
+}
+
+extern "C" int gam_init_test_problem(gam_handle* h, int32_t which, double a, double b) {
+    if (!h || which < GAM_IC_ADV1D || which > GAM_IC_ALFVEN) return GAM_EINVAL;
+    if (!h->haveXyz) return fail(h, GAM_ESTATE, "the problem set-ups integrate over cells and edges: call gam_set_geometry first");
+    if (11 * h->b.fs > 27 * n_face(h->b)) return fail(h, GAM_EINVAL, "staging too small");
+    double* Gas64 = h->staging;
+    double* mf64 = h->staging + 5 * h->b.fs;
+    double* lA = h->staging + 8 * h->b.fs;
+    gam_geom_fill(Gas64, 8 * h->b.fs, 0.0, h->s);
+    gam_geom_ic_case(h->b, h->gd.xyz, h->gd.xyzcc, h->gd.vol, Gas64, mf64, lA, h->p.gamma, which - GAM_IC_ADV1D, a, b,
+                     h->s);
     return init_common(h, Gas64, mf64);
 }
 

@@ -393,6 +393,110 @@ __global__ void k_ic_bw_gas(GamBox b, const double* __restrict__ xyz, const doub
     Gas[3 * fs + c] = Mz;
     Gas[4 * fs + c] = IntE + KinE;
 }
+// The reference's test problems (prob.F90), pointwise at the cell centres of
+// is..ie+1 x js..je+1 x ks..ke+1 like the reference's loops: 0 initADV1D
+// (:671-736), 1 initADV2D (:739-797), 2 initLoop's gas (:436-470); a = V0,
+// b = alpha (degrees). Default-real literals are the float values, as the
+// reference's single-precision constants under gfortran.
+__global__ void k_ic_case_gas(GamBox b, const double* __restrict__ xyzcc, double* Gas, double* mf, double gamma,
+                              int which, double a, double bdeg) {
+    int a0, a1, a2;
+    const int G = GAM_NG;
+    if (!tid3(b.Nip + 1, b.Njp + 1, b.Nkp + 1, a0, a1, a2)) return;
+    const long c = lidx(b, G + a0, G + a1, G + a2);
+    const long fs = b.fs;
+    const double PI = 3.141592653589793;
+    const double xc = xyzcc[c], yc = xyzcc[fs + c];
+    double Rho, Vx, Vy, Vz = 0.0, P;
+    if (which == 0) {
+        const double f01 = (double)0.1f;
+        const double q1 = (xc + (double)0.7f) / (double)0.05f;
+        double Rho1 = exp(-(q1 * q1));
+        double Rho2 = fabs(xc + (double)0.3f) <= f01 ? 1.0 : 0.0;
+        double Rho3 = fabs(xc - f01) <= f01 ? 1.0 - fabs(10.0 * (xc - f01)) : 0.0;
+        double q = (double)(0.1f * 0.1f) - (xc - 0.5) * (xc - 0.5);
+        double Rho4 = q >= 0 ? 10.0 * sqrt(q) : 0.0;
+        Rho = f01 + Rho1 + Rho2 + Rho3 + Rho4;
+        Vx = 1.0;
+        Vy = 0.0;
+        P = 1.0;
+    } else {
+        const double Rho0 = 1.0;
+        Vx = a * sin(bdeg * PI / 180.0);
+        Vy = a * cos(bdeg * PI / 180.0);
+        P = 1.0;
+        Rho = Rho0;
+        if (which == 1 && sqrt(xc * xc + yc * yc) < 0.3) Rho = Rho0 * 2.0;
+    }
+    Gas[c] = Rho;
+    Gas[fs + c] = Rho * Vx;
+    Gas[2 * fs + c] = Rho * Vy;
+    Gas[3 * fs + c] = Rho * Vz;
+    const double KinE = 0.5 * Rho * (Vx * Vx + Vy * Vy + Vz * Vz);
+    Gas[4 * fs + c] = KinE + P / (gamma - 1);
+    if (which != 2) {
+        mf[c] = 0.0;
+        mf[fs + c] = 0.0;
+        mf[2 * fs + c] = 0.0;
+    }
+}
+// GasIC2State (gridutils.F90:144-189) with the circularly polarised Alfven
+// wave of initALFVEN (prob.F90:1027-1083) along alp
+__global__ void k_ic_alf_gas(GamBox b, const double* __restrict__ xyz, const double* __restrict__ vol, double* Gas,
+                             double gamma, double alp) {
+    int a0, a1, a2;
+    const int G = GAM_NG;
+    if (!tid3(b.Nip, b.Njp, b.Nkp, a0, a1, a2)) return;
+    const int ii = G + a0, jj = G + a1, kk = G + a2;
+    const double PI = 3.141592653589793, f01 = (double)0.1f;
+    double C[8][3];
+    cell_corners(b, xyz, ii, jj, kk, C);
+    double I[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int i = 0; i < 12; i++)
+        for (int j = 0; j < 12; j++)
+            for (int k = 0; k < 12; k++) {
+                double xp[3], wg;
+                gauss_point(C, i, j, k, xp, wg);
+                const double ph = 2 * PI * (xp[0] * cos(alp) + xp[1] * sin(alp));
+                const double Wp[5] = {1.0, 0.0 * cos(alp) - f01 * sin(ph) * sin(alp),
+                                      0.0 * sin(alp) + f01 * sin(ph) * cos(alp), f01 * cos(ph), f01};
+                for (int v = 0; v < 5; v++) I[v] = I[v] + wg * Wp[v];
+            }
+    const long c = lidx(b, ii, jj, kk);
+    const long fs = b.fs;
+    const double dV = vol[c];
+    for (int v = 0; v < 5; v++) I[v] = I[v] / dV;
+    const double D = I[0];
+    const double Mx = D * I[1], My = D * I[2], Mz = D * I[3];
+    const double KinE = 0.5 * (Mx * Mx + My * My + Mz * Mz) / D;
+    Gas[c] = D;
+    Gas[fs + c] = Mx;
+    Gas[2 * fs + c] = My;
+    Gas[3 * fs + c] = Mz;
+    Gas[4 * fs + c] = I[4] / (gamma - 1.0) + KinE;
+}
+// the field loop's A = (0, 0, max(0, A0 (R0 - r))) (prob.F90:488-498) and the
+// Alfven wave's potential (prob.F90:1059-1067)
+struct PotLoop {
+    double A0, R0;
+    __device__ void operator()(const double* p, double* A) const {
+        const double r = sqrt(p[0] * p[0] + p[1] * p[1]);
+        A[0] = 0.0;
+        A[1] = 0.0;
+        A[2] = fmax(0.0, A0 * (R0 - r));
+    }
+};
+struct PotAlfven {
+    double alp;
+    __device__ void operator()(const double* p, double* A) const {
+        const double PI = 3.141592653589793, f01 = (double)0.1f;
+        const double ph = 2 * PI * (p[0] * cos(alp) + p[1] * sin(alp));
+        A[0] = 1.0 * sin(alp) * p[2];
+        A[1] = -1.0 * 1.0 * cos(alp) * p[2] + f01 * sin(ph) / (2 * PI * cos(alp));
+        A[2] = f01 * cos(ph) / (2 * PI);
+    }
+};
+
 // Vector potentials handed to VectorPot2Flux (gridutils.F90:193-237):
 // the blast wave's A = (0, bSclz x, bScl (y - x)) (prob.F90:252-262) and a
 // uniform field B as A = (B x r)/2.
@@ -698,6 +802,24 @@ void gam_geom_ic_bw(const GamBox& b, const double* xyz, const double* vol, doubl
     gam_geom_fill(lA, 3 * b.fs, 0.0, s);
     dim3 blk(32, 4, 1);
     k_ic_lA<PotBW><<<g3(b.Ni - 1, b.Nj - 1, b.Nk - 1, blk), blk, 0, s>>>(b, xyz, lA, PotBW{bScl, 0.0});
+    k_ic_flux<<<g3(b.Ni - 1, b.Nj - 1, b.Nk - 1, blk), blk, 0, s>>>(b, lA, mf);
+}
+
+// The reference's test problems: 0 ADV1D, 1 ADV2D (a = V0, b = alpha),
+// 2 LOOP2D (a = V0, b = alpha), 3 ALFVEN (a = alp). lA: 3-component scratch.
+void gam_geom_ic_case(const GamBox& b, const double* xyz, const double* xyzcc, const double* vol, double* Gas,
+                      double* mf, double* lA, double gamma, int which, double a, double bb, cudaStream_t s) {
+    dim3 blk(32, 4, 1);
+    if (which <= 2)
+        k_ic_case_gas<<<g3(b.Nip + 1, b.Njp + 1, b.Nkp + 1, blk), blk, 0, s>>>(b, xyzcc, Gas, mf, gamma, which, a, bb);
+    else
+        k_ic_alf_gas<<<g3(b.Nip, b.Njp, b.Nkp, dim3(64, 1, 1)), dim3(64, 1, 1), 0, s>>>(b, xyz, vol, Gas, gamma, a);
+    if (which < 2) return;
+    gam_geom_fill(lA, 3 * b.fs, 0.0, s);
+    if (which == 2)
+        k_ic_lA<PotLoop><<<g3(b.Ni - 1, b.Nj - 1, b.Nk - 1, blk), blk, 0, s>>>(b, xyz, lA, PotLoop{1.0e-3, 0.3});
+    else
+        k_ic_lA<PotAlfven><<<g3(b.Ni - 1, b.Nj - 1, b.Nk - 1, blk), blk, 0, s>>>(b, xyz, lA, PotAlfven{a});
     k_ic_flux<<<g3(b.Ni - 1, b.Nj - 1, b.Nk - 1, blk), blk, 0, s>>>(b, lA, mf);
 }
 

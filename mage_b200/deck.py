@@ -18,8 +18,12 @@ sections compared without regard to case, logicals read as Fortran list input
     sim/dFloor, then floors/dFloor; sim/pFloor, then floors/pFloor; TINY
   genGridXML (src/gamera/init.F90:564-790), uniform Cartesian only
     idir/jdir/kdir N, min, max
-  initOT2D / initBW (src/gamera/prob.F90:74-298) via sim/icType OT2D | BW
-    prob/x0, y0, z0 (0), D0 (1), P0 (0.1), pRat (100), dRat (1), rC (0.1), B0 (1)
+  the set-ups of src/gamera/prob.F90 via sim/icType
+    OT2D (:74-119); BW (:190-298) with prob/x0, y0, z0 (0), D0 (1), P0 (0.1),
+    pRat (100), dRat (1), rC (0.1), B0 (1); ADV1D (:671-736, physics/gamma
+    defaults to 1.4 for it); ADV2D (:739-797) and LOOP2D (:436-500) with
+    prob/V0 (1), alpha (60); ALFVEN (:1027-1083) with prob/alp (pi/3); their
+    other prob/ keys at the reference's defaults
 
 Keys that switch on parts the GPU step does not have (resistivity,
 multifluid, CPR, curvilinear grid generators, HDF5 grids or restarts, a moving
@@ -120,7 +124,10 @@ def params(d: Deck, precision: int = FP64, strict: bool = False) -> GamParams:
     pFloor = d.float("sim/pFloor", TINY)
     pFloor = d.float("floors/pFloor", pFloor)
     fixed = d.float("time/fixedTimestep", -1.0)
-    return GamParams(N[0], N[1], N[2], gamma=d.float("physics/gamma", 5.0 / 3.0), CFL=d.float("sim/CFL", C0),
+    if N[1] < 4:
+        raise ValueError("jdir/N < 4: the GPU step fills 4 ghost layers from active ones (use N >= 4 for a 1-D problem)")
+    gamma0 = 1.4 if d.str("sim/icType", "OT2D").upper() == "ADV1D" else 5.0 / 3.0  # initADV1D, prob.F90:682
+    return GamParams(N[0], N[1], N[2], gamma=d.float("physics/gamma", gamma0), CFL=d.float("sim/CFL", C0),
                      pdmb=pdmb, Vd0=d.float("sim/Vd0", 0.5),
                      cHogH=d.float("physics/cHogH", 0.25) if doHogs else 0.0,
                      cHogM=d.float("physics/cHogM", 0.25) if doHogs else 0.0,
@@ -151,17 +158,32 @@ def blast_wave_args(d: Deck) -> dict:
             "dRat": d.float("prob/dRat", 1.0), "rC": d.float("prob/rC", 0.1), "B0": d.float("prob/B0", 1.0)}
 
 
+# prob/ keys the device set-ups take at the reference's defaults only
+_FIXED_PROB = {"ADV2D": {"d0": 1.0, "P0": 1.0, "R0": 0.3, "x0": 0.0, "y0": 0.0},
+               "LOOP2D": {"d0": 1.0, "P0": 1.0, "Vz0": 0.0, "A0": 1.0e-3, "R0": 0.3, "x0": 0.0, "y0": 0.0},
+               "ALFVEN": {"d0": 1.0, "P0": 0.1, "B_para": 1.0, "V_para": 0.0}}
+
+
 def load(source: str, precision: int = FP64, strict: bool = False, lib_path: str = LIB_PATH):
     """A GameraGPU handle set up from the deck (grid, initial condition by
     sim/icType) and the deck itself."""
     d = Deck(source)
     ic = d.str("sim/icType", "OT2D").upper()
-    if ic not in ("OT2D", "BW"):
-        raise ValueError(f"sim/icType = {ic}: the GPU step has the OT2D and BW initial conditions")
+    if ic not in ("OT2D", "BW", "ADV1D", "ADV2D", "LOOP2D", "ALFVEN"):
+        raise ValueError(f"sim/icType = {ic}: not one of the set-ups of the GPU step")
+    for k, v in _FIXED_PROB.get(ic, {}).items():
+        if d.has(f"prob/{k}") and abs(d.float(f"prob/{k}", v) - v) > 1e-12 * max(1.0, abs(v)):
+            raise ValueError(f"prob/{k} = {d.str('prob/' + k, '')}: the GPU set-up of {ic} takes the default {v}")
     g = GameraGPU(params(d, precision, strict), lib_path=lib_path)
     g.set_geometry(corners(d))
     if ic == "OT2D":
         g.init_orszag_tang()
-    else:
+    elif ic == "BW":
         g.init_blast_wave(**blast_wave_args(d))
+    elif ic in ("ADV2D", "LOOP2D"):
+        g.init_test_problem(ic, d.float("prob/V0", 1.0), d.float("prob/alpha", 60.0))
+    elif ic == "ALFVEN":
+        g.init_test_problem(ic, d.float("prob/alp", float(np.pi) / 3.0))
+    else:
+        g.init_test_problem(ic)
     return g, d

@@ -124,6 +124,13 @@ module gamgpu
             type(c_ptr), value :: xyzBS
             real(c_double), value :: Bx0, ByC, BzC
         end function
+        ! the reference's test problems: which = 2 ADV1D, 3 ADV2D, 4 LOOP2D, 5 ALFVEN
+        integer(c_int) function gam_init_test_problem(h, which, a, b) bind(C, name="gam_init_test_problem")
+            import :: c_int, c_ptr, c_int32_t, c_double
+            type(c_ptr), value :: h
+            integer(c_int32_t), value :: which
+            real(c_double), value :: a, b
+        end function
         integer(c_int) function gam_set_inflow(h, state) bind(C, name="gam_set_inflow")
             import :: c_int, c_ptr, c_double
             type(c_ptr), value :: h

@@ -55,7 +55,7 @@ EXPORTED = (
     "gam_set_geometry_arrays", "gam_get_geometry_arrays", "gam_upload_state", "gam_download_state", "gam_step",
     "gam_calc_dt", "gam_divb", "gam_totals", "gam_last_step_ms", "gam_advance_model", "gam_init_orszag_tang",
     "gam_init_blast_wave", "gam_profile_step", "gam_totals_noalloc", "gam_set_background", "gam_get_background",
-    "gam_set_background_dipole", "gam_set_wind", "gam_set_wind_series", "gam_set_inflow", "gam_set_oostate", "gam_get_oostate", "gam_bounds_status", "gam_init_dipole_wind", "gam_write_restart", "gam_read_restart",
+    "gam_set_background_dipole", "gam_set_wind", "gam_set_wind_series", "gam_init_test_problem", "gam_set_inflow", "gam_set_oostate", "gam_get_oostate", "gam_bounds_status", "gam_init_dipole_wind", "gam_write_restart", "gam_read_restart",
     "gam_halo_bytes", "gam_halo_pack", "gam_halo_unpack", "gam_init_finish_halo", "gam_set_start", "gam_step_begin",
     "gam_dt_partial", "gam_step_end", "gam_set_slab_edges", "gam_flux_forward", "gam_flux_adjoint",
     "gam_efield_forward", "gam_efield_adjoint", "gam_predict_stage", "gam_update_stage",
@@ -101,6 +101,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     L.gam_set_background_dipole.argtypes = [C.c_void_p, C.c_double]
     L.gam_set_wind.argtypes = [C.c_void_p, _dp]
     L.gam_set_inflow.argtypes = [C.c_void_p, _dp]
+    L.gam_init_test_problem.argtypes = [C.c_void_p, C.c_int32, C.c_double, C.c_double]
     L.gam_set_wind_series.argtypes = [C.c_void_p, C.c_int32] + [_dp] * 6 + [C.c_double] * 3
     L.gam_set_oostate.argtypes = [C.c_void_p, _dp, C.c_double]
     L.gam_get_oostate.argtypes = [C.c_void_p, _dp, _dp]
@@ -297,6 +298,13 @@ class GameraGPU:
     # --- problems -------------------------------------------------------------
     def init_orszag_tang(self):
         self._check(self.L.gam_init_orszag_tang(self.h))
+
+    TEST_PROBLEMS = {"ADV1D": 2, "ADV2D": 3, "LOOP2D": 4, "ALFVEN": 5}
+
+    def init_test_problem(self, name: str, a: float = 0.0, b: float = 0.0):
+        """initADV1D / initADV2D (a = V0, b = alpha) / initLoop (a = V0, b = alpha) /
+        initALFVEN (a = alp) of prob.F90."""
+        self._check(self.L.gam_init_test_problem(self.h, self.TEST_PROBLEMS[name.upper()], float(a), float(b)))
 
     def init_blast_wave(self, x0=0.5, y0=0.5, z0=0.5, D0=1.0, P0=0.1, pRat=100.0, dRat=1.0, rC=0.1, B0=1.0):
         bw = np.array([x0, y0, z0, D0, P0, pRat, dRat, rC, B0], dtype=np.float64)

@@ -73,3 +73,44 @@ def test_alfven(oracle_built):
     tot0 = q0.sum()
     assert abs(q1.sum() - tot0) / tot0 <= 0.001, abs(q1.sum() - tot0) / tot0
     assert np.abs(q0 - q1).sum() / tot0 <= 0.01, np.abs(q0 - q1).sum() / tot0
+
+
+@pytest.mark.parametrize("case,N,bounds,kw,a,b", [
+    ("adv1d", (128, 4, 1), (-1.0, 1.0, -0.5, 0.5, -0.5, 0.5), dict(doMHD=False, gamma=1.4), 0.0, 0.0),
+    ("adv2d", (64, 64, 1), (-0.5, 0.5, -0.5, 0.5, -0.5, 0.5), {}, 1.41421356237, 45.0),
+    ("loop2d", (64, 64, 1), (-0.5, 0.5, -0.5, 0.5, -0.5, 0.5), {}, 1.41421356237, 45.0),
+    ("alfven", (64, 128, 1), (0.0, 2.0, 0.0, 1.15470053838, -0.5, 0.5), {}, 1.0471975512, 0.0)])
+def test_device_setups_match_oracle(oracle_built, case, N, bounds, kw, a, b):
+    """gam_init_test_problem (device set-ups of prob.F90) against the CPU
+    restatement's: equal to CUDA's sin/cos/exp against libm's (<= 1e-13)."""
+    from mage_b200.gamera import GameraGPU, GamParams
+    xyz = grids.uniform_corners(*N, bounds=bounds)
+    o = Oracle(OracleParams(*N, do25D=True, **kw), xyz, "strict")
+    o.ic_case(case, a, b)
+    assert o.init_finish() == 0
+    g = GameraGPU(GamParams(*N, do25D=True, **kw))
+    g.set_geometry(xyz)
+    g.init_test_problem(case, a, b)
+    s = g.download_state()
+    for k in ("Gas", "magFlux", "Bxyz"):
+        ref = o.array(k)
+        den = max(float(np.abs(ref).max()), 1e-300)
+        assert float(np.abs(s[k] - ref).max()) <= 1e-13 * den, (case, k)
+
+
+@pytest.mark.parametrize("deck_name,tol_total,tol_diss,what", [("loop2d_ref.xml", 0.005, 0.05, "flux"),
+                                                               ("adv2d_ref.xml", 1.0e-4, 0.05, "density"),
+                                                               ("alfven_ref.xml", 0.001, 0.01, "flux")])
+def test_reference_case_decks(deck_name, tol_total, tol_diss, what):
+    """The case decks' parameters through the product path (mage_b200.deck:
+    device set-up, GPU step to tFin) against testCases.pf's criteria."""
+    import os
+    from mage_b200 import deck
+    g, d = deck.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "decks", deck_name))
+    s0 = g.download_state(old=False)
+    q0 = _flux_norm(s0["magFlux"]) if what == "flux" else s0["Gas"][0].copy()
+    s = _to_tfin(g, d.float("time/tFin", 1.0))
+    q1 = _flux_norm(s["magFlux"]) if what == "flux" else s["Gas"][0]
+    tot0 = q0.sum()
+    assert abs(q1.sum() - tot0) / tot0 <= tol_total
+    assert np.abs(q0 - q1).sum() / tot0 <= tol_diss
