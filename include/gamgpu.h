@@ -346,6 +346,31 @@ int gam_update_stage(const gam_params* p, int32_t fp32, const void* const* in, c
                      const double* dpB0, double dt, void* const* out, const void* const* din, void* sU, void* sM,
                      void* const* dst, void* stream);
 
+/* One whole stepGamera of the differentiation form (fixed dt, AB2, 8CENT, no
+ * Boris) and its adjoint, on caller-owned device arrays in the layout above:
+ * the stages above plus the step's boundary conditions (periodic I and K,
+ * periodic or zero-gradient J; bcs.F90:279-450, 853-892, applied in
+ * EnforceBCs' order, step.F90:17-55) and bFlux2Fld (gridutils.F90:281-301).
+ * geo = {volume, face, xfc, xyzcc, dxf (fp32 only, else NULL), edge, Te, Teb,
+ * Tf}; bg = {fcB0, bFlux0, edgB0, dpB0} (FP64) with doBackground, else NULL;
+ * st = {curGas, curMf, oldGas, oldMf} (State and oState; the State's Bxyz is
+ * bFlux2Fld of its fluxes, as EnforceBCs leaves it); dt and odt = time - otime
+ * as for gam_predict_stage; work = gam_step_work_bytes bytes of device memory.
+ * gam_step_fwd_save writes nxt = {nxtGas, nxtMf, nxtB} (the State after the
+ * step, ghosts filled, Bxyz on every cell) and keeps the step's intermediate
+ * arrays in work. gam_step_adj adds into dst = {dcurGas, dcurMf, doldGas,
+ * doldMf} the adjoints of st for the adjoints dnxt = {dGas, dMf, dB} of nxt
+ * (dB may be NULL); saved = 1 reuses the intermediates that gam_step_fwd_save
+ * left in work for the same st, saved = 0 recomputes them first. Enqueued on
+ * stream; GAM_EINVAL for other boundaries, Boris, AB3, 7UP or 2.5-D.
+ * No counterpart in the reference, which has no adjoint. */
+int gam_step_work_bytes(const gam_params* p, int32_t fp32, int64_t* bytes);
+int gam_step_fwd_save(const gam_params* p, int32_t fp32, const void* const* geo, const double* const* bg,
+                      const void* const* st, double dt, double odt, void* const* nxt, void* work, void* stream);
+int gam_step_adj(const gam_params* p, int32_t fp32, const void* const* geo, const double* const* bg,
+                 const void* const* st, double dt, double odt, int32_t saved, const void* const* dnxt,
+                 void* const* dst, void* work, void* stream);
+
 /* Conserved totals for callers that cannot allocate device memory.
  * No counterpart in the reference. Some callers cannot call cudaMalloc while
  * they run: their device memory belongs to another framework's pool, or they

@@ -1,0 +1,416 @@
+// One whole stepGamera of the differentiation form and its adjoint behind two
+// C entry points (gam_step_fwd_save, gam_step_adj), on caller-owned device
+// arrays in the unpadded box layout of the stage entry points
+// (component-major (nc, Nk+1, Nj+1, Ni+1), i fastest). The stages are the
+// ones gam_predict_stage, gam_efield_*, gam_flux_* and gam_update_stage run;
+// this file adds what lies between them in the step:
+//   * bFlux2Fld / gamCellBxyz (gridutils.F90:281-301, 648-680) on every cell
+//     of the box, for the limiter field of the step's start and the field of
+//     its end, and the adjoint of that linear map;
+//   * the boundary conditions that copy values (periodic, bcs.F90:279-450;
+//     zero-gradient J, bcs.F90:853-892), which EnforceBCs (step.F90:17-55)
+//     applies I, then J, then K, composed into one source index per box
+//     position (the K rule acts on the position first, then J, then I), as a gather from the update's result, and the adjoint of that
+//     gather: every source position sums the adjoints of the positions copied
+//     from it in ascending index order (deterministic, no atomics). With a
+//     zero-gradient J the composed map is not a projection (the upper ghost
+//     faces of I copy J-ghost faces that the map itself fills), so the gather
+//     reads the update's result, never its own output.
+// Compiled with -fmad=false: the cell-field map evaluates in the same order
+// and rounding as the element-wise PyTorch restatement of the step, so both
+// give the same bits.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string.h>
+
+#include "../../include/gamgpu.h"
+
+namespace gam_stepadj {
+
+constexpr int G = 4;  // ghost layers (nG, init.F90:327)
+
+struct Box {
+    int Nip, Njp, Nkp, Ni, Nj, Nk;  // active cells; cells with ghosts
+    int nx, ny, nz;                 // box extents Ni+1, Nj+1, Nk+1
+    long n;                         // elements of one component
+    int bc[6];
+};
+
+Box make_box(const gam_params* p) {
+    Box b;
+    b.Nip = p->Nip; b.Njp = p->Njp; b.Nkp = p->Nkp;
+    b.Ni = b.Nip + 2 * G; b.Nj = b.Njp + 2 * G; b.Nk = b.Nkp + 2 * G;
+    b.nx = b.Ni + 1; b.ny = b.Nj + 1; b.nz = b.Nk + 1;
+    b.n = (long)b.nx * b.ny * b.nz;
+    for (int s = 0; s < 6; s++) b.bc[s] = p->bc[s];
+    return b;
+}
+
+// lower / upper ghost rule of one axis with nn active cells; `normal`: the
+// face flux of this axis' direction, whose upper face G+nn is active
+__device__ __forceinline__ int lo_rule(int kind, int x, int nn) {
+    if (x < G) {
+        if (kind == GAM_BC_PERIODIC) return x + nn;
+        if (kind == GAM_BC_ZEROGRAD) return G;
+    }
+    return x;
+}
+__device__ __forceinline__ int hi_rule(int kind, int x, int nn, bool normal) {
+    const bool m = normal ? (x >= G + nn + 1 && x <= G + nn + 4) : (x >= G + nn && x <= G + nn + 3);
+    if (m) {
+        if (kind == GAM_BC_PERIODIC) return x - nn;
+        if (kind == GAM_BC_ZEROGRAD) return normal ? G + nn : G + nn - 1;
+    }
+    return x;
+}
+// flat source index of box position (i, j, k); comp -1: cell values, 0/1/2:
+// face fluxes of direction comp. K rule, then J (over the cell ranges of i and
+// k only when J is not periodic), then I.
+__device__ __forceinline__ long bc_source(const Box& b, int comp, int i, int j, int k) {
+    if (comp < 0 && (i >= b.Ni || j >= b.Nj || k >= b.Nk)) return ((long)k * b.ny + j) * b.nx + i;
+    int sk = k;
+    if (b.bc[4] == GAM_BC_PERIODIC) sk = hi_rule(GAM_BC_PERIODIC, lo_rule(GAM_BC_PERIODIC, k, b.Nkp), b.Nkp, comp == 2);
+    const int sjm = hi_rule(b.bc[3], lo_rule(b.bc[2], j, b.Njp), b.Njp, comp == 1);
+    const bool cond = b.bc[2] == GAM_BC_PERIODIC || (i < b.Ni && sk < b.Nk);
+    const int sj = cond ? sjm : j;
+    int si = i;
+    if (b.bc[0] == GAM_BC_PERIODIC) si = hi_rule(GAM_BC_PERIODIC, lo_rule(GAM_BC_PERIODIC, i, b.Nip), b.Nip, comp == 0);
+    return ((long)sk * b.ny + sj) * b.nx + si;
+}
+
+__device__ __forceinline__ bool pos_of(const Box& b, long t, int& i, int& j, int& k) {
+    if (t >= b.n) return false;
+    i = (int)(t % b.nx);
+    j = (int)((t / b.nx) % b.ny);
+    k = (int)(t / ((long)b.nx * b.ny));
+    return true;
+}
+
+// out[c][t] = in[c][src(t)] for the nc components of a field
+template <class R>
+__global__ void k_bc_gather(Box b, int comp, int nc, const R* __restrict__ in, R* __restrict__ out) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    int i, j, k;
+    if (!pos_of(b, t, i, j, k)) return;
+    const long s = bc_source(b, comp, i, j, k);
+    for (int c = 0; c < nc; c++) out[c * b.n + t] = in[c * b.n + s];
+}
+
+// candidate positions of one axis that the ghost rules can send to x, in
+// ascending order: x - nn, x, x + nn and, for zero-gradient sides, the ghost
+// layer of the side x is the edge of
+__device__ __forceinline__ int axis_candidates(int x, int nn, int extent, bool zg_lo, bool zg_hi, int* out) {
+    int c[13], m = 0;
+    if (zg_lo && x == G)
+        for (int q = 0; q < G; q++) c[m++] = q;
+    c[m++] = x - nn;
+    c[m++] = x;
+    c[m++] = x + nn;
+    if (zg_hi && (x == G + nn - 1 || x == G + nn))
+        for (int q = 0; q <= G; q++) c[m++] = G + nn + q;
+    // insertion sort, keep the distinct in-range values
+    for (int a = 1; a < m; a++) {
+        const int v = c[a];
+        int q = a - 1;
+        while (q >= 0 && c[q] > v) {
+            c[q + 1] = c[q];
+            q--;
+        }
+        c[q + 1] = v;
+    }
+    int r = 0;
+    for (int a = 0; a < m; a++)
+        if (c[a] >= 0 && c[a] < extent && (r == 0 || out[r - 1] != c[a])) out[r++] = c[a];
+    return r;
+}
+
+// adjoint of the gather: out[c][s] = (g[c][s] if src(s) = s, else 0) +
+// (sum over t != s with src(t) = s, ascending t). The candidates t differ
+// from s by +-nn in i, j or k, or lie in the zero-gradient ghost layer next to
+// s; a position that is a source without being a fixed point is a J ghost,
+// copied only with its own j.
+template <class R>
+__global__ void k_bc_gather_adj(Box b, int comp, int nc, const R* __restrict__ g, R* __restrict__ out) {
+    const long s = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    int i, j, k;
+    if (!pos_of(b, s, i, j, k)) return;
+    const bool fixed = bc_source(b, comp, i, j, k) == s;
+    const bool zg = b.bc[2] == GAM_BC_ZEROGRAD;
+    int ci[13], cj[13], ck[13];
+    const int ni = b.bc[0] == GAM_BC_PERIODIC ? axis_candidates(i, b.Nip, b.nx, false, false, ci) : (ci[0] = i, 1);
+    const int nj = axis_candidates(j, b.Njp, b.ny, zg, b.bc[3] == GAM_BC_ZEROGRAD, cj);
+    const int nk = b.bc[4] == GAM_BC_PERIODIC ? axis_candidates(k, b.Nkp, b.nz, false, false, ck) : (ck[0] = k, 1);
+    for (int c = 0; c < nc; c++) {
+        const R* gc = g + c * b.n;
+        R acc = (R)0;
+        bool any = false;
+        for (int a = 0; a < nk; a++)
+            for (int e = 0; e < nj; e++)
+                for (int f = 0; f < ni; f++) {
+                    const long t = ((long)ck[a] * b.ny + cj[e]) * b.nx + ci[f];
+                    if (t == s || bc_source(b, comp, ci[f], cj[e], ck[a]) != s) continue;
+                    acc = any ? acc + gc[t] : gc[t];
+                    any = true;
+                }
+        const R own = fixed ? gc[s] : (R)0;
+        out[c * b.n + s] = any ? own + acc : own;
+    }
+}
+
+// gamCellBxyz on every cell of the box: B = (sum over faces of +-flux x face
+// centroid)/V - div * cell centroid / V in FP64; in FP32 with the face-minus-
+// cell centroid offsets dxf (x + 6 d: lower face of direction d, x + 3 + 6 d:
+// upper face)
+template <class R>
+__global__ void k_box_bxyz(Box b, const R* __restrict__ vol, const R* __restrict__ xfc, const R* __restrict__ xyzcc,
+                           const R* __restrict__ dxf, const R* __restrict__ mf, R* __restrict__ B) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    int i, j, k;
+    if (!pos_of(b, t, i, j, k) || i >= b.Ni || j >= b.Nj || k >= b.Nk) return;
+    const long n = b.n, sj = b.nx, sk = (long)b.nx * b.ny;
+    const R fI = mf[t], fIp = mf[t + 1], fJ = mf[n + t], fJp = mf[n + t + sj], fK = mf[2 * n + t],
+            fKp = mf[2 * n + t + sk];
+    const R dV = vol[t];
+    if (dxf) {
+        for (int x = 0; x < 3; x++) {
+            const R s = fIp * dxf[(x + 3) * n + t] + fJp * dxf[(x + 9) * n + t] + fKp * dxf[(x + 15) * n + t] -
+                        fI * dxf[x * n + t] - fJ * dxf[(x + 6) * n + t] - fK * dxf[(x + 12) * n + t];
+            B[x * n + t] = s / dV;
+        }
+        return;
+    }
+    const R Div = fIp - fI + fJp - fJ + fKp - fK;
+    for (int x = 0; x < 3; x++) {
+        const R s = fIp * xfc[x * n + t + 1] + fJp * xfc[(x + 3) * n + t + sj] + fKp * xfc[(x + 6) * n + t + sk] -
+                    fI * xfc[x * n + t] - fJ * xfc[(x + 3) * n + t] - fK * xfc[(x + 6) * n + t];
+        const R tt = s / dV;
+        B[x * n + t] = tt - Div * xyzcc[x * n + t] / dV;
+    }
+}
+
+// adjoint of k_box_bxyz: every face of direction d adds the adjoints of the
+// two cells it bounds (the cell below as its upper face, the cell at its own
+// index as its lower face)
+template <class R>
+__global__ void k_box_bxyz_adj(Box b, const R* __restrict__ vol, const R* __restrict__ xfc,
+                               const R* __restrict__ xyzcc, const R* __restrict__ dxf, const R* __restrict__ gB,
+                               R* __restrict__ dmf) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    int i, j, k;
+    if (!pos_of(b, t, i, j, k)) return;
+    const long n = b.n;
+    const long st[3] = {1, (long)b.nx, (long)b.nx * b.ny};
+    const int p[3] = {i, j, k};
+    const int N[3] = {b.Ni, b.Nj, b.Nk};
+    const bool inCell = i < b.Ni && j < b.Nj && k < b.Nk;
+    for (int d = 0; d < 3; d++) {
+        bool below = p[d] >= 1;
+        for (int a = 0; a < 3; a++)
+            if (p[a] >= N[a] + (a == d ? 1 : 0)) below = false;
+        R acc = (R)0;
+        if (below) {
+            const long c = t - st[d];
+            for (int x = 0; x < 3; x++) {
+                const R w = dxf ? dxf[(x + 3 + 6 * d) * n + c] : xfc[(x + 3 * d) * n + t] - xyzcc[x * n + c];
+                acc = acc + gB[x * n + c] * w / vol[c];
+            }
+        }
+        if (inCell) {
+            for (int x = 0; x < 3; x++) {
+                const R w = dxf ? dxf[(x + 6 * d) * n + t] : xfc[(x + 3 * d) * n + t] - xyzcc[x * n + t];
+                acc = acc - gB[x * n + t] * w / vol[t];
+            }
+        }
+        dmf[d * n + t] += acc;
+    }
+}
+
+unsigned blocks(long n, int blk) { return (unsigned)((n + blk - 1) / blk); }
+
+// work arrays, each of nc components; a start on 64 elements
+enum Slot {
+    QW, Wn, Dh, VdV, QB, abh, Bnf, bn, AVf, E, Blim, gF, mF,                                      // forward
+    dQW, dWn, dDh, dVdV, dQB, dabh, dBnf, dbn, dAVf, dE, dgF, dmF, dBlim, sU, sM, aB, dnG, dnM, tM,  // adjoint
+    NSLOT
+};
+constexpr int slot_nc[NSLOT] = {5, 5, 1, 3, 3, 3, 3, 3, 9, 3, 3, 15, 9,
+                                5, 5, 1, 3, 3, 3, 3, 3, 3, 3, 15, 9, 3, 5, 3, 3, 5, 3, 3};
+
+struct Work {
+    void* p[NSLOT];
+    size_t fwd_bytes, bytes;
+};
+Work layout(const Box& b, int fp32, void* base) {
+    const size_t es = fp32 ? 4 : 8;
+    Work w;
+    size_t off = 0;
+    for (int s = 0; s < NSLOT; s++) {
+        if (s == dQW) w.fwd_bytes = off;
+        w.p[s] = base ? (void*)((char*)base + off) : nullptr;
+        const size_t bytes = (size_t)slot_nc[s] * (size_t)b.n * es;
+        off += (bytes + 255) / 256 * 256;
+    }
+    w.bytes = off;
+    return w;
+}
+
+int check(const gam_params* p) {
+    if (!p) return GAM_EINVAL;
+    if (p->rmeth != GAM_RECON_8CENT || p->doBoris || p->doAB3 || !p->doLFMLim || !p->doMHD) return GAM_EINVAL;
+    if (p->nG != 4 || p->Nip < 1 || p->Njp < 4 || p->Nkp < 1 || p->do25D) return GAM_EBADDIM;
+    // boundaries: periodic I and K, periodic or zero-gradient J
+    if (p->bc[0] != GAM_BC_PERIODIC || p->bc[1] != GAM_BC_PERIODIC) return GAM_EINVAL;
+    if (p->bc[4] != GAM_BC_PERIODIC || p->bc[5] != GAM_BC_PERIODIC) return GAM_EINVAL;
+    const bool jp = p->bc[2] == GAM_BC_PERIODIC && p->bc[3] == GAM_BC_PERIODIC;
+    const bool jz = p->bc[2] == GAM_BC_ZEROGRAD && p->bc[3] == GAM_BC_ZEROGRAD;
+    if (!jp && !jz) return GAM_EINVAL;
+    return GAM_OK;
+}
+
+template <class R>
+int launch_bxyz(const Box& b, const void* const* geo, const void* mf, void* B, cudaStream_t s) {
+    k_box_bxyz<R><<<blocks(b.n, 256), 256, 0, s>>>(b, (const R*)geo[0], (const R*)geo[2], (const R*)geo[3],
+                                                   (const R*)geo[4], (const R*)mf, (R*)B);
+    return cudaGetLastError() == cudaSuccess ? GAM_OK : GAM_ECUDA;
+}
+template <class R>
+int launch_bxyz_adj(const Box& b, const void* const* geo, const void* gB, void* dmf, cudaStream_t s) {
+    k_box_bxyz_adj<R><<<blocks(b.n, 256), 256, 0, s>>>(b, (const R*)geo[0], (const R*)geo[2], (const R*)geo[3],
+                                                       (const R*)geo[4], (const R*)gB, (R*)dmf);
+    return cudaGetLastError() == cudaSuccess ? GAM_OK : GAM_ECUDA;
+}
+template <class R>
+int launch_gather(const Box& b, int comp, int nc, const void* in, void* out, cudaStream_t s) {
+    k_bc_gather<R><<<blocks(b.n, 256), 256, 0, s>>>(b, comp, nc, (const R*)in, (R*)out);
+    return cudaGetLastError() == cudaSuccess ? GAM_OK : GAM_ECUDA;
+}
+template <class R>
+int launch_gather_adj(const Box& b, int comp, int nc, const void* g, void* out, cudaStream_t s) {
+    k_bc_gather_adj<R><<<blocks(b.n, 128), 128, 0, s>>>(b, comp, nc, (const R*)g, (R*)out);
+    return cudaGetLastError() == cudaSuccess ? GAM_OK : GAM_ECUDA;
+}
+
+#define TRY(x)              \
+    do {                    \
+        int rc_ = (x);      \
+        if (rc_) return rc_; \
+    } while (0)
+
+// predictor, the limiter field of the start, electric field and fluxes into
+// the forward slots of the work area
+int forward_stages(const gam_params* p, int fp32, const Box& b, const Work& w, const void* const* geo,
+                   const double* const* bg, const void* const* st, double dt, double odt, cudaStream_t s) {
+    if (cudaMemsetAsync(w.p[0], 0, w.fwd_bytes, s) != cudaSuccess) return GAM_ECUDA;
+    const void* g5[5] = {geo[0], geo[1], geo[2], geo[3], geo[4]};
+    void* out8[8] = {w.p[QW], w.p[Wn], w.p[Dh], w.p[VdV], w.p[QB], w.p[abh], w.p[Bnf], w.p[bn]};
+    TRY(gam_predict_stage(p, fp32, st, g5, 0.5 * dt, odt, out8, nullptr, nullptr, nullptr, s));
+    TRY(fp32 ? launch_bxyz<float>(b, geo, st[1], w.p[Blim], s) : launch_bxyz<double>(b, geo, st[1], w.p[Blim], s));
+    TRY(gam_efield_forward(p, fp32, w.p[Dh], w.p[abh], w.p[bn], w.p[VdV], geo[0], geo[1], geo[5], geo[6], geo[7],
+                           bg ? bg[2] : nullptr, dt, w.p[AVf], w.p[E], s));
+    TRY(gam_flux_forward(p, fp32, w.p[QW], w.p[Wn], w.p[QB], w.p[Blim], w.p[Bnf], geo[0], geo[1], geo[8],
+                         bg ? bg[0] : nullptr, bg ? bg[1] : nullptr, w.p[gF], w.p[mF], s));
+    return GAM_OK;
+}
+
+int args_ok(const gam_params* p, const void* const* geo, const double* const* bg, const void* const* st, int fp32,
+            void* work) {
+    if (!geo || !st || !work) return GAM_EINVAL;
+    for (int q = 0; q < 9; q++)
+        if (!geo[q] && q != 4) return GAM_EINVAL;
+    if (fp32 && !geo[4]) return GAM_EINVAL;
+    for (int q = 0; q < 4; q++)
+        if (!st[q]) return GAM_EINVAL;
+    if (p->doBackground && (!bg || !bg[0] || !bg[1] || !bg[2] || !bg[3])) return GAM_EINVAL;
+    return GAM_OK;
+}
+
+}  // namespace gam_stepadj
+
+using namespace gam_stepadj;
+
+extern "C" int gam_step_work_bytes(const gam_params* p, int32_t fp32, int64_t* bytes) {
+    TRY(check(p));
+    if (!bytes) return GAM_EINVAL;
+    *bytes = (int64_t)layout(make_box(p), fp32, nullptr).bytes;
+    return GAM_OK;
+}
+
+extern "C" int gam_step_fwd_save(const gam_params* p, int32_t fp32, const void* const* geo, const double* const* bg,
+                                 const void* const* st, double dt, double odt, void* const* nxt, void* work,
+                                 void* stream) {
+    TRY(check(p));
+    TRY(args_ok(p, geo, bg, st, fp32, work));
+    if (!nxt || !nxt[0] || !nxt[1] || !nxt[2]) return GAM_EINVAL;
+    cudaStream_t s = (cudaStream_t)stream;
+    const Box b = make_box(p);
+    const Work w = layout(b, fp32, work);
+    const size_t es = fp32 ? 4 : 8;
+    TRY(forward_stages(p, fp32, b, w, geo, bg, st, dt, odt, s));
+    // applyUpdate into the work area (the adjoint's dnG, dnM arrays, free until
+    // gam_step_adj), nxtB as its scratch
+    void* upd[3] = {w.p[dnG], w.p[dnM], nxt[2]};
+    if (cudaMemsetAsync(w.p[dnG], 0, 5 * b.n * es, s) != cudaSuccess ||
+        cudaMemsetAsync(w.p[dnM], 0, 3 * b.n * es, s) != cudaSuccess ||
+        cudaMemsetAsync(nxt[2], 0, 3 * b.n * es, s) != cudaSuccess)
+        return GAM_ECUDA;
+    const void* in5[5] = {st[0], st[1], w.p[E], w.p[gF], w.p[mF]};
+    const void* g4[4] = {geo[0], geo[2], geo[3], geo[4]};
+    TRY(gam_update_stage(p, fp32, in5, g4, bg ? bg[3] : nullptr, dt, upd, nullptr, nullptr, nullptr, nullptr, s));
+    // EnforceBCs, then the closing bFlux2Fld
+    if (fp32) {
+        TRY(launch_gather<float>(b, -1, 5, upd[0], nxt[0], s));
+        for (int d = 0; d < 3; d++)
+            TRY(launch_gather<float>(b, d, 1, (float*)upd[1] + d * b.n, (float*)nxt[1] + d * b.n, s));
+    } else {
+        TRY(launch_gather<double>(b, -1, 5, upd[0], nxt[0], s));
+        for (int d = 0; d < 3; d++)
+            TRY(launch_gather<double>(b, d, 1, (double*)upd[1] + d * b.n, (double*)nxt[1] + d * b.n, s));
+    }
+    if (cudaMemsetAsync(nxt[2], 0, 3 * b.n * es, s) != cudaSuccess) return GAM_ECUDA;
+    return fp32 ? launch_bxyz<float>(b, geo, nxt[1], nxt[2], s) : launch_bxyz<double>(b, geo, nxt[1], nxt[2], s);
+}
+
+extern "C" int gam_step_adj(const gam_params* p, int32_t fp32, const void* const* geo, const double* const* bg,
+                            const void* const* st, double dt, double odt, int32_t saved, const void* const* dnxt,
+                            void* const* dst, void* work, void* stream) {
+    TRY(check(p));
+    TRY(args_ok(p, geo, bg, st, fp32, work));
+    if (!dnxt || !dnxt[0] || !dnxt[1] || !dst || !dst[0] || !dst[1] || !dst[2] || !dst[3]) return GAM_EINVAL;
+    cudaStream_t s = (cudaStream_t)stream;
+    const Box b = make_box(p);
+    const Work w = layout(b, fp32, work);
+    const size_t es = fp32 ? 4 : 8;
+    if (!saved) TRY(forward_stages(p, fp32, b, w, geo, bg, st, dt, odt, s));
+    if (cudaMemsetAsync(w.p[dQW], 0, w.bytes - w.fwd_bytes, s) != cudaSuccess) return GAM_ECUDA;
+    // adjoint of the state's field: B = bFlux2Fld(magFlux)
+    if (cudaMemcpyAsync(w.p[tM], dnxt[1], 3 * b.n * es, cudaMemcpyDeviceToDevice, s) != cudaSuccess) return GAM_ECUDA;
+    if (dnxt[2]) TRY(fp32 ? launch_bxyz_adj<float>(b, geo, dnxt[2], w.p[tM], s)
+                          : launch_bxyz_adj<double>(b, geo, dnxt[2], w.p[tM], s));
+    // adjoint of EnforceBCs
+    if (fp32) {
+        TRY(launch_gather_adj<float>(b, -1, 5, dnxt[0], w.p[dnG], s));
+        for (int d = 0; d < 3; d++)
+            TRY(launch_gather_adj<float>(b, d, 1, (float*)w.p[tM] + d * b.n, (float*)w.p[dnM] + d * b.n, s));
+    } else {
+        TRY(launch_gather_adj<double>(b, -1, 5, dnxt[0], w.p[dnG], s));
+        for (int d = 0; d < 3; d++)
+            TRY(launch_gather_adj<double>(b, d, 1, (double*)w.p[tM] + d * b.n, (double*)w.p[dnM] + d * b.n, s));
+    }
+    // applyUpdate, CalcStress, CalcElecField, the limiter field, Predictor
+    const void* in5[5] = {st[0], st[1], w.p[E], w.p[gF], w.p[mF]};
+    const void* g4[4] = {geo[0], geo[2], geo[3], geo[4]};
+    const void* dup[2] = {w.p[dnG], w.p[dnM]};
+    void* dsu[5] = {dst[0], dst[1], w.p[dE], w.p[dgF], w.p[dmF]};
+    TRY(gam_update_stage(p, fp32, in5, g4, bg ? bg[3] : nullptr, dt, nullptr, dup, w.p[sU], w.p[sM], dsu, s));
+    TRY(gam_flux_adjoint(p, fp32, w.p[QW], w.p[Wn], w.p[QB], w.p[Blim], w.p[Bnf], geo[0], geo[1], geo[8],
+                         bg ? bg[0] : nullptr, bg ? bg[1] : nullptr, w.p[dgF], w.p[dmF], w.p[dQW], w.p[dWn],
+                         w.p[dQB], w.p[dBlim], w.p[dBnf], s));
+    TRY(gam_efield_adjoint(p, fp32, w.p[Dh], w.p[abh], w.p[bn], w.p[VdV], geo[0], geo[1], geo[5], geo[6], geo[7],
+                           bg ? bg[2] : nullptr, dt, w.p[AVf], w.p[dE], w.p[dDh], w.p[dabh], w.p[dbn], w.p[dVdV],
+                           w.p[dAVf], s));
+    TRY(fp32 ? launch_bxyz_adj<float>(b, geo, w.p[dBlim], dst[1], s)
+             : launch_bxyz_adj<double>(b, geo, w.p[dBlim], dst[1], s));
+    const void* g5[5] = {geo[0], geo[1], geo[2], geo[3], geo[4]};
+    const void* din8[8] = {w.p[dQW], w.p[dWn], w.p[dDh], w.p[dVdV], w.p[dQB], w.p[dabh], w.p[dBnf], w.p[dbn]};
+    return gam_predict_stage(p, fp32, st, g5, 0.5 * dt, odt, nullptr, din8, w.p[aB], dst, s);
+}

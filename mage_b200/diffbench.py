@@ -30,7 +30,7 @@ import numpy as np
 import torch
 
 from mage_b200 import dipole, grids
-from mage_b200.diffstep import DiffParams, Grid, cell_c2p, cell_p2c, loss_and_grad, loss_b2, run, win, G
+from mage_b200.diffstep import DiffParams, Grid, cell_c2p, cell_p2c, loss_and_grad, loss_and_grad_c, loss_b2, run, win, G
 from mage_b200.gamera import GameraGPU, GamParams
 from mage_b200.workloads import DIPOLE_BCS
 
@@ -97,6 +97,14 @@ def c4(N=(64, 64, 64), nsteps=20, sigma=1e-3, seed=2024):
         out[name] = {"loss": L, "fwd_plus_adjoint_s": el, "peak_hbm_gb": mem}
         grads[name] = (gG, gF)
     out["fp32_grad_rel_l2_vs_fp64"] = _rel_l2(grads["fp32"], grads["fp64"])
+    # the same sweep through the whole-step C entry points (gam_step_fwd_save,
+    # gam_step_adj: boundary gathers and bFlux2Fld adjoints on the device too)
+    for name, dtype in (("fp64", torch.float64), ("fp32", torch.float32)):
+        gg = g if dtype == torch.float64 else Grid(DiffParams(*N), geo, dtype=dtype, device="cuda")
+        loss_and_grad_c(gg, Gas64.to(dtype), mf64.to(dtype), dt, nsteps)
+        (L, gG, gF), el, mem = _timed(lambda: loss_and_grad_c(gg, Gas64.to(dtype), mf64.to(dtype), dt, nsteps))
+        out[name + "_whole_step_c"] = {"loss": L, "fwd_plus_adjoint_s": el, "peak_hbm_gb": mem,
+                                       "grad_rel_l2_vs_autograd_sweep": _rel_l2((gG, gF), grads[name])}
     # the same FP64 gradient with the flux stage differentiated by autograd
     # instead of the hand-written CUDA adjoint
     g.cuda_flux = False

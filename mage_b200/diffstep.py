@@ -866,6 +866,72 @@ class _UpdateFn(torch.autograd.Function):
         return (*dst, None, None)
 
 
+class WholeStep:
+    """One stepGamera and its adjoint as one C call each (gam_step_fwd_save,
+    gam_step_adj): the stage kernels of the classes above plus the step's
+    boundary gathers and bFlux2Fld on the device, without autograd. Periodic
+    I and K, periodic or zero-gradient J; the work area (gam_step_work_bytes)
+    holds one step's intermediate arrays."""
+
+    def __init__(self, g: Grid):
+        import ctypes as C
+        from mage_b200.gamera import GamError, GamParams, load_library
+        P = g.P
+        self.g, self.L = g, load_library()
+        self.p = GamParams(P.Nip, P.Njp, P.Nkp, gamma=P.gamma, CFL=P.CFL, pdmb=P.pdmb, Vd0=P.Vd0, cHogH=P.cHogH,
+                           dFloor=P.dFloor, pFloor=P.pFloor, doBackground=g.bg is not None, bc=tuple(P.bc)).to_c()
+        self.f32 = int(g.dtype == torch.float32)
+        nb = C.c_int64()
+        rc = self.L.gam_step_work_bytes(C.byref(self.p), self.f32, C.byref(nb))
+        if rc != 0:
+            raise GamError(rc, "gam_step_work_bytes: the whole-step adjoint does not cover these parameters")
+        self.work = torch.empty(nb.value, dtype=torch.uint8, device=g.device)
+        self._geo = [g.vol, g.face, g.xfc, g.xyzcc, g.dxf if self.f32 else None, g.edge, g.Te, g.Teb, g.Tf]
+        self._geo = [t.contiguous() if t is not None else None for t in self._geo]
+        self.geo = _vp([t.data_ptr() if t is not None else 0 for t in self._geo])
+        self.bg = None
+        if g.bg is not None:
+            self._bg = [g.bg[k].contiguous() for k in ("fcB0", "bFlux0", "edgB0", "dpB0")]
+            self.bg = _vp([t.data_ptr() for t in self._bg])
+
+    def _st(self, cur, old):
+        ts = [t.contiguous() for t in (cur["Gas"], cur["mf"], old["Gas"], old["mf"])]
+        return ts, _vp([t.data_ptr() for t in ts])
+
+    def forward(self, cur: dict, old: dict, dt: float, odt: float) -> dict:
+        """State after the step (gam_step_fwd_save); cur/old as for step()."""
+        import ctypes as C
+        from mage_b200.gamera import GamError
+        ts, st = self._st(cur, old)
+        nxt = {"Gas": torch.empty_like(ts[0]), "mf": torch.empty_like(ts[1]), "B": torch.empty_like(ts[1])}
+        rc = self.L.gam_step_fwd_save(C.byref(self.p), self.f32, self.geo, self.bg, st, float(dt), float(odt),
+                                      _vp([nxt[k].data_ptr() for k in ("Gas", "mf", "B")]),
+                                      C.c_void_p(self.work.data_ptr()),
+                                      C.c_void_p(torch.cuda.current_stream().cuda_stream))
+        if rc != 0:
+            raise GamError(rc, "gam_step_fwd_save failed")
+        return nxt
+
+    def adjoint(self, cur: dict, old: dict, dt: float, odt: float, dnxt: dict, acc=None, saved: bool = False):
+        """Adjoints (dcurGas, dcurMf, doldGas, doldMf) of the step's start for
+        the adjoints dnxt = {"Gas", "mf", "B" (optional)} of its result, added
+        to acc (four tensors) when given (gam_step_adj)."""
+        import ctypes as C
+        from mage_b200.gamera import GamError
+        ts, st = self._st(cur, old)
+        dn = [dnxt["Gas"].contiguous(), dnxt["mf"].contiguous()]
+        dB = dnxt.get("B")
+        dB = dB.contiguous() if dB is not None else None
+        dst = [a.contiguous() for a in acc] if acc is not None else [torch.zeros_like(t) for t in ts]
+        rc = self.L.gam_step_adj(C.byref(self.p), self.f32, self.geo, self.bg, st, float(dt), float(odt), int(saved),
+                                 _vp([dn[0].data_ptr(), dn[1].data_ptr(), dB.data_ptr() if dB is not None else 0]),
+                                 _vp([t.data_ptr() for t in dst]), C.c_void_p(self.work.data_ptr()),
+                                 C.c_void_p(torch.cuda.current_stream().cuda_stream))
+        if rc != 0:
+            raise GamError(rc, "gam_step_adj failed")
+        return dst
+
+
 def _face_proj(g: Grid, d: int, idx, B):
     """face * (n . B) on face d at box index idx (zeroGrad_obcI, bcs.F90:842-844)."""
     t = [g.Tf[q + 9 * d][idx] for q in range(3)]
@@ -1057,3 +1123,48 @@ def loss_and_grad(g: Grid, Gas0, mf0, dt: float, nsteps: int, seg: int | None = 
             lam_cur = dict(zip(("Gas", "mf", "B"), gl[:3]))
             lam_old = dict(zip(("Gas", "mf", "B"), gl[3:]))
     raise AssertionError("unreachable")
+
+
+def loss_and_grad_c(g: Grid, Gas0, mf0, dt: float, nsteps: int, seg: int | None = None, lossf=loss_b2):
+    """loss_and_grad through the whole-step C entry points: the same
+    checkpointing (the (State, oState) pair at the start of each segment of
+    seg steps), the segment's states recomputed with gam_step_fwd_save, then
+    gam_step_adj one step at a time backwards; autograd only for the loss's
+    own gradient. The adjoint of oState at step n is the adjoint of State at
+    step n-1, so it seeds that step's accumulators."""
+    ws = WholeStep(g)
+    seg = seg or max(1, int(round(nsteps ** 0.5)))
+    with torch.no_grad():
+        cur = {"Gas": Gas0.contiguous(), "mf": mf0.contiguous(), "B": g.bxyz(mf0)}
+        old = cur
+        ckpt = []
+        n = 0
+        while n < nsteps:
+            ckpt.append((n, cur, old))
+            for _ in range(min(seg, nsteps - n)):
+                cur, old = ws.forward(cur, old, dt, dt), cur
+            n += min(seg, nsteps - n)
+        fin = {k: v.detach().clone().requires_grad_(True) for k, v in cur.items()}
+    with torch.enable_grad():
+        L = lossf(g, fin)
+        gl = torch.autograd.grad(L, [fin["Gas"], fin["mf"], fin["B"]], allow_unused=True)
+    lam = {k: (torch.zeros_like(fin[k]) if v is None else v) for k, v in zip(("Gas", "mf", "B"), gl)}
+    carry = None  # adjoint of the oState of the step after the current one
+    with torch.no_grad():
+        for n0, c0, o0 in reversed(ckpt):
+            m = min(seg, nsteps - n0)
+            sts = [(c0, o0)]
+            for _ in range(m - 1):
+                c, o = sts[-1]
+                sts.append((ws.forward(c, o, dt, dt), c))
+            for c, o in reversed(sts):
+                acc = [torch.zeros_like(c["Gas"]), torch.zeros_like(c["mf"]), torch.zeros_like(o["Gas"]),
+                       torch.zeros_like(o["mf"])]
+                if carry is not None:
+                    acc[0].add_(carry[0])
+                    acc[1].add_(carry[1])
+                d = ws.adjoint(c, o, dt, dt, lam, acc)
+                lam = {"Gas": d[0], "mf": d[1]}
+                carry = (d[2], d[3])
+    # step 0 starts from State = oState = (Gas0, mf0)
+    return float(L.detach()), lam["Gas"] + carry[0], lam["mf"] + carry[1]

@@ -288,6 +288,30 @@ module gamgpu
             type(c_ptr), value :: dpB0, out, din, sU, sM, dst, stream
             real(c_double), value :: dt
         end function
+        integer(c_int) function gam_step_work_bytes(p, fp32, bytes) bind(C, name="gam_step_work_bytes")
+            import :: c_int, c_int32_t, c_int64_t, gam_params
+            type(gam_params), intent(in) :: p
+            integer(c_int32_t), value :: fp32
+            integer(c_int64_t), intent(out) :: bytes
+        end function
+        integer(c_int) function gam_step_fwd_save(p, fp32, geo, bg, st, dt, odt, nxt, work, stream) &
+                bind(C, name="gam_step_fwd_save")
+            import :: c_int, c_ptr, c_int32_t, c_double, gam_params
+            type(gam_params), intent(in) :: p
+            integer(c_int32_t), value :: fp32
+            type(c_ptr), intent(in) :: geo(9), st(4), nxt(3)
+            type(c_ptr), value :: bg, work, stream
+            real(c_double), value :: dt, odt
+        end function
+        integer(c_int) function gam_step_adj(p, fp32, geo, bg, st, dt, odt, saved, dnxt, dst, work, stream) &
+                bind(C, name="gam_step_adj")
+            import :: c_int, c_ptr, c_int32_t, c_double, gam_params
+            type(gam_params), intent(in) :: p
+            integer(c_int32_t), value :: fp32, saved
+            type(c_ptr), intent(in) :: geo(9), st(4), dnxt(3), dst(4)
+            type(c_ptr), value :: bg, work, stream
+            real(c_double), value :: dt, odt
+        end function
         integer(c_int) function gam_write_restart(h, path) bind(C, name="gam_write_restart")
             import :: c_int, c_ptr, c_char
             type(c_ptr), value :: h

@@ -58,7 +58,8 @@ EXPORTED = (
     "gam_set_background_dipole", "gam_set_wind", "gam_set_wind_series", "gam_init_test_problem", "gam_set_inflow", "gam_set_oostate", "gam_get_oostate", "gam_bounds_status", "gam_init_dipole_wind", "gam_write_restart", "gam_read_restart",
     "gam_halo_bytes", "gam_halo_pack", "gam_halo_unpack", "gam_init_finish_halo", "gam_set_start", "gam_step_begin",
     "gam_dt_partial", "gam_step_end", "gam_set_slab_edges", "gam_flux_forward", "gam_flux_adjoint",
-    "gam_efield_forward", "gam_efield_adjoint", "gam_predict_stage", "gam_update_stage",
+    "gam_efield_forward", "gam_efield_adjoint", "gam_predict_stage", "gam_update_stage", "gam_step_work_bytes",
+    "gam_step_fwd_save", "gam_step_adj",
 )
 
 # Background-field arrays (Grid_T, gamtypes.F90:233-242): name, components;
@@ -119,6 +120,11 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
                                     C.c_void_p, _vpp, C.c_void_p]
     L.gam_update_stage.argtypes = [C.POINTER(_Params), C.c_int32, _vpp, _vpp, _dp, C.c_double, _vpp, _vpp,
                                    C.c_void_p, C.c_void_p, _vpp, C.c_void_p]
+    L.gam_step_work_bytes.argtypes = [C.POINTER(_Params), C.c_int32, C.POINTER(C.c_int64)]
+    L.gam_step_fwd_save.argtypes = [C.POINTER(_Params), C.c_int32, _vpp, _vpp, _vpp, C.c_double, C.c_double, _vpp,
+                                    C.c_void_p, C.c_void_p]
+    L.gam_step_adj.argtypes = [C.POINTER(_Params), C.c_int32, _vpp, _vpp, _vpp, C.c_double, C.c_double, C.c_int32,
+                               _vpp, _vpp, C.c_void_p, C.c_void_p]
     L.gam_halo_pack.argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
     L.gam_halo_unpack.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32]
     L.gam_init_finish_halo.argtypes = [C.c_void_p, _dp]

@@ -47,3 +47,25 @@ def test_fortran_module_binds_every_entry_point():
         if "::" in line:
             names += [n.strip().split("(")[0] for n in line.split("::")[1].split(",") if n.strip()]
     assert names == [f for f, _ in gamera._Params._fields_], names
+
+
+def test_whole_step_work_bytes_and_coverage():
+    """gam_step_work_bytes (host arithmetic only): the work area of the
+    whole-step adjoint is 146 box-sized arrays, each started on 256 bytes; the
+    entry points refuse what the adjoint does not cover (inner-I inflow,
+    Boris, 7UP)."""
+    L = gamera.load_library()
+    nb = C.c_int64()
+    N = (16, 24, 8)
+    box = (N[0] + 9) * (N[1] + 9) * (N[2] + 9)
+    nc = [5, 5, 1, 3, 3, 3, 3, 3, 9, 3, 3, 15, 9, 5, 5, 1, 3, 3, 3, 3, 3, 3, 3, 15, 9, 3, 5, 3, 3, 5, 3, 3]
+    assert sum(nc) == 146
+    for fp32, es in ((0, 8), (1, 4)):
+        p = gamera.GamParams(*N).to_c()
+        assert L.gam_step_work_bytes(C.byref(p), fp32, C.byref(nb)) == 0
+        assert nb.value == sum((c * box * es + 255) // 256 * 256 for c in nc)
+    p = gamera.GamParams(*N, bc=(0, 0, 2, 2, 0, 0)).to_c()
+    assert L.gam_step_work_bytes(C.byref(p), 0, C.byref(nb)) == 0
+    for kw in ({"bc": (6, 2, 2, 2, 0, 0)}, {"doBoris": True, "Ca": 1.0}, {"rmeth": gamera.RECON_7UP}):
+        p = gamera.GamParams(*N, **kw).to_c()
+        assert L.gam_step_work_bytes(C.byref(p), 0, C.byref(nb)) == gamera.GAM_EINVAL, kw
