@@ -26,7 +26,8 @@ __device__ __forceinline__ double sgnz(double x) { return x > 0.0 ? 1.0 : (x < 0
 // reverse of lrs_from_qdv (8CENT) for one variable: scatter the adjoints of
 // Ql, Qr to the 8-point operand stencil and the 4-point limiter stencil
 template <class R>
-__device__ void lrs_adj(R pdmb, const R* qdv, const R* v, R Vi, double aL, double aR, double* aq, double* av) {
+__device__ void lrs_adj(R pdmb, const R* qdv, const R* v, R Vi, double rVi, double aL, double aR, double* aq,
+                        double* av) {
     R s = (R)0;
 #pragma unroll
     for (int n = 0; n < 8; n++) s += Rc<R>(w8(n)) * qdv[n];
@@ -59,7 +60,7 @@ __device__ void lrs_adj(R pdmb, const R* qdv, const R* v, R Vi, double aL, doubl
     if (maxV < Qi) a_maxV = a_t; else a_Qi = a_t;
     if (v2 < v1) a2 += a_minV; else a1 += a_minV;
     if (v1 < v2) a2 += a_maxV; else a1 += a_maxV;
-    const double a_s = a_Qi / (double)Vi;
+    const double a_s = a_Qi * rVi;
 #pragma unroll
     for (int n = 0; n < 8; n++) aq[n] = w8(n) * a_s;
     av[0] = a0; av[1] = a1; av[2] = a2; av[3] = a3;
@@ -74,18 +75,20 @@ __device__ void mag_adj(const DevParams<R>& P, double sgn, const R* W, const R* 
     const double Bx = Bm[0], By = Bm[1], Bz = Bm[2];
     const double N[3] = {T[0], T[1], T[2]};
     const double dPb = 0.5 * (Bx * Bx + By * By + Bz * Bz);
+    const double rD = 1.0 / D;
     double S[3] = {Bx, By, Bz};
     double Va2;
     if (P.doBackground) {
         S[0] += B0[0]; S[1] += B0[1]; S[2] += B0[2];
-        Va2 = (S[0] * S[0] + S[1] * S[1] + S[2] * S[2]) / D;
+        Va2 = (S[0] * S[0] + S[1] * S[1] + S[2] * S[2]) * rD;
     } else {
-        Va2 = 2.0 * dPb / D;
+        Va2 = 2.0 * dPb * rD;
     }
     const double Vn = N[0] * W[1] + N[1] * W[2] + N[2] * W[3];
-    const double den = 2.0 * Pr / D + Va2;
+    const double den = 2.0 * Pr * rD + Va2;
     const double lam = 1.0 / den;
     const double s = sqrt(lam);
+    const double rs = sqrt(den);  // 1 / s
     const double z = sgn * s * Vn;
     const double Vn0 = 0.5 * erfc(z);
     const double B[3] = {Bx, By, Bz};
@@ -112,20 +115,20 @@ __device__ void mag_adj(const DevParams<R>& P, double sgn, const R* W, const R* 
     if (P.doBackground)
         for (int x = 0; x < 3; x++) aB[x] += sumCN * B0[x];
     if (Va2 > 0.0) a_Va2 += aVaD * 0.25 / sqrt(Va2);
-    const double a_z = a_Vn0 * (-exp(-z * z) / sqrt(PI_D));
+    const double a_z = a_Vn0 * (-exp(-z * z) * (1.0 / sqrt(PI_D)));
     const double a_s = a_z * sgn * Vn;
     a_Vn += a_z * sgn * s;
-    const double a_lam = a_s * 0.5 / s;
+    const double a_lam = a_s * 0.5 * rs;
     const double a_den = -a_lam * lam * lam;
-    aW[4] += a_den * 2.0 / D;
-    aW[0] += -a_den * 2.0 * Pr / (D * D);
+    aW[4] += a_den * 2.0 * rD;
+    aW[0] += -a_den * 2.0 * Pr * rD * rD;
     a_Va2 += a_den;
     if (P.doBackground) {
-        for (int x = 0; x < 3; x++) aB[x] += a_Va2 * 2.0 * S[x] / D;
-        aW[0] += -a_Va2 * (S[0] * S[0] + S[1] * S[1] + S[2] * S[2]) / (D * D);
+        for (int x = 0; x < 3; x++) aB[x] += a_Va2 * 2.0 * S[x] * rD;
+        aW[0] += -a_Va2 * (S[0] * S[0] + S[1] * S[1] + S[2] * S[2]) * rD * rD;
     } else {
-        a_dPb += a_Va2 * 2.0 / D;
-        aW[0] += -a_Va2 * 2.0 * dPb / (D * D);
+        a_dPb += a_Va2 * 2.0 * rD;
+        aW[0] += -a_Va2 * 2.0 * dPb * rD * rD;
     }
     for (int x = 0; x < 3; x++) {
         aW[1 + x] += a_Vn * N[x];
@@ -139,21 +142,24 @@ template <class R>
 __device__ void gas_adj(const DevParams<R>& P, double sgn, const R* W, const R* T, const double* aG, const double* aDW,
                         double* aW) {
     const double D = W[0], Pr = W[4], V[3] = {W[1], W[2], W[3]};
-    const double gm1 = P.gm1;
+    const double gm1 = P.gm1, rgm1 = 1.0 / gm1;
     const double V2 = V[0] * V[0] + V[1] * V[1] + V[2] * V[2];
-    const double E = 0.5 * D * V2 + Pr / gm1;
-    const double lam = D / (2.0 * Pr);
+    const double E = 0.5 * D * V2 + Pr * rgm1;
+    const double r2P = 1.0 / (2.0 * Pr);
+    const double lam = D * r2P;
     double N[3], T1[3], T2[3];
     for (int x = 0; x < 3; x++) { N[x] = T[x]; T1[x] = T[3 + x]; T2[x] = T[6 + x]; }
     const double Vn = N[0] * V[0] + N[1] * V[1] + N[2] * V[2];
     const double Vt1 = T1[0] * V[0] + T1[1] * V[1] + T1[2] * V[2];
     const double Vt2 = T2[0] * V[0] + T2[1] * V[1] + T2[2] * V[2];
     const double s = sqrt(lam);
+    const double rs = 1.0 / s;
     const double z = sgn * s * Vn;
     const double Vn0 = 0.5 * erfc(z);
     const double ex = exp(-(lam * Vn * Vn));
-    const double sq = sqrt(PI_D * lam);
-    const double Vn1 = Vn * Vn0 - 0.5 * sgn * ex / sq;
+    const double sq = sqrt(PI_D) * s;
+    const double rsq = rs * (1.0 / sqrt(PI_D));
+    const double Vn1 = Vn * Vn0 - 0.5 * sgn * ex * rsq;
     double a_fMn = 0.0, a_fMt1 = 0.0, a_fMt2 = 0.0;
     for (int x = 0; x < 3; x++) {
         a_fMn += aG[1 + x] * N[x];
@@ -173,20 +179,20 @@ __device__ void gas_adj(const DevParams<R>& P, double sgn, const R* W, const R* 
     // Vn1 = Vn Vn0 - 0.5 sgn ex / sq
     a_Vn += a_Vn1 * Vn0;
     a_Vn0 += a_Vn1 * Vn;
-    const double a_ex = -a_Vn1 * 0.5 * sgn / sq;
-    const double a_sq = a_Vn1 * 0.5 * sgn * ex / (sq * sq);
-    double a_lam = a_sq * PI_D * 0.5 / sq;
+    const double a_ex = -a_Vn1 * 0.5 * sgn * rsq;
+    const double a_sq = a_Vn1 * 0.5 * sgn * ex * rsq * rsq;
+    double a_lam = a_sq * PI_D * 0.5 * rsq;
     a_lam += -a_ex * ex * Vn * Vn;
     a_Vn += -a_ex * ex * 2.0 * lam * Vn;
-    const double a_z = a_Vn0 * (-exp(-z * z) / sqrt(PI_D));
+    const double a_z = a_Vn0 * (-exp(-z * z) * (1.0 / sqrt(PI_D)));
     const double a_s = a_z * sgn * Vn;
     a_Vn += a_z * sgn * s;
-    a_lam += a_s * 0.5 / s;
-    a_D += a_lam / (2.0 * Pr);
-    a_Pr += -a_lam * D / (2.0 * Pr * Pr);
+    a_lam += a_s * 0.5 * rs;
+    a_D += a_lam * r2P;
+    a_Pr += -a_lam * D * 2.0 * r2P * r2P;
     a_D += a_E * 0.5 * V2;
     for (int x = 0; x < 3; x++) a_V[x] += a_E * D * V[x];
-    a_Pr += a_E / gm1;
+    a_Pr += a_E * rgm1;
     for (int x = 0; x < 3; x++) a_V[x] += a_Vn * N[x] + a_Vt1 * T1[x] + a_Vt2 * T2[x];
     aW[0] += a_D;
     aW[1] += a_V[0];
@@ -265,14 +271,15 @@ __global__ void __launch_bounds__(128, (sizeof(R) == 8 ? 3 : 4)) k_stress_adj(Ga
     }
     // reverse of the reconstruction: scatter to the stencils
     double aq[8], av[4];
+    const double rVi = 1.0 / (double)Vi;
     for (int v = 0; v < 5; v++) {
-        lrs_adj(P.pdmb, qW[v], nW[v], Vi, aWL[v], aWR[v], aq, av);
+        lrs_adj(P.pdmb, qW[v], nW[v], Vi, rVi, aWL[v], aWR[v], aq, av);
         for (int n = 0; n < 8; n++) atomicAdd(&dQW[v * fs + c + (n - 4) * s], (R)aq[n]);
         for (int m = 0; m < 4; m++) atomicAdd(&dWn[v * fs + c + (m - 2) * s], (R)av[m]);
     }
     if (P.doMHD)
         for (int x = 0; x < 3; x++) {
-            lrs_adj(P.pdmb, qB[x], nB[x], Vi, aBL[x], aBR[x], aq, av);
+            lrs_adj(P.pdmb, qB[x], nB[x], Vi, rVi, aBL[x], aBR[x], aq, av);
             for (int n = 0; n < 8; n++) atomicAdd(&dQB[x * fs + c + (n - 4) * s], (R)aq[n]);
             for (int m = 0; m < 4; m++) atomicAdd(&dBlim[x * fs + c + (m - 2) * s], (R)av[m]);
         }
@@ -294,7 +301,7 @@ __device__ void edge_lrs_adj(const GamBox& b, const DevParams<R>& P, const Geo<R
     for (int m = 0; m < 4; m++) nmag[m] = w.bn[a * fs + c + (m - 2) * s];
     const R Vi = central8(area);
     double aq[8], av[4];
-    lrs_adj(P.pdmb, qdv, nmag, Vi, aBL * (double)Vi, aBR * (double)Vi, aq, av);
+    lrs_adj(P.pdmb, qdv, nmag, Vi, 1.0 / (double)Vi, aBL * (double)Vi, aBR * (double)Vi, aq, av);
     for (int n = 0; n < 8; n++) atomicAdd(&dabh[a * fs + c + (n - 4) * s], (R)aq[n]);
     for (int m = 0; m < 4; m++) atomicAdd(&dbn[a * fs + c + (m - 2) * s], (R)av[m]);
 }
@@ -362,27 +369,32 @@ __global__ void __launch_bounds__(128) k_vxb_adj(GamBox b, DevParams<R> P, Geo<R
     const double a_vDiff = a_e * P.Vd0 * Jd, a_Jd = a_e * P.Vd0 * vDiff;
     const double a_vDp = (cap < vDp) ? 0.0 : a_vDiff;
     double a_b1 = a_b1e, a_b2 = a_b2e, a_v1t = a_v1, a_v2t = a_v2;
-    const double a_m = a_vDp / (double)q;
-    const double a_q = -a_vDp * (double)m / ((double)q * (double)q);
-    const double a_Dc = a_q * 0.5 / (double)q;
+    const double rq = 1.0 / (double)q;
+    const double a_m = a_vDp * rq;
+    const double a_q = -a_vDp * (double)m * rq * rq;
+    const double a_Dc = a_q * 0.5 * rq;
     if (m > (R)0) {
-        a_b1 += a_m * b1 / m;
-        a_b2 += a_m * b2 / m;
+        const double rm = 1.0 / (double)m;
+        a_b1 += a_m * b1 * rm;
+        a_b2 += a_m * b2 * rm;
     }
     if (vD0 > (R)0) {
-        a_v1t += a_vDp * v1 / vD0;
-        a_v2t += a_vDp * v2 / vD0;
+        const double rv = 1.0 / (double)vD0;
+        a_v1t += a_vDp * v1 * rv;
+        a_v2t += a_vDp * v2 * rv;
     }
     const double a_bT1 = a_b1 * detT * ynj - a_b2 * detT * xnj;
     const double a_bT2 = -a_b1 * detT * yni + a_b2 * detT * xni;
     const double a_db2 = a_Jd, a_db1 = -a_Jd;
-    const double aT1R = a_db1 / fA1 + a_bT1 * 0.5 / fA1, aT1L = -a_db1 / fA1 + a_bT1 * 0.5 / fA1;
-    const double aT2R = a_db2 / fA2 + a_bT2 * 0.5 / fA2, aT2L = -a_db2 / fA2 + a_bT2 * 0.5 / fA2;
+    const double rA1 = 1.0 / (double)fA1, rA2 = 1.0 / (double)fA2;
+    const double aT1R = (a_db1 + a_bT1 * 0.5) * rA1, aT1L = (-a_db1 + a_bT1 * 0.5) * rA1;
+    const double aT2R = (a_db2 + a_bT2 * 0.5) * rA2, aT2L = (-a_db2 + a_bT2 * 0.5) * rA2;
     edge_lrs_adj(b, P, g, w, c, dT1, dT2, aT1L, aT1R, dabh, dbn);
     edge_lrs_adj(b, P, g, w, c, dT2, dT1, aT2L, aT2R, dabh, dbn);
+    const double rdA = 1.0 / (double)dA;
     for (int x = 0; x < 3; x++) {
-        const double aVC = a_v1t * T1[x] + a_v2t * T2[x];
-        for (int n = 0; n < 8; n++) atomicAdd(&dAVf[x * fs + c + (n - 4) * s2v], (R)(w8(n) * aVC / (double)dA));
+        const double aVC = (a_v1t * T1[x] + a_v2t * T2[x]) * rdA;
+        for (int n = 0; n < 8; n++) atomicAdd(&dAVf[x * fs + c + (n - 4) * s2v], (R)(w8(n) * aVC));
     }
     const long cc[4] = {c, c - s1, c - s2, c - s1 - s2};
     for (int n = 0; n < 4; n++) atomicAdd(&dDh[cc[n]], (R)(0.25 * a_Dc));
@@ -403,8 +415,9 @@ __global__ void __launch_bounds__(256) k_m2f_adj(GamBox b, Geo<R> g, int eD, Ran
     for (int n = 0; n < 8; n++) vol[n] = g.vol[c + (n - 4) * s];
     const R dV = rmax(central8(vol), (R)TINY);
     const R A = g.face[dT1 * fs + c];
+    const double AdV = (double)A / (double)dV;
     for (int x = 0; x < 3; x++) {
-        const double a = (double)dAVf[x * fs + c] * (double)A / (double)dV;
+        const double a = (double)dAVf[x * fs + c] * AdV;
         if (a == 0.0) continue;
         for (int n = 0; n < 8; n++) atomicAdd(&dVdV[x * fs + c + (n - 4) * s], (R)(w8(n) * a));
     }
@@ -413,8 +426,8 @@ __global__ void __launch_bounds__(256) k_m2f_adj(GamBox b, Geo<R> g, int eD, Ran
 // ----------------------------------------------------------------- predictor and update
 // reverse of cell_c2p (CellC2P): aW (5) -> aU (5)
 __device__ void c2p_adj(double dF, double pF, double gm1, const double* U, const double* aW, double* aU) {
-    const double rho = U[0];
-    const double V[3] = {U[1] / rho, U[2] / rho, U[3] / rho};
+    const double rho = U[0], rr = 1.0 / rho;
+    const double V[3] = {U[1] * rr, U[2] * rr, U[3] * rr};
     const double KinE = 0.5 * rho * (V[0] * V[0] + V[1] * V[1] + V[2] * V[2]);
     const double p = gm1 * (U[4] - KinE);
     double a_rho = (rho < dF) ? 0.0 : aW[0];
@@ -424,8 +437,8 @@ __device__ void c2p_adj(double dF, double pF, double gm1, const double* U, const
     a_rho += a_KinE * 0.5 * (V[0] * V[0] + V[1] * V[1] + V[2] * V[2]);
     for (int x = 0; x < 3; x++) a_V[x] += a_KinE * rho * V[x];
     for (int x = 0; x < 3; x++) {
-        aU[1 + x] += a_V[x] / rho;
-        a_rho += -a_V[x] * V[x] / rho;
+        aU[1 + x] += a_V[x] * rr;
+        a_rho += -a_V[x] * V[x] * rr;
     }
     aU[0] += a_rho;
     aU[4] += a_E;
@@ -445,27 +458,27 @@ __device__ void p2c_adj(double dF, double pF, double gm1, const double* W, const
 }
 // reverse of block_c2p (BlockCon2Prim): aW (5) -> aU (5)
 __device__ void bc2p_adj(double dF, double pF, double gm1, const double* U, const double* aW, double* aU) {
-    const double D = U[0] < dF ? dF : U[0];
+    const double D = U[0] < dF ? dF : U[0], rD = 1.0 / D;
     const double M[3] = {U[1], U[2], U[3]};
     const double M2 = M[0] * M[0] + M[1] * M[1] + M[2] * M[2];
-    const double KinE = 0.5 * M2 / D;
+    const double KinE = 0.5 * M2 * rD;
     const double p = gm1 * (U[4] - KinE);
     double a_D = aW[0], a_M[3];
     for (int x = 0; x < 3; x++) {
-        a_M[x] = aW[1 + x] / D;
-        a_D += -aW[1 + x] * M[x] / (D * D);
+        a_M[x] = aW[1 + x] * rD;
+        a_D += -aW[1 + x] * M[x] * rD * rD;
     }
     double a_E = 0.0, a_KinE = 0.0;
     if (!(p < pF)) { a_E = aW[4] * gm1; a_KinE = -aW[4] * gm1; }
-    for (int x = 0; x < 3; x++) a_M[x] += a_KinE * M[x] / D;
-    a_D += -a_KinE * 0.5 * M2 / (D * D);
+    for (int x = 0; x < 3; x++) a_M[x] += a_KinE * M[x] * rD;
+    a_D += -a_KinE * 0.5 * M2 * rD * rD;
     aU[0] += (U[0] < dF) ? 0.0 : a_D;
     for (int x = 0; x < 3; x++) aU[1 + x] += a_M[x];
     aU[4] += a_E;
 }
 
-// d B_x / d (flux of face f of cell c), f = 0..5 (I-, I+, J-, J+, K-, K+), as
-// in gamCellBxyz: (xfc - xyzcc)/V with the sign of the face
+// V d B_x / d (flux of face f of cell c), f = 0..5 (I-, I+, J-, J+, K-, K+),
+// as in gamCellBxyz: xfc - xyzcc with the sign of the face
 template <class R>
 __device__ __forceinline__ double dbdf(const GamBox& b, const Geo<R>& g, long c, int f, int x) {
     const long fs = b.fs;
@@ -477,7 +490,7 @@ __device__ __forceinline__ double dbdf(const GamBox& b, const Geo<R>& g, long c,
         const long cf = c + (up ? dstride(b, d) : 0L);
         off = (double)g.xfc[(x + 3 * d) * fs + cf] - (double)g.xyzcc[x * fs + c];
     }
-    return (up ? off : -off) / (double)g.vol[c];
+    return up ? off : -off;
 }
 
 // predictor adjoint, cells: dQW, dWn, dDh, dVdV, dQB -> dGas, doGas; writes
@@ -494,8 +507,8 @@ __global__ void __launch_bounds__(128) k_predict_adj_cells(GamBox b, DevParams<R
     double Q[5], oQ[5], W[5], oW[5], pW[5], pWf[5], pQ[5];
     for (int v = 0; v < 5; v++) { Q[v] = cur.Gas[v * fs + c]; oQ[v] = old.Gas[v * fs + c]; }
     auto c2p = [&](const double* U, double* Wo) {
-        const double rho = U[0];
-        const double Vx = U[1] / rho, Vy = U[2] / rho, Vz = U[3] / rho;
+        const double rho = U[0], rr = 1.0 / rho;
+        const double Vx = U[1] * rr, Vy = U[2] * rr, Vz = U[3] * rr;
         const double KinE = 0.5 * rho * (Vx * Vx + Vy * Vy + Vz * Vz);
         Wo[0] = rho < dF ? dF : rho; Wo[1] = Vx; Wo[2] = Vy; Wo[3] = Vz;
         const double pp = gm1 * (U[4] - KinE);
@@ -503,13 +516,14 @@ __global__ void __launch_bounds__(128) k_predict_adj_cells(GamBox b, DevParams<R
     };
     c2p(Q, W);
     c2p(oQ, oW);
-    for (int v = 0; v < 5; v++) pW[v] = W[v] + pdt * ((W[v] - oW[v]) / odt);
+    const double rodt = 1.0 / odt, pr = pdt * rodt;
+    for (int v = 0; v < 5; v++) pW[v] = W[v] + pdt * ((W[v] - oW[v]) * rodt);
     for (int v = 0; v < 5; v++) pWf[v] = pW[v];
     pWf[0] = pW[0] < dF ? dF : pW[0];
     pWf[4] = pW[4] < pF ? pF : pW[4];
     {
         const double rho = pWf[0] < dF ? dF : pWf[0];
-        const double IntE = (pWf[4] < pF ? pF : pWf[4]) / gm1;
+        const double IntE = (pWf[4] < pF ? pF : pWf[4]) * (1.0 / gm1);
         const double KinE = 0.5 * rho * (pWf[1] * pWf[1] + pWf[2] * pWf[2] + pWf[3] * pWf[3]);
         pQ[0] = rho; pQ[1] = rho * pWf[1]; pQ[2] = rho * pWf[2]; pQ[3] = rho * pWf[3]; pQ[4] = IntE + KinE;
     }
@@ -517,12 +531,12 @@ __global__ void __launch_bounds__(128) k_predict_adj_cells(GamBox b, DevParams<R
     double aWh[5], apQ[5] = {0, 0, 0, 0, 0};
     for (int v = 0; v < 5; v++) aWh[v] = vol * (double)dw.QW[v * fs + c];
     aWh[0] += dw.Dh[c];
-    const double Dm = pQ[0] < dF ? dF : pQ[0];
+    const double Dm = pQ[0] < dF ? dF : pQ[0], rDm = 1.0 / Dm;
     double aDm = 0.0;
     for (int x = 0; x < 3; x++) {
         const double a = dw.VdV[x * fs + c];
-        apQ[1 + x] += vol * a / Dm;
-        aDm += -vol * pQ[1 + x] * a / (Dm * Dm);
+        apQ[1 + x] += vol * a * rDm;
+        aDm += -vol * pQ[1 + x] * a * rDm * rDm;
     }
     if (!(pQ[0] < dF)) apQ[0] += aDm;
     bc2p_adj(dF, pF, gm1, pQ, aWh, apQ);
@@ -534,8 +548,8 @@ __global__ void __launch_bounds__(128) k_predict_adj_cells(GamBox b, DevParams<R
     apW[4] = (pW[4] < pF) ? 0.0 : apWf[4];
     double aW[5], aoW[5];
     for (int v = 0; v < 5; v++) {
-        aW[v] = apW[v] + apW[v] * pdt / odt;
-        aoW[v] = -apW[v] * pdt / odt;
+        aW[v] = apW[v] + apW[v] * pr;
+        aoW[v] = -apW[v] * pr;
     }
     double aQ[5] = {0, 0, 0, 0, 0}, aoQ[5] = {0, 0, 0, 0, 0};
     c2p_adj(dF, pF, gm1, Q, aW, aQ);
@@ -562,10 +576,13 @@ __global__ void __launch_bounds__(256) k_predict_adj_faces(GamBox b, DevParams<R
     const long fs = b.fs, c = lidx(b, ii, jj, kk);
     if (!P.doMHD) return;
     const int ijk[3] = {ii, jj, kk}, n[3] = {b.Ni, b.Nj, b.Nk};
+    const double pr = pdt / odt;
+    double rv = 0.0;
+    if (ii < b.Ni && jj < b.Nj && kk < b.Nk) rv = 1.0 / (double)g.vol[c];
     for (int d = 0; d < 3; d++) {
         const double A = g.face[d * fs + c];
-        const double Am = A < TINY ? TINY : A;
-        double ahm = (double)dw.abh[d * fs + c] * A / Am + (double)dw.Bnf[d * fs + c] / A;
+        const double Am = A < TINY ? TINY : A, rAm = 1.0 / Am;
+        double ahm = (double)dw.abh[d * fs + c] * A * rAm + (double)dw.Bnf[d * fs + c] / A;
         // cells c (this is its lower face d) and c - s_d (its upper face)
         bool inLo = true, inUp = true;
         for (int e = 0; e < 3; e++) {
@@ -574,13 +591,14 @@ __global__ void __launch_bounds__(256) k_predict_adj_faces(GamBox b, DevParams<R
             if (lo < 0 || lo >= n[e]) inUp = false;
         }
         if (inLo)
-            for (int x = 0; x < 3; x++) ahm += (double)aB[x * fs + c] * dbdf(b, g, c, 2 * d, x);
+            for (int x = 0; x < 3; x++) ahm += (double)aB[x * fs + c] * rv * dbdf(b, g, c, 2 * d, x);
         if (inUp) {
             const long cu = c - dstride(b, d);
-            for (int x = 0; x < 3; x++) ahm += (double)aB[x * fs + cu] * dbdf(b, g, cu, 2 * d + 1, x);
+            const double rvu = 1.0 / (double)g.vol[cu];
+            for (int x = 0; x < 3; x++) ahm += (double)aB[x * fs + cu] * rvu * dbdf(b, g, cu, 2 * d + 1, x);
         }
-        dmf[d * fs + c] += (R)(ahm + ahm * pdt / odt + (double)dw.bn[d * fs + c] / Am);
-        domf[d * fs + c] += (R)(-ahm * pdt / odt);
+        dmf[d * fs + c] += (R)(ahm + ahm * pr + (double)dw.bn[d * fs + c] * rAm);
+        domf[d * fs + c] += (R)(-ahm * pr);
     }
 }
 
@@ -601,14 +619,14 @@ __global__ void __launch_bounds__(128) k_update_adj_cells(GamBox b, DevParams<R>
         return;
     }
     const double dF = P.dFloor, pF = P.pFloor, gm1 = P.gm1;
-    const double dV = g.vol[c];
+    const double dV = g.vol[c], rdV = 1.0 / dV;
     const long sj = b.sx, sk = b.sk;
     double U[5], dGasM[3] = {0, 0, 0};
     for (int v = 0; v < 5; v++) {
         const R* gI = w.gF + (v + 0) * fs;
         const R* gJ = w.gF + (v + 5) * fs;
         const R* gK = w.gF + (v + 10) * fs;
-        const double dGasH = ((double)gI[c] - gI[c + 1] + gJ[c] - gJ[c + sj] + gK[c] - gK[c + sk]) / dV;
+        const double dGasH = ((double)gI[c] - gI[c + 1] + gJ[c] - gJ[c + sj] + gK[c] - gK[c + sk]) * rdV;
         U[v] = (double)cur.Gas[v * fs + c] + dt * dGasH;
     }
     double aU[5], aM3[3] = {0, 0, 0};
@@ -619,21 +637,21 @@ __global__ void __launch_bounds__(128) k_update_adj_cells(GamBox b, DevParams<R>
             const R* mI = w.mF + (x + 0) * fs;
             const R* mJ = w.mF + (x + 3) * fs;
             const R* mK = w.mF + (x + 6) * fs;
-            dGasM[x] = ((double)mI[c] - mI[c + 1] + mJ[c] - mJ[c + sj] + mK[c] - mK[c + sk]) / dV;
+            dGasM[x] = ((double)mI[c] - mI[c + 1] + mJ[c] - mJ[c + sj] + mK[c] - mK[c + sk]) * rdV;
             if (P.doBackground) dGasM[x] += g.dpB0[x * fs + c];
         }
         // CellMaxwell (mhdgroup.F90:299-329) backwards
-        const double D = U[0] < dF ? dF : U[0];
+        const double D = U[0] < dF ? dF : U[0], rD = 1.0 / D;
         const double M[3] = {U[1], U[2], U[3]};
-        const double KinE = 0.5 * (M[0] * M[0] + M[1] * M[1] + M[2] * M[2]) / D;
+        const double KinE = 0.5 * (M[0] * M[0] + M[1] * M[1] + M[2] * M[2]) * rD;
         const double p = gm1 * (U[4] - KinE);
         double Mn[3];
         for (int x = 0; x < 3; x++) Mn[x] = M[x] + dt * dGasM[x];
         const double Mn2 = Mn[0] * Mn[0] + Mn[1] * Mn[1] + Mn[2] * Mn[2];
         double a_D = ao[0], a_Mn[3];
-        const double a_KinEn = ao[4], a_Pr = ao[4] / gm1;
-        for (int x = 0; x < 3; x++) a_Mn[x] = ao[1 + x] + a_KinEn * Mn[x] / D;
-        a_D += -a_KinEn * 0.5 * Mn2 / (D * D);
+        const double a_KinEn = ao[4], a_Pr = ao[4] * (1.0 / gm1);
+        for (int x = 0; x < 3; x++) a_Mn[x] = ao[1 + x] + a_KinEn * Mn[x] * rD;
+        a_D += -a_KinEn * 0.5 * Mn2 * rD * rD;
         double a_M[3];
         for (int x = 0; x < 3; x++) {
             a_M[x] = a_Mn[x];
@@ -641,8 +659,8 @@ __global__ void __launch_bounds__(128) k_update_adj_cells(GamBox b, DevParams<R>
         }
         double a_U4 = 0.0, a_KinE = 0.0;
         if (!(p < pF)) { a_U4 = a_Pr * gm1; a_KinE = -a_Pr * gm1; }
-        for (int x = 0; x < 3; x++) a_M[x] += a_KinE * M[x] / D;
-        a_D += -a_KinE * 0.5 * (M[0] * M[0] + M[1] * M[1] + M[2] * M[2]) / (D * D);
+        for (int x = 0; x < 3; x++) a_M[x] += a_KinE * M[x] * rD;
+        a_D += -a_KinE * 0.5 * (M[0] * M[0] + M[1] * M[1] + M[2] * M[2]) * rD * rD;
         aU[0] = (U[0] < dF) ? 0.0 : a_D;
         for (int x = 0; x < 3; x++) aU[1 + x] = a_M[x];
         aU[4] = a_U4;
@@ -651,9 +669,9 @@ __global__ void __launch_bounds__(128) k_update_adj_cells(GamBox b, DevParams<R>
     }
     for (int v = 0; v < 5; v++) {
         dGas[v * fs + c] += (R)aU[v];
-        sU[v * fs + c] = (R)(dt * aU[v] / dV);
+        sU[v * fs + c] = (R)(dt * aU[v] * rdV);
     }
-    for (int x = 0; x < 3; x++) sM[x * fs + c] = (R)(aM3[x] / dV);
+    for (int x = 0; x < 3; x++) sM[x * fs + c] = (R)(aM3[x] * rdV);
 }
 
 // update adjoint, faces: face fluxes gF/mF from the two cells, E2Flux -> dE,

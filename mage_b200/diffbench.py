@@ -3,6 +3,7 @@
   python -m mage_b200.diffbench c4            # 64^3 curvilinear blast wave, 20 steps
   python -m mage_b200.diffbench c4_inflow      # the same with an x-inflow / x-outflow
   python -m mage_b200.diffbench c5 --steps 200  # 192x192x256 dipole in the wind
+  python -m mage_b200.diffbench cost            # adjoint / forward cost of one step
 
 c4: loss = sum of |B|^2 over the cells centred in [0.6, 0.8]^3 after N fixed-dt
 steps from the blast-wave start with seeded Gaussian noise (relative sigma on
@@ -19,6 +20,13 @@ gradients with checkpoints every 14 steps and one step's graph at a time.
 
 Both report the time of forward + reverse sweep, peak device memory and the
 FP32 gradient's relative L2 distance from the FP64 one.
+
+cost: device time of one step of the product forward (gam_step, the step's
+CUDA graph), of the whole-step forward that keeps its intermediates
+(gam_step_fwd_save) and of its reverse (gam_step_adj, with the kept
+intermediates and with their recomputation), on the blast-wave start at 64^3
+(the c4 grid) and 128^3, FP64 and FP32; the adjoint / forward cost is the
+reverse's time over the product forward's.
 """
 from __future__ import annotations
 
@@ -263,14 +271,71 @@ def c5(N=(192, 192, 256), nsteps=200, seg=14, precisions=("fp32", "fp64"), seed=
     return out
 
 
+def _ev_ms(fn, reps):
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    fn()
+    torch.cuda.synchronize()
+    s.record()
+    for _ in range(reps):
+        fn()
+    e.record()
+    torch.cuda.synchronize()
+    return s.elapsed_time(e) / reps
+
+
+def cost(sizes=((64, 64, 64), (128, 128, 128)), reps=20):
+    from mage_b200.diffstep import WholeStep
+    from mage_b200.gamera import FP32, FP64
+    out = {"what": "device ms per step (CUDA events, after warm-up) on the blast-wave start with a fixed dt; "
+                   "adjoint_over_forward = gam_step_adj (saved intermediates) / the product forward step",
+           "sizes": {}}
+    for N in sizes:
+        xyz = grids.warped_periodic_corners(*N)
+        g0 = GameraGPU(GamParams(*N))
+        g0.set_geometry(xyz)
+        g0.init_blast_wave()
+        st = g0.download_state(old=False)
+        dt = 0.5 * st["dt"]
+        geo = g0.get_geometry_arrays()
+        del g0
+        row = {}
+        for name, prec, dtype in (("fp64", FP64, torch.float64), ("fp32", FP32, torch.float32)):
+            gpu = GameraGPU(GamParams(*N, fixedTimestep=dt, precision=prec))
+            gpu.set_geometry(xyz)
+            gpu.init_blast_wave()
+            gpu.step_gamera(3)
+            gpu.step_gamera(reps)
+            fwd = gpu.last_step_ms() / reps
+            del gpu
+            g = Grid(DiffParams(*N), geo, dtype=dtype, device="cuda")
+            G0, F0 = g.cell_box(st["Gas"]), g.face_box(st["magFlux"])
+            cur = {"Gas": G0, "mf": F0, "B": g.bxyz(F0)}
+            ws = WholeStep(g)
+            dn = {"Gas": torch.full_like(G0, 1e-3), "mf": torch.full_like(F0, 1e-3)}
+            acc = [torch.zeros_like(G0), torch.zeros_like(F0), torch.zeros_like(G0), torch.zeros_like(F0)]
+            ws.forward(cur, cur, dt, dt)
+            fsave = _ev_ms(lambda: ws.forward(cur, cur, dt, dt), reps)
+            ws.forward(cur, cur, dt, dt)
+            adj = _ev_ms(lambda: ws.adjoint(cur, cur, dt, dt, dn, acc, saved=True), reps)
+            adj0 = _ev_ms(lambda: ws.adjoint(cur, cur, dt, dt, dn, acc, saved=False), reps)
+            row[name] = {"product_forward_ms": fwd, "fwd_save_ms": fsave, "adjoint_ms": adj,
+                         "adjoint_with_recompute_ms": adj0, "adjoint_over_forward": adj / fwd}
+            del ws, g
+            torch.cuda.empty_cache()
+        out["sizes"]["x".join(map(str, N))] = row
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("config", choices=["c4", "c4_inflow", "c5"])
+    ap.add_argument("config", choices=["c4", "c4_inflow", "c5", "cost"])
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--precisions", default="fp32,fp64")
     a = ap.parse_args()
     if a.config == "c4":
         res = c4(nsteps=a.steps or 20)
+    elif a.config == "cost":
+        res = cost()
     elif a.config == "c4_inflow":
         res = c4_inflow(nsteps=a.steps or 20)
     else:
