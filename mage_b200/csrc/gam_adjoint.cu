@@ -221,22 +221,24 @@ __global__ void __launch_bounds__(128, (sizeof(R) == 8 ? 3 : 4)) k_stress_adj(Ga
     R vol[8];
     for (int n = 0; n < 8; n++) vol[n] = g.vol[c + (n - 4) * s];
     const R Vi = central8(vol);
-    // forward states
+    // forward states; the stencils are loaded again for the reverse of the
+    // reconstruction rather than kept live (fewer registers, more warps)
     R WL[5], WR[5], MagL[3] = {(R)0, (R)0, (R)0}, MagR[3] = {(R)0, (R)0, (R)0};
-    R qW[5][8], nW[5][4], qB[3][8], nB[3][4];
     for (int v = 0; v < 5; v++) {
-        for (int n = 0; n < 8; n++) qW[v][n] = w.QW[v * fs + c + (n - 4) * s];
-        for (int m = 0; m < 4; m++) nW[v][m] = w.Wn[v * fs + c + (m - 2) * s];
-        lrs_from_qdv(P, qW[v], nW[v], Quot<R>(Vi), WL[v], WR[v]);
+        R qW[8], nW[4];
+        for (int n = 0; n < 8; n++) qW[n] = w.QW[v * fs + c + (n - 4) * s];
+        for (int m = 0; m < 4; m++) nW[m] = w.Wn[v * fs + c + (m - 2) * s];
+        lrs_from_qdv(P, qW, nW, Quot<R>(Vi), WL[v], WR[v]);
     }
     R Bn = (R)0;
     double B0[3] = {0.0, 0.0, 0.0}, B0n = 0.0;
     if (P.doMHD) {
         Bn = w.Bnf[D * fs + c];
         for (int x = 0; x < 3; x++) {
-            for (int n = 0; n < 8; n++) qB[x][n] = w.QB[x * fs + c + (n - 4) * s];
-            for (int m = 0; m < 4; m++) nB[x][m] = Blim[x * fs + c + (m - 2) * s];
-            lrs_from_qdv(P, qB[x], nB[x], Quot<R>(Vi), MagL[x], MagR[x]);
+            R qB[8], nB[4];
+            for (int n = 0; n < 8; n++) qB[n] = w.QB[x * fs + c + (n - 4) * s];
+            for (int m = 0; m < 4; m++) nB[m] = Blim[x * fs + c + (m - 2) * s];
+            lrs_from_qdv(P, qB, nB, Quot<R>(Vi), MagL[x], MagR[x]);
         }
         if (P.doBackground) {
             for (int x = 0; x < 3; x++) B0[x] = g.fcB0[(x + 3 * D) * fs + c];
@@ -273,13 +275,19 @@ __global__ void __launch_bounds__(128, (sizeof(R) == 8 ? 3 : 4)) k_stress_adj(Ga
     double aq[8], av[4];
     const double rVi = 1.0 / (double)Vi;
     for (int v = 0; v < 5; v++) {
-        lrs_adj(P.pdmb, qW[v], nW[v], Vi, rVi, aWL[v], aWR[v], aq, av);
+        R qW[8], nW[4];
+        for (int n = 0; n < 8; n++) qW[n] = w.QW[v * fs + c + (n - 4) * s];
+        for (int m = 0; m < 4; m++) nW[m] = w.Wn[v * fs + c + (m - 2) * s];
+        lrs_adj(P.pdmb, qW, nW, Vi, rVi, aWL[v], aWR[v], aq, av);
         for (int n = 0; n < 8; n++) atomicAdd(&dQW[v * fs + c + (n - 4) * s], (R)aq[n]);
         for (int m = 0; m < 4; m++) atomicAdd(&dWn[v * fs + c + (m - 2) * s], (R)av[m]);
     }
     if (P.doMHD)
         for (int x = 0; x < 3; x++) {
-            lrs_adj(P.pdmb, qB[x], nB[x], Vi, rVi, aBL[x], aBR[x], aq, av);
+            R qB[8], nB[4];
+            for (int n = 0; n < 8; n++) qB[n] = w.QB[x * fs + c + (n - 4) * s];
+            for (int m = 0; m < 4; m++) nB[m] = Blim[x * fs + c + (m - 2) * s];
+            lrs_adj(P.pdmb, qB, nB, Vi, rVi, aBL[x], aBR[x], aq, av);
             for (int n = 0; n < 8; n++) atomicAdd(&dQB[x * fs + c + (n - 4) * s], (R)aq[n]);
             for (int m = 0; m < 4; m++) atomicAdd(&dBlim[x * fs + c + (m - 2) * s], (R)av[m]);
         }

@@ -136,6 +136,18 @@ __global__ void k_bc_gather_adj(Box b, int comp, int nc, const R* __restrict__ g
     if (!pos_of(b, s, i, j, k)) return;
     const bool fixed = bc_source(b, comp, i, j, k) == s;
     const bool zg = b.bc[2] == GAM_BC_ZEROGRAD;
+    // most positions receive from no other: none of their coordinates is
+    // within Nactive of a ghost layer that copies it, nor a zero-gradient edge
+    auto may_receive = [](int x, int nn, int extent, bool periodic, bool zlo, bool zhi) {
+        if (periodic) return (x - nn >= 0 && x - nn < G) || (x >= G && x + nn < extent);
+        return (zlo && x == G) || (zhi && (x == G + nn - 1 || x == G + nn));
+    };
+    if (!may_receive(i, b.Nip, b.nx, b.bc[0] == GAM_BC_PERIODIC, false, false) &&
+        !may_receive(j, b.Njp, b.ny, !zg, zg, b.bc[3] == GAM_BC_ZEROGRAD) &&
+        !may_receive(k, b.Nkp, b.nz, b.bc[4] == GAM_BC_PERIODIC, false, false)) {
+        for (int c = 0; c < nc; c++) out[c * b.n + s] = fixed ? g[c * b.n + s] : (R)0;
+        return;
+    }
     int ci[13], cj[13], ck[13];
     const int ni = b.bc[0] == GAM_BC_PERIODIC ? axis_candidates(i, b.Nip, b.nx, false, false, ci) : (ci[0] = i, 1);
     const int nj = axis_candidates(j, b.Njp, b.ny, zg, b.bc[3] == GAM_BC_ZEROGRAD, cj);
