@@ -426,8 +426,10 @@ def main():
 
     adj = None
     if not args.no_adjoint and rank == 0:
-        from mage_b200.diffbench import c4
+        from mage_b200.diffbench import c4, cost
         adj = c4()
+        # adjoint / forward cost of one step (gam_step_adj over the product step)
+        adj["cost_per_step"] = cost()
 
     peak, peak_kind = measured_peak()
     bpc = BYTES_PER_CELL_B0 if w["problem"] == "dipole" else BYTES_PER_CELL

@@ -317,7 +317,7 @@ __device__ void edge_lrs_adj(const GamBox& b, const DevParams<R>& P, const Geo<R
 // Adjoint of the edge EMF of direction eD (k_vxb) over the range r: dE ->
 // dDh, dabh, dbn, dAVf (the AVf of this eD, 3 components, caller-zeroed)
 template <class R>
-__global__ void __launch_bounds__(128) k_vxb_adj(GamBox b, DevParams<R> P, Geo<R> g, Work<R> w, int eD, Range r,
+__global__ void __launch_bounds__(128, 6) k_vxb_adj(GamBox b, DevParams<R> P, Geo<R> g, Work<R> w, int eD, Range r,
                                                  double dt, const R* __restrict__ dE, R* dDh, R* dabh, R* dbn,
                                                  R* dAVf) {
     int ii, jj, kk;
