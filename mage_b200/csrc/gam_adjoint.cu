@@ -206,7 +206,7 @@ __device__ void gas_adj(const DevParams<R>& P, double sgn, const R* W, const R* 
 // unbounded kernel took 214-240 registers (2 blocks); bounded it spills a
 // little but runs the C5 reverse sweep 15 % faster in FP32 (measured).
 template <class R, int D>
-__global__ void __launch_bounds__(128, (sizeof(R) == 8 ? 3 : 4)) k_stress_adj(GamBox b, DevParams<R> P, Geo<R> g, const R* __restrict__ Blim,
+__global__ void __launch_bounds__(128, (sizeof(R) == 8 ? 4 : 5)) k_stress_adj(GamBox b, DevParams<R> P, Geo<R> g, const R* __restrict__ Blim,
                                                     Work<R> w, Range r, const R* __restrict__ dgF,
                                                     const R* __restrict__ dmF, R* dQW, R* dWn, R* dQB, R* dBlim,
                                                     R* dBnf) {
