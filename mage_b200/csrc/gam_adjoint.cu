@@ -202,9 +202,10 @@ __device__ void gas_adj(const DevParams<R>& P, double sgn, const R* W, const R* 
 }
 
 // Adjoint of the face fluxes of direction D over the range r (one face per
-// thread): recompute, then reverse. 3 (FP64) / 4 (FP32) blocks per SM: the
-// unbounded kernel took 214-240 registers (2 blocks); bounded it spills a
-// little but runs the C5 reverse sweep 15 % faster in FP32 (measured).
+// thread): recompute, then reverse. 4 (FP64) / 5 (FP32) blocks per SM: the
+// unbounded kernel took 214-240 registers (2 blocks); bounded it spills
+// (local memory, L1-resident) but hides more load latency (measured on
+// 128^3: 3 -> 4 FP64 blocks took the adjoint step from 5.9 to 5.7 ms).
 template <class R, int D>
 __global__ void __launch_bounds__(128, (sizeof(R) == 8 ? 4 : 5)) k_stress_adj(GamBox b, DevParams<R> P, Geo<R> g, const R* __restrict__ Blim,
                                                     Work<R> w, Range r, const R* __restrict__ dgF,
