@@ -4,6 +4,7 @@
   python -m mage_b200.diffbench c4_inflow      # the same with an x-inflow / x-outflow
   python -m mage_b200.diffbench c5 --steps 200  # 192x192x256 dipole in the wind
   python -m mage_b200.diffbench cost            # adjoint / forward cost of one step
+  python -m mage_b200.diffbench adjstep --n 128 --precisions fp64   # one step's adjoint, 5 calls (profiling)
 
 c4: loss = sum of |B|^2 over the cells centred in [0.6, 0.8]^3 after N fixed-dt
 steps from the blast-wave start with seeded Gaussian noise (relative sigma on
@@ -326,9 +327,35 @@ def cost(sizes=((64, 64, 64), (128, 128, 128)), reps=20):
     return out
 
 
+def adjstep(n=128, dtype=torch.float64):
+    """The whole-step forward and adjoint on the n^3 blast-wave start: two
+    forward + adjoint pairs, then three adjoints with the kept intermediates
+    (a short, fixed launch sequence for profilers); returns their mean time."""
+    from mage_b200.diffstep import WholeStep
+    N = (n, n, n)
+    g0 = GameraGPU(GamParams(*N))
+    g0.set_geometry(grids.warped_periodic_corners(*N))
+    g0.init_blast_wave()
+    st = g0.download_state(old=False)
+    geo = g0.get_geometry_arrays()
+    del g0
+    g = Grid(DiffParams(*N), geo, dtype=dtype, device="cuda")
+    G0, F0 = g.cell_box(st["Gas"]), g.face_box(st["magFlux"])
+    cur = {"Gas": G0, "mf": F0, "B": g.bxyz(F0)}
+    ws = WholeStep(g)
+    dt = 0.5 * st["dt"]
+    dn = {"Gas": torch.full_like(G0, 1e-3), "mf": torch.full_like(F0, 1e-3)}
+    for _ in range(2):
+        ws.forward(cur, cur, dt, dt)
+        ws.adjoint(cur, cur, dt, dt, dn, saved=True)
+    ms = _ev_ms(lambda: ws.adjoint(cur, cur, dt, dt, dn, saved=True), 2)  # 1 + 2 calls
+    return {"grid": list(N), "dtype": str(dtype), "adjoint_ms": ms, "work_gb": ws.work.numel() / 1e9}
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("config", choices=["c4", "c4_inflow", "c5", "cost"])
+    ap.add_argument("config", choices=["c4", "c4_inflow", "c5", "cost", "adjstep"])
+    ap.add_argument("--n", type=int, default=128)
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--precisions", default="fp32,fp64")
     a = ap.parse_args()
@@ -336,6 +363,8 @@ def main():
         res = c4(nsteps=a.steps or 20)
     elif a.config == "cost":
         res = cost()
+    elif a.config == "adjstep":
+        res = adjstep(a.n, torch.float32 if a.precisions == "fp32" else torch.float64)
     elif a.config == "c4_inflow":
         res = c4_inflow(nsteps=a.steps or 20)
     else:
