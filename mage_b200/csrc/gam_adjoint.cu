@@ -21,13 +21,13 @@ namespace gam_adj {
 
 __device__ GamScalars g_adj_scalars;  // zero: not halted
 
-__device__ __forceinline__ double sgnz(double x) { return x > 0.0 ? 1.0 : (x < 0.0 ? -1.0 : 0.0); }
+template <class A> __device__ __forceinline__ A sgnz(A x) { return x > (A)0 ? (A)1 : (x < (A)0 ? (A)-1 : (A)0); }
 
 // reverse of lrs_from_qdv (8CENT) for one variable: scatter the adjoints of
 // Ql, Qr to the 8-point operand stencil and the 4-point limiter stencil
-template <class R>
-__device__ void lrs_adj(R pdmb, const R* qdv, const R* v, R Vi, double rVi, double aL, double aR, double* aq,
-                        double* av) {
+template <class R, class A>
+__device__ void lrs_adj(R pdmb, const R* qdv, const R* v, R Vi, A rVi, A aL, A aR, A* aq,
+                        A* av) {
     R s = (R)0;
 #pragma unroll
     for (int n = 0; n < 8; n++) s += Rc<R>(w8(n)) * qdv[n];
@@ -41,12 +41,12 @@ __device__ void lrs_adj(R pdmb, const R* qdv, const R* v, R Vi, double rVi, doub
     const R q0 = fabs(s0 + s1), q1 = fabs(s1 + s2);
     const R dvL = vN - v1, dvR = v2 - vN;
     const R uL = fabs(dvL) - q0 * fabs(dv0), uR = fabs(dvR) - q1 * fabs(dv2);
-    double a_vN = aL + aR;
-    const double a_mL = -(double)s1 * aL, a_mR = (double)s1 * aR;
-    const double a_uL = ((R)0 < uL) ? a_mL : 0.0, a_uR = ((R)0 < uR) ? a_mR : 0.0;
-    const double a_dvL = a_uL * sgnz(dvL), a_dv0 = -a_uL * q0 * sgnz(dv0);
-    const double a_dvR = a_uR * sgnz(dvR), a_dv2 = -a_uR * q1 * sgnz(dv2);
-    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    A a_vN = aL + aR;
+    const A a_mL = -(A)s1 * aL, a_mR = (A)s1 * aR;
+    const A a_uL = ((R)0 < uL) ? a_mL : (A)0.0, a_uR = ((R)0 < uR) ? a_mR : (A)0.0;
+    const A a_dvL = a_uL * sgnz((A)dvL), a_dv0 = -a_uL * q0 * sgnz((A)dv0);
+    const A a_dvR = a_uR * sgnz((A)dvR), a_dv2 = -a_uR * q1 * sgnz((A)dv2);
+    A a0 = (A)0.0, a1 = (A)0.0, a2 = (A)0.0, a3 = (A)0.0;
     a_vN += a_dvL;
     a1 -= a_dvL;
     a2 += a_dvR;
@@ -55,56 +55,57 @@ __device__ void lrs_adj(R pdmb, const R* qdv, const R* v, R Vi, double rVi, doub
     a0 -= pdmb * a_dv0;
     a3 += pdmb * a_dv2;
     a2 -= pdmb * a_dv2;
-    double a_t = 0.0, a_minV = 0.0, a_maxV = 0.0, a_Qi = 0.0;
+    A a_t = (A)0.0, a_minV = (A)0.0, a_maxV = (A)0.0, a_Qi = (A)0.0;
     if (minV < t) a_t = a_vN; else a_minV = a_vN;
     if (maxV < Qi) a_maxV = a_t; else a_Qi = a_t;
     if (v2 < v1) a2 += a_minV; else a1 += a_minV;
     if (v1 < v2) a2 += a_maxV; else a1 += a_maxV;
-    const double a_s = a_Qi * rVi;
+    const A a_s = a_Qi * rVi;
 #pragma unroll
-    for (int n = 0; n < 8; n++) aq[n] = w8(n) * a_s;
+    for (int n = 0; n < 8; n++) aq[n] = (A)w8(n) * a_s;
     av[0] = a0; av[1] = a1; av[2] = a2; av[3] = a3;
 }
 
 // reverse of mag_kin_flux for one side: adjoints aM (of the mF sums) and aVaD
 // (of the VaD sum) -> a_W (5), a_B (3), a_Bn
-template <class R>
-__device__ void mag_adj(const DevParams<R>& P, double sgn, const R* W, const R* Bm, R Bn, const R* T, const double* B0,
-                        double B0n, const double* aM, double aVaD, double* aW, double* aB, double& aBn) {
-    const double D = W[0], Pr = W[4];
-    const double Bx = Bm[0], By = Bm[1], Bz = Bm[2];
-    const double N[3] = {T[0], T[1], T[2]};
-    const double dPb = 0.5 * (Bx * Bx + By * By + Bz * Bz);
-    const double rD = 1.0 / D;
-    double S[3] = {Bx, By, Bz};
-    double Va2;
+template <class R, class A>
+__device__ void mag_adj(const DevParams<R>& P, A sgn, const R* W, const R* Bm, R Bn, const R* T, const double* B0d,
+                        double B0nd, const A* aM, A aVaD, A* aW, A* aB, A& aBn) {
+    const A B0[3] = {(A)B0d[0], (A)B0d[1], (A)B0d[2]}, B0n = (A)B0nd;
+    const A D = W[0], Pr = W[4];
+    const A Bx = Bm[0], By = Bm[1], Bz = Bm[2];
+    const A N[3] = {T[0], T[1], T[2]};
+    const A dPb = (A)0.5 * (Bx * Bx + By * By + Bz * Bz);
+    const A rD = (A)1.0 / D;
+    A S[3] = {Bx, By, Bz};
+    A Va2;
     if (P.doBackground) {
         S[0] += B0[0]; S[1] += B0[1]; S[2] += B0[2];
         Va2 = (S[0] * S[0] + S[1] * S[1] + S[2] * S[2]) * rD;
     } else {
-        Va2 = 2.0 * dPb * rD;
+        Va2 = (A)2.0 * dPb * rD;
     }
-    const double Vn = N[0] * W[1] + N[1] * W[2] + N[2] * W[3];
-    const double den = 2.0 * Pr * rD + Va2;
-    const double lam = 1.0 / den;
-    const double s = sqrt(lam);
-    const double rs = sqrt(den);  // 1 / s
-    const double z = sgn * s * Vn;
-    const double Vn0 = 0.5 * erfc(z);
-    const double B[3] = {Bx, By, Bz};
-    double C[3];
-    for (int x = 0; x < 3; x++) C[x] = dPb * N[x] - B[x] * (double)Bn;
-    double BdB0 = 0.0;
+    const A Vn = N[0] * W[1] + N[1] * W[2] + N[2] * W[3];
+    const A den = (A)2.0 * Pr * rD + Va2;
+    const A lam = (A)1.0 / den;
+    const A s = Mth<A>::sqrt_(lam);
+    const A rs = Mth<A>::sqrt_(den);  // 1 / s
+    const A z = sgn * s * Vn;
+    const A Vn0 = (A)0.5 * Mth<A>::erfc_(z);
+    const A B[3] = {Bx, By, Bz};
+    A C[3];
+    for (int x = 0; x < 3; x++) C[x] = dPb * N[x] - B[x] * (A)Bn;
+    A BdB0 = (A)0.0;
     if (P.doBackground) {
         BdB0 = B0[0] * Bx + B0[1] * By + B0[2] * Bz;
-        for (int x = 0; x < 3; x++) C[x] += -(B0[x] * (double)Bn) - B[x] * B0n + BdB0 * N[x];
+        for (int x = 0; x < 3; x++) C[x] += -(B0[x] * (A)Bn) - B[x] * B0n + BdB0 * N[x];
     }
-    double a_Vn0 = 0.0, a_dPb = 0.0, a_Va2 = 0.0, a_Vn = 0.0, sumCN = 0.0;
+    A a_Vn0 = (A)0.0, a_dPb = (A)0.0, a_Va2 = (A)0.0, a_Vn = (A)0.0, sumCN = (A)0.0;
     for (int x = 0; x < 3; x++) {
         a_Vn0 += aM[x] * C[x];
-        const double aC = aM[x] * Vn0;
+        const A aC = aM[x] * Vn0;
         a_dPb += aC * N[x];
-        aB[x] += -aC * (double)Bn;
+        aB[x] += -aC * (A)Bn;
         aBn += -aC * B[x];
         if (P.doBackground) {
             aB[x] += -aC * B0n;
@@ -114,21 +115,21 @@ __device__ void mag_adj(const DevParams<R>& P, double sgn, const R* W, const R* 
     }
     if (P.doBackground)
         for (int x = 0; x < 3; x++) aB[x] += sumCN * B0[x];
-    if (Va2 > 0.0) a_Va2 += aVaD * 0.25 / sqrt(Va2);
-    const double a_z = a_Vn0 * (-exp(-z * z) * (1.0 / sqrt(PI_D)));
-    const double a_s = a_z * sgn * Vn;
+    if (Va2 > (A)0.0) a_Va2 += aVaD * (A)0.25 / Mth<A>::sqrt_(Va2);
+    const A a_z = a_Vn0 * (-Mth<A>::exp_(-z * z) * ((A)1.0 / Mth<A>::sqrt_((A)PI_D)));
+    const A a_s = a_z * sgn * Vn;
     a_Vn += a_z * sgn * s;
-    const double a_lam = a_s * 0.5 * rs;
-    const double a_den = -a_lam * lam * lam;
-    aW[4] += a_den * 2.0 * rD;
-    aW[0] += -a_den * 2.0 * Pr * rD * rD;
+    const A a_lam = a_s * (A)0.5 * rs;
+    const A a_den = -a_lam * lam * lam;
+    aW[4] += a_den * (A)2.0 * rD;
+    aW[0] += -a_den * (A)2.0 * Pr * rD * rD;
     a_Va2 += a_den;
     if (P.doBackground) {
-        for (int x = 0; x < 3; x++) aB[x] += a_Va2 * 2.0 * S[x] * rD;
+        for (int x = 0; x < 3; x++) aB[x] += a_Va2 * (A)2.0 * S[x] * rD;
         aW[0] += -a_Va2 * (S[0] * S[0] + S[1] * S[1] + S[2] * S[2]) * rD * rD;
     } else {
-        a_dPb += a_Va2 * 2.0 * rD;
-        aW[0] += -a_Va2 * 2.0 * dPb * rD * rD;
+        a_dPb += a_Va2 * (A)2.0 * rD;
+        aW[0] += -a_Va2 * (A)2.0 * dPb * rD * rD;
     }
     for (int x = 0; x < 3; x++) {
         aW[1 + x] += a_Vn * N[x];
@@ -138,59 +139,59 @@ __device__ void mag_adj(const DevParams<R>& P, double sgn, const R* W, const R* 
 
 // reverse of gas_kin_flux for one side: adjoints aG (of the gF sums) and aD
 // (of the dW sums) -> a_W (5)
-template <class R>
-__device__ void gas_adj(const DevParams<R>& P, double sgn, const R* W, const R* T, const double* aG, const double* aDW,
-                        double* aW) {
-    const double D = W[0], Pr = W[4], V[3] = {W[1], W[2], W[3]};
-    const double gm1 = P.gm1, rgm1 = 1.0 / gm1;
-    const double V2 = V[0] * V[0] + V[1] * V[1] + V[2] * V[2];
-    const double E = 0.5 * D * V2 + Pr * rgm1;
-    const double r2P = 1.0 / (2.0 * Pr);
-    const double lam = D * r2P;
-    double N[3], T1[3], T2[3];
+template <class R, class A>
+__device__ void gas_adj(const DevParams<R>& P, A sgn, const R* W, const R* T, const A* aG, const A* aDW,
+                        A* aW) {
+    const A D = W[0], Pr = W[4], V[3] = {W[1], W[2], W[3]};
+    const A gm1 = P.gm1, rgm1 = (A)1.0 / gm1;
+    const A V2 = V[0] * V[0] + V[1] * V[1] + V[2] * V[2];
+    const A E = (A)0.5 * D * V2 + Pr * rgm1;
+    const A r2P = (A)1.0 / ((A)2.0 * Pr);
+    const A lam = D * r2P;
+    A N[3], T1[3], T2[3];
     for (int x = 0; x < 3; x++) { N[x] = T[x]; T1[x] = T[3 + x]; T2[x] = T[6 + x]; }
-    const double Vn = N[0] * V[0] + N[1] * V[1] + N[2] * V[2];
-    const double Vt1 = T1[0] * V[0] + T1[1] * V[1] + T1[2] * V[2];
-    const double Vt2 = T2[0] * V[0] + T2[1] * V[1] + T2[2] * V[2];
-    const double s = sqrt(lam);
-    const double rs = 1.0 / s;
-    const double z = sgn * s * Vn;
-    const double Vn0 = 0.5 * erfc(z);
-    const double ex = exp(-(lam * Vn * Vn));
-    const double sq = sqrt(PI_D) * s;
-    const double rsq = rs * (1.0 / sqrt(PI_D));
-    const double Vn1 = Vn * Vn0 - 0.5 * sgn * ex * rsq;
-    double a_fMn = 0.0, a_fMt1 = 0.0, a_fMt2 = 0.0;
+    const A Vn = N[0] * V[0] + N[1] * V[1] + N[2] * V[2];
+    const A Vt1 = T1[0] * V[0] + T1[1] * V[1] + T1[2] * V[2];
+    const A Vt2 = T2[0] * V[0] + T2[1] * V[1] + T2[2] * V[2];
+    const A s = Mth<A>::sqrt_(lam);
+    const A rs = (A)1.0 / s;
+    const A z = sgn * s * Vn;
+    const A Vn0 = (A)0.5 * Mth<A>::erfc_(z);
+    const A ex = Mth<A>::exp_(-(lam * Vn * Vn));
+    const A sq = Mth<A>::sqrt_((A)PI_D) * s;
+    const A rsq = rs * ((A)1.0 / Mth<A>::sqrt_((A)PI_D));
+    const A Vn1 = Vn * Vn0 - (A)0.5 * sgn * ex * rsq;
+    A a_fMn = (A)0.0, a_fMt1 = (A)0.0, a_fMt2 = (A)0.0;
     for (int x = 0; x < 3; x++) {
         a_fMn += aG[1 + x] * N[x];
         a_fMt1 += aG[1 + x] * T1[x];
         a_fMt2 += aG[1 + x] * T2[x];
     }
-    double a_Vn1 = aG[0] * D + aG[4] * (E + 0.5 * Pr) + a_fMn * D * Vn + a_fMt1 * D * Vt1 + a_fMt2 * D * Vt2;
-    double a_Vn0 = aG[4] * 0.5 * Pr * Vn + a_fMn * Pr;
-    double a_D = aG[0] * Vn1 + a_fMn * Vn * Vn1 + a_fMt1 * Vt1 * Vn1 + a_fMt2 * Vt2 * Vn1 + aDW[0] * sgn;
+    A a_Vn1 = aG[0] * D + aG[4] * (E + (A)0.5 * Pr) + a_fMn * D * Vn + a_fMt1 * D * Vt1 + a_fMt2 * D * Vt2;
+    A a_Vn0 = aG[4] * (A)0.5 * Pr * Vn + a_fMn * Pr;
+    A a_D = aG[0] * Vn1 + a_fMn * Vn * Vn1 + a_fMt1 * Vt1 * Vn1 + a_fMt2 * Vt2 * Vn1 + aDW[0] * sgn;
     for (int x = 0; x < 3; x++) a_D += aDW[1 + x] * sgn * V[x];
-    const double a_E = aG[4] * Vn1 + aDW[4] * sgn;
-    double a_Pr = aG[4] * (0.5 * Vn1 + 0.5 * Vn0 * Vn) + a_fMn * Vn0;
-    double a_Vn = aG[4] * 0.5 * Pr * Vn0 + a_fMn * D * Vn1;
-    const double a_Vt1 = a_fMt1 * D * Vn1, a_Vt2 = a_fMt2 * D * Vn1;
-    double a_V[3];
+    const A a_E = aG[4] * Vn1 + aDW[4] * sgn;
+    A a_Pr = aG[4] * ((A)0.5 * Vn1 + (A)0.5 * Vn0 * Vn) + a_fMn * Vn0;
+    A a_Vn = aG[4] * (A)0.5 * Pr * Vn0 + a_fMn * D * Vn1;
+    const A a_Vt1 = a_fMt1 * D * Vn1, a_Vt2 = a_fMt2 * D * Vn1;
+    A a_V[3];
     for (int x = 0; x < 3; x++) a_V[x] = aDW[1 + x] * sgn * D;
-    // Vn1 = Vn Vn0 - 0.5 sgn ex / sq
+    // Vn1 = Vn Vn0 - (A)0.5 sgn ex / sq
     a_Vn += a_Vn1 * Vn0;
     a_Vn0 += a_Vn1 * Vn;
-    const double a_ex = -a_Vn1 * 0.5 * sgn * rsq;
-    const double a_sq = a_Vn1 * 0.5 * sgn * ex * rsq * rsq;
-    double a_lam = a_sq * PI_D * 0.5 * rsq;
+    const A a_ex = -a_Vn1 * (A)0.5 * sgn * rsq;
+    const A a_sq = a_Vn1 * (A)0.5 * sgn * ex * rsq * rsq;
+    A a_lam = a_sq * (A)PI_D * (A)0.5 * rsq;
     a_lam += -a_ex * ex * Vn * Vn;
-    a_Vn += -a_ex * ex * 2.0 * lam * Vn;
-    const double a_z = a_Vn0 * (-exp(-z * z) * (1.0 / sqrt(PI_D)));
-    const double a_s = a_z * sgn * Vn;
+    a_Vn += -a_ex * ex * (A)2.0 * lam * Vn;
+    const A a_z = a_Vn0 * (-Mth<A>::exp_(-z * z) * ((A)1.0 / Mth<A>::sqrt_((A)PI_D)));
+    const A a_s = a_z * sgn * Vn;
     a_Vn += a_z * sgn * s;
-    a_lam += a_s * 0.5 * rs;
+    a_lam += a_s * (A)0.5 * rs;
     a_D += a_lam * r2P;
-    a_Pr += -a_lam * D * 2.0 * r2P * r2P;
-    a_D += a_E * 0.5 * V2;
+    a_Pr += -a_lam * D * (A)2.0 * r2P * r2P;
+    a_D += a_E * (A)0.5 * V2;
     for (int x = 0; x < 3; x++) a_V[x] += a_E * D * V[x];
     a_Pr += a_E * rgm1;
     for (int x = 0; x < 3; x++) a_V[x] += a_Vn * N[x] + a_Vt1 * T1[x] + a_Vt2 * T2[x];
@@ -256,25 +257,27 @@ __global__ void __launch_bounds__(128, (sizeof(R) == 8 ? 4 : 5)) k_stress_adj(Ga
     gas_kin_flux(P, (R)-1, WL, T, gFs, dW);
     gas_kin_flux(P, (R)1, WR, T, gFs, dW);
     // reverse of the outputs gF = fa (gFs - cHogH VaD dW), mF = fa mFs
-    double aG[5], aDW[5], aVaD = 0.0, aM[3] = {0.0, 0.0, 0.0};
+    // in the form's precision (A = R): FP64 for the drop-in, FP32 for the FP32 form
+    using A = R;
+    A aG[5], aDW[5], aVaD = (A)0, aM[3] = {(A)0, (A)0, (A)0};
     for (int v = 0; v < 5; v++) {
-        const double Gv = dgF[(v + 5 * D) * fs + c];
-        aG[v] = (double)fa * Gv;
-        aDW[v] = -(double)fa * P.cHogH * (double)VaD * Gv;
-        aVaD += -(double)fa * P.cHogH * Gv * (double)dW[v];
+        const A Gv = dgF[(v + 5 * D) * fs + c];
+        aG[v] = (A)fa * Gv;
+        aDW[v] = -(A)fa * (A)P.cHogH * (A)VaD * Gv;
+        aVaD += -(A)fa * (A)P.cHogH * Gv * (A)dW[v];
     }
-    double aWL[5] = {0, 0, 0, 0, 0}, aWR[5] = {0, 0, 0, 0, 0}, aBL[3] = {0, 0, 0}, aBR[3] = {0, 0, 0}, aBn = 0.0;
-    gas_adj(P, -1.0, WL, T, aG, aDW, aWL);
-    gas_adj(P, 1.0, WR, T, aG, aDW, aWR);
+    A aWL[5] = {0, 0, 0, 0, 0}, aWR[5] = {0, 0, 0, 0, 0}, aBL[3] = {0, 0, 0}, aBR[3] = {0, 0, 0}, aBn = (A)0;
+    gas_adj(P, (A)-1, WL, T, aG, aDW, aWL);
+    gas_adj(P, (A)1, WR, T, aG, aDW, aWR);
     if (P.doMHD) {
-        for (int x = 0; x < 3; x++) aM[x] = (double)fa * dmF[(x + 3 * D) * fs + c];
-        mag_adj(P, -1.0, WL, MagL, Bn, T, B0, B0n, aM, aVaD, aWL, aBL, aBn);
-        mag_adj(P, 1.0, WR, MagR, Bn, T, B0, B0n, aM, aVaD, aWR, aBR, aBn);
+        for (int x = 0; x < 3; x++) aM[x] = (A)fa * dmF[(x + 3 * D) * fs + c];
+        mag_adj(P, (A)-1, WL, MagL, Bn, T, B0, B0n, aM, aVaD, aWL, aBL, aBn);
+        mag_adj(P, (A)1, WR, MagR, Bn, T, B0, B0n, aM, aVaD, aWR, aBR, aBn);
         dBnf[D * fs + c] += (R)aBn;
     }
     // reverse of the reconstruction: scatter to the stencils
-    double aq[8], av[4];
-    const double rVi = 1.0 / (double)Vi;
+    A aq[8], av[4];
+    const A rVi = (A)1 / (A)Vi;
     for (int v = 0; v < 5; v++) {
         R qW[8], nW[4];
         for (int n = 0; n < 8; n++) qW[n] = w.QW[v * fs + c + (n - 4) * s];
@@ -310,7 +313,7 @@ __device__ void edge_lrs_adj(const GamBox& b, const DevParams<R>& P, const Geo<R
     for (int m = 0; m < 4; m++) nmag[m] = w.bn[a * fs + c + (m - 2) * s];
     const R Vi = central8(area);
     double aq[8], av[4];
-    lrs_adj(P.pdmb, qdv, nmag, Vi, 1.0 / (double)Vi, aBL * (double)Vi, aBR * (double)Vi, aq, av);
+    lrs_adj<R, double>(P.pdmb, qdv, nmag, Vi, 1.0 / (double)Vi, aBL * (double)Vi, aBR * (double)Vi, aq, av);
     for (int n = 0; n < 8; n++) atomicAdd(&dabh[a * fs + c + (n - 4) * s], (R)aq[n]);
     for (int m = 0; m < 4; m++) atomicAdd(&dbn[a * fs + c + (m - 2) * s], (R)av[m]);
 }
