@@ -300,9 +300,9 @@ __global__ void __launch_bounds__(128, (sizeof(R) == 8 ? 4 : 5)) k_stress_adj(Ga
 
 // reverse of edge_lrs (EdgeLRs for faces of direction a along bd): adjoints of
 // bL*Vi, bR*Vi -> the abh (8) and bn (4) stencils
-template <class R>
+template <class R, class A>
 __device__ void edge_lrs_adj(const GamBox& b, const DevParams<R>& P, const Geo<R>& g, const Work<R>& w, long c, int a,
-                             int bd, double aBL, double aBR, R* dabh, R* dbn) {
+                             int bd, A aBL, A aBR, R* dabh, R* dbn) {
     const long fs = b.fs;
     const long s = dstride(b, bd);
     R qdv[8], area[8], nmag[4];
@@ -312,8 +312,8 @@ __device__ void edge_lrs_adj(const GamBox& b, const DevParams<R>& P, const Geo<R
     }
     for (int m = 0; m < 4; m++) nmag[m] = w.bn[a * fs + c + (m - 2) * s];
     const R Vi = central8(area);
-    double aq[8], av[4];
-    lrs_adj<R, double>(P.pdmb, qdv, nmag, Vi, 1.0 / (double)Vi, aBL * (double)Vi, aBR * (double)Vi, aq, av);
+    A aq[8], av[4];
+    lrs_adj<R, A>(P.pdmb, qdv, nmag, Vi, (A)1.0 / (A)Vi, aBL * (A)Vi, aBR * (A)Vi, aq, av);
     for (int n = 0; n < 8; n++) atomicAdd(&dabh[a * fs + c + (n - 4) * s], (R)aq[n]);
     for (int m = 0; m < 4; m++) atomicAdd(&dbn[a * fs + c + (m - 2) * s], (R)av[m]);
 }
@@ -375,41 +375,42 @@ __global__ void __launch_bounds__(128, 6) k_vxb_adj(GamBox b, DevParams<R> P, Ge
     const R edge = g.edge[eD * fs + c];
     const R cap = P.CFL * edge / (R)dt;
     const R vDiff = rmin(vDp, cap);
-    // reverse
-    const double a_e = (double)dE[eD * fs + c] * (double)edge;
-    const double a_v1 = -a_e * b2, a_b2e = -a_e * v1, a_v2 = a_e * b1, a_b1e = a_e * v2;
-    const double a_vDiff = a_e * P.Vd0 * Jd, a_Jd = a_e * P.Vd0 * vDiff;
-    const double a_vDp = (cap < vDp) ? 0.0 : a_vDiff;
-    double a_b1 = a_b1e, a_b2 = a_b2e, a_v1t = a_v1, a_v2t = a_v2;
-    const double rq = 1.0 / (double)q;
-    const double a_m = a_vDp * rq;
-    const double a_q = -a_vDp * (double)m * rq * rq;
-    const double a_Dc = a_q * 0.5 * rq;
+    // reverse, in the form's precision
+    using A = R;
+    const A a_e = (A)dE[eD * fs + c] * (A)edge;
+    const A a_v1 = -a_e * b2, a_b2e = -a_e * v1, a_v2 = a_e * b1, a_b1e = a_e * v2;
+    const A a_vDiff = a_e * P.Vd0 * Jd, a_Jd = a_e * P.Vd0 * vDiff;
+    const A a_vDp = (cap < vDp) ? (A)0.0 : a_vDiff;
+    A a_b1 = a_b1e, a_b2 = a_b2e, a_v1t = a_v1, a_v2t = a_v2;
+    const A rq = (A)1.0 / (A)q;
+    const A a_m = a_vDp * rq;
+    const A a_q = -a_vDp * (A)m * rq * rq;
+    const A a_Dc = a_q * (A)0.5 * rq;
     if (m > (R)0) {
-        const double rm = 1.0 / (double)m;
+        const A rm = (A)1.0 / (A)m;
         a_b1 += a_m * b1 * rm;
         a_b2 += a_m * b2 * rm;
     }
     if (vD0 > (R)0) {
-        const double rv = 1.0 / (double)vD0;
+        const A rv = (A)1.0 / (A)vD0;
         a_v1t += a_vDp * v1 * rv;
         a_v2t += a_vDp * v2 * rv;
     }
-    const double a_bT1 = a_b1 * detT * ynj - a_b2 * detT * xnj;
-    const double a_bT2 = -a_b1 * detT * yni + a_b2 * detT * xni;
-    const double a_db2 = a_Jd, a_db1 = -a_Jd;
-    const double rA1 = 1.0 / (double)fA1, rA2 = 1.0 / (double)fA2;
-    const double aT1R = (a_db1 + a_bT1 * 0.5) * rA1, aT1L = (-a_db1 + a_bT1 * 0.5) * rA1;
-    const double aT2R = (a_db2 + a_bT2 * 0.5) * rA2, aT2L = (-a_db2 + a_bT2 * 0.5) * rA2;
-    edge_lrs_adj(b, P, g, w, c, dT1, dT2, aT1L, aT1R, dabh, dbn);
-    edge_lrs_adj(b, P, g, w, c, dT2, dT1, aT2L, aT2R, dabh, dbn);
-    const double rdA = 1.0 / (double)dA;
+    const A a_bT1 = a_b1 * detT * ynj - a_b2 * detT * xnj;
+    const A a_bT2 = -a_b1 * detT * yni + a_b2 * detT * xni;
+    const A a_db2 = a_Jd, a_db1 = -a_Jd;
+    const A rA1 = (A)1.0 / (A)fA1, rA2 = (A)1.0 / (A)fA2;
+    const A aT1R = (a_db1 + a_bT1 * (A)0.5) * rA1, aT1L = (-a_db1 + a_bT1 * (A)0.5) * rA1;
+    const A aT2R = (a_db2 + a_bT2 * (A)0.5) * rA2, aT2L = (-a_db2 + a_bT2 * (A)0.5) * rA2;
+    edge_lrs_adj<R, A>(b, P, g, w, c, dT1, dT2, aT1L, aT1R, dabh, dbn);
+    edge_lrs_adj<R, A>(b, P, g, w, c, dT2, dT1, aT2L, aT2R, dabh, dbn);
+    const A rdA = (A)1.0 / (A)dA;
     for (int x = 0; x < 3; x++) {
-        const double aVC = (a_v1t * T1[x] + a_v2t * T2[x]) * rdA;
-        for (int n = 0; n < 8; n++) atomicAdd(&dAVf[x * fs + c + (n - 4) * s2v], (R)(w8(n) * aVC));
+        const A aVC = (a_v1t * T1[x] + a_v2t * T2[x]) * rdA;
+        for (int n = 0; n < 8; n++) atomicAdd(&dAVf[x * fs + c + (n - 4) * s2v], (R)((A)w8(n) * aVC));
     }
     const long cc[4] = {c, c - s1, c - s2, c - s1 - s2};
-    for (int n = 0; n < 4; n++) atomicAdd(&dDh[cc[n]], (R)(0.25 * a_Dc));
+    for (int n = 0; n < 4; n++) atomicAdd(&dDh[cc[n]], (R)((A)0.25 * a_Dc));
 }
 
 // Adjoint of Mom2Face for edge direction eD over the range r: dAVf -> dVdV
