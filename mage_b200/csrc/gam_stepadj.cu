@@ -78,11 +78,14 @@ __device__ __forceinline__ long bc_source(const Box& b, int comp, int i, int j, 
     return ((long)sk * b.ny + sj) * b.nx + si;
 }
 
+// box position of flat index t, in 32-bit arithmetic (a box holds fewer than
+// 2^31 elements; 64-bit division is a long instruction sequence)
 __device__ __forceinline__ bool pos_of(const Box& b, long t, int& i, int& j, int& k) {
     if (t >= b.n) return false;
-    i = (int)(t % b.nx);
-    j = (int)((t / b.nx) % b.ny);
-    k = (int)(t / ((long)b.nx * b.ny));
+    const unsigned u = (unsigned)t, q = u / (unsigned)b.nx;
+    i = (int)(u - q * (unsigned)b.nx);
+    k = (int)(q / (unsigned)b.ny);
+    j = (int)(q - (unsigned)k * (unsigned)b.ny);
     return true;
 }
 
@@ -270,6 +273,7 @@ int check(const gam_params* p) {
     if (!p) return GAM_EINVAL;
     if (p->rmeth != GAM_RECON_8CENT || p->doBoris || p->doAB3 || !p->doLFMLim || !p->doMHD) return GAM_EINVAL;
     if (p->nG != 4 || p->Nip < 1 || p->Njp < 4 || p->Nkp < 1 || p->do25D) return GAM_EBADDIM;
+    if ((double)(p->Nip + 9) * (p->Njp + 9) * (p->Nkp + 9) >= 2147483648.0) return GAM_EBADDIM;  // 32-bit indexing
     // boundaries: periodic I and K, periodic or zero-gradient J
     if (p->bc[0] != GAM_BC_PERIODIC || p->bc[1] != GAM_BC_PERIODIC) return GAM_EINVAL;
     if (p->bc[4] != GAM_BC_PERIODIC || p->bc[5] != GAM_BC_PERIODIC) return GAM_EINVAL;
