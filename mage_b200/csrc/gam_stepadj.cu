@@ -397,7 +397,9 @@ extern "C" int gam_step_adj(const gam_params* p, int32_t fp32, const void* const
     const Work w = layout(b, fp32, work);
     const size_t es = fp32 ? 4 : 8;
     if (!saved) TRY(forward_stages(p, fp32, b, w, geo, bg, st, dt, odt, s));
-    if (cudaMemsetAsync(w.p[dQW], 0, w.bytes - w.fwd_bytes, s) != cudaSuccess) return GAM_ECUDA;
+    // zero what the adjoint stages add into (dQW .. dBlim); sU, sM and aB are
+    // written before they are read, dnG, dnM and tM are written whole
+    if (cudaMemsetAsync(w.p[dQW], 0, (size_t)((char*)w.p[sU] - (char*)w.p[dQW]), s) != cudaSuccess) return GAM_ECUDA;
     // adjoint of the state's field: B = bFlux2Fld(magFlux)
     if (cudaMemcpyAsync(w.p[tM], dnxt[1], 3 * b.n * es, cudaMemcpyDeviceToDevice, s) != cudaSuccess) return GAM_ECUDA;
     if (dnxt[2]) TRY(fp32 ? launch_bxyz_adj<float>(b, geo, dnxt[2], w.p[tM], s)
