@@ -438,16 +438,17 @@ __global__ void __launch_bounds__(256) k_m2f_adj(GamBox b, Geo<R> g, int eD, Ran
 
 // ----------------------------------------------------------------- predictor and update
 // reverse of cell_c2p (CellC2P): aW (5) -> aU (5)
-__device__ void c2p_adj(double dF, double pF, double gm1, const double* U, const double* aW, double* aU) {
-    const double rho = U[0], rr = 1.0 / rho;
-    const double V[3] = {U[1] * rr, U[2] * rr, U[3] * rr};
-    const double KinE = 0.5 * rho * (V[0] * V[0] + V[1] * V[1] + V[2] * V[2]);
-    const double p = gm1 * (U[4] - KinE);
-    double a_rho = (rho < dF) ? 0.0 : aW[0];
-    double a_V[3] = {aW[1], aW[2], aW[3]};
-    double a_E = 0.0, a_KinE = 0.0;
+template <class A>
+__device__ void c2p_adj(A dF, A pF, A gm1, const A* U, const A* aW, A* aU) {
+    const A rho = U[0], rr = (A)1.0 / rho;
+    const A V[3] = {U[1] * rr, U[2] * rr, U[3] * rr};
+    const A KinE = (A)0.5 * rho * (V[0] * V[0] + V[1] * V[1] + V[2] * V[2]);
+    const A p = gm1 * (U[4] - KinE);
+    A a_rho = (rho < dF) ? (A)0.0 : aW[0];
+    A a_V[3] = {aW[1], aW[2], aW[3]};
+    A a_E = (A)0.0, a_KinE = (A)0.0;
     if (!(p < pF)) { a_E = aW[4] * gm1; a_KinE = -aW[4] * gm1; }
-    a_rho += a_KinE * 0.5 * (V[0] * V[0] + V[1] * V[1] + V[2] * V[2]);
+    a_rho += a_KinE * (A)0.5 * (V[0] * V[0] + V[1] * V[1] + V[2] * V[2]);
     for (int x = 0; x < 3; x++) a_V[x] += a_KinE * rho * V[x];
     for (int x = 0; x < 3; x++) {
         aU[1 + x] += a_V[x] * rr;
@@ -457,35 +458,37 @@ __device__ void c2p_adj(double dF, double pF, double gm1, const double* U, const
     aU[4] += a_E;
 }
 // reverse of cell_p2c (CellP2C): aU (5) -> aW (5)
-__device__ void p2c_adj(double dF, double pF, double gm1, const double* W, const double* aU, double* aW) {
-    const double rho = W[0] < dF ? dF : W[0];
-    const double V[3] = {W[1], W[2], W[3]};
-    const double V2 = V[0] * V[0] + V[1] * V[1] + V[2] * V[2];
-    double a_rho = aU[0] + aU[4] * 0.5 * V2;
+template <class A>
+__device__ void p2c_adj(A dF, A pF, A gm1, const A* W, const A* aU, A* aW) {
+    const A rho = W[0] < dF ? dF : W[0];
+    const A V[3] = {W[1], W[2], W[3]};
+    const A V2 = V[0] * V[0] + V[1] * V[1] + V[2] * V[2];
+    A a_rho = aU[0] + aU[4] * (A)0.5 * V2;
     for (int x = 0; x < 3; x++) {
         a_rho += aU[1 + x] * V[x];
         aW[1 + x] += aU[1 + x] * rho + aU[4] * rho * V[x];
     }
-    aW[4] += (W[4] < pF) ? 0.0 : aU[4] / gm1;
-    aW[0] += (W[0] < dF) ? 0.0 : a_rho;
+    aW[4] += (W[4] < pF) ? (A)0.0 : aU[4] / gm1;
+    aW[0] += (W[0] < dF) ? (A)0.0 : a_rho;
 }
 // reverse of block_c2p (BlockCon2Prim): aW (5) -> aU (5)
-__device__ void bc2p_adj(double dF, double pF, double gm1, const double* U, const double* aW, double* aU) {
-    const double D = U[0] < dF ? dF : U[0], rD = 1.0 / D;
-    const double M[3] = {U[1], U[2], U[3]};
-    const double M2 = M[0] * M[0] + M[1] * M[1] + M[2] * M[2];
-    const double KinE = 0.5 * M2 * rD;
-    const double p = gm1 * (U[4] - KinE);
-    double a_D = aW[0], a_M[3];
+template <class A>
+__device__ void bc2p_adj(A dF, A pF, A gm1, const A* U, const A* aW, A* aU) {
+    const A D = U[0] < dF ? dF : U[0], rD = (A)1.0 / D;
+    const A M[3] = {U[1], U[2], U[3]};
+    const A M2 = M[0] * M[0] + M[1] * M[1] + M[2] * M[2];
+    const A KinE = (A)0.5 * M2 * rD;
+    const A p = gm1 * (U[4] - KinE);
+    A a_D = aW[0], a_M[3];
     for (int x = 0; x < 3; x++) {
         a_M[x] = aW[1 + x] * rD;
         a_D += -aW[1 + x] * M[x] * rD * rD;
     }
-    double a_E = 0.0, a_KinE = 0.0;
+    A a_E = (A)0.0, a_KinE = (A)0.0;
     if (!(p < pF)) { a_E = aW[4] * gm1; a_KinE = -aW[4] * gm1; }
     for (int x = 0; x < 3; x++) a_M[x] += a_KinE * M[x] * rD;
-    a_D += -a_KinE * 0.5 * M2 * rD * rD;
-    aU[0] += (U[0] < dF) ? 0.0 : a_D;
+    a_D += -a_KinE * (A)0.5 * M2 * rD * rD;
+    aU[0] += (U[0] < dF) ? (A)0.0 : a_D;
     for (int x = 0; x < 3; x++) aU[1 + x] += a_M[x];
     aU[4] += a_E;
 }
@@ -493,7 +496,7 @@ __device__ void bc2p_adj(double dF, double pF, double gm1, const double* U, cons
 // V d B_x / d (flux of face f of cell c), f = 0..5 (I-, I+, J-, J+, K-, K+),
 // as in gamCellBxyz: xfc - xyzcc with the sign of the face
 template <class R>
-__device__ __forceinline__ double dbdf(const GamBox& b, const Geo<R>& g, long c, int f, int x) {
+__device__ __forceinline__ R dbdf(const GamBox& b, const Geo<R>& g, long c, int f, int x) {
     const long fs = b.fs;
     const int d = f >> 1, up = f & 1;
     double off;
@@ -512,62 +515,63 @@ template <class R>
 __global__ void __launch_bounds__(128) k_predict_adj_cells(GamBox b, DevParams<R> P, Geo<R> g, StateBuf<R> cur,
                                                            StateBuf<R> old, double pdt, double odt, Work<R> dw,
                                                            R* dGas, R* doGas, R* aB) {
+    using A = R;  // accumulation in the form's precision
     int ii, jj, kk;
     Range r{0, b.Ni - 1, 0, b.Nj - 1, 0, b.Nk - 1};
     if (!thread_ijk(r, ii, jj, kk)) return;
     const long fs = b.fs, c = lidx(b, ii, jj, kk);
-    const double dF = P.dFloor, pF = P.pFloor, gm1 = P.gm1;
-    double Q[5], oQ[5], W[5], oW[5], pW[5], pWf[5], pQ[5];
+    const A dF = P.dFloor, pF = P.pFloor, gm1 = P.gm1;
+    A Q[5], oQ[5], W[5], oW[5], pW[5], pWf[5], pQ[5];
     for (int v = 0; v < 5; v++) { Q[v] = cur.Gas[v * fs + c]; oQ[v] = old.Gas[v * fs + c]; }
-    auto c2p = [&](const double* U, double* Wo) {
-        const double rho = U[0], rr = 1.0 / rho;
-        const double Vx = U[1] * rr, Vy = U[2] * rr, Vz = U[3] * rr;
-        const double KinE = 0.5 * rho * (Vx * Vx + Vy * Vy + Vz * Vz);
+    auto c2p = [&](const A* U, A* Wo) {
+        const A rho = U[0], rr = (A)1.0 / rho;
+        const A Vx = U[1] * rr, Vy = U[2] * rr, Vz = U[3] * rr;
+        const A KinE = (A)0.5 * rho * (Vx * Vx + Vy * Vy + Vz * Vz);
         Wo[0] = rho < dF ? dF : rho; Wo[1] = Vx; Wo[2] = Vy; Wo[3] = Vz;
-        const double pp = gm1 * (U[4] - KinE);
+        const A pp = gm1 * (U[4] - KinE);
         Wo[4] = pp < pF ? pF : pp;
     };
     c2p(Q, W);
     c2p(oQ, oW);
-    const double rodt = 1.0 / odt, pr = pdt * rodt;
+    const A rodt = (A)1.0 / odt, pr = pdt * rodt;
     for (int v = 0; v < 5; v++) pW[v] = W[v] + pdt * ((W[v] - oW[v]) * rodt);
     for (int v = 0; v < 5; v++) pWf[v] = pW[v];
     pWf[0] = pW[0] < dF ? dF : pW[0];
     pWf[4] = pW[4] < pF ? pF : pW[4];
     {
-        const double rho = pWf[0] < dF ? dF : pWf[0];
-        const double IntE = (pWf[4] < pF ? pF : pWf[4]) * (1.0 / gm1);
-        const double KinE = 0.5 * rho * (pWf[1] * pWf[1] + pWf[2] * pWf[2] + pWf[3] * pWf[3]);
+        const A rho = pWf[0] < dF ? dF : pWf[0];
+        const A IntE = (pWf[4] < pF ? pF : pWf[4]) * ((A)1.0 / gm1);
+        const A KinE = (A)0.5 * rho * (pWf[1] * pWf[1] + pWf[2] * pWf[2] + pWf[3] * pWf[3]);
         pQ[0] = rho; pQ[1] = rho * pWf[1]; pQ[2] = rho * pWf[2]; pQ[3] = rho * pWf[3]; pQ[4] = IntE + KinE;
     }
-    const double vol = g.vol[c];
-    double aWh[5], apQ[5] = {0, 0, 0, 0, 0};
-    for (int v = 0; v < 5; v++) aWh[v] = vol * (double)dw.QW[v * fs + c];
+    const A vol = g.vol[c];
+    A aWh[5], apQ[5] = {0, 0, 0, 0, 0};
+    for (int v = 0; v < 5; v++) aWh[v] = vol * (A)dw.QW[v * fs + c];
     aWh[0] += dw.Dh[c];
-    const double Dm = pQ[0] < dF ? dF : pQ[0], rDm = 1.0 / Dm;
-    double aDm = 0.0;
+    const A Dm = pQ[0] < dF ? dF : pQ[0], rDm = (A)1.0 / Dm;
+    A aDm = (A)0.0;
     for (int x = 0; x < 3; x++) {
-        const double a = dw.VdV[x * fs + c];
+        const A a = dw.VdV[x * fs + c];
         apQ[1 + x] += vol * a * rDm;
         aDm += -vol * pQ[1 + x] * a * rDm * rDm;
     }
     if (!(pQ[0] < dF)) apQ[0] += aDm;
     bc2p_adj(dF, pF, gm1, pQ, aWh, apQ);
-    double apWf[5] = {0, 0, 0, 0, 0};
+    A apWf[5] = {0, 0, 0, 0, 0};
     p2c_adj(dF, pF, gm1, pWf, apQ, apWf);
-    double apW[5];
+    A apW[5];
     for (int v = 0; v < 5; v++) apW[v] = apWf[v];
-    apW[0] = (pW[0] < dF) ? 0.0 : apWf[0];
-    apW[4] = (pW[4] < pF) ? 0.0 : apWf[4];
-    double aW[5], aoW[5];
+    apW[0] = (pW[0] < dF) ? (A)0.0 : apWf[0];
+    apW[4] = (pW[4] < pF) ? (A)0.0 : apWf[4];
+    A aW[5], aoW[5];
     for (int v = 0; v < 5; v++) {
         aW[v] = apW[v] + apW[v] * pr;
         aoW[v] = -apW[v] * pr;
     }
-    double aQ[5] = {0, 0, 0, 0, 0}, aoQ[5] = {0, 0, 0, 0, 0};
+    A aQ[5] = {0, 0, 0, 0, 0}, aoQ[5] = {0, 0, 0, 0, 0};
     c2p_adj(dF, pF, gm1, Q, aW, aQ);
     c2p_adj(dF, pF, gm1, oQ, aoW, aoQ);
-    double aWn[5];
+    A aWn[5];
     for (int v = 0; v < 5; v++) aWn[v] = dw.Wn[v * fs + c];
     bc2p_adj(dF, pF, gm1, Q, aWn, aQ);
     for (int v = 0; v < 5; v++) {
@@ -575,7 +579,7 @@ __global__ void __launch_bounds__(128) k_predict_adj_cells(GamBox b, DevParams<R
         doGas[v * fs + c] += (R)aoQ[v];
     }
     if (P.doMHD)
-        for (int x = 0; x < 3; x++) aB[x * fs + c] = (R)(vol * (double)dw.QB[x * fs + c]);
+        for (int x = 0; x < 3; x++) aB[x * fs + c] = (R)(vol * (A)dw.QB[x * fs + c]);
 }
 
 // predictor adjoint, faces: dabh, dBnf, dbn and the Bxyz adjoints of the two
@@ -583,19 +587,20 @@ __global__ void __launch_bounds__(128) k_predict_adj_cells(GamBox b, DevParams<R
 template <class R>
 __global__ void __launch_bounds__(256) k_predict_adj_faces(GamBox b, DevParams<R> P, Geo<R> g, double pdt, double odt,
                                                            Work<R> dw, const R* __restrict__ aB, R* dmf, R* domf) {
+    using A = R;
     int ii, jj, kk;
     Range r{0, b.Ni, 0, b.Nj, 0, b.Nk};
     if (!thread_ijk(r, ii, jj, kk)) return;
     const long fs = b.fs, c = lidx(b, ii, jj, kk);
     if (!P.doMHD) return;
     const int ijk[3] = {ii, jj, kk}, n[3] = {b.Ni, b.Nj, b.Nk};
-    const double pr = pdt / odt;
-    double rv = 0.0;
-    if (ii < b.Ni && jj < b.Nj && kk < b.Nk) rv = 1.0 / (double)g.vol[c];
+    const A pr = pdt / odt;
+    A rv = (A)0.0;
+    if (ii < b.Ni && jj < b.Nj && kk < b.Nk) rv = (A)1.0 / (A)g.vol[c];
     for (int d = 0; d < 3; d++) {
-        const double A = g.face[d * fs + c];
-        const double Am = A < TINY ? TINY : A, rAm = 1.0 / Am;
-        double ahm = (double)dw.abh[d * fs + c] * A * rAm + (double)dw.Bnf[d * fs + c] / A;
+        const A Af = g.face[d * fs + c];
+        const A Am = Af < (A)TINY ? (A)TINY : Af, rAm = (A)1.0 / Am;
+        A ahm = (A)dw.abh[d * fs + c] * Af * rAm + (A)dw.Bnf[d * fs + c] / Af;
         // cells c (this is its lower face d) and c - s_d (its upper face)
         bool inLo = true, inUp = true;
         for (int e = 0; e < 3; e++) {
@@ -604,13 +609,13 @@ __global__ void __launch_bounds__(256) k_predict_adj_faces(GamBox b, DevParams<R
             if (lo < 0 || lo >= n[e]) inUp = false;
         }
         if (inLo)
-            for (int x = 0; x < 3; x++) ahm += (double)aB[x * fs + c] * rv * dbdf(b, g, c, 2 * d, x);
+            for (int x = 0; x < 3; x++) ahm += (A)aB[x * fs + c] * rv * dbdf(b, g, c, 2 * d, x);
         if (inUp) {
             const long cu = c - dstride(b, d);
-            const double rvu = 1.0 / (double)g.vol[cu];
-            for (int x = 0; x < 3; x++) ahm += (double)aB[x * fs + cu] * rvu * dbdf(b, g, cu, 2 * d + 1, x);
+            const A rvu = (A)1.0 / (A)g.vol[cu];
+            for (int x = 0; x < 3; x++) ahm += (A)aB[x * fs + cu] * rvu * dbdf(b, g, cu, 2 * d + 1, x);
         }
-        dmf[d * fs + c] += (R)(ahm + ahm * pr + (double)dw.bn[d * fs + c] * rAm);
+        dmf[d * fs + c] += (R)(ahm + ahm * pr + (A)dw.bn[d * fs + c] * rAm);
         domf[d * fs + c] += (R)(-ahm * pr);
     }
 }
@@ -621,6 +626,7 @@ template <class R>
 __global__ void __launch_bounds__(128) k_update_adj_cells(GamBox b, DevParams<R> P, Geo<R> g, StateBuf<R> cur,
                                                           Work<R> w, double dt, const R* __restrict__ dnGas, R* dGas,
                                                           R* sU, R* sM) {
+    using A = R;
     int ii, jj, kk;
     Range r{0, b.Ni - 1, 0, b.Nj - 1, 0, b.Nk - 1};
     if (!thread_ijk(r, ii, jj, kk)) return;
@@ -631,50 +637,50 @@ __global__ void __launch_bounds__(128) k_update_adj_cells(GamBox b, DevParams<R>
         for (int v = 0; v < 5; v++) dGas[v * fs + c] += dnGas[v * fs + c];
         return;
     }
-    const double dF = P.dFloor, pF = P.pFloor, gm1 = P.gm1;
-    const double dV = g.vol[c], rdV = 1.0 / dV;
+    const A dF = P.dFloor, pF = P.pFloor, gm1 = P.gm1;
+    const A dV = g.vol[c], rdV = (A)1.0 / dV;
     const long sj = b.sx, sk = b.sk;
-    double U[5], dGasM[3] = {0, 0, 0};
+    A U[5], dGasM[3] = {0, 0, 0};
     for (int v = 0; v < 5; v++) {
         const R* gI = w.gF + (v + 0) * fs;
         const R* gJ = w.gF + (v + 5) * fs;
         const R* gK = w.gF + (v + 10) * fs;
-        const double dGasH = ((double)gI[c] - gI[c + 1] + gJ[c] - gJ[c + sj] + gK[c] - gK[c + sk]) * rdV;
-        U[v] = (double)cur.Gas[v * fs + c] + dt * dGasH;
+        const A dGasH = ((A)gI[c] - gI[c + 1] + gJ[c] - gJ[c + sj] + gK[c] - gK[c + sk]) * rdV;
+        U[v] = (A)cur.Gas[v * fs + c] + dt * dGasH;
     }
-    double aU[5], aM3[3] = {0, 0, 0};
-    double ao[5];
+    A aU[5], aM3[3] = {0, 0, 0};
+    A ao[5];
     for (int v = 0; v < 5; v++) ao[v] = dnGas[v * fs + c];
     if (P.doMHD) {
         for (int x = 0; x < 3; x++) {
             const R* mI = w.mF + (x + 0) * fs;
             const R* mJ = w.mF + (x + 3) * fs;
             const R* mK = w.mF + (x + 6) * fs;
-            dGasM[x] = ((double)mI[c] - mI[c + 1] + mJ[c] - mJ[c + sj] + mK[c] - mK[c + sk]) * rdV;
+            dGasM[x] = ((A)mI[c] - mI[c + 1] + mJ[c] - mJ[c + sj] + mK[c] - mK[c + sk]) * rdV;
             if (P.doBackground) dGasM[x] += g.dpB0[x * fs + c];
         }
         // CellMaxwell (mhdgroup.F90:299-329) backwards
-        const double D = U[0] < dF ? dF : U[0], rD = 1.0 / D;
-        const double M[3] = {U[1], U[2], U[3]};
-        const double KinE = 0.5 * (M[0] * M[0] + M[1] * M[1] + M[2] * M[2]) * rD;
-        const double p = gm1 * (U[4] - KinE);
-        double Mn[3];
+        const A D = U[0] < dF ? dF : U[0], rD = (A)1.0 / D;
+        const A M[3] = {U[1], U[2], U[3]};
+        const A KinE = (A)0.5 * (M[0] * M[0] + M[1] * M[1] + M[2] * M[2]) * rD;
+        const A p = gm1 * (U[4] - KinE);
+        A Mn[3];
         for (int x = 0; x < 3; x++) Mn[x] = M[x] + dt * dGasM[x];
-        const double Mn2 = Mn[0] * Mn[0] + Mn[1] * Mn[1] + Mn[2] * Mn[2];
-        double a_D = ao[0], a_Mn[3];
-        const double a_KinEn = ao[4], a_Pr = ao[4] * (1.0 / gm1);
+        const A Mn2 = Mn[0] * Mn[0] + Mn[1] * Mn[1] + Mn[2] * Mn[2];
+        A a_D = ao[0], a_Mn[3];
+        const A a_KinEn = ao[4], a_Pr = ao[4] * ((A)1.0 / gm1);
         for (int x = 0; x < 3; x++) a_Mn[x] = ao[1 + x] + a_KinEn * Mn[x] * rD;
-        a_D += -a_KinEn * 0.5 * Mn2 * rD * rD;
-        double a_M[3];
+        a_D += -a_KinEn * (A)0.5 * Mn2 * rD * rD;
+        A a_M[3];
         for (int x = 0; x < 3; x++) {
             a_M[x] = a_Mn[x];
             aM3[x] = a_Mn[x] * dt;
         }
-        double a_U4 = 0.0, a_KinE = 0.0;
+        A a_U4 = (A)0.0, a_KinE = (A)0.0;
         if (!(p < pF)) { a_U4 = a_Pr * gm1; a_KinE = -a_Pr * gm1; }
         for (int x = 0; x < 3; x++) a_M[x] += a_KinE * M[x] * rD;
-        a_D += -a_KinE * 0.5 * (M[0] * M[0] + M[1] * M[1] + M[2] * M[2]) * rD * rD;
-        aU[0] = (U[0] < dF) ? 0.0 : a_D;
+        a_D += -a_KinE * (A)0.5 * (M[0] * M[0] + M[1] * M[1] + M[2] * M[2]) * rD * rD;
+        aU[0] = (U[0] < dF) ? (A)0.0 : a_D;
         for (int x = 0; x < 3; x++) aU[1 + x] = a_M[x];
         aU[4] = a_U4;
     } else {
@@ -693,6 +699,7 @@ template <class R>
 __global__ void __launch_bounds__(256) k_update_adj_faces(GamBox b, DevParams<R> P, double dt,
                                                           const R* __restrict__ sU, const R* __restrict__ sM,
                                                           const R* __restrict__ dnmf, R* dmf, R* dgF, R* dmF, R* dE) {
+    using A = R;
     int ii, jj, kk;
     Range r{0, b.Ni, 0, b.Nj, 0, b.Nk};
     if (!thread_ijk(r, ii, jj, kk)) return;
@@ -707,14 +714,14 @@ __global__ void __launch_bounds__(256) k_update_adj_faces(GamBox b, DevParams<R>
         const bool inUp = act(ii - (d == 0), jj - (d == 1), kk - (d == 2));
         const long cu = c - dstride(b, d);
         for (int v = 0; v < 5; v++) {
-            double a = 0.0;
+            A a = (A)0.0;
             if (inLo) a += sU[v * fs + c];
             if (inUp) a -= sU[v * fs + cu];
             dgF[(v + 5 * d) * fs + c] += (R)a;
         }
         if (P.doMHD)
             for (int x = 0; x < 3; x++) {
-                double a = 0.0;
+                A a = (A)0.0;
                 if (inLo) a += sM[x * fs + c];
                 if (inUp) a -= sM[x * fs + cu];
                 dmF[(x + 3 * d) * fs + c] += (R)a;
@@ -727,14 +734,14 @@ __global__ void __launch_bounds__(256) k_update_adj_faces(GamBox b, DevParams<R>
         return a0 >= G && a0 <= G + b.Nip && a1 >= G && a1 <= G + b.Njp && a2 >= G && a2 <= G + b.Nkp;
     };
     const long sj = b.sx, sk = b.sk;
-    auto A = [&](int q, int a0, int a1, int a2) -> double {
-        return inr(a0, a1, a2) ? (double)dnmf[q * fs + c + (a0 - ii) + (long)(a1 - jj) * sj + (long)(a2 - kk) * sk] : 0.0;
+    auto An = [&](int q, int a0, int a1, int a2) -> A {
+        return inr(a0, a1, a2) ? (A)dnmf[q * fs + c + (a0 - ii) + (long)(a1 - jj) * sj + (long)(a2 - kk) * sk] : (A)0.0;
     };
-    const double a0c = A(0, ii, jj, kk), a1c = A(1, ii, jj, kk), a2c = A(2, ii, jj, kk);
+    const A a0c = An(0, ii, jj, kk), a1c = An(1, ii, jj, kk), a2c = An(2, ii, jj, kk);
     // mf0 -= dt (E2[+j] - E2 - E1[+k] + E1); mf1 -= dt (E0[+k] - E0 - E2[+i] + E2); mf2 -= dt (E1[+i] - E1 - E0[+j] + E0)
-    const double aE2 = -dt * (A(0, ii, jj - 1, kk) - a0c - A(1, ii - 1, jj, kk) + a1c);
-    const double aE1 = -dt * (-A(0, ii, jj, kk - 1) + a0c + A(2, ii - 1, jj, kk) - a2c);
-    const double aE0 = -dt * (A(1, ii, jj, kk - 1) - a1c - A(2, ii, jj - 1, kk) + a2c);
+    const A aE2 = -dt * (An(0, ii, jj - 1, kk) - a0c - An(1, ii - 1, jj, kk) + a1c);
+    const A aE1 = -dt * (-An(0, ii, jj, kk - 1) + a0c + An(2, ii - 1, jj, kk) - a2c);
+    const A aE0 = -dt * (An(1, ii, jj, kk - 1) - a1c - An(2, ii, jj - 1, kk) + a2c);
     dE[c] += (R)aE0;
     dE[fs + c] += (R)aE1;
     dE[2 * fs + c] += (R)aE2;
