@@ -24,70 +24,9 @@
 #include <string.h>
 
 #include "../../include/gamgpu.h"
+#include "gam_bcmap.cuh"
 
 namespace gam_stepadj {
-
-constexpr int G = 4;  // ghost layers (nG, init.F90:327)
-
-struct Box {
-    int Nip, Njp, Nkp, Ni, Nj, Nk;  // active cells; cells with ghosts
-    int nx, ny, nz;                 // box extents Ni+1, Nj+1, Nk+1
-    long n;                         // elements of one component
-    int bc[6];
-};
-
-Box make_box(const gam_params* p) {
-    Box b;
-    b.Nip = p->Nip; b.Njp = p->Njp; b.Nkp = p->Nkp;
-    b.Ni = b.Nip + 2 * G; b.Nj = b.Njp + 2 * G; b.Nk = b.Nkp + 2 * G;
-    b.nx = b.Ni + 1; b.ny = b.Nj + 1; b.nz = b.Nk + 1;
-    b.n = (long)b.nx * b.ny * b.nz;
-    for (int s = 0; s < 6; s++) b.bc[s] = p->bc[s];
-    return b;
-}
-
-// lower / upper ghost rule of one axis with nn active cells; `normal`: the
-// face flux of this axis' direction, whose upper face G+nn is active
-__device__ __forceinline__ int lo_rule(int kind, int x, int nn) {
-    if (x < G) {
-        if (kind == GAM_BC_PERIODIC) return x + nn;
-        if (kind == GAM_BC_ZEROGRAD) return G;
-    }
-    return x;
-}
-__device__ __forceinline__ int hi_rule(int kind, int x, int nn, bool normal) {
-    const bool m = normal ? (x >= G + nn + 1 && x <= G + nn + 4) : (x >= G + nn && x <= G + nn + 3);
-    if (m) {
-        if (kind == GAM_BC_PERIODIC) return x - nn;
-        if (kind == GAM_BC_ZEROGRAD) return normal ? G + nn : G + nn - 1;
-    }
-    return x;
-}
-// flat source index of box position (i, j, k); comp -1: cell values, 0/1/2:
-// face fluxes of direction comp. K rule, then J (over the cell ranges of i and
-// k only when J is not periodic), then I.
-__device__ __forceinline__ long bc_source(const Box& b, int comp, int i, int j, int k) {
-    if (comp < 0 && (i >= b.Ni || j >= b.Nj || k >= b.Nk)) return ((long)k * b.ny + j) * b.nx + i;
-    int sk = k;
-    if (b.bc[4] == GAM_BC_PERIODIC) sk = hi_rule(GAM_BC_PERIODIC, lo_rule(GAM_BC_PERIODIC, k, b.Nkp), b.Nkp, comp == 2);
-    const int sjm = hi_rule(b.bc[3], lo_rule(b.bc[2], j, b.Njp), b.Njp, comp == 1);
-    const bool cond = b.bc[2] == GAM_BC_PERIODIC || (i < b.Ni && sk < b.Nk);
-    const int sj = cond ? sjm : j;
-    int si = i;
-    if (b.bc[0] == GAM_BC_PERIODIC) si = hi_rule(GAM_BC_PERIODIC, lo_rule(GAM_BC_PERIODIC, i, b.Nip), b.Nip, comp == 0);
-    return ((long)sk * b.ny + sj) * b.nx + si;
-}
-
-// box position of flat index t, in 32-bit arithmetic (a box holds fewer than
-// 2^31 elements; 64-bit division is a long instruction sequence)
-__device__ __forceinline__ bool pos_of(const Box& b, long t, int& i, int& j, int& k) {
-    if (t >= b.n) return false;
-    const unsigned u = (unsigned)t, q = u / (unsigned)b.nx;
-    i = (int)(u - q * (unsigned)b.nx);
-    k = (int)(q / (unsigned)b.ny);
-    j = (int)(q - (unsigned)k * (unsigned)b.ny);
-    return true;
-}
 
 // out[c][t] = in[c][src(t)] for the nc components of a field
 template <class R>
@@ -97,34 +36,6 @@ __global__ void k_bc_gather(Box b, int comp, int nc, const R* __restrict__ in, R
     if (!pos_of(b, t, i, j, k)) return;
     const long s = bc_source(b, comp, i, j, k);
     for (int c = 0; c < nc; c++) out[c * b.n + t] = in[c * b.n + s];
-}
-
-// candidate positions of one axis that the ghost rules can send to x, in
-// ascending order: x - nn, x, x + nn and, for zero-gradient sides, the ghost
-// layer of the side x is the edge of
-__device__ __forceinline__ int axis_candidates(int x, int nn, int extent, bool zg_lo, bool zg_hi, int* out) {
-    int c[13], m = 0;
-    if (zg_lo && x == G)
-        for (int q = 0; q < G; q++) c[m++] = q;
-    c[m++] = x - nn;
-    c[m++] = x;
-    c[m++] = x + nn;
-    if (zg_hi && (x == G + nn - 1 || x == G + nn))
-        for (int q = 0; q <= G; q++) c[m++] = G + nn + q;
-    // insertion sort, keep the distinct in-range values
-    for (int a = 1; a < m; a++) {
-        const int v = c[a];
-        int q = a - 1;
-        while (q >= 0 && c[q] > v) {
-            c[q + 1] = c[q];
-            q--;
-        }
-        c[q + 1] = v;
-    }
-    int r = 0;
-    for (int a = 0; a < m; a++)
-        if (c[a] >= 0 && c[a] < extent && (r == 0 || out[r - 1] != c[a])) out[r++] = c[a];
-    return r;
 }
 
 // adjoint of the gather: out[c][s] = (g[c][s] if src(s) = s, else 0) +
@@ -139,12 +50,7 @@ __global__ void k_bc_gather_adj(Box b, int comp, int nc, const R* __restrict__ g
     if (!pos_of(b, s, i, j, k)) return;
     const bool fixed = bc_source(b, comp, i, j, k) == s;
     const bool zg = b.bc[2] == GAM_BC_ZEROGRAD;
-    // most positions receive from no other: none of their coordinates is
-    // within Nactive of a ghost layer that copies it, nor a zero-gradient edge
-    auto may_receive = [](int x, int nn, int extent, bool periodic, bool zlo, bool zhi) {
-        if (periodic) return (x - nn >= 0 && x - nn < G) || (x >= G && x + nn < extent);
-        return (zlo && x == G) || (zhi && (x == G + nn - 1 || x == G + nn));
-    };
+    // most positions receive from no other
     if (!may_receive(i, b.Nip, b.nx, b.bc[0] == GAM_BC_PERIODIC, false, false) &&
         !may_receive(j, b.Njp, b.ny, !zg, zg, b.bc[3] == GAM_BC_ZEROGRAD) &&
         !may_receive(k, b.Nkp, b.nz, b.bc[4] == GAM_BC_PERIODIC, false, false)) {
