@@ -5,17 +5,21 @@ Workload (default): the 3-D MHD blast wave on the non-orthogonal curvilinear
 192^3 grid x = xi + 0.05 sin(2 pi xi) sin(2 pi eta) sin(2 pi zeta) (y, z
 likewise) on the unit cube, triply periodic; rho = 1, p = 0.1 outside and
 p = 10 inside r < 0.1, B = (1,1,0)/sqrt(2), gamma = 5/3, CFL 0.3, FP64 drop-in
-form. A step is one stepGamera over the whole grid; the metric is cell-updates/s
-(= 1000 x the reference's kZCs, src/gamera/output.F90:64-85).
+form (the strict build: IEEE operations in the reference's order, no FMA
+contraction). A step is one stepGamera over the whole grid; the metric is
+cell-updates/s (= 1000 x the reference's kZCs, src/gamera/output.F90:64-85).
 
   value : device time of K steps (CUDA events on the library's stream, inputs
           resident in HBM; the step's arrays, ~13 GB, are far larger than L2)
   e2e   : the same metric through the C ABI with host buffers: every step
-          uploads State and oState from pinned host memory, runs one step and
-          reads the new State back
+          uploads State from pinned host memory, runs one step and reads the
+          new State back
+  fp64_other_form : the FP64 FMA form (FMA contraction, CUDA's erfc/exp;
+          not the drop-in) on the same workload
   fp32  : the precision form on the same workload, with its error vs FP64
   cpu_baseline : the CPU restatement (-O3 -ffast-math, all host threads) on a
-          bounded number of steps of the same workload
+          bounded number of steps of the same workload, with the IEEE-strict
+          build of the restatement timed beside it
 
 --impl reference times that CPU restatement alone (the reference is Fortran and
 no Fortran compiler exists on these machines), on rank 0.
@@ -50,54 +54,75 @@ def env_rank():
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    """SM clock and clock-event reasons sampled through NVML every 5 ms in a
+    thread while the timed region runs (nvidia-smi's -lms floor of 100 ms
+    gives one or two samples in a sub-second timed region)."""
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"))
 
     def __init__(self, index):
         self.index = index
-        self.proc = None
-        self.lines = []
+        self.samples = []
+        self.reasons = set()
+        self.smax = None
+        self._stop = threading.Event()
+        self.t = None
+        self.nv = None
+
+    def _handle(self):
+        import pynvml as nv
+        nv.nvmlInit()
+        try:
+            import torch
+            p = torch.cuda.get_device_properties(self.index)
+            bus = "%08X:%02X:%02X.0" % (p.pci_domain_id, p.pci_bus_id, p.pci_device_id)
+            return nv, nv.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return nv, nv.nvmlDeviceGetHandleByIndex(self.index)
 
     def start(self):
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
-        except OSError:
-            self.proc = None
+            self.nv, self.h = self._handle()
+            self.smax = float(self.nv.nvmlDeviceGetMaxClockInfo(self.h, self.nv.NVML_CLOCK_SM))
+        except Exception:
+            self.nv = None
+            return
+        self.t = threading.Thread(target=self._run, daemon=True)
+        self.t.start()
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+    def _run(self):
+        nv = self.nv
+        while not self._stop.is_set():
+            try:
+                self.samples.append(float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)))
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                for name, const in self.REASONS:
+                    if r & getattr(nv, const):
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            time.sleep(0.005)
 
     def stop(self):
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        sm, smax, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            f = [x.strip() for x in ln.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                smax.append(float(f[2]))
-            except ValueError:
-                continue
-            for nm, v in zip(names, f[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(nm)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        if self.nv is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["NVML unavailable"], "samples": 0}
+        self._stop.set()
+        self.t.join(timeout=5)
+        sm = self.samples
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.smax,
+                "reasons": sorted(self.reasons), "samples": len(sm), "sampler": "NVML, 5 ms"}
+
+
+def cpu_model():
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.startswith("model name"):
+                return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
 
 
 def measured_peak():
@@ -124,15 +149,18 @@ def committed_traffic(workload, dtype):
     return d.get(workload, {}).get(dtype)
 
 
-def cpu_sample(g, w, params, budget_s=12.0, max_steps=6):
-    """Bounded CPU baseline: the oracle (fast build, all host threads) on the
-    same workload; metric and state are taken from the GPU set-up."""
+def cpu_sample(g, w, params, budget_s=12.0, max_steps=6, variant="fast"):
+    """Bounded CPU baseline: the oracle (all host threads) on the same
+    workload; metric and state are taken from the GPU set-up. variant "fast"
+    is built with the reference's Release flags (-O3 -march=native
+    -ffast-math), "strict" is the IEEE-strict parity build (-O2
+    -ffp-contract=off)."""
     from oracle.oracle import Oracle, OracleParams
     from tests.helpers import GEO_FROM_ORACLE
     N = w["N"]
     op = OracleParams(*N, do25D=(N[2] == 1), CFL=params.CFL, noMetric=True)
     xyz = np.zeros((3, N[2] + 9, N[1] + 9, N[0] + 9))
-    o = Oracle(op, xyz, "fast")
+    o = Oracle(op, xyz, variant)
     geo = g.get_geometry_arrays()
     for name, v in geo.items():
         o.array(GEO_FROM_ORACLE[name])[...] = v
@@ -151,9 +179,11 @@ def cpu_sample(g, w, params, budget_s=12.0, max_steps=6):
             break
     el = time.perf_counter() - t0
     cells = N[0] * N[1] * N[2]
+    flags = {"fast": "-O3 -march=native -ffast-math", "strict": "-O2 -fno-fast-math -ffp-contract=off"}[variant]
     return {"value": cells * n / el, "unit": "cell-updates/s", "cores": int(o.L.orc_num_threads()),
-            "kind": "port", "sample": f"{n} timed steps (after 1 warm-up) of the full {N[0]}x{N[1]}x{N[2]} grid, "
-                                      f"oracle -O3 -march=native -ffast-math, OpenMP"}
+            "cpu_model": cpu_model(), "kind": "port",
+            "sample": f"{n} timed steps (after 1 warm-up) of the full {N[0]}x{N[1]}x{N[2]} grid, "
+                      f"oracle {variant} build ({flags}), OpenMP"}
 
 
 def slab_main(args, w, rank, local, world, dist, barrier, max_over_ranks):
@@ -173,9 +203,9 @@ def slab_main(args, w, rank, local, world, dist, barrier, max_over_ranks):
     clk = ClockSampler(local)
     clk.start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
+    e0.record(sl.stream)  # the slabs' kernels, reductions and exchange all run on sl.stream
     sl.step(args.steps)
-    e1.record()
+    e1.record(sl.stream)
     torch.cuda.synchronize()
     clocks = clk.stop()
     ms = max_over_ranks(e0.elapsed_time(e1))
@@ -280,11 +310,15 @@ def main():
     ap.add_argument("--no-fp32", action="store_true")
     ap.add_argument("--no-dipole", action="store_true", help="skip the dipole-in-wind FP64/FP32 section")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the differentiation-form section")
+    ap.add_argument("--no-other-fp64", dest="other_fp64", action="store_false",
+                    help="skip timing the other FP64 build (the FMA form beside the drop-in)")
     ap.add_argument("--replicas", action="store_true", help="N>1: independent replicas instead of k-slabs")
     ap.add_argument("--slabs", action="store_true", help="k-slab path also on one GPU (its halo sent to itself)")
-    ap.add_argument("--strict", action="store_true", help="time the FP64 kernels built without FMA contraction")
+    ap.add_argument("--fma", action="store_true",
+                    help="headline FP64 number from the FMA form instead of the drop-in (strict) kernels")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    args.strict = not args.fma
     if args.impl == "reference":
         return run_reference(args)
 
@@ -369,6 +403,22 @@ def main():
         e2e_value = world * cells * args.e2e_steps / e2e_s
         del cur, old, spare
 
+    # ---- the FP64 FMA form (not the drop-in): the same workload on the
+    # kernels built with FMA contraction, CUDA's erfc/exp and shared reciprocals
+    other = None
+    if args.other_fp64:
+        gf = make(0, not args.strict)
+        gf.step_gamera(args.warmup)
+        barrier()
+        gf.step_gamera(args.steps)
+        msf = max_over_ranks(gf.last_step_ms())
+        vf = world * cells * args.steps / (msf / 1e3)
+        other = {"form": "FP64 FMA form (not the drop-in)" if args.strict else "FP64 drop-in (strict)",
+                 "value": vf, "unit": "cell-updates/s", "ms_per_step": msf / args.steps,
+                 "ratio_vs_headline": vf / value,
+                 "roofline_frac": (vf / world) * BYTES_PER_CELL["f64"] / 1e9 / measured_peak()[0]}
+        del gf
+
     # ---- FP32 precision form
     fp32 = None
     if not args.no_fp32:
@@ -379,7 +429,7 @@ def main():
         ms32 = max_over_ranks(g32.last_step_ms())
         v32 = world * cells * args.steps / (ms32 / 1e3)
         # error vs FP64 after the same number of steps from the same start
-        a = make(0)
+        a = make(0, True)
         b = make(FP32)
         nerr = 20
         a.step_gamera(nerr)
@@ -406,7 +456,7 @@ def main():
         dip = {"workload": wd["desc"], "grid": list(Nd), "steps": DIPOLE_STEPS, "unit": "cell-updates/s"}
         final = {}
         for prec, name in ((0, "fp64"), (FP32, "fp32")):
-            gd = make_app(DIPOLE_WORKLOAD, prec, xyz=xyzd)
+            gd = make_app(DIPOLE_WORKLOAD, prec, strict=(prec == 0 and args.strict), xyz=xyzd)
             gd.step_gamera(args.warmup)
             barrier()
             gd.step_gamera(DIPOLE_STEPS - args.warmup)
@@ -443,13 +493,17 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_sample(g, w, g.params)
+        # the IEEE-strict parity build of the restatement, timed beside it
+        cpu["oracle_strict"] = cpu_sample(g, w, g.params, budget_s=10.0, max_steps=3, variant="strict")
     if rank == 0:
         line = {
             "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": w["desc"], "grid": list(N),
-                       "precision": "FP64 drop-in" + (" (strict: no FMA contraction)" if args.strict else ""),
+                       "precision": ("FP64 drop-in (strict build: IEEE operations in the reference's order, no FMA "
+                                     "contraction; equals the IEEE-strict restatement bit for bit)") if args.strict
+                       else "FP64 FMA form (not the drop-in)",
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                        "l2": "inputs larger than L2 (~13 GB of state, metric and work arrays per step)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
@@ -472,6 +526,7 @@ def main():
                             "(Bxyz computed from the fluxes on the device; oState stays on the device: the State "
                             "before the last step), gam_step(1), gam_download_state (new Gas, magFlux, Bxyz to "
                             "pinned host memory)"},
+            "fp64_other_form": other,
             "fp32": fp32,
             "dipole": dip,
             "adjoint": adj,

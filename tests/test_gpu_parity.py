@@ -1,9 +1,10 @@
 """GPU parity tests: the CUDA step (through the C ABI) against the oracle.
 
-* strict build (no FMA contraction) vs the oracle built with the same
-  self-written erfc/exp: identical bits after N steps;
-* product build (FMA contraction) vs the IEEE-strict oracle with libm
-  erfc/exp: <= 1e-12 relative (max-norm per variable) after N steps;
+* strict build (no FMA contraction; the FP64 drop-in) vs the oracle built with
+  the same self-written erfc/exp: identical bits after N steps;
+* the drop-in vs the IEEE-strict oracle with libm erfc/exp: <= 1e-12 relative
+  per conserved variable on C1 (100 steps) and C2 (192^3, 200 steps);
+* the FMA form vs the libm oracle, to its stated bounds;
 * GPU metric from corners and GPU initial conditions vs the oracle's;
 * FP32 form: relative L2 error per conserved variable vs FP64, stated.
 """
@@ -50,37 +51,101 @@ def _errs(a, b, comps):
     return out
 
 
-@pytest.mark.parametrize("prob,N", [("ot", (128, 128, 4)), ("bw", (32, 32, 32))])
-def test_product_step_matches_reference(oracle_built, prob, N):
-    """Configuration C1 (OT 128x128x4) and a 32^3 curvilinear blast wave:
-    product kernels (FMA contraction) vs the IEEE-strict restatement with libm
-    erfc/exp. After 10 steps: <= 1e-12 relative (max norm) per conserved
-    variable and face flux. After 100 steps the flow has amplified last-bit
-    differences: two IEEE-strict CPU builds that differ only in whose erfc/exp
-    they call (libm vs self-written, both within a few ulp) already differ by
-    ~1e-11; the GPU must stay within 10x of that intrinsic spread."""
-    ref, _ = make_oracle(prob, N, variant="strict")
-    alt, _ = make_oracle(prob, N, variant="gm")
-    g = gpu_from_oracle(ref, strict=False)
+def test_dropin_matches_reference_c1(oracle_built):
+    """Configuration C1 (Orszag-Tang 128x128x4, 100 steps): the FP64 drop-in
+    (the strict build: IEEE operations in the reference's order, no FMA
+    contraction) against the IEEE-strict restatement that calls libm's
+    erfc/exp, as gfortran's reference does. Relative L2 error per conserved
+    variable and per face-flux component <= 1e-12 after 100 steps; max norm
+    <= 1e-12 after 10 steps. The two differ only where the self-written
+    erfc/exp and libm's round differently; the vortex amplifies those last
+    bits by ~1e3 over 100 steps."""
+    ref, _ = make_oracle("ot", (128, 128, 4), variant="strict")
+    g = gpu_from_oracle(ref, strict=True)
     done = 0
     for nst in (10, 100):
-        assert ref.step(nst - done) == 0 and alt.step(nst - done) == 0
+        assert ref.step(nst - done) == 0
         g.step_gamera(nst - done)
         done = nst
         s = g.download_state(old=False)
         for k, nc in (("Gas", 5), ("magFlux", 3)):
-            e_gpu = _errs(s[k], ref.array(k), range(nc))
-            e_cpu = _errs(alt.array(k), ref.array(k), range(nc))
-            worst = max(e[0] for e in e_gpu)
-            spread = max(max(e[0] for e in e_cpu), 1e-14)
-            print(f"{prob} {N} {nst} steps {k}: GPU vs strict Linf {worst:.2e} L2 {max(e[1] for e in e_gpu):.2e};"
-                  f" libm-vs-own-erfc CPU spread Linf {spread:.2e}")
+            e = _errs(s[k], ref.array(k), range(nc))
+            print(f"C1 drop-in {nst} steps {k}: Linf {max(x[0] for x in e):.2e} L2 {max(x[1] for x in e):.2e}")
             if nst == 10:
-                assert worst <= 1e-12, (k, worst)
+                assert max(x[0] for x in e) <= 1e-12, (k, e)
+            assert max(x[1] for x in e) <= 1e-12, (k, nst, e)
+    assert abs(g.download_state(old=False)["dt"] - ref.scalars()["dt"]) <= 1e-12 * ref.scalars()["dt"]
+
+
+@pytest.mark.parametrize("prob,N", [("ot", (128, 128, 4)), ("bw", (32, 32, 32))])
+def test_fma_form_vs_reference(oracle_built, prob, N):
+    """The FP64 FMA form (FMA contraction, CUDA's erfc/exp, shared reciprocals;
+    not the drop-in) against the IEEE-strict libm restatement: max norm
+    <= 1e-12 after 10 steps. After 100 Orszag-Tang steps its last-bit
+    differences have grown like any second implementation's (the restatement
+    built with the reference's Release flags, -O3 -ffast-math, reaches 2e-12
+    relative L2 there): bounded by 5e-12 relative L2 and 1e-10 max norm."""
+    ref, _ = make_oracle(prob, N, variant="strict")
+    g = gpu_from_oracle(ref, strict=False)
+    done = 0
+    for nst in (10, 100):
+        assert ref.step(nst - done) == 0
+        g.step_gamera(nst - done)
+        done = nst
+        s = g.download_state(old=False)
+        for k, nc in (("Gas", 5), ("magFlux", 3)):
+            e = _errs(s[k], ref.array(k), range(nc))
+            linf, l2 = max(x[0] for x in e), max(x[1] for x in e)
+            print(f"FMA form {prob} {N} {nst} steps {k}: Linf {linf:.2e} L2 {l2:.2e}")
+            if nst == 10:
+                assert linf <= 1e-12, (k, linf)
             else:
-                assert worst <= 10 * spread, (k, worst, spread)
-    # Model%dt after the last step (CalcDT before the boundary fill)
-    assert abs(g.download_state(old=False)["dt"] - ref.scalars()["dt"]) <= 1e-10 * ref.scalars()["dt"]
+                assert l2 <= 5e-12 and linf <= 1e-10, (k, linf, l2)
+
+
+def test_dropin_matches_reference_c2_full_size(oracle_built):
+    """Configuration C2 at its stated size: the curvilinear 192^3 blast wave,
+    200 steps of the FP64 drop-in (strict build) against the IEEE-strict libm
+    restatement started from the same metric and state (the device's metric
+    and initial state equal the restatement's bit for bit,
+    test_metric_from_corners_is_bit_exact and test_blast_wave_init_is_bit_exact;
+    here they are computed once on the device and copied, because the
+    restatement's 12^3-point quadrature of the start takes too long on the
+    host at this size). Relative L2 and max-norm error per conserved variable
+    and face-flux component <= 1e-12 after 200 steps; div B (DivB,
+    gridutils.F90:717-770) after every step at round-off: <= 1e-13 of the
+    summed absolute face flux."""
+    from oracle.oracle import Oracle, OracleParams
+    N = (192, 192, 192)
+    g = GameraGPU(GamParams(*N, strict=True))
+    g.set_geometry(grids.warped_periodic_corners(*N))
+    g.init_blast_wave()
+    o = Oracle(OracleParams(*N, noMetric=True), np.zeros((3, N[2] + 9, N[1] + 9, N[0] + 9)), "strict")
+    geo = g.get_geometry_arrays()
+    for name, v in geo.items():
+        o.array(GEO_FROM_ORACLE[name])[...] = v
+    del geo
+    s = g.download_state()
+    for k in STATE:
+        o.array(k)[...] = s[k]
+    o.set_scalars(t=s["time"], dt=s["dt"], time=s["time"], otime=s["otime"], ts=s["ts"])
+    phi = float(np.abs(s["magFlux"][:, 4:-4, 4:-4, 4:-4]).sum())
+    del s
+    divb = []
+    for n in range(200):
+        g.step_gamera(1)
+        divb.append(g.divb())
+    assert o.step(200) == 0
+    worst = max(divb) / phi
+    print(f"C2 192^3 200 steps: max div B / sum|flux| over the steps {worst:.2e}")
+    assert worst <= 1e-13, worst
+    s = g.download_state(old=False)
+    for k, nc in (("Gas", 5), ("magFlux", 3)):
+        e = _errs(s[k], o.array(k), range(nc))
+        linf, l2 = max(x[0] for x in e), max(x[1] for x in e)
+        print(f"C2 192^3 drop-in 200 steps {k}: Linf {linf:.2e} L2 {l2:.2e}")
+        assert l2 <= 1e-12 and linf <= 1e-12, (k, e)
+    assert abs(o.divb() - g.divb()) <= 1e-13 * phi
 
 
 def test_metric_from_corners_is_bit_exact(oracle_built):
