@@ -223,6 +223,7 @@ __global__ void __launch_bounds__(128, (sizeof(R) == 8 ? 4 : 5)) k_stress_adj(Ga
     R vol[8];
     for (int n = 0; n < 8; n++) vol[n] = g.vol[c + (n - 4) * s];
     const R Vi = central8(vol);
+    const Quot<R> qVi(Vi);  // the 8 reconstructions share the divisor
     // forward states; the stencils are loaded again for the reverse of the
     // reconstruction rather than kept live (fewer registers, more warps)
     R WL[5], WR[5], MagL[3] = {(R)0, (R)0, (R)0}, MagR[3] = {(R)0, (R)0, (R)0};
@@ -230,7 +231,7 @@ __global__ void __launch_bounds__(128, (sizeof(R) == 8 ? 4 : 5)) k_stress_adj(Ga
         R qW[8], nW[4];
         for (int n = 0; n < 8; n++) qW[n] = w.QW[v * fs + c + (n - 4) * s];
         for (int m = 0; m < 4; m++) nW[m] = w.Wn[v * fs + c + (m - 2) * s];
-        lrs_from_qdv(P, qW, nW, Quot<R>(Vi), WL[v], WR[v]);
+        lrs_from_qdv(P, qW, nW, qVi, WL[v], WR[v]);
     }
     R Bn = (R)0;
     double B0[3] = {0.0, 0.0, 0.0}, B0n = 0.0;
@@ -240,7 +241,7 @@ __global__ void __launch_bounds__(128, (sizeof(R) == 8 ? 4 : 5)) k_stress_adj(Ga
             R qB[8], nB[4];
             for (int n = 0; n < 8; n++) qB[n] = w.QB[x * fs + c + (n - 4) * s];
             for (int m = 0; m < 4; m++) nB[m] = Blim[x * fs + c + (m - 2) * s];
-            lrs_from_qdv(P, qB, nB, Quot<R>(Vi), MagL[x], MagR[x]);
+            lrs_from_qdv(P, qB, nB, qVi, MagL[x], MagR[x]);
         }
         if (P.doBackground) {
             for (int x = 0; x < 3; x++) B0[x] = g.fcB0[(x + 3 * D) * fs + c];

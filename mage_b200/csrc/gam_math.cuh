@@ -4,20 +4,28 @@
 // (stress.F90:432-599, GasKinFlux / MagKinFlux). Library implementations of
 // these functions differ by an ulp or two between the host libm and the GPU,
 // which is enough to stop a bit-for-bit comparison of a GPU step against a CPU
-// step. These two functions use only +, -, *, / and comparisons (all IEEE
-// correctly rounded on both sides), so a GPU kernel built without FMA
-// contraction and a CPU build with -ffp-contract=off produce identical bits.
+// step. These two functions use only IEEE operations that both sides round
+// the same way: +, -, *, /, fma (called explicitly: one rounding), comparisons
+// and exact scalings, so a GPU kernel and a CPU build produce identical bits
+// (the kernels of the strict step are built without implicit FMA contraction,
+// the CPU restatement with -ffp-contract=off; the explicit fma calls below are
+// fused on both).
 //
 // Construction (see gen_gam_math.py, which generates the coefficients):
-//   gam_exp(a, b) = e^(a+b): x = k*ln2 + r with ln2 split in a 32-bit head and
-//     a tail (k*ln2_hi exact), e^r from its Taylor series to degree 13 (Estrin
-//     evaluation, short dependency chains for the GPU), exact scaling by 2^k.
-//     The split argument lets erfc pass -x^2 as an exact head plus a small tail.
+//   gam_exp(a, b) = e^(a+b): table-driven (Tang, ACM TOMS 15(2), 1989):
+//     a+b = (128 m + j) ln2/128 + r, |r| <= ln2/256 (ln2/128 split in a
+//     32-bit head and a tail, k*head exact), e^(a+b) = 2^m (T_hi + T_lo) e^r
+//     with 2^(j/128) = T_hi + T_lo from a 128-entry table and e^r - 1 by its
+//     degree-5 Taylor polynomial; the result is T_hi + (T_hi p + T_lo), one
+//     rounding of a sum whose small part carries ~2^-60 relative error
+//     (about 0.51 ulp in total). The split argument lets erfc pass -x^2 as an
+//     exact head plus a small tail.
 //   gam_erfc(x) = exp(-x^2) * g(s) / (x + 4), s = (A x - B)/(x + 4) for x >= 0,
 //     g a degree-22 Chebyshev fit of erfcx(x)*(x+4) on [0, 27.5], evaluated by
-//     Estrin's scheme;
-//     erfc(x) = 2 - erfc(-x) for x < 0.
-// Accuracy against mpmath: a few ulp over the whole range (tests/test_gam_math.py).
+//     Estrin's scheme with fmas; erfc(x) = 2 - erfc(-x) for x < 0.
+// Accuracy against mpmath: exp within 0.51 ulp, erfc within a few ulp (the
+// golden values in tests/golden/erfc_exp.json, checked by
+// test_erfc_exp_golden in tests/test_oracle.py).
 #pragma once
 
 #include <stdint.h>
@@ -52,6 +60,20 @@ GAM_HD double round_even(double x) {
 #endif
 }
 
+// 2^(j/128) = T_hi + T_lo, j = 0..127 (pairs), for host and device code
+#if defined(__CUDACC__)
+static __device__ const double gam_exp_tab_d[2 * GAM_EXP_N] = GAM_EXP_TAB_INIT;
+#endif
+static const double gam_exp_tab_h[2 * GAM_EXP_N] = GAM_EXP_TAB_INIT;
+
+GAM_HD double exp_tab(int i) {
+#if defined(__CUDA_ARCH__)
+    return __ldg(&gam_exp_tab_d[i]);
+#else
+    return gam_exp_tab_h[i];
+#endif
+}
+
 // e^(a+b); b may carry a small tail of the exponent that a could not hold.
 GAM_HD double exp_ab(double a, double b) {
     const double x = a + b;
@@ -60,22 +82,22 @@ GAM_HD double exp_ab(double a, double b) {
         if (x > 709.782712893384) return INFINITY;
     }
     if (x < -745.2) return 0.0;
-    const double kd = round_even(x * GAM_INV_LN2);
+    const double kd = round_even(x * GAM_INV_LN2N);
     const int k = (int)kd;
-    double r = (a - kd * GAM_LN2_HI) + b;  // a - k*ln2_hi is exact
-    r = r - kd * GAM_LN2_LO;
-    // Taylor polynomial by Estrin's scheme (dependency depth 5 instead of 13)
-    const double r2 = r * r, r4 = r2 * r2, r8 = r4 * r4;
-    const double p01 = GAM_EXP_C0 + GAM_EXP_C1 * r, p23 = GAM_EXP_C2 + GAM_EXP_C3 * r;
-    const double p45 = GAM_EXP_C4 + GAM_EXP_C5 * r, p67 = GAM_EXP_C6 + GAM_EXP_C7 * r;
-    const double p89 = GAM_EXP_C8 + GAM_EXP_C9 * r, pab = GAM_EXP_C10 + GAM_EXP_C11 * r;
-    const double pcd = GAM_EXP_C12 + GAM_EXP_C13 * r;
-    const double q0 = p01 + p23 * r2, q1 = p45 + p67 * r2, q2 = p89 + pab * r2;
-    const double o0 = q0 + q1 * r4, o1 = q2 + pcd * r4;
-    const double p = o0 + o1 * r8;
-    if (k > 1023) return (p * 2.0) * pow2i(k - 1);
-    if (k < -1021) return (p * pow2i(k + 600)) * pow2i(-600);
-    return p * pow2i(k);
+    double r = fma(-kd, GAM_LN2N_HI, a) + b;  // a - k*head is exact
+    r = fma(-kd, GAM_LN2N_LO, r);
+    // e^r - 1 = r + r^2 (C2 + r (C3 + r (C4 + r C5)))
+    double c = fma(r, GAM_EXP_C5, GAM_EXP_C4);
+    c = fma(r, c, GAM_EXP_C3);
+    c = fma(r, c, GAM_EXP_C2);
+    const double p = fma(r * r, c, r);
+    const int j = k & (GAM_EXP_N - 1);
+    const int m = (k - j) / GAM_EXP_N;  // exact: k - j is a multiple of 128
+    const double th = exp_tab(2 * j), tl = exp_tab(2 * j + 1);
+    const double y = th + fma(th, p, tl);
+    if (m > 1023) return (y * 2.0) * pow2i(m - 1);
+    if (m < -1021) return (y * pow2i(m + 600)) * pow2i(-600);
+    return y * pow2i(m);
 }
 
 GAM_HD double gam_exp(double x) { return exp_ab(x, 0.0); }
@@ -87,20 +109,20 @@ GAM_HD double gam_erfc(double x) {
         res = 0.0;
     } else {
         const double q = 1.0 / (ax + GAM_ERFC_L);
-        const double s = (GAM_ERFC_A * ax - GAM_ERFC_B) * q;
-        // g(s) by Estrin's scheme (dependency depth 6 instead of 22)
+        const double s = fma(GAM_ERFC_A, ax, -GAM_ERFC_B) * q;
+        // g(s) by Estrin's scheme with fmas (dependency depth 6 instead of 22)
         const double s2 = s * s, s4 = s2 * s2, s8 = s4 * s4, s16 = s8 * s8;
-        const double a0 = GAM_ERFC_G0 + GAM_ERFC_G1 * s, a1 = GAM_ERFC_G2 + GAM_ERFC_G3 * s;
-        const double a2 = GAM_ERFC_G4 + GAM_ERFC_G5 * s, a3 = GAM_ERFC_G6 + GAM_ERFC_G7 * s;
-        const double a4 = GAM_ERFC_G8 + GAM_ERFC_G9 * s, a5 = GAM_ERFC_G10 + GAM_ERFC_G11 * s;
-        const double a6 = GAM_ERFC_G12 + GAM_ERFC_G13 * s, a7 = GAM_ERFC_G14 + GAM_ERFC_G15 * s;
-        const double a8 = GAM_ERFC_G16 + GAM_ERFC_G17 * s, a9 = GAM_ERFC_G18 + GAM_ERFC_G19 * s;
-        const double a10 = GAM_ERFC_G20 + GAM_ERFC_G21 * s;
-        const double b0 = a0 + a1 * s2, b1 = a2 + a3 * s2, b2 = a4 + a5 * s2, b3 = a6 + a7 * s2;
-        const double b4 = a8 + a9 * s2, b5 = a10 + GAM_ERFC_G22 * s2;
-        const double c0 = b0 + b1 * s4, c1 = b2 + b3 * s4, c2 = b4 + b5 * s4;
-        const double d0 = c0 + c1 * s8;
-        const double g = d0 + c2 * s16;
+        const double a0 = fma(GAM_ERFC_G1, s, GAM_ERFC_G0), a1 = fma(GAM_ERFC_G3, s, GAM_ERFC_G2);
+        const double a2 = fma(GAM_ERFC_G5, s, GAM_ERFC_G4), a3 = fma(GAM_ERFC_G7, s, GAM_ERFC_G6);
+        const double a4 = fma(GAM_ERFC_G9, s, GAM_ERFC_G8), a5 = fma(GAM_ERFC_G11, s, GAM_ERFC_G10);
+        const double a6 = fma(GAM_ERFC_G13, s, GAM_ERFC_G12), a7 = fma(GAM_ERFC_G15, s, GAM_ERFC_G14);
+        const double a8 = fma(GAM_ERFC_G17, s, GAM_ERFC_G16), a9 = fma(GAM_ERFC_G19, s, GAM_ERFC_G18);
+        const double a10 = fma(GAM_ERFC_G21, s, GAM_ERFC_G20);
+        const double b0 = fma(a1, s2, a0), b1 = fma(a3, s2, a2), b2 = fma(a5, s2, a4), b3 = fma(a7, s2, a6);
+        const double b4 = fma(a9, s2, a8), b5 = fma(GAM_ERFC_G22, s2, a10);
+        const double c0 = fma(b1, s4, b0), c1 = fma(b3, s4, b2), c2 = fma(b5, s4, b4);
+        const double d0 = fma(c1, s8, c0);
+        const double g = fma(c2, s16, d0);
         // -x^2 = -xh^2 (exact, xh = x truncated to 1/16) - (x-xh)(x+xh)
         const double xh = trunc(ax * 16.0) * 0.0625;
         const double e = exp_ab(-(xh * xh), -((ax - xh) * (ax + xh)));

@@ -35,6 +35,7 @@
 #include <type_traits>
 #include "gam_layout.cuh"
 #include "gam_math.cuh"
+#include "gam_quot.cuh"
 #include "gam_types.cuh"
 
 #ifndef GAM_NS
@@ -96,10 +97,13 @@ template <> struct Mth<float> {
     static __device__ __forceinline__ float rsqrt_(float x) { return rsqrtf(x); }
 };
 
-// Quotients a/d that share the divisor d. The product build (GAM_FAST_RECIP)
+// Quotients a/d that share the divisor d. The FMA form (GAM_FAST_RECIP)
 // takes one reciprocal and multiplies (at most one ulp more than the division,
-// and a fraction of its instructions); every other build divides, so the
-// strict kernels keep the reference's IEEE operations.
+// and a fraction of its instructions). Every other build returns the IEEE
+// quotient bit for bit: FP64 through gam::QuotExact (one division per divisor,
+// three fmas and a multiply per numerator), FP32 by plain division.
+// Quot1 is the same for a divisor with a single numerator, where QuotExact
+// would cost more than the division it replaces.
 template <class R> struct Quot {
 #ifdef GAM_FAST_RECIP
     R r;
@@ -109,6 +113,30 @@ template <class R> struct Quot {
     R d;
     __device__ __forceinline__ explicit Quot(R dd) : d(dd) {}
     __device__ __forceinline__ R operator()(R a) const { return a / d; }
+#endif
+};
+#ifndef GAM_FAST_RECIP
+template <> struct Quot<double> {
+    gam::QuotExact q;
+    __device__ __forceinline__ explicit Quot(double d) : q(d) {}
+    __device__ __forceinline__ double operator()(double a) const { return q(a); }
+};
+#endif
+// a/d for a finite nonzero divisor d, equal to the IEEE quotient. A zero
+// numerator returns a*d (the signed zero of a/d) without entering the
+// division, whose IEEE routine leaves its fast path for a zero numerator;
+// zero numerators are common in the step (velocities and field components
+// that are exactly zero over much of a grid).
+template <class R> __device__ __forceinline__ R qdiv(R a, R d) { return a == (R)0 ? a * d : a / d; }
+template <class R> struct Quot1 {
+#ifdef GAM_FAST_RECIP
+    R r;
+    __device__ __forceinline__ explicit Quot1(R d) : r((R)1 / d) {}
+    __device__ __forceinline__ R operator()(R a) const { return a * r; }
+#else
+    R d;
+    __device__ __forceinline__ explicit Quot1(R dd) : d(dd) {}
+    __device__ __forceinline__ R operator()(R a) const { return qdiv(a, d); }
 #endif
 };
 
@@ -163,8 +191,8 @@ template <class R> __device__ __forceinline__ R central8(const R* q) {
 // GetLRs = Cen8LRs (recon.F90:125-158) or Up7LRs (:162-198) on the volume
 // weighted stencil QdV[0..7] = dV*Q at cells -4..3 (precomputed per cell),
 // limiter nq[0..3] at cells -2..1, and the volume interpolant Vi.
-template <class R>
-__device__ __forceinline__ void lrs_from_qdv(const DevParams<R>& P, const R* QdV, const R* nq, const Quot<R>& Vi, R& Ql,
+template <class R, class Q>
+__device__ __forceinline__ void lrs_from_qdv(const DevParams<R>& P, const R* QdV, const R* nq, const Q& Vi, R& Ql,
                                              R& Qr) {
     if (!P.up7) {
         R s = (R)0;
@@ -272,8 +300,8 @@ __device__ __forceinline__ void predict_cell(const DevParams<R>& P, const R* Q, 
 
 // ExtrapAB3 (mhdgroup.F90:721-731)
 template <class R> __device__ __forceinline__ R extrap_ab3(R dt, R Q, R oQ, R ooQ, R odt, R oodt) {
-    R dQ = (Q - oQ) / odt;
-    R odQ = (oQ - ooQ) / oodt;
+    R dQ = qdiv(Q - oQ, odt);
+    R odQ = qdiv(oQ - ooQ, oodt);
     R tScl = (dt + odt) / (odt + oodt);
     return Q + dt * dQ + dt * tScl * (dQ - odQ);
 }
@@ -297,13 +325,12 @@ __device__ __forceinline__ void predict_cell_ab3(const DevParams<R>& P, const R*
 // gridutils.F90:91-93, gamutils.F90:356-358)
 template <class T> __device__ __forceinline__ T boris_speed(T Ca, T v) { return Ca * v / sqrt(Ca * Ca + v * v); }
 
-// gamCellBxyz (gridutils.F90:648-680) from the six face fluxes of cell c
+// gamCellBxyz (gridutils.F90:648-680) from the six face fluxes of cell c,
+// with the quotient by the cell volume qV
 template <class R>
 __device__ __forceinline__ void cell_bxyz(const GamBox& b, const Geo<R>& g, long c, R fI, R fIp, R fJ, R fJp, R fK,
-                                          R fKp, R* B) {
+                                          R fKp, const Quot<R>& qV, R* B) {
     const long fs = b.fs;
-    R dV = g.vol[c];
-    const Quot<R> qV(dV);
     if constexpr (std::is_same<R, float>::value) {
         // sum of flux x (face centroid - cell centroid): the same value as the
         // form below, without the cancellation of absolute coordinates
@@ -327,6 +354,11 @@ __device__ __forceinline__ void cell_bxyz(const GamBox& b, const Geo<R>& g, long
         R t = qV(fIp * xfIp + fJp * xfJp + fKp * xfKp - fI * xfI - fJ * xfJ - fK * xfK);
         B[x] = t - qV(Div * g.xyzcc[x * fs + c]);
     }
+}
+template <class R>
+__device__ __forceinline__ void cell_bxyz(const GamBox& b, const Geo<R>& g, long c, R fI, R fIp, R fJ, R fJp, R fK,
+                                          R fKp, R* B) {
+    cell_bxyz(b, g, c, fI, fIp, fJ, fJp, fK, fKp, Quot<R>(g.vol[c]), B);
 }
 
 // ----------------------------------------------------------------- bounds checks
@@ -432,7 +464,7 @@ __global__ void __launch_bounds__(256, MINB) k_predict(GamBox b, DevParams<R> P,
             const Quot<R> qAm(Am);
             R bh = qAm(hm[d]);
             w.abh[d * fs + c] = A * bh;
-            w.Bnf[d * fs + c] = hm[d] / A;
+            w.Bnf[d * fs + c] = qdiv(hm[d], A);
             w.bn[d * fs + c] = P.doLFMLim ? qAm(fQ[d]) : bh;
         }
     }
@@ -532,7 +564,10 @@ __device__ __forceinline__ void edge_lrs(const GamBox& b, const DevParams<R>& P,
 #pragma unroll
     for (int m = 0; m < 4; m++) nmag[m] = w.bn[a * fs + c + (m - 2) * s];
     const R Vi = central8(area);
-    lrs_from_qdv(P, qdv, nmag, Quot<R>(Vi), bL, bR);
+    if (P.up7)
+        lrs_from_qdv(P, qdv, nmag, Quot<R>(Vi), bL, bR);
+    else
+        lrs_from_qdv(P, qdv, nmag, Quot1<R>(Vi), bL, bR);
     fA = Vi;  // dot_product(interpWgt, AreaB) again: the same value
     bL = bL * fA;
     bR = bR * fA;
@@ -594,7 +629,7 @@ __global__ void __launch_bounds__(128, MINB) k_vxb(GamBox b, DevParams<R> P, Geo
         b1 = b1 + (R)g.edgB0[(0 + 2 * eD) * fs + c];
         b2 = b2 + (R)g.edgB0[(1 + 2 * eD) * fs + c];
     }
-    R vA = Mth<R>::sqrt_(b1 * b1 + b2 * b2) / Mth<R>::sqrt_(Dc);
+    R vA = qdiv(Mth<R>::sqrt_(b1 * b1 + b2 * b2), Mth<R>::sqrt_(Dc));
     if (P.doBoris) vA = boris_speed((R)P.Ca, vA);
     vDiff = vDiff + vA;
     const R edge = g.edge[eD * fs + c];
@@ -663,9 +698,9 @@ __device__ __forceinline__ void gas_kin_flux(const DevParams<R>& P, R sgn, const
     R Vn0 = (R)0.5 * Mth<R>::erfc_(sgn * sqlam * Vn);
 #ifdef GAM_FAST_RECIP
     // sqrt(pi lambda) = sqrt(pi) sqrt(lambda): one square root instead of two
-    R Vn1 = Vn * Vn0 - (R)0.5 * sgn * Mth<R>::exp_(-(lambda * Vn * Vn)) / ((R)SQRT_PI_D * sqlam);
+    R Vn1 = Vn * Vn0 - qdiv((R)0.5 * sgn * Mth<R>::exp_(-(lambda * Vn * Vn)), (R)SQRT_PI_D * sqlam);
 #else
-    R Vn1 = Vn * Vn0 - (R)0.5 * sgn * Mth<R>::exp_(-(lambda * Vn * Vn)) / Mth<R>::sqrt_((R)PI_D * lambda);
+    R Vn1 = Vn * Vn0 - qdiv((R)0.5 * sgn * Mth<R>::exp_(-(lambda * Vn * Vn)), Mth<R>::sqrt_((R)PI_D * lambda));
 #endif
     gF[0] = gF[0] + D * Vn1;
     gF[4] = gF[4] + (E + (R)0.5 * Pr) * Vn1 + (R)0.5 * Pr * Vn0 * Vn;
@@ -727,7 +762,7 @@ __global__ void __launch_bounds__(128, MINB) k_stress(GamBox b, DevParams<R> P, 
         if (P.doBackground) {
 #pragma unroll
             for (int x = 0; x < 3; x++) B0[x] = g.fcB0[(x + 3 * D) * fs + c];
-            B0n = g.bFlux0[D * fs + c] / (double)fa;
+            B0n = qdiv(g.bFlux0[D * fs + c], (double)fa);
         }
     }
     R WL[5], WR[5];
@@ -752,7 +787,7 @@ __global__ void __launch_bounds__(128, MINB) k_stress(GamBox b, DevParams<R> P, 
 #pragma unroll
             for (int x = 0; x < 3; x++) {
                 R deeV = WR[1 + x] - WL[1 + x];
-                R deeP = bbD * deeV / (Ca * Ca);
+                R deeP = qdiv(bbD * deeV, Ca * Ca);
                 mF[x] = mF[x] - P.cHogM * VaD * deeP;
             }
         }
@@ -857,7 +892,7 @@ __device__ __forceinline__ double cell_dt(const DevParams<R>& P, const double* U
     double Valf = 0.0;
     if (P.doMHD) {
         double MagB = sqrt(Bt[0] * Bt[0] + Bt[1] * Bt[1] + Bt[2] * Bt[2]);
-        Valf = MagB / sqrt(rho);
+        Valf = qdiv(MagB, sqrt(rho));
         if constexpr (BORIS) Valf = boris_speed(P.Ca, Valf);
     }
     double vCFL = MagV + sqrt(Cs * Cs + Valf * Valf) + 0.0;
@@ -877,7 +912,7 @@ __device__ __forceinline__ void cell_boris(const DevParams<R>& P, R* U2, const R
     R V0[3], B1[3], dPGas[3], dPMag[3], bhat1[3], dMom[3];
 #pragma unroll
     for (int x = 0; x < 3; x++) {
-        V0[x] = U0[1 + x] / D0;
+        V0[x] = qdiv(U0[1 + x], D0);
         B1[x] = (R)0.5 * (B2[x] + B0[x]);
     }
     const R alpha = (B1[0] * B1[0] + B1[1] * B1[1] + B1[2] * B1[2]) / (D2 * Ca * Ca);
@@ -935,15 +970,15 @@ __global__ void __launch_bounds__(128, MINB) k_update_cells(GamBox b, DevParams<
         const R dt = (R)sc->dt;
         R U[5];
         R Bc[3] = {(R)0, (R)0, (R)0};
+        // bFlux2Fld and Flux2Deltas divide by the same cell volume
+        const Quot<R> qdV(g.vol[c]);
         if (P.doMHD) {
             const long sj = b.sx, sk = b.sk;
             cell_bxyz(b, g, c, nxt.mf[c], nxt.mf[c + 1], nxt.mf[fs + c], nxt.mf[fs + c + sj], nxt.mf[2 * fs + c],
-                      nxt.mf[2 * fs + c + sk], Bc);
+                      nxt.mf[2 * fs + c + sk], qdV, Bc);
         }
         if (active) {
             const long sj = b.sx, sk = b.sk;
-            const R dV = g.vol[c];
-            const Quot<R> qdV(dV);
             R dGasH[5];
 #pragma unroll
             for (int v = 0; v < 5; v++) {
@@ -1817,6 +1852,7 @@ template <class R> __device__ __forceinline__ R* halo_ptr(const StateBuf<R>& S, 
 template <class R>
 __global__ void __launch_bounds__(256) k_halo(GamBox b, StateBuf<R> S, R* __restrict__ buf, int side, int unpack,
                                               int copyB, const GamScalars* sc) {
+    if (sc->halted) return;  // a failed step keeps its state, ghosts included
     const long nx = b.Ni + 1, ny = b.Nj + 1;
     const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
     if (t >= 4 * nx * ny) return;
@@ -1837,6 +1873,7 @@ __global__ void __launch_bounds__(256) k_halo(GamBox b, StateBuf<R> S, R* __rest
 // Bxyz of the unpacked ghost cells from their faces (the final bFlux2Fld)
 template <class R>
 __global__ void __launch_bounds__(256) k_halo_bxyz(GamBox b, Geo<R> g, StateBuf<R> S, int side, const GamScalars* sc) {
+    if (sc->halted) return;
     const long nx = b.Ni, ny = b.Nj;
     const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
     if (t >= 4 * nx * ny) return;
