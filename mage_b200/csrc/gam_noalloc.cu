@@ -9,6 +9,7 @@
 // and Grid%volume on the device, writes the five totals to the caller's device
 // buffer, and keeps its block partial sums in the fixed file-scope array below
 // instead of calling cudaMalloc.
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <mutex>
 #include <stdio.h>
@@ -28,7 +29,40 @@ static __device__ __align__(256) double g_totals_scratch[5 * NA_MAXB];
 
 constexpr int NA_MAX_DEVICES = 64;
 std::mutex g_mu;
+// Per device: the array's address and the id of the context it belongs to.
+// cudaDeviceReset destroys the context (and the module that holds the array);
+// the next call then runs in a new context with a new id and looks the
+// address up again instead of passing a stale one.
 double* g_scratch_addr[NA_MAX_DEVICES] = {nullptr};
+unsigned long long g_scratch_ctx[NA_MAX_DEVICES] = {0};
+
+// Id of the calling thread's current context (0 if none), through the
+// driver's entry points as the runtime exposes them (no link to libcuda).
+unsigned long long current_ctx_id() {
+    typedef CUresult (*CtxGetCurrent)(CUcontext*);
+    typedef CUresult (*CtxGetId)(CUcontext, unsigned long long*);
+    static CtxGetCurrent get_cur = nullptr;
+    static CtxGetId get_id = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_cur = (CtxGetCurrent)f;
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = (CtxGetId)f;
+    }
+    if (!get_cur || !get_id) return 0;
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (get_cur(&ctx) != CUDA_SUCCESS || !ctx) return 0;
+    if (get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
 
 // Block b sums the active cells [b*CHUNK, (b+1)*CHUNK) of Gas*volume in a
 // fixed pattern and tree, so the result does not depend on timing.
@@ -109,10 +143,13 @@ extern "C" int gam_totals_noalloc(const double* Gas, const double* volume, int32
     }
     double* scratch;
     {
-        // first call on this device: host address of the device array (set-up
-        // happens here, so make that first call outside any stream capture)
+        // set-up, once per device and context: the device address of the
+        // array, looked up with this device current (the first call on a
+        // device does this, so make it outside any stream capture); looked up
+        // again after cudaDeviceReset, which gives the device a new context
         std::lock_guard<std::mutex> lock(g_mu);
-        if (!g_scratch_addr[dev]) {
+        const unsigned long long id = current_ctx_id();
+        if (!g_scratch_addr[dev] || id == 0 || id != g_scratch_ctx[dev]) {
             void* p = nullptr;
             e = cudaGetSymbolAddress(&p, g_totals_scratch);
             if (e != cudaSuccess) {
@@ -120,12 +157,20 @@ extern "C" int gam_totals_noalloc(const double* Gas, const double* volume, int32
                 return GAM_ECUDA;
             }
             g_scratch_addr[dev] = (double*)p;
+            g_scratch_ctx[dev] = current_ctx_id();  // the lookup made the context current if it was not
         }
         scratch = g_scratch_addr[dev];
     }
     const int nb = (int)((ncells + NA_CHUNK - 1) / NA_CHUNK);
     cudaStream_t s = (cudaStream_t)stream;
+    // an error left pending by an earlier, unrelated launch on this thread is
+    // reported here as this call's GAM_ECUDA
     k_na_partials<<<nb, NA_NT, 0, s>>>(Gas, volume, Nip, Njp, Nkp, ncells, scratch);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        put_err(err, errlen, cudaGetErrorString(e));
+        return GAM_ECUDA;
+    }
     k_na_final<<<1, NA_NT, 0, s>>>(scratch, nb, out);
     e = cudaGetLastError();
     if (e != cudaSuccess) {
