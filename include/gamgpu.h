@@ -287,6 +287,36 @@ int gam_step_begin(gam_handle* h);
 int gam_dt_partial(gam_handle* h, uint64_t* dtmin_bits, int32_t* nbad);
 int gam_step_end(gam_handle* h, uint64_t dtmin_bits, int32_t nbad, double* dt, double* t);
 
+/* The same k-slab step without host round trips, for a caller that reduces
+ * on the device (an NCCL all-reduce of device buffers); the dt AllReduce(MIN)
+ * of gamapp_mpi.F90:495-512 then never leaves the GPUs.
+ *   gam_set_stream(h, stream)           enqueue all of this handle's work on
+ *                                       the caller's stream (a non-default
+ *                                       cudaStream_t; NULL: the handle's own);
+ *                                       halo pack/unpack then return at once
+ *   gam_step_begin_dev(h)               predictor .. cell update
+ *   gam_dt_partial_dev(h, bits, nbad)   writes this slab's dt candidate bits
+ *                                       and bad-cell count to the device
+ *                                       int64 bits[0], nbad[0]
+ *   (caller: MIN-reduce bits, SUM-reduce nbad over the slabs, in place)
+ *   gam_step_end_dev(h, bits, nbad)     reads the reduced values from device
+ *                                       memory: dt decision, local boundaries
+ *   halo exchange as above
+ *   gam_step_status(h, &dt, &t)         waits for the handle's stream; dt and
+ *                                       t after the last step, and the status
+ *                                       of the steps since the previous check
+ * Every call only enqueues work (no host synchronisation) except
+ * gam_step_status. A step that fails CalcDT halts the kernels of the later
+ * steps and halo exchanges on the device (the state stays as the failing
+ * step left it); every slab takes the same decision from the same reduced
+ * values, and gam_step_status returns it (GAM_EDT_BAD / GAM_EDT_DISASTER).
+ * No counterpart in the reference, whose MPI reduction is a host call. */
+int gam_set_stream(gam_handle* h, void* stream);
+int gam_step_begin_dev(gam_handle* h);
+int gam_dt_partial_dev(gam_handle* h, int64_t* dtmin_bits, int64_t* nbad);
+int gam_step_end_dev(gam_handle* h, const int64_t* dtmin_bits, const int64_t* nbad);
+int gam_step_status(gam_handle* h, double* dt, double* t);
+
 /* Flux stage of the step and its hand-written adjoint (differentiation form),
  * on caller-owned device arrays in the unpadded box layout: each field is
  * (nc, Nk+1, Nj+1, Ni+1) contiguous, i fastest, Ni = Nip + 8 (cell fields
@@ -385,8 +415,13 @@ int gam_step_adj(const gam_params* p, int32_t fp32, const void* const* geo, cons
  * limits a call to Nip*Njp*Nkp <= 67,108,864 active cells; larger grids are
  * rejected with GAM_EINVAL and a message in err (errlen bytes, may be NULL).
  * The first call on a device looks up that array's address (set-up): make it
- * before any stream capture. All calls share the array: calls whose kernels
- * overlap on the GPU (different streams or devices in flight at once) race. */
+ * before any stream capture. The address is kept per device and context, and
+ * looked up again when the device's context changes (after cudaDeviceReset).
+ * Every call on a device shares that device's array and finds it holding the
+ * last call's partial sums: calls whose kernels overlap on the same device
+ * (for example enqueued on different streams) race; calls on different devices
+ * do not, each device holding its own copy. An error left pending by an
+ * earlier launch on the calling thread is returned as this call's GAM_ECUDA. */
 int gam_totals_noalloc(const double* Gas, const double* volume, int32_t Nip, int32_t Njp, int32_t Nkp, double* out,
                        void* stream, char* err, int32_t errlen);
 

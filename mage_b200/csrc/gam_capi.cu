@@ -81,6 +81,8 @@ struct gam_handle {
     double* windTab = nullptr;  // device: wC, wF(3), sF(3) of the solar-wind BC
     bool haveBg = false, haveWind = false, haveInflow = false;
     cudaStream_t s = nullptr;
+    cudaStream_t own_s = nullptr;  // the handle's own stream (s unless gam_set_stream gave another)
+    int nasync = 0;                // device-resident k-slab steps since the last gam_step_status
     bool f32 = false;
     std::vector<void*> allocs;
     GeoD gd{};
@@ -267,6 +269,7 @@ extern "C" int gam_create(const gam_params* p, gam_handle** out) {
     h->b = gam_make_box(p->Nip, p->Njp, p->Nkp);
     h->f32 = p->precision == GAM_FP32;
     if (cudaStreamCreateWithFlags(&h->s, cudaStreamNonBlocking) != cudaSuccess) return bad(GAM_ECUDA, "no CUDA device");
+    h->own_s = h->s;
     cudaEventCreate(&h->ev0);
     cudaEventCreate(&h->ev1);
     cudaError_t e = cudaSuccess;
@@ -349,7 +352,7 @@ extern "C" int gam_destroy(gam_handle* h) {
         if (h->evs[q]) cudaEventDestroy(h->evs[q]);
     for (int q = 0; q < 5; q++)
         if (h->aux[q]) cudaStreamDestroy(h->aux[q]);
-    if (h->s) cudaStreamDestroy(h->s);
+    if (h->own_s) cudaStreamDestroy(h->own_s);  // a stream given by gam_set_stream stays the caller's
     delete h;
     return GAM_OK;
 }
@@ -1249,7 +1252,7 @@ static int halo_call(gam_handle* h, int side, int unpack, int copyB, void* buf) 
     else
         gam_fast_halo_f64(h->cd, h->cur, h->s, side, unpack, copyB, buf);
     CK(h, cudaGetLastError());
-    CK(h, cudaStreamSynchronize(h->s));
+    if (h->s == h->own_s) CK(h, cudaStreamSynchronize(h->s));
     return GAM_OK;
 }
 extern "C" int gam_halo_pack(gam_handle* h, int32_t side, void* dev_buf) { return halo_call(h, side, 0, 0, dev_buf); }
@@ -1323,6 +1326,76 @@ extern "C" int gam_step_end(gam_handle* h, uint64_t dtmin_bits, int32_t nbad, do
     cudaEventElapsedTime(&ms, h->ev0, h->ev1);
     h->lastMs = ms;
     h->cur ^= 1;
+    if (dt) *dt = s.dt;
+    if (t) *t = s.t;
+    if (int rcb = check_bounds(h, s)) return rcb;
+    if (s.halted)
+        return fail(h, s.status == 5 ? GAM_EDT_DISASTER : GAM_EDT_BAD,
+                    s.status == 5 ? "CalcDT: timestep too small or not finite" : "CalcDT: timestep dropped 10x or below limDT0");
+    return GAM_OK;
+}
+
+// device-resident k-slab steps: the dt candidate leaves and the reduced
+// value returns through device memory
+__global__ void k_partial_out(const GamScalars* sc, int64_t* bits, int64_t* nbad) {
+    *bits = (int64_t)sc->dtmin_bits;
+    *nbad = (int64_t)sc->nbad;
+}
+__global__ void k_partial_in(GamScalars* sc, const int64_t* bits, const int64_t* nbad) {
+    sc->dtmin_bits = (unsigned long long)*bits;
+    sc->nbad = (int)*nbad;
+}
+
+extern "C" int gam_set_stream(gam_handle* h, void* stream) {
+    if (!h) return GAM_EINVAL;
+    cudaStream_t ns = stream ? (cudaStream_t)stream : h->own_s;
+    if (ns != h->s) CK(h, cudaStreamSynchronize(h->s));  // work already enqueued finishes first
+    h->s = ns;
+    return GAM_OK;
+}
+
+extern "C" int gam_step_begin_dev(gam_handle* h) {
+    if (!h) return GAM_EINVAL;
+    int rc = require_slab(h);
+    if (rc) return rc;
+    if ((rc = ensure_phase_graph(h, h->cur, 0))) return rc;
+    if ((rc = ensure_phase_graph(h, h->cur, 1))) return rc;
+    if (h->nasync == 0) CK(h, cudaEventRecord(h->ev0, h->s));
+    CK(h, cudaGraphLaunch(h->pgraph[h->cur][0], h->s));
+    return GAM_OK;
+}
+
+extern "C" int gam_dt_partial_dev(gam_handle* h, int64_t* dtmin_bits, int64_t* nbad) {
+    if (!h || !dtmin_bits || !nbad) return GAM_EINVAL;
+    k_partial_out<<<1, 1, 0, h->s>>>(h->sc, dtmin_bits, nbad);
+    CK(h, cudaGetLastError());
+    return GAM_OK;
+}
+
+extern "C" int gam_step_end_dev(gam_handle* h, const int64_t* dtmin_bits, const int64_t* nbad) {
+    if (!h || !dtmin_bits || !nbad) return GAM_EINVAL;
+    int rc = require_slab(h);
+    if (rc) return rc;
+    k_partial_in<<<1, 1, 0, h->s>>>(h->sc, dtmin_bits, nbad);
+    CK(h, cudaGetLastError());
+    CK(h, cudaGraphLaunch(h->pgraph[h->cur][1], h->s));
+    CK(h, cudaEventRecord(h->ev1, h->s));
+    h->cur ^= 1;
+    h->nasync++;
+    return GAM_OK;
+}
+
+extern "C" int gam_step_status(gam_handle* h, double* dt, double* t) {
+    if (!h) return GAM_EINVAL;
+    GamScalars s;
+    CK(h, cudaMemcpyAsync(&s, h->sc, sizeof(s), cudaMemcpyDeviceToHost, h->s));
+    CK(h, cudaStreamSynchronize(h->s));
+    if (h->nasync > 0) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+        h->lastMs = ms;
+    }
+    h->nasync = 0;
     if (dt) *dt = s.dt;
     if (t) *t = s.t;
     if (int rcb = check_bounds(h, s)) return rcb;

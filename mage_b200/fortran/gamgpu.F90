@@ -205,6 +205,30 @@ module gamgpu
             integer(c_int32_t), value :: nbad
             real(c_double), intent(out) :: dt, t
         end function
+        ! the same step with the dt reduction on the device: bits and nbad are
+        ! device addresses (c_devptr of CUDA Fortran, or c_ptr of a device
+        ! buffer) of one int64 each; stream is a cudaStream_t
+        integer(c_int) function gam_set_stream(h, stream) bind(C, name="gam_set_stream")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h, stream
+        end function
+        integer(c_int) function gam_step_begin_dev(h) bind(C, name="gam_step_begin_dev")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h
+        end function
+        integer(c_int) function gam_dt_partial_dev(h, bits, nbad) bind(C, name="gam_dt_partial_dev")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h, bits, nbad
+        end function
+        integer(c_int) function gam_step_end_dev(h, bits, nbad) bind(C, name="gam_step_end_dev")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: h, bits, nbad
+        end function
+        integer(c_int) function gam_step_status(h, dt, t) bind(C, name="gam_step_status")
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: h
+            real(c_double), intent(out) :: dt, t
+        end function
         integer(c_int) function gam_get_geometry_arrays(h, face, xfc, Tf, volume, xyzcc, di, dj, dk, edge, Te, Teb) &
                 bind(C, name="gam_get_geometry_arrays")
             import :: c_int, c_ptr

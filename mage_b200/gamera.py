@@ -57,7 +57,8 @@ EXPORTED = (
     "gam_init_blast_wave", "gam_profile_step", "gam_totals_noalloc", "gam_set_background", "gam_get_background",
     "gam_set_background_dipole", "gam_set_wind", "gam_set_wind_series", "gam_init_test_problem", "gam_set_inflow", "gam_set_oostate", "gam_get_oostate", "gam_bounds_status", "gam_init_dipole_wind", "gam_write_restart", "gam_read_restart",
     "gam_halo_bytes", "gam_halo_pack", "gam_halo_unpack", "gam_init_finish_halo", "gam_set_start", "gam_step_begin",
-    "gam_dt_partial", "gam_step_end", "gam_set_slab_edges", "gam_flux_forward", "gam_flux_adjoint",
+    "gam_dt_partial", "gam_step_end", "gam_set_slab_edges", "gam_set_stream", "gam_step_begin_dev",
+    "gam_dt_partial_dev", "gam_step_end_dev", "gam_step_status", "gam_flux_forward", "gam_flux_adjoint",
     "gam_efield_forward", "gam_efield_adjoint", "gam_predict_stage", "gam_update_stage", "gam_step_work_bytes",
     "gam_step_fwd_save", "gam_step_adj",
 )
@@ -132,6 +133,11 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     L.gam_step_begin.argtypes = [C.c_void_p]
     L.gam_dt_partial.argtypes = [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_int32)]
     L.gam_step_end.argtypes = [C.c_void_p, C.c_uint64, C.c_int32, _dp, _dp]
+    L.gam_set_stream.argtypes = [C.c_void_p, C.c_void_p]
+    L.gam_step_begin_dev.argtypes = [C.c_void_p]
+    L.gam_dt_partial_dev.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    L.gam_step_end_dev.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    L.gam_step_status.argtypes = [C.c_void_p, _dp, _dp]
     L.gam_read_restart.argtypes = [C.c_void_p, C.c_char_p]
     L.gam_init_dipole_wind.argtypes = [C.c_void_p, _dp, C.c_uint64, C.c_double]
     L.gam_totals_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p,
@@ -368,11 +374,14 @@ class GameraGPU:
         self._check(self.L.gam_halo_bytes(self.h, C.byref(n)))
         return n.value
 
-    def halo_pack(self, side: int, dev_ptr: int):
-        self._check(self.L.gam_halo_pack(self.h, int(side), C.c_void_p(dev_ptr)))
+    def halo_pack(self, side: int, buf):
+        """Pack side 0 (down) or 1 (up) into a device buffer (a tensor or a pointer)."""
+        ptr = buf.data_ptr() if hasattr(buf, "data_ptr") else int(buf)
+        self._check(self.L.gam_halo_pack(self.h, int(side), C.c_void_p(ptr)))
 
-    def halo_unpack(self, side: int, dev_ptr: int, copyB: bool = False):
-        self._check(self.L.gam_halo_unpack(self.h, int(side), C.c_void_p(dev_ptr), int(copyB)))
+    def halo_unpack(self, side: int, buf, copyB: bool = False):
+        ptr = buf.data_ptr() if hasattr(buf, "data_ptr") else int(buf)
+        self._check(self.L.gam_halo_unpack(self.h, int(side), C.c_void_p(ptr), int(copyB)))
 
     def init_finish_halo(self) -> float:
         dt = C.c_double()
@@ -393,6 +402,31 @@ class GameraGPU:
     def step_end(self, bits: int, nbad: int):
         dt, t = C.c_double(), C.c_double()
         self._check(self.L.gam_step_end(self.h, C.c_uint64(bits), int(nbad), C.byref(dt), C.byref(t)))
+        return dt.value, t.value
+
+    # device-resident k-slab steps (no host round trip per step)
+    def set_stream(self, stream_ptr: int | None):
+        """Enqueue this handle's work on the caller's CUDA stream (a
+        non-default stream; None: the handle's own)."""
+        self._check(self.L.gam_set_stream(self.h, C.c_void_p(stream_ptr) if stream_ptr else None))
+
+    def step_begin_dev(self):
+        self._check(self.L.gam_step_begin_dev(self.h))
+
+    def dt_partial_dev(self, bits, nbad):
+        """Write this slab's dt candidate bits and bad-cell count into the
+        one-element int64 device tensors bits and nbad."""
+        self._check(self.L.gam_dt_partial_dev(self.h, C.c_void_p(bits.data_ptr()), C.c_void_p(nbad.data_ptr())))
+
+    def step_end_dev(self, bits, nbad):
+        """Finish the step with the reduced values in device tensors bits, nbad."""
+        self._check(self.L.gam_step_end_dev(self.h, C.c_void_p(bits.data_ptr()), C.c_void_p(nbad.data_ptr())))
+
+    def step_status(self):
+        """Wait for the handle's stream; (dt, t) after the last step, raising
+        GamError if one of the steps since the previous check failed."""
+        dt, t = C.c_double(), C.c_double()
+        self._check(self.L.gam_step_status(self.h, C.byref(dt), C.byref(t)))
         return dt.value, t.value
 
     # --- restart files --------------------------------------------------------

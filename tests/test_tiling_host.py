@@ -1,7 +1,15 @@
-"""Host logic of the k-slab halo exchange (mage_b200.tiling.exchange_dist) on
-CPU ranks over gloo: every rank receives its lower ghosts from the slab below
-(that slab's upward pack) and its upper ghosts from the slab above, periodic
-in k, with 2 ranks (both neighbours the same rank) and with 3."""
+"""Host logic of the k-slab tiling on CPU ranks over gloo:
+
+* the halo exchange (mage_b200.tiling.exchange_dist): every rank receives its
+  lower ghosts from the slab below (that slab's upward pack) and its upper
+  ghosts from the slab above, periodic in k, with 2 ranks (both neighbours the
+  same rank) and with 3;
+* the orchestration of Slabs.step with a host stand-in for the GPU handle:
+  every rank finishes each step with the MIN of the slabs' dt bits and the
+  SUM of their bad-cell counts (the dt AllReduce of gamapp_mpi.F90:495-512),
+  takes the same failure decision when one rank holds a bad cell, and runs
+  the calls of a step in the same order (begin, candidate, end, pack down,
+  pack up, unpack lower, unpack upper)."""
 import os
 import socket
 
@@ -59,3 +67,110 @@ def test_slab_corners_overlap():
     for r, p in enumerate(parts):
         assert p.shape == (3, 4 + 9, 25, 25)
         assert np.array_equal(p, xyz[:, 4 * r:4 * r + 13])
+
+
+class _FakeSlab:
+    """Stands in for GameraGPU inside Slabs: the slab's dt candidate in step n
+    is dt0 (1 + n/10) (1 + rank/100); plant_bad = (rank, step) gives that rank
+    one bad cell in that step. The halo buffers carry 100 rank + side."""
+
+    def __init__(self, rank, plant_bad=None):
+        self.rank, self.plant_bad = rank, plant_bad
+        self.n, self.log, self.recv = 0, [], {}
+        self.failed, self.dt, self.seen = False, None, []
+
+    def halo_bytes(self):
+        return 16
+
+    def halo_pack(self, side, buf):
+        buf.fill_(100 * self.rank + side)
+        self.log.append(("pack", side))
+
+    def halo_unpack(self, side, buf, copyB=False):
+        self.recv[side] = int(buf[0])
+        self.log.append(("unpack", side))
+
+    def init_finish_halo(self):
+        return 0.5 + self.rank
+
+    def set_start(self, dt):
+        self.start = dt
+
+    def step_begin_dev(self):
+        self.n += 1
+        self.log.append(("begin",))
+
+    def dt_partial_dev(self, bits, nbad):
+        import struct
+        dt = 1e-3 * (1 + self.n / 10) * (1 + self.rank / 100)
+        bits[0] = struct.unpack("<q", struct.pack("<d", dt))[0]
+        nbad[0] = 1 if self.plant_bad == (self.rank, self.n) else 0
+        self.log.append(("partial",))
+
+    def step_end_dev(self, bits, nbad):
+        import struct
+        self.seen.append((int(bits[0]), int(nbad[0])))
+        self.dt = struct.unpack("<d", struct.pack("<q", int(bits[0])))[0]
+        if int(nbad[0]) > 0:
+            self.failed = True
+        self.log.append(("end",))
+
+    def step_status(self):
+        from mage_b200.gamera import GamError
+        if self.failed:
+            raise GamError(5, "CalcDT: timestep too small or not finite")
+        return self.dt, float(self.n)
+
+
+def _slab_worker(rank, n, port, plant, q):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=n)
+    try:
+        from mage_b200.tiling import Slabs
+        sl = Slabs((16, 16, 4 * n), None, n, comm="dist", device=torch.device("cpu"),
+                   make_app=lambda r: _FakeSlab(r, plant))
+        app = sl.apps[0]
+        app.log.clear()
+        code = 0
+        try:
+            dt, _ = sl.step(3)
+        except Exception as e:  # the stand-in's GamError
+            dt, code = None, getattr(e, "code", -1)
+        q.put((rank, app.start, dt, code, app.seen, app.recv, app.log))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("plant", [None, (1, 2)], ids=["ok", "bad-cell-on-rank1"])
+def test_slab_step_orchestration(plant):
+    import struct
+    n = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_slab_worker, args=(r, n, port, plant, q)) for r in range(n)]
+    for p in procs:
+        p.start()
+    got = {}
+    for _ in range(n):
+        r = q.get(timeout=180)
+        got[r[0]] = r[1:]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    step = [("begin",), ("partial",), ("end",), ("pack", 0), ("pack", 1), ("unpack", 0), ("unpack", 1)]
+    for r in range(n):
+        start, dt, code, seen, recv, log = got[r]
+        assert start == 0.5  # min over the slabs of the start dt
+        assert log == step * 3
+        assert recv == {0: 100 * ((r - 1) % n) + 1, 1: 100 * ((r + 1) % n) + 0}
+        for k, (bits, nbad) in enumerate(seen):  # the reduced candidate of step k+1: rank 0's
+            want = 1e-3 * (1 + (k + 1) / 10)
+            assert bits == struct.unpack("<q", struct.pack("<d", want))[0], (r, k)
+            assert nbad == (1 if plant is not None and plant[1] == k + 1 else 0)
+        if plant is None:
+            assert code == 0 and dt == 1e-3 * 1.3
+        else:
+            assert code == 5 and dt is None  # the same decision on every rank
+    assert got[0][3] == got[1][3]  # both ranks saw the same reduced values every step
