@@ -21,6 +21,16 @@ namespace gam_adj {
 
 __device__ GamScalars g_adj_scalars;  // zero: not halted
 
+// the stage scalars, written on the stream by a kernel from its arguments
+// (a copy from host memory would make the host wait for the stream)
+__global__ void k_adj_scalars(GamScalars* sc, double dt, double pdt, double odt, int fixedTimestep) {
+    *sc = GamScalars{};
+    sc->dt = dt;
+    sc->pdt = pdt;
+    sc->odt = odt;
+    sc->fixedTimestep = fixedTimestep;
+}
+
 template <class A> __device__ __forceinline__ A sgnz(A x) { return x > (A)0 ? (A)1 : (x < (A)0 ? (A)-1 : (A)0); }
 
 // reverse of lrs_from_qdv (8CENT) for one variable: scatter the adjoints of
@@ -699,7 +709,8 @@ __global__ void __launch_bounds__(128) k_update_adj_cells(GamBox b, DevParams<R>
 template <class R>
 __global__ void __launch_bounds__(256) k_update_adj_faces(GamBox b, DevParams<R> P, double dt,
                                                           const R* __restrict__ sU, const R* __restrict__ sM,
-                                                          const R* __restrict__ dnmf, R* dmf, R* dgF, R* dmF, R* dE) {
+                                                          const R* __restrict__ dnmf, R* dmf, R* dgF, R* dmF, R* dE,
+                                                          int assign) {
     using A = R;
     int ii, jj, kk;
     Range r{0, b.Ni, 0, b.Nj, 0, b.Nk};
@@ -718,14 +729,20 @@ __global__ void __launch_bounds__(256) k_update_adj_faces(GamBox b, DevParams<R>
             A a = (A)0.0;
             if (inLo) a += sU[v * fs + c];
             if (inUp) a -= sU[v * fs + cu];
-            dgF[(v + 5 * d) * fs + c] += (R)a;
+            if (assign)
+                dgF[(v + 5 * d) * fs + c] = (R)a;
+            else
+                dgF[(v + 5 * d) * fs + c] += (R)a;
         }
         if (P.doMHD)
             for (int x = 0; x < 3; x++) {
                 A a = (A)0.0;
                 if (inLo) a += sM[x * fs + c];
                 if (inUp) a -= sM[x * fs + cu];
-                dmF[(x + 3 * d) * fs + c] += (R)a;
+                if (assign)
+                    dmF[(x + 3 * d) * fs + c] = (R)a;
+                else
+                    dmF[(x + 3 * d) * fs + c] += (R)a;
             }
         dmf[d * fs + c] += dnmf[d * fs + c];
     }
@@ -743,9 +760,15 @@ __global__ void __launch_bounds__(256) k_update_adj_faces(GamBox b, DevParams<R>
     const A aE2 = -dt * (An(0, ii, jj - 1, kk) - a0c - An(1, ii - 1, jj, kk) + a1c);
     const A aE1 = -dt * (-An(0, ii, jj, kk - 1) + a0c + An(2, ii - 1, jj, kk) - a2c);
     const A aE0 = -dt * (An(1, ii, jj, kk - 1) - a1c - An(2, ii, jj - 1, kk) + a2c);
-    dE[c] += (R)aE0;
-    dE[fs + c] += (R)aE1;
-    dE[2 * fs + c] += (R)aE2;
+    if (assign) {
+        dE[c] = (R)aE0;
+        dE[fs + c] = (R)aE1;
+        dE[2 * fs + c] = (R)aE2;
+    } else {
+        dE[c] += (R)aE0;
+        dE[fs + c] += (R)aE1;
+        dE[2 * fs + c] += (R)aE2;
+    }
 }
 }  // namespace gam_adj
 
@@ -865,7 +888,7 @@ template <class R>
 int efield_call(const gam_params* p, const void* Dh, const void* abh, const void* bn, const void* VdV, const void* vol,
                 const void* face, const void* edge, const void* Te, const void* Teb, const double* edgB0, double dt,
                 void* AVf, void* E, const void* dE, void* dDh, void* dabh, void* dbn, void* dVdV, void* dAVf,
-                cudaStream_t s) {
+                cudaStream_t s, bool avf_saved = false) {
     using namespace gam_adj;
     const GamBox b = torch_box(p->Nip, p->Njp, p->Nkp);
     const DevParams<R> P = dev_params<R>(p);
@@ -876,13 +899,9 @@ int efield_call(const gam_params* p, const void* Dh, const void* abh, const void
     Work<R> w;
     memset(&w, 0, sizeof(w));
     w.Dh = (R*)Dh; w.abh = (R*)abh; w.bn = (R*)bn; w.VdV = (R*)VdV; w.AVf = (R*)AVf; w.E = (R*)E;
-    GamScalars hs;
-    memset(&hs, 0, sizeof(hs));
-    hs.dt = dt;
-    if (cudaMemcpyToSymbolAsync(g_adj_scalars, &hs, sizeof(hs), 0, cudaMemcpyHostToDevice, s) != cudaSuccess)
-        return GAM_ECUDA;
     GamScalars* sc = nullptr;
     if (cudaGetSymbolAddress((void**)&sc, g_adj_scalars) != cudaSuccess) return GAM_ECUDA;
+    k_adj_scalars<<<1, 1, 0, s>>>(sc, dt, 0.0, 0.0, 0);
     const int G = GAM_NG;
     const Range mf[3] = {{0, b.Ni - 1, G, G + b.Njp, 0, b.Nk - 1},
                          {0, b.Ni - 1, 0, b.Nj - 1, G, G + b.Nkp},
@@ -896,7 +915,8 @@ int efield_call(const gam_params* p, const void* Dh, const void* abh, const void
                     (unsigned)((r.k1 - r.k0 + 1 + blk.z - 1) / blk.z));
     };
     for (int eD = 0; eD < 3; eD++) {
-        k_mom2face<R><<<grid(mf[eD]), blk, 0, s>>>(b, P, g, w, eD, mf[eD], sc);
+        // the adjoint of a whole step finds AVf as its forward left it
+        if (!(dE && avf_saved)) k_mom2face<R><<<grid(mf[eD]), blk, 0, s>>>(b, P, g, w, eD, mf[eD], sc);
         if (!dE) {
             k_vxb<R><<<grid(ed[eD]), blk, 0, s>>>(b, P, g, w, eD, ed[eD], sc);
         } else {
@@ -955,12 +975,9 @@ template <class R> Geo<R> geo_of(const void* vol, const void* face, const void* 
     return g;
 }
 int set_scalars(double dt, double pdt, double odt, cudaStream_t s, GamScalars** sc) {
-    GamScalars hs;
-    memset(&hs, 0, sizeof(hs));
-    hs.dt = dt; hs.pdt = pdt; hs.odt = odt; hs.fixedTimestep = 1;
-    if (cudaMemcpyToSymbolAsync(gam_adj::g_adj_scalars, &hs, sizeof(hs), 0, cudaMemcpyHostToDevice, s) != cudaSuccess)
-        return GAM_ECUDA;
-    return cudaGetSymbolAddress((void**)sc, gam_adj::g_adj_scalars) == cudaSuccess ? GAM_OK : GAM_ECUDA;
+    if (cudaGetSymbolAddress((void**)sc, gam_adj::g_adj_scalars) != cudaSuccess) return GAM_ECUDA;
+    gam_adj::k_adj_scalars<<<1, 1, 0, s>>>(*sc, dt, pdt, odt, 1);
+    return cudaGetLastError() == cudaSuccess ? GAM_OK : GAM_ECUDA;
 }
 dim3 grid3(const Range& r, dim3 blk) {
     return dim3((unsigned)((r.i1 - r.i0 + 1 + blk.x - 1) / blk.x), (unsigned)((r.j1 - r.j0 + 1 + blk.y - 1) / blk.y),
@@ -999,7 +1016,8 @@ int predict_call(const gam_params* p, const void* const* st, const void* const* 
 }
 template <class R>
 int update_call(const gam_params* p, const void* const* in, const void* const* geo, const double* dpB0, double dt,
-                void* const* out, const void* const* din, void* sU, void* sM, void* const* dst, cudaStream_t s) {
+                void* const* out, const void* const* din, void* sU, void* sM, void* const* dst, cudaStream_t s,
+                bool assign = false) {
     using namespace gam_adj;
     const GamBox b = torch_box(p->Nip, p->Njp, p->Nkp);
     const DevParams<R> P = dev_params<R>(p);
@@ -1022,7 +1040,8 @@ int update_call(const gam_params* p, const void* const* in, const void* const* g
         k_update_adj_cells<R><<<grid3(cells, blk), blk, 0, s>>>(b, P, g, cur, w, dt, (const R*)din[0], (R*)dst[0],
                                                                  (R*)sU, (R*)sM);
         k_update_adj_faces<R><<<grid3(all, blk), blk, 0, s>>>(b, P, dt, (const R*)sU, (const R*)sM, (const R*)din[1],
-                                                               (R*)dst[1], (R*)dst[3], (R*)dst[4], (R*)dst[2]);
+                                                               (R*)dst[1], (R*)dst[3], (R*)dst[4], (R*)dst[2],
+                                                               assign ? 1 : 0);
     }
     return cudaGetLastError() == cudaSuccess ? GAM_OK : GAM_ECUDA;
 }
@@ -1054,4 +1073,30 @@ extern "C" int gam_update_stage(const gam_params* p, int32_t fp32, const void* c
     cudaStream_t s = (cudaStream_t)stream;
     return fp32 ? update_call<float>(p, in, geo, dpB0, dt, out, din, sU, sM, dst, s)
                 : update_call<double>(p, in, geo, dpB0, dt, out, din, sU, sM, dst, s);
+}
+
+// For the whole-step adjoint (gam_stepadj.cu), which owns its work area: the
+// update stage's adjoint stores the face, flux and edge adjoints (dst[2..4])
+// instead of adding into caller-zeroed arrays, and the E-field adjoint finds
+// AVf as the step's forward left it instead of recomputing Mom2Face.
+int gam_update_adjoint_store(const gam_params* p, int32_t fp32, const void* const* in, const void* const* geo,
+                             const double* dpB0, double dt, const void* const* din, void* sU, void* sM,
+                             void* const* dst, void* stream) {
+    int rc = check(p, fp32);
+    if (rc) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    return fp32 ? update_call<float>(p, in, geo, dpB0, dt, nullptr, din, sU, sM, dst, s, true)
+                : update_call<double>(p, in, geo, dpB0, dt, nullptr, din, sU, sM, dst, s, true);
+}
+int gam_efield_adjoint_saved(const gam_params* p, int32_t fp32, const void* Dh, const void* abh, const void* bn,
+                             const void* VdV, const void* volume, const void* face, const void* edge, const void* Te,
+                             const void* Teb, const double* edgB0, double dt, void* AVf, const void* dE, void* dDh,
+                             void* dabh, void* dbn, void* dVdV, void* dAVf, void* stream) {
+    int rc = check(p, fp32);
+    if (rc) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    return fp32 ? efield_call<float>(p, Dh, abh, bn, VdV, volume, face, edge, Te, Teb, edgB0, dt, AVf, nullptr, dE,
+                                     dDh, dabh, dbn, dVdV, dAVf, s, true)
+                : efield_call<double>(p, Dh, abh, bn, VdV, volume, face, edge, Te, Teb, edgB0, dt, AVf, nullptr, dE,
+                                      dDh, dabh, dbn, dVdV, dAVf, s, true);
 }

@@ -41,6 +41,9 @@
 #ifndef GAM_NS
 #error "GAM_NS must name the namespace of this build"
 #endif
+#ifndef GAM_STRICT_KERNELS
+#define GAM_STRICT_KERNELS 0  // 1: the strict build (launch bounds measured for it)
+#endif
 
 namespace GAM_NS {
 
@@ -1627,8 +1630,9 @@ template <class R, class F> void for_each_kernel(const Ctx<R>& C, int cur, cudaS
                                                                                           C.oomf);
         else if (C.kvar & 8)
             k_predict<R, 1><<<grid_for(all, pblk), pblk, 0, s>>>(b, C.P, C.g, S, O, C.w, C.sc, nullptr);
-        else
-            k_predict<R, sizeof(R) == 8 ? 3 : 4><<<grid_for(all, pblk), pblk, 0, s>>>(b, C.P, C.g, S, O, C.w, C.sc, nullptr);
+        else  // FP64: 3 blocks/SM (4 for the strict build, measured); FP32: 4
+            k_predict<R, (sizeof(R) == 8 && !GAM_STRICT_KERNELS) ? 3 : 4><<<grid_for(all, pblk), pblk, 0, s>>>(
+                b, C.P, C.g, S, O, C.w, C.sc, nullptr);
     });
     if (C.P.doMHD) {
         const Range mf[3] = {{0, b.Ni - 1, G, G + b.Njp, 0, b.Nk - 1},

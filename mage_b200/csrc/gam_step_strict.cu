@@ -2,6 +2,7 @@
 // operation is one IEEE-rounded +, -, *, / or sqrt in the reference's order,
 // so the result equals an IEEE-strict CPU evaluation of the same step.
 #define GAM_NS gam_strict
+#define GAM_STRICT_KERNELS 1
 #include "gam_step_impl.cuh"
 
 void gam_strict_step_f64(const Ctx<double>& C, int cur, cudaStream_t s) { gam_strict::launch_step<double>(C, cur, s); }

@@ -26,6 +26,15 @@
 #include "../../include/gamgpu.h"
 #include "gam_bcmap.cuh"
 
+// stage adjoints for a whole step (gam_adjoint.cu)
+int gam_update_adjoint_store(const gam_params* p, int32_t fp32, const void* const* in, const void* const* geo,
+                             const double* dpB0, double dt, const void* const* din, void* sU, void* sM,
+                             void* const* dst, void* stream);
+int gam_efield_adjoint_saved(const gam_params* p, int32_t fp32, const void* Dh, const void* abh, const void* bn,
+                             const void* VdV, const void* volume, const void* face, const void* edge, const void* Te,
+                             const void* Teb, const double* edgB0, double dt, void* AVf, const void* dE, void* dDh,
+                             void* dabh, void* dbn, void* dVdV, void* dAVf, void* stream);
+
 namespace gam_stepadj {
 
 // out[c][t] = in[c][src(t)] for the nc components of a field
@@ -303,9 +312,12 @@ extern "C" int gam_step_adj(const gam_params* p, int32_t fp32, const void* const
     const Work w = layout(b, fp32, work);
     const size_t es = fp32 ? 4 : 8;
     if (!saved) TRY(forward_stages(p, fp32, b, w, geo, bg, st, dt, odt, s));
-    // zero what the adjoint stages add into (dQW .. dBlim); sU, sM and aB are
-    // written before they are read, dnG, dnM and tM are written whole
-    if (cudaMemsetAsync(w.p[dQW], 0, (size_t)((char*)w.p[sU] - (char*)w.p[dQW]), s) != cudaSuccess) return GAM_ECUDA;
+    // zero what the adjoint stages add into (dQW .. dAVf, dBlim); the update
+    // stage stores dE, dgF and dmF whole, sU, sM and aB are written before
+    // they are read, dnG, dnM and tM are written whole
+    if (cudaMemsetAsync(w.p[dQW], 0, (size_t)((char*)w.p[dE] - (char*)w.p[dQW]), s) != cudaSuccess ||
+        cudaMemsetAsync(w.p[dBlim], 0, (size_t)((char*)w.p[sU] - (char*)w.p[dBlim]), s) != cudaSuccess)
+        return GAM_ECUDA;
     // adjoint of the state's field: B = bFlux2Fld(magFlux)
     if (cudaMemcpyAsync(w.p[tM], dnxt[1], 3 * b.n * es, cudaMemcpyDeviceToDevice, s) != cudaSuccess) return GAM_ECUDA;
     if (dnxt[2]) TRY(fp32 ? launch_bxyz_adj<float>(b, geo, dnxt[2], w.p[tM], s)
@@ -325,13 +337,13 @@ extern "C" int gam_step_adj(const gam_params* p, int32_t fp32, const void* const
     const void* g4[4] = {geo[0], geo[2], geo[3], geo[4]};
     const void* dup[2] = {w.p[dnG], w.p[dnM]};
     void* dsu[5] = {dst[0], dst[1], w.p[dE], w.p[dgF], w.p[dmF]};
-    TRY(gam_update_stage(p, fp32, in5, g4, bg ? bg[3] : nullptr, dt, nullptr, dup, w.p[sU], w.p[sM], dsu, s));
+    TRY(gam_update_adjoint_store(p, fp32, in5, g4, bg ? bg[3] : nullptr, dt, dup, w.p[sU], w.p[sM], dsu, s));
     TRY(gam_flux_adjoint(p, fp32, w.p[QW], w.p[Wn], w.p[QB], w.p[Blim], w.p[Bnf], geo[0], geo[1], geo[8],
                          bg ? bg[0] : nullptr, bg ? bg[1] : nullptr, w.p[dgF], w.p[dmF], w.p[dQW], w.p[dWn],
                          w.p[dQB], w.p[dBlim], w.p[dBnf], s));
-    TRY(gam_efield_adjoint(p, fp32, w.p[Dh], w.p[abh], w.p[bn], w.p[VdV], geo[0], geo[1], geo[5], geo[6], geo[7],
-                           bg ? bg[2] : nullptr, dt, w.p[AVf], w.p[dE], w.p[dDh], w.p[dabh], w.p[dbn], w.p[dVdV],
-                           w.p[dAVf], s));
+    TRY(gam_efield_adjoint_saved(p, fp32, w.p[Dh], w.p[abh], w.p[bn], w.p[VdV], geo[0], geo[1], geo[5], geo[6],
+                                 geo[7], bg ? bg[2] : nullptr, dt, w.p[AVf], w.p[dE], w.p[dDh], w.p[dabh], w.p[dbn],
+                                 w.p[dVdV], w.p[dAVf], s));
     TRY(fp32 ? launch_bxyz_adj<float>(b, geo, w.p[dBlim], dst[1], s)
              : launch_bxyz_adj<double>(b, geo, w.p[dBlim], dst[1], s));
     const void* g5[5] = {geo[0], geo[1], geo[2], geo[3], geo[4]};

@@ -39,7 +39,8 @@ import numpy as np
 import torch
 
 from mage_b200 import dipole, grids
-from mage_b200.diffstep import DiffParams, Grid, cell_c2p, cell_p2c, loss_and_grad, loss_and_grad_c, loss_b2, run, win, G
+from mage_b200.diffstep import (DiffParams, Grid, KinkCounter, cell_c2p, cell_p2c, count_kinks, loss_and_grad,  # noqa: E501
+                               loss_and_grad_c, loss_b2, run, win, G)
 from mage_b200.gamera import GameraGPU, GamParams
 from mage_b200.workloads import DIPOLE_BCS
 
@@ -137,14 +138,34 @@ def c4(N=(64, 64, 64), nsteps=20, sigma=1e-3, seed=2024):
             ce, _ = run(g, c, c, dt, nsteps)
             return float(loss_b2(g, ce))
 
-    # the limiter's kinks make a central difference approach the reverse mode
-    # only as eps -> 0 (each kink crossed inside +-eps adds a jump term; on
-    # 64^3 the difference is 1e-2 at eps 1e-9 and 1e-5 at 1e-11)
-    fd = {"reverse_mode": ad, "cuda": {}, "torch": {}}
-    for eps in (1e-9, 1e-10, 1e-11):
-        for name, f in (("cuda", cuda_loss), ("torch", torch_loss)):
-            d = (f(Gas64 + eps * vG, mf64 + eps * vF) - f(Gas64 - eps * vG, mf64 - eps * vF)) / (2 * eps)
-            fd[name][f"{eps:g}"] = {"central_difference": d, "rel_err": abs(d - ad) / abs(ad)}
+    # The limiter's kinks (the max/min and sign branches of PDM, the floors)
+    # make a central difference approach the reverse mode only as eps -> 0:
+    # every decision that switches between the +eps and the -eps run adds a
+    # jump term. The PyTorch restatement counts them (KinkCounter) on the same
+    # two runs of the PyTorch stages (the torch column). The differentiation
+    # form's stated check is a central difference at eps = 1e-6 in FP64.
+    fd = {"reverse_mode": ad, "direction": "seeded normal noise x |Gas| on the cells, normal noise on the face fluxes",
+          "cuda": {}, "torch": {}, "kinks_crossed": {}}
+    for eps in (1e-6, 1e-8, 1e-9, 1e-10, 1e-11):
+        d = (cuda_loss(Gas64 + eps * vG, mf64 + eps * vF) - cuda_loss(Gas64 - eps * vG, mf64 - eps * vF)) / (2 * eps)
+        fd["cuda"][f"{eps:g}"] = {"central_difference": d, "rel_err": abs(d - ad) / abs(ad)}
+        if eps not in (1e-6, 1e-8, 1e-10):
+            continue
+        k = KinkCounter()
+        count_kinks(k)
+        g.cuda_flux = False  # every stage as PyTorch expressions, whose branches the counter sees
+        try:
+            lp = torch_loss(Gas64 + eps * vG, mf64 + eps * vF)
+            k.compare()
+            lm = torch_loss(Gas64 - eps * vG, mf64 - eps * vF)
+        finally:
+            count_kinks(None)
+            g.cuda_flux = True
+        d = (lp - lm) / (2 * eps)
+        fd["torch"][f"{eps:g}"] = {"central_difference": d, "rel_err": abs(d - ad) / abs(ad)}
+        fd["kinks_crossed"][f"{eps:g}"] = {"switched": k.crossed, "of_decisions": k.decisions}
+        del k
+        torch.cuda.empty_cache()
     out["fd_check"] = fd
     out["forward_loss_cuda_vs_torch"] = [cuda_loss(Gas64, mf64), torch_loss(Gas64, mf64)]
     return out

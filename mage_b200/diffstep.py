@@ -53,20 +53,71 @@ class DiffParams:
     bc: tuple = (0, 0, 0, 0, 0, 0)
 
 
+# ----------------------------------------------------------------- kinks
+class KinkCounter:
+    """Counts the non-smooth decisions (max/min operands, signs, |x| and the
+    sqrt at 0, the limiter's branches) that differ between two evaluations of
+    the PyTorch step: "record" stores every decision of the first run in
+    order, "compare" walks the second run's decisions against them and counts
+    the elements that switched (kinks crossed between the two inputs)."""
+
+    def __init__(self):
+        self.mode, self.masks, self.pos, self.crossed, self.decisions = "record", [], 0, 0, 0
+
+    def see(self, m):
+        if self.mode == "record":
+            self.masks.append(m.detach().clone())
+            self.decisions += m.numel()
+        else:
+            self.crossed += int((self.masks[self.pos] != m.detach()).sum())
+            self.pos += 1
+
+    def compare(self):
+        self.mode, self.pos, self.crossed = "compare", 0, 0
+
+
+_KINKS: KinkCounter | None = None
+
+
+def count_kinks(counter: KinkCounter | None):
+    """Install (or remove, with None) the counter the branch helpers report to."""
+    global _KINKS
+    _KINKS = counter
+
+
+def _see(m):
+    if _KINKS is not None:
+        _KINKS.see(m)
+    return m
+
+
 # ----------------------------------------------------------------- helpers
 def rmax(a, b):
     """std::max: (a < b) ? b : a."""
-    return torch.where(a < b, b, a)
+    return torch.where(_see(a < b), b, a)
 
 
 def rmin(a, b):
     """std::min: (b < a) ? b : a."""
-    return torch.where(b < a, b, a)
+    return torch.where(_see(b < a), b, a)
+
+
+def kabs(x):
+    """|x|, its kink at 0 reported to the kink counter."""
+    _see(x < 0)
+    return torch.abs(x)
+
+
+def ksign(x):
+    """copysign(1, x), its switch at 0 reported to the kink counter."""
+    one = torch.ones_like(x)
+    _see(torch.signbit(x))
+    return torch.copysign(one, x)
 
 
 def safe_sqrt(x):
     """sqrt with a zero (sub)gradient at 0 instead of inf * 0."""
-    pos = x > 0
+    pos = _see(x > 0)
     return torch.where(pos, torch.sqrt(torch.where(pos, x, torch.ones_like(x))), torch.zeros_like(x))
 
 
@@ -109,13 +160,12 @@ def pdm_lr(pdmb, v, Qi):
     maxV, minV = rmax(v1, v2), rmin(v1, v2)
     vN = rmax(minV, rmin(Qi, maxV))
     dv0, dv1, dv2 = pdmb * (v1 - v0), pdmb * (v2 - v1), pdmb * (v3 - v2)
-    one = torch.ones_like(vN)
-    s0, s1, s2 = torch.copysign(one, dv0), torch.copysign(one, dv1), torch.copysign(one, dv2)
+    s0, s1, s2 = ksign(dv0), ksign(dv1), ksign(dv2)
     q0, q1 = torch.abs(s0 + s1), torch.abs(s1 + s2)
     dvL, dvR = vN - v1, v2 - vN
     zero = torch.zeros_like(vN)
-    Ql = vN - s1 * rmax(zero, torch.abs(dvL) - q0 * torch.abs(dv0))
-    Qr = vN + s1 * rmax(zero, torch.abs(dvR) - q1 * torch.abs(dv2))
+    Ql = vN - s1 * rmax(zero, kabs(dvL) - q0 * kabs(dv0))
+    Qr = vN + s1 * rmax(zero, kabs(dvR) - q1 * kabs(dv2))
     return Ql, Qr
 
 
@@ -124,11 +174,10 @@ def pdm1(pdmb, q0, q1, q2, qI):
     maxQ, minQ = rmax(q1, q2), rmin(q1, q2)
     qN = rmax(minQ, rmin(qI, maxQ))
     dq0, dq1 = pdmb * (q1 - q0), pdmb * (q2 - q1)
-    one = torch.ones_like(qN)
-    s0, s1 = torch.copysign(one, dq0), torch.copysign(one, dq1)
+    s0, s1 = ksign(dq0), ksign(dq1)
     s01 = torch.abs(s0 + s1)
     dqL = qN - q1
-    return qN - s1 * rmax(torch.zeros_like(qN), torch.abs(dqL) - s01 * torch.abs(dq0))
+    return qN - s1 * rmax(torch.zeros_like(qN), kabs(dqL) - s01 * kabs(dq0))
 
 
 def lrs_from_qdv(P: DiffParams, qdv, nq, Vi):
@@ -993,7 +1042,7 @@ def _iside_bcs(g: Grid, Gas, mf, B):
         nH = [g.Tf[q][cellsJK + (ip + 1,)] for q in range(3)]
         V = [gW_in[1], gW_in[2], gW_in[3]]
         dn = V[0] * nH[0] + V[1] * nH[1] + V[2] * nH[2]
-        fix = dn < Cx  # MinMach = 1
+        fix = _see(dn < Cx)  # MinMach = 1
         V = [torch.where(fix, V[x] - dn * nH[x] + Cx * nH[x], V[x]) for x in range(3)]
         fin = [mf[0, :, :, ip + 1].clone(), mf[1, :, :, ip].clone(), mf[2, :, :, ip].clone()]
         Gas = Gas.clone()

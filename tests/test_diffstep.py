@@ -4,14 +4,18 @@
   <= 1e-15 relative (only erfc/exp implementations differ);
 * reverse mode: the checkpointed gradient equals the single-segment one
   exactly, and agrees with a central finite difference of the loss along a
-  random direction (eps = 1e-8, FP64) to <= 1e-6 relative.
+  random direction (eps = 1e-8, FP64) to <= 1e-6 relative;
+* the kink counter: the limiter decisions that switch between the +eps and
+  -eps runs fall with eps (about 3e4, 4e2 and 0 at eps = 1e-5, 1e-7, 1e-9 on
+  this case), and once none switches the central difference meets the
+  reverse mode to 1e-8.
 """
 import numpy as np
 import pytest
 import torch
 
 from mage_b200 import grids
-from mage_b200.diffstep import DiffParams, Grid, loss_and_grad, loss_b2, run
+from mage_b200.diffstep import DiffParams, Grid, KinkCounter, count_kinks, loss_and_grad, loss_b2, run
 from oracle.oracle import Oracle, OracleParams
 from tests.helpers import GEO_FROM_ORACLE
 
@@ -69,6 +73,25 @@ def test_gradient_checkpointing_and_finite_differences(oracle_built):
     fd = (Lf(Gas0 + eps * vG, mf0 + eps * vF) - Lf(Gas0 - eps * vG, mf0 - eps * vF)) / (2 * eps)
     ad = float((gG * vG).sum() + (gF * vF).sum())
     assert abs(fd - ad) <= 1e-6 * abs(ad), (fd, ad)
+    # kinks crossed inside +-eps, and the difference without any
+    crossed, errs = [], []
+    for eps in (1e-5, 1e-7, 1e-9):  # below ~1e-10 the difference's FP64 cancellation dominates
+        k = KinkCounter()
+        count_kinks(k)
+        try:
+            lp = Lf(Gas0 + eps * vG, mf0 + eps * vF)
+            k.compare()
+            lm = Lf(Gas0 - eps * vG, mf0 - eps * vF)
+        finally:
+            count_kinks(None)
+        crossed.append(k.crossed)
+        errs.append(abs((lp - lm) / (2 * eps) - ad) / abs(ad))
+        assert k.decisions > 10**6
+    assert crossed[0] > crossed[1] > crossed[2], crossed
+    assert crossed[-1] == 0, crossed
+    for c, e in zip(crossed, errs):
+        if c == 0:
+            assert e <= 1e-8, (crossed, errs)
 
 
 def test_per_step_checkpointing_matches(oracle_built):
