@@ -133,11 +133,15 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
-# Lane-instructions per active cell-update of the FP64 step: ncu sum of
-# smsp__inst_executed x 32 over one 96^3 step (profiles/
-# blast96_fp64_step_kernels_full.md: 14,776), scaled to 192^3 by the ratio of
-# ghosted to active cells ((200/192)^3 / (104/96)^3).
-INST_PER_CELL_F64 = 14776 * (200 / 192) ** 3 / (104 / 96) ** 3
+# Instructions per active cell-update of the FP64 drop-in step, from the
+# single-kernel ncu captures of the 96^3 step (profiles/
+# blast96_fp64_strict_kernels.md; the I-face flux kernel counted for all three
+# directions), scaled to 192^3 by the ratio of ghosted to active cells
+# ((200/192)^3 / (104/96)^3): warp instructions x 32 (issue slots) and the FP64
+# arithmetic instructions of active threads (DADD + DMUL + DFMA).
+_SCALE_96_TO_192 = (200 / 192) ** 3 / (104 / 96) ** 3
+INST_PER_CELL_F64 = (3 * 544 + 2208 + 3 * 3182 + 1759 + 3 * 1168) * _SCALE_96_TO_192
+FP64_OPS_PER_CELL = (3 * 110 + 545 + 3 * 1027 + 334 + 3 * 322) * _SCALE_96_TO_192
 
 
 def committed_traffic(workload, dtype):
@@ -484,7 +488,7 @@ def main():
     peak, peak_kind = measured_peak()
     bpc = BYTES_PER_CELL_B0 if w["problem"] == "dipole" else BYTES_PER_CELL
     achieved = per_gpu * bpc["f64"] / 1e9
-    traffic = committed_traffic(args.workload, "f64")
+    traffic = committed_traffic(args.workload, "f64" if args.strict else "f64_fma")
     # per-kernel device times of one step (CUDA events, each kernel repeated on
     # the current state; gam_profile_step leaves the state unchanged)
     kms = {k: v for k, v in g.profile_step(3).items() if v > 0}
@@ -518,8 +522,13 @@ def main():
                             "peak_lane_inst_per_s": 148 * 4 * 32 * clocks["sm_mhz"] * 1e6 if clocks.get("sm_mhz") else None,
                             "frac": (per_gpu * INST_PER_CELL_F64 / (148 * 4 * 32 * clocks["sm_mhz"] * 1e6))
                             if clocks.get("sm_mhz") else None,
-                            "note": "148 SMs x 4 schedulers x 1 warp-instruction (32 lanes) per clock at the median "
-                                    "SM clock sampled in the timed region"} if w["problem"] == "bw" else None,
+                            "fp64_ops_per_cell_update": FP64_OPS_PER_CELL,
+                            "fp64_pipe_frac": (per_gpu * FP64_OPS_PER_CELL / (148 * 64 * clocks["sm_mhz"] * 1e6))
+                            if clocks.get("sm_mhz") else None,
+                            "note": "issue: 148 SMs x 4 schedulers x 1 warp-instruction (32 lanes) per clock; FP64 "
+                                    "pipe: 148 SMs x 64 FP64 lanes per clock (a DFMA counts once); both at the median "
+                                    "SM clock sampled in the timed region; instruction counts of the drop-in (strict) "
+                                    "kernels"} if (w["problem"] == "bw" and args.strict) else None,
             "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "steps": args.e2e_steps,
                     "what": "per step: gam_upload_state of State%Gas and State%magFlux from pinned host memory "
