@@ -37,7 +37,7 @@ template <class A> __device__ __forceinline__ A sgnz(A x) { return x > (A)0 ? (A
 // Ql, Qr to the 8-point operand stencil and the 4-point limiter stencil
 template <class R, class A>
 __device__ void lrs_adj(R pdmb, const R* qdv, const R* v, R Vi, A rVi, A aL, A aR, A* aq,
-                        A* av) {
+                        A* av, A* a_scale = nullptr) {
     R s = (R)0;
 #pragma unroll
     for (int n = 0; n < 8; n++) s += Rc<R>(w8(n)) * qdv[n];
@@ -71,6 +71,7 @@ __device__ void lrs_adj(R pdmb, const R* qdv, const R* v, R Vi, A rVi, A aL, A a
     if (v2 < v1) a2 += a_minV; else a1 += a_minV;
     if (v1 < v2) a2 += a_maxV; else a1 += a_maxV;
     const A a_s = a_Qi * rVi;
+    if (a_scale) *a_scale = a_s;  // aq[n] = w8(n) * a_s
 #pragma unroll
     for (int n = 0; n < 8; n++) aq[n] = (A)w8(n) * a_s;
     av[0] = a0; av[1] = a1; av[2] = a2; av[3] = a3;
@@ -221,7 +222,7 @@ template <class R, int D>
 __global__ void __launch_bounds__(128, (sizeof(R) == 8 ? 4 : 5)) k_stress_adj(GamBox b, DevParams<R> P, Geo<R> g, const R* __restrict__ Blim,
                                                     Work<R> w, Range r, const R* __restrict__ dgF,
                                                     const R* __restrict__ dmF, R* dQW, R* dWn, R* dQB, R* dBlim,
-                                                    R* dBnf) {
+                                                    R* dBnf, R* __restrict__ rs) {
     int ii, jj, kk;
     if (!thread_ijk(r, ii, jj, kk)) return;
     const long fs = b.fs;
@@ -293,7 +294,13 @@ __global__ void __launch_bounds__(128, (sizeof(R) == 8 ? 4 : 5)) k_stress_adj(Ga
         R qW[8], nW[4];
         for (int n = 0; n < 8; n++) qW[n] = w.QW[v * fs + c + (n - 4) * s];
         for (int m = 0; m < 4; m++) nW[m] = w.Wn[v * fs + c + (m - 2) * s];
-        lrs_adj(P.pdmb, qW, nW, Vi, rVi, aWL[v], aWR[v], aq, av);
+        A as;
+        lrs_adj(P.pdmb, qW, nW, Vi, rVi, aWL[v], aWR[v], aq, av, &as);
+        if (rs) {  // per face: the stencil weight scale and the 4 limiter adjoints
+            rs[(5 * v) * fs + c] = (R)as;
+            for (int m = 0; m < 4; m++) rs[(5 * v + 1 + m) * fs + c] = (R)av[m];
+            continue;
+        }
         for (int n = 0; n < 8; n++) atomicAdd(&dQW[v * fs + c + (n - 4) * s], (R)aq[n]);
         for (int m = 0; m < 4; m++) atomicAdd(&dWn[v * fs + c + (m - 2) * s], (R)av[m]);
     }
@@ -302,10 +309,97 @@ __global__ void __launch_bounds__(128, (sizeof(R) == 8 ? 4 : 5)) k_stress_adj(Ga
             R qB[8], nB[4];
             for (int n = 0; n < 8; n++) qB[n] = w.QB[x * fs + c + (n - 4) * s];
             for (int m = 0; m < 4; m++) nB[m] = Blim[x * fs + c + (m - 2) * s];
-            lrs_adj(P.pdmb, qB, nB, Vi, rVi, aBL[x], aBR[x], aq, av);
+            A as;
+            lrs_adj(P.pdmb, qB, nB, Vi, rVi, aBL[x], aBR[x], aq, av, &as);
+            if (rs) {
+                rs[(5 * (5 + x)) * fs + c] = (R)as;
+                for (int m = 0; m < 4; m++) rs[(5 * (5 + x) + 1 + m) * fs + c] = (R)av[m];
+                continue;
+            }
             for (int n = 0; n < 8; n++) atomicAdd(&dQB[x * fs + c + (n - 4) * s], (R)aq[n]);
             for (int m = 0; m < 4; m++) atomicAdd(&dBlim[x * fs + c + (m - 2) * s], (R)av[m]);
         }
+}
+
+
+// The stencil adjoints of the faces of all three directions gathered per
+// cell, in a fixed order (deterministic, no atomics), and stored: cell c is
+// point n of the 8-point operand stencil of face c + (4 - n) e_D (adjoint
+// w8(n) * scale of that face) and point m of the 4-point limiter stencil of
+// face c + (2 - m) e_D; faces outside the range r[D] carry nothing. rs holds
+// per direction D (40 components from 40 D) per face and variable (0-4
+// QW/Wn, 5-7 QB/Blim) the scale and the 4 limiter adjoints. The sums run
+// over n (m) per direction, then I, J, K, as three passes adding into a
+// zeroed array would.
+template <class R>
+__global__ void __launch_bounds__(256) k_stress_adj_gather3(GamBox b, Range r0, Range r1, Range r2,
+                                                            const R* __restrict__ rs, int nvar, R* __restrict__ dQW,
+                                                            R* __restrict__ dWn, R* __restrict__ dQB,
+                                                            R* __restrict__ dBlim) {
+    using A = R;
+    int ii, jj, kk;
+    const Range all{0, b.Ni - 1, 0, b.Nj - 1, 0, b.Nk - 1};
+    if (!thread_ijk(all, ii, jj, kk)) return;
+    const int p[3] = {ii, jj, kk};
+    const Range rr[3] = {r0, r1, r2};
+    bool line[3];
+#pragma unroll
+    for (int D = 0; D < 3; D++) {
+        const int lo[3] = {rr[D].i0, rr[D].j0, rr[D].k0}, hi[3] = {rr[D].i1, rr[D].j1, rr[D].k1};
+        bool ok = p[D] >= lo[D] - 4 && p[D] <= hi[D] + 3;
+        for (int a = 0; a < 3; a++)
+            if (a != D && (p[a] < lo[a] || p[a] > hi[a])) ok = false;
+        line[D] = ok;
+    }
+    const long fs = b.fs;
+    const long c = lidx(b, ii, jj, kk);
+    for (int v = 0; v < nvar; v++) {
+        A qs[3], ls[3];
+#pragma unroll
+        for (int D = 0; D < 3; D++) {
+            const long s = D == 0 ? 1L : (D == 1 ? (long)b.sx : b.sk);
+            const int lo = D == 0 ? rr[D].i0 : (D == 1 ? rr[D].j0 : rr[D].k0);
+            const int hi = D == 0 ? rr[D].i1 : (D == 1 ? rr[D].j1 : rr[D].k1);
+            const R* q0 = rs + (40 * D + 5 * v) * fs + c;
+            A q = (A)0, l = (A)0;
+            if (line[D] && p[D] - 3 >= lo && p[D] + 4 <= hi) {
+                // every face of both stencils in range: loads first, then the sums
+                R x[8], y[4];
+#pragma unroll
+                for (int n = 0; n < 8; n++) x[n] = q0[(4 - n) * s];
+#pragma unroll
+                for (int m = 0; m < 4; m++) y[m] = q0[(1 + m) * fs + (2 - m) * s];
+#pragma unroll
+                for (int n = 0; n < 8; n++) q += (A)w8(n) * (A)x[n];
+#pragma unroll
+                for (int m = 0; m < 4; m++) l += (A)y[m];
+            } else if (line[D]) {
+#pragma unroll
+                for (int n = 0; n < 8; n++) {
+                    const int f = p[D] + 4 - n;
+                    if (f >= lo && f <= hi) q += (A)w8(n) * (A)q0[(4 - n) * s];
+                }
+#pragma unroll
+                for (int m = 0; m < 4; m++) {
+                    const int f = p[D] + 2 - m;
+                    if (f >= lo && f <= hi) l += (A)q0[(1 + m) * fs + (2 - m) * s];
+                }
+            }
+            qs[D] = q;
+            ls[D] = l;
+        }
+        A q = (A)0, l = (A)0;
+#pragma unroll
+        for (int D = 0; D < 3; D++)
+            if (line[D]) {
+                q += qs[D];
+                l += ls[D];
+            }
+        R* dq = v < 5 ? dQW + v * fs : dQB + (v - 5) * fs;
+        R* dl = v < 5 ? dWn + v * fs : dBlim + (v - 5) * fs;
+        dq[c] = (R)q;
+        dl[c] = (R)l;
+    }
 }
 
 
@@ -313,7 +407,7 @@ __global__ void __launch_bounds__(128, (sizeof(R) == 8 ? 4 : 5)) k_stress_adj(Ga
 // bL*Vi, bR*Vi -> the abh (8) and bn (4) stencils
 template <class R, class A>
 __device__ void edge_lrs_adj(const GamBox& b, const DevParams<R>& P, const Geo<R>& g, const Work<R>& w, long c, int a,
-                             int bd, A aBL, A aBR, R* dabh, R* dbn) {
+                             int bd, A aBL, A aBR, R* dabh, R* dbn, R* es = nullptr) {
     const long fs = b.fs;
     const long s = dstride(b, bd);
     R qdv[8], area[8], nmag[4];
@@ -323,18 +417,27 @@ __device__ void edge_lrs_adj(const GamBox& b, const DevParams<R>& P, const Geo<R
     }
     for (int m = 0; m < 4; m++) nmag[m] = w.bn[a * fs + c + (m - 2) * s];
     const R Vi = central8(area);
-    A aq[8], av[4];
-    lrs_adj<R, A>(P.pdmb, qdv, nmag, Vi, (A)1.0 / (A)Vi, aBL * (A)Vi, aBR * (A)Vi, aq, av);
+    A aq[8], av[4], as;
+    lrs_adj<R, A>(P.pdmb, qdv, nmag, Vi, (A)1.0 / (A)Vi, aBL * (A)Vi, aBR * (A)Vi, aq, av, &as);
+    if (es) {  // per edge: the stencil weight scale and the 4 limiter adjoints (es[0..4 fs])
+        es[c] = (R)as;
+        for (int m = 0; m < 4; m++) es[(1 + m) * fs + c] = (R)av[m];
+        return;
+    }
     for (int n = 0; n < 8; n++) atomicAdd(&dabh[a * fs + c + (n - 4) * s], (R)aq[n]);
     for (int m = 0; m < 4; m++) atomicAdd(&dbn[a * fs + c + (m - 2) * s], (R)av[m]);
 }
 
 // Adjoint of the edge EMF of direction eD (k_vxb) over the range r: dE ->
-// dDh, dabh, dbn, dAVf (the AVf of this eD, 3 components, caller-zeroed)
+// dDh, dabh, dbn, dAVf (the AVf of this eD, 3 components, caller-zeroed) by
+// atomics, or, with es, the edge's own adjoints stored per edge (14
+// components: 0-4 and 5-9 the scale and limiter adjoints of the EdgeLRs of
+// dT1 and dT2 faces, 10-12 the velocity adjoint aVC, 13 the corner density's)
+// for a gather in a fixed order
 template <class R>
 __global__ void __launch_bounds__(128, 6) k_vxb_adj(GamBox b, DevParams<R> P, Geo<R> g, Work<R> w, int eD, Range r,
                                                  double dt, const R* __restrict__ dE, R* dDh, R* dabh, R* dbn,
-                                                 R* dAVf) {
+                                                 R* dAVf, R* __restrict__ es) {
     int ii, jj, kk;
     if (!thread_ijk(r, ii, jj, kk)) return;
     int dT1, dT2;
@@ -413,15 +516,208 @@ __global__ void __launch_bounds__(128, 6) k_vxb_adj(GamBox b, DevParams<R> P, Ge
     const A rA1 = (A)1.0 / (A)fA1, rA2 = (A)1.0 / (A)fA2;
     const A aT1R = (a_db1 + a_bT1 * (A)0.5) * rA1, aT1L = (-a_db1 + a_bT1 * (A)0.5) * rA1;
     const A aT2R = (a_db2 + a_bT2 * (A)0.5) * rA2, aT2L = (-a_db2 + a_bT2 * (A)0.5) * rA2;
-    edge_lrs_adj<R, A>(b, P, g, w, c, dT1, dT2, aT1L, aT1R, dabh, dbn);
-    edge_lrs_adj<R, A>(b, P, g, w, c, dT2, dT1, aT2L, aT2R, dabh, dbn);
+    edge_lrs_adj<R, A>(b, P, g, w, c, dT1, dT2, aT1L, aT1R, dabh, dbn, es);
+    edge_lrs_adj<R, A>(b, P, g, w, c, dT2, dT1, aT2L, aT2R, dabh, dbn, es ? es + 5 * fs : nullptr);
     const A rdA = (A)1.0 / (A)dA;
     for (int x = 0; x < 3; x++) {
         const A aVC = (a_v1t * T1[x] + a_v2t * T2[x]) * rdA;
+        if (es) {
+            es[(10 + x) * fs + c] = (R)aVC;
+            continue;
+        }
         for (int n = 0; n < 8; n++) atomicAdd(&dAVf[x * fs + c + (n - 4) * s2v], (R)((A)w8(n) * aVC));
+    }
+    if (es) {
+        es[13 * fs + c] = (R)a_Dc;
+        return;
     }
     const long cc[4] = {c, c - s1, c - s2, c - s1 - s2};
     for (int n = 0; n < 4; n++) atomicAdd(&dDh[cc[n]], (R)((A)0.25 * a_Dc));
+}
+
+struct Range3 {
+    Range r[3];
+};
+
+// The adjoints the edges of the three directions hold in es (k_vxb_adj; 14
+// components from es + 14 eD fs), gathered per position in a fixed order
+// (deterministic, no atomics) and stored: for the faces of each direction fa
+// their operand and limiter stencil adjoints (dabh, dbn) from the edges
+// whose EdgeLRs run over them, for the cells the corner densities' dDh and,
+// per edge direction, the velocity stencil's dAVf times face area /
+// interpolated volume of Mom2Face (aS + 3 eD fs; zero outside the Mom2Face
+// range mf[eD]). Edges outside their range ed[eD] carry nothing. The sums
+// run over the stencil, then eD = I, J, K, as three passes adding into a
+// zeroed array would.
+template <class R>
+__global__ void __launch_bounds__(256) k_vxb_adj_gather3(GamBox b, Geo<R> g, Range3 ed, Range3 mf,
+                                                         const R* __restrict__ es, R* __restrict__ dDh,
+                                                         R* __restrict__ dabh, R* __restrict__ dbn,
+                                                         R* __restrict__ aS) {
+    using A = R;
+    int ii, jj, kk;
+    const Range all{0, b.Ni, 0, b.Nj, 0, b.Nk};
+    if (!thread_ijk(all, ii, jj, kk)) return;
+    const long fs = b.fs;
+    const long c = lidx(b, ii, jj, kk);
+    const int p[3] = {ii, jj, kk};
+    A fq[3] = {(A)0, (A)0, (A)0}, fl[3] = {(A)0, (A)0, (A)0};
+    const bool isCell = ii < b.Ni && jj < b.Nj && kk < b.Nk;
+    A d = (A)0;
+#pragma unroll
+    for (int eD = 0; eD < 3; eD++) {
+        const Range r = ed.r[eD];
+        const int lo[3] = {r.i0, r.j0, r.k0}, hi[3] = {r.i1, r.j1, r.k1};
+        // is the edge at p + k e_dd inside the range?
+        auto in_r = [&](int dd, int k) {
+            bool ok = true;
+#pragma unroll
+            for (int a = 0; a < 3; a++) {
+                const int q = p[a] + (a == dd ? k : 0);
+                ok = ok && q >= lo[a] && q <= hi[a];
+            }
+            return ok;
+        };
+        int dT1, dT2;
+        edge_dirs(eD, dT1, dT2);
+        const R* e = es + 14L * eD * fs + c;
+        // every edge within -3..4 of p along dT1 and along dT2 in range
+        const bool full = in_r(dT1, -3) && in_r(dT1, 4) && in_r(dT2, -3) && in_r(dT2, 4);
+#pragma unroll
+        for (int side = 0; side < 2; side++) {
+            const int fa = side == 0 ? dT1 : dT2, bd = side == 0 ? dT2 : dT1;
+            const R* e0 = e + (5 * side) * fs;
+            const long sb = dstride(b, bd);
+            A q = (A)0, l = (A)0;
+            bool any = false;
+            if (full) {
+                R x[8], y[4];
+#pragma unroll
+                for (int n = 0; n < 8; n++) x[n] = e0[(4 - n) * sb];
+#pragma unroll
+                for (int m = 0; m < 4; m++) y[m] = e0[(1 + m) * fs + (2 - m) * sb];
+#pragma unroll
+                for (int n = 0; n < 8; n++) q += (A)w8(n) * (A)x[n];
+#pragma unroll
+                for (int m = 0; m < 4; m++) l += (A)y[m];
+                any = true;
+            } else {
+#pragma unroll
+                for (int n = 0; n < 8; n++)
+                    if (in_r(bd, 4 - n)) {
+                        q += (A)w8(n) * (A)e0[(4 - n) * sb];
+                        any = true;
+                    }
+#pragma unroll
+                for (int m = 0; m < 4; m++)
+                    if (in_r(bd, 2 - m)) {
+                        l += (A)e0[(1 + m) * fs + (2 - m) * sb];
+                        any = true;
+                    }
+            }
+            if (any) {
+                fq[fa] += q;
+                fl[fa] += l;
+            }
+        }
+        if (!isCell) continue;
+        // the velocity stencil along dT2, scaled as Mom2Face's adjoint
+        const Range rm = mf.r[eD];
+        const bool inm = ii >= rm.i0 && ii <= rm.i1 && jj >= rm.j0 && jj <= rm.j1 && kk >= rm.k0 && kk <= rm.k1;
+        const long s2 = dstride(b, dT2);
+        double AdV = 0.0;
+        if (inm) {
+            const long s1 = dstride(b, dT1);
+            R vol[8];
+            for (int n = 0; n < 8; n++) vol[n] = g.vol[c + (n - 4) * s1];
+            const R dV = rmax(central8(vol), (R)TINY);
+            AdV = (double)g.face[dT1 * fs + c] / (double)dV;
+        }
+#pragma unroll
+        for (int x = 0; x < 3; x++) {
+            A v = (A)0;
+            if (inm && full) {
+                R y[8];
+#pragma unroll
+                for (int n = 0; n < 8; n++) y[n] = e[(10 + x) * fs + (4 - n) * s2];
+#pragma unroll
+                for (int n = 0; n < 8; n++) v += (A)w8(n) * (A)y[n];
+            } else if (inm) {
+#pragma unroll
+                for (int n = 0; n < 8; n++)
+                    if (in_r(dT2, 4 - n)) v += (A)w8(n) * (A)e[(10 + x) * fs + (4 - n) * s2];
+            }
+            aS[(3 * eD + x) * fs + c] = inm ? (R)((double)(R)v * AdV) : (R)0;
+        }
+        // the 4 corners of GetCornerD: edges c, c + s1, c + s2, c + s1 + s2
+        const int e1 = eD == 0 ? 1 : 0, e2 = eD == 2 ? 1 : 2;
+        const long t1 = dstride(b, e1), t2 = dstride(b, e2);
+        A dd = (A)0;
+        bool anyd = false;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int o1 = q & 1, o2 = q >> 1;
+            bool ok = true;
+#pragma unroll
+            for (int a = 0; a < 3; a++) {
+                const int v = p[a] + (a == e1 ? o1 : 0) + (a == e2 ? o2 : 0);
+                ok = ok && v >= lo[a] && v <= hi[a];
+            }
+            if (ok) {
+                dd += (A)0.25 * (A)e[13 * fs + o1 * t1 + o2 * t2];
+                anyd = true;
+            }
+        }
+        if (anyd) d += dd;
+    }
+#pragma unroll
+    for (int fa = 0; fa < 3; fa++) {
+        dabh[fa * fs + c] = (R)fq[fa];
+        dbn[fa * fs + c] = (R)fl[fa];
+    }
+    if (isCell) dDh[c] = (R)d;
+}
+
+// Mom2Face's adjoint gathered per cell: dVdV = sum over eD of the 8-point
+// stencil along dT1 of the scaled dAVf (aS + 3 eD fs) over the faces of the
+// Mom2Face range mf[eD], in FP64 per eD, then eD = I, J, K; stored.
+template <class R>
+__global__ void __launch_bounds__(256) k_m2f_adj_gather3(GamBox b, Range3 mf, const R* __restrict__ aS,
+                                                         R* __restrict__ dVdV) {
+    int ii, jj, kk;
+    const Range all{0, b.Ni - 1, 0, b.Nj - 1, 0, b.Nk - 1};
+    if (!thread_ijk(all, ii, jj, kk)) return;
+    const long fs = b.fs, c = lidx(b, ii, jj, kk);
+    const int p[3] = {ii, jj, kk};
+    R out[3] = {(R)0, (R)0, (R)0};
+#pragma unroll
+    for (int eD = 0; eD < 3; eD++) {
+        int dT1, dT2;
+        edge_dirs(eD, dT1, dT2);
+        const Range r = mf.r[eD];
+        const int lo[3] = {r.i0, r.j0, r.k0}, hi[3] = {r.i1, r.j1, r.k1};
+        bool line = true;
+#pragma unroll
+        for (int a = 0; a < 3; a++)
+            if (a != dT1 && (p[a] < lo[a] || p[a] > hi[a])) line = false;
+        if (!line) continue;
+        const long s = dstride(b, dT1);
+        const R* a0 = aS + 3L * eD * fs + c;
+        double acc[3] = {0.0, 0.0, 0.0};
+        bool any = false;
+#pragma unroll
+        for (int n = 0; n < 8; n++) {
+            const int f = p[dT1] + 4 - n;
+            if (f >= lo[dT1] && f <= hi[dT1]) {
+                any = true;
+#pragma unroll
+                for (int x = 0; x < 3; x++) acc[x] += w8(n) * (double)a0[x * fs + (4 - n) * s];
+            }
+        }
+        if (any)
+            for (int x = 0; x < 3; x++) out[x] += (R)acc[x];
+    }
+    for (int x = 0; x < 3; x++) dVdV[x * fs + c] = out[x];
 }
 
 // Adjoint of Mom2Face for edge direction eD over the range r: dAVf -> dVdV
@@ -801,7 +1097,7 @@ template <class R>
 int flux_call(const gam_params* p, const void* QW, const void* Wn, const void* QB, const void* Blim, const void* Bnf,
               const void* vol, const void* face, const void* Tf, const double* fcB0, const double* bFlux0, void* gF,
               void* mF, const void* dgF, const void* dmF, void* dQW, void* dWn, void* dQB, void* dBlim, void* dBnf,
-              cudaStream_t s) {
+              cudaStream_t s, void* rscratch = nullptr) {
     using namespace gam_adj;
     const GamBox b = torch_box(p->Nip, p->Njp, p->Nkp);
     const DevParams<R> P = dev_params<R>(p);
@@ -831,12 +1127,24 @@ int flux_call(const gam_params* p, const void* QW, const void* Wn, const void* Q
     } else {
         const R* a = (const R*)dgF;
         const R* m = (const R*)dmF;
+        // rs null: scatter with atomics; else each direction stores per face
+        // (40 components from rs + 40 D fs), then one gather per cell stores
+        // dQW, dWn, dQB and dBlim
+        R* rs = (R*)rscratch;
+        const long fs40 = 40L * b.fs;
         k_stress_adj<R, 0><<<grid(fr[0]), blk, 0, s>>>(b, P, g, Bl, w, fr[0], a, m, (R*)dQW, (R*)dWn, (R*)dQB,
-                                                        (R*)dBlim, (R*)dBnf);
+                                                        (R*)dBlim, (R*)dBnf, rs);
         k_stress_adj<R, 1><<<grid(fr[1]), blk, 0, s>>>(b, P, g, Bl, w, fr[1], a, m, (R*)dQW, (R*)dWn, (R*)dQB,
-                                                        (R*)dBlim, (R*)dBnf);
+                                                        (R*)dBlim, (R*)dBnf, rs ? rs + fs40 : nullptr);
         k_stress_adj<R, 2><<<grid(fr[2]), blk, 0, s>>>(b, P, g, Bl, w, fr[2], a, m, (R*)dQW, (R*)dWn, (R*)dQB,
-                                                        (R*)dBlim, (R*)dBnf);
+                                                        (R*)dBlim, (R*)dBnf, rs ? rs + 2 * fs40 : nullptr);
+        if (rs) {
+            const dim3 gblk(32, 8, 1);
+            const dim3 ggrid((unsigned)((b.Ni + gblk.x - 1) / gblk.x), (unsigned)((b.Nj + gblk.y - 1) / gblk.y),
+                             (unsigned)b.Nk);
+            k_stress_adj_gather3<R><<<ggrid, gblk, 0, s>>>(b, fr[0], fr[1], fr[2], rs, p->doMHD ? 8 : 5, (R*)dQW,
+                                                           (R*)dWn, (R*)dQB, (R*)dBlim);
+        }
     }
     return cudaGetLastError() == cudaSuccess ? GAM_OK : GAM_ECUDA;
 }
@@ -888,7 +1196,7 @@ template <class R>
 int efield_call(const gam_params* p, const void* Dh, const void* abh, const void* bn, const void* VdV, const void* vol,
                 const void* face, const void* edge, const void* Te, const void* Teb, const double* edgB0, double dt,
                 void* AVf, void* E, const void* dE, void* dDh, void* dabh, void* dbn, void* dVdV, void* dAVf,
-                cudaStream_t s, bool avf_saved = false) {
+                cudaStream_t s, bool avf_saved = false, void* escratch = nullptr) {
     using namespace gam_adj;
     const GamBox b = torch_box(p->Nip, p->Njp, p->Nkp);
     const DevParams<R> P = dev_params<R>(p);
@@ -919,10 +1227,23 @@ int efield_call(const gam_params* p, const void* Dh, const void* abh, const void
         if (!(dE && avf_saved)) k_mom2face<R><<<grid(mf[eD]), blk, 0, s>>>(b, P, g, w, eD, mf[eD], sc);
         if (!dE) {
             k_vxb<R><<<grid(ed[eD]), blk, 0, s>>>(b, P, g, w, eD, ed[eD], sc);
+        } else if (escratch) {
+            // deterministic: the edges store their adjoints (14 components
+            // from escratch + 14 eD fs), gathered per position after the third
+            k_vxb_adj<R><<<grid(ed[eD]), blk, 0, s>>>(b, P, g, w, eD, ed[eD], dt, (const R*)dE, (R*)dDh, (R*)dabh,
+                                                       (R*)dbn, (R*)dAVf, (R*)escratch + 14L * eD * b.fs);
+            if (eD == 2) {
+                R* es = (R*)escratch;
+                R* aS = es + 42L * b.fs;  // the scaled dAVf of the three edge directions
+                const Range allF{0, b.Ni, 0, b.Nj, 0, b.Nk}, allC{0, b.Ni - 1, 0, b.Nj - 1, 0, b.Nk - 1};
+                const Range3 ed3{{ed[0], ed[1], ed[2]}}, mf3{{mf[0], mf[1], mf[2]}};
+                k_vxb_adj_gather3<R><<<grid(allF), blk, 0, s>>>(b, g, ed3, mf3, es, (R*)dDh, (R*)dabh, (R*)dbn, aS);
+                k_m2f_adj_gather3<R><<<grid(allC), blk, 0, s>>>(b, mf3, aS, (R*)dVdV);
+            }
         } else {
             if (cudaMemsetAsync(dAVf, 0, 3 * b.fs * sizeof(R), s) != cudaSuccess) return GAM_ECUDA;
             k_vxb_adj<R><<<grid(ed[eD]), blk, 0, s>>>(b, P, g, w, eD, ed[eD], dt, (const R*)dE, (R*)dDh, (R*)dabh,
-                                                       (R*)dbn, (R*)dAVf);
+                                                       (R*)dbn, (R*)dAVf, nullptr);
             k_m2f_adj<R><<<grid(mf[eD]), blk, 0, s>>>(b, g, eD, mf[eD], (const R*)dAVf, (R*)dVdV);
         }
     }
@@ -1077,8 +1398,12 @@ extern "C" int gam_update_stage(const gam_params* p, int32_t fp32, const void* c
 
 // For the whole-step adjoint (gam_stepadj.cu), which owns its work area: the
 // update stage's adjoint stores the face, flux and edge adjoints (dst[2..4])
-// instead of adding into caller-zeroed arrays, and the E-field adjoint finds
-// AVf as the step's forward left it instead of recomputing Mom2Face.
+// instead of adding into caller-zeroed arrays; the E-field adjoint finds AVf
+// as the step's forward left it instead of recomputing Mom2Face; the flux and
+// E-field adjoints store their stencil adjoints per face and per edge in
+// scratch (120 and 51 box-sized components) and gather them per position in a
+// fixed order, so that every call gives the same bits, and store (not add)
+// dQW, dWn, dQB, dBlim, dDh, dabh, dbn and dVdV.
 int gam_update_adjoint_store(const gam_params* p, int32_t fp32, const void* const* in, const void* const* geo,
                              const double* dpB0, double dt, const void* const* din, void* sU, void* sM,
                              void* const* dst, void* stream) {
@@ -1091,12 +1416,26 @@ int gam_update_adjoint_store(const gam_params* p, int32_t fp32, const void* cons
 int gam_efield_adjoint_saved(const gam_params* p, int32_t fp32, const void* Dh, const void* abh, const void* bn,
                              const void* VdV, const void* volume, const void* face, const void* edge, const void* Te,
                              const void* Teb, const double* edgB0, double dt, void* AVf, const void* dE, void* dDh,
-                             void* dabh, void* dbn, void* dVdV, void* dAVf, void* stream) {
+                             void* dabh, void* dbn, void* dVdV, void* dAVf, void* scratch, void* stream) {
     int rc = check(p, fp32);
     if (rc) return rc;
+    if (!scratch) return GAM_EINVAL;
     cudaStream_t s = (cudaStream_t)stream;
     return fp32 ? efield_call<float>(p, Dh, abh, bn, VdV, volume, face, edge, Te, Teb, edgB0, dt, AVf, nullptr, dE,
-                                     dDh, dabh, dbn, dVdV, dAVf, s, true)
+                                     dDh, dabh, dbn, dVdV, dAVf, s, true, scratch)
                 : efield_call<double>(p, Dh, abh, bn, VdV, volume, face, edge, Te, Teb, edgB0, dt, AVf, nullptr, dE,
-                                      dDh, dabh, dbn, dVdV, dAVf, s, true);
+                                      dDh, dabh, dbn, dVdV, dAVf, s, true, scratch);
+}
+int gam_flux_adjoint_gather(const gam_params* p, int32_t fp32, const void* QW, const void* Wn, const void* QB,
+                            const void* Blim, const void* Bnf, const void* volume, const void* face, const void* Tf,
+                            const double* fcB0, const double* bFlux0, const void* dgF, const void* dmF, void* dQW,
+                            void* dWn, void* dQB, void* dBlim, void* dBnf, void* scratch, void* stream) {
+    int rc = check(p, fp32);
+    if (rc) return rc;
+    if (!scratch) return GAM_EINVAL;
+    cudaStream_t s = (cudaStream_t)stream;
+    return fp32 ? flux_call<float>(p, QW, Wn, QB, Blim, Bnf, volume, face, Tf, fcB0, bFlux0, nullptr, nullptr, dgF,
+                                   dmF, dQW, dWn, dQB, dBlim, dBnf, s, scratch)
+                : flux_call<double>(p, QW, Wn, QB, Blim, Bnf, volume, face, Tf, fcB0, bFlux0, nullptr, nullptr, dgF,
+                                    dmF, dQW, dWn, dQB, dBlim, dBnf, s, scratch);
 }

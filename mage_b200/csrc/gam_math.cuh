@@ -74,14 +74,10 @@ GAM_HD double exp_tab(int i) {
 #endif
 }
 
-// e^(a+b); b may carry a small tail of the exponent that a could not hold.
-GAM_HD double exp_ab(double a, double b) {
-    const double x = a + b;
-    if (!(x < 709.78)) {  // overflow threshold, also catches NaN
-        if (x != x) return x;
-        if (x > 709.782712893384) return INFINITY;
-    }
-    if (x < -745.2) return 0.0;
+// e^(a+b) from the reduced argument: x = a + b = k ln2/128 + r, e^x =
+// 2^(k/128) e^r with 2^(j/128) from the table (j = k mod 128) and the scale
+// 2^m = 2^((k-j)/128) applied in one (m in the normal range) or two steps.
+GAM_HD double exp_ab_core(double a, double b, double x, bool wide) {
     const double kd = round_even(x * GAM_INV_LN2N);
     const int k = (int)kd;
     double r = fma(-kd, GAM_LN2N_HI, a) + b;  // a - k*head is exact
@@ -95,9 +91,29 @@ GAM_HD double exp_ab(double a, double b) {
     const int m = (k - j) / GAM_EXP_N;  // exact: k - j is a multiple of 128
     const double th = exp_tab(2 * j), tl = exp_tab(2 * j + 1);
     const double y = th + fma(th, p, tl);
-    if (m > 1023) return (y * 2.0) * pow2i(m - 1);
-    if (m < -1021) return (y * pow2i(m + 600)) * pow2i(-600);
+    if (wide) {
+        if (m > 1023) return (y * 2.0) * pow2i(m - 1);
+        if (m < -1021) return (y * pow2i(m + 600)) * pow2i(-600);
+    }
     return y * pow2i(m);
+}
+
+// the arguments near or beyond the ends of the range, and NaN
+GAM_HD double exp_ab_edge(double a, double b, double x) {
+    if (!(x < 709.78)) {  // overflow threshold, also catches NaN
+        if (x != x) return x;
+        if (x > 709.782712893384) return INFINITY;
+    }
+    if (x < -745.2) return 0.0;
+    return exp_ab_core(a, b, x, true);
+}
+
+// e^(a+b); b may carry a small tail of the exponent that a could not hold.
+// |x| < 707 keeps k / 128 within [-1020, 1020]: one scaling, no special cases.
+GAM_HD double exp_ab(double a, double b) {
+    const double x = a + b;
+    if (fabs(x) < 707.0) return exp_ab_core(a, b, x, false);
+    return exp_ab_edge(a, b, x);
 }
 
 GAM_HD double gam_exp(double x) { return exp_ab(x, 0.0); }

@@ -20,11 +20,14 @@
 // and rounding as the element-wise PyTorch restatement of the step, so both
 // give the same bits.
 #include <cuda_runtime.h>
+
+#include <algorithm>
 #include <stdint.h>
 #include <string.h>
 
 #include "../../include/gamgpu.h"
 #include "gam_bcmap.cuh"
+#include "gam_quot.cuh"
 
 // stage adjoints for a whole step (gam_adjoint.cu)
 int gam_update_adjoint_store(const gam_params* p, int32_t fp32, const void* const* in, const void* const* geo,
@@ -33,7 +36,11 @@ int gam_update_adjoint_store(const gam_params* p, int32_t fp32, const void* cons
 int gam_efield_adjoint_saved(const gam_params* p, int32_t fp32, const void* Dh, const void* abh, const void* bn,
                              const void* VdV, const void* volume, const void* face, const void* edge, const void* Te,
                              const void* Teb, const double* edgB0, double dt, void* AVf, const void* dE, void* dDh,
-                             void* dabh, void* dbn, void* dVdV, void* dAVf, void* stream);
+                             void* dabh, void* dbn, void* dVdV, void* dAVf, void* scratch, void* stream);
+int gam_flux_adjoint_gather(const gam_params* p, int32_t fp32, const void* QW, const void* Wn, const void* QB,
+                            const void* Blim, const void* Bnf, const void* volume, const void* face, const void* Tf,
+                            const double* fcB0, const double* bFlux0, const void* dgF, const void* dmF, void* dQW,
+                            void* dWn, void* dQB, void* dBlim, void* dBnf, void* scratch, void* stream);
 
 namespace gam_stepadj {
 
@@ -52,39 +59,99 @@ __global__ void k_bc_gather(Box b, int comp, int nc, const R* __restrict__ in, R
 // from s by +-nn in i, j or k, or lie in the zero-gradient ghost layer next to
 // s; a position that is a source without being a fixed point is a J ghost,
 // copied only with its own j.
+__device__ inline bool receives(const Box& b, int i, int j, int k) {
+    const bool zg = b.bc[2] == GAM_BC_ZEROGRAD;
+    return may_receive(i, b.Nip, b.nx, b.bc[0] == GAM_BC_PERIODIC, false, false) ||
+           may_receive(j, b.Njp, b.ny, !zg, zg, b.bc[3] == GAM_BC_ZEROGRAD) ||
+           may_receive(k, b.Nkp, b.nz, b.bc[4] == GAM_BC_PERIODIC, false, false);
+}
+
+// the positions that receive from no other (most of the box): their own value
+// where the map fixes them, else zero
 template <class R>
-__global__ void k_bc_gather_adj(Box b, int comp, int nc, const R* __restrict__ g, R* __restrict__ out) {
+__global__ void k_bc_gather_adj_bulk(Box b, int comp, int nc, const R* __restrict__ g, R* __restrict__ out) {
     const long s = (long)blockIdx.x * blockDim.x + threadIdx.x;
     int i, j, k;
-    if (!pos_of(b, s, i, j, k)) return;
+    if (!pos_of(b, s, i, j, k) || receives(b, i, j, k)) return;
+    const bool fixed = bc_source(b, comp, i, j, k) == s;
+    for (int c = 0; c < nc; c++) out[c * b.n + s] = fixed ? g[c * b.n + s] : (R)0;
+}
+
+template <class R>
+__device__ void gather_adj_at(const Box& b, int comp, int nc, const R* __restrict__ g, R* __restrict__ out, long s,
+                              int i, int j, int k) {
     const bool fixed = bc_source(b, comp, i, j, k) == s;
     const bool zg = b.bc[2] == GAM_BC_ZEROGRAD;
-    // most positions receive from no other
-    if (!may_receive(i, b.Nip, b.nx, b.bc[0] == GAM_BC_PERIODIC, false, false) &&
-        !may_receive(j, b.Njp, b.ny, !zg, zg, b.bc[3] == GAM_BC_ZEROGRAD) &&
-        !may_receive(k, b.Nkp, b.nz, b.bc[4] == GAM_BC_PERIODIC, false, false)) {
-        for (int c = 0; c < nc; c++) out[c * b.n + s] = fixed ? g[c * b.n + s] : (R)0;
-        return;
-    }
     int ci[13], cj[13], ck[13];
-    const int ni = b.bc[0] == GAM_BC_PERIODIC ? axis_candidates(i, b.Nip, b.nx, false, false, ci) : (ci[0] = i, 1);
-    const int nj = axis_candidates(j, b.Njp, b.ny, zg, b.bc[3] == GAM_BC_ZEROGRAD, cj);
-    const int nk = b.bc[4] == GAM_BC_PERIODIC ? axis_candidates(k, b.Nkp, b.nz, false, false, ck) : (ck[0] = k, 1);
-    for (int c = 0; c < nc; c++) {
-        const R* gc = g + c * b.n;
-        R acc = (R)0;
-        bool any = false;
-        for (int a = 0; a < nk; a++)
-            for (int e = 0; e < nj; e++)
-                for (int f = 0; f < ni; f++) {
-                    const long t = ((long)ck[a] * b.ny + cj[e]) * b.nx + ci[f];
-                    if (t == s || bc_source(b, comp, ci[f], cj[e], ck[a]) != s) continue;
-                    acc = any ? acc + gc[t] : gc[t];
-                    any = true;
-                }
-        const R own = fixed ? gc[s] : (R)0;
-        out[c * b.n + s] = any ? own + acc : own;
+    int ni = b.bc[0] == GAM_BC_PERIODIC ? axis_candidates(i, b.Nip, b.nx, false, false, ci) : (ci[0] = i, 1);
+    int nj = axis_candidates(j, b.Njp, b.ny, zg, b.bc[3] == GAM_BC_ZEROGRAD, cj);
+    int nk = b.bc[4] == GAM_BC_PERIODIC ? axis_candidates(k, b.Nkp, b.nz, false, false, ck) : (ck[0] = k, 1);
+    // keep the candidates whose own axis rule can reach i, j, k (the I and K
+    // rules act on their axis alone; J keeps j itself, which the rule may
+    // leave unmapped), so that bc_source runs on few combinations
+    auto keep = [](int* c, int n, int x, auto rule) {
+        int m = 0;
+        for (int q = 0; q < n; q++)
+            if (rule(c[q]) == x) c[m++] = c[q];
+        return m;
+    };
+    if (b.bc[0] == GAM_BC_PERIODIC)
+        ni = keep(ci, ni, i, [&](int x) {
+            return hi_rule(GAM_BC_PERIODIC, lo_rule(GAM_BC_PERIODIC, x, b.Nip), b.Nip, comp == 0);
+        });
+    if (b.bc[4] == GAM_BC_PERIODIC)
+        nk = keep(ck, nk, k, [&](int x) {
+            return hi_rule(GAM_BC_PERIODIC, lo_rule(GAM_BC_PERIODIC, x, b.Nkp), b.Nkp, comp == 2);
+        });
+    nj = keep(cj, nj, j, [&](int x) {
+        const int y = hi_rule(b.bc[3], lo_rule(b.bc[2], x, b.Njp), b.Njp, comp == 1);
+        return y == j ? j : x;
+    });
+    // the sums of every component in one pass over the matches (ascending t)
+    R acc[5] = {(R)0, (R)0, (R)0, (R)0, (R)0};
+    bool any = false;
+    for (int a = 0; a < nk; a++)
+        for (int e = 0; e < nj; e++)
+            for (int f = 0; f < ni; f++) {
+                const long t = ((long)ck[a] * b.ny + cj[e]) * b.nx + ci[f];
+                if (t == s || bc_source(b, comp, ci[f], cj[e], ck[a]) != s) continue;
+#pragma unroll
+                for (int c = 0; c < 5; c++)
+                    if (c < nc) acc[c] = any ? acc[c] + g[c * b.n + t] : g[c * b.n + t];
+                any = true;
+            }
+#pragma unroll
+    for (int c = 0; c < 5; c++)
+        if (c < nc) {
+            const R own = fixed ? g[c * b.n + s] : (R)0;
+            out[c * b.n + s] = any ? own + acc[c] : own;
+        }
+}
+
+// the planes of positions that may receive: one plane per listed value of one
+// axis (blockIdx.z = the plane; x, y over the other two axes); a position on
+// two planes is written twice with the same value
+struct Slabs {
+    int n;          // planes
+    int axis[40];   // axis of plane q
+    int value[40];  // its coordinate
+};
+template <class R>
+__global__ void k_bc_gather_adj_slabs(Box b, Slabs sl, int comp, int nc, const R* __restrict__ g,
+                                      R* __restrict__ out) {
+    const int q = blockIdx.z;
+    const int a = sl.axis[q];
+    const int u = blockIdx.x * blockDim.x + threadIdx.x, v = blockIdx.y * blockDim.y + threadIdx.y;
+    int i, j, k;
+    if (a == 0) {
+        i = sl.value[q]; j = u; k = v;
+    } else if (a == 1) {
+        i = u; j = sl.value[q]; k = v;
+    } else {
+        i = u; j = v; k = sl.value[q];
     }
+    if (i >= b.nx || j >= b.ny || k >= b.nz || !receives(b, i, j, k)) return;
+    gather_adj_at(b, comp, nc, g, out, ((long)k * b.ny + j) * b.nx + i, i, j, k);
 }
 
 // gamCellBxyz on every cell of the box: B = (sum over faces of +-flux x face
@@ -121,6 +188,21 @@ __global__ void k_box_bxyz(Box b, const R* __restrict__ vol, const R* __restrict
 // adjoint of k_box_bxyz: every face of direction d adds the adjoints of the
 // two cells it bounds (the cell below as its upper face, the cell at its own
 // index as its lower face)
+// quotients by one divisor, equal to the IEEE quotient (FP64: gam::QuotExact,
+// one division per divisor; FP32: the division)
+template <class R>
+struct DivBy {
+    R d;
+    __device__ explicit DivBy(R dd) : d(dd) {}
+    __device__ R operator()(R a) const { return a / d; }
+};
+template <>
+struct DivBy<double> {
+    gam::QuotExact q;
+    __device__ explicit DivBy(double dd) : q(dd) {}
+    __device__ double operator()(double a) const { return q(a); }
+};
+
 template <class R>
 __global__ void k_box_bxyz_adj(Box b, const R* __restrict__ vol, const R* __restrict__ xfc,
                                const R* __restrict__ xyzcc, const R* __restrict__ dxf, const R* __restrict__ gB,
@@ -133,6 +215,8 @@ __global__ void k_box_bxyz_adj(Box b, const R* __restrict__ vol, const R* __rest
     const int p[3] = {i, j, k};
     const int N[3] = {b.Ni, b.Nj, b.Nk};
     const bool inCell = i < b.Ni && j < b.Nj && k < b.Nk;
+    const DivBy<R> byV(inCell ? vol[t] : (R)1);
+#pragma unroll
     for (int d = 0; d < 3; d++) {
         bool below = p[d] >= 1;
         for (int a = 0; a < 3; a++)
@@ -140,15 +224,16 @@ __global__ void k_box_bxyz_adj(Box b, const R* __restrict__ vol, const R* __rest
         R acc = (R)0;
         if (below) {
             const long c = t - st[d];
+            const DivBy<R> byVc(vol[c]);
             for (int x = 0; x < 3; x++) {
                 const R w = dxf ? dxf[(x + 3 + 6 * d) * n + c] : xfc[(x + 3 * d) * n + t] - xyzcc[x * n + c];
-                acc = acc + gB[x * n + c] * w / vol[c];
+                acc = acc + byVc(gB[x * n + c] * w);
             }
         }
         if (inCell) {
             for (int x = 0; x < 3; x++) {
                 const R w = dxf ? dxf[(x + 6 * d) * n + t] : xfc[(x + 3 * d) * n + t] - xyzcc[x * n + t];
-                acc = acc - gB[x * n + t] * w / vol[t];
+                acc = acc - byV(gB[x * n + t] * w);
             }
         }
         dmf[d * n + t] += acc;
@@ -161,10 +246,12 @@ unsigned blocks(long n, int blk) { return (unsigned)((n + blk - 1) / blk); }
 enum Slot {
     QW, Wn, Dh, VdV, QB, abh, Bnf, bn, AVf, E, Blim, gF, mF,                                      // forward
     dQW, dWn, dDh, dVdV, dQB, dabh, dBnf, dbn, dAVf, dE, dgF, dmF, dBlim, sU, sM, aB, dnG, dnM, tM,  // adjoint
+    RS,  // scratch of the deterministic gathers: the flux adjoint's per-face reconstruction adjoints
+         // (3 directions x 8 variables x 5), then the edge adjoints (3 x 14) and the scaled dAVf (3 x 3)
     NSLOT
 };
 constexpr int slot_nc[NSLOT] = {5, 5, 1, 3, 3, 3, 3, 3, 9, 3, 3, 15, 9,
-                                5, 5, 1, 3, 3, 3, 3, 3, 3, 3, 15, 9, 3, 5, 3, 3, 5, 3, 3};
+                                5, 5, 1, 3, 3, 3, 3, 3, 3, 3, 15, 9, 3, 5, 3, 3, 5, 3, 3, 120};
 
 struct Work {
     void* p[NSLOT];
@@ -217,7 +304,29 @@ int launch_gather(const Box& b, int comp, int nc, const void* in, void* out, cud
 }
 template <class R>
 int launch_gather_adj(const Box& b, int comp, int nc, const void* g, void* out, cudaStream_t s) {
-    k_bc_gather_adj<R><<<blocks(b.n, 128), 128, 0, s>>>(b, comp, nc, (const R*)g, (R*)out);
+    // the planes that may receive, per axis (the device rules, run on the host)
+    Slabs sl;
+    sl.n = 0;
+    const bool zg = b.bc[2] == GAM_BC_ZEROGRAD;
+    const int ext[3] = {b.nx, b.ny, b.nz};
+    int w = 0, h = 0;
+    for (int a = 0; a < 3; a++)
+        for (int x = 0; x < ext[a]; x++) {
+            const bool r = a == 0   ? may_receive(x, b.Nip, b.nx, b.bc[0] == GAM_BC_PERIODIC, false, false)
+                           : a == 1 ? may_receive(x, b.Njp, b.ny, !zg, zg, b.bc[3] == GAM_BC_ZEROGRAD)
+                                    : may_receive(x, b.Nkp, b.nz, b.bc[4] == GAM_BC_PERIODIC, false, false);
+            if (!r) continue;
+            if (sl.n == 40) return GAM_EBADDIM;  // the ghost rules make at most 9 planes per axis
+            sl.axis[sl.n] = a;
+            sl.value[sl.n++] = x;
+            w = std::max(w, a == 0 ? b.ny : b.nx);
+            h = std::max(h, a == 2 ? b.ny : b.nz);
+        }
+    k_bc_gather_adj_bulk<R><<<blocks(b.n, 256), 256, 0, s>>>(b, comp, nc, (const R*)g, (R*)out);
+    if (sl.n > 0) {
+        const dim3 blk(32, 4, 1), grd((unsigned)((w + 31) / 32), (unsigned)((h + 3) / 4), (unsigned)sl.n);
+        k_bc_gather_adj_slabs<R><<<grd, blk, 0, s>>>(b, sl, comp, nc, (const R*)g, (R*)out);
+    }
     return cudaGetLastError() == cudaSuccess ? GAM_OK : GAM_ECUDA;
 }
 
@@ -338,12 +447,14 @@ extern "C" int gam_step_adj(const gam_params* p, int32_t fp32, const void* const
     const void* dup[2] = {w.p[dnG], w.p[dnM]};
     void* dsu[5] = {dst[0], dst[1], w.p[dE], w.p[dgF], w.p[dmF]};
     TRY(gam_update_adjoint_store(p, fp32, in5, g4, bg ? bg[3] : nullptr, dt, dup, w.p[sU], w.p[sM], dsu, s));
-    TRY(gam_flux_adjoint(p, fp32, w.p[QW], w.p[Wn], w.p[QB], w.p[Blim], w.p[Bnf], geo[0], geo[1], geo[8],
-                         bg ? bg[0] : nullptr, bg ? bg[1] : nullptr, w.p[dgF], w.p[dmF], w.p[dQW], w.p[dWn],
-                         w.p[dQB], w.p[dBlim], w.p[dBnf], s));
+    // the flux and E-field adjoints gather their stencil adjoints through RS
+    // in a fixed order: the same bits on every call
+    TRY(gam_flux_adjoint_gather(p, fp32, w.p[QW], w.p[Wn], w.p[QB], w.p[Blim], w.p[Bnf], geo[0], geo[1], geo[8],
+                                bg ? bg[0] : nullptr, bg ? bg[1] : nullptr, w.p[dgF], w.p[dmF], w.p[dQW], w.p[dWn],
+                                w.p[dQB], w.p[dBlim], w.p[dBnf], w.p[RS], s));
     TRY(gam_efield_adjoint_saved(p, fp32, w.p[Dh], w.p[abh], w.p[bn], w.p[VdV], geo[0], geo[1], geo[5], geo[6],
                                  geo[7], bg ? bg[2] : nullptr, dt, w.p[AVf], w.p[dE], w.p[dDh], w.p[dabh], w.p[dbn],
-                                 w.p[dVdV], w.p[dAVf], s));
+                                 w.p[dVdV], w.p[dAVf], w.p[RS], s));
     TRY(fp32 ? launch_bxyz_adj<float>(b, geo, w.p[dBlim], dst[1], s)
              : launch_bxyz_adj<double>(b, geo, w.p[dBlim], dst[1], s));
     const void* g5[5] = {geo[0], geo[1], geo[2], geo[3], geo[4]};
