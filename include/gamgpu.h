@@ -391,8 +391,10 @@ int gam_update_stage(const gam_params* p, int32_t fp32, const void* const* in, c
  * arrays in work. gam_step_adj adds into dst = {dcurGas, dcurMf, doldGas,
  * doldMf} the adjoints of st for the adjoints dnxt = {dGas, dMf, dB} of nxt
  * (dB may be NULL); saved = 1 reuses the intermediates that gam_step_fwd_save
- * left in work for the same st, saved = 0 recomputes them first. Enqueued on
- * stream; GAM_EINVAL for other boundaries, Boris, AB3, 7UP or 2.5-D.
+ * left in work for the same st, saved = 0 recomputes them first. The adjoint
+ * sums every stencil's contributions in a fixed order (no atomics), so equal
+ * inputs give equal bits on every call. Enqueued on stream; GAM_EINVAL for
+ * other boundaries, Boris, AB3, 7UP or 2.5-D.
  * No counterpart in the reference, which has no adjoint. */
 int gam_step_work_bytes(const gam_params* p, int32_t fp32, int64_t* bytes);
 int gam_step_fwd_save(const gam_params* p, int32_t fp32, const void* const* geo, const double* const* bg,
