@@ -376,11 +376,42 @@ int gam_update_stage(const gam_params* p, int32_t fp32, const void* const* in, c
                      const double* dpB0, double dt, void* const* out, const void* const* din, void* sU, void* sM,
                      void* const* dst, void* stream);
 
+/* The non-periodic I boundaries of the differentiation form and their
+ * adjoint, on caller-owned device arrays in the layout above (the step
+ * restatement's boundary fills): bc[0] = GAM_BC_SPHIN (the SphIn copy of the
+ * first active cell and its faces, bcs.F90:934-957) or GAM_BC_INFLOW (the
+ * uniform inflow state and its face fluxes), bc[1] = GAM_BC_ZEROGRAD
+ * (zeroGrad_obcI, bcs.F90:820-850) or GAM_BC_WIND (the constant solar wind
+ * blended with the last active cell, apps/wind.F90:206-374, MinMach = 1),
+ * on the 4 ghost layers of every (j, k); both I sides periodic is a no-op.
+ * The tables are in the form's precision (FP64, or FP32 with fp32 = 1). */
+typedef struct {
+    double inflow[8];  /* bc[0] = GAM_BC_INFLOW: rho, P, Vx, Vy, Vz, Bx, By, Bz */
+    double wind[8];    /* bc[1] = GAM_BC_WIND: the constant wind, same order */
+    const void* wC;    /* bc[1] = GAM_BC_WIND: (Nk+8, Nj+8, 4) wind weight of ghost cell n of row (j, k) */
+    const void* wF[3]; /* (Nk+9, Nj+9, 4): wind weight of the ghost faces of direction d */
+    const void* sF[3]; /* (Nk+9, Nj+9, 4): the wind's flux through those faces */
+} gam_iside;
+/* gam_iside_fill fills the ghosts of Gas and mf in place; B = bFlux2Fld of
+ * mf before the fill (zeroGrad_obcI and the wind read the last active cell's
+ * field); geo = {face, Tf}. gam_iside_adjoint takes Gas and B as the fill
+ * found them (it reads only the first and last active cells, which the fill
+ * does not change) and the adjoints dGas, dMf of the filled arrays: in place,
+ * every filled ghost passes its adjoint on and is zeroed; it adds into dB (the
+ * adjoint of B) and, with bc[0] = GAM_BC_INFLOW and dinflow not NULL, into
+ * the 8 adjoints of the inflow state (a device array, fixed-order sums).
+ * No counterpart in the reference, which has no adjoint. */
+int gam_iside_fill(const gam_params* p, int32_t fp32, const void* const* geo, const gam_iside* is, const void* B,
+                   void* Gas, void* mf, void* stream);
+int gam_iside_adjoint(const gam_params* p, int32_t fp32, const void* const* geo, const gam_iside* is,
+                      const void* Gas, const void* B, void* dGas, void* dMf, void* dB, void* dinflow, void* stream);
+
 /* One whole stepGamera of the differentiation form (fixed dt, AB2, 8CENT, no
  * Boris) and its adjoint, on caller-owned device arrays in the layout above:
  * the stages above plus the step's boundary conditions (periodic I and K,
  * periodic or zero-gradient J; bcs.F90:279-450, 853-892, applied in
- * EnforceBCs' order, step.F90:17-55) and bFlux2Fld (gridutils.F90:281-301).
+ * EnforceBCs' order, step.F90:17-55) and bFlux2Fld (gridutils.F90:281-301);
+ * the _iside variants below add the non-periodic I boundaries.
  * geo = {volume, face, xfc, xyzcc, dxf (fp32 only, else NULL), edge, Te, Teb,
  * Tf}; bg = {fcB0, bFlux0, edgB0, dpB0} (FP64) with doBackground, else NULL;
  * st = {curGas, curMf, oldGas, oldMf} (State and oState; the State's Bxyz is
@@ -402,6 +433,21 @@ int gam_step_fwd_save(const gam_params* p, int32_t fp32, const void* const* geo,
 int gam_step_adj(const gam_params* p, int32_t fp32, const void* const* geo, const double* const* bg,
                  const void* const* st, double dt, double odt, int32_t saved, const void* const* dnxt,
                  void* const* dst, void* work, void* stream);
+/* The same with the non-periodic I boundaries of gam_iside_fill (bc[0] =
+ * GAM_BC_SPHIN or GAM_BC_INFLOW with bc[1] = GAM_BC_ZEROGRAD or GAM_BC_WIND):
+ * after applyUpdate the step forms bFlux2Fld of the updated fluxes, fills
+ * the I ghosts from it, then runs the copying boundaries of J and K and the
+ * closing bFlux2Fld; the adjoint runs those backwards with
+ * gam_iside_adjoint and, with bc[0] = GAM_BC_INFLOW and dinflow not NULL,
+ * adds the adjoints of the 8 inflow values into the device array dinflow.
+ * gam_step_fwd_save and gam_step_adj return GAM_EINVAL for these boundaries.
+ * No counterpart in the reference. */
+int gam_step_fwd_save_iside(const gam_params* p, int32_t fp32, const void* const* geo, const double* const* bg,
+                            const gam_iside* is, const void* const* st, double dt, double odt, void* const* nxt,
+                            void* work, void* stream);
+int gam_step_adj_iside(const gam_params* p, int32_t fp32, const void* const* geo, const double* const* bg,
+                       const gam_iside* is, const void* const* st, double dt, double odt, int32_t saved,
+                       const void* const* dnxt, void* const* dst, void* dinflow, void* work, void* stream);
 
 /* Conserved totals for callers that cannot allocate device memory.
  * No counterpart in the reference. Some callers cannot call cudaMalloc while

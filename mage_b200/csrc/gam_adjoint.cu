@@ -1066,6 +1066,319 @@ __global__ void __launch_bounds__(256) k_update_adj_faces(GamBox b, DevParams<R>
         dE[2 * fs + c] += (R)aE2;
     }
 }
+// ----------------------------------------------------------------- I-side boundaries
+// The non-periodic I boundaries of the differentiation form, as the step
+// restatement writes them (mage_b200/diffstep.py, _iside_bcs): the uniform
+// inflow or the SphIn copy (bcs.F90:934-957) on the inner side, the constant
+// solar wind (apps/wind.F90:206-374, MinMach = 1) or zeroGrad_obcI
+// (bcs.F90:820-850) on the outer side, on ghost layers n = 1..4. One thread
+// per (j, k) of the face box; a thread writes its own row only, and reads the
+// first / last active cell and its faces, which no fill writes.
+template <class R>
+struct ISideDev {
+    R inflow[8], wind[8];   // rho, P, Vx, Vy, Vz, Bx, By, Bz
+    const R* wC;            // (Nk, Nj, 4) blend weights of the ghost cells
+    const R* wF[3];         // (Nk+1, Nj+1, 4) face blend weights
+    const R* sF[3];         // (Nk+1, Nj+1, 4) wind face fluxes
+};
+
+template <class R>
+__device__ __forceinline__ R iside_proj(const GamBox& b, const R* face, const R* Tf, int d, long c, const R* B) {
+    const long fs = b.fs;
+    const R* n = Tf + (long)(9 * d) * fs + c;
+    return face[d * fs + c] * (B[0] * n[0] + B[1] * n[fs] + B[2] * n[2 * fs]);
+}
+
+// the wind's MHD-side primitives of the last active cell: CellC2P, then the
+// MinMach fix of the normal velocity with the fast speed of Con2Fast
+template <class R>
+struct WindEdge {
+    R gC[5], Bin[3], gWin[5], V[3], nH[3];
+    R rho, Vf[3], KinE, Pv, Pr, Cs, S, MagB, sq, Va, Cx, dn;
+    bool fix;
+    __device__ void eval(const DevParams<R>& P, const R* Gas, const R* B, const R* Tf, long fs, long cp) {
+        for (int v = 0; v < 5; v++) gC[v] = Gas[v * fs + cp];
+        for (int x = 0; x < 3; x++) Bin[x] = B[x * fs + cp];
+        cell_c2p(P, gC, gWin);
+        rho = rmax(gC[0], P.dFloor);
+        for (int x = 0; x < 3; x++) Vf[x] = gC[1 + x] / rho;
+        KinE = (R)0.5 * rho * (Vf[0] * Vf[0] + Vf[1] * Vf[1] + Vf[2] * Vf[2]);
+        Pv = P.gm1 * (gC[4] - KinE);
+        Pr = rmax(Pv, P.pFloor);
+        Cs = Mth<R>::sqrt_(P.gamma * Pr / rho);
+        S = Bin[0] * Bin[0] + Bin[1] * Bin[1] + Bin[2] * Bin[2];
+        MagB = S > (R)0 ? Mth<R>::sqrt_(S) : (R)0;
+        sq = Mth<R>::sqrt_(gC[0]);
+        Va = MagB / sq;
+        Cx = Mth<R>::sqrt_(Cs * Cs + Va * Va);
+        const long cf = cp + 1;  // the I face ip + 1
+        for (int x = 0; x < 3; x++) nH[x] = Tf[x * fs + cf];
+        for (int x = 0; x < 3; x++) V[x] = gWin[1 + x];
+        dn = V[0] * nH[0] + V[1] * nH[1] + V[2] * nH[2];
+        fix = dn < Cx;
+        if (fix)
+            for (int x = 0; x < 3; x++) V[x] = V[x] - dn * nH[x] + Cx * nH[x];
+    }
+    // the blended primitives of ghost layer n (weight wSW of the wind)
+    __device__ void blend(const ISideDev<R>& is, R wSW, R* gW) const {
+        const R wMHD = (R)1 - wSW;
+        const R sw = wSW > (R)TINY ? (R)1 : (R)0, mh = wMHD > (R)TINY ? (R)1 : (R)0;
+        const R gW_sw[5] = {sw * is.wind[0], sw * is.wind[2], sw * is.wind[3], sw * is.wind[4], sw * is.wind[1]};
+        const R gWi[5] = {mh * gWin[0], mh * V[0], mh * V[1], mh * V[2], mh * gWin[4]};
+        for (int v = 0; v < 5; v++) gW[v] = wSW * gW_sw[v] + wMHD * gWi[v];
+    }
+};
+
+template <class R>
+__global__ void __launch_bounds__(256) k_iside_fill(GamBox b, DevParams<R> P, const R* __restrict__ face,
+                                                    const R* __restrict__ Tf, ISideDev<R> is,
+                                                    const R* __restrict__ B, R* Gas, R* mf) {
+    const int jj = blockIdx.x * blockDim.x + threadIdx.x, kk = blockIdx.y * blockDim.y + threadIdx.y;
+    if (jj > b.Nj || kk > b.Nk) return;
+    const bool cellJK = jj < b.Nj && kk < b.Nk;
+    const long fs = b.fs;
+    const int G = GAM_NG, ip = G + b.Nip - 1;
+    auto at = [&](int i) { return lidx(b, i, jj, kk); };
+    if (P.bc[0] == BCK_INFLOW && cellJK) {
+        const R gW[5] = {is.inflow[0], is.inflow[2], is.inflow[3], is.inflow[4], is.inflow[1]};
+        R gC[5];
+        cell_p2c(P, gW, gC);
+        const R Bw[3] = {is.inflow[5], is.inflow[6], is.inflow[7]};
+        for (int n = 1; n <= 4; n++) {
+            const long c = at(G - n);
+            for (int v = 0; v < 5; v++) Gas[v * fs + c] = gC[v];
+            for (int d = 0; d < 3; d++) mf[d * fs + c] = iside_proj(b, face, Tf, d, c, Bw);
+        }
+    }
+    if (P.bc[1] == BCK_ZEROGRAD && cellJK) {
+        const long cp = at(ip);
+        const R Bc[3] = {B[cp], B[fs + cp], B[2 * fs + cp]};
+        R g0[5];
+        for (int v = 0; v < 5; v++) g0[v] = Gas[v * fs + cp];
+        for (int n = 1; n <= 4; n++) {
+            const long cg = at(ip + n);
+            for (int v = 0; v < 5; v++) Gas[v * fs + cg] = g0[v];
+            mf[cg + 1] = iside_proj(b, face, Tf, 0, cg + 1, Bc);
+            mf[fs + cg] = iside_proj(b, face, Tf, 1, cg, Bc);
+            mf[2 * fs + cg] = iside_proj(b, face, Tf, 2, cg, Bc);
+        }
+    }
+    if (P.bc[0] == BCK_SPHIN && cellJK) {
+        const long src = at(G);
+        R g0[5], f0[3];
+        for (int v = 0; v < 5; v++) g0[v] = Gas[v * fs + src];
+        for (int x = 0; x < 3; x++) f0[x] = mf[x * fs + src];
+        for (int n = 1; n <= 4; n++) {
+            const long dst = at(G - n);
+            for (int v = 0; v < 5; v++) Gas[v * fs + dst] = g0[v];
+            for (int x = 0; x < 3; x++) mf[x * fs + dst] = f0[x];
+        }
+    }
+    if (P.bc[1] != BCK_WIND) return;
+    const R fin[3] = {mf[at(ip + 1)], mf[fs + at(ip)], mf[2 * fs + at(ip)]};
+    const long tf = ((long)kk * (b.Nj + 1) + jj) * 4;
+    if (cellJK) {
+        WindEdge<R> we;
+        we.eval(P, Gas, B, Tf, fs, at(ip));
+        const long tc = ((long)kk * b.Nj + jj) * 4;
+        for (int n = 1; n <= 4; n++) {
+            R gW[5], gC[5];
+            we.blend(is, is.wC[tc + n - 1], gW);
+            cell_p2c(P, gW, gC);
+            const long cg = at(ip + n);
+            for (int v = 0; v < 5; v++) Gas[v * fs + cg] = gC[v];
+        }
+    }
+    for (int n = 1; n <= 4; n++)
+        for (int d = 0; d < 3; d++) {
+            const R w = is.wF[d][tf + n - 1];
+            const long cf = d == 0 ? at(ip + n + 1) : at(ip + n);
+            mf[d * fs + cf] = w * is.sF[d][tf + n - 1] + ((R)1 - w) * fin[d];
+        }
+}
+
+// Adjoint of k_iside_fill: Gas and B as the fill found them at the first /
+// last active cell (the fill leaves those unchanged), dGas and dMf the
+// adjoints of the filled arrays. In place: every ghost the fill wrote passes
+// its adjoint to what it was computed from and is zeroed; dB (the field of
+// the update's fluxes) is added into at the last active cells. Follows the
+// forward's branches (floors, the MinMach switch, sqrt at 0 with a zero
+// derivative).
+template <class R>
+__global__ void __launch_bounds__(256) k_iside_adj(GamBox b, DevParams<R> P, const R* __restrict__ face,
+                                                   const R* __restrict__ Tf, ISideDev<R> is,
+                                                   const R* __restrict__ Gas, const R* __restrict__ B, R* dG, R* dM,
+                                                   R* dB) {
+    using A = R;
+    const int jj = blockIdx.x * blockDim.x + threadIdx.x, kk = blockIdx.y * blockDim.y + threadIdx.y;
+    if (jj > b.Nj || kk > b.Nk) return;
+    const bool cellJK = jj < b.Nj && kk < b.Nk;
+    const long fs = b.fs;
+    const int G = GAM_NG, ip = G + b.Nip - 1;
+    auto at = [&](int i) { return lidx(b, i, jj, kk); };
+    const long cp = at(ip);
+    if (P.bc[1] == BCK_WIND) {
+        const long tf = ((long)kk * (b.Nj + 1) + jj) * 4;
+        A afin[3] = {(A)0, (A)0, (A)0};
+        for (int n = 1; n <= 4; n++)
+            for (int d = 0; d < 3; d++) {
+                const long cf = d == 0 ? at(ip + n + 1) : at(ip + n);
+                afin[d] += ((A)1 - (A)is.wF[d][tf + n - 1]) * (A)dM[d * fs + cf];
+                dM[d * fs + cf] = (R)0;
+            }
+        dM[at(ip + 1)] += (R)afin[0];
+        dM[fs + cp] += (R)afin[1];
+        dM[2 * fs + cp] += (R)afin[2];
+        if (cellJK) {
+            WindEdge<R> we;
+            we.eval(P, Gas, B, Tf, fs, cp);
+            const long tc = ((long)kk * b.Nj + jj) * 4;
+            A aWin0 = (A)0, aWin4 = (A)0, aVn[3] = {(A)0, (A)0, (A)0};
+            for (int n = 1; n <= 4; n++) {
+                const R wSW = is.wC[tc + n - 1];
+                R gW[5];
+                we.blend(is, wSW, gW);
+                const long cg = at(ip + n);
+                A aU[5], aW[5] = {(A)0, (A)0, (A)0, (A)0, (A)0};
+                for (int v = 0; v < 5; v++) {
+                    aU[v] = dG[v * fs + cg];
+                    dG[v * fs + cg] = (R)0;
+                }
+                p2c_adj<A>(P.dFloor, P.pFloor, P.gm1, gW, aU, aW);
+                const A wMHD = (A)1 - (A)wSW;
+                const A mh = wMHD > (A)TINY ? (A)1 : (A)0;
+                aWin0 += mh * wMHD * aW[0];
+                for (int x = 0; x < 3; x++) aVn[x] += mh * wMHD * aW[1 + x];
+                aWin4 += mh * wMHD * aW[4];
+            }
+            // the MinMach fix: V' = V - dn nH + Cx nH, dn = V . nH
+            A aV[3] = {aVn[0], aVn[1], aVn[2]}, aCx = (A)0;
+            if (we.fix) {
+                A s = (A)0;
+                for (int x = 0; x < 3; x++) s += aVn[x] * (A)we.nH[x];
+                aCx = s;
+                for (int x = 0; x < 3; x++) aV[x] += -s * (A)we.nH[x];
+            }
+            // CellC2P of the edge cell
+            const A aWc[5] = {aWin0, aV[0], aV[1], aV[2], aWin4};
+            A aG[5] = {(A)0, (A)0, (A)0, (A)0, (A)0};
+            c2p_adj<A>(P.dFloor, P.pFloor, P.gm1, we.gC, aWc, aG);
+            // Con2Fast: Cx = sqrt(Cs^2 + Va^2), Va = MagB / sqrt(rho_c),
+            // MagB = |B|, Cs = sqrt(gamma Pr / rho)
+            A aB[3] = {(A)0, (A)0, (A)0};
+            if (aCx != (A)0 && we.Cx > (R)0) {
+                const A aCs = aCx * (A)we.Cs / (A)we.Cx, aVa = aCx * (A)we.Va / (A)we.Cx;
+                const A aMagB = aVa / (A)we.sq;
+                aG[0] += -aVa * (A)we.Va * (A)0.5 / (A)we.gC[0];
+                if (we.S > (R)0)
+                    for (int x = 0; x < 3; x++) aB[x] = aMagB * (A)we.Bin[x] / (A)we.MagB;
+                A arho = (A)0;
+                if (we.Cs > (R)0) {
+                    const A aX = aCs * (A)0.5 / (A)we.Cs;
+                    const A aPr = aX * (A)P.gamma / (A)we.rho;
+                    arho += -aX * (A)P.gamma * (A)we.Pr / ((A)we.rho * (A)we.rho);
+                    if (!(we.Pv < P.pFloor)) {
+                        aG[4] += aPr * (A)P.gm1;
+                        const A aKinE = -aPr * (A)P.gm1;
+                        arho += aKinE * (A)0.5 *
+                                ((A)we.Vf[0] * (A)we.Vf[0] + (A)we.Vf[1] * (A)we.Vf[1] + (A)we.Vf[2] * (A)we.Vf[2]);
+                        for (int x = 0; x < 3; x++) {
+                            const A aVf = aKinE * (A)we.rho * (A)we.Vf[x];
+                            aG[1 + x] += aVf / (A)we.rho;
+                            arho += -aVf * (A)we.Vf[x] / (A)we.rho;
+                        }
+                    }
+                }
+                if (!(we.gC[0] < P.dFloor)) aG[0] += arho;
+            }
+            for (int v = 0; v < 5; v++) dG[v * fs + cp] += (R)aG[v];
+            for (int x = 0; x < 3; x++) dB[x * fs + cp] += (R)aB[x];
+        }
+    }
+    if (P.bc[1] == BCK_ZEROGRAD && cellJK) {
+        A ag[5] = {(A)0, (A)0, (A)0, (A)0, (A)0}, aB[3] = {(A)0, (A)0, (A)0};
+        for (int n = 1; n <= 4; n++) {
+            const long cg = at(ip + n);
+            for (int v = 0; v < 5; v++) {
+                ag[v] += (A)dG[v * fs + cg];
+                dG[v * fs + cg] = (R)0;
+            }
+            const long cf[3] = {cg + 1, cg, cg};
+            for (int d = 0; d < 3; d++) {
+                const A a = (A)dM[d * fs + cf[d]] * (A)face[d * fs + cf[d]];
+                dM[d * fs + cf[d]] = (R)0;
+                for (int x = 0; x < 3; x++) aB[x] += a * (A)Tf[(9 * d + x) * fs + cf[d]];
+            }
+        }
+        for (int v = 0; v < 5; v++) dG[v * fs + cp] += (R)ag[v];
+        for (int x = 0; x < 3; x++) dB[x * fs + cp] += (R)aB[x];
+    }
+    if (P.bc[0] == BCK_SPHIN && cellJK) {
+        const long src = at(G);
+        A ag[5] = {(A)0, (A)0, (A)0, (A)0, (A)0}, af[3] = {(A)0, (A)0, (A)0};
+        for (int n = 1; n <= 4; n++) {
+            const long dst = at(G - n);
+            for (int v = 0; v < 5; v++) {
+                ag[v] += (A)dG[v * fs + dst];
+                dG[v * fs + dst] = (R)0;
+            }
+            for (int x = 0; x < 3; x++) {
+                af[x] += (A)dM[x * fs + dst];
+                dM[x * fs + dst] = (R)0;
+            }
+        }
+        for (int v = 0; v < 5; v++) dG[v * fs + src] += (R)ag[v];
+        for (int x = 0; x < 3; x++) dM[x * fs + src] += (R)af[x];
+    }
+    if (P.bc[0] == BCK_INFLOW && cellJK)
+        for (int n = 1; n <= 4; n++) {
+            const long c = at(G - n);
+            for (int v = 0; v < 5; v++) dG[v * fs + c] = (R)0;
+            for (int d = 0; d < 3; d++) dM[d * fs + c] = (R)0;
+        }
+}
+
+// Adjoint of the inflow state (rho, P, Vx, Vy, Vz, Bx, By, Bz) from the
+// adjoints of the inflow's ghost cells and faces (before k_iside_adj zeroes
+// them): one block, each thread a fixed set of (j, k) rows, then a fixed
+// tree over the threads, in FP64 (deterministic); added into dw.
+template <class R>
+__global__ void __launch_bounds__(256) k_inflow_adj(GamBox b, DevParams<R> P, const R* __restrict__ face,
+                                                    const R* __restrict__ Tf, ISideDev<R> is,
+                                                    const R* __restrict__ dG, const R* __restrict__ dM, R* dw) {
+    __shared__ double red[8][256];
+    const int t = threadIdx.x;
+    const long fs = b.fs;
+    const int G = GAM_NG;
+    const R gW[5] = {is.inflow[0], is.inflow[2], is.inflow[3], is.inflow[4], is.inflow[1]};
+    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    const long rows = (long)b.Nj * b.Nk;
+    for (long q = t; q < rows; q += 256) {
+        const int jj = (int)(q % b.Nj), kk = (int)(q / b.Nj);
+        for (int n = 1; n <= 4; n++) {
+            const long c = lidx(b, G - n, jj, kk);
+            R aU[5], aW[5] = {(R)0, (R)0, (R)0, (R)0, (R)0};
+            for (int v = 0; v < 5; v++) aU[v] = dG[v * fs + c];
+            p2c_adj<R>(P.dFloor, P.pFloor, P.gm1, gW, aU, aW);
+            acc[0] += (double)aW[0];
+            acc[1] += (double)aW[4];
+            for (int x = 0; x < 3; x++) acc[2 + x] += (double)aW[1 + x];
+            for (int d = 0; d < 3; d++) {
+                const double a = (double)dM[d * fs + c] * (double)face[d * fs + c];
+                for (int x = 0; x < 3; x++) acc[5 + x] += a * (double)Tf[(9 * d + x) * fs + c];
+            }
+        }
+    }
+    for (int q = 0; q < 8; q++) red[q][t] = acc[q];
+    __syncthreads();
+    for (int h = 128; h > 0; h >>= 1) {
+        if (t < h)
+            for (int q = 0; q < 8; q++) red[q][t] += red[q][t + h];
+        __syncthreads();
+    }
+    if (t < 8) dw[t] += (R)red[t][0];
+}
+
 }  // namespace gam_adj
 
 // ------------------------------------------------------------ C ABI
@@ -1438,4 +1751,81 @@ int gam_flux_adjoint_gather(const gam_params* p, int32_t fp32, const void* QW, c
                                    dmF, dQW, dWn, dQB, dBlim, dBnf, s, scratch)
                 : flux_call<double>(p, QW, Wn, QB, Blim, Bnf, volume, face, Tf, fcB0, bFlux0, nullptr, nullptr, dgF,
                                     dmF, dQW, dWn, dQB, dBlim, dBnf, s, scratch);
+}
+
+// ------------------------------------------------------------ I-side boundaries (C ABI)
+namespace {
+int iside_check(const gam_params* p) {
+    const int a = p->bc[0], c = p->bc[1];
+    const bool pin = a == GAM_BC_PERIODIC, pout = c == GAM_BC_PERIODIC;
+    if (pin != pout) return GAM_EINVAL;
+    if (!pin && a != GAM_BC_SPHIN && a != GAM_BC_INFLOW) return GAM_EINVAL;
+    if (!pout && c != GAM_BC_ZEROGRAD && c != GAM_BC_WIND) return GAM_EINVAL;
+    return GAM_OK;
+}
+template <class R>
+int iside_dev(const gam_params* p, const gam_iside* is, gam_adj::ISideDev<R>& d) {
+    memset(&d, 0, sizeof(d));
+    const bool inflow = p->bc[0] == GAM_BC_INFLOW, wind = p->bc[1] == GAM_BC_WIND;
+    if ((inflow || wind) && !is) return GAM_EINVAL;
+    if (is)
+        for (int q = 0; q < 8; q++) {
+            d.inflow[q] = (R)is->inflow[q];
+            d.wind[q] = (R)is->wind[q];
+        }
+    if (wind) {
+        if (!is->wC) return GAM_EINVAL;
+        d.wC = (const R*)is->wC;
+        for (int x = 0; x < 3; x++) {
+            if (!is->wF[x] || !is->sF[x]) return GAM_EINVAL;
+            d.wF[x] = (const R*)is->wF[x];
+            d.sF[x] = (const R*)is->sF[x];
+        }
+    }
+    return GAM_OK;
+}
+template <class R>
+int iside_call(const gam_params* p, const void* const* geo, const gam_iside* is, const void* Gas, const void* B,
+               void* oGas, void* omf, void* dG, void* dM, void* dB, void* dw, cudaStream_t s) {
+    using namespace gam_adj;
+    ISideDev<R> d;
+    int rc = iside_dev<R>(p, is, d);
+    if (rc) return rc;
+    const GamBox b = torch_box(p->Nip, p->Njp, p->Nkp);
+    const DevParams<R> P = dev_params<R>(p);
+    const R* face = (const R*)geo[0];
+    const R* Tf = (const R*)geo[1];
+    const dim3 blk(32, 8, 1), grd((unsigned)((b.Nj + 1 + 31) / 32), (unsigned)((b.Nk + 1 + 7) / 8), 1);
+    if (oGas) {
+        k_iside_fill<R><<<grd, blk, 0, s>>>(b, P, face, Tf, d, (const R*)B, (R*)oGas, (R*)omf);
+    } else {
+        if (dw && p->bc[0] == GAM_BC_INFLOW)
+            k_inflow_adj<R><<<1, 256, 0, s>>>(b, P, face, Tf, d, (const R*)dG, (const R*)dM, (R*)dw);
+        k_iside_adj<R><<<grd, blk, 0, s>>>(b, P, face, Tf, d, (const R*)Gas, (const R*)B, (R*)dG, (R*)dM, (R*)dB);
+    }
+    return cudaGetLastError() == cudaSuccess ? GAM_OK : GAM_ECUDA;
+}
+}  // namespace
+
+extern "C" int gam_iside_fill(const gam_params* p, int32_t fp32, const void* const* geo, const gam_iside* is,
+                              const void* B, void* Gas, void* mf, void* stream) {
+    int rc = check(p, fp32);
+    if (rc) return rc;
+    if ((rc = iside_check(p))) return rc;
+    if (!geo || !geo[0] || !geo[1] || !B || !Gas || !mf) return GAM_EINVAL;
+    cudaStream_t s = (cudaStream_t)stream;
+    return fp32 ? iside_call<float>(p, geo, is, nullptr, B, Gas, mf, nullptr, nullptr, nullptr, nullptr, s)
+                : iside_call<double>(p, geo, is, nullptr, B, Gas, mf, nullptr, nullptr, nullptr, nullptr, s);
+}
+
+extern "C" int gam_iside_adjoint(const gam_params* p, int32_t fp32, const void* const* geo, const gam_iside* is,
+                                 const void* Gas, const void* B, void* dGas, void* dMf, void* dB, void* dinflow,
+                                 void* stream) {
+    int rc = check(p, fp32);
+    if (rc) return rc;
+    if ((rc = iside_check(p))) return rc;
+    if (!geo || !geo[0] || !geo[1] || !Gas || !B || !dGas || !dMf || !dB) return GAM_EINVAL;
+    cudaStream_t s = (cudaStream_t)stream;
+    return fp32 ? iside_call<float>(p, geo, is, Gas, B, nullptr, nullptr, dGas, dMf, dB, dinflow, s)
+                : iside_call<double>(p, geo, is, Gas, B, nullptr, nullptr, dGas, dMf, dB, dinflow, s);
 }

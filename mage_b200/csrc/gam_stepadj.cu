@@ -248,23 +248,27 @@ enum Slot {
     dQW, dWn, dDh, dVdV, dQB, dabh, dBnf, dbn, dAVf, dE, dgF, dmF, dBlim, sU, sM, aB, dnG, dnM, tM,  // adjoint
     RS,  // scratch of the deterministic gathers: the flux adjoint's per-face reconstruction adjoints
          // (3 directions x 8 variables x 5), then the edge adjoints (3 x 14) and the scaled dAVf (3 x 3)
+    UG, UM, UB, aBm,  // non-periodic I only: the update's result after the I-side fills, the field of its
+                      // fluxes before them, and that field's adjoint
     NSLOT
 };
 constexpr int slot_nc[NSLOT] = {5, 5, 1, 3, 3, 3, 3, 3, 9, 3, 3, 15, 9,
-                                5, 5, 1, 3, 3, 3, 3, 3, 3, 3, 15, 9, 3, 5, 3, 3, 5, 3, 3, 120};
+                                5, 5, 1, 3, 3, 3, 3, 3, 3, 3, 15, 9, 3, 5, 3, 3, 5, 3, 3, 120,
+                                5, 3, 3, 3};
+bool has_iside(const gam_params* p) { return p->bc[0] != GAM_BC_PERIODIC; }
 
 struct Work {
     void* p[NSLOT];
     size_t fwd_bytes, bytes;
 };
-Work layout(const Box& b, int fp32, void* base) {
+Work layout(const Box& b, int fp32, void* base, bool iside) {
     const size_t es = fp32 ? 4 : 8;
     Work w;
     size_t off = 0;
     for (int s = 0; s < NSLOT; s++) {
         if (s == dQW) w.fwd_bytes = off;
         w.p[s] = base ? (void*)((char*)base + off) : nullptr;
-        const size_t bytes = (size_t)slot_nc[s] * (size_t)b.n * es;
+        const size_t bytes = (s >= UG && !iside) ? 0 : (size_t)slot_nc[s] * (size_t)b.n * es;
         off += (bytes + 255) / 256 * 256;
     }
     w.bytes = off;
@@ -276,8 +280,12 @@ int check(const gam_params* p) {
     if (p->rmeth != GAM_RECON_8CENT || p->doBoris || p->doAB3 || !p->doLFMLim || !p->doMHD) return GAM_EINVAL;
     if (p->nG != 4 || p->Nip < 1 || p->Njp < 4 || p->Nkp < 1 || p->do25D) return GAM_EBADDIM;
     if ((double)(p->Nip + 9) * (p->Njp + 9) * (p->Nkp + 9) >= 2147483648.0) return GAM_EBADDIM;  // 32-bit indexing
-    // boundaries: periodic I and K, periodic or zero-gradient J
-    if (p->bc[0] != GAM_BC_PERIODIC || p->bc[1] != GAM_BC_PERIODIC) return GAM_EINVAL;
+    // boundaries: periodic I, or SphIn / inflow inside and zero-gradient /
+    // wind outside; periodic K; periodic or zero-gradient J
+    const bool ip = p->bc[0] == GAM_BC_PERIODIC && p->bc[1] == GAM_BC_PERIODIC;
+    const bool is = (p->bc[0] == GAM_BC_SPHIN || p->bc[0] == GAM_BC_INFLOW) &&
+                    (p->bc[1] == GAM_BC_ZEROGRAD || p->bc[1] == GAM_BC_WIND);
+    if (!ip && !is) return GAM_EINVAL;
     if (p->bc[4] != GAM_BC_PERIODIC || p->bc[5] != GAM_BC_PERIODIC) return GAM_EINVAL;
     const bool jp = p->bc[2] == GAM_BC_PERIODIC && p->bc[3] == GAM_BC_PERIODIC;
     const bool jz = p->bc[2] == GAM_BC_ZEROGRAD && p->bc[3] == GAM_BC_ZEROGRAD;
@@ -371,21 +379,59 @@ using namespace gam_stepadj;
 extern "C" int gam_step_work_bytes(const gam_params* p, int32_t fp32, int64_t* bytes) {
     TRY(check(p));
     if (!bytes) return GAM_EINVAL;
-    *bytes = (int64_t)layout(make_box(p), fp32, nullptr).bytes;
+    *bytes = (int64_t)layout(make_box(p), fp32, nullptr, has_iside(p)).bytes;
     return GAM_OK;
 }
 
-extern "C" int gam_step_fwd_save(const gam_params* p, int32_t fp32, const void* const* geo, const double* const* bg,
-                                 const void* const* st, double dt, double odt, void* const* nxt, void* work,
-                                 void* stream) {
+namespace gam_stepadj {
+// applyUpdate into UG, UM (Bs its scratch), bFlux2Fld of its fluxes into UB,
+// then the I-side fills of UG, UM in place
+int update_and_fill(const gam_params* p, int fp32, const Box& b, const Work& w, const void* const* geo,
+                    const double* const* bg, const void* const* st, double dt, const gam_iside* is, void* Bs,
+                    cudaStream_t s) {
+    const size_t es = fp32 ? 4 : 8;
+    if (cudaMemsetAsync(w.p[UG], 0, 5 * b.n * es, s) != cudaSuccess ||
+        cudaMemsetAsync(w.p[UM], 0, 3 * b.n * es, s) != cudaSuccess ||
+        cudaMemsetAsync(w.p[UB], 0, 3 * b.n * es, s) != cudaSuccess ||
+        cudaMemsetAsync(Bs, 0, 3 * b.n * es, s) != cudaSuccess)
+        return GAM_ECUDA;
+    const void* in5[5] = {st[0], st[1], w.p[E], w.p[gF], w.p[mF]};
+    const void* g4[4] = {geo[0], geo[2], geo[3], geo[4]};
+    void* upd[3] = {w.p[UG], w.p[UM], Bs};
+    TRY(gam_update_stage(p, fp32, in5, g4, bg ? bg[3] : nullptr, dt, upd, nullptr, nullptr, nullptr, nullptr, s));
+    TRY(fp32 ? launch_bxyz<float>(b, geo, w.p[UM], w.p[UB], s) : launch_bxyz<double>(b, geo, w.p[UM], w.p[UB], s));
+    const void* g2[2] = {geo[1], geo[8]};
+    return gam_iside_fill(p, fp32, g2, is, w.p[UB], w.p[UG], w.p[UM], s);
+}
+
+int step_fwd_save(const gam_params* p, int32_t fp32, const void* const* geo, const double* const* bg,
+                  const gam_iside* is, const void* const* st, double dt, double odt, void* const* nxt, void* work,
+                  void* stream) {
     TRY(check(p));
     TRY(args_ok(p, geo, bg, st, fp32, work));
     if (!nxt || !nxt[0] || !nxt[1] || !nxt[2]) return GAM_EINVAL;
     cudaStream_t s = (cudaStream_t)stream;
     const Box b = make_box(p);
-    const Work w = layout(b, fp32, work);
+    const bool iside = has_iside(p);
+    const Work w = layout(b, fp32, work, iside);
     const size_t es = fp32 ? 4 : 8;
     TRY(forward_stages(p, fp32, b, w, geo, bg, st, dt, odt, s));
+    if (iside) {
+        // applyUpdate and the I-side fills into UG, UM (kept for the adjoint),
+        // then the copying boundaries and the closing bFlux2Fld
+        TRY(update_and_fill(p, fp32, b, w, geo, bg, st, dt, is, nxt[2], s));
+        if (fp32) {
+            TRY(launch_gather<float>(b, -1, 5, w.p[UG], nxt[0], s));
+            for (int d = 0; d < 3; d++)
+                TRY(launch_gather<float>(b, d, 1, (float*)w.p[UM] + d * b.n, (float*)nxt[1] + d * b.n, s));
+        } else {
+            TRY(launch_gather<double>(b, -1, 5, w.p[UG], nxt[0], s));
+            for (int d = 0; d < 3; d++)
+                TRY(launch_gather<double>(b, d, 1, (double*)w.p[UM] + d * b.n, (double*)nxt[1] + d * b.n, s));
+        }
+        if (cudaMemsetAsync(nxt[2], 0, 3 * b.n * es, s) != cudaSuccess) return GAM_ECUDA;
+        return fp32 ? launch_bxyz<float>(b, geo, nxt[1], nxt[2], s) : launch_bxyz<double>(b, geo, nxt[1], nxt[2], s);
+    }
     // applyUpdate into the work area (the adjoint's dnG, dnM arrays, free until
     // gam_step_adj), nxtB as its scratch
     void* upd[3] = {w.p[dnG], w.p[dnM], nxt[2]};
@@ -410,17 +456,19 @@ extern "C" int gam_step_fwd_save(const gam_params* p, int32_t fp32, const void* 
     return fp32 ? launch_bxyz<float>(b, geo, nxt[1], nxt[2], s) : launch_bxyz<double>(b, geo, nxt[1], nxt[2], s);
 }
 
-extern "C" int gam_step_adj(const gam_params* p, int32_t fp32, const void* const* geo, const double* const* bg,
-                            const void* const* st, double dt, double odt, int32_t saved, const void* const* dnxt,
-                            void* const* dst, void* work, void* stream) {
+int step_adj(const gam_params* p, int32_t fp32, const void* const* geo, const double* const* bg, const gam_iside* is,
+             const void* const* st, double dt, double odt, int32_t saved, const void* const* dnxt, void* const* dst,
+             void* dinflow, void* work, void* stream) {
     TRY(check(p));
     TRY(args_ok(p, geo, bg, st, fp32, work));
     if (!dnxt || !dnxt[0] || !dnxt[1] || !dst || !dst[0] || !dst[1] || !dst[2] || !dst[3]) return GAM_EINVAL;
     cudaStream_t s = (cudaStream_t)stream;
     const Box b = make_box(p);
-    const Work w = layout(b, fp32, work);
+    const bool iside = has_iside(p);
+    const Work w = layout(b, fp32, work, iside);
     const size_t es = fp32 ? 4 : 8;
     if (!saved) TRY(forward_stages(p, fp32, b, w, geo, bg, st, dt, odt, s));
+    if (!saved && iside) TRY(update_and_fill(p, fp32, b, w, geo, bg, st, dt, is, w.p[aBm], s));
     // zero what the adjoint stages add into (dQW .. dAVf, dBlim); the update
     // stage stores dE, dgF and dmF whole, sU, sM and aB are written before
     // they are read, dnG, dnM and tM are written whole
@@ -441,6 +489,15 @@ extern "C" int gam_step_adj(const gam_params* p, int32_t fp32, const void* const
         for (int d = 0; d < 3; d++)
             TRY(launch_gather_adj<double>(b, d, 1, (double*)w.p[tM] + d * b.n, (double*)w.p[dnM] + d * b.n, s));
     }
+    if (iside) {
+        // the I-side fills (in place on dnG, dnM; the field they read gets
+        // its adjoint in aBm), then bFlux2Fld of the update's fluxes
+        if (cudaMemsetAsync(w.p[aBm], 0, 3 * b.n * es, s) != cudaSuccess) return GAM_ECUDA;
+        const void* g2[2] = {geo[1], geo[8]};
+        TRY(gam_iside_adjoint(p, fp32, g2, is, w.p[UG], w.p[UB], w.p[dnG], w.p[dnM], w.p[aBm], dinflow, s));
+        TRY(fp32 ? launch_bxyz_adj<float>(b, geo, w.p[aBm], w.p[dnM], s)
+                 : launch_bxyz_adj<double>(b, geo, w.p[aBm], w.p[dnM], s));
+    }
     // applyUpdate, CalcStress, CalcElecField, the limiter field, Predictor
     const void* in5[5] = {st[0], st[1], w.p[E], w.p[gF], w.p[mF]};
     const void* g4[4] = {geo[0], geo[2], geo[3], geo[4]};
@@ -460,4 +517,29 @@ extern "C" int gam_step_adj(const gam_params* p, int32_t fp32, const void* const
     const void* g5[5] = {geo[0], geo[1], geo[2], geo[3], geo[4]};
     const void* din8[8] = {w.p[dQW], w.p[dWn], w.p[dDh], w.p[dVdV], w.p[dQB], w.p[dabh], w.p[dBnf], w.p[dbn]};
     return gam_predict_stage(p, fp32, st, g5, 0.5 * dt, odt, nullptr, din8, w.p[aB], dst, s);
+}
+}  // namespace gam_stepadj
+
+extern "C" int gam_step_fwd_save(const gam_params* p, int32_t fp32, const void* const* geo, const double* const* bg,
+                                 const void* const* st, double dt, double odt, void* const* nxt, void* work,
+                                 void* stream) {
+    if (p && has_iside(p)) return GAM_EINVAL;  // the I-side boundaries need gam_step_fwd_save_iside
+    return step_fwd_save(p, fp32, geo, bg, nullptr, st, dt, odt, nxt, work, stream);
+}
+extern "C" int gam_step_adj(const gam_params* p, int32_t fp32, const void* const* geo, const double* const* bg,
+                            const void* const* st, double dt, double odt, int32_t saved, const void* const* dnxt,
+                            void* const* dst, void* work, void* stream) {
+    if (p && has_iside(p)) return GAM_EINVAL;
+    return step_adj(p, fp32, geo, bg, nullptr, st, dt, odt, saved, dnxt, dst, nullptr, work, stream);
+}
+extern "C" int gam_step_fwd_save_iside(const gam_params* p, int32_t fp32, const void* const* geo,
+                                       const double* const* bg, const gam_iside* is, const void* const* st, double dt,
+                                       double odt, void* const* nxt, void* work, void* stream) {
+    return step_fwd_save(p, fp32, geo, bg, is, st, dt, odt, nxt, work, stream);
+}
+extern "C" int gam_step_adj_iside(const gam_params* p, int32_t fp32, const void* const* geo, const double* const* bg,
+                                  const gam_iside* is, const void* const* st, double dt, double odt, int32_t saved,
+                                  const void* const* dnxt, void* const* dst, void* dinflow, void* work,
+                                  void* stream) {
+    return step_adj(p, fp32, geo, bg, is, st, dt, odt, saved, dnxt, dst, dinflow, work, stream);
 }

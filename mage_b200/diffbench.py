@@ -216,6 +216,13 @@ def c4_inflow(N=(64, 64, 64), nsteps=20, sigma=1e-3, seed=2024):
                                                                     params=[g.inflow]))
         out[name] = {"loss": L, "fwd_plus_adjoint_s": el, "peak_hbm_gb": mem,
                      "dloss_dinflow": {names[q]: float(gp[q]) for q in (0, 1, 2, 7)}}
+        loss_and_grad_c(g, Gas0, mf0, dt, nsteps, lossf=lossf, params=[g.inflow])  # warm-up
+        (Lc, gGc, gFc, (gpc,)), elc, memc = _timed(lambda: loss_and_grad_c(g, Gas0, mf0, dt, nsteps, lossf=lossf,
+                                                                          params=[g.inflow]))
+        out[name + "_whole_step_c"] = {
+            "loss": Lc, "fwd_plus_adjoint_s": elc, "peak_hbm_gb": memc,
+            "grad_rel_l2_vs_autograd_sweep": _rel_l2((gGc.cpu(), gFc.cpu()), (gG.cpu(), gF.cpu())),
+            "inflow_grad_rel_l2_vs_autograd_sweep": float((gpc - gp).double().norm() / gp.double().norm())}
         grads[name] = gp.double().cpu()
         if name == "fp64":
             lossf64 = lossf
@@ -265,9 +272,10 @@ def c5(N=(192, 192, 256), nsteps=200, seg=14, precisions=("fp32", "fp64"), seed=
     out = {"config": f"dipole in a solar wind, spherical {N[0]}x{N[1]}x{N[2]}, {nsteps} fixed-dt steps (dt = {dt:.4g})",
            "loss": "sum |Bxyz|^2 (field without the dipole) over active cells with r < 6",
            "wrt": "start Gas and face fluxes",
-           "impl": "reverse sweep of mage_b200.diffstep: predictor, electric field, fluxes and update by "
-                   "hand-written CUDA adjoints, boundaries (inner sphere, wind, gathers) and bFlux2Fld by PyTorch "
-                   f"autograd; checkpoint every {seg} steps, one step's graph at a time"}
+           "impl": "reverse sweep of mage_b200.diffstep: predictor, electric field, fluxes, update and the "
+                   "inner-sphere / wind fills by hand-written CUDA adjoints, boundary gathers and bFlux2Fld by "
+                   f"PyTorch autograd; checkpoint every {seg} steps, one step's graph at a time; *_whole_step_c: "
+                   "the same sweep through gam_step_fwd_save_iside / gam_step_adj_iside (no autograd)"}
     grads = {}
     for name in precisions:
         dtype = torch.float64 if name == "fp64" else torch.float32
@@ -285,8 +293,16 @@ def c5(N=(192, 192, 256), nsteps=200, seg=14, precisions=("fp32", "fp64"), seed=
         (L, gG, gF), el, mem = _timed(lambda: loss_and_grad(g, Gas0, mf0, dt, nsteps, seg=seg, lossf=lossf,
                                                              per_step=True))
         out[name] = {"loss": L, "fwd_plus_adjoint_s": el, "s_per_step": el / nsteps, "peak_hbm_gb": mem}
+        # the same sweep through the whole-step C entry points (boundary
+        # fills, gathers and bFlux2Fld adjoints as kernels, no autograd)
+        torch.cuda.empty_cache()
+        (Lc, gGc, gFc), elc, memc = _timed(lambda: loss_and_grad_c(g, Gas0, mf0, dt, nsteps, seg=seg, lossf=lossf))
+        out[name + "_whole_step_c"] = {"loss": Lc, "fwd_plus_adjoint_s": elc, "s_per_step": elc / nsteps,
+                                       "peak_hbm_gb": memc,
+                                       "grad_rel_l2_vs_autograd_sweep": _rel_l2((gGc.cpu(), gFc.cpu()),
+                                                                                (gG.cpu(), gF.cpu()))}
         grads[name] = (gG.cpu(), gF.cpu())
-        del g, Gas0, mf0, gG, gF
+        del g, Gas0, mf0, gG, gF, gGc, gFc
         torch.cuda.empty_cache()
     if "fp32" in grads and "fp64" in grads:
         out["fp32_grad_rel_l2_vs_fp64"] = _rel_l2(grads["fp32"], grads["fp64"])

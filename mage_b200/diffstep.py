@@ -684,7 +684,10 @@ def step(g: Grid, cur: dict, old: dict, dt: float, odt: float):
     # --- EnforceBCs: inner sphere and solar wind in place, then the gathers
     # (periodic, zero-gradient J), then the final bFlux2Fld
     if P.bc[0] in (3, 6) or P.bc[1] in (2, 4):
-        Gas, mfn = _iside_bcs(g, Gas, mfn, g.bxyz(mfn))
+        if g.cuda_flux:
+            Gas, mfn = _ISideFn.apply(Gas, mfn, g.bxyz(mfn), g.inflow, g)
+        else:
+            Gas, mfn = _iside_bcs(g, Gas, mfn, g.bxyz(mfn))
     shp = Gas.shape
     Gas = _GatherFn.apply(Gas.reshape(5, -1), g.bc_src[-1], g.bc_adj[-1]).reshape(shp)
     mfs = mfn.reshape(3, -1)
@@ -915,12 +918,91 @@ class _UpdateFn(torch.autograd.Function):
         return (*dst, None, None)
 
 
+def _iside_struct(g: Grid, inflow=None):
+    """gam_iside for the grid's I boundaries, and the tensors it points to."""
+    from mage_b200.gamera import ISide
+    P = g.P
+    s, keep = ISide(), []
+    if P.bc[0] == 6:
+        w = (g.inflow if inflow is None else inflow).detach().double().cpu().tolist()
+        for q in range(8):
+            s.inflow[q] = w[q]
+    if P.bc[1] == 4:
+        W = g.wind
+        for q in range(8):
+            s.wind[q] = float(W["state"][q])
+        keep = [W["wC"].contiguous()] + [W[f"wF{d}"].contiguous() for d in range(3)] + \
+               [W[f"sF{d}"].contiguous() for d in range(3)]
+        s.wC = keep[0].data_ptr()
+        for d in range(3):
+            s.wF[d] = keep[1 + d].data_ptr()
+            s.sF[d] = keep[4 + d].data_ptr()
+    return s, keep
+
+
+def _bc_params(g: Grid):
+    from mage_b200.gamera import GamParams
+    P = g.P
+    return GamParams(P.Nip, P.Njp, P.Nkp, gamma=P.gamma, CFL=P.CFL, pdmb=P.pdmb, Vd0=P.Vd0, cHogH=P.cHogH,
+                     dFloor=P.dFloor, pFloor=P.pFloor, doBackground=g.bg is not None, bc=tuple(P.bc)).to_c()
+
+
+class _ISideFn(torch.autograd.Function):
+    """The non-periodic I boundaries (the inflow or SphIn inside, zeroGrad_obcI
+    or the constant wind outside) by gam_iside_fill, with gam_iside_adjoint as
+    backward; _iside_bcs is the same fill as PyTorch expressions. B is the
+    field of the update's fluxes, inflow the inflow state (or None)."""
+
+    @staticmethod
+    def forward(ctx, Gas, mf, B, inflow, g):
+        import ctypes as C
+        from mage_b200.gamera import GamError, load_library
+        L = load_library()
+        Gas, mf, B = Gas.contiguous().clone(), mf.contiguous().clone(), B.contiguous()
+        s, keep = _iside_struct(g, inflow)
+        f32 = int(g.dtype == torch.float32)
+        geo = _vp([g.face.data_ptr(), g.Tf.data_ptr()])
+        rc = L.gam_iside_fill(C.byref(_bc_params(g)), f32, geo, C.byref(s), C.c_void_p(B.data_ptr()),
+                              C.c_void_p(Gas.data_ptr()), C.c_void_p(mf.data_ptr()),
+                              C.c_void_p(torch.cuda.current_stream().cuda_stream))
+        if rc != 0:
+            raise GamError(rc, "gam_iside_fill failed")
+        ctx.save_for_backward(Gas, B)
+        ctx.g, ctx.inflow = g, inflow
+        return Gas, mf
+
+    @staticmethod
+    def backward(ctx, dG, dM):
+        import ctypes as C
+        from mage_b200.gamera import GamError, load_library
+        L = load_library()
+        g = ctx.g
+        Gas, B = ctx.saved_tensors
+        dG = torch.zeros_like(Gas) if dG is None else dG.contiguous().clone()
+        dM = torch.zeros_like(B) if dM is None else dM.contiguous().clone()
+        dB = torch.zeros_like(B)
+        dw = None
+        if ctx.inflow is not None and ctx.needs_input_grad[3]:
+            dw = torch.zeros(8, dtype=g.dtype, device=Gas.device)
+        s, keep = _iside_struct(g, ctx.inflow)
+        f32 = int(g.dtype == torch.float32)
+        geo = _vp([g.face.data_ptr(), g.Tf.data_ptr()])
+        rc = L.gam_iside_adjoint(C.byref(_bc_params(g)), f32, geo, C.byref(s), C.c_void_p(Gas.data_ptr()),
+                                 C.c_void_p(B.data_ptr()), C.c_void_p(dG.data_ptr()), C.c_void_p(dM.data_ptr()),
+                                 C.c_void_p(dB.data_ptr()), C.c_void_p(dw.data_ptr()) if dw is not None else None,
+                                 C.c_void_p(torch.cuda.current_stream().cuda_stream))
+        if rc != 0:
+            raise GamError(rc, "gam_iside_adjoint failed")
+        return dG, dM, dB, dw, None
+
+
 class WholeStep:
     """One stepGamera and its adjoint as one C call each (gam_step_fwd_save,
-    gam_step_adj): the stage kernels of the classes above plus the step's
-    boundary gathers and bFlux2Fld on the device, without autograd. Periodic
-    I and K, periodic or zero-gradient J; the work area (gam_step_work_bytes)
-    holds one step's intermediate arrays."""
+    gam_step_adj, or their _iside variants): the stage kernels of the classes
+    above plus the step's boundaries and bFlux2Fld on the device, without
+    autograd. Periodic K, periodic or zero-gradient J, periodic I or the
+    inflow / SphIn inside with zeroGrad_obcI / the wind outside; the work
+    area (gam_step_work_bytes) holds one step's intermediate arrays."""
 
     def __init__(self, g: Grid):
         import ctypes as C
@@ -953,18 +1035,26 @@ class WholeStep:
         from mage_b200.gamera import GamError
         ts, st = self._st(cur, old)
         nxt = {"Gas": torch.empty_like(ts[0]), "mf": torch.empty_like(ts[1]), "B": torch.empty_like(ts[1])}
-        rc = self.L.gam_step_fwd_save(C.byref(self.p), self.f32, self.geo, self.bg, st, float(dt), float(odt),
-                                      _vp([nxt[k].data_ptr() for k in ("Gas", "mf", "B")]),
-                                      C.c_void_p(self.work.data_ptr()),
-                                      C.c_void_p(torch.cuda.current_stream().cuda_stream))
+        out = _vp([nxt[k].data_ptr() for k in ("Gas", "mf", "B")])
+        stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+        if self.g.P.bc[0] != 0:
+            s, keep = _iside_struct(self.g)
+            rc = self.L.gam_step_fwd_save_iside(C.byref(self.p), self.f32, self.geo, self.bg, C.byref(s), st,
+                                                float(dt), float(odt), out, C.c_void_p(self.work.data_ptr()), stream)
+        else:
+            rc = self.L.gam_step_fwd_save(C.byref(self.p), self.f32, self.geo, self.bg, st, float(dt), float(odt),
+                                          out, C.c_void_p(self.work.data_ptr()), stream)
         if rc != 0:
             raise GamError(rc, "gam_step_fwd_save failed")
         return nxt
 
-    def adjoint(self, cur: dict, old: dict, dt: float, odt: float, dnxt: dict, acc=None, saved: bool = False):
+    def adjoint(self, cur: dict, old: dict, dt: float, odt: float, dnxt: dict, acc=None, saved: bool = False,
+                dinflow=None):
         """Adjoints (dcurGas, dcurMf, doldGas, doldMf) of the step's start for
         the adjoints dnxt = {"Gas", "mf", "B" (optional)} of its result, added
-        to acc (four tensors) when given (gam_step_adj)."""
+        to acc (four tensors) when given (gam_step_adj); with the inflow
+        boundary, the inflow state's adjoints are added into dinflow (8
+        values on the device) when given."""
         import ctypes as C
         from mage_b200.gamera import GamError
         ts, st = self._st(cur, old)
@@ -972,10 +1062,18 @@ class WholeStep:
         dB = dnxt.get("B")
         dB = dB.contiguous() if dB is not None else None
         dst = [a.contiguous() for a in acc] if acc is not None else [torch.zeros_like(t) for t in ts]
-        rc = self.L.gam_step_adj(C.byref(self.p), self.f32, self.geo, self.bg, st, float(dt), float(odt), int(saved),
-                                 _vp([dn[0].data_ptr(), dn[1].data_ptr(), dB.data_ptr() if dB is not None else 0]),
-                                 _vp([t.data_ptr() for t in dst]), C.c_void_p(self.work.data_ptr()),
-                                 C.c_void_p(torch.cuda.current_stream().cuda_stream))
+        dnp = _vp([dn[0].data_ptr(), dn[1].data_ptr(), dB.data_ptr() if dB is not None else 0])
+        dsp = _vp([t.data_ptr() for t in dst])
+        stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+        if self.g.P.bc[0] != 0:
+            s, keep = _iside_struct(self.g)
+            rc = self.L.gam_step_adj_iside(C.byref(self.p), self.f32, self.geo, self.bg, C.byref(s), st, float(dt),
+                                           float(odt), int(saved), dnp, dsp,
+                                           C.c_void_p(dinflow.data_ptr()) if dinflow is not None else None,
+                                           C.c_void_p(self.work.data_ptr()), stream)
+        else:
+            rc = self.L.gam_step_adj(C.byref(self.p), self.f32, self.geo, self.bg, st, float(dt), float(odt),
+                                     int(saved), dnp, dsp, C.c_void_p(self.work.data_ptr()), stream)
         if rc != 0:
             raise GamError(rc, "gam_step_adj failed")
         return dst
@@ -1174,13 +1272,20 @@ def loss_and_grad(g: Grid, Gas0, mf0, dt: float, nsteps: int, seg: int | None = 
     raise AssertionError("unreachable")
 
 
-def loss_and_grad_c(g: Grid, Gas0, mf0, dt: float, nsteps: int, seg: int | None = None, lossf=loss_b2):
+def loss_and_grad_c(g: Grid, Gas0, mf0, dt: float, nsteps: int, seg: int | None = None, lossf=loss_b2,
+                    params=None):
     """loss_and_grad through the whole-step C entry points: the same
     checkpointing (the (State, oState) pair at the start of each segment of
     seg steps), the segment's states recomputed with gam_step_fwd_save, then
     gam_step_adj one step at a time backwards; autograd only for the loss's
     own gradient. The adjoint of oState at step n is the adjoint of State at
-    step n-1, so it seeds that step's accumulators."""
+    step n-1, so it seeds that step's accumulators. params = [g.inflow]
+    also returns the loss's gradient w.r.t. the inflow state (the sum of
+    every step's inflow adjoints), as a fourth result."""
+    params = list(params or [])
+    for q in params:
+        assert q is g.inflow, "loss_and_grad_c differentiates w.r.t. the inflow state only"
+    dw = torch.zeros(8, dtype=g.dtype, device=Gas0.device) if params else None
     ws = WholeStep(g)
     seg = seg or max(1, int(round(nsteps ** 0.5)))
     with torch.no_grad():
@@ -1212,8 +1317,10 @@ def loss_and_grad_c(g: Grid, Gas0, mf0, dt: float, nsteps: int, seg: int | None 
                 if carry is not None:
                     acc[0].add_(carry[0])
                     acc[1].add_(carry[1])
-                d = ws.adjoint(c, o, dt, dt, lam, acc)
+                d = ws.adjoint(c, o, dt, dt, lam, acc, dinflow=dw)
                 lam = {"Gas": d[0], "mf": d[1]}
                 carry = (d[2], d[3])
     # step 0 starts from State = oState = (Gas0, mf0)
+    if params:
+        return float(L.detach()), lam["Gas"] + carry[0], lam["mf"] + carry[1], [dw]
     return float(L.detach()), lam["Gas"] + carry[0], lam["mf"] + carry[1]

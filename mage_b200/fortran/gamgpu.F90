@@ -27,6 +27,13 @@ module gamgpu
         integer(c_int32_t) :: doAB3
     end type gam_params
 
+    ! inflow and wind values and wind tables of the differentiation form's
+    ! I-side boundaries (device pointers in the form's precision)
+    type, bind(C) :: gam_iside
+        real(c_double) :: inflow(8), wind(8)
+        type(c_ptr) :: wC, wF(3), sF(3)
+    end type gam_iside
+
     interface
         integer(c_int) function gam_default_params(p, Nip, Njp, Nkp) bind(C, name="gam_default_params")
             import :: c_int, c_int32_t, gam_params
@@ -334,6 +341,44 @@ module gamgpu
             integer(c_int32_t), value :: fp32, saved
             type(c_ptr), intent(in) :: geo(9), st(4), dnxt(3), dst(4)
             type(c_ptr), value :: bg, work, stream
+            real(c_double), value :: dt, odt
+        end function
+        integer(c_int) function gam_iside_fill(p, fp32, geo, is, B, Gas, mf, stream) &
+                bind(C, name="gam_iside_fill")
+            import :: c_int, c_ptr, c_int32_t, gam_params, gam_iside
+            type(gam_params), intent(in) :: p
+            integer(c_int32_t), value :: fp32
+            type(c_ptr), intent(in) :: geo(2)
+            type(gam_iside), intent(in) :: is
+            type(c_ptr), value :: B, Gas, mf, stream
+        end function
+        integer(c_int) function gam_iside_adjoint(p, fp32, geo, is, Gas, B, dGas, dMf, dB, dinflow, stream) &
+                bind(C, name="gam_iside_adjoint")
+            import :: c_int, c_ptr, c_int32_t, gam_params, gam_iside
+            type(gam_params), intent(in) :: p
+            integer(c_int32_t), value :: fp32
+            type(c_ptr), intent(in) :: geo(2)
+            type(gam_iside), intent(in) :: is
+            type(c_ptr), value :: Gas, B, dGas, dMf, dB, dinflow, stream
+        end function
+        integer(c_int) function gam_step_fwd_save_iside(p, fp32, geo, bg, is, st, dt, odt, nxt, work, stream) &
+                bind(C, name="gam_step_fwd_save_iside")
+            import :: c_int, c_ptr, c_int32_t, c_double, gam_params, gam_iside
+            type(gam_params), intent(in) :: p
+            integer(c_int32_t), value :: fp32
+            type(c_ptr), intent(in) :: geo(9), st(4), nxt(3)
+            type(gam_iside), intent(in) :: is
+            type(c_ptr), value :: bg, work, stream
+            real(c_double), value :: dt, odt
+        end function
+        integer(c_int) function gam_step_adj_iside(p, fp32, geo, bg, is, st, dt, odt, saved, dnxt, dst, dinflow, &
+                                                   work, stream) bind(C, name="gam_step_adj_iside")
+            import :: c_int, c_ptr, c_int32_t, c_double, gam_params, gam_iside
+            type(gam_params), intent(in) :: p
+            integer(c_int32_t), value :: fp32, saved
+            type(c_ptr), intent(in) :: geo(9), st(4), dnxt(3), dst(4)
+            type(gam_iside), intent(in) :: is
+            type(c_ptr), value :: bg, dinflow, work, stream
             real(c_double), value :: dt, odt
         end function
         integer(c_int) function gam_write_restart(h, path) bind(C, name="gam_write_restart")

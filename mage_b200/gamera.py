@@ -38,6 +38,14 @@ class GamError(RuntimeError):
         self.code = code
 
 
+class ISide(C.Structure):
+    """gam_iside: the inflow and wind values and the wind tables (device
+    pointers in the form's precision) of the differentiation form's I-side
+    boundaries."""
+    _fields_ = [("inflow", C.c_double * 8), ("wind", C.c_double * 8), ("wC", C.c_void_p),
+                ("wF", C.c_void_p * 3), ("sF", C.c_void_p * 3)]
+
+
 class _Params(C.Structure):
     _fields_ = [
         ("Nip", C.c_int32), ("Njp", C.c_int32), ("Nkp", C.c_int32), ("nG", C.c_int32),
@@ -60,7 +68,8 @@ EXPORTED = (
     "gam_dt_partial", "gam_step_end", "gam_set_slab_edges", "gam_set_stream", "gam_step_begin_dev",
     "gam_dt_partial_dev", "gam_step_end_dev", "gam_step_status", "gam_flux_forward", "gam_flux_adjoint",
     "gam_efield_forward", "gam_efield_adjoint", "gam_predict_stage", "gam_update_stage", "gam_step_work_bytes",
-    "gam_step_fwd_save", "gam_step_adj",
+    "gam_step_fwd_save", "gam_step_adj", "gam_iside_fill", "gam_iside_adjoint", "gam_step_fwd_save_iside",
+    "gam_step_adj_iside",
 )
 
 # Background-field arrays (Grid_T, gamtypes.F90:233-242): name, components;
@@ -126,6 +135,14 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
                                     C.c_void_p, C.c_void_p]
     L.gam_step_adj.argtypes = [C.POINTER(_Params), C.c_int32, _vpp, _vpp, _vpp, C.c_double, C.c_double, C.c_int32,
                                _vpp, _vpp, C.c_void_p, C.c_void_p]
+    _isp = C.POINTER(ISide)
+    L.gam_iside_fill.argtypes = [C.POINTER(_Params), C.c_int32, _vpp, _isp, C.c_void_p, C.c_void_p, C.c_void_p,
+                                 C.c_void_p]
+    L.gam_iside_adjoint.argtypes = [C.POINTER(_Params), C.c_int32, _vpp, _isp] + [C.c_void_p] * 7
+    L.gam_step_fwd_save_iside.argtypes = [C.POINTER(_Params), C.c_int32, _vpp, _vpp, _isp, _vpp, C.c_double,
+                                          C.c_double, _vpp, C.c_void_p, C.c_void_p]
+    L.gam_step_adj_iside.argtypes = [C.POINTER(_Params), C.c_int32, _vpp, _vpp, _isp, _vpp, C.c_double, C.c_double,
+                                     C.c_int32, _vpp, _vpp, C.c_void_p, C.c_void_p, C.c_void_p]
     L.gam_halo_pack.argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
     L.gam_halo_unpack.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32]
     L.gam_init_finish_halo.argtypes = [C.c_void_p, _dp]

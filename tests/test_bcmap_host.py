@@ -3,7 +3,8 @@ compiled for the host with g++ (no GPU):
 
 * its composed source index equals the PyTorch restatement's
   (mage_b200.diffstep.Grid._bc_maps) at every box position, for cells and the
-  three face directions, periodic and zero-gradient J;
+  three face directions, periodic and zero-gradient J, with periodic I and
+  with the non-periodic I sides (whose fills run before the gather);
 * the candidates the gather's adjoint scans, filtered by the map, are exactly
   the positions the map copies from each position (brute-force preimages);
 * the adjoint's skip test (may_receive) never skips a position that is copied.
@@ -37,12 +38,13 @@ int main(int argc, char** argv) {
         for (int k = 0; k < b.nz; k++) for (int j = 0; j < b.ny; j++) for (int i = 0; i < b.nx; i++) {
             const long s = ((long)k * b.ny + j) * b.nx + i;
             int ci[13], cj[13], ck[13];
-            const int ni = axis_candidates(i, b.Nip, b.nx, false, false, ci);
+            const bool pi = b.bc[0] == GAM_BC_PERIODIC, pk = b.bc[4] == GAM_BC_PERIODIC;
+            const int ni = pi ? axis_candidates(i, b.Nip, b.nx, false, false, ci) : (ci[0] = i, 1);
             const int nj = axis_candidates(j, b.Njp, b.ny, zg, b.bc[3] == GAM_BC_ZEROGRAD, cj);
-            const int nk = axis_candidates(k, b.Nkp, b.nz, false, false, ck);
-            const bool mr = may_receive(i, b.Nip, b.nx, true, false, false) ||
+            const int nk = pk ? axis_candidates(k, b.Nkp, b.nz, false, false, ck) : (ck[0] = k, 1);
+            const bool mr = may_receive(i, b.Nip, b.nx, pi, false, false) ||
                             may_receive(j, b.Njp, b.ny, !zg, zg, b.bc[3] == GAM_BC_ZEROGRAD) ||
-                            may_receive(k, b.Nkp, b.nz, true, false, false);
+                            may_receive(k, b.Nkp, b.nz, pk, false, false);
             printf("P %d %ld %d", comp, s, (int)mr);
             for (int a = 0; a < nk; a++) for (int e = 0; e < nj; e++) for (int f = 0; f < ni; f++) {
                 const long t = ((long)ck[a] * b.ny + cj[e]) * b.nx + ci[f];
@@ -78,7 +80,8 @@ class _Box:
 
 
 @pytest.mark.parametrize("N", [(16, 16, 16), (16, 24, 8), (8, 4, 4), (4, 6, 5)])
-@pytest.mark.parametrize("bc", [(0, 0, 0, 0, 0, 0), (0, 0, 2, 2, 0, 0)], ids=["periodic", "zerogradJ"])
+@pytest.mark.parametrize("bc", [(0, 0, 0, 0, 0, 0), (0, 0, 2, 2, 0, 0), (3, 4, 2, 2, 0, 0), (6, 2, 0, 0, 0, 0)],
+                         ids=["periodic", "zerogradJ", "sphin-wind-zerogradJ", "inflow-obcI"])
 def test_bc_map_matches_restatement(harness, N, bc):
     out = subprocess.run([harness, *map(str, N), *map(str, bc)], capture_output=True, text=True,
                          check=True).stdout.split("\n")

@@ -51,9 +51,10 @@ def test_fortran_module_binds_every_entry_point():
 
 def test_whole_step_work_bytes_and_coverage():
     """gam_step_work_bytes (host arithmetic only): the work area of the
-    whole-step adjoint is 266 box-sized arrays, each started on 256 bytes; the
-    entry points refuse what the adjoint does not cover (inner-I inflow,
-    Boris, 7UP)."""
+    whole-step adjoint is 266 box-sized arrays, each started on 256 bytes, and
+    14 more with non-periodic I boundaries (the update's result, its field
+    and that field's adjoint); the entry points refuse what the adjoint does
+    not cover (one I side periodic and the other not, Boris, 7UP)."""
     L = gamera.load_library()
     nb = C.c_int64()
     N = (16, 24, 8)
@@ -66,6 +67,11 @@ def test_whole_step_work_bytes_and_coverage():
         assert nb.value == sum((c * box * es + 255) // 256 * 256 for c in nc)
     p = gamera.GamParams(*N, bc=(0, 0, 2, 2, 0, 0)).to_c()
     assert L.gam_step_work_bytes(C.byref(p), 0, C.byref(nb)) == 0
-    for kw in ({"bc": (6, 2, 2, 2, 0, 0)}, {"doBoris": True, "Ca": 1.0}, {"rmeth": gamera.RECON_7UP}):
+    for bc in ((6, 2, 2, 2, 0, 0), (3, 4, 2, 2, 0, 0), (6, 2, 0, 0, 0, 0)):
+        p = gamera.GamParams(*N, bc=bc).to_c()
+        assert L.gam_step_work_bytes(C.byref(p), 0, C.byref(nb)) == 0
+        assert nb.value == sum((c * box * 8 + 255) // 256 * 256 for c in nc + [5, 3, 3, 3])
+    for kw in ({"bc": (6, 0, 2, 2, 0, 0)}, {"bc": (0, 4, 0, 0, 0, 0)}, {"doBoris": True, "Ca": 1.0},
+               {"rmeth": gamera.RECON_7UP}):
         p = gamera.GamParams(*N, **kw).to_c()
         assert L.gam_step_work_bytes(C.byref(p), 0, C.byref(nb)) == gamera.GAM_EINVAL, kw
