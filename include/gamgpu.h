@@ -46,10 +46,12 @@ enum {
  * GAM_BC_INFLOW has no counterpart in the reference: the 4 inner-I ghost
  * layers hold a uniform state (gam_set_inflow) and the face fluxes of its
  * field, the shape of zeroGrad_obcI with a given state in place of the last
- * active cell. */
+ * active cell. GAM_BC_ION (inner I) is the ionospheric boundary of the
+ * magnetosphere (IonInnerBC_T, voltron/ICs/earthcmi.F90:441-583) together
+ * with the model hooks that come with it (gam_set_ionosphere). */
 enum { GAM_BC_PERIODIC = 0, GAM_BC_NONE = 1, GAM_BC_ZEROGRAD = 2, GAM_BC_SPHIN = 3, GAM_BC_WIND = 4,
        GAM_BC_HALO = 5 /* INK and OUTK of a k-slab: filled by the caller's halo exchange */,
-       GAM_BC_INFLOW = 6 };
+       GAM_BC_INFLOW = 6, GAM_BC_ION = 7 };
 enum { GAM_RECON_8CENT = 0, GAM_RECON_7UP = 1 };
 enum { GAM_FP64 = 0, GAM_FP32 = 1 };
 
@@ -218,6 +220,39 @@ int gam_set_wind_series(gam_handle* h, int32_t n, const double* t, const double*
  * fluxes (steps recompute every ghost's Bxyz). Call before the initial
  * condition; calling it later changes the boundary from the next step on. */
 int gam_set_inflow(gam_handle* h, const double state[8]);
+
+/* The ionospheric inner boundary (bc[0] = GAM_BC_ION) and the per-step model
+ * hooks of the reference's magnetosphere set-up that act on it
+ * (voltron/ICs/earthcmi.F90 with its defaults: IonInnerBC_T, EFix, PerStep):
+ *   - the boundary (IonInner :441-583, CellPlasmaBC msphingest.F90:268-372,
+ *     single fluid, no ingestion): ghost cell is-n takes the density and
+ *     pressure of its mirror cell is+n-1 (k wrapped into the active range)
+ *     and the E x B velocity of the coupling field inExyz(5-n) in the dipole
+ *     field at its centre, perpendicular to the radius, with only the inward
+ *     part of its radial component; its faces take zero flux;
+ *   - HackE (EFix :321-354): IonEFix (msphutils.F90:214-240), the J and K
+ *     EMFs of the first shell from the coupling field inEijk(5), then
+ *     FixEFieldLFM (gamdebug.F90:149-175), the I and J EMFs of the two
+ *     periodic k ends set to their mean;
+ *   - HackStep (PerStep :224-263): PushIon (:586-663), which moves the
+ *     velocity of the first nIonP active shells towards the E x B velocity at
+ *     the rate dt / (shell * dtCpl), before CalcDT;
+ *   - with the solar wind outside (bc[1] = GAM_BC_WIND, the constant wind of
+ *     gam_set_wind): WindEFix (apps/wind.F90:489-566), the EMFs of the outer
+ *     4 shells blended with the wind's -V x B by the wind weight at each
+ *     edge centre, plus DiffuseOuter (:570-616) on the outermost, between
+ *     IonEFix and FixEFieldLFM; NudgeSW (:394-486), the last active cell
+ *     nudged towards the wind over max(dtSW0 / weight, dt), after PushIon.
+ * inExyz is the Fortran array (1:5, jsg:jeg, ksg:keg, 1:3) and inEijk
+ * (1:6, jsg:jeg+1, ksg:keg+1, 1:3) as the coupler holds them (PsiSh = 5
+ * shells), M0 the dipole moment of VecDipole (code units, m = (0, 0, M0)),
+ * dtCpl the coupling time scale (code time), dtSW0 the nudging time scale
+ * (the reference's one minute, 60 s / gT0). Needs the geometry and, with the
+ * wind outside, gam_set_wind first (a wind time series is refused); call
+ * before the initial condition, again whenever the coupler updates the
+ * fields, and after every gam_set_wind. */
+int gam_set_ionosphere(gam_handle* h, const double* inExyz, const double* inEijk, double M0, double dtCpl,
+                       int32_t doIonPush, int32_t nIonP, double dtSW0);
 
 /* ooState of the AB3 predictor (doAB3): its face fluxes (Fortran
  * magFlux(isg:ieg+1,...,1:3)) and time. The predictor reads nothing else of

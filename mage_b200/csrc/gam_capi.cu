@@ -79,7 +79,11 @@ struct gam_handle {
     GamBox b;
     BgD bg{};
     double* windTab = nullptr;  // device: wC, wF(3), sF(3) of the solar-wind BC
-    bool haveBg = false, haveWind = false, haveInflow = false;
+    double* ionTab = nullptr;   // device: the ionospheric boundary's tables (gam_set_ionosphere)
+    long ionCap = 0;
+    double* ionWind = nullptr;  // device: the wind side of its hooks (WindEFix, NudgeSW weights)
+    double ionDtSW0 = 0.0;
+    bool haveBg = false, haveWind = false, haveInflow = false, haveIon = false;
     cudaStream_t s = nullptr;
     cudaStream_t own_s = nullptr;  // the handle's own stream (s unless gam_set_stream gave another)
     int nasync = 0;                // device-resident k-slab steps since the last gam_step_status
@@ -108,6 +112,7 @@ static int fail(gam_handle* h, int code, const std::string& msg) {
     if (h) h->err = msg;
     return code;
 }
+static int ion_wind_tables(gam_handle* h);
 #define CK(h, call)                                                                            \
     do {                                                                                       \
         cudaError_t e_ = (call);                                                               \
@@ -243,12 +248,12 @@ extern "C" int gam_create(const gam_params* p, gam_handle** out) {
     if (p->precision != GAM_FP64 && p->precision != GAM_FP32) return bad(GAM_EINVAL, "unknown precision");
     if (p->precision == GAM_FP32 && p->strict) return bad(GAM_EINVAL, "strict applies to the FP64 form only");
     {
-        // boundary kinds per side: inner I periodic/none/SphIn/inflow, outer I
+        // boundary kinds per side: inner I periodic/none/SphIn/inflow/ionosphere, outer I
         // periodic/none/wind/zero-gradient, J periodic/none/zero-gradient,
         // K periodic/none (or halo)
         const int* c = p->bc;
         auto in = [](int v, int a, int b2, int c2) { return v == a || v == b2 || v == c2; };
-        if (!(in(c[0], GAM_BC_PERIODIC, GAM_BC_NONE, GAM_BC_SPHIN) || c[0] == GAM_BC_INFLOW) ||
+        if (!(in(c[0], GAM_BC_PERIODIC, GAM_BC_NONE, GAM_BC_SPHIN) || c[0] == GAM_BC_INFLOW || c[0] == GAM_BC_ION) ||
             !(in(c[1], GAM_BC_PERIODIC, GAM_BC_NONE, GAM_BC_WIND) || c[1] == GAM_BC_ZEROGRAD) ||
             !in(c[2], GAM_BC_PERIODIC, GAM_BC_NONE, GAM_BC_ZEROGRAD) ||
             !in(c[3], GAM_BC_PERIODIC, GAM_BC_NONE, GAM_BC_ZEROGRAD) ||
@@ -259,6 +264,8 @@ extern "C" int gam_create(const gam_params* p, gam_handle** out) {
                 return bad(GAM_EINVAL, "a periodic direction needs both sides periodic");
         if ((c[4] == GAM_BC_HALO) != (c[5] == GAM_BC_HALO))
             return bad(GAM_EINVAL, "a k-slab exchanges both k sides");
+        if (c[0] == GAM_BC_ION && c[4] != GAM_BC_PERIODIC)
+            return bad(GAM_EINVAL, "the ionospheric boundary wraps k: the k boundaries must be periodic");
         if (c[0] == GAM_BC_PERIODIC && (c[2] == GAM_BC_ZEROGRAD || c[3] == GAM_BC_ZEROGRAD))
             return bad(GAM_EINVAL, "zero-gradient J with periodic I is not supported");
     }
@@ -669,6 +676,8 @@ extern "C" int gam_step(gam_handle* h, int32_t nsteps, double* dt, double* t) {
     if (h->p.bc[1] == GAM_BC_WIND && !h->haveWind) return fail(h, GAM_ESTATE, "wind boundary: call gam_set_wind first");
     if (h->p.bc[0] == GAM_BC_INFLOW && !h->haveInflow)
         return fail(h, GAM_ESTATE, "inflow boundary: call gam_set_inflow first");
+    if (h->p.bc[0] == GAM_BC_ION && (!h->haveIon || (h->p.bc[1] == GAM_BC_WIND && !h->cd.P.ion.wind)))
+        return fail(h, GAM_ESTATE, "ionospheric boundary: call gam_set_ionosphere (and gam_set_wind) first");
     if (h->p.bc[4] == GAM_BC_HALO)
         return fail(h, GAM_ESTATE, "a k-slab steps with gam_step_begin / gam_step_end and a halo exchange");
     int rc;
@@ -870,6 +879,8 @@ void gam_fast_init_f32(const Ctx<float>& C, int cur, cudaStream_t s);
 static int init_common(gam_handle* h, double* Gas64, double* mf64) {
     if (h->p.bc[0] == GAM_BC_INFLOW && !h->haveInflow)
         return fail(h, GAM_ESTATE, "inflow boundary: call gam_set_inflow before the initial condition");
+    if (h->p.bc[0] == GAM_BC_ION && !h->haveIon)
+        return fail(h, GAM_ESTATE, "ionospheric boundary: call gam_set_ionosphere before the initial condition");
     int rc = h->f32 ? finish_init<float>(h, h->cf, Gas64, mf64, 0.0) : finish_init<double>(h, h->cd, Gas64, mf64, 0.0);
     if (rc) return rc;
     // Bxyz of State, first BCs, copy to oState (init.F90:217-238)
@@ -1065,6 +1076,7 @@ extern "C" int gam_set_wind(gam_handle* h, const double wind[8]) {
     h->cf.P.wind = W;
     drop_graphs(h);
     h->haveWind = true;
+    if (h->p.bc[0] == GAM_BC_ION && h->haveIon) return ion_wind_tables(h);  // the hooks' wind side
     return GAM_OK;
 }
 
@@ -1109,6 +1121,10 @@ extern "C" int gam_set_wind_series(gam_handle* h, int32_t n, const double* t, co
     }
     drop_graphs(h);
     h->haveWind = true;
+    if (h->p.bc[0] == GAM_BC_ION) {  // the hooks' wind side takes the constant wind only
+        h->cd.P.ion.wind = h->cf.P.ion.wind = 0;
+        h->haveIon = false;
+    }
     return GAM_OK;
 }
 
@@ -1122,6 +1138,245 @@ extern "C" int gam_set_inflow(gam_handle* h, const double state[8]) {
     }
     drop_graphs(h);
     h->haveInflow = true;
+    return GAM_OK;
+}
+
+
+// ---- the ionospheric inner boundary (bc[0] = GAM_BC_ION)
+namespace {
+// NORM2 as gfortran evaluates it (scaled sum of squares)
+double ion_norm2(const double* a) {
+    double scale = 1.0, res = 0.0;
+    for (int q = 0; q < 3; q++)
+        if (a[q] != 0.0) {
+            const double ax = std::fabs(a[q]);
+            if (scale < ax) {
+                const double val = scale / ax;
+                res = 1.0 + res * val * val;
+                scale = ax;
+            } else {
+                const double val = ax / scale;
+                res += val * val;
+            }
+        }
+    return scale * std::sqrt(res);
+}
+// VecDipole (msphutils.F90:534-559), m = (0, 0, M0)
+void ion_dipole(double M0, const double* r, double* B) {
+    const double rad = ion_norm2(r);
+    const double m[3] = {0.0, 0.0, M0};
+    const double d = m[0] * r[0] + m[1] * r[1] + m[2] * r[2];
+    const double p5 = std::pow(rad, 5.0), p3 = std::pow(rad, 3.0);
+    for (int x = 0; x < 3; x++) B[x] = 3 * d * r[x] / p5 - m[x] / p3;
+}
+// E x B / |B|^2 (cross, math.F90:265-274) with its radial part removed
+// (Vec2Perp, math.F90:371-376); vr: the radial part
+void ion_exb_perp(const double* E, const double* B, const double* rh, double* v, double* vr) {
+    const double c[3] = {E[1] * B[2] - E[2] * B[1], E[2] * B[0] - E[0] * B[2], E[0] * B[1] - E[1] * B[0]};
+    const double bb = B[0] * B[0] + B[1] * B[1] + B[2] * B[2];
+    double veb[3];
+    for (int x = 0; x < 3; x++) veb[x] = c[x] / bb;
+    const double d = veb[0] * rh[0] + veb[1] * rh[1] + veb[2] * rh[2];
+    for (int x = 0; x < 3; x++) v[x] = veb[x] - d * rh[x];
+    *vr = d;
+}
+}  // namespace
+
+static int ion_wind_tables(gam_handle* h) {
+    const GamBox& b = h->b;
+    const int G = 4, Nj = b.Nj, Nk = b.Nk;
+    const long nrow = (long)(Nj + 1) * (Nk + 1), fs = b.fs;
+    const GeoD& g = h->gd;
+    const long nWe = 7L * 4 * (b.Njp + 1) * (b.Nkp + 1), nWn = (long)b.Njp * b.Nkp;
+    std::vector<double> tab(nWe + nWn, 0.0);
+    double* We = tab.data();
+    double* Wn = We + nWe;
+    double vSW = 0.0;
+    {
+        // WindEFix (apps/wind.F90:489-566) for the constant wind: the front
+        // velocity (-|V|, 0, 0) of RefreshWind with ByC = BzC = 0, the wind
+        // EMF -V x B along each edge of shells ie-2 .. ie+1, the weights at
+        // the edge centres (host libm, as the constant wind's BC weights)
+        const double* ws = h->cd.P.wind.state;
+        const double V[3] = {ws[2], ws[3], ws[4]}, Bw[3] = {ws[5], ws[6], ws[7]};
+        const double vFr[3] = {-ion_norm2(V), 0.0, 0.0};
+        const double Ca = h->p.doBoris ? h->p.Ca : 1.0e12;
+        vSW = std::min(ion_norm2(vFr), Ca);
+        const double c[3] = {V[1] * Bw[2] - V[2] * Bw[1], V[2] * Bw[0] - V[0] * Bw[2], V[0] * Bw[1] - V[1] * Bw[0]};
+        const double swE[3] = {-c[0], -c[1], -c[2]};
+        const int c0 = G + b.Nip - 3, nc = 5;  // corner columns ie-2 .. ie+2
+        std::vector<double> xv(3 * nc * nrow), xcn(3 * nrow);
+        for (int x = 0; x < 3; x++) {
+            CK(h, cudaMemcpy2DAsync(xv.data() + (size_t)x * nc * nrow, nc * sizeof(double), g.xyz + x * fs + c0,
+                                    (size_t)b.sx * sizeof(double), nc * sizeof(double), (size_t)nrow,
+                                    cudaMemcpyDeviceToHost, h->s));
+            CK(h, cudaMemcpy2DAsync(xcn.data() + (size_t)x * nrow, sizeof(double), g.xyzcc + x * fs + G + b.Nip - 1,
+                                    (size_t)b.sx * sizeof(double), sizeof(double), (size_t)nrow,
+                                    cudaMemcpyDeviceToHost, h->s));
+        }
+        CK(h, cudaStreamSynchronize(h->s));
+        auto corner = [&](int col, int jj, int kk, double* r) {
+            for (int x = 0; x < 3; x++)
+                r[x] = xv[(size_t)x * nc * nrow + ((size_t)jj + (size_t)(Nj + 1) * kk) * nc + col];
+        };
+        const int ie = b.Nip;  // Fortran indices: is = 1, ie = Nip, box column ii = i + 3
+        for (int kk = G; kk <= G + b.Nkp; kk++)
+            for (int jj = G; jj <= G + b.Njp; jj++)
+                for (int sh = 0; sh < 4; sh++) {
+                    const int col = sh, i = ie - 2 + sh;
+                    double* t = We + 7 * (sh + 4 * ((long)(jj - G) + (long)(b.Njp + 1) * (kk - G)));
+                    double wSW = 0.0;
+                    for (int n = 0; n < 3; n++) {
+                        double e1[3], e2[3], ecc[3], de[3];
+                        corner(col, jj, kk, e1);
+                        corner(col + (n == 0), jj + (n == 1), kk + (n == 2), e2);
+                        for (int x = 0; x < 3; x++) {
+                            ecc[x] = 0.5 * (e1[x] + e2[x]);
+                            de[x] = e2[x] - e1[x];
+                        }
+                        wSW = wgt_wind(V, ecc);
+                        t[n] = -1.0;  // unchanged
+                        t[3 + n] = 0.0;
+                        if (wSW > 1.0e-12) {
+                            if (i <= ie) wSW = wSW / (1.0 + ie + 1 - i);
+                            t[n] = wSW;
+                            t[3 + n] = swE[0] * de[0] + swE[1] * de[1] + swE[2] * de[2];
+                        }
+                    }
+                    t[6] = wSW;  // DiffuseOuter's weight: the K edge's
+                }
+        // NudgeSW's weights of the last active cells
+        for (int kk = G; kk < G + b.Nkp; kk++)
+            for (int jj = G; jj < G + b.Njp; jj++) {
+                const long row = jj + (long)(Nj + 1) * kk;
+                const double r[3] = {xcn[row], xcn[nrow + row], xcn[2 * nrow + row]};
+                Wn[(jj - G) + (long)b.Njp * (kk - G)] = wgt_wind(V, r);
+            }
+    }
+    if (!h->ionWind) {
+        cudaError_t e = cudaSuccess;
+        h->ionWind = dalloc<double>(h, nWe + nWn, &e);
+        if (e != cudaSuccess) return fail(h, GAM_ECUDA, "device allocation failed");
+    }
+    CK(h, cudaMemcpyAsync(h->ionWind, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice, h->s));
+    CK(h, cudaStreamSynchronize(h->s));
+    for (IonData* I : {&h->cd.P.ion, &h->cf.P.ion}) {
+        I->wind = 1;
+        I->vSW = vSW;
+        I->dtSW0 = h->ionDtSW0;
+        I->We = h->ionWind;
+        I->Wn = h->ionWind + nWe;
+    }
+    drop_graphs(h);
+    return GAM_OK;
+}
+
+extern "C" int gam_set_ionosphere(gam_handle* h, const double* inExyz, const double* inEijk, double M0, double dtCpl,
+                                  int32_t doIonPush, int32_t nIonP, double dtSW0) {
+    if (!h || !inExyz || !inEijk) return GAM_EINVAL;
+    if (h->p.bc[0] != GAM_BC_ION) return fail(h, GAM_ESTATE, "the inner I boundary is not the ionosphere");
+    if (!h->haveGeo) return fail(h, GAM_ESTATE, "set the geometry first");
+    const GamBox& b = h->b;
+    if (!doIonPush) nIonP = 0;
+    if (doIonPush && (!(dtCpl > 0.0) || nIonP < 1 || nIonP > b.Nip))
+        return fail(h, GAM_EINVAL, "PushIon needs dtCpl > 0 and 1 <= nIonP <= Nip");
+    const bool windHooks = h->p.bc[1] == GAM_BC_WIND;
+    if (windHooks) {
+        if (!h->haveXyz) return fail(h, GAM_ESTATE, "WindEFix needs the grid corners: set the geometry with gam_set_geometry");
+        if (h->haveWind && h->cd.P.wind.n != 0)
+            return fail(h, GAM_ESTATE, "the wind side of the hooks takes the constant wind (gam_set_wind)");
+        if (!(dtSW0 > 0.0)) return fail(h, GAM_EINVAL, "NudgeSW needs dtSW0 > 0");
+        if (nIonP >= b.Nip) return fail(h, GAM_EINVAL, "PushIon and NudgeSW would act on the same shell");
+    }
+    const int G = 4, Nj = b.Nj, Nk = b.Nk, ncol = G + nIonP;
+    const long nrow = (long)(Nj + 1) * (Nk + 1);
+    // box columns 0 .. G+nIonP-1 of xyzcc (3) and column G of the J, K edge lengths
+    std::vector<double> xc(3 * ncol * nrow), el(2 * nrow);
+    const GeoD& g = h->gd;
+    const long fs = b.fs;
+    for (int x = 0; x < 3; x++)
+        CK(h, cudaMemcpy2DAsync(xc.data() + (size_t)x * ncol * nrow, ncol * sizeof(double), g.xyzcc + x * fs,
+                                (size_t)b.sx * sizeof(double), ncol * sizeof(double), (size_t)nrow,
+                                cudaMemcpyDeviceToHost, h->s));
+    for (int d = 1; d < 3; d++)
+        CK(h, cudaMemcpy2DAsync(el.data() + (size_t)(d - 1) * nrow, sizeof(double), g.edge + d * fs + G,
+                                (size_t)b.sx * sizeof(double), sizeof(double), (size_t)nrow, cudaMemcpyDeviceToHost,
+                                h->s));
+    CK(h, cudaStreamSynchronize(h->s));
+    auto X = [&](int ii, int jj, int kk, double* r) {
+        for (int x = 0; x < 3; x++) r[x] = xc[(size_t)x * ncol * nrow + ((size_t)jj + (size_t)(Nj + 1) * kk) * ncol + ii];
+    };
+    // inExyz(s, j, k, x): (1:5, jsg:jeg, ksg:keg, 1:3); inEijk (1:6, jsg:jeg+1, ksg:keg+1, 1:3)
+    auto Exyz = [&](int sh, int jj, int kk, int x) { return inExyz[sh + 5 * (jj + (long)Nj * (kk + (long)Nk * x))]; };
+    auto Eijk = [&](int sh, int jj, int kk, int x) {
+        return inEijk[sh + 6 * (jj + (long)(Nj + 1) * (kk + (long)(Nk + 1) * x))];
+    };
+    const long nVg = 3L * 4 * Nj * Nk, nVp = 3L * nIonP * b.Njp * b.Nkp, nEe = 2L * Nj * Nk;
+    std::vector<double> tab(nVg + nVp + nEe, 0.0);
+    double* Vg = tab.data();
+    double* Vp = Vg + nVg;
+    double* Ee = Vp + nVp;
+    // ghost cells (IonInner, earthcmi.F90:466-528 with CellPlasmaBC): the
+    // E x B velocity of shell 5-n at the ghost cell's centre (k wrapped),
+    // perpendicular to the radius plus its inward radial part
+    for (int kk = 0; kk < Nk; kk++)
+        for (int jj = 0; jj < Nj; jj++) {
+            int kp = kk;
+            if (kk < G) kp = kk + b.Nkp;
+            else if (kk >= G + b.Nkp) kp = kk - b.Nkp;
+            for (int n = 1; n <= 4; n++) {
+                double r[3], B[3], rh[3], E[3], v[3], vr;
+                X(G - n, jj, kp, r);
+                ion_dipole(M0, r, B);
+                for (int x = 0; x < 3; x++) E[x] = Exyz(4 - n, jj, kp, x);
+                norm_vec(r, rh);
+                ion_exb_perp(E, B, rh, v, &vr);
+                const double vin = std::min(vr, 0.0);
+                double* o = Vg + 3 * ((n - 1) + 4 * ((long)jj + (long)Nj * kk));
+                for (int x = 0; x < 3; x++) o[x] = v[x] + vin * rh[x];
+            }
+        }
+    // PushIon's target velocity (earthcmi.F90:618-630): shell 5's E x B in
+    // the dipole at the cell centre, perpendicular to the radius
+    for (int kk = G; kk < G + b.Nkp; kk++)
+        for (int jj = G; jj < G + b.Njp; jj++)
+            for (int ii = G; ii < G + nIonP; ii++) {
+                double r[3], B[3], rh[3], E[3], vr;
+                X(ii, jj, kk, r);
+                ion_dipole(M0, r, B);
+                for (int x = 0; x < 3; x++) E[x] = Exyz(4, jj, kk, x);
+                norm_vec(r, rh);
+                ion_exb_perp(E, B, rh, Vp + 3 * ((ii - G) + (long)nIonP * ((jj - G) + (long)b.Njp * (kk - G))), &vr);
+            }
+    // IonEFix (msphutils.F90:225-238): edge x inEijk(5) on the first shell
+    for (int kk = 0; kk < Nk; kk++)
+        for (int jj = 0; jj < Nj; jj++) {
+            const long row = jj + (long)(Nj + 1) * kk, q = jj + (long)Nj * kk;
+            Ee[2 * q] = el[row] * Eijk(4, jj, kk, 1);
+            Ee[2 * q + 1] = el[nrow + row] * Eijk(4, jj, kk, 2);
+        }
+    if ((long)tab.size() > h->ionCap) {
+        cudaError_t e = cudaSuccess;
+        h->ionTab = dalloc<double>(h, (long)tab.size(), &e);
+        if (e != cudaSuccess) return fail(h, GAM_ECUDA, "device allocation failed");
+        h->ionCap = (long)tab.size();
+    }
+    CK(h, cudaMemcpyAsync(h->ionTab, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice, h->s));
+    CK(h, cudaStreamSynchronize(h->s));
+    IonData I{};
+    I.push = doIonPush ? 1 : 0;
+    I.nIonP = nIonP;
+    I.dtCpl = dtCpl;
+    I.Vg = h->ionTab;
+    I.Vp = h->ionTab + nVg;
+    I.Ee = h->ionTab + nVg + nVp;
+    h->cd.P.ion = I;
+    h->cf.P.ion = I;
+    h->ionDtSW0 = dtSW0;
+    drop_graphs(h);
+    h->haveIon = true;
+    // the wind side of the hooks, now or when the constant wind is set
+    if (windHooks && h->haveWind) return ion_wind_tables(h);
     return GAM_OK;
 }
 

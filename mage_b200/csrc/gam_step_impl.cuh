@@ -1040,8 +1040,11 @@ __global__ void __launch_bounds__(128, MINB) k_update_cells(GamBox b, DevParams<
         }
         // dt range isDT..ieDT = is-1..ie+1 (init.F90:511-530, single domain);
         // evaluated before the stores so that none of its loads waits on them
+        // (PushIon and NudgeSW change the first shells and the last one after
+        // the update: their dt is taken after them, by k_ion_push / k_nudge_sw)
         const bool indt = ii >= G - 1 && ii <= G + b.Nip && jj >= G - 1 && jj <= G + b.Njp && kk >= G - P.dtKlo &&
-                          kk <= G + b.Nkp - 1 + P.dtKhi;
+                          kk <= G + b.Nkp - 1 + P.dtKhi && !(P.ion.push && active && ii < G + P.ion.nIonP) &&
+                          !(P.ion.wind && active && ii == G + b.Nip - 1);
         if (indt && !sc->fixedTimestep) {
             double Ud[5], Bt[3];
 #pragma unroll
@@ -1067,6 +1070,224 @@ __global__ void __launch_bounds__(128, MINB) k_update_cells(GamBox b, DevParams<
     const int lane = (threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z)) & 31;
     const int wid = (threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z)) >> 5;
     const int nw = (blockDim.x * blockDim.y * blockDim.z + 31) >> 5;
+    if (lane == 0) smin[wid] = mydt;
+    unsigned anybad = __syncthreads_or(bad ? 1 : 0);
+    if (wid == 0) {
+        double v = lane < nw ? smin[lane] : HUGE_DT;
+        for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+        if (lane == 0) {
+            if (v < HUGE_DT) atomicMin(&sc->dtmin_bits, dbits(v));
+            if (anybad) atomicAdd(&sc->nbad, 1);
+        }
+    }
+}
+
+// ---- model hooks of the ionospheric boundary (bc[0] = 7; earthcmi.F90)
+// HackE, first part: IonEFix (msphutils.F90:214-240), the J and K EMFs of
+// the first shell i = is over jsg..jeg, ksg..keg from the coupling field
+// (edge length x inEijk(5), formed on the host)
+template <class R>
+__global__ void __launch_bounds__(256) k_ion_efix(GamBox b, DevParams<R> P, Work<R> w, const GamScalars* sc) {
+    if (sc->halted) return;
+    const long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (q >= (long)b.Nj * b.Nk) return;
+    const int jj = (int)(q % b.Nj), kk = (int)(q / b.Nj);
+    const long c = lidx(b, GAM_NG, jj, kk);
+    GAM_BOX_CHECK(c, c, 15);
+    w.E[b.fs + c] = (R)P.ion.Ee[2 * q];
+    w.E[2 * b.fs + c] = (R)P.ion.Ee[2 * q + 1];
+}
+// HackE, last part: FixEFieldLFM (gamdebug.F90:149-175), the I and J EMFs
+// of k = ks and ke+1 set to their mean, i = is..ie+1, j = js..je+1
+template <class R>
+__global__ void __launch_bounds__(256) k_fix_e_lfm(GamBox b, Work<R> w, const GamScalars* sc) {
+    if (sc->halted) return;
+    const int G = GAM_NG;
+    const long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    const int ni = b.Nip + 1;
+    if (q >= (long)ni * (b.Njp + 1)) return;
+    const int ii = G + (int)(q % ni), jj = G + (int)(q / ni);
+    const long c0 = lidx(b, ii, jj, G), c1 = lidx(b, ii, jj, G + b.Nkp);
+    GAM_BOX_CHECK(c0, c1, 15);
+    const long fs = b.fs;
+    const R Ei = (R)0.5 * (w.E[c0] + w.E[c1]);
+    const R Ej = (R)0.5 * (w.E[fs + c0] + w.E[fs + c1]);
+    w.E[c0] = Ei;
+    w.E[c1] = Ei;
+    w.E[fs + c0] = Ej;
+    w.E[fs + c1] = Ej;
+}
+// HackStep: PushIon (earthcmi.F90:586-663) on the first nIonP active
+// shells after the update, then CalcDT's CellDT of those cells (k_update_cells
+// leaves them out) into the step's dt minimum
+template <class R, bool BORIS>
+__global__ void __launch_bounds__(128) k_ion_push(GamBox b, DevParams<R> P, Geo<R> g, StateBuf<R> nxt,
+                                                  GamScalars* sc, double gamma_d, double gm1_d) {
+    __shared__ double smin[32];
+    if (sc->halted) return;
+    const int G = GAM_NG;
+    const long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    const int np = P.ion.nIonP;
+    double mydt = HUGE_DT;
+    bool bad = false;
+    if (q < (long)np * b.Njp * b.Nkp) {
+        const int ii = G + (int)(q % np);
+        const long r = q / np;
+        const int jj = G + (int)(r % b.Njp), kk = G + (int)(r / b.Njp);
+        const long fs = b.fs, c = lidx(b, ii, jj, kk);
+        GAM_BOX_CHECK(c, c, 15);
+        R U[5], W[5];
+#pragma unroll
+        for (int v = 0; v < 5; v++) U[v] = nxt.Gas[v * fs + c];
+        if (!(U[0] < (R)0)) {  // RhoMin(BLK) = 0
+            cell_c2p(P, U, W);
+            const int dN = ii - G + 1;
+            double f = sc->dt / ((double)dN * P.ion.dtCpl);
+            f = (1.0 < f) ? 1.0 : f;  // min(dt, 1.0)
+            const R fr = (R)f;
+            const double* Vp = P.ion.Vp + 3 * q;
+#pragma unroll
+            for (int x = 0; x < 3; x++) {
+                const R dV = (R)Vp[x] - W[1 + x];
+                W[1 + x] = W[1 + x] + fr * dV;
+            }
+            cell_p2c(P, W, U);
+#pragma unroll
+            for (int v = 0; v < 5; v++) nxt.Gas[v * fs + c] = U[v];
+        }
+        if (!sc->fixedTimestep) {
+            double Ud[5], Bt[3];
+#pragma unroll
+            for (int v = 0; v < 5; v++) Ud[v] = (double)U[v];
+#pragma unroll
+            for (int x = 0; x < 3; x++) {
+                Bt[x] = (double)nxt.B[x * fs + c];
+                if (P.doBackground) Bt[x] = Bt[x] + g.B0[x * fs + c];
+            }
+            const double dtc = cell_dt<R, BORIS>(P, Ud, Bt, (double)g.dl[c], gamma_d, gm1_d, sc->CFL);
+            if (dtc > 0.0 && dtc < 1.0e300) mydt = dtc;
+            else bad = true;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) mydt = fmin(mydt, __shfl_xor_sync(0xffffffffu, mydt, o));
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    if (lane == 0) smin[wid] = mydt;
+    unsigned anybad = __syncthreads_or(bad ? 1 : 0);
+    if (wid == 0) {
+        double v = lane < nw ? smin[lane] : HUGE_DT;
+        for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+        if (lane == 0) {
+            if (v < HUGE_DT) atomicMin(&sc->dtmin_bits, dbits(v));
+            if (anybad) atomicAdd(&sc->nbad, 1);
+        }
+    }
+}
+
+// HackE, wind part: WindEFix (apps/wind.F90:489-566), the EMFs of shells
+// ie-2..ie+1 blended with the wind's (weights and wind EMFs formed on the
+// host), then DiffuseOuter (:570-616) on the outermost, from State n's fluxes
+template <class R>
+__global__ void __launch_bounds__(256) k_wind_efix(GamBox b, DevParams<R> P, Geo<R> g, StateBuf<R> S, Work<R> w,
+                                                   const GamScalars* sc) {
+    if (sc->halted) return;
+    const int G = GAM_NG;
+    const long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (q >= 4L * (b.Njp + 1) * (b.Nkp + 1)) return;
+    const int sh = (int)(q & 3);
+    const long r = q >> 2;
+    const int jj = G + (int)(r % (b.Njp + 1)), kk = G + (int)(r / (b.Njp + 1));
+    const int ii = G + b.Nip - 3 + sh;
+    const long fs = b.fs, c = lidx(b, ii, jj, kk);
+    GAM_BOX_CHECK(c - b.sk, c, 15);
+    const double* t = P.ion.We + 7 * q;
+    // CalcElecField starts every step from E = 0 (fields.F90:88): the edges it
+    // does not compute (I edges at ie+1, J edges at je+1, K edges at ke+1) hold
+    // zero when the wind blends into them; here they hold last step's blend
+    const bool computed[3] = {ii < G + b.Nip, jj < G + b.Njp, kk < G + b.Nkp};
+#pragma unroll
+    for (int n = 0; n < 3; n++) {
+        const R mhdE = computed[n] ? w.E[n * fs + c] : (R)0;
+        if (t[n] >= 0.0) {
+            const R wSW = (R)t[n];
+            w.E[n * fs + c] = ((R)1 - wSW) * mhdE + wSW * (R)t[3 + n];
+        } else {
+            w.E[n * fs + c] = mhdE;
+        }
+    }
+    if (sh != 3) return;
+    const long sj = b.sx, sk = b.sk;
+    const R* mf = S.mf;
+    const R* fa = g.face;
+    R bP = mf[fs + c] / rmax(fa[fs + c], (R)TINY);
+    R bM = mf[fs + c - 1] / rmax(fa[fs + c - 1], (R)TINY);
+    R db2 = bP - bM;
+    bP = mf[c] / fa[c];
+    bM = mf[c - sj] / fa[c - sj];
+    R db1 = bP - bM;
+    const R JdK = db2 - db1;
+    bP = mf[c] / fa[c];
+    bM = mf[c - sk] / fa[c - sk];
+    db2 = bP - bM;
+    bP = mf[2 * fs + c] / fa[2 * fs + c];
+    bM = mf[2 * fs + c - 1] / fa[2 * fs + c - 1];
+    db1 = bP - bM;
+    const R JdJ = db2 - db1;
+    const R dl = Mth<R>::sqrt_(g.edge[fs + c] * g.edge[2 * fs + c]);
+    const R Vd = rmin((R)P.ion.vSW, P.CFL * dl / (R)sc->dt);
+    const R Ed[3] = {(R)0, Vd * JdJ * dl, Vd * JdK * dl};
+    const R wK = (R)t[6];
+#pragma unroll
+    for (int x = 0; x < 3; x++) w.E[x * fs + c] = w.E[x * fs + c] + wK * Ed[x];
+}
+// HackStep, wind part: NudgeSW (apps/wind.F90:394-486), the last active cell
+// nudged towards the wind, then its CellDT into the step's dt minimum
+template <class R, bool BORIS>
+__global__ void __launch_bounds__(128) k_nudge_sw(GamBox b, DevParams<R> P, Geo<R> g, StateBuf<R> nxt,
+                                                  GamScalars* sc, double gamma_d, double gm1_d) {
+    __shared__ double smin[32];
+    if (sc->halted) return;
+    const int G = GAM_NG;
+    const long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    double mydt = HUGE_DT;
+    bool bad = false;
+    if (q < (long)b.Njp * b.Nkp) {
+        const int jj = G + (int)(q % b.Njp), kk = G + (int)(q / b.Njp), ii = G + b.Nip - 1;
+        const long fs = b.fs, c = lidx(b, ii, jj, kk);
+        GAM_BOX_CHECK(c, c, 15);
+        R U[5];
+#pragma unroll
+        for (int v = 0; v < 5; v++) U[v] = nxt.Gas[v * fs + c];
+        const double wSW = P.ion.Wn[q];
+        if (wSW > TINY) {
+            const double a = P.ion.dtSW0 / wSW, dt = sc->dt;
+            const double dtSW = (a < dt) ? dt : a;  // max(dtSW0 / wSW, dt)
+            const R f = (R)(dt / dtSW);
+            const double* ws = P.wind.state;
+            const R gWs[5] = {(R)ws[0], (R)ws[2], (R)ws[3], (R)ws[4], (R)ws[1]};
+            R gWm[5], gW[5];
+            cell_c2p(P, U, gWm);
+#pragma unroll
+            for (int v = 0; v < 5; v++) gW[v] = gWm[v] + f * (gWs[v] - gWm[v]);
+            cell_p2c(P, gW, U);
+#pragma unroll
+            for (int v = 0; v < 5; v++) nxt.Gas[v * fs + c] = U[v];
+        }
+        if (!sc->fixedTimestep) {
+            double Ud[5], Bt[3];
+#pragma unroll
+            for (int v = 0; v < 5; v++) Ud[v] = (double)U[v];
+#pragma unroll
+            for (int x = 0; x < 3; x++) {
+                Bt[x] = (double)nxt.B[x * fs + c];
+                if (P.doBackground) Bt[x] = Bt[x] + g.B0[x * fs + c];
+            }
+            const double dtc = cell_dt<R, BORIS>(P, Ud, Bt, (double)g.dl[c], gamma_d, gm1_d, sc->CFL);
+            if (dtc > 0.0 && dtc < 1.0e300) mydt = dtc;
+            else bad = true;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) mydt = fmin(mydt, __shfl_xor_sync(0xffffffffu, mydt, o));
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
     if (lane == 0) smin[wid] = mydt;
     unsigned anybad = __syncthreads_or(bad ? 1 : 0);
     if (wid == 0) {
@@ -1109,7 +1330,8 @@ __global__ void k_dt_finalize(GamScalars* sc) {
 
 // Boundary kinds: 0 periodic, 1 none, 2 zero-gradient, 3 inner sphere,
 // 4 solar wind, 6 uniform inflow (include/gamgpu.h).
-enum { BCK_PERIODIC = 0, BCK_NONE = 1, BCK_ZEROGRAD = 2, BCK_SPHIN = 3, BCK_WIND = 4, BCK_INFLOW = 6 };
+enum { BCK_PERIODIC = 0, BCK_NONE = 1, BCK_ZEROGRAD = 2, BCK_SPHIN = 3, BCK_WIND = 4, BCK_HALO = 5, BCK_INFLOW = 6,
+       BCK_ION = 7 };
 
 // Gather maps of the boundary conditions that copy values (bcs.F90:279-450
 // periodic, :799-892 zero-gradient, :934-957 SphIn). x is the box index along
@@ -1271,6 +1493,33 @@ __global__ void __launch_bounds__(256) k_bc_iside(GamBox b, DevParams<R> P, Geo<
 #pragma unroll
         for (int x = 0; x < 3; x++) s.B[x * fs + dst] = s.B[x * fs + src];
     }
+    if (P.bc[0] == BCK_ION) {
+        // IonInner (earthcmi.F90:441-583) with CellPlasmaBC (msphingest.F90:
+        // 268-372, single fluid, no ingestion): density and pressure of the
+        // mirror cell is+n-1 (k wrapped, lfmIJKcc ringutils.F90:482-518), the
+        // velocity of the table; zero flux through the ghost layer's faces
+        // (isGoodFaceIJK ranges, gridutils.F90:985-1015)
+        const long cg = lidx(b, G - n, jj, kk);
+        if (cellJK) {
+            int kp = kk;
+            if (kk < G) kp = kk + b.Nkp;
+            else if (kk >= G + b.Nkp) kp = kk - b.Nkp;
+            const long src = lidx(b, G + n - 1, jj, kp);
+            GAM_BOX_CHECK(src, src, 14);
+            R pU[5], pW[5], gC[5];
+#pragma unroll
+            for (int v = 0; v < 5; v++) pU[v] = s.Gas[v * fs + src];
+            cell_c2p(P, pU, pW);
+            const double* V = P.ion.Vg + 3 * ((n - 1) + 4 * ((long)jj + (long)b.Nj * kk));
+            const R gW[5] = {pW[0], (R)V[0], (R)V[1], (R)V[2], pW[4]};
+            cell_p2c(P, gW, gC);
+#pragma unroll
+            for (int v = 0; v < 5; v++) s.Gas[v * fs + cg] = gC[v];
+        }
+        if (jj < b.Nj && kk < b.Nk) s.mf[cg] = (R)0;
+        if (jj <= b.Nj && kk < b.Nk) s.mf[fs + cg] = (R)0;
+        if (jj < b.Nj && kk <= b.Nk) s.mf[2 * fs + cg] = (R)0;
+    }
     if (P.bc[0] == BCK_INFLOW && cellJK) {
         const double* w = P.inflow;
         R gW[5] = {(R)w[0], (R)w[2], (R)w[3], (R)w[4], (R)w[1]}, gC[5];
@@ -1392,7 +1641,7 @@ __global__ void __launch_bounds__(256) k_bc_iside(GamBox b, DevParams<R> P, Geo<
 // new fluxes: ig = ie + n (outer) or is - n (inner)
 template <class R>
 __global__ void __launch_bounds__(256) k_bc_iside_b(GamBox b, Geo<R> g, StateBuf<R> s, const GamScalars* sc,
-                                                    int outer) {
+                                                    int outer, int wrapk = 0) {
     if (sc->halted) return;
     const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
     const int n = 1 + (int)(t & 3);
@@ -1400,10 +1649,18 @@ __global__ void __launch_bounds__(256) k_bc_iside_b(GamBox b, Geo<R> g, StateBuf
     const int jj = (int)(q % b.Nj), kk = (int)(q / b.Nj);
     if (kk >= b.Nk) return;
     const long fs = b.fs;
-    const long c = lidx(b, outer ? GAM_NG + b.Nip - 1 + n : GAM_NG - n, jj, kk);
-    GAM_BOX_CHECK(c, c + b.sk, 14);
+    const int ii = outer ? GAM_NG + b.Nip - 1 + n : GAM_NG - n;
+    const long c = lidx(b, ii, jj, kk);
+    // the ionospheric boundary takes the field of the k-wrapped cell
+    // (IonInner's CellBxyz of lfmIJKcc's cell, earthcmi.F90:530-543)
+    int kp = kk;
+    if (wrapk && kk < GAM_NG) kp = kk + b.Nkp;
+    else if (wrapk && kk >= GAM_NG + b.Nkp) kp = kk - b.Nkp;
+    const long cs = lidx(b, ii, jj, kp);
+    GAM_BOX_CHECK(cs, cs + b.sk, 14);
     R B[3];
-    cell_bxyz(b, g, c, s.mf[c], s.mf[c + 1], s.mf[fs + c], s.mf[fs + c + b.sx], s.mf[2 * fs + c], s.mf[2 * fs + c + b.sk], B);
+    cell_bxyz(b, g, cs, s.mf[cs], s.mf[cs + 1], s.mf[fs + cs], s.mf[fs + cs + b.sx], s.mf[2 * fs + cs],
+              s.mf[2 * fs + cs + b.sk], B);
 #pragma unroll
     for (int x = 0; x < 3; x++) s.B[x * fs + c] = B[x];
 }
@@ -1537,8 +1794,8 @@ __global__ void __launch_bounds__(256) k_bc(GamBox b, DevParams<R> P, Geo<R> g, 
 // All boundary conditions of one EnforceBCs (+ final bFlux2Fld unless copyB).
 template <class R> void launch_bcs(const Ctx<R>& C, const StateBuf<R>& S, cudaStream_t s, int copyB) {
     const GamBox& b = C.b;
-    const bool iside = C.P.bc[0] == BCK_SPHIN || C.P.bc[0] == BCK_INFLOW || C.P.bc[1] == BCK_WIND ||
-                       C.P.bc[1] == BCK_ZEROGRAD;
+    const bool iside = C.P.bc[0] == BCK_SPHIN || C.P.bc[0] == BCK_INFLOW || C.P.bc[0] == BCK_ION ||
+                       C.P.bc[1] == BCK_WIND || C.P.bc[1] == BCK_ZEROGRAD;
     if (iside) {
         const long n = 4L * (b.Nj + 1) * (b.Nk + 1);
         k_bc_iside<R><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(b, C.P, C.g, S, C.sc);
@@ -1550,6 +1807,8 @@ template <class R> void launch_bcs(const Ctx<R>& C, const StateBuf<R>& S, cudaSt
             k_bc_iside_b<R><<<(unsigned)((m + 255) / 256), 256, 0, s>>>(b, C.g, S, C.sc, 1);
         if (C.P.bc[0] == BCK_INFLOW && copyB)
             k_bc_iside_b<R><<<(unsigned)((m + 255) / 256), 256, 0, s>>>(b, C.g, S, C.sc, 0);
+        if (C.P.bc[0] == BCK_ION && copyB)
+            k_bc_iside_b<R><<<(unsigned)((m + 255) / 256), 256, 0, s>>>(b, C.g, S, C.sc, 0, 1);
     }
     const Shell sh = make_shell(b);
     const long nsh = sh.nA + sh.nB + sh.nC;
@@ -1688,7 +1947,19 @@ template <class R, class F> void for_each_kernel(const Ctx<R>& C, int cur, cudaS
     f(8, [&] { stress(std::integral_constant<int, 0>()); });
     f(9, [&] { stress(std::integral_constant<int, 1>()); });
     if (!C.P.do25D) f(10, [&] { stress(std::integral_constant<int, 2>()); });
-    f(11, [&] { k_update_faces<R><<<grid_for(all, blk), blk, 0, s>>>(b, C.P, S, O, C.w, C.sc, C.oomf); });
+    f(11, [&] {
+        if (C.P.bc[0] == BCK_ION && C.P.doMHD) {  // HackE (EFix, earthcmi.F90:321-354)
+            const long ne = (long)b.Nj * b.Nk, nf = (long)(b.Nip + 1) * (b.Njp + 1);
+            k_ion_efix<R><<<(unsigned)((ne + 255) / 256), 256, 0, s>>>(b, C.P, C.w, C.sc);
+            if (C.P.ion.wind) {
+                const long nw = 4L * (b.Njp + 1) * (b.Nkp + 1);
+                k_wind_efix<R><<<(unsigned)((nw + 255) / 256), 256, 0, s>>>(b, C.P, C.g, S, C.w, C.sc);
+            }
+            if (C.P.bc[4] != BCK_HALO)
+                k_fix_e_lfm<R><<<(unsigned)((nf + 255) / 256), 256, 0, s>>>(b, C.w, C.sc);
+        }
+        k_update_faces<R><<<grid_for(all, blk), blk, 0, s>>>(b, C.P, S, O, C.w, C.sc, C.oomf);
+    });
     f(12, [&] {
         if (C.P.doBoris)
             k_update_cells<R, sizeof(R) == 8 ? 6 : 8, true><<<grid_for(cells, blk), blk, 0, s>>>(b, C.P, C.g, S, O, C.w, C.sc, C.gamma, C.gm1);
@@ -1696,6 +1967,20 @@ template <class R, class F> void for_each_kernel(const Ctx<R>& C, int cur, cudaS
             k_update_cells<R, 1><<<grid_for(cells, blk), blk, 0, s>>>(b, C.P, C.g, S, O, C.w, C.sc, C.gamma, C.gm1);
         else
             k_update_cells<R, 8><<<grid_for(cells, blk), blk, 0, s>>>(b, C.P, C.g, S, O, C.w, C.sc, C.gamma, C.gm1);
+        if (C.P.ion.push) {  // HackStep (PerStep, earthcmi.F90:224-263): PushIon, before CalcDT
+            const long np = (long)C.P.ion.nIonP * b.Njp * b.Nkp;
+            if (C.P.doBoris)
+                k_ion_push<R, true><<<(unsigned)((np + 127) / 128), 128, 0, s>>>(b, C.P, C.g, O, C.sc, C.gamma, C.gm1);
+            else
+                k_ion_push<R, false><<<(unsigned)((np + 127) / 128), 128, 0, s>>>(b, C.P, C.g, O, C.sc, C.gamma, C.gm1);
+        }
+        if (C.P.ion.wind) {  // HackStep, wind part: NudgeSW
+            const long nn = (long)b.Njp * b.Nkp;
+            if (C.P.doBoris)
+                k_nudge_sw<R, true><<<(unsigned)((nn + 127) / 128), 128, 0, s>>>(b, C.P, C.g, O, C.sc, C.gamma, C.gm1);
+            else
+                k_nudge_sw<R, false><<<(unsigned)((nn + 127) / 128), 128, 0, s>>>(b, C.P, C.g, O, C.sc, C.gamma, C.gm1);
+        }
     });
     f(13, [&] { k_dt_finalize<<<1, 1, 0, s>>>(C.sc); });
     f(14, [&] { launch_bcs(C, O, s, 0); });

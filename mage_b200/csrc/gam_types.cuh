@@ -21,6 +21,24 @@ struct WindData {
     const double* ts;
 };
 
+// The ionospheric inner boundary (bc[0] = 7) and its model hooks: tables
+// computed on the host from the coupling fields (gam_set_ionosphere)
+struct IonData {
+    int push, nIonP;   // PushIon on the first nIonP active shells
+    double dtCpl;      // coupling time scale (code time)
+    const double* Vg;  // ghost-cell velocity, 3 per (n-1) + 4 (jj + Nj kk), n = 1..4
+    const double* Vp;  // PushIon's target velocity, 3 per (ii - G) + nIonP ((jj - G) + Njp (kk - G))
+    const double* Ee;  // the first shell's J and K EMFs (IonEFix), 2 per jj + Nj kk
+    // the wind's part (bc[1] = 4, constant wind): WindEFix and NudgeSW
+    int wind;          // 1: apply them
+    double vSW;        // DiffuseOuter's speed min(|vFr|, Ca)
+    double dtSW0;      // NudgeSW's time scale
+    const double* We;  // 7 per s + 4 (jj - G + (Njp+1) (kk - G)), s = 0..3 for i = ie-2+s: the blend
+                       // weight of the I, J, K edges (negative: unchanged), their wind EMF, and
+                       // DiffuseOuter's weight
+    const double* Wn;  // NudgeSW's weight of the last active cell, per (jj - G) + Njp (kk - G)
+};
+
 template <class R> struct DevParams {
     R gamma, gm1, CFL, pdmb, Vd0, cHogH, cHogM, dFloor, pFloor;
     int doMHD, doLFMLim, do25D, doBackground, up7;
@@ -33,6 +51,7 @@ template <class R> struct DevParams {
     int dtKlo, dtKhi;
     WindData wind;
     double inflow[8];  // uniform inner-I inflow (bc[0] = 6): rho, P, Vx, Vy, Vz, Bx, By, Bz
+    IonData ion;       // ionospheric inner boundary and its hooks (bc[0] = 7)
 };
 
 template <class R> struct Geo {  // Grid_T arrays on the device (gamtypes.F90:168-250)

@@ -12,7 +12,8 @@ module gamgpu
                                  GAM_EDT_BAD = 4, GAM_EDT_DISASTER = 5, GAM_ESTATE = 6, GAM_EHOOK = 7, &
                                  GAM_EBOUNDS = 8
     integer(c_int), parameter :: GAM_BC_PERIODIC = 0, GAM_BC_NONE = 1, GAM_BC_ZEROGRAD = 2, GAM_BC_SPHIN = 3, &
-                                 GAM_BC_WIND = 4, GAM_BC_HALO = 5, GAM_BC_INFLOW = 6
+                                 GAM_BC_WIND = 4, GAM_BC_HALO = 5, GAM_BC_INFLOW = 6, &
+                                 GAM_BC_ION = 7
     integer(c_int), parameter :: GAM_RECON_8CENT = 0, GAM_RECON_7UP = 1
     integer(c_int), parameter :: GAM_FP64 = 0, GAM_FP32 = 1
 
@@ -342,6 +343,14 @@ module gamgpu
             type(c_ptr), intent(in) :: geo(9), st(4), dnxt(3), dst(4)
             type(c_ptr), value :: bg, work, stream
             real(c_double), value :: dt, odt
+        end function
+        integer(c_int) function gam_set_ionosphere(h, inExyz, inEijk, M0, dtCpl, doIonPush, nIonP, dtSW0) &
+                bind(C, name="gam_set_ionosphere")
+            import :: c_int, c_ptr, c_double, c_int32_t
+            type(c_ptr), value :: h
+            real(c_double), intent(in) :: inExyz(*), inEijk(*)
+            real(c_double), value :: M0, dtCpl, dtSW0
+            integer(c_int32_t), value :: doIonPush, nIonP
         end function
         integer(c_int) function gam_iside_fill(p, fp32, geo, is, B, Gas, mf, stream) &
                 bind(C, name="gam_iside_fill")

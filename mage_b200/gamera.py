@@ -24,7 +24,7 @@ LIB_PATH = os.path.join(HERE, "libgamgpu.so")
 CHECK_LIB_PATH = os.path.join(HERE, "libgamgpu_check.so")
 
 GAM_OK, GAM_EINVAL, GAM_EBADDIM, GAM_ECUDA, GAM_EDT_BAD, GAM_EDT_DISASTER, GAM_ESTATE, GAM_EHOOK, GAM_EBOUNDS = range(9)
-BC_PERIODIC, BC_NONE, BC_ZEROGRAD, BC_SPHIN, BC_WIND, BC_HALO, BC_INFLOW = 0, 1, 2, 3, 4, 5, 6
+BC_PERIODIC, BC_NONE, BC_ZEROGRAD, BC_SPHIN, BC_WIND, BC_HALO, BC_INFLOW, BC_ION = 0, 1, 2, 3, 4, 5, 6, 7
 RECON_8CENT, RECON_7UP = 0, 1
 FP64, FP32 = 0, 1
 
@@ -63,7 +63,8 @@ EXPORTED = (
     "gam_set_geometry_arrays", "gam_get_geometry_arrays", "gam_upload_state", "gam_download_state", "gam_step",
     "gam_calc_dt", "gam_divb", "gam_totals", "gam_last_step_ms", "gam_advance_model", "gam_init_orszag_tang",
     "gam_init_blast_wave", "gam_profile_step", "gam_totals_noalloc", "gam_set_background", "gam_get_background",
-    "gam_set_background_dipole", "gam_set_wind", "gam_set_wind_series", "gam_init_test_problem", "gam_set_inflow", "gam_set_oostate", "gam_get_oostate", "gam_bounds_status", "gam_init_dipole_wind", "gam_write_restart", "gam_read_restart",
+    "gam_set_background_dipole", "gam_set_wind", "gam_set_wind_series", "gam_init_test_problem", "gam_set_inflow",
+    "gam_set_ionosphere", "gam_set_oostate", "gam_get_oostate", "gam_bounds_status", "gam_init_dipole_wind", "gam_write_restart", "gam_read_restart",
     "gam_halo_bytes", "gam_halo_pack", "gam_halo_unpack", "gam_init_finish_halo", "gam_set_start", "gam_step_begin",
     "gam_dt_partial", "gam_step_end", "gam_set_slab_edges", "gam_set_stream", "gam_step_begin_dev",
     "gam_dt_partial_dev", "gam_step_end_dev", "gam_step_status", "gam_flux_forward", "gam_flux_adjoint",
@@ -112,6 +113,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     L.gam_set_background_dipole.argtypes = [C.c_void_p, C.c_double]
     L.gam_set_wind.argtypes = [C.c_void_p, _dp]
     L.gam_set_inflow.argtypes = [C.c_void_p, _dp]
+    L.gam_set_ionosphere.argtypes = [C.c_void_p, _dp, _dp, C.c_double, C.c_double, C.c_int32, C.c_int32, C.c_double]
     L.gam_init_test_problem.argtypes = [C.c_void_p, C.c_int32, C.c_double, C.c_double]
     L.gam_set_wind_series.argtypes = [C.c_void_p, C.c_int32] + [_dp] * 6 + [C.c_double] * 3
     L.gam_set_oostate.argtypes = [C.c_void_p, _dp, C.c_double]
@@ -375,6 +377,19 @@ class GameraGPU:
         w = np.ascontiguousarray(state, dtype=np.float64)
         assert w.shape == (8,)
         self._check(self.L.gam_set_inflow(self.h, _ptr(w)))
+
+    def set_ionosphere(self, inExyz, inEijk, M0: float, dtCpl: float = 0.0, doIonPush: bool = True, nIonP: int = 1,
+                       dtSW0: float = 60.0 / 63.8):
+        """Coupling fields of the ionospheric inner boundary (bc[0] = BC_ION):
+        inExyz (3, Nk+8, Nj+8, 5) and inEijk (3, Nk+9, Nj+9, 6) in C order,
+        i.e. the Fortran arrays (1:5, jsg:jeg, ksg:keg, 1:3) and
+        (1:6, jsg:jeg+1, ksg:keg+1, 1:3); M0 the dipole moment; dtCpl the
+        coupling time scale of PushIon and dtSW0 that of NudgeSW (code time;
+        60 s in Earth units, the reference's one minute, is the default)."""
+        E = np.ascontiguousarray(inExyz, dtype=np.float64)
+        Ee = np.ascontiguousarray(inEijk, dtype=np.float64)
+        self._check(self.L.gam_set_ionosphere(self.h, _ptr(E), _ptr(Ee), float(M0), float(dtCpl),
+                                              int(bool(doIonPush)), int(nIonP), float(dtSW0)))
 
     def init_dipole_wind(self, wind, seed: int = 31337, amp: float = 0.01):
         """Wind state with a seeded density perturbation and the wind's uniform field."""

@@ -67,7 +67,7 @@ static const int SgnLR[2] = {-1, 1};  // stress.F90:19
 
 // boundary kinds (a subset of bcs.F90 / apps/wind.F90; BC_INFLOW is a uniform
 // inflow of this library, with no counterpart in the reference)
-enum { BC_PERIODIC = 0, BC_NONE = 1, BC_ZEROGRAD = 2, BC_SPHIN = 3, BC_WIND = 4, BC_INFLOW = 6 };
+enum { BC_PERIODIC = 0, BC_NONE = 1, BC_ZEROGRAD = 2, BC_SPHIN = 3, BC_WIND = 4, BC_INFLOW = 6, BC_ION = 7 };
 
 // interpolation weights, recon.F90:22-23,28-29
 static double interpWgt[8], interpWgt6[8], Up7C[7];
@@ -145,6 +145,16 @@ struct Model {
         std::vector<double> tW, Q, B, xyzBS;  // Q: n x (D, Vx, Vy, Vz, P); B, xyzBS: n x 3
         double tMin = 0, tMax = 0, dtW = 0, Bx0 = 0, ByC = 0, BzC = 0;
     } ws;
+    // ionospheric inner boundary (IonInnerBC_T, voltron/ICs/earthcmi.F90:33-48)
+    // and the magnetosphere hooks that come with it (EFix, PerStep)
+    struct Ion {
+        std::vector<double> inExyz;  // (1:PsiSh, jsg:jeg, ksg:keg, 1:3), PsiSh = 5 (cmidefs.F90:13)
+        std::vector<double> inEijk;  // (1:PsiSh+1, jsg:jeg+1, ksg:keg+1, 1:3)
+        double M0 = 0.0, dtCpl = 0.0;
+        bool doIonPush = true;
+        int nIonP = 1;
+        double dtSW0 = 0.0;  // NudgeSW's time scale: one minute of the wind series (apps/wind.F90:414)
+    } ion;
 };
 
 struct Grid {
@@ -1061,10 +1071,12 @@ static void zeroGrad_obcJ(const Grid& G, State& S);
 static void WindBC(const Model& M, const Grid& G, State& S);
 static void InflowBC(const Model& M, const Grid& G, State& S);
 static void zeroGrad_obcI(const Grid& G, State& S);
+static void IonInner(const Model& M, const Grid& G, State& S);
 static void EnforceBCs(const Model& M, const Grid& G, State& S) {
     if (G.bc[0] == BC_PERIODIC) periodic_ibcI(G, S);
     else if (G.bc[0] == BC_SPHIN) SphIn(G, S);
     else if (G.bc[0] == BC_INFLOW) InflowBC(M, G, S);
+    else if (G.bc[0] == BC_ION) IonInner(M, G, S);
     if (G.bc[1] == BC_PERIODIC) periodic_obcI(G, S);
     else if (G.bc[1] == BC_WIND) WindBC(M, G, S);
     else if (G.bc[1] == BC_ZEROGRAD) zeroGrad_obcI(G, S);
@@ -1074,6 +1086,237 @@ static void EnforceBCs(const Model& M, const Grid& G, State& S) {
     else if (G.bc[3] == BC_ZEROGRAD) zeroGrad_obcJ(G, S);
     if (G.bc[4] == BC_PERIODIC) periodic_ibcK(M, G, S);
     if (G.bc[5] == BC_PERIODIC) periodic_obcK(M, G, S);
+}
+
+
+// ---------------------------------------------------------------- ionosphere
+// The ionospheric inner boundary of the magnetosphere and its model hooks,
+// as voltron/ICs/earthcmi.F90 sets them up (the reference's default Voltron
+// IC file), for a grid without rings (Model%Ring%doS = doE = F): PsiSh = 5,
+// PsiSt = -3 (cmidefs.F90:13-14); single fluid, no ingestion.
+static const int PsiSh = 5, PsiSt = -3;
+static double inExyz(const Model& M, const Grid& G, int s, int j, int k, int x) {  // s = 1..PsiSh
+    const long nj = G.jeg - G.jsg + 1, nk = G.keg - G.ksg + 1;
+    return M.ion.inExyz[(s - 1) + PsiSh * ((j - G.jsg) + nj * ((k - G.ksg) + nk * x))];
+}
+static double inEijk(const Model& M, const Grid& G, int s, int j, int k, int x) {  // s = 1..PsiSh+1
+    const long nj = G.jeg - G.jsg + 2, nk = G.keg - G.ksg + 2;
+    return M.ion.inEijk[(s - 1) + (PsiSh + 1) * ((j - G.jsg) + nj * ((k - G.ksg) + nk * x))];
+}
+// ringutils.F90:482-518 lfmIJKcc without rings: k into the active range
+static void lfmIJKcc(const Grid& G, int i, int j, int k, int& ip, int& jp, int& kp) {
+    const int Np = G.Nkp;
+    ip = i;
+    if (k < G.ks) kp = k + Np;
+    else if (k > G.ke) kp = k - Np;
+    else kp = k;
+    jp = j;
+}
+// math.F90:265-274 cross, :332-343 normVec, :365-376 Vec2Perp
+static void cross3(const double* a, const double* b, double* c) {
+    c[0] = a[1] * b[2] - a[2] * b[1];
+    c[1] = a[2] * b[0] - a[0] * b[2];
+    c[2] = a[0] * b[1] - a[1] * b[0];
+}
+static void normVec3(const double* a, double* n) {
+    const double nA = std::sqrt(dot3(a, a));
+    for (int x = 0; x < 3; x++) n[x] = nA <= TINY ? 0.0 : a[x] / nA;
+}
+static void Vec2Perp(const double* A, const double* n, double* P) {
+    const double d = dot3(A, n);
+    for (int x = 0; x < 3; x++) P[x] = A[x] - d * n[x];
+}
+static void Dipole(double M0, const double* r, double* A);
+// E x B / |B|^2 in the dipole at xyz (earthcmi.F90:484-490, 624-629)
+static void ExB(const Model& M, const double* xyz, const double* E, double* Veb) {
+    double Bd[3], c[3];
+    Dipole(M.ion.M0, xyz, Bd);
+    cross3(E, Bd, c);
+    const double bb = dot3(Bd, Bd);
+    for (int x = 0; x < 3; x++) Veb[x] = c[x] / bb;
+}
+// msphingest.F90:268-372 CellPlasmaBC, single fluid without ingestion data:
+// the active cell's density and pressure, the E x B velocity perpendicular
+// to the radius plus the inward part of its radial component
+static void CellPlasmaBC(const Model& M, double* gU, const double* pU, const double* Veb, const double* rHat) {
+    double pW[5], gW[5] = {0, 0, 0, 0, 0}, Vp[3];
+    const double Vr = dot3(Veb, rHat);
+    CellC2P(M, pU, pW);
+    gW[DEN] = pW[DEN];
+    gW[PRESSURE] = pW[PRESSURE];
+    Vec2Perp(Veb, rHat, Vp);
+    const double vin = std::min(Vr, 0.0);
+    for (int x = 0; x < 3; x++) gW[VELX + x] = Vp[x] + vin * rHat[x];
+    CellP2C(M, gW, gU);
+}
+// earthcmi.F90:441-583 IonInner (rings off)
+static void IonInner(const Model& M, const Grid& G, State& S) {
+    for (int k = G.ksg; k <= G.keg + 1; k++)
+        for (int j = G.jsg; j <= G.jeg + 1; j++)
+            for (int n = 1; n <= 4; n++) {
+                const int ig = G.is - n, ip = G.is + n - 1, np = 4 - n + 1;
+                if (k <= G.keg && j <= G.jeg) {  // isCellCenterG
+                    int idip, jp, kp;
+                    lfmIJKcc(G, ig, j, k, idip, jp, kp);
+                    const double xc[3] = {G.xyzcc(idip, jp, kp, XDIR), G.xyzcc(idip, jp, kp, YDIR),
+                                          G.xyzcc(idip, jp, kp, ZDIR)};
+                    const double E[3] = {inExyz(M, G, np, jp, kp, 0), inExyz(M, G, np, jp, kp, 1),
+                                         inExyz(M, G, np, jp, kp, 2)};
+                    double Veb[3], rHat[3], gU[5], pU[5];
+                    ExB(M, xc, E, Veb);
+                    normVec3(xc, rHat);
+                    for (int v = 0; v < NVAR; v++) pU[v] = S.Gas(ip, jp, kp, v);
+                    CellPlasmaBC(M, gU, pU, Veb, rHat);
+                    for (int v = 0; v < NVAR; v++) S.Gas(ig, j, k, v) = gU[v];
+                }
+                // isGoodFaceIJK (gridutils.F90:985-1015): the faces of the box
+                if (j <= G.jeg && k <= G.keg) S.magFlux(ig, j, k, IDIR) = 0.0;
+                if (k <= G.keg) S.magFlux(ig, j, k, JDIR) = 0.0;
+                if (j <= G.jeg) S.magFlux(ig, j, k, KDIR) = 0.0;
+            }
+    // Bxyz of each ghost from the fluxes of its conjugate cell (:530-543)
+    for (int k = G.ksg; k <= G.keg; k++)
+        for (int j = G.jsg; j <= G.jeg; j++)
+            for (int n = 1; n <= 4; n++) {
+                const int ig = G.is - n;
+                int ip, jp, kp;
+                lfmIJKcc(G, ig, j, k, ip, jp, kp);
+                double B[3];
+                gamCellBxyz(G, S.magFlux, ip, jp, kp, B);
+                for (int x = 0; x < 3; x++) S.Bxyz(ig, j, k, x) = B[x];
+            }
+}
+// HackE = EFix (earthcmi.F90:321-354): IonEFix (msphutils.F90:214-240),
+// WindEFix with the wind outside (below), then FixEFieldLFM
+// (gamdebug.F90:149-175)
+static void IonEFix(const Model& M, const Grid& G, State& S) {
+    if (PsiSh + PsiSt >= 1) {  // the inner tile holds shell is = 1
+        const int is0 = 1 - PsiSt + 1;
+        for (int k = G.ksg; k <= G.keg; k++)
+            for (int j = G.jsg; j <= G.jeg; j++) {
+                S.Efld(G.is, j, k, JDIR) = G.edge(G.is, j, k, JDIR) * inEijk(M, G, is0, j, k, 1);
+                S.Efld(G.is, j, k, KDIR) = G.edge(G.is, j, k, KDIR) * inEijk(M, G, is0, j, k, 2);
+            }
+    }
+}
+static void FixEFieldLFM(const Grid& G, F4& E) {
+    for (int j = G.js; j <= G.je + 1; j++)
+        for (int i = G.is; i <= G.ie + 1; i++) {
+            const double Ei = 0.5 * (E(i, j, G.ks, IDIR) + E(i, j, G.ke + 1, IDIR));
+            const double Ej = 0.5 * (E(i, j, G.ks, JDIR) + E(i, j, G.ke + 1, JDIR));
+            E(i, j, G.ks, IDIR) = Ei;
+            E(i, j, G.ke + 1, IDIR) = Ei;
+            E(i, j, G.ks, JDIR) = Ej;
+            E(i, j, G.ke + 1, JDIR) = Ej;
+        }
+}
+// HackStep = PerStep (earthcmi.F90:224-263): PushIon (:586-663), then
+// NudgeSW with the wind outside (below)
+static void PushIon(const Model& M, const Grid& G, State& S) {
+    for (int k = G.ks; k <= G.ke; k++)
+        for (int j = G.js; j <= G.je; j++)
+            for (int i = G.is; i <= G.is + M.ion.nIonP - 1; i++) {
+                const double xcc[3] = {G.xyzcc(i, j, k, XDIR), G.xyzcc(i, j, k, YDIR), G.xyzcc(i, j, k, ZDIR)};
+                const double E[3] = {inExyz(M, G, PsiSh, j, k, 0), inExyz(M, G, PsiSh, j, k, 1),
+                                     inExyz(M, G, PsiSh, j, k, 2)};
+                double Veb[3], rHat[3], Vp[3], pCon[5], pW[5];
+                ExB(M, xcc, E, Veb);
+                normVec3(xcc, rHat);
+                Vec2Perp(Veb, rHat, Vp);
+                for (int v = 0; v < NVAR; v++) pCon[v] = S.Gas(i, j, k, v);
+                CellC2P(M, pCon, pW);
+                if (pCon[DEN] < 0.0) continue;  // RhoMin(BLK) = 0
+                const int dN = i - G.is + 1;
+                double dt = M.dt / (dN * M.ion.dtCpl);
+                dt = std::min(dt, 1.0);
+                for (int x = 0; x < 3; x++) {
+                    const double dV = Vp[x] - pW[VELX + x];
+                    pW[VELX + x] = pW[VELX + x] + dt * dV;
+                }
+                CellP2C(M, pW, pCon);
+                for (int v = 0; v < NVAR; v++) S.Gas(i, j, k, v) = pCon[v];
+            }
+}
+
+// The wind's part of the same hooks, for the constant wind (a series of
+// constant rows with ByC = BzC = 0, so RefreshWind's front velocity is
+// (-|V|, 0, 0)): WindEFix (apps/wind.F90:489-566) with DiffuseOuter
+// (:570-616, doSWDiffuse = T) in HackE, NudgeSW (:394-486) in HackStep.
+static double wgtWind(const double* V, const double* xyz);
+static void DiffuseOuter(const Model& M, const Grid& G, const State& S, int i, int j, int k, double vSW, double* Ed) {
+    double Jd[3] = {0.0, 0.0, 0.0};
+    double bP = S.magFlux(i, j, k, JDIR) / std::max(G.face(i, j, k, JDIR), TINY);
+    double bM = S.magFlux(i - 1, j, k, JDIR) / std::max(G.face(i - 1, j, k, JDIR), TINY);
+    double db2 = bP - bM;
+    bP = S.magFlux(i, j, k, IDIR) / G.face(i, j, k, IDIR);
+    bM = S.magFlux(i, j - 1, k, IDIR) / G.face(i, j - 1, k, IDIR);
+    double db1 = bP - bM;
+    Jd[KDIR] = db2 - db1;
+    bP = S.magFlux(i, j, k, IDIR) / G.face(i, j, k, IDIR);
+    bM = S.magFlux(i, j, k - 1, IDIR) / G.face(i, j, k - 1, IDIR);
+    db2 = bP - bM;
+    bP = S.magFlux(i, j, k, KDIR) / G.face(i, j, k, KDIR);
+    bM = S.magFlux(i - 1, j, k, KDIR) / G.face(i - 1, j, k, KDIR);
+    db1 = bP - bM;
+    Jd[JDIR] = db2 - db1;
+    const double dl = std::sqrt(G.edge(i, j, k, JDIR) * G.edge(i, j, k, KDIR));
+    const double Vd = std::min(vSW, M.CFL * dl / M.dt);
+    Ed[IDIR] = 0.0;
+    Ed[JDIR] = Vd * Jd[JDIR] * dl;
+    Ed[KDIR] = Vd * Jd[KDIR] * dl;
+}
+static void WindEFix(const Model& M, const Grid& G, State& S) {
+    const double V[3] = {M.wind[2], M.wind[3], M.wind[4]}, B[3] = {M.wind[5], M.wind[6], M.wind[7]};
+    const double vFr[3] = {-norm2s(V, 3), 0.0, 0.0};
+    const double vSW = std::min(norm2s(vFr, 3), M.doBoris ? M.Ca : HUGE_);
+    double c[3], swE[3];
+    cross3(V, B, c);
+    for (int x = 0; x < 3; x++) swE[x] = -c[x];
+    for (int k = G.ks; k <= G.ke + 1; k++)
+        for (int j = G.js; j <= G.je + 1; j++)
+            for (int i = G.ie - 2; i <= G.ie + 1; i++) {
+                double wSW = 0.0;
+                for (int n = 0; n < 3; n++) {
+                    const int i2 = n == IDIR ? i + 1 : i, j2 = n == JDIR ? j + 1 : j, k2 = n == KDIR ? k + 1 : k;
+                    double e1[3], e2[3], ecc[3], de[3];
+                    for (int x = 0; x < 3; x++) {
+                        e1[x] = G.xyz(i, j, k, x);
+                        e2[x] = G.xyz(i2, j2, k2, x);
+                        ecc[x] = 0.5 * (e1[x] + e2[x]);
+                        de[x] = e2[x] - e1[x];
+                    }
+                    wSW = wgtWind(V, ecc);
+                    if (wSW > TINY) {
+                        if (i <= G.ie) wSW = wSW / (1.0 + G.ie + 1 - i);
+                        const double mhdE = S.Efld(i, j, k, n);
+                        S.Efld(i, j, k, n) = (1.0 - wSW) * mhdE + wSW * dot3(swE, de);
+                    }
+                }
+                if (i == G.ie + 1) {
+                    double Ed[3];
+                    DiffuseOuter(M, G, S, i, j, k, vSW, Ed);
+                    for (int x = 0; x < 3; x++) S.Efld(i, j, k, x) = S.Efld(i, j, k, x) + wSW * Ed[x];
+                }
+            }
+}
+static void NudgeSW(const Model& M, const Grid& G, State& S) {
+    const double V[3] = {M.wind[2], M.wind[3], M.wind[4]};
+    const int ip = G.ie;
+    for (int k = G.ks; k <= G.ke; k++)
+        for (int j = G.js; j <= G.je; j++) {
+            const double xcc[3] = {G.xyzcc(ip, j, k, XDIR), G.xyzcc(ip, j, k, YDIR), G.xyzcc(ip, j, k, ZDIR)};
+            const double wSW = wgtWind(V, xcc);
+            if (wSW > TINY) {
+                const double dtSW = std::max(M.ion.dtSW0 / wSW, M.dt);
+                const double gW_sw[5] = {M.wind[0], M.wind[2], M.wind[3], M.wind[4], M.wind[1]};
+                double gCon[5], gW_mhd[5], gW[5];
+                for (int v = 0; v < NVAR; v++) gCon[v] = S.Gas(ip, j, k, v);
+                CellC2P(M, gCon, gW_mhd);
+                for (int v = 0; v < NVAR; v++) gW[v] = gW_mhd[v] + (M.dt / dtSW) * (gW_sw[v] - gW_mhd[v]);
+                CellP2C(M, gW, gCon);
+                for (int v = 0; v < NVAR; v++) S.Gas(ip, j, k, v) = gCon[v];
+            }
+        }
 }
 
 // ---------------------------------------------------------------- dt
@@ -2065,13 +2308,24 @@ static void allocState(const Grid& G, State& S) {
 static void AdvanceMHD(App& A, double dt) {
     if (std::fabs(A.oS.time - A.S.time) < TINY) A.oS.time = A.S.time - A.M.dt;
     Predictor(A.M, A.G, A.S, A.oS, A.ooS, A.hS, 0.5 * dt);
-    if (A.M.doMHD) CalcElecField(A.M, A.G, A.S, A.hS, A.Vf, A.S.Efld);
+    if (A.M.doMHD) {
+        CalcElecField(A.M, A.G, A.S, A.hS, A.Vf, A.S.Efld);
+        if (A.G.bc[0] == BC_ION) {  // HackE
+            IonEFix(A.M, A.G, A.S);
+            if (A.G.bc[1] == BC_WIND) WindEFix(A.M, A.G, A.S);
+            FixEFieldLFM(A.G, A.S.Efld);
+        }
+    }
     CalcStress(A.M, A.G, A.S, A.hS, A.gFlx, A.mFlx, A.dGasH, A.dGasM);
     applyUpdate(A.M, A.G, A.S, A.oS, A.ooS, dt, A.dGasH, A.dGasM, A.S.Efld);
 }
 // gamapp.F90:73-113 stepGamera + UpdateStateData
 static int stepGamera(App& A) {
     AdvanceMHD(A, A.M.dt);
+    if (A.G.bc[0] == BC_ION) {  // HackStep
+        if (A.M.ion.doIonPush) PushIon(A.M, A.G, A.S);
+        if (A.G.bc[1] == BC_WIND) NudgeSW(A.M, A.G, A.S);
+    }
     A.M.ts = A.M.ts + 1;
     A.M.t = A.M.t + A.M.dt;
     int st;
@@ -2144,6 +2398,21 @@ void* orc_create(const Params* p, const double* xyz) {
 }
 
 void orc_destroy(void* h) { delete (App*)h; }
+
+// the coupling fields and settings of the ionospheric inner boundary
+void orc_set_ionosphere(void* h, const double* inE, const double* inEe, double M0, double dtCpl, int doIonPush,
+                        int nIonP, double dtSW0) {
+    App* A = (App*)h;
+    const Grid& G = A->G;
+    const long nj = G.jeg - G.jsg + 1, nk = G.keg - G.ksg + 1;
+    A->M.ion.inExyz.assign(inE, inE + PsiSh * nj * nk * 3);
+    A->M.ion.inEijk.assign(inEe, inEe + (PsiSh + 1) * (nj + 1) * (nk + 1) * 3);
+    A->M.ion.M0 = M0;
+    A->M.ion.dtCpl = dtCpl;
+    A->M.ion.doIonPush = doIonPush != 0;
+    A->M.ion.nIonP = nIonP;
+    A->M.ion.dtSW0 = dtSW0;
+}
 
 // Pointers to internal Fortran-ordered arrays, for numpy views.
 // which: 0 Gas,1 magFlux,2 Bxyz,3 oGas,4 omagFlux,5 oBxyz,6 xyzcc,7 xfc,8 volume,

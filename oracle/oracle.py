@@ -144,6 +144,8 @@ def lib(variant: str = "strict") -> C.CDLL:
         L.orc_num_threads.restype = C.c_int
         L.orc_ic_case.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double]
         L.orc_set_wind_series.argtypes = [C.c_void_p, C.c_int] + [C.POINTER(C.c_double)] * 6 + [C.c_double] * 3
+        L.orc_set_ionosphere.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_double,
+                                         C.c_double, C.c_int, C.c_int, C.c_double]
         _libs[variant] = L
     return _libs[variant]
 
@@ -222,6 +224,18 @@ class Oracle:
         self._ws = arrs + [xb]
         self.L.orc_set_wind_series(self.h, len(arrs[0]), *[_dptr(a) for a in arrs], None if xb is None else _dptr(xb),
                                    Bx0, ByC, BzC)
+
+    def set_ionosphere(self, inExyz, inEijk, M0: float, dtCpl: float, doIonPush: bool = True, nIonP: int = 1,
+                       dtSW0: float = 60.0 / 63.8):
+        """Coupling fields of the ionospheric inner boundary (bc[0] = 7):
+        inExyz (3, Nk+8, Nj+8, 5) and inEijk (3, Nk+9, Nj+9, 6), the C-order
+        views of the Fortran arrays (1:5, jsg:jeg, ksg:keg, 1:3) and
+        (1:6, jsg:jeg+1, ksg:keg+1, 1:3); dtSW0 NudgeSW's time scale (code
+        time; the reference's one minute in Earth units)."""
+        self._ionE = np.ascontiguousarray(inExyz, dtype=np.float64)
+        self._ionEe = np.ascontiguousarray(inEijk, dtype=np.float64)
+        self.L.orc_set_ionosphere(self.h, _dptr(self._ionE), _dptr(self._ionEe), float(M0), float(dtCpl),
+                                  int(bool(doIonPush)), int(nIonP), float(dtSW0))
 
     def divb(self) -> float:
         return self.L.orc_divb(self.h)
