@@ -42,7 +42,8 @@ enum {
  * GAM_BC_SPHIN (bcs.F90:934-957) or GAM_BC_INFLOW; OUTI periodic, none,
  * GAM_BC_WIND (constant solar wind, apps/wind.F90:206-391) or GAM_BC_ZEROGRAD
  * (zeroGrad_obcI, bcs.F90:820-850); INJ/OUTJ periodic, none or
- * GAM_BC_ZEROGRAD (bcs.F90:853-892); INK/OUTK periodic or none.
+ * GAM_BC_ZEROGRAD (bcs.F90:853-892); INK/OUTK periodic or none. Any side of
+ * a tile may be GAM_BC_HALO instead (filled by the caller's halo exchange).
  * GAM_BC_INFLOW has no counterpart in the reference: the 4 inner-I ghost
  * layers hold a uniform state (gam_set_inflow) and the face fluxes of its
  * field, the shape of zeroGrad_obcI with a given state in place of the last
@@ -50,7 +51,7 @@ enum {
  * magnetosphere (IonInnerBC_T, voltron/ICs/earthcmi.F90:441-583) together
  * with the model hooks that come with it (gam_set_ionosphere). */
 enum { GAM_BC_PERIODIC = 0, GAM_BC_NONE = 1, GAM_BC_ZEROGRAD = 2, GAM_BC_SPHIN = 3, GAM_BC_WIND = 4,
-       GAM_BC_HALO = 5 /* INK and OUTK of a k-slab: filled by the caller's halo exchange */,
+       GAM_BC_HALO = 5 /* a tile's side towards a neighbour: filled by the caller's halo exchange */,
        GAM_BC_INFLOW = 6, GAM_BC_ION = 7 };
 enum { GAM_RECON_8CENT = 0, GAM_RECON_7UP = 1 };
 enum { GAM_FP64 = 0, GAM_FP32 = 1 };
@@ -250,7 +251,15 @@ int gam_set_inflow(gam_handle* h, const double state[8]);
  * (the reference's one minute, 60 s / gT0). Needs the geometry and, with the
  * wind outside, gam_set_wind first (a wind time series is refused); call
  * before the initial condition, again whenever the coupler updates the
- * fields, and after every gam_set_wind. */
+ * fields, and after every gam_set_wind. Also sets CalcDT's range to the
+ * active cells (isDT..ieDT = is..ie, earthcmi.F90:136-142).
+ * A tile of the magnetosphere away from the inner boundary (bc[0] =
+ * GAM_BC_HALO) calls it too, with inExyz = inEijk = NULL: it takes the hooks
+ * of its other sides (WindEFix and NudgeSW if its outer side is the wind,
+ * FixEFieldLFM) and the DT range, as every rank of the reference's MPI run
+ * does (EFix and PerStep test hasLowerBC / hasUpperBC). The k boundaries must
+ * be periodic (the reference stops on a k decomposition of the magnetosphere,
+ * earthcmi.F90:145-148). */
 int gam_set_ionosphere(gam_handle* h, const double* inExyz, const double* inEijk, double M0, double dtCpl,
                        int32_t doIonPush, int32_t nIonP, double dtSW0);
 
@@ -291,27 +300,42 @@ int gam_init_dipole_wind(gam_handle* h, const double wind[8], uint64_t seed, dou
 int gam_write_restart(gam_handle* h, const char* path);
 int gam_read_restart(gam_handle* h, const char* path);
 
-/* k-slab tiling (the MPI step of gamAppMpi_T, gamapp_mpi.F90:495-782, for a
- * decomposition along k; one handle per GPU, bc[4] = bc[5] = GAM_BC_HALO).
- * A step is
+/* Tiling (the MPI step of gamAppMpi_T, gamapp_mpi.F90:495-782): the grid cut
+ * into tiles along i, j and k, one handle per tile (per GPU), with
+ * GAM_BC_HALO on every side that faces a neighbour (both sides of a periodic
+ * direction that is cut) and the grid's own boundary kinds on the others.
+ * The functions named gam_halo_* / gam_set_slab_edges are the k-direction
+ * forms kept for k-slabs (dir = 2). A step is
  *   gam_step_begin(h)                      predictor .. cell update
  *   gam_dt_partial(h, &bits, &nbad)        this slab's dt candidate
  *   (caller: min of bits and sum of nbad over all slabs, e.g. an NCCL
  *    all-reduce; bits are the IEEE-754 bits of a positive double, so the
  *    integer min is the double min)
  *   gam_step_end(h, bits, nbad, &dt, &t)   dt decision, local boundaries
- *   gam_halo_pack(h, 0|1, buf) / send / receive / gam_halo_unpack(h, 0|1, buf, 0)
- * Side 0 of a pack is what goes down to the slab below (it fills that slab's
- * side-1 ghosts), side 1 what goes up. Buffers are device memory of
- * gam_halo_bytes bytes; pack and unpack return after their kernels finished.
- * After a gam_init_*: exchange with copyB = 1 (Bxyz copied, like the first
- * EnforceBCs), then gam_init_finish_halo (oState = State, this slab's CalcDT),
- * min over slabs, gam_set_start(h, dt). With one slab that sends to itself the
- * result equals the periodic single-domain step bit for bit. */
-/* Whether this slab is the lowest / highest in k: CalcDT's range (isDT..ieDT =
- * is-1..ie+1, init.F90:511-530) takes the ghost layer below / above only on
- * the grid's own edges, not where a neighbour's cells are. Call before the
- * gam_init_* of the slab (default: both, as for the whole grid). */
+ *   for dir = 0 (I), then 1 (J), then 2 (K), over the halo sides of dir:
+ *     gam_tile_halo_pack(h, dir, 0|1, buf) / send / receive /
+ *     gam_tile_halo_unpack(h, dir, 0|1, buf, 0)
+ * Side 0 of a pack is what goes down to the tile below in dir (it fills that
+ * tile's side-1 ghosts), side 1 what goes up. A pack covers the 4 layers next
+ * to that side across the whole ghosted extent of the other two directions,
+ * so exchanging the directions in turn, each after the previous one has been
+ * unpacked on every tile, also fills the edge and corner ghosts. Buffers are
+ * device memory of gam_tile_halo_bytes bytes; pack and unpack return after
+ * their kernels finished. A pack or unpack of a side that is not a halo is
+ * GAM_ESTATE. After a gam_init_*: exchange with copyB = 1 (Bxyz copied, like
+ * the first EnforceBCs), then gam_init_finish_halo (oState = State, this
+ * tile's CalcDT), min over tiles, gam_set_start(h, dt). Alternatively upload
+ * a whole state with its ghosts (gam_upload_state). The tiles' states equal
+ * the single grid's bit for bit, ghosts included. */
+int gam_tile_halo_bytes(gam_handle* h, int32_t dir, int64_t* bytes);
+int gam_tile_halo_pack(gam_handle* h, int32_t dir, int32_t side, void* dev_buf);
+int gam_tile_halo_unpack(gam_handle* h, int32_t dir, int32_t side, const void* dev_buf, int32_t copyB);
+/* Whether this tile is the lowest / highest in dir: CalcDT's range (isDT..ieDT
+ * = is-1..ie+1, init.F90:511-530) takes the ghost layer below / above only on
+ * the grid's own edges, not where a neighbour's cells are (and nowhere under
+ * the magnetosphere's bounds). Call before the tile's gam_init_* (default:
+ * both, as for the whole grid). */
+int gam_set_tile_edges(gam_handle* h, int32_t dir, int32_t lowest, int32_t highest);
 int gam_set_slab_edges(gam_handle* h, int32_t lowest, int32_t highest);
 int gam_halo_bytes(gam_handle* h, int64_t* bytes);
 int gam_halo_pack(gam_handle* h, int32_t side, void* dev_buf);
@@ -322,7 +346,7 @@ int gam_step_begin(gam_handle* h);
 int gam_dt_partial(gam_handle* h, uint64_t* dtmin_bits, int32_t* nbad);
 int gam_step_end(gam_handle* h, uint64_t dtmin_bits, int32_t nbad, double* dt, double* t);
 
-/* The same k-slab step without host round trips, for a caller that reduces
+/* The same tile step without host round trips, for a caller that reduces
  * on the device (an NCCL all-reduce of device buffers); the dt AllReduce(MIN)
  * of gamapp_mpi.F90:495-512 then never leaves the GPUs.
  *   gam_set_stream(h, stream)           enqueue all of this handle's work on

@@ -1404,6 +1404,7 @@ template <class R> DevParams<R> dev_params(const gam_params* p) {
     P.up7 = p->rmeth == GAM_RECON_7UP;
     for (int n = 0; n < 6; n++) P.bc[n] = p->bc[n];
     P.dtKlo = P.dtKhi = 1;
+    P.dtIlo = P.dtIhi = P.dtJlo = P.dtJhi = 1;
     return P;
 }
 template <class R>

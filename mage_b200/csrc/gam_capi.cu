@@ -27,9 +27,9 @@ void gam_fast_prepare_f64();
 void gam_fast_phase_f64(const Ctx<double>& C, int cur, cudaStream_t s, int phase);
 void gam_fast_phase_f32(const Ctx<float>& C, int cur, cudaStream_t s, int phase);
 void gam_strict_phase_f64(const Ctx<double>& C, int cur, cudaStream_t s, int phase);
-void gam_fast_halo_f64(const Ctx<double>& C, int cur, cudaStream_t s, int side, int unpack, int copyB, void* buf);
-void gam_fast_halo_f32(const Ctx<float>& C, int cur, cudaStream_t s, int side, int unpack, int copyB, void* buf);
-void gam_strict_halo_f64(const Ctx<double>& C, int cur, cudaStream_t s, int side, int unpack, int copyB, void* buf);
+void gam_fast_halo_f64(const Ctx<double>& C, int cur, cudaStream_t s, int dside, int unpack, int copyB, void* buf);
+void gam_fast_halo_f32(const Ctx<float>& C, int cur, cudaStream_t s, int dside, int unpack, int copyB, void* buf);
+void gam_strict_halo_f64(const Ctx<double>& C, int cur, cudaStream_t s, int dside, int unpack, int copyB, void* buf);
 void gam_fast_prepare_f32();
 // set-up (gam_geom.cu)
 void gam_geom_fortran_to_box_d(const GamBox& b, const double* src, double* dst, bool face, int nc, cudaStream_t s);
@@ -86,7 +86,11 @@ struct gam_handle {
     bool haveBg = false, haveWind = false, haveInflow = false, haveIon = false;
     cudaStream_t s = nullptr;
     cudaStream_t own_s = nullptr;  // the handle's own stream (s unless gam_set_stream gave another)
-    int nasync = 0;                // device-resident k-slab steps since the last gam_step_status
+    int nasync = 0;                // device-resident tile steps since the last gam_step_status
+    // per side (I lo, I hi, J lo, J hi, K lo, K hi): the side is an edge of
+    // the whole grid (gam_set_tile_edges), where CalcDT takes the ghost layer
+    int tileEdge[6] = {1, 1, 1, 1, 1, 1};
+    bool dtActive = false;         // CalcDT over the active cells only (the magnetosphere's bounds)
     bool f32 = false;
     std::vector<void*> allocs;
     GeoD gd{};
@@ -98,7 +102,7 @@ struct gam_handle {
     double* partial = nullptr;  // device, reduction partials
     double* dres = nullptr;     // device, reduction results
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
-    cudaGraphExec_t pgraph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [parity][phase] (k-slab steps)
+    cudaGraphExec_t pgraph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [parity][phase] (tile steps)
     int cur = 0;
     bool haveGeo = false, haveState = false, haveXyz = false;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -111,6 +115,11 @@ struct gam_handle {
 static int fail(gam_handle* h, int code, const std::string& msg) {
     if (h) h->err = msg;
     return code;
+}
+static bool is_tile(const gam_handle* h) {
+    for (int n = 0; n < 6; n++)
+        if (h->p.bc[n] == GAM_BC_HALO) return true;
+    return false;
 }
 static int ion_wind_tables(gam_handle* h);
 #define CK(h, call)                                                                            \
@@ -170,6 +179,7 @@ template <class R> static void fill_dev_params(DevParams<R>& P, const gam_params
     P.up7 = p.rmeth == GAM_RECON_7UP;
     for (int n = 0; n < 6; n++) P.bc[n] = p.bc[n];
     P.dtKlo = P.dtKhi = 1;
+    P.dtIlo = P.dtIhi = P.dtJlo = P.dtJhi = 1;
 }
 
 template <class R> static int alloc_bulk(gam_handle* h, Ctx<R>& C) {
@@ -250,20 +260,18 @@ extern "C" int gam_create(const gam_params* p, gam_handle** out) {
     {
         // boundary kinds per side: inner I periodic/none/SphIn/inflow/ionosphere, outer I
         // periodic/none/wind/zero-gradient, J periodic/none/zero-gradient,
-        // K periodic/none (or halo)
+        // K periodic/none; any side of a tile may be a halo instead
         const int* c = p->bc;
-        auto in = [](int v, int a, int b2, int c2) { return v == a || v == b2 || v == c2; };
+        auto in = [](int v, int a, int b2, int c2) { return v == a || v == b2 || v == c2 || v == GAM_BC_HALO; };
         if (!(in(c[0], GAM_BC_PERIODIC, GAM_BC_NONE, GAM_BC_SPHIN) || c[0] == GAM_BC_INFLOW || c[0] == GAM_BC_ION) ||
             !(in(c[1], GAM_BC_PERIODIC, GAM_BC_NONE, GAM_BC_WIND) || c[1] == GAM_BC_ZEROGRAD) ||
             !in(c[2], GAM_BC_PERIODIC, GAM_BC_NONE, GAM_BC_ZEROGRAD) ||
             !in(c[3], GAM_BC_PERIODIC, GAM_BC_NONE, GAM_BC_ZEROGRAD) ||
-            !in(c[4], GAM_BC_PERIODIC, GAM_BC_NONE, GAM_BC_HALO) || !in(c[5], GAM_BC_PERIODIC, GAM_BC_NONE, GAM_BC_HALO))
+            !in(c[4], GAM_BC_PERIODIC, GAM_BC_NONE, GAM_BC_NONE) || !in(c[5], GAM_BC_PERIODIC, GAM_BC_NONE, GAM_BC_NONE))
             return bad(GAM_EINVAL, "unsupported boundary kind for this side");
         for (int d = 0; d < 3; d++)
             if ((c[2 * d] == GAM_BC_PERIODIC) != (c[2 * d + 1] == GAM_BC_PERIODIC))
                 return bad(GAM_EINVAL, "a periodic direction needs both sides periodic");
-        if ((c[4] == GAM_BC_HALO) != (c[5] == GAM_BC_HALO))
-            return bad(GAM_EINVAL, "a k-slab exchanges both k sides");
         if (c[0] == GAM_BC_ION && c[4] != GAM_BC_PERIODIC)
             return bad(GAM_EINVAL, "the ionospheric boundary wraps k: the k boundaries must be periodic");
         if (c[0] == GAM_BC_PERIODIC && (c[2] == GAM_BC_ZEROGRAD || c[3] == GAM_BC_ZEROGRAD))
@@ -668,18 +676,24 @@ extern "C" int gam_bounds_status(gam_handle* h, int32_t* fired, int32_t* kernel,
     return GAM_OK;
 }
 
-extern "C" int gam_step(gam_handle* h, int32_t nsteps, double* dt, double* t) {
-    if (!h || nsteps < 0) return GAM_EINVAL;
+// what a step needs besides the kernels
+static int step_ready(gam_handle* h) {
     if (!h->haveGeo) return fail(h, GAM_ESTATE, "gam_step before gam_set_geometry");
     if (!h->haveState) return fail(h, GAM_ESTATE, "gam_step before gam_upload_state");
     if (h->p.doBackground && !h->haveBg) return fail(h, GAM_ESTATE, "doBackground: set the background field first");
     if (h->p.bc[1] == GAM_BC_WIND && !h->haveWind) return fail(h, GAM_ESTATE, "wind boundary: call gam_set_wind first");
     if (h->p.bc[0] == GAM_BC_INFLOW && !h->haveInflow)
         return fail(h, GAM_ESTATE, "inflow boundary: call gam_set_inflow first");
-    if (h->p.bc[0] == GAM_BC_ION && (!h->haveIon || (h->p.bc[1] == GAM_BC_WIND && !h->cd.P.ion.wind)))
+    if ((h->p.bc[0] == GAM_BC_ION && !h->haveIon) || (h->haveIon && h->p.bc[1] == GAM_BC_WIND && !h->cd.P.ion.wind))
         return fail(h, GAM_ESTATE, "ionospheric boundary: call gam_set_ionosphere (and gam_set_wind) first");
-    if (h->p.bc[4] == GAM_BC_HALO)
-        return fail(h, GAM_ESTATE, "a k-slab steps with gam_step_begin / gam_step_end and a halo exchange");
+    return GAM_OK;
+}
+
+extern "C" int gam_step(gam_handle* h, int32_t nsteps, double* dt, double* t) {
+    if (!h || nsteps < 0) return GAM_EINVAL;
+    if (int rc0 = step_ready(h)) return rc0;
+    if (is_tile(h))
+        return fail(h, GAM_ESTATE, "a tile steps with gam_step_begin / gam_step_end and a halo exchange");
     int rc;
     if ((rc = ensure_graph(h, 0))) return rc;
     if ((rc = ensure_graph(h, 1))) return rc;
@@ -891,9 +905,9 @@ static int init_common(gam_handle* h, double* Gas64, double* mf64) {
     else
         gam_fast_init_f64(h->cd, 0, h->s);
     CK(h, cudaGetLastError());
-    // a k-slab's ghosts arrive with the first halo exchange; the caller
+    // a tile's ghosts arrive with the first halo exchange; the caller
     // finishes with gam_init_finish_halo and gam_set_start
-    if (h->p.bc[4] == GAM_BC_HALO) return GAM_OK;
+    if (is_tile(h)) return GAM_OK;
     double dt;
     rc = gam_calc_dt(h, &dt);
     if (rc) return rc;
@@ -939,11 +953,32 @@ extern "C" int gam_init_blast_wave(gam_handle* h, const double* bw9) {
 
 // ------------------------------------------------------------ background field and solar wind
 static void drop_graphs(gam_handle* h) {
-    for (int q = 0; q < 2; q++)
+    for (int q = 0; q < 2; q++) {
         if (h->graph[q]) {
             cudaGraphExecDestroy(h->graph[q]);
             h->graph[q] = nullptr;
         }
+        for (int ph = 0; ph < 2; ph++)
+            if (h->pgraph[q][ph]) {
+                cudaGraphExecDestroy(h->pgraph[q][ph]);
+                h->pgraph[q][ph] = nullptr;
+            }
+    }
+}
+// CalcDT's range per side: the ghost layer where the side is an edge of the
+// whole grid (SetDomain, init.F90:511-530; a tile's inner sides stop at its
+// active cells, as hasLowerBC / hasUpperBC are false there), the active cells
+// only under the magnetosphere's bounds (earthcmi.F90:136-142)
+static void set_dt_range(gam_handle* h) {
+    int v[6];
+    for (int n = 0; n < 6; n++) v[n] = (h->tileEdge[n] && !h->dtActive) ? 1 : 0;
+    h->cd.P.dtIlo = h->cf.P.dtIlo = v[0];
+    h->cd.P.dtIhi = h->cf.P.dtIhi = v[1];
+    h->cd.P.dtJlo = h->cf.P.dtJlo = v[2];
+    h->cd.P.dtJhi = h->cf.P.dtJhi = v[3];
+    h->cd.P.dtKlo = h->cf.P.dtKlo = v[4];
+    h->cd.P.dtKhi = h->cf.P.dtKhi = v[5];
+    drop_graphs(h);
 }
 
 extern "C" int gam_set_background(gam_handle* h, const double* fcB0, const double* bFlux0, const double* edgB0,
@@ -1076,7 +1111,7 @@ extern "C" int gam_set_wind(gam_handle* h, const double wind[8]) {
     h->cf.P.wind = W;
     drop_graphs(h);
     h->haveWind = true;
-    if (h->p.bc[0] == GAM_BC_ION && h->haveIon) return ion_wind_tables(h);  // the hooks' wind side
+    if (h->haveIon) return ion_wind_tables(h);  // the hooks' wind side
     return GAM_OK;
 }
 
@@ -1273,11 +1308,20 @@ static int ion_wind_tables(gam_handle* h) {
 
 extern "C" int gam_set_ionosphere(gam_handle* h, const double* inExyz, const double* inEijk, double M0, double dtCpl,
                                   int32_t doIonPush, int32_t nIonP, double dtSW0) {
-    if (!h || !inExyz || !inEijk) return GAM_EINVAL;
-    if (h->p.bc[0] != GAM_BC_ION) return fail(h, GAM_ESTATE, "the inner I boundary is not the ionosphere");
+    if (!h) return GAM_EINVAL;
+    // a tile of the magnetosphere away from the inner boundary takes the
+    // hooks of its other sides (WindEFix, NudgeSW, FixEFieldLFM) and the DT
+    // bounds; the inner tile also the boundary itself (hasLowerBC(IDIR))
+    const bool inner = h->p.bc[0] == GAM_BC_ION;
+    if (!inner && h->p.bc[0] != GAM_BC_HALO)
+        return fail(h, GAM_ESTATE, "the inner I boundary is not the ionosphere (nor a tile's halo)");
+    if (h->p.bc[4] != GAM_BC_PERIODIC)
+        return fail(h, GAM_EINVAL, "the magnetosphere's hooks need the whole periodic k range on every tile");
+    if (inner && (!inExyz || !inEijk)) return GAM_EINVAL;
     if (!h->haveGeo) return fail(h, GAM_ESTATE, "set the geometry first");
     const GamBox& b = h->b;
-    if (!doIonPush) nIonP = 0;
+    if (!doIonPush || !inner) nIonP = 0;
+    if (!inner) doIonPush = 0;
     if (doIonPush && (!(dtCpl > 0.0) || nIonP < 1 || nIonP > b.Nip))
         return fail(h, GAM_EINVAL, "PushIon needs dtCpl > 0 and 1 <= nIonP <= Nip");
     const bool windHooks = h->p.bc[1] == GAM_BC_WIND;
@@ -1287,6 +1331,18 @@ extern "C" int gam_set_ionosphere(gam_handle* h, const double* inExyz, const dou
             return fail(h, GAM_ESTATE, "the wind side of the hooks takes the constant wind (gam_set_wind)");
         if (!(dtSW0 > 0.0)) return fail(h, GAM_EINVAL, "NudgeSW needs dtSW0 > 0");
         if (nIonP >= b.Nip) return fail(h, GAM_EINVAL, "PushIon and NudgeSW would act on the same shell");
+    }
+    if (!inner) {
+        IonData I{};
+        I.on = 1;
+        h->cd.P.ion = I;
+        h->cf.P.ion = I;
+        h->ionDtSW0 = dtSW0;
+        h->dtActive = true;
+        set_dt_range(h);
+        h->haveIon = true;
+        if (windHooks && h->haveWind) return ion_wind_tables(h);
+        return GAM_OK;
     }
     const int G = 4, Nj = b.Nj, Nk = b.Nk, ncol = G + nIonP;
     const long nrow = (long)(Nj + 1) * (Nk + 1);
@@ -1364,6 +1420,7 @@ extern "C" int gam_set_ionosphere(gam_handle* h, const double* inExyz, const dou
     CK(h, cudaMemcpyAsync(h->ionTab, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice, h->s));
     CK(h, cudaStreamSynchronize(h->s));
     IonData I{};
+    I.on = 1;
     I.push = doIonPush ? 1 : 0;
     I.nIonP = nIonP;
     I.dtCpl = dtCpl;
@@ -1373,7 +1430,8 @@ extern "C" int gam_set_ionosphere(gam_handle* h, const double* inExyz, const dou
     h->cd.P.ion = I;
     h->cf.P.ion = I;
     h->ionDtSW0 = dtSW0;
-    drop_graphs(h);
+    h->dtActive = true;
+    set_dt_range(h);
     h->haveIon = true;
     // the wind side of the hooks, now or when the constant wind is set
     if (windHooks && h->haveWind) return ion_wind_tables(h);
@@ -1465,7 +1523,7 @@ extern "C" int gam_read_restart(gam_handle* h, const char* path) {
     return GAM_OK;
 }
 
-// ------------------------------------------------------------ k-slab tiling
+// ------------------------------------------------------------ tiles (k-slabs and I/J/K tiles)
 static void launch_phase(gam_handle* h, int cur, int phase) {
     if (h->f32)
         gam_fast_phase_f32(h->cf, cur, h->s, phase);
@@ -1485,34 +1543,46 @@ static int ensure_phase_graph(gam_handle* h, int cur, int phase) {
     return GAM_OK;
 }
 static int require_slab(gam_handle* h) {
-    if (h->p.bc[4] != GAM_BC_HALO) return fail(h, GAM_ESTATE, "the handle is not a k-slab (bc[4] = bc[5] = GAM_BC_HALO)");
+    if (!is_tile(h)) return fail(h, GAM_ESTATE, "the handle is not a tile (no side is GAM_BC_HALO)");
     if (!h->haveGeo || !h->haveState) return fail(h, GAM_ESTATE, "set the geometry and the state first");
     return GAM_OK;
 }
 
-extern "C" int gam_halo_bytes(gam_handle* h, int64_t* bytes) {
-    if (!h || !bytes) return GAM_EINVAL;
-    *bytes = 11L * 4 * (h->b.Ni + 1) * (h->b.Nj + 1) * (h->f32 ? 4 : 8);
+extern "C" int gam_tile_halo_bytes(gam_handle* h, int32_t dir, int64_t* bytes) {
+    if (!h || !bytes || dir < 0 || dir > 2) return GAM_EINVAL;
+    const GamBox& b = h->b;
+    // 11 components x 4 layers x the face-box extents across dir
+    const long nu = dir == 0 ? b.Nj + 1 : b.Ni + 1, nv = dir == 2 ? b.Nj + 1 : b.Nk + 1;
+    *bytes = 11L * 4 * nu * nv * (h->f32 ? 4 : 8);
     return GAM_OK;
 }
+extern "C" int gam_halo_bytes(gam_handle* h, int64_t* bytes) { return gam_tile_halo_bytes(h, 2, bytes); }
 
-static int halo_call(gam_handle* h, int side, int unpack, int copyB, void* buf) {
-    if (!h || !buf || (side != 0 && side != 1)) return GAM_EINVAL;
+static int halo_call(gam_handle* h, int dir, int side, int unpack, int copyB, void* buf) {
+    if (!h || !buf || (side != 0 && side != 1) || dir < 0 || dir > 2) return GAM_EINVAL;
     int rc = require_slab(h);
     if (rc) return rc;
+    if (h->p.bc[2 * dir + side] != GAM_BC_HALO) return fail(h, GAM_ESTATE, "this side of the tile is not a halo");
+    const int dside = side + 2 * dir;
     if (h->f32)
-        gam_fast_halo_f32(h->cf, h->cur, h->s, side, unpack, copyB, buf);
+        gam_fast_halo_f32(h->cf, h->cur, h->s, dside, unpack, copyB, buf);
     else if (h->p.strict)
-        gam_strict_halo_f64(h->cd, h->cur, h->s, side, unpack, copyB, buf);
+        gam_strict_halo_f64(h->cd, h->cur, h->s, dside, unpack, copyB, buf);
     else
-        gam_fast_halo_f64(h->cd, h->cur, h->s, side, unpack, copyB, buf);
+        gam_fast_halo_f64(h->cd, h->cur, h->s, dside, unpack, copyB, buf);
     CK(h, cudaGetLastError());
     if (h->s == h->own_s) CK(h, cudaStreamSynchronize(h->s));
     return GAM_OK;
 }
-extern "C" int gam_halo_pack(gam_handle* h, int32_t side, void* dev_buf) { return halo_call(h, side, 0, 0, dev_buf); }
+extern "C" int gam_tile_halo_pack(gam_handle* h, int32_t dir, int32_t side, void* dev_buf) {
+    return halo_call(h, dir, side, 0, 0, dev_buf);
+}
+extern "C" int gam_tile_halo_unpack(gam_handle* h, int32_t dir, int32_t side, const void* dev_buf, int32_t copyB) {
+    return halo_call(h, dir, side, 1, copyB ? 1 : 0, const_cast<void*>(dev_buf));
+}
+extern "C" int gam_halo_pack(gam_handle* h, int32_t side, void* dev_buf) { return halo_call(h, 2, side, 0, 0, dev_buf); }
 extern "C" int gam_halo_unpack(gam_handle* h, int32_t side, const void* dev_buf, int32_t copyB) {
-    return halo_call(h, side, 1, copyB ? 1 : 0, const_cast<void*>(dev_buf));
+    return halo_call(h, 2, side, 1, copyB ? 1 : 0, const_cast<void*>(dev_buf));
 }
 
 extern "C" int gam_init_finish_halo(gam_handle* h, double* dt_local) {
@@ -1542,7 +1612,7 @@ extern "C" int gam_set_start(gam_handle* h, double dt) {
 extern "C" int gam_step_begin(gam_handle* h) {
     if (!h) return GAM_EINVAL;
     int rc = require_slab(h);
-    if (rc) return rc;
+    if (rc || (rc = step_ready(h))) return rc;
     GamScalars s;
     CK(h, cudaMemcpyAsync(&s, h->sc, sizeof(s), cudaMemcpyDeviceToHost, h->s));
     CK(h, cudaStreamSynchronize(h->s));
@@ -1612,7 +1682,7 @@ extern "C" int gam_set_stream(gam_handle* h, void* stream) {
 extern "C" int gam_step_begin_dev(gam_handle* h) {
     if (!h) return GAM_EINVAL;
     int rc = require_slab(h);
-    if (rc) return rc;
+    if (rc || (rc = step_ready(h))) return rc;
     if ((rc = ensure_phase_graph(h, h->cur, 0))) return rc;
     if ((rc = ensure_phase_graph(h, h->cur, 1))) return rc;
     if (h->nasync == 0) CK(h, cudaEventRecord(h->ev0, h->s));
@@ -1660,17 +1730,14 @@ extern "C" int gam_step_status(gam_handle* h, double* dt, double* t) {
     return GAM_OK;
 }
 
-extern "C" int gam_set_slab_edges(gam_handle* h, int32_t lowest, int32_t highest) {
-    if (!h) return GAM_EINVAL;
-    if (h->p.bc[4] != GAM_BC_HALO) return fail(h, GAM_ESTATE, "the handle is not a k-slab");
-    h->cd.P.dtKlo = h->cf.P.dtKlo = lowest ? 1 : 0;
-    h->cd.P.dtKhi = h->cf.P.dtKhi = highest ? 1 : 0;
-    drop_graphs(h);
-    for (int q = 0; q < 2; q++)
-        for (int ph = 0; ph < 2; ph++)
-            if (h->pgraph[q][ph]) {
-                cudaGraphExecDestroy(h->pgraph[q][ph]);
-                h->pgraph[q][ph] = nullptr;
-            }
+extern "C" int gam_set_tile_edges(gam_handle* h, int32_t dir, int32_t lowest, int32_t highest) {
+    if (!h || dir < 0 || dir > 2) return GAM_EINVAL;
+    if (!is_tile(h)) return fail(h, GAM_ESTATE, "the handle is not a tile");
+    h->tileEdge[2 * dir] = lowest ? 1 : 0;
+    h->tileEdge[2 * dir + 1] = highest ? 1 : 0;
+    set_dt_range(h);
     return GAM_OK;
+}
+extern "C" int gam_set_slab_edges(gam_handle* h, int32_t lowest, int32_t highest) {
+    return gam_set_tile_edges(h, 2, lowest, highest);
 }

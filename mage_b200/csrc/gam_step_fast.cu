@@ -18,6 +18,6 @@ void gam_fast_prepare_f32() { gam_fast::prepare<float>(); }
 void gam_fast_profile_f64(const Ctx<double>& C, int cur, cudaStream_t s, int reps, double* ms) { gam_fast::profile_step<double>(C, cur, s, reps, ms); }
 void gam_fast_profile_f32(const Ctx<float>& C, int cur, cudaStream_t s, int reps, double* ms) { gam_fast::profile_step<float>(C, cur, s, reps, ms); }
 void gam_fast_phase_f64(const Ctx<double>& C, int cur, cudaStream_t s, int phase) { gam_fast::launch_step_phase<double>(C, cur, s, phase); }
-void gam_fast_halo_f64(const Ctx<double>& C, int cur, cudaStream_t s, int side, int unpack, int copyB, void* buf) { gam_fast::launch_halo<double>(C, cur, s, side, unpack, copyB, buf); }
+void gam_fast_halo_f64(const Ctx<double>& C, int cur, cudaStream_t s, int dside, int unpack, int copyB, void* buf) { gam_fast::launch_halo<double>(C, cur, s, dside, unpack, copyB, buf); }
 void gam_fast_phase_f32(const Ctx<float>& C, int cur, cudaStream_t s, int phase) { gam_fast::launch_step_phase<float>(C, cur, s, phase); }
-void gam_fast_halo_f32(const Ctx<float>& C, int cur, cudaStream_t s, int side, int unpack, int copyB, void* buf) { gam_fast::launch_halo<float>(C, cur, s, side, unpack, copyB, buf); }
+void gam_fast_halo_f32(const Ctx<float>& C, int cur, cudaStream_t s, int dside, int unpack, int copyB, void* buf) { gam_fast::launch_halo<float>(C, cur, s, dside, unpack, copyB, buf); }

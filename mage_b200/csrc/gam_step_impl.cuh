@@ -1042,7 +1042,8 @@ __global__ void __launch_bounds__(128, MINB) k_update_cells(GamBox b, DevParams<
         // evaluated before the stores so that none of its loads waits on them
         // (PushIon and NudgeSW change the first shells and the last one after
         // the update: their dt is taken after them, by k_ion_push / k_nudge_sw)
-        const bool indt = ii >= G - 1 && ii <= G + b.Nip && jj >= G - 1 && jj <= G + b.Njp && kk >= G - P.dtKlo &&
+        const bool indt = ii >= G - P.dtIlo && ii <= G + b.Nip - 1 + P.dtIhi && jj >= G - P.dtJlo &&
+                          jj <= G + b.Njp - 1 + P.dtJhi && kk >= G - P.dtKlo &&
                           kk <= G + b.Nkp - 1 + P.dtKhi && !(P.ion.push && active && ii < G + P.ion.nIonP) &&
                           !(P.ion.wind && active && ii == G + b.Nip - 1);
         if (indt && !sc->fixedTimestep) {
@@ -1822,7 +1823,8 @@ __global__ void __launch_bounds__(128) k_dt_only(GamBox b, DevParams<R> P, Geo<R
                                                  GamScalars* sc, double gamma_d, double gm1_d) {
     int ii, jj, kk;
     const int G = GAM_NG;
-    Range r{G - 1, G + b.Nip, G - 1, G + b.Njp, G - P.dtKlo, G + b.Nkp - 1 + P.dtKhi};
+    Range r{G - P.dtIlo, G + b.Nip - 1 + P.dtIhi, G - P.dtJlo, G + b.Njp - 1 + P.dtJhi, G - P.dtKlo,
+            G + b.Nkp - 1 + P.dtKhi};
     double mydt = HUGE_DT;
     if (thread_ijk(r, ii, jj, kk) && GAM_BOX_OK(lidx(b, ii, jj, kk), lidx(b, ii, jj, kk), 13)) {
         const long fs = b.fs;
@@ -1948,9 +1950,10 @@ template <class R, class F> void for_each_kernel(const Ctx<R>& C, int cur, cudaS
     f(9, [&] { stress(std::integral_constant<int, 1>()); });
     if (!C.P.do25D) f(10, [&] { stress(std::integral_constant<int, 2>()); });
     f(11, [&] {
-        if (C.P.bc[0] == BCK_ION && C.P.doMHD) {  // HackE (EFix, earthcmi.F90:321-354)
+        if (C.P.ion.on && C.P.doMHD) {  // HackE (EFix, earthcmi.F90:321-354)
             const long ne = (long)b.Nj * b.Nk, nf = (long)(b.Nip + 1) * (b.Njp + 1);
-            k_ion_efix<R><<<(unsigned)((ne + 255) / 256), 256, 0, s>>>(b, C.P, C.w, C.sc);
+            if (C.P.bc[0] == BCK_ION)  // the inner tile (hasLowerBC(IDIR))
+                k_ion_efix<R><<<(unsigned)((ne + 255) / 256), 256, 0, s>>>(b, C.P, C.w, C.sc);
             if (C.P.ion.wind) {
                 const long nw = 4L * (b.Njp + 1) * (b.Nkp + 1);
                 k_wind_efix<R><<<(unsigned)((nw + 255) / 256), 256, 0, s>>>(b, C.P, C.g, S, C.w, C.sc);
@@ -2079,7 +2082,8 @@ template <class R> void launch_dt_only(const Ctx<R>& C, int cur, cudaStream_t s)
     const GamBox& b = C.b;
     const int G = GAM_NG;
     const dim3 blk(32, 4, 1);
-    const Range r{G - 1, G + b.Nip, G - 1, G + b.Njp, G - C.P.dtKlo, G + b.Nkp - 1 + C.P.dtKhi};
+    const Range r{G - C.P.dtIlo, G + b.Nip - 1 + C.P.dtIhi, G - C.P.dtJlo, G + b.Njp - 1 + C.P.dtJhi,
+                  G - C.P.dtKlo, G + b.Nkp - 1 + C.P.dtKhi};
     k_dt_only<R><<<grid_for(r, blk), blk, 0, s>>>(b, C.P, C.g, C.st[cur], C.sc, C.gamma, C.gm1);
 }
 
@@ -2119,39 +2123,52 @@ template <class R> void launch_step_phase(const Ctx<R>& C, int cur, cudaStream_t
     });
 }
 
-// Halo of a k-slab (the depth-4 exchange of updateMpiBCs/haloUpdate,
-// gamapp_mpi.F90:573-782, for a decomposition along k): 11 components
-// (Gas 0-4, magFlux 5-7, Bxyz 8-10) x 4 layers x the full ghosted i x j
-// extent, element (q, l, jj, ii) at ((q * 4 + l) * (Nj+1) + jj) * (Ni+1) + ii.
-// Pack side 0 = what this domain sends down (cells and I, J faces at
-// k = G..G+3, K faces at G+1..G+4: the neighbour's upper ghosts); side 1 =
-// what it sends up (everything at k = Nkp..Nkp+3: the neighbour's lower
-// ghosts). Unpack side 0 fills this domain's lower ghosts (k = 0..3), side 1
-// its upper ghosts (cells, I and J faces at G+Nkp.., K faces at G+Nkp+1..),
-// the same indices the periodic K rule of bcs.F90:397-450 uses.
-__device__ __forceinline__ int halo_k(const GamBox& b, int side, bool unpack, int q, int l) {
+// Halo of a tile (the depth-4 exchange of updateMpiBCs/haloUpdate,
+// gamapp_mpi.F90:573-782) along direction d (0 I, 1 J, 2 K): 11 components
+// (Gas 0-4, magFlux 5-7, Bxyz 8-10) x 4 layers along d x the full ghosted
+// face-box extents (u, v) of the other two directions (u the lower of the
+// two), element (q, l, v, u) at ((q * 4 + l) * nv + v) * nu + u. Pack side 0
+// = what this tile sends down (cells and the other faces at G..G+3 along d,
+// d-faces at G+1..G+4: the neighbour's upper ghosts); side 1 = what it sends
+// up (everything at Nd..Nd+3: the neighbour's lower ghosts). Unpack side 0
+// fills this tile's lower ghosts (0..3), side 1 its upper ghosts (cells and
+// the other faces at G+Nd.., d-faces at G+Nd+1..), the indices the periodic
+// rules of bcs.F90:279-450 use. Exchanging I, then J, then K with the full
+// extents carries the edge and corner ghosts through the earlier exchanges.
+// The k-slab API's sides are d = 2.
+__device__ __forceinline__ int halo_pos(const GamBox& b, int d, int side, bool unpack, int q, int l) {
     const int G = GAM_NG;
-    const bool kface = q == 7;
-    if (!unpack) return side == 0 ? G + l + (kface ? 1 : 0) : b.Nkp + l;
-    return side == 0 ? l : G + b.Nkp + l + (kface ? 1 : 0);
+    const int Nd = d == 0 ? b.Nip : (d == 1 ? b.Njp : b.Nkp);
+    const bool dface = q == 5 + d;
+    if (!unpack) return side == 0 ? G + l + (dface ? 1 : 0) : Nd + l;
+    return side == 0 ? l : G + Nd + l + (dface ? 1 : 0);
 }
 template <class R> __device__ __forceinline__ R* halo_ptr(const StateBuf<R>& S, long fs, int q) {
     return q < 5 ? S.Gas + (long)q * fs : (q < 8 ? S.mf + (long)(q - 5) * fs : S.B + (long)(q - 8) * fs);
 }
+// face-box extents across direction d: nu (the lower other direction), nv
+__host__ __device__ __forceinline__ void halo_extents(const GamBox& b, int d, long& nu, long& nv) {
+    nu = d == 0 ? b.Nj + 1 : b.Ni + 1;
+    nv = d == 2 ? b.Nj + 1 : b.Nk + 1;
+}
+__device__ __forceinline__ long halo_cell(const GamBox& b, int d, int pos, int u, int v) {
+    return d == 0 ? lidx(b, pos, u, v) : (d == 1 ? lidx(b, u, pos, v) : lidx(b, u, v, pos));
+}
 template <class R>
-__global__ void __launch_bounds__(256) k_halo(GamBox b, StateBuf<R> S, R* __restrict__ buf, int side, int unpack,
-                                              int copyB, const GamScalars* sc) {
+__global__ void __launch_bounds__(256) k_halo(GamBox b, StateBuf<R> S, R* __restrict__ buf, int d, int side,
+                                              int unpack, int copyB, const GamScalars* sc) {
     if (sc->halted) return;  // a failed step keeps its state, ghosts included
-    const long nx = b.Ni + 1, ny = b.Nj + 1;
+    long nu, nv;
+    halo_extents(b, d, nu, nv);
     const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
-    if (t >= 4 * nx * ny) return;
-    const int ii = (int)(t % nx), jj = (int)((t / nx) % ny), l = (int)(t / (nx * ny));
+    if (t >= 4 * nu * nv) return;
+    const int u = (int)(t % nu), v = (int)((t / nu) % nv), l = (int)(t / (nu * nv));
     const long fs = b.fs;
     for (int q = 0; q < 11; q++) {
         if (unpack && q >= 8 && !copyB) break;
-        const long c = lidx(b, ii, jj, halo_k(b, side, unpack != 0, q, l));
+        const long c = halo_cell(b, d, halo_pos(b, d, side, unpack != 0, q, l), u, v);
         GAM_BOX_CHECK(c, c, 15);
-        const long e = ((long)(q * 4 + l) * ny + jj) * nx + ii;
+        const long e = ((long)(q * 4 + l) * nv + v) * nu + u;
         R* p = halo_ptr(S, fs, q);
         if (unpack)
             p[c] = buf[e];
@@ -2161,14 +2178,16 @@ __global__ void __launch_bounds__(256) k_halo(GamBox b, StateBuf<R> S, R* __rest
 }
 // Bxyz of the unpacked ghost cells from their faces (the final bFlux2Fld)
 template <class R>
-__global__ void __launch_bounds__(256) k_halo_bxyz(GamBox b, Geo<R> g, StateBuf<R> S, int side, const GamScalars* sc) {
+__global__ void __launch_bounds__(256) k_halo_bxyz(GamBox b, Geo<R> g, StateBuf<R> S, int d, int side,
+                                                   const GamScalars* sc) {
     if (sc->halted) return;
-    const long nx = b.Ni, ny = b.Nj;
+    const long nu = d == 0 ? b.Nj : b.Ni, nv = d == 2 ? b.Nj : b.Nk;  // cell extents
     const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
-    if (t >= 4 * nx * ny) return;
-    const int ii = (int)(t % nx), jj = (int)((t / nx) % ny), l = (int)(t / (nx * ny));
-    const int kk = side == 0 ? l : GAM_NG + b.Nkp + l;
-    const long fs = b.fs, c = lidx(b, ii, jj, kk);
+    if (t >= 4 * nu * nv) return;
+    const int u = (int)(t % nu), v = (int)((t / nu) % nv), l = (int)(t / (nu * nv));
+    const int Nd = d == 0 ? b.Nip : (d == 1 ? b.Njp : b.Nkp);
+    const int pos = side == 0 ? l : GAM_NG + Nd + l;
+    const long fs = b.fs, c = halo_cell(b, d, pos, u, v);
     GAM_BOX_CHECK(c, c + b.sk, 15);
     R B[3];
     cell_bxyz(b, g, c, S.mf[c], S.mf[c + 1], S.mf[fs + c], S.mf[fs + c + b.sx], S.mf[2 * fs + c],
@@ -2176,14 +2195,18 @@ __global__ void __launch_bounds__(256) k_halo_bxyz(GamBox b, Geo<R> g, StateBuf<
 #pragma unroll
     for (int x = 0; x < 3; x++) S.B[x * fs + c] = B[x];
 }
-template <class R> void launch_halo(const Ctx<R>& C, int cur, cudaStream_t s, int side, int unpack, int copyB, void* buf) {
+// dside = side + 2 d
+template <class R> void launch_halo(const Ctx<R>& C, int cur, cudaStream_t s, int dside, int unpack, int copyB, void* buf) {
     const GamBox& b = C.b;
+    const int d = dside >> 1, side = dside & 1;
     const StateBuf<R> S = C.st[cur];
-    const long n = 4L * (b.Ni + 1) * (b.Nj + 1);
-    k_halo<R><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(b, S, (R*)buf, side, unpack, copyB, C.sc);
+    long nu, nv;
+    halo_extents(b, d, nu, nv);
+    const long n = 4L * nu * nv;
+    k_halo<R><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(b, S, (R*)buf, d, side, unpack, copyB, C.sc);
     if (unpack && !copyB && C.P.doMHD) {
-        const long m = 4L * b.Ni * b.Nj;
-        k_halo_bxyz<R><<<(unsigned)((m + 255) / 256), 256, 0, s>>>(b, C.g, S, side, C.sc);
+        const long m = 4L * (d == 0 ? b.Nj : b.Ni) * (d == 2 ? b.Nj : b.Nk);
+        k_halo_bxyz<R><<<(unsigned)((m + 255) / 256), 256, 0, s>>>(b, C.g, S, d, side, C.sc);
     }
 }
 

@@ -12,4 +12,4 @@ void gam_strict_bfield_f64(const Ctx<double>& C, int cur, cudaStream_t s) { gam_
 void gam_strict_prepare_f64() { gam_strict::prepare<double>(); }
 void gam_strict_profile_f64(const Ctx<double>& C, int cur, cudaStream_t s, int reps, double* ms) { gam_strict::profile_step<double>(C, cur, s, reps, ms); }
 void gam_strict_phase_f64(const Ctx<double>& C, int cur, cudaStream_t s, int phase) { gam_strict::launch_step_phase<double>(C, cur, s, phase); }
-void gam_strict_halo_f64(const Ctx<double>& C, int cur, cudaStream_t s, int side, int unpack, int copyB, void* buf) { gam_strict::launch_halo<double>(C, cur, s, side, unpack, copyB, buf); }
+void gam_strict_halo_f64(const Ctx<double>& C, int cur, cudaStream_t s, int dside, int unpack, int copyB, void* buf) { gam_strict::launch_halo<double>(C, cur, s, dside, unpack, copyB, buf); }

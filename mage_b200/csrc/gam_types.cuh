@@ -24,6 +24,7 @@ struct WindData {
 // The ionospheric inner boundary (bc[0] = 7) and its model hooks: tables
 // computed on the host from the coupling fields (gam_set_ionosphere)
 struct IonData {
+    int on;            // the magnetosphere's hooks (HackE) run on this grid or tile
     int push, nIonP;   // PushIon on the first nIonP active shells
     double dtCpl;      // coupling time scale (code time)
     const double* Vg;  // ghost-cell velocity, 3 per (n-1) + 4 (jj + Nj kk), n = 1..4
@@ -46,9 +47,11 @@ template <class R> struct DevParams {
     double Ca;
     int doAB3;    // third-order (AB3) predictor with ooState (init.F90:377)
     int bc[6];
-    // CalcDT covers the ghost layer below / above the active k range (1, the
-    // reference's isDT..ieDT); a k-slab drops it where a neighbour's cells lie
+    // CalcDT covers the ghost layer below / above the active range per
+    // direction (1, the reference's isDT..ieDT); a tile drops it where a
+    // neighbour's cells lie, the magnetosphere everywhere
     int dtKlo, dtKhi;
+    int dtIlo, dtIhi, dtJlo, dtJhi;
     WindData wind;
     double inflow[8];  // uniform inner-I inflow (bc[0] = 6): rho, P, Vx, Vy, Vz, Bx, By, Bz
     IonData ion;       // ionospheric inner boundary and its hooks (bc[0] = 7)

@@ -164,8 +164,31 @@ module gamgpu
             real(c_double), intent(out) :: oomagFlux(*)
             real(c_double), intent(out) :: ootime
         end function
-        ! k-slab tiling: the MPI driver (gamAppMpi_T) packs/unpacks halos in
-        ! device buffers and reduces dt between gam_step_begin and gam_step_end
+        ! tiling: the MPI driver (gamAppMpi_T) packs/unpacks halos in device
+        ! buffers, direction by direction (I, J, K), and reduces dt between
+        ! gam_step_begin and gam_step_end; the gam_halo_* forms are dir = 2
+        integer(c_int) function gam_set_tile_edges(h, dir, lowest, highest) bind(C, name="gam_set_tile_edges")
+            import :: c_int, c_ptr, c_int32_t
+            type(c_ptr), value :: h
+            integer(c_int32_t), value :: dir, lowest, highest
+        end function
+        integer(c_int) function gam_tile_halo_bytes(h, dir, nbytes) bind(C, name="gam_tile_halo_bytes")
+            import :: c_int, c_ptr, c_int32_t, c_int64_t
+            type(c_ptr), value :: h
+            integer(c_int32_t), value :: dir
+            integer(c_int64_t), intent(out) :: nbytes
+        end function
+        integer(c_int) function gam_tile_halo_pack(h, dir, side, dev_buf) bind(C, name="gam_tile_halo_pack")
+            import :: c_int, c_ptr, c_int32_t
+            type(c_ptr), value :: h, dev_buf
+            integer(c_int32_t), value :: dir, side
+        end function
+        integer(c_int) function gam_tile_halo_unpack(h, dir, side, dev_buf, copyB) &
+                bind(C, name="gam_tile_halo_unpack")
+            import :: c_int, c_ptr, c_int32_t
+            type(c_ptr), value :: h, dev_buf
+            integer(c_int32_t), value :: dir, side, copyB
+        end function
         integer(c_int) function gam_set_slab_edges(h, lowest, highest) bind(C, name="gam_set_slab_edges")
             import :: c_int, c_ptr, c_int32_t
             type(c_ptr), value :: h
@@ -344,11 +367,12 @@ module gamgpu
             type(c_ptr), value :: bg, work, stream
             real(c_double), value :: dt, odt
         end function
+        ! a tile away from the inner boundary leaves out both fields (NULL)
         integer(c_int) function gam_set_ionosphere(h, inExyz, inEijk, M0, dtCpl, doIonPush, nIonP, dtSW0) &
                 bind(C, name="gam_set_ionosphere")
             import :: c_int, c_ptr, c_double, c_int32_t
             type(c_ptr), value :: h
-            real(c_double), intent(in) :: inExyz(*), inEijk(*)
+            real(c_double), intent(in), optional :: inExyz(*), inEijk(*)
             real(c_double), value :: M0, dtCpl, dtSW0
             integer(c_int32_t), value :: doIonPush, nIonP
         end function

@@ -70,7 +70,8 @@ EXPORTED = (
     "gam_dt_partial_dev", "gam_step_end_dev", "gam_step_status", "gam_flux_forward", "gam_flux_adjoint",
     "gam_efield_forward", "gam_efield_adjoint", "gam_predict_stage", "gam_update_stage", "gam_step_work_bytes",
     "gam_step_fwd_save", "gam_step_adj", "gam_iside_fill", "gam_iside_adjoint", "gam_step_fwd_save_iside",
-    "gam_step_adj_iside",
+    "gam_step_adj_iside", "gam_tile_halo_bytes", "gam_tile_halo_pack", "gam_tile_halo_unpack",
+    "gam_set_tile_edges",
 )
 
 # Background-field arrays (Grid_T, gamtypes.F90:233-242): name, components;
@@ -121,6 +122,10 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     L.gam_write_restart.argtypes = [C.c_void_p, C.c_char_p]
     L.gam_halo_bytes.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
     L.gam_set_slab_edges.argtypes = [C.c_void_p, C.c_int32, C.c_int32]
+    L.gam_set_tile_edges.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32]
+    L.gam_tile_halo_bytes.argtypes = [C.c_void_p, C.c_int32, C.POINTER(C.c_int64)]
+    L.gam_tile_halo_pack.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p]
+    L.gam_tile_halo_unpack.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_int32]
     L.gam_flux_forward.argtypes = [C.POINTER(_Params), C.c_int32] + [C.c_void_p] * 8 + [_dp, _dp] + [C.c_void_p] * 3
     L.gam_flux_adjoint.argtypes = [C.POINTER(_Params), C.c_int32] + [C.c_void_p] * 8 + [_dp, _dp] + [C.c_void_p] * 8
     L.gam_efield_forward.argtypes = [C.POINTER(_Params), C.c_int32] + [C.c_void_p] * 9 + [_dp, C.c_double] + \
@@ -385,10 +390,17 @@ class GameraGPU:
         i.e. the Fortran arrays (1:5, jsg:jeg, ksg:keg, 1:3) and
         (1:6, jsg:jeg+1, ksg:keg+1, 1:3); M0 the dipole moment; dtCpl the
         coupling time scale of PushIon and dtSW0 that of NudgeSW (code time;
-        60 s in Earth units, the reference's one minute, is the default)."""
-        E = np.ascontiguousarray(inExyz, dtype=np.float64)
-        Ee = np.ascontiguousarray(inEijk, dtype=np.float64)
-        self._check(self.L.gam_set_ionosphere(self.h, _ptr(E), _ptr(Ee), float(M0), float(dtCpl),
+        60 s in Earth units, the reference's one minute, is the default).
+        A tile away from the inner boundary (bc[0] = BC_HALO) passes None for
+        both fields: it takes the hooks of its other sides and the DT range."""
+        if inExyz is None:
+            E = Ee = None
+            pE = pEe = None
+        else:
+            E = np.ascontiguousarray(inExyz, dtype=np.float64)
+            Ee = np.ascontiguousarray(inEijk, dtype=np.float64)
+            pE, pEe = _ptr(E), _ptr(Ee)
+        self._check(self.L.gam_set_ionosphere(self.h, pE, pEe, float(M0), float(dtCpl),
                                               int(bool(doIonPush)), int(nIonP), float(dtSW0)))
 
     def init_dipole_wind(self, wind, seed: int = 31337, amp: float = 0.01):
@@ -397,9 +409,29 @@ class GameraGPU:
         assert w.shape == (8,)
         self._check(self.L.gam_init_dipole_wind(self.h, _ptr(w), int(seed), float(amp)))
 
-    # --- k-slab tiling (see mage_b200.tiling) --------------------------------------
+    # --- tiling (see mage_b200.tiling) ---------------------------------------------
     def set_slab_edges(self, lowest: bool, highest: bool):
         self._check(self.L.gam_set_slab_edges(self.h, int(lowest), int(highest)))
+
+    def set_tile_edges(self, d: int, lowest: bool, highest: bool):
+        """Whether this tile's lower / upper side in direction d (0 I, 1 J,
+        2 K) is an edge of the whole grid (CalcDT's ghost layer)."""
+        self._check(self.L.gam_set_tile_edges(self.h, int(d), int(lowest), int(highest)))
+
+    def tile_halo_bytes(self, d: int) -> int:
+        n = C.c_int64()
+        self._check(self.L.gam_tile_halo_bytes(self.h, int(d), C.byref(n)))
+        return n.value
+
+    def tile_halo_pack(self, d: int, side: int, buf):
+        """Pack the halo of side 0 (down) or 1 (up) of direction d into a
+        device buffer (a tensor or a pointer)."""
+        ptr = buf.data_ptr() if hasattr(buf, "data_ptr") else int(buf)
+        self._check(self.L.gam_tile_halo_pack(self.h, int(d), int(side), C.c_void_p(ptr)))
+
+    def tile_halo_unpack(self, d: int, side: int, buf, copyB: bool = False):
+        ptr = buf.data_ptr() if hasattr(buf, "data_ptr") else int(buf)
+        self._check(self.L.gam_tile_halo_unpack(self.h, int(d), int(side), C.c_void_p(ptr), int(copyB)))
 
     def halo_bytes(self) -> int:
         n = C.c_int64()
@@ -436,7 +468,7 @@ class GameraGPU:
         self._check(self.L.gam_step_end(self.h, C.c_uint64(bits), int(nbad), C.byref(dt), C.byref(t)))
         return dt.value, t.value
 
-    # device-resident k-slab steps (no host round trip per step)
+    # device-resident tile steps (no host round trip per step)
     def set_stream(self, stream_ptr: int | None):
         """Enqueue this handle's work on the caller's CUDA stream (a
         non-default stream; None: the handle's own)."""

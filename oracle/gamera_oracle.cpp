@@ -2412,6 +2412,11 @@ void orc_set_ionosphere(void* h, const double* inE, const double* inEe, double M
     A->M.ion.doIonPush = doIonPush != 0;
     A->M.ion.nIonP = nIonP;
     A->M.ion.dtSW0 = dtSW0;
+    // the magnetosphere's DT bounds: the active cells only (earthcmi.F90:136-142)
+    Grid& Gw = A->G;
+    Gw.isDT = Gw.is; Gw.ieDT = Gw.ie;
+    Gw.jsDT = Gw.js; Gw.jeDT = Gw.je;
+    Gw.ksDT = Gw.ks; Gw.keDT = Gw.ke;
 }
 
 // Pointers to internal Fortran-ordered arrays, for numpy views.

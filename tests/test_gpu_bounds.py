@@ -6,7 +6,8 @@ and the device arrays start as NaN canaries instead of zeros.
   canary, i.e. no read of memory nothing wrote, reaches a result) and no
   check fires, over the configurations the step supports: curvilinear blast
   wave (with AB3, with Boris), 2.5-D Orszag-Tang, the dipole in the wind, the
-  inflow / outflow boundaries, FP32, and two emulated k-slabs;
+  inflow / outflow boundaries, FP32, two emulated k-slabs and 2 x 2 x 2
+  emulated tiles;
 * the reporting path: a limit below the box size (GAM_BOUNDS_LIMIT, read at
   handle creation) makes in-bounds indices fail the check; the step returns
   GAM_EBOUNDS with the kernel recorded and no memory outside the box is
@@ -95,6 +96,24 @@ def test_checked_build_fp32_and_slabs(oracle_built):
     sl.step(4)
     for a in sl.apps:
         assert a.bounds_status()["fired"] == 0
+
+
+def test_checked_build_tiles():
+    """Tiles along i, j and k: the halo kernels of every direction and side
+    stay inside the box, and the tiles equal the checked single grid."""
+    from mage_b200.tiling import Tiles, tile_box
+    N = (32, 16, 16)
+    xyz = grids.warped_periodic_corners(*N)
+    one = GameraGPU(GamParams(*N, strict=True), lib_path=CHECK_LIB_PATH)
+    one.set_geometry(xyz)
+    one.init_blast_wave()
+    tl = Tiles(N, xyz, (2, 2, 2), strict=True, lib_path=CHECK_LIB_PATH)
+    assert one.step_gamera(3) == tl.step(3)
+    ref = one.download_state()
+    assert one.bounds_status()["fired"] == 0
+    for t, a in zip(tl.tiles, tl.apps):
+        assert a.bounds_status()["fired"] == 0
+        assert np.array_equal(a.download_state()["Gas"], tile_box(ref["Gas"], N, tl.dims, t.t)), t.t
 
 
 def test_bounds_report_path():
