@@ -70,3 +70,27 @@ def spherical_corners(Nr: int, Nth: int, Nph: int, r0: float = 2.0, r1: float = 
     xyz[1] = R * np.sin(TH) * np.sin(PH)
     xyz[2] = R * np.cos(TH) * np.ones_like(PH)
     return xyz
+
+
+def lfm_corners(Nr: int, Nth: int, Nph: int, r0: float = 2.0, r1: float = 30.0, th0: float = 0.0) -> np.ndarray:
+    """LFM-style corners: spherical about the x axis, the polar angle th on
+    [th0, pi - th0] from +x (j, the axis at js and je+1 when th0 = 0), the
+    azimuth ph on [0, 2 pi) around x (k, periodic), r log-spaced on [r0, r1]
+    (i): x = r cos(th), y = r sin(th) cos(ph), z = r sin(th) sin(ph). Ghost
+    corners continue the formulas, so with th0 = 0 the ghosts across the axis
+    fall on the cells that the pole boundary maps them to (mirrored j,
+    k + Nph/2)."""
+    i = np.arange(1 - NG, Nr + NG + 2, dtype=np.float64)
+    j = np.arange(1 - NG, Nth + NG + 2, dtype=np.float64)
+    k = np.arange(1 - NG, Nph + NG + 2, dtype=np.float64)
+    r = r0 * (r1 / r0) ** ((i - 1.0) / Nr)
+    th = th0 + (np.pi - 2.0 * th0) * (j - 1.0) / Nth
+    ph = 2.0 * np.pi * (k - 1.0) / Nph
+    R = r[None, None, :]
+    TH = th[None, :, None]
+    PH = ph[:, None, None]
+    xyz = np.empty((3, k.size, j.size, i.size), dtype=np.float64)
+    xyz[0] = R * np.cos(TH) * np.ones_like(PH)
+    xyz[1] = R * np.sin(TH) * np.cos(PH)
+    xyz[2] = R * np.sin(TH) * np.sin(PH)
+    return xyz

@@ -67,7 +67,7 @@ static const int SgnLR[2] = {-1, 1};  // stress.F90:19
 
 // boundary kinds (a subset of bcs.F90 / apps/wind.F90; BC_INFLOW is a uniform
 // inflow of this library, with no counterpart in the reference)
-enum { BC_PERIODIC = 0, BC_NONE = 1, BC_ZEROGRAD = 2, BC_SPHIN = 3, BC_WIND = 4, BC_INFLOW = 6, BC_ION = 7 };
+enum { BC_PERIODIC = 0, BC_NONE = 1, BC_ZEROGRAD = 2, BC_SPHIN = 3, BC_WIND = 4, BC_INFLOW = 6, BC_ION = 7, BC_LFM = 8 };
 
 // interpolation weights, recon.F90:22-23,28-29
 static double interpWgt[8], interpWgt6[8], Up7C[7];
@@ -125,6 +125,12 @@ struct Params {  // mirrored by oracle/oracle.py (ctypes)
     int doBoris;         // physics/doBoris (init.F90:417-423)
     double Ca;           // physics/Ca: the Boris speed of light (code units)
     int doAB3;           // sim/doAB3 (init.F90:377): third-order predictor with ooState
+    // ring averaging about the LFM axis (ring/doRing with ring/gid = "lfm"):
+    // ringNumR rings (0: off), chunks per ring, ring/rngrec (0 PPM, 1 PLM,
+    // 2 PCM), ringknobs/NMag, ringknobs/doClean, ringknobs/doFastClean
+    int ringNumR;
+    int ringNch[32];
+    int ringRecon, ringNFT, ringClean, ringFast;
 };
 
 struct Model {
@@ -164,6 +170,14 @@ struct Grid {
     F4 xyz, xyzcc, xfc, di, dj, dk, volume, Tf, Te, Teb, face, edge;
     F4 fcB0, edgB0, B0, bFlux0, dpB0;  // background (cell-sized, background.F90:43-47)
     int bc[6];
+    // ring averaging about the LFM axis (Model%Ring, ringutils.F90:37-236 for
+    // gid "lfm": the pole along k, Np = Nkp, slices over i); doS / doE: the
+    // grid holds the pole at js / je+1 (J boundary GAM_BC_LFM)
+    struct Ring {
+        bool on = false, doS = false, doE = false, doClean = true, doFast = true;
+        int NumR = 0, Np = 0, recon = 0, NFTMAG = 1;
+        int Nch[32] = {0};
+    } ring;
     // allocation helpers
     void cellArr(F4& a, int nc, double f = 0.0) const { a.alloc(isg, ieg, jsg, jeg, ksg, keg, nc, f); }
     void faceArr(F4& a, int nc, double f = 0.0) const { a.alloc(isg, ieg + 1, jsg, jeg + 1, ksg, keg + 1, nc, f); }
@@ -173,6 +187,47 @@ struct State {
     double time = -HUGE_;
     F4 Gas, magFlux, Efld, Bxyz;
 };
+
+// ringutils.F90:650-659 WrapK
+static inline int WrapK(int k, int Np) {
+    int kp = k + Np / 2;
+    if (kp > Np) kp = kp - Np;
+    return kp;
+}
+// ringutils.F90:521-586 lfmIJKfc: face-centred conjugate of face d
+static void lfmIJKcc(const Grid& G, int i, int j, int k, int& ip, int& jp, int& kp);
+static void lfmIJKfc(const Grid& G, int d, int i, int j, int k, int& ip, int& jp, int& kp) {
+    const int Np = G.Nkp;
+    ip = i;
+    if (d == 0) {
+        lfmIJKcc(G, i, j, k, ip, jp, kp);
+        return;
+    }
+    kp = k;
+    if (k < G.ks) kp = k + Np;
+    if (d == 1 && k > G.ke) kp = k - Np;
+    if (d == 2 && k > G.ke + 1) kp = k - Np;
+    jp = j;
+    if (d == 1) {  // J faces: the pole face itself is seen once
+        if (G.ring.doS && j < G.js) {
+            jp = G.js + (G.js - j);
+            kp = WrapK(k, Np);
+        }
+        if (G.ring.doE && j > G.je + 1) {
+            jp = G.je + 1 - (j - G.je) + 1;
+            kp = WrapK(k, Np);
+        }
+    } else {
+        if (G.ring.doS && j < G.js) {
+            jp = G.js + (G.js - j) - 1;
+            kp = WrapK(k, Np);
+        }
+        if (G.ring.doE && j > G.je) {
+            jp = G.je - (j - G.je) + 1;
+            kp = WrapK(k, Np);
+        }
+    }
+}
 
 // global limiter parameters (recon.F90:27 pdmb, gdefs.F90:12 floors)
 static double pdmb = 0.75, dFloor = TINY, pFloor = TINY;
@@ -516,6 +571,36 @@ static void Fluxes(const Model& M, const Grid& G, const State& nS, const State& 
 }
 
 // stress.F90:41-198 CalcStress
+// ringutils.F90:662-678 RingFlux: no flux through the pole faces, then
+// FixGasFluxLFM (gamdebug.F90:91-124): the K fluxes of the two periodic k
+// ends set to their mean
+static void RingFlux(const Model& M, const Grid& G, F4& gFlx, F4& mFlx) {
+    const int jz[2] = {G.js, G.je + 1};
+    const bool on[2] = {G.ring.doS, G.ring.doE};
+    for (int p = 0; p < 2; p++) {
+        if (!on[p]) continue;
+        for (int k = G.ksg; k <= G.keg; k++)
+            for (int i = G.isg; i <= G.ieg; i++) {
+                for (int nv = 0; nv < NVAR; nv++) gFlx(i, jz[p], k, nv + 5 * JDIR) = 0.0;
+                if (M.doMHD)
+                    for (int x = 0; x < NDIM; x++) mFlx(i, jz[p], k, x + 3 * JDIR) = 0.0;
+            }
+    }
+    if (!M.doMHD) return;
+    for (int j = G.js; j <= G.je; j++)
+        for (int i = G.is; i <= G.ie; i++) {
+            for (int nv = 0; nv < NVAR; nv++) {
+                const double gF = 0.5 * (gFlx(i, j, G.ks, nv + 5 * KDIR) + gFlx(i, j, G.ke + 1, nv + 5 * KDIR));
+                gFlx(i, j, G.ks, nv + 5 * KDIR) = gF;
+                gFlx(i, j, G.ke + 1, nv + 5 * KDIR) = gF;
+            }
+            for (int x = 0; x < NDIM; x++) {
+                const double mF = 0.5 * (mFlx(i, j, G.ks, x + 3 * KDIR) + mFlx(i, j, G.ke + 1, x + 3 * KDIR));
+                mFlx(i, j, G.ks, x + 3 * KDIR) = mF;
+                mFlx(i, j, G.ke + 1, x + 3 * KDIR) = mF;
+            }
+        }
+}
 static void CalcStress(const Model& M, const Grid& G, const State& nS, const State& hS, F4& gFlx, F4& mFlx,
                        F4& dGasH, F4& dGasM) {
     int nFlx = M.do25D ? 2 : 3;
@@ -541,6 +626,7 @@ static void CalcStress(const Model& M, const Grid& G, const State& nS, const Sta
             }
         }
     }
+    if (G.ring.on) RingFlux(M, G, gFlx, mFlx);  // stress.F90:137-139
 #pragma omp parallel for collapse(2)
     for (int k = G.ks; k <= G.ke; k++)
         for (int j = G.js; j <= G.je; j++)
@@ -785,6 +871,24 @@ static inline void gamCellBxyz(const Grid& G, const F4& mf, int i, int j, int k,
         B[x] = b - Div * G.xyzcc(i, j, k, x) / dV;
     }
 }
+// ringutils.F90:393-444 RingFlux2FieldFix: the cells across the pole take
+// the Bxyz of their conjugate
+static void RingFlux2FieldFix(const Grid& G, F4& Bxyz) {
+    if (!G.ring.on || !(G.ring.doS || G.ring.doE)) return;
+    for (int k = G.ksg; k <= G.keg; k++)
+        for (int i = G.isg; i <= G.ieg; i++)
+            for (int n = 1; n <= 4; n++) {
+                int ip, jp, kp;
+                if (G.ring.doS) {
+                    lfmIJKcc(G, i, G.js - n, k, ip, jp, kp);
+                    for (int x = 0; x < 3; x++) Bxyz(i, G.js - n, k, x) = Bxyz(ip, jp, kp, x);
+                }
+                if (G.ring.doE) {
+                    lfmIJKcc(G, i, G.je + n, k, ip, jp, kp);
+                    for (int x = 0; x < 3; x++) Bxyz(i, G.je + n, k, x) = Bxyz(ip, jp, kp, x);
+                }
+            }
+}
 // gridutils.F90:281-301 bFlux2Fld
 static void bFlux2Fld(const Grid& G, const F4& magFlux, F4& Bxyz) {
 #pragma omp parallel for collapse(2)
@@ -795,6 +899,7 @@ static void bFlux2Fld(const Grid& G, const F4& magFlux, F4& Bxyz) {
                 gamCellBxyz(G, magFlux, i, j, k, B);
                 for (int x = 0; x < 3; x++) Bxyz(i, j, k, x) = B[x];
             }
+    RingFlux2FieldFix(G, Bxyz);
 }
 
 // ---------------------------------------------------------------- update
@@ -854,9 +959,10 @@ static void CopyState(const Grid& G, const State& a, State& b) {  // mhdgroup.F9
     b.magFlux.v = a.magFlux.v;
     b.time = a.time;
 }
+static void PoleE(const Grid& G, F4& E);
 // mhdgroup.F90:79-200 applyUpdate (single fluid)
 static void applyUpdate(const Model& M, const Grid& G, State& S, State& oS, State& ooS, double dt, const F4& dGasH,
-                        const F4& dGasM, const F4& E) {
+                        const F4& dGasM, F4& E) {
     if (M.doAB3) CopyState(G, oS, ooS);
     CopyState(G, S, oS);
     S.time = S.time + dt;
@@ -867,6 +973,7 @@ static void applyUpdate(const Model& M, const Grid& G, State& S, State& oS, Stat
                 for (int nv = 0; nv < NVAR; nv++)  // CellReynolds with Model%dt (mhdgroup.F90:121)
                     S.Gas(i, j, k, nv) = S.Gas(i, j, k, nv) + M.dt * dGasH(i, j, k, nv);
     if (!M.doMHD) return;
+    if (G.ring.on && (G.ring.doS || G.ring.doE)) PoleE(G, E);  // mhdgroup.F90:140-142
     E2Flux(G, S.magFlux, E, dt);
     bFlux2Fld(G, S.magFlux, S.Bxyz);
 #pragma omp parallel for collapse(2)
@@ -1072,6 +1179,7 @@ static void WindBC(const Model& M, const Grid& G, State& S);
 static void InflowBC(const Model& M, const Grid& G, State& S);
 static void zeroGrad_obcI(const Grid& G, State& S);
 static void IonInner(const Model& M, const Grid& G, State& S);
+static void lfmPole(const Grid& G, State& S, int p);
 static void EnforceBCs(const Model& M, const Grid& G, State& S) {
     if (G.bc[0] == BC_PERIODIC) periodic_ibcI(G, S);
     else if (G.bc[0] == BC_SPHIN) SphIn(G, S);
@@ -1082,8 +1190,10 @@ static void EnforceBCs(const Model& M, const Grid& G, State& S) {
     else if (G.bc[1] == BC_ZEROGRAD) zeroGrad_obcI(G, S);
     if (G.bc[2] == BC_PERIODIC) periodic_ibcJ(G, S);
     else if (G.bc[2] == BC_ZEROGRAD) zeroGrad_ibcJ(G, S);
+    else if (G.bc[2] == BC_LFM) lfmPole(G, S, 0);
     if (G.bc[3] == BC_PERIODIC) periodic_obcJ(G, S);
     else if (G.bc[3] == BC_ZEROGRAD) zeroGrad_obcJ(G, S);
+    else if (G.bc[3] == BC_LFM) lfmPole(G, S, 1);
     if (G.bc[4] == BC_PERIODIC) periodic_ibcK(M, G, S);
     if (G.bc[5] == BC_PERIODIC) periodic_obcK(M, G, S);
 }
@@ -1103,7 +1213,8 @@ static double inEijk(const Model& M, const Grid& G, int s, int j, int k, int x) 
     const long nj = G.jeg - G.jsg + 2, nk = G.keg - G.ksg + 2;
     return M.ion.inEijk[(s - 1) + (PsiSh + 1) * ((j - G.jsg) + nj * ((k - G.ksg) + nk * x))];
 }
-// ringutils.F90:482-518 lfmIJKcc without rings: k into the active range
+// ringutils.F90:482-518 lfmIJKcc: k into the active range; with rings, a
+// ghost j across the pole maps to its conjugate (mirrored j, k + Np/2)
 static void lfmIJKcc(const Grid& G, int i, int j, int k, int& ip, int& jp, int& kp) {
     const int Np = G.Nkp;
     ip = i;
@@ -1111,6 +1222,14 @@ static void lfmIJKcc(const Grid& G, int i, int j, int k, int& ip, int& jp, int& 
     else if (k > G.ke) kp = k - Np;
     else kp = k;
     jp = j;
+    if (G.ring.doS && j < G.js) {
+        jp = G.js + (G.js - j) - 1;
+        kp = WrapK(k, Np);
+    }
+    if (G.ring.doE && j > G.je) {
+        jp = G.je - (j - G.je) + 1;
+        kp = WrapK(k, Np);
+    }
 }
 // math.F90:265-274 cross, :332-343 normVec, :365-376 Vec2Perp
 static void cross3(const double* a, const double* b, double* c) {
@@ -1185,6 +1304,20 @@ static void IonInner(const Model& M, const Grid& G, State& S) {
                 gamCellBxyz(G, S.magFlux, ip, jp, kp, B);
                 for (int x = 0; x < 3; x++) S.Bxyz(ig, j, k, x) = B[x];
             }
+    // the ghosts across the pole take their conjugate's Bxyz (:545-572)
+    for (int k = G.ksg; k <= G.keg; k++)
+        for (int i = G.isg; i <= G.is - 1; i++)
+            for (int n = 1; n <= 4; n++) {
+                int ip, jp, kp;
+                if (G.ring.doS) {
+                    lfmIJKcc(G, i, G.js - n, k, ip, jp, kp);
+                    for (int x = 0; x < 3; x++) S.Bxyz(i, G.js - n, k, x) = S.Bxyz(ip, jp, kp, x);
+                }
+                if (G.ring.doE) {
+                    lfmIJKcc(G, i, G.je + n, k, ip, jp, kp);
+                    for (int x = 0; x < 3; x++) S.Bxyz(i, G.je + n, k, x) = S.Bxyz(ip, jp, kp, x);
+                }
+            }
 }
 // HackE = EFix (earthcmi.F90:321-354): IonEFix (msphutils.F90:214-240),
 // WindEFix with the wind outside (below), then FixEFieldLFM
@@ -1209,6 +1342,332 @@ static void FixEFieldLFM(const Grid& G, F4& E) {
             E(i, j, G.ks, JDIR) = Ej;
             E(i, j, G.ke + 1, JDIR) = Ej;
         }
+}
+
+// ---------------------------------------------------------------- ring averaging
+// Ring averaging about the LFM axis (ringav.F90, ringrecon.F90, ringutils.F90
+// for Model%Ring%GridID = "lfm"): rings are the k circles of the first NumR
+// j rows next to each pole, sliced by i; with the reference's defaults
+// (doShift, doVClean, doMassRA and multifluid off; NFTVEL unused).
+enum { SPOLE = 1, EPOLE = 2 };
+static const int NFTMAX = 2;
+// ringav.F90:394-430 PoleE: K EMFs on the pole zero, I EMFs on the pole
+// their ring mean, then FixEFieldLFM
+static void PoleE(const Grid& G, F4& E) {
+    const int Np = G.ring.Np;
+    const int jp[2] = {G.js, G.je + 1};
+    const bool on[2] = {G.ring.doS, G.ring.doE};
+    for (int nS = G.is; nS <= G.ie + 1; nS++)
+        for (int p = 0; p < 2; p++) {
+            if (!on[p]) continue;
+            for (int k = G.ksg; k <= G.keg; k++) E(nS, jp[p], k, KDIR) = 0.0;
+            double s = 0.0;
+            for (int k = G.ks; k <= G.ke; k++) s = s + E(nS, jp[p], k, IDIR);
+            const double avg = s / Np;
+            for (int k = G.ksg; k <= G.keg; k++) E(nS, jp[p], k, IDIR) = avg;
+        }
+    FixEFieldLFM(G, E);
+}
+// math.F90:192-197 minmod (sign() as copysign, min() as a < b)
+static inline double fmin2(double a, double b) { return b < a ? b : a; }
+static inline double minmod(double x, double y) {
+    return 0.5 * (std::copysign(1.0, x) + std::copysign(1.0, y)) * fmin2(std::fabs(x), std::fabs(y));
+}
+// ringrecon.F90:251-285 PPM_IntLR, :235-249 PLM_IntLR, :224-232 PCM_IntLR
+static void RingLR(int recon, double fm2, double fm1, double f, double fp1, double fp2, double& vm, double& vp) {
+    if (recon == 2) {
+        vm = f;
+        vp = f;
+        return;
+    }
+    if (recon == 1) {
+        const double dwL = f - fm1, dwR = fp1 - f, dwC = (fp1 - fm1) / 2.0;
+        const double min1 = fmin2(2 * std::fabs(dwL), 2 * std::fabs(dwR));
+        const double min2 = fmin2(min1, std::fabs(dwC));
+        const double dwM = std::copysign(min2, dwC);
+        vp = f + 0.5 * dwM;
+        vm = f - 0.5 * dwM;
+        return;
+    }
+    const double dvm2 = fm1 - fm2, dvm1 = f - fm1, dvp1 = fp1 - f, dvp2 = fp2 - fp1;
+    double dvc = 0.5 * (dvm2 + dvm1), SM = 2.0 * minmod(dvm2, dvm1);
+    const double Sm1 = minmod(dvc, SM);
+    dvc = 0.5 * (dvm1 + dvp1);
+    SM = 2.0 * minmod(dvm1, dvp1);
+    const double Sp1 = minmod(dvc, SM);
+    dvc = 0.5 * (dvp2 + dvp1);
+    SM = 2.0 * minmod(dvp2, dvp1);
+    const double Sp2 = minmod(dvc, SM);
+    vp = 0.5 * (f + fp1) - (Sp2 - Sp1) / 6.0;
+    vm = 0.5 * (f + fm1) - (Sp1 - Sm1) / 6.0;
+    double ap = vp - f, am = vm - f;
+    if (ap * am >= 0.0) {
+        ap = 0.0;
+        am = 0.0;
+    } else {
+        if (std::fabs(ap) >= 2.0 * std::fabs(am)) ap = -2.0 * am;
+        if (std::fabs(am) >= 2.0 * std::fabs(ap)) am = -2.0 * ap;
+    }
+    vp = f + ap;
+    vm = f + am;
+}
+// ringrecon.F90:34-91 ReconstructRing: the chunk values (each chunk's first
+// element, all equal after chunk averaging) with 2 periodic ghosts, an
+// interval L/R per chunk, and the parabola's cell averages within it
+static void ReconstructRing(const Grid& G, double* rW, int Nc) {
+    const int Np = G.ring.Np, dJ = Np / Nc, Ng = 2;
+    std::vector<double> chW(Nc + 2 * Ng);
+    auto ch = [&](int n) -> double& { return chW[n - 1 + Ng]; };  // n = 1-Ng .. Nc+Ng
+    for (int n = 1; n <= Nc; n++) ch(n) = rW[(n - 1) * dJ];
+    for (int n = 1; n <= Ng; n++) {
+        ch(1 - n) = ch(Nc - n + 1);
+        ch(Nc + n) = ch(n);
+    }
+    for (int n = 1; n <= Nc; n++) {
+        const int mS = 1 + (n - 1) * dJ;
+        double fL, fR;
+        RingLR(G.ring.recon, ch(n - 2), ch(n - 1), ch(n), ch(n + 1), ch(n + 2), fL, fR);
+        const double f = ch(n);
+        const double a = 3 * (fL + fR - 2 * f), b = 2 * (3 * f - fR - 2 * fL), c = fL;
+        for (int m = 1; m <= dJ; m++) {
+            const double fI = (a / 3.0) * (3 * m * m - 3 * m + 1) / (dJ * dJ) + 0.5 * b * (2 * m - 1) / dJ + c;
+            rW[mS + m - 2] = fI;
+        }
+    }
+}
+// ringav.F90:433-493 CleanRing / DirtyRing: Fourier modes 0..numFT of a ring
+// at the cell centres phi_n = (n - 1/2) 2 pi / Np removed and put back
+static void CleanRing(const Grid& G, double* Q, double cFT[NFTMAX + 1][2], int numFT) {
+    const int Np = G.ring.Np;
+    for (int m = 0; m <= NFTMAX; m++) cFT[m][0] = cFT[m][1] = 0.0;
+    const double aScl = (double)(2.0f / (float)Np), dp = 2.0 * PI / Np;  // 2.0/Np in default real
+    for (int n = 1; n <= Np; n++) {
+        const double phi = dp * n - 0.5 * dp;
+        for (int m = 0; m <= numFT; m++) {
+            cFT[m][0] = cFT[m][0] + Q[n - 1] * std::cos(1.0 * m * phi);
+            cFT[m][1] = cFT[m][1] + Q[n - 1] * std::sin(1.0 * m * phi);
+        }
+    }
+    for (int c = 0; c < 2; c++) cFT[0][c] = 0.5 * aScl * cFT[0][c];
+    for (int m = 1; m <= numFT; m++)
+        for (int c = 0; c < 2; c++) cFT[m][c] = 1.0 * aScl * cFT[m][c];
+    for (int n = 1; n <= Np; n++) {
+        const double phi = dp * n - 0.5 * dp;
+        for (int m = 0; m <= numFT; m++)
+            Q[n - 1] = Q[n - 1] - cFT[m][0] * std::cos(1.0 * m * phi) - cFT[m][1] * std::sin(1.0 * m * phi);
+    }
+}
+static void DirtyRing(const Grid& G, double* Q, const double cFT[NFTMAX + 1][2], int numFT) {
+    const int Np = G.ring.Np;
+    const double dp = 2.0 * PI / Np;
+    for (int n = 1; n <= Np; n++) {
+        const double phi = dp * n - 0.5 * dp;
+        for (int m = 0; m <= numFT; m++)
+            Q[n - 1] = Q[n - 1] + cFT[m][0] * std::cos(1.0 * m * phi) + cFT[m][1] * std::sin(1.0 * m * phi);
+    }
+}
+// ringav.F90:212-344 CalcSmoothE: per slice and ring, the face fluxes through
+// the ring (J faces -> I EMFs, I faces -> J EMFs) cleaned of their low Fourier
+// modes, chunk-averaged, reconstructed and dirtied again; the change of each
+// face's flux accumulated along the chunk into the EMF that makes it
+static void CalcSmoothE(const Grid& G, const State& S, F4& SmoothE, int pole) {
+    const int Np = G.ring.Np;
+    const int fDIRS[2] = {JDIR, IDIR}, eDIRS[2] = {IDIR, JDIR};
+    const double eScls[2] = {1.0, -1.0};
+    std::vector<double> bFlx(3 * Np), dEr(3 * Np), rFlx(Np), raFlx(Np), dFlx(Np);
+    for (int nS = G.is; nS <= G.ie + 1; nS++)
+        for (int nR = 1; nR <= G.ring.NumR; nR++) {
+            const int NumCh = G.ring.Nch[nR - 1], dC = Np / NumCh;
+            // PullRingI (ringutils.F90:760-800)
+            for (int n = 0; n < Np; n++) {
+                const int k = G.ks + n;
+                if (pole == SPOLE) {
+                    bFlx[n] = S.magFlux(nS, G.js + nR - 1, k, IDIR);
+                    bFlx[Np + n] = S.magFlux(nS, G.js + nR, k, JDIR);
+                    bFlx[2 * Np + n] = S.magFlux(nS, G.js + nR - 1, k, KDIR);
+                } else {
+                    for (int d = 0; d < 3; d++) bFlx[d * Np + n] = S.magFlux(nS, G.je - nR + 1, k, d);
+                }
+            }
+            std::fill(dEr.begin(), dEr.end(), 0.0);
+            for (int dd = 0; dd < 2; dd++) {
+                const int fD = fDIRS[dd], eD = eDIRS[dd];
+                const double eScl = eScls[dd];
+                for (int n = 0; n < Np; n++) rFlx[n] = bFlx[fD * Np + n];
+                double cFT[NFTMAX + 1][2];
+                CleanRing(G, rFlx.data(), cFT, G.ring.NFTMAG);
+                for (int c = 1; c <= NumCh; c++) {
+                    const int lRs = 1 + (c - 1) * dC, lRe = lRs + dC - 1;
+                    double s = 0.0;
+                    for (int l = lRs; l <= lRe; l++) s = s + rFlx[l - 1];
+                    for (int l = lRs; l <= lRe; l++) raFlx[l - 1] = s / dC;
+                }
+                ReconstructRing(G, raFlx.data(), NumCh);
+                DirtyRing(G, raFlx.data(), cFT, G.ring.NFTMAG);
+                for (int n = 0; n < Np; n++) dFlx[n] = raFlx[n] - bFlx[fD * Np + n];
+                for (int c = 1; c <= NumCh; c++) {
+                    const int lRs = 1 + (c - 1) * dC;
+                    double cumFlx = -dFlx[lRs - 1];
+                    for (int m = 2; m <= dC; m++) {
+                        dEr[eD * Np + lRs + m - 2] = eScl * cumFlx;
+                        cumFlx = cumFlx - dFlx[lRs + m - 2];
+                    }
+                }
+            }
+            for (int n = 0; n < Np; n++) {
+                const int k = G.ks + n;
+                if (pole == SPOLE) {
+                    SmoothE(nS, G.js + nR, k, IDIR) = dEr[n];
+                    SmoothE(nS, G.js + nR - 1, k, JDIR) = dEr[Np + n];
+                    SmoothE(nS, G.js + nR - 1, k, KDIR) = dEr[2 * Np + n];
+                } else {
+                    for (int d = 0; d < 3; d++) SmoothE(nS, G.je - nR + 1, k, d) = dEr[d * Np + n];
+                }
+            }
+            if (pole == SPOLE) {
+                SmoothE(nS, G.js + nR, G.ke + 1, IDIR) = SmoothE(nS, G.js + nR, G.ks, IDIR);
+                SmoothE(nS, G.js + nR - 1, G.ke + 1, JDIR) = SmoothE(nS, G.js + nR - 1, G.ks, JDIR);
+            } else {
+                SmoothE(nS, G.je - nR + 1, G.ke + 1, IDIR) = SmoothE(nS, G.je - nR + 1, G.ks, IDIR);
+                SmoothE(nS, G.je - nR + 1, G.ke + 1, JDIR) = SmoothE(nS, G.je - nR + 1, G.ks, JDIR);
+            }
+        }
+}
+// ringav.F90:347-391 CleanLoops: the K flux through the first ring's cells
+// (the faces around the pole) loses its ring mean
+static void CleanLoops(const Grid& G, State& S) {
+    const int Np = G.ring.Np;
+    const double tScl = G.ring.doFast ? 1.0 : (double)(1.0f / (float)Np);  // 1.0/Np in default real
+    const int jr[2] = {G.js, G.je};
+    const bool on[2] = {G.ring.doS, G.ring.doE};
+    for (int nS = G.is; nS <= G.ie + 1; nS++)
+        for (int p = 0; p < 2; p++) {
+            if (!on[p]) continue;
+            double s = 0.0;
+            for (int k = G.ks; k <= G.ke; k++) s = s + S.magFlux(nS, jr[p], k, KDIR);
+            const double avgFlx = s / Np;
+            for (int k = G.ks; k <= G.ke + 1; k++)
+                S.magFlux(nS, jr[p], k, KDIR) = S.magFlux(nS, jr[p], k, KDIR) - tScl * avgFlx;
+        }
+}
+// ringutils.F90:804-856 Gas2Ring / Ring2Gas (doMassRA = F: rho, momentum,
+// internal energy)
+static void Gas2Ring(const Model& M, double* W) {
+    const double D = std::max(W[DEN], dFloor);
+    const double KinE = 0.5 * (W[MOMX] * W[MOMX] + W[MOMY] * W[MOMY] + W[MOMZ] * W[MOMZ]) / D;
+    const double P = std::max((M.gamma - 1) * (W[ENERGY] - KinE), pFloor);
+    W[DEN] = D;
+    W[ENERGY] = P / (M.gamma - 1);
+}
+static void Ring2Gas(const Model& M, double* W) {
+    const double D = std::max(W[DEN], dFloor);
+    double P = (M.gamma - 1) * W[ENERGY];
+    P = std::max(P, pFloor);
+    const double KinE = 0.5 * (W[MOMX] * W[MOMX] + W[MOMY] * W[MOMY] + W[MOMZ] * W[MOMZ]) / D;
+    W[DEN] = D;
+    W[ENERGY] = KinE + P / (M.gamma - 1);
+}
+// ringav.F90:78-210 SmoothGas: per slice and ring the ring variables are
+// chunk-averaged and reconstructed, then written back as gas
+static void SmoothGas(const Model& M, const Grid& G, State& S, int pole) {
+    const int Np = G.ring.Np;
+    std::vector<double> rW(NVAR * Np), raW(NVAR * Np);
+    for (int nS = G.is; nS <= G.ie; nS++)
+        for (int nR = 1; nR <= G.ring.NumR; nR++) {
+            const int NumCh = G.ring.Nch[nR - 1], dC = Np / NumCh;
+            const int jr = pole == SPOLE ? G.js + nR - 1 : G.je - nR + 1;
+            for (int n = 0; n < Np; n++) {
+                double W[NVAR];
+                for (int v = 0; v < NVAR; v++) W[v] = S.Gas(nS, jr, G.ks + n, v);
+                Gas2Ring(M, W);
+                for (int v = 0; v < NVAR; v++) rW[v * Np + n] = W[v];
+            }
+            for (int v = 0; v < NVAR; v++)
+                for (int c = 1; c <= NumCh; c++) {
+                    const int lRs = 1 + (c - 1) * dC, lRe = lRs + dC - 1;
+                    double s = 0.0;
+                    for (int l = lRs; l <= lRe; l++) s = s + rW[v * Np + l - 1];
+                    for (int l = lRs; l <= lRe; l++) raW[v * Np + l - 1] = s / dC;
+                }
+            for (int v = 0; v < NVAR; v++) ReconstructRing(G, raW.data() + v * Np, NumCh);
+            for (int n = 0; n < Np; n++) {
+                double W[NVAR];
+                for (int v = 0; v < NVAR; v++) W[v] = raW[v * Np + n];
+                Ring2Gas(M, W);
+                for (int v = 0; v < NVAR; v++) S.Gas(nS, jr, G.ks + n, v) = W[v];
+            }
+        }
+}
+// ringav.F90:26-75 RingAverage (after the update, mhdgroup.F90:69-74)
+static void RingAverage(const Model& M, const Grid& G, State& S, F4& SmoothE) {
+    SmoothE.fill(0.0);
+    if (G.ring.doS) CalcSmoothE(G, S, SmoothE, SPOLE);
+    if (G.ring.doE) CalcSmoothE(G, S, SmoothE, EPOLE);
+    PoleE(G, SmoothE);
+    E2Flux(G, S.magFlux, SmoothE, 1.0);
+    if (G.ring.doClean) CleanLoops(G, S);
+    bFlux2Fld(G, S.magFlux, S.Bxyz);
+    if (G.ring.doS) SmoothGas(M, G, S, SPOLE);
+    if (G.ring.doE) SmoothGas(M, G, S, EPOLE);
+}
+// ringutils.F90:242-391 RingGridFix: the CFL length along k of ring cells
+// scaled by their chunk size, the ghost metric across the pole taken from the
+// conjugate cells and faces (J and K face normals reversed)
+static void RingGridFix(Grid& G) {
+    const Grid::Ring& R = G.ring;
+    for (int iR = 1; iR <= R.NumR; iR++) {
+        const int dJ = R.Np / R.Nch[iR - 1];
+        for (int k = G.ksg; k <= G.keg; k++)
+            for (int i = G.isg; i <= G.ieg; i++) {
+                if (R.doS) G.dk(i, G.js + iR - 1, k) = dJ * G.dk(i, G.js + iR - 1, k);
+                if (R.doE) G.dk(i, G.je - iR + 1, k) = dJ * G.dk(i, G.je - iR + 1, k);
+            }
+    }
+    for (int k = G.ksg; k <= G.keg + 1; k++)
+        for (int i = G.isg; i <= G.ieg + 1; i++)
+            for (int n = 1; n <= 4; n++)
+                for (int p = 0; p < 2; p++) {
+                    if (!(p == 0 ? R.doS : R.doE)) continue;
+                    const int jg = p == 0 ? G.js - n : G.je + n;
+                    int ip, jp, kp;
+                    if (k <= G.keg && i <= G.ieg) {
+                        lfmIJKcc(G, i, jg, k, ip, jp, kp);
+                        G.volume(i, jg, k) = G.volume(ip, jp, kp);
+                        G.di(i, jg, k) = G.di(ip, jp, kp);
+                        G.dj(i, jg, k) = G.dj(ip, jp, kp);
+                        G.dk(i, jg, k) = G.dk(ip, jp, kp);
+                    }
+                    for (int d = 0; d < 3; d++) {
+                        const int jf = (d == JDIR && p == 1) ? jg + 1 : jg;  // the E side's first ghost J face
+                        const double sg = d == IDIR ? 1.0 : -1.0;
+                        lfmIJKfc(G, d, i, jf, k, ip, jp, kp);
+                        for (int x = 0; x < 3; x++)
+                            G.Tf(i, jf, k, NORMX + x + 9 * d) = sg * G.Tf(ip, jp, kp, NORMX + x + 9 * d);
+                        G.face(i, jf, k, d) = G.face(ip, jp, kp, d);
+                    }
+                }
+}
+// bcs.F90:1019-1106 lfmIn / lfmOut: ghost cells across the pole take their
+// conjugate's gas and Bxyz, ghost faces its flux (J and K fluxes reversed)
+static void lfmPole(const Grid& G, State& S, int p) {
+    for (int k = G.ksg; k <= G.keg + 1; k++)
+        for (int i = G.isg; i <= G.ieg + 1; i++)
+            for (int n = 1; n <= 4; n++) {
+                const int jg = p == 0 ? G.js - n : G.je + n;
+                int ip, jp, kp;
+                if (isCellCenterG(G, i, jg, k)) {
+                    lfmIJKcc(G, i, jg, k, ip, jp, kp);
+                    for (int v = 0; v < NVAR; v++) S.Gas(i, jg, k, v) = S.Gas(ip, jp, kp, v);
+                    for (int x = 0; x < 3; x++) S.Bxyz(i, jg, k, x) = S.Bxyz(ip, jp, kp, x);
+                }
+                lfmIJKfc(G, IDIR, i, jg, k, ip, jp, kp);
+                S.magFlux(i, jg, k, IDIR) = S.magFlux(ip, jp, kp, IDIR);
+                const int jf = p == 0 ? jg : jg + 1;
+                lfmIJKfc(G, JDIR, i, jf, k, ip, jp, kp);
+                S.magFlux(i, jf, k, JDIR) = -S.magFlux(ip, jp, kp, JDIR);
+                lfmIJKfc(G, KDIR, i, jg, k, ip, jp, kp);
+                S.magFlux(i, jg, k, KDIR) = -S.magFlux(ip, jp, kp, KDIR);
+            }
 }
 // HackStep = PerStep (earthcmi.F90:224-263): PushIon (:586-663), then
 // NudgeSW with the wind outside (below)
@@ -1243,6 +1702,7 @@ static void PushIon(const Model& M, const Grid& G, State& S) {
 // (-|V|, 0, 0)): WindEFix (apps/wind.F90:489-566) with DiffuseOuter
 // (:570-616, doSWDiffuse = T) in HackE, NudgeSW (:394-486) in HackStep.
 static double wgtWind(const double* V, const double* xyz);
+static double Con2Fast(const Model& M, const double* gCon, const double* B);
 static void DiffuseOuter(const Model& M, const Grid& G, const State& S, int i, int j, int k, double vSW, double* Ed) {
     double Jd[3] = {0.0, 0.0, 0.0};
     double bP = S.magFlux(i, j, k, JDIR) / std::max(G.face(i, j, k, JDIR), TINY);
@@ -1298,6 +1758,21 @@ static void WindEFix(const Model& M, const Grid& G, State& S) {
                     for (int x = 0; x < 3; x++) S.Efld(i, j, k, x) = S.Efld(i, j, k, x) + wSW * Ed[x];
                 }
             }
+    if (G.ring.on) {  // the pole's EMFs of these shells (:549-564)
+        const int jp[2] = {G.je + 1, G.js};
+        const bool on[2] = {G.ring.doE, G.ring.doS};
+        for (int n = G.ie - 2; n <= G.ie + 1; n++)
+            for (int p = 0; p < 2; p++) {
+                if (!on[p]) continue;
+                double s = 0.0;
+                for (int k = G.ks; k <= G.ke; k++) s = s + S.Efld(n, jp[p], k, IDIR);
+                const double avgEi = s / G.ring.Np;
+                for (int k = G.ksg; k <= G.keg; k++) {
+                    S.Efld(n, jp[p], k, IDIR) = avgEi;
+                    S.Efld(n, jp[p], k, KDIR) = 0.0;
+                }
+            }
+    }
 }
 static void NudgeSW(const Model& M, const Grid& G, State& S) {
     const double V[3] = {M.wind[2], M.wind[3], M.wind[4]};
@@ -1317,6 +1792,22 @@ static void NudgeSW(const Model& M, const Grid& G, State& S) {
                 for (int v = 0; v < NVAR; v++) S.Gas(ip, j, k, v) = gCon[v];
             }
         }
+    if (G.ring.on && G.ring.doE) {  // the small ring about the axis flows out (:458-484)
+        for (int k = G.ks; k <= G.ke; k++)
+            for (int n = 0; n <= 1; n++) {
+                const int i = G.ie, j = G.je + n;
+                if (S.Gas(i, j, k, MOMX) > 0) {
+                    double gCon[5], gW[5], B[3];
+                    for (int v = 0; v < NVAR; v++) gCon[v] = S.Gas(i, j, k, v);
+                    for (int x = 0; x < 3; x++) B[x] = S.Bxyz(i, j, k, x);
+                    const double Cx = Con2Fast(M, gCon, B);
+                    CellC2P(M, gCon, gW);
+                    gW[VELX] = -Cx;
+                    CellP2C(M, gW, gCon);
+                    for (int v = 0; v < NVAR; v++) S.Gas(i, j, k, v) = gCon[v];
+                }
+            }
+    }
 }
 
 // ---------------------------------------------------------------- dt
@@ -1492,6 +1983,7 @@ static void ebGeom(const Grid& G, F4& Teb, int c0, int dNorm, int dT1, int dT2) 
                 }
             }
 }
+static void RingGridFix(Grid& G);
 // init.F90:793-1072 Corners2Grid
 static void Corners2Grid(const Model& M, Grid& G) {
     G.cellArr(G.xyzcc, 3);
@@ -1573,6 +2065,7 @@ static void Corners2Grid(const Model& M, Grid& G) {
                 fA = std::max(G.face(i, j, k + 1, KDIR), G.face(i, j, k, KDIR));
                 G.dk(i, j, k) = G.volume(i, j, k) / fA;
             }
+    if (G.ring.on) RingGridFix(G);  // init.F90:960
     G.faceArr(G.edge, 3, 1.0);
     G.faceArr(G.Te, 27);
     for (int d = 0; d < 3; d++) {
@@ -2278,13 +2771,30 @@ static void WindBC(const Model& M, const Grid& G, State& S) {
                     S.magFlux(ig, j, k, d) = wSW * swFlx + (1 - wSW) * inFlx;
                 }
             }
+    // Bxyz of each ghost from its conjugate cell's fluxes (:335-347), then
+    // the ghosts across the pole from their conjugate (:349-373)
 #pragma omp parallel for collapse(2)
     for (int k = G.ksg; k <= G.keg; k++)
         for (int j = G.jsg; j <= G.jeg; j++)
             for (int n = 1; n <= 4; n++) {
+                int ip, jp, kp;
+                lfmIJKcc(G, G.ie + n, j, k, ip, jp, kp);
                 double B[3];
-                gamCellBxyz(G, S.magFlux, G.ie + n, j, k, B);
+                gamCellBxyz(G, S.magFlux, ip, jp, kp, B);
                 for (int x = 0; x < 3; x++) S.Bxyz(G.ie + n, j, k, x) = B[x];
+            }
+    for (int k = G.ksg; k <= G.keg; k++)
+        for (int i = G.ie + 1; i <= G.ieg; i++)
+            for (int n = 1; n <= 4; n++) {
+                int ip, jp, kp;
+                if (G.ring.doS) {
+                    lfmIJKcc(G, i, G.js - n, k, ip, jp, kp);
+                    for (int x = 0; x < 3; x++) S.Bxyz(i, G.js - n, k, x) = S.Bxyz(ip, jp, kp, x);
+                }
+                if (G.ring.doE) {
+                    lfmIJKcc(G, i, G.je + n, k, ip, jp, kp);
+                    for (int x = 0; x < 3; x++) S.Bxyz(i, G.je + n, k, x) = S.Bxyz(ip, jp, kp, x);
+                }
             }
 }
 
@@ -2294,6 +2804,7 @@ struct App {
     Grid G;
     State S, oS, ooS, hS;
     F4 gFlx, mFlx, dGasH, dGasM, Vf;
+    F4 SmoothE;  // ring averaging's smoothing EMFs
     int status = 0;
 };
 
@@ -2318,6 +2829,7 @@ static void AdvanceMHD(App& A, double dt) {
     }
     CalcStress(A.M, A.G, A.S, A.hS, A.gFlx, A.mFlx, A.dGasH, A.dGasM);
     applyUpdate(A.M, A.G, A.S, A.oS, A.ooS, dt, A.dGasH, A.dGasM, A.S.Efld);
+    if (A.G.ring.on && (A.G.ring.doS || A.G.ring.doE)) RingAverage(A.M, A.G, A.S, A.SmoothE);
 }
 // gamapp.F90:73-113 stepGamera + UpdateStateData
 static int stepGamera(App& A) {
@@ -2373,6 +2885,18 @@ void* orc_create(const Params* p, const double* xyz) {
     G.is = 1; G.ie = G.Nip; G.js = 1; G.je = G.Njp; G.ks = 1; G.ke = G.Nkp;
     G.isg = G.is - 4; G.ieg = G.ie + 4; G.jsg = G.js - 4; G.jeg = G.je + 4; G.ksg = G.ks - 4; G.keg = G.ke + 4;
     for (int n = 0; n < 6; n++) G.bc[n] = p->bc[n];
+    if (p->ringNumR > 0) {  // InitRings (ringutils.F90:37-236), gid "lfm", single domain
+        G.ring.on = true;
+        G.ring.doS = p->bc[2] == BC_LFM;
+        G.ring.doE = p->bc[3] == BC_LFM;
+        G.ring.NumR = p->ringNumR;
+        G.ring.Np = p->Nkp;
+        for (int n = 0; n < p->ringNumR && n < 32; n++) G.ring.Nch[n] = p->ringNch[n];
+        G.ring.recon = p->ringRecon;
+        G.ring.NFTMAG = p->ringNFT;
+        G.ring.doClean = p->ringClean != 0;
+        G.ring.doFast = p->ringFast != 0;
+    }
     G.faceArr(G.xyz, 3);
     std::memcpy(G.xyz.v.data(), xyz, G.xyz.v.size() * sizeof(double));
     SetDomain(G);
@@ -2394,6 +2918,7 @@ void* orc_create(const Params* p, const double* xyz) {
     G.cellArr(A->dGasH, 5);
     G.cellArr(A->dGasM, 3);
     G.cellArr(A->Vf, 3);
+    if (G.ring.on) G.cellArr(A->SmoothE, 3);
     return A;
 }
 

@@ -26,6 +26,8 @@ BC_ZEROGRAD = 2
 BC_SPHIN = 3
 BC_WIND = 4
 BC_INFLOW = 6
+BC_ION = 7
+BC_LFM = 8
 
 
 def build(quiet: bool = True) -> None:
@@ -44,7 +46,8 @@ class _Params(C.Structure):
         ("tFin", C.c_double), ("dt0", C.c_double), ("limDT0", C.c_double), ("fixedDT", C.c_double),
         ("bc", C.c_int * 6), ("noMetric", C.c_int), ("M0", C.c_double), ("wind", C.c_double * 8),
         ("inflow", C.c_double * 8), ("doBoris", C.c_int), ("Ca", C.c_double),
-        ("doAB3", C.c_int),
+        ("doAB3", C.c_int), ("ringNumR", C.c_int), ("ringNch", C.c_int * 32), ("ringRecon", C.c_int),
+        ("ringNFT", C.c_int), ("ringClean", C.c_int), ("ringFast", C.c_int),
     ]
 
 
@@ -86,12 +89,24 @@ class OracleParams:
     doBoris: bool = False
     Ca: float = 0.0
     doAB3: bool = False
+    # ring averaging about the LFM axis: chunks per ring (empty: off), ring
+    # reconstruction (0 PPM, 1 PLM, 2 PCM), Fourier modes removed from the
+    # fluxes, loop cleaning and its fast form
+    ringNch: tuple = ()
+    ringRecon: int = 0
+    ringNFT: int = 1
+    ringClean: bool = True
+    ringFast: bool = True
 
     def to_c(self) -> _Params:
         p = _Params()
         for f, _ in _Params._fields_:
             if f == "bc":
                 p.bc[:] = list(self.bc)
+            elif f == "ringNumR":
+                p.ringNumR = len(self.ringNch)
+            elif f == "ringNch":
+                p.ringNch[:len(self.ringNch)] = list(self.ringNch)
             elif f in ("wind", "inflow"):
                 getattr(p, f)[:] = list(getattr(self, f))
             else:
