@@ -52,7 +52,8 @@ enum {
  * with the model hooks that come with it (gam_set_ionosphere). */
 enum { GAM_BC_PERIODIC = 0, GAM_BC_NONE = 1, GAM_BC_ZEROGRAD = 2, GAM_BC_SPHIN = 3, GAM_BC_WIND = 4,
        GAM_BC_HALO = 5 /* a tile's side towards a neighbour: filled by the caller's halo exchange */,
-       GAM_BC_INFLOW = 6, GAM_BC_ION = 7 };
+       GAM_BC_INFLOW = 6, GAM_BC_ION = 7,
+       GAM_BC_LFM = 8 /* INJ / OUTJ on the LFM axis (lfmIn / lfmOut, bcs.F90:1019-1106), with rings */ };
 enum { GAM_RECON_8CENT = 0, GAM_RECON_7UP = 1 };
 enum { GAM_FP64 = 0, GAM_FP32 = 1 };
 
@@ -260,6 +261,41 @@ int gam_set_inflow(gam_handle* h, const double state[8]);
  * does (EFix and PerStep test hasLowerBC / hasUpperBC). The k boundaries must
  * be periodic (the reference stops on a k decomposition of the magnetosphere,
  * earthcmi.F90:145-148). */
+/* Ring averaging about the LFM axis (ring/doRing with ring/gid = "lfm":
+ * InitRings ringutils.F90:37-236, RingAverage ringav.F90:26-75). A grid with
+ * bc[2] and/or bc[3] = GAM_BC_LFM has the pole (the x axis) at js and/or
+ * je+1; the other J side may be a tile's halo. The k boundaries must be
+ * periodic with an even Nkp >= 8 (WrapK maps a ghost across the axis to
+ * k + Nkp/2). Call before the geometry: the metric takes RingGridFix. With
+ * it the step does what the reference does for such a grid:
+ *   - the pole boundaries lfmIn / lfmOut (ghost cells take their conjugate
+ *     across the axis, J and K face fluxes reversed) and RingFlux2FieldFix
+ *     in every bFlux2Fld;
+ *   - RingFlux (no flux through the pole faces) with FixGasFluxLFM, PoleE
+ *     (with FixEFieldLFM) before the face update;
+ *   - RingAverage after the update: the smoothing EMFs of the rings
+ *     (Fourier modes 0..NFTmag of the ring fluxes removed, chunk averages
+ *     reconstructed, modes put back), PoleE on them, E2Flux, CleanLoops
+ *     (doClean, doFastClean), bFlux2Fld, SmoothGas (ring variables rho,
+ *     momentum, internal energy chunk-averaged and reconstructed);
+ *   - CalcDT after the ring average and the hooks (gamapp.F90:78-80);
+ *   - with the ionosphere and the wind: the ring branches of IonInner,
+ *     WindBC, WindEFix and NudgeSW.
+ * NumR rings per pole with Nch[0..NumR-1] chunks each (each dividing Nkp;
+ * gam_ring_defaults gives the reference's table by Nkp), recon the ring
+ * reconstruction (ring/rngrec: 0 PPM, 1 PLM, 2 PCM), NFTmag the Fourier
+ * modes removed from the fluxes (ringknobs/NMag, -1..2). The rings of the two
+ * poles must not meet: Njp > 2 NumR + 2. The reference's defaults keep
+ * doShift, doVClean and doMassRA off (and WENO reconstruction is not built).
+ * The driver's own metric (gam_set_geometry_arrays) already holds
+ * RingGridFix. */
+int gam_set_rings(gam_handle* h, int32_t NumR, const int32_t* Nch, int32_t recon, int32_t NFTmag, int32_t doClean,
+                  int32_t doFastClean);
+/* The reference's default rings for Np cells around the axis (InitRings,
+ * ringutils.F90:126-190; aggressive = ring/doAggressive): NumR and Nch[0..31].
+ * GAM_EINVAL for an Np without defaults (the reference has none either). */
+int gam_ring_defaults(int32_t Np, int32_t aggressive, int32_t* NumR, int32_t* Nch);
+
 int gam_set_ionosphere(gam_handle* h, const double* inExyz, const double* inEijk, double M0, double dtCpl,
                        int32_t doIonPush, int32_t nIonP, double dtSW0);
 

@@ -6,6 +6,7 @@
 #include <stdlib.h>
 #include <string.h>
 #include <algorithm>
+#include <cmath>
 #include <string>
 #include <vector>
 #include "../../include/gamgpu.h"
@@ -40,7 +41,8 @@ void gam_geom_fill(double* p, long n, double v, cudaStream_t s);
 void gam_geom_d2f(const double* src, float* dst, long n, cudaStream_t s);
 void gam_geom_dxf(const GamBox& b, const double* xfc, const double* xyzcc, float* dxf, cudaStream_t s);
 void gam_geom_metric(const GamBox& b, const double* xyz, double* face, double* xfc, double* Tf, double* vol,
-                     double* xyzcc, double* dijk, double* dl, double* edge, double* Te, double* Teb, cudaStream_t s);
+                     double* xyzcc, double* dijk, double* dl, double* edge, double* Te, double* Teb,
+                     const GamRingGeo& ring, cudaStream_t s);
 void gam_geom_ic_ot(const GamBox& b, const double* xyzcc, const double* face, double* Gas, double* mf, double gamma,
                     cudaStream_t s);
 void gam_geom_ic_case(const GamBox& b, const double* xyz, const double* xyzcc, const double* vol, double* Gas,
@@ -80,6 +82,8 @@ struct gam_handle {
     BgD bg{};
     double* windTab = nullptr;  // device: wC, wF(3), sF(3) of the solar-wind BC
     double* ionTab = nullptr;   // device: the ionospheric boundary's tables (gam_set_ionosphere)
+    GamRingGeo ringGeo{};       // ring averaging about the LFM axis (gam_set_rings)
+    bool haveRings = false;
     long ionCap = 0;
     double* ionWind = nullptr;  // device: the wind side of its hooks (WindEFix, NudgeSW weights)
     double ionDtSW0 = 0.0;
@@ -116,6 +120,7 @@ static int fail(gam_handle* h, int code, const std::string& msg) {
     if (h) h->err = msg;
     return code;
 }
+static void drop_graphs(gam_handle* h);
 static bool is_tile(const gam_handle* h) {
     for (int n = 0; n < 6; n++)
         if (h->p.bc[n] == GAM_BC_HALO) return true;
@@ -265,8 +270,8 @@ extern "C" int gam_create(const gam_params* p, gam_handle** out) {
         auto in = [](int v, int a, int b2, int c2) { return v == a || v == b2 || v == c2 || v == GAM_BC_HALO; };
         if (!(in(c[0], GAM_BC_PERIODIC, GAM_BC_NONE, GAM_BC_SPHIN) || c[0] == GAM_BC_INFLOW || c[0] == GAM_BC_ION) ||
             !(in(c[1], GAM_BC_PERIODIC, GAM_BC_NONE, GAM_BC_WIND) || c[1] == GAM_BC_ZEROGRAD) ||
-            !in(c[2], GAM_BC_PERIODIC, GAM_BC_NONE, GAM_BC_ZEROGRAD) ||
-            !in(c[3], GAM_BC_PERIODIC, GAM_BC_NONE, GAM_BC_ZEROGRAD) ||
+            !(in(c[2], GAM_BC_PERIODIC, GAM_BC_NONE, GAM_BC_ZEROGRAD) || c[2] == GAM_BC_LFM) ||
+            !(in(c[3], GAM_BC_PERIODIC, GAM_BC_NONE, GAM_BC_ZEROGRAD) || c[3] == GAM_BC_LFM) ||
             !in(c[4], GAM_BC_PERIODIC, GAM_BC_NONE, GAM_BC_NONE) || !in(c[5], GAM_BC_PERIODIC, GAM_BC_NONE, GAM_BC_NONE))
             return bad(GAM_EINVAL, "unsupported boundary kind for this side");
         for (int d = 0; d < 3; d++)
@@ -276,6 +281,13 @@ extern "C" int gam_create(const gam_params* p, gam_handle** out) {
             return bad(GAM_EINVAL, "the ionospheric boundary wraps k: the k boundaries must be periodic");
         if (c[0] == GAM_BC_PERIODIC && (c[2] == GAM_BC_ZEROGRAD || c[3] == GAM_BC_ZEROGRAD))
             return bad(GAM_EINVAL, "zero-gradient J with periodic I is not supported");
+        if (c[2] == GAM_BC_LFM || c[3] == GAM_BC_LFM) {
+            const bool ok2 = c[2] == GAM_BC_LFM || c[2] == GAM_BC_HALO, ok3 = c[3] == GAM_BC_LFM || c[3] == GAM_BC_HALO;
+            if (!ok2 || !ok3) return bad(GAM_EINVAL, "an LFM pole's other J side is the other pole or a tile's halo");
+            if (c[4] != GAM_BC_PERIODIC || p->do25D)
+                return bad(GAM_EINVAL, "the LFM pole wraps k: the k boundaries must be periodic (3-D)");
+            if (p->Nkp < 8 || p->Nkp % 2) return bad(GAM_EBADDIM, "the LFM pole needs an even Nkp >= 8");
+        }
     }
     if (p->do25D && (p->bc[4] != GAM_BC_PERIODIC || p->bc[5] != GAM_BC_PERIODIC))
         return bad(GAM_EINVAL, "do25D replicates k: the k boundaries must be periodic");
@@ -421,12 +433,128 @@ static void sync_geo_f32(gam_handle* h) {
     gam_geom_dxf(h->b, h->gd.xfc, h->gd.xyzcc, (float*)g.dxf, h->s);
 }
 
+static bool has_lfm(const gam_handle* h) { return h->p.bc[2] == GAM_BC_LFM || h->p.bc[3] == GAM_BC_LFM; }
+
+// ------------------------------------------------------------ rings (LFM axis)
+// InitRings's defaults for gid "lfm" (ringutils.F90:126-190)
+extern "C" int gam_ring_defaults(int32_t Np, int32_t aggressive, int32_t* NumR, int32_t* Nch) {
+    if (!NumR || !Nch) return GAM_EINVAL;
+    static const int d8[] = {4}, d16[] = {8}, d32[] = {8, 16}, d64[] = {8, 16, 32, 32},
+                     d64a[] = {8, 16, 32, 32, 32, 32, 32, 32}, d128[] = {8, 16, 32, 32, 64, 64, 64, 64},
+                     d128a[] = {8, 16, 32, 32, 64, 64, 64, 64, 64, 64, 64, 64},
+                     d256[] = {8, 16, 32, 32, 64, 64, 64, 64, 128, 128, 128, 128},
+                     d256a[] = {8, 16, 32, 32, 64, 64, 64, 64, 128, 128, 128, 128, 128, 128, 128, 128},
+                     d512[] = {8, 16, 32, 32, 64, 64, 64, 64, 128, 128, 128, 128, 256, 256, 256, 256},
+                     d512a[] = {8, 16, 32, 32, 64, 64, 64, 64, 128, 128, 128, 128, 128, 128, 256, 256, 256, 256,
+                                256, 256, 256, 256};
+    const int* t = nullptr;
+    int n = 0;
+#define GAM_RING_CASE(np, a, b2)                                   \
+    case np:                                                       \
+        if (aggressive) { t = a; n = sizeof(a) / sizeof(int); }     \
+        else { t = b2; n = sizeof(b2) / sizeof(int); }               \
+        break;
+    switch (Np) {
+        GAM_RING_CASE(8, d8, d8)
+        GAM_RING_CASE(16, d16, d16)
+        GAM_RING_CASE(32, d32, d32)
+        GAM_RING_CASE(64, d64a, d64)
+        GAM_RING_CASE(128, d128a, d128)
+        GAM_RING_CASE(256, d256a, d256)
+        GAM_RING_CASE(512, d512a, d512)
+        default: return GAM_EINVAL;
+    }
+#undef GAM_RING_CASE
+    *NumR = n;
+    for (int q = 0; q < 32; q++) Nch[q] = q < n ? t[q] : 0;
+    return GAM_OK;
+}
+
+extern "C" int gam_set_rings(gam_handle* h, int32_t NumR, const int32_t* Nch, int32_t recon, int32_t NFTmag,
+                             int32_t doClean, int32_t doFastClean) {
+    if (!h || !Nch) return GAM_EINVAL;
+    if (!has_lfm(h)) return fail(h, GAM_ESTATE, "no J side is the LFM pole (GAM_BC_LFM)");
+    if (h->haveGeo) return fail(h, GAM_ESTATE, "the rings enter the metric: set them before the geometry");
+    const GamBox& b = h->b;
+    const int Np = b.Nkp;
+    const bool doS = h->p.bc[2] == GAM_BC_LFM, doE = h->p.bc[3] == GAM_BC_LFM;
+    if (NumR < 1 || NumR > 32 || NumR >= b.Njp) return fail(h, GAM_EINVAL, "1 <= NumR <= 32 and NumR < Njp");
+    if (doS && doE && b.Njp <= 2 * NumR + 2) return fail(h, GAM_EINVAL, "the rings of the two poles meet: Njp > 2 NumR + 2");
+    if (recon < 0 || recon > 2) return fail(h, GAM_EINVAL, "ring reconstruction: 0 PPM, 1 PLM, 2 PCM");
+    if (NFTmag < -1 || NFTmag > 2) return fail(h, GAM_EINVAL, "NFTmag in -1..2 (NFTMAX = 2)");
+    int ncMax = 0;
+    for (int q = 0; q < NumR; q++) {
+        if (Nch[q] < 1 || Np % Nch[q]) return fail(h, GAM_EINVAL, "every ring's chunk count must divide Nkp");
+        ncMax = std::max(ncMax, (int)Nch[q]);
+    }
+    GamRingGeo& rg = h->ringGeo;
+    rg = GamRingGeo{};
+    rg.on = 1;
+    rg.doS = doS;
+    rg.doE = doE;
+    rg.NumR = NumR;
+    rg.Np = Np;
+    for (int q = 0; q < NumR; q++) rg.Nch[q] = Nch[q];
+    // cos / sin of m phi_n at the ring cell centres (CleanRing, ringav.F90:
+    // 446-453), host libm like the CPU code: phi = dp n - dp/2, dp = 2 pi / Np
+    const double PI = 3.141592653589793;
+    std::vector<double> ft(6L * Np);
+    const double dp = 2.0 * PI / Np;
+    for (int m = 0; m <= 2; m++)
+        for (int n = 1; n <= Np; n++) {
+            const double phi = dp * n - 0.5 * dp;
+            ft[(2 * m) * Np + n - 1] = std::cos(1.0 * m * phi);
+            ft[(2 * m + 1) * Np + n - 1] = std::sin(1.0 * m * phi);
+        }
+    cudaError_t e = cudaSuccess;
+    double* dft = dalloc<double>(h, 6L * Np, &e);
+    if (e != cudaSuccess) return fail(h, GAM_ECUDA, "device allocation failed (ring tables)");
+    CK(h, cudaMemcpyAsync(dft, ft.data(), ft.size() * sizeof(double), cudaMemcpyHostToDevice, h->s));
+    const size_t w = h->f32 ? 4 : 8;
+    const long nthr = 2L * (b.Nip + 1) * NumR, stride = 5L * (ncMax + 4);
+    void* sE = nullptr;
+    void* ch = nullptr;
+    if (h->f32) {
+        sE = dalloc<float>(h, 3 * b.fs, &e);
+        if (e == cudaSuccess) ch = dalloc<float>(h, nthr * stride, &e);
+    } else {
+        sE = dalloc<double>(h, 3 * b.fs, &e);
+        if (e == cudaSuccess) ch = dalloc<double>(h, nthr * stride, &e);
+    }
+    (void)w;
+    if (e != cudaSuccess) return fail(h, GAM_ECUDA, "device allocation failed (ring work arrays)");
+    RingData R{};
+    R.on = 1;
+    R.doS = doS;
+    R.doE = doE;
+    R.NumR = NumR;
+    R.Np = Np;
+    R.recon = recon;
+    R.nft = NFTmag;
+    R.clean = doClean ? 1 : 0;
+    R.tScl = doFastClean ? 1.0 : (double)(1.0f / (float)Np);  // 1.0/Np in default real
+    R.aScl = (double)(2.0f / (float)Np);                          // 2.0/Np in default real
+    for (int q = 0; q < NumR; q++) R.Nch[q] = Nch[q];
+    R.chunkStride = (int)stride;
+    R.ftab = dft;
+    R.smoothE = sE;
+    R.chunk = ch;
+    h->cd.P.ring = R;
+    h->cf.P.ring = R;
+    CK(h, cudaStreamSynchronize(h->s));
+    drop_graphs(h);
+    h->haveRings = true;
+    return GAM_OK;
+}
+
 extern "C" int gam_set_geometry(gam_handle* h, const double* xyz) {
     if (!h || !xyz) return GAM_EINVAL;
+    if (has_lfm(h) && !h->haveRings) return fail(h, GAM_ESTATE, "an LFM pole: call gam_set_rings before the geometry");
     int rc = up_d(h, xyz, h->gd.xyz, true, 3);
     if (rc) return rc;
     GeoD& g = h->gd;
-    gam_geom_metric(h->b, g.xyz, g.face, g.xfc, g.Tf, g.vol, g.xyzcc, g.dijk, g.dl, g.edge, g.Te, g.Teb, h->s);
+    gam_geom_metric(h->b, g.xyz, g.face, g.xfc, g.Tf, g.vol, g.xyzcc, g.dijk, g.dl, g.edge, g.Te, g.Teb, h->ringGeo,
+                    h->s);
     sync_geo_f32(h);
     CK(h, cudaGetLastError());
     CK(h, cudaStreamSynchronize(h->s));
@@ -439,6 +567,7 @@ extern "C" int gam_set_geometry_arrays(gam_handle* h, const double* face, const 
                                        const double* volume, const double* xyzcc, const double* di, const double* dj,
                                        const double* dk, const double* edge, const double* Te, const double* Teb) {
     if (!h || !face || !xfc || !Tf || !volume || !xyzcc || !di || !dj || !dk || !edge || !Te || !Teb) return GAM_EINVAL;
+    if (has_lfm(h) && !h->haveRings) return fail(h, GAM_ESTATE, "an LFM pole: call gam_set_rings before the geometry");
     GeoD& g = h->gd;
     const long fs = h->b.fs;
     int rc;
@@ -1377,14 +1506,21 @@ extern "C" int gam_set_ionosphere(gam_handle* h, const double* inExyz, const dou
     // perpendicular to the radius plus its inward radial part
     for (int kk = 0; kk < Nk; kk++)
         for (int jj = 0; jj < Nj; jj++) {
-            int kp = kk;
+            int kp = kk, jp = jj;
             if (kk < G) kp = kk + b.Nkp;
             else if (kk >= G + b.Nkp) kp = kk - b.Nkp;
+            // across the LFM pole: the conjugate (mirrored j, k + Nkp/2)
+            const GamRingGeo& rg = h->ringGeo;
+            if (rg.on && ((rg.doS && jj < G) || (rg.doE && jj > G + b.Njp - 1 && jj <= G + b.Njp + 3))) {
+                jp = jj < G ? 2 * G - 1 - jj : 2 * G + 2 * b.Njp - 1 - jj;
+                kp = kk + b.Nkp / 2;
+                if (kp > G + b.Nkp - 1) kp -= b.Nkp;
+            }
             for (int n = 1; n <= 4; n++) {
                 double r[3], B[3], rh[3], E[3], v[3], vr;
-                X(G - n, jj, kp, r);
+                X(G - n, jp, kp, r);
                 ion_dipole(M0, r, B);
-                for (int x = 0; x < 3; x++) E[x] = Exyz(4 - n, jj, kp, x);
+                for (int x = 0; x < 3; x++) E[x] = Exyz(4 - n, jp, kp, x);
                 norm_vec(r, rh);
                 ion_exb_perp(E, B, rh, v, &vr);
                 const double vin = std::min(vr, 0.0);

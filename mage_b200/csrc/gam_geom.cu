@@ -761,10 +761,70 @@ void gam_geom_d2f(const double* src, float* dst, long n, cudaStream_t s) {
     if (n > 0) k_d2f<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(src, dst, n);
 }
 
+// RingGridFix (ringutils.F90:242-391) for the LFM axis, between the CFL
+// lengths and the edge metric (init.F90:960): the k length of the ring cells
+// scaled by their chunk size (every i and k), then the ghost metric across
+// the pole from the conjugate cells and faces.
+__device__ __forceinline__ int geo_wrapk(const GamBox& b, int kk) {
+    int kp = kk + b.Nkp / 2;
+    if (kp > GAM_NG + b.Nkp - 1) kp -= b.Nkp;
+    return kp;
+}
+__global__ void k_ring_dk(GamBox b, GamRingGeo rg, double* dijk, double* dl) {
+    const long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    const long nrow = (long)b.Ni * b.Nk;
+    if (q >= 2L * rg.NumR * nrow) return;
+    const int pole = (int)(q / (rg.NumR * nrow));
+    if (!(pole == 0 ? rg.doS : rg.doE)) return;
+    const long r = q % (rg.NumR * nrow);
+    const int iR = 1 + (int)(r / nrow), ii = (int)(r % nrow % b.Ni), kk = (int)(r % nrow / b.Ni);
+    const int jj = pole == 0 ? GAM_NG + iR - 1 : GAM_NG + b.Njp - iR;
+    const long c = lidx(b, ii, jj, kk), fs = b.fs;
+    const int dJ = rg.Np / rg.Nch[iR - 1];
+    const double dk = dJ * dijk[2 * fs + c];
+    dijk[2 * fs + c] = dk;
+    double m = dijk[c];
+    if (dijk[fs + c] < m) m = dijk[fs + c];
+    if (dk < m) m = dk;
+    dl[c] = m;
+}
+__global__ void k_ring_ghost_metric(GamBox b, GamRingGeo rg, double* face, double* Tf, double* vol, double* dijk,
+                                    double* dl) {
+    const long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    const int ni = b.Ni + 1, nk = b.Nk + 1;
+    const long nrow = (long)ni * nk;
+    if (q >= 8L * nrow) return;  // 2 poles x 4 ghost rows
+    const int pole = (int)(q / (4 * nrow)), n = 1 + (int)(q / nrow % 4);
+    if (!(pole == 0 ? rg.doS : rg.doE)) return;
+    const int ii = (int)(q % nrow % ni), kk = (int)(q % nrow / ni);
+    const int G = GAM_NG, N = b.Njp;
+    const int jg = pole == 0 ? G - n : G + N - 1 + n;
+    const int kc = geo_wrapk(b, kk);
+    const long fs = b.fs;
+    // conjugate cell (lfmIJKcc): also the I and K faces' conjugate row
+    const int jc = pole == 0 ? 2 * G - 1 - jg : 2 * G + 2 * N - 1 - jg;
+    if (ii < b.Ni && kk < b.Nk) {
+        const long c = lidx(b, ii, jg, kk), cc = lidx(b, ii, jc, kc);
+        vol[c] = vol[cc];
+        for (int x = 0; x < 3; x++) dijk[x * fs + c] = dijk[x * fs + cc];
+        dl[c] = dl[cc];
+    }
+    for (int d = 0; d < 3; d++) {
+        // the E side's first ghost J face is je+2; J faces see the pole once
+        const int jf = (d == 1 && pole == 1) ? jg + 1 : jg;
+        const int jp = d == 1 ? (pole == 0 ? 2 * G - jf : 2 * G + 2 * N - jf) : jc;
+        const long c = lidx(b, ii, jf, kk), cc = lidx(b, ii, jp, kc);
+        const double sg = d == 0 ? 1.0 : -1.0;
+        for (int x = 0; x < 3; x++) Tf[(x + 9 * d) * fs + c] = sg * Tf[(x + 9 * d) * fs + cc];
+        face[d * fs + c] = face[d * fs + cc];
+    }
+}
+
 // Metric from corners already in the box layout (xyz: 3 comps).
 // dijk: 3 comps; dl: min(di,dj,dk).
 void gam_geom_metric(const GamBox& b, const double* xyz, double* face, double* xfc, double* Tf, double* vol,
-                     double* xyzcc, double* dijk, double* dl, double* edge, double* Te, double* Teb, cudaStream_t s) {
+                     double* xyzcc, double* dijk, double* dl, double* edge, double* Te, double* Teb,
+                     const GamRingGeo& ring, cudaStream_t s) {
     const long fs = b.fs;
     gam_geom_fill(face, 3 * fs, 1.0, s);
     gam_geom_fill(xfc, 9 * fs, 0.0, s);
@@ -778,6 +838,11 @@ void gam_geom_metric(const GamBox& b, const double* xyz, double* face, double* x
     dim3 blkv(64, 1, 1);
     k_geo_cells<<<g3(b.Ni, b.Nj, b.Nk, blkv), blkv, 0, s>>>(b, xyz, vol, xyzcc);
     k_geo_dijk<<<g3(b.Ni, b.Nj, b.Nk, blk), blk, 0, s>>>(b, vol, face, dijk, dl);
+    if (ring.on) {
+        const long n1 = 2L * ring.NumR * b.Ni * b.Nk, n2 = 8L * (b.Ni + 1) * (b.Nk + 1);
+        k_ring_dk<<<(unsigned)((n1 + 255) / 256), 256, 0, s>>>(b, ring, dijk, dl);
+        k_ring_ghost_metric<<<(unsigned)((n2 + 255) / 256), 256, 0, s>>>(b, ring, face, Tf, vol, dijk, dl);
+    }
     for (int d = 0; d < 3; d++) k_geo_edges<<<g3(b.Ni + 1, b.Nj + 1, b.Nk + 1, blk), blk, 0, s>>>(b, xyz, edge, Te, d);
     for (int dN = 0; dN < 3; dN++) {
         int T1 = (dN + 1) % 3, T2 = (dN + 2) % 3;

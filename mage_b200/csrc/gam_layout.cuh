@@ -32,6 +32,13 @@ static inline GamBox gam_make_box(int Nip, int Njp, int Nkp) {
     return b;
 }
 
+// The ring configuration the metric needs (RingGridFix): rings per pole and
+// their chunks, which poles this grid holds
+struct GamRingGeo {
+    int on, doS, doE, NumR, Np;
+    int Nch[32];
+};
+
 // Scalars of Model_T / State_T that change every step; they live in device
 // memory so a sequence of steps runs without host round trips.
 struct GamScalars {

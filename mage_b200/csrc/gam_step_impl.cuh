@@ -29,6 +29,7 @@
 // strict build reproduces an IEEE-strict CPU step bit for bit.
 #pragma once
 
+#include <algorithm>
 #include <cuda_runtime.h>
 #include <nvtx3/nvToolsExt.h>
 #include <stdint.h>
@@ -392,6 +393,52 @@ __device__ __forceinline__ bool box_ok(const GamBox& b, long lo, long hi, const 
     } while (0)
 #endif
 
+// ----------------------------------------------------------------- LFM pole
+// Index maps across the LFM axis (ringutils.F90:482-659, box indices): the
+// pole at js (doS) / je+1 (doE), k shifted by half a ring (WrapK).
+__device__ __forceinline__ int ring_wrapk(const GamBox& b, int kk) {
+    int kp = kk + b.Nkp / 2;
+    if (kp > GAM_NG + b.Nkp - 1) kp -= b.Nkp;
+    return kp;
+}
+// lfmIJKcc for a ghost row across the pole: its conjugate cell (true) or
+// nothing (false)
+__device__ __forceinline__ bool ring_conj_cc(const GamBox& b, const RingData& Rg, int& jj, int& kk) {
+    const int G = GAM_NG;
+    if (Rg.doS && jj < G) {
+        jj = 2 * G - 1 - jj;
+        kk = ring_wrapk(b, kk);
+        return true;
+    }
+    if (Rg.doE && jj > G + b.Njp - 1 && jj <= G + b.Njp + 3) {
+        jj = 2 * G + 2 * b.Njp - 1 - jj;
+        kk = ring_wrapk(b, kk);
+        return true;
+    }
+    return false;
+}
+// The pole boundary lfmIn / lfmOut (bcs.F90:1019-1106) as a map of value
+// comp (-1 cell, 0..2 face normal) at (jj, kk): the source and its sign
+// (J and K faces reversed); the J faces' pole face itself is not mirrored
+__device__ __forceinline__ int ring_bc_jmap(const GamBox& b, const RingData& Rg, int comp, int& jj, int& kk) {
+    const int G = GAM_NG, N = b.Njp;
+    if (comp == 1) {
+        if (Rg.doS && jj < G) {
+            jj = 2 * G - jj;
+            kk = ring_wrapk(b, kk);
+            return -1;
+        }
+        if (Rg.doE && jj >= G + N + 1 && jj <= G + N + 4) {
+            jj = 2 * G + 2 * N - jj;
+            kk = ring_wrapk(b, kk);
+            return -1;
+        }
+        return 1;
+    }
+    if (ring_conj_cc(b, Rg, jj, kk)) return comp == 2 ? -1 : 1;
+    return 1;
+}
+
 // ----------------------------------------------------------------- kernels
 // AdvanceMHD entry: time trap and AB2 spacing (mhdgroup.F90:25-31, 457)
 __global__ void k_step_begin(GamScalars* sc) {
@@ -504,7 +551,28 @@ __global__ void __launch_bounds__(256, MINB) k_predict(GamBox b, DevParams<R> P,
             }
         }
         R B[3];
-        cell_bxyz(b, g, c, hm[0], up[0], hm[1], up[1], hm[2], up[2], B);
+        int jc = jj, kc = kk;
+        if (P.ring.on && ring_conj_cc(b, P.ring, jc, kc)) {
+            // RingFlux2FieldFix in the predictor's bFlux2Fld: the conjugate
+            // cell's field from its own extrapolated fluxes
+            const long cc = lidx(b, ii, jc, kc);
+            const long off[3] = {1, (long)b.sx, b.sk};
+            R lo[3], hi[3];
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                const long f0 = d * fs + cc, f1 = f0 + off[d];
+                if constexpr (AB3) {
+                    lo[d] = extrap_ab3(pdt, cur.mf[f0], old.mf[f0], oomf[f0], odt, oodt);
+                    hi[d] = extrap_ab3(pdt, cur.mf[f1], old.mf[f1], oomf[f1], odt, oodt);
+                } else {
+                    lo[d] = cur.mf[f0] + pdt * qodt(cur.mf[f0] - old.mf[f0]);
+                    hi[d] = cur.mf[f1] + pdt * qodt(cur.mf[f1] - old.mf[f1]);
+                }
+            }
+            cell_bxyz(b, g, cc, lo[0], hi[0], lo[1], hi[1], lo[2], hi[2], B);
+        } else {
+            cell_bxyz(b, g, c, hm[0], up[0], hm[1], up[1], hm[2], up[2], B);
+        }
 #pragma unroll
         for (int x = 0; x < 3; x++) {
             w.QB[x * fs + c] = vol * B[x];
@@ -977,8 +1045,12 @@ __global__ void __launch_bounds__(128, MINB) k_update_cells(GamBox b, DevParams<
         const Quot<R> qdV(g.vol[c]);
         if (P.doMHD) {
             const long sj = b.sx, sk = b.sk;
-            cell_bxyz(b, g, c, nxt.mf[c], nxt.mf[c + 1], nxt.mf[fs + c], nxt.mf[fs + c + sj], nxt.mf[2 * fs + c],
-                      nxt.mf[2 * fs + c + sk], qdV, Bc);
+            int jc = jj, kc = kk;
+            // RingFlux2FieldFix: a cell across the pole takes its conjugate's
+            // field (the same volume, so the same quotient)
+            const long cb = (P.ring.on && ring_conj_cc(b, P.ring, jc, kc)) ? lidx(b, ii, jc, kc) : c;
+            cell_bxyz(b, g, cb, nxt.mf[cb], nxt.mf[cb + 1], nxt.mf[fs + cb], nxt.mf[fs + cb + sj], nxt.mf[2 * fs + cb],
+                      nxt.mf[2 * fs + cb + sk], qdV, Bc);
         }
         if (active) {
             const long sj = b.sx, sk = b.sk;
@@ -1046,7 +1118,7 @@ __global__ void __launch_bounds__(128, MINB) k_update_cells(GamBox b, DevParams<
                           jj <= G + b.Njp - 1 + P.dtJhi && kk >= G - P.dtKlo &&
                           kk <= G + b.Nkp - 1 + P.dtKhi && !(P.ion.push && active && ii < G + P.ion.nIonP) &&
                           !(P.ion.wind && active && ii == G + b.Nip - 1);
-        if (indt && !sc->fixedTimestep) {
+        if (indt && !sc->fixedTimestep && !P.ring.on) {
             double Ud[5], Bt[3];
 #pragma unroll
             for (int v = 0; v < 5; v++) Ud[v] = (double)U[v];
@@ -1099,24 +1171,24 @@ __global__ void __launch_bounds__(256) k_ion_efix(GamBox b, DevParams<R> P, Work
     w.E[2 * b.fs + c] = (R)P.ion.Ee[2 * q + 1];
 }
 // HackE, last part: FixEFieldLFM (gamdebug.F90:149-175), the I and J EMFs
-// of k = ks and ke+1 set to their mean, i = is..ie+1, j = js..je+1
+// of k = ks and ke+1 set to their mean, i = is..ie+1, j = j0..j1 (js..je+1)
 template <class R>
-__global__ void __launch_bounds__(256) k_fix_e_lfm(GamBox b, Work<R> w, const GamScalars* sc) {
+__global__ void __launch_bounds__(256) k_fix_e_lfm(GamBox b, R* __restrict__ E, int j0, int j1, const GamScalars* sc) {
     if (sc->halted) return;
     const int G = GAM_NG;
     const long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
     const int ni = b.Nip + 1;
-    if (q >= (long)ni * (b.Njp + 1)) return;
-    const int ii = G + (int)(q % ni), jj = G + (int)(q / ni);
+    if (q >= (long)ni * (j1 - j0 + 1)) return;
+    const int ii = G + (int)(q % ni), jj = j0 + (int)(q / ni);
     const long c0 = lidx(b, ii, jj, G), c1 = lidx(b, ii, jj, G + b.Nkp);
     GAM_BOX_CHECK(c0, c1, 15);
     const long fs = b.fs;
-    const R Ei = (R)0.5 * (w.E[c0] + w.E[c1]);
-    const R Ej = (R)0.5 * (w.E[fs + c0] + w.E[fs + c1]);
-    w.E[c0] = Ei;
-    w.E[c1] = Ei;
-    w.E[fs + c0] = Ej;
-    w.E[fs + c1] = Ej;
+    const R Ei = (R)0.5 * (E[c0] + E[c1]);
+    const R Ej = (R)0.5 * (E[fs + c0] + E[fs + c1]);
+    E[c0] = Ei;
+    E[c1] = Ei;
+    E[fs + c0] = Ej;
+    E[fs + c1] = Ej;
 }
 // HackStep: PushIon (earthcmi.F90:586-663) on the first nIonP active
 // shells after the update, then CalcDT's CellDT of those cells (k_update_cells
@@ -1156,7 +1228,7 @@ __global__ void __launch_bounds__(128) k_ion_push(GamBox b, DevParams<R> P, Geo<
 #pragma unroll
             for (int v = 0; v < 5; v++) nxt.Gas[v * fs + c] = U[v];
         }
-        if (!sc->fixedTimestep) {
+        if (!sc->fixedTimestep && !P.ring.on) {  // with rings, CalcDT runs after the ring average
             double Ud[5], Bt[3];
 #pragma unroll
             for (int v = 0; v < 5; v++) Ud[v] = (double)U[v];
@@ -1273,7 +1345,7 @@ __global__ void __launch_bounds__(128) k_nudge_sw(GamBox b, DevParams<R> P, Geo<
 #pragma unroll
             for (int v = 0; v < 5; v++) nxt.Gas[v * fs + c] = U[v];
         }
-        if (!sc->fixedTimestep) {
+        if (!sc->fixedTimestep && !P.ring.on) {  // with rings, CalcDT runs after the ring average
             double Ud[5], Bt[3];
 #pragma unroll
             for (int v = 0; v < 5; v++) Ud[v] = (double)U[v];
@@ -1299,6 +1371,444 @@ __global__ void __launch_bounds__(128) k_nudge_sw(GamBox b, DevParams<R> P, Geo<
             if (anybad) atomicAdd(&sc->nbad, 1);
         }
     }
+}
+
+
+// ----------------------------------------------------------------- ring averaging
+// Ring averaging about the LFM axis (ringav.F90, ringrecon.F90,
+// ringutils.F90; gid "lfm" with the reference's defaults: no shift, no
+// velocity cleaning, ring variables rho, momentum, internal energy). One
+// thread per ring (pole, slice i, ring nR): the ring is the k circle of row
+// js+nR-1 (S) or je-nR+1 (E); its work is sequential along k in the
+// reference's order, so the bits match the CPU restatement.
+
+// PoleE (ringav.F90:394-430) over slices i0..i1, or the same touch-up of
+// WindEFix (apps/wind.F90:549-564): on each pole row the K EMFs zero and the
+// I EMFs their mean over ks..ke, over the whole ghosted k range
+template <class R>
+__global__ void __launch_bounds__(128) k_ring_pole_e(GamBox b, RingData Rg, R* __restrict__ E, int i0, int i1,
+                                                     const GamScalars* sc) {
+    if (sc->halted) return;
+    const int G = GAM_NG;
+    const long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    const int ni = i1 - i0 + 1;
+    if (q >= 2L * ni) return;
+    const int pole = (int)(q / ni), ii = i0 + (int)(q % ni);
+    if (!(pole == 0 ? Rg.doS : Rg.doE)) return;
+    const int jp = pole == 0 ? G : G + b.Njp;
+    const long fs = b.fs;
+    GAM_BOX_CHECK(lidx(b, ii, jp, 0), lidx(b, ii, jp, b.Nk - 1), 15);
+    R sum = (R)0;
+    for (int kk = G; kk < G + b.Nkp; kk++) sum = sum + E[lidx(b, ii, jp, kk)];
+    const R avg = sum / (R)Rg.Np;
+    for (int kk = 0; kk < b.Nk; kk++) {
+        const long c = lidx(b, ii, jp, kk);
+        E[2 * fs + c] = (R)0;
+        E[c] = avg;
+    }
+}
+
+// RingFlux (ringutils.F90:662-678): no flux through the pole faces (every i,
+// k), then FixGasFluxLFM (gamdebug.F90:91-124): the K fluxes of k = ks and
+// ke+1 set to their mean, i = is..ie, j = js..je
+template <class R>
+__global__ void __launch_bounds__(256) k_ring_flux(GamBox b, DevParams<R> P, Work<R> w, const GamScalars* sc) {
+    if (sc->halted) return;
+    const int G = GAM_NG;
+    const long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    const long fs = b.fs;
+    const long nz = (long)b.Ni * b.Nk;
+    if (q < 2 * nz) {
+        const int pole = (int)(q / nz);
+        if (!(pole == 0 ? P.ring.doS : P.ring.doE)) return;
+        const long r = q % nz;
+        const int ii = (int)(r % b.Ni), kk = (int)(r / b.Ni);
+        const long c = lidx(b, ii, pole == 0 ? G : G + b.Njp, kk);
+        GAM_BOX_CHECK(c, c, 15);
+#pragma unroll
+        for (int v = 0; v < 5; v++) w.gF[(v + 5) * fs + c] = (R)0;
+        if (P.doMHD) {
+#pragma unroll
+            for (int x = 0; x < 3; x++) w.mF[(x + 3) * fs + c] = (R)0;
+        }
+        return;
+    }
+    if (!P.doMHD) return;
+    const long r = q - 2 * nz;
+    if (r >= (long)b.Nip * b.Njp) return;
+    const int ii = G + (int)(r % b.Nip), jj = G + (int)(r / b.Nip);
+    const long c0 = lidx(b, ii, jj, G), c1 = lidx(b, ii, jj, G + b.Nkp);
+    GAM_BOX_CHECK(c0, c1, 15);
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+        R* gK = w.gF + (v + 10) * fs;
+        const R gFa = (R)0.5 * (gK[c0] + gK[c1]);
+        gK[c0] = gFa;
+        gK[c1] = gFa;
+    }
+#pragma unroll
+    for (int x = 0; x < 3; x++) {
+        R* mK = w.mF + (x + 6) * fs;
+        const R mFa = (R)0.5 * (mK[c0] + mK[c1]);
+        mK[c0] = mFa;
+        mK[c1] = mFa;
+    }
+}
+
+// the smoothing EMF rows each step starts from zero (InitRAVec): S rows
+// js..js+NumR+1, E rows je-NumR..je+1, every i and k
+template <class R> __global__ void __launch_bounds__(256) k_ring_zero_e(GamBox b, RingData Rg, const GamScalars* sc) {
+    if (sc->halted) return;
+    const int G = GAM_NG, nr = Rg.NumR + 2;
+    const long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    const long nrow = (long)b.Ni * b.Nk;
+    if (q >= 2L * nr * nrow) return;
+    const int pole = (int)(q / (nr * nrow));
+    if (!(pole == 0 ? Rg.doS : Rg.doE)) return;
+    const long r = q % (nr * nrow);
+    const int row = (int)(r / nrow), ii = (int)(r % nrow % b.Ni), kk = (int)(r % nrow / b.Ni);
+    const int jj = pole == 0 ? G + row : G + b.Njp - Rg.NumR - 1 + row;
+    R* E = (R*)Rg.smoothE;
+    const long c = lidx(b, ii, jj, kk), fs = b.fs;
+#pragma unroll
+    for (int x = 0; x < 3; x++) E[x * fs + c] = (R)0;
+}
+
+// minmod (math.F90:192-197): sign() as copysign, min() as a < b
+template <class R> __device__ __forceinline__ R ring_min(R a, R b2) { return b2 < a ? b2 : a; }
+template <class R> __device__ __forceinline__ R ring_minmod(R x, R y) {
+    return (R)0.5 * (copysign((R)1, x) + copysign((R)1, y)) * ring_min(fabs(x), fabs(y));
+}
+// the interval L/R of a chunk (ringrecon.F90:224-285: PPM, PLM, PCM)
+template <class R>
+__device__ __forceinline__ void ring_lr(int recon, R fm2, R fm1, R f, R fp1, R fp2, R& vm, R& vp) {
+    if (recon == 2) {
+        vm = f;
+        vp = f;
+        return;
+    }
+    if (recon == 1) {
+        const R dwL = f - fm1, dwR = fp1 - f, dwC = (fp1 - fm1) / (R)2;
+        const R min1 = ring_min((R)2 * fabs(dwL), (R)2 * fabs(dwR));
+        const R min2 = ring_min(min1, fabs(dwC));
+        const R dwM = copysign(min2, dwC);
+        vp = f + (R)0.5 * dwM;
+        vm = f - (R)0.5 * dwM;
+        return;
+    }
+    const R dvm2 = fm1 - fm2, dvm1 = f - fm1, dvp1 = fp1 - f, dvp2 = fp2 - fp1;
+    R dvc = (R)0.5 * (dvm2 + dvm1), SM = (R)2 * ring_minmod(dvm2, dvm1);
+    const R Sm1 = ring_minmod(dvc, SM);
+    dvc = (R)0.5 * (dvm1 + dvp1);
+    SM = (R)2 * ring_minmod(dvm1, dvp1);
+    const R Sp1 = ring_minmod(dvc, SM);
+    dvc = (R)0.5 * (dvp2 + dvp1);
+    SM = (R)2 * ring_minmod(dvp2, dvp1);
+    const R Sp2 = ring_minmod(dvc, SM);
+    vp = (R)0.5 * (f + fp1) - (Sp2 - Sp1) / (R)6;
+    vm = (R)0.5 * (f + fm1) - (Sp1 - Sm1) / (R)6;
+    R ap = vp - f, am = vm - f;
+    if (ap * am >= (R)0) {
+        ap = (R)0;
+        am = (R)0;
+    } else {
+        if (fabs(ap) >= (R)2 * fabs(am)) ap = (R)(-2) * am;
+        if (fabs(am) >= (R)2 * fabs(ap)) am = (R)(-2) * ap;
+    }
+    vp = f + ap;
+    vm = f + am;
+}
+// the parabola of chunk c (1-based) from the chunk values chv(1-2 .. Nc+2)
+// (ReconstructRing, ringrecon.F90:34-91): coefficients a, b, c
+template <class R>
+__device__ __forceinline__ void ring_parabola(int recon, const R* chW, int c, R& a, R& bq, R& cq) {
+    R fL, fR;
+    const R* p = chW + c + 1;  // chv(c) = chW[c + 1]
+    ring_lr(recon, p[-2], p[-1], p[0], p[1], p[2], fL, fR);
+    const R f = p[0];
+    a = (R)3 * (fL + fR - (R)2 * f);
+    bq = (R)2 * ((R)3 * f - fR - (R)2 * fL);
+    cq = fL;
+}
+template <class R> __device__ __forceinline__ R ring_interp(R a, R bq, R cq, int m, int dJ) {
+    return (a / (R)3) * (R)(3 * m * m - 3 * m + 1) / (R)(dJ * dJ) + (R)0.5 * bq * (R)(2 * m - 1) / (R)dJ + cq;
+}
+// periodic ghosts of the chunk values chv(1..Nc)
+template <class R> __device__ __forceinline__ void ring_chunk_ghosts(R* chW, int Nc) {
+    for (int n = 1; n <= 2; n++) {
+        chW[1 - n + 1] = chW[Nc - n + 1 + 1];
+        chW[Nc + n + 1] = chW[n + 1];
+    }
+}
+
+// CalcSmoothE (ringav.F90:212-344) for one ring: the J fluxes through the
+// ring (then the I fluxes) cleaned of Fourier modes 0..nft, chunk-averaged,
+// reconstructed, dirtied again; the change of each face's flux accumulated
+// along its chunk into the I (J) EMFs of the smoothing field
+template <class R>
+__global__ void __launch_bounds__(64) k_ring_smooth_e(GamBox b, RingData Rg, StateBuf<R> S, const GamScalars* sc) {
+    if (sc->halted) return;
+    const int G = GAM_NG, Np = Rg.Np, nsl = b.Nip + 1;
+    const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    const long nper = (long)nsl * Rg.NumR;
+    if (t >= 2 * nper) return;
+    const int pole = (int)(t / nper);
+    if (!(pole == 0 ? Rg.doS : Rg.doE)) return;
+    const int nS = G + (int)(t % nper % nsl), nR = 1 + (int)(t % nper / nsl);
+    const int NumCh = Rg.Nch[nR - 1], dC = Np / NumCh;
+    R* chW = (R*)Rg.chunk + t * Rg.chunkStride;
+    R* E = (R*)Rg.smoothE;
+    const long fs = b.fs;
+    const double* cs = Rg.ftab;
+    for (int dd = 0; dd < 2; dd++) {
+        const int fD = dd == 0 ? 1 : 0, eD = dd == 0 ? 0 : 1;
+        const R eScl = dd == 0 ? (R)1 : (R)(-1);
+        const int jf = pole == 1 ? G + b.Njp - nR : (fD == 1 ? G + nR : G + nR - 1);
+        const int je = pole == 1 ? G + b.Njp - nR : (eD == 0 ? G + nR : G + nR - 1);
+        const R* mf = S.mf + fD * fs;
+        GAM_BOX_CHECK(lidx(b, nS, jf, G), lidx(b, nS, jf, G + Np - 1), 15);
+        // CleanRing: coefficients
+        R cC[3] = {(R)0, (R)0, (R)0}, cS[3] = {(R)0, (R)0, (R)0};
+        for (int n = 1; n <= Np; n++) {
+            const R Q = mf[lidx(b, nS, jf, G + n - 1)];
+            for (int m = 0; m <= Rg.nft; m++) {
+                cC[m] = cC[m] + Q * (R)cs[(2 * m) * Np + n - 1];
+                cS[m] = cS[m] + Q * (R)cs[(2 * m + 1) * Np + n - 1];
+            }
+        }
+        if (Rg.nft >= 0) {
+            const R h = (R)0.5 * (R)Rg.aScl;
+            cC[0] = h * cC[0];
+            cS[0] = h * cS[0];
+        }
+        for (int m = 1; m <= Rg.nft; m++) {
+            const R a1 = (R)1 * (R)Rg.aScl;
+            cC[m] = a1 * cC[m];
+            cS[m] = a1 * cS[m];
+        }
+        auto cleaned = [&](int n) -> R {  // 1-based n
+            R Q = mf[lidx(b, nS, jf, G + n - 1)];
+            for (int m = 0; m <= Rg.nft; m++)
+                Q = Q - cC[m] * (R)cs[(2 * m) * Np + n - 1] - cS[m] * (R)cs[(2 * m + 1) * Np + n - 1];
+            return Q;
+        };
+        // chunk averages
+        for (int c = 1; c <= NumCh; c++) {
+            const int lRs = 1 + (c - 1) * dC;
+            R sum = (R)0;
+            for (int l = lRs; l < lRs + dC; l++) sum = sum + cleaned(l);
+            chW[c + 1] = sum / (R)dC;
+        }
+        ring_chunk_ghosts(chW, NumCh);
+        // reconstruct, dirty, accumulate the flux changes into the EMFs
+        for (int c = 1; c <= NumCh; c++) {
+            R a, bq, cq;
+            ring_parabola(Rg.recon, chW, c, a, bq, cq);
+            const int lRs = 1 + (c - 1) * dC;
+            R cum = (R)0;
+            for (int m = 1; m <= dC; m++) {
+                const int n = lRs + m - 1;
+                R ra = ring_interp(a, bq, cq, m, dC);
+                for (int mm = 0; mm <= Rg.nft; mm++)
+                    ra = ra + cC[mm] * (R)cs[(2 * mm) * Np + n - 1] + cS[mm] * (R)cs[(2 * mm + 1) * Np + n - 1];
+                const R d = ra - mf[lidx(b, nS, jf, G + n - 1)];
+                const long ce = eD * fs + lidx(b, nS, je, G + n - 1);
+                if (m == 1) {
+                    E[ce] = (R)0;
+                    cum = -d;
+                } else {
+                    E[ce] = eScl * cum;
+                    cum = cum - d;
+                }
+            }
+        }
+        // replicate k = ks at ke+1
+        E[eD * fs + lidx(b, nS, je, G + Np)] = E[eD * fs + lidx(b, nS, je, G)];
+    }
+}
+
+// E2Flux with the smoothing field and dt = 1 (fields.F90:18-51) over the
+// faces it changes: rows js..js+NumR and je-NumR..je, i = is..ie+1, k = ks..ke+1
+template <class R> __global__ void __launch_bounds__(256) k_ring_e2flux(GamBox b, RingData Rg, StateBuf<R> S,
+                                                                          const GamScalars* sc) {
+    if (sc->halted) return;
+    const int G = GAM_NG, nr = Rg.NumR + 1;
+    const long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    const int ni = b.Nip + 1, nk = b.Nkp + 1;
+    const long nrow = (long)ni * nk;
+    if (q >= 2L * nr * nrow) return;
+    const int pole = (int)(q / (nr * nrow));
+    if (!(pole == 0 ? Rg.doS : Rg.doE)) return;
+    const long r = q % (nr * nrow);
+    const int row = (int)(r / nrow), ii = G + (int)(r % nrow % ni), kk = G + (int)(r % nrow / ni);
+    const int jj = pole == 0 ? G + row : G + b.Njp - 1 - Rg.NumR + row;
+    const R* E = (const R*)Rg.smoothE;
+    const long fs = b.fs, c = lidx(b, ii, jj, kk), sj = b.sx, sk = b.sk;
+    GAM_BOX_CHECK(c, c + sj + sk + 1, 15);
+    const R* Ei = E;
+    const R* Ej = E + fs;
+    const R* Ek = E + 2 * fs;
+    const R dfi = Ek[c + sj] - Ek[c] - Ej[c + sk] + Ej[c];
+    const R dfj = Ei[c + sk] - Ei[c] - Ek[c + 1] + Ek[c];
+    const R dfk = Ej[c + 1] - Ej[c] - Ei[c + sj] + Ei[c];
+    S.mf[c] = S.mf[c] - (R)1 * dfi;
+    S.mf[fs + c] = S.mf[fs + c] - (R)1 * dfj;
+    S.mf[2 * fs + c] = S.mf[2 * fs + c] - (R)1 * dfk;
+}
+
+// CleanLoops (ringav.F90:347-391): the K fluxes of the pole's first ring
+// lose their mean, slices is..ie+1
+template <class R> __global__ void __launch_bounds__(128) k_ring_clean_loops(GamBox b, RingData Rg, StateBuf<R> S,
+                                                                               const GamScalars* sc) {
+    if (sc->halted) return;
+    const int G = GAM_NG;
+    const long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    const int ni = b.Nip + 1;
+    if (q >= 2L * ni) return;
+    const int pole = (int)(q / ni), ii = G + (int)(q % ni);
+    if (!(pole == 0 ? Rg.doS : Rg.doE)) return;
+    const int jr = pole == 0 ? G : G + b.Njp - 1;
+    R* mK = S.mf + 2 * b.fs;
+    GAM_BOX_CHECK(lidx(b, ii, jr, G), lidx(b, ii, jr, G + b.Nkp), 15);
+    R sum = (R)0;
+    for (int kk = G; kk < G + b.Nkp; kk++) sum = sum + mK[lidx(b, ii, jr, kk)];
+    const R avg = sum / (R)Rg.Np;
+    const R tScl = (R)Rg.tScl;
+    for (int kk = G; kk <= G + b.Nkp; kk++) {
+        const long c = lidx(b, ii, jr, kk);
+        mK[c] = mK[c] - tScl * avg;
+    }
+}
+
+// bFlux2Fld with RingFlux2FieldFix over the cells whose faces the ring
+// average changed: j rows 0..js+NumR(+1) and je-NumR-1..Nj-1, every i and k
+template <class R> __global__ void __launch_bounds__(128) k_ring_bfield(GamBox b, Geo<R> g, RingData Rg,
+                                                                          StateBuf<R> S, const GamScalars* sc) {
+    if (sc->halted) return;
+    const int G = GAM_NG, nr = G + Rg.NumR + 2;
+    const long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    const long nrow = (long)b.Ni * b.Nk;
+    if (q >= 2L * nr * nrow) return;
+    const int pole = (int)(q / (nr * nrow));
+    if (!(pole == 0 ? Rg.doS : Rg.doE)) return;
+    const long r = q % (nr * nrow);
+    const int row = (int)(r / nrow), ii = (int)(r % nrow % b.Ni), kk = (int)(r % nrow / b.Ni);
+    const int jj = pole == 0 ? row : b.Nj - nr + row;
+    const long fs = b.fs, c = lidx(b, ii, jj, kk);
+    int jc = jj, kc = kk;
+    const long cb = ring_conj_cc(b, Rg, jc, kc) ? lidx(b, ii, jc, kc) : c;
+    GAM_BOX_CHECK(cb, cb + b.sk, 15);
+    R B[3];
+    cell_bxyz(b, g, cb, S.mf[cb], S.mf[cb + 1], S.mf[fs + cb], S.mf[fs + cb + b.sx], S.mf[2 * fs + cb],
+              S.mf[2 * fs + cb + b.sk], B);
+#pragma unroll
+    for (int x = 0; x < 3; x++) S.B[x * fs + c] = B[x];
+}
+
+// SmoothGas (ringav.F90:78-210) for one ring: the ring variables (rho,
+// momentum, internal energy; Gas2Ring, ringutils.F90:804-830) chunk-averaged,
+// reconstructed per chunk and written back as gas (Ring2Gas :832-856)
+template <class R>
+__global__ void __launch_bounds__(64) k_ring_smooth_gas(GamBox b, DevParams<R> P, StateBuf<R> S, const GamScalars* sc) {
+    if (sc->halted) return;
+    const RingData& Rg = P.ring;
+    const int G = GAM_NG, Np = Rg.Np, nsl = b.Nip;
+    const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    const long nper = (long)nsl * Rg.NumR;
+    if (t >= 2 * nper) return;
+    const int pole = (int)(t / nper);
+    if (!(pole == 0 ? Rg.doS : Rg.doE)) return;
+    const int nS = G + (int)(t % nper % nsl), nR = 1 + (int)(t % nper / nsl);
+    const int NumCh = Rg.Nch[nR - 1], dC = Np / NumCh;
+    const int jr = pole == 0 ? G + nR - 1 : G + b.Njp - nR;
+    const int cst = NumCh + 4;
+    R* chW = (R*)Rg.chunk + t * Rg.chunkStride;
+    const long fs = b.fs;
+    GAM_BOX_CHECK(lidx(b, nS, jr, G), lidx(b, nS, jr, G + Np - 1), 15);
+    auto ring_var = [&](int n, R* W) {  // Gas2Ring of ring cell n (1-based)
+        const long c = lidx(b, nS, jr, G + n - 1);
+#pragma unroll
+        for (int v = 0; v < 5; v++) W[v] = S.Gas[v * fs + c];
+        const R D = rmax(W[0], P.dFloor);
+        const R KinE = (R)0.5 * (W[1] * W[1] + W[2] * W[2] + W[3] * W[3]) / D;
+        const R Pr = rmax(P.gm1 * (W[4] - KinE), P.pFloor);
+        W[0] = D;
+        W[4] = Pr / P.gm1;
+    };
+    // chunk averages of the five ring variables
+    for (int c = 1; c <= NumCh; c++) {
+        const int lRs = 1 + (c - 1) * dC;
+        R sum[5] = {(R)0, (R)0, (R)0, (R)0, (R)0};
+        for (int l = lRs; l < lRs + dC; l++) {
+            R W[5];
+            ring_var(l, W);
+#pragma unroll
+            for (int v = 0; v < 5; v++) sum[v] = sum[v] + W[v];
+        }
+#pragma unroll
+        for (int v = 0; v < 5; v++) chW[v * cst + c + 1] = sum[v] / (R)dC;
+    }
+    for (int v = 0; v < 5; v++) ring_chunk_ghosts(chW + v * cst, NumCh);
+    // reconstruct and write back
+    for (int c = 1; c <= NumCh; c++) {
+        R a[5], bq[5], cq[5];
+#pragma unroll
+        for (int v = 0; v < 5; v++) ring_parabola(Rg.recon, chW + v * cst, c, a[v], bq[v], cq[v]);
+        const int lRs = 1 + (c - 1) * dC;
+        for (int m = 1; m <= dC; m++) {
+            R W[5];
+#pragma unroll
+            for (int v = 0; v < 5; v++) W[v] = ring_interp(a[v], bq[v], cq[v], m, dC);
+            const R D = rmax(W[0], P.dFloor);
+            R Pr = P.gm1 * W[4];
+            Pr = rmax(Pr, P.pFloor);
+            const R KinE = (R)0.5 * (W[1] * W[1] + W[2] * W[2] + W[3] * W[3]) / D;
+            const long c2 = lidx(b, nS, jr, G + lRs + m - 2);
+            S.Gas[c2] = D;
+            S.Gas[fs + c2] = W[1];
+            S.Gas[2 * fs + c2] = W[2];
+            S.Gas[3 * fs + c2] = W[3];
+            S.Gas[4 * fs + c2] = KinE + Pr / P.gm1;
+        }
+    }
+}
+
+// Con2Fast (gamutils.F90:255-269 with CellPress2Cs :238-253, Boris :356-358)
+template <class R> __device__ __forceinline__ R con2fast(const DevParams<R>& P, const R* gCon, const R* Bin) {
+    R rho = rmax(gCon[0], P.dFloor);
+    R Vx = gCon[1] / rho, Vy = gCon[2] / rho, Vz = gCon[3] / rho;
+    R KinE = (R)0.5 * rho * (Vx * Vx + Vy * Vy + Vz * Vz);
+    R Pr = rmax(P.gm1 * (gCon[4] - KinE), P.pFloor);
+    R Cs = Mth<R>::sqrt_(P.gamma * Pr / rho);
+    double Bd[3] = {(double)Bin[0], (double)Bin[1], (double)Bin[2]};
+    R MagB = (R)norm2s3(Bd);
+    R Va = MagB / Mth<R>::sqrt_(gCon[0]);
+    if (P.doBoris) Va = boris_speed((R)P.Ca, Va);
+    return Mth<R>::sqrt_(Cs * Cs + Va * Va);
+}
+// NudgeSW's ring branch (apps/wind.F90:458-484): the last active cell and the
+// one across the E pole flow out at the fast speed when they flow in
+template <class R>
+__global__ void __launch_bounds__(128) k_ring_nudge_axis(GamBox b, DevParams<R> P, StateBuf<R> S, const GamScalars* sc) {
+    if (sc->halted) return;
+    const int G = GAM_NG;
+    const long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (q >= 2L * b.Nkp) return;
+    const int kk = G + (int)(q % b.Nkp), jj = G + b.Njp - 1 + (int)(q / b.Nkp), ii = G + b.Nip - 1;
+    const long fs = b.fs, c = lidx(b, ii, jj, kk);
+    GAM_BOX_CHECK(c, c, 15);
+    if (!(S.Gas[fs + c] > (R)0)) return;
+    R U[5], W[5], B[3];
+#pragma unroll
+    for (int v = 0; v < 5; v++) U[v] = S.Gas[v * fs + c];
+#pragma unroll
+    for (int x = 0; x < 3; x++) B[x] = S.B[x * fs + c];
+    const R Cx = con2fast(P, U, B);
+    cell_c2p(P, U, W);
+    W[1] = -Cx;
+    cell_p2c(P, W, U);
+#pragma unroll
+    for (int v = 0; v < 5; v++) S.Gas[v * fs + c] = U[v];
 }
 
 // UpdateStateData time bookkeeping + CalcDT decisions (gamapp.F90:110-111,
@@ -1332,7 +1842,7 @@ __global__ void k_dt_finalize(GamScalars* sc) {
 // Boundary kinds: 0 periodic, 1 none, 2 zero-gradient, 3 inner sphere,
 // 4 solar wind, 6 uniform inflow (include/gamgpu.h).
 enum { BCK_PERIODIC = 0, BCK_NONE = 1, BCK_ZEROGRAD = 2, BCK_SPHIN = 3, BCK_WIND = 4, BCK_HALO = 5, BCK_INFLOW = 6,
-       BCK_ION = 7 };
+       BCK_ION = 7, BCK_LFM = 8 };
 
 // Gather maps of the boundary conditions that copy values (bcs.F90:279-450
 // periodic, :799-892 zero-gradient, :934-957 SphIn). x is the box index along
@@ -1372,17 +1882,23 @@ __device__ __forceinline__ int bmap_25d(int x) {
 // map applies only over its loop ranges: periodic over the whole box,
 // zero-gradient and SphIn over cell ranges of the other two indices. The
 // non-periodic I sides (SphIn, wind) were applied before, in place. withB:
-// follow only the BCs that also copy Bxyz (periodic; zero-gradient does not).
+// follow only the BCs that also copy Bxyz (periodic and the LFM pole;
+// zero-gradient does not). The LFM pole (lfmIn / lfmOut, over the whole
+// box) maps a ghost row to its conjugate across the axis and reverses J and
+// K fluxes: the return value is the sign of the source.
 template <class R>
-__device__ __forceinline__ void bc_source(const GamBox& b, const DevParams<R>& P, int comp, bool withB, int& ii,
-                                          int& jj, int& kk) {
+__device__ __forceinline__ int bc_source(const GamBox& b, const DevParams<R>& P, int comp, bool withB, int& ii,
+                                         int& jj, int& kk) {
+    int sgn = 1;
     if (P.do25D)
         kk = bmap_25d(kk);
     else if (P.bc[4] == BCK_PERIODIC) {
         kk = bmap_lo(BCK_PERIODIC, kk, b.Nkp);
         kk = bmap_hi(BCK_PERIODIC, kk, b.Nkp, comp == 2);
     }
-    if (P.bc[2] == BCK_PERIODIC || (!withB && ii < b.Ni && kk < b.Nk)) {
+    if (P.ring.on) {
+        sgn = ring_bc_jmap(b, P.ring, comp, jj, kk);
+    } else if (P.bc[2] == BCK_PERIODIC || (!withB && ii < b.Ni && kk < b.Nk)) {
         jj = bmap_lo(P.bc[2], jj, b.Njp);
         jj = bmap_hi(P.bc[3], jj, b.Njp, comp == 1);
     }
@@ -1390,6 +1906,7 @@ __device__ __forceinline__ void bc_source(const GamBox& b, const DevParams<R>& P
         ii = bmap_lo(BCK_PERIODIC, ii, b.Nip);
         ii = bmap_hi(BCK_PERIODIC, ii, b.Nip, comp == 0);
     }
+    return sgn;
 }
 
 
@@ -1502,10 +2019,14 @@ __global__ void __launch_bounds__(256) k_bc_iside(GamBox b, DevParams<R> P, Geo<
         // (isGoodFaceIJK ranges, gridutils.F90:985-1015)
         const long cg = lidx(b, G - n, jj, kk);
         if (cellJK) {
-            int kp = kk;
+            int kp = kk, jp = jj;
             if (kk < G) kp = kk + b.Nkp;
             else if (kk >= G + b.Nkp) kp = kk - b.Nkp;
-            const long src = lidx(b, G + n - 1, jj, kp);
+            if (P.ring.on) {  // across the LFM pole: the conjugate's mirror cell
+                int kr = kk;
+                if (ring_conj_cc(b, P.ring, jp, kr)) kp = kr;
+            }
+            const long src = lidx(b, G + n - 1, jp, kp);
             GAM_BOX_CHECK(src, src, 14);
             R pU[5], pW[5], gC[5];
 #pragma unroll
@@ -1738,9 +2259,12 @@ __global__ void __launch_bounds__(256) k_bc(GamBox b, DevParams<R> P, Geo<R> g, 
 #pragma unroll
     for (int d = 0; d < 3; d++) {
         int x = ii, y = jj, z = kk;
-        bc_source(b, P, d, false, x, y, z);
+        const int sg = bc_source(b, P, d, false, x, y, z);
         GAM_BOX_CHECK(lidx(b, x, y, z), lidx(b, x, y, z), 14);
-        if (x != ii || y != jj || z != kk) s.mf[d * fs + c] = s.mf[d * fs + lidx(b, x, y, z)];
+        if (x != ii || y != jj || z != kk) {
+            const R v = s.mf[d * fs + lidx(b, x, y, z)];
+            s.mf[d * fs + c] = sg < 0 ? -v : v;
+        }
     }
     if (ii >= b.Ni || jj >= b.Nj || kk >= b.Nk) return;
     // cell
@@ -1771,9 +2295,12 @@ __global__ void __launch_bounds__(256) k_bc(GamBox b, DevParams<R> P, Geo<R> g, 
         bc_source(b, P, d, false, x, y, z);
         return lidx(b, x, y, z);
     };
-    const long fI = srcf(0, ii, jj, kk), fIp = srcf(0, ii + 1, jj, kk);
-    const long fJ = srcf(1, ii, jj, kk), fJp = srcf(1, ii, jj + 1, kk);
-    const long fK = srcf(2, ii, jj, kk), fKp = srcf(2, ii, jj, kk + 1);
+    // RingFlux2FieldFix: a cell across the LFM pole takes its conjugate's field
+    int jb = jj, kb = kk;
+    const bool conj = P.ring.on && ring_conj_cc(b, P.ring, jb, kb);
+    const long fI = srcf(0, ii, jb, kb), fIp = srcf(0, ii + 1, jb, kb);
+    const long fJ = srcf(1, ii, jb, kb), fJp = srcf(1, ii, jb + 1, kb);
+    const long fK = srcf(2, ii, jb, kb), fKp = srcf(2, ii, jb, kb + 1);
     {
         long lo = fI, hi = fI;
         for (long v : {fIp, fJ, fJp, fK, fKp}) {
@@ -1787,7 +2314,8 @@ __global__ void __launch_bounds__(256) k_bc(GamBox b, DevParams<R> P, Geo<R> g, 
     const bool ghost = ii < G || ii >= G + b.Nip || jj < G || jj >= G + b.Njp || kk < G || kk >= G + b.Nkp;
     if (!(ghost || facesMapped)) return;
     R B[3];
-    cell_bxyz(b, g, c, s.mf[fI], s.mf[fIp], s.mf[fs + fJ], s.mf[fs + fJp], s.mf[2 * fs + fK], s.mf[2 * fs + fKp], B);
+    cell_bxyz(b, g, conj ? lidx(b, ii, jb, kb) : c, s.mf[fI], s.mf[fIp], s.mf[fs + fJ], s.mf[fs + fJp],
+              s.mf[2 * fs + fK], s.mf[2 * fs + fKp], B);
 #pragma unroll
     for (int x = 0; x < 3; x++) s.B[x * fs + c] = B[x];
 }
@@ -1820,7 +2348,7 @@ template <class R> void launch_bcs(const Ctx<R>& C, const StateBuf<R>& S, cudaSt
 // the dt range into sc->dtmin_bits.
 template <class R>
 __global__ void __launch_bounds__(128) k_dt_only(GamBox b, DevParams<R> P, Geo<R> g, StateBuf<R> s,
-                                                 GamScalars* sc, double gamma_d, double gm1_d) {
+                                                 GamScalars* sc, double gamma_d, double gm1_d, int countBad) {
     int ii, jj, kk;
     const int G = GAM_NG;
     Range r{G - P.dtIlo, G + b.Nip - 1 + P.dtIhi, G - P.dtJlo, G + b.Njp - 1 + P.dtJhi, G - P.dtKlo,
@@ -1842,7 +2370,9 @@ __global__ void __launch_bounds__(128) k_dt_only(GamBox b, DevParams<R> P, Geo<R
         double dtc = P.doBoris ? cell_dt<R, true>(P, Ud, Bt, (double)g.dl[c], gamma_d, gm1_d, sc->CFL)
                                 : cell_dt<R, false>(P, Ud, Bt, (double)g.dl[c], gamma_d, gm1_d, sc->CFL);
         if (dtc > 0.0 && dtc < 1.0e300) mydt = dtc;
+        else if (countBad && !sc->fixedTimestep) atomicAdd(&sc->nbad, 1);
     }
+    if (sc->fixedTimestep && countBad) return;
     for (int o = 16; o > 0; o >>= 1) mydt = fmin(mydt, __shfl_xor_sync(0xffffffffu, mydt, o));
     if ((threadIdx.x & 31) == 0 && mydt < HUGE_DT) atomicMin(&sc->dtmin_bits, dbits(mydt));
 }
@@ -1850,15 +2380,19 @@ __global__ void __launch_bounds__(128) k_dt_only(GamBox b, DevParams<R> P, Geo<R
 
 // bFlux2Fld over every cell of a state (gridutils.F90:281-301)
 template <class R>
-__global__ void __launch_bounds__(128) k_bfield_all(GamBox b, Geo<R> g, StateBuf<R> s, const GamScalars* sc) {
+__global__ void __launch_bounds__(128) k_bfield_all(GamBox b, Geo<R> g, StateBuf<R> s, const GamScalars* sc,
+                                                    RingData ring) {
     int ii, jj, kk;
     Range r{0, b.Ni - 1, 0, b.Nj - 1, 0, b.Nk - 1};
     if (!thread_ijk(r, ii, jj, kk)) return;
     const long fs = b.fs;
     const long c = lidx(b, ii, jj, kk);
-    GAM_BOX_CHECK(c, c + b.sk, 16);
+    int jc = jj, kc = kk;
+    const long cb = (ring.on && ring_conj_cc(b, ring, jc, kc)) ? lidx(b, ii, jc, kc) : c;
+    GAM_BOX_CHECK(cb, cb + b.sk, 16);
     R B[3];
-    cell_bxyz(b, g, c, s.mf[c], s.mf[c + 1], s.mf[fs + c], s.mf[fs + c + b.sx], s.mf[2 * fs + c], s.mf[2 * fs + c + b.sk], B);
+    cell_bxyz(b, g, cb, s.mf[cb], s.mf[cb + 1], s.mf[fs + cb], s.mf[fs + cb + b.sx], s.mf[2 * fs + cb],
+              s.mf[2 * fs + cb + b.sk], B);
 #pragma unroll
     for (int x = 0; x < 3; x++) s.B[x * fs + c] = B[x];
 }
@@ -1867,6 +2401,38 @@ __global__ void __launch_bounds__(128) k_bfield_all(GamBox b, Geo<R> g, StateBuf
 static inline dim3 grid_for(const Range& r, dim3 blk) {
     return dim3((unsigned)((r.i1 - r.i0 + 1 + blk.x - 1) / blk.x), (unsigned)((r.j1 - r.j0 + 1 + blk.y - 1) / blk.y),
                 (unsigned)((r.k1 - r.k0 + 1 + blk.z - 1) / blk.z));
+}
+
+// RingAverage (ringav.F90:26-75) on the updated state: smoothing EMFs of both
+// poles, PoleE and FixEFieldLFM on them, E2Flux with dt = 1, CleanLoops,
+// bFlux2Fld of the cells around the rings, SmoothGas of both poles
+template <class R> void launch_ring_average(const Ctx<R>& C, const StateBuf<R>& O, cudaStream_t s) {
+    const GamBox& b = C.b;
+    const RingData& Rg = C.P.ring;
+    const int G = GAM_NG;
+    if (C.P.doMHD) {
+        const long nz = 2L * (Rg.NumR + 2) * b.Ni * b.Nk;
+        k_ring_zero_e<R><<<(unsigned)((nz + 255) / 256), 256, 0, s>>>(b, Rg, C.sc);
+        const long ne = 2L * (b.Nip + 1) * Rg.NumR;
+        k_ring_smooth_e<R><<<(unsigned)((ne + 63) / 64), 64, 0, s>>>(b, Rg, O, C.sc);
+        R* E = (R*)Rg.smoothE;
+        const int ni = b.Nip + 1;
+        k_ring_pole_e<R><<<(unsigned)((2 * ni + 127) / 128), 128, 0, s>>>(b, Rg, E, G, G + b.Nip, C.sc);
+        // FixEFieldLFM over the rows that can be nonzero (the others hold zeros)
+        const int sj1 = std::min(G + Rg.NumR + 1, G + b.Njp), ej0 = std::max(G + b.Njp - 1 - Rg.NumR, G);
+        if (Rg.doS)
+            k_fix_e_lfm<R><<<(unsigned)(((long)ni * (sj1 - G + 1) + 255) / 256), 256, 0, s>>>(b, E, G, sj1, C.sc);
+        if (Rg.doE)
+            k_fix_e_lfm<R><<<(unsigned)(((long)ni * (G + b.Njp - ej0 + 1) + 255) / 256), 256, 0, s>>>(
+                b, E, ej0, G + b.Njp, C.sc);
+        const long nf = 2L * (Rg.NumR + 1) * (b.Nip + 1) * (b.Nkp + 1);
+        k_ring_e2flux<R><<<(unsigned)((nf + 255) / 256), 256, 0, s>>>(b, Rg, O, C.sc);
+        if (Rg.clean) k_ring_clean_loops<R><<<(unsigned)((2 * ni + 127) / 128), 128, 0, s>>>(b, Rg, O, C.sc);
+        const long nb = 2L * (G + Rg.NumR + 2) * b.Ni * b.Nk;
+        k_ring_bfield<R><<<(unsigned)((nb + 127) / 128), 128, 0, s>>>(b, C.g, Rg, O, C.sc);
+    }
+    const long ng = 2L * b.Nip * Rg.NumR;
+    k_ring_smooth_gas<R><<<(unsigned)((ng + 63) / 64), 64, 0, s>>>(b, C.P, O, C.sc);
 }
 
 // The kernels of one stepGamera in order, each handed to f(id, launch) with
@@ -1957,19 +2523,33 @@ template <class R, class F> void for_each_kernel(const Ctx<R>& C, int cur, cudaS
             if (C.P.ion.wind) {
                 const long nw = 4L * (b.Njp + 1) * (b.Nkp + 1);
                 k_wind_efix<R><<<(unsigned)((nw + 255) / 256), 256, 0, s>>>(b, C.P, C.g, S, C.w, C.sc);
+                if (C.P.ring.on)  // WindEFix's touch-up of the pole rows of its shells
+                    k_ring_pole_e<R><<<1, 128, 0, s>>>(b, C.P.ring, C.w.E, GAM_NG + b.Nip - 3, GAM_NG + b.Nip, C.sc);
             }
             if (C.P.bc[4] != BCK_HALO)
-                k_fix_e_lfm<R><<<(unsigned)((nf + 255) / 256), 256, 0, s>>>(b, C.w, C.sc);
+                k_fix_e_lfm<R><<<(unsigned)((nf + 255) / 256), 256, 0, s>>>(b, C.w.E, GAM_NG, GAM_NG + b.Njp, C.sc);
+        }
+        if (C.P.ring.on && C.P.doMHD) {  // PoleE before E2Flux (mhdgroup.F90:140-142)
+            const int ni = b.Nip + 1;
+            k_ring_pole_e<R><<<(unsigned)((2 * ni + 127) / 128), 128, 0, s>>>(b, C.P.ring, C.w.E, GAM_NG, GAM_NG + b.Nip,
+                                                                            C.sc);
+            const long nf = (long)ni * (b.Njp + 1);
+            k_fix_e_lfm<R><<<(unsigned)((nf + 255) / 256), 256, 0, s>>>(b, C.w.E, GAM_NG, GAM_NG + b.Njp, C.sc);
         }
         k_update_faces<R><<<grid_for(all, blk), blk, 0, s>>>(b, C.P, S, O, C.w, C.sc, C.oomf);
     });
     f(12, [&] {
+        if (C.P.ring.on) {  // RingFlux (stress.F90:137-139), before the fluxes become deltas
+            const long n = 2L * b.Ni * b.Nk + (long)b.Nip * b.Njp;
+            k_ring_flux<R><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(b, C.P, C.w, C.sc);
+        }
         if (C.P.doBoris)
             k_update_cells<R, sizeof(R) == 8 ? 6 : 8, true><<<grid_for(cells, blk), blk, 0, s>>>(b, C.P, C.g, S, O, C.w, C.sc, C.gamma, C.gm1);
         else if (C.kvar & 4)
             k_update_cells<R, 1><<<grid_for(cells, blk), blk, 0, s>>>(b, C.P, C.g, S, O, C.w, C.sc, C.gamma, C.gm1);
         else
             k_update_cells<R, 8><<<grid_for(cells, blk), blk, 0, s>>>(b, C.P, C.g, S, O, C.w, C.sc, C.gamma, C.gm1);
+        if (C.P.ring.on) launch_ring_average(C, O, s);  // mhdgroup.F90:69-74
         if (C.P.ion.push) {  // HackStep (PerStep, earthcmi.F90:224-263): PushIon, before CalcDT
             const long np = (long)C.P.ion.nIonP * b.Njp * b.Nkp;
             if (C.P.doBoris)
@@ -1983,6 +2563,14 @@ template <class R, class F> void for_each_kernel(const Ctx<R>& C, int cur, cudaS
                 k_nudge_sw<R, true><<<(unsigned)((nn + 127) / 128), 128, 0, s>>>(b, C.P, C.g, O, C.sc, C.gamma, C.gm1);
             else
                 k_nudge_sw<R, false><<<(unsigned)((nn + 127) / 128), 128, 0, s>>>(b, C.P, C.g, O, C.sc, C.gamma, C.gm1);
+            if (C.P.ring.on && C.P.ring.doE)
+                k_ring_nudge_axis<R><<<(unsigned)((2 * b.Nkp + 127) / 128), 128, 0, s>>>(b, C.P, O, C.sc);
+        }
+        if (C.P.ring.on) {  // CalcDT after the ring average and the hooks (gamapp.F90:78-80)
+            const dim3 blk2(32, 4, 1);
+            const Range r{GAM_NG - C.P.dtIlo, GAM_NG + b.Nip - 1 + C.P.dtIhi, GAM_NG - C.P.dtJlo,
+                          GAM_NG + b.Njp - 1 + C.P.dtJhi, GAM_NG - C.P.dtKlo, GAM_NG + b.Nkp - 1 + C.P.dtKhi};
+            k_dt_only<R><<<grid_for(r, blk2), blk2, 0, s>>>(b, C.P, C.g, O, C.sc, C.gamma, C.gm1, 1);
         }
     });
     f(13, [&] { k_dt_finalize<<<1, 1, 0, s>>>(C.sc); });
@@ -2084,7 +2672,7 @@ template <class R> void launch_dt_only(const Ctx<R>& C, int cur, cudaStream_t s)
     const dim3 blk(32, 4, 1);
     const Range r{G - C.P.dtIlo, G + b.Nip - 1 + C.P.dtIhi, G - C.P.dtJlo, G + b.Njp - 1 + C.P.dtJhi,
                   G - C.P.dtKlo, G + b.Nkp - 1 + C.P.dtKhi};
-    k_dt_only<R><<<grid_for(r, blk), blk, 0, s>>>(b, C.P, C.g, C.st[cur], C.sc, C.gamma, C.gm1);
+    k_dt_only<R><<<grid_for(r, blk), blk, 0, s>>>(b, C.P, C.g, C.st[cur], C.sc, C.gamma, C.gm1, 0);
 }
 
 // CalcGridInfo after the initial condition (init.F90:217-238): Bxyz from the
@@ -2094,7 +2682,7 @@ template <class R> void launch_bfield(const Ctx<R>& C, int cur, cudaStream_t s) 
     const GamBox& b = C.b;
     const dim3 blk(32, 4, 1);
     const Range cells{0, b.Ni - 1, 0, b.Nj - 1, 0, b.Nk - 1};
-    k_bfield_all<R><<<grid_for(cells, blk), blk, 0, s>>>(b, C.g, C.st[cur], C.sc);
+    k_bfield_all<R><<<grid_for(cells, blk), blk, 0, s>>>(b, C.g, C.st[cur], C.sc, C.P.ring);
 }
 
 template <class R> void launch_init(const Ctx<R>& C, int cur, cudaStream_t s) {
@@ -2103,7 +2691,7 @@ template <class R> void launch_init(const Ctx<R>& C, int cur, cudaStream_t s) {
     const Range all{0, b.Ni, 0, b.Nj, 0, b.Nk};
     const Range cells{0, b.Ni - 1, 0, b.Nj - 1, 0, b.Nk - 1};
     const StateBuf<R> S = C.st[cur], O = C.st[1 - cur];
-    if (C.P.doMHD) k_bfield_all<R><<<grid_for(cells, blk), blk, 0, s>>>(b, C.g, S, C.sc);
+    if (C.P.doMHD) k_bfield_all<R><<<grid_for(cells, blk), blk, 0, s>>>(b, C.g, S, C.sc, C.P.ring);
     launch_bcs(C, S, s, 1);
     cudaMemcpyAsync(O.Gas, S.Gas, 5 * b.fs * sizeof(R), cudaMemcpyDeviceToDevice, s);
     cudaMemcpyAsync(O.mf, S.mf, 3 * b.fs * sizeof(R), cudaMemcpyDeviceToDevice, s);
@@ -2179,7 +2767,7 @@ __global__ void __launch_bounds__(256) k_halo(GamBox b, StateBuf<R> S, R* __rest
 // Bxyz of the unpacked ghost cells from their faces (the final bFlux2Fld)
 template <class R>
 __global__ void __launch_bounds__(256) k_halo_bxyz(GamBox b, Geo<R> g, StateBuf<R> S, int d, int side,
-                                                   const GamScalars* sc) {
+                                                   const GamScalars* sc, RingData ring) {
     if (sc->halted) return;
     const long nu = d == 0 ? b.Nj : b.Ni, nv = d == 2 ? b.Nj : b.Nk;  // cell extents
     const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
@@ -2188,10 +2776,14 @@ __global__ void __launch_bounds__(256) k_halo_bxyz(GamBox b, Geo<R> g, StateBuf<
     const int Nd = d == 0 ? b.Nip : (d == 1 ? b.Njp : b.Nkp);
     const int pos = side == 0 ? l : GAM_NG + Nd + l;
     const long fs = b.fs, c = halo_cell(b, d, pos, u, v);
-    GAM_BOX_CHECK(c, c + b.sk, 15);
+    // a ghost across the LFM pole takes its conjugate's field
+    const int ic = d == 0 ? pos : u;
+    int jc = d == 1 ? pos : (d == 0 ? u : v), kc = d == 2 ? pos : v;
+    const long cb = (ring.on && ring_conj_cc(b, ring, jc, kc)) ? lidx(b, ic, jc, kc) : c;
+    GAM_BOX_CHECK(cb, cb + b.sk, 15);
     R B[3];
-    cell_bxyz(b, g, c, S.mf[c], S.mf[c + 1], S.mf[fs + c], S.mf[fs + c + b.sx], S.mf[2 * fs + c],
-              S.mf[2 * fs + c + b.sk], B);
+    cell_bxyz(b, g, cb, S.mf[cb], S.mf[cb + 1], S.mf[fs + cb], S.mf[fs + cb + b.sx], S.mf[2 * fs + cb],
+              S.mf[2 * fs + cb + b.sk], B);
 #pragma unroll
     for (int x = 0; x < 3; x++) S.B[x * fs + c] = B[x];
 }
@@ -2206,7 +2798,7 @@ template <class R> void launch_halo(const Ctx<R>& C, int cur, cudaStream_t s, in
     k_halo<R><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(b, S, (R*)buf, d, side, unpack, copyB, C.sc);
     if (unpack && !copyB && C.P.doMHD) {
         const long m = 4L * (d == 0 ? b.Nj : b.Ni) * (d == 2 ? b.Nj : b.Nk);
-        k_halo_bxyz<R><<<(unsigned)((m + 255) / 256), 256, 0, s>>>(b, C.g, S, d, side, C.sc);
+        k_halo_bxyz<R><<<(unsigned)((m + 255) / 256), 256, 0, s>>>(b, C.g, S, d, side, C.sc, C.P.ring);
     }
 }
 

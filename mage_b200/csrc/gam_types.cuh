@@ -40,6 +40,24 @@ struct IonData {
     const double* Wn;  // NudgeSW's weight of the last active cell, per (jj - G) + Njp (kk - G)
 };
 
+// Ring averaging about the LFM axis (ringav.F90, gid "lfm"): rings are the k
+// circles of the first NumR j rows next to each pole (GAM_BC_LFM sides),
+// sliced by i (gam_set_rings)
+struct RingData {
+    int on, doS, doE;     // doS / doE: the pole at js / je+1 belongs to this grid
+    int NumR, Np;         // rings per pole, cells per ring (Nkp)
+    int recon;            // ring reconstruction: 0 PPM, 1 PLM, 2 PCM
+    int nft;              // Fourier modes 0..nft removed from the fluxes (-1: none)
+    int clean;            // CleanLoops
+    double tScl;          // CleanLoops' scale (1 with doFastClean)
+    double aScl;          // CleanRing's 2/Np (in default real)
+    int Nch[32];          // chunks of ring 1..NumR
+    int chunkStride;      // scratch values per ring thread
+    const double* ftab;   // cos / sin (m phi_n): [(2 m + c) Np + n - 1], m = 0..2
+    void* smoothE;        // smoothing EMFs, 3 components of the box (compute precision)
+    void* chunk;          // per ring thread: chunk values
+};
+
 template <class R> struct DevParams {
     R gamma, gm1, CFL, pdmb, Vd0, cHogH, cHogM, dFloor, pFloor;
     int doMHD, doLFMLim, do25D, doBackground, up7;
@@ -55,6 +73,7 @@ template <class R> struct DevParams {
     WindData wind;
     double inflow[8];  // uniform inner-I inflow (bc[0] = 6): rho, P, Vx, Vy, Vz, Bx, By, Bz
     IonData ion;       // ionospheric inner boundary and its hooks (bc[0] = 7)
+    RingData ring;     // ring averaging about the LFM axis (bc[2] / bc[3] = 8)
 };
 
 template <class R> struct Geo {  // Grid_T arrays on the device (gamtypes.F90:168-250)

@@ -13,7 +13,7 @@ module gamgpu
                                  GAM_EBOUNDS = 8
     integer(c_int), parameter :: GAM_BC_PERIODIC = 0, GAM_BC_NONE = 1, GAM_BC_ZEROGRAD = 2, GAM_BC_SPHIN = 3, &
                                  GAM_BC_WIND = 4, GAM_BC_HALO = 5, GAM_BC_INFLOW = 6, &
-                                 GAM_BC_ION = 7
+                                 GAM_BC_ION = 7, GAM_BC_LFM = 8
     integer(c_int), parameter :: GAM_RECON_8CENT = 0, GAM_RECON_7UP = 1
     integer(c_int), parameter :: GAM_FP64 = 0, GAM_FP32 = 1
 
@@ -366,6 +366,19 @@ module gamgpu
             type(c_ptr), intent(in) :: geo(9), st(4), dnxt(3), dst(4)
             type(c_ptr), value :: bg, work, stream
             real(c_double), value :: dt, odt
+        end function
+        ! ring averaging about the LFM axis, before the geometry
+        integer(c_int) function gam_set_rings(h, NumR, Nch, recon, NFTmag, doClean, doFastClean) &
+                bind(C, name="gam_set_rings")
+            import :: c_int, c_ptr, c_int32_t
+            type(c_ptr), value :: h
+            integer(c_int32_t), value :: NumR, recon, NFTmag, doClean, doFastClean
+            integer(c_int32_t), intent(in) :: Nch(*)
+        end function
+        integer(c_int) function gam_ring_defaults(Np, aggressive, NumR, Nch) bind(C, name="gam_ring_defaults")
+            import :: c_int, c_int32_t
+            integer(c_int32_t), value :: Np, aggressive
+            integer(c_int32_t), intent(out) :: NumR, Nch(32)
         end function
         ! a tile away from the inner boundary leaves out both fields (NULL)
         integer(c_int) function gam_set_ionosphere(h, inExyz, inEijk, M0, dtCpl, doIonPush, nIonP, dtSW0) &

@@ -24,7 +24,8 @@ LIB_PATH = os.path.join(HERE, "libgamgpu.so")
 CHECK_LIB_PATH = os.path.join(HERE, "libgamgpu_check.so")
 
 GAM_OK, GAM_EINVAL, GAM_EBADDIM, GAM_ECUDA, GAM_EDT_BAD, GAM_EDT_DISASTER, GAM_ESTATE, GAM_EHOOK, GAM_EBOUNDS = range(9)
-BC_PERIODIC, BC_NONE, BC_ZEROGRAD, BC_SPHIN, BC_WIND, BC_HALO, BC_INFLOW, BC_ION = 0, 1, 2, 3, 4, 5, 6, 7
+BC_PERIODIC, BC_NONE, BC_ZEROGRAD, BC_SPHIN, BC_WIND, BC_HALO, BC_INFLOW, BC_ION, BC_LFM = 0, 1, 2, 3, 4, 5, 6, 7, 8
+RING_PPM, RING_PLM, RING_PCM = 0, 1, 2
 RECON_8CENT, RECON_7UP = 0, 1
 FP64, FP32 = 0, 1
 
@@ -71,7 +72,7 @@ EXPORTED = (
     "gam_efield_forward", "gam_efield_adjoint", "gam_predict_stage", "gam_update_stage", "gam_step_work_bytes",
     "gam_step_fwd_save", "gam_step_adj", "gam_iside_fill", "gam_iside_adjoint", "gam_step_fwd_save_iside",
     "gam_step_adj_iside", "gam_tile_halo_bytes", "gam_tile_halo_pack", "gam_tile_halo_unpack",
-    "gam_set_tile_edges",
+    "gam_set_tile_edges", "gam_set_rings", "gam_ring_defaults",
 )
 
 # Background-field arrays (Grid_T, gamtypes.F90:233-242): name, components;
@@ -115,6 +116,9 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     L.gam_set_wind.argtypes = [C.c_void_p, _dp]
     L.gam_set_inflow.argtypes = [C.c_void_p, _dp]
     L.gam_set_ionosphere.argtypes = [C.c_void_p, _dp, _dp, C.c_double, C.c_double, C.c_int32, C.c_int32, C.c_double]
+    L.gam_set_rings.argtypes = [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.c_int32, C.c_int32, C.c_int32,
+                                C.c_int32]
+    L.gam_ring_defaults.argtypes = [C.c_int32, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
     L.gam_init_test_problem.argtypes = [C.c_void_p, C.c_int32, C.c_double, C.c_double]
     L.gam_set_wind_series.argtypes = [C.c_void_p, C.c_int32] + [_dp] * 6 + [C.c_double] * 3
     L.gam_set_oostate.argtypes = [C.c_void_p, _dp, C.c_double]
@@ -227,11 +231,23 @@ GEOMETRY_ARRAYS = (("face", "face", 3), ("xfc", "face", 9), ("Tf", "face", 27), 
                    ("edge", "face", 3), ("Te", "face", 27), ("Teb", "face", 12))
 
 
+def ring_defaults(Np: int, aggressive: bool = False, lib_path: str = LIB_PATH) -> list:
+    """The reference's default chunks per ring for Np cells around the LFM axis."""
+    L = load_library(lib_path)
+    n = C.c_int32()
+    a = (C.c_int32 * 32)()
+    rc = L.gam_ring_defaults(int(Np), int(bool(aggressive)), C.byref(n), a)
+    if rc:
+        raise GamError(rc, f"no default rings for Np = {Np}")
+    return [int(a[q]) for q in range(n.value)]
+
+
 class GameraGPU:
     """One GAMERA app whose Grid and State live on the GPU."""
 
     def __init__(self, params: GamParams, lib_path: str = LIB_PATH):
         self.L = load_library(lib_path)
+        self._lib_path = lib_path
         self.params = params
         self._cp = params.to_c()
         h = C.c_void_p()
@@ -382,6 +398,17 @@ class GameraGPU:
         w = np.ascontiguousarray(state, dtype=np.float64)
         assert w.shape == (8,)
         self._check(self.L.gam_set_inflow(self.h, _ptr(w)))
+
+    def set_rings(self, Nch=None, recon: int = RING_PPM, nft: int = 1, clean: bool = True, fast_clean: bool = True):
+        """Ring averaging about the LFM axis (bc[2] / bc[3] = BC_LFM), before
+        the geometry: chunks per ring (default: the reference's table for
+        Nkp), ring reconstruction, Fourier modes removed from the fluxes,
+        CleanLoops and its fast form."""
+        if Nch is None:
+            Nch = ring_defaults(self.params.Nkp, lib_path=self._lib_path)
+        a = (C.c_int32 * 32)(*[int(x) for x in Nch])
+        self._check(self.L.gam_set_rings(self.h, len(Nch), a, int(recon), int(nft), int(bool(clean)),
+                                         int(bool(fast_clean))))
 
     def set_ionosphere(self, inExyz, inEijk, M0: float, dtCpl: float = 0.0, doIonPush: bool = True, nIonP: int = 1,
                        dtSW0: float = 60.0 / 63.8):

@@ -38,7 +38,7 @@ from dataclasses import dataclass
 import numpy as np
 import torch
 
-from mage_b200.gamera import BC_HALO, BC_PERIODIC, LIB_PATH, GameraGPU, GamParams
+from mage_b200.gamera import BC_HALO, BC_LFM, BC_PERIODIC, LIB_PATH, GameraGPU, GamParams
 
 NG = 4
 
@@ -97,11 +97,13 @@ class Tiles:
     set-up of a handle whose geometry is set (fields, background, wind) and
     uploads its whole state with ghosts and its scalars (gam_upload_state).
     halo_dirs: the directions exchanged (default: those cut in more than one
-    tile); a periodic direction in it with one tile sends to itself."""
+    tile); a periodic direction in it with one tile sends to itself. rings:
+    the keyword arguments of GameraGPU.set_rings for the tiles that hold an
+    LFM pole (set before their geometry)."""
 
     def __init__(self, N, xyz: np.ndarray, dims, comm=None, precision: int = 0, strict: bool = False,
                  problem="bw", bc=None, lib_path: str = LIB_PATH, make_app=None, device=None, halo_dirs=None,
-                 params: dict | None = None):
+                 params: dict | None = None, rings: dict | None = None):
         self.N, self.dims = tuple(N), tuple(dims)
         for d in range(3):
             assert self.N[d] % self.dims[d] == 0, "the tiles must divide the grid"
@@ -135,6 +137,8 @@ class Tiles:
             for d in range(3):
                 if tl.bc[2 * d] == BC_HALO or tl.bc[2 * d + 1] == BC_HALO:
                     g.set_tile_edges(d, tl.edge[2 * d], tl.edge[2 * d + 1])
+            if BC_LFM in tl.bc[2:4]:
+                g.set_rings(**(rings or {}))
             g.set_geometry(tile_corners(xyz, self.N, self.dims, tl.t))
             if problem == "bw":
                 g.init_blast_wave()
