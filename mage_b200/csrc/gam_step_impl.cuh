@@ -1455,6 +1455,26 @@ __global__ void __launch_bounds__(256) k_ring_flux(GamBox b, DevParams<R> P, Wor
     }
 }
 
+// HackFlux = IonFlux (earthcmi.F90:357-404) on the inner tile with rings: the
+// I fluxes of the first face ring at each pole (i = is, j = je then js) set
+// to their ring mean, one thread per pole and component
+template <class R> __global__ void __launch_bounds__(32) k_ion_flux(GamBox b, DevParams<R> P, Work<R> w,
+                                                                      const GamScalars* sc) {
+    if (sc->halted) return;
+    const int G = GAM_NG, q = threadIdx.x;
+    if (q >= 16) return;
+    const int pole = q / 8, comp = q % 8;  // pole 0: E (je), 1: S (js); comp 0-4 gas, 5-7 magnetic
+    if (!(pole == 0 ? P.ring.doE : P.ring.doS)) return;
+    if (comp >= 5 && !P.doMHD) return;
+    const int jr = pole == 0 ? G + b.Njp - 1 : G;
+    R* f = comp < 5 ? w.gF + (long)comp * b.fs : w.mF + (long)(comp - 5) * b.fs;  // the I direction's components
+    GAM_BOX_CHECK(lidx(b, G, jr, G), lidx(b, G, jr, G + b.Nkp - 1), 15);
+    R sum = (R)0;
+    for (int kk = G; kk < G + b.Nkp; kk++) sum = sum + f[lidx(b, G, jr, kk)];
+    const R avg = sum / (R)P.ring.Np;
+    for (int kk = G; kk < G + b.Nkp; kk++) f[lidx(b, G, jr, kk)] = avg;
+}
+
 // the smoothing EMF rows each step starts from zero (InitRAVec): S rows
 // js..js+NumR+1, E rows je-NumR..je+1, every i and k
 template <class R> __global__ void __launch_bounds__(256) k_ring_zero_e(GamBox b, RingData Rg, const GamScalars* sc) {
@@ -2542,6 +2562,7 @@ template <class R, class F> void for_each_kernel(const Ctx<R>& C, int cur, cudaS
         if (C.P.ring.on) {  // RingFlux (stress.F90:137-139), before the fluxes become deltas
             const long n = 2L * b.Ni * b.Nk + (long)b.Nip * b.Njp;
             k_ring_flux<R><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(b, C.P, C.w, C.sc);
+            if (C.P.bc[0] == BCK_ION && C.P.ion.on) k_ion_flux<R><<<1, 32, 0, s>>>(b, C.P, C.w, C.sc);
         }
         if (C.P.doBoris)
             k_update_cells<R, sizeof(R) == 8 ? 6 : 8, true><<<grid_for(cells, blk), blk, 0, s>>>(b, C.P, C.g, S, O, C.w, C.sc, C.gamma, C.gm1);

@@ -627,6 +627,28 @@ static void CalcStress(const Model& M, const Grid& G, const State& nS, const Sta
         }
     }
     if (G.ring.on) RingFlux(M, G, gFlx, mFlx);  // stress.F90:137-139
+    // HackFlux = IonFlux (earthcmi.F90:357-404) on the inner tile with rings:
+    // the I fluxes of the first face ring at each pole set to their ring mean
+    if (G.ring.on && G.bc[0] == BC_ION) {
+        const int jr[2] = {G.je, G.js};
+        const bool on[2] = {G.ring.doE, G.ring.doS};
+        for (int p = 0; p < 2; p++) {
+            if (!on[p]) continue;
+            if (M.doMHD)
+                for (int x = 0; x < NDIM; x++) {
+                    double s = 0.0;
+                    for (int k = G.ks; k <= G.ke; k++) s = s + mFlx(G.is, jr[p], k, x + 3 * IDIR);
+                    const double avg = s / G.ring.Np;
+                    for (int k = G.ks; k <= G.ke; k++) mFlx(G.is, jr[p], k, x + 3 * IDIR) = avg;
+                }
+            for (int nv = 0; nv < NVAR; nv++) {
+                double s = 0.0;
+                for (int k = G.ks; k <= G.ke; k++) s = s + gFlx(G.is, jr[p], k, nv + 5 * IDIR);
+                const double avg = s / G.ring.Np;
+                for (int k = G.ks; k <= G.ke; k++) gFlx(G.is, jr[p], k, nv + 5 * IDIR) = avg;
+            }
+        }
+    }
 #pragma omp parallel for collapse(2)
     for (int k = G.ks; k <= G.ke; k++)
         for (int j = G.js; j <= G.je; j++)
