@@ -45,6 +45,7 @@ BYTES_PER_CELL = {"f64": 8 * (27 + 79), "f32": 4 * (27 + 79)}
 BYTES_PER_CELL_B0 = {"f64": 8 * (27 + 79 + 24), "f32": 4 * (27 + 79) + 8 * 24}
 KERNELS_PER_STEP = 15  # begin, predict, 3x(mom2face, vxb), 3x stress, faces, cells, dt, bc
 DIPOLE_WORKLOAD, DIPOLE_STEPS = "dipole96", 500
+MAGSPHERE_WORKLOAD, MAGSPHERE_STEPS = "lfm96", 100
 
 from mage_b200.workloads import WORKLOADS, corners, make_app  # noqa: E402
 
@@ -190,6 +191,45 @@ def cpu_sample(g, w, params, budget_s=12.0, max_steps=6, variant="fast"):
                       f"oracle {variant} build ({flags}), OpenMP"}
 
 
+def cpu_sample_magsphere(g, w, budget_s=12.0, max_steps=4):
+    """The CPU restatement (fast build, all host threads) of the magnetosphere
+    step: metric, background, state and scalars taken from the GPU set-up."""
+    from oracle.oracle import Oracle, OracleParams
+    from tests.helpers import GEO_FROM_ORACLE
+    from mage_b200 import dipole
+    from mage_b200.gamera import ring_defaults
+    from mage_b200.workloads import ION_DTCPL, MAGSPHERE_BCS, ion_fields
+    N = w["N"]
+    op = OracleParams(*N, CFL=g.params.CFL, noMetric=True, doBackground=True, M0=dipole.M0,
+                      wind=tuple(dipole.wind_code_units()), bc=MAGSPHERE_BCS, ringNch=tuple(ring_defaults(N[2])))
+    o = Oracle(op, np.zeros((3, N[2] + 9, N[1] + 9, N[0] + 9)), "fast")
+    for name, v in g.get_geometry_arrays().items():
+        o.array(GEO_FROM_ORACLE[name])[...] = v
+    o.alloc_background()
+    for name, v in g.get_background().items():
+        o.array(name)[...] = v
+    E, Ee = ion_fields(N)
+    o.set_ionosphere(E, Ee, dipole.M0, ION_DTCPL, True, 1)
+    s = g.download_state()
+    for k in ("Gas", "magFlux", "Bxyz", "oGas", "omagFlux"):
+        o.array(k)[...] = s[k]
+    o.set_scalars(t=s["time"], dt=s["dt"], time=s["time"], otime=s["otime"], ts=s["ts"])
+    del s
+    o.step(1)  # warm-up
+    n, t0 = 0, time.perf_counter()
+    while n < max_steps:
+        o.step(1)
+        n += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    el = time.perf_counter() - t0
+    cells = N[0] * N[1] * N[2]
+    return {"value": cells * n / el, "unit": "cell-updates/s", "cores": int(o.L.orc_num_threads()),
+            "cpu_model": cpu_model(), "kind": "port",
+            "sample": f"{n} timed steps (after 1 warm-up) of the full {N[0]}x{N[1]}x{N[2]} magnetosphere, "
+                      f"oracle fast build (-O3 -march=native -ffast-math), OpenMP"}
+
+
 def slab_main(args, w, rank, local, world, dist, barrier, max_over_ranks):
     """N > 1 GPUs: the grid of N slabs of the workload's size stacked in k (weak
     scaling: every GPU keeps a 192^3 slab), one slab per rank, halo exchange
@@ -314,6 +354,8 @@ def main():
     ap.add_argument("--no-fp32", action="store_true")
     ap.add_argument("--no-dipole", action="store_true", help="skip the dipole-in-wind FP64/FP32 section")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the differentiation-form section")
+    ap.add_argument("--no-magsphere", action="store_true",
+                    help="skip the magnetosphere (LFM grid, rings, ionosphere, wind) section")
     ap.add_argument("--no-other-fp64", dest="other_fp64", action="store_false",
                     help="skip timing the other FP64 build (the FMA form beside the drop-in)")
     ap.add_argument("--replicas", action="store_true", help="N>1: independent replicas instead of k-slabs")
@@ -478,6 +520,29 @@ def main():
                                       if np.abs(A[v]).max() > 1e-8}
         del final, A, B
 
+    # ---- the magnetosphere on an LFM grid (ionospheric boundary with its hooks,
+    # wind, LFM pole with rings): the drop-in and the FP32 form, and the CPU
+    # restatement of the same step on the host cores
+    mag = None
+    if not args.no_magsphere and rank == 0 and world == 1:
+        wm = WORKLOADS[MAGSPHERE_WORKLOAD]
+        Nm = wm["N"]
+        cm = Nm[0] * Nm[1] * Nm[2]
+        xyzm = corners(wm)
+        mag = {"workload": wm["desc"], "grid": list(Nm), "steps": MAGSPHERE_STEPS, "unit": "cell-updates/s"}
+        for prec, name in ((0, "fp64"), (FP32, "fp32")):
+            gm = make_app(MAGSPHERE_WORKLOAD, prec, strict=(prec == 0 and args.strict), xyz=xyzm)
+            gm.step_gamera(args.warmup)
+            gm.step_gamera(MAGSPHERE_STEPS)
+            msm = gm.last_step_ms()
+            mag[name] = {"value": cm * MAGSPHERE_STEPS / (msm / 1e3), "ms_per_step": msm / MAGSPHERE_STEPS}
+            if prec == 0 and not args.no_cpu:
+                mag["cpu_baseline"] = cpu_sample_magsphere(gm, wm)
+            del gm
+        mag["speedup_fp32_vs_fp64"] = mag["fp32"]["value"] / mag["fp64"]["value"]
+        if mag.get("cpu_baseline"):
+            mag["gpu_over_cpu"] = mag["fp64"]["value"] / mag["cpu_baseline"]["value"]
+
     adj = None
     if not args.no_adjoint and rank == 0:
         from mage_b200.diffbench import c4, cost
@@ -538,6 +603,7 @@ def main():
             "fp64_other_form": other,
             "fp32": fp32,
             "dipole": dip,
+            "magnetosphere": mag,
             "adjoint": adj,
             "cpu_baseline": cpu,
             "clocks": clocks,
