@@ -510,18 +510,8 @@ extern "C" int gam_set_rings(gam_handle* h, int32_t NumR, const int32_t* Nch, in
     double* dft = dalloc<double>(h, 6L * Np, &e);
     if (e != cudaSuccess) return fail(h, GAM_ECUDA, "device allocation failed (ring tables)");
     CK(h, cudaMemcpyAsync(dft, ft.data(), ft.size() * sizeof(double), cudaMemcpyHostToDevice, h->s));
-    const size_t w = h->f32 ? 4 : 8;
-    const long nthr = 2L * (b.Nip + 1) * NumR, stride = 5L * (ncMax + 4);
-    void* sE = nullptr;
-    void* ch = nullptr;
-    if (h->f32) {
-        sE = dalloc<float>(h, 3 * b.fs, &e);
-        if (e == cudaSuccess) ch = dalloc<float>(h, nthr * stride, &e);
-    } else {
-        sE = dalloc<double>(h, 3 * b.fs, &e);
-        if (e == cudaSuccess) ch = dalloc<double>(h, nthr * stride, &e);
-    }
-    (void)w;
+    const long stride = 5L * (ncMax + 4);  // the chunk values of one ring's 5 variables (shared memory)
+    void* sE = h->f32 ? (void*)dalloc<float>(h, 3 * b.fs, &e) : (void*)dalloc<double>(h, 3 * b.fs, &e);
     if (e != cudaSuccess) return fail(h, GAM_ECUDA, "device allocation failed (ring work arrays)");
     RingData R{};
     R.on = 1;
@@ -538,7 +528,6 @@ extern "C" int gam_set_rings(gam_handle* h, int32_t NumR, const int32_t* Nch, in
     R.chunkStride = (int)stride;
     R.ftab = dft;
     R.smoothE = sE;
-    R.chunk = ch;
     h->cd.P.ring = R;
     h->cf.P.ring = R;
     CK(h, cudaStreamSynchronize(h->s));

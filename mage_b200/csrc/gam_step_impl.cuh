@@ -1561,22 +1561,28 @@ template <class R> __device__ __forceinline__ void ring_chunk_ghosts(R* chW, int
     }
 }
 
-// CalcSmoothE (ringav.F90:212-344) for one ring: the J fluxes through the
-// ring (then the I fluxes) cleaned of Fourier modes 0..nft, chunk-averaged,
-// reconstructed, dirtied again; the change of each face's flux accumulated
-// along its chunk into the I (J) EMFs of the smoothing field
+// CalcSmoothE (ringav.F90:212-344) for one ring, one warp per ring: the J
+// fluxes through the ring (then the I fluxes) cleaned of Fourier modes
+// 0..nft, chunk-averaged, reconstructed, dirtied again; the change of each
+// face's flux accumulated along its chunk into the I (J) EMFs of the
+// smoothing field. Every sum keeps the sequential order of the CPU code
+// (one lane per sum); the lanes split the independent cells and chunks.
 template <class R>
-__global__ void __launch_bounds__(64) k_ring_smooth_e(GamBox b, RingData Rg, StateBuf<R> S, const GamScalars* sc) {
+__global__ void __launch_bounds__(32) k_ring_smooth_e(GamBox b, RingData Rg, StateBuf<R> S, const GamScalars* sc) {
     if (sc->halted) return;
-    const int G = GAM_NG, Np = Rg.Np, nsl = b.Nip + 1;
-    const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    const int G = GAM_NG, Np = Rg.Np, nsl = b.Nip + 1, lane = threadIdx.x;
+    const long t = blockIdx.x;
     const long nper = (long)nsl * Rg.NumR;
     if (t >= 2 * nper) return;
     const int pole = (int)(t / nper);
     if (!(pole == 0 ? Rg.doS : Rg.doE)) return;
     const int nS = G + (int)(t % nper % nsl), nR = 1 + (int)(t % nper / nsl);
     const int NumCh = Rg.Nch[nR - 1], dC = Np / NumCh;
-    R* chW = (R*)Rg.chunk + t * Rg.chunkStride;
+    extern __shared__ __align__(16) unsigned char ring_smem[];
+    R* bF = (R*)ring_smem;  // the ring's fluxes
+    R* cl = bF + Np;        // cleaned fluxes, then the flux changes
+    R* chW = cl + Np;       // chunk values with 2 periodic ghosts each side
+    __shared__ R cf[6];     // CleanRing's coefficients (m, cos / sin)
     R* E = (R*)Rg.smoothE;
     const long fs = b.fs;
     const double* cs = Rg.ftab;
@@ -1586,64 +1592,63 @@ __global__ void __launch_bounds__(64) k_ring_smooth_e(GamBox b, RingData Rg, Sta
         const int jf = pole == 1 ? G + b.Njp - nR : (fD == 1 ? G + nR : G + nR - 1);
         const int je = pole == 1 ? G + b.Njp - nR : (eD == 0 ? G + nR : G + nR - 1);
         const R* mf = S.mf + fD * fs;
-        GAM_BOX_CHECK(lidx(b, nS, jf, G), lidx(b, nS, jf, G + Np - 1), 15);
-        // CleanRing: coefficients
-        R cC[3] = {(R)0, (R)0, (R)0}, cS[3] = {(R)0, (R)0, (R)0};
-        for (int n = 1; n <= Np; n++) {
-            const R Q = mf[lidx(b, nS, jf, G + n - 1)];
-            for (int m = 0; m <= Rg.nft; m++) {
-                cC[m] = cC[m] + Q * (R)cs[(2 * m) * Np + n - 1];
-                cS[m] = cS[m] + Q * (R)cs[(2 * m + 1) * Np + n - 1];
-            }
+        if (!GAM_BOX_OK(lidx(b, nS, jf, G), lidx(b, nS, jf, G + Np - 1), 15)) return;
+        for (int n = lane; n < Np; n += 32) bF[n] = mf[lidx(b, nS, jf, G + n)];
+        __syncwarp();
+        // CleanRing's coefficients: one lane per sum, sequential over the ring
+        if (lane < 2 * (Rg.nft + 1)) {
+            const int m = lane >> 1;
+            const double* tab = cs + (long)lane * Np;  // (2 m + c) Np
+            R acc = (R)0;
+            for (int n = 0; n < Np; n++) acc = acc + bF[n] * (R)tab[n];
+            cf[lane] = (m == 0 ? (R)0.5 * (R)Rg.aScl : (R)1 * (R)Rg.aScl) * acc;
         }
-        if (Rg.nft >= 0) {
-            const R h = (R)0.5 * (R)Rg.aScl;
-            cC[0] = h * cC[0];
-            cS[0] = h * cS[0];
-        }
-        for (int m = 1; m <= Rg.nft; m++) {
-            const R a1 = (R)1 * (R)Rg.aScl;
-            cC[m] = a1 * cC[m];
-            cS[m] = a1 * cS[m];
-        }
-        auto cleaned = [&](int n) -> R {  // 1-based n
-            R Q = mf[lidx(b, nS, jf, G + n - 1)];
+        __syncwarp();
+        for (int n = lane; n < Np; n += 32) {
+            R Q = bF[n];
             for (int m = 0; m <= Rg.nft; m++)
-                Q = Q - cC[m] * (R)cs[(2 * m) * Np + n - 1] - cS[m] * (R)cs[(2 * m + 1) * Np + n - 1];
-            return Q;
-        };
-        // chunk averages
-        for (int c = 1; c <= NumCh; c++) {
-            const int lRs = 1 + (c - 1) * dC;
-            R sum = (R)0;
-            for (int l = lRs; l < lRs + dC; l++) sum = sum + cleaned(l);
-            chW[c + 1] = sum / (R)dC;
+                Q = Q - cf[2 * m] * (R)cs[(2 * m) * Np + n] - cf[2 * m + 1] * (R)cs[(2 * m + 1) * Np + n];
+            cl[n] = Q;
         }
-        ring_chunk_ghosts(chW, NumCh);
-        // reconstruct, dirty, accumulate the flux changes into the EMFs
-        for (int c = 1; c <= NumCh; c++) {
+        __syncwarp();
+        for (int c = lane; c < NumCh; c += 32) {
+            R sum = (R)0;
+            for (int l = c * dC; l < (c + 1) * dC; l++) sum = sum + cl[l];
+            chW[c + 2] = sum / (R)dC;
+        }
+        __syncwarp();
+        if (lane == 0) ring_chunk_ghosts(chW, NumCh);
+        __syncwarp();
+        // reconstruct and dirty each cell, then its flux change
+        for (int n = lane; n < Np; n += 32) {
+            const int c = n / dC, m = n - c * dC + 1;
             R a, bq, cq;
-            ring_parabola(Rg.recon, chW, c, a, bq, cq);
-            const int lRs = 1 + (c - 1) * dC;
+            ring_parabola(Rg.recon, chW, c + 1, a, bq, cq);
+            R ra = ring_interp(a, bq, cq, m, dC);
+            for (int mm = 0; mm <= Rg.nft; mm++)
+                ra = ra + cf[2 * mm] * (R)cs[(2 * mm) * Np + n] + cf[2 * mm + 1] * (R)cs[(2 * mm + 1) * Np + n];
+            cl[n] = ra - bF[n];
+        }
+        __syncwarp();
+        // the changes accumulated along each chunk into the EMFs
+        for (int c = lane; c < NumCh; c += 32) {
             R cum = (R)0;
-            for (int m = 1; m <= dC; m++) {
-                const int n = lRs + m - 1;
-                R ra = ring_interp(a, bq, cq, m, dC);
-                for (int mm = 0; mm <= Rg.nft; mm++)
-                    ra = ra + cC[mm] * (R)cs[(2 * mm) * Np + n - 1] + cS[mm] * (R)cs[(2 * mm + 1) * Np + n - 1];
-                const R d = ra - mf[lidx(b, nS, jf, G + n - 1)];
-                const long ce = eD * fs + lidx(b, nS, je, G + n - 1);
-                if (m == 1) {
+            for (int m = 0; m < dC; m++) {
+                const int n = c * dC + m;
+                const long ce = eD * fs + lidx(b, nS, je, G + n);
+                if (m == 0) {
                     E[ce] = (R)0;
-                    cum = -d;
+                    cum = -cl[n];
                 } else {
                     E[ce] = eScl * cum;
-                    cum = cum - d;
+                    cum = cum - cl[n];
                 }
             }
         }
-        // replicate k = ks at ke+1
-        E[eD * fs + lidx(b, nS, je, G + Np)] = E[eD * fs + lidx(b, nS, je, G)];
+        __syncwarp();
+        // replicate k = ks at ke+1 (chunk 0 is lane 0's)
+        if (lane == 0) E[eD * fs + lidx(b, nS, je, G + Np)] = E[eD * fs + lidx(b, nS, je, G)];
+        __syncwarp();
     }
 }
 
@@ -1725,15 +1730,16 @@ template <class R> __global__ void __launch_bounds__(128) k_ring_bfield(GamBox b
     for (int x = 0; x < 3; x++) S.B[x * fs + c] = B[x];
 }
 
-// SmoothGas (ringav.F90:78-210) for one ring: the ring variables (rho,
-// momentum, internal energy; Gas2Ring, ringutils.F90:804-830) chunk-averaged,
-// reconstructed per chunk and written back as gas (Ring2Gas :832-856)
+// SmoothGas (ringav.F90:78-210) for one ring, one warp per ring: the ring
+// variables (rho, momentum, internal energy; Gas2Ring, ringutils.F90:
+// 804-830) chunk-averaged, reconstructed per chunk and written back as gas
+// (Ring2Gas :832-856); each chunk sum sequential on one lane
 template <class R>
-__global__ void __launch_bounds__(64) k_ring_smooth_gas(GamBox b, DevParams<R> P, StateBuf<R> S, const GamScalars* sc) {
+__global__ void __launch_bounds__(32) k_ring_smooth_gas(GamBox b, DevParams<R> P, StateBuf<R> S, const GamScalars* sc) {
     if (sc->halted) return;
     const RingData& Rg = P.ring;
-    const int G = GAM_NG, Np = Rg.Np, nsl = b.Nip;
-    const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    const int G = GAM_NG, Np = Rg.Np, nsl = b.Nip, lane = threadIdx.x;
+    const long t = blockIdx.x;
     const long nper = (long)nsl * Rg.NumR;
     if (t >= 2 * nper) return;
     const int pole = (int)(t / nper);
@@ -1742,11 +1748,14 @@ __global__ void __launch_bounds__(64) k_ring_smooth_gas(GamBox b, DevParams<R> P
     const int NumCh = Rg.Nch[nR - 1], dC = Np / NumCh;
     const int jr = pole == 0 ? G + nR - 1 : G + b.Njp - nR;
     const int cst = NumCh + 4;
-    R* chW = (R*)Rg.chunk + t * Rg.chunkStride;
+    extern __shared__ __align__(16) unsigned char ring_smem[];
+    R* rW = (R*)ring_smem;  // 5 x Np ring variables
+    R* chW = rW + 5 * Np;   // 5 x (NumCh + 4) chunk values
     const long fs = b.fs;
-    GAM_BOX_CHECK(lidx(b, nS, jr, G), lidx(b, nS, jr, G + Np - 1), 15);
-    auto ring_var = [&](int n, R* W) {  // Gas2Ring of ring cell n (1-based)
-        const long c = lidx(b, nS, jr, G + n - 1);
+    if (!GAM_BOX_OK(lidx(b, nS, jr, G), lidx(b, nS, jr, G + Np - 1), 15)) return;
+    for (int n = lane; n < Np; n += 32) {
+        const long c = lidx(b, nS, jr, G + n);
+        R W[5];
 #pragma unroll
         for (int v = 0; v < 5; v++) W[v] = S.Gas[v * fs + c];
         const R D = rmax(W[0], P.dFloor);
@@ -1754,42 +1763,38 @@ __global__ void __launch_bounds__(64) k_ring_smooth_gas(GamBox b, DevParams<R> P
         const R Pr = rmax(P.gm1 * (W[4] - KinE), P.pFloor);
         W[0] = D;
         W[4] = Pr / P.gm1;
-    };
-    // chunk averages of the five ring variables
-    for (int c = 1; c <= NumCh; c++) {
-        const int lRs = 1 + (c - 1) * dC;
-        R sum[5] = {(R)0, (R)0, (R)0, (R)0, (R)0};
-        for (int l = lRs; l < lRs + dC; l++) {
-            R W[5];
-            ring_var(l, W);
 #pragma unroll
-            for (int v = 0; v < 5; v++) sum[v] = sum[v] + W[v];
-        }
-#pragma unroll
-        for (int v = 0; v < 5; v++) chW[v * cst + c + 1] = sum[v] / (R)dC;
+        for (int v = 0; v < 5; v++) rW[v * Np + n] = W[v];
     }
-    for (int v = 0; v < 5; v++) ring_chunk_ghosts(chW + v * cst, NumCh);
-    // reconstruct and write back
-    for (int c = 1; c <= NumCh; c++) {
-        R a[5], bq[5], cq[5];
+    __syncwarp();
+    for (int q = lane; q < 5 * NumCh; q += 32) {
+        const int v = q / NumCh, c = q % NumCh;
+        R sum = (R)0;
+        for (int l = c * dC; l < (c + 1) * dC; l++) sum = sum + rW[v * Np + l];
+        chW[v * cst + c + 2] = sum / (R)dC;
+    }
+    __syncwarp();
+    if (lane < 5) ring_chunk_ghosts(chW + lane * cst, NumCh);
+    __syncwarp();
+    for (int n = lane; n < Np; n += 32) {
+        const int c = n / dC, m = n - c * dC + 1;
+        R W[5];
 #pragma unroll
-        for (int v = 0; v < 5; v++) ring_parabola(Rg.recon, chW + v * cst, c, a[v], bq[v], cq[v]);
-        const int lRs = 1 + (c - 1) * dC;
-        for (int m = 1; m <= dC; m++) {
-            R W[5];
-#pragma unroll
-            for (int v = 0; v < 5; v++) W[v] = ring_interp(a[v], bq[v], cq[v], m, dC);
-            const R D = rmax(W[0], P.dFloor);
-            R Pr = P.gm1 * W[4];
-            Pr = rmax(Pr, P.pFloor);
-            const R KinE = (R)0.5 * (W[1] * W[1] + W[2] * W[2] + W[3] * W[3]) / D;
-            const long c2 = lidx(b, nS, jr, G + lRs + m - 2);
-            S.Gas[c2] = D;
-            S.Gas[fs + c2] = W[1];
-            S.Gas[2 * fs + c2] = W[2];
-            S.Gas[3 * fs + c2] = W[3];
-            S.Gas[4 * fs + c2] = KinE + Pr / P.gm1;
+        for (int v = 0; v < 5; v++) {
+            R a, bq, cq;
+            ring_parabola(Rg.recon, chW + v * cst, c + 1, a, bq, cq);
+            W[v] = ring_interp(a, bq, cq, m, dC);
         }
+        const R D = rmax(W[0], P.dFloor);
+        R Pr = P.gm1 * W[4];
+        Pr = rmax(Pr, P.pFloor);
+        const R KinE = (R)0.5 * (W[1] * W[1] + W[2] * W[2] + W[3] * W[3]) / D;
+        const long c2 = lidx(b, nS, jr, G + n);
+        S.Gas[c2] = D;
+        S.Gas[fs + c2] = W[1];
+        S.Gas[2 * fs + c2] = W[2];
+        S.Gas[3 * fs + c2] = W[3];
+        S.Gas[4 * fs + c2] = KinE + Pr / P.gm1;
     }
 }
 
@@ -2434,7 +2439,8 @@ template <class R> void launch_ring_average(const Ctx<R>& C, const StateBuf<R>& 
         const long nz = 2L * (Rg.NumR + 2) * b.Ni * b.Nk;
         k_ring_zero_e<R><<<(unsigned)((nz + 255) / 256), 256, 0, s>>>(b, Rg, C.sc);
         const long ne = 2L * (b.Nip + 1) * Rg.NumR;
-        k_ring_smooth_e<R><<<(unsigned)((ne + 63) / 64), 64, 0, s>>>(b, Rg, O, C.sc);
+        const size_t smE = (size_t)(2 * Rg.Np + Rg.chunkStride / 5) * sizeof(R);
+        k_ring_smooth_e<R><<<(unsigned)ne, 32, smE, s>>>(b, Rg, O, C.sc);
         R* E = (R*)Rg.smoothE;
         const int ni = b.Nip + 1;
         k_ring_pole_e<R><<<(unsigned)((2 * ni + 127) / 128), 128, 0, s>>>(b, Rg, E, G, G + b.Nip, C.sc);
@@ -2452,7 +2458,8 @@ template <class R> void launch_ring_average(const Ctx<R>& C, const StateBuf<R>& 
         k_ring_bfield<R><<<(unsigned)((nb + 127) / 128), 128, 0, s>>>(b, C.g, Rg, O, C.sc);
     }
     const long ng = 2L * b.Nip * Rg.NumR;
-    k_ring_smooth_gas<R><<<(unsigned)((ng + 63) / 64), 64, 0, s>>>(b, C.P, O, C.sc);
+    const size_t smG = (size_t)(5 * Rg.Np + Rg.chunkStride) * sizeof(R);
+    k_ring_smooth_gas<R><<<(unsigned)ng, 32, smG, s>>>(b, C.P, O, C.sc);
 }
 
 // The kernels of one stepGamera in order, each handed to f(id, launch) with

@@ -52,10 +52,9 @@ struct RingData {
     double tScl;          // CleanLoops' scale (1 with doFastClean)
     double aScl;          // CleanRing's 2/Np (in default real)
     int Nch[32];          // chunks of ring 1..NumR
-    int chunkStride;      // scratch values per ring thread
+    int chunkStride;      // 5 (max chunks + 4): shared-memory chunk values of one ring
     const double* ftab;   // cos / sin (m phi_n): [(2 m + c) Np + n - 1], m = 0..2
     void* smoothE;        // smoothing EMFs, 3 components of the box (compute precision)
-    void* chunk;          // per ring thread: chunk values
 };
 
 template <class R> struct DevParams {
