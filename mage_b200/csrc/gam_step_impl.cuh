@@ -1385,23 +1385,31 @@ __global__ void __launch_bounds__(128) k_nudge_sw(GamBox b, DevParams<R> P, Geo<
 // PoleE (ringav.F90:394-430) over slices i0..i1, or the same touch-up of
 // WindEFix (apps/wind.F90:549-564): on each pole row the K EMFs zero and the
 // I EMFs their mean over ks..ke, over the whole ghosted k range
+// One warp per (pole, slice): the row is staged in shared memory by the
+// lanes and summed by lane 0 in k order (the CPU code's sum).
+template <class R> __device__ __forceinline__ R ring_row_mean(const R* __restrict__ f, long c0, long sk, int Np, R* row) {
+    const int lane = threadIdx.x;
+    for (int n = lane; n < Np; n += 32) row[n] = f[c0 + n * sk];
+    __syncwarp();
+    R sum = (R)0;
+    if (lane == 0)
+        for (int n = 0; n < Np; n++) sum = sum + row[n];
+    sum = __shfl_sync(0xffffffffu, sum, 0);
+    return sum / (R)Np;
+}
 template <class R>
-__global__ void __launch_bounds__(128) k_ring_pole_e(GamBox b, RingData Rg, R* __restrict__ E, int i0, int i1,
-                                                     const GamScalars* sc) {
+__global__ void __launch_bounds__(32) k_ring_pole_e(GamBox b, RingData Rg, R* __restrict__ E, int i0, int i1,
+                                                    const GamScalars* sc) {
     if (sc->halted) return;
-    const int G = GAM_NG;
-    const long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
-    const int ni = i1 - i0 + 1;
-    if (q >= 2L * ni) return;
-    const int pole = (int)(q / ni), ii = i0 + (int)(q % ni);
+    const int G = GAM_NG, ni = i1 - i0 + 1;
+    const int pole = blockIdx.x / ni, ii = i0 + (int)(blockIdx.x % ni);
     if (!(pole == 0 ? Rg.doS : Rg.doE)) return;
     const int jp = pole == 0 ? G : G + b.Njp;
     const long fs = b.fs;
-    GAM_BOX_CHECK(lidx(b, ii, jp, 0), lidx(b, ii, jp, b.Nk - 1), 15);
-    R sum = (R)0;
-    for (int kk = G; kk < G + b.Nkp; kk++) sum = sum + E[lidx(b, ii, jp, kk)];
-    const R avg = sum / (R)Rg.Np;
-    for (int kk = 0; kk < b.Nk; kk++) {
+    if (!GAM_BOX_OK(lidx(b, ii, jp, 0), lidx(b, ii, jp, b.Nk - 1), 15)) return;
+    extern __shared__ __align__(16) unsigned char ring_smem[];
+    const R avg = ring_row_mean(E, lidx(b, ii, jp, G), b.sk, Rg.Np, (R*)ring_smem);
+    for (int kk = threadIdx.x; kk < b.Nk; kk += 32) {
         const long c = lidx(b, ii, jp, kk);
         E[2 * fs + c] = (R)0;
         E[c] = avg;
@@ -1461,18 +1469,16 @@ __global__ void __launch_bounds__(256) k_ring_flux(GamBox b, DevParams<R> P, Wor
 template <class R> __global__ void __launch_bounds__(32) k_ion_flux(GamBox b, DevParams<R> P, Work<R> w,
                                                                       const GamScalars* sc) {
     if (sc->halted) return;
-    const int G = GAM_NG, q = threadIdx.x;
-    if (q >= 16) return;
-    const int pole = q / 8, comp = q % 8;  // pole 0: E (je), 1: S (js); comp 0-4 gas, 5-7 magnetic
+    const int G = GAM_NG;
+    const int pole = blockIdx.x / 8, comp = blockIdx.x % 8;  // pole 0: E (je), 1: S (js); comp 0-4 gas, 5-7 magnetic
     if (!(pole == 0 ? P.ring.doE : P.ring.doS)) return;
     if (comp >= 5 && !P.doMHD) return;
     const int jr = pole == 0 ? G + b.Njp - 1 : G;
     R* f = comp < 5 ? w.gF + (long)comp * b.fs : w.mF + (long)(comp - 5) * b.fs;  // the I direction's components
-    GAM_BOX_CHECK(lidx(b, G, jr, G), lidx(b, G, jr, G + b.Nkp - 1), 15);
-    R sum = (R)0;
-    for (int kk = G; kk < G + b.Nkp; kk++) sum = sum + f[lidx(b, G, jr, kk)];
-    const R avg = sum / (R)P.ring.Np;
-    for (int kk = G; kk < G + b.Nkp; kk++) f[lidx(b, G, jr, kk)] = avg;
+    if (!GAM_BOX_OK(lidx(b, G, jr, G), lidx(b, G, jr, G + b.Nkp - 1), 15)) return;
+    extern __shared__ __align__(16) unsigned char ring_smem[];
+    const R avg = ring_row_mean(f, lidx(b, G, jr, G), b.sk, P.ring.Np, (R*)ring_smem);
+    for (int kk = G + threadIdx.x; kk < G + b.Nkp; kk += 32) f[lidx(b, G, jr, kk)] = avg;
 }
 
 // the smoothing EMF rows each step starts from zero (InitRAVec): S rows
@@ -1683,23 +1689,19 @@ template <class R> __global__ void __launch_bounds__(256) k_ring_e2flux(GamBox b
 
 // CleanLoops (ringav.F90:347-391): the K fluxes of the pole's first ring
 // lose their mean, slices is..ie+1
-template <class R> __global__ void __launch_bounds__(128) k_ring_clean_loops(GamBox b, RingData Rg, StateBuf<R> S,
-                                                                               const GamScalars* sc) {
+template <class R> __global__ void __launch_bounds__(32) k_ring_clean_loops(GamBox b, RingData Rg, StateBuf<R> S,
+                                                                              const GamScalars* sc) {
     if (sc->halted) return;
-    const int G = GAM_NG;
-    const long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
-    const int ni = b.Nip + 1;
-    if (q >= 2L * ni) return;
-    const int pole = (int)(q / ni), ii = G + (int)(q % ni);
+    const int G = GAM_NG, ni = b.Nip + 1;
+    const int pole = blockIdx.x / ni, ii = G + (int)(blockIdx.x % ni);
     if (!(pole == 0 ? Rg.doS : Rg.doE)) return;
     const int jr = pole == 0 ? G : G + b.Njp - 1;
     R* mK = S.mf + 2 * b.fs;
-    GAM_BOX_CHECK(lidx(b, ii, jr, G), lidx(b, ii, jr, G + b.Nkp), 15);
-    R sum = (R)0;
-    for (int kk = G; kk < G + b.Nkp; kk++) sum = sum + mK[lidx(b, ii, jr, kk)];
-    const R avg = sum / (R)Rg.Np;
+    if (!GAM_BOX_OK(lidx(b, ii, jr, G), lidx(b, ii, jr, G + b.Nkp), 15)) return;
+    extern __shared__ __align__(16) unsigned char ring_smem[];
+    const R avg = ring_row_mean(mK, lidx(b, ii, jr, G), b.sk, Rg.Np, (R*)ring_smem);
     const R tScl = (R)Rg.tScl;
-    for (int kk = G; kk <= G + b.Nkp; kk++) {
+    for (int kk = G + threadIdx.x; kk <= G + b.Nkp; kk += 32) {
         const long c = lidx(b, ii, jr, kk);
         mK[c] = mK[c] - tScl * avg;
     }
@@ -2443,7 +2445,7 @@ template <class R> void launch_ring_average(const Ctx<R>& C, const StateBuf<R>& 
         k_ring_smooth_e<R><<<(unsigned)ne, 32, smE, s>>>(b, Rg, O, C.sc);
         R* E = (R*)Rg.smoothE;
         const int ni = b.Nip + 1;
-        k_ring_pole_e<R><<<(unsigned)((2 * ni + 127) / 128), 128, 0, s>>>(b, Rg, E, G, G + b.Nip, C.sc);
+        k_ring_pole_e<R><<<(unsigned)(2 * ni), 32, Rg.Np * sizeof(R), s>>>(b, Rg, E, G, G + b.Nip, C.sc);
         // FixEFieldLFM over the rows that can be nonzero (the others hold zeros)
         const int sj1 = std::min(G + Rg.NumR + 1, G + b.Njp), ej0 = std::max(G + b.Njp - 1 - Rg.NumR, G);
         if (Rg.doS)
@@ -2453,7 +2455,7 @@ template <class R> void launch_ring_average(const Ctx<R>& C, const StateBuf<R>& 
                 b, E, ej0, G + b.Njp, C.sc);
         const long nf = 2L * (Rg.NumR + 1) * (b.Nip + 1) * (b.Nkp + 1);
         k_ring_e2flux<R><<<(unsigned)((nf + 255) / 256), 256, 0, s>>>(b, Rg, O, C.sc);
-        if (Rg.clean) k_ring_clean_loops<R><<<(unsigned)((2 * ni + 127) / 128), 128, 0, s>>>(b, Rg, O, C.sc);
+        if (Rg.clean) k_ring_clean_loops<R><<<(unsigned)(2 * ni), 32, Rg.Np * sizeof(R), s>>>(b, Rg, O, C.sc);
         const long nb = 2L * (G + Rg.NumR + 2) * b.Ni * b.Nk;
         k_ring_bfield<R><<<(unsigned)((nb + 127) / 128), 128, 0, s>>>(b, C.g, Rg, O, C.sc);
     }
@@ -2551,15 +2553,16 @@ template <class R, class F> void for_each_kernel(const Ctx<R>& C, int cur, cudaS
                 const long nw = 4L * (b.Njp + 1) * (b.Nkp + 1);
                 k_wind_efix<R><<<(unsigned)((nw + 255) / 256), 256, 0, s>>>(b, C.P, C.g, S, C.w, C.sc);
                 if (C.P.ring.on)  // WindEFix's touch-up of the pole rows of its shells
-                    k_ring_pole_e<R><<<1, 128, 0, s>>>(b, C.P.ring, C.w.E, GAM_NG + b.Nip - 3, GAM_NG + b.Nip, C.sc);
+                    k_ring_pole_e<R><<<8, 32, C.P.ring.Np * sizeof(R), s>>>(b, C.P.ring, C.w.E, GAM_NG + b.Nip - 3,
+                                                                          GAM_NG + b.Nip, C.sc);
             }
             if (C.P.bc[4] != BCK_HALO)
                 k_fix_e_lfm<R><<<(unsigned)((nf + 255) / 256), 256, 0, s>>>(b, C.w.E, GAM_NG, GAM_NG + b.Njp, C.sc);
         }
         if (C.P.ring.on && C.P.doMHD) {  // PoleE before E2Flux (mhdgroup.F90:140-142)
             const int ni = b.Nip + 1;
-            k_ring_pole_e<R><<<(unsigned)((2 * ni + 127) / 128), 128, 0, s>>>(b, C.P.ring, C.w.E, GAM_NG, GAM_NG + b.Nip,
-                                                                            C.sc);
+            k_ring_pole_e<R><<<(unsigned)(2 * ni), 32, C.P.ring.Np * sizeof(R), s>>>(b, C.P.ring, C.w.E, GAM_NG,
+                                                                                    GAM_NG + b.Nip, C.sc);
             const long nf = (long)ni * (b.Njp + 1);
             k_fix_e_lfm<R><<<(unsigned)((nf + 255) / 256), 256, 0, s>>>(b, C.w.E, GAM_NG, GAM_NG + b.Njp, C.sc);
         }
@@ -2569,7 +2572,8 @@ template <class R, class F> void for_each_kernel(const Ctx<R>& C, int cur, cudaS
         if (C.P.ring.on) {  // RingFlux (stress.F90:137-139), before the fluxes become deltas
             const long n = 2L * b.Ni * b.Nk + (long)b.Nip * b.Njp;
             k_ring_flux<R><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(b, C.P, C.w, C.sc);
-            if (C.P.bc[0] == BCK_ION && C.P.ion.on) k_ion_flux<R><<<1, 32, 0, s>>>(b, C.P, C.w, C.sc);
+            if (C.P.bc[0] == BCK_ION && C.P.ion.on)
+                k_ion_flux<R><<<16, 32, C.P.ring.Np * sizeof(R), s>>>(b, C.P, C.w, C.sc);
         }
         if (C.P.doBoris)
             k_update_cells<R, sizeof(R) == 8 ? 6 : 8, true><<<grid_for(cells, blk), blk, 0, s>>>(b, C.P, C.g, S, O, C.w, C.sc, C.gamma, C.gm1);
