@@ -259,18 +259,22 @@ def slab_main(args, w, rank, local, world, dist, barrier, max_over_ranks):
     if args.e2e_steps > 0:
         g = sl.apps[0]
         st = g.download_state()
-        pin = {k: torch.from_numpy(np.ascontiguousarray(st[k])).pin_memory().numpy()
-               for k in ("Gas", "magFlux", "Bxyz", "oGas", "omagFlux")}
-        spare = {k: torch.from_numpy(np.empty_like(st[k])).pin_memory().numpy() for k in ("Gas", "magFlux", "Bxyz")}
-        h2d = sum(pin[k].nbytes for k in pin)
-        d2h = pin["Gas"].nbytes + pin["magFlux"].nbytes + pin["Bxyz"].nbytes
+        pin = {k: torch.from_numpy(np.ascontiguousarray(st[k])).pin_memory().numpy() for k in ("Gas", "magFlux")}
+        spare = {k: torch.from_numpy(np.empty_like(st[k])).pin_memory().numpy() for k in ("Gas", "magFlux")}
+        h2d = pin["Gas"].nbytes + pin["magFlux"].nbytes
+        d2h = pin["Gas"].nbytes + pin["magFlux"].nbytes
+        time_, otime_, dt_, ts_ = st["time"], st["otime"], st["dt"], st["ts"]
+        del st
         barrier()
         t0 = time.perf_counter()
         for _ in range(args.e2e_steps):
-            g.upload_state(pin["Gas"], pin["magFlux"], pin["Bxyz"], pin["oGas"], pin["omagFlux"], st["time"],
-                           st["otime"], st["dt"], st["ts"])
+            # as on one GPU: State's Gas and fluxes cross PCIe, oState stays on
+            # the device, Bxyz is formed there from the fluxes
+            g.upload_state(pin["Gas"], pin["magFlux"], None, None, None, time_, otime_, dt_, ts_)
             sl.step(1)
-            g.download_state(into=spare, old=False)
+            r = g.download_state(into=spare, names=("Gas", "magFlux"))
+            pin, spare = {"Gas": r["Gas"], "magFlux": r["magFlux"]}, pin
+            otime_, time_, dt_, ts_ = time_, r["time"], r["dt"], r["ts"]
         barrier()
         e2e_value = world * cells * args.e2e_steps / max_over_ranks(time.perf_counter() - t0)
     peak, peak_kind = measured_peak()
@@ -289,8 +293,9 @@ def slab_main(args, w, rank, local, world, dist, barrier, max_over_ranks):
                          "unit_of_launch": "one step per GPU"},
             "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "steps": args.e2e_steps,
-                    "what": "per step and rank: gam_upload_state of the slab from pinned host memory, one tiled step "
-                            "(halo exchange included), gam_download_state of the slab's State"},
+                    "what": "per step and rank: gam_upload_state of the slab's State%Gas and State%magFlux from "
+                            "pinned host memory (oState stays on the device, Bxyz formed there), one tiled step (halo "
+                            "exchange included), gam_download_state of the new Gas and magFlux"},
             "cpu_baseline": None,
             "clocks": clocks,
             "gpu_launches": 21 * args.steps,
@@ -423,11 +428,11 @@ def main():
         def pinned(a):
             return torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
 
-        cur = {k: pinned(st[k]) for k in ("Gas", "magFlux", "Bxyz")}
+        cur = {k: pinned(st[k]) for k in ("Gas", "magFlux")}
         old = {"Gas": pinned(st["oGas"]), "magFlux": pinned(st["omagFlux"])}
-        spare = {k: pinned(np.empty_like(st[k])) for k in ("Gas", "magFlux", "Bxyz")}
+        spare = {k: pinned(np.empty_like(st[k])) for k in ("Gas", "magFlux")}
         h2d = cur["Gas"].nbytes + cur["magFlux"].nbytes
-        d2h = sum(cur[k].nbytes for k in cur)
+        d2h = cur["Gas"].nbytes + cur["magFlux"].nbytes
         time_, otime_, dt_, ts_ = st["time"], st["otime"], st["dt"], st["ts"]
         del st
         barrier()
@@ -438,11 +443,12 @@ def main():
             # Bxyz is bFlux2Fld of the fluxes: computed on the device, not sent
             g.upload_state(cur["Gas"], cur["magFlux"], None, None, None, time_, otime_, dt_, ts_)
             g.step_gamera(1)
-            r = g.download_state(into=spare, old=False)
+            # the new State's Gas and fluxes: all the next step takes (its
+            # Bxyz is bFlux2Fld of the fluxes, formed on the device again)
+            r = g.download_state(into=spare, names=("Gas", "magFlux"))
             # the host driver keeps oState = the previous State; rotate the pinned buffers
             old["Gas"], old["magFlux"], spare["Gas"], spare["magFlux"] = cur["Gas"], cur["magFlux"], old["Gas"], old["magFlux"]
             cur["Gas"], cur["magFlux"] = r["Gas"], r["magFlux"]
-            cur["Bxyz"], spare["Bxyz"] = r["Bxyz"], cur["Bxyz"]
             otime_, time_, dt_, ts_ = time_, r["time"], r["dt"], r["ts"]
         barrier()
         e2e_s = max_over_ranks((time.perf_counter() - t0))
@@ -598,8 +604,9 @@ def main():
                     "steps": args.e2e_steps,
                     "what": "per step: gam_upload_state of State%Gas and State%magFlux from pinned host memory "
                             "(Bxyz computed from the fluxes on the device; oState stays on the device: the State "
-                            "before the last step), gam_step(1), gam_download_state (new Gas, magFlux, Bxyz to "
-                            "pinned host memory)"},
+                            "before the last step), gam_step(1), gam_download_state of the new State%Gas and "
+                            "State%magFlux to pinned host memory (what the next step takes; its Bxyz is bFlux2Fld of "
+                            "the fluxes, formed on the device at the upload)"},
             "fp64_other_form": other,
             "fp32": fp32,
             "dipole": dip,

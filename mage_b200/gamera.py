@@ -328,10 +328,12 @@ class GameraGPU:
         self._check(self.L.gam_get_oostate(self.h, _ptr(a), C.byref(t)))
         return {"oomagFlux": a, "ootime": t.value}
 
-    def download_state(self, into: dict | None = None, old: bool = True) -> dict:
+    def download_state(self, into: dict | None = None, old: bool = True, names=None) -> dict:
         """State (and with ``old`` the previous state) in Fortran layout;
-        ``into`` may supply preallocated (e.g. pinned) arrays."""
-        names = ("Gas", "magFlux", "Bxyz", "oGas", "omagFlux") if old else ("Gas", "magFlux", "Bxyz")
+        ``into`` may supply preallocated (e.g. pinned) arrays; ``names`` picks
+        the arrays (the others are not copied)."""
+        if names is None:
+            names = ("Gas", "magFlux", "Bxyz", "oGas", "omagFlux") if old else ("Gas", "magFlux", "Bxyz")
         kinds = {"Gas": ("cell", 5), "magFlux": ("face", 3), "Bxyz": ("cell", 3), "oGas": ("cell", 5),
                  "omagFlux": ("face", 3)}
         out = {}
