@@ -214,11 +214,12 @@ __device__ void gas_adj(const DevParams<R>& P, A sgn, const R* W, const R* T, co
 }
 
 // Adjoint of the face fluxes of direction D over the range r (one face per
-// thread): recompute, then reverse. 4 (FP64) / 5 (FP32) blocks per SM: the
-// unbounded kernel took 214-240 registers (2 blocks); bounded it spills
+// thread): recompute (SAVED: load the face states the forward stored in
+// w.fsv), then reverse. 4 (FP64) / 5 (FP32) blocks per SM: the unbounded
+// recomputing kernel took 214-240 registers (2 blocks); bounded it spills
 // (local memory, L1-resident) but hides more load latency (measured on
 // 128^3: 3 -> 4 FP64 blocks took the adjoint step from 5.9 to 5.7 ms).
-template <class R, int D>
+template <class R, int D, bool SAVED = false>
 __global__ void __launch_bounds__(128, (sizeof(R) == 8 ? 4 : 5)) k_stress_adj(GamBox b, DevParams<R> P, Geo<R> g, const R* __restrict__ Blim,
                                                     Work<R> w, Range r, const R* __restrict__ dgF,
                                                     const R* __restrict__ dmF, R* dQW, R* dWn, R* dQB, R* dBlim,
@@ -234,40 +235,54 @@ __global__ void __launch_bounds__(128, (sizeof(R) == 8 ? 4 : 5)) k_stress_adj(Ga
     R vol[8];
     for (int n = 0; n < 8; n++) vol[n] = g.vol[c + (n - 4) * s];
     const R Vi = central8(vol);
-    const Quot<R> qVi(Vi);  // the 8 reconstructions share the divisor
-    // forward states; the stencils are loaded again for the reverse of the
-    // reconstruction rather than kept live (fewer registers, more warps)
     R WL[5], WR[5], MagL[3] = {(R)0, (R)0, (R)0}, MagR[3] = {(R)0, (R)0, (R)0};
-    for (int v = 0; v < 5; v++) {
-        R qW[8], nW[4];
-        for (int n = 0; n < 8; n++) qW[n] = w.QW[v * fs + c + (n - 4) * s];
-        for (int m = 0; m < 4; m++) nW[m] = w.Wn[v * fs + c + (m - 2) * s];
-        lrs_from_qdv(P, qW, nW, qVi, WL[v], WR[v]);
-    }
     R Bn = (R)0;
     double B0[3] = {0.0, 0.0, 0.0}, B0n = 0.0;
     if (P.doMHD) {
         Bn = w.Bnf[D * fs + c];
-        for (int x = 0; x < 3; x++) {
-            R qB[8], nB[4];
-            for (int n = 0; n < 8; n++) qB[n] = w.QB[x * fs + c + (n - 4) * s];
-            for (int m = 0; m < 4; m++) nB[m] = Blim[x * fs + c + (m - 2) * s];
-            lrs_from_qdv(P, qB, nB, qVi, MagL[x], MagR[x]);
-        }
         if (P.doBackground) {
             for (int x = 0; x < 3; x++) B0[x] = g.fcB0[(x + 3 * D) * fs + c];
             B0n = g.bFlux0[D * fs + c] / (double)fa;
         }
     }
-    R VaD = (R)0, bbD = (R)0;
-    if (P.doMHD) {
-        R mFs[3] = {(R)0, (R)0, (R)0};
-        mag_kin_flux(P, (R)-1, WL, MagL, Bn, T, B0, B0n, mFs, bbD, VaD);
-        mag_kin_flux(P, (R)1, WR, MagR, Bn, T, B0, B0n, mFs, bbD, VaD);
+    R VaD = (R)0, dW[5] = {(R)0, (R)0, (R)0, (R)0, (R)0};
+    if constexpr (SAVED) {
+        const R* o = w.fsv + (long)(GAM_FSV_NC * D) * fs + c;
+        for (int v = 0; v < 5; v++) {
+            WL[v] = o[v * fs];
+            WR[v] = o[(5 + v) * fs];
+            dW[v] = o[(17 + v) * fs];
+        }
+        for (int x = 0; x < 3; x++) {
+            MagL[x] = o[(10 + x) * fs];
+            MagR[x] = o[(13 + x) * fs];
+        }
+        VaD = o[16 * fs];
+    } else {
+        // forward states; the stencils are loaded again for the reverse of
+        // the reconstruction rather than kept live (fewer registers, more warps)
+        const Quot<R> qVi(Vi);  // the 8 reconstructions share the divisor
+        for (int v = 0; v < 5; v++) {
+            R qW[8], nW[4];
+            for (int n = 0; n < 8; n++) qW[n] = w.QW[v * fs + c + (n - 4) * s];
+            for (int m = 0; m < 4; m++) nW[m] = w.Wn[v * fs + c + (m - 2) * s];
+            lrs_from_qdv(P, qW, nW, qVi, WL[v], WR[v]);
+        }
+        if (P.doMHD) {
+            for (int x = 0; x < 3; x++) {
+                R qB[8], nB[4];
+                for (int n = 0; n < 8; n++) qB[n] = w.QB[x * fs + c + (n - 4) * s];
+                for (int m = 0; m < 4; m++) nB[m] = Blim[x * fs + c + (m - 2) * s];
+                lrs_from_qdv(P, qB, nB, qVi, MagL[x], MagR[x]);
+            }
+            R mFs[3] = {(R)0, (R)0, (R)0}, bbD = (R)0;
+            mag_kin_flux(P, (R)-1, WL, MagL, Bn, T, B0, B0n, mFs, bbD, VaD);
+            mag_kin_flux(P, (R)1, WR, MagR, Bn, T, B0, B0n, mFs, bbD, VaD);
+        }
+        R gFs[5] = {(R)0, (R)0, (R)0, (R)0, (R)0};
+        gas_kin_flux(P, (R)-1, WL, T, gFs, dW);
+        gas_kin_flux(P, (R)1, WR, T, gFs, dW);
     }
-    R gFs[5] = {(R)0, (R)0, (R)0, (R)0, (R)0}, dW[5] = {(R)0, (R)0, (R)0, (R)0, (R)0};
-    gas_kin_flux(P, (R)-1, WL, T, gFs, dW);
-    gas_kin_flux(P, (R)1, WR, T, gFs, dW);
     // reverse of the outputs gF = fa (gFs - cHogH VaD dW), mF = fa mFs
     // in the form's precision (A = R): FP64 for the drop-in, FP32 for the FP32 form
     using A = R;
@@ -433,8 +448,9 @@ __device__ void edge_lrs_adj(const GamBox& b, const DevParams<R>& P, const Geo<R
 // atomics, or, with es, the edge's own adjoints stored per edge (14
 // components: 0-4 and 5-9 the scale and limiter adjoints of the EdgeLRs of
 // dT1 and dT2 faces, 10-12 the velocity adjoint aVC, 13 the corner density's)
-// for a gather in a fixed order
-template <class R>
+// for a gather in a fixed order. SAVED: the corner values come from w.esv
+// (stored by the forward) instead of being recomputed.
+template <class R, bool SAVED = false>
 __global__ void __launch_bounds__(128, 6) k_vxb_adj(GamBox b, DevParams<R> P, Geo<R> g, Work<R> w, int eD, Range r,
                                                  double dt, const R* __restrict__ dE, R* dDh, R* dabh, R* dbn,
                                                  R* dAVf, R* __restrict__ es) {
@@ -446,20 +462,32 @@ __global__ void __launch_bounds__(128, 6) k_vxb_adj(GamBox b, DevParams<R> P, Ge
     const long c = lidx(b, ii, jj, kk);
     const int e1 = eD == 0 ? 1 : 0, e2 = eD == 2 ? 1 : 2;
     const long s1 = dstride(b, e1), s2 = dstride(b, e2);
-    // forward recompute (k_vxb)
-    const R Dc = (R)0.25 * (w.Dh[c] + w.Dh[c - s1] + w.Dh[c - s2] + w.Dh[c - s1 - s2]);
-    R area1[8], area2[8];
-    R bT1L, bT1R, fA1, bT2L, bT2R, fA2;
-    edge_lrs(b, P, g, w, c, dT1, dT2, area1, bT1L, bT1R, fA1);
-    edge_lrs(b, P, g, w, c, dT2, dT1, area2, bT2L, bT2R, fA2);
-    const R dA = rmax(fA1, (R)TINY);
-    R VC[3];
+    // forward recompute (k_vxb), or its saved corner values
+    R Dc, bT1L, bT1R, fA1, bT2L, bT2R, fA2, VC[3];
     const long s2v = dstride(b, dT2);
-    for (int x = 0; x < 3; x++) {
-        R acc = (R)0;
-        for (int n = 0; n < 8; n++) acc += Rc<R>(w8(n)) * w.AVf[(x + 3 * eD) * fs + c + (n - 4) * s2v];
-        VC[x] = acc / dA;
+    if constexpr (SAVED) {
+        const R* o = w.esv + (long)(GAM_ESV_NC * eD) * fs + c;
+        Dc = o[0];
+        bT1L = o[fs];
+        bT1R = o[2 * fs];
+        fA1 = o[3 * fs];
+        bT2L = o[4 * fs];
+        bT2R = o[5 * fs];
+        fA2 = o[6 * fs];
+        for (int x = 0; x < 3; x++) VC[x] = o[(7 + x) * fs];
+    } else {
+        Dc = (R)0.25 * (w.Dh[c] + w.Dh[c - s1] + w.Dh[c - s2] + w.Dh[c - s1 - s2]);
+        R area1[8], area2[8];
+        edge_lrs(b, P, g, w, c, dT1, dT2, area1, bT1L, bT1R, fA1);
+        edge_lrs(b, P, g, w, c, dT2, dT1, area2, bT2L, bT2R, fA2);
+        const R dA0 = rmax(fA1, (R)TINY);
+        for (int x = 0; x < 3; x++) {
+            R acc = (R)0;
+            for (int n = 0; n < 8; n++) acc += Rc<R>(w8(n)) * w.AVf[(x + 3 * eD) * fs + c + (n - 4) * s2v];
+            VC[x] = acc / dA0;
+        }
     }
+    const R dA = rmax(fA1, (R)TINY);
     const R* Te = g.Te;
     R T1[3], T2[3];
     for (int x = 0; x < 3; x++) {
@@ -1411,7 +1439,7 @@ template <class R>
 int flux_call(const gam_params* p, const void* QW, const void* Wn, const void* QB, const void* Blim, const void* Bnf,
               const void* vol, const void* face, const void* Tf, const double* fcB0, const double* bFlux0, void* gF,
               void* mF, const void* dgF, const void* dmF, void* dQW, void* dWn, void* dQB, void* dBlim, void* dBnf,
-              cudaStream_t s, void* rscratch = nullptr) {
+              cudaStream_t s, void* rscratch = nullptr, void* fstates = nullptr) {
     using namespace gam_adj;
     const GamBox b = torch_box(p->Nip, p->Njp, p->Nkp);
     const DevParams<R> P = dev_params<R>(p);
@@ -1422,6 +1450,7 @@ int flux_call(const gam_params* p, const void* QW, const void* Wn, const void* Q
     Work<R> w;
     memset(&w, 0, sizeof(w));
     w.QW = (R*)QW; w.Wn = (R*)Wn; w.QB = (R*)QB; w.Bnf = (R*)Bnf; w.gF = (R*)gF; w.mF = (R*)mF;
+    w.fsv = (R*)fstates;  // non-null: the forward stores the face states, the adjoint loads them
     GamScalars* sc = nullptr;
     if (cudaGetSymbolAddress((void**)&sc, g_adj_scalars) != cudaSuccess) return GAM_ECUDA;
     const int G = GAM_NG;
@@ -1434,10 +1463,32 @@ int flux_call(const gam_params* p, const void* QW, const void* Wn, const void* Q
                     (unsigned)((r.k1 - r.k0 + 1 + blk.z - 1) / blk.z));
     };
     const R* Bl = (const R*)Blim;
-    if (!dgF) {
+    if (!dgF && fstates) {
+        k_stress<R, 0, 1, false, true><<<grid(fr[0]), blk, 0, s>>>(b, P, g, Bl, w, fr[0], sc, nullptr, nullptr);
+        k_stress<R, 1, 1, false, true><<<grid(fr[1]), blk, 0, s>>>(b, P, g, Bl, w, fr[1], sc, nullptr, nullptr);
+        k_stress<R, 2, 1, false, true><<<grid(fr[2]), blk, 0, s>>>(b, P, g, Bl, w, fr[2], sc, nullptr, nullptr);
+    } else if (!dgF) {
         k_stress<R, 0, 1><<<grid(fr[0]), blk, 0, s>>>(b, P, g, Bl, w, fr[0], sc, nullptr, nullptr);
         k_stress<R, 1, 1><<<grid(fr[1]), blk, 0, s>>>(b, P, g, Bl, w, fr[1], sc, nullptr, nullptr);
         k_stress<R, 2, 1><<<grid(fr[2]), blk, 0, s>>>(b, P, g, Bl, w, fr[2], sc, nullptr, nullptr);
+    } else if (fstates) {
+        R* rs = (R*)rscratch;
+        const long fs40 = 40L * b.fs;
+        const R* a = (const R*)dgF;
+        const R* m = (const R*)dmF;
+        k_stress_adj<R, 0, true><<<grid(fr[0]), blk, 0, s>>>(b, P, g, Bl, w, fr[0], a, m, (R*)dQW, (R*)dWn, (R*)dQB,
+                                                              (R*)dBlim, (R*)dBnf, rs);
+        k_stress_adj<R, 1, true><<<grid(fr[1]), blk, 0, s>>>(b, P, g, Bl, w, fr[1], a, m, (R*)dQW, (R*)dWn, (R*)dQB,
+                                                              (R*)dBlim, (R*)dBnf, rs ? rs + fs40 : nullptr);
+        k_stress_adj<R, 2, true><<<grid(fr[2]), blk, 0, s>>>(b, P, g, Bl, w, fr[2], a, m, (R*)dQW, (R*)dWn, (R*)dQB,
+                                                              (R*)dBlim, (R*)dBnf, rs ? rs + 2 * fs40 : nullptr);
+        if (rs) {
+            const dim3 gblk(32, 8, 1);
+            const dim3 ggrid((unsigned)((b.Ni + gblk.x - 1) / gblk.x), (unsigned)((b.Nj + gblk.y - 1) / gblk.y),
+                             (unsigned)b.Nk);
+            k_stress_adj_gather3<R><<<ggrid, gblk, 0, s>>>(b, fr[0], fr[1], fr[2], rs, p->doMHD ? 8 : 5, (R*)dQW,
+                                                           (R*)dWn, (R*)dQB, (R*)dBlim);
+        }
     } else {
         const R* a = (const R*)dgF;
         const R* m = (const R*)dmF;
@@ -1510,7 +1561,7 @@ template <class R>
 int efield_call(const gam_params* p, const void* Dh, const void* abh, const void* bn, const void* VdV, const void* vol,
                 const void* face, const void* edge, const void* Te, const void* Teb, const double* edgB0, double dt,
                 void* AVf, void* E, const void* dE, void* dDh, void* dabh, void* dbn, void* dVdV, void* dAVf,
-                cudaStream_t s, bool avf_saved = false, void* escratch = nullptr) {
+                cudaStream_t s, bool avf_saved = false, void* escratch = nullptr, void* estates = nullptr) {
     using namespace gam_adj;
     const GamBox b = torch_box(p->Nip, p->Njp, p->Nkp);
     const DevParams<R> P = dev_params<R>(p);
@@ -1521,6 +1572,7 @@ int efield_call(const gam_params* p, const void* Dh, const void* abh, const void
     Work<R> w;
     memset(&w, 0, sizeof(w));
     w.Dh = (R*)Dh; w.abh = (R*)abh; w.bn = (R*)bn; w.VdV = (R*)VdV; w.AVf = (R*)AVf; w.E = (R*)E;
+    w.esv = (R*)estates;  // non-null: the forward stores the corner values, the adjoint loads them
     GamScalars* sc = nullptr;
     if (cudaGetSymbolAddress((void**)&sc, g_adj_scalars) != cudaSuccess) return GAM_ECUDA;
     k_adj_scalars<<<1, 1, 0, s>>>(sc, dt, 0.0, 0.0, 0);
@@ -1539,13 +1591,20 @@ int efield_call(const gam_params* p, const void* Dh, const void* abh, const void
     for (int eD = 0; eD < 3; eD++) {
         // the adjoint of a whole step finds AVf as its forward left it
         if (!(dE && avf_saved)) k_mom2face<R><<<grid(mf[eD]), blk, 0, s>>>(b, P, g, w, eD, mf[eD], sc);
-        if (!dE) {
+        if (!dE && estates) {
+            k_vxb<R, 1, true><<<grid(ed[eD]), blk, 0, s>>>(b, P, g, w, eD, ed[eD], sc);
+        } else if (!dE) {
             k_vxb<R><<<grid(ed[eD]), blk, 0, s>>>(b, P, g, w, eD, ed[eD], sc);
         } else if (escratch) {
             // deterministic: the edges store their adjoints (14 components
             // from escratch + 14 eD fs), gathered per position after the third
-            k_vxb_adj<R><<<grid(ed[eD]), blk, 0, s>>>(b, P, g, w, eD, ed[eD], dt, (const R*)dE, (R*)dDh, (R*)dabh,
-                                                       (R*)dbn, (R*)dAVf, (R*)escratch + 14L * eD * b.fs);
+            if (estates)
+                k_vxb_adj<R, true><<<grid(ed[eD]), blk, 0, s>>>(b, P, g, w, eD, ed[eD], dt, (const R*)dE, (R*)dDh,
+                                                                 (R*)dabh, (R*)dbn, (R*)dAVf,
+                                                                 (R*)escratch + 14L * eD * b.fs);
+            else
+                k_vxb_adj<R><<<grid(ed[eD]), blk, 0, s>>>(b, P, g, w, eD, ed[eD], dt, (const R*)dE, (R*)dDh,
+                                                           (R*)dabh, (R*)dbn, (R*)dAVf, (R*)escratch + 14L * eD * b.fs);
             if (eD == 2) {
                 R* es = (R*)escratch;
                 R* aS = es + 42L * b.fs;  // the scaled dAVf of the three edge directions
@@ -1730,28 +1789,61 @@ int gam_update_adjoint_store(const gam_params* p, int32_t fp32, const void* cons
 int gam_efield_adjoint_saved(const gam_params* p, int32_t fp32, const void* Dh, const void* abh, const void* bn,
                              const void* VdV, const void* volume, const void* face, const void* edge, const void* Te,
                              const void* Teb, const double* edgB0, double dt, void* AVf, const void* dE, void* dDh,
-                             void* dabh, void* dbn, void* dVdV, void* dAVf, void* scratch, void* stream) {
+                             void* dabh, void* dbn, void* dVdV, void* dAVf, void* scratch, const void* estates,
+                             void* stream) {
     int rc = check(p, fp32);
     if (rc) return rc;
-    if (!scratch) return GAM_EINVAL;
+    if (!scratch || !estates) return GAM_EINVAL;
     cudaStream_t s = (cudaStream_t)stream;
+    void* esv = const_cast<void*>(estates);
     return fp32 ? efield_call<float>(p, Dh, abh, bn, VdV, volume, face, edge, Te, Teb, edgB0, dt, AVf, nullptr, dE,
-                                     dDh, dabh, dbn, dVdV, dAVf, s, true, scratch)
+                                     dDh, dabh, dbn, dVdV, dAVf, s, true, scratch, esv)
                 : efield_call<double>(p, Dh, abh, bn, VdV, volume, face, edge, Te, Teb, edgB0, dt, AVf, nullptr, dE,
-                                      dDh, dabh, dbn, dVdV, dAVf, s, true, scratch);
+                                      dDh, dabh, dbn, dVdV, dAVf, s, true, scratch, esv);
+}
+// CalcElecField into AVf, E that also stores the corner values (GAM_ESV_NC
+// per edge and direction) for gam_efield_adjoint_saved
+int gam_efield_forward_save(const gam_params* p, int32_t fp32, const void* Dh, const void* abh, const void* bn,
+                            const void* VdV, const void* volume, const void* face, const void* edge, const void* Te,
+                            const void* Teb, const double* edgB0, double dt, void* AVf, void* E, void* estates,
+                            void* stream) {
+    int rc = check(p, fp32);
+    if (rc) return rc;
+    if (!AVf || !E || !estates || !(dt > 0.0)) return GAM_EINVAL;
+    cudaStream_t s = (cudaStream_t)stream;
+    return fp32 ? efield_call<float>(p, Dh, abh, bn, VdV, volume, face, edge, Te, Teb, edgB0, dt, AVf, E, nullptr,
+                                     nullptr, nullptr, nullptr, nullptr, nullptr, s, false, nullptr, estates)
+                : efield_call<double>(p, Dh, abh, bn, VdV, volume, face, edge, Te, Teb, edgB0, dt, AVf, E, nullptr,
+                                      nullptr, nullptr, nullptr, nullptr, nullptr, s, false, nullptr, estates);
 }
 int gam_flux_adjoint_gather(const gam_params* p, int32_t fp32, const void* QW, const void* Wn, const void* QB,
                             const void* Blim, const void* Bnf, const void* volume, const void* face, const void* Tf,
                             const double* fcB0, const double* bFlux0, const void* dgF, const void* dmF, void* dQW,
-                            void* dWn, void* dQB, void* dBlim, void* dBnf, void* scratch, void* stream) {
+                            void* dWn, void* dQB, void* dBlim, void* dBnf, void* scratch, const void* fstates,
+                            void* stream) {
     int rc = check(p, fp32);
     if (rc) return rc;
-    if (!scratch) return GAM_EINVAL;
+    if (!scratch || !fstates) return GAM_EINVAL;
     cudaStream_t s = (cudaStream_t)stream;
+    void* fsv = const_cast<void*>(fstates);
     return fp32 ? flux_call<float>(p, QW, Wn, QB, Blim, Bnf, volume, face, Tf, fcB0, bFlux0, nullptr, nullptr, dgF,
-                                   dmF, dQW, dWn, dQB, dBlim, dBnf, s, scratch)
+                                   dmF, dQW, dWn, dQB, dBlim, dBnf, s, scratch, fsv)
                 : flux_call<double>(p, QW, Wn, QB, Blim, Bnf, volume, face, Tf, fcB0, bFlux0, nullptr, nullptr, dgF,
-                                    dmF, dQW, dWn, dQB, dBlim, dBnf, s, scratch);
+                                    dmF, dQW, dWn, dQB, dBlim, dBnf, s, scratch, fsv);
+}
+// CalcStress into gF, mF that also stores the face states (GAM_FSV_NC per
+// face and direction) for gam_flux_adjoint_gather
+int gam_flux_forward_save(const gam_params* p, int32_t fp32, const void* QW, const void* Wn, const void* QB,
+                          const void* Blim, const void* Bnf, const void* volume, const void* face, const void* Tf,
+                          const double* fcB0, const double* bFlux0, void* gF, void* mF, void* fstates, void* stream) {
+    int rc = check(p, fp32);
+    if (rc) return rc;
+    if (!gF || !mF || !fstates) return GAM_EINVAL;
+    cudaStream_t s = (cudaStream_t)stream;
+    return fp32 ? flux_call<float>(p, QW, Wn, QB, Blim, Bnf, volume, face, Tf, fcB0, bFlux0, gF, mF, nullptr, nullptr,
+                                   nullptr, nullptr, nullptr, nullptr, nullptr, s, nullptr, fstates)
+                : flux_call<double>(p, QW, Wn, QB, Blim, Bnf, volume, face, Tf, fcB0, bFlux0, gF, mF, nullptr, nullptr,
+                                    nullptr, nullptr, nullptr, nullptr, nullptr, s, nullptr, fstates);
 }
 
 // ------------------------------------------------------------ I-side boundaries (C ABI)

@@ -644,8 +644,9 @@ __device__ __forceinline__ void edge_lrs(const GamBox& b, const DevParams<R>& P,
     bR = bR * fA;
 }
 
-// VxB edge loop for direction eD (fields.F90:184-228).
-template <class R, int MINB = 1>
+// VxB edge loop for direction eD (fields.F90:184-228). SAVE (the
+// differentiation form's forward) also stores the corner values in w.esv.
+template <class R, int MINB = 1, bool SAVE = false>
 __global__ void __launch_bounds__(128, MINB) k_vxb(GamBox b, DevParams<R> P, Geo<R> g, Work<R> w, int eD, Range r,
                                              const GamScalars* sc) {
     if (sc->halted) return;
@@ -707,6 +708,18 @@ __global__ void __launch_bounds__(128, MINB) k_vxb(GamBox b, DevParams<R> P, Geo
     vDiff = rmin(vDiff, P.CFL * edge / (R)sc->dt);
     R e = -(v1 * b2 - v2 * b1) + P.Vd0 * vDiff * Jd;
     w.E[eD * fs + c] = e * edge;
+    if constexpr (SAVE) {
+        R* o = w.esv + (long)(GAM_ESV_NC * eD) * fs + c;
+        o[0] = Dc;
+        o[fs] = bT1L;
+        o[2 * fs] = bT1R;
+        o[3 * fs] = fA1;
+        o[4 * fs] = bT2L;
+        o[5 * fs] = bT2R;
+        o[6 * fs] = fA2;
+#pragma unroll
+        for (int x = 0; x < 3; x++) o[(7 + x) * fs] = VC[x];
+    }
 }
 
 // One-sided Gaussian-moment fluxes for one side q (sgn = -1 LEFT, +1 RIGHT).
@@ -794,8 +807,9 @@ __device__ __forceinline__ void gas_kin_flux(const DevParams<R>& P, R sgn, const
 // Face fluxes of direction D (Fluxes, stress.F90:204-429), one face per
 // thread. The stencil operands are the per-cell products volume*primitive and
 // volume*B of the half state (QdV of Cen8LRs) and the limiter values, read
-// along D through L1; MINB bounds the registers for occupancy.
-template <class R, int D, int MINB, bool BORIS = false>
+// along D through L1; MINB bounds the registers for occupancy. SAVE (the
+// differentiation form's forward) also stores the face states in w.fsv.
+template <class R, int D, int MINB, bool BORIS = false, bool SAVE = false>
 __global__ void __launch_bounds__(128, MINB) k_stress(GamBox b, DevParams<R> P, Geo<R> g, const R* __restrict__ Blim,
                                                       Work<R> w, Range r, const GamScalars* sc,
                                                       const R* __restrict__ gasN, const R* __restrict__ gasO) {
@@ -905,6 +919,21 @@ __global__ void __launch_bounds__(128, MINB) k_stress(GamBox b, DevParams<R> P, 
     }
 #pragma unroll
     for (int v = 0; v < 5; v++) w.gF[(v + 5 * D) * fs + c] = fa * gv[v];
+    if constexpr (SAVE) {
+        R* o = w.fsv + (long)(GAM_FSV_NC * D) * fs + c;
+#pragma unroll
+        for (int v = 0; v < 5; v++) {
+            o[v * fs] = WL[v];
+            o[(5 + v) * fs] = WR[v];
+            o[(17 + v) * fs] = dW[v];
+        }
+#pragma unroll
+        for (int x = 0; x < 3; x++) {
+            o[(10 + x) * fs] = MagL[x];
+            o[(13 + x) * fs] = MagR[x];
+        }
+        o[16 * fs] = VaD;
+    }
 }
 
 // E2Flux into the new buffer; faces outside its range are copied. With

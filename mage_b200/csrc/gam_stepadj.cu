@@ -36,11 +36,20 @@ int gam_update_adjoint_store(const gam_params* p, int32_t fp32, const void* cons
 int gam_efield_adjoint_saved(const gam_params* p, int32_t fp32, const void* Dh, const void* abh, const void* bn,
                              const void* VdV, const void* volume, const void* face, const void* edge, const void* Te,
                              const void* Teb, const double* edgB0, double dt, void* AVf, const void* dE, void* dDh,
-                             void* dabh, void* dbn, void* dVdV, void* dAVf, void* scratch, void* stream);
+                             void* dabh, void* dbn, void* dVdV, void* dAVf, void* scratch, const void* estates,
+                             void* stream);
+int gam_efield_forward_save(const gam_params* p, int32_t fp32, const void* Dh, const void* abh, const void* bn,
+                            const void* VdV, const void* volume, const void* face, const void* edge, const void* Te,
+                            const void* Teb, const double* edgB0, double dt, void* AVf, void* E, void* estates,
+                            void* stream);
 int gam_flux_adjoint_gather(const gam_params* p, int32_t fp32, const void* QW, const void* Wn, const void* QB,
                             const void* Blim, const void* Bnf, const void* volume, const void* face, const void* Tf,
                             const double* fcB0, const double* bFlux0, const void* dgF, const void* dmF, void* dQW,
-                            void* dWn, void* dQB, void* dBlim, void* dBnf, void* scratch, void* stream);
+                            void* dWn, void* dQB, void* dBlim, void* dBnf, void* scratch, const void* fstates,
+                            void* stream);
+int gam_flux_forward_save(const gam_params* p, int32_t fp32, const void* QW, const void* Wn, const void* QB,
+                          const void* Blim, const void* Bnf, const void* volume, const void* face, const void* Tf,
+                          const double* fcB0, const double* bFlux0, void* gF, void* mF, void* fstates, void* stream);
 
 namespace gam_stepadj {
 
@@ -245,6 +254,8 @@ unsigned blocks(long n, int blk) { return (unsigned)((n + blk - 1) / blk); }
 // work arrays, each of nc components; a start on 64 elements
 enum Slot {
     QW, Wn, Dh, VdV, QB, abh, Bnf, bn, AVf, E, Blim, gF, mF,                                      // forward
+    FSV, ESV,  // the flux kernels' face states and the edge kernels' corner values per direction
+               // (written before they are read: not zeroed)
     dQW, dWn, dDh, dVdV, dQB, dabh, dBnf, dbn, dAVf, dE, dgF, dmF, dBlim, sU, sM, aB, dnG, dnM, tM,  // adjoint
     RS,  // scratch of the deterministic gathers: the flux adjoint's per-face reconstruction adjoints
          // (3 directions x 8 variables x 5), then the edge adjoints (3 x 14) and the scaled dAVf (3 x 3)
@@ -252,7 +263,7 @@ enum Slot {
                       // fluxes before them, and that field's adjoint
     NSLOT
 };
-constexpr int slot_nc[NSLOT] = {5, 5, 1, 3, 3, 3, 3, 3, 9, 3, 3, 15, 9,
+constexpr int slot_nc[NSLOT] = {5, 5, 1, 3, 3, 3, 3, 3, 9, 3, 3, 15, 9, 66, 30,  // 3 x GAM_FSV_NC, 3 x GAM_ESV_NC
                                 5, 5, 1, 3, 3, 3, 3, 3, 3, 3, 15, 9, 3, 5, 3, 3, 5, 3, 3, 120,
                                 5, 3, 3, 3};
 bool has_iside(const gam_params* p) { return p->bc[0] != GAM_BC_PERIODIC; }
@@ -266,7 +277,7 @@ Work layout(const Box& b, int fp32, void* base, bool iside) {
     Work w;
     size_t off = 0;
     for (int s = 0; s < NSLOT; s++) {
-        if (s == dQW) w.fwd_bytes = off;
+        if (s == FSV) w.fwd_bytes = off;
         w.p[s] = base ? (void*)((char*)base + off) : nullptr;
         const size_t bytes = (s >= UG && !iside) ? 0 : (size_t)slot_nc[s] * (size_t)b.n * es;
         off += (bytes + 255) / 256 * 256;
@@ -353,10 +364,10 @@ int forward_stages(const gam_params* p, int fp32, const Box& b, const Work& w, c
     void* out8[8] = {w.p[QW], w.p[Wn], w.p[Dh], w.p[VdV], w.p[QB], w.p[abh], w.p[Bnf], w.p[bn]};
     TRY(gam_predict_stage(p, fp32, st, g5, 0.5 * dt, odt, out8, nullptr, nullptr, nullptr, s));
     TRY(fp32 ? launch_bxyz<float>(b, geo, st[1], w.p[Blim], s) : launch_bxyz<double>(b, geo, st[1], w.p[Blim], s));
-    TRY(gam_efield_forward(p, fp32, w.p[Dh], w.p[abh], w.p[bn], w.p[VdV], geo[0], geo[1], geo[5], geo[6], geo[7],
-                           bg ? bg[2] : nullptr, dt, w.p[AVf], w.p[E], s));
-    TRY(gam_flux_forward(p, fp32, w.p[QW], w.p[Wn], w.p[QB], w.p[Blim], w.p[Bnf], geo[0], geo[1], geo[8],
-                         bg ? bg[0] : nullptr, bg ? bg[1] : nullptr, w.p[gF], w.p[mF], s));
+    TRY(gam_efield_forward_save(p, fp32, w.p[Dh], w.p[abh], w.p[bn], w.p[VdV], geo[0], geo[1], geo[5], geo[6],
+                                geo[7], bg ? bg[2] : nullptr, dt, w.p[AVf], w.p[E], w.p[ESV], s));
+    TRY(gam_flux_forward_save(p, fp32, w.p[QW], w.p[Wn], w.p[QB], w.p[Blim], w.p[Bnf], geo[0], geo[1], geo[8],
+                              bg ? bg[0] : nullptr, bg ? bg[1] : nullptr, w.p[gF], w.p[mF], w.p[FSV], s));
     return GAM_OK;
 }
 
@@ -508,10 +519,10 @@ int step_adj(const gam_params* p, int32_t fp32, const void* const* geo, const do
     // in a fixed order: the same bits on every call
     TRY(gam_flux_adjoint_gather(p, fp32, w.p[QW], w.p[Wn], w.p[QB], w.p[Blim], w.p[Bnf], geo[0], geo[1], geo[8],
                                 bg ? bg[0] : nullptr, bg ? bg[1] : nullptr, w.p[dgF], w.p[dmF], w.p[dQW], w.p[dWn],
-                                w.p[dQB], w.p[dBlim], w.p[dBnf], w.p[RS], s));
+                                w.p[dQB], w.p[dBlim], w.p[dBnf], w.p[RS], w.p[FSV], s));
     TRY(gam_efield_adjoint_saved(p, fp32, w.p[Dh], w.p[abh], w.p[bn], w.p[VdV], geo[0], geo[1], geo[5], geo[6],
                                  geo[7], bg ? bg[2] : nullptr, dt, w.p[AVf], w.p[dE], w.p[dDh], w.p[dabh], w.p[dbn],
-                                 w.p[dVdV], w.p[dAVf], w.p[RS], s));
+                                 w.p[dVdV], w.p[dAVf], w.p[RS], w.p[ESV], s));
     TRY(fp32 ? launch_bxyz_adj<float>(b, geo, w.p[dBlim], dst[1], s)
              : launch_bxyz_adj<double>(b, geo, w.p[dBlim], dst[1], s));
     const void* g5[5] = {geo[0], geo[1], geo[2], geo[3], geo[4]};

@@ -117,7 +117,16 @@ template <class R> struct Work {
     R* E;    // edge, 3
     R* gF;   // face, 15: gas flux v + 5*d (already times face area)
     R* mF;   // face, 9: magnetic flux x + 3*d
+    // differentiation form only (null in the step): the flux kernels' face
+    // states, 22 per face and direction, q + 22*d: WL, WR (5 each), MagL,
+    // MagR (3 each), VaD and the diffusion sums dW (5)
+    R* fsv;
+    // differentiation form only: the edge kernels' corner values, 10 per
+    // edge and direction, q + 10*eD: Dc, bT1L, bT1R, fA1, bT2L, bT2R, fA2, VC (3)
+    R* esv;
 };
+constexpr int GAM_FSV_NC = 22;
+constexpr int GAM_ESV_NC = 10;
 
 struct Range {  // inclusive box-index range
     int i0, i1, j0, j1, k0, k1;
