@@ -519,8 +519,13 @@ int gam_iside_adjoint(const gam_params* p, int32_t fp32, const void* const* geo,
  * (dB may be NULL); saved = 1 reuses the intermediates that gam_step_fwd_save
  * left in work for the same st, saved = 0 recomputes them first. The adjoint
  * sums every stencil's contributions in a fixed order (no atomics), so equal
- * inputs give equal bits on every call. Enqueued on stream; GAM_EINVAL for
- * other boundaries, Boris, AB3, 7UP or 2.5-D.
+ * inputs give equal bits on every call. Enqueued on stream (the adjoint forks
+ * independent stages onto the library's own side streams of the device and
+ * joins them back before it returns, so the work stays ordered on stream and
+ * may be captured into a CUDA graph from it); the stage and whole-step calls
+ * of this form share device-global scratch scalars, so issue them from one
+ * host thread per device. GAM_EINVAL for other boundaries, Boris, AB3, 7UP
+ * or 2.5-D.
  * No counterpart in the reference, which has no adjoint. */
 int gam_step_work_bytes(const gam_params* p, int32_t fp32, int64_t* bytes);
 int gam_step_fwd_save(const gam_params* p, int32_t fp32, const void* const* geo, const double* const* bg,

@@ -22,6 +22,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <mutex>
 #include <stdint.h>
 #include <string.h>
 
@@ -251,6 +252,47 @@ __global__ void k_box_bxyz_adj(Box b, const R* __restrict__ vol, const R* __rest
 
 unsigned blocks(long n, int blk) { return (unsigned)((n + blk - 1) / blk); }
 
+// Side streams of the adjoint step (created once per device, non-blocking):
+// independent stages run on them between a fork and a join by events, on
+// the caller's stream or inside a graph captured from it.
+constexpr int NSIDE = 2;
+struct SideStreams {
+    cudaStream_t s[NSIDE];
+    cudaEvent_t fork, join[NSIDE];
+    bool ok;
+};
+SideStreams* side_streams() {
+    static std::mutex mu;
+    static SideStreams per[64];
+    static bool made[64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    std::lock_guard<std::mutex> lock(mu);
+    SideStreams& t = per[dev];
+    if (!made[dev]) {
+        made[dev] = true;
+        t.ok = cudaEventCreateWithFlags(&t.fork, cudaEventDisableTiming) == cudaSuccess;
+        for (int i = 0; i < NSIDE && t.ok; i++)
+            t.ok = cudaStreamCreateWithFlags(&t.s[i], cudaStreamNonBlocking) == cudaSuccess &&
+                   cudaEventCreateWithFlags(&t.join[i], cudaEventDisableTiming) == cudaSuccess;
+    }
+    return t.ok ? &t : nullptr;
+}
+// the side streams i < n wait for the work issued so far on s
+int fork(const SideStreams* t, int n, cudaStream_t s) {
+    if (cudaEventRecord(t->fork, s) != cudaSuccess) return GAM_ECUDA;
+    for (int i = 0; i < n; i++)
+        if (cudaStreamWaitEvent(t->s[i], t->fork, 0) != cudaSuccess) return GAM_ECUDA;
+    return GAM_OK;
+}
+// s waits for the work issued so far on the side streams i < n
+int join(const SideStreams* t, int n, cudaStream_t s) {
+    for (int i = 0; i < n; i++)
+        if (cudaEventRecord(t->join[i], t->s[i]) != cudaSuccess || cudaStreamWaitEvent(s, t->join[i], 0) != cudaSuccess)
+            return GAM_ECUDA;
+    return GAM_OK;
+}
+
 // work arrays, each of nc components; a start on 64 elements
 enum Slot {
     QW, Wn, Dh, VdV, QB, abh, Bnf, bn, AVf, E, Blim, gF, mF,                                      // forward
@@ -258,13 +300,14 @@ enum Slot {
                // (written before they are read: not zeroed)
     dQW, dWn, dDh, dVdV, dQB, dabh, dBnf, dbn, dAVf, dE, dgF, dmF, dBlim, sU, sM, aB, dnG, dnM, tM,  // adjoint
     RS,  // scratch of the deterministic gathers: the flux adjoint's per-face reconstruction adjoints
-         // (3 directions x 8 variables x 5), then the edge adjoints (3 x 14) and the scaled dAVf (3 x 3)
+         // (3 directions x 8 variables x 5), after them the edge adjoints (3 x 14) and the scaled dAVf
+         // (3 x 3), apart so that the two adjoints run at the same time
     UG, UM, UB, aBm,  // non-periodic I only: the update's result after the I-side fills, the field of its
                       // fluxes before them, and that field's adjoint
     NSLOT
 };
 constexpr int slot_nc[NSLOT] = {5, 5, 1, 3, 3, 3, 3, 3, 9, 3, 3, 15, 9, 66, 30,  // 3 x GAM_FSV_NC, 3 x GAM_ESV_NC
-                                5, 5, 1, 3, 3, 3, 3, 3, 3, 3, 15, 9, 3, 5, 3, 3, 5, 3, 3, 120,
+                                5, 5, 1, 3, 3, 3, 3, 3, 3, 3, 15, 9, 3, 5, 3, 3, 5, 3, 3, 171,
                                 5, 3, 3, 3};
 bool has_iside(const gam_params* p) { return p->bc[0] != GAM_BC_PERIODIC; }
 
@@ -490,16 +533,20 @@ int step_adj(const gam_params* p, int32_t fp32, const void* const* geo, const do
     if (cudaMemcpyAsync(w.p[tM], dnxt[1], 3 * b.n * es, cudaMemcpyDeviceToDevice, s) != cudaSuccess) return GAM_ECUDA;
     if (dnxt[2]) TRY(fp32 ? launch_bxyz_adj<float>(b, geo, dnxt[2], w.p[tM], s)
                           : launch_bxyz_adj<double>(b, geo, dnxt[2], w.p[tM], s));
-    // adjoint of EnforceBCs
+    // adjoint of EnforceBCs: the gas on a side stream, the fluxes here
+    const SideStreams* side = side_streams();
+    cudaStream_t s0 = side ? side->s[0] : s, s1 = side ? side->s[1] : s;
+    if (side) TRY(fork(side, 1, s));
     if (fp32) {
-        TRY(launch_gather_adj<float>(b, -1, 5, dnxt[0], w.p[dnG], s));
+        TRY(launch_gather_adj<float>(b, -1, 5, dnxt[0], w.p[dnG], s0));
         for (int d = 0; d < 3; d++)
             TRY(launch_gather_adj<float>(b, d, 1, (float*)w.p[tM] + d * b.n, (float*)w.p[dnM] + d * b.n, s));
     } else {
-        TRY(launch_gather_adj<double>(b, -1, 5, dnxt[0], w.p[dnG], s));
+        TRY(launch_gather_adj<double>(b, -1, 5, dnxt[0], w.p[dnG], s0));
         for (int d = 0; d < 3; d++)
             TRY(launch_gather_adj<double>(b, d, 1, (double*)w.p[tM] + d * b.n, (double*)w.p[dnM] + d * b.n, s));
     }
+    if (side) TRY(join(side, 1, s));
     if (iside) {
         // the I-side fills (in place on dnG, dnM; the field they read gets
         // its adjoint in aBm), then bFlux2Fld of the update's fluxes
@@ -515,16 +562,21 @@ int step_adj(const gam_params* p, int32_t fp32, const void* const* geo, const do
     const void* dup[2] = {w.p[dnG], w.p[dnM]};
     void* dsu[5] = {dst[0], dst[1], w.p[dE], w.p[dgF], w.p[dmF]};
     TRY(gam_update_adjoint_store(p, fp32, in5, g4, bg ? bg[3] : nullptr, dt, dup, w.p[sU], w.p[sM], dsu, s));
-    // the flux and E-field adjoints gather their stencil adjoints through RS
-    // in a fixed order: the same bits on every call
+    // the flux and E-field adjoints gather their stencil adjoints through
+    // their own parts of RS in a fixed order (the same bits on every call);
+    // they read and write disjoint arrays, so the E-field adjoint runs on a
+    // side stream beside the flux adjoint and the bFlux2Fld adjoint after it
+    if (side) TRY(fork(side, 2, s));
+    const size_t rsE = (size_t)120 * b.n * es;  // the flux adjoint's 120 components come first
+    TRY(gam_efield_adjoint_saved(p, fp32, w.p[Dh], w.p[abh], w.p[bn], w.p[VdV], geo[0], geo[1], geo[5], geo[6],
+                                 geo[7], bg ? bg[2] : nullptr, dt, w.p[AVf], w.p[dE], w.p[dDh], w.p[dabh], w.p[dbn],
+                                 w.p[dVdV], w.p[dAVf], (char*)w.p[RS] + rsE, w.p[ESV], s1));
     TRY(gam_flux_adjoint_gather(p, fp32, w.p[QW], w.p[Wn], w.p[QB], w.p[Blim], w.p[Bnf], geo[0], geo[1], geo[8],
                                 bg ? bg[0] : nullptr, bg ? bg[1] : nullptr, w.p[dgF], w.p[dmF], w.p[dQW], w.p[dWn],
                                 w.p[dQB], w.p[dBlim], w.p[dBnf], w.p[RS], w.p[FSV], s));
-    TRY(gam_efield_adjoint_saved(p, fp32, w.p[Dh], w.p[abh], w.p[bn], w.p[VdV], geo[0], geo[1], geo[5], geo[6],
-                                 geo[7], bg ? bg[2] : nullptr, dt, w.p[AVf], w.p[dE], w.p[dDh], w.p[dabh], w.p[dbn],
-                                 w.p[dVdV], w.p[dAVf], w.p[RS], w.p[ESV], s));
     TRY(fp32 ? launch_bxyz_adj<float>(b, geo, w.p[dBlim], dst[1], s)
              : launch_bxyz_adj<double>(b, geo, w.p[dBlim], dst[1], s));
+    if (side) TRY(join(side, 2, s));
     const void* g5[5] = {geo[0], geo[1], geo[2], geo[3], geo[4]};
     const void* din8[8] = {w.p[dQW], w.p[dWn], w.p[dDh], w.p[dVdV], w.p[dQB], w.p[dabh], w.p[dBnf], w.p[dbn]};
     return gam_predict_stage(p, fp32, st, g5, 0.5 * dt, odt, nullptr, din8, w.p[aB], dst, s);
