@@ -522,7 +522,9 @@ int gam_iside_adjoint(const gam_params* p, int32_t fp32, const void* const* geo,
  * inputs give equal bits on every call. Enqueued on stream (the adjoint forks
  * independent stages onto the library's own side streams of the device and
  * joins them back before it returns, so the work stays ordered on stream and
- * may be captured into a CUDA graph from it); the stage and whole-step calls
+ * may be captured into a CUDA graph from it, once the first gam_step_adj call
+ * on the same grid configuration and device has uploaded the tables of its
+ * boundary-gather adjoint with synchronous copies); the stage and whole-step calls
  * of this form share device-global scratch scalars, so issue them from one
  * host thread per device. GAM_EINVAL for other boundaries, Boris, AB3, 7UP
  * or 2.5-D.

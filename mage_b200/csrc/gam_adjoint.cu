@@ -1575,7 +1575,9 @@ int efield_call(const gam_params* p, const void* Dh, const void* abh, const void
     w.esv = (R*)estates;  // non-null: the forward stores the corner values, the adjoint loads them
     GamScalars* sc = nullptr;
     if (cudaGetSymbolAddress((void**)&sc, g_adj_scalars) != cudaSuccess) return GAM_ECUDA;
-    k_adj_scalars<<<1, 1, 0, s>>>(sc, dt, 0.0, 0.0, 0);
+    // the forward kernels read dt from the scalars; the adjoint with AVf kept
+    // launches none of them
+    if (!(dE && avf_saved)) k_adj_scalars<<<1, 1, 0, s>>>(sc, dt, 0.0, 0.0, 0);
     const int G = GAM_NG;
     const Range mf[3] = {{0, b.Ni - 1, G, G + b.Njp, 0, b.Nk - 1},
                          {0, b.Ni - 1, 0, b.Nj - 1, G, G + b.Nkp},

@@ -1,7 +1,7 @@
 // Boundary-copy map of the whole-step kernels (gam_stepadj.cu): the box
 // geometry, the ghost rules of the periodic and zero-gradient boundaries
-// composed into one source index per box position, and the candidate
-// positions the adjoint of that gather scans. Host- and device-callable, so
+// composed into one source index per box position, and the tables of the
+// adjoint of that gather (host). Host- and device-callable, so
 // that the host test suite checks the map against the PyTorch restatement's
 // (mage_b200/diffstep.py, Grid._bc_maps) without a GPU.
 #pragma once
@@ -10,6 +10,8 @@
 #else
 #define GAM_HD
 #endif
+#include <vector>
+
 #include "../../include/gamgpu.h"
 
 namespace gam_stepadj {
@@ -76,40 +78,40 @@ GAM_HD inline bool pos_of(const Box& b, long t, int& i, int& j, int& k) {
     return true;
 }
 
-// candidate positions of one axis that the ghost rules can send to x, in
-// ascending order: x - nn, x, x + nn and, for zero-gradient sides, the ghost
-// layer of the side x is the edge of
-GAM_HD inline int axis_candidates(int x, int nn, int extent, bool zg_lo, bool zg_hi, int* out) {
-    int c[13], m = 0;
-    if (zg_lo && x == G)
-        for (int q = 0; q < G; q++) c[m++] = q;
-    c[m++] = x - nn;
-    c[m++] = x;
-    c[m++] = x + nn;
-    if (zg_hi && (x == G + nn - 1 || x == G + nn))
-        for (int q = 0; q <= G; q++) c[m++] = G + nn + q;
-    // insertion sort, keep the distinct in-range values
-    for (int a = 1; a < m; a++) {
-        const int v = c[a];
-        int q = a - 1;
-        while (q >= 0 && c[q] > v) {
-            c[q + 1] = c[q];
-            q--;
-        }
-        c[q + 1] = v;
+// The adjoint of the gather out[t] = in[src(t)] as tables, built on the host
+// once per configuration and field (comp as for bc_source): code[s] = (1 if
+// src(s) = s) + 2 (row + 1), row -1 where no other position copies s; the
+// rows, one per position s that others copy (s ascending), list those
+// positions t in ascending order (src from rowStart[row] to rowStart[row+1]).
+// The adjoint at s is then (in[s] if code bit 0) + the sum over its row in
+// that order: the same bits on every call.
+inline void bc_adj_tables(const Box& b, int comp, std::vector<int>& code, std::vector<int>& rowStart,
+                          std::vector<int>& src) {
+    const long n = b.n;
+    std::vector<int> from((size_t)n), cnt((size_t)n, 0), rowOf((size_t)n, -1);
+    for (long t = 0; t < n; t++) {
+        int i, j, k;
+        pos_of(b, t, i, j, k);
+        from[t] = (int)bc_source(b, comp, i, j, k);
+        if (from[t] != t) cnt[from[t]]++;
     }
-    int r = 0;
-    for (int a = 0; a < m; a++)
-        if (c[a] >= 0 && c[a] < extent && (r == 0 || out[r - 1] != c[a])) out[r++] = c[a];
-    return r;
-}
-
-// whether some other position may copy x along one axis: x lies within
-// Nactive of a ghost layer that the periodic rule fills from it, or is the
-// edge a zero-gradient side copies (a superset; the adjoint filters exactly)
-GAM_HD inline bool may_receive(int x, int nn, int extent, bool periodic, bool zlo, bool zhi) {
-    if (periodic) return (x - nn >= 0 && x - nn < G) || (x >= G && x + nn < extent);
-    return (zlo && x == G) || (zhi && (x == G + nn - 1 || x == G + nn));
+    code.assign((size_t)n, 0);
+    rowStart.assign(1, 0);
+    int rows = 0;
+    for (long s = 0; s < n; s++) {
+        if (cnt[s]) {
+            rowOf[s] = rows++;
+            rowStart.push_back(rowStart.back() + cnt[s]);
+        }
+        code[s] = (from[s] == s ? 1 : 0) + 2 * (rowOf[s] + 1);
+    }
+    src.assign((size_t)rowStart.back(), 0);
+    std::vector<int> fill((size_t)rows, 0);
+    for (long t = 0; t < n; t++)
+        if (from[t] != t) {
+            const int r = rowOf[from[t]];
+            src[rowStart[r] + fill[r]++] = (int)t;
+        }
 }
 
 }  // namespace gam_stepadj

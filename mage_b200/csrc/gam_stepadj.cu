@@ -64,104 +64,45 @@ __global__ void k_bc_gather(Box b, int comp, int nc, const R* __restrict__ in, R
     for (int c = 0; c < nc; c++) out[c * b.n + t] = in[c * b.n + s];
 }
 
-// adjoint of the gather: out[c][s] = (g[c][s] if src(s) = s, else 0) +
-// (sum over t != s with src(t) = s, ascending t). The candidates t differ
-// from s by +-nn in i, j or k, or lie in the zero-gradient ghost layer next to
-// s; a position that is a source without being a fixed point is a J ghost,
-// copied only with its own j.
-__device__ inline bool receives(const Box& b, int i, int j, int k) {
-    const bool zg = b.bc[2] == GAM_BC_ZEROGRAD;
-    return may_receive(i, b.Nip, b.nx, b.bc[0] == GAM_BC_PERIODIC, false, false) ||
-           may_receive(j, b.Njp, b.ny, !zg, zg, b.bc[3] == GAM_BC_ZEROGRAD) ||
-           may_receive(k, b.Nkp, b.nz, b.bc[4] == GAM_BC_PERIODIC, false, false);
-}
-
-// the positions that receive from no other (most of the box): their own value
-// where the map fixes them, else zero
-template <class R>
-__global__ void k_bc_gather_adj_bulk(Box b, int comp, int nc, const R* __restrict__ g, R* __restrict__ out) {
-    const long s = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    int i, j, k;
-    if (!pos_of(b, s, i, j, k) || receives(b, i, j, k)) return;
-    const bool fixed = bc_source(b, comp, i, j, k) == s;
-    for (int c = 0; c < nc; c++) out[c * b.n + s] = fixed ? g[c * b.n + s] : (R)0;
-}
-
-template <class R>
-__device__ void gather_adj_at(const Box& b, int comp, int nc, const R* __restrict__ g, R* __restrict__ out, long s,
-                              int i, int j, int k) {
-    const bool fixed = bc_source(b, comp, i, j, k) == s;
-    const bool zg = b.bc[2] == GAM_BC_ZEROGRAD;
-    int ci[13], cj[13], ck[13];
-    int ni = b.bc[0] == GAM_BC_PERIODIC ? axis_candidates(i, b.Nip, b.nx, false, false, ci) : (ci[0] = i, 1);
-    int nj = axis_candidates(j, b.Njp, b.ny, zg, b.bc[3] == GAM_BC_ZEROGRAD, cj);
-    int nk = b.bc[4] == GAM_BC_PERIODIC ? axis_candidates(k, b.Nkp, b.nz, false, false, ck) : (ck[0] = k, 1);
-    // keep the candidates whose own axis rule can reach i, j, k (the I and K
-    // rules act on their axis alone; J keeps j itself, which the rule may
-    // leave unmapped), so that bc_source runs on few combinations
-    auto keep = [](int* c, int n, int x, auto rule) {
-        int m = 0;
-        for (int q = 0; q < n; q++)
-            if (rule(c[q]) == x) c[m++] = c[q];
-        return m;
-    };
-    if (b.bc[0] == GAM_BC_PERIODIC)
-        ni = keep(ci, ni, i, [&](int x) {
-            return hi_rule(GAM_BC_PERIODIC, lo_rule(GAM_BC_PERIODIC, x, b.Nip), b.Nip, comp == 0);
-        });
-    if (b.bc[4] == GAM_BC_PERIODIC)
-        nk = keep(ck, nk, k, [&](int x) {
-            return hi_rule(GAM_BC_PERIODIC, lo_rule(GAM_BC_PERIODIC, x, b.Nkp), b.Nkp, comp == 2);
-        });
-    nj = keep(cj, nj, j, [&](int x) {
-        const int y = hi_rule(b.bc[3], lo_rule(b.bc[2], x, b.Njp), b.Njp, comp == 1);
-        return y == j ? j : x;
-    });
-    // the sums of every component in one pass over the matches (ascending t)
-    R acc[5] = {(R)0, (R)0, (R)0, (R)0, (R)0};
-    bool any = false;
-    for (int a = 0; a < nk; a++)
-        for (int e = 0; e < nj; e++)
-            for (int f = 0; f < ni; f++) {
-                const long t = ((long)ck[a] * b.ny + cj[e]) * b.nx + ci[f];
-                if (t == s || bc_source(b, comp, ci[f], cj[e], ck[a]) != s) continue;
-#pragma unroll
-                for (int c = 0; c < 5; c++)
-                    if (c < nc) acc[c] = any ? acc[c] + g[c * b.n + t] : g[c * b.n + t];
-                any = true;
-            }
-#pragma unroll
-    for (int c = 0; c < 5; c++)
-        if (c < nc) {
-            const R own = fixed ? g[c * b.n + s] : (R)0;
-            out[c * b.n + s] = any ? own + acc[c] : own;
-        }
-}
-
-// the planes of positions that may receive: one plane per listed value of one
-// axis (blockIdx.z = the plane; x, y over the other two axes); a position on
-// two planes is written twice with the same value
-struct Slabs {
-    int n;          // planes
-    int axis[40];   // axis of plane q
-    int value[40];  // its coordinate
+// adjoint of the four gathers of EnforceBCs (the gas, 5 components, and the
+// flux of each direction) in one launch, blockIdx.y = the field f (0 gas,
+// 1 + d flux d), from the tables of bc_adj_tables: out[s] = (g[s] where the
+// map fixes s, else 0) + the sum of g over the positions that copy s, in
+// ascending order
+struct BcAdjDev {
+    const int* code[4];
+    const int* rowStart[4];
+    const int* src[4];
 };
 template <class R>
-__global__ void k_bc_gather_adj_slabs(Box b, Slabs sl, int comp, int nc, const R* __restrict__ g,
-                                      R* __restrict__ out) {
-    const int q = blockIdx.z;
-    const int a = sl.axis[q];
-    const int u = blockIdx.x * blockDim.x + threadIdx.x, v = blockIdx.y * blockDim.y + threadIdx.y;
-    int i, j, k;
-    if (a == 0) {
-        i = sl.value[q]; j = u; k = v;
-    } else if (a == 1) {
-        i = u; j = sl.value[q]; k = v;
-    } else {
-        i = u; j = v; k = sl.value[q];
+__global__ void __launch_bounds__(256) k_bc_gather_adj_tab(Box b, BcAdjDev tab, const R* __restrict__ gG,
+                                                           R* __restrict__ oG, const R* __restrict__ gM,
+                                                           R* __restrict__ oM) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= b.n) return;
+    const int f = blockIdx.y;
+    const long n = b.n;
+    const int nc = f == 0 ? 5 : 1;
+    const R* g = f == 0 ? gG : gM + (long)(f - 1) * n;
+    R* out = f == 0 ? oG : oM + (long)(f - 1) * n;
+    const int code = tab.code[f][t];
+    const int row = (code >> 1) - 1;
+    int q0 = 0, q1 = 0;
+    if (row >= 0) {
+        q0 = tab.rowStart[f][row];
+        q1 = tab.rowStart[f][row + 1];
     }
-    if (i >= b.nx || j >= b.ny || k >= b.nz || !receives(b, i, j, k)) return;
-    gather_adj_at(b, comp, nc, g, out, ((long)k * b.ny + j) * b.nx + i, i, j, k);
+    const int* src = tab.src[f];
+    for (int c = 0; c < nc; c++) {
+        const R own = (code & 1) ? g[c * n + t] : (R)0;
+        if (q1 > q0) {
+            R acc = g[c * n + src[q0]];
+            for (int q = q0 + 1; q < q1; q++) acc = acc + g[c * n + src[q]];
+            out[c * n + t] = own + acc;
+        } else {
+            out[c * n + t] = own;
+        }
+    }
 }
 
 // gamCellBxyz on every cell of the box: B = (sum over faces of +-flux x face
@@ -255,7 +196,7 @@ unsigned blocks(long n, int blk) { return (unsigned)((n + blk - 1) / blk); }
 // Side streams of the adjoint step (created once per device, non-blocking):
 // independent stages run on them between a fork and a join by events, on
 // the caller's stream or inside a graph captured from it.
-constexpr int NSIDE = 2;
+constexpr int NSIDE = 1;
 struct SideStreams {
     cudaStream_t s[NSIDE];
     cudaEvent_t fork, join[NSIDE];
@@ -364,32 +305,46 @@ int launch_gather(const Box& b, int comp, int nc, const void* in, void* out, cud
     k_bc_gather<R><<<blocks(b.n, 256), 256, 0, s>>>(b, comp, nc, (const R*)in, (R*)out);
     return cudaGetLastError() == cudaSuccess ? GAM_OK : GAM_ECUDA;
 }
-template <class R>
-int launch_gather_adj(const Box& b, int comp, int nc, const void* g, void* out, cudaStream_t s) {
-    // the planes that may receive, per axis (the device rules, run on the host)
-    Slabs sl;
-    sl.n = 0;
-    const bool zg = b.bc[2] == GAM_BC_ZEROGRAD;
-    const int ext[3] = {b.nx, b.ny, b.nz};
-    int w = 0, h = 0;
-    for (int a = 0; a < 3; a++)
-        for (int x = 0; x < ext[a]; x++) {
-            const bool r = a == 0   ? may_receive(x, b.Nip, b.nx, b.bc[0] == GAM_BC_PERIODIC, false, false)
-                           : a == 1 ? may_receive(x, b.Njp, b.ny, !zg, zg, b.bc[3] == GAM_BC_ZEROGRAD)
-                                    : may_receive(x, b.Nkp, b.nz, b.bc[4] == GAM_BC_PERIODIC, false, false);
-            if (!r) continue;
-            if (sl.n == 40) return GAM_EBADDIM;  // the ghost rules make at most 9 planes per axis
-            sl.axis[sl.n] = a;
-            sl.value[sl.n++] = x;
-            w = std::max(w, a == 0 ? b.ny : b.nx);
-            h = std::max(h, a == 2 ? b.ny : b.nz);
+// the tables of the EnforceBCs adjoint for this configuration on the current
+// device, built and uploaded on first use (synchronous copies) and kept for
+// the life of the process
+int bc_adj_device_tables(const Box& b, BcAdjDev* out) {
+    struct Entry {
+        int dev, Nip, Njp, Nkp, bc[6];
+        BcAdjDev d;
+    };
+    static std::mutex mu;
+    static std::vector<Entry> cache;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return GAM_ECUDA;
+    std::lock_guard<std::mutex> lock(mu);
+    for (const Entry& e : cache)
+        if (e.dev == dev && e.Nip == b.Nip && e.Njp == b.Njp && e.Nkp == b.Nkp &&
+            std::equal(e.bc, e.bc + 6, b.bc)) {
+            *out = e.d;
+            return GAM_OK;
         }
-    k_bc_gather_adj_bulk<R><<<blocks(b.n, 256), 256, 0, s>>>(b, comp, nc, (const R*)g, (R*)out);
-    if (sl.n > 0) {
-        const dim3 blk(32, 4, 1), grd((unsigned)((w + 31) / 32), (unsigned)((h + 3) / 4), (unsigned)sl.n);
-        k_bc_gather_adj_slabs<R><<<grd, blk, 0, s>>>(b, sl, comp, nc, (const R*)g, (R*)out);
+    Entry e;
+    e.dev = dev; e.Nip = b.Nip; e.Njp = b.Njp; e.Nkp = b.Nkp;
+    std::copy(b.bc, b.bc + 6, e.bc);
+    for (int f = 0; f < 4; f++) {
+        std::vector<int> code, rowStart, src;
+        bc_adj_tables(b, f - 1, code, rowStart, src);
+        const std::vector<int>* v[3] = {&code, &rowStart, &src};
+        const int** dst[3] = {&e.d.code[f], &e.d.rowStart[f], &e.d.src[f]};
+        for (int q = 0; q < 3; q++) {
+            int* d = nullptr;
+            const size_t bytes = std::max<size_t>(1, v[q]->size()) * sizeof(int);
+            if (cudaMalloc((void**)&d, bytes) != cudaSuccess) return GAM_ECUDA;
+            if (!v[q]->empty() && cudaMemcpy(d, v[q]->data(), v[q]->size() * sizeof(int), cudaMemcpyHostToDevice) !=
+                                      cudaSuccess)
+                return GAM_ECUDA;
+            *dst[q] = d;
+        }
     }
-    return cudaGetLastError() == cudaSuccess ? GAM_OK : GAM_ECUDA;
+    cache.push_back(e);
+    *out = e.d;
+    return GAM_OK;
 }
 
 #define TRY(x)              \
@@ -533,20 +488,19 @@ int step_adj(const gam_params* p, int32_t fp32, const void* const* geo, const do
     if (cudaMemcpyAsync(w.p[tM], dnxt[1], 3 * b.n * es, cudaMemcpyDeviceToDevice, s) != cudaSuccess) return GAM_ECUDA;
     if (dnxt[2]) TRY(fp32 ? launch_bxyz_adj<float>(b, geo, dnxt[2], w.p[tM], s)
                           : launch_bxyz_adj<double>(b, geo, dnxt[2], w.p[tM], s));
-    // adjoint of EnforceBCs: the gas on a side stream, the fluxes here
+    // adjoint of EnforceBCs: the gas and the three flux directions in one launch
+    BcAdjDev tab;
+    TRY(bc_adj_device_tables(b, &tab));
+    const dim3 tgrid(blocks(b.n, 256), 4);
+    if (fp32)
+        k_bc_gather_adj_tab<float><<<tgrid, 256, 0, s>>>(b, tab, (const float*)dnxt[0], (float*)w.p[dnG],
+                                                        (const float*)w.p[tM], (float*)w.p[dnM]);
+    else
+        k_bc_gather_adj_tab<double><<<tgrid, 256, 0, s>>>(b, tab, (const double*)dnxt[0], (double*)w.p[dnG],
+                                                         (const double*)w.p[tM], (double*)w.p[dnM]);
+    if (cudaGetLastError() != cudaSuccess) return GAM_ECUDA;
     const SideStreams* side = side_streams();
-    cudaStream_t s0 = side ? side->s[0] : s, s1 = side ? side->s[1] : s;
-    if (side) TRY(fork(side, 1, s));
-    if (fp32) {
-        TRY(launch_gather_adj<float>(b, -1, 5, dnxt[0], w.p[dnG], s0));
-        for (int d = 0; d < 3; d++)
-            TRY(launch_gather_adj<float>(b, d, 1, (float*)w.p[tM] + d * b.n, (float*)w.p[dnM] + d * b.n, s));
-    } else {
-        TRY(launch_gather_adj<double>(b, -1, 5, dnxt[0], w.p[dnG], s0));
-        for (int d = 0; d < 3; d++)
-            TRY(launch_gather_adj<double>(b, d, 1, (double*)w.p[tM] + d * b.n, (double*)w.p[dnM] + d * b.n, s));
-    }
-    if (side) TRY(join(side, 1, s));
+    cudaStream_t s1 = side ? side->s[0] : s;
     if (iside) {
         // the I-side fills (in place on dnG, dnM; the field they read gets
         // its adjoint in aBm), then bFlux2Fld of the update's fluxes
@@ -564,9 +518,9 @@ int step_adj(const gam_params* p, int32_t fp32, const void* const* geo, const do
     TRY(gam_update_adjoint_store(p, fp32, in5, g4, bg ? bg[3] : nullptr, dt, dup, w.p[sU], w.p[sM], dsu, s));
     // the flux and E-field adjoints gather their stencil adjoints through
     // their own parts of RS in a fixed order (the same bits on every call);
-    // they read and write disjoint arrays, so the E-field adjoint runs on a
+    // they read and write disjoint arrays, so the E-field adjoint runs on the
     // side stream beside the flux adjoint and the bFlux2Fld adjoint after it
-    if (side) TRY(fork(side, 2, s));
+    if (side) TRY(fork(side, 1, s));
     const size_t rsE = (size_t)120 * b.n * es;  // the flux adjoint's 120 components come first
     TRY(gam_efield_adjoint_saved(p, fp32, w.p[Dh], w.p[abh], w.p[bn], w.p[VdV], geo[0], geo[1], geo[5], geo[6],
                                  geo[7], bg ? bg[2] : nullptr, dt, w.p[AVf], w.p[dE], w.p[dDh], w.p[dabh], w.p[dbn],
@@ -576,7 +530,7 @@ int step_adj(const gam_params* p, int32_t fp32, const void* const* geo, const do
                                 w.p[dQB], w.p[dBlim], w.p[dBnf], w.p[RS], w.p[FSV], s));
     TRY(fp32 ? launch_bxyz_adj<float>(b, geo, w.p[dBlim], dst[1], s)
              : launch_bxyz_adj<double>(b, geo, w.p[dBlim], dst[1], s));
-    if (side) TRY(join(side, 2, s));
+    if (side) TRY(join(side, 1, s));
     const void* g5[5] = {geo[0], geo[1], geo[2], geo[3], geo[4]};
     const void* din8[8] = {w.p[dQW], w.p[dWn], w.p[dDh], w.p[dVdV], w.p[dQB], w.p[dabh], w.p[dBnf], w.p[dbn]};
     return gam_predict_stage(p, fp32, st, g5, 0.5 * dt, odt, nullptr, din8, w.p[aB], dst, s);

@@ -5,9 +5,9 @@ compiled for the host with g++ (no GPU):
   (mage_b200.diffstep.Grid._bc_maps) at every box position, for cells and the
   three face directions, periodic and zero-gradient J, with periodic I and
   with the non-periodic I sides (whose fills run before the gather);
-* the candidates the gather's adjoint scans, filtered by the map, are exactly
-  the positions the map copies from each position (brute-force preimages);
-* the adjoint's skip test (may_receive) never skips a position that is copied.
+* the tables of the gather's adjoint (bc_adj_tables) list for each position
+  exactly the positions the map copies from it, in ascending order
+  (brute-force preimages), and flag the positions the map fixes.
 """
 import os
 import shutil
@@ -33,25 +33,17 @@ int main(int argc, char** argv) {
     for (int comp = -1; comp < 3; comp++)
         for (int k = 0; k < b.nz; k++) for (int j = 0; j < b.ny; j++) for (int i = 0; i < b.nx; i++)
             printf("%ld\n", bc_source(b, comp, i, j, k));
-    const bool zg = b.bc[2] == GAM_BC_ZEROGRAD;
-    for (int comp = -1; comp < 3; comp++)
-        for (int k = 0; k < b.nz; k++) for (int j = 0; j < b.ny; j++) for (int i = 0; i < b.nx; i++) {
-            const long s = ((long)k * b.ny + j) * b.nx + i;
-            int ci[13], cj[13], ck[13];
-            const bool pi = b.bc[0] == GAM_BC_PERIODIC, pk = b.bc[4] == GAM_BC_PERIODIC;
-            const int ni = pi ? axis_candidates(i, b.Nip, b.nx, false, false, ci) : (ci[0] = i, 1);
-            const int nj = axis_candidates(j, b.Njp, b.ny, zg, b.bc[3] == GAM_BC_ZEROGRAD, cj);
-            const int nk = pk ? axis_candidates(k, b.Nkp, b.nz, false, false, ck) : (ck[0] = k, 1);
-            const bool mr = may_receive(i, b.Nip, b.nx, pi, false, false) ||
-                            may_receive(j, b.Njp, b.ny, !zg, zg, b.bc[3] == GAM_BC_ZEROGRAD) ||
-                            may_receive(k, b.Nkp, b.nz, pk, false, false);
-            printf("P %d %ld %d", comp, s, (int)mr);
-            for (int a = 0; a < nk; a++) for (int e = 0; e < nj; e++) for (int f = 0; f < ni; f++) {
-                const long t = ((long)ck[a] * b.ny + cj[e]) * b.nx + ci[f];
-                if (t != s && bc_source(b, comp, ci[f], cj[e], ck[a]) == s) printf(" %ld", t);
-            }
+    for (int comp = -1; comp < 3; comp++) {
+        std::vector<int> code, rowStart, src;
+        bc_adj_tables(b, comp, code, rowStart, src);
+        for (long s = 0; s < b.n; s++) {
+            const int row = (code[s] >> 1) - 1;
+            printf("P %d %ld %d", comp, s, code[s] & 1);
+            if (row >= 0)
+                for (int q = rowStart[row]; q < rowStart[row + 1]; q++) printf(" %d", src[q]);
             printf("\n");
         }
+    }
     return 0;
 }
 """
@@ -96,9 +88,9 @@ def test_bc_map_matches_restatement(harness, N, bc):
         if not line.startswith("P"):
             continue
         f = line.split()
-        c, s, mr = int(f[1]), int(f[2]), int(f[3])
+        c, s, fixed = int(f[1]), int(f[2]), int(f[3])
         got = [int(x) for x in f[4:]]
         m = src[c + 1]
         want = idx[(m == s) & (idx != s)].tolist()
         assert got == want, (c, s, got, want)
-        assert mr or not want, (c, s)
+        assert fixed == int(m[s] == s), (c, s)
