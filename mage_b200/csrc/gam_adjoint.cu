@@ -1687,8 +1687,8 @@ int predict_call(const gam_params* p, const void* const* st, const void* const* 
     const DevParams<R> P = dev_params<R>(p);
     const Geo<R> g = geo_of<R>(geo[0], geo[1], geo[2], geo[3], geo[4], nullptr);
     StateBuf<R> cur{(R*)st[0], (R*)st[1], nullptr}, old{(R*)st[2], (R*)st[3], nullptr};
-    GamScalars* sc;
-    if (set_scalars(0.0, pdt, odt, s, &sc)) return GAM_ECUDA;
+    GamScalars* sc = nullptr;  // the forward kernels read pdt, odt from the scalars; the adjoint takes them as arguments
+    if (out && set_scalars(0.0, pdt, odt, s, &sc)) return GAM_ECUDA;
     const Range all{0, b.Ni, 0, b.Nj, 0, b.Nk}, cells{0, b.Ni - 1, 0, b.Nj - 1, 0, b.Nk - 1};
     if (out) {
         Work<R> w;
@@ -1723,8 +1723,8 @@ int update_call(const gam_params* p, const void* const* in, const void* const* g
     Work<R> w;
     memset(&w, 0, sizeof(w));
     w.E = (R*)in[2]; w.gF = (R*)in[3]; w.mF = (R*)in[4];
-    GamScalars* sc;
-    if (set_scalars(dt, 0.0, 0.0, s, &sc)) return GAM_ECUDA;
+    GamScalars* sc = nullptr;  // the forward kernels read dt from the scalars; the adjoint takes it as an argument
+    if (out && set_scalars(dt, 0.0, 0.0, s, &sc)) return GAM_ECUDA;
     const Range all{0, b.Ni, 0, b.Nj, 0, b.Nk}, cells{0, b.Ni - 1, 0, b.Nj - 1, 0, b.Nk - 1};
     const dim3 blk(32, 4, 1);
     if (out) {

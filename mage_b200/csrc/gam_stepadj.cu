@@ -484,20 +484,26 @@ int step_adj(const gam_params* p, int32_t fp32, const void* const* geo, const do
     if (cudaMemsetAsync(w.p[dQW], 0, (size_t)((char*)w.p[dE] - (char*)w.p[dQW]), s) != cudaSuccess ||
         cudaMemsetAsync(w.p[dBlim], 0, (size_t)((char*)w.p[sU] - (char*)w.p[dBlim]), s) != cudaSuccess)
         return GAM_ECUDA;
-    // adjoint of the state's field: B = bFlux2Fld(magFlux)
-    if (cudaMemcpyAsync(w.p[tM], dnxt[1], 3 * b.n * es, cudaMemcpyDeviceToDevice, s) != cudaSuccess) return GAM_ECUDA;
-    if (dnxt[2]) TRY(fp32 ? launch_bxyz_adj<float>(b, geo, dnxt[2], w.p[tM], s)
-                          : launch_bxyz_adj<double>(b, geo, dnxt[2], w.p[tM], s));
+    // adjoint of the state's field: B = bFlux2Fld(magFlux), added to a copy
+    // of the flux adjoint (read in place when there is no field adjoint)
+    const void* gMf = dnxt[1];
+    if (dnxt[2]) {
+        if (cudaMemcpyAsync(w.p[tM], dnxt[1], 3 * b.n * es, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+            return GAM_ECUDA;
+        TRY(fp32 ? launch_bxyz_adj<float>(b, geo, dnxt[2], w.p[tM], s)
+                 : launch_bxyz_adj<double>(b, geo, dnxt[2], w.p[tM], s));
+        gMf = w.p[tM];
+    }
     // adjoint of EnforceBCs: the gas and the three flux directions in one launch
     BcAdjDev tab;
     TRY(bc_adj_device_tables(b, &tab));
     const dim3 tgrid(blocks(b.n, 256), 4);
     if (fp32)
         k_bc_gather_adj_tab<float><<<tgrid, 256, 0, s>>>(b, tab, (const float*)dnxt[0], (float*)w.p[dnG],
-                                                        (const float*)w.p[tM], (float*)w.p[dnM]);
+                                                        (const float*)gMf, (float*)w.p[dnM]);
     else
         k_bc_gather_adj_tab<double><<<tgrid, 256, 0, s>>>(b, tab, (const double*)dnxt[0], (double*)w.p[dnG],
-                                                         (const double*)w.p[tM], (double*)w.p[dnM]);
+                                                         (const double*)gMf, (double*)w.p[dnM]);
     if (cudaGetLastError() != cudaSuccess) return GAM_ECUDA;
     const SideStreams* side = side_streams();
     cudaStream_t s1 = side ? side->s[0] : s;
