@@ -215,12 +215,13 @@ __device__ void gas_adj(const DevParams<R>& P, A sgn, const R* W, const R* T, co
 
 // Adjoint of the face fluxes of direction D over the range r (one face per
 // thread): recompute (SAVED: load the face states the forward stored in
-// w.fsv), then reverse. 4 (FP64) / 5 (FP32) blocks per SM: the unbounded
+// w.fsv), then reverse. 4 (FP64) / 6 (FP32) blocks per SM: the unbounded
 // recomputing kernel took 214-240 registers (2 blocks); bounded it spills
 // (local memory, L1-resident) but hides more load latency (measured on
-// 128^3: 3 -> 4 FP64 blocks took the adjoint step from 5.9 to 5.7 ms).
+// 128^3: 3 -> 4 FP64 blocks took the adjoint step from 5.9 to 5.7 ms; with
+// the saved states, 5 -> 6 FP32 blocks about 1 %).
 template <class R, int D, bool SAVED = false>
-__global__ void __launch_bounds__(128, (sizeof(R) == 8 ? 4 : 5)) k_stress_adj(GamBox b, DevParams<R> P, Geo<R> g, const R* __restrict__ Blim,
+__global__ void __launch_bounds__(128, (sizeof(R) == 8 ? 4 : 6)) k_stress_adj(GamBox b, DevParams<R> P, Geo<R> g, const R* __restrict__ Blim,
                                                     Work<R> w, Range r, const R* __restrict__ dgF,
                                                     const R* __restrict__ dmF, R* dQW, R* dWn, R* dQB, R* dBlim,
                                                     R* dBnf, R* __restrict__ rs) {

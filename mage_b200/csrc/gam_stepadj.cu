@@ -478,12 +478,13 @@ int step_adj(const gam_params* p, int32_t fp32, const void* const* geo, const do
     const size_t es = fp32 ? 4 : 8;
     if (!saved) TRY(forward_stages(p, fp32, b, w, geo, bg, st, dt, odt, s));
     if (!saved && iside) TRY(update_and_fill(p, fp32, b, w, geo, bg, st, dt, is, w.p[aBm], s));
-    // zero what the adjoint stages add into (dQW .. dAVf, dBlim); the update
-    // stage stores dE, dgF and dmF whole, sU, sM and aB are written before
-    // they are read, dnG, dnM and tM are written whole
-    if (cudaMemsetAsync(w.p[dQW], 0, (size_t)((char*)w.p[dE] - (char*)w.p[dQW]), s) != cudaSuccess ||
-        cudaMemsetAsync(w.p[dBlim], 0, (size_t)((char*)w.p[sU] - (char*)w.p[dBlim]), s) != cudaSuccess)
-        return GAM_ECUDA;
+    // zero what the adjoint stages add into: dBnf (each flux adds its face's
+    // part). The gathers store dQW, dWn, dQB, dBlim, dDh and dVdV on every
+    // cell and dabh, dbn on every position, which is all the later stages
+    // read of them; dAVf is not used with the gathers; the update stage stores
+    // dE, dgF and dmF whole, sU, sM and aB are written before they are read,
+    // dnG and dnM are written whole
+    if (cudaMemsetAsync(w.p[dBnf], 0, 3 * b.n * es, s) != cudaSuccess) return GAM_ECUDA;
     // adjoint of the state's field: B = bFlux2Fld(magFlux), added to a copy
     // of the flux adjoint (read in place when there is no field adjoint)
     const void* gMf = dnxt[1];
