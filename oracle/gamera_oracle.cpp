@@ -3140,6 +3140,16 @@ double orc_divb(void* h) {
     return tot;
 }
 
+// RingAverage alone on the current state (ringav.F90:26-75), the call that
+// tests/voltron/testring.pf (ringAvgConservationTest) makes; 1 if the grid
+// has no rings
+int orc_ring_average(void* h) {
+    App* A = (App*)h;
+    if (!A->G.ring.on) return 1;
+    RingAverage(A->M, A->G, A->S, A->SmoothE);
+    return 0;
+}
+
 // Known-answer hooks for tests/gamera/testgamutils.pf
 void orc_c2p(double gamma, const double* con, double* prim) {
     Model M; M.gamma = gamma;

@@ -151,6 +151,8 @@ def lib(variant: str = "strict") -> C.CDLL:
         L.orc_set_scalars.argtypes = [C.c_void_p, C.POINTER(_Scalars)]
         L.orc_divb.argtypes = [C.c_void_p]
         L.orc_divb.restype = C.c_double
+        L.orc_ring_average.argtypes = [C.c_void_p]
+        L.orc_ring_average.restype = C.c_int
         for f in ("orc_c2p", "orc_p2c"):
             getattr(L, f).argtypes = [C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_double)]
         for f in ("orc_erfc", "orc_exp"):
@@ -254,6 +256,10 @@ class Oracle:
 
     def divb(self) -> float:
         return self.L.orc_divb(self.h)
+
+    def ring_average(self) -> int:
+        """RingAverage alone on the current state (ringav.F90:26-75)."""
+        return self.L.orc_ring_average(self.h)
 
 
 def c2p(con, gamma=5.0 / 3.0, variant="strict"):

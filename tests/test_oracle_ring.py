@@ -82,3 +82,38 @@ def test_axisymmetric_blast_stays_axisymmetric(oracle_built):
     # the density; the momentum rotates with k, and the energy picks up the
     # limiters' response to Cartesian components
     assert spread[0] <= 1e-14 * scale[0], spread / scale
+
+
+@pytest.mark.parametrize("nch", [(8,), (2, 4, 8)], ids=["1ring", "3rings"])
+def test_ring_average_conserves_ring_sums_as_reference_test(oracle_built, nch):
+    """The reference's own check of RingAverage (tests/voltron/testring.pf,
+    ringAvgConservationTest), restated on this grid: the ring rows next to
+    both poles get density 1 (k < ke/2) or 2, momenta sin(n k pi) times the
+    density (n = 1, 2, 3) and fluxes sin(n k pi) (n = 4, 5, 6); one RingAverage
+    alone keeps the density and momentum sum of every ring to 1e-15 and the
+    total div B to 2e-13, the reference's tolerances."""
+    o = _oracle(y0=1.0, nch=nch)
+    assert o.step(1) == 0
+    G, Njp, Nkp = 4, N[1], N[2]
+    Gas, mf = o.array("Gas"), o.array("magFlux")
+    NumR = len(nch)  # one ring per chunk count
+    ks, ke = 1, Nkp
+    rows = [G + r - 1 for r in range(1, NumR + 1)] + [G + Njp - r for r in range(1, NumR + 1)]
+    for kf in range(ks, ke + 1):
+        kk = kf - 1 + G
+        den = 1.0 if kf < ke // 2 else 2.0
+        for jj in rows:
+            Gas[0, kk, jj, G:G + N[0]] = den
+            for n in range(3):
+                Gas[1 + n, kk, jj, G:G + N[0]] = np.sin((n + 1) * kf * np.pi) * den
+            for d in range(3):
+                mf[d, kk, jj, G:G + N[0]] = np.sin((4 + d) * kf * np.pi)
+    before = {jj: Gas[0:4, G:G + Nkp, jj, G:G + N[0]].sum(axis=1) for jj in rows}
+    den0 = Gas[0, G:G + Nkp, rows[0], G:G + N[0]].copy()
+    div0 = o.divb()
+    assert o.ring_average() == 0
+    assert np.abs(Gas[0, G:G + Nkp, rows[0], G:G + N[0]] - den0).max() > 0.1  # the average acted
+    for jj in rows:
+        after = Gas[0:4, G:G + Nkp, jj, G:G + N[0]].sum(axis=1)
+        assert np.abs(after - before[jj]).max() <= 1e-15, (jj, np.abs(after - before[jj]).max())
+    assert abs(o.divb() - div0) <= 2e-13, (o.divb(), div0)
