@@ -117,3 +117,35 @@ def test_ring_average_conserves_ring_sums_as_reference_test(oracle_built, nch):
         after = Gas[0:4, G:G + Nkp, jj, G:G + N[0]].sum(axis=1)
         assert np.abs(after - before[jj]).max() <= 1e-15, (jj, np.abs(after - before[jj]).max())
     assert abs(o.divb() - div0) <= 2e-13, (o.divb(), div0)
+
+
+def test_metric_periodic_in_k_as_reference_test(oracle_built):
+    """The reference's metric check on its LFM grid (tests/gamera/testfields.pf,
+    testFaceMetricFields / testEdgeMetricFields), restated: with corners
+    periodic in k (the k = ke+1.. layers copies of ks..), the K-face triads and
+    areas at ks equal those at ke+1, and the I- and J-edge triads, edge maps
+    and lengths at ks equal those at ke+1, exactly (the reference asserts a
+    difference <= 0)."""
+    G, Nip, Njp, Nkp = 4, N[0], N[1], N[2]
+    xyz = grids.lfm_corners(*N, th0=0.01)
+    # corner layer kk = G + Nkp + m repeats kk = G + m (and the lower ghosts the upper actives)
+    for m in range(0, G + 1):
+        xyz[:, G + Nkp + m] = xyz[:, G + m]
+    for m in range(1, G + 1):
+        xyz[:, G - m] = xyz[:, G + Nkp - m]
+    o = Oracle(OracleParams(*N, bc=BCS, ringNch=(8,)), xyz, "strict")
+    Tf, face, Te, Teb, edge = (o.array(n) for n in ("Tf", "face", "Te", "Teb", "edge"))
+    a, b = G, G + Nkp  # ks and ke+1
+    iA, jA = slice(G, G + Nip), slice(G, G + Njp)
+    # K faces (d = 2) of the active cells
+    assert np.array_equal(Tf[18:27, a, jA, iA], Tf[18:27, b, jA, iA])
+    assert np.array_equal(face[2, a, jA, iA], face[2, b, jA, iA])
+    # I edges (d = 0): i in is..ie, j in js..je+1; J edges (d = 1): i in is..ie+1, j in js..je
+    iE, jE = slice(G, G + Nip), slice(G, G + Njp + 1)
+    assert np.array_equal(Te[0:9, a, jE, iE], Te[0:9, b, jE, iE])
+    assert np.array_equal(Teb[0:4, a, jE, iE], Teb[0:4, b, jE, iE])
+    assert np.array_equal(edge[0, a, jE, iE], edge[0, b, jE, iE])
+    iE, jE = slice(G, G + Nip + 1), slice(G, G + Njp)
+    assert np.array_equal(Te[9:18, a, jE, iE], Te[9:18, b, jE, iE])
+    assert np.array_equal(Teb[4:8, a, jE, iE], Teb[4:8, b, jE, iE])
+    assert np.array_equal(edge[1, a, jE, iE], edge[1, b, jE, iE])
