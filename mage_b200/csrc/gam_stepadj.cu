@@ -28,6 +28,7 @@
 
 #include "../../include/gamgpu.h"
 #include "gam_bcmap.cuh"
+#include "gam_ctx.cuh"
 #include "gam_quot.cuh"
 
 // stage adjoints for a whole step (gam_adjoint.cu)
@@ -206,12 +207,17 @@ SideStreams* side_streams() {
     static std::mutex mu;
     static SideStreams per[64];
     static bool made[64];
+    static unsigned long long ctx[64];
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
     std::lock_guard<std::mutex> lock(mu);
     SideStreams& t = per[dev];
-    if (!made[dev]) {
+    // made again in a new context of the device (after cudaDeviceReset); the
+    // old handles died with their context
+    const unsigned long long id = gam_current_ctx_id();
+    if (!made[dev] || id != ctx[dev]) {
         made[dev] = true;
+        ctx[dev] = id;
         t.ok = cudaEventCreateWithFlags(&t.fork, cudaEventDisableTiming) == cudaSuccess;
         for (int i = 0; i < NSIDE && t.ok; i++)
             t.ok = cudaStreamCreateWithFlags(&t.s[i], cudaStreamNonBlocking) == cudaSuccess &&
@@ -306,11 +312,12 @@ int launch_gather(const Box& b, int comp, int nc, const void* in, void* out, cud
     return cudaGetLastError() == cudaSuccess ? GAM_OK : GAM_ECUDA;
 }
 // the tables of the EnforceBCs adjoint for this configuration on the current
-// device, built and uploaded on first use (synchronous copies) and kept for
-// the life of the process
+// device and context, built and uploaded on first use (synchronous copies)
+// and kept for the life of the process
 int bc_adj_device_tables(const Box& b, BcAdjDev* out) {
     struct Entry {
         int dev, Nip, Njp, Nkp, bc[6];
+        unsigned long long ctx;  // uploaded again in a new context of the device (after cudaDeviceReset)
         BcAdjDev d;
     };
     static std::mutex mu;
@@ -318,14 +325,15 @@ int bc_adj_device_tables(const Box& b, BcAdjDev* out) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return GAM_ECUDA;
     std::lock_guard<std::mutex> lock(mu);
+    const unsigned long long ctx = gam_current_ctx_id();
     for (const Entry& e : cache)
-        if (e.dev == dev && e.Nip == b.Nip && e.Njp == b.Njp && e.Nkp == b.Nkp &&
+        if (e.dev == dev && e.ctx == ctx && e.Nip == b.Nip && e.Njp == b.Njp && e.Nkp == b.Nkp &&
             std::equal(e.bc, e.bc + 6, b.bc)) {
             *out = e.d;
             return GAM_OK;
         }
     Entry e;
-    e.dev = dev; e.Nip = b.Nip; e.Njp = b.Njp; e.Nkp = b.Nkp;
+    e.dev = dev; e.ctx = ctx; e.Nip = b.Nip; e.Njp = b.Njp; e.Nkp = b.Nkp;
     std::copy(b.bc, b.bc + 6, e.bc);
     for (int f = 0; f < 4; f++) {
         std::vector<int> code, rowStart, src;
